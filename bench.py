@@ -1,0 +1,309 @@
+#!/usr/bin/env python
+"""Benchmark of the PD hot path: inverse-stiffness beam, forward + adjoint.
+
+Workload (one bench step = one gradient evaluation of the inverse-stiffness
+problem): 40x8x8 cubes of 0.05 m, 5 tets each (3,321 vertices, 12,800 tets),
+per-tet E log-uniform in [1e4, 1e6] Pa (seed 1234), both ends pinned, gravity,
+h = 1/100 s, 20 local-global iterations, 60 time steps.  A step refactors H
+for the current moduli, runs the 60 steps forward, and the adjoint of all 60
+steps back to dL/dE for L = |x_60 - x_60^target|^2 (target from the seed-5678
+modulus field).  The metric is simulated time steps per second of
+forward + adjoint (60 per bench step), summed over GPUs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference ...   # CPU reference arm (FP64 oracle port)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIM_STEPS = 60
+METRIC = "fwd+adjoint sim steps/s (inverse stiffness 12,800 tets, K=20)"
+UNIT = "steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    return p.parse_args()
+
+
+def workload_config(precision: str) -> dict:
+    return {
+        "workload": "inverse_stiffness beam 40x8x8 cubes x5 tets (12,800 tets, 3,321 vertices), "
+                    "E~logU[1e4,1e6] seed 1234, both ends pinned, h=1/100, K=20, 60 steps, fwd+adjoint dL/dE",
+        "tets": 12800, "vertices": 3321, "sim_steps_per_bench_step": SIM_STEPS, "pd_iterations": 20,
+        "precision": precision, "parallelism": "replicas (one independent scene per GPU)",
+    }
+
+
+# ----------------------------------------------------------------- clocks ---
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------ CPU oracle ---
+
+def oracle_sample(threads: int, sim_steps: int = 2) -> dict:
+    """Time the FP64 oracle port on a bounded sample of the same workload:
+    `sim_steps` steps forward + adjoint of the inverse-stiffness beam."""
+    from diff_fem_b200 import scene as S
+    from oracle import oracle as O
+    d = S.inverse_stiffness()
+    o = O.OracleScene(d)
+    x = d.x0.reshape(-1).copy()
+    v = np.zeros_like(x)
+    t0 = time.perf_counter()
+    o.set_materials(d.youngs, d.poisson)
+    r = o.forward(x, v, n_steps=sim_steps, threads=threads)
+    o.backward(2 * (r["x"] - x), np.zeros_like(x))
+    dt = time.perf_counter() - t0
+    return {"value": sim_steps / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sim_steps} of the 60 time steps, forward + adjoint incl. refactorisation, "
+                      f"FP64 C++ oracle ({threads} host thread{'s' if threads > 1 else ''})",
+            "seconds": dt}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    oracle_sample(threads, 1)  # warm-up (also builds the library if needed)
+    vals = []
+    for _ in range(max(1, args.warmup)):
+        oracle_sample(threads, 1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(oracle_sample(threads, 2)["seconds"])
+    total = sum(vals)
+    value = 2 * args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config("fp64"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": "each bench step = 2 of the 60 time steps forward + adjoint incl. "
+                                       "refactorisation, FP64 C++ oracle, local step on all host threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------------- GPU ---
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from diff_fem_b200 import scene as S
+    from diff_fem_b200._capi import DFEM_PREC_FP64, DFEM_PREC_MIXED
+    from diff_fem_b200.engine import Scene
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    prec = DFEM_PREC_FP64 if args.precision == "fp64" else DFEM_PREC_MIXED
+    d = S.inverse_stiffness(precision=prec)
+    sc = Scene(d, device=local)
+    info = sc.info()
+    N, T = d.n_vertices, d.n_tets
+    E0 = torch.tensor(d.youngs, device=dev)
+    nu = torch.tensor(d.poisson, device=dev)
+    Et = torch.tensor(S.log_uniform_moduli(T, 5678), device=dev)
+    x0 = torch.tensor(d.x0.reshape(-1), device=dev)
+    v0 = torch.zeros_like(x0)
+    sc.set_materials(Et, nu)
+    target, _ = sc.forward(x0, v0, n_steps=SIM_STEPS)
+    target = target.clone()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2 (126 MB)
+
+    def grad_eval(E):
+        sc.set_materials(E, nu)
+        x, v = sc.forward(x0, v0, n_steps=SIM_STEPS)
+        gx = 2.0 * (x - target)
+        g = sc.backward(gx, torch.zeros_like(gx))
+        return g["E"]
+
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(max(3, args.warmup)):
+        grad_eval(E0)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches0 = sc.launch_count()
+    elapsed = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            grad_eval(E0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            elapsed += e0.elapsed_time(e1) / 1e3
+    launches = sc.launch_count() - launches0
+    if world > 1:
+        dist.barrier()
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = world * SIM_STEPS * args.steps / elapsed
+
+    # forward-only rate (same scene, device-resident)
+    torch.cuda.synchronize()
+    ef0, ef1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ef0.record(stream)
+    for _ in range(args.steps):
+        sc.forward(x0, v0, n_steps=SIM_STEPS)
+    ef1.record(stream)
+    torch.cuda.synchronize()
+    fwd_rate = SIM_STEPS * args.steps / (ef0.elapsed_time(ef1) / 1e3)
+    iters = sc.iterations(SIM_STEPS)
+
+    # end to end through the public API with host buffers (pinned), copies inside the timed region
+    E_h = torch.tensor(d.youngs).pin_memory()
+    nu_h = torch.tensor(d.poisson).pin_memory()
+    x0_h = torch.tensor(d.x0.reshape(-1)).pin_memory()
+    v0_h = torch.zeros(3 * N, dtype=torch.float64).pin_memory()
+    tgt_h = target.cpu()
+    t_e2e = 0.0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sc.set_materials(E_h, nu_h)
+        xh, vh = sc.forward(x0_h, v0_h, n_steps=SIM_STEPS)
+        gxh = 2.0 * (torch.from_numpy(xh) - tgt_h)
+        gh = sc.backward(gxh.numpy(), np.zeros(3 * N))
+        _ = float(np.sum(gh["E"]))
+        t_e2e += time.perf_counter() - t0
+    e2e = {"value": world * SIM_STEPS * args.steps / t_e2e if world == 1 else None, "unit": UNIT,
+           "h2d_bytes_per_step": 8 * (2 * T + 3 * N * 4), "d2h_bytes_per_step": 8 * (3 * N * 4 + 2 * T)}
+    if world > 1:
+        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e["value"] = world * SIM_STEPS * args.steps / float(t.item())
+
+    # roofline of the dominant kernel phase (CUDA events on the engine's stream)
+    sc.forward(x0, v0, n_steps=1)
+    ph = sc.profile_phases(reps=50)
+    n_it = int(iters.sum())
+    share = {"local": 2 * n_it * ph["local"], "solve": 3 * n_it * ph["solve"], "adj_local": n_it * ph["adj_local"],
+             "gather": 3 * n_it * ph["gather"]}
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_note = "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
+    nnz = int(info["nnz_factor"])
+    solve_bytes = 2 * nnz * 12 + 96 * N                      # 2 sweeps x (value + index) + in/out vectors
+    local_bytes = T * (16 + 72 + 16) + N * 72                 # tet tables + x, b, rhs per vertex
+    dom = max(share, key=share.get)
+    if dom == "solve":
+        achieved = solve_bytes / (ph["solve"] * 1e-3) / 1e9
+        traffic_note = "per solve (both sweeps)"
+    else:
+        achieved = local_bytes / (ph[dom] * 1e-3) / 1e9
+        traffic_note = f"per {dom} launch"
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_source": peak_note,
+                "algorithmic_bytes": solve_bytes if dom == "solve" else local_bytes, "per": traffic_note,
+                "phase_ms": ph, "phase_share_ms_per_bench_step": share}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": dict(workload_config(args.precision), l2="flushed between timed steps (256 MB write)",
+                           factor={"supernodes": info["n_supernodes"], "levels": info["n_levels"], "nnz": nnz}),
+            "forward_only_steps_per_s": world * fwd_rate, "pd_iterations_total": n_it,
+            "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0 and world == 1:
+        try:
+            line["cpu_baseline"] = oracle_sample(1, 2)
+        except Exception as ex:  # the baseline must not kill the GPU line
+            line["cpu_baseline"] = {"value": None, "error": str(ex)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sc.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

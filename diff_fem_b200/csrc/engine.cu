@@ -1,0 +1,581 @@
+// engine.cu — host driver of the PD engine and the C ABI of include/dfem.h.
+//
+// A scene owns one CUDA stream, its device arrays, and two CUDA graphs built
+// on first use: the forward time step and the adjoint of one time step.  The
+// step index lives in device memory, so one graph serves every step.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/dfem.h"
+#include "pd_kernels.cu"
+#include "scene.h"
+
+namespace dfem {
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(DFEM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
+  } while (0)
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  ~DBuf() { if (p) cudaFree(p); }
+  cudaError_t alloc(size_t count) {
+    if (p) { cudaFree(p); p = nullptr; }
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc(&p, count * sizeof(T));
+  }
+  cudaError_t upload(const std::vector<T>& h) {
+    cudaError_t e = alloc(h.size());
+    if (e != cudaSuccess || h.empty()) return e;
+    return cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+  }
+};
+
+}  // namespace dfem
+
+using namespace dfem;
+
+struct dfem_scene {
+  HostScene hs;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // constraint tables
+  DBuf<double> mass, gmask, tinv, twr, twv, tvol, tE, tnu, minv, mw, mfib, srest, ssw, bbeta, bw, brest, attach_jd;
+  DBuf<int4> tv, tslot, mv, mslot;
+  DBuf<int2> sv, sslot;
+  DBuf<int> mseg, seg_ptr, seg_mus, boff, bv, bslot, vslot_ptr, hs_ptr, hs_col, to_user, to_internal;
+  DBuf<double> hs_val;
+  // factor
+  DBuf<int> lrow_ptr, lrow_col, sn_c0, sn_w, sn_r, sn_rofs, rowidx, sn_lofs, sn_dofs, lvl_sn;
+  DBuf<double> lrow_val, Lcm, Dinv;
+  std::vector<int> lvl_ptr;
+  int max_w = 1;
+  // state
+  DBuf<double> xt, vt, qn, c0, xk, rhs, y, slot, hist, io_a, io_b;
+  DBuf<double> partial, errv;
+  DBuf<unsigned> counter;
+  DBuf<int> flag, iters, step, status, write_traj;
+  DBuf<double> act_all, act_cur;   // per-step activations; current activations
+  DBuf<double> ckpt_x, ckpt_v, traj;
+  int cap_steps = 0;
+  // adjoint
+  DBuf<double> xkb, xtb, bb, gE, gnu, mg, gact;
+  // graphs
+  cudaGraphExec_t g_step = nullptr, g_adj = nullptr;
+  size_t step_nodes = 0, adj_nodes = 0;   // kernel nodes per graph
+  int64_t launches = 0;                   // kernels launched by this scene (graph nodes included)
+  int rec_steps = 0;
+  int nblk_v = 1;   // blocks of the vertex-parallel kernels
+  SceneDev sd{};
+  FactorDev fd{};
+  ~dfem_scene() {
+    if (g_step) cudaGraphExecDestroy(g_step);
+    if (g_adj) cudaGraphExecDestroy(g_adj);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace dfem {
+
+static int upload_factor(dfem_scene* sc) {
+  const SupernodalFactor& F = sc->hs.F;
+  if (F.lrow_ptr.back() > INT32_MAX || F.sn_lofs.back() > INT32_MAX || F.sn_dofs.back() > INT32_MAX)
+    return fail(DFEM_ERR_INVALID, "factor too large for 32-bit offsets");
+  auto to32 = [](const std::vector<int64_t>& v) { return std::vector<int>(v.begin(), v.end()); };
+  CK(sc->lrow_ptr.upload(to32(F.lrow_ptr)));
+  CK(sc->lrow_col.upload(F.lrow_col));
+  CK(sc->lrow_val.upload(F.lrow_val));
+  CK(sc->sn_c0.upload(F.sn_c0));
+  CK(sc->sn_w.upload(F.sn_w));
+  CK(sc->sn_r.upload(F.sn_r));
+  CK(sc->sn_rofs.upload(to32(F.sn_rofs)));
+  CK(sc->rowidx.upload(F.rowidx));
+  CK(sc->sn_lofs.upload(to32(F.sn_lofs)));
+  CK(sc->Lcm.upload(F.Lcm));
+  CK(sc->sn_dofs.upload(to32(F.sn_dofs)));
+  CK(sc->Dinv.upload(F.Dinv));
+  CK(sc->lvl_sn.upload(F.lvl_sn));
+  sc->lvl_ptr = F.lvl_ptr;
+  sc->max_w = 1;
+  for (int w : F.sn_w) sc->max_w = std::max(sc->max_w, w);
+  sc->fd = FactorDev{sc->lrow_ptr.p, sc->lrow_col.p, sc->lrow_val.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p,
+                     sc->sn_rofs.p, sc->rowidx.p, sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->lvl_sn.p};
+  return DFEM_OK;
+}
+
+static int upload_materials(dfem_scene* sc) {
+  HostScene& s = sc->hs;
+  std::vector<double> wr(s.T), wv(s.T);
+  for (int e = 0; e < s.T; ++e) {
+    double mu = s.tE[e] / (1.0 + s.tnu[e]);  // CorotateFEMConstraint: mMu = E/(1+nu)
+    wr[e] = mu * s.tvol[e];
+    wv[e] = wr[e] * s.tnu[e];                // second block scaled by nu (EvaluateJMatrix)
+  }
+  CK(sc->twr.upload(wr));
+  CK(sc->twv.upload(wv));
+  CK(sc->tE.upload(s.tE));
+  CK(sc->tnu.upload(s.tnu));
+  std::vector<int> hp(s.Hs.ptr.begin(), s.Hs.ptr.end());
+  CK(sc->hs_ptr.upload(hp));
+  CK(sc->hs_col.upload(s.Hs.col));
+  CK(sc->hs_val.upload(s.Hs.val));
+  return upload_factor(sc);
+}
+
+template <typename T>
+static std::vector<T> planes(const std::vector<T>& aos, int n, int k) {  // AoS (k per item) -> k planes
+  std::vector<T> out((size_t)n * k);
+  for (int e = 0; e < n; ++e)
+    for (int q = 0; q < k; ++q) out[(size_t)q * n + e] = aos[(size_t)e * k + q];
+  return out;
+}
+
+static int upload_scene(dfem_scene* sc) {
+  HostScene& s = sc->hs;
+  CK(sc->mass.upload(s.mass));
+  CK(sc->gmask.upload(s.gmask));
+  CK(sc->tinv.upload(planes(s.tinv, s.T, 9)));
+  CK(sc->tvol.upload(s.tvol));
+  std::vector<int4> tv(s.T), tsl(s.T);
+  for (int e = 0; e < s.T; ++e) {
+    tv[e] = make_int4(s.tv[4 * e], s.tv[4 * e + 1], s.tv[4 * e + 2], s.tv[4 * e + 3]);
+    tsl[e] = make_int4(s.tslot[4 * e], s.tslot[4 * e + 1], s.tslot[4 * e + 2], s.tslot[4 * e + 3]);
+  }
+  CK(sc->tv.upload(tv));
+  CK(sc->tslot.upload(tsl));
+  std::vector<int4> mv(s.M), msl(s.M);
+  std::vector<double> mw(s.M);
+  for (int m = 0; m < s.M; ++m) {
+    mv[m] = make_int4(s.mv[4 * m], s.mv[4 * m + 1], s.mv[4 * m + 2], s.mv[4 * m + 3]);
+    msl[m] = make_int4(s.mslot[4 * m], s.mslot[4 * m + 1], s.mslot[4 * m + 2], s.mslot[4 * m + 3]);
+    mw[m] = s.mvol[m] * s.mk[m];
+  }
+  CK(sc->mv.upload(mv));
+  CK(sc->mslot.upload(msl));
+  CK(sc->mw.upload(mw));
+  CK(sc->minv.upload(planes(s.minv, s.M, 9)));
+  CK(sc->mfib.upload(planes(s.mfib, s.M, 3)));
+  CK(sc->mseg.upload(s.mseg));
+  CK(sc->seg_ptr.upload(s.seg_ptr));
+  CK(sc->seg_mus.upload(s.seg_mus));
+  std::vector<int2> sv(s.S), ssl(s.S);
+  for (int k = 0; k < s.S; ++k) {
+    sv[k] = make_int2(s.sv[2 * k], s.sv[2 * k + 1]);
+    ssl[k] = make_int2(s.sslot[2 * k], s.sslot[2 * k + 1]);
+  }
+  CK(sc->sv.upload(sv));
+  CK(sc->sslot.upload(ssl));
+  CK(sc->srest.upload(s.srest));
+  CK(sc->ssw.upload(s.ssw));
+  CK(sc->boff.upload(s.boff));
+  CK(sc->bv.upload(s.bv));
+  CK(sc->bslot.upload(s.bslot));
+  CK(sc->bbeta.upload(s.bbeta));
+  CK(sc->bw.upload(s.bw));
+  CK(sc->brest.upload(s.brest));
+  CK(sc->vslot_ptr.upload(s.vslot_ptr));
+  std::vector<double> ajd(3 * (size_t)s.N, 0.0);  // AttachmentConstraint: J d = k p
+  for (int a = 0; a < s.A; ++a)
+    for (int c = 0; c < 3; ++c) ajd[3 * (size_t)s.av[a] + c] += s.ak[a] * s.ap[3 * a + c];
+  CK(sc->attach_jd.upload(ajd));
+  CK(sc->to_user.upload(s.to_user));
+  CK(sc->to_internal.upload(s.to_internal));
+  int rc = upload_materials(sc);
+  if (rc) return rc;
+  const size_t n3 = 3 * (size_t)s.N;
+  CK(sc->xt.alloc(n3)); CK(sc->vt.alloc(n3)); CK(sc->qn.alloc(n3)); CK(sc->c0.alloc(n3));
+  CK(sc->xk.alloc(n3)); CK(sc->rhs.alloc(n3)); CK(sc->y.alloc(n3)); CK(sc->io_a.alloc(n3)); CK(sc->io_b.alloc(n3));
+  CK(sc->slot.alloc(3 * (size_t)std::max(1, s.nslots)));
+  CK(sc->hist.alloc(n3 * (size_t)(s.K + 1)));
+  CK(sc->xkb.alloc(n3)); CK(sc->xtb.alloc(n3)); CK(sc->bb.alloc(n3));
+  CK(sc->gE.alloc(std::max(1, s.T))); CK(sc->gnu.alloc(std::max(1, s.T))); CK(sc->mg.alloc(std::max(1, s.M)));
+  sc->nblk_v = (s.N + 127) / 128;
+  CK(sc->partial.alloc(std::max(sc->nblk_v, 1)));
+  CK(sc->errv.alloc(1));
+  CK(sc->counter.alloc(1));
+  CK(sc->flag.alloc(1)); CK(sc->step.alloc(1)); CK(sc->status.alloc(1)); CK(sc->write_traj.alloc(1));
+  CK(cudaMemset(sc->counter.p, 0, sizeof(unsigned)));
+  CK(cudaMemset(sc->status.p, 0, sizeof(int)));
+  CK(sc->act_cur.alloc(std::max(1, s.nseg)));
+  CK(cudaMemset(sc->act_cur.p, 0, sizeof(double) * std::max(1, s.nseg)));
+  sc->sd = SceneDev{s.N, s.T, s.M, s.S, s.B, s.nseg, s.h, s.damping, s.g[0], s.g[1], s.g[2],
+                    sc->mass.p, sc->gmask.p, sc->tv.p, sc->tinv.p, sc->twr.p, sc->twv.p, sc->tvol.p, sc->tE.p, sc->tnu.p,
+                    sc->tslot.p, sc->mv.p, sc->minv.p, sc->mw.p, sc->mfib.p, sc->mseg.p, sc->mslot.p, sc->seg_ptr.p,
+                    sc->seg_mus.p, sc->sv.p, sc->srest.p, sc->ssw.p, sc->sslot.p, sc->boff.p, sc->bv.p, sc->bbeta.p,
+                    sc->bw.p, sc->brest.p, sc->bslot.p, sc->vslot_ptr.p, sc->attach_jd.p, sc->hs_ptr.p, sc->hs_col.p,
+                    sc->hs_val.p};
+  return DFEM_OK;
+}
+
+static int ensure_steps(dfem_scene* sc, int n_steps) {
+  if (n_steps <= sc->cap_steps) return DFEM_OK;
+  const HostScene& s = sc->hs;
+  int cap = std::max(n_steps, 2 * sc->cap_steps);
+  const size_t n3 = 3 * (size_t)s.N;
+  CK(sc->ckpt_x.alloc(n3 * cap));
+  CK(sc->ckpt_v.alloc(n3 * cap));
+  CK(sc->traj.alloc(n3 * cap));
+  CK(sc->iters.alloc(cap));
+  CK(sc->act_all.alloc((size_t)cap * std::max(1, s.nseg)));
+  CK(sc->gact.alloc((size_t)cap * std::max(1, s.nseg)));
+  sc->cap_steps = cap;
+  // graphs hold the old pointers
+  if (sc->g_step) { cudaGraphExecDestroy(sc->g_step); sc->g_step = nullptr; }
+  if (sc->g_adj) { cudaGraphExecDestroy(sc->g_adj); sc->g_adj = nullptr; }
+  return DFEM_OK;
+}
+
+// one forward step: enqueue the kernel sequence on the stream (captured into a graph)
+static void enqueue_solve(dfem_scene* sc, Gate gate, const double* rhs, double* y) {
+  const int L = (int)sc->lvl_ptr.size() - 1;
+  size_t shm = 3 * sizeof(double) * (size_t)sc->max_w;
+  for (int l = 0; l < L; ++l) {
+    int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
+    k_fwd_level<<<nb, 128, shm, sc->stream>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
+  }
+  for (int l = L - 1; l >= 0; --l) {
+    int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
+    k_bwd_level<<<nb, 128, shm, sc->stream>>>(sc->fd, sc->lvl_ptr[l], gate, y);
+  }
+}
+
+static void enqueue_step(dfem_scene* sc) {
+  const HostScene& s = sc->hs;
+  const int nb = sc->nblk_v;
+  k_step_begin<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
+                                          sc->hist.p, sc->ckpt_x.p, sc->ckpt_v.p, sc->flag.p, sc->iters.p,
+                                          sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
+  Gate gate{sc->flag.p, nullptr, nullptr, 0};
+  const int ncons = s.T + s.M + s.S + s.B;
+  for (int k = 0; k < s.K; ++k) {
+    if (ncons > 0)
+      k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, gate, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p);
+    k_gather<<<nb, 128, 0, sc->stream>>>(s.N, gate, sc->vslot_ptr.p, sc->slot.p, sc->c0.p, sc->rhs.p);
+    enqueue_solve(sc, gate, sc->rhs.p, sc->y.p);
+    k_update<<<nb, 128, 0, sc->stream>>>(s.N, gate, k, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->step.p, sc->flag.p,
+                                         sc->iters.p, sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
+  }
+  k_step_end<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->xk.p, sc->traj.p, sc->to_user.p,
+                                        sc->write_traj.p);
+  k_next_step<<<1, 1, 0, sc->stream>>>(sc->step.p);
+}
+
+static void enqueue_adjoint(dfem_scene* sc) {
+  const HostScene& s = sc->hs;
+  const int nb = sc->nblk_v;
+  // gradient w.r.t. the step's output lives in io_a (x) / io_b (v); overwritten with the input's
+  k_adj_begin<<<nb, 128, 0, sc->stream>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, sc->xkb.p, sc->xtb.p, sc->bb.p);
+  const int ncons = s.T + s.M + s.S + s.B;
+  const int nthr = std::max(ncons, s.N);
+  for (int k = s.K - 1; k >= 0; --k) {
+    Gate gate{nullptr, sc->iters.p, sc->step.p, k};
+    enqueue_solve(sc, gate, sc->xkb.p, sc->y.p);
+    k_adj_local<<<(nthr + 127) / 128, 128, 0, sc->stream>>>(sc->sd, gate, k, sc->hist.p, sc->y.p, sc->bb.p, sc->act_all.p,
+                                                            sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+    k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, gate, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
+    if (s.nseg > 0)
+      k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, gate, sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p,
+                                                                 sc->gact.p);
+  }
+  k_adj_end<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->xkb.p, sc->xtb.p, sc->bb.p, sc->io_a.p, sc->io_b.p);
+}
+
+static int build_graph(dfem_scene* sc, void (*fn)(dfem_scene*), cudaGraphExec_t* out, size_t* nodes) {
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(sc->stream, cudaStreamCaptureModeThreadLocal));
+  fn(sc);
+  cudaError_t e = cudaStreamEndCapture(sc->stream, &g);
+  if (e != cudaSuccess) return fail(DFEM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphGetNodes(g, nullptr, nodes);
+  if (e != cudaSuccess) { cudaGraphDestroy(g); return fail(DFEM_ERR_CUDA, cudaGetErrorString(e)); }
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(DFEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return DFEM_OK;
+}
+
+static int copy_in(dfem_scene* sc, const double* src, size_t n, double* dst, int mem) {
+  CK(cudaMemcpyAsync(dst, src, n * sizeof(double), mem == DFEM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     sc->stream));
+  return DFEM_OK;
+}
+static int copy_out(dfem_scene* sc, const double* src, size_t n, double* dst, int mem) {
+  CK(cudaMemcpyAsync(dst, src, n * sizeof(double), mem == DFEM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                     sc->stream));
+  return DFEM_OK;
+}
+
+}  // namespace dfem
+
+#define RC(x) do { int rc_ = (x); if (rc_) return rc_; } while (0)
+
+extern "C" {
+
+const char* dfem_last_error(void) { return g_last_error.c_str(); }
+int dfem_abi_version(void) { return DFEM_ABI_VERSION; }
+
+int dfem_scene_create(const dfem_scene_desc* desc, int device, dfem_scene** out) {
+  if (!desc || !out) return fail(DFEM_ERR_INVALID, "null argument");
+  *out = nullptr;
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(DFEM_ERR_INVALID, "device index out of range");
+  CK(cudaSetDevice(device));
+  std::unique_ptr<dfem_scene> sc(new dfem_scene());
+  sc->device = device;
+  std::string err;
+  if (!build_host_scene(*desc, sc->hs, err))
+    return fail(err.find("factor") != std::string::npos ? DFEM_ERR_FACTOR : DFEM_ERR_INVALID, err);
+  if (!refactorize(sc->hs.Hs, sc->hs.F, err)) return fail(DFEM_ERR_FACTOR, err);
+  CK(cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking));
+  RC(upload_scene(sc.get()));
+  RC(ensure_steps(sc.get(), 1));
+  CK(cudaDeviceSynchronize());
+  *out = sc.release();
+  g_last_error.clear();
+  return DFEM_OK;
+}
+
+int dfem_scene_destroy(dfem_scene* scene) {
+  if (!scene) return DFEM_OK;
+  cudaSetDevice(scene->device);
+  if (scene->stream) cudaStreamSynchronize(scene->stream);
+  delete scene;
+  return DFEM_OK;
+}
+
+int dfem_scene_get_info(const dfem_scene* sc, dfem_scene_info* info) {
+  if (!sc || !info) return fail(DFEM_ERR_INVALID, "null argument");
+  const HostScene& s = sc->hs;
+  info->n_vertices = s.N; info->n_tets = s.T; info->n_attach = s.A; info->n_muscle = s.M;
+  info->n_springs = s.S; info->n_bending = s.B;
+  info->n_supernodes = s.F.nsuper; info->n_levels = s.F.nlevels; info->nnz_factor = s.F.nnz_factor;
+  info->n_slots = s.nslots; info->device = sc->device; info->factor_regularisation = s.F.reg;
+  return DFEM_OK;
+}
+
+int dfem_set_materials(dfem_scene* sc, const double* youngs, const double* poisson, int mem) {
+  if (!sc || !youngs || !poisson) return fail(DFEM_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(sc->device));
+  const int T = sc->hs.T;
+  std::vector<double> E(T), nu(T);
+  if (mem == DFEM_MEM_DEVICE) {
+    CK(cudaMemcpy(E.data(), youngs, T * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nu.data(), poisson, T * sizeof(double), cudaMemcpyDeviceToHost));
+  } else {
+    std::copy(youngs, youngs + T, E.begin());
+    std::copy(poisson, poisson + T, nu.begin());
+  }
+  std::string err;
+  CK(cudaStreamSynchronize(sc->stream));
+  if (!update_materials(sc->hs, E.data(), nu.data(), err)) return fail(DFEM_ERR_FACTOR, err);
+  RC(upload_materials(sc));
+  CK(cudaDeviceSynchronize());
+  return DFEM_OK;
+}
+
+int dfem_set_activations(dfem_scene* sc, const double* act, int mem) {
+  if (!sc || (!act && sc->hs.nseg > 0)) return fail(DFEM_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(sc->device));
+  if (sc->hs.nseg == 0) return DFEM_OK;
+  RC(copy_in(sc, act, sc->hs.nseg, sc->act_cur.p, mem));
+  CK(cudaStreamSynchronize(sc->stream));
+  return DFEM_OK;
+}
+
+int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const double* act, int32_t n_steps,
+                      double* x_out, double* v_out, double* traj_x, int mem) {
+  if (!sc || !x || !v || !x_out || !v_out) return fail(DFEM_ERR_INVALID, "null argument");
+  if (n_steps < 1) return fail(DFEM_ERR_INVALID, "n_steps must be >= 1");
+  CK(cudaSetDevice(sc->device));
+  RC(ensure_steps(sc, n_steps));
+  const HostScene& s = sc->hs;
+  const size_t n3 = 3 * (size_t)s.N;
+  const int nseg = s.nseg;
+  if (nseg > 0) {
+    if (act) {
+      RC(copy_in(sc, act, (size_t)n_steps * nseg, sc->act_all.p, mem));
+    } else {
+      for (int st = 0; st < n_steps; ++st)
+        CK(cudaMemcpyAsync(sc->act_all.p + (size_t)st * nseg, sc->act_cur.p, nseg * sizeof(double), cudaMemcpyDeviceToDevice,
+                           sc->stream));
+    }
+  }
+  RC(copy_in(sc, x, n3, sc->io_a.p, mem));
+  RC(copy_in(sc, v, n3, sc->io_b.p, mem));
+  const int nb = sc->nblk_v;
+  k_to_internal<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_internal.p, sc->io_a.p, sc->xt.p);
+  k_to_internal<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_internal.p, sc->io_b.p, sc->vt.p);
+  k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, 0);
+  k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, traj_x ? 1 : 0);
+  k_set_int<<<1, 1, 0, sc->stream>>>(sc->status.p, 0);
+  CK(cudaGetLastError());
+  if (!sc->g_step) RC(build_graph(sc, enqueue_step, &sc->g_step, &sc->step_nodes));
+  for (int st = 0; st < n_steps; ++st) CK(cudaGraphLaunch(sc->g_step, sc->stream));
+  sc->launches += 7 + (int64_t)n_steps * (int64_t)sc->step_nodes;
+  k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->xt.p, sc->io_a.p);
+  k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->vt.p, sc->io_b.p);
+  RC(copy_out(sc, sc->io_a.p, n3, x_out, mem));
+  RC(copy_out(sc, sc->io_b.p, n3, v_out, mem));
+  if (traj_x) RC(copy_out(sc, sc->traj.p, n3 * n_steps, traj_x, mem));
+  int status = 0;
+  CK(cudaMemcpyAsync(&status, sc->status.p, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+  CK(cudaStreamSynchronize(sc->stream));
+  sc->rec_steps = n_steps;
+  if (status) return fail(DFEM_ERR_NONFINITE, "non-finite value in the PD iteration");
+  return DFEM_OK;
+}
+
+int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_out, double* gx, double* gv,
+                       double* g_youngs, double* g_poisson, double* g_act, int mem) {
+  if (!sc || !gx_out || !gv_out || !gx || !gv) return fail(DFEM_ERR_INVALID, "null argument");
+  if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_step_backward needs a preceding dfem_step_forward");
+  CK(cudaSetDevice(sc->device));
+  const HostScene& s = sc->hs;
+  const size_t n3 = 3 * (size_t)s.N;
+  const int nb = sc->nblk_v;
+  // incoming cotangents -> internal order, kept in xk (x) and vt? no: use dedicated buffers
+  RC(copy_in(sc, gx_out, n3, sc->rhs.p, mem));
+  RC(copy_in(sc, gv_out, n3, sc->c0.p, mem));
+  k_to_internal<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_internal.p, sc->rhs.p, sc->io_a.p);
+  k_to_internal<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_internal.p, sc->c0.p, sc->io_b.p);
+  CK(cudaMemsetAsync(sc->gE.p, 0, sizeof(double) * std::max(1, s.T), sc->stream));
+  CK(cudaMemsetAsync(sc->gnu.p, 0, sizeof(double) * std::max(1, s.T), sc->stream));
+  CK(cudaMemsetAsync(sc->gact.p, 0, sizeof(double) * (size_t)sc->rec_steps * std::max(1, s.nseg), sc->stream));
+  k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, 0);
+  if (!sc->g_step) RC(build_graph(sc, enqueue_step, &sc->g_step, &sc->step_nodes));
+  if (!sc->g_adj) RC(build_graph(sc, enqueue_adjoint, &sc->g_adj, &sc->adj_nodes));
+  for (int st = sc->rec_steps - 1; st >= 0; --st) {
+    // recompute the step's iterates from its checkpoint (the step graph re-records the same checkpoint)
+    CK(cudaMemcpyAsync(sc->xt.p, sc->ckpt_x.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaMemcpyAsync(sc->vt.p, sc->ckpt_v.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+    k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
+    CK(cudaGraphLaunch(sc->g_step, sc->stream));
+    k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
+    CK(cudaGraphLaunch(sc->g_adj, sc->stream));
+  }
+  sc->launches += 5 + (int64_t)sc->rec_steps * (int64_t)(2 + sc->step_nodes + sc->adj_nodes);
+  k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_a.p, sc->rhs.p);
+  k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_b.p, sc->c0.p);
+  RC(copy_out(sc, sc->rhs.p, n3, gx, mem));
+  RC(copy_out(sc, sc->c0.p, n3, gv, mem));
+  if (g_youngs) RC(copy_out(sc, sc->gE.p, s.T, g_youngs, mem));
+  if (g_poisson) RC(copy_out(sc, sc->gnu.p, s.T, g_poisson, mem));
+  if (g_act && s.nseg > 0) RC(copy_out(sc, sc->gact.p, (size_t)sc->rec_steps * s.nseg, g_act, mem));
+  CK(cudaStreamSynchronize(sc->stream));
+  return DFEM_OK;
+}
+
+int dfem_get_iterations(const dfem_scene* sc, int32_t* iters, int32_t n) {
+  if (!sc || !iters) return fail(DFEM_ERR_INVALID, "null argument");
+  if (n > sc->cap_steps) return fail(DFEM_ERR_INVALID, "n exceeds recorded steps");
+  CK(cudaSetDevice(sc->device));
+  CK(cudaMemcpy(iters, sc->iters.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+  return DFEM_OK;
+}
+
+int dfem_host_factor_solve(const dfem_scene_desc* desc, const double* b, double* x, dfem_scene_info* info) {
+  if (!desc || !b || !x) return fail(DFEM_ERR_INVALID, "null argument");
+  HostScene hs;
+  std::string err;
+  if (!build_host_scene(*desc, hs, err)) return fail(DFEM_ERR_INVALID, err);
+  if (!refactorize(hs.Hs, hs.F, err)) return fail(DFEM_ERR_FACTOR, err);
+  const int N = hs.N;
+  std::vector<double> bi(3 * (size_t)N), xi(3 * (size_t)N);
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) bi[3 * (size_t)hs.to_internal[i] + c] = b[3 * (size_t)i + c];
+  host_solve(hs.F, bi.data(), xi.data());
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) x[3 * (size_t)i + c] = xi[3 * (size_t)hs.to_internal[i] + c];
+  if (info) {
+    info->n_vertices = hs.N; info->n_tets = hs.T; info->n_attach = hs.A; info->n_muscle = hs.M;
+    info->n_springs = hs.S; info->n_bending = hs.B; info->n_supernodes = hs.F.nsuper;
+    info->n_levels = hs.F.nlevels; info->nnz_factor = hs.F.nnz_factor; info->n_slots = hs.nslots;
+    info->device = -1; info->factor_regularisation = hs.F.reg;
+  }
+  return DFEM_OK;
+}
+
+int dfem_get_launch_count(const dfem_scene* sc, int64_t* count) {
+  if (!sc || !count) return fail(DFEM_ERR_INVALID, "null argument");
+  *count = sc->launches;
+  return DFEM_OK;
+}
+
+int dfem_profile_phases(dfem_scene* sc, int32_t reps, double* ms) {
+  if (!sc || !ms || reps < 1) return fail(DFEM_ERR_INVALID, "bad argument");
+  if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_profile_phases needs a preceding dfem_step_forward");
+  CK(cudaSetDevice(sc->device));
+  const HostScene& s = sc->hs;
+  const int nb = sc->nblk_v;
+  const int ncons = s.T + s.M + s.S + s.B;
+  const int nthr = std::max(ncons, s.N);
+  // open gates: forward flag cleared, adjoint iteration count of step 0 = K
+  k_set_int<<<1, 1, 0, sc->stream>>>(sc->flag.p, 0);
+  k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, 0);
+  k_set_int<<<1, 1, 0, sc->stream>>>(sc->iters.p, s.K);
+  Gate gf{sc->flag.p, nullptr, nullptr, 0};
+  Gate ga{nullptr, sc->iters.p, sc->step.p, 0};
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto timed = [&](int phase, auto&& launch) -> int {
+    launch();  // warm-up
+    CK(cudaEventRecord(e0, sc->stream));
+    for (int r = 0; r < reps; ++r) launch();
+    CK(cudaEventRecord(e1, sc->stream));
+    CK(cudaEventSynchronize(e1));
+    float t = 0;
+    CK(cudaEventElapsedTime(&t, e0, e1));
+    ms[phase] = (double)t / reps;
+    sc->launches += reps + 1;
+    return DFEM_OK;
+  };
+  int rc = DFEM_OK;
+  if (!rc && ncons > 0)
+    rc = timed(0, [&] { k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, gf, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p); });
+  if (!rc) rc = timed(1, [&] { k_gather<<<nb, 128, 0, sc->stream>>>(s.N, gf, sc->vslot_ptr.p, sc->slot.p, sc->c0.p, sc->rhs.p); });
+  if (!rc) rc = timed(2, [&] { enqueue_solve(sc, gf, sc->rhs.p, sc->y.p); });
+  if (!rc && ncons > 0)
+    rc = timed(3, [&] {
+      k_adj_local<<<(nthr + 127) / 128, 128, 0, sc->stream>>>(sc->sd, ga, 0, sc->hist.p, sc->y.p, sc->bb.p, sc->act_all.p,
+                                                              sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+    });
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(sc->stream));
+  // the solve phase counted one launch per call above; it is 2 * levels kernels
+  sc->launches += (int64_t)(reps + 1) * (2 * ((int64_t)sc->lvl_ptr.size() - 1) - 1);
+  sc->rec_steps = 0;  // gates and iteration counts were overwritten: no backward of the old forward
+  return DFEM_OK;
+}
+
+int dfem_synchronize(dfem_scene* sc) {
+  if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(sc->device));
+  CK(cudaStreamSynchronize(sc->stream));
+  return DFEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,480 @@
+// pd_kernels.cu — the PD step kernels (FP64 plain form) and the adjoint kernels.
+//
+// One time step (diff_fem World::TimeStepping + ProjectiveDynamicsMethod,
+// sim/fem/World.h:673-720, 835-917) is this kernel sequence, captured once as
+// a CUDA graph and replayed for every step:
+//   k_step_begin        v_wc = v + g h, q_n = x + h v_wc, c0 = M/h^2 q_n - Hs x + J_att d_att,
+//                       x^0 = q_n, convergence test of the reference's first iteration
+//   K x { k_local       per-constraint projection d and its J*d slot contributions
+//         k_gather      rhs_i = c0_i + sum of vertex i's slots           (ori_c - Qf x)
+//         k_fwd_level   L y = rhs, one launch per level of the supernodal tree
+//         k_bwd_level   L^T z = y, levels in reverse (z = hvf)
+//         k_update      x^{k+1} = x + z, ||x^{k+1}-x^k|| / 3N < 5e-7 -> converged flag }
+//   k_step_end          v = damping (x^K - x)/h, x = x^K
+#include "kernels.cuh"
+
+namespace dfem {
+
+// ------------------------------------------------------------- utilities ----
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic grid reduction: per-block partial sums, the last block to
+// finish sums the partials in block order.  Returns true in thread 0 of the
+// last block, with *total set.
+__device__ bool grid_reduce(double v, double* partial, unsigned* counter, double* total) {
+  __shared__ double ws[32];
+  __shared__ bool last;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) ws[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) s += ws[w];
+    partial[blockIdx.x] = s;
+    __threadfence();
+    unsigned ticket = atomicAdd(counter, 1u);
+    last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    double s = 0;
+    for (unsigned b = 0; b < gridDim.x; ++b) s += ((volatile double*)partial)[b];
+    *total = s;
+    *counter = 0u;
+    return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ Vec3<double> ld3(const double* p, int i) {
+  return mk3(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
+}
+__device__ __forceinline__ void st3(double* p, int i, Vec3<double> v) {
+  p[3 * i] = v.x; p[3 * i + 1] = v.y; p[3 * i + 2] = v.z;
+}
+
+// G[v][j] coefficients from invDm planes: F(:,j) = sum_v G[v][j] x_v
+__device__ __forceinline__ void load_g(const double* inv, int n, int e, double G[4][3]) {
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    double a = inv[(0 * 3 + j) * n + e], b = inv[(1 * 3 + j) * n + e], c = inv[(2 * 3 + j) * n + e];
+    G[1][j] = a; G[2][j] = b; G[3][j] = c;
+    G[0][j] = -(a + b + c);
+  }
+}
+
+__device__ __forceinline__ Mat3<double> deformation(const double G[4][3], const Vec3<double> xv[4]) {
+  Mat3<double> F;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    F.c[j] = G[0][j] * xv[0] + G[1][j] * xv[1] + G[2][j] * xv[2] + G[3][j] * xv[3];
+  return F;
+}
+
+// --------------------------------------------------------------- forward ----
+
+__global__ void k_step_begin(SceneDev d, const int* step, double* xt, double* vt, double* qn,
+                             double* c0, double* xk, double* hist, double* ckpt_x, double* ckpt_v,
+                             int* flag, int* iters, double* partial, unsigned* counter, double* errv,
+                             int* status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = *step;
+  double q2 = 0;
+  if (i < d.N) {
+    Vec3<double> x = ld3(xt, i), v = ld3(vt, i);
+    if (ckpt_x) { st3(ckpt_x + (size_t)s * 3 * d.N, i, x); st3(ckpt_v + (size_t)s * 3 * d.N, i, v); }
+    // Environment::Step adds g h to v (gravity-enabled bodies); TimeStepping:
+    // v_wc = v + h M^-1 f_ext (f_ext = 0), q_n = x + h v_wc
+    double gm = d.gmask[i] * d.h;
+    Vec3<double> vwc = mk3(v.x + gm * d.g0, v.y + gm * d.g1, v.z + gm * d.g2);
+    Vec3<double> q = x + d.h * vwc;
+    st3(qn, i, q);
+    st3(xk, i, q);
+    if (hist) st3(hist, i, q);
+    // c0 = M/h^2 q_n - Hs x + J_att d_att   (b - Qf*mNonrigidX plus the constant attachment term)
+    double m = d.mass[i] / (d.h * d.h);
+    Vec3<double> acc = m * q;
+    for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) {
+      double a = d.hs_val[k];
+      Vec3<double> xj = ld3(xt, d.hs_col[k]);
+      acc = acc - a * xj;
+    }
+    acc = acc + ld3(d.attach_jd, i);
+    st3(c0, i, acc);
+    q2 = dot3(q, q);
+  }
+  if (i == 0) { iters[s] = 0; }
+  double tot;
+  if (grid_reduce(q2, partial, counter, &tot)) {
+    // iteration 0 of the reference compares q_n with a zero vector
+    double e = sqrt(tot) / (3.0 * d.N);
+    *errv = e;
+    *flag = (e < kConvergenceEps) ? 1 : 0;
+    if (!isfinite(tot)) *status = 4;
+  }
+}
+
+// Local step: every constraint projects and writes its J*d contribution to its
+// slots.  One thread per constraint; constraint types are consecutive ranges.
+__global__ void __launch_bounds__(128) k_local(SceneDev d, Gate gate, const double* __restrict__ x,
+                                               const double* __restrict__ act_all, const int* step,
+                                               double* __restrict__ slot) {
+  if (gate.skip()) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.T) {
+    // corotated FEM (CorotateFEMConstraint::EvaluateDVector + EvaluateJMatrix)
+    int4 v = d.tv[t];
+    Vec3<double> xv[4] = {ld3(x, v.x), ld3(x, v.y), ld3(x, v.z), ld3(x, v.w)};
+    double G[4][3];
+    load_g(d.tinv, d.T, t, G);
+    Mat3<double> F = deformation(G, xv), md, mdv;
+    corot_project(F, md, mdv);
+    double wr = d.twr[t], wv = d.twv[t];
+    Vec3<double> P[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) P[j] = wr * md.c[j] + wv * mdv.c[j];
+    int4 sl = d.tslot[t];
+    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st3(slot, sv[a], G[a][0] * P[0] + G[a][1] * P[1] + G[a][2] * P[2]);
+    return;
+  }
+  t -= d.T;
+  if (t < d.M) {
+    // muscle (LinearMuscleConstraint::Computep0 + EvaluateJMatrix): d = (1-a) F f
+    int4 v = d.mv[t];
+    Vec3<double> xv[4] = {ld3(x, v.x), ld3(x, v.y), ld3(x, v.z), ld3(x, v.w)};
+    double G[4][3];
+    load_g(d.minv, d.M, t, G);
+    Vec3<double> f = mk3(d.mfib[t], d.mfib[d.M + t], d.mfib[2 * d.M + t]);
+    double c[4];
+    Vec3<double> Ff = mk3(0.0, 0.0, 0.0);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      c[a] = G[a][0] * f.x + G[a][1] * f.y + G[a][2] * f.z;
+      Ff = Ff + c[a] * xv[a];
+    }
+    double a_act = act_all[(size_t)(*step) * d.nseg + d.mseg[t]];
+    Vec3<double> p0 = (1.0 - a_act) * Ff;
+    double w = d.mw[t];
+    int4 sl = d.mslot[t];
+    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st3(slot, sv[a], (w * c[a]) * p0);
+    return;
+  }
+  t -= d.M;
+  if (t < d.S) {
+    // spring (SpringConstraint::EvaluateDVector): d = rest * (x0-x1)/|x0-x1|, J = sqrt(w) [I; -I]
+    int2 v = d.sv[t];
+    Vec3<double> e = ld3(x, v.x) - ld3(x, v.y);
+    Vec3<double> dd = (d.srest[t] * rsqrt(dot3(e, e))) * e;
+    double w = d.ssw[t];
+    int2 sl = d.sslot[t];
+    st3(slot, sl.x, w * dd);
+    st3(slot, sl.y, (-w) * dd);
+    return;
+  }
+  t -= d.S;
+  if (t < d.B) {
+    // bending (BendingConstraint::EvaluateDVector): d = w * lap * rest/|lap|, J = w beta
+    int o0 = d.boff[t], o1 = d.boff[t + 1];
+    Vec3<double> lap = mk3(0.0, 0.0, 0.0);
+    for (int k = o0; k < o1; ++k) lap = lap + d.bbeta[k] * ld3(x, d.bv[k]);
+    double ln = sqrt(dot3(lap, lap));
+    double w = d.bw[t];
+    Vec3<double> dd = mk3(0.0, 0.0, 0.0);
+    if (ln > 1e-25) dd = (w * d.brest[t] / ln) * lap;
+    for (int k = o0; k < o1; ++k) st3(slot, d.bslot[k], (w * d.bbeta[k]) * dd);
+  }
+}
+
+// rhs_i = c0_i + sum of the slots of vertex i
+__global__ void k_gather(int N, Gate gate, const int* __restrict__ vslot_ptr, const double* __restrict__ slot,
+                         const double* __restrict__ c0, double* __restrict__ rhs) {
+  if (gate.skip()) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  Vec3<double> acc = ld3(c0, i);
+  for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
+  st3(rhs, i, acc);
+}
+
+// Forward solve of one level: for each supernode s of the level,
+//   t = rhs_s - L_{s,<} y_<   (row-wise CSR, warp per row)
+//   y_s = Dinv_s t            (warp per row)
+__global__ void __launch_bounds__(128) k_fwd_level(FactorDev f, int lvl_begin, Gate gate,
+                                                   const double* __restrict__ rhs, double* y) {
+  if (gate.skip()) return;
+  extern __shared__ double tsh[];
+  const int s = f.lvl_sn[lvl_begin + blockIdx.x];
+  const int c0 = f.sn_c0[s], w = f.sn_w[s];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c = warp; c < w; c += nw) {
+    const int i = c0 + c;
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int k = f.lrow_ptr[i] + lane; k < f.lrow_ptr[i + 1]; k += 32) {
+      int j = f.lrow_col[k];
+      double l = f.lrow_val[k];
+      a0 += l * y[3 * j]; a1 += l * y[3 * j + 1]; a2 += l * y[3 * j + 2];
+    }
+    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+    if (lane == 0) { tsh[3 * c] = rhs[3 * i] - a0; tsh[3 * c + 1] = rhs[3 * i + 1] - a1; tsh[3 * c + 2] = rhs[3 * i + 2] - a2; }
+  }
+  __syncthreads();
+  const double* Di = f.Dinv + f.sn_dofs[s];
+  for (int c = warp; c < w; c += nw) {
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int k = lane; k <= c; k += 32) {
+      double dv = Di[c * w + k];
+      a0 += dv * tsh[3 * k]; a1 += dv * tsh[3 * k + 1]; a2 += dv * tsh[3 * k + 2];
+    }
+    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+    if (lane == 0) { y[3 * (c0 + c)] = a0; y[3 * (c0 + c) + 1] = a1; y[3 * (c0 + c) + 2] = a2; }
+  }
+}
+
+// Backward solve of one level (in place in y): for each supernode s,
+//   u = y_s - L_{R,s}^T y_R  (column-major block, warp per column)
+//   y_s = Dinv_s^T u
+__global__ void __launch_bounds__(128) k_bwd_level(FactorDev f, int lvl_begin, Gate gate, double* y) {
+  if (gate.skip()) return;
+  extern __shared__ double tsh[];
+  const int s = f.lvl_sn[lvl_begin + blockIdx.x];
+  const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
+  const int* R = f.rowidx + f.sn_rofs[s];
+  const double* Lc = f.Lcm + f.sn_lofs[s];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c = warp; c < w; c += nw) {
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int a = lane; a < r; a += 32) {
+      double l = Lc[(size_t)c * r + a];
+      int i = R[a];
+      a0 += l * y[3 * i]; a1 += l * y[3 * i + 1]; a2 += l * y[3 * i + 2];
+    }
+    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+    if (lane == 0) {
+      int i = c0 + c;
+      tsh[3 * c] = y[3 * i] - a0; tsh[3 * c + 1] = y[3 * i + 1] - a1; tsh[3 * c + 2] = y[3 * i + 2] - a2;
+    }
+  }
+  __syncthreads();
+  const double* Di = f.Dinv + f.sn_dofs[s];
+  for (int c = warp; c < w; c += nw) {
+    double a0 = 0, a1 = 0, a2 = 0;
+    for (int k = c + lane; k < w; k += 32) {
+      double dv = Di[k * w + c];
+      a0 += dv * tsh[3 * k]; a1 += dv * tsh[3 * k + 1]; a2 += dv * tsh[3 * k + 2];
+    }
+    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+    if (lane == 0) { y[3 * (c0 + c)] = a0; y[3 * (c0 + c) + 1] = a1; y[3 * (c0 + c) + 2] = a2; }
+  }
+}
+
+// x^{k+1} = x_t + hvf; convergence test for the next iteration
+__global__ void k_update(int N, Gate gate, int k, const double* __restrict__ xt, const double* __restrict__ z,
+                         double* xk, double* hist, const int* step, int* flag, int* iters,
+                         double* partial, unsigned* counter, double* errv, int* status) {
+  if (gate.skip()) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e2 = 0;
+  if (i < N) {
+    Vec3<double> xn = ld3(xt, i) + ld3(z, i);
+    Vec3<double> dlt = xn - ld3(xk, i);
+    e2 = dot3(dlt, dlt);
+    st3(xk, i, xn);
+    if (hist) st3(hist + (size_t)(k + 1) * 3 * N, i, xn);
+  }
+  double tot;
+  if (grid_reduce(e2, partial, counter, &tot)) {
+    double e = sqrt(tot) / (3.0 * N);
+    *errv = e;
+    iters[*step] += 1;
+    if (e < kConvergenceEps) *flag = 1;
+    if (!isfinite(tot)) { *status = 4; *flag = 1; }
+  }
+}
+
+// v = damping (x^K - x)/h ; x = x^K ; optional trajectory row in user order
+__global__ void k_step_end(SceneDev d, int* step, double* xt, double* vt, const double* xk,
+                           double* traj, const int* to_user, const int* write_traj) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = *step;
+  if (i < d.N) {
+    Vec3<double> x1 = ld3(xk, i), x0 = ld3(xt, i);
+    st3(vt, i, (d.damping / d.h) * (x1 - x0));
+    st3(xt, i, x1);
+    if (traj && *write_traj) st3(traj + (size_t)s * 3 * d.N, to_user[i], x1);
+  }
+  // the step counter is advanced by k_next_step (a separate launch, so every
+  // block of this kernel has read it first)
+}
+
+__global__ void k_next_step(int* step) { *step += 1; }
+__global__ void k_set_int(int* p, int v) { *p = v; }
+
+// permutation between user and internal vertex order (3 doubles per vertex)
+__global__ void k_to_internal(int N, const int* to_internal, const double* src, double* dst) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) st3(dst, to_internal[i], ld3(src, i));
+}
+__global__ void k_to_user(int N, const int* to_user, const double* src, double* dst) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) st3(dst, to_user[i], ld3(src, i));
+}
+
+// ---------------------------------------------------------------- adjoint ---
+//
+// Reverse of one step.  With x^{k+1} = Hs^-1 (b + J d(x^k)) (the reference's
+// delta form x + Hs^-1(ori_c - Hs x) is the same map), for k = it-1 .. 0:
+//   ybar = Hs^-1 xbar^{k+1}; bbar += ybar; xbar^k = (dd/dx)^T J^T ybar;
+//   dE_t += ybar^T (dJ/dE_t d^k - dHs/dE_t x^{k+1}); dnu_t likewise; da_seg += -(J^T ybar).(F f)
+// then qbar = xbar^0 + M/h^2 bbar, xbar = -damping/h vbar' + qbar, vbar = h qbar.
+
+__global__ void k_adj_begin(int N, double c, const double* gx1, const double* gv1, double* xkb,
+                            double* xtb, double* bb) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  Vec3<double> gv = ld3(gv1, i);
+  st3(xkb, i, ld3(gx1, i) + c * gv);
+  st3(xtb, i, (-c) * gv);
+  st3(bb, i, mk3(0.0, 0.0, 0.0));
+}
+
+__global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, int k, const double* __restrict__ hist,
+                                                   const double* __restrict__ yb, double* bb,
+                                                   const double* __restrict__ act_all, double* __restrict__ slot,
+                                                   double* gE, double* gnu, double* mg) {
+  if (gate.skip()) return;
+  const double* x = hist + (size_t)k * 3 * d.N;
+  const double* x1 = hist + (size_t)(k + 1) * 3 * d.N;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.N) {  // bbar += ybar (b = M/h^2 q_n enters every iteration)
+    st3(bb, t, ld3(bb, t) + ld3(yb, t));
+  }
+  if (t < d.T) {
+    int4 v = d.tv[t];
+    const int vi[4] = {v.x, v.y, v.z, v.w};
+    Vec3<double> xv[4], yv[4], x1v[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) { xv[a] = ld3(x, vi[a]); yv[a] = ld3(yb, vi[a]); x1v[a] = ld3(x1, vi[a]); }
+    double G[4][3];
+    load_g(d.tinv, d.T, t, G);
+    Mat3<double> F = deformation(G, xv), F1 = deformation(G, x1v), Y = deformation(G, yv), md, mdv;
+    corot_project(F, md, mdv);
+    double E = d.tE[t], nu = d.tnu[t], vol = d.tvol[t];
+    double yr = 0, yvv = 0, yh = 0;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { yr += dot3(Y.c[j], md.c[j]); yvv += dot3(Y.c[j], mdv.c[j]); yh += dot3(Y.c[j], F1.c[j]); }
+    double opn = 1.0 + nu;
+    if (gE) gE[t] += vol / opn * (yr + nu * yvv) - vol * yh;
+    if (gnu) gnu[t] += E * vol / (opn * opn) * (yvv - yr);
+    double wr = d.twr[t], wv = d.twv[t];
+    Mat3<double> gmd, gmdv;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) { gmd.c[j] = wr * Y.c[j]; gmdv.c[j] = wv * Y.c[j]; }
+    Mat3<double> gF = corot_vjp(F, gmd, gmdv);
+    int4 sl = d.tslot[t];
+    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st3(slot, sv[a], G[a][0] * gF.c[0] + G[a][1] * gF.c[1] + G[a][2] * gF.c[2]);
+    return;
+  }
+  t -= d.T;
+  if (t < d.M) {
+    int4 v = d.mv[t];
+    const int vi[4] = {v.x, v.y, v.z, v.w};
+    double G[4][3];
+    load_g(d.minv, d.M, t, G);
+    Vec3<double> f = mk3(d.mfib[t], d.mfib[d.M + t], d.mfib[2 * d.M + t]);
+    double w = d.mw[t];
+    double c[4];
+    Vec3<double> db = mk3(0.0, 0.0, 0.0), Ff = mk3(0.0, 0.0, 0.0);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      c[a] = G[a][0] * f.x + G[a][1] * f.y + G[a][2] * f.z;
+      db = db + (w * c[a]) * ld3(yb, vi[a]);
+      Ff = Ff + c[a] * ld3(x, vi[a]);
+    }
+    double a_act = act_all[(size_t)(*gate.step) * d.nseg + d.mseg[t]];
+    mg[t] = -dot3(db, Ff);
+    int4 sl = d.mslot[t];
+    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st3(slot, sv[a], ((1.0 - a_act) * c[a]) * db);
+    return;
+  }
+  t -= d.M;
+  if (t < d.S) {
+    int2 v = d.sv[t];
+    double w = d.ssw[t];
+    Vec3<double> db = w * (ld3(yb, v.x) - ld3(yb, v.y));
+    Vec3<double> e = ld3(x, v.x) - ld3(x, v.y);
+    double inv = rsqrt(dot3(e, e));
+    Vec3<double> eh = inv * e;
+    Vec3<double> ge = (d.srest[t] * inv) * (db - dot3(eh, db) * eh);
+    int2 sl = d.sslot[t];
+    st3(slot, sl.x, ge);
+    st3(slot, sl.y, (-1.0) * ge);
+    return;
+  }
+  t -= d.S;
+  if (t < d.B) {
+    int o0 = d.boff[t], o1 = d.boff[t + 1];
+    double w = d.bw[t];
+    Vec3<double> db = mk3(0.0, 0.0, 0.0), lap = mk3(0.0, 0.0, 0.0);
+    for (int q = o0; q < o1; ++q) {
+      db = db + (w * d.bbeta[q]) * ld3(yb, d.bv[q]);
+      lap = lap + d.bbeta[q] * ld3(x, d.bv[q]);
+    }
+    double ln = sqrt(dot3(lap, lap));
+    Vec3<double> gl = mk3(0.0, 0.0, 0.0);
+    if (ln > 1e-25) {
+      Vec3<double> lh = (1.0 / ln) * lap;
+      gl = (w * d.brest[t] / ln) * (db - dot3(lh, db) * lh);
+    }
+    for (int q = o0; q < o1; ++q) st3(slot, d.bslot[q], d.bbeta[q] * gl);
+  }
+}
+
+// xbar^k = sum of the slots (constraints without x dependence contribute nothing)
+__global__ void k_adj_gather(int N, Gate gate, const int* __restrict__ vslot_ptr, const double* __restrict__ slot,
+                             double* xkb) {
+  if (gate.skip()) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  Vec3<double> acc = mk3(0.0, 0.0, 0.0);
+  for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
+  st3(xkb, i, acc);
+}
+
+// activation gradient of the step: sum over the muscle constraints of each segment
+__global__ void k_seg_reduce(int nseg, Gate gate, const int* seg_ptr, const int* seg_mus, const double* mg,
+                             double* gact) {
+  if (gate.skip()) return;
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nseg) return;
+  double s = 0;
+  for (int k = seg_ptr[q]; k < seg_ptr[q + 1]; ++k) s += mg[seg_mus[k]];
+  gact[(size_t)(*gate.step) * nseg + q] += s;
+}
+
+__global__ void k_adj_end(SceneDev d, const double* xkb, const double* xtb, const double* bb,
+                          double* gx, double* gv) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  double m = d.mass[i] / (d.h * d.h);
+  Vec3<double> qb = ld3(xkb, i) + m * ld3(bb, i);
+  st3(gx, i, ld3(xtb, i) + qb);
+  st3(gv, i, d.h * qb);
+}
+
+}  // namespace dfem

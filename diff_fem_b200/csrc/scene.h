@@ -1,0 +1,67 @@
+// scene.h — host-side preprocessing of a dfem_scene_desc into the constraint
+// tables, the scalar system matrix Hs and the slot layout the kernels use.
+//
+// Internally every vertex is renumbered into the fill-reducing order of the
+// Cholesky factor, so the local step, the rhs gather, the triangular solves
+// and the position update all work in one numbering and the permutation is
+// applied only at the API boundary.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/dfem.h"
+#include "cholesky.h"
+
+namespace dfem {
+
+struct HostScene {
+  int N = 0;
+  std::vector<double> x0, mass, gmask;  // internal order
+
+  // corotated tets: re-oriented vertices, invDm (row-major 9), weights
+  int T = 0;
+  std::vector<int> tv;                  // 4T (internal ids)
+  std::vector<double> tinv;             // 9T
+  std::vector<double> tvol, tE, tnu;
+  std::vector<int> tslot;               // 4T slot positions
+
+  int M = 0, nseg = 0;                  // muscle constraints
+  std::vector<int> mv;                  // 4M
+  std::vector<double> minv, mvol, mk, mfib;  // 9M, M, M, 3M
+  std::vector<int> mseg, mslot;
+  std::vector<int> seg_ptr, seg_mus;    // CSR segment -> muscle constraints
+
+  int S = 0;                            // springs
+  std::vector<int> sv, sslot;           // 2S
+  std::vector<double> srest, ssw;       // rest length, sqrt(weight)
+
+  int B = 0;                            // bending stencils
+  std::vector<int> boff, bv, bslot;     // CSR (centre first), slots
+  std::vector<double> bbeta, bw, brest;
+
+  int A = 0;                            // attachments
+  std::vector<int> av;
+  std::vector<double> ap, ak;
+
+  int nslots = 0;
+  std::vector<int> vslot_ptr;           // N+1, slots sorted by vertex
+
+  SparseSym Hs;                         // internal order
+  SupernodalFactor F;                   // factor of Hs (perm = identity after renumbering)
+  std::vector<int> to_internal;         // user vertex id -> internal id
+  std::vector<int> to_user;             // internal id -> user vertex id
+
+  double h = 0.01, damping = 1.0, g[3] = {0, 0, 0};
+  int K = 10;
+  int precision = DFEM_PREC_FP64;
+  int checkpoint_every = 1;
+};
+
+// Build everything (including ordering + factorisation).  Returns false with err.
+bool build_host_scene(const dfem_scene_desc& d, HostScene& hs, std::string& err);
+
+// Re-assemble Hs values after material changes and refactor (same structure).
+bool update_materials(HostScene& hs, const double* E_user_order, const double* nu_user_order, std::string& err);
+
+}  // namespace dfem

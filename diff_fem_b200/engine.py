@@ -1,0 +1,155 @@
+"""Python handle over one engine scene (C-ABI calls through ctypes).
+
+Buffers may be numpy arrays (host, FP64) or torch tensors (host or CUDA, FP64,
+contiguous); CUDA tensors are passed to the engine as device pointers, so a
+step reads and writes HBM directly with no host round trip.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _capi
+from ._capi import DFEM_MEM_DEVICE, DFEM_MEM_HOST, check, lib
+
+try:  # torch is optional for the host-array path
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+def _is_cuda_tensor(a) -> bool:
+    return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
+
+
+def _ptr(a):
+    """(pointer, mem kind, keepalive) of a numpy array or torch tensor (FP64)."""
+    if a is None:
+        return None, None, None
+    if torch is not None and isinstance(a, torch.Tensor):
+        if a.dtype != torch.float64 or not a.is_contiguous():
+            raise TypeError("engine buffers must be contiguous float64 tensors")
+        return a.data_ptr(), (DFEM_MEM_DEVICE if a.is_cuda else DFEM_MEM_HOST), a
+    arr = np.ascontiguousarray(a, dtype=np.float64)
+    return arr.ctypes.data, DFEM_MEM_HOST, arr
+
+
+class Scene:
+    """One simulated world on one GPU (an opaque ``dfem_scene``)."""
+
+    def __init__(self, desc, device: int = 0):
+        self.desc = desc
+        cdesc, keep = desc.to_c()
+        h = C.c_void_p()
+        check(lib().dfem_scene_create(C.byref(cdesc), int(device), C.byref(h)))
+        self._h = h
+        self.device = device
+        self.N = desc.n_vertices
+        self.T = desc.n_tets
+        self.nseg = int(desc.n_segments)
+        self._last_steps = 0
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().dfem_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> dict:
+        inf = _capi.SceneInfoC()
+        check(lib().dfem_scene_get_info(self._h, C.byref(inf)))
+        return {name: getattr(inf, name) for name, _ in inf._fields_}
+
+    def set_materials(self, youngs, poisson):
+        pe, me, ke = _ptr(youngs)
+        pn, mn, kn = _ptr(poisson)
+        if me != mn:
+            raise ValueError("youngs and poisson must live in the same memory")
+        check(lib().dfem_set_materials(self._h, pe, pn, me))
+
+    def set_activations(self, act):
+        p, m, k = _ptr(act)
+        check(lib().dfem_set_activations(self._h, p, m))
+
+    def forward(self, x, v, n_steps: int = 1, act=None, traj: bool = False):
+        """Run n_steps steps from (x, v).  Returns (x_out, v_out[, traj]) in the
+        input's memory kind (numpy for host input, CUDA tensors for device input)."""
+        dev = _is_cuda_tensor(x)
+        n3 = 3 * self.N
+        if dev:
+            xo = torch.empty(n3, dtype=torch.float64, device=x.device)
+            vo = torch.empty_like(xo)
+            tr = torch.empty((n_steps, n3), dtype=torch.float64, device=x.device) if traj else None
+        else:
+            xo, vo = np.empty(n3), np.empty(n3)
+            tr = np.empty((n_steps, n3)) if traj else None
+        px, mx, kx = _ptr(x)
+        pv, mv, kv = _ptr(v)
+        pa, ma, ka = _ptr(act)
+        pxo, _, _ = _ptr(xo)
+        pvo, _, _ = _ptr(vo)
+        ptr_, _, _ = _ptr(tr)
+        if mx != mv or (ma is not None and ma != mx):
+            raise ValueError("x, v and act must live in the same memory")
+        check(lib().dfem_step_forward(self._h, px, pv, pa, int(n_steps), pxo, pvo, ptr_, mx))
+        self._last_steps = n_steps
+        return (xo, vo, tr) if traj else (xo, vo)
+
+    def backward(self, gx, gv):
+        """VJP of the last forward call.  Returns dict with x, v, E, nu, act."""
+        dev = _is_cuda_tensor(gx)
+        n3 = 3 * self.N
+        if dev:
+            mk = lambda *s: torch.empty(*s, dtype=torch.float64, device=gx.device)
+        else:
+            mk = lambda *s: np.empty(s if len(s) > 1 else s[0])
+        ox, ov = mk(n3), mk(n3)
+        gE, gnu = mk(max(1, self.T)), mk(max(1, self.T))
+        ga = mk(max(1, self._last_steps * self.nseg))
+        p = [_ptr(a)[0] for a in (gx, gv, ox, ov, gE, gnu, ga)]
+        mem = _ptr(gx)[1]
+        check(lib().dfem_step_backward(self._h, p[0], p[1], p[2], p[3], p[4], p[5], p[6] if self.nseg else None, mem))
+        act = ga[: self._last_steps * self.nseg]
+        act = act.reshape(self._last_steps, self.nseg)
+        return {"x": ox, "v": ov, "E": gE[: self.T], "nu": gnu[: self.T], "act": act}
+
+    def iterations(self, n: Optional[int] = None) -> np.ndarray:
+        n = self._last_steps if n is None else n
+        out = np.zeros(n, np.int32)
+        check(lib().dfem_get_iterations(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)), int(n)))
+        return out
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        check(lib().dfem_get_launch_count(self._h, C.byref(n)))
+        return int(n.value)
+
+    def profile_phases(self, reps: int = 20) -> dict:
+        ms = (C.c_double * 4)()
+        check(lib().dfem_profile_phases(self._h, int(reps), ms))
+        return {"local": ms[0], "gather": ms[1], "solve": ms[2], "adj_local": ms[3]}
+
+    def synchronize(self):
+        check(lib().dfem_synchronize(self._h))
+
+
+def host_factor_solve(desc, b) -> tuple:
+    """Host-only diagnostic: solve Hs X = B with the engine's own ordering and
+    supernodal factor (no GPU).  Returns (X (3N,), info dict)."""
+    cdesc, keep = desc.to_c()
+    b = np.ascontiguousarray(b, np.float64).reshape(-1)
+    x = np.empty_like(b)
+    inf = _capi.SceneInfoC()
+    check(lib().dfem_host_factor_solve(C.byref(cdesc), b.ctypes.data, x.ctypes.data, C.byref(inf)))
+    return x, {name: getattr(inf, name) for name, _ in inf._fields_}

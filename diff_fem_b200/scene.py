@@ -1,0 +1,349 @@
+"""Scene descriptors and builders (host side, setup time).
+
+A :class:`SceneDesc` holds plain numpy arrays that map one-to-one onto the
+C-ABI ``dfem_scene_desc`` (include/dfem.h).  The builders here generate the
+synthetic workloads (cube-grid beams, the muscle star, cloth) and apply the
+reference's setup rules where the engine expects precomputed inputs:
+
+* tet meshes of regular cube grids, 5 tets per cube with alternating parity so
+  neighbouring cubes share conforming faces;
+* lumped masses as in diff_fem ``Dfobj::Initialize`` (sim/Dfobj.h:506-525):
+  with "Is Mass Same" each vertex gets ``Mass / totvol * sum(vol/4)`` of its
+  tets, otherwise ``Mass / N``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+from ._capi import DFEM_PREC_FP64, SceneDescC
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+
+
+@dataclass
+class SceneDesc:
+    x0: np.ndarray                       # (N, 3)
+    mass: np.ndarray                     # (N,)
+    tets: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.int32))
+    youngs: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    poisson: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    gravity_mask: Optional[np.ndarray] = None
+    attach_vertex: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    attach_target: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    attach_stiffness: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    muscle_tets: np.ndarray = field(default_factory=lambda: np.zeros((0, 4), np.int32))
+    muscle_fiber: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    muscle_stiffness: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    muscle_segment: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    n_segments: int = 0
+    spring_vertices: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
+    spring_rest: Optional[np.ndarray] = None
+    spring_weight: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    bend_offsets: np.ndarray = field(default_factory=lambda: np.zeros(1, np.int32))
+    bend_vertices: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    bend_weight: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    contact_vertices: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    contact_faces: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    obstacle_x: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    obstacle_faces: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    time_step: float = 0.01
+    max_iterations: int = 10
+    damping: float = 0.9999
+    gravity: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    handle_collision: bool = False
+    self_collision: bool = False
+    alpha: float = 1.0
+    friction: float = 1.0
+    obstacle_friction: float = 1.0
+    precision: int = DFEM_PREC_FP64
+    checkpoint_every: int = 1
+    name: str = "scene"
+
+    @property
+    def n_vertices(self) -> int:
+        return int(np.asarray(self.x0).reshape(-1, 3).shape[0])
+
+    @property
+    def n_tets(self) -> int:
+        return int(np.asarray(self.tets).reshape(-1, 4).shape[0])
+
+    def to_c(self) -> Tuple[SceneDescC, list]:
+        """ctypes struct + the arrays it points into (keep them alive)."""
+        keep: list = []
+
+        def P(arr, conv, ctype):
+            if arr is None:
+                return None
+            a = conv(arr).reshape(-1)
+            keep.append(a)
+            if a.size == 0:
+                return None
+            return a.ctypes.data_as(C.POINTER(ctype))
+
+        d = SceneDescC()
+        x0 = _f64(self.x0).reshape(-1, 3)
+        d.n_vertices = x0.shape[0]
+        d.x0 = P(x0, _f64, C.c_double)
+        d.mass = P(self.mass, _f64, C.c_double)
+        d.gravity_mask = (P(np.asarray(self.gravity_mask, np.uint8), lambda a: np.ascontiguousarray(a, np.uint8), C.c_uint8)
+                          if self.gravity_mask is not None else None)
+        d.n_tets = self.n_tets
+        d.tets = P(self.tets, _i32, C.c_int32)
+        d.youngs = P(self.youngs, _f64, C.c_double)
+        d.poisson = P(self.poisson, _f64, C.c_double)
+        d.n_attach = int(np.asarray(self.attach_vertex).size)
+        d.attach_vertex = P(self.attach_vertex, _i32, C.c_int32)
+        d.attach_target = P(self.attach_target, _f64, C.c_double)
+        d.attach_stiffness = P(self.attach_stiffness, _f64, C.c_double)
+        d.n_muscle = int(np.asarray(self.muscle_segment).size)
+        d.muscle_tets = P(self.muscle_tets, _i32, C.c_int32)
+        d.muscle_fiber = P(self.muscle_fiber, _f64, C.c_double)
+        d.muscle_stiffness = P(self.muscle_stiffness, _f64, C.c_double)
+        d.muscle_segment = P(self.muscle_segment, _i32, C.c_int32)
+        d.n_segments = int(self.n_segments)
+        d.n_springs = int(np.asarray(self.spring_weight).size)
+        d.spring_vertices = P(self.spring_vertices, _i32, C.c_int32)
+        d.spring_rest = P(self.spring_rest, _f64, C.c_double)
+        d.spring_weight = P(self.spring_weight, _f64, C.c_double)
+        d.n_bending = int(np.asarray(self.bend_weight).size)
+        d.bend_offsets = P(self.bend_offsets, _i32, C.c_int32)
+        d.bend_vertices = P(self.bend_vertices, _i32, C.c_int32)
+        d.bend_weight = P(self.bend_weight, _f64, C.c_double)
+        d.n_contact_vertices = int(np.asarray(self.contact_vertices).size)
+        d.contact_vertices = P(self.contact_vertices, _i32, C.c_int32)
+        d.n_contact_faces = int(np.asarray(self.contact_faces).reshape(-1, 3).shape[0])
+        d.contact_faces = P(self.contact_faces, _i32, C.c_int32)
+        d.n_obstacle_vertices = int(np.asarray(self.obstacle_x).reshape(-1, 3).shape[0])
+        d.obstacle_x = P(self.obstacle_x, _f64, C.c_double)
+        d.n_obstacle_faces = int(np.asarray(self.obstacle_faces).reshape(-1, 3).shape[0])
+        d.obstacle_faces = P(self.obstacle_faces, _i32, C.c_int32)
+        d.time_step = float(self.time_step)
+        d.max_iterations = int(self.max_iterations)
+        d.damping = float(self.damping)
+        for c in range(3):
+            d.gravity[c] = float(self.gravity[c])
+        d.handle_collision = int(bool(self.handle_collision))
+        d.self_collision = int(bool(self.self_collision))
+        d.alpha = float(self.alpha)
+        d.friction = float(self.friction)
+        d.obstacle_friction = float(self.obstacle_friction)
+        d.precision = int(self.precision)
+        d.checkpoint_every = int(self.checkpoint_every)
+        return d, keep
+
+
+# ------------------------------------------------------------------ meshes ---
+
+# 5-tet split of the unit cube; corners indexed by (i, j, k) bits.  Parity 0
+# keeps the even corners as the central tet, parity 1 the odd ones, so that
+# neighbouring cubes of alternating parity cut shared faces along the same diagonal.
+_EVEN = [(0, 0, 0), (1, 1, 0), (1, 0, 1), (0, 1, 1)]
+_ODD = [(1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 1)]
+
+
+def _five_tets(parity: int):
+    central, corners = (_EVEN, _ODD) if parity == 0 else (_ODD, _EVEN)
+    tets = [list(central)]
+    for c in corners:
+        nb = [q for q in central if sum(abs(a - b) for a, b in zip(q, c)) == 1]
+        tets.append([c] + nb)
+    return tets
+
+
+def cube_grid(nx: int, ny: int, nz: int, edge: float, origin=(0.0, 0.0, 0.0),
+              edge_xyz: Optional[Tuple[float, float, float]] = None):
+    """Vertices (N,3) and tets (T,4) of an nx x ny x nz grid of cubes, 5 tets each."""
+    ex, ey, ez = edge_xyz if edge_xyz is not None else (edge, edge, edge)
+    vid = lambda i, j, k: (i * (ny + 1) + j) * (nz + 1) + k
+    ii, jj, kk = np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1), indexing="ij")
+    x0 = np.stack([ii.ravel() * ex, jj.ravel() * ey, kk.ravel() * ez], axis=1) + np.asarray(origin, np.float64)
+    pat = [_five_tets(0), _five_tets(1)]
+    tets = []
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                for tet in pat[(i + j + k) & 1]:
+                    tets.append([vid(i + a, j + b, k + c) for (a, b, c) in tet])
+    return x0, np.asarray(tets, dtype=np.int32)
+
+
+def tet_volumes(x0: np.ndarray, tets: np.ndarray) -> np.ndarray:
+    p = x0[tets]
+    return np.abs(np.einsum("ij,ij->i", p[:, 1] - p[:, 0], np.cross(p[:, 2] - p[:, 0], p[:, 3] - p[:, 0]))) / 6.0
+
+
+def lumped_masses(x0: np.ndarray, tets: np.ndarray, total_mass: float, is_mass_same: bool = True) -> np.ndarray:
+    """diff_fem Dfobj::Initialize mass rule (sim/Dfobj.h:506-525)."""
+    n = x0.shape[0]
+    if not is_mass_same:
+        return np.full(n, total_mass / n)
+    vol = tet_volumes(x0, tets)
+    m = np.zeros(n)
+    np.add.at(m, tets.reshape(-1), np.repeat(0.25 * vol, 4))
+    return total_mass / vol.sum() * m
+
+
+# --------------------------------------------------------------- workloads ---
+
+def cantilever(precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Cantilever beam: 10x4x4 cubes of 0.05 m (275 vertices, 800 tets),
+    E = 1e5 Pa, nu = 0.3, 1000 kg/m^3 (20 kg, volume-lumped), x = 0 face pinned
+    (25 attachments, k = 1e10), gravity -9.8, h = 1/60, 10 iterations."""
+    x0, tets = cube_grid(10, 4, 4, 0.05)
+    mass = lumped_masses(x0, tets, 1000.0 * 0.5 * 0.2 * 0.2, True)
+    pins = np.nonzero(np.isclose(x0[:, 0], 0.0))[0].astype(np.int32)
+    T = tets.shape[0]
+    return SceneDesc(
+        x0=x0, mass=mass, tets=tets, youngs=np.full(T, 1e5), poisson=np.full(T, 0.3),
+        attach_vertex=pins, attach_target=x0[pins], attach_stiffness=np.full(pins.size, 1e10),
+        time_step=1.0 / 60.0, max_iterations=10, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name="cantilever_10x4x4",
+    )
+
+
+def log_uniform_moduli(n: int, seed: int, lo: float = 1e4, hi: float = 1e6) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return 10.0 ** rng.uniform(np.log10(lo), np.log10(hi), size=n)
+
+
+def inverse_stiffness(nx: int = 40, ny: int = 8, nz: int = 8, seed: int = 1234,
+                      precision: int = DFEM_PREC_FP64, max_iterations: int = 20) -> SceneDesc:
+    """Inverse-stiffness beam: nx x ny x nz cubes of 0.05 m (default 41x9x9 =
+    3,321 vertices, 12,800 tets), per-tet E log-uniform in [1e4, 1e6] Pa from
+    `seed`, nu = 0.3, 1000 kg/m^3, both x ends pinned (k = 1e10), gravity,
+    h = 1/100, 20 iterations."""
+    x0, tets = cube_grid(nx, ny, nz, 0.05)
+    mass = lumped_masses(x0, tets, 1000.0 * nx * ny * nz * 0.05 ** 3, True)
+    xmax = x0[:, 0].max()
+    pins = np.nonzero(np.isclose(x0[:, 0], 0.0) | np.isclose(x0[:, 0], xmax))[0].astype(np.int32)
+    T = tets.shape[0]
+    return SceneDesc(
+        x0=x0, mass=mass, tets=tets, youngs=log_uniform_moduli(T, seed), poisson=np.full(T, 0.3),
+        attach_vertex=pins, attach_target=x0[pins], attach_stiffness=np.full(pins.size, 1e10),
+        time_step=1.0 / 100.0, max_iterations=max_iterations, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name=f"inverse_stiffness_{nx}x{ny}x{nz}",
+    )
+
+
+# ------------------------------------------------------------------ muscles ---
+
+def _point_segment_distance(p: np.ndarray, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    ab = b - a
+    t = np.clip(((p - a) @ ab) / max(ab @ ab, 1e-300), 0.0, 1.0)
+    return np.linalg.norm(p - (a + t[:, None] * ab), axis=1)
+
+
+def muscle_constraints(x0: np.ndarray, tets: np.ndarray, segments, stiffness: float,
+                       weight_scale: float = 0.005, radius: Optional[float] = None):
+    """Muscle constraints for fibre segments [(start, end), ...] following the
+    rule of diff_fem ``Muscle::Initialize`` (sim/Muscle.h:109-215): every tet the
+    segment passes through, or whose centre lies close enough that
+    w = exp(-dist / 0.005) > 0.2, gets a LinearMuscleConstraint with fibre
+    direction (end - start)/|end - start| and stiffness k_m * w.  Here "passes
+    through" is taken as: centre within `radius` (default: half the mean edge)
+    of the segment.  Returns (tets, fibres, stiffness, segment ids)."""
+    centers = x0[tets].mean(axis=1)
+    if radius is None:
+        e = np.linalg.norm(x0[tets[:, 1]] - x0[tets[:, 0]], axis=1).mean()
+        radius = 0.5 * e
+    mt, mf, mk, ms = [], [], [], []
+    for q, (a, b) in enumerate(segments):
+        a = np.asarray(a, np.float64)
+        b = np.asarray(b, np.float64)
+        f = (b - a) / np.linalg.norm(b - a)
+        dist = _point_segment_distance(centers, a, b)
+        w = np.exp(-np.abs(dist) / weight_scale)
+        sel = np.nonzero((dist < radius) | (w > 0.2))[0]
+        for t in sel:
+            mt.append(tets[t]); mf.append(f); mk.append(stiffness * max(w[t], 1e-3)); ms.append(q)
+    if not mt:
+        return (np.zeros((0, 4), np.int32), np.zeros((0, 3)), np.zeros(0), np.zeros(0, np.int32))
+    return (np.asarray(mt, np.int32), np.asarray(mf), np.asarray(mk), np.asarray(ms, np.int32))
+
+
+def muscle_beam(nx: int = 8, ny: int = 3, nz: int = 3, n_chains: int = 2, n_seg: int = 3,
+                stiffness: float = 5e3, precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Small muscle-driven beam (parity cases): fibre chains along x, left end pinned."""
+    edge = 0.05
+    x0, tets = cube_grid(nx, ny, nz, edge)
+    mass = lumped_masses(x0, tets, 1000.0 * nx * ny * nz * edge ** 3, True)
+    L = nx * edge
+    segs = []
+    for c in range(n_chains):
+        y = edge * (0.5 + (c % ny)) if ny > 1 else 0.5 * edge
+        z = edge * (0.5 + ((c // ny) % nz)) if nz > 1 else 0.5 * edge
+        for s in range(n_seg):
+            segs.append(((L * s / n_seg, y, z), (L * (s + 1) / n_seg, y, z)))
+    mt, mf, mk, ms = muscle_constraints(x0, tets, segs, stiffness)
+    pins = np.nonzero(np.isclose(x0[:, 0], 0.0))[0].astype(np.int32)
+    T = tets.shape[0]
+    return SceneDesc(
+        x0=x0, mass=mass, tets=tets, youngs=np.full(T, 5e4), poisson=np.full(T, 0.3),
+        attach_vertex=pins, attach_target=x0[pins], attach_stiffness=np.full(pins.size, 1e8),
+        muscle_tets=mt, muscle_fiber=mf, muscle_stiffness=mk, muscle_segment=ms, n_segments=len(segs),
+        time_step=1.0 / 60.0, max_iterations=15, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name=f"muscle_beam_{nx}x{ny}x{nz}",
+    )
+
+
+# -------------------------------------------------------------------- cloth ---
+
+def cloth_grid(nv_x: int, nv_z: int, edge: float, origin=(0.0, 0.0, 0.0)):
+    """Flat cloth in the xz plane: (nv_x * nv_z) vertices, two triangles per quad
+    (diagonal (i,j)-(i+1,j+1)), springs on every edge, bending stencils on every
+    interior vertex (centre + 6-ring in cyclic order).  Returns
+    (x0, triangles, springs, bend_offsets, bend_vertices)."""
+    vid = lambda i, j: i * nv_z + j
+    ii, jj = np.meshgrid(np.arange(nv_x), np.arange(nv_z), indexing="ij")
+    x0 = np.stack([ii.ravel() * edge, np.zeros(ii.size), jj.ravel() * edge], axis=1) + np.asarray(origin, np.float64)
+    tris, springs = [], set()
+    for i in range(nv_x - 1):
+        for j in range(nv_z - 1):
+            a, b, c, d = vid(i, j), vid(i + 1, j), vid(i + 1, j + 1), vid(i, j + 1)
+            tris.append((a, b, c)); tris.append((a, c, d))
+            for e in ((a, b), (b, c), (a, c), (c, d), (d, a)):
+                springs.add((min(e), max(e)))
+    boff, bvert = [0], []
+    for i in range(1, nv_x - 1):
+        for j in range(1, nv_z - 1):
+            ring = [vid(i + 1, j), vid(i + 1, j + 1), vid(i, j + 1), vid(i - 1, j), vid(i - 1, j - 1), vid(i, j - 1)]
+            bvert.extend([vid(i, j)] + ring)
+            boff.append(len(bvert))
+    return (x0, np.asarray(tris, np.int32), np.asarray(sorted(springs), np.int32),
+            np.asarray(boff, np.int32), np.asarray(bvert, np.int32))
+
+
+def triangle_masses(x0: np.ndarray, tris: np.ndarray, density: float) -> np.ndarray:
+    """Area-lumped cloth masses: each vertex gets density * area / 3 of its
+    triangles (diff_fem Dfcloth::Initialize + CollisionMesh::getTriangleMass)."""
+    p = x0[tris]
+    area = 0.5 * np.linalg.norm(np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), axis=1)
+    m = np.zeros(x0.shape[0])
+    np.add.at(m, tris.reshape(-1), np.repeat(density * area / 3.0, 3))
+    return m
+
+
+def cloth_sheet(nv: int = 8, edge: float = 0.02, stretch: float = 200.0, bend: float = 1e-3,
+                density: float = 1.5, pin_corners: bool = True, precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Small hanging cloth (parity cases): springs + bending, two corners pinned."""
+    x0, tris, springs, boff, bvert = cloth_grid(nv, nv, edge)
+    mass = triangle_masses(x0, tris, density)
+    pins = np.asarray([0, (nv - 1) * nv], np.int32) if pin_corners else np.zeros(0, np.int32)
+    return SceneDesc(
+        x0=x0, mass=mass, spring_vertices=springs, spring_weight=np.full(len(springs), stretch),
+        bend_offsets=boff, bend_vertices=bvert, bend_weight=np.full(len(boff) - 1, bend),
+        attach_vertex=pins, attach_target=x0[pins], attach_stiffness=np.full(pins.size, 1e5),
+        contact_faces=tris,
+        time_step=1.0 / 120.0, max_iterations=20, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name=f"cloth_{nv}x{nv}",
+    )

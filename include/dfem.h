@@ -1,0 +1,202 @@
+/*
+ * dfem.h — C ABI of the B200 projective-dynamics (PD) engine.
+ *
+ * This is the drop-in boundary for the hot path of diff_fem: one time step of
+ * local–global projective dynamics (corotated FEM tets, muscle segments,
+ * attachments, cloth strain/bending springs, obstacle contact with friction)
+ * and the vector–Jacobian product (VJP) of that step.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (DFEM_OK == 0).  On failure the
+ *    message is available from dfem_last_error() (thread-local).
+ *  - All buffers are caller-owned.  Positions/velocities are interleaved FP64
+ *    [x0 y0 z0 x1 y1 z1 ...] of length 3N, ordered as the scene descriptor
+ *    lists its vertices (diff_fem: Meshes, then Clothes; obstacles excluded).
+ *  - `mem` arguments say where a buffer lives: DFEM_MEM_HOST or DFEM_MEM_DEVICE
+ *    (a pointer on the scene's CUDA device).
+ *  - One CUDA stream per scene; no process-wide mutable state apart from the
+ *    thread-local error string.
+ *
+ * The reference interface each entry point replaces is cited beside it
+ * (paths relative to the diff_fem repository).
+ */
+#ifndef DFEM_H_
+#define DFEM_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DFEM_ABI_VERSION 1
+
+enum dfem_status {
+  DFEM_OK = 0,
+  DFEM_ERR_INVALID = 1,       /* bad argument / descriptor                       */
+  DFEM_ERR_CUDA = 2,          /* CUDA runtime error                              */
+  DFEM_ERR_FACTOR = 3,        /* Cholesky failed even after regularisation      */
+  DFEM_ERR_NONFINITE = 4,     /* NaN/Inf met in a step (status word set on GPU)  */
+  DFEM_ERR_STATE = 5,         /* call out of order (e.g. backward before forward)*/
+  DFEM_ERR_CAP = 6,           /* a bounded loop hit its cap (contact passes)     */
+  DFEM_ERR_NOMEM = 7          /* allocation failed                               */
+};
+
+enum dfem_mem { DFEM_MEM_HOST = 0, DFEM_MEM_DEVICE = 1 };
+
+enum dfem_precision {
+  DFEM_PREC_FP64 = 0,   /* plain form: everything FP64                          */
+  DFEM_PREC_MIXED = 1   /* FP32 projections/contact, FP64 factor + residual     */
+};
+
+/*
+ * Scene descriptor: plain arrays, read once by dfem_scene_create.
+ * Replaces the scene assembly of Environment::Environment / Dfobj::Initialize /
+ * Dfcloth::Initialize / World::AddBody / World::Initialize
+ * (sim/Environment.h:86-225, sim/Dfobj.h:442-611, sim/Dfcloth.h:198-300,
+ *  sim/fem/World.h:248-591).  Optional arrays may be NULL when their count is 0.
+ */
+typedef struct dfem_scene_desc {
+  /* vertices */
+  int32_t n_vertices;
+  const double *x0;            /* 3N rest positions                                  */
+  const double *mass;          /* N lumped masses (World::mUnitMass)                 */
+  const uint8_t *gravity_mask; /* N flags: 1 = vertex receives gravity (NULL = all)  */
+
+  /* corotated FEM tets (CorotateFEMConstraint) */
+  int32_t n_tets;
+  const int32_t *tets;         /* 4T vertex indices (re-oriented like Dfobj.h:474-487)*/
+  const double *youngs;        /* T Young's moduli E                                  */
+  const double *poisson;       /* T Poisson ratios nu                                 */
+
+  /* attachments (AttachmentConstraint) */
+  int32_t n_attach;
+  const int32_t *attach_vertex;   /* n_attach                                       */
+  const double *attach_target;    /* 3*n_attach target points                        */
+  const double *attach_stiffness; /* n_attach                                        */
+
+  /* muscle constraints (LinearMuscleConstraint), grouped into segments */
+  int32_t n_muscle;
+  const int32_t *muscle_tets;     /* 4*n_muscle                                      */
+  const double *muscle_fiber;     /* 3*n_muscle unit fibre directions                */
+  const double *muscle_stiffness; /* n_muscle: muscle stiffness x distance weight    */
+  const int32_t *muscle_segment;  /* n_muscle segment ids in [0, n_segments)         */
+  int32_t n_segments;
+
+  /* cloth strain springs (SpringConstraint) */
+  int32_t n_springs;
+  const int32_t *spring_vertices; /* 2*n_springs                                     */
+  const double *spring_rest;      /* n_springs rest lengths (NULL = from x0)         */
+  const double *spring_weight;    /* n_springs weights w (J and L use sqrt(w))       */
+
+  /* cloth bending stencils (BendingConstraint): centre vertex then 1-ring in order */
+  int32_t n_bending;
+  const int32_t *bend_offsets;    /* n_bending+1 offsets into bend_vertices          */
+  const int32_t *bend_vertices;   /* centre first, then the ring (>= 3 vertices)     */
+  const double *bend_weight;      /* n_bending weights                               */
+
+  /* contact: soft surface (vertices + faces, global vertex ids) and obstacles */
+  int32_t n_contact_vertices;
+  const int32_t *contact_vertices;
+  int32_t n_contact_faces;
+  const int32_t *contact_faces;   /* 3 per face, global vertex ids                   */
+  int32_t n_obstacle_vertices;
+  const double *obstacle_x;       /* 3 per obstacle vertex (static)                  */
+  int32_t n_obstacle_faces;
+  const int32_t *obstacle_faces;  /* 3 per face, obstacle vertex ids                 */
+
+  /* parameters (Environment.h:108-155, World.h:216-235) */
+  double time_step;               /* h = 1 / "Simulation HZ"                         */
+  int32_t max_iterations;         /* "Max Iteration" K                               */
+  double damping;                 /* "Damping coefficient"                           */
+  double gravity[3];
+  int32_t handle_collision;       /* "Handle collision"                              */
+  int32_t self_collision;         /* "Self-collision"                                */
+  double alpha;                   /* "World Alpha" relaxation of the contact rhs     */
+  double friction;                /* "World Friction" (soft-soft contact mu)         */
+  double obstacle_friction;       /* obstacle mu (diff_fem hardcodes 1)              */
+  int32_t precision;              /* enum dfem_precision                             */
+  int32_t checkpoint_every;       /* adjoint checkpoint interval in steps (>= 1)     */
+} dfem_scene_desc;
+
+typedef struct dfem_scene dfem_scene;  /* opaque */
+
+typedef struct dfem_scene_info {
+  int32_t n_vertices, n_tets, n_attach, n_muscle, n_springs, n_bending;
+  int32_t n_supernodes, n_levels;      /* supernodal Cholesky of the N x N matrix Hs */
+  int64_t nnz_factor;                  /* stored entries of the Cholesky factor      */
+  int32_t n_slots;                     /* per-constraint vertex slots of J*d         */
+  int32_t device;
+  double factor_regularisation;        /* 0 unless the retry loop added reg * I      */
+} dfem_scene_info;
+
+/* Build a scene on `device`: precomputation of J, L, H = M/h^2 + L and its
+ * prefactorisation.  Replaces World::Initialize + World::PreComputation +
+ * World::FactorizeLDLT (sim/fem/World.h:248-384, 1089-1139, 1212-1232). */
+int dfem_scene_create(const dfem_scene_desc *desc, int device, dfem_scene **out);
+int dfem_scene_destroy(dfem_scene *scene);
+int dfem_scene_get_info(const dfem_scene *scene, dfem_scene_info *info);
+
+/* Per-tet materials; refactors H.  Replaces the COROTATE parameter update +
+ * PreComputation of forward_all (python/pydifem.cc:207-221). */
+int dfem_set_materials(dfem_scene *scene, const double *youngs, const double *poisson, int mem);
+
+/* Muscle activation per segment for the next forward call(s).  Replaces
+ * MuscleSegment::SetActivationLevel (sim/MuscleSegment.h:72-78). */
+int dfem_set_activations(dfem_scene *scene, const double *activations, int mem);
+
+/* Run n_steps time steps from (x, v); writes the final state, and optionally
+ * every step's positions to traj_x ((n_steps) * 3N, may be NULL).
+ * `activations`, if non-NULL, holds n_steps * n_segments values (one row per
+ * step) and overrides dfem_set_activations for this call.
+ * Records checkpoints so that dfem_step_backward can follow.
+ * Replaces Environment::Step + World::TimeStepping + ProjectiveDynamicsMethod
+ * (sim/Environment.h:228-293, sim/fem/World.h:673-1029) as driven by
+ * forward_act / forward_all (python/pydifem.cc:39-86, 183-259). */
+int dfem_step_forward(dfem_scene *scene, const double *x, const double *v,
+                      const double *activations, int32_t n_steps,
+                      double *x_out, double *v_out, double *traj_x, int mem);
+
+/* VJP of the last dfem_step_forward call: given dL/dx_out and dL/dv_out,
+ * writes dL/dx, dL/dv (3N each), dL/dE and dL/dnu per tet (may be NULL) and
+ * dL/dactivation (n_steps * n_segments, may be NULL).
+ * Replaces the CppAD tape + ADFun::Jacobian of backward_act / backward_all
+ * (python/pydifem.cc:91-180, 262-301). */
+int dfem_step_backward(dfem_scene *scene, const double *gx_out, const double *gv_out,
+                       double *gx, double *gv, double *g_youngs, double *g_poisson,
+                       double *g_activations, int mem);
+
+/* Iteration counts of the last forward call (n_steps values), host buffer. */
+int dfem_get_iterations(const dfem_scene *scene, int32_t *iters, int32_t n);
+
+/* Host-only diagnostic, needs no GPU: builds the scene's fill-reducing
+ * ordering and supernodal Cholesky factor of Hs = M/h^2 + L_s on the host and
+ * solves Hs X = B for 3 interleaved right-hand sides (3N, user vertex order).
+ * `info` (may be NULL) receives the factor statistics.  Same role as
+ * World::PreComputation + mDynamicSolver.solve (sim/fem/World.h:1089-1139,1660). */
+int dfem_host_factor_solve(const dfem_scene_desc *desc, const double *b, double *x, dfem_scene_info *info);
+
+/* Number of kernels this scene has launched so far (CUDA-graph nodes counted
+ * individually).  Instrumentation; no counterpart in the reference. */
+int dfem_get_launch_count(const dfem_scene *scene, int64_t *count);
+
+/* CUDA-event timing of the step's phases on the scene's stream, each phase
+ * launched `reps` times after one warm-up on the state of the last forward
+ * call: ms[0] local step (projection + J*d slots), ms[1] rhs gather,
+ * ms[2] one full triangular solve (all levels, both sweeps), ms[3] adjoint
+ * local step.  Instrumentation (diff_fem's TIMER_* macros, sim/utils/timer.h). */
+int dfem_profile_phases(dfem_scene *scene, int32_t reps, double *ms);
+
+/* Synchronise the scene's stream. */
+int dfem_synchronize(dfem_scene *scene);
+
+/* Last error message of the calling thread ("" if none). */
+const char *dfem_last_error(void);
+
+/* ABI version (DFEM_ABI_VERSION). */
+int dfem_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DFEM_H_ */

@@ -1,0 +1,996 @@
+/*
+ * pd_oracle.cpp — CPU FP64 restatement of diff_fem's projective-dynamics step
+ * and a hand-written adjoint of it.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker the CUDA engine is
+ * compared against; the product (diff_fem_b200) never links, imports or calls
+ * it.  Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
+ * --impl reference leg may load the oracle library.
+ *
+ * PARITY UNPINNED against the reference binary: diff_fem cannot be built or
+ * imported here (Eigen, CppAD, CGAL and Boost are absent and there is no
+ * network), and the reference ships no tests, golden vectors or fixtures with
+ * outputs.  This restatement is pinned instead by known-answer invariants,
+ * central finite differences of its adjoint, and the reference's own data
+ * scenes (tests/test_oracle.py).
+ *
+ * What it restates (paths relative to the diff_fem repository):
+ *   - World::TimeStepping / UpdatePositionsAndVelocities   sim/fem/World.h:673-720,757-766
+ *   - World::ProjectiveDynamicsMethod main loop           sim/fem/World.h:835-917
+ *   - World::ComputeSolution (no-bones branch)            sim/fem/World.h:1601-1670
+ *   - World::PreComputation / FactorizeLDLT (retry)       sim/fem/World.h:1089-1139,1212-1232
+ *   - CorotateFEMConstraint (F, SVD, reflection, volume)   sim/fem/Constraint/CorotateFEMConstraint.h:64-392
+ *   - LinearMuscleConstraint                              sim/fem/Constraint/LinearMuscleConstraint.h:91-270
+ *   - AttachmentConstraint                                sim/fem/Constraint/AttachmentConstraint.h:70-99
+ *   - SpringConstraint                                    sim/fem/Constraint/SpringConstraint.h:51-144
+ *   - BendingConstraint                                   sim/fem/Constraint/BendingConstraint.h:66-187,220-300
+ *   - Environment::Step gravity                           sim/Environment.h:228-259
+ *   - Dfobj::Initialize tet re-orientation and masses     sim/Dfobj.h:442-525
+ *
+ * Choices that differ in mechanism but not in result:
+ *   - The 3N x 3N H of the reference is kron(Hs, I3); the oracle factors the
+ *     scalar N x N Hs (envelope Cholesky after reverse Cuthill–McKee) and
+ *     solves 3 right-hand sides.  orc_full_L_triplets() rebuilds the
+ *     reference's 3N x 3N triplets so a test can check the kron identity.
+ *   - 3x3 SVD: one-sided Jacobi on F (Hestenes), singular values >= 0 like
+ *     Eigen::JacobiSVD.  R = U V^T and U diag(g(S)) V^T do not depend on the
+ *     SVD's sign/permutation choices, so any exact SVD gives the same d.
+ */
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <queue>
+#include <string>
+#include <vector>
+#include <thread>
+
+#include "../include/dfem.h"
+
+namespace orc {
+
+struct V3 { double x, y, z; };
+static inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline V3 operator*(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+static inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+static inline double norm(V3 a) { return std::sqrt(dot(a, a)); }
+
+/* column-major 3x3: m[c][r] is row r of column c */
+struct M3 { double m[3][3]; };
+static inline double& at(M3& a, int r, int c) { return a.m[c][r]; }
+static inline double at(const M3& a, int r, int c) { return a.m[c][r]; }
+static M3 mul(const M3& a, const M3& b) {
+  M3 o{};
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += at(a, r, k) * at(b, k, c);
+      at(o, r, c) = s;
+    }
+  return o;
+}
+static M3 mulT(const M3& a, const M3& b) { /* a * b^T */
+  M3 o{};
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += at(a, r, k) * at(b, c, k);
+      at(o, r, c) = s;
+    }
+  return o;
+}
+static M3 Tmul(const M3& a, const M3& b) { /* a^T * b */
+  M3 o{};
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += at(a, k, r) * at(b, k, c);
+      at(o, r, c) = s;
+    }
+  return o;
+}
+static double det(const M3& a) {
+  return at(a, 0, 0) * (at(a, 1, 1) * at(a, 2, 2) - at(a, 1, 2) * at(a, 2, 1)) -
+         at(a, 0, 1) * (at(a, 1, 0) * at(a, 2, 2) - at(a, 1, 2) * at(a, 2, 0)) +
+         at(a, 0, 2) * (at(a, 1, 0) * at(a, 2, 1) - at(a, 1, 1) * at(a, 2, 0));
+}
+static M3 inverse(const M3& a) {
+  double d = det(a);
+  M3 o{};
+  at(o, 0, 0) = (at(a, 1, 1) * at(a, 2, 2) - at(a, 1, 2) * at(a, 2, 1)) / d;
+  at(o, 0, 1) = (at(a, 0, 2) * at(a, 2, 1) - at(a, 0, 1) * at(a, 2, 2)) / d;
+  at(o, 0, 2) = (at(a, 0, 1) * at(a, 1, 2) - at(a, 0, 2) * at(a, 1, 1)) / d;
+  at(o, 1, 0) = (at(a, 1, 2) * at(a, 2, 0) - at(a, 1, 0) * at(a, 2, 2)) / d;
+  at(o, 1, 1) = (at(a, 0, 0) * at(a, 2, 2) - at(a, 0, 2) * at(a, 2, 0)) / d;
+  at(o, 1, 2) = (at(a, 0, 2) * at(a, 1, 0) - at(a, 0, 0) * at(a, 1, 2)) / d;
+  at(o, 2, 0) = (at(a, 1, 0) * at(a, 2, 1) - at(a, 1, 1) * at(a, 2, 0)) / d;
+  at(o, 2, 1) = (at(a, 0, 1) * at(a, 2, 0) - at(a, 0, 0) * at(a, 2, 1)) / d;
+  at(o, 2, 2) = (at(a, 0, 0) * at(a, 1, 1) - at(a, 0, 1) * at(a, 1, 0)) / d;
+  return o;
+}
+static inline V3 col(const M3& a, int c) { return {a.m[c][0], a.m[c][1], a.m[c][2]}; }
+static inline void setcol(M3& a, int c, V3 v) { a.m[c][0] = v.x; a.m[c][1] = v.y; a.m[c][2] = v.z; }
+
+/* ---- 3x3 SVD: one-sided (Hestenes) Jacobi on the columns of F ------------ */
+struct SVD3 { M3 U, V; double s[3]; };
+
+static SVD3 svd3(const M3& F) {
+  M3 B = F;
+  M3 V{};
+  at(V, 0, 0) = at(V, 1, 1) = at(V, 2, 2) = 1.0;
+  const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  for (int sweep = 0; sweep < 30; ++sweep) {
+    bool rotated = false;
+    for (auto& pq : pairs) {
+      int p = pq[0], q = pq[1];
+      V3 bp = col(B, p), bq = col(B, q);
+      double a = dot(bp, bp), b = dot(bq, bq), g = dot(bp, bq);
+      if (std::fabs(g) <= 1e-15 * std::sqrt(a * b) || g == 0.0) continue;
+      rotated = true;
+      double zeta = (b - a) / (2.0 * g);
+      double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+      double c = 1.0 / std::sqrt(1.0 + t * t), s = c * t;
+      setcol(B, p, c * bp - s * bq);
+      setcol(B, q, s * bp + c * bq);
+      V3 vp = col(V, p), vq = col(V, q);
+      setcol(V, p, c * vp - s * vq);
+      setcol(V, q, s * vp + c * vq);
+    }
+    if (!rotated) break;
+  }
+  SVD3 out;
+  double sig[3];
+  for (int i = 0; i < 3; ++i) sig[i] = norm(col(B, i));
+  int order[3] = {0, 1, 2};
+  std::sort(order, order + 3, [&](int i, int j) { return sig[i] > sig[j]; });
+  M3 Bs{}, Vs{};
+  for (int k = 0; k < 3; ++k) {
+    setcol(Bs, k, col(B, order[k]));
+    setcol(Vs, k, col(V, order[k]));
+    out.s[k] = sig[order[k]];
+  }
+  out.V = Vs;
+  const double tiny = 1e-300;
+  /* U columns: normalised B columns; a (near) zero singular value takes the
+     direction that completes an orthonormal basis. */
+  for (int k = 0; k < 3; ++k) {
+    if (out.s[k] > tiny && out.s[k] > 1e-14 * out.s[0]) {
+      setcol(out.U, k, (1.0 / out.s[k]) * col(Bs, k));
+    } else if (k == 2) {
+      setcol(out.U, 2, cross(col(out.U, 0), col(out.U, 1)));
+    } else {
+      V3 u0 = col(out.U, 0);
+      V3 e = std::fabs(u0.x) < 0.9 ? V3{1, 0, 0} : V3{0, 1, 0};
+      V3 u1 = cross(u0, e);
+      setcol(out.U, 1, (1.0 / norm(u1)) * u1);
+      setcol(out.U, 2, cross(u0, col(out.U, 1)));
+      break;
+    }
+  }
+  return out;
+}
+
+/* ---- the 5-step Newton projection of S onto prod = 1 ---------------------
+ * CorotateFEMConstraint.h:362-374.  Also returns, for the adjoint, the
+ * Jacobian dg/ds (forward mode) and the exact divided differences
+ * (g_i - g_j)/(s_i - s_j) via the recurrence r <- 1 - c * p_k * r. */
+struct VolProj { double g[3]; double J[3][3]; double dd[3]; /* pairs 01,02,12 */ };
+
+static VolProj volume_projection(const double s[3], bool want_derivs) {
+  double D[3] = {0, 0, 0};
+  double dD[3][3] = {{0}};      /* dD[i][dir] */
+  double r[3] = {1, 1, 1};      /* divided-difference ratios for pairs 01,02,12 */
+  const int pk[3] = {2, 1, 0};  /* third index of each pair */
+  for (int it = 0; it < 5; ++it) {
+    double p[3] = {s[0] + D[0], s[1] + D[1], s[2] + D[2]};
+    double CD = p[0] * p[1] * p[2] - 1.0;
+    double gr[3] = {p[1] * p[2], p[0] * p[2], p[0] * p[1]};
+    double gg = gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2];
+    double num = gr[0] * D[0] + gr[1] * D[1] + gr[2] * D[2] - CD;
+    double c = num / gg;
+    if (want_derivs) {
+      for (int q = 0; q < 3; ++q) r[q] = 1.0 - c * p[pk[q]] * r[q];
+      double ndD[3][3];
+      for (int dir = 0; dir < 3; ++dir) {
+        double dp[3];
+        for (int i = 0; i < 3; ++i) dp[i] = (i == dir ? 1.0 : 0.0) + dD[i][dir];
+        double dC = gr[0] * dp[0] + gr[1] * dp[1] + gr[2] * dp[2];
+        double dgr[3] = {dp[1] * p[2] + p[1] * dp[2], dp[0] * p[2] + p[0] * dp[2], dp[0] * p[1] + p[0] * dp[1]};
+        double dnum = dgr[0] * D[0] + dgr[1] * D[1] + dgr[2] * D[2] +
+                      gr[0] * dD[0][dir] + gr[1] * dD[1][dir] + gr[2] * dD[2][dir] - dC;
+        double dgg = 2.0 * (gr[0] * dgr[0] + gr[1] * dgr[1] + gr[2] * dgr[2]);
+        double dc = (dnum * gg - num * dgg) / (gg * gg);
+        for (int i = 0; i < 3; ++i) ndD[i][dir] = dc * gr[i] + c * dgr[i];
+      }
+      std::memcpy(dD, ndD, sizeof(dD));
+    }
+    for (int i = 0; i < 3; ++i) D[i] = c * gr[i];
+  }
+  VolProj o;
+  for (int i = 0; i < 3; ++i) {
+    o.g[i] = s[i] + D[i];
+    for (int j = 0; j < 3; ++j) o.J[i][j] = (i == j ? 1.0 : 0.0) + dD[i][j];
+  }
+  for (int q = 0; q < 3; ++q) o.dd[q] = r[q];
+  return o;
+}
+
+/* ---- scene ----------------------------------------------------------------- */
+struct Tet { int v[4]; M3 invDm; double vol; double G[4][3]; };
+
+static Tet make_tet(const double* x0, const int* idx) {
+  /* Dfobj.h:474-503: swap vertices 1 and 2 when det(Dm) < 0; vol = det/6. */
+  Tet t;
+  int i0 = idx[0], i1 = idx[1], i2 = idx[2], i3 = idx[3];
+  auto P = [&](int i) { return V3{x0[3 * i], x0[3 * i + 1], x0[3 * i + 2]}; };
+  M3 Dm{};
+  setcol(Dm, 0, P(i1) - P(i0));
+  setcol(Dm, 1, P(i2) - P(i0));
+  setcol(Dm, 2, P(i3) - P(i0));
+  if (det(Dm) < 0) {
+    std::swap(i1, i2);
+    setcol(Dm, 0, P(i1) - P(i0));
+    setcol(Dm, 1, P(i2) - P(i0));
+  }
+  t.v[0] = i0; t.v[1] = i1; t.v[2] = i2; t.v[3] = i3;
+  t.vol = det(Dm) / 6.0;
+  t.invDm = inverse(Dm);
+  /* Rows of the selection matrix A (CorotateFEMConstraint.h:236-245):
+     F(:,j) = sum_v G[v][j] x_v with G[0][j] = -sum_k invDm(k,j), G[k+1][j] = invDm(k,j). */
+  for (int j = 0; j < 3; ++j) {
+    double s = 0;
+    for (int k = 0; k < 3; ++k) { t.G[k + 1][j] = at(t.invDm, k, j); s += at(t.invDm, k, j); }
+    t.G[0][j] = -s;
+  }
+  return t;
+}
+
+struct Bend { std::vector<int> v; std::vector<double> beta; double rest_norm; double w; };
+
+static double bend_cos(V3 a, V3 b, V3 c) { V3 e1 = a - b, e2 = c - b; return dot(e1, e2) / (norm(e1) * norm(e2)); }
+static double bend_sin(V3 a, V3 b, V3 c) { V3 e1 = a - b, e2 = c - b; return norm(cross(e1, e2)) / (norm(e1) * norm(e2)); }
+static double mean_value(V3 a, V3 b, V3 c) {
+  double num = 1.0 - bend_cos(a, b, c);
+  if (num == 0) return 0;
+  return num / bend_sin(a, b, c);
+}
+
+struct Scene {
+  int N = 0;
+  std::vector<double> x0, mass, gmask;
+  std::vector<Tet> tets; std::vector<double> E, nu;
+  std::vector<int> att_v; std::vector<V3> att_p; std::vector<double> att_k;
+  std::vector<Tet> mtets; std::vector<V3> mfib; std::vector<double> mk; std::vector<int> mseg; int nseg = 0;
+  std::vector<double> seg_act;
+  std::vector<int> sp_v; std::vector<double> sp_rest, sp_w;
+  std::vector<Bend> bends;
+  double h = 0.01, damping = 1.0; int K = 10; V3 g{0, 0, 0};
+  /* envelope Cholesky of Hs in RCM order */
+  std::vector<int> perm, iperm;  /* perm[new] = old */
+  std::vector<int> first;        /* first column of row i in the envelope */
+  std::vector<int64_t> rowptr;   /* start of row i in env */
+  std::vector<double> env;
+  std::vector<std::vector<std::pair<int, double>>> Hrows; /* Hs rows (old numbering) */
+  double reg = 0.0;
+  std::string err;
+  /* recorded forward trajectory for the adjoint */
+  int rec_steps = 0;
+  std::vector<double> rec_x, rec_v;        /* step-start states */
+  std::vector<double> rec_act;             /* per step activations */
+  std::vector<int> rec_iters;
+};
+
+static void add_H(std::vector<std::vector<std::pair<int, double>>>& rows, int i, int j, double v) {
+  rows[i].push_back({j, v});
+}
+
+/* Hs = M/h^2 + L_s, with L = kron(L_s, I3) (World.h:1093-1098). */
+static void assemble_H(Scene& S) {
+  int N = S.N;
+  std::vector<std::vector<std::pair<int, double>>> rows(N);
+  double ih2 = 1.0 / (S.h * S.h);
+  for (int i = 0; i < N; ++i) add_H(rows, i, i, S.mass[i] * ih2);
+  for (size_t t = 0; t < S.tets.size(); ++t) {
+    const Tet& T = S.tets[t];
+    /* mu * vol * (1 + nu) * G G^T  (CorotateFEMConstraint.h:289-350: two blocks, the second scaled by nu) */
+    double mu = S.E[t] / (1.0 + S.nu[t]);
+    double w = mu * T.vol * (1.0 + S.nu[t]);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        double s = 0;
+        for (int j = 0; j < 3; ++j) s += T.G[a][j] * T.G[b][j];
+        add_H(rows, T.v[a], T.v[b], w * s);
+      }
+  }
+  for (size_t a = 0; a < S.att_v.size(); ++a) add_H(rows, S.att_v[a], S.att_v[a], S.att_k[a]);
+  for (size_t m = 0; m < S.mtets.size(); ++m) {
+    const Tet& T = S.mtets[m];
+    /* LinearMuscleConstraint.h:213-247: vol * k * A^T A with A = kron(c, I3), c = G f */
+    double c[4];
+    for (int v = 0; v < 4; ++v) c[v] = T.G[v][0] * S.mfib[m].x + T.G[v][1] * S.mfib[m].y + T.G[v][2] * S.mfib[m].z;
+    double w = T.vol * S.mk[m];
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) add_H(rows, T.v[a], T.v[b], w * c[a] * c[b]);
+  }
+  for (size_t s = 0; s < S.sp_w.size(); ++s) {
+    /* SpringConstraint.h:109: sqrt(w) * A^T A, A = [I, -I] */
+    double w = std::sqrt(S.sp_w[s]);
+    int i0 = S.sp_v[2 * s], i1 = S.sp_v[2 * s + 1];
+    add_H(rows, i0, i0, w); add_H(rows, i1, i1, w);
+    add_H(rows, i0, i1, -w); add_H(rows, i1, i0, -w);
+  }
+  for (const Bend& B : S.bends) {
+    /* BendingConstraint.h:139-160: mBend * A^T A with A = mBend * beta: w^3 beta beta^T */
+    double w3 = B.w * B.w * B.w;
+    for (size_t a = 0; a < B.v.size(); ++a)
+      for (size_t b = 0; b < B.v.size(); ++b) add_H(rows, B.v[a], B.v[b], w3 * B.beta[a] * B.beta[b]);
+  }
+  /* merge duplicates */
+  for (auto& r : rows) {
+    std::sort(r.begin(), r.end(), [](auto& a, auto& b) { return a.first < b.first; });
+    std::vector<std::pair<int, double>> m;
+    for (auto& e : r) {
+      if (!m.empty() && m.back().first == e.first) m.back().second += e.second;
+      else m.push_back(e);
+    }
+    r.swap(m);
+  }
+  S.Hrows.swap(rows);
+}
+
+static void rcm_order(Scene& S) {
+  int N = S.N;
+  std::vector<int> deg(N);
+  for (int i = 0; i < N; ++i) deg[i] = (int)S.Hrows[i].size();
+  std::vector<char> seen(N, 0);
+  std::vector<int> order;
+  order.reserve(N);
+  for (int start0 = 0; start0 < N; ++start0) {
+    if (seen[start0]) continue;
+    /* pseudo-peripheral start: a few BFS sweeps from the min-degree vertex of this component */
+    int start = start0;
+    for (int sweep = 0; sweep < 3; ++sweep) {
+      std::vector<int> lvl(N, -1);
+      std::queue<int> q; q.push(start); lvl[start] = 0; int last = start;
+      while (!q.empty()) {
+        int u = q.front(); q.pop(); last = u;
+        for (auto& e : S.Hrows[u]) if (lvl[e.first] < 0 && !seen[e.first]) { lvl[e.first] = lvl[u] + 1; q.push(e.first); }
+      }
+      start = last;
+    }
+    std::queue<int> q; q.push(start); seen[start] = 1;
+    while (!q.empty()) {
+      int u = q.front(); q.pop(); order.push_back(u);
+      std::vector<int> nb;
+      for (auto& e : S.Hrows[u]) if (!seen[e.first]) { seen[e.first] = 1; nb.push_back(e.first); }
+      std::sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] < deg[b] || (deg[a] == deg[b] && a < b); });
+      for (int v : nb) q.push(v);
+    }
+  }
+  std::reverse(order.begin(), order.end());
+  S.perm = order;
+  S.iperm.assign(N, 0);
+  for (int i = 0; i < N; ++i) S.iperm[order[i]] = i;
+}
+
+/* Envelope Cholesky with the regularise-and-retry loop of World::FactorizeLDLT
+ * (World.h:1219-1229; reg starts at 1e-5, x10, bounded here). */
+static bool factor(Scene& S) {
+  int N = S.N;
+  S.first.assign(N, 0);
+  for (int i = 0; i < N; ++i) {
+    int f = i;
+    for (auto& e : S.Hrows[S.perm[i]]) f = std::min(f, S.iperm[e.first]);
+    S.first[i] = f;
+  }
+  S.rowptr.assign(N + 1, 0);
+  for (int i = 0; i < N; ++i) S.rowptr[i + 1] = S.rowptr[i] + (i - S.first[i] + 1);
+  double reg = 0.0;
+  for (int attempt = 0; attempt < 25; ++attempt) {
+    S.env.assign(S.rowptr[N], 0.0);
+    for (int i = 0; i < N; ++i)
+      for (auto& e : S.Hrows[S.perm[i]]) {
+        int j = S.iperm[e.first];
+        if (j <= i) S.env[S.rowptr[i] + (j - S.first[i])] += e.second;
+      }
+    for (int i = 0; i < N; ++i) S.env[S.rowptr[i] + (i - S.first[i])] += reg;
+    bool ok = true;
+    for (int i = 0; i < N && ok; ++i) {
+      double* Li = &S.env[S.rowptr[i]];
+      int fi = S.first[i];
+      for (int j = fi; j < i; ++j) {
+        const double* Lj = &S.env[S.rowptr[j]];
+        int fj = S.first[j];
+        int k0 = std::max(fi, fj);
+        double s = Li[j - fi];
+        for (int k = k0; k < j; ++k) s -= Li[k - fi] * Lj[k - fj];
+        Li[j - fi] = s / Lj[j - fj];
+      }
+      double d = Li[i - fi];
+      for (int k = fi; k < i; ++k) d -= Li[k - fi] * Li[k - fi];
+      if (!(d > 0) || !std::isfinite(d)) { ok = false; break; }
+      Li[i - fi] = std::sqrt(d);
+    }
+    if (ok) { S.reg = reg; return true; }
+    reg = (reg == 0.0) ? 1e-5 : reg * 10.0;
+  }
+  S.err = "factorisation failed after regularisation retries";
+  return false;
+}
+
+/* solve Hs X = B for 3 right-hand sides; B and X interleaved (3N) */
+static void solve(const Scene& S, const double* b, double* x) {
+  int N = S.N;
+  std::vector<double> y(3 * N);
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) y[3 * i + c] = b[3 * S.perm[i] + c];
+  for (int i = 0; i < N; ++i) {
+    const double* Li = &S.env[S.rowptr[i]];
+    int fi = S.first[i];
+    double s0 = y[3 * i], s1 = y[3 * i + 1], s2 = y[3 * i + 2];
+    for (int k = fi; k < i; ++k) {
+      double l = Li[k - fi];
+      s0 -= l * y[3 * k]; s1 -= l * y[3 * k + 1]; s2 -= l * y[3 * k + 2];
+    }
+    double d = Li[i - fi];
+    y[3 * i] = s0 / d; y[3 * i + 1] = s1 / d; y[3 * i + 2] = s2 / d;
+  }
+  for (int i = N - 1; i >= 0; --i) {
+    const double* Li = &S.env[S.rowptr[i]];
+    int fi = S.first[i];
+    double d = Li[i - fi];
+    double v0 = y[3 * i] / d, v1 = y[3 * i + 1] / d, v2 = y[3 * i + 2] / d;
+    y[3 * i] = v0; y[3 * i + 1] = v1; y[3 * i + 2] = v2;
+    for (int k = fi; k < i; ++k) {
+      double l = Li[k - fi];
+      y[3 * k] -= l * v0; y[3 * k + 1] -= l * v1; y[3 * k + 2] -= l * v2;
+    }
+  }
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) x[3 * S.perm[i] + c] = y[3 * i + c];
+}
+
+static void H_mul(const Scene& S, const double* x, double* y) {
+  for (int i = 0; i < S.N; ++i) {
+    double a = 0, b = 0, c = 0;
+    for (auto& e : S.Hrows[i]) { a += e.second * x[3 * e.first]; b += e.second * x[3 * e.first + 1]; c += e.second * x[3 * e.first + 2]; }
+    y[3 * i] = a; y[3 * i + 1] = b; y[3 * i + 2] = c;
+  }
+}
+
+static inline V3 getx(const double* x, int i) { return {x[3 * i], x[3 * i + 1], x[3 * i + 2]}; }
+static inline void addx(double* f, int i, V3 v) { f[3 * i] += v.x; f[3 * i + 1] += v.y; f[3 * i + 2] += v.z; }
+
+static M3 deformation(const Tet& T, const double* x) {
+  /* F = Ds * invDm (CorotateFEMConstraint.h:87-101), written as F(:,j) = sum_v G[v][j] x_v */
+  M3 F{};
+  for (int j = 0; j < 3; ++j) {
+    V3 s{0, 0, 0};
+    for (int v = 0; v < 4; ++v) s = s + T.G[v][j] * getx(x, T.v[v]);
+    setcol(F, j, s);
+  }
+  return F;
+}
+
+/* corotated projection (CorotateFEMConstraint.h:354-377): md and md_volume */
+static void corot_project(const M3& F, M3& md, M3& mdv) {
+  SVD3 s = svd3(F);
+  M3 R = mulT(s.U, s.V);
+  md = R;
+  if (det(F) < 0) setcol(md, 2, -1.0 * col(R, 2));
+  VolProj vp = volume_projection(s.s, false);
+  M3 Ug = s.U;
+  for (int k = 0; k < 3; ++k) setcol(Ug, k, vp.g[k] * col(s.U, k));
+  mdv = mulT(Ug, s.V);
+}
+
+/* J*d accumulated per vertex: f += J d(x).  Constraint order and weights follow
+ * EvaluateJMatrix of each constraint type. */
+static void local_Jd(const Scene& S, const double* x, const double* act, double* f, int nthreads) {
+  int NT = (int)S.tets.size();
+  std::vector<double> tf((size_t)NT * 12);
+  auto tet_range = [&](int t0, int t1) {
+  for (int t = t0; t < t1; ++t) {
+    const Tet& T = S.tets[t];
+    M3 F = deformation(T, x), md, mdv;
+    corot_project(F, md, mdv);
+    double mu = S.E[t] / (1.0 + S.nu[t]);
+    double wr = mu * T.vol, wv = wr * S.nu[t];
+    for (int v = 0; v < 4; ++v) {
+      V3 s{0, 0, 0};
+      for (int j = 0; j < 3; ++j) s = s + T.G[v][j] * (wr * col(md, j) + wv * col(mdv, j));
+      tf[12 * t + 3 * v] = s.x; tf[12 * t + 3 * v + 1] = s.y; tf[12 * t + 3 * v + 2] = s.z;
+    }
+  }
+  };
+  /* element loop over nthreads host threads (the reference's loop is serial,
+     World.h:1200 has its OpenMP pragma commented out) */
+  if (nthreads <= 1 || NT < 256) {
+    tet_range(0, NT);
+  } else {
+    std::vector<std::thread> pool;
+    int chunk = (NT + nthreads - 1) / nthreads;
+    for (int k = 0; k < nthreads; ++k) {
+      int t0 = k * chunk, t1 = std::min(NT, t0 + chunk);
+      if (t0 < t1) pool.emplace_back(tet_range, t0, t1);
+    }
+    for (auto& th : pool) th.join();
+  }
+  for (int t = 0; t < NT; ++t)
+    for (int v = 0; v < 4; ++v) addx(f, S.tets[t].v[v], V3{tf[12 * t + 3 * v], tf[12 * t + 3 * v + 1], tf[12 * t + 3 * v + 2]});
+  for (size_t a = 0; a < S.att_v.size(); ++a) addx(f, S.att_v[a], S.att_k[a] * S.att_p[a]);
+  for (size_t m = 0; m < S.mtets.size(); ++m) {
+    const Tet& T = S.mtets[m];
+    M3 F = deformation(T, x);
+    V3 fib = S.mfib[m];
+    V3 Ff = fib.x * col(F, 0) + fib.y * col(F, 1) + fib.z * col(F, 2);
+    V3 p0 = (1.0 - act[S.mseg[m]]) * Ff;  /* Computep0, LinearMuscleConstraint.h:269 */
+    double w = T.vol * S.mk[m];
+    for (int v = 0; v < 4; ++v) {
+      double c = T.G[v][0] * fib.x + T.G[v][1] * fib.y + T.G[v][2] * fib.z;
+      addx(f, T.v[v], (w * c) * p0);
+    }
+  }
+  for (size_t s = 0; s < S.sp_w.size(); ++s) {
+    int i0 = S.sp_v[2 * s], i1 = S.sp_v[2 * s + 1];
+    V3 e = getx(x, i0) - getx(x, i1);
+    V3 d = (S.sp_rest[s] / norm(e)) * e;  /* SpringConstraint.h:135-144 */
+    double w = std::sqrt(S.sp_w[s]);
+    addx(f, i0, w * d);
+    addx(f, i1, -w * d);
+  }
+  for (const Bend& B : S.bends) {
+    V3 lap{0, 0, 0};
+    for (size_t a = 0; a < B.v.size(); ++a) lap = lap + B.beta[a] * getx(x, B.v[a]);
+    double ln = norm(lap);
+    V3 d{0, 0, 0};
+    if (ln > 1e-25) d = (B.w * B.rest_norm / ln) * lap;  /* BendingConstraint.h:164-187 */
+    for (size_t a = 0; a < B.v.size(); ++a) addx(f, B.v[a], (B.w * B.beta[a]) * d);
+  }
+}
+
+/* ProjectiveDynamicsMethod (World.h:835-917) with the iterate history */
+static int pd_solve(const Scene& S, const double* x, const double* qn, const double* act,
+                    std::vector<double>* hist, double* out, int nthreads) {
+  int N = S.N, n3 = 3 * N;
+  std::vector<double> b(n3), Hx(n3), xk(qn, qn + n3), xold(n3, 0.0), rhs(n3), hvf(n3);
+  double ih2 = 1.0 / (S.h * S.h);
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) b[3 * i + c] = S.mass[i] * ih2 * qn[3 * i + c];
+  H_mul(S, x, Hx.data());  /* Qf * mNonrigidX, constant over the step */
+  if (hist) hist->assign(xk.begin(), xk.end());
+  int it = 0;
+  for (int i = 0; i < S.K; ++i) {
+    double e2 = 0;
+    for (int k = 0; k < n3; ++k) { double d = xk[k] - xold[k]; e2 += d * d; }
+    if (std::sqrt(e2) / n3 < 5e-7) break;  /* EPS, World.h:214,891-895 */
+    xold = xk;
+    for (int k = 0; k < n3; ++k) rhs[k] = b[k] - Hx[k];
+    local_Jd(S, xk.data(), act, rhs.data(), nthreads);  /* ori_c = b + J d; mcf = ori_c - Qf x */
+    solve(S, rhs.data(), hvf.data());
+    for (int k = 0; k < n3; ++k) xk[k] = x[k] + hvf[k];
+    ++it;
+    if (hist) hist->insert(hist->end(), xk.begin(), xk.end());
+  }
+  std::copy(xk.begin(), xk.end(), out);
+  return it;
+}
+
+static void step_prep(const Scene& S, const double* x, const double* v, double* vwc, double* qn) {
+  /* Environment::Step adds g*h to v of gravity-enabled bodies; TimeStepping:
+     v_wc = v + h M^-1 f_ext (f_ext = 0), q_n = x + h v_wc. */
+  for (int i = 0; i < S.N; ++i) {
+    double gm = S.gmask[i];
+    double g3[3] = {S.g.x, S.g.y, S.g.z};
+    for (int c = 0; c < 3; ++c) {
+      vwc[3 * i + c] = v[3 * i + c] + gm * g3[c] * S.h;
+      qn[3 * i + c] = x[3 * i + c] + S.h * vwc[3 * i + c];
+    }
+  }
+}
+
+/* ---- adjoint ---------------------------------------------------------------- */
+
+/* VJP of the corotated projection: given dmd, dmdv (3x3) return dF */
+static M3 corot_vjp(const M3& F, const M3& gmd, const M3& gmdv) {
+  SVD3 s = svd3(F);
+  VolProj vp = volume_projection(s.s, true);
+  M3 gR = gmd;
+  if (det(F) < 0) setcol(gR, 2, -1.0 * col(gmd, 2));
+  M3 MR = mul(Tmul(s.U, gR), s.V);     /* U^T gR V */
+  M3 MG = mul(Tmul(s.U, gmdv), s.V);   /* U^T gG V */
+  M3 P{};
+  const int pair_of[3][3] = {{-1, 0, 1}, {0, -1, 2}, {1, 2, -1}};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      if (i == j) {
+        double d = 0;
+        for (int k = 0; k < 3; ++k) d += at(MG, k, k) * vp.J[k][i];
+        at(P, i, i) = d;
+      } else {
+        double ssum = s.s[i] + s.s[j];
+        double b = (vp.g[i] + vp.g[j]) / ssum;
+        double a = vp.dd[pair_of[i][j]];
+        double symG = 0.5 * (at(MG, i, j) + at(MG, j, i));
+        double asymG = 0.5 * (at(MG, i, j) - at(MG, j, i));
+        double asymR = (at(MR, i, j) - at(MR, j, i)) / ssum;
+        at(P, i, j) = a * symG + b * asymG + asymR;
+      }
+    }
+  return mulT(mul(s.U, P), s.V);  /* U P V^T */
+}
+
+struct Grad {
+  std::vector<double> gE, gnu, gact;  /* gact per segment for one step */
+};
+
+/* adjoint of local_Jd: given ybar (3N), accumulate xbar += (dJd/dx)^T ybar and
+ * parameter gradients of  ybar . J(theta) d(x, theta). */
+static void local_Jd_vjp(const Scene& S, const double* x, const double* act, const double* yb,
+                         double* xb, double* gE, double* gnu, double* gact) {
+  int NT = (int)S.tets.size();
+  for (int t = 0; t < NT; ++t) {
+    const Tet& T = S.tets[t];
+    M3 F = deformation(T, x), md, mdv;
+    corot_project(F, md, mdv);
+    double E = S.E[t], nu = S.nu[t];
+    double mu = E / (1.0 + nu);
+    double wr = mu * T.vol, wv = wr * nu;
+    /* dbar for the two 3x3 blocks: column j of md gets wr * sum_v G[v][j] yb_v */
+    M3 Y{};
+    for (int j = 0; j < 3; ++j) {
+      V3 s{0, 0, 0};
+      for (int v = 0; v < 4; ++v) s = s + T.G[v][j] * getx(yb, T.v[v]);
+      setcol(Y, j, s);
+    }
+    /* parameter gradients: ybar . (dJ/dtheta) d */
+    double yr = 0, yv = 0;
+    for (int j = 0; j < 3; ++j) { yr += dot(col(Y, j), col(md, j)); yv += dot(col(Y, j), col(mdv, j)); }
+    if (gE) gE[t] += (T.vol / (1.0 + nu)) * (yr + nu * yv);
+    if (gnu) gnu[t] += (-E * T.vol / ((1.0 + nu) * (1.0 + nu))) * yr + (E * T.vol / ((1.0 + nu) * (1.0 + nu))) * yv;
+    M3 gmd{}, gmdv{};
+    for (int j = 0; j < 3; ++j) { setcol(gmd, j, wr * col(Y, j)); setcol(gmdv, j, wv * col(Y, j)); }
+    M3 gF = corot_vjp(F, gmd, gmdv);
+    for (int v = 0; v < 4; ++v) {
+      V3 s{0, 0, 0};
+      for (int j = 0; j < 3; ++j) s = s + T.G[v][j] * col(gF, j);
+      addx(xb, T.v[v], s);
+    }
+  }
+  for (size_t m = 0; m < S.mtets.size(); ++m) {
+    const Tet& T = S.mtets[m];
+    V3 fib = S.mfib[m];
+    double w = T.vol * S.mk[m];
+    double c[4];
+    V3 db{0, 0, 0};
+    for (int v = 0; v < 4; ++v) {
+      c[v] = T.G[v][0] * fib.x + T.G[v][1] * fib.y + T.G[v][2] * fib.z;
+      db = db + (w * c[v]) * getx(yb, T.v[v]);
+    }
+    M3 F = deformation(T, x);
+    V3 Ff = fib.x * col(F, 0) + fib.y * col(F, 1) + fib.z * col(F, 2);
+    double a = act[S.mseg[m]];
+    if (gact) gact[S.mseg[m]] += -dot(db, Ff);
+    /* d = (1-a) F f, F f = sum_v c_v x_v */
+    for (int v = 0; v < 4; ++v) addx(xb, T.v[v], ((1.0 - a) * c[v]) * db);
+  }
+  for (size_t s = 0; s < S.sp_w.size(); ++s) {
+    int i0 = S.sp_v[2 * s], i1 = S.sp_v[2 * s + 1];
+    double w = std::sqrt(S.sp_w[s]);
+    V3 db = w * (getx(yb, i0) - getx(yb, i1));
+    V3 e = getx(x, i0) - getx(x, i1);
+    double n = norm(e);
+    V3 eh = (1.0 / n) * e;
+    V3 ge = (S.sp_rest[s] / n) * (db - dot(eh, db) * eh);
+    addx(xb, i0, ge);
+    addx(xb, i1, -1.0 * ge);
+  }
+  for (const Bend& B : S.bends) {
+    V3 db{0, 0, 0};
+    for (size_t a = 0; a < B.v.size(); ++a) db = db + (B.w * B.beta[a]) * getx(yb, B.v[a]);
+    V3 lap{0, 0, 0};
+    for (size_t a = 0; a < B.v.size(); ++a) lap = lap + B.beta[a] * getx(x, B.v[a]);
+    double ln = norm(lap);
+    if (!(ln > 1e-25)) continue;
+    V3 lh = (1.0 / ln) * lap;
+    V3 gl = (B.w * B.rest_norm / ln) * (db - dot(lh, db) * lh);
+    for (size_t a = 0; a < B.v.size(); ++a) addx(xb, B.v[a], B.beta[a] * gl);
+  }
+}
+
+/* ybar . (dH/dE_t) x per tet, subtracted from gE (and dH/dnu = 0: the L block
+ * of a tet is E * vol * G G^T). */
+static void H_param_vjp(const Scene& S, const double* yb, const double* x, double* gE) {
+  if (!gE) return;
+  for (size_t t = 0; t < S.tets.size(); ++t) {
+    const Tet& T = S.tets[t];
+    double s = 0;
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        double gg = 0;
+        for (int j = 0; j < 3; ++j) gg += T.G[a][j] * T.G[b][j];
+        s += gg * dot(getx(yb, T.v[a]), getx(x, T.v[b]));
+      }
+    gE[t] -= T.vol * s;
+  }
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+void* orc_create(const dfem_scene_desc* d) {
+  Scene* S = new Scene();
+  int N = d->n_vertices;
+  S->N = N;
+  S->x0.assign(d->x0, d->x0 + 3 * N);
+  S->mass.assign(d->mass, d->mass + N);
+  S->gmask.assign(N, 1.0);
+  if (d->gravity_mask)
+    for (int i = 0; i < N; ++i) S->gmask[i] = d->gravity_mask[i] ? 1.0 : 0.0;
+  for (int t = 0; t < d->n_tets; ++t) {
+    S->tets.push_back(make_tet(d->x0, d->tets + 4 * t));
+    S->E.push_back(d->youngs[t]);
+    S->nu.push_back(d->poisson[t]);
+  }
+  for (int a = 0; a < d->n_attach; ++a) {
+    S->att_v.push_back(d->attach_vertex[a]);
+    S->att_p.push_back(V3{d->attach_target[3 * a], d->attach_target[3 * a + 1], d->attach_target[3 * a + 2]});
+    S->att_k.push_back(d->attach_stiffness[a]);
+  }
+  S->nseg = d->n_segments;
+  S->seg_act.assign(std::max(0, d->n_segments), 0.0);
+  for (int m = 0; m < d->n_muscle; ++m) {
+    S->mtets.push_back(make_tet(d->x0, d->muscle_tets + 4 * m));
+    S->mfib.push_back(V3{d->muscle_fiber[3 * m], d->muscle_fiber[3 * m + 1], d->muscle_fiber[3 * m + 2]});
+    S->mk.push_back(d->muscle_stiffness[m]);
+    S->mseg.push_back(d->muscle_segment[m]);
+  }
+  for (int s = 0; s < d->n_springs; ++s) {
+    int i0 = d->spring_vertices[2 * s], i1 = d->spring_vertices[2 * s + 1];
+    S->sp_v.push_back(i0); S->sp_v.push_back(i1);
+    double rest = d->spring_rest ? d->spring_rest[s] : norm(getx(d->x0, i0) - getx(d->x0, i1));
+    S->sp_rest.push_back(rest);
+    S->sp_w.push_back(d->spring_weight[s]);
+  }
+  for (int b = 0; b < d->n_bending; ++b) {
+    Bend B;
+    int o0 = d->bend_offsets[b], o1 = d->bend_offsets[b + 1];
+    for (int k = o0; k < o1; ++k) B.v.push_back(d->bend_vertices[k]);
+    B.w = d->bend_weight[b];
+    /* mean-value Laplace-Beltrami coefficients (BendingConstraint.h:220-260) */
+    V3 mid = getx(d->x0, B.v[0]);
+    int nr = (int)B.v.size() - 1;
+    std::vector<double> coeff(nr);
+    for (int i = 0; i < nr; ++i) {
+      V3 vi = getx(d->x0, B.v[1 + i]);
+      V3 cw = getx(d->x0, B.v[1 + (i + 1) % nr]);
+      V3 ccw = getx(d->x0, B.v[1 + (i + nr - 1) % nr]);
+      double dist = norm(vi - mid);
+      coeff[i] = (mean_value(vi, mid, cw) + mean_value(vi, ccw, mid)) / dist;
+    }
+    B.beta.assign(nr + 1, 0.0);
+    for (int i = 0; i < nr; ++i) { B.beta[0] += coeff[i]; B.beta[1 + i] = -coeff[i]; }
+    /* BendingConstraint.h:83-95 evaluates applyA() on the rest state before
+       m_beltrami_coefficients is filled, so the stored rest norm is always 0
+       (the projection target d vanishes; only the w^3 beta beta^T term of L
+       acts).  The oracle follows that. */
+    B.rest_norm = 0.0;
+    S->bends.push_back(B);
+  }
+  S->h = d->time_step;
+  S->K = d->max_iterations;
+  S->damping = d->damping;
+  S->g = V3{d->gravity[0], d->gravity[1], d->gravity[2]};
+  assemble_H(*S);
+  rcm_order(*S);
+  if (!factor(*S)) { delete S; return nullptr; }
+  return S;
+}
+
+void orc_destroy(void* s) { delete static_cast<Scene*>(s); }
+
+double orc_regularisation(void* s) { return static_cast<Scene*>(s)->reg; }
+
+int orc_set_materials(void* s, const double* E, const double* nu) {
+  Scene* S = static_cast<Scene*>(s);
+  for (size_t t = 0; t < S->tets.size(); ++t) { S->E[t] = E[t]; S->nu[t] = nu[t]; }
+  assemble_H(*S);
+  rcm_order(*S);
+  return factor(*S) ? 0 : 3;
+}
+
+/* Forward: n_steps steps from (x, v); act = n_steps * n_segments (may be NULL);
+ * traj = n_steps * 3N positions (may be NULL); iters = n_steps (may be NULL). */
+int orc_forward(void* s, const double* x, const double* v, const double* act, int n_steps,
+                double* x_out, double* v_out, double* traj, int* iters, int nthreads) {
+  Scene* S = static_cast<Scene*>(s);
+  int n3 = 3 * S->N;
+  std::vector<double> xc(x, x + n3), vc(v, v + n3), vwc(n3), qn(n3), xn(n3);
+  S->rec_steps = n_steps;
+  S->rec_x.assign((size_t)n_steps * n3, 0.0);
+  S->rec_v.assign((size_t)n_steps * n3, 0.0);
+  S->rec_act.assign((size_t)n_steps * std::max(1, S->nseg), 0.0);
+  S->rec_iters.assign(n_steps, 0);
+  std::vector<double> zero_act(std::max(1, S->nseg), 0.0);
+  for (int st = 0; st < n_steps; ++st) {
+    const double* a = act ? act + (size_t)st * S->nseg : zero_act.data();
+    std::copy(xc.begin(), xc.end(), S->rec_x.begin() + (size_t)st * n3);
+    std::copy(vc.begin(), vc.end(), S->rec_v.begin() + (size_t)st * n3);
+    if (S->nseg > 0) std::copy(a, a + S->nseg, S->rec_act.begin() + (size_t)st * S->nseg);
+    step_prep(*S, xc.data(), vc.data(), vwc.data(), qn.data());
+    int it = pd_solve(*S, xc.data(), qn.data(), a, nullptr, xn.data(), nthreads);
+    S->rec_iters[st] = it;
+    if (iters) iters[st] = it;
+    for (int k = 0; k < n3; ++k) {
+      vc[k] = (xn[k] - xc[k]) * (1.0 / S->h) * S->damping;  /* World.h:708,757-766 */
+      xc[k] = xn[k];
+    }
+    if (traj) std::copy(xc.begin(), xc.end(), traj + (size_t)st * n3);
+    for (int k = 0; k < n3; ++k)
+      if (!std::isfinite(xc[k])) { S->err = "non-finite state"; return 4; }
+  }
+  std::copy(xc.begin(), xc.end(), x_out);
+  std::copy(vc.begin(), vc.end(), v_out);
+  return 0;
+}
+
+/* Adjoint of the last orc_forward (recomputes each step's iterates). */
+int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx, double* gv,
+                 double* gE, double* gnu, double* gact) {
+  Scene* S = static_cast<Scene*>(s);
+  if (S->rec_steps <= 0) return 5;
+  int N = S->N, n3 = 3 * N;
+  int NT = (int)S->tets.size();
+  std::vector<double> xb(gx_out, gx_out + n3), vb(gv_out, gv_out + n3);
+  if (gE) std::fill(gE, gE + NT, 0.0);
+  if (gnu) std::fill(gnu, gnu + NT, 0.0);
+  if (gact) std::fill(gact, gact + (size_t)S->rec_steps * S->nseg, 0.0);
+  std::vector<double> vwc(n3), qn(n3), xn(n3), hist, ybar(n3), xkb(n3), bb(n3), tmp(n3);
+  double ih2 = 1.0 / (S->h * S->h);
+  for (int st = S->rec_steps - 1; st >= 0; --st) {
+    const double* x = &S->rec_x[(size_t)st * n3];
+    const double* v = &S->rec_v[(size_t)st * n3];
+    const double* a = &S->rec_act[(size_t)st * std::max(1, S->nseg)];
+    step_prep(*S, x, v, vwc.data(), qn.data());
+    int it = pd_solve(*S, x, qn.data(), a, &hist, xn.data(), 1);
+    /* v' = damping (x' - x)/h; x' = x^it */
+    double c = S->damping / S->h;
+    std::vector<double> xtb(n3);
+    for (int k = 0; k < n3; ++k) { xkb[k] = xb[k] + c * vb[k]; xtb[k] = -c * vb[k]; }
+    std::fill(bb.begin(), bb.end(), 0.0);
+    for (int k = it - 1; k >= 0; --k) {
+      const double* xk = &hist[(size_t)k * n3];
+      const double* xk1 = &hist[(size_t)(k + 1) * n3];
+      solve(*S, xkb.data(), ybar.data());          /* H symmetric */
+      for (int q = 0; q < n3; ++q) bb[q] += ybar[q];
+      std::fill(tmp.begin(), tmp.end(), 0.0);
+      local_Jd_vjp(*S, xk, a, ybar.data(), tmp.data(), gE, gnu, gact ? gact + (size_t)st * S->nseg : nullptr);
+      H_param_vjp(*S, ybar.data(), xk1, gE);
+      xkb = tmp;
+    }
+    /* x^0 = q_n and b = M/h^2 q_n */
+    std::vector<double> qnb(n3);
+    for (int i = 0; i < N; ++i)
+      for (int cc = 0; cc < 3; ++cc) qnb[3 * i + cc] = xkb[3 * i + cc] + S->mass[i] * ih2 * bb[3 * i + cc];
+    for (int k = 0; k < n3; ++k) {
+      xb[k] = xtb[k] + qnb[k];
+      vb[k] = S->h * qnb[k];
+    }
+  }
+  std::copy(xb.begin(), xb.end(), gx);
+  std::copy(vb.begin(), vb.end(), gv);
+  return 0;
+}
+
+/* Lumped masses of a tet mesh: Dfobj.h:506-525 (Is Mass Same = true: mass per
+ * vertex = total / totvol * sum 0.25 vol; false: total / N). */
+int orc_lumped_masses(int N, const double* x0, int T, const int* tets, double total_mass,
+                      int is_mass_same, double* mass) {
+  std::fill(mass, mass + N, 0.0);
+  double totvol = 0;
+  for (int t = 0; t < T; ++t) {
+    Tet tt = make_tet(x0, tets + 4 * t);
+    totvol += tt.vol;
+    for (int k = 0; k < 4; ++k) mass[tets[4 * t + k]] += 0.25 * tt.vol;
+  }
+  for (int i = 0; i < N; ++i) mass[i] = is_mass_same ? total_mass / totvol * mass[i] : total_mass / N;
+  return 0;
+}
+
+/* Corotated projection of one F (column-major 9): md, md_volume (column-major). */
+void orc_corot_project(const double* F9, double* md9, double* mdv9) {
+  M3 F; std::memcpy(F.m, F9, sizeof(F.m));
+  M3 md, mdv;
+  corot_project(F, md, mdv);
+  std::memcpy(md9, md.m, sizeof(md.m));
+  std::memcpy(mdv9, mdv.m, sizeof(mdv.m));
+}
+
+void orc_corot_vjp(const double* F9, const double* gmd9, const double* gmdv9, double* gF9) {
+  M3 F, a, b; std::memcpy(F.m, F9, 72); std::memcpy(a.m, gmd9, 72); std::memcpy(b.m, gmdv9, 72);
+  M3 g = corot_vjp(F, a, b);
+  std::memcpy(gF9, g.m, 72);
+}
+
+/* SVD of one F: U, V column-major, s descending */
+void orc_svd3(const double* F9, double* U9, double* s3, double* V9) {
+  M3 F; std::memcpy(F.m, F9, 72);
+  SVD3 s = svd3(F);
+  std::memcpy(U9, s.U.m, 72); std::memcpy(V9, s.V.m, 72);
+  for (int i = 0; i < 3; ++i) s3[i] = s.s[i];
+}
+
+/* Hs as COO (row, col, value), merged; returns nnz, fills up to cap. */
+int64_t orc_hs_coo(void* s, int* rows, int* cols, double* vals, int64_t cap) {
+  Scene* S = static_cast<Scene*>(s);
+  int64_t k = 0;
+  for (int i = 0; i < S->N; ++i)
+    for (auto& e : S->Hrows[i]) {
+      if (k < cap) { rows[k] = i; cols[k] = e.first; vals[k] = e.second; }
+      ++k;
+    }
+  return k;
+}
+
+/* The reference's 3N x 3N L triplets from per-constraint A_i (EvaluateLMatrix of
+ * the corotated, attachment, muscle and spring constraints), unmerged. */
+int64_t orc_full_L_triplets(void* s, int* rows, int* cols, double* vals, int64_t cap) {
+  Scene* S = static_cast<Scene*>(s);
+  int64_t k = 0;
+  auto push = [&](int r, int c, double v) { if (k < cap) { rows[k] = r; cols[k] = c; vals[k] = v; } ++k; };
+  for (size_t t = 0; t < S->tets.size(); ++t) {
+    const Tet& T = S->tets[t];
+    /* A_i rows 3j+c, columns 3v+c': delta_{cc'} G[v][j] (CorotateFEMConstraint.h:236-245) */
+    double A[9][12] = {{0}};
+    for (int j = 0; j < 3; ++j)
+      for (int c = 0; c < 3; ++c)
+        for (int v = 0; v < 4; ++v) A[3 * j + c][3 * v + c] = T.G[v][j];
+    double mu = S->E[t] / (1.0 + S->nu[t]);
+    for (int blk = 0; blk < 2; ++blk) {
+      double w = mu * T.vol * (blk ? S->nu[t] : 1.0);
+      for (int a = 0; a < 12; ++a)
+        for (int b = 0; b < 12; ++b) {
+          double sum = 0;
+          for (int r = 0; r < 9; ++r) sum += A[r][a] * A[r][b];
+          push(3 * T.v[a / 3] + a % 3, 3 * T.v[b / 3] + b % 3, w * sum);
+        }
+    }
+  }
+  for (size_t a = 0; a < S->att_v.size(); ++a)
+    for (int c = 0; c < 3; ++c) push(3 * S->att_v[a] + c, 3 * S->att_v[a] + c, S->att_k[a]);
+  for (size_t m = 0; m < S->mtets.size(); ++m) {
+    const Tet& T = S->mtets[m];
+    V3 fib = S->mfib[m];
+    double A[3][12] = {{0}};
+    for (int v = 0; v < 4; ++v) {
+      double c = T.G[v][0] * fib.x + T.G[v][1] * fib.y + T.G[v][2] * fib.z;
+      for (int cc = 0; cc < 3; ++cc) A[cc][3 * v + cc] = c;
+    }
+    double w = T.vol * S->mk[m];
+    for (int a = 0; a < 12; ++a)
+      for (int b = 0; b < 12; ++b) {
+        double sum = 0;
+        for (int r = 0; r < 3; ++r) sum += A[r][a] * A[r][b];
+        push(3 * T.v[a / 3] + a % 3, 3 * T.v[b / 3] + b % 3, w * sum);
+      }
+  }
+  for (size_t sp = 0; sp < S->sp_w.size(); ++sp) {
+    double w = std::sqrt(S->sp_w[sp]);
+    int iv[2] = {S->sp_v[2 * sp], S->sp_v[2 * sp + 1]};
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b)
+        for (int c = 0; c < 3; ++c) push(3 * iv[a] + c, 3 * iv[b] + c, w * (a == b ? 1.0 : -1.0));
+  }
+  return k;
+}
+
+const char* orc_last_error(void* s) { return static_cast<Scene*>(s)->err.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,131 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the CPU FP64 oracle.
+
+Tolerances (plain FP64 form): positions and velocities within 1e-9 relative
+to the oracle's scale, gradients within 1e-8 relative, iteration counts equal.
+"""
+import numpy as np
+import pytest
+
+from diff_fem_b200 import _capi, scene as S
+from diff_fem_b200.engine import Scene
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-9
+GRAD_TOL = 1e-8
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def run_both(d, n_steps, act=None, x=None, v=None, seed=0):
+    rng = np.random.default_rng(seed)
+    if x is None:
+        x = d.x0.reshape(-1).copy()
+    if v is None:
+        v = np.zeros_like(x)
+    g = Scene(d)
+    o = O.OracleScene(d)
+    xg, vg, tg = g.forward(x, v, n_steps=n_steps, act=act, traj=True)
+    ro = o.forward(x, v, n_steps=n_steps, act=act, traj=True)
+    return g, o, (xg, vg, tg), ro
+
+
+def test_cantilever_forward_100_steps():
+    d = S.cantilever()
+    g, o, (xg, vg, tg), ro = run_both(d, 100)
+    assert np.array_equal(g.iterations(100), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    assert rel(xg, ro["x"]) < POS_TOL
+    assert rel(vg, ro["v"]) < POS_TOL
+
+
+def test_inverse_stiffness_forward_and_adjoint():
+    d = S.inverse_stiffness()
+    n = 4
+    g, o, (xg, vg, tg), ro = run_both(d, n)
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    rng = np.random.default_rng(1)
+    gx, gv = rng.standard_normal(xg.size), rng.standard_normal(xg.size)
+    bg = g.backward(gx, gv)
+    bo = o.backward(gx, gv)
+    for k in ("x", "v", "E", "nu"):
+        assert rel(bg[k], bo[k]) < GRAD_TOL, k
+
+
+def test_muscles_forward_and_adjoint():
+    d = S.muscle_beam()
+    n = 5
+    act = np.random.default_rng(2).uniform(0, 1, (n, d.n_segments))
+    g, o, (xg, vg, tg), ro = run_both(d, n, act=act)
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    rng = np.random.default_rng(3)
+    gx, gv = rng.standard_normal(xg.size), rng.standard_normal(xg.size)
+    bg, bo = g.backward(gx, gv), o.backward(gx, gv)
+    for k in ("x", "v", "E", "nu", "act"):
+        assert rel(bg[k], bo[k]) < GRAD_TOL, k
+
+
+def test_cloth_forward_and_adjoint():
+    d = S.cloth_sheet(nv=10)
+    n = 6
+    g, o, (xg, vg, tg), ro = run_both(d, n)
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    rng = np.random.default_rng(4)
+    gx, gv = rng.standard_normal(xg.size), rng.standard_normal(xg.size)
+    bg, bo = g.backward(gx, gv), o.backward(gx, gv)
+    for k in ("x", "v"):
+        assert rel(bg[k], bo[k]) < GRAD_TOL, k
+
+
+def test_device_pointers_match_host_path_and_are_deterministic():
+    import torch
+    d = S.inverse_stiffness(nx=12, ny=4, nz=4)
+    g = Scene(d)
+    x = d.x0.reshape(-1).copy()
+    v = np.zeros_like(x)
+    xh, vh = g.forward(x, v, n_steps=3)
+    xd, vd = g.forward(torch.tensor(x, device="cuda"), torch.tensor(v, device="cuda"), n_steps=3)
+    assert np.array_equal(xh, xd.cpu().numpy()) and np.array_equal(vh, vd.cpu().numpy())
+    xh2, vh2 = g.forward(x, v, n_steps=3)
+    assert np.array_equal(xh, xh2) and np.array_equal(vh, vh2)
+
+
+def test_set_materials_refactors():
+    d = S.inverse_stiffness(nx=10, ny=3, nz=3)
+    g = Scene(d)
+    o = O.OracleScene(d)
+    E2 = S.log_uniform_moduli(d.n_tets, 5678)
+    g.set_materials(E2, d.poisson)
+    o.set_materials(E2, d.poisson)
+    x = d.x0.reshape(-1).copy()
+    xg, vg = g.forward(x, np.zeros_like(x), n_steps=5)
+    ro = o.forward(x, np.zeros_like(x), n_steps=5)
+    assert rel(xg, ro["x"]) < POS_TOL
+
+
+def test_backward_before_forward_is_a_state_error():
+    d = S.cantilever()
+    g = Scene(d)
+    with pytest.raises(_capi.DfemError) as e:
+        g.backward(np.zeros(3 * d.n_vertices), np.zeros(3 * d.n_vertices))
+    assert e.value.code == 5
+
+
+def test_nonfinite_input_reports_status():
+    d = S.cantilever()
+    g = Scene(d)
+    x = d.x0.reshape(-1).copy()
+    x[7] = np.nan
+    with pytest.raises(_capi.DfemError) as e:
+        g.forward(x, np.zeros_like(x), n_steps=1)
+    assert e.value.code == 4
+    # the context stays usable
+    xg, _ = g.forward(d.x0.reshape(-1).copy(), np.zeros_like(x), n_steps=1)
+    assert np.all(np.isfinite(xg))

@@ -1,0 +1,193 @@
+"""Pins the CPU FP64 oracle (the checker) before anything is compared with it.
+
+diff_fem ships no tests, golden vectors or output fixtures, and cannot be
+built here, so the oracle is pinned by known-answer invariants of the
+reference's algorithm, central finite differences of the hand-written
+adjoint, and the committed golden fixtures in tests/golden/ (generated by
+tests/golden/make_golden.py from the oracle itself, so later changes to the
+oracle are caught).
+"""
+import numpy as np
+import pytest
+
+from diff_fem_b200 import scene as S
+from oracle import oracle as O
+
+RNG = np.random.default_rng(42)
+
+
+def rand_F(det_sign=1):
+    while True:
+        F = np.eye(3) + 0.4 * RNG.standard_normal((3, 3))
+        if np.sign(np.linalg.det(F)) == det_sign and abs(np.linalg.det(F)) > 0.05:
+            return F
+
+
+def test_svd_reconstruction():
+    for sign in (1, -1):
+        for _ in range(20):
+            F = rand_F(sign)
+            U, s, V = O.svd3(F)
+            assert np.allclose(U @ np.diag(s) @ V.T, F, atol=1e-13)
+            assert np.allclose(U.T @ U, np.eye(3), atol=1e-13)
+            assert np.allclose(V.T @ V, np.eye(3), atol=1e-13)
+            assert np.all(s >= 0) and np.all(np.diff(s) <= 0)
+
+
+def test_corotated_projection_rules():
+    """md = polar rotation R (column 2 negated when det F < 0); md_volume has det +-1."""
+    for sign in (1, -1):
+        for _ in range(20):
+            F = rand_F(sign)
+            md, mdv = O.corot_project(F)
+            U, s, Vt = np.linalg.svd(F)
+            R = U @ Vt  # polar factor (numpy's SVD, independent of the oracle's)
+            exp = R.copy()
+            if np.linalg.det(F) < 0:
+                exp[:, 2] *= -1
+            assert np.allclose(md, exp, atol=1e-12)
+            # volume projection: exactly 5 Newton steps on prod(S + D) = 1
+            # (CorotateFEMConstraint.h:366-374), restated here with numpy
+            D = np.zeros(3)
+            for _ in range(5):
+                p = s + D
+                C = p.prod() - 1.0
+                gr = np.array([p[1] * p[2], p[0] * p[2], p[0] * p[1]])
+                D = (gr @ D - C) / (gr @ gr) * gr
+            assert np.allclose(mdv, U @ np.diag(s + D) @ Vt, atol=1e-12)
+            assert np.sign(np.linalg.det(mdv)) == np.sign(np.linalg.det(F))
+
+
+def test_corotated_vjp_matches_finite_differences():
+    for sign in (1, -1):
+        for _ in range(10):
+            F = rand_F(sign)
+            gmd = RNG.standard_normal((3, 3))
+            gmdv = RNG.standard_normal((3, 3))
+            gF = O.corot_vjp(F, gmd, gmdv)
+            dF = RNG.standard_normal((3, 3))
+            eps = 1e-6
+            mp, vp = O.corot_project(F + eps * dF)
+            mm, vm = O.corot_project(F - eps * dF)
+            fd = (np.sum(gmd * (mp - mm)) + np.sum(gmdv * (vp - vm))) / (2 * eps)
+            assert abs(np.sum(gF * dF) - fd) < 1e-7 * max(1.0, abs(fd))
+
+
+def test_vjp_equal_singular_values():
+    """Exact divided differences: no blow-up for repeated singular values."""
+    Q, _ = np.linalg.qr(RNG.standard_normal((3, 3)))
+    for F in (np.eye(3) * 1.1, Q @ np.diag([1.2, 1.2, 0.9]) @ Q.T):
+        g = O.corot_vjp(F, RNG.standard_normal((3, 3)), RNG.standard_normal((3, 3)))
+        assert np.all(np.isfinite(g))
+
+
+def test_lumped_masses_match_builder():
+    d = S.cantilever()
+    m = O.lumped_masses(d.x0, d.tets, 20.0, True)
+    assert np.allclose(m, d.mass, rtol=1e-14)
+    m2 = O.lumped_masses(d.x0, d.tets, 20.0, False)
+    assert np.allclose(m2, 20.0 / d.n_vertices)
+
+
+def test_kron_structure_of_L():
+    """The reference's 3N x 3N L (per-constraint A_i^T A_i triplets) equals kron(L_s, I3)."""
+    for d in (S.cantilever(), S.muscle_beam(), S.cloth_sheet(nv=5)):
+        d.bend_weight = d.bend_weight * 0  # bending enters Hs only; checked via Hs below
+        o = O.OracleScene(d)
+        N = d.n_vertices
+        r, c, v = o.full_L_triplets()
+        L3 = np.zeros((3 * N, 3 * N))
+        np.add.at(L3, (r, c), v)
+        hr, hc, hv = o.hs_coo()
+        Hs = np.zeros((N, N))
+        np.add.at(Hs, (hr, hc), hv)
+        Ls = Hs - np.diag(d.mass / d.time_step ** 2)
+        assert np.allclose(L3, np.kron(Ls, np.eye(3)), rtol=1e-12, atol=1e-9 * np.abs(Ls).max())
+
+
+def test_rest_state_is_a_fixed_point():
+    """No gravity, zero velocity, rest positions: every projection reproduces the
+    rest configuration, so the state stays put."""
+    for d in (S.cantilever(), S.muscle_beam(), S.cloth_sheet(nv=6)):
+        d.gravity = (0.0, 0.0, 0.0)
+        o = O.OracleScene(d)
+        x = d.x0.reshape(-1).copy()
+        r = o.forward(x, np.zeros_like(x), n_steps=3)
+        assert np.abs(r["x"] - x).max() < 1e-9 * max(1.0, np.abs(x).max())
+
+
+def test_free_fall_is_exact():
+    """Unpinned body in its rest shape: x' = x + h (v + g h), v' = damping (v + g h)."""
+    d = S.cantilever()
+    d.attach_vertex = np.zeros(0, np.int32)
+    d.attach_target = np.zeros((0, 3))
+    d.attach_stiffness = np.zeros(0)
+    o = O.OracleScene(d)
+    x = d.x0.reshape(-1).copy()
+    v = np.tile([0.3, 0.1, -0.2], d.n_vertices)
+    r = o.forward(x, v, n_steps=1)
+    g = np.tile(d.gravity, d.n_vertices)
+    vwc = v + g * d.time_step
+    assert np.allclose(r["x"], x + d.time_step * vwc, atol=1e-10)
+    assert np.allclose(r["v"], d.damping * vwc, atol=1e-8)
+
+
+def test_deterministic():
+    d = S.muscle_beam()
+    o = O.OracleScene(d)
+    x = d.x0.reshape(-1).copy()
+    act = RNG.uniform(0, 1, (4, d.n_segments))
+    a = o.forward(x, np.zeros_like(x), n_steps=4, act=act)
+    b = o.forward(x, np.zeros_like(x), n_steps=4, act=act)
+    assert np.array_equal(a["x"], b["x"]) and np.array_equal(a["v"], b["v"])
+
+
+def test_multithreaded_local_step_is_identical():
+    d = S.inverse_stiffness(nx=8, ny=4, nz=4)
+    o = O.OracleScene(d)
+    x = d.x0.reshape(-1).copy()
+    a = o.forward(x, np.zeros_like(x), n_steps=2, threads=1)
+    b = o.forward(x, np.zeros_like(x), n_steps=2, threads=4)
+    assert np.array_equal(a["x"], b["x"])
+
+
+def _loss(o, x, v, gx, gv, n, act=None):
+    r = o.forward(x, v, n_steps=n, act=act)
+    return gx @ r["x"] + gv @ r["v"], r["iters"]
+
+
+@pytest.mark.parametrize("builder", ["cantilever", "muscle_beam", "cloth_sheet"])
+def test_adjoint_matches_central_differences(builder):
+    d = getattr(S, builder)()
+    o = O.OracleScene(d)
+    n = 3
+    x = d.x0.reshape(-1) + 1e-3 * RNG.standard_normal(3 * d.n_vertices)
+    v = 0.05 * RNG.standard_normal(3 * d.n_vertices)
+    gx = RNG.standard_normal(x.size)
+    gv = RNG.standard_normal(x.size)
+    act = RNG.uniform(0, 1, (n, d.n_segments)) if d.n_segments else None
+    _, it0 = _loss(o, x, v, gx, gv, n, act)
+    g = o.backward(gx, gv)
+    checks = []
+    dx = RNG.standard_normal(x.size)
+    eps = 1e-6
+    (lp, ip), (lm, im) = _loss(o, x + eps * dx, v, gx, gv, n, act), _loss(o, x - eps * dx, v, gx, gv, n, act)
+    checks.append((g["x"] @ dx, (lp - lm) / (2 * eps), ip, im))
+    dv = RNG.standard_normal(x.size)
+    (lp, ip), (lm, im) = _loss(o, x, v + eps * dv, gx, gv, n, act), _loss(o, x, v - eps * dv, gx, gv, n, act)
+    checks.append((g["v"] @ dv, (lp - lm) / (2 * eps), ip, im))
+    if d.n_tets:
+        E, nu = d.youngs.copy(), d.poisson.copy()
+        dE = RNG.standard_normal(E.size) * E
+        rel = 1e-5
+        o.set_materials(E + rel * dE, nu); lp, ip = _loss(o, x, v, gx, gv, n, act)
+        o.set_materials(E - rel * dE, nu); lm, im = _loss(o, x, v, gx, gv, n, act)
+        o.set_materials(E, nu)
+        checks.append((g["E"] @ dE, (lp - lm) / (2 * rel), ip, im))
+    if act is not None:
+        da = RNG.standard_normal(act.shape)
+        (lp, ip), (lm, im) = _loss(o, x, v, gx, gv, n, act + eps * da), _loss(o, x, v, gx, gv, n, act - eps * da)
+        checks.append((np.sum(g["act"] * da), (lp - lm) / (2 * eps), ip, im))
+    for adj, fd, ip, im in checks:
+        assert np.array_equal(ip, it0) and np.array_equal(im, it0), "iteration count changed under perturbation"
+        assert abs(adj - fd) <= 1e-5 * max(1.0, abs(fd)), (adj, fd)
