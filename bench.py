@@ -40,7 +40,12 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    return p.parse_args()
+    p.add_argument("--sim-steps", type=int, default=60,
+                   help="time steps per gradient evaluation (60 is the workload; fewer only for profiler captures)")
+    a = p.parse_args()
+    global SIM_STEPS
+    SIM_STEPS = a.sim_steps
+    return a
 
 
 def workload_config(precision: str) -> dict:
@@ -48,6 +53,7 @@ def workload_config(precision: str) -> dict:
         "workload": "inverse_stiffness beam 40x8x8 cubes x5 tets (12,800 tets, 3,321 vertices), "
                     "E~logU[1e4,1e6] seed 1234, both ends pinned, h=1/100, K=20, 60 steps, fwd+adjoint dL/dE",
         "tets": 12800, "vertices": 3321, "sim_steps_per_bench_step": SIM_STEPS, "pd_iterations": 20,
+        **({} if SIM_STEPS == 60 else {"note": "reduced time steps: profiler capture only, not a bench value"}),
         "precision": precision, "parallelism": "replicas (one independent scene per GPU)",
     }
 

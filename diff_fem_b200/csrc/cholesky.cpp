@@ -288,27 +288,6 @@ bool numeric(const SparseSym& A, SupernodalFactor& F, double reg) {
     for (int c = 0; c < w; ++c)
       for (int a = 0; a < r; ++a) Lc[(size_t)c * r + a] = B[(w + a) + (size_t)c * L];
   }
-  // row-wise CSR of the below-diagonal-block entries
-  std::vector<int64_t> cnt(F.n + 1, 0);
-  for (int s = 0; s < ns; ++s)
-    for (int a = 0; a < F.sn_r[s]; ++a) cnt[F.rowidx[F.sn_rofs[s] + a] + 1] += F.sn_w[s];
-  for (int i = 0; i < F.n; ++i) cnt[i + 1] += cnt[i];
-  F.lrow_ptr = cnt;
-  F.lrow_col.assign(cnt[F.n], 0);
-  F.lrow_val.assign(cnt[F.n], 0.0);
-  std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
-  for (int s = 0; s < ns; ++s) {
-    const int w = F.sn_w[s], r = F.sn_r[s];
-    const double* Lc = &F.Lcm[F.sn_lofs[s]];
-    for (int a = 0; a < r; ++a) {
-      int i = F.rowidx[F.sn_rofs[s] + a];
-      for (int c = 0; c < w; ++c) {
-        int64_t k = fill[i]++;
-        F.lrow_col[k] = F.sn_c0[s] + c;
-        F.lrow_val[k] = Lc[(size_t)c * r + a];
-      }
-    }
-  }
   F.reg = reg;
   return true;
 }
@@ -426,6 +405,15 @@ bool factorize(const SparseSym& A, const double* coords, const FactorOptions& op
     F.sn_lofs[s + 1] = F.sn_lofs[s] + (int64_t)st.size() * w;
     F.sn_dofs[s + 1] = F.sn_dofs[s] + (int64_t)w * w;
   }
+  // row -> contribution slots (positions in rowidx holding that row)
+  F.rseg_ptr.assign(n + 1, 0);
+  for (int i : F.rowidx) F.rseg_ptr[i + 1]++;
+  for (int i = 0; i < n; ++i) F.rseg_ptr[i + 1] += F.rseg_ptr[i];
+  F.rseg_pos.assign(F.rowidx.size(), 0);
+  {
+    std::vector<int> fill(F.rseg_ptr.begin(), F.rseg_ptr.end() - 1);
+    for (size_t p = 0; p < F.rowidx.size(); ++p) F.rseg_pos[fill[F.rowidx[p]]++] = (int)p;
+  }
   F.sn_parent.assign(F.nsuper, -1);
   for (int s = 0; s < F.nsuper; ++s) {
     int last = F.sn_c0[s] + F.sn_w[s] - 1;
@@ -462,17 +450,17 @@ void host_solve(const SupernodalFactor& F, const double* b, double* x) {
   std::vector<double> y(3 * (size_t)n);
   for (int i = 0; i < n; ++i)
     for (int c = 0; c < 3; ++c) y[3 * i + c] = b[3 * F.perm[i] + c];
-  // forward: L y = b, supernode by supernode
+  // forward: L y = b, supernode by supernode, push form
+  std::vector<double> contrib(3 * F.rowidx.size(), 0.0);
   for (int s = 0; s < F.nsuper; ++s) {
-    int c0 = F.sn_c0[s], w = F.sn_w[s];
+    int c0 = F.sn_c0[s], w = F.sn_w[s], r = F.sn_r[s];
     std::vector<double> t(3 * (size_t)w);
     for (int c = 0; c < w; ++c) {
       int i = c0 + c;
       double a0 = y[3 * i], a1 = y[3 * i + 1], a2 = y[3 * i + 2];
-      for (int64_t k = F.lrow_ptr[i]; k < F.lrow_ptr[i + 1]; ++k) {
-        int j = F.lrow_col[k];
-        double l = F.lrow_val[k];
-        a0 -= l * y[3 * j]; a1 -= l * y[3 * j + 1]; a2 -= l * y[3 * j + 2];
+      for (int k = F.rseg_ptr[i]; k < F.rseg_ptr[i + 1]; ++k) {
+        const double* q = &contrib[3 * (size_t)F.rseg_pos[k]];
+        a0 -= q[0]; a1 -= q[1]; a2 -= q[2];
       }
       t[3 * c] = a0; t[3 * c + 1] = a1; t[3 * c + 2] = a2;
     }
@@ -484,6 +472,16 @@ void host_solve(const SupernodalFactor& F, const double* b, double* x) {
         a0 += d * t[3 * k]; a1 += d * t[3 * k + 1]; a2 += d * t[3 * k + 2];
       }
       y[3 * (c0 + c)] = a0; y[3 * (c0 + c) + 1] = a1; y[3 * (c0 + c) + 2] = a2;
+    }
+    const double* Lc = &F.Lcm[F.sn_lofs[s]];
+    for (int a = 0; a < r; ++a) {
+      double a0 = 0, a1 = 0, a2 = 0;
+      for (int c = 0; c < w; ++c) {
+        double l = Lc[(size_t)c * r + a];
+        a0 += l * y[3 * (c0 + c)]; a1 += l * y[3 * (c0 + c) + 1]; a2 += l * y[3 * (c0 + c) + 2];
+      }
+      double* q = &contrib[3 * (size_t)(F.sn_rofs[s] + a)];
+      q[0] = a0; q[1] = a1; q[2] = a2;
     }
   }
   // backward: L^T x = y

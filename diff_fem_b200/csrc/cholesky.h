@@ -39,10 +39,11 @@ struct SupernodalFactor {
   std::vector<double> Ldiag, Dinv;            // diagonal block and its inverse (both lower)
   std::vector<int> sn_parent;                 // -1 for roots
   std::vector<int> col_sn;                    // supernode of each column
-  // row-wise CSR of all below-diagonal-block entries (forward solve)
-  std::vector<int64_t> lrow_ptr;
-  std::vector<int> lrow_col;
-  std::vector<double> lrow_val;
+  // forward solve in push form: supernode s writes L_{R_s,s} y_s to the
+  // contribution slots sn_rofs[s] .. sn_rofs[s]+r_s (one per below-diagonal row);
+  // row i then subtracts the contributions listed in rseg_pos[rseg_ptr[i] ..]
+  std::vector<int> rseg_ptr;   // n+1
+  std::vector<int> rseg_pos;   // positions into rowidx (== contribution slots)
   // level schedule: level 0 = leaves
   int nlevels = 0;
   std::vector<int> lvl_ptr, lvl_sn;

@@ -43,9 +43,14 @@ struct DBuf {
     if (count == 0) return cudaSuccess;
     return cudaMalloc(&p, count * sizeof(T));
   }
+  // copies into the existing allocation when the size is unchanged, so device
+  // pointers captured in CUDA graphs stay valid across material updates
   cudaError_t upload(const std::vector<T>& h) {
-    cudaError_t e = alloc(h.size());
-    if (e != cudaSuccess || h.empty()) return e;
+    if (!(p && n == h.size())) {
+      cudaError_t e = alloc(h.size());
+      if (e != cudaSuccess || h.empty()) return e;
+    }
+    if (h.empty()) return cudaSuccess;
     return cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
   }
 };
@@ -65,10 +70,10 @@ struct dfem_scene {
   DBuf<int> mseg, seg_ptr, seg_mus, boff, bv, bslot, vslot_ptr, hs_ptr, hs_col, to_user, to_internal;
   DBuf<double> hs_val;
   // factor
-  DBuf<int> lrow_ptr, lrow_col, sn_c0, sn_w, sn_r, sn_rofs, rowidx, sn_lofs, sn_dofs, lvl_sn;
-  DBuf<double> lrow_val, Lcm, Dinv;
+  DBuf<int> rseg_ptr, rseg_pos, sn_c0, sn_w, sn_r, sn_rofs, rowidx, sn_lofs, sn_dofs, lvl_sn;
+  DBuf<double> contrib, Lcm, Dinv;
   std::vector<int> lvl_ptr;
-  int max_w = 1;
+  int max_w = 1, max_r = 0;
   // state
   DBuf<double> xt, vt, qn, c0, xk, rhs, y, slot, hist, io_a, io_b;
   DBuf<double> partial, errv;
@@ -96,14 +101,32 @@ struct dfem_scene {
 
 namespace dfem {
 
+// Captured graphs bake in device pointers; any change of them invalidates the graphs.
+static void invalidate_graphs(dfem_scene* sc) {
+  if (sc->g_step) { cudaGraphExecDestroy(sc->g_step); sc->g_step = nullptr; }
+  if (sc->g_adj) { cudaGraphExecDestroy(sc->g_adj); sc->g_adj = nullptr; }
+}
+
+static void refresh_scene_view(dfem_scene* sc) {
+  const HostScene& s = sc->hs;
+  SceneDev sd{s.N, s.T, s.M, s.S, s.B, s.nseg, s.h, s.damping, s.g[0], s.g[1], s.g[2],
+              sc->mass.p, sc->gmask.p, sc->tv.p, sc->tinv.p, sc->twr.p, sc->twv.p, sc->tvol.p, sc->tE.p, sc->tnu.p,
+              sc->tslot.p, sc->mv.p, sc->minv.p, sc->mw.p, sc->mfib.p, sc->mseg.p, sc->mslot.p, sc->seg_ptr.p,
+              sc->seg_mus.p, sc->sv.p, sc->srest.p, sc->ssw.p, sc->sslot.p, sc->boff.p, sc->bv.p, sc->bbeta.p,
+              sc->bw.p, sc->brest.p, sc->bslot.p, sc->vslot_ptr.p, sc->attach_jd.p, sc->hs_ptr.p, sc->hs_col.p,
+              sc->hs_val.p};
+  if (std::memcmp(&sd, &sc->sd, sizeof(sd)) != 0) invalidate_graphs(sc);
+  sc->sd = sd;
+}
+
 static int upload_factor(dfem_scene* sc) {
   const SupernodalFactor& F = sc->hs.F;
-  if (F.lrow_ptr.back() > INT32_MAX || F.sn_lofs.back() > INT32_MAX || F.sn_dofs.back() > INT32_MAX)
+  if (F.sn_rofs.back() > INT32_MAX / 3 || F.sn_lofs.back() > INT32_MAX || F.sn_dofs.back() > INT32_MAX)
     return fail(DFEM_ERR_INVALID, "factor too large for 32-bit offsets");
   auto to32 = [](const std::vector<int64_t>& v) { return std::vector<int>(v.begin(), v.end()); };
-  CK(sc->lrow_ptr.upload(to32(F.lrow_ptr)));
-  CK(sc->lrow_col.upload(F.lrow_col));
-  CK(sc->lrow_val.upload(F.lrow_val));
+  CK(sc->rseg_ptr.upload(F.rseg_ptr));
+  CK(sc->rseg_pos.upload(F.rseg_pos));
+  if (sc->contrib.n != 3 * F.rowidx.size() || !sc->contrib.p) CK(sc->contrib.alloc(3 * std::max<size_t>(1, F.rowidx.size())));
   CK(sc->sn_c0.upload(F.sn_c0));
   CK(sc->sn_w.upload(F.sn_w));
   CK(sc->sn_r.upload(F.sn_r));
@@ -117,8 +140,16 @@ static int upload_factor(dfem_scene* sc) {
   sc->lvl_ptr = F.lvl_ptr;
   sc->max_w = 1;
   for (int w : F.sn_w) sc->max_w = std::max(sc->max_w, w);
-  sc->fd = FactorDev{sc->lrow_ptr.p, sc->lrow_col.p, sc->lrow_val.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p,
-                     sc->sn_rofs.p, sc->rowidx.p, sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->lvl_sn.p};
+  sc->max_r = 0;
+  for (int r : F.sn_r) sc->max_r = std::max(sc->max_r, r);
+  const size_t shm_b = 3 * sizeof(double) * (size_t)(sc->max_w + sc->max_r);
+  if (shm_b > 200 * 1024)
+    return fail(DFEM_ERR_INVALID, "supernode row count too large for the shared-memory staging of the backward solve");
+  CK(cudaFuncSetAttribute(k_bwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm_b + 1024));
+  FactorDev fd{sc->rseg_ptr.p, sc->rseg_pos.p, sc->contrib.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p,
+               sc->sn_rofs.p, sc->rowidx.p, sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->lvl_sn.p};
+  if (std::memcmp(&fd, &sc->fd, sizeof(fd)) != 0) invalidate_graphs(sc);
+  sc->fd = fd;
   return DFEM_OK;
 }
 
@@ -217,12 +248,7 @@ static int upload_scene(dfem_scene* sc) {
   CK(cudaMemset(sc->status.p, 0, sizeof(int)));
   CK(sc->act_cur.alloc(std::max(1, s.nseg)));
   CK(cudaMemset(sc->act_cur.p, 0, sizeof(double) * std::max(1, s.nseg)));
-  sc->sd = SceneDev{s.N, s.T, s.M, s.S, s.B, s.nseg, s.h, s.damping, s.g[0], s.g[1], s.g[2],
-                    sc->mass.p, sc->gmask.p, sc->tv.p, sc->tinv.p, sc->twr.p, sc->twv.p, sc->tvol.p, sc->tE.p, sc->tnu.p,
-                    sc->tslot.p, sc->mv.p, sc->minv.p, sc->mw.p, sc->mfib.p, sc->mseg.p, sc->mslot.p, sc->seg_ptr.p,
-                    sc->seg_mus.p, sc->sv.p, sc->srest.p, sc->ssw.p, sc->sslot.p, sc->boff.p, sc->bv.p, sc->bbeta.p,
-                    sc->bw.p, sc->brest.p, sc->bslot.p, sc->vslot_ptr.p, sc->attach_jd.p, sc->hs_ptr.p, sc->hs_col.p,
-                    sc->hs_val.p};
+  refresh_scene_view(sc);
   return DFEM_OK;
 }
 
@@ -238,23 +264,22 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   CK(sc->act_all.alloc((size_t)cap * std::max(1, s.nseg)));
   CK(sc->gact.alloc((size_t)cap * std::max(1, s.nseg)));
   sc->cap_steps = cap;
-  // graphs hold the old pointers
-  if (sc->g_step) { cudaGraphExecDestroy(sc->g_step); sc->g_step = nullptr; }
-  if (sc->g_adj) { cudaGraphExecDestroy(sc->g_adj); sc->g_adj = nullptr; }
+  invalidate_graphs(sc);  // graphs hold the old pointers
   return DFEM_OK;
 }
 
 // one forward step: enqueue the kernel sequence on the stream (captured into a graph)
 static void enqueue_solve(dfem_scene* sc, Gate gate, const double* rhs, double* y) {
   const int L = (int)sc->lvl_ptr.size() - 1;
-  size_t shm = 3 * sizeof(double) * (size_t)sc->max_w;
+  size_t shm_f = 6 * sizeof(double) * (size_t)sc->max_w;                   // t and y_s of one supernode
+  size_t shm_b = 3 * sizeof(double) * (size_t)(sc->max_w + sc->max_r);     // u and the gathered x_R
   for (int l = 0; l < L; ++l) {
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_fwd_level<<<nb, 128, shm, sc->stream>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
+    k_fwd_level<<<nb, 256, shm_f, sc->stream>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
   }
   for (int l = L - 1; l >= 0; --l) {
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_bwd_level<<<nb, 128, shm, sc->stream>>>(sc->fd, sc->lvl_ptr[l], gate, y);
+    k_bwd_level<<<nb, 256, shm_b, sc->stream>>>(sc->fd, sc->lvl_ptr[l], gate, y);
   }
 }
 
@@ -346,7 +371,7 @@ int dfem_scene_create(const dfem_scene_desc* desc, int device, dfem_scene** out)
   if (!build_host_scene(*desc, sc->hs, err))
     return fail(err.find("factor") != std::string::npos ? DFEM_ERR_FACTOR : DFEM_ERR_INVALID, err);
   if (!refactorize(sc->hs.Hs, sc->hs.F, err)) return fail(DFEM_ERR_FACTOR, err);
-  CK(cudaStreamCreateWithFlags(&sc->stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreate(&sc->stream));  // blocking: orders with the legacy default stream callers use
   RC(upload_scene(sc.get()));
   RC(ensure_steps(sc.get(), 1));
   CK(cudaDeviceSynchronize());
@@ -389,6 +414,7 @@ int dfem_set_materials(dfem_scene* sc, const double* youngs, const double* poiss
   CK(cudaStreamSynchronize(sc->stream));
   if (!update_materials(sc->hs, E.data(), nu.data(), err)) return fail(DFEM_ERR_FACTOR, err);
   RC(upload_materials(sc));
+  refresh_scene_view(sc);
   CK(cudaDeviceSynchronize());
   return DFEM_OK;
 }

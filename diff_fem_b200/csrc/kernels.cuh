@@ -81,9 +81,9 @@ struct SceneDev {
 };
 
 struct FactorDev {
-  const int* lrow_ptr;
-  const int* lrow_col;
-  const double* lrow_val;
+  const int* rseg_ptr;   // row -> its contribution slots (push-form forward solve)
+  const int* rseg_pos;
+  double* contrib;       // 3 doubles per below-diagonal row of every supernode
   const int* sn_c0;
   const int* sn_w;
   const int* sn_r;

@@ -208,28 +208,28 @@ __global__ void k_gather(int N, Gate gate, const int* __restrict__ vslot_ptr, co
   st3(rhs, i, acc);
 }
 
-// Forward solve of one level: for each supernode s of the level,
-//   t = rhs_s - L_{s,<} y_<   (row-wise CSR, warp per row)
-//   y_s = Dinv_s t            (warp per row)
-__global__ void __launch_bounds__(128) k_fwd_level(FactorDev f, int lvl_begin, Gate gate,
+// Forward solve of one level, push form: for each supernode s of the level,
+//   t   = rhs_s - (contributions pushed to s's rows by its descendants)
+//   y_s = Dinv_s t                       (warp per row)
+//   contrib[R_s] = L_{R_s,s} y_s         (thread per below-diagonal row; read by ancestors)
+__global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, Gate gate,
                                                    const double* __restrict__ rhs, double* y) {
   if (gate.skip()) return;
-  extern __shared__ double tsh[];
+  extern __shared__ double tsh[];  // t (3w) then y_s (3w)
   const int s = f.lvl_sn[lvl_begin + blockIdx.x];
-  const int c0 = f.sn_c0[s], w = f.sn_w[s];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int c = warp; c < w; c += nw) {
+  const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
+  double* ysh = tsh + 3 * w;
+  for (int c = threadIdx.x; c < w; c += blockDim.x) {
     const int i = c0 + c;
-    double a0 = 0, a1 = 0, a2 = 0;
-    for (int k = f.lrow_ptr[i] + lane; k < f.lrow_ptr[i + 1]; k += 32) {
-      int j = f.lrow_col[k];
-      double l = f.lrow_val[k];
-      a0 += l * y[3 * j]; a1 += l * y[3 * j + 1]; a2 += l * y[3 * j + 2];
+    double a0 = rhs[3 * i], a1 = rhs[3 * i + 1], a2 = rhs[3 * i + 2];
+    for (int k = f.rseg_ptr[i]; k < f.rseg_ptr[i + 1]; ++k) {
+      const double* q = f.contrib + 3 * (size_t)f.rseg_pos[k];
+      a0 -= q[0]; a1 -= q[1]; a2 -= q[2];
     }
-    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
-    if (lane == 0) { tsh[3 * c] = rhs[3 * i] - a0; tsh[3 * c + 1] = rhs[3 * i + 1] - a1; tsh[3 * c + 2] = rhs[3 * i + 2] - a2; }
+    tsh[3 * c] = a0; tsh[3 * c + 1] = a1; tsh[3 * c + 2] = a2;
   }
   __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const double* Di = f.Dinv + f.sn_dofs[s];
   for (int c = warp; c < w; c += nw) {
     double a0 = 0, a1 = 0, a2 = 0;
@@ -238,27 +238,48 @@ __global__ void __launch_bounds__(128) k_fwd_level(FactorDev f, int lvl_begin, G
       a0 += dv * tsh[3 * k]; a1 += dv * tsh[3 * k + 1]; a2 += dv * tsh[3 * k + 2];
     }
     a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
-    if (lane == 0) { y[3 * (c0 + c)] = a0; y[3 * (c0 + c) + 1] = a1; y[3 * (c0 + c) + 2] = a2; }
+    if (lane == 0) {
+      y[3 * (c0 + c)] = a0; y[3 * (c0 + c) + 1] = a1; y[3 * (c0 + c) + 2] = a2;
+      ysh[3 * c] = a0; ysh[3 * c + 1] = a1; ysh[3 * c + 2] = a2;
+    }
+  }
+  __syncthreads();
+  const double* Lc = f.Lcm + f.sn_lofs[s];
+  double* out = f.contrib + 3 * (size_t)f.sn_rofs[s];
+  for (int a = threadIdx.x; a < r; a += blockDim.x) {
+    double a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll 8
+    for (int c = 0; c < w; ++c) {
+      double l = __ldg(Lc + (size_t)c * r + a);
+      a0 += l * ysh[3 * c]; a1 += l * ysh[3 * c + 1]; a2 += l * ysh[3 * c + 2];
+    }
+    out[3 * a] = a0; out[3 * a + 1] = a1; out[3 * a + 2] = a2;
   }
 }
 
 // Backward solve of one level (in place in y): for each supernode s,
 //   u = y_s - L_{R,s}^T y_R  (column-major block, warp per column)
 //   y_s = Dinv_s^T u
-__global__ void __launch_bounds__(128) k_bwd_level(FactorDev f, int lvl_begin, Gate gate, double* y) {
+__global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, Gate gate, double* y) {
   if (gate.skip()) return;
-  extern __shared__ double tsh[];
+  extern __shared__ double tsh[];  // u (3w) then the gathered ancestor rows x_R (3r)
   const int s = f.lvl_sn[lvl_begin + blockIdx.x];
   const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
   const int* R = f.rowidx + f.sn_rofs[s];
   const double* Lc = f.Lcm + f.sn_lofs[s];
+  double* xr = tsh + 3 * w;
+  for (int a = threadIdx.x; a < r; a += blockDim.x) {
+    int i = R[a];
+    xr[3 * a] = y[3 * i]; xr[3 * a + 1] = y[3 * i + 1]; xr[3 * a + 2] = y[3 * i + 2];
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int c = warp; c < w; c += nw) {
     double a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll 4
     for (int a = lane; a < r; a += 32) {
-      double l = Lc[(size_t)c * r + a];
-      int i = R[a];
-      a0 += l * y[3 * i]; a1 += l * y[3 * i + 1]; a2 += l * y[3 * i + 2];
+      double l = __ldg(Lc + (size_t)c * r + a);
+      a0 += l * xr[3 * a]; a1 += l * xr[3 * a + 1]; a2 += l * xr[3 * a + 2];
     }
     a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
     if (lane == 0) {

@@ -24,6 +24,14 @@ def _is_cuda_tensor(a) -> bool:
     return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
 
 
+def _sync_torch(*arrays):
+    """Make pending work of torch's current stream visible to the engine's stream."""
+    for a in arrays:
+        if _is_cuda_tensor(a):
+            torch.cuda.current_stream(a.device).synchronize()
+            return
+
+
 def _ptr(a):
     """(pointer, mem kind, keepalive) of a numpy array or torch tensor (FP64)."""
     if a is None:
@@ -76,6 +84,7 @@ class Scene:
         pn, mn, kn = _ptr(poisson)
         if me != mn:
             raise ValueError("youngs and poisson must live in the same memory")
+        _sync_torch(youngs, poisson)
         check(lib().dfem_set_materials(self._h, pe, pn, me))
 
     def set_activations(self, act):
@@ -102,6 +111,7 @@ class Scene:
         ptr_, _, _ = _ptr(tr)
         if mx != mv or (ma is not None and ma != mx):
             raise ValueError("x, v and act must live in the same memory")
+        _sync_torch(x, v, act)
         check(lib().dfem_step_forward(self._h, px, pv, pa, int(n_steps), pxo, pvo, ptr_, mx))
         self._last_steps = n_steps
         return (xo, vo, tr) if traj else (xo, vo)
@@ -119,6 +129,7 @@ class Scene:
         ga = mk(max(1, self._last_steps * self.nseg))
         p = [_ptr(a)[0] for a in (gx, gv, ox, ov, gE, gnu, ga)]
         mem = _ptr(gx)[1]
+        _sync_torch(gx, gv)
         check(lib().dfem_step_backward(self._h, p[0], p[1], p[2], p[3], p[4], p[5], p[6] if self.nseg else None, mem))
         act = ga[: self._last_steps * self.nseg]
         act = act.reshape(self._last_steps, self.nseg)
