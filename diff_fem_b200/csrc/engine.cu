@@ -25,6 +25,7 @@ static int fail(int code, const std::string& msg) {
   return code;
 }
 
+
 #define CK(call)                                                                             \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \
@@ -78,7 +79,7 @@ struct dfem_scene {
   DBuf<double> xt, vt, qn, c0, xk, rhs, y, slot, hist, io_a, io_b;
   DBuf<double> partial, errv;
   DBuf<unsigned> counter;
-  DBuf<int> flag, iters, step, status, write_traj;
+  DBuf<int> flag, iters, step, status, write_traj, zero;
   DBuf<double> act_all, act_cur;   // per-step activations; current activations
   DBuf<double> ckpt_x, ckpt_v, traj;
   int cap_steps = 0;
@@ -244,6 +245,7 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->errv.alloc(1));
   CK(sc->counter.alloc(1));
   CK(sc->flag.alloc(1)); CK(sc->step.alloc(1)); CK(sc->status.alloc(1)); CK(sc->write_traj.alloc(1));
+  CK(sc->zero.alloc(1));
   CK(cudaMemset(sc->counter.p, 0, sizeof(unsigned)));
   CK(cudaMemset(sc->status.p, 0, sizeof(int)));
   CK(sc->act_cur.alloc(std::max(1, s.nseg)));
@@ -507,6 +509,29 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   if (g_youngs) RC(copy_out(sc, sc->gE.p, s.T, g_youngs, mem));
   if (g_poisson) RC(copy_out(sc, sc->gnu.p, s.T, g_poisson, mem));
   if (g_act && s.nseg > 0) RC(copy_out(sc, sc->gact.p, (size_t)sc->rec_steps * s.nseg, g_act, mem));
+  CK(cudaStreamSynchronize(sc->stream));
+  return DFEM_OK;
+}
+
+int dfem_eval_local(dfem_scene* sc, const double* x, double* jd_out, int mem) {
+  if (!sc || !x || !jd_out) return fail(DFEM_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(sc->device));
+  const HostScene& s = sc->hs;
+  const size_t n3 = 3 * (size_t)s.N;
+  const int nb = sc->nblk_v;
+  const int ncons = s.T + s.M + s.S + s.B;
+  const Gate open{nullptr, nullptr, nullptr, 0};
+  RC(copy_in(sc, x, n3, sc->io_a.p, mem));
+  k_to_internal<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_internal.p, sc->io_a.p, sc->rhs.p);
+  k_set_int<<<1, 1, 0, sc->stream>>>(sc->zero.p, 0);
+  if (ncons > 0)
+    k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, open, sc->rhs.p, sc->act_cur.p, sc->zero.p, sc->slot.p);
+  // J d = attachment term + the constraints' slots (c0 := J_att d_att)
+  k_gather<<<nb, 128, 0, sc->stream>>>(s.N, open, sc->vslot_ptr.p, sc->slot.p, sc->attach_jd.p, sc->io_b.p);
+  k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_b.p, sc->io_a.p);
+  CK(cudaGetLastError());
+  sc->launches += 5;
+  RC(copy_out(sc, sc->io_a.p, n3, jd_out, mem));
   CK(cudaStreamSynchronize(sc->stream));
   return DFEM_OK;
 }

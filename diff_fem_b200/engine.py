@@ -135,6 +135,16 @@ class Scene:
         act = act.reshape(self._last_steps, self.nseg)
         return {"x": ox, "v": ov, "E": gE[: self.T], "nu": gnu[: self.T], "act": act}
 
+    def eval_local(self, x):
+        """J d(x): the local step's contribution to the global rhs at positions x."""
+        dev = _is_cuda_tensor(x)
+        out = torch.empty(3 * self.N, dtype=torch.float64, device=x.device) if dev else np.empty(3 * self.N)
+        px, mx, kx = _ptr(x)
+        po, _, _ = _ptr(out)
+        _sync_torch(x)
+        check(lib().dfem_eval_local(self._h, px, po, mx))
+        return out
+
     def iterations(self, n: Optional[int] = None) -> np.ndarray:
         n = self._last_steps if n is None else n
         out = np.zeros(n, np.int32)

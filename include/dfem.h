@@ -166,6 +166,12 @@ int dfem_step_backward(dfem_scene *scene, const double *gx_out, const double *gv
                        double *gx, double *gv, double *g_youngs, double *g_poisson,
                        double *g_activations, int mem);
 
+/* The local step alone at positions x (3N, user order): every constraint's
+ * projection d(x) and jd_out = J d(x) (3N, user order), i.e. the ori_c - b
+ * of one PD iteration.  Uses the segment activations of dfem_set_activations.
+ * Replaces World::EvaluateDVector + mJ * d (sim/fem/World.h:898-901,1194-1210). */
+int dfem_eval_local(dfem_scene *scene, const double *x, double *jd_out, int mem);
+
 /* Iteration counts of the last forward call (n_steps values), host buffer. */
 int dfem_get_iterations(const dfem_scene *scene, int32_t *iters, int32_t n);
 

@@ -42,6 +42,7 @@ def lib() -> C.CDLL:
         L.orc_forward.argtypes = [vp, pd, pd, pd, C.c_int, pd, pd, pd, pi, C.c_int]
         L.orc_backward.argtypes = [vp, pd, pd, pd, pd, pd, pd, pd]
         L.orc_lumped_masses.argtypes = [C.c_int, pd, C.c_int, pi, C.c_double, C.c_int, pd]
+        L.orc_eval_local.argtypes = [vp, pd, pd, pd]
         L.orc_corot_project.argtypes = [pd, pd, pd]
         L.orc_corot_vjp.argtypes = [pd, pd, pd, pd]
         L.orc_svd3.argtypes = [pd, pd, pd, pd]
@@ -120,6 +121,14 @@ class OracleScene:
             raise RuntimeError(f"oracle: backward failed ({rc})")
         return {"x": ox, "v": ov, "E": gE[: self.T], "nu": gnu[: self.T],
                 "act": ga[: self._steps * self.nseg].reshape(self._steps, self.nseg)}
+
+    def eval_local(self, x, act=None):
+        """J d(x) of all constraints (3N)."""
+        x = np.ascontiguousarray(x, np.float64).reshape(-1)
+        a = None if act is None else np.ascontiguousarray(act, np.float64).reshape(-1)
+        out = np.zeros(3 * self.N)
+        lib().orc_eval_local(self.h, _pd(x), _pd(a), _pd(out))
+        return out
 
     def hs_coo(self):
         cap = lib().orc_hs_coo(self.h, None, None, None, 0)

@@ -889,6 +889,16 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
   return 0;
 }
 
+/* J d(x) of all constraints (World::EvaluateDVector + mJ * d, World.h:898-901);
+ * act = per-segment activations (may be NULL = all zero). */
+int orc_eval_local(void* s, const double* x, const double* act, double* out) {
+  Scene* S = static_cast<Scene*>(s);
+  std::vector<double> zero_act(std::max(1, S->nseg), 0.0);
+  std::fill(out, out + 3 * (size_t)S->N, 0.0);
+  local_Jd(*S, x, act ? act : zero_act.data(), out, 1);
+  return 0;
+}
+
 /* Lumped masses of a tet mesh: Dfobj.h:506-525 (Is Mass Same = true: mass per
  * vertex = total / totvol * sum 0.25 vol; false: total / N). */
 int orc_lumped_masses(int N, const double* x0, int T, const int* tets, double total_mass,

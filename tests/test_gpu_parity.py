@@ -110,6 +110,19 @@ def test_set_materials_refactors():
     assert rel(xg, ro["x"]) < POS_TOL
 
 
+@pytest.mark.parametrize("builder", ["cantilever", "muscle_beam", "cloth_sheet"])
+def test_eval_local_matches_oracle(builder):
+    d = getattr(S, builder)()
+    g = Scene(d)
+    o = O.OracleScene(d)
+    rng = np.random.default_rng(9)
+    x = d.x0.reshape(-1) + 0.01 * rng.standard_normal(3 * d.n_vertices)
+    act = rng.uniform(0, 1, d.n_segments) if d.n_segments else None
+    if act is not None:
+        g.set_activations(act)
+    assert rel(g.eval_local(x), o.eval_local(x, act)) < POS_TOL
+
+
 def test_backward_before_forward_is_a_state_error():
     d = S.cantilever()
     g = Scene(d)
