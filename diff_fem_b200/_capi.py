@@ -71,6 +71,8 @@ SIGNATURES = [
     ("dfem_step_forward", C.c_int, [_VP, _VP, _VP, _VP, C.c_int32, _VP, _VP, _VP, C.c_int]),
     ("dfem_step_backward", C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, C.c_int]),
     ("dfem_eval_local", C.c_int, [_VP, _VP, _VP, C.c_int]),
+    ("dfem_eval_corotated_noalloc", C.c_int,
+     [C.c_int32, C.c_int32, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("dfem_get_iterations", C.c_int, [_VP, _pi, C.c_int32]),
     ("dfem_host_factor_solve", C.c_int, [C.POINTER(SceneDescC), _VP, _VP, C.POINTER(SceneInfoC)]),
     ("dfem_get_launch_count", C.c_int, [_VP, C.POINTER(C.c_int64)]),

@@ -25,6 +25,8 @@ static int fail(int code, const std::string& msg) {
   return code;
 }
 
+// error reporting for entry points defined in other translation units
+int report_error(int code, const std::string& msg) { return fail(code, msg); }
 
 #define CK(call)                                                                             \
   do {                                                                                       \

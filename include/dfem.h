@@ -172,6 +172,27 @@ int dfem_step_backward(dfem_scene *scene, const double *gx_out, const double *gv
  * Replaces World::EvaluateDVector + mJ * d (sim/fem/World.h:898-901,1194-1210). */
 int dfem_eval_local(dfem_scene *scene, const double *x, double *jd_out, int mem);
 
+/* Corotated-tet local step (J d of FEM tets) for callers that cannot allocate
+ * device memory — e.g. code that must hand the library only pre-allocated
+ * buffers from a pool owning the device heap, or a path where a cudaMalloc
+ * would stall other work.  No counterpart in the reference.
+ *
+ * Allocates nothing: x (3N), tets (4T, already re-oriented), inv_dm (9T,
+ * row-major Dm^-1 per tet), w_rot = mu*vol and w_vol = nu*mu*vol (T each),
+ * the vertex -> (4*tet + corner) incidence CSR vtx_ptr (N+1) / vtx_slot (4T)
+ * and jd_out (3N) are caller-owned device buffers; the work is enqueued on
+ * `stream` (a cudaStream_t, NULL = default stream) and not synchronised.
+ * The per-(tet, corner) scratch is a static device array of
+ * DFEM_NOALLOC_MAX_TETS * 12 doubles (6 MiB) that every GPU loading the
+ * library holds until exit; n_tets above the limit is rejected with
+ * DFEM_ERR_INVALID.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race. */
+#define DFEM_NOALLOC_MAX_TETS 65536
+int dfem_eval_corotated_noalloc(int32_t n_vertices, int32_t n_tets, const double *x, const int32_t *tets,
+                                const double *inv_dm, const double *w_rot, const double *w_vol,
+                                const int32_t *vtx_ptr, const int32_t *vtx_slot, double *jd_out, void *stream);
+
 /* Iteration counts of the last forward call (n_steps values), host buffer. */
 int dfem_get_iterations(const dfem_scene *scene, int32_t *iters, int32_t n);
 
