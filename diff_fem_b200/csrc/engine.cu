@@ -35,6 +35,14 @@ int report_error(int code, const std::string& msg) { return fail(code, msg); }
       return fail(DFEM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
   } while (0)
 
+#define RC(x) do { int rc_ = (x); if (rc_) return rc_; } while (0)
+
+struct LoopGraph {
+  cudaGraphExec_t exec = nullptr;
+  size_t outside = 0;  // kernels outside the loop
+  size_t body = 0;     // kernels per loop iteration
+};
+
 template <typename T>
 struct DBuf {
   T* p = nullptr;
@@ -88,17 +96,20 @@ struct dfem_scene {
   // adjoint
   DBuf<double> xkb, xtb, bb, gE, gnu, mg, gact;
   // graphs
-  cudaGraphExec_t g_step = nullptr, g_adj = nullptr;
-  size_t step_nodes = 0, adj_nodes = 0;   // kernel nodes per graph
+  LoopGraph g_step, g_adj;
+  cudaStream_t stream2 = nullptr;         // capture stream of the loop bodies
+  DBuf<int> kiter;                        // device-side iteration counter of the loops
   int64_t launches = 0;                   // kernels launched by this scene (graph nodes included)
   int rec_steps = 0;
+  std::vector<int> rec_iters;  // iteration counts of the recorded forward call
   int nblk_v = 1;   // blocks of the vertex-parallel kernels
   SceneDev sd{};
   FactorDev fd{};
   ~dfem_scene() {
-    if (g_step) cudaGraphExecDestroy(g_step);
-    if (g_adj) cudaGraphExecDestroy(g_adj);
+    if (g_step.exec) cudaGraphExecDestroy(g_step.exec);
+    if (g_adj.exec) cudaGraphExecDestroy(g_adj.exec);
     if (stream) cudaStreamDestroy(stream);
+    if (stream2) cudaStreamDestroy(stream2);
   }
 };
 
@@ -106,8 +117,8 @@ namespace dfem {
 
 // Captured graphs bake in device pointers; any change of them invalidates the graphs.
 static void invalidate_graphs(dfem_scene* sc) {
-  if (sc->g_step) { cudaGraphExecDestroy(sc->g_step); sc->g_step = nullptr; }
-  if (sc->g_adj) { cudaGraphExecDestroy(sc->g_adj); sc->g_adj = nullptr; }
+  if (sc->g_step.exec) { cudaGraphExecDestroy(sc->g_step.exec); sc->g_step.exec = nullptr; }
+  if (sc->g_adj.exec) { cudaGraphExecDestroy(sc->g_adj.exec); sc->g_adj.exec = nullptr; }
 }
 
 static void refresh_scene_view(dfem_scene* sc) {
@@ -273,72 +284,144 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
 }
 
 // one forward step: enqueue the kernel sequence on the stream (captured into a graph)
-static void enqueue_solve(dfem_scene* sc, Gate gate, const double* rhs, double* y) {
+static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
   const int L = (int)sc->lvl_ptr.size() - 1;
   size_t shm_f = 6 * sizeof(double) * (size_t)sc->max_w;                   // t and y_s of one supernode
   size_t shm_b = 3 * sizeof(double) * (size_t)(sc->max_w + sc->max_r);     // u and the gathered x_R
   for (int l = 0; l < L; ++l) {
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_fwd_level<<<nb, 256, shm_f, sc->stream>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
+    k_fwd_level<<<nb, 256, shm_f, st>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
   }
   for (int l = L - 1; l >= 0; --l) {
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_bwd_level<<<nb, 256, shm_b, sc->stream>>>(sc->fd, sc->lvl_ptr[l], gate, y);
+    k_bwd_level<<<nb, 256, shm_b, st>>>(sc->fd, sc->lvl_ptr[l], gate, y);
   }
 }
 
-static void enqueue_step(dfem_scene* sc) {
+// A time step (and the adjoint of one) is a CUDA graph: pre-loop kernels, a
+// conditional WHILE node whose body is one PD iteration, post-loop kernels.
+// The body's last kernel advances a device-side iteration counter and sets
+// the loop condition, so converged steps launch no further iterations and no
+// host round trip is needed.
+static const Gate kOpen{nullptr, nullptr, nullptr, 0};
+
+static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
+  const int nb = sc->nblk_v;
+  k_step_begin<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
+                                   sc->hist.p, sc->ckpt_x.p, sc->ckpt_v.p, sc->flag.p, sc->iters.p,
+                                   sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
+  k_loop_enter<<<1, 1, 0, st>>>(sc->kiter.p, sc->flag.p, sc->hs.K, h);
+}
+
+static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   const HostScene& s = sc->hs;
   const int nb = sc->nblk_v;
-  k_step_begin<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
-                                          sc->hist.p, sc->ckpt_x.p, sc->ckpt_v.p, sc->flag.p, sc->iters.p,
-                                          sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
-  Gate gate{sc->flag.p, nullptr, nullptr, 0};
   const int ncons = s.T + s.M + s.S + s.B;
-  for (int k = 0; k < s.K; ++k) {
-    if (ncons > 0)
-      k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, gate, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p);
-    k_gather<<<nb, 128, 0, sc->stream>>>(s.N, gate, sc->vslot_ptr.p, sc->slot.p, sc->c0.p, sc->rhs.p);
-    enqueue_solve(sc, gate, sc->rhs.p, sc->y.p);
-    k_update<<<nb, 128, 0, sc->stream>>>(s.N, gate, k, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->step.p, sc->flag.p,
-                                         sc->iters.p, sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
-  }
-  k_step_end<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->xk.p, sc->traj.p, sc->to_user.p,
-                                        sc->write_traj.p);
-  k_next_step<<<1, 1, 0, sc->stream>>>(sc->step.p);
+  if (ncons > 0)
+    k_local<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, kOpen, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p);
+  k_gather<<<nb, 128, 0, st>>>(s.N, kOpen, sc->vslot_ptr.p, sc->slot.p, sc->c0.p, sc->rhs.p);
+  enqueue_solve(sc, st, kOpen, sc->rhs.p, sc->y.p);
+  k_update<<<nb, 128, 0, st>>>(s.N, kOpen, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->step.p,
+                               sc->flag.p, sc->iters.p, sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
+  k_loop_ctl<<<1, 1, 0, st>>>(sc->kiter.p, sc->flag.p, s.K, h);
 }
 
-static void enqueue_adjoint(dfem_scene* sc) {
-  const HostScene& s = sc->hs;
+static void step_post(dfem_scene* sc, cudaStream_t st) {
   const int nb = sc->nblk_v;
-  // gradient w.r.t. the step's output lives in io_a (x) / io_b (v); overwritten with the input's
-  k_adj_begin<<<nb, 128, 0, sc->stream>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, sc->xkb.p, sc->xtb.p, sc->bb.p);
+  k_step_end<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->xk.p, sc->traj.p, sc->to_user.p,
+                                 sc->write_traj.p);
+  k_next_step<<<1, 1, 0, st>>>(sc->step.p);
+}
+
+static void adj_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
+  const HostScene& s = sc->hs;
+  // the cotangent of the step's output lives in io_a (x) / io_b (v); k_adj_end overwrites it with the input's
+  k_adj_begin<<<sc->nblk_v, 128, 0, st>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, sc->xkb.p, sc->xtb.p, sc->bb.p);
+  k_adj_loop_enter<<<1, 1, 0, st>>>(sc->kiter.p, sc->iters.p, sc->step.p, s.K, h);
+}
+
+static void adj_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
+  const HostScene& s = sc->hs;
   const int ncons = s.T + s.M + s.S + s.B;
   const int nthr = std::max(ncons, s.N);
-  for (int k = s.K - 1; k >= 0; --k) {
-    Gate gate{nullptr, sc->iters.p, sc->step.p, k};
-    enqueue_solve(sc, gate, sc->xkb.p, sc->y.p);
-    k_adj_local<<<(nthr + 127) / 128, 128, 0, sc->stream>>>(sc->sd, gate, k, sc->hist.p, sc->y.p, sc->bb.p, sc->act_all.p,
-                                                            sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
-    k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, gate, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
-    if (s.nseg > 0)
-      k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, gate, sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p,
-                                                                 sc->gact.p);
-  }
-  k_adj_end<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->xkb.p, sc->xtb.p, sc->bb.p, sc->io_a.p, sc->io_b.p);
+  enqueue_solve(sc, st, kOpen, sc->xkb.p, sc->y.p);
+  k_adj_local<<<(nthr + 127) / 128, 128, 0, st>>>(sc->sd, kOpen, sc->kiter.p, sc->step.p, sc->hist.p, sc->y.p, sc->bb.p,
+                                                  sc->act_all.p, sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+  k_adj_gather<<<sc->nblk_v, 128, 0, st>>>(s.N, kOpen, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
+  if (s.nseg > 0)
+    k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, st>>>(s.nseg, kOpen, sc->step.p, sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p,
+                                                       sc->gact.p);
+  k_adj_loop_ctl<<<1, 1, 0, st>>>(sc->kiter.p, h);
 }
 
-static int build_graph(dfem_scene* sc, void (*fn)(dfem_scene*), cudaGraphExec_t* out, size_t* nodes) {
-  cudaGraph_t g;
-  CK(cudaStreamBeginCapture(sc->stream, cudaStreamCaptureModeThreadLocal));
-  fn(sc);
-  cudaError_t e = cudaStreamEndCapture(sc->stream, &g);
-  if (e != cudaSuccess) return fail(DFEM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-  e = cudaGraphGetNodes(g, nullptr, nodes);
-  if (e != cudaSuccess) { cudaGraphDestroy(g); return fail(DFEM_ERR_CUDA, cudaGetErrorString(e)); }
-  e = cudaGraphInstantiate(out, g, 0);
+static void adj_post(dfem_scene* sc, cudaStream_t st) {
+  k_adj_end<<<sc->nblk_v, 128, 0, st>>>(sc->sd, sc->xkb.p, sc->xtb.p, sc->bb.p, sc->io_a.p, sc->io_b.p);
+}
+
+using PreFn = void (*)(dfem_scene*, cudaStream_t, cudaGraphConditionalHandle);
+using BodyFn = void (*)(dfem_scene*, cudaStream_t, cudaGraphConditionalHandle);
+using PostFn = void (*)(dfem_scene*, cudaStream_t);
+
+static int build_loop_graph(dfem_scene* sc, PreFn pre, BodyFn body, PostFn post, LoopGraph* out) {
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) { cudaGraphDestroy(g); return fail(DFEM_ERR_CUDA, std::string("conditional handle: ") + cudaGetErrorString(e)); }
+  std::string where;
+  cudaGraph_t body_g = nullptr;
+  e = cudaStreamBeginCaptureToGraph(sc->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    pre(sc, sc->stream, h);
+    cudaStreamCaptureStatus st;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraph_t cg = nullptr;
+    e = cudaStreamGetCaptureInfo(sc->stream, &st, nullptr, &cg, &deps, &nd);
+    cudaGraphNode_t cn = nullptr;
+    cudaGraphNodeParams p{};
+    if (e == cudaSuccess) {
+      p.type = cudaGraphNodeTypeConditional;
+      p.conditional.handle = h;
+      p.conditional.type = cudaGraphCondTypeWhile;
+      p.conditional.size = 1;
+      e = cudaGraphAddNode(&cn, cg, deps, nd, &p);
+      where = "add conditional node";
+    }
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(sc->stream, &cn, 1, cudaStreamSetCaptureDependencies);
+    if (e == cudaSuccess) {
+      body_g = p.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(sc->stream2, body_g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      where = "capture loop body";
+      if (e == cudaSuccess) {
+        body(sc, sc->stream2, h);
+        cudaGraph_t tmp;
+        e = cudaStreamEndCapture(sc->stream2, &tmp);
+      }
+    }
+    if (e == cudaSuccess) post(sc, sc->stream);
+    cudaGraph_t done = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(sc->stream, &done);  // always leave capture mode
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    size_t top = 0, inner = 0;
+    cudaGraphGetNodes(g, nullptr, &top);
+    cudaGraphGetNodes(body_g, nullptr, &inner);
+    out->body = inner;
+    out->outside = top - 1;  // the conditional node itself launches nothing
+    e = cudaGraphInstantiate(&out->exec, g, 0);
+    where = "instantiate";
+  }
   cudaGraphDestroy(g);
-  if (e != cudaSuccess) return fail(DFEM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  if (e != cudaSuccess) return fail(DFEM_ERR_CUDA, "loop graph (" + where + "): " + cudaGetErrorString(e));
+  return DFEM_OK;
+}
+
+static int ensure_graphs(dfem_scene* sc) {
+  if (!sc->g_step.exec) RC(build_loop_graph(sc, step_pre, step_body, step_post, &sc->g_step));
+  if (!sc->g_adj.exec) RC(build_loop_graph(sc, adj_pre, adj_body, adj_post, &sc->g_adj));
   return DFEM_OK;
 }
 
@@ -354,8 +437,6 @@ static int copy_out(dfem_scene* sc, const double* src, size_t n, double* dst, in
 }
 
 }  // namespace dfem
-
-#define RC(x) do { int rc_ = (x); if (rc_) return rc_; } while (0)
 
 extern "C" {
 
@@ -376,6 +457,8 @@ int dfem_scene_create(const dfem_scene_desc* desc, int device, dfem_scene** out)
     return fail(err.find("factor") != std::string::npos ? DFEM_ERR_FACTOR : DFEM_ERR_INVALID, err);
   if (!refactorize(sc->hs.Hs, sc->hs.F, err)) return fail(DFEM_ERR_FACTOR, err);
   CK(cudaStreamCreate(&sc->stream));  // blocking: orders with the legacy default stream callers use
+  CK(cudaStreamCreateWithFlags(&sc->stream2, cudaStreamNonBlocking));  // only used to capture loop bodies
+  CK(sc->kiter.alloc(1));
   RC(upload_scene(sc.get()));
   RC(ensure_steps(sc.get(), 1));
   CK(cudaDeviceSynchronize());
@@ -459,9 +542,8 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, traj_x ? 1 : 0);
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->status.p, 0);
   CK(cudaGetLastError());
-  if (!sc->g_step) RC(build_graph(sc, enqueue_step, &sc->g_step, &sc->step_nodes));
-  for (int st = 0; st < n_steps; ++st) CK(cudaGraphLaunch(sc->g_step, sc->stream));
-  sc->launches += 7 + (int64_t)n_steps * (int64_t)sc->step_nodes;
+  RC(ensure_graphs(sc));
+  for (int st = 0; st < n_steps; ++st) CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->xt.p, sc->io_a.p);
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->vt.p, sc->io_b.p);
   RC(copy_out(sc, sc->io_a.p, n3, x_out, mem));
@@ -469,7 +551,11 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   if (traj_x) RC(copy_out(sc, sc->traj.p, n3 * n_steps, traj_x, mem));
   int status = 0;
   CK(cudaMemcpyAsync(&status, sc->status.p, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+  sc->rec_iters.assign(n_steps, 0);
+  CK(cudaMemcpyAsync(sc->rec_iters.data(), sc->iters.p, n_steps * sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
   CK(cudaStreamSynchronize(sc->stream));
+  sc->launches += 7;
+  for (int it : sc->rec_iters) sc->launches += (int64_t)(sc->g_step.outside + (size_t)it * sc->g_step.body);
   sc->rec_steps = n_steps;
   if (status) return fail(DFEM_ERR_NONFINITE, "non-finite value in the PD iteration");
   return DFEM_OK;
@@ -492,18 +578,20 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   CK(cudaMemsetAsync(sc->gnu.p, 0, sizeof(double) * std::max(1, s.T), sc->stream));
   CK(cudaMemsetAsync(sc->gact.p, 0, sizeof(double) * (size_t)sc->rec_steps * std::max(1, s.nseg), sc->stream));
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, 0);
-  if (!sc->g_step) RC(build_graph(sc, enqueue_step, &sc->g_step, &sc->step_nodes));
-  if (!sc->g_adj) RC(build_graph(sc, enqueue_adjoint, &sc->g_adj, &sc->adj_nodes));
+  RC(ensure_graphs(sc));
   for (int st = sc->rec_steps - 1; st >= 0; --st) {
     // recompute the step's iterates from its checkpoint (the step graph re-records the same checkpoint)
     CK(cudaMemcpyAsync(sc->xt.p, sc->ckpt_x.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
     CK(cudaMemcpyAsync(sc->vt.p, sc->ckpt_v.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
     k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
-    CK(cudaGraphLaunch(sc->g_step, sc->stream));
+    CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
     k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
-    CK(cudaGraphLaunch(sc->g_adj, sc->stream));
+    CK(cudaGraphLaunch(sc->g_adj.exec, sc->stream));
   }
-  sc->launches += 5 + (int64_t)sc->rec_steps * (int64_t)(2 + sc->step_nodes + sc->adj_nodes);
+  sc->launches += 5;
+  for (int st = 0; st < sc->rec_steps && st < (int)sc->rec_iters.size(); ++st)
+    sc->launches += (int64_t)(2 + sc->g_step.outside + sc->g_adj.outside +
+                              (size_t)sc->rec_iters[st] * (sc->g_step.body + sc->g_adj.body));
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_a.p, sc->rhs.p);
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_b.p, sc->c0.p);
   RC(copy_out(sc, sc->rhs.p, n3, gx, mem));
@@ -582,12 +670,10 @@ int dfem_profile_phases(dfem_scene* sc, int32_t reps, double* ms) {
   const int nb = sc->nblk_v;
   const int ncons = s.T + s.M + s.S + s.B;
   const int nthr = std::max(ncons, s.N);
-  // open gates: forward flag cleared, adjoint iteration count of step 0 = K
-  k_set_int<<<1, 1, 0, sc->stream>>>(sc->flag.p, 0);
+  // every phase is launched ungated on the state of the last forward call (step 0, iteration 0)
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, 0);
-  k_set_int<<<1, 1, 0, sc->stream>>>(sc->iters.p, s.K);
-  Gate gf{sc->flag.p, nullptr, nullptr, 0};
-  Gate ga{nullptr, sc->iters.p, sc->step.p, 0};
+  k_set_int<<<1, 1, 0, sc->stream>>>(sc->zero.p, 0);
+  const Gate gf = kOpen, ga = kOpen;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -607,11 +693,12 @@ int dfem_profile_phases(dfem_scene* sc, int32_t reps, double* ms) {
   if (!rc && ncons > 0)
     rc = timed(0, [&] { k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, gf, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p); });
   if (!rc) rc = timed(1, [&] { k_gather<<<nb, 128, 0, sc->stream>>>(s.N, gf, sc->vslot_ptr.p, sc->slot.p, sc->c0.p, sc->rhs.p); });
-  if (!rc) rc = timed(2, [&] { enqueue_solve(sc, gf, sc->rhs.p, sc->y.p); });
+  if (!rc) rc = timed(2, [&] { enqueue_solve(sc, sc->stream, gf, sc->rhs.p, sc->y.p); });
   if (!rc && ncons > 0)
     rc = timed(3, [&] {
-      k_adj_local<<<(nthr + 127) / 128, 128, 0, sc->stream>>>(sc->sd, ga, 0, sc->hist.p, sc->y.p, sc->bb.p, sc->act_all.p,
-                                                              sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+      k_adj_local<<<(nthr + 127) / 128, 128, 0, sc->stream>>>(sc->sd, ga, sc->zero.p, sc->step.p, sc->hist.p, sc->y.p,
+                                                              sc->bb.p, sc->act_all.p, sc->slot.p, sc->gE.p, sc->gnu.p,
+                                                              sc->mg.p);
     });
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -300,11 +300,12 @@ __global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, G
   }
 }
 
-// x^{k+1} = x_t + hvf; convergence test for the next iteration
-__global__ void k_update(int N, Gate gate, int k, const double* __restrict__ xt, const double* __restrict__ z,
+// x^{k+1} = x_t + hvf; convergence test for the next iteration (k read from device memory)
+__global__ void k_update(int N, Gate gate, const int* kptr, const double* __restrict__ xt, const double* __restrict__ z,
                          double* xk, double* hist, const int* step, int* flag, int* iters,
                          double* partial, unsigned* counter, double* errv, int* status) {
   if (gate.skip()) return;
+  const int k = *kptr;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double e2 = 0;
   if (i < N) {
@@ -340,6 +341,34 @@ __global__ void k_step_end(SceneDev d, int* step, double* xt, double* vt, const 
 }
 
 __global__ void k_next_step(int* step) { *step += 1; }
+
+// Loop control of the PD iterations (body of a conditional WHILE graph node):
+// advance the device-side iteration counter and continue while not converged
+// and k < K.  The counter advances on every body execution, so the loop runs
+// at most K times whatever the convergence flag says.
+__global__ void k_loop_ctl(int* kptr, const int* flag, int K, cudaGraphConditionalHandle h) {
+  int k = *kptr + 1;
+  *kptr = k;
+  cudaGraphSetConditional(h, (*flag == 0 && k < K) ? 1u : 0u);
+}
+
+// Before the loop: run the body at all only if the first test did not converge.
+__global__ void k_loop_enter(int* kptr, const int* flag, int K, cudaGraphConditionalHandle h) {
+  *kptr = 0;
+  cudaGraphSetConditional(h, (*flag == 0 && K > 0) ? 1u : 0u);
+}
+
+// Reverse loop of the adjoint: k = iters-1 .. 0 (counter decreases every body execution).
+__global__ void k_adj_loop_enter(int* kptr, const int* iters, const int* step, int K, cudaGraphConditionalHandle h) {
+  int n = min(max(iters[*step], 0), K);  // recorded by the forward body (<= K); clamped regardless
+  *kptr = n - 1;
+  cudaGraphSetConditional(h, n > 0 ? 1u : 0u);
+}
+__global__ void k_adj_loop_ctl(int* kptr, cudaGraphConditionalHandle h) {
+  int k = *kptr - 1;
+  *kptr = k;
+  cudaGraphSetConditional(h, k >= 0 ? 1u : 0u);
+}
 __global__ void k_set_int(int* p, int v) { *p = v; }
 
 // permutation between user and internal vertex order (3 doubles per vertex)
@@ -370,11 +399,12 @@ __global__ void k_adj_begin(int N, double c, const double* gx1, const double* gv
   st3(bb, i, mk3(0.0, 0.0, 0.0));
 }
 
-__global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, int k, const double* __restrict__ hist,
-                                                   const double* __restrict__ yb, double* bb,
-                                                   const double* __restrict__ act_all, double* __restrict__ slot,
-                                                   double* gE, double* gnu, double* mg) {
+__global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const int* kptr, const int* step,
+                                                   const double* __restrict__ hist, const double* __restrict__ yb,
+                                                   double* bb, const double* __restrict__ act_all,
+                                                   double* __restrict__ slot, double* gE, double* gnu, double* mg) {
   if (gate.skip()) return;
+  const int k = *kptr;
   const double* x = hist + (size_t)k * 3 * d.N;
   const double* x1 = hist + (size_t)(k + 1) * 3 * d.N;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -425,7 +455,7 @@ __global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, int k,
       db = db + (w * c[a]) * ld3(yb, vi[a]);
       Ff = Ff + c[a] * ld3(x, vi[a]);
     }
-    double a_act = act_all[(size_t)(*gate.step) * d.nseg + d.mseg[t]];
+    double a_act = act_all[(size_t)(*step) * d.nseg + d.mseg[t]];
     mg[t] = -dot3(db, Ff);
     int4 sl = d.mslot[t];
     const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
@@ -478,14 +508,14 @@ __global__ void k_adj_gather(int N, Gate gate, const int* __restrict__ vslot_ptr
 }
 
 // activation gradient of the step: sum over the muscle constraints of each segment
-__global__ void k_seg_reduce(int nseg, Gate gate, const int* seg_ptr, const int* seg_mus, const double* mg,
-                             double* gact) {
+__global__ void k_seg_reduce(int nseg, Gate gate, const int* step, const int* seg_ptr, const int* seg_mus,
+                             const double* mg, double* gact) {
   if (gate.skip()) return;
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nseg) return;
   double s = 0;
   for (int k = seg_ptr[q]; k < seg_ptr[q + 1]; ++k) s += mg[seg_mus[k]];
-  gact[(size_t)(*gate.step) * nseg + q] += s;
+  gact[(size_t)(*step) * nseg + q] += s;
 }
 
 __global__ void k_adj_end(SceneDev d, const double* xkb, const double* xtb, const double* bb,
