@@ -402,8 +402,11 @@ bool factorize(const SparseSym& A, const double* coords, const FactorOptions& op
     F.sn_r.push_back((int)st.size());
     F.rowidx.insert(F.rowidx.end(), st.begin(), st.end());
     F.sn_rofs[s + 1] = F.sn_rofs[s] + (int64_t)st.size();
-    F.sn_lofs[s + 1] = F.sn_lofs[s] + (int64_t)st.size() * w;
-    F.sn_dofs[s + 1] = F.sn_dofs[s] + (int64_t)w * w;
+    // dense blocks start and end on 16 bytes (even count of doubles) so the GPU
+    // can move each one with a single bulk asynchronous copy
+    auto even = [](int64_t v) { return (v + 1) & ~int64_t(1); };
+    F.sn_lofs[s + 1] = F.sn_lofs[s] + even((int64_t)st.size() * w);
+    F.sn_dofs[s + 1] = F.sn_dofs[s] + even((int64_t)w * w);
   }
   // row -> contribution slots (positions in rowidx holding that row)
   F.rseg_ptr.assign(n + 1, 0);

@@ -85,6 +85,7 @@ struct dfem_scene {
   DBuf<double> contrib, Lcm, Dinv;
   std::vector<int> lvl_ptr;
   int max_w = 1, max_r = 0;
+  size_t shm_fwd = 0, shm_bwd = 0;  // dynamic shared memory of the level kernels
   // state
   DBuf<double> xt, vt, qn, c0, xk, rhs, y, slot, hist, io_a, io_b;
   DBuf<double> partial, errv;
@@ -156,12 +157,32 @@ static int upload_factor(dfem_scene* sc) {
   for (int w : F.sn_w) sc->max_w = std::max(sc->max_w, w);
   sc->max_r = 0;
   for (int r : F.sn_r) sc->max_r = std::max(sc->max_r, r);
-  const size_t shm_b = 3 * sizeof(double) * (size_t)(sc->max_w + sc->max_r);
-  if (shm_b > 200 * 1024)
-    return fail(DFEM_ERR_INVALID, "supernode row count too large for the shared-memory staging of the backward solve");
-  CK(cudaFuncSetAttribute(k_bwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm_b + 1024));
+  // dynamic shared memory of the level kernels (doubles, blocks padded to even counts):
+  //   fwd: Dinv + [L_{R,s}] + t + y_s      bwd: Dinv + [L_{R,s}] + u + x_R
+  // L_{R,s} is staged too when the largest supernode still fits.
+  auto even = [](size_t v) { return (v + 1) & ~size_t(1); };
+  size_t need_f[2] = {0, 0}, need_b[2] = {0, 0};  // [without, with] staged L
+  for (int q = 0; q < F.nsuper; ++q) {
+    size_t w = F.sn_w[q], r = F.sn_r[q];
+    size_t nseg = (size_t)(F.rseg_ptr[F.sn_c0[q] + w] - F.rseg_ptr[F.sn_c0[q]]);
+    for (int st = 0; st < 2; ++st) {
+      size_t l = st ? even(r * w) : 0;
+      // + row -> segment offsets ((w+1) ints) + gathered contributions (3 per segment)
+      need_f[st] = std::max(need_f[st], sizeof(double) * (even(w * w) + l + 6 * w + (w + 2) / 2 + 3 * nseg));
+      need_b[st] = std::max(need_b[st], sizeof(double) * (even(w * w) + l + 3 * w + 3 * r));
+    }
+  }
+  const size_t budget = 220 * 1024;
+  const int stage_l = (need_f[1] <= budget && need_b[1] <= budget) ? 1 : 0;
+  sc->shm_fwd = need_f[stage_l];
+  sc->shm_bwd = need_b[stage_l];
+  if (sc->shm_bwd > budget || sc->shm_fwd > budget)
+    return fail(DFEM_ERR_INVALID, "supernode too large for the shared-memory staging of the triangular solves");
+  CK(cudaFuncSetAttribute(k_fwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_fwd));
+  CK(cudaFuncSetAttribute(k_bwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_bwd));
   FactorDev fd{sc->rseg_ptr.p, sc->rseg_pos.p, sc->contrib.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p,
-               sc->sn_rofs.p, sc->rowidx.p, sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->lvl_sn.p};
+               sc->sn_rofs.p, sc->rowidx.p, sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->lvl_sn.p,
+               stage_l, sc->status.p};
   if (std::memcmp(&fd, &sc->fd, sizeof(fd)) != 0) invalidate_graphs(sc);
   sc->fd = fd;
   return DFEM_OK;
@@ -257,7 +278,7 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->partial.alloc(std::max(sc->nblk_v, 1)));
   CK(sc->errv.alloc(1));
   CK(sc->counter.alloc(1));
-  CK(sc->flag.alloc(1)); CK(sc->step.alloc(1)); CK(sc->status.alloc(1)); CK(sc->write_traj.alloc(1));
+  CK(sc->flag.alloc(1)); CK(sc->step.alloc(1)); CK(sc->write_traj.alloc(1));
   CK(sc->zero.alloc(1));
   CK(cudaMemset(sc->counter.p, 0, sizeof(unsigned)));
   CK(cudaMemset(sc->status.p, 0, sizeof(int)));
@@ -286,15 +307,13 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
 // one forward step: enqueue the kernel sequence on the stream (captured into a graph)
 static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
   const int L = (int)sc->lvl_ptr.size() - 1;
-  size_t shm_f = 6 * sizeof(double) * (size_t)sc->max_w;                   // t and y_s of one supernode
-  size_t shm_b = 3 * sizeof(double) * (size_t)(sc->max_w + sc->max_r);     // u and the gathered x_R
   for (int l = 0; l < L; ++l) {
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_fwd_level<<<nb, 256, shm_f, st>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
+    k_fwd_level<<<nb, 256, sc->shm_fwd, st>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
   }
   for (int l = L - 1; l >= 0; --l) {
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_bwd_level<<<nb, 256, shm_b, st>>>(sc->fd, sc->lvl_ptr[l], gate, y);
+    k_bwd_level<<<nb, 256, sc->shm_bwd, st>>>(sc->fd, sc->lvl_ptr[l], gate, y);
   }
 }
 
@@ -459,6 +478,7 @@ int dfem_scene_create(const dfem_scene_desc* desc, int device, dfem_scene** out)
   CK(cudaStreamCreate(&sc->stream));  // blocking: orders with the legacy default stream callers use
   CK(cudaStreamCreateWithFlags(&sc->stream2, cudaStreamNonBlocking));  // only used to capture loop bodies
   CK(sc->kiter.alloc(1));
+  CK(sc->status.alloc(1));  // before the factor upload, whose kernels report into it
   RC(upload_scene(sc.get()));
   RC(ensure_steps(sc.get(), 1));
   CK(cudaDeviceSynchronize());
@@ -557,6 +577,7 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   sc->launches += 7;
   for (int it : sc->rec_iters) sc->launches += (int64_t)(sc->g_step.outside + (size_t)it * sc->g_step.body);
   sc->rec_steps = n_steps;
+  if (status == DFEM_ERR_CAP) return fail(DFEM_ERR_CAP, "a bounded wait in the triangular solve gave up");
   if (status) return fail(DFEM_ERR_NONFINITE, "non-finite value in the PD iteration");
   return DFEM_OK;
 }

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "pd_math.cuh"
+#include "tma.cuh"
 
 namespace dfem {
 
@@ -94,6 +95,8 @@ struct FactorDev {
   const int* sn_dofs;
   const double* Dinv;
   const int* lvl_sn;
+  int stage_l;   // 1: the below-diagonal blocks are staged in shared memory too
+  int* status;   // error status word (6: a bounded wait gave up)
 };
 
 }  // namespace dfem

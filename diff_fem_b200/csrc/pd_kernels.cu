@@ -212,29 +212,76 @@ __global__ void k_gather(int N, Gate gate, const int* __restrict__ vslot_ptr, co
 //   t   = rhs_s - (contributions pushed to s's rows by its descendants)
 //   y_s = Dinv_s t                       (warp per row)
 //   contrib[R_s] = L_{R_s,s} y_s         (thread per below-diagonal row; read by ancestors)
+// Latency rather than bandwidth bounds these kernels (a few KB per supernode).
+// At kernel entry one thread moves the supernode's dense blocks (the inverse
+// of the diagonal block and, when it fits, the below-diagonal block) into
+// shared memory with TMA bulk copies; while they are in flight the warps sum
+// each row's descendant contributions (lanes over segments).  Everything
+// after the barrier runs from shared memory.
+
+// Stage Dinv (and L_{R,s} if stage_l) of supernode s; returns false (uniformly
+// across the CTA) when the copies did not complete within the bounded wait.
+__device__ __forceinline__ void stage_blocks_issue(const FactorDev& f, int s, int w, int r, double* Dsh, double* Lsh,
+                                                   uint64_t* bar) {
+  if (threadIdx.x == 0) {
+    const unsigned bd = (unsigned)(((w * w + 1) & ~1) * sizeof(double));
+    const unsigned bl = f.stage_l ? (unsigned)(((r * w + 1) & ~1) * sizeof(double)) : 0u;
+    mbar_expect_tx(bar, bd + bl);
+    bulk_copy_g2s(Dsh, f.Dinv + f.sn_dofs[s], bd, bar);
+    if (bl) bulk_copy_g2s(Lsh, f.Lcm + f.sn_lofs[s], bl, bar);
+  }
+}
+
+__device__ __forceinline__ bool stage_blocks_wait(const FactorDev& f, uint64_t* bar) {
+  const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0) != 0;
+  if (!ok && threadIdx.x == 0) {
+    *f.status = 6;                 // DFEM_ERR_CAP: bounded wait gave up
+    mbar_wait_bounded(bar, 0);     // give in-flight copies one more bounded chance to land
+  }
+  return ok;
+}
+
 __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, Gate gate,
                                                    const double* __restrict__ rhs, double* y) {
   if (gate.skip()) return;
-  extern __shared__ double tsh[];  // t (3w) then y_s (3w)
+  extern __shared__ __align__(16) double sh[];  // Dinv (w*w, even) | L_{R,s} (r*w, even; if staged) | t (3w) | y_s (3w)
+  __shared__ __align__(8) uint64_t bar;
   const int s = f.lvl_sn[lvl_begin + blockIdx.x];
   const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
+  double* Dsh = sh;
+  double* Lsh = sh + ((w * w + 1) & ~1);
+  double* tsh = Lsh + (f.stage_l ? ((r * w + 1) & ~1) : 0);
   double* ysh = tsh + 3 * w;
+  int* psh = reinterpret_cast<int*>(ysh + 3 * w);  // row -> segment range (w+1 ints)
+  double* qsh = ysh + 3 * w + (w + 2) / 2;         // gathered contributions (3 per segment)
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  stage_blocks_issue(f, s, w, r, Dsh, Lsh, &bar);
+  // The descendants' contributions to this supernode's rows are one contiguous
+  // range of the row-segment list (its rows are contiguous): fetch it with all
+  // threads at once, then reduce each row in a fixed order.
+  const int seg0 = f.rseg_ptr[c0], nseg = f.rseg_ptr[c0 + w] - seg0;
+  for (int c = threadIdx.x; c <= w; c += blockDim.x) psh[c] = f.rseg_ptr[c0 + c] - seg0;
+  for (int k = threadIdx.x; k < nseg; k += blockDim.x) {
+    const double* q = f.contrib + 3 * (size_t)f.rseg_pos[seg0 + k];
+    qsh[3 * k] = q[0]; qsh[3 * k + 1] = q[1]; qsh[3 * k + 2] = q[2];
+  }
   for (int c = threadIdx.x; c < w; c += blockDim.x) {
     const int i = c0 + c;
-    double a0 = rhs[3 * i], a1 = rhs[3 * i + 1], a2 = rhs[3 * i + 2];
-    for (int k = f.rseg_ptr[i]; k < f.rseg_ptr[i + 1]; ++k) {
-      const double* q = f.contrib + 3 * (size_t)f.rseg_pos[k];
-      a0 -= q[0]; a1 -= q[1]; a2 -= q[2];
-    }
-    tsh[3 * c] = a0; tsh[3 * c + 1] = a1; tsh[3 * c + 2] = a2;
+    tsh[3 * c] = rhs[3 * i]; tsh[3 * c + 1] = rhs[3 * i + 1]; tsh[3 * c + 2] = rhs[3 * i + 2];
   }
   __syncthreads();
+  for (int c = threadIdx.x; c < w; c += blockDim.x) {
+    double a0 = tsh[3 * c], a1 = tsh[3 * c + 1], a2 = tsh[3 * c + 2];
+    for (int k = psh[c]; k < psh[c + 1]; ++k) { a0 -= qsh[3 * k]; a1 -= qsh[3 * k + 1]; a2 -= qsh[3 * k + 2]; }
+    tsh[3 * c] = a0; tsh[3 * c + 1] = a1; tsh[3 * c + 2] = a2;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const double* Di = f.Dinv + f.sn_dofs[s];
+  if (!stage_blocks_wait(f, &bar)) return;  // includes the CTA barrier
   for (int c = warp; c < w; c += nw) {
     double a0 = 0, a1 = 0, a2 = 0;
     for (int k = lane; k <= c; k += 32) {
-      double dv = Di[c * w + k];
+      double dv = Dsh[c * w + k];
       a0 += dv * tsh[3 * k]; a1 += dv * tsh[3 * k + 1]; a2 += dv * tsh[3 * k + 2];
     }
     a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
@@ -244,13 +291,13 @@ __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, G
     }
   }
   __syncthreads();
-  const double* Lc = f.Lcm + f.sn_lofs[s];
+  const double* Lc = f.stage_l ? Lsh : f.Lcm + f.sn_lofs[s];
   double* out = f.contrib + 3 * (size_t)f.sn_rofs[s];
   for (int a = threadIdx.x; a < r; a += blockDim.x) {
     double a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll 8
+#pragma unroll 16
     for (int c = 0; c < w; ++c) {
-      double l = __ldg(Lc + (size_t)c * r + a);
+      double l = Lc[(size_t)c * r + a];
       a0 += l * ysh[3 * c]; a1 += l * ysh[3 * c + 1]; a2 += l * ysh[3 * c + 2];
     }
     out[3 * a] = a0; out[3 * a + 1] = a1; out[3 * a + 2] = a2;
@@ -262,37 +309,57 @@ __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, G
 //   y_s = Dinv_s^T u
 __global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, Gate gate, double* y) {
   if (gate.skip()) return;
-  extern __shared__ double tsh[];  // u (3w) then the gathered ancestor rows x_R (3r)
+  extern __shared__ __align__(16) double sh[];  // Dinv | L_{R,s} (if staged) | u (3w) | gathered ancestor rows x_R (3r)
+  __shared__ __align__(8) uint64_t bar;
   const int s = f.lvl_sn[lvl_begin + blockIdx.x];
   const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
   const int* R = f.rowidx + f.sn_rofs[s];
-  const double* Lc = f.Lcm + f.sn_lofs[s];
+  double* Dsh = sh;
+  double* Lsh = sh + ((w * w + 1) & ~1);
+  double* tsh = Lsh + (f.stage_l ? ((r * w + 1) & ~1) : 0);
   double* xr = tsh + 3 * w;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  stage_blocks_issue(f, s, w, r, Dsh, Lsh, &bar);
   for (int a = threadIdx.x; a < r; a += blockDim.x) {
     int i = R[a];
     xr[3 * a] = y[3 * i]; xr[3 * a + 1] = y[3 * i + 1]; xr[3 * a + 2] = y[3 * i + 2];
   }
-  __syncthreads();
+  for (int c = threadIdx.x; c < w; c += blockDim.x) {
+    const int i = c0 + c;
+    tsh[3 * c] = y[3 * i]; tsh[3 * c + 1] = y[3 * i + 1]; tsh[3 * c + 2] = y[3 * i + 2];
+  }
+  if (!stage_blocks_wait(f, &bar)) return;  // includes the CTA barrier
+  const double* Lc = f.stage_l ? Lsh : f.Lcm + f.sn_lofs[s];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int c = warp; c < w; c += nw) {
-    double a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll 4
+  // four columns per warp pass: four independent load streams per lane
+  for (int cb = warp; cb < w; cb += 4 * nw) {
+    double acc[4][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0;
     for (int a = lane; a < r; a += 32) {
-      double l = __ldg(Lc + (size_t)c * r + a);
-      a0 += l * xr[3 * a]; a1 += l * xr[3 * a + 1]; a2 += l * xr[3 * a + 2];
+      const double x0 = xr[3 * a], x1 = xr[3 * a + 1], x2 = xr[3 * a + 2];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int c = cb + q * nw;
+        if (c < w) {
+          double l = Lc[(size_t)c * r + a];
+          acc[q][0] += l * x0; acc[q][1] += l * x1; acc[q][2] += l * x2;
+        }
+      }
     }
-    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
-    if (lane == 0) {
-      int i = c0 + c;
-      tsh[3 * c] = y[3 * i] - a0; tsh[3 * c + 1] = y[3 * i + 1] - a1; tsh[3 * c + 2] = y[3 * i + 2] - a2;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int c = cb + q * nw;
+      double a0 = warp_sum(acc[q][0]), a1 = warp_sum(acc[q][1]), a2 = warp_sum(acc[q][2]);
+      if (lane == 0 && c < w) { tsh[3 * c] -= a0; tsh[3 * c + 1] -= a1; tsh[3 * c + 2] -= a2; }
     }
   }
   __syncthreads();
-  const double* Di = f.Dinv + f.sn_dofs[s];
   for (int c = warp; c < w; c += nw) {
     double a0 = 0, a1 = 0, a2 = 0;
     for (int k = c + lane; k < w; k += 32) {
-      double dv = Di[k * w + c];
+      double dv = Dsh[k * w + c];
       a0 += dv * tsh[3 * k]; a1 += dv * tsh[3 * k + 1]; a2 += dv * tsh[3 * k + 2];
     }
     a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
