@@ -1,0 +1,285 @@
+// contact_kernels.cuh — obstacle contact phase of a PD step on the GPU.
+//
+// After the local-global iterations, diff_fem (sim/fem/World.h:925-1023)
+// alternates (1) continuous collision detection of the soft surface vertices
+// against the static obstacle triangles (arcsim vertex-face test,
+// sim/utils/arcsim/collision.cpp:127-326) and (2) up to K Jacobi iterations of
+// the global step in velocity form, whose right-hand side at contact vertices
+// is replaced by the Coulomb-cone reaction (CollisionHandling, World.h:1317-1430).
+// The loop ends when a detection pass finds no impact.  Here the phase is one
+// conditional WHILE graph node driven by a device-side state machine
+//   state = [mode (0 detect, 1 Jacobi), pass, it, any, active]
+// whose body runs at most max_passes * (K + 2) + 1 times.
+#pragma once
+#include "kernels.cuh"
+
+namespace dfem {
+
+enum { CS_MODE = 0, CS_PASS = 1, CS_IT = 2, CS_ANY = 3, CS_ACTIVE = 4, CS_BODIES = 5, CS_SIZE = 6 };
+
+// per-step record of the phase: [passes, loop-body executions]
+__global__ void k_contact_record(const int* step, const int* state, int* rec) {
+  rec[2 * (*step)] = state[CS_PASS];
+  rec[2 * (*step) + 1] = state[CS_BODIES];
+}
+
+// ---- vertex-face CCD (one vertex moving p0 -> p1, static face q0 q1 q2) ----
+
+__device__ __forceinline__ double stp3(Vec3<double> u, Vec3<double> v, Vec3<double> w) { return dot3(u, cross3(v, w)); }
+__device__ __forceinline__ Vec3<double> unit3(Vec3<double> a) { return (1.0 / sqrt(dot3(a, a))) * a; }
+__device__ __forceinline__ double sgn1(double x) { return x < 0 ? -1.0 : 1.0; }
+
+__device__ int ccd_quadratic(double a, double b, double c, double x[2]) {
+  double d = b * b - 4 * a * c;
+  if (d < 0) { x[0] = -b / (2 * a); return 0; }
+  double q = -(b + sgn1(b) * sqrt(d)) / 2;
+  int i = 0;
+  if (fabs(a) > 1e-12 * fabs(q)) x[i++] = q / a;
+  if (fabs(q) > 1e-12 * fabs(c)) x[i++] = c / q;
+  if (i == 2 && x[0] > x[1]) { double t = x[0]; x[0] = x[1]; x[1] = t; }
+  return i;
+}
+
+__device__ double ccd_newton(double a, double b, double c, double d, double x0, int init_dir) {
+  if (init_dir != 0) {
+    double y0 = d + x0 * (c + x0 * (b + x0 * a)), ddy0 = 2 * b + x0 * (6 * a);
+    x0 += init_dir * sqrt(fabs(2 * y0 / ddy0));
+  }
+  for (int iter = 0; iter < 100; ++iter) {  // bounded like the reference's
+    double y = d + x0 * (c + x0 * (b + x0 * a));
+    double dy = c + x0 * (2 * b + x0 * 3 * a);
+    if (dy == 0) return x0;
+    double x1 = x0 - y / dy;
+    if (fabs(x0 - x1) < 1e-6) return x0;
+    x0 = x1;
+  }
+  return x0;
+}
+
+__device__ int ccd_cubic(double a, double b, double c, double d, double x[3]) {
+  // start Newton's method at 0 when the quadratic helper finds no root (the
+  // reference leaves that start uninitialised)
+  double xc[2] = {0.0, 0.0};
+  int ncrit = ccd_quadratic(3 * a, 2 * b, c, xc);
+  if (ncrit == 0) { x[0] = ccd_newton(a, b, c, d, xc[0], 0); return 1; }
+  if (ncrit == 1) return ccd_quadratic(b, c, d, x);
+  double yc0 = d + xc[0] * (c + xc[0] * (b + xc[0] * a)), yc1 = d + xc[1] * (c + xc[1] * (b + xc[1] * a));
+  int i = 0;
+  if (yc0 * a >= 0) x[i++] = ccd_newton(a, b, c, d, xc[0], -1);
+  if (yc0 * yc1 <= 0) {
+    int closer = fabs(yc0) < fabs(yc1) ? 0 : 1;
+    x[i++] = ccd_newton(a, b, c, d, xc[closer], closer == 0 ? 1 : -1);
+  }
+  if (yc1 * a <= 0) x[i++] = ccd_newton(a, b, c, d, xc[1], 1);
+  return i;
+}
+
+__device__ bool vf_impact(Vec3<double> p0, Vec3<double> p1, Vec3<double> q0, Vec3<double> q1, Vec3<double> q2,
+                          double mult, Vec3<double>* n_out) {
+  const double thick = kContactThickness * mult;
+  // swept vertex box against the face box dilated by the thickness
+  if (fmax(p0.x, p1.x) < fmin(q0.x, fmin(q1.x, q2.x)) - thick || fmin(p0.x, p1.x) > fmax(q0.x, fmax(q1.x, q2.x)) + thick) return false;
+  if (fmax(p0.y, p1.y) < fmin(q0.y, fmin(q1.y, q2.y)) - thick || fmin(p0.y, p1.y) > fmax(q0.y, fmax(q1.y, q2.y)) + thick) return false;
+  if (fmax(p0.z, p1.z) < fmin(q0.z, fmin(q1.z, q2.z)) - thick || fmin(p0.z, p1.z) > fmax(q0.z, fmax(q1.z, q2.z)) + thick) return false;
+  Vec3<double> v0 = p1 - p0;
+  Vec3<double> x1 = q0 - p0, x2 = q1 - p0, x3 = q2 - p0;
+  Vec3<double> v1 = (-1.0) * v0;  // static face: every face vertex moves by -v0 relative to the vertex
+  double a0 = stp3(x1, x2, x3);
+  double a1 = stp3(v1, x2, x3) + stp3(x1, v1, x3) + stp3(x1, x2, v1);
+  double a2 = stp3(x1, v1, v1) + stp3(v1, x2, v1) + stp3(v1, v1, x3);
+  double a3 = stp3(v1, v1, v1);
+  double t[4];
+  int nsol = ccd_cubic(a3, a2, a1, a0, t);
+  t[nsol++] = 1;
+  for (int i = 0; i < nsol; ++i) {
+    if (t[i] < 0 || t[i] > 1) continue;
+    Vec3<double> xt = p0 + t[i] * v0;
+    // signed distance to the face plane and barycentric weights
+    Vec3<double> n = cross3(unit3(q1 - q0), unit3(q2 - q0));
+    double d, w1, w2, w3;
+    if (dot3(n, n) < 1e-6) {
+      d = INFINITY; w1 = w2 = w3 = 0.0;
+    } else {
+      n = unit3(n);
+      d = dot3(xt - q0, n);
+      double b0 = stp3(q1 - xt, q2 - xt, n), b1 = stp3(q2 - xt, q0 - xt, n), b2 = stp3(q0 - xt, q1 - xt, n);
+      double sb = b0 + b1 + b2;
+      w1 = -b0 / sb; w2 = -b1 / sb; w3 = -b2 / sb;
+    }
+    bool inside = fmin(fmin(-w1, -w2), -w3) >= -1e-6;
+    if (t[i] == 1) {
+      inside = inside || sqrt(dot3(xt - q0, xt - q0)) < thick || sqrt(dot3(xt - q1, xt - q1)) < thick ||
+               sqrt(dot3(xt - q2, xt - q2)) < thick;
+      Vec3<double> e;
+      e = xt - q0 - (dot3(xt - q0, q1 - q0) / dot3(q1 - q0, q1 - q0)) * (q1 - q0);
+      inside = inside || sqrt(dot3(e, e)) < thick;
+      e = xt - q1 - (dot3(xt - q1, q2 - q1) / dot3(q2 - q1, q2 - q1)) * (q2 - q1);
+      inside = inside || sqrt(dot3(e, e)) < thick;
+      e = xt - q2 - (dot3(xt - q2, q0 - q2) / dot3(q0 - q2, q0 - q2)) * (q0 - q2);
+      inside = inside || sqrt(dot3(e, e)) < thick;
+    }
+    Vec3<double> fn = cross3(unit3(q1 - q0), unit3(q2 - q0));
+    if (dot3(n, w1 * v1 + w2 * v1 + w3 * v1) > 0) n = (-1.0) * fn; else n = fn;
+    if (fabs(d) < thick && inside) { *n_out = n; return true; }
+  }
+  return false;
+}
+
+// contact basis [n, t, b] (CollisionBrutal::computeBasis)
+__device__ __forceinline__ void contact_basis(Vec3<double> nrm, Vec3<double> B[3]) {
+  Vec3<double> tg = cross3(nrm, mk3(1.0, 0.0, 0.0));
+  if (sqrt(dot3(tg, tg)) < 1e-15) tg = cross3(nrm, mk3(0.0, 1.0, 0.0));
+  tg = unit3(tg);
+  B[0] = unit3(nrm); B[1] = tg; B[2] = unit3(cross3(nrm, tg));
+}
+
+// ---- phase kernels ---------------------------------------------------------------
+
+// Before the loop: x_n1 = PD result, xold = 0, L x_t, empty impact lists.
+__global__ void k_contact_begin(SceneDev d, ContactDev c, const double* xt, const double* xk,
+                                cudaGraphConditionalHandle h) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < d.N) {
+    st3(c.xn1, i, ld3(xk, i));
+    st3(c.xold, i, mk3(0.0, 0.0, 0.0));
+    Vec3<double> acc = mk3(0.0, 0.0, 0.0);
+    for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) acc = acc + d.hs_val[k] * ld3(xt, d.hs_col[k]);
+    st3(c.lxt, i, acc - (d.mass[i] / (d.h * d.h)) * ld3(xt, i));
+  }
+  if (i < c.nc) c.imp_cnt[i] = 0;
+  if (i == 0) {
+    for (int k = 0; k < CS_SIZE; ++k) c.state[k] = 0;
+    cudaGraphSetConditional(h, (c.nc > 0 && c.nof > 0) ? 1u : 0u);
+  }
+}
+
+// Detection pass (mode 0): every contact vertex against every obstacle face.
+__global__ void k_contact_detect(ContactDev c, const double* xt, const double* xk, int* status) {
+  if (c.state[CS_MODE] != 0) return;
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= c.nc) return;
+  int gv = c.cverts[a];
+  Vec3<double> p0 = ld3(xt, gv), p1 = ld3(xk, gv);
+  bool any = false;
+  for (int f = 0; f < c.nof; ++f) {
+    Vec3<double> n;
+    const int* fv = c.obs_f + 3 * f;
+    if (!vf_impact(p0, p1, ld3(c.obs_x, fv[0]), ld3(c.obs_x, fv[1]), ld3(c.obs_x, fv[2]), 1.0, &n)) continue;
+    any = true;
+    int cnt = c.imp_cnt[a], slot = -1;
+    for (int q = 0; q < cnt; ++q)
+      if (c.imp_face[a * kMaxImpactsPerVertex + q] == f) slot = q;
+    if (slot < 0) {
+      if (cnt >= kMaxImpactsPerVertex) { atomicExch(status, 6); continue; }
+      slot = cnt;
+      c.imp_face[a * kMaxImpactsPerVertex + slot] = f;
+      c.imp_cnt[a] = cnt + 1;
+    }
+    st3(c.imp_n, a * kMaxImpactsPerVertex + slot, n);
+  }
+  if (any) atomicOr(&c.state[CS_ANY], 1);
+}
+
+// After detection: finish when nothing was hit (or the pass cap is reached), else start Jacobi iterations.
+__global__ void k_contact_ctl_detect(ContactDev c, cudaGraphConditionalHandle h) {
+  if (c.state[CS_MODE] != 0) return;
+  if (c.state[CS_ANY] == 0 || c.state[CS_PASS] >= c.max_passes) {
+    cudaGraphSetConditional(h, 0u);
+    return;
+  }
+  c.state[CS_ANY] = 0;
+  c.state[CS_MODE] = 1;
+  c.state[CS_IT] = 0;
+  c.state[CS_PASS] += 1;
+}
+
+// Jacobi iteration, part 1 (mode 1): ori_x = x_n1 and the max-norm test against xold.
+__global__ void k_contact_prep(int N, ContactDev c, double* xk, double* partial, unsigned* counter) {
+  if (c.state[CS_MODE] != 1) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0;
+  if (i < N) {
+    Vec3<double> x = ld3(c.xn1, i);
+    st3(xk, i, x);
+    Vec3<double> dl = x - ld3(c.xold, i);
+    e = fmax(fabs(dl.x), fmax(fabs(dl.y), fabs(dl.z)));
+  }
+  // deterministic grid max
+  __shared__ double ws[32];
+  __shared__ bool last;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+  if (lane == 0) ws[warp] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) m = fmax(m, ws[w]);
+    partial[blockIdx.x] = m;
+    __threadfence();
+    last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double m = 0;
+    for (unsigned b = 0; b < gridDim.x; ++b) m = fmax(m, ((volatile double*)partial)[b]);
+    *counter = 0u;
+    bool conv = m < kConvergenceEps;
+    c.state[CS_ACTIVE] = conv ? 0 : 1;
+    if (conv) c.state[CS_MODE] = 0;  // back to detection
+  }
+}
+
+// Jacobi iteration, part 2: right-hand side in velocity form, contact reaction, relaxation, update.
+//   rhs = M v_wc + h (J d - L x_t) - h C (ori_x - x_t),  C = off-diagonal of Hs
+//   contact vertex: rhs := B r, r = -B^T rhs with the tangential part clamped to mu r_n (last impact wins)
+//   prev = alpha rhs + (1 - alpha) prev  (prev = rhs before the contact step on the first iteration)
+//   x_n1 = x_t + prev / (h diag(Hs)),  xold = ori_x
+__global__ void k_contact_rhs(SceneDev d, ContactDev c, const double* __restrict__ slot, const double* xt,
+                              const double* xk) {
+  if (c.state[CS_MODE] != 1 || c.state[CS_ACTIVE] == 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  Vec3<double> jd = ld3(d.attach_jd, i);
+  for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) jd = jd + ld3(slot, k);
+  Vec3<double> cdx = mk3(0.0, 0.0, 0.0);
+  for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) {
+    int j = d.hs_col[k];
+    if (j != i) cdx = cdx + d.hs_val[k] * (ld3(xk, j) - ld3(xt, j));
+  }
+  Vec3<double> rhs = d.mass[i] * ld3(c.vwc, i) + d.h * (jd - ld3(c.lxt, i)) - d.h * cdx;
+  const bool first = c.state[CS_IT] == 0;
+  Vec3<double> prev = first ? rhs : ld3(c.prev, i);
+  int a = c.cidx[i];
+  if (a >= 0) {
+    Vec3<double> f = rhs;
+    int cnt = c.imp_cnt[a];
+    for (int q = 0; q < cnt; ++q) {
+      Vec3<double> B[3];
+      contact_basis(ld3(c.imp_n, a * kMaxImpactsPerVertex + q), B);
+      double f0 = dot3(B[0], f), f1 = dot3(B[1], f), f2 = dot3(B[2], f);
+      if (f0 > 0) continue;  // take-off
+      double r0 = -f0, r1 = -f1, r2 = -f2;
+      double rt = sqrt(r1 * r1 + r2 * r2);
+      if (rt > c.mu * r0) { r1 *= c.mu * r0 / rt; r2 *= c.mu * r0 / rt; }
+      rhs = r0 * B[0] + r1 * B[1] + r2 * B[2];
+    }
+  }
+  prev = c.alpha * rhs + (1.0 - c.alpha) * prev;
+  st3(c.prev, i, prev);
+  st3(c.xn1, i, ld3(xt, i) + (1.0 / (d.h * c.hdiag[i])) * prev);
+  st3(c.xold, i, ld3(xk, i));
+}
+
+// End of a Jacobi iteration: count it; after K iterations return to detection.
+// (Also counts loop-body executions, for the launch statistics.)
+__global__ void k_contact_ctl_iter(ContactDev c, int K) {
+  c.state[CS_BODIES] += 1;
+  if (c.state[CS_MODE] != 1 || c.state[CS_ACTIVE] == 0) return;
+  int it = c.state[CS_IT] + 1;
+  c.state[CS_IT] = it;
+  c.state[CS_ACTIVE] = 0;
+  if (it >= K) c.state[CS_MODE] = 0;
+}
+
+}  // namespace dfem

@@ -14,6 +14,7 @@
 
 #include "../../include/dfem.h"
 #include "pd_kernels.cu"
+#include "contact_kernels.cuh"
 #include "scene.h"
 
 namespace dfem {
@@ -39,8 +40,9 @@ int report_error(int code, const std::string& msg) { return fail(code, msg); }
 
 struct LoopGraph {
   cudaGraphExec_t exec = nullptr;
-  size_t outside = 0;  // kernels outside the loop
-  size_t body = 0;     // kernels per loop iteration
+  size_t outside = 0;  // kernels outside the loops
+  size_t body = 0;     // kernels per iteration of the first loop
+  size_t body2 = 0;    // kernels per iteration of the second loop (contact phase), if any
 };
 
 template <typename T>
@@ -96,6 +98,12 @@ struct dfem_scene {
   int cap_steps = 0;
   // adjoint
   DBuf<double> xkb, xtb, bb, gE, gnu, mg, gact;
+  // obstacle contact phase
+  bool has_contact = false;
+  DBuf<int> cverts, cidx, obs_f, imp_cnt, imp_face, cstate, cpasses;
+  DBuf<double> obs_x, hdiag, imp_n, xn1, xold, cprev, lxt, vwc;
+  ContactDev cd{};
+  std::vector<int> rec_passes;
   // graphs
   LoopGraph g_step, g_adj;
   cudaStream_t stream2 = nullptr;         // capture stream of the loop bodies
@@ -284,6 +292,31 @@ static int upload_scene(dfem_scene* sc) {
   CK(cudaMemset(sc->status.p, 0, sizeof(int)));
   CK(sc->act_cur.alloc(std::max(1, s.nseg)));
   CK(cudaMemset(sc->act_cur.p, 0, sizeof(double) * std::max(1, s.nseg)));
+  // obstacle contact phase
+  const int nc = (int)s.cverts.size(), nof = (int)s.obs_f.size() / 3;
+  sc->has_contact = s.collide && nc > 0 && nof > 0;
+  if (sc->has_contact) {
+    std::vector<int> cidx(s.N, -1);
+    for (int a = 0; a < nc; ++a) cidx[s.cverts[a]] = a;
+    std::vector<double> hd(s.N, 0.0);
+    for (int i = 0; i < s.N; ++i)
+      for (int64_t k = s.Hs.ptr[i]; k < s.Hs.ptr[i + 1]; ++k)
+        if (s.Hs.col[k] == i) hd[i] = s.Hs.val[k];
+    CK(sc->cverts.upload(s.cverts));
+    CK(sc->cidx.upload(cidx));
+    CK(sc->obs_x.upload(s.obs_x));
+    CK(sc->obs_f.upload(s.obs_f));
+    CK(sc->hdiag.upload(hd));
+    CK(sc->imp_cnt.alloc(nc));
+    CK(sc->imp_face.alloc((size_t)nc * kMaxImpactsPerVertex));
+    CK(sc->imp_n.alloc((size_t)nc * kMaxImpactsPerVertex * 3));
+    CK(sc->xn1.alloc(n3)); CK(sc->xold.alloc(n3)); CK(sc->cprev.alloc(n3)); CK(sc->lxt.alloc(n3)); CK(sc->vwc.alloc(n3));
+    CK(sc->cstate.alloc(CS_SIZE));
+    CK(cudaMemset(sc->cstate.p, 0, sizeof(int) * CS_SIZE));
+    sc->cd = ContactDev{nc, nof, s.K, kMaxContactPasses, s.alpha, s.mu_obs, sc->cverts.p, sc->cidx.p, sc->obs_x.p,
+                        sc->obs_f.p, sc->hdiag.p, sc->imp_cnt.p, sc->imp_face.p, sc->imp_n.p, sc->xn1.p, sc->xold.p,
+                        sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p};
+  }
   refresh_scene_view(sc);
   return DFEM_OK;
 }
@@ -299,6 +332,8 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   CK(sc->iters.alloc(cap));
   CK(sc->act_all.alloc((size_t)cap * std::max(1, s.nseg)));
   CK(sc->gact.alloc((size_t)cap * std::max(1, s.nseg)));
+  CK(sc->cpasses.alloc(2 * (size_t)cap));
+  CK(cudaMemset(sc->cpasses.p, 0, sizeof(int) * 2 * (size_t)cap));
   sc->cap_steps = cap;
   invalidate_graphs(sc);  // graphs hold the old pointers
   return DFEM_OK;
@@ -328,8 +363,29 @@ static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle
   const int nb = sc->nblk_v;
   k_step_begin<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
                                    sc->hist.p, sc->ckpt_x.p, sc->ckpt_v.p, sc->flag.p, sc->iters.p,
-                                   sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
+                                   sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p,
+                                   sc->has_contact ? sc->vwc.p : nullptr);
   k_loop_enter<<<1, 1, 0, st>>>(sc->kiter.p, sc->flag.p, sc->hs.K, h);
+}
+
+// obstacle contact phase (second conditional loop of the step graph)
+static void contact_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
+  const int n = std::max(sc->hs.N, sc->cd.nc);
+  k_contact_begin<<<(n + 127) / 128, 128, 0, st>>>(sc->sd, sc->cd, sc->xt.p, sc->xk.p, h);
+}
+
+static void contact_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
+  const HostScene& s = sc->hs;
+  const int nb = sc->nblk_v;
+  const int ncons = s.T + s.M + s.S + s.B;
+  k_contact_detect<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd, sc->xt.p, sc->xk.p, sc->status.p);
+  k_contact_ctl_detect<<<1, 1, 0, st>>>(sc->cd, h);
+  k_contact_prep<<<nb, 128, 0, st>>>(s.N, sc->cd, sc->xk.p, sc->partial.p, sc->counter.p);
+  Gate active{nullptr, nullptr, nullptr, 0, sc->cstate.p + CS_ACTIVE};
+  if (ncons > 0)
+    k_local<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, active, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p);
+  k_contact_rhs<<<nb, 128, 0, st>>>(sc->sd, sc->cd, sc->slot.p, sc->xt.p, sc->xk.p);
+  k_contact_ctl_iter<<<1, 1, 0, st>>>(sc->cd, s.K);
 }
 
 static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
@@ -347,6 +403,7 @@ static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandl
 
 static void step_post(dfem_scene* sc, cudaStream_t st) {
   const int nb = sc->nblk_v;
+  if (sc->has_contact) k_contact_record<<<1, 1, 0, st>>>(sc->step.p, sc->cstate.p, sc->cpasses.p);
   k_step_end<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->xk.p, sc->traj.p, sc->to_user.p,
                                  sc->write_traj.p);
   k_next_step<<<1, 1, 0, st>>>(sc->step.p);
@@ -381,41 +438,53 @@ using PreFn = void (*)(dfem_scene*, cudaStream_t, cudaGraphConditionalHandle);
 using BodyFn = void (*)(dfem_scene*, cudaStream_t, cudaGraphConditionalHandle);
 using PostFn = void (*)(dfem_scene*, cudaStream_t);
 
-static int build_loop_graph(dfem_scene* sc, PreFn pre, BodyFn body, PostFn post, LoopGraph* out) {
+struct LoopStage {
+  PreFn pre;
+  BodyFn body;
+};
+
+// Graph = for each stage: pre kernels, then a conditional WHILE node with the
+// stage's body; then the post kernels.  Each stage has its own condition handle.
+static int build_loop_graph(dfem_scene* sc, const std::vector<LoopStage>& stages, PostFn post, LoopGraph* out) {
   cudaGraph_t g = nullptr;
   CK(cudaGraphCreate(&g, 0));
-  cudaGraphConditionalHandle h;
-  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
-  if (e != cudaSuccess) { cudaGraphDestroy(g); return fail(DFEM_ERR_CUDA, std::string("conditional handle: ") + cudaGetErrorString(e)); }
-  std::string where;
-  cudaGraph_t body_g = nullptr;
-  e = cudaStreamBeginCaptureToGraph(sc->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  std::string where = "capture";
+  std::vector<cudaGraph_t> bodies;
+  cudaError_t e = cudaStreamBeginCaptureToGraph(sc->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
-    pre(sc, sc->stream, h);
-    cudaStreamCaptureStatus st;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t nd = 0;
-    cudaGraph_t cg = nullptr;
-    e = cudaStreamGetCaptureInfo(sc->stream, &st, nullptr, &cg, &deps, &nd);
-    cudaGraphNode_t cn = nullptr;
-    cudaGraphNodeParams p{};
-    if (e == cudaSuccess) {
-      p.type = cudaGraphNodeTypeConditional;
-      p.conditional.handle = h;
-      p.conditional.type = cudaGraphCondTypeWhile;
-      p.conditional.size = 1;
-      e = cudaGraphAddNode(&cn, cg, deps, nd, &p);
-      where = "add conditional node";
-    }
-    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(sc->stream, &cn, 1, cudaStreamSetCaptureDependencies);
-    if (e == cudaSuccess) {
-      body_g = p.conditional.phGraph_out[0];
-      e = cudaStreamBeginCaptureToGraph(sc->stream2, body_g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-      where = "capture loop body";
+    for (const LoopStage& stage : stages) {
+      if (e != cudaSuccess) break;
+      cudaStreamCaptureStatus st;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t nd = 0;
+      cudaGraph_t cg = nullptr;
+      e = cudaStreamGetCaptureInfo(sc->stream, &st, nullptr, &cg, &deps, &nd);
+      cudaGraphConditionalHandle h{};
+      if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault);
+      if (e != cudaSuccess) { where = "conditional handle"; break; }
+      stage.pre(sc, sc->stream, h);
+      e = cudaStreamGetCaptureInfo(sc->stream, &st, nullptr, &cg, &deps, &nd);
+      cudaGraphNode_t cn = nullptr;
+      cudaGraphNodeParams p{};
       if (e == cudaSuccess) {
-        body(sc, sc->stream2, h);
-        cudaGraph_t tmp;
-        e = cudaStreamEndCapture(sc->stream2, &tmp);
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        e = cudaGraphAddNode(&cn, cg, deps, nd, &p);
+        where = "add conditional node";
+      }
+      if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(sc->stream, &cn, 1, cudaStreamSetCaptureDependencies);
+      if (e == cudaSuccess) {
+        cudaGraph_t body_g = p.conditional.phGraph_out[0];
+        bodies.push_back(body_g);
+        e = cudaStreamBeginCaptureToGraph(sc->stream2, body_g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        where = "capture loop body";
+        if (e == cudaSuccess) {
+          stage.body(sc, sc->stream2, h);
+          cudaGraph_t tmp;
+          e = cudaStreamEndCapture(sc->stream2, &tmp);
+        }
       }
     }
     if (e == cudaSuccess) post(sc, sc->stream);
@@ -425,11 +494,14 @@ static int build_loop_graph(dfem_scene* sc, PreFn pre, BodyFn body, PostFn post,
   }
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e == cudaSuccess) {
-    size_t top = 0, inner = 0;
+    size_t top = 0;
     cudaGraphGetNodes(g, nullptr, &top);
-    cudaGraphGetNodes(body_g, nullptr, &inner);
-    out->body = inner;
-    out->outside = top - 1;  // the conditional node itself launches nothing
+    out->outside = top - bodies.size();  // conditional nodes launch nothing themselves
+    for (size_t k = 0; k < 2; ++k) {
+      size_t inner = 0;
+      if (k < bodies.size()) cudaGraphGetNodes(bodies[k], nullptr, &inner);
+      (k == 0 ? out->body : out->body2) = inner;
+    }
     e = cudaGraphInstantiate(&out->exec, g, 0);
     where = "instantiate";
   }
@@ -439,8 +511,12 @@ static int build_loop_graph(dfem_scene* sc, PreFn pre, BodyFn body, PostFn post,
 }
 
 static int ensure_graphs(dfem_scene* sc) {
-  if (!sc->g_step.exec) RC(build_loop_graph(sc, step_pre, step_body, step_post, &sc->g_step));
-  if (!sc->g_adj.exec) RC(build_loop_graph(sc, adj_pre, adj_body, adj_post, &sc->g_adj));
+  if (!sc->g_step.exec) {
+    std::vector<LoopStage> st{{step_pre, step_body}};
+    if (sc->has_contact) st.push_back({contact_pre, contact_body});
+    RC(build_loop_graph(sc, st, step_post, &sc->g_step));
+  }
+  if (!sc->g_adj.exec) RC(build_loop_graph(sc, {{adj_pre, adj_body}}, adj_post, &sc->g_adj));
   return DFEM_OK;
 }
 
@@ -573,11 +649,16 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   CK(cudaMemcpyAsync(&status, sc->status.p, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
   sc->rec_iters.assign(n_steps, 0);
   CK(cudaMemcpyAsync(sc->rec_iters.data(), sc->iters.p, n_steps * sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+  sc->rec_passes.assign(2 * (size_t)n_steps, 0);
+  if (sc->has_contact)
+    CK(cudaMemcpyAsync(sc->rec_passes.data(), sc->cpasses.p, 2 * n_steps * sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
   CK(cudaStreamSynchronize(sc->stream));
   sc->launches += 7;
-  for (int it : sc->rec_iters) sc->launches += (int64_t)(sc->g_step.outside + (size_t)it * sc->g_step.body);
+  for (int st = 0; st < n_steps; ++st)
+    sc->launches += (int64_t)(sc->g_step.outside + (size_t)sc->rec_iters[st] * sc->g_step.body +
+                              (size_t)sc->rec_passes[2 * st + 1] * sc->g_step.body2);
   sc->rec_steps = n_steps;
-  if (status == DFEM_ERR_CAP) return fail(DFEM_ERR_CAP, "a bounded wait in the triangular solve gave up");
+  if (status == DFEM_ERR_CAP) return fail(DFEM_ERR_CAP, "a bounded loop or wait gave up (solve staging or contact impacts per vertex)");
   if (status) return fail(DFEM_ERR_NONFINITE, "non-finite value in the PD iteration");
   return DFEM_OK;
 }
@@ -586,11 +667,14 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
                        double* g_youngs, double* g_poisson, double* g_act, int mem) {
   if (!sc || !gx_out || !gv_out || !gx || !gv) return fail(DFEM_ERR_INVALID, "null argument");
   if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_step_backward needs a preceding dfem_step_forward");
+  for (int st = 0; st < sc->rec_steps && 2 * st < (int)sc->rec_passes.size(); ++st)
+    if (sc->rec_passes[2 * st] > 0)
+      return fail(DFEM_ERR_STATE, "the recorded forward call had obstacle contacts; the adjoint of the contact phase is not available");
   CK(cudaSetDevice(sc->device));
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N;
   const int nb = sc->nblk_v;
-  // incoming cotangents -> internal order, kept in xk (x) and vt? no: use dedicated buffers
+  // incoming cotangents -> internal order (staged through rhs / c0)
   RC(copy_in(sc, gx_out, n3, sc->rhs.p, mem));
   RC(copy_in(sc, gv_out, n3, sc->c0.p, mem));
   k_to_internal<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_internal.p, sc->rhs.p, sc->io_a.p);
@@ -644,6 +728,12 @@ int dfem_eval_local(dfem_scene* sc, const double* x, double* jd_out, int mem) {
   sc->launches += 5;
   RC(copy_out(sc, sc->io_a.p, n3, jd_out, mem));
   CK(cudaStreamSynchronize(sc->stream));
+  return DFEM_OK;
+}
+
+int dfem_get_contact_passes(const dfem_scene* sc, int32_t* passes, int32_t n) {
+  if (!sc || !passes) return fail(DFEM_ERR_INVALID, "null argument");
+  for (int st = 0; st < n; ++st) passes[st] = (2 * st < (int)sc->rec_passes.size()) ? sc->rec_passes[2 * st] : 0;
   return DFEM_OK;
 }
 

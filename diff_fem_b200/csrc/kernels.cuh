@@ -29,9 +29,11 @@ struct Gate {
   const int* iters;  // adjoint: per-step iteration counts
   const int* step;   // adjoint: current step index
   int k;
+  const int* active = nullptr;  // contact phase: run only while *active == 1
   __device__ __forceinline__ bool skip() const {
     if (flag && *flag) return true;
     if (iters && k >= iters[*step]) return true;
+    if (active && *active != 1) return true;
     return false;
   }
 };
@@ -79,6 +81,29 @@ struct SceneDev {
   const int* hs_ptr;
   const int* hs_col;
   const double* hs_val;
+};
+
+// Contact phase state (World::ProjectiveDynamicsMethod, sim/fem/World.h:925-1023).
+constexpr int kMaxImpactsPerVertex = 4;
+constexpr int kMaxContactPasses = 64;       // the reference's detection loop has no cap
+constexpr double kContactThickness = 1e-4;  // arcsim Impact::thickness
+struct ContactDev {
+  int nc, nof, K, max_passes;
+  double alpha, mu;
+  const int* cverts;      // contact vertices (internal ids)
+  const int* cidx;        // N: contact index or -1
+  const double* obs_x;    // 3 per obstacle vertex
+  const int* obs_f;       // 3 per obstacle face
+  const double* hdiag;    // N: diagonal of Hs
+  int* imp_cnt;           // nc
+  int* imp_face;          // nc * kMax
+  double* imp_n;          // nc * kMax * 3
+  double* xn1;            // 3N: x_n1 of the reference's contact loop
+  double* xold;           // 3N
+  double* prev;           // 3N: relaxed rhs
+  double* lxt;            // 3N: L x_t
+  double* vwc;            // 3N: v + g h of the step
+  int* state;             // [mode, pass, it, any, active]
 };
 
 struct FactorDev {

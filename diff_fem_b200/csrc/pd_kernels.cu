@@ -84,7 +84,7 @@ __device__ __forceinline__ Mat3<double> deformation(const double G[4][3], const 
 __global__ void k_step_begin(SceneDev d, const int* step, double* xt, double* vt, double* qn,
                              double* c0, double* xk, double* hist, double* ckpt_x, double* ckpt_v,
                              int* flag, int* iters, double* partial, unsigned* counter, double* errv,
-                             int* status) {
+                             int* status, double* vwc_out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int s = *step;
   double q2 = 0;
@@ -95,6 +95,7 @@ __global__ void k_step_begin(SceneDev d, const int* step, double* xt, double* vt
     // v_wc = v + h M^-1 f_ext (f_ext = 0), q_n = x + h v_wc
     double gm = d.gmask[i] * d.h;
     Vec3<double> vwc = mk3(v.x + gm * d.g0, v.y + gm * d.g1, v.z + gm * d.g2);
+    if (vwc_out) st3(vwc_out, i, vwc);
     Vec3<double> q = x + d.h * vwc;
     st3(qn, i, q);
     st3(xk, i, q);

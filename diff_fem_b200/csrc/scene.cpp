@@ -154,7 +154,7 @@ void build_slots(HostScene& s) {
 
 void renumber(HostScene& s, const std::vector<int>& to_int) {
   auto remap = [&](std::vector<int>& v) { for (int& i : v) i = to_int[i]; };
-  remap(s.tv); remap(s.mv); remap(s.sv); remap(s.bv); remap(s.av);
+  remap(s.tv); remap(s.mv); remap(s.sv); remap(s.bv); remap(s.av); remap(s.cverts);
   std::vector<double> x(3 * (size_t)s.N), m(s.N), g(s.N);
   for (int i = 0; i < s.N; ++i) {
     int j = to_int[i];
@@ -213,6 +213,19 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& s, std::string& err) 
     REQ(element(d.x0, d.tets + 4 * e, &s.tv[4 * e], &s.tinv[9 * e], s.tvol[e]), "descriptor: degenerate tet (zero volume)");
     REQ(std::isfinite(s.tE[e]) && std::isfinite(s.tnu[e]) && s.tnu[e] > -1.0, "descriptor: invalid material");
   }
+  REQ(d.n_contact_vertices >= 0 && d.n_obstacle_vertices >= 0 && d.n_obstacle_faces >= 0, "descriptor: negative contact count");
+  REQ(d.n_contact_vertices == 0 || d.contact_vertices, "descriptor: contact_vertices missing");
+  REQ(inrange(d.contact_vertices, d.n_contact_vertices), "descriptor: contact vertex out of range");
+  REQ(d.n_obstacle_faces == 0 || (d.obstacle_faces && d.obstacle_x), "descriptor: obstacle arrays missing");
+  for (int64_t k = 0; k < 3LL * d.n_obstacle_faces; ++k)
+    REQ(d.obstacle_faces[k] >= 0 && d.obstacle_faces[k] < d.n_obstacle_vertices, "descriptor: obstacle face index out of range");
+  s.collide = d.handle_collision != 0;
+  s.alpha = d.alpha;
+  s.mu_obs = d.obstacle_friction;
+  s.cverts.assign(d.contact_vertices, d.contact_vertices + d.n_contact_vertices);
+  s.obs_x.assign(d.obstacle_x, d.obstacle_x + 3 * (size_t)d.n_obstacle_vertices);
+  s.obs_f.assign(d.obstacle_faces, d.obstacle_faces + 3 * (size_t)d.n_obstacle_faces);
+
   s.A = d.n_attach;
   s.av.assign(d.attach_vertex, d.attach_vertex + s.A);
   s.ap.assign(d.attach_target, d.attach_target + 3 * (size_t)s.A);

@@ -44,6 +44,13 @@ struct HostScene {
   std::vector<int> av;
   std::vector<double> ap, ak;
 
+  // obstacle contact (internal ids for the soft surface vertices)
+  bool collide = false;
+  double alpha = 1.0, mu_obs = 1.0;
+  std::vector<int> cverts;
+  std::vector<double> obs_x;
+  std::vector<int> obs_f;
+
   int nslots = 0;
   std::vector<int> vslot_ptr;           // N+1, slots sorted by vertex
 

@@ -151,6 +151,12 @@ class Scene:
         check(lib().dfem_get_iterations(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)), int(n)))
         return out
 
+    def contact_passes(self, n: Optional[int] = None) -> np.ndarray:
+        n = self._last_steps if n is None else n
+        out = np.zeros(n, np.int32)
+        check(lib().dfem_get_contact_passes(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)), int(n)))
+        return out
+
     def launch_count(self) -> int:
         n = C.c_int64()
         check(lib().dfem_get_launch_count(self._h, C.byref(n)))

@@ -296,6 +296,73 @@ def muscle_beam(nx: int = 8, ny: int = 3, nz: int = 3, n_chains: int = 2, n_seg:
     )
 
 
+# ------------------------------------------------------------------ contact ---
+
+def tet_surface(tets: np.ndarray):
+    """Boundary triangles of a tet mesh (faces used by exactly one tet) and the
+    surface vertices in first-appearance order — the contact set of diff_fem
+    ``Dfobj::Initialize`` (sim/Dfobj.h:542-565), found with a hash instead of
+    the reference's O(F^2) duplicate test.  Faces are oriented outward."""
+    faces = {}
+    for t, tet in enumerate(tets):
+        for drop in range(4):
+            f = tuple(int(tet[k]) for k in range(4) if k != drop)
+            key = tuple(sorted(f))
+            faces.setdefault(key, []).append((t, drop, f))
+    tris, verts, seen = [], [], set()
+    for key, lst in faces.items():
+        if len(lst) != 1:
+            continue
+        t, drop, f = lst[0]
+        tris.append((t, drop, f))
+    return tris
+
+
+def surface_of(x0: np.ndarray, tets: np.ndarray):
+    """(surface faces (F,3) outward, contact vertices in first-appearance order)."""
+    out_f, verts, seen = [], [], set()
+    for t, drop, f in tet_surface(tets):
+        a, b, c = f
+        opp = x0[tets[t][drop]]
+        n = np.cross(x0[b] - x0[a], x0[c] - x0[a])
+        if np.dot(n, opp - x0[a]) > 0:
+            a, b = b, a
+        out_f.append((a, b, c))
+        for v in (a, b, c):
+            if v not in seen:
+                seen.add(v)
+                verts.append(v)
+    return np.asarray(out_f, np.int32), np.asarray(verts, np.int32)
+
+
+def ground_quad(y: float, half: float, center=(0.0, 0.0)):
+    """Static ground obstacle: one quad (two triangles) at height y, normal +y."""
+    cx, cz = center
+    xs = np.array([[cx - half, y, cz - half], [cx + half, y, cz - half], [cx + half, y, cz + half], [cx - half, y, cz + half]])
+    faces = np.array([[0, 2, 1], [0, 3, 2]], np.int32)
+    return xs, faces
+
+
+def drop_box(nx: int = 4, ny: int = 2, nz: int = 4, height: float = 0.02, v0: float = -1.0,
+             mu: float = 1.0, precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Small soft box dropped onto a ground quad (obstacle contact parity cases)."""
+    edge = 0.05
+    x0, tets = cube_grid(nx, ny, nz, edge, origin=(0.0, height, 0.0))
+    mass = lumped_masses(x0, tets, 1000.0 * nx * ny * nz * edge ** 3, True)
+    faces, cverts = surface_of(x0, tets)
+    gx, gf = ground_quad(0.0, 1.0, center=(0.5 * nx * edge, 0.5 * nz * edge))
+    T = tets.shape[0]
+    d = SceneDesc(
+        x0=x0, mass=mass, tets=tets, youngs=np.full(T, 5e4), poisson=np.full(T, 0.3),
+        contact_vertices=cverts, contact_faces=faces, obstacle_x=gx, obstacle_faces=gf,
+        handle_collision=True, obstacle_friction=mu,
+        time_step=1.0 / 60.0, max_iterations=15, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name=f"drop_box_{nx}x{ny}x{nz}",
+    )
+    d.initial_velocity = np.tile([0.0, v0, 0.0], x0.shape[0])
+    return d
+
+
 # -------------------------------------------------------------------- cloth ---
 
 def cloth_grid(nv_x: int, nv_z: int, edge: float, origin=(0.0, 0.0, 0.0)):

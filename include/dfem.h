@@ -193,6 +193,11 @@ int dfem_eval_corotated_noalloc(int32_t n_vertices, int32_t n_tets, const double
                                 const double *inv_dm, const double *w_rot, const double *w_vol,
                                 const int32_t *vtx_ptr, const int32_t *vtx_slot, double *jd_out, void *stream);
 
+/* Contact passes (detection rounds that found impacts) of each step of the
+ * last forward call, host buffer of n values (0 without obstacle contact).
+ * The loop of World::ProjectiveDynamicsMethod (sim/fem/World.h:928-1022). */
+int dfem_get_contact_passes(const dfem_scene *scene, int32_t *passes, int32_t n);
+
 /* Iteration counts of the last forward call (n_steps values), host buffer. */
 int dfem_get_iterations(const dfem_scene *scene, int32_t *iters, int32_t n);
 

@@ -43,6 +43,8 @@ def lib() -> C.CDLL:
         L.orc_backward.argtypes = [vp, pd, pd, pd, pd, pd, pd, pd]
         L.orc_lumped_masses.argtypes = [C.c_int, pd, C.c_int, pi, C.c_double, C.c_int, pd]
         L.orc_eval_local.argtypes = [vp, pd, pd, pd]
+        L.orc_contact_passes.argtypes = [vp, pi, C.c_int]
+        L.orc_vf_impact.argtypes = [pd, pd, pd, pd, pd, C.c_double, pd]
         L.orc_corot_project.argtypes = [pd, pd, pd]
         L.orc_corot_vjp.argtypes = [pd, pd, pd, pd]
         L.orc_svd3.argtypes = [pd, pd, pd, pd]
@@ -130,6 +132,11 @@ class OracleScene:
         lib().orc_eval_local(self.h, _pd(x), _pd(a), _pd(out))
         return out
 
+    def contact_passes(self):
+        out = np.zeros(max(1, self._steps), np.int32)
+        lib().orc_contact_passes(self.h, _pi(out), self._steps)
+        return out[: self._steps]
+
     def hs_coo(self):
         cap = lib().orc_hs_coo(self.h, None, None, None, 0)
         r, c, v = np.zeros(cap, np.int32), np.zeros(cap, np.int32), np.zeros(cap)
@@ -167,6 +174,14 @@ def svd3(F):
     s = np.zeros(3)
     lib().orc_svd3(_pd(F), _pd(U), _pd(s), _pd(V))
     return np.array(U), s, np.array(V)
+
+
+def vf_impact(p0, p1, q0, q1, q2, mult=1.0):
+    """One vertex-face CCD test; returns (hit, normal)."""
+    a = [np.ascontiguousarray(v, np.float64) for v in (p0, p1, q0, q1, q2)]
+    n = np.zeros(3)
+    hit = lib().orc_vf_impact(*[_pd(v) for v in a], float(mult), _pd(n))
+    return bool(hit), n
 
 
 def lumped_masses(x0, tets, total_mass, is_mass_same=True):

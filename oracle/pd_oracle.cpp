@@ -45,6 +45,8 @@
 #include <queue>
 #include <string>
 #include <vector>
+#include <array>
+#include <limits>
 #include <thread>
 
 #include "../include/dfem.h"
@@ -269,6 +271,15 @@ struct Scene {
   std::vector<int> sp_v; std::vector<double> sp_rest, sp_w;
   std::vector<Bend> bends;
   double h = 0.01, damping = 1.0; int K = 10; V3 g{0, 0, 0};
+  /* contact: World::ProjectiveDynamicsMethod contact phase (World.h:925-1023),
+     obstacle branch of CollisionHandling (World.h:1317-1430), vertex-face CCD */
+  bool collide = false;
+  double alpha = 1.0, mu_obs = 1.0;
+  int max_passes = 64;
+  std::vector<int> cverts;
+  std::vector<V3> obs_x;
+  std::vector<std::array<int, 3>> obs_f;
+  int last_passes = 0;
   /* envelope Cholesky of Hs in RCM order */
   std::vector<int> perm, iperm;  /* perm[new] = old */
   std::vector<int> first;        /* first column of row i in the envelope */
@@ -282,6 +293,7 @@ struct Scene {
   std::vector<double> rec_x, rec_v;        /* step-start states */
   std::vector<double> rec_act;             /* per step activations */
   std::vector<int> rec_iters;
+  std::vector<int> rec_passes;             /* contact passes per step */
 };
 
 static void add_H(std::vector<std::vector<std::pair<int, double>>>& rows, int i, int j, double v) {
@@ -593,6 +605,207 @@ static void step_prep(const Scene& S, const double* x, const double* v, double* 
   }
 }
 
+/* ---- contact ------------------------------------------------------------------
+ * Vertex-face continuous collision test restated from the arcsim routines the
+ * reference calls (sim/utils/arcsim/collision.cpp:127-326):  the vertex moves
+ * from its step-start position p0 to p1, the obstacle face is static; the
+ * times where the four points are coplanar are the roots in [0,1] of a cubic
+ * (plus t = 1); at each, an impact is reported when the vertex is within
+ * thickness * mult of the face plane and inside the face (at t = 1 also
+ * within that distance of a face vertex or edge line).  The normal is the
+ * (unnormalised) face normal oriented against the relative approach. */
+static const double kThickness = 1e-4;  /* Impact::thickness */
+
+static inline double stp(V3 u, V3 v, V3 w) { return dot(u, cross(v, w)); }
+static inline V3 normalize(V3 a) { double n = norm(a); return (1.0 / n) * a; }
+static inline double sgnd(double x) { return x < 0 ? -1.0 : 1.0; }
+
+static int ccd_quadratic(double a, double b, double c, double x[2]) {
+  double d = b * b - 4 * a * c;
+  if (d < 0) { x[0] = -b / (2 * a); return 0; }
+  double q = -(b + sgnd(b) * std::sqrt(d)) / 2;
+  int i = 0;
+  if (std::fabs(a) > 1e-12 * std::fabs(q)) x[i++] = q / a;
+  if (std::fabs(q) > 1e-12 * std::fabs(c)) x[i++] = c / q;
+  if (i == 2 && x[0] > x[1]) std::swap(x[0], x[1]);
+  return i;
+}
+
+static double ccd_newton(double a, double b, double c, double d, double x0, int init_dir) {
+  if (init_dir != 0) {
+    double y0 = d + x0 * (c + x0 * (b + x0 * a)), ddy0 = 2 * b + x0 * (6 * a);
+    x0 += init_dir * std::sqrt(std::fabs(2 * y0 / ddy0));
+  }
+  for (int iter = 0; iter < 100; ++iter) {
+    double y = d + x0 * (c + x0 * (b + x0 * a));
+    double dy = c + x0 * (2 * b + x0 * 3 * a);
+    if (dy == 0) return x0;
+    double x1 = x0 - y / dy;
+    if (std::fabs(x0 - x1) < 1e-6) return x0;
+    x0 = x1;
+  }
+  return x0;
+}
+
+static int ccd_cubic(double a, double b, double c, double d, double x[3]) {
+  /* arcsim's solve_quadratic leaves xc[0] unset when it finds no root and the
+     discriminant is >= 0 (the linear case of a static face); the reference
+     then starts Newton's method from an uninitialised value.  0 here. */
+  double xc[2] = {0.0, 0.0};
+  int ncrit = ccd_quadratic(3 * a, 2 * b, c, xc);
+  if (ncrit == 0) { x[0] = ccd_newton(a, b, c, d, xc[0], 0); return 1; }
+  if (ncrit == 1) return ccd_quadratic(b, c, d, x);
+  double yc[2] = {d + xc[0] * (c + xc[0] * (b + xc[0] * a)), d + xc[1] * (c + xc[1] * (b + xc[1] * a))};
+  int i = 0;
+  if (yc[0] * a >= 0) x[i++] = ccd_newton(a, b, c, d, xc[0], -1);
+  if (yc[0] * yc[1] <= 0) {
+    int closer = std::fabs(yc[0]) < std::fabs(yc[1]) ? 0 : 1;
+    x[i++] = ccd_newton(a, b, c, d, xc[closer], closer == 0 ? 1 : -1);
+  }
+  if (yc[1] * a <= 0) x[i++] = ccd_newton(a, b, c, d, xc[1], 1);
+  return i;
+}
+
+static double signed_vf(V3 x, V3 y0, V3 y1, V3 y2, V3* n, double w[4]) {
+  *n = cross(normalize(y1 - y0), normalize(y2 - y0));
+  if (dot(*n, *n) < 1e-6) return std::numeric_limits<double>::infinity();
+  *n = normalize(*n);
+  double h = dot(x - y0, *n);
+  double b0 = stp(y1 - x, y2 - x, *n), b1 = stp(y2 - x, y0 - x, *n), b2 = stp(y0 - x, y1 - x, *n);
+  w[0] = 1; w[1] = -b0 / (b0 + b1 + b2); w[2] = -b1 / (b0 + b1 + b2); w[3] = -b2 / (b0 + b1 + b2);
+  return h;
+}
+
+/* vertex (p0 -> p1) against a static face (q0, q1, q2); mult = 1 for obstacles */
+static bool vf_impact(V3 p0, V3 p1, V3 q0, V3 q1, V3 q2, double mult, V3* n_out) {
+  const double thick = kThickness * mult;
+  /* box overlap of the vertex's swept box and the face box dilated by thick (collision.cpp:132) */
+  double lo[3], hi[3], flo[3], fhi[3];
+  const double pv[2][3] = {{p0.x, p0.y, p0.z}, {p1.x, p1.y, p1.z}};
+  const double qv[3][3] = {{q0.x, q0.y, q0.z}, {q1.x, q1.y, q1.z}, {q2.x, q2.y, q2.z}};
+  for (int c = 0; c < 3; ++c) {
+    lo[c] = std::min(pv[0][c], pv[1][c]); hi[c] = std::max(pv[0][c], pv[1][c]);
+    flo[c] = std::min(qv[0][c], std::min(qv[1][c], qv[2][c])) - thick;
+    fhi[c] = std::max(qv[0][c], std::max(qv[1][c], qv[2][c])) + thick;
+    if (hi[c] < flo[c] || lo[c] > fhi[c]) return false;
+  }
+  V3 x0 = p0, v0 = p1 - p0;
+  V3 x1 = q0 - x0, x2 = q1 - x0, x3 = q2 - x0;
+  V3 v1 = -1.0 * v0, v2 = -1.0 * v0, v3 = -1.0 * v0;  /* static face: relative velocities */
+  double a0 = stp(x1, x2, x3);
+  double a1 = stp(v1, x2, x3) + stp(x1, v2, x3) + stp(x1, x2, v3);
+  double a2 = stp(x1, v2, v3) + stp(v1, x2, v3) + stp(v1, v2, x3);
+  double a3 = stp(v1, v2, v3);
+  double t[4];
+  int nsol = ccd_cubic(a3, a2, a1, a0, t);
+  t[nsol++] = 1;
+  for (int i = 0; i < nsol; ++i) {
+    if (t[i] < 0 || t[i] > 1) continue;
+    V3 xt = p0 + t[i] * v0;
+    V3 n{0, 0, 0};
+    double w[4] = {0, 0, 0, 0};
+    double d = signed_vf(xt, q0, q1, q2, &n, w);
+    bool inside = std::min(std::min(-w[1], -w[2]), -w[3]) >= -1e-6;
+    if (t[i] == 1) {
+      inside = inside || norm(xt - q0) < thick || norm(xt - q1) < thick || norm(xt - q2) < thick;
+      inside = inside || norm(xt - q0 - (dot(xt - q0, q1 - q0) / dot(q1 - q0, q1 - q0)) * (q1 - q0)) < thick;
+      inside = inside || norm(xt - q1 - (dot(xt - q1, q2 - q1) / dot(q2 - q1, q2 - q1)) * (q2 - q1)) < thick;
+      inside = inside || norm(xt - q2 - (dot(xt - q2, q0 - q2) / dot(q0 - q2, q0 - q2)) * (q0 - q2)) < thick;
+    }
+    V3 fn = cross(normalize(q1 - q0), normalize(q2 - q0));
+    if (dot(n, w[1] * v1 + w[2] * v2 + w[3] * v3) > 0) n = -1.0 * fn; else n = fn;
+    if (std::fabs(d) < thick && inside) { *n_out = n; return true; }
+  }
+  return false;
+}
+
+/* contact basis [n, t, b] (CollisionBrutal::computeBasis, collisionBrutal.h:408-426) */
+static void contact_basis(V3 normal, V3 B[3]) {
+  V3 tg = cross(normal, V3{1, 0, 0});
+  if (norm(tg) < 1e-15) tg = cross(normal, V3{0, 1, 0});
+  tg = normalize(tg);
+  V3 bt = normalize(cross(normal, tg));
+  B[0] = normalize(normal); B[1] = tg; B[2] = bt;
+}
+
+struct ObsImpact { int face; V3 n; };
+
+/* Contact phase of ProjectiveDynamicsMethod (World.h:925-1023), obstacle
+ * contacts only.  ori_x enters as the PD result and leaves as the returned
+ * positions; x_n1 follows the reference's (x_n1, ori_x) bookkeeping exactly. */
+static void contact_phase(Scene& S, const double* x_t, const double* vwc, const double* act, double* ori_x) {
+  const int N = S.N, n3 = 3 * N, nc = (int)S.cverts.size();
+  S.last_passes = 0;
+  if (!S.collide || nc == 0 || S.obs_f.empty()) return;
+  std::vector<std::vector<ObsImpact>> imp(nc);
+  std::vector<double> xold(n3, 0.0), x_n1(ori_x, ori_x + n3), rhs(n3), prev(n3, 0.0), jd(n3), Lxt(n3), Hx(n3);
+  /* L x_t = Hs x_t - M/h^2 x_t ; C = Hs - diag(Hs) */
+  H_mul(S, x_t, Hx.data());
+  const double ih2 = 1.0 / (S.h * S.h);
+  std::vector<double> hd(N, 0.0);
+  for (int i = 0; i < N; ++i) {
+    for (auto& e : S.Hrows[i]) if (e.first == i) hd[i] = e.second;
+    for (int c = 0; c < 3; ++c) Lxt[3 * i + c] = Hx[3 * i + c] - S.mass[i] * ih2 * x_t[3 * i + c];
+  }
+  for (int pass = 0; pass < S.max_passes; ++pass) {
+    /* detection at ori_x (vertex start positions: x_t) */
+    bool any = false;
+    for (int a = 0; a < nc; ++a) {
+      int gv = S.cverts[a];
+      V3 p0 = getx(x_t, gv), p1 = getx(ori_x, gv);
+      for (int f = 0; f < (int)S.obs_f.size(); ++f) {
+        V3 n;
+        if (!vf_impact(p0, p1, S.obs_x[S.obs_f[f][0]], S.obs_x[S.obs_f[f][1]], S.obs_x[S.obs_f[f][2]], 1.0, &n)) continue;
+        any = true;
+        bool found = false;
+        for (auto& r : imp[a]) if (r.face == f) { r.n = n; found = true; }
+        if (!found) imp[a].push_back({f, n});
+      }
+    }
+    if (!any) break;
+    S.last_passes = pass + 1;
+    for (int it = 0; it < S.K; ++it) {
+      for (int k = 0; k < n3; ++k) ori_x[k] = x_n1[k];
+      double err = 0;
+      for (int k = 0; k < n3; ++k) err = std::max(err, std::fabs(ori_x[k] - xold[k]));
+      if (err < 5e-7) break;
+      std::fill(jd.begin(), jd.end(), 0.0);
+      local_Jd(S, ori_x, act, jd.data(), 1);
+      /* m_rhs_speed = M v_wc + h (J d - L x_t) - h^2 C (ori_x - x_t)/h */
+      for (int i = 0; i < N; ++i) {
+        double cdx[3] = {0, 0, 0};
+        for (auto& e : S.Hrows[i])
+          if (e.first != i)
+            for (int c = 0; c < 3; ++c) cdx[c] += e.second * (ori_x[3 * e.first + c] - x_t[3 * e.first + c]);
+        for (int c = 0; c < 3; ++c)
+          rhs[3 * i + c] = S.mass[i] * vwc[3 * i + c] + S.h * (jd[3 * i + c] - Lxt[3 * i + c]) - S.h * cdx[c];
+      }
+      if (it == 0) prev = rhs;
+      /* CollisionHandling, obstacle contacts, no self-collision: rhs of the
+         contact vertex := B r (overwritten; the last contact wins) */
+      for (int a = 0; a < nc; ++a) {
+        int gv = S.cverts[a];
+        V3 f = getx(rhs.data(), gv);
+        for (auto& r : imp[a]) {
+          V3 B[3];
+          contact_basis(r.n, B);
+          double fl[3] = {dot(B[0], f), dot(B[1], f), dot(B[2], f)};
+          if (fl[0] > 0) continue;
+          double rr[3] = {-fl[0], -fl[1], -fl[2]};
+          double rt = std::sqrt(rr[1] * rr[1] + rr[2] * rr[2]);
+          if (rt > S.mu_obs * rr[0]) { rr[1] *= S.mu_obs * rr[0] / rt; rr[2] *= S.mu_obs * rr[0] / rt; }
+          V3 out = rr[0] * B[0] + rr[1] * B[1] + rr[2] * B[2];
+          rhs[3 * gv] = out.x; rhs[3 * gv + 1] = out.y; rhs[3 * gv + 2] = out.z;
+        }
+      }
+      for (int k = 0; k < n3; ++k) prev[k] = S.alpha * rhs[k] + (1.0 - S.alpha) * prev[k];
+      for (int i = 0; i < N; ++i)
+        for (int c = 0; c < 3; ++c) x_n1[3 * i + c] = x_t[3 * i + c] + prev[3 * i + c] / S.h / hd[i];
+      for (int k = 0; k < n3; ++k) xold[k] = ori_x[k];
+    }
+  }
+}
+
 /* ---- adjoint ---------------------------------------------------------------- */
 
 /* VJP of the corotated projection: given dmd, dmdv (3x3) return dF */
@@ -784,6 +997,14 @@ void* orc_create(const dfem_scene_desc* d) {
     B.rest_norm = 0.0;
     S->bends.push_back(B);
   }
+  S->collide = d->handle_collision != 0;
+  S->alpha = d->alpha;
+  S->mu_obs = d->obstacle_friction;
+  for (int k = 0; k < d->n_contact_vertices; ++k) S->cverts.push_back(d->contact_vertices[k]);
+  for (int k = 0; k < d->n_obstacle_vertices; ++k)
+    S->obs_x.push_back(V3{d->obstacle_x[3 * k], d->obstacle_x[3 * k + 1], d->obstacle_x[3 * k + 2]});
+  for (int k = 0; k < d->n_obstacle_faces; ++k)
+    S->obs_f.push_back({d->obstacle_faces[3 * k], d->obstacle_faces[3 * k + 1], d->obstacle_faces[3 * k + 2]});
   S->h = d->time_step;
   S->K = d->max_iterations;
   S->damping = d->damping;
@@ -818,6 +1039,7 @@ int orc_forward(void* s, const double* x, const double* v, const double* act, in
   S->rec_v.assign((size_t)n_steps * n3, 0.0);
   S->rec_act.assign((size_t)n_steps * std::max(1, S->nseg), 0.0);
   S->rec_iters.assign(n_steps, 0);
+  S->rec_passes.assign(n_steps, 0);
   std::vector<double> zero_act(std::max(1, S->nseg), 0.0);
   for (int st = 0; st < n_steps; ++st) {
     const double* a = act ? act + (size_t)st * S->nseg : zero_act.data();
@@ -826,6 +1048,8 @@ int orc_forward(void* s, const double* x, const double* v, const double* act, in
     if (S->nseg > 0) std::copy(a, a + S->nseg, S->rec_act.begin() + (size_t)st * S->nseg);
     step_prep(*S, xc.data(), vc.data(), vwc.data(), qn.data());
     int it = pd_solve(*S, xc.data(), qn.data(), a, nullptr, xn.data(), nthreads);
+    contact_phase(*S, xc.data(), vwc.data(), a, xn.data());
+    S->rec_passes[st] = S->last_passes;
     S->rec_iters[st] = it;
     if (iters) iters[st] = it;
     for (int k = 0; k < n3; ++k) {
@@ -846,6 +1070,8 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
                  double* gE, double* gnu, double* gact) {
   Scene* S = static_cast<Scene*>(s);
   if (S->rec_steps <= 0) return 5;
+  for (int p : S->rec_passes)
+    if (p > 0) { S->err = "adjoint through the contact phase is not restated"; return 5; }
   int N = S->N, n3 = 3 * N;
   int NT = (int)S->tets.size();
   std::vector<double> xb(gx_out, gx_out + n3), vb(gv_out, gv_out + n3);
@@ -891,6 +1117,22 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
 
 /* J d(x) of all constraints (World::EvaluateDVector + mJ * d, World.h:898-901);
  * act = per-segment activations (may be NULL = all zero). */
+/* contact passes of each step of the last forward call */
+int orc_contact_passes(void* s, int* out, int n) {
+  Scene* S = static_cast<Scene*>(s);
+  for (int k = 0; k < n && k < (int)S->rec_passes.size(); ++k) out[k] = S->rec_passes[k];
+  return 0;
+}
+
+/* one vertex-face CCD test (vertex p0 -> p1 against the static face q0 q1 q2) */
+int orc_vf_impact(const double* p0, const double* p1, const double* q0, const double* q1, const double* q2,
+                  double mult, double* n_out) {
+  V3 n{0, 0, 0};
+  bool hit = vf_impact(getx(p0, 0), getx(p1, 0), getx(q0, 0), getx(q1, 0), getx(q2, 0), mult, &n);
+  n_out[0] = n.x; n_out[1] = n.y; n_out[2] = n.z;
+  return hit ? 1 : 0;
+}
+
 int orc_eval_local(void* s, const double* x, const double* act, double* out) {
   Scene* S = static_cast<Scene*>(s);
   std::vector<double> zero_act(std::max(1, S->nseg), 0.0);

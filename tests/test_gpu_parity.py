@@ -110,6 +110,27 @@ def test_set_materials_refactors():
     assert rel(xg, ro["x"]) < POS_TOL
 
 
+@pytest.mark.parametrize("mu", [1.0, 0.3])
+def test_obstacle_contact_forward(mu):
+    """Soft box dropped on a ground quad: CCD, Coulomb-cone reaction, Jacobi contact iterations."""
+    d = S.drop_box(mu=mu)
+    n = 30
+    x = d.x0.reshape(-1).copy()
+    v = d.initial_velocity.copy()
+    g = Scene(d)
+    o = O.OracleScene(d)
+    xg, vg, tg = g.forward(x, v, n_steps=n, traj=True)
+    ro = o.forward(x, v, n_steps=n, traj=True)
+    assert np.array_equal(g.contact_passes(n), o.contact_passes())
+    assert o.contact_passes().sum() > 0
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    # backward through contact is refused explicitly rather than silently wrong
+    with pytest.raises(_capi.DfemError) as e:
+        g.backward(np.ones_like(xg), np.zeros_like(vg))
+    assert e.value.code == 5
+
+
 @pytest.mark.parametrize("builder", ["cantilever", "muscle_beam", "cloth_sheet"])
 def test_eval_local_matches_oracle(builder):
     d = getattr(S, builder)()

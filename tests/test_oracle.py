@@ -81,6 +81,32 @@ def test_vjp_equal_singular_values():
         assert np.all(np.isfinite(g))
 
 
+def test_ccd_known_answers():
+    """Vertex-face CCD against a static triangle in the y = 0 plane."""
+    tri = ([0, 0, 0], [1, 0, 1], [1, 0, 0])
+    hit, n = O.vf_impact([0.2, 0.1, 0.2], [0.2, -0.1, 0.2], *tri)       # crossing
+    assert hit and abs(abs(n[1]) - np.sin(np.pi / 4)) < 1e-12
+    assert not O.vf_impact([0.2, 0.1, 0.2], [0.3, 0.1, 0.2], *tri)[0]  # parallel, above
+    assert O.vf_impact([0.2, 0.1, 0.2], [0.2, 5e-5, 0.2], *tri)[0]     # ends within the thickness
+    assert not O.vf_impact([0.2, 0.1, 0.2], [0.2, 2e-4, 0.2], *tri)[0] # ends outside the thickness
+    assert not O.vf_impact([2, 0.1, 0.2], [2, -0.1, 0.2], *tri)[0]     # misses the face
+    assert O.vf_impact([1.00005, 0.1, 0.5], [1.00005, -0.1, 0.5], *tri)[0] is False  # outside edge, crossing
+    assert O.vf_impact([1.00005, 0.1, 0.5], [1.00005, 0.00005, 0.5], *tri)[0]       # near the edge at t = 1
+
+
+def test_contact_keeps_the_body_above_the_ground():
+    d = S.drop_box()
+    o = O.OracleScene(d)
+    r = o.forward(d.x0.reshape(-1).copy(), d.initial_velocity.copy(), n_steps=40, traj=True)
+    assert o.contact_passes().sum() > 0
+    assert r["traj"].reshape(40, -1, 3)[:, :, 1].min() > -1e-3
+    # the same box without contact falls through
+    d.handle_collision = False
+    o2 = O.OracleScene(d)
+    r2 = o2.forward(d.x0.reshape(-1).copy(), d.initial_velocity.copy(), n_steps=40, traj=True)
+    assert r2["traj"].reshape(40, -1, 3)[:, :, 1].min() < -0.1
+
+
 def test_lumped_masses_match_builder():
     d = S.cantilever()
     m = O.lumped_masses(d.x0, d.tets, 20.0, True)
