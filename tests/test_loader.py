@@ -1,0 +1,54 @@
+"""Scene loading in diff_fem's file formats (CPU)."""
+import os
+
+import numpy as np
+import pytest
+
+from diff_fem_b200 import loader, scene as S
+from diff_fem_b200.engine import host_factor_solve
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+REF_DATA = "/root/reference/data"
+
+
+def test_fixture_scene_loads():
+    L = loader.load_scene("beam_scene/beam.json", 3, data_root=GOLDEN)
+    d = L.desc
+    assert d.n_vertices == 7 * 3 * 3 and d.n_tets == 6 * 2 * 2 * 5
+    assert np.isclose(d.mass.sum(), 1.2)                     # "Mass" with Is Mass Same
+    assert d.attach_vertex.size == 9 and np.all(d.attach_stiffness == 1e8)
+    assert np.isclose(d.time_step, 0.01) and d.max_iterations == 10
+    assert d.handle_collision and d.obstacle_faces.shape == (2, 3)
+    assert d.n_segments > 0 and d.muscle_segment.size > 0
+    assert np.allclose(d.x0.max(axis=0), [0.3, 0.1, 0.1])    # Scale 0.05
+    # the engine's host factorisation accepts it and solves
+    x, info = host_factor_solve(d, np.ones(3 * d.n_vertices))
+    assert np.all(np.isfinite(x))
+
+
+def test_surface_extraction_and_orientation():
+    x0, tets = S.cube_grid(2, 2, 2, 1.0)
+    faces, verts = S.surface_of(x0, tets)
+    assert faces.shape[0] == 6 * 2 * 2 * 2            # 2 triangles per boundary cube face
+    assert len(set(verts.tolist())) == 26              # every vertex but the centre
+    c = x0.mean(axis=0)
+    for f in faces:                                    # outward normals
+        n = np.cross(x0[f[1]] - x0[f[0]], x0[f[2]] - x0[f[0]])
+        assert np.dot(n, x0[f].mean(axis=0) - c) > 0
+
+
+@pytest.mark.skipif(not os.path.exists(REF_DATA), reason="reference data not mounted")
+def test_reference_scenes_load():
+    """The reference's own data scenes (read in place, not copied)."""
+    d = loader.load_scene("bridgesus/bridgesus.json", 3, data_root=REF_DATA).desc
+    assert (d.n_vertices, d.n_tets, d.attach_vertex.size) == (212, 668, 65)
+    assert np.isclose(d.mass.sum(), 10.0) and np.isclose(d.time_step, 1 / 200)
+    o = O.OracleScene(d)  # the oracle accepts it (attach stiffness 1e20)
+    r = o.forward(d.x0.reshape(-1).copy(), np.zeros(3 * d.n_vertices), n_steps=2)
+    assert np.all(np.isfinite(r["x"]))
+    b = loader.load_scene("baymax/baymax.json", 3, data_root=REF_DATA).desc
+    assert (b.n_vertices, b.n_tets) == (775, 3078) and b.obstacle_faces.shape[0] > 0
+    c = loader.load_scene("cloth_ball/cloth_ball.json", 3, data_root=REF_DATA)
+    assert [bd.kind for bd in c.bodies] == ["mesh", "cloth"] and c.desc.spring_weight.size > 0
+    assert np.all(c.desc.spring_weight == 200.0) and not c.desc.gravity_mask[c.bodies[1].offset:].any()
