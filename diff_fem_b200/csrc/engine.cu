@@ -82,6 +82,7 @@ struct dfem_scene {
   DBuf<int2> sv, sslot;
   DBuf<int> mseg, seg_ptr, seg_mus, boff, bv, bslot, vslot_ptr, hs_ptr, hs_col, to_user, to_internal;
   DBuf<double> hs_val;
+  DBuf<float> tinv32, twr32, twv32;  // mixed form: FP32 copies of the tet tables
   // factor
   DBuf<int> rseg_ptr, rseg_pos, sn_c0, sn_w, sn_r, sn_rofs, rowidx, sn_lofs, sn_dofs, lvl_sn;
   DBuf<double> contrib, Lcm, Dinv;
@@ -137,7 +138,7 @@ static void refresh_scene_view(dfem_scene* sc) {
               sc->tslot.p, sc->mv.p, sc->minv.p, sc->mw.p, sc->mfib.p, sc->mseg.p, sc->mslot.p, sc->seg_ptr.p,
               sc->seg_mus.p, sc->sv.p, sc->srest.p, sc->ssw.p, sc->sslot.p, sc->boff.p, sc->bv.p, sc->bbeta.p,
               sc->bw.p, sc->brest.p, sc->bslot.p, sc->vslot_ptr.p, sc->attach_jd.p, sc->hs_ptr.p, sc->hs_col.p,
-              sc->hs_val.p};
+              sc->hs_val.p, sc->tinv32.p, sc->twr32.p, sc->twv32.p};
   if (std::memcmp(&sd, &sc->sd, sizeof(sd)) != 0) invalidate_graphs(sc);
   sc->sd = sd;
 }
@@ -206,6 +207,10 @@ static int upload_materials(dfem_scene* sc) {
   }
   CK(sc->twr.upload(wr));
   CK(sc->twv.upload(wv));
+  if (s.precision == DFEM_PREC_MIXED) {
+    CK(sc->twr32.upload(std::vector<float>(wr.begin(), wr.end())));
+    CK(sc->twv32.upload(std::vector<float>(wv.begin(), wv.end())));
+  }
   CK(sc->tE.upload(s.tE));
   CK(sc->tnu.upload(s.tnu));
   std::vector<int> hp(s.Hs.ptr.begin(), s.Hs.ptr.end());
@@ -228,6 +233,10 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->mass.upload(s.mass));
   CK(sc->gmask.upload(s.gmask));
   CK(sc->tinv.upload(planes(s.tinv, s.T, 9)));
+  if (s.precision == DFEM_PREC_MIXED) {
+    std::vector<double> tp = planes(s.tinv, s.T, 9);
+    CK(sc->tinv32.upload(std::vector<float>(tp.begin(), tp.end())));
+  }
   CK(sc->tvol.upload(s.tvol));
   std::vector<int4> tv(s.T), tsl(s.T);
   for (int e = 0; e < s.T; ++e) {
@@ -289,7 +298,7 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->flag.alloc(1)); CK(sc->step.alloc(1)); CK(sc->write_traj.alloc(1));
   CK(sc->zero.alloc(1));
   CK(cudaMemset(sc->counter.p, 0, sizeof(unsigned)));
-  CK(cudaMemset(sc->status.p, 0, sizeof(int)));
+  CK(cudaMemset(sc->status.p, 0, 4 * sizeof(int)));
   CK(sc->act_cur.alloc(std::max(1, s.nseg)));
   CK(cudaMemset(sc->act_cur.p, 0, sizeof(double) * std::max(1, s.nseg)));
   // obstacle contact phase
@@ -359,6 +368,49 @@ static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const doub
 // host round trip is needed.
 static const Gate kOpen{nullptr, nullptr, nullptr, 0};
 
+// The local step and its gather in the scene's precision form. The mixed form
+// writes FP32 slots into the same buffer (half of it) and accumulates them in
+// FP32; the contact phase always runs the FP64 form.
+static bool mixed(const dfem_scene* sc) { return sc->hs.precision == DFEM_PREC_MIXED; }
+static float* slot32(dfem_scene* sc) { return reinterpret_cast<float*>(sc->slot.p); }
+
+static void launch_local(dfem_scene* sc, cudaStream_t st, Gate g, const double* x, const double* act, const int* step) {
+  const HostScene& s = sc->hs;
+  const int ncons = s.T + s.M + s.S + s.B;
+  if (ncons == 0) return;
+  if (mixed(sc))
+    k_local_f32<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, g, x, act, step, slot32(sc));
+  else
+    k_local<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, g, x, act, step, sc->slot.p);
+}
+
+static void launch_gather(dfem_scene* sc, cudaStream_t st, Gate g, const double* c0, double* rhs) {
+  const int N = sc->hs.N;
+  if (mixed(sc))
+    k_gather_f32<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vslot_ptr.p, slot32(sc), c0, rhs);
+  else
+    k_gather<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
+}
+
+static void launch_adj_local(dfem_scene* sc, cudaStream_t st, Gate g, const int* kptr) {
+  const HostScene& s = sc->hs;
+  const int nthr = std::max(s.T + s.M + s.S + s.B, s.N);
+  if (mixed(sc))
+    k_adj_local_f32<<<(nthr + 127) / 128, 128, 0, st>>>(sc->sd, g, kptr, sc->step.p, sc->hist.p, sc->y.p, sc->bb.p,
+                                                         sc->act_all.p, slot32(sc), sc->gE.p, sc->gnu.p, sc->mg.p);
+  else
+    k_adj_local<<<(nthr + 127) / 128, 128, 0, st>>>(sc->sd, g, kptr, sc->step.p, sc->hist.p, sc->y.p, sc->bb.p,
+                                                     sc->act_all.p, sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+}
+
+static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
+  const int N = sc->hs.N;
+  if (mixed(sc))
+    k_adj_gather_f32<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vslot_ptr.p, slot32(sc), sc->xkb.p);
+  else
+    k_adj_gather<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
+}
+
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   const int nb = sc->nblk_v;
   k_step_begin<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
@@ -391,10 +443,8 @@ static void contact_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHa
 static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   const HostScene& s = sc->hs;
   const int nb = sc->nblk_v;
-  const int ncons = s.T + s.M + s.S + s.B;
-  if (ncons > 0)
-    k_local<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, kOpen, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p);
-  k_gather<<<nb, 128, 0, st>>>(s.N, kOpen, sc->vslot_ptr.p, sc->slot.p, sc->c0.p, sc->rhs.p);
+  launch_local(sc, st, kOpen, sc->xk.p, sc->act_all.p, sc->step.p);
+  launch_gather(sc, st, kOpen, sc->c0.p, sc->rhs.p);
   enqueue_solve(sc, st, kOpen, sc->rhs.p, sc->y.p);
   k_update<<<nb, 128, 0, st>>>(s.N, kOpen, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->step.p,
                                sc->flag.p, sc->iters.p, sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
@@ -418,12 +468,9 @@ static void adj_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle 
 
 static void adj_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   const HostScene& s = sc->hs;
-  const int ncons = s.T + s.M + s.S + s.B;
-  const int nthr = std::max(ncons, s.N);
   enqueue_solve(sc, st, kOpen, sc->xkb.p, sc->y.p);
-  k_adj_local<<<(nthr + 127) / 128, 128, 0, st>>>(sc->sd, kOpen, sc->kiter.p, sc->step.p, sc->hist.p, sc->y.p, sc->bb.p,
-                                                  sc->act_all.p, sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
-  k_adj_gather<<<sc->nblk_v, 128, 0, st>>>(s.N, kOpen, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
+  launch_adj_local(sc, st, kOpen, sc->kiter.p);
+  launch_adj_gather(sc, st, kOpen);
   if (s.nseg > 0)
     k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, st>>>(s.nseg, kOpen, sc->step.p, sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p,
                                                        sc->gact.p);
@@ -531,6 +578,17 @@ static int copy_out(dfem_scene* sc, const double* src, size_t n, double* dst, in
   return DFEM_OK;
 }
 
+// The device status word: [code, supernode, solve (1 forward / 2 backward), blocks that gave up].
+static int status_error(const int st4[4]) {
+  if (st4[0] == DFEM_ERR_CAP && st4[2] > 0)
+    return fail(DFEM_ERR_CAP, "a staged-copy wait of the " + std::string(st4[2] == 1 ? "forward" : "backward") +
+                                  " solve gave up (supernode " + std::to_string(st4[1]) + ", " +
+                                  std::to_string(st4[3]) + " blocks)");
+  if (st4[0] == DFEM_ERR_CAP) return fail(DFEM_ERR_CAP, "a bounded loop gave up (contact impacts per vertex)");
+  if (st4[0]) return fail(DFEM_ERR_NONFINITE, "non-finite value in the PD iteration");
+  return DFEM_OK;
+}
+
 }  // namespace dfem
 
 extern "C" {
@@ -554,7 +612,7 @@ int dfem_scene_create(const dfem_scene_desc* desc, int device, dfem_scene** out)
   CK(cudaStreamCreate(&sc->stream));  // blocking: orders with the legacy default stream callers use
   CK(cudaStreamCreateWithFlags(&sc->stream2, cudaStreamNonBlocking));  // only used to capture loop bodies
   CK(sc->kiter.alloc(1));
-  CK(sc->status.alloc(1));  // before the factor upload, whose kernels report into it
+  CK(sc->status.alloc(4));  // before the factor upload, whose kernels report into it
   RC(upload_scene(sc.get()));
   RC(ensure_steps(sc.get(), 1));
   CK(cudaDeviceSynchronize());
@@ -636,7 +694,7 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   k_to_internal<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_internal.p, sc->io_b.p, sc->vt.p);
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, 0);
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, traj_x ? 1 : 0);
-  k_set_int<<<1, 1, 0, sc->stream>>>(sc->status.p, 0);
+  CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
   CK(cudaGetLastError());
   RC(ensure_graphs(sc));
   for (int st = 0; st < n_steps; ++st) CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
@@ -645,8 +703,8 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   RC(copy_out(sc, sc->io_a.p, n3, x_out, mem));
   RC(copy_out(sc, sc->io_b.p, n3, v_out, mem));
   if (traj_x) RC(copy_out(sc, sc->traj.p, n3 * n_steps, traj_x, mem));
-  int status = 0;
-  CK(cudaMemcpyAsync(&status, sc->status.p, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+  int st4[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost, sc->stream));
   sc->rec_iters.assign(n_steps, 0);
   CK(cudaMemcpyAsync(sc->rec_iters.data(), sc->iters.p, n_steps * sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
   sc->rec_passes.assign(2 * (size_t)n_steps, 0);
@@ -658,8 +716,7 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
     sc->launches += (int64_t)(sc->g_step.outside + (size_t)sc->rec_iters[st] * sc->g_step.body +
                               (size_t)sc->rec_passes[2 * st + 1] * sc->g_step.body2);
   sc->rec_steps = n_steps;
-  if (status == DFEM_ERR_CAP) return fail(DFEM_ERR_CAP, "a bounded loop or wait gave up (solve staging or contact impacts per vertex)");
-  if (status) return fail(DFEM_ERR_NONFINITE, "non-finite value in the PD iteration");
+  RC(status_error(st4));
   return DFEM_OK;
 }
 
@@ -683,6 +740,7 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   CK(cudaMemsetAsync(sc->gnu.p, 0, sizeof(double) * std::max(1, s.T), sc->stream));
   CK(cudaMemsetAsync(sc->gact.p, 0, sizeof(double) * (size_t)sc->rec_steps * std::max(1, s.nseg), sc->stream));
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, 0);
+  CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
   RC(ensure_graphs(sc));
   for (int st = sc->rec_steps - 1; st >= 0; --st) {
     // recompute the step's iterates from its checkpoint (the step graph re-records the same checkpoint)
@@ -704,8 +762,10 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   if (g_youngs) RC(copy_out(sc, sc->gE.p, s.T, g_youngs, mem));
   if (g_poisson) RC(copy_out(sc, sc->gnu.p, s.T, g_poisson, mem));
   if (g_act && s.nseg > 0) RC(copy_out(sc, sc->gact.p, (size_t)sc->rec_steps * s.nseg, g_act, mem));
+  int st4[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost, sc->stream));
   CK(cudaStreamSynchronize(sc->stream));
-  return DFEM_OK;
+  return status_error(st4);
 }
 
 int dfem_eval_local(dfem_scene* sc, const double* x, double* jd_out, int mem) {
@@ -714,15 +774,13 @@ int dfem_eval_local(dfem_scene* sc, const double* x, double* jd_out, int mem) {
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N;
   const int nb = sc->nblk_v;
-  const int ncons = s.T + s.M + s.S + s.B;
   const Gate open{nullptr, nullptr, nullptr, 0};
   RC(copy_in(sc, x, n3, sc->io_a.p, mem));
   k_to_internal<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_internal.p, sc->io_a.p, sc->rhs.p);
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->zero.p, 0);
-  if (ncons > 0)
-    k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, open, sc->rhs.p, sc->act_cur.p, sc->zero.p, sc->slot.p);
+  launch_local(sc, sc->stream, open, sc->rhs.p, sc->act_cur.p, sc->zero.p);
   // J d = attachment term + the constraints' slots (c0 := J_att d_att)
-  k_gather<<<nb, 128, 0, sc->stream>>>(s.N, open, sc->vslot_ptr.p, sc->slot.p, sc->attach_jd.p, sc->io_b.p);
+  launch_gather(sc, sc->stream, open, sc->attach_jd.p, sc->io_b.p);
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_b.p, sc->io_a.p);
   CK(cudaGetLastError());
   sc->launches += 5;
@@ -778,12 +836,11 @@ int dfem_profile_phases(dfem_scene* sc, int32_t reps, double* ms) {
   if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_profile_phases needs a preceding dfem_step_forward");
   CK(cudaSetDevice(sc->device));
   const HostScene& s = sc->hs;
-  const int nb = sc->nblk_v;
   const int ncons = s.T + s.M + s.S + s.B;
-  const int nthr = std::max(ncons, s.N);
   // every phase is launched ungated on the state of the last forward call (step 0, iteration 0)
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, 0);
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->zero.p, 0);
+  CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
   const Gate gf = kOpen, ga = kOpen;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -801,21 +858,18 @@ int dfem_profile_phases(dfem_scene* sc, int32_t reps, double* ms) {
     return DFEM_OK;
   };
   int rc = DFEM_OK;
-  if (!rc && ncons > 0)
-    rc = timed(0, [&] { k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, gf, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p); });
-  if (!rc) rc = timed(1, [&] { k_gather<<<nb, 128, 0, sc->stream>>>(s.N, gf, sc->vslot_ptr.p, sc->slot.p, sc->c0.p, sc->rhs.p); });
+  if (!rc && ncons > 0) rc = timed(0, [&] { launch_local(sc, sc->stream, gf, sc->xk.p, sc->act_all.p, sc->step.p); });
+  if (!rc) rc = timed(1, [&] { launch_gather(sc, sc->stream, gf, sc->c0.p, sc->rhs.p); });
   if (!rc) rc = timed(2, [&] { enqueue_solve(sc, sc->stream, gf, sc->rhs.p, sc->y.p); });
-  if (!rc && ncons > 0)
-    rc = timed(3, [&] {
-      k_adj_local<<<(nthr + 127) / 128, 128, 0, sc->stream>>>(sc->sd, ga, sc->zero.p, sc->step.p, sc->hist.p, sc->y.p,
-                                                              sc->bb.p, sc->act_all.p, sc->slot.p, sc->gE.p, sc->gnu.p,
-                                                              sc->mg.p);
-    });
+  if (!rc && ncons > 0) rc = timed(3, [&] { launch_adj_local(sc, sc->stream, ga, sc->zero.p); });
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
   CK(cudaGetLastError());
+  int st4[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost, sc->stream));
   CK(cudaStreamSynchronize(sc->stream));
+  RC(status_error(st4));
   // the solve phase counted one launch per call above; it is 2 * levels kernels
   sc->launches += (int64_t)(reps + 1) * (2 * ((int64_t)sc->lvl_ptr.size() - 1) - 1);
   sc->rec_steps = 0;  // gates and iteration counts were overwritten: no backward of the old forward

@@ -81,6 +81,10 @@ struct SceneDev {
   const int* hs_ptr;
   const int* hs_col;
   const double* hs_val;
+  // mixed form: FP32 copies of the tet tables (null in the plain form)
+  const float* tinv32;
+  const float* twr32;
+  const float* twv32;
 };
 
 // Contact phase state (World::ProjectiveDynamicsMethod, sim/fem/World.h:925-1023).

@@ -198,6 +198,123 @@ __global__ void __launch_bounds__(128) k_local(SceneDev d, Gate gate, const doub
   }
 }
 
+// ---- mixed form: FP32 projections, FP32 slots and accumulation ----------------
+// Positions stay FP64; each element forms Ds = x_k - x_0 in FP64 (no
+// cancellation from absolute coordinates), then projects in FP32.  Elements
+// that are nearly flat or inverted (smallest/largest singular value below
+// kDegenerateRatio) are recomputed in FP64.
+
+__device__ __forceinline__ Vec3<float> to_f(Vec3<double> a) { return mk3((float)a.x, (float)a.y, (float)a.z); }
+__device__ __forceinline__ Vec3<double> to_d(Vec3<float> a) { return mk3((double)a.x, (double)a.y, (double)a.z); }
+__device__ __forceinline__ void st3f(float* p, int i, Vec3<float> v) { p[3 * i] = v.x; p[3 * i + 1] = v.y; p[3 * i + 2] = v.z; }
+__device__ __forceinline__ Vec3<float> ld3f(const float* p, int i) { return mk3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
+
+// F(:,j) = sum_k invDm[k][j] (x_{k+1} - x_0) from FP32 invDm planes and FP64 edges
+__device__ __forceinline__ void tet_f32(const float* inv, int n, int e, const Vec3<double> xv[4], float G[4][3],
+                                        Mat3<float>& F) {
+  Vec3<float> ds[3] = {to_f(xv[1] - xv[0]), to_f(xv[2] - xv[0]), to_f(xv[3] - xv[0])};
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    float a = inv[(0 * 3 + j) * n + e], b = inv[(1 * 3 + j) * n + e], c = inv[(2 * 3 + j) * n + e];
+    G[1][j] = a; G[2][j] = b; G[3][j] = c; G[0][j] = -(a + b + c);
+    F.c[j] = a * ds[0] + b * ds[1] + c * ds[2];
+  }
+}
+
+__global__ void __launch_bounds__(128) k_local_f32(SceneDev d, Gate gate, const double* __restrict__ x,
+                                                   const double* __restrict__ act_all, const int* step,
+                                                   float* __restrict__ slot) {
+  if (gate.skip()) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.T) {
+    int4 v = d.tv[t];
+    Vec3<double> xv[4] = {ld3(x, v.x), ld3(x, v.y), ld3(x, v.z), ld3(x, v.w)};
+    float G[4][3];
+    Mat3<float> F, md, mdv;
+    tet_f32(d.tinv32, d.T, t, xv, G, F);
+    float ratio;
+    corot_project(F, md, mdv, &ratio);
+    Vec3<float> P[3];
+    if (ratio >= kDegenerateRatio) {
+      float wr = d.twr32[t], wv = d.twv32[t];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) P[j] = wr * md.c[j] + wv * mdv.c[j];
+    } else {  // near-degenerate element: FP64
+      double Gd[4][3];
+      load_g(d.tinv, d.T, t, Gd);
+      Mat3<double> Fd = deformation(Gd, xv), mdd, mdvd;
+      corot_project(Fd, mdd, mdvd);
+      double wr = d.twr[t], wv = d.twv[t];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) P[j] = to_f(wr * mdd.c[j] + wv * mdvd.c[j]);
+    }
+    int4 sl = d.tslot[t];
+    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], G[a][0] * P[0] + G[a][1] * P[1] + G[a][2] * P[2]);
+    return;
+  }
+  t -= d.T;
+  if (t < d.M) {
+    int4 v = d.mv[t];
+    Vec3<double> x0 = ld3(x, v.x);
+    Vec3<float> ds[3] = {to_f(ld3(x, v.y) - x0), to_f(ld3(x, v.z) - x0), to_f(ld3(x, v.w) - x0)};
+    Vec3<float> f = mk3((float)d.mfib[t], (float)d.mfib[d.M + t], (float)d.mfib[2 * d.M + t]);
+    float c[4] = {0, 0, 0, 0};
+    Vec3<float> Ff = mk3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float ck = (float)d.minv[(k * 3 + 0) * d.M + t] * f.x + (float)d.minv[(k * 3 + 1) * d.M + t] * f.y +
+                 (float)d.minv[(k * 3 + 2) * d.M + t] * f.z;
+      c[k + 1] = ck;
+      c[0] -= ck;
+      Ff = Ff + ck * ds[k];
+    }
+    float a_act = (float)act_all[(size_t)(*step) * d.nseg + d.mseg[t]];
+    Vec3<float> p0 = (1.0f - a_act) * Ff;
+    float w = (float)d.mw[t];
+    int4 sl = d.mslot[t];
+    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], (w * c[a]) * p0);
+    return;
+  }
+  t -= d.M;
+  if (t < d.S) {
+    int2 v = d.sv[t];
+    Vec3<float> e = to_f(ld3(x, v.x) - ld3(x, v.y));
+    Vec3<float> dd = ((float)d.srest[t] * rsqrtf(dot3(e, e))) * e;
+    float w = (float)d.ssw[t];
+    int2 sl = d.sslot[t];
+    st3f(slot, sl.x, w * dd);
+    st3f(slot, sl.y, (-w) * dd);
+    return;
+  }
+  t -= d.S;
+  if (t < d.B) {
+    int o0 = d.boff[t], o1 = d.boff[t + 1];
+    Vec3<double> xc = ld3(x, d.bv[o0]);
+    Vec3<float> lap = mk3(0.0f, 0.0f, 0.0f);
+    for (int k = o0; k < o1; ++k) lap = lap + (float)d.bbeta[k] * to_f(ld3(x, d.bv[k]) - xc);  // sum beta = 0
+    float ln = sqrtf(dot3(lap, lap));
+    float w = (float)d.bw[t];
+    Vec3<float> dd = mk3(0.0f, 0.0f, 0.0f);
+    if (ln > 1e-25f) dd = (w * (float)d.brest[t] / ln) * lap;
+    for (int k = o0; k < o1; ++k) st3f(slot, d.bslot[k], (w * (float)d.bbeta[k]) * dd);
+  }
+}
+
+// rhs_i = c0_i (FP64) + the FP32 sum of vertex i's slots
+__global__ void k_gather_f32(int N, Gate gate, const int* __restrict__ vslot_ptr, const float* __restrict__ slot,
+                             const double* __restrict__ c0, double* __restrict__ rhs) {
+  if (gate.skip()) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  Vec3<float> acc = mk3(0.0f, 0.0f, 0.0f);
+  for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3f(slot, k);
+  st3(rhs, i, ld3(c0, i) + to_d(acc));
+}
+
 // rhs_i = c0_i + sum of the slots of vertex i
 __global__ void k_gather(int N, Gate gate, const int* __restrict__ vslot_ptr, const double* __restrict__ slot,
                          const double* __restrict__ c0, double* __restrict__ rhs) {
@@ -233,10 +350,15 @@ __device__ __forceinline__ void stage_blocks_issue(const FactorDev& f, int s, in
   }
 }
 
-__device__ __forceinline__ bool stage_blocks_wait(const FactorDev& f, uint64_t* bar) {
+// status[0] = 6 (DFEM_ERR_CAP) when the wait gave up; status[1] = the supernode,
+// status[2] = 1 (forward) / 2 (backward), status[3] counts the blocks that gave up.
+__device__ __forceinline__ bool stage_blocks_wait(const FactorDev& f, uint64_t* bar, int s, int which) {
   const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0) != 0;
   if (!ok && threadIdx.x == 0) {
-    *f.status = 6;                 // DFEM_ERR_CAP: bounded wait gave up
+    f.status[0] = 6;
+    f.status[1] = s;
+    f.status[2] = which;
+    atomicAdd(f.status + 3, 1);
     mbar_wait_bounded(bar, 0);     // give in-flight copies one more bounded chance to land
   }
   return ok;
@@ -278,7 +400,7 @@ __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, G
     tsh[3 * c] = a0; tsh[3 * c + 1] = a1; tsh[3 * c + 2] = a2;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (!stage_blocks_wait(f, &bar)) return;  // includes the CTA barrier
+  if (!stage_blocks_wait(f, &bar, s, 1)) return;  // includes the CTA barrier
   for (int c = warp; c < w; c += nw) {
     double a0 = 0, a1 = 0, a2 = 0;
     for (int k = lane; k <= c; k += 32) {
@@ -330,7 +452,7 @@ __global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, G
     const int i = c0 + c;
     tsh[3 * c] = y[3 * i]; tsh[3 * c + 1] = y[3 * i + 1]; tsh[3 * c + 2] = y[3 * i + 2];
   }
-  if (!stage_blocks_wait(f, &bar)) return;  // includes the CTA barrier
+  if (!stage_blocks_wait(f, &bar, s, 2)) return;  // includes the CTA barrier
   const double* Lc = f.stage_l ? Lsh : f.Lcm + f.sn_lofs[s];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   // four columns per warp pass: four independent load streams per lane
@@ -562,6 +684,140 @@ __global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const 
     }
     for (int q = o0; q < o1; ++q) st3(slot, d.bslot[q], d.bbeta[q] * gl);
   }
+}
+
+// Mixed-form adjoint of the local step: FP32 VJPs (FP64 for near-degenerate
+// elements), FP32 slots; parameter gradients accumulate in FP64.
+__global__ void __launch_bounds__(128) k_adj_local_f32(SceneDev d, Gate gate, const int* kptr, const int* step,
+                                                       const double* __restrict__ hist, const double* __restrict__ yb,
+                                                       double* bb, const double* __restrict__ act_all,
+                                                       float* __restrict__ slot, double* gE, double* gnu, double* mg) {
+  if (gate.skip()) return;
+  const int k = *kptr;
+  const double* x = hist + (size_t)k * 3 * d.N;
+  const double* x1 = hist + (size_t)(k + 1) * 3 * d.N;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.N) st3(bb, t, ld3(bb, t) + ld3(yb, t));
+  if (t < d.T) {
+    int4 v = d.tv[t];
+    const int vi[4] = {v.x, v.y, v.z, v.w};
+    Vec3<double> xv[4], x1v[4];
+    Vec3<float> yv[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) { xv[a] = ld3(x, vi[a]); x1v[a] = ld3(x1, vi[a]); yv[a] = to_f(ld3(yb, vi[a])); }
+    float G[4][3];
+    Mat3<float> F, F1, Y, md, mdv;
+    tet_f32(d.tinv32, d.T, t, xv, G, F);
+    tet_f32(d.tinv32, d.T, t, x1v, G, F1);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) Y.c[j] = G[0][j] * yv[0] + G[1][j] * yv[1] + G[2][j] * yv[2] + G[3][j] * yv[3];
+    float ratio;
+    corot_project(F, md, mdv, &ratio);
+    Mat3<float> gF;
+    const double E = d.tE[t], nu = d.tnu[t], vol = d.tvol[t];
+    double yr = 0, yvv = 0, yh = 0;
+    if (ratio >= kDegenerateRatio) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { yr += dot3(Y.c[j], md.c[j]); yvv += dot3(Y.c[j], mdv.c[j]); yh += dot3(Y.c[j], F1.c[j]); }
+      float wr = d.twr32[t], wv = d.twv32[t];
+      Mat3<float> gmd, gmdv;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { gmd.c[j] = wr * Y.c[j]; gmdv.c[j] = wv * Y.c[j]; }
+      gF = corot_vjp(F, gmd, gmdv);
+    } else {  // near-degenerate element: FP64
+      double Gd[4][3];
+      load_g(d.tinv, d.T, t, Gd);
+      Vec3<double> ydv[4] = {ld3(yb, vi[0]), ld3(yb, vi[1]), ld3(yb, vi[2]), ld3(yb, vi[3])};
+      Mat3<double> Fd = deformation(Gd, xv), F1d = deformation(Gd, x1v), Yd = deformation(Gd, ydv), mdd, mdvd;
+      corot_project(Fd, mdd, mdvd);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { yr += dot3(Yd.c[j], mdd.c[j]); yvv += dot3(Yd.c[j], mdvd.c[j]); yh += dot3(Yd.c[j], F1d.c[j]); }
+      Mat3<double> gmd, gmdv;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) { gmd.c[j] = d.twr[t] * Yd.c[j]; gmdv.c[j] = d.twv[t] * Yd.c[j]; }
+      Mat3<double> gFd = corot_vjp(Fd, gmd, gmdv);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) gF.c[j] = to_f(gFd.c[j]);
+    }
+    double opn = 1.0 + nu;
+    if (gE) gE[t] += vol / opn * (yr + nu * yvv) - vol * yh;
+    if (gnu) gnu[t] += E * vol / (opn * opn) * (yvv - yr);
+    int4 sl = d.tslot[t];
+    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], G[a][0] * gF.c[0] + G[a][1] * gF.c[1] + G[a][2] * gF.c[2]);
+    return;
+  }
+  t -= d.T;
+  if (t < d.M) {
+    int4 v = d.mv[t];
+    const int vi[4] = {v.x, v.y, v.z, v.w};
+    Vec3<float> f = mk3((float)d.mfib[t], (float)d.mfib[d.M + t], (float)d.mfib[2 * d.M + t]);
+    float w = (float)d.mw[t];
+    float c[4] = {0, 0, 0, 0};
+    Vec3<double> x0 = ld3(x, vi[0]);
+    Vec3<float> Ff = mk3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      float cq = (float)d.minv[(q * 3 + 0) * d.M + t] * f.x + (float)d.minv[(q * 3 + 1) * d.M + t] * f.y +
+                 (float)d.minv[(q * 3 + 2) * d.M + t] * f.z;
+      c[q + 1] = cq;
+      c[0] -= cq;
+      Ff = Ff + cq * to_f(ld3(x, vi[q + 1]) - x0);
+    }
+    Vec3<float> db = mk3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int a = 0; a < 4; ++a) db = db + (w * c[a]) * to_f(ld3(yb, vi[a]));
+    float a_act = (float)act_all[(size_t)(*step) * d.nseg + d.mseg[t]];
+    mg[t] = -(double)dot3(db, Ff);
+    int4 sl = d.mslot[t];
+    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], ((1.0f - a_act) * c[a]) * db);
+    return;
+  }
+  t -= d.M;
+  if (t < d.S) {
+    int2 v = d.sv[t];
+    float w = (float)d.ssw[t];
+    Vec3<float> db = w * to_f(ld3(yb, v.x) - ld3(yb, v.y));
+    Vec3<float> e = to_f(ld3(x, v.x) - ld3(x, v.y));
+    float inv = rsqrtf(dot3(e, e));
+    Vec3<float> eh = inv * e;
+    Vec3<float> ge = ((float)d.srest[t] * inv) * (db - dot3(eh, db) * eh);
+    int2 sl = d.sslot[t];
+    st3f(slot, sl.x, ge);
+    st3f(slot, sl.y, (-1.0f) * ge);
+    return;
+  }
+  t -= d.S;
+  if (t < d.B) {
+    int o0 = d.boff[t], o1 = d.boff[t + 1];
+    float w = (float)d.bw[t];
+    Vec3<double> xc = ld3(x, d.bv[o0]);
+    Vec3<float> db = mk3(0.0f, 0.0f, 0.0f), lap = mk3(0.0f, 0.0f, 0.0f);
+    for (int q = o0; q < o1; ++q) {
+      db = db + (w * (float)d.bbeta[q]) * to_f(ld3(yb, d.bv[q]));
+      lap = lap + (float)d.bbeta[q] * to_f(ld3(x, d.bv[q]) - xc);
+    }
+    float ln = sqrtf(dot3(lap, lap));
+    Vec3<float> gl = mk3(0.0f, 0.0f, 0.0f);
+    if (ln > 1e-25f) {
+      Vec3<float> lh = (1.0f / ln) * lap;
+      gl = (w * (float)d.brest[t] / ln) * (db - dot3(lh, db) * lh);
+    }
+    for (int q = o0; q < o1; ++q) st3f(slot, d.bslot[q], (float)d.bbeta[q] * gl);
+  }
+}
+
+__global__ void k_adj_gather_f32(int N, Gate gate, const int* __restrict__ vslot_ptr, const float* __restrict__ slot,
+                                 double* xkb) {
+  if (gate.skip()) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  Vec3<float> acc = mk3(0.0f, 0.0f, 0.0f);
+  for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3f(slot, k);
+  st3(xkb, i, to_d(acc));
 }
 
 // xbar^k = sum of the slots (constraints without x dependence contribute nothing)

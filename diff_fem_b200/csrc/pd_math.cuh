@@ -164,8 +164,13 @@ __device__ __forceinline__ void volume_projection_d(const T s[3], T g[3], T J[3]
 
 // md (reflected rotation) and md_volume of the corotated constraint
 template <typename T>
-__device__ __forceinline__ void corot_project(const Mat3<T>& F, Mat3<T>& md, Mat3<T>& mdv) {
+__device__ __forceinline__ void corot_project(const Mat3<T>& F, Mat3<T>& md, Mat3<T>& mdv, T* s_ratio = nullptr) {
   Svd3<T> sv = svd3(F);
+  if (s_ratio) {  // smallest / largest singular value (conditioning of the element)
+    T smax = sv.s[0] > sv.s[1] ? (sv.s[0] > sv.s[2] ? sv.s[0] : sv.s[2]) : (sv.s[1] > sv.s[2] ? sv.s[1] : sv.s[2]);
+    T smin = sv.s[0] < sv.s[1] ? (sv.s[0] < sv.s[2] ? sv.s[0] : sv.s[2]) : (sv.s[1] < sv.s[2] ? sv.s[1] : sv.s[2]);
+    *s_ratio = smax > T(0) ? smin / smax : T(0);
+  }
   T g[3];
   volume_projection(sv.s, g);
   // R = sum_i u_i v_i^T ; G = sum_i g_i u_i v_i^T   (column j of u v^T is v[j] * u)
@@ -178,14 +183,24 @@ __device__ __forceinline__ void corot_project(const Mat3<T>& F, Mat3<T>& md, Mat
   if (det3(F) < T(0)) md.c[2] = T(-1) * md.c[2];
 }
 
+// Near-degenerate test for the mixed form: an element whose smallest singular
+// value is below kDegenerateRatio of its largest (nearly flat or inverted)
+// has a badly conditioned U/V in FP32 and is recomputed in FP64.
+constexpr float kDegenerateRatio = 0.05f;
+
 // VJP of (md, md_volume) with respect to F.  gmd, gmdv: cotangents (3x3).
 //   P_bar_ij (i != j) = a_ij sym(M_G)_ij + b_ij asym(M_G)_ij + (M_R_ij - M_R_ji)/(s_i + s_j)
 //   P_bar_ii = sum_k (M_G)_kk dg_k/ds_i
 //   with M_X = U^T X V, a_ij = (g_i - g_j)/(s_i - s_j), b_ij = (g_i + g_j)/(s_i + s_j);
 //   F_bar = U P_bar V^T.
 template <typename T>
-__device__ __forceinline__ Mat3<T> corot_vjp(const Mat3<T>& F, Mat3<T> gmd, const Mat3<T>& gmdv) {
+__device__ __forceinline__ Mat3<T> corot_vjp(const Mat3<T>& F, Mat3<T> gmd, const Mat3<T>& gmdv, T* s_ratio = nullptr) {
   Svd3<T> sv = svd3(F);
+  if (s_ratio) {
+    T smax = sv.s[0] > sv.s[1] ? (sv.s[0] > sv.s[2] ? sv.s[0] : sv.s[2]) : (sv.s[1] > sv.s[2] ? sv.s[1] : sv.s[2]);
+    T smin = sv.s[0] < sv.s[1] ? (sv.s[0] < sv.s[2] ? sv.s[0] : sv.s[2]) : (sv.s[1] < sv.s[2] ? sv.s[1] : sv.s[2]);
+    *s_ratio = smax > T(0) ? smin / smax : T(0);
+  }
   T g[3], J[3][3], dd[3];
   volume_projection_d(sv.s, g, J, dd);
   if (det3(F) < T(0)) gmd.c[2] = T(-1) * gmd.c[2];

@@ -38,7 +38,7 @@ enum dfem_status {
   DFEM_ERR_FACTOR = 3,        /* Cholesky failed even after regularisation      */
   DFEM_ERR_NONFINITE = 4,     /* NaN/Inf met in a step (status word set on GPU)  */
   DFEM_ERR_STATE = 5,         /* call out of order (e.g. backward before forward)*/
-  DFEM_ERR_CAP = 6,           /* a bounded loop hit its cap (contact passes)     */
+  DFEM_ERR_CAP = 6,           /* a bounded loop or wait hit its cap              */
   DFEM_ERR_NOMEM = 7          /* allocation failed                               */
 };
 
