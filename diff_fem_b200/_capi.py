@@ -64,6 +64,8 @@ class SceneInfoC(C.Structure):
 _VP = C.c_void_p
 SIGNATURES = [
     ("dfem_scene_create", C.c_int, [C.POINTER(SceneDescC), C.c_int, C.POINTER(_VP)]),
+    ("dfem_scene_create_batch", C.c_int, [C.POINTER(SceneDescC), C.c_int32, C.c_int, C.POINTER(_VP)]),
+    ("dfem_batch_layout", C.c_int, [_VP, _pi, _pi, _pi, _pi]),
     ("dfem_scene_destroy", C.c_int, [_VP]),
     ("dfem_scene_get_info", C.c_int, [_VP, C.POINTER(SceneInfoC)]),
     ("dfem_set_materials", C.c_int, [_VP, _VP, _VP, C.c_int]),

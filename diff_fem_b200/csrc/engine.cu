@@ -7,8 +7,11 @@
 
 #include <cmath>
 #include <cstdio>
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -88,7 +91,12 @@ struct dfem_scene {
   DBuf<double> contrib, Lcm, Dinv;
   std::vector<int> lvl_ptr;
   int max_w = 1, max_r = 0;
-  size_t shm_fwd = 0, shm_bwd = 0;  // dynamic shared memory of the level kernels
+  std::vector<size_t> shm_fwd, shm_bwd;  // dynamic shared memory of the level kernels, per level
+  // batch layout (a single scene is one part)
+  std::vector<HostScene> parts;          // the parts of a batch (empty for a single scene)
+  DBuf<int> vpart, seg_part, sn_part, part_v0, part_b0, blk_part, blk_v0;
+  int nblk_p = 1;                        // part-aligned blocks of the reducing vertex kernels
+  PartDev pd{};
   // state
   DBuf<double> xt, vt, qn, c0, xk, rhs, y, slot, hist, io_a, io_b;
   DBuf<double> partial, errv;
@@ -111,7 +119,7 @@ struct dfem_scene {
   DBuf<int> kiter;                        // device-side iteration counter of the loops
   int64_t launches = 0;                   // kernels launched by this scene (graph nodes included)
   int rec_steps = 0;
-  std::vector<int> rec_iters;  // iteration counts of the recorded forward call
+  std::vector<int> rec_iters;  // per step: largest iteration count over the parts (recorded forward call)
   int nblk_v = 1;   // blocks of the vertex-parallel kernels
   SceneDev sd{};
   FactorDev fd{};
@@ -138,7 +146,7 @@ static void refresh_scene_view(dfem_scene* sc) {
               sc->tslot.p, sc->mv.p, sc->minv.p, sc->mw.p, sc->mfib.p, sc->mseg.p, sc->mslot.p, sc->seg_ptr.p,
               sc->seg_mus.p, sc->sv.p, sc->srest.p, sc->ssw.p, sc->sslot.p, sc->boff.p, sc->bv.p, sc->bbeta.p,
               sc->bw.p, sc->brest.p, sc->bslot.p, sc->vslot_ptr.p, sc->attach_jd.p, sc->hs_ptr.p, sc->hs_col.p,
-              sc->hs_val.p, sc->tinv32.p, sc->twr32.p, sc->twv32.p};
+              sc->hs_val.p, sc->tinv32.p, sc->twr32.p, sc->twv32.p, sc->vpart.p, sc->seg_part.p};
   if (std::memcmp(&sd, &sc->sd, sizeof(sd)) != 0) invalidate_graphs(sc);
   sc->sd = sd;
 }
@@ -168,30 +176,51 @@ static int upload_factor(dfem_scene* sc) {
   for (int r : F.sn_r) sc->max_r = std::max(sc->max_r, r);
   // dynamic shared memory of the level kernels (doubles, blocks padded to even counts):
   //   fwd: Dinv + [L_{R,s}] + t + y_s      bwd: Dinv + [L_{R,s}] + u + x_R
-  // L_{R,s} is staged too when the largest supernode still fits.
+  // L_{R,s} is staged too when the largest supernode still fits.  Each level
+  // is launched with the largest need of its own supernodes, so levels of
+  // small supernodes keep several blocks per SM.
   auto even = [](size_t v) { return (v + 1) & ~size_t(1); };
-  size_t need_f[2] = {0, 0}, need_b[2] = {0, 0};  // [without, with] staged L
-  for (int q = 0; q < F.nsuper; ++q) {
+  auto need = [&](int q, int st, size_t* nf, size_t* nb) {
     size_t w = F.sn_w[q], r = F.sn_r[q];
     size_t nseg = (size_t)(F.rseg_ptr[F.sn_c0[q] + w] - F.rseg_ptr[F.sn_c0[q]]);
+    size_t l = st ? even(r * w) : 0;
+    // + row -> segment offsets ((w+1) ints) + gathered contributions (3 per segment)
+    *nf = sizeof(double) * (even(w * w) + l + 6 * w + (w + 2) / 2 + 3 * nseg);
+    *nb = sizeof(double) * (even(w * w) + l + 3 * w + 3 * r);
+  };
+  size_t need_f[2] = {0, 0}, need_b[2] = {0, 0};  // [without, with] staged L
+  for (int q = 0; q < F.nsuper; ++q)
     for (int st = 0; st < 2; ++st) {
-      size_t l = st ? even(r * w) : 0;
-      // + row -> segment offsets ((w+1) ints) + gathered contributions (3 per segment)
-      need_f[st] = std::max(need_f[st], sizeof(double) * (even(w * w) + l + 6 * w + (w + 2) / 2 + 3 * nseg));
-      need_b[st] = std::max(need_b[st], sizeof(double) * (even(w * w) + l + 3 * w + 3 * r));
+      size_t nf, nb;
+      need(q, st, &nf, &nb);
+      need_f[st] = std::max(need_f[st], nf);
+      need_b[st] = std::max(need_b[st], nb);
     }
-  }
   const size_t budget = 220 * 1024;
   const int stage_l = (need_f[1] <= budget && need_b[1] <= budget) ? 1 : 0;
-  sc->shm_fwd = need_f[stage_l];
-  sc->shm_bwd = need_b[stage_l];
-  if (sc->shm_bwd > budget || sc->shm_fwd > budget)
+  if (need_f[stage_l] > budget || need_b[stage_l] > budget)
     return fail(DFEM_ERR_INVALID, "supernode too large for the shared-memory staging of the triangular solves");
-  CK(cudaFuncSetAttribute(k_fwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_fwd));
-  CK(cudaFuncSetAttribute(k_bwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_bwd));
+  const int L = (int)F.lvl_ptr.size() - 1;
+  sc->shm_fwd.assign(L, 0);
+  sc->shm_bwd.assign(L, 0);
+  for (int l = 0; l < L; ++l)
+    for (int k = F.lvl_ptr[l]; k < F.lvl_ptr[l + 1]; ++k) {
+      size_t nf, nb;
+      need(F.lvl_sn[k], stage_l, &nf, &nb);
+      sc->shm_fwd[l] = std::max(sc->shm_fwd[l], nf);
+      sc->shm_bwd[l] = std::max(sc->shm_bwd[l], nb);
+    }
+  CK(cudaFuncSetAttribute(k_fwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_f[stage_l]));
+  CK(cudaFuncSetAttribute(k_bwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_b[stage_l]));
+  if (sc->hs.nparts > 1) {
+    std::vector<int> snp(F.nsuper);
+    for (int q = 0; q < F.nsuper; ++q)
+      snp[q] = (int)(std::upper_bound(sc->hs.part_v0.begin(), sc->hs.part_v0.end(), F.sn_c0[q]) - sc->hs.part_v0.begin()) - 1;
+    CK(sc->sn_part.upload(snp));
+  }
   FactorDev fd{sc->rseg_ptr.p, sc->rseg_pos.p, sc->contrib.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p,
                sc->sn_rofs.p, sc->rowidx.p, sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->lvl_sn.p,
-               stage_l, sc->status.p};
+               stage_l, sc->status.p, sc->hs.nparts > 1 ? sc->sn_part.p : nullptr};
   if (std::memcmp(&fd, &sc->fd, sizeof(fd)) != 0) invalidate_graphs(sc);
   sc->fd = fd;
   return DFEM_OK;
@@ -292,12 +321,34 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->xkb.alloc(n3)); CK(sc->xtb.alloc(n3)); CK(sc->bb.alloc(n3));
   CK(sc->gE.alloc(std::max(1, s.T))); CK(sc->gnu.alloc(std::max(1, s.T))); CK(sc->mg.alloc(std::max(1, s.M)));
   sc->nblk_v = (s.N + 127) / 128;
-  CK(sc->partial.alloc(std::max(sc->nblk_v, 1)));
-  CK(sc->errv.alloc(1));
-  CK(sc->counter.alloc(1));
-  CK(sc->flag.alloc(1)); CK(sc->step.alloc(1)); CK(sc->write_traj.alloc(1));
+  // part tables: part-aligned blocks of the reducing vertex kernels
+  const int np = s.nparts;
+  std::vector<int> pb0(np + 1, 0), bpart, bv0;
+  for (int p = 0; p < np; ++p) {
+    for (int v = s.part_v0[p]; v < s.part_v0[p + 1]; v += kPartBlock) { bpart.push_back(p); bv0.push_back(v); }
+    pb0[p + 1] = (int)bpart.size();
+  }
+  sc->nblk_p = (int)bpart.size();
+  CK(sc->part_v0.upload(s.part_v0));
+  CK(sc->part_b0.upload(pb0));
+  CK(sc->blk_part.upload(bpart));
+  CK(sc->blk_v0.upload(bv0));
+  sc->pd = PartDev{np, sc->part_v0.p, sc->part_b0.p, sc->blk_part.p, sc->blk_v0.p};
+  if (np > 1) {
+    std::vector<int> vp(s.N), sp(std::max(1, s.nseg), 0);
+    for (int p = 0; p < np; ++p) {
+      for (int v = s.part_v0[p]; v < s.part_v0[p + 1]; ++v) vp[v] = p;
+      for (int q = s.part_seg0[p]; q < s.part_seg0[p + 1]; ++q) sp[q] = p;
+    }
+    CK(sc->vpart.upload(vp));
+    CK(sc->seg_part.upload(sp));
+  }
+  CK(sc->partial.alloc(std::max(sc->nblk_p, 1)));
+  CK(sc->errv.alloc(np));
+  CK(sc->counter.alloc(np));
+  CK(sc->flag.alloc(np)); CK(sc->step.alloc(1)); CK(sc->write_traj.alloc(1));
   CK(sc->zero.alloc(1));
-  CK(cudaMemset(sc->counter.p, 0, sizeof(unsigned)));
+  CK(cudaMemset(sc->counter.p, 0, sizeof(unsigned) * np));
   CK(cudaMemset(sc->status.p, 0, 4 * sizeof(int)));
   CK(sc->act_cur.alloc(std::max(1, s.nseg)));
   CK(cudaMemset(sc->act_cur.p, 0, sizeof(double) * std::max(1, s.nseg)));
@@ -338,7 +389,7 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   CK(sc->ckpt_x.alloc(n3 * cap));
   CK(sc->ckpt_v.alloc(n3 * cap));
   CK(sc->traj.alloc(n3 * cap));
-  CK(sc->iters.alloc(cap));
+  CK(sc->iters.alloc((size_t)cap * sc->hs.nparts));
   CK(sc->act_all.alloc((size_t)cap * std::max(1, s.nseg)));
   CK(sc->gact.alloc((size_t)cap * std::max(1, s.nseg)));
   CK(sc->cpasses.alloc(2 * (size_t)cap));
@@ -353,11 +404,11 @@ static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const doub
   const int L = (int)sc->lvl_ptr.size() - 1;
   for (int l = 0; l < L; ++l) {
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_fwd_level<<<nb, 256, sc->shm_fwd, st>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
+    k_fwd_level<<<nb, 256, sc->shm_fwd[l], st>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
   }
   for (int l = L - 1; l >= 0; --l) {
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_bwd_level<<<nb, 256, sc->shm_bwd, st>>>(sc->fd, sc->lvl_ptr[l], gate, y);
+    k_bwd_level<<<nb, 256, sc->shm_bwd[l], st>>>(sc->fd, sc->lvl_ptr[l], gate, y);
   }
 }
 
@@ -366,7 +417,22 @@ static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const doub
 // The body's last kernel advances a device-side iteration counter and sets
 // the loop condition, so converged steps launch no further iterations and no
 // host round trip is needed.
-static const Gate kOpen{nullptr, nullptr, nullptr, 0};
+static const Gate kOpen{};
+
+// Per-part gates of a batch (a single scene's loops never run a gated-off
+// iteration, so it takes the open gate and saves the lookups).
+static Gate fwd_gate(const dfem_scene* sc) {
+  Gate g;
+  if (sc->hs.nparts > 1) { g.flag = sc->flag.p; g.nparts = sc->hs.nparts; }
+  return g;
+}
+static Gate adj_gate(const dfem_scene* sc) {
+  Gate g;
+  if (sc->hs.nparts > 1) {
+    g.iters = sc->iters.p; g.step = sc->step.p; g.kptr = sc->kiter.p; g.nparts = sc->hs.nparts;
+  }
+  return g;
+}
 
 // The local step and its gather in the scene's precision form. The mixed form
 // writes FP32 slots into the same buffer (half of it) and accumulates them in
@@ -387,9 +453,9 @@ static void launch_local(dfem_scene* sc, cudaStream_t st, Gate g, const double* 
 static void launch_gather(dfem_scene* sc, cudaStream_t st, Gate g, const double* c0, double* rhs) {
   const int N = sc->hs.N;
   if (mixed(sc))
-    k_gather_f32<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vslot_ptr.p, slot32(sc), c0, rhs);
+    k_gather_f32<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vpart.p, sc->vslot_ptr.p, slot32(sc), c0, rhs);
   else
-    k_gather<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
+    k_gather<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
 }
 
 static void launch_adj_local(dfem_scene* sc, cudaStream_t st, Gate g, const int* kptr) {
@@ -406,18 +472,17 @@ static void launch_adj_local(dfem_scene* sc, cudaStream_t st, Gate g, const int*
 static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
   const int N = sc->hs.N;
   if (mixed(sc))
-    k_adj_gather_f32<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vslot_ptr.p, slot32(sc), sc->xkb.p);
+    k_adj_gather_f32<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vpart.p, sc->vslot_ptr.p, slot32(sc), sc->xkb.p);
   else
-    k_adj_gather<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
+    k_adj_gather<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
 }
 
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
-  const int nb = sc->nblk_v;
-  k_step_begin<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
+  k_step_begin<<<sc->nblk_p, kPartBlock, 0, st>>>(sc->sd, sc->pd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
                                    sc->hist.p, sc->ckpt_x.p, sc->ckpt_v.p, sc->flag.p, sc->iters.p,
                                    sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p,
                                    sc->has_contact ? sc->vwc.p : nullptr);
-  k_loop_enter<<<1, 1, 0, st>>>(sc->kiter.p, sc->flag.p, sc->hs.K, h);
+  k_loop_enter<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, sc->hs.nparts, sc->hs.K, h);
 }
 
 // obstacle contact phase (second conditional loop of the step graph)
@@ -433,7 +498,8 @@ static void contact_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHa
   k_contact_detect<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd, sc->xt.p, sc->xk.p, sc->status.p);
   k_contact_ctl_detect<<<1, 1, 0, st>>>(sc->cd, h);
   k_contact_prep<<<nb, 128, 0, st>>>(s.N, sc->cd, sc->xk.p, sc->partial.p, sc->counter.p);
-  Gate active{nullptr, nullptr, nullptr, 0, sc->cstate.p + CS_ACTIVE};
+  Gate active;
+  active.active = sc->cstate.p + CS_ACTIVE;
   if (ncons > 0)
     k_local<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, active, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p);
   k_contact_rhs<<<nb, 128, 0, st>>>(sc->sd, sc->cd, sc->slot.p, sc->xt.p, sc->xk.p);
@@ -442,13 +508,13 @@ static void contact_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHa
 
 static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   const HostScene& s = sc->hs;
-  const int nb = sc->nblk_v;
-  launch_local(sc, st, kOpen, sc->xk.p, sc->act_all.p, sc->step.p);
-  launch_gather(sc, st, kOpen, sc->c0.p, sc->rhs.p);
-  enqueue_solve(sc, st, kOpen, sc->rhs.p, sc->y.p);
-  k_update<<<nb, 128, 0, st>>>(s.N, kOpen, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->step.p,
+  const Gate g = fwd_gate(sc);
+  launch_local(sc, st, g, sc->xk.p, sc->act_all.p, sc->step.p);
+  launch_gather(sc, st, g, sc->c0.p, sc->rhs.p);
+  enqueue_solve(sc, st, g, sc->rhs.p, sc->y.p);
+  k_update<<<sc->nblk_p, kPartBlock, 0, st>>>(s.N, sc->pd, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->step.p,
                                sc->flag.p, sc->iters.p, sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
-  k_loop_ctl<<<1, 1, 0, st>>>(sc->kiter.p, sc->flag.p, s.K, h);
+  k_loop_ctl<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, s.nparts, s.K, h);
 }
 
 static void step_post(dfem_scene* sc, cudaStream_t st) {
@@ -463,17 +529,18 @@ static void adj_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle 
   const HostScene& s = sc->hs;
   // the cotangent of the step's output lives in io_a (x) / io_b (v); k_adj_end overwrites it with the input's
   k_adj_begin<<<sc->nblk_v, 128, 0, st>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, sc->xkb.p, sc->xtb.p, sc->bb.p);
-  k_adj_loop_enter<<<1, 1, 0, st>>>(sc->kiter.p, sc->iters.p, sc->step.p, s.K, h);
+  k_adj_loop_enter<<<1, 256, 0, st>>>(sc->kiter.p, sc->iters.p, sc->step.p, s.nparts, s.K, h);
 }
 
 static void adj_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   const HostScene& s = sc->hs;
-  enqueue_solve(sc, st, kOpen, sc->xkb.p, sc->y.p);
-  launch_adj_local(sc, st, kOpen, sc->kiter.p);
-  launch_adj_gather(sc, st, kOpen);
+  const Gate g = adj_gate(sc);
+  enqueue_solve(sc, st, g, sc->xkb.p, sc->y.p);
+  launch_adj_local(sc, st, g, sc->kiter.p);
+  launch_adj_gather(sc, st, g);
   if (s.nseg > 0)
-    k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, st>>>(s.nseg, kOpen, sc->step.p, sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p,
-                                                       sc->gact.p);
+    k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, st>>>(s.nseg, g, sc->seg_part.p, sc->step.p, sc->seg_ptr.p,
+                                                       sc->seg_mus.p, sc->mg.p, sc->gact.p);
   k_adj_loop_ctl<<<1, 1, 0, st>>>(sc->kiter.p, h);
 }
 
@@ -589,6 +656,33 @@ static int status_error(const int st4[4]) {
   return DFEM_OK;
 }
 
+// Device side of scene creation, once sc->hs (and sc->parts for a batch) is built.
+static int create_on_device(std::unique_ptr<dfem_scene>& sc, int device, dfem_scene** out) {
+  CK(cudaStreamCreate(&sc->stream));  // blocking: orders with the legacy default stream callers use
+  CK(cudaStreamCreateWithFlags(&sc->stream2, cudaStreamNonBlocking));  // only used to capture loop bodies
+  CK(sc->kiter.alloc(1));
+  CK(sc->status.alloc(4));  // before the factor upload, whose kernels report into it
+  RC(upload_scene(sc.get()));
+  RC(ensure_steps(sc.get(), 1));
+  CK(cudaDeviceSynchronize());
+  *out = sc.release();
+  g_last_error.clear();
+  return DFEM_OK;
+}
+
+// Run f(0) .. f(n-1) on up to hardware_concurrency host threads.
+template <typename Fn>
+static void parallel_for(int n, Fn f) {
+  const int nt = std::max(1, std::min(n, (int)std::thread::hardware_concurrency()));
+  std::atomic<int> next{0};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&] {
+      for (int i = next++; i < n; i = next++) f(i);
+    });
+  for (auto& th : pool) th.join();
+}
+
 }  // namespace dfem
 
 extern "C" {
@@ -609,15 +703,44 @@ int dfem_scene_create(const dfem_scene_desc* desc, int device, dfem_scene** out)
   if (!build_host_scene(*desc, sc->hs, err))
     return fail(err.find("factor") != std::string::npos ? DFEM_ERR_FACTOR : DFEM_ERR_INVALID, err);
   if (!refactorize(sc->hs.Hs, sc->hs.F, err)) return fail(DFEM_ERR_FACTOR, err);
-  CK(cudaStreamCreate(&sc->stream));  // blocking: orders with the legacy default stream callers use
-  CK(cudaStreamCreateWithFlags(&sc->stream2, cudaStreamNonBlocking));  // only used to capture loop bodies
-  CK(sc->kiter.alloc(1));
-  CK(sc->status.alloc(4));  // before the factor upload, whose kernels report into it
-  RC(upload_scene(sc.get()));
-  RC(ensure_steps(sc.get(), 1));
-  CK(cudaDeviceSynchronize());
-  *out = sc.release();
-  g_last_error.clear();
+  return create_on_device(sc, device, out);
+}
+
+int dfem_scene_create_batch(const dfem_scene_desc* descs, int32_t n_scenes, int device, dfem_scene** out) {
+  if (!descs || !out || n_scenes < 1) return fail(DFEM_ERR_INVALID, "null argument or n_scenes < 1");
+  *out = nullptr;
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(DFEM_ERR_INVALID, "device index out of range");
+  CK(cudaSetDevice(device));
+  std::unique_ptr<dfem_scene> sc(new dfem_scene());
+  sc->device = device;
+  sc->parts.resize(n_scenes);
+  std::vector<std::string> errs(n_scenes);
+  std::vector<int> codes(n_scenes, DFEM_OK);
+  parallel_for(n_scenes, [&](int i) {  // each part: preprocessing, ordering and factorisation
+    if (!build_host_scene(descs[i], sc->parts[i], errs[i]))
+      codes[i] = errs[i].find("factor") != std::string::npos ? DFEM_ERR_FACTOR : DFEM_ERR_INVALID;
+    else if (!refactorize(sc->parts[i].Hs, sc->parts[i].F, errs[i]))
+      codes[i] = DFEM_ERR_FACTOR;
+  });
+  for (int i = 0; i < n_scenes; ++i)
+    if (codes[i]) return fail(codes[i], "scene " + std::to_string(i) + ": " + errs[i]);
+  std::string err;
+  if (!merge_parts(sc->parts, sc->hs, err)) return fail(DFEM_ERR_INVALID, err);
+  return create_on_device(sc, device, out);
+}
+
+int dfem_batch_layout(const dfem_scene* sc, int32_t* n_parts, int32_t* vertex_offsets, int32_t* tet_offsets,
+                      int32_t* segment_offsets) {
+  if (!sc || !n_parts) return fail(DFEM_ERR_INVALID, "null argument");
+  const HostScene& s = sc->hs;
+  *n_parts = s.nparts;
+  for (int p = 0; p <= s.nparts; ++p) {
+    if (vertex_offsets) vertex_offsets[p] = s.part_v0[p];
+    if (tet_offsets) tet_offsets[p] = s.part_t0[p];
+    if (segment_offsets) segment_offsets[p] = s.part_seg0[p];
+  }
   return DFEM_OK;
 }
 
@@ -653,7 +776,20 @@ int dfem_set_materials(dfem_scene* sc, const double* youngs, const double* poiss
   }
   std::string err;
   CK(cudaStreamSynchronize(sc->stream));
-  if (!update_materials(sc->hs, E.data(), nu.data(), err)) return fail(DFEM_ERR_FACTOR, err);
+  if (sc->parts.empty()) {
+    if (!update_materials(sc->hs, E.data(), nu.data(), err)) return fail(DFEM_ERR_FACTOR, err);
+  } else {  // refactor every part on its own (its own regularisation), then copy into the union
+    const int np = (int)sc->parts.size();
+    std::vector<std::string> errs(np);
+    std::vector<int> ok(np, 1);
+    parallel_for(np, [&](int p) {
+      const int t0 = sc->hs.part_t0[p];
+      ok[p] = update_materials(sc->parts[p], E.data() + t0, nu.data() + t0, errs[p]) ? 1 : 0;
+    });
+    for (int p = 0; p < np; ++p)
+      if (!ok[p]) return fail(DFEM_ERR_FACTOR, "scene " + std::to_string(p) + ": " + errs[p]);
+    merge_numeric(sc->parts, sc->hs);
+  }
   RC(upload_materials(sc));
   refresh_scene_view(sc);
   CK(cudaDeviceSynchronize());
@@ -705,12 +841,16 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   if (traj_x) RC(copy_out(sc, sc->traj.p, n3 * n_steps, traj_x, mem));
   int st4[4] = {0, 0, 0, 0};
   CK(cudaMemcpyAsync(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost, sc->stream));
-  sc->rec_iters.assign(n_steps, 0);
-  CK(cudaMemcpyAsync(sc->rec_iters.data(), sc->iters.p, n_steps * sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+  const int np = s.nparts;
+  std::vector<int> it_all((size_t)n_steps * np, 0);
+  CK(cudaMemcpyAsync(it_all.data(), sc->iters.p, it_all.size() * sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
   sc->rec_passes.assign(2 * (size_t)n_steps, 0);
   if (sc->has_contact)
     CK(cudaMemcpyAsync(sc->rec_passes.data(), sc->cpasses.p, 2 * n_steps * sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
   CK(cudaStreamSynchronize(sc->stream));
+  sc->rec_iters.assign(n_steps, 0);
+  for (int st = 0; st < n_steps; ++st)
+    for (int p = 0; p < np; ++p) sc->rec_iters[st] = std::max(sc->rec_iters[st], it_all[(size_t)st * np + p]);
   sc->launches += 7;
   for (int st = 0; st < n_steps; ++st)
     sc->launches += (int64_t)(sc->g_step.outside + (size_t)sc->rec_iters[st] * sc->g_step.body +
@@ -799,7 +939,7 @@ int dfem_get_iterations(const dfem_scene* sc, int32_t* iters, int32_t n) {
   if (!sc || !iters) return fail(DFEM_ERR_INVALID, "null argument");
   if (n > sc->cap_steps) return fail(DFEM_ERR_INVALID, "n exceeds recorded steps");
   CK(cudaSetDevice(sc->device));
-  CK(cudaMemcpy(iters, sc->iters.p, n * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(iters, sc->iters.p, (size_t)n * sc->hs.nparts * sizeof(int), cudaMemcpyDeviceToHost));
   return DFEM_OK;
 }
 

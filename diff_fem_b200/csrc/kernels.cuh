@@ -20,22 +20,37 @@ namespace dfem {
 
 constexpr double kConvergenceEps = 5e-7;  // World.h:214 (EPS)
 
-// Kernels of a PD iteration are gated on device state so a whole step runs as
-// one CUDA graph with no host round trip: forward kernels return early once
-// the convergence flag is set; adjoint kernels of reverse iteration k return
-// when k >= the iteration count recorded for the step.
+// Kernels of a PD iteration are gated on device state, per part of a batch (a
+// single scene is a batch of one part): in the forward loop a part whose
+// convergence flag is set does no further work; in the reverse loop a part
+// skips the iterations k >= its recorded count; in the contact phase kernels
+// run only while the phase is active.  The conditional graph loops stop once
+// every part is done, so a single scene never executes a gated-off iteration.
 struct Gate {
-  const int* flag;   // forward: nonzero -> converged, skip
-  const int* iters;  // adjoint: per-step iteration counts
-  const int* step;   // adjoint: current step index
-  int k;
+  const int* flag = nullptr;    // forward: per-part converged flags
+  const int* iters = nullptr;   // adjoint: iteration counts [step][part]
+  const int* step = nullptr;    // adjoint: current step index
+  const int* kptr = nullptr;    // adjoint: current reverse iteration
+  int nparts = 1;
   const int* active = nullptr;  // contact phase: run only while *active == 1
-  __device__ __forceinline__ bool skip() const {
-    if (flag && *flag) return true;
-    if (iters && k >= iters[*step]) return true;
+  __device__ __forceinline__ bool skip(int part) const {
+    if (flag && flag[part]) return true;
+    if (iters && *kptr >= iters[(size_t)(*step) * nparts + part]) return true;
     if (active && *active != 1) return true;
     return false;
   }
+};
+
+// Part-aligned blocks of the vertex kernels with per-part reductions: block b
+// covers vertices [blk_v0[b], min(blk_v0[b] + 128, part_v0[p + 1])) of part
+// p = blk_part[b]; the blocks of part p are part_b0[p] .. part_b0[p + 1] - 1.
+constexpr int kPartBlock = 128;
+struct PartDev {
+  int nparts;
+  const int* part_v0;   // nparts + 1
+  const int* part_b0;   // nparts + 1
+  const int* blk_part;
+  const int* blk_v0;
 };
 
 struct SceneDev {
@@ -85,7 +100,25 @@ struct SceneDev {
   const float* tinv32;
   const float* twr32;
   const float* twv32;
+  // batch: part of every vertex and muscle segment (null for a single scene)
+  const int* vpart;
+  const int* seg_part;
 };
+
+__device__ __forceinline__ int vpart_of(const SceneDev& d, int i) { return d.vpart ? d.vpart[i] : 0; }
+
+// part of constraint t (tets, muscles, springs, bending stencils in that order)
+__device__ __forceinline__ int cons_part(const SceneDev& d, int t) {
+  if (!d.vpart) return 0;
+  if (t < d.T) return d.vpart[d.tv[t].x];
+  t -= d.T;
+  if (t < d.M) return d.vpart[d.mv[t].x];
+  t -= d.M;
+  if (t < d.S) return d.vpart[d.sv[t].x];
+  t -= d.S;
+  if (t < d.B) return d.vpart[d.bv[d.boff[t]]];
+  return 0;
+}
 
 // Contact phase state (World::ProjectiveDynamicsMethod, sim/fem/World.h:925-1023).
 constexpr int kMaxImpactsPerVertex = 4;
@@ -126,6 +159,7 @@ struct FactorDev {
   const int* lvl_sn;
   int stage_l;   // 1: the below-diagonal blocks are staged in shared memory too
   int* status;   // error status word (6: a bounded wait gave up)
+  const int* sn_part;  // batch: part of every supernode (null for a single scene)
 };
 
 }  // namespace dfem

@@ -23,10 +23,11 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Deterministic grid reduction: per-block partial sums, the last block to
-// finish sums the partials in block order.  Returns true in thread 0 of the
-// last block, with *total set.
-__device__ bool grid_reduce(double v, double* partial, unsigned* counter, double* total) {
+// Deterministic per-part reduction over part-aligned blocks: every block of
+// the part writes its partial sum, the last block of the part to finish
+// (counter) adds the partials b0 .. b0+nb-1 in block order.  Returns true in
+// thread 0 of that block, with *total set.
+__device__ bool part_reduce(double v, double* partial, unsigned* counter, int b0, int nb, double* total) {
   __shared__ double ws[32];
   __shared__ bool last;
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -39,14 +40,14 @@ __device__ bool grid_reduce(double v, double* partial, unsigned* counter, double
     partial[blockIdx.x] = s;
     __threadfence();
     unsigned ticket = atomicAdd(counter, 1u);
-    last = (ticket == gridDim.x - 1);
+    last = (ticket == (unsigned)nb - 1);
   }
   __syncthreads();
   if (!last) return false;
   if (threadIdx.x == 0) {
     __threadfence();
     double s = 0;
-    for (unsigned b = 0; b < gridDim.x; ++b) s += ((volatile double*)partial)[b];
+    for (int b = b0; b < b0 + nb; ++b) s += ((volatile double*)partial)[b];
     *total = s;
     *counter = 0u;
     return true;
@@ -81,14 +82,16 @@ __device__ __forceinline__ Mat3<double> deformation(const double G[4][3], const 
 
 // --------------------------------------------------------------- forward ----
 
-__global__ void k_step_begin(SceneDev d, const int* step, double* xt, double* vt, double* qn,
+__global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt, double* vt, double* qn,
                              double* c0, double* xk, double* hist, double* ckpt_x, double* ckpt_v,
                              int* flag, int* iters, double* partial, unsigned* counter, double* errv,
                              int* status, double* vwc_out) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.x, p = pd.blk_part[b];
+  const int pv0 = pd.part_v0[p], pv1 = pd.part_v0[p + 1];
+  const int i = pd.blk_v0[b] + threadIdx.x;
   const int s = *step;
   double q2 = 0;
-  if (i < d.N) {
+  if (i < pv1) {
     Vec3<double> x = ld3(xt, i), v = ld3(vt, i);
     if (ckpt_x) { st3(ckpt_x + (size_t)s * 3 * d.N, i, x); st3(ckpt_v + (size_t)s * 3 * d.N, i, v); }
     // Environment::Step adds g h to v (gravity-enabled bodies); TimeStepping:
@@ -112,13 +115,13 @@ __global__ void k_step_begin(SceneDev d, const int* step, double* xt, double* vt
     st3(c0, i, acc);
     q2 = dot3(q, q);
   }
-  if (i == 0) { iters[s] = 0; }
+  if (threadIdx.x == 0 && b == pd.part_b0[p]) iters[(size_t)s * pd.nparts + p] = 0;
   double tot;
-  if (grid_reduce(q2, partial, counter, &tot)) {
+  if (part_reduce(q2, partial, counter + p, pd.part_b0[p], pd.part_b0[p + 1] - pd.part_b0[p], &tot)) {
     // iteration 0 of the reference compares q_n with a zero vector
-    double e = sqrt(tot) / (3.0 * d.N);
-    *errv = e;
-    *flag = (e < kConvergenceEps) ? 1 : 0;
+    double e = sqrt(tot) / (3.0 * (pv1 - pv0));
+    errv[p] = e;
+    flag[p] = (e < kConvergenceEps) ? 1 : 0;
     if (!isfinite(tot)) *status = 4;
   }
 }
@@ -128,8 +131,8 @@ __global__ void k_step_begin(SceneDev d, const int* step, double* xt, double* vt
 __global__ void __launch_bounds__(128) k_local(SceneDev d, Gate gate, const double* __restrict__ x,
                                                const double* __restrict__ act_all, const int* step,
                                                double* __restrict__ slot) {
-  if (gate.skip()) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gate.skip(cons_part(d, t))) return;
   if (t < d.T) {
     // corotated FEM (CorotateFEMConstraint::EvaluateDVector + EvaluateJMatrix)
     int4 v = d.tv[t];
@@ -224,8 +227,8 @@ __device__ __forceinline__ void tet_f32(const float* inv, int n, int e, const Ve
 __global__ void __launch_bounds__(128) k_local_f32(SceneDev d, Gate gate, const double* __restrict__ x,
                                                    const double* __restrict__ act_all, const int* step,
                                                    float* __restrict__ slot) {
-  if (gate.skip()) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gate.skip(cons_part(d, t))) return;
   if (t < d.T) {
     int4 v = d.tv[t];
     Vec3<double> xv[4] = {ld3(x, v.x), ld3(x, v.y), ld3(x, v.z), ld3(x, v.w)};
@@ -305,22 +308,22 @@ __global__ void __launch_bounds__(128) k_local_f32(SceneDev d, Gate gate, const 
 }
 
 // rhs_i = c0_i (FP64) + the FP32 sum of vertex i's slots
-__global__ void k_gather_f32(int N, Gate gate, const int* __restrict__ vslot_ptr, const float* __restrict__ slot,
+__global__ void k_gather_f32(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
+                             const float* __restrict__ slot,
                              const double* __restrict__ c0, double* __restrict__ rhs) {
-  if (gate.skip()) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
   Vec3<float> acc = mk3(0.0f, 0.0f, 0.0f);
   for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3f(slot, k);
   st3(rhs, i, ld3(c0, i) + to_d(acc));
 }
 
 // rhs_i = c0_i + sum of the slots of vertex i
-__global__ void k_gather(int N, Gate gate, const int* __restrict__ vslot_ptr, const double* __restrict__ slot,
+__global__ void k_gather(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
+                             const double* __restrict__ slot,
                          const double* __restrict__ c0, double* __restrict__ rhs) {
-  if (gate.skip()) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
   Vec3<double> acc = ld3(c0, i);
   for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
   st3(rhs, i, acc);
@@ -366,10 +369,10 @@ __device__ __forceinline__ bool stage_blocks_wait(const FactorDev& f, uint64_t* 
 
 __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, Gate gate,
                                                    const double* __restrict__ rhs, double* y) {
-  if (gate.skip()) return;
   extern __shared__ __align__(16) double sh[];  // Dinv (w*w, even) | L_{R,s} (r*w, even; if staged) | t (3w) | y_s (3w)
   __shared__ __align__(8) uint64_t bar;
   const int s = f.lvl_sn[lvl_begin + blockIdx.x];
+  if (gate.skip(f.sn_part ? f.sn_part[s] : 0)) return;
   const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
   double* Dsh = sh;
   double* Lsh = sh + ((w * w + 1) & ~1);
@@ -431,10 +434,10 @@ __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, G
 //   u = y_s - L_{R,s}^T y_R  (column-major block, warp per column)
 //   y_s = Dinv_s^T u
 __global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, Gate gate, double* y) {
-  if (gate.skip()) return;
   extern __shared__ __align__(16) double sh[];  // Dinv | L_{R,s} (if staged) | u (3w) | gathered ancestor rows x_R (3r)
   __shared__ __align__(8) uint64_t bar;
   const int s = f.lvl_sn[lvl_begin + blockIdx.x];
+  if (gate.skip(f.sn_part ? f.sn_part[s] : 0)) return;
   const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
   const int* R = f.rowidx + f.sn_rofs[s];
   double* Dsh = sh;
@@ -490,15 +493,18 @@ __global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, G
   }
 }
 
-// x^{k+1} = x_t + hvf; convergence test for the next iteration (k read from device memory)
-__global__ void k_update(int N, Gate gate, const int* kptr, const double* __restrict__ xt, const double* __restrict__ z,
+// x^{k+1} = x_t + hvf; per-part convergence test for the next iteration (k read
+// from device memory).  Part-aligned blocks; a converged part's blocks do nothing.
+__global__ void k_update(int N, PartDev pd, const int* kptr, const double* __restrict__ xt, const double* __restrict__ z,
                          double* xk, double* hist, const int* step, int* flag, int* iters,
                          double* partial, unsigned* counter, double* errv, int* status) {
-  if (gate.skip()) return;
+  const int b = blockIdx.x, p = pd.blk_part[b];
+  if (flag[p]) return;
   const int k = *kptr;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pv0 = pd.part_v0[p], pv1 = pd.part_v0[p + 1];
+  const int i = pd.blk_v0[b] + threadIdx.x;
   double e2 = 0;
-  if (i < N) {
+  if (i < pv1) {
     Vec3<double> xn = ld3(xt, i) + ld3(z, i);
     Vec3<double> dlt = xn - ld3(xk, i);
     e2 = dot3(dlt, dlt);
@@ -506,12 +512,12 @@ __global__ void k_update(int N, Gate gate, const int* kptr, const double* __rest
     if (hist) st3(hist + (size_t)(k + 1) * 3 * N, i, xn);
   }
   double tot;
-  if (grid_reduce(e2, partial, counter, &tot)) {
-    double e = sqrt(tot) / (3.0 * N);
-    *errv = e;
-    iters[*step] += 1;
-    if (e < kConvergenceEps) *flag = 1;
-    if (!isfinite(tot)) { *status = 4; *flag = 1; }
+  if (part_reduce(e2, partial, counter + p, pd.part_b0[p], pd.part_b0[p + 1] - pd.part_b0[p], &tot)) {
+    double e = sqrt(tot) / (3.0 * (pv1 - pv0));
+    errv[p] = e;
+    iters[(size_t)(*step) * pd.nparts + p] += 1;
+    if (e < kConvergenceEps) flag[p] = 1;
+    if (!isfinite(tot)) { *status = 4; flag[p] = 1; }
   }
 }
 
@@ -532,27 +538,50 @@ __global__ void k_step_end(SceneDev d, int* step, double* xt, double* vt, const 
 
 __global__ void k_next_step(int* step) { *step += 1; }
 
-// Loop control of the PD iterations (body of a conditional WHILE graph node):
-// advance the device-side iteration counter and continue while not converged
-// and k < K.  The counter advances on every body execution, so the loop runs
-// at most K times whatever the convergence flag says.
-__global__ void k_loop_ctl(int* kptr, const int* flag, int K, cudaGraphConditionalHandle h) {
-  int k = *kptr + 1;
-  *kptr = k;
-  cudaGraphSetConditional(h, (*flag == 0 && k < K) ? 1u : 0u);
+// Loop control of the PD iterations (body of a conditional WHILE graph node),
+// one block over the parts: advance the device-side iteration counter and
+// continue while some part has not converged and k < K.  The counter advances
+// on every body execution, so the loop runs at most K times whatever the
+// convergence flags say.
+__global__ void k_loop_ctl(int* kptr, const int* flag, int nparts, int K, cudaGraphConditionalHandle h) {
+  int open = 0;
+  for (int p = threadIdx.x; p < nparts; p += blockDim.x) open |= (flag[p] == 0);
+  open = __syncthreads_or(open);
+  if (threadIdx.x == 0) {
+    int k = *kptr + 1;
+    *kptr = k;
+    cudaGraphSetConditional(h, (open && k < K) ? 1u : 0u);
+  }
 }
 
-// Before the loop: run the body at all only if the first test did not converge.
-__global__ void k_loop_enter(int* kptr, const int* flag, int K, cudaGraphConditionalHandle h) {
-  *kptr = 0;
-  cudaGraphSetConditional(h, (*flag == 0 && K > 0) ? 1u : 0u);
+// Before the loop: run the body at all only if some part did not converge in the first test.
+__global__ void k_loop_enter(int* kptr, const int* flag, int nparts, int K, cudaGraphConditionalHandle h) {
+  int open = 0;
+  for (int p = threadIdx.x; p < nparts; p += blockDim.x) open |= (flag[p] == 0);
+  open = __syncthreads_or(open);
+  if (threadIdx.x == 0) {
+    *kptr = 0;
+    cudaGraphSetConditional(h, (open && K > 0) ? 1u : 0u);
+  }
 }
 
-// Reverse loop of the adjoint: k = iters-1 .. 0 (counter decreases every body execution).
-__global__ void k_adj_loop_enter(int* kptr, const int* iters, const int* step, int K, cudaGraphConditionalHandle h) {
-  int n = min(max(iters[*step], 0), K);  // recorded by the forward body (<= K); clamped regardless
-  *kptr = n - 1;
-  cudaGraphSetConditional(h, n > 0 ? 1u : 0u);
+// Reverse loop of the adjoint: k = n-1 .. 0, n the largest iteration count of
+// the step over the parts (each part skips its k >= own count); the counter
+// decreases every body execution.
+__global__ void k_adj_loop_enter(int* kptr, const int* iters, const int* step, int nparts, int K,
+                                 cudaGraphConditionalHandle h) {
+  __shared__ int mx;
+  if (threadIdx.x == 0) mx = 0;
+  __syncthreads();
+  const size_t row = (size_t)(*step) * nparts;
+  int n = 0;
+  for (int p = threadIdx.x; p < nparts; p += blockDim.x) n = max(n, min(max(iters[row + p], 0), K));
+  atomicMax(&mx, n);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *kptr = mx - 1;
+    cudaGraphSetConditional(h, mx > 0 ? 1u : 0u);
+  }
 }
 __global__ void k_adj_loop_ctl(int* kptr, cudaGraphConditionalHandle h) {
   int k = *kptr - 1;
@@ -593,14 +622,14 @@ __global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const 
                                                    const double* __restrict__ hist, const double* __restrict__ yb,
                                                    double* bb, const double* __restrict__ act_all,
                                                    double* __restrict__ slot, double* gE, double* gnu, double* mg) {
-  if (gate.skip()) return;
   const int k = *kptr;
   const double* x = hist + (size_t)k * 3 * d.N;
   const double* x1 = hist + (size_t)(k + 1) * 3 * d.N;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < d.N) {  // bbar += ybar (b = M/h^2 q_n enters every iteration)
+  if (t < d.N && !gate.skip(vpart_of(d, t))) {  // bbar += ybar (b = M/h^2 q_n enters every iteration)
     st3(bb, t, ld3(bb, t) + ld3(yb, t));
   }
+  if (gate.skip(cons_part(d, t))) return;
   if (t < d.T) {
     int4 v = d.tv[t];
     const int vi[4] = {v.x, v.y, v.z, v.w};
@@ -692,12 +721,12 @@ __global__ void __launch_bounds__(128) k_adj_local_f32(SceneDev d, Gate gate, co
                                                        const double* __restrict__ hist, const double* __restrict__ yb,
                                                        double* bb, const double* __restrict__ act_all,
                                                        float* __restrict__ slot, double* gE, double* gnu, double* mg) {
-  if (gate.skip()) return;
   const int k = *kptr;
   const double* x = hist + (size_t)k * 3 * d.N;
   const double* x1 = hist + (size_t)(k + 1) * 3 * d.N;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < d.N) st3(bb, t, ld3(bb, t) + ld3(yb, t));
+  if (t < d.N && !gate.skip(vpart_of(d, t))) st3(bb, t, ld3(bb, t) + ld3(yb, t));
+  if (gate.skip(cons_part(d, t))) return;
   if (t < d.T) {
     int4 v = d.tv[t];
     const int vi[4] = {v.x, v.y, v.z, v.w};
@@ -810,33 +839,32 @@ __global__ void __launch_bounds__(128) k_adj_local_f32(SceneDev d, Gate gate, co
   }
 }
 
-__global__ void k_adj_gather_f32(int N, Gate gate, const int* __restrict__ vslot_ptr, const float* __restrict__ slot,
+__global__ void k_adj_gather_f32(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
+                                 const float* __restrict__ slot,
                                  double* xkb) {
-  if (gate.skip()) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
   Vec3<float> acc = mk3(0.0f, 0.0f, 0.0f);
   for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3f(slot, k);
   st3(xkb, i, to_d(acc));
 }
 
 // xbar^k = sum of the slots (constraints without x dependence contribute nothing)
-__global__ void k_adj_gather(int N, Gate gate, const int* __restrict__ vslot_ptr, const double* __restrict__ slot,
+__global__ void k_adj_gather(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
+                                 const double* __restrict__ slot,
                              double* xkb) {
-  if (gate.skip()) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
+  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
   Vec3<double> acc = mk3(0.0, 0.0, 0.0);
   for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
   st3(xkb, i, acc);
 }
 
 // activation gradient of the step: sum over the muscle constraints of each segment
-__global__ void k_seg_reduce(int nseg, Gate gate, const int* step, const int* seg_ptr, const int* seg_mus,
-                             const double* mg, double* gact) {
-  if (gate.skip()) return;
+__global__ void k_seg_reduce(int nseg, Gate gate, const int* seg_part, const int* step, const int* seg_ptr,
+                             const int* seg_mus, const double* mg, double* gact) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nseg) return;
+  if (q >= nseg || gate.skip(seg_part ? seg_part[q] : 0)) return;
   double s = 0;
   for (int k = seg_ptr[q]; k < seg_ptr[q + 1]; ++k) s += mg[seg_mus[k]];
   gact[(size_t)(*step) * nseg + q] += s;

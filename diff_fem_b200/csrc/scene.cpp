@@ -261,7 +261,8 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& s, std::string& err) 
   }
 
   s.B = d.n_bending;
-  s.boff.assign(d.bend_offsets, d.bend_offsets + s.B + 1);
+  if (d.bend_offsets) s.boff.assign(d.bend_offsets, d.bend_offsets + s.B + 1);
+  else s.boff.assign(1, 0);
   if (s.B > 0) {
     REQ(s.boff[0] == 0, "descriptor: bend_offsets must start at 0");
     for (int b = 0; b < s.B; ++b) REQ(s.boff[b + 1] - s.boff[b] >= 4, "descriptor: bending stencil needs a ring of >= 3");
@@ -301,7 +302,119 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& s, std::string& err) 
   for (int i = 0; i < N; ++i) { s.F.perm[i] = i; s.F.iperm[i] = i; }
   s.Hs = assemble_hs(s);
   build_slots(s);
+  s.nparts = 1;
+  s.part_v0 = {0, s.N};
+  s.part_t0 = {0, s.T};
+  s.part_seg0 = {0, s.nseg};
   return true;
+}
+
+namespace {
+template <typename T>
+void cat(std::vector<T>& dst, const std::vector<T>& src) { dst.insert(dst.end(), src.begin(), src.end()); }
+template <typename T, typename O>
+void cat_off(std::vector<T>& dst, const std::vector<T>& src, O off) {
+  for (const T& v : src) dst.push_back(static_cast<T>(v + off));
+}
+// CSR pointer arrays: append src[1..] shifted by off (dst already holds its leading 0)
+template <typename T, typename O>
+void cat_ptr(std::vector<T>& dst, const std::vector<T>& src, O off) {
+  for (size_t k = 1; k < src.size(); ++k) dst.push_back(static_cast<T>(src[k] + off));
+}
+}  // namespace
+
+bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err) {
+  REQ(!P.empty(), "batch: no scenes");
+  const HostScene& a = P[0];
+  int64_t totN = 0, totT = 0, totSlots = 0, totRows = 0, totL = 0, totD = 0;
+  for (const HostScene& p : P) {
+    REQ(p.h == a.h && p.damping == a.damping && p.g[0] == a.g[0] && p.g[1] == a.g[1] && p.g[2] == a.g[2] &&
+            p.K == a.K && p.precision == a.precision && p.checkpoint_every == a.checkpoint_every,
+        "batch: scenes must share time_step, damping, gravity, max_iterations, precision and checkpoint_every");
+    REQ(!(p.collide && !p.cverts.empty() && !p.obs_f.empty()), "batch: obstacle contact is supported for single scenes only");
+    REQ(p.nparts == 1, "batch: parts must be single scenes");
+    totN += p.N; totT += p.T; totSlots += p.nslots; totRows += (int64_t)p.F.rowidx.size();
+    totL += (int64_t)p.F.Lcm.size(); totD += (int64_t)p.F.Dinv.size();
+  }
+  REQ(totN < INT32_MAX / 3 && totT < INT32_MAX / 4 && totSlots < INT32_MAX / 3 && totRows < INT32_MAX / 3 &&
+          totL < INT32_MAX && totD < INT32_MAX,
+      "batch: total size exceeds the 32-bit index range of the kernels");
+  u = HostScene();
+  u.h = a.h; u.damping = a.damping; u.g[0] = a.g[0]; u.g[1] = a.g[1]; u.g[2] = a.g[2];
+  u.K = a.K; u.precision = a.precision; u.checkpoint_every = a.checkpoint_every;
+  u.collide = false;
+  u.nparts = (int)P.size();
+  u.part_v0 = {0}; u.part_t0 = {0}; u.part_seg0 = {0};
+  u.seg_ptr = {0}; u.boff = {0}; u.vslot_ptr = {0};
+  u.Hs.ptr = {0};
+  SupernodalFactor& F = u.F;
+  F.sn_rofs = {0}; F.sn_lofs = {0}; F.sn_dofs = {0}; F.rseg_ptr = {0};
+  int voff = 0, moff = 0, segoff = 0, slotoff = 0, bvoff = 0, snoff = 0, rsegoff = 0;
+  int64_t hsoff = 0, rofs = 0, lofs = 0, dofs = 0;
+  std::vector<int> sn_base(P.size());
+  for (size_t q = 0; q < P.size(); ++q) {
+    const HostScene& p = P[q];
+    cat(u.x0, p.x0); cat(u.mass, p.mass); cat(u.gmask, p.gmask);
+    cat_off(u.tv, p.tv, voff); cat(u.tinv, p.tinv); cat(u.tvol, p.tvol); cat(u.tE, p.tE); cat(u.tnu, p.tnu);
+    cat_off(u.tslot, p.tslot, slotoff);
+    cat_off(u.mv, p.mv, voff); cat(u.minv, p.minv); cat(u.mvol, p.mvol); cat(u.mk, p.mk); cat(u.mfib, p.mfib);
+    cat_off(u.mseg, p.mseg, segoff); cat_off(u.mslot, p.mslot, slotoff);
+    cat_ptr(u.seg_ptr, p.seg_ptr, moff); cat_off(u.seg_mus, p.seg_mus, moff);
+    cat_off(u.sv, p.sv, voff); cat_off(u.sslot, p.sslot, slotoff); cat(u.srest, p.srest); cat(u.ssw, p.ssw);
+    cat_ptr(u.boff, p.boff, bvoff); cat_off(u.bv, p.bv, voff); cat_off(u.bslot, p.bslot, slotoff);
+    cat(u.bbeta, p.bbeta); cat(u.bw, p.bw); cat(u.brest, p.brest);
+    cat_off(u.av, p.av, voff); cat(u.ap, p.ap); cat(u.ak, p.ak);
+    cat_ptr(u.vslot_ptr, p.vslot_ptr, slotoff);
+    cat_ptr(u.Hs.ptr, p.Hs.ptr, hsoff); cat_off(u.Hs.col, p.Hs.col, voff); cat(u.Hs.val, p.Hs.val);
+    cat_off(u.to_internal, p.to_internal, voff); cat_off(u.to_user, p.to_user, voff);
+    // factor (block diagonal)
+    const SupernodalFactor& G = p.F;
+    cat_off(F.perm, G.perm, voff); cat_off(F.iperm, G.iperm, voff);
+    cat_off(F.sn_c0, G.sn_c0, voff); cat(F.sn_w, G.sn_w); cat(F.sn_r, G.sn_r);
+    cat_ptr(F.sn_rofs, G.sn_rofs, rofs); cat_off(F.rowidx, G.rowidx, voff);
+    cat_ptr(F.sn_lofs, G.sn_lofs, lofs); cat(F.Lcm, G.Lcm);
+    cat_ptr(F.sn_dofs, G.sn_dofs, dofs); cat(F.Ldiag, G.Ldiag); cat(F.Dinv, G.Dinv);
+    for (int par : G.sn_parent) F.sn_parent.push_back(par < 0 ? -1 : par + snoff);
+    cat_off(F.col_sn, G.col_sn, snoff);
+    cat_ptr(F.rseg_ptr, G.rseg_ptr, rsegoff); cat_off(F.rseg_pos, G.rseg_pos, (int)rofs);
+    F.nnz_factor += G.nnz_factor;
+    F.reg = std::max(F.reg, G.reg);
+    F.nlevels = std::max(F.nlevels, G.nlevels);
+    sn_base[q] = snoff;
+    voff += p.N; moff += p.M; segoff += p.nseg; slotoff += p.nslots; bvoff += (int)p.bv.size();
+    snoff += G.nsuper; rsegoff += (int)G.rseg_pos.size();
+    hsoff += p.Hs.ptr[p.N]; rofs += (int64_t)G.rowidx.size(); lofs += (int64_t)G.Lcm.size(); dofs += (int64_t)G.Dinv.size();
+    u.T += p.T; u.M += p.M; u.S += p.S; u.B += p.B; u.A += p.A;
+    u.part_v0.push_back(voff); u.part_t0.push_back(u.T); u.part_seg0.push_back(segoff);
+  }
+  u.N = voff; u.nseg = segoff; u.nslots = slotoff;
+  u.Hs.n = voff;
+  F.n = voff; F.nsuper = snoff;
+  F.lvl_ptr = {0};
+  for (int l = 0; l < F.nlevels; ++l) {
+    for (size_t q = 0; q < P.size(); ++q) {
+      const SupernodalFactor& G = P[q].F;
+      if (l >= G.nlevels) continue;
+      for (int k = G.lvl_ptr[l]; k < G.lvl_ptr[l + 1]; ++k) F.lvl_sn.push_back(G.lvl_sn[k] + sn_base[q]);
+    }
+    F.lvl_ptr.push_back((int)F.lvl_sn.size());
+  }
+  return true;
+}
+
+void merge_numeric(const std::vector<HostScene>& P, HostScene& u) {
+  size_t t = 0, h = 0, l = 0, d = 0;
+  u.F.reg = 0.0;
+  for (const HostScene& p : P) {
+    std::copy(p.tE.begin(), p.tE.end(), u.tE.begin() + t);
+    std::copy(p.tnu.begin(), p.tnu.end(), u.tnu.begin() + t);
+    std::copy(p.Hs.val.begin(), p.Hs.val.end(), u.Hs.val.begin() + h);
+    std::copy(p.F.Lcm.begin(), p.F.Lcm.end(), u.F.Lcm.begin() + l);
+    std::copy(p.F.Ldiag.begin(), p.F.Ldiag.end(), u.F.Ldiag.begin() + d);
+    std::copy(p.F.Dinv.begin(), p.F.Dinv.end(), u.F.Dinv.begin() + d);
+    u.F.reg = std::max(u.F.reg, p.F.reg);
+    t += p.tE.size(); h += p.Hs.val.size(); l += p.F.Lcm.size(); d += p.F.Dinv.size();
+  }
 }
 
 bool update_materials(HostScene& s, const double* E, const double* nu, std::string& err) {

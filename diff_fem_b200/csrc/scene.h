@@ -63,6 +63,13 @@ struct HostScene {
   int K = 10;
   int precision = DFEM_PREC_FP64;
   int checkpoint_every = 1;
+
+  // A batch is the disjoint union of independent parts (scenes); a single
+  // scene is a batch of one.  Part p owns vertices [part_v0[p], part_v0[p+1]),
+  // tets [part_t0[p], ..), muscle segments [part_seg0[p], ..) — contiguous in
+  // both the user and the internal numbering.
+  int nparts = 1;
+  std::vector<int> part_v0, part_t0, part_seg0;
 };
 
 // Build everything (including ordering + factorisation).  Returns false with err.
@@ -70,5 +77,16 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& hs, std::string& err)
 
 // Re-assemble Hs values after material changes and refactor (same structure).
 bool update_materials(HostScene& hs, const double* E_user_order, const double* nu_user_order, std::string& err);
+
+// Union of independent scenes: every table concatenated with its indices
+// offset, Hs and the supernodal factor block-diagonal, the level schedules
+// merged level by level (level l of the union = level l of every part).  The
+// parts must share time_step, damping, gravity, max_iterations, precision and
+// checkpoint_every; obstacle contact is not supported in a batch.
+bool merge_parts(const std::vector<HostScene>& parts, HostScene& u, std::string& err);
+
+// Copy the parts' material-dependent values (moduli, Hs values, factor blocks)
+// into the union after the parts were refactored (same structure).
+void merge_numeric(const std::vector<HostScene>& parts, HostScene& u);
 
 }  // namespace dfem

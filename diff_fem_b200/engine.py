@@ -45,18 +45,49 @@ def _ptr(a):
 
 
 class Scene:
-    """One simulated world on one GPU (an opaque ``dfem_scene``)."""
+    """One simulated world on one GPU (an opaque ``dfem_scene``), or a batch
+    of independent worlds stepped together (``Scene.batch``)."""
 
     def __init__(self, desc, device: int = 0):
         self.desc = desc
         cdesc, keep = desc.to_c()
         h = C.c_void_p()
         check(lib().dfem_scene_create(C.byref(cdesc), int(device), C.byref(h)))
+        self._init_handle(h, device)
+
+    @classmethod
+    def batch(cls, descs, device: int = 0) -> "Scene":
+        """Independent scenes as one handle: x, v, materials, activations and
+        gradients are the concatenation of the scenes' arrays (``offsets``
+        gives each part's first vertex, tet and segment); every part keeps its
+        own convergence test and iteration count."""
+        descs = list(descs)
+        arr = (_capi.SceneDescC * len(descs))()
+        keep = []
+        for i, d in enumerate(descs):
+            c, k = d.to_c()
+            arr[i] = c
+            keep.append((c, k))
+        h = C.c_void_p()
+        check(lib().dfem_scene_create_batch(arr, len(descs), int(device), C.byref(h)))
+        self = cls.__new__(cls)
+        self.desc = descs
+        self._init_handle(h, device)
+        return self
+
+    def _init_handle(self, h, device):
         self._h = h
         self.device = device
-        self.N = desc.n_vertices
-        self.T = desc.n_tets
-        self.nseg = int(desc.n_segments)
+        n = C.c_int32()
+        check(lib().dfem_batch_layout(h, C.byref(n), None, None, None))
+        self.nparts = int(n.value)
+        vo, to, so = (np.zeros(self.nparts + 1, np.int32) for _ in range(3))
+        P = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        check(lib().dfem_batch_layout(h, C.byref(n), P(vo), P(to), P(so)))
+        self.offsets = {"vertices": vo, "tets": to, "segments": so}
+        self.N = int(vo[-1])
+        self.T = int(to[-1])
+        self.nseg = int(so[-1])
         self._last_steps = 0
 
     def close(self):
@@ -146,10 +177,12 @@ class Scene:
         return out
 
     def iterations(self, n: Optional[int] = None) -> np.ndarray:
+        """PD iterations per step of the last forward call: shape (n,) for a
+        single scene, (n, parts) for a batch."""
         n = self._last_steps if n is None else n
-        out = np.zeros(n, np.int32)
+        out = np.zeros(n * self.nparts, np.int32)
         check(lib().dfem_get_iterations(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)), int(n)))
-        return out
+        return out if self.nparts == 1 else out.reshape(n, self.nparts)
 
     def contact_passes(self, n: Optional[int] = None) -> np.ndarray:
         n = self._last_steps if n is None else n

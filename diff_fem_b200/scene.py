@@ -296,6 +296,136 @@ def muscle_beam(nx: int = 8, ny: int = 3, nz: int = 3, n_chains: int = 2, n_seg:
     )
 
 
+def cell_mesh(cells, ex: float, ey: float, ez: float):
+    """Conforming tet mesh of a set of unit cells (i, j, k) of a global grid,
+    5 tets per cell with the parity of the global index (neighbouring cells
+    share faces).  Returns (x0 (N,3), tets (T,4))."""
+    vid = {}
+    xs = []
+
+    def v(i, j, k):
+        key = (i, j, k)
+        if key not in vid:
+            vid[key] = len(xs)
+            xs.append((i * ex, j * ey, k * ez))
+        return vid[key]
+
+    pat = [_five_tets(0), _five_tets(1)]
+    tets = []
+    for (i, j, k) in sorted(cells):
+        for tet in pat[(i + j + k) & 1]:
+            tets.append([v(i + a, j + b, k + c) for (a, b, c) in tet])
+    return np.asarray(xs, np.float64), np.asarray(tets, np.int32)
+
+
+def star_cells(refine: int = 2):
+    """Cells of the 8-arm star: a central 6x6x3 cube block (x, z horizontal, y
+    up) and two 12x2x2 arms leaving each of its four sides, in units of the
+    0.05 m cube; x and z are refined `refine` times.  Returns (cells, arms)
+    with arms[a] = (axis, sign, lateral cell range, length in cells)."""
+    r = refine
+    C, L, W, H = 6 * r, 12 * r, 2 * r, 2   # centre width, arm length, arm width (cells)
+    cells = {(i, j, k) for i in range(C) for j in range(3) for k in range(C)}
+    arms = []
+    for axis in (0, 2):
+        for sign in (-1, 1):
+            for lat0 in (0, C - W):            # two arms per side, flush with the side's ends
+                arms.append((axis, sign, (lat0, lat0 + W), L))
+                for a in range(L):
+                    o = C + a if sign > 0 else -1 - a
+                    for lat in range(lat0, lat0 + W):
+                        for j in range(H):
+                            cells.add((o, j, lat) if axis == 0 else (lat, j, o))
+    return cells, arms
+
+
+def muscle_star(refine: int = 2, chains_per_arm: int = 8, seg_per_chain: int = 6, stiffness: float = 5e3,
+                youngs: float = 5e4, ground: bool = True, mu: float = 0.5,
+                precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Muscle star: a central 6x6x3 block of 0.05 m cubes with 8 arms of 12x2x2
+    cubes (two per side), x and z refined `refine` times (refine=2: 0.025 m x
+    0.05 m x 0.025 m cells, 1,968 cells, 9,840 tets; refine=1: 2,460 tets).
+    `chains_per_arm` fibre chains run along every arm (one per cross-section
+    cell for refine=2: 64 chains), each split into `seg_per_chain` segments
+    (384 segments); muscle stiffness 5e3.  With `ground`, an obstacle quad lies
+    1e-3 below the body with friction `mu`.  h = 1/60, 15 iterations."""
+    ex, ey, ez = 0.05 / refine, 0.05, 0.05 / refine
+    cells, arms = star_cells(refine)
+    x0, tets = cell_mesh(cells, ex, ey, ez)
+    vol = tet_volumes(x0, tets).sum()
+    mass = lumped_masses(x0, tets, 1000.0 * vol, True)
+    C = 6 * refine
+    segs = []
+    for (axis, sign, (l0, l1), L) in arms:
+        lats = [(l0 + a + 0.5) for a in range(l1 - l0)]
+        heights = [0.5, 1.5]
+        spots = [(lat, h) for h in heights for lat in lats][:chains_per_arm]
+        start = C if sign > 0 else 0
+        for (lat, h) in spots:
+            for q in range(seg_per_chain):
+                a0 = start + sign * L * q / seg_per_chain
+                a1 = start + sign * L * (q + 1) / seg_per_chain
+                if axis == 0:
+                    p0, p1 = (a0 * ex, h * ey, lat * ez), (a1 * ex, h * ey, lat * ez)
+                else:
+                    p0, p1 = (lat * ex, h * ey, a0 * ez), (lat * ex, h * ey, a1 * ez)
+                segs.append((p0, p1))
+    mt, mf, mk, ms = muscle_constraints(x0, tets, segs, stiffness, radius=0.5 * min(ex, ey, ez))
+    T = tets.shape[0]
+    kw = {}
+    if ground:
+        faces, cverts = surface_of(x0, tets)
+        ctr = x0.mean(axis=0)
+        gx, gf = ground_quad(x0[:, 1].min() - 1e-3, 2.0, center=(ctr[0], ctr[2]))
+        kw = dict(contact_vertices=cverts, contact_faces=faces, obstacle_x=gx, obstacle_faces=gf,
+                  handle_collision=True, obstacle_friction=mu)
+    return SceneDesc(
+        x0=x0, mass=mass, tets=tets, youngs=np.full(T, youngs), poisson=np.full(T, 0.3),
+        muscle_tets=mt, muscle_fiber=mf, muscle_stiffness=mk, muscle_segment=ms, n_segments=len(segs),
+        time_step=1.0 / 60.0, max_iterations=15, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name=f"muscle_star_r{refine}", **kw,
+    )
+
+
+def uneven_batch(n_scenes: int = 256, seed: int = 7, t_lo: float = 1e3, t_hi: float = 5e4,
+                 precision: int = DFEM_PREC_FP64, max_iterations: int = 15):
+    """Batch of independent scenes of uneven size: tet counts log-uniform in
+    [t_lo, t_hi] from `seed`, alternating beams (cube-grid bars as the
+    cantilever / inverse-stiffness scenes, cross-section ny = nz, length 5x the
+    width, x = 0 face pinned) and muscle stars without ground (arm length and
+    refinement chosen to approach the target count).  Per-scene log-uniform
+    moduli in [1e4, 1e6] Pa.  All share h = 1/60, 15 iterations, damping 0.9999
+    and gravity.  Returns (descs, target tet counts)."""
+    import dataclasses
+    rng = np.random.default_rng(seed)
+    targets = np.exp(rng.uniform(np.log(t_lo), np.log(t_hi), size=n_scenes))
+    descs = []
+    stars = {}  # the star geometry depends only on the refinement: build each once
+    for q, tgt in enumerate(targets):
+        if q % 2 == 0:
+            w = max(2, int(round((tgt / 25.0) ** (1.0 / 3.0))))
+            nx = max(2, int(round(tgt / (5.0 * w * w))))
+            x0, tets = cube_grid(nx, w, w, 0.05)
+            mass = lumped_masses(x0, tets, 1000.0 * nx * w * w * 0.05 ** 3, True)
+            pins = np.nonzero(np.isclose(x0[:, 0], 0.0))[0].astype(np.int32)
+            T = tets.shape[0]
+            d = SceneDesc(
+                x0=x0, mass=mass, tets=tets, youngs=log_uniform_moduli(T, 1000 + q), poisson=np.full(T, 0.3),
+                attach_vertex=pins, attach_target=x0[pins], attach_stiffness=np.full(pins.size, 1e10),
+                time_step=1.0 / 60.0, max_iterations=max_iterations, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+                precision=precision, name=f"beam_{nx}x{w}x{w}")
+        else:
+            refine = 1 if tgt < 2460 * 1.7 else (2 if tgt < 9840 * 1.7 else 3)
+            if refine not in stars:
+                stars[refine] = muscle_star(refine=refine, chains_per_arm=min(8, 4 * refine), ground=False,
+                                            precision=precision)
+            base = stars[refine]
+            d = dataclasses.replace(base, youngs=log_uniform_moduli(base.n_tets, 1000 + q),
+                                    max_iterations=max_iterations)
+        descs.append(d)
+    return descs, targets
+
+
 # ------------------------------------------------------------------ contact ---
 
 def tet_surface(tets: np.ndarray):

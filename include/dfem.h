@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define DFEM_ABI_VERSION 1
+#define DFEM_ABI_VERSION 2
 
 enum dfem_status {
   DFEM_OK = 0,
@@ -134,6 +134,25 @@ typedef struct dfem_scene_info {
  * prefactorisation.  Replaces World::Initialize + World::PreComputation +
  * World::FactorizeLDLT (sim/fem/World.h:248-384, 1089-1139, 1212-1232). */
 int dfem_scene_create(const dfem_scene_desc *desc, int device, dfem_scene **out);
+
+/* A batch: n_scenes independent scenes stepped together as one handle.  The
+ * parts are the disjoint union of the scenes: every per-vertex, per-tet and
+ * per-segment array of the other calls (x, v, traj_x, youngs, poisson,
+ * activations rows, gradients) is the concatenation of the scenes' arrays in
+ * the given order.  Every part keeps its own convergence test and iteration
+ * count (one World each, as a loop over scenes in the reference would run
+ * them), its own factor and its own regularisation retry; the triangular
+ * solves of all parts share one level schedule.  The scenes must share
+ * time_step, damping, gravity, max_iterations, precision and
+ * checkpoint_every; obstacle contact is not supported in a batch. */
+int dfem_scene_create_batch(const dfem_scene_desc *descs, int32_t n_scenes, int device, dfem_scene **out);
+
+/* Part layout of a scene handle (a single scene is one part).  The offset
+ * arrays (n_parts + 1 entries each; may be NULL) receive the first vertex,
+ * tet and muscle segment of every part. */
+int dfem_batch_layout(const dfem_scene *scene, int32_t *n_parts, int32_t *vertex_offsets,
+                      int32_t *tet_offsets, int32_t *segment_offsets);
+
 int dfem_scene_destroy(dfem_scene *scene);
 int dfem_scene_get_info(const dfem_scene *scene, dfem_scene_info *info);
 
@@ -198,7 +217,8 @@ int dfem_eval_corotated_noalloc(int32_t n_vertices, int32_t n_tets, const double
  * The loop of World::ProjectiveDynamicsMethod (sim/fem/World.h:928-1022). */
 int dfem_get_contact_passes(const dfem_scene *scene, int32_t *passes, int32_t n);
 
-/* Iteration counts of the last forward call (n_steps values), host buffer. */
+/* Iteration counts of the last forward call: n steps x n_parts values
+ * (row per step), host buffer. */
 int dfem_get_iterations(const dfem_scene *scene, int32_t *iters, int32_t n);
 
 /* Host-only diagnostic, needs no GPU: builds the scene's fill-reducing

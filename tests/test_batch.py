@@ -1,0 +1,101 @@
+"""Batches of independent scenes (dfem_scene_create_batch) against the same
+scenes stepped one at a time.
+
+Every part of a batch runs the same arithmetic in the same order as the scene
+alone (its own convergence test, iteration count and factor; part-aligned
+reduction blocks), so positions, velocities, iteration counts and gradients
+must agree bit for bit.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from diff_fem_b200 import _capi, scene as S
+from diff_fem_b200.engine import Scene
+
+pytestmark = pytest.mark.gpu
+
+
+def harmonise(descs, precision=_capi.DFEM_PREC_FP64):
+    """Batch members share time step, iteration cap, damping and gravity."""
+    return [dataclasses.replace(d, time_step=1.0 / 60.0, max_iterations=15, damping=0.9999,
+                                gravity=(0.0, -9.8, 0.0), precision=precision) for d in descs]
+
+
+def mixed_scenes(precision=_capi.DFEM_PREC_FP64):
+    return harmonise([S.inverse_stiffness(nx=10, ny=3, nz=3), S.muscle_beam(), S.cantilever(),
+                      S.cloth_sheet(nv=8), S.inverse_stiffness(nx=6, ny=2, nz=2, seed=7)], precision)
+
+
+def concat_state(descs):
+    x = np.concatenate([d.x0.reshape(-1) for d in descs])
+    return x, np.zeros_like(x)
+
+
+def split(a, offs, scale=3):
+    return [a[scale * offs[i]: scale * offs[i + 1]] for i in range(len(offs) - 1)]
+
+
+@pytest.mark.parametrize("precision", [_capi.DFEM_PREC_FP64, _capi.DFEM_PREC_MIXED])
+def test_batch_matches_scenes_one_at_a_time(precision):
+    descs = mixed_scenes(precision)
+    n = 6
+    b = Scene.batch(descs)
+    assert b.nparts == len(descs)
+    vo = b.offsets["vertices"]
+    assert list(np.diff(vo)) == [d.n_vertices for d in descs]
+    nseg = [d.n_segments for d in descs]
+    rng = np.random.default_rng(3)
+    acts = [rng.uniform(0, 1, (n, k)) for k in nseg]
+    act = np.concatenate(acts, axis=1) if sum(nseg) else None
+    x, v = concat_state(descs)
+    xb, vb, tb = b.forward(x, v, n_steps=n, act=act, traj=True)
+    itb = b.iterations(n)
+    assert itb.shape == (n, len(descs))
+    gx = rng.standard_normal(x.size)
+    gv = rng.standard_normal(x.size)
+    gb = b.backward(gx, gv)
+    to = b.offsets["tets"]
+    so = b.offsets["segments"]
+    for p, d in enumerate(descs):
+        s = Scene(d)
+        xs, vs, ts = s.forward(d.x0.reshape(-1), np.zeros(3 * d.n_vertices), n_steps=n,
+                               act=acts[p] if nseg[p] else None, traj=True)
+        assert np.array_equal(s.iterations(n), itb[:, p]), p
+        assert np.array_equal(split(xb, vo)[p], xs), p
+        assert np.array_equal(split(vb, vo)[p], vs), p
+        assert np.array_equal(tb[:, 3 * vo[p]: 3 * vo[p + 1]], ts), p
+        gs = s.backward(split(gx, vo)[p], split(gv, vo)[p])
+        assert np.array_equal(split(gb["x"], vo)[p], gs["x"]), p
+        assert np.array_equal(split(gb["v"], vo)[p], gs["v"]), p
+        assert np.array_equal(gb["E"][to[p]:to[p + 1]], gs["E"]), p
+        assert np.array_equal(gb["nu"][to[p]:to[p + 1]], gs["nu"]), p
+        if nseg[p]:
+            assert np.array_equal(gb["act"][:, so[p]:so[p + 1]], gs["act"]), p
+        s.close()
+    b.close()
+
+
+def test_batch_set_materials_refactors_each_part():
+    descs = harmonise([S.inverse_stiffness(nx=8, ny=3, nz=3, seed=s) for s in (1, 2, 3)])
+    b = Scene.batch(descs)
+    E = np.concatenate([S.log_uniform_moduli(d.n_tets, 100 + i) for i, d in enumerate(descs)])
+    nu = np.full(E.size, 0.3)
+    b.set_materials(E, nu)
+    x, v = concat_state(descs)
+    xb, _ = b.forward(x, v, n_steps=4)
+    vo, to = b.offsets["vertices"], b.offsets["tets"]
+    for p, d in enumerate(descs):
+        s = Scene(d)
+        s.set_materials(E[to[p]:to[p + 1]], nu[to[p]:to[p + 1]])
+        xs, _ = s.forward(d.x0.reshape(-1), np.zeros(3 * d.n_vertices), n_steps=4)
+        assert np.array_equal(split(xb, vo)[p], xs)
+        s.close()
+    b.close()
+
+
+def test_batch_rejects_mismatched_time_steps():
+    descs = [S.cantilever(), S.inverse_stiffness(nx=6, ny=2, nz=2)]
+    with pytest.raises(_capi.DfemError, match="time_step"):
+        Scene.batch(descs)
