@@ -458,23 +458,18 @@ static void launch_gather(dfem_scene* sc, cudaStream_t st, Gate g, const double*
     k_gather<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
 }
 
+// The adjoint of the local step runs in FP64 in both forms: its parameter
+// terms Y:(md - F) cancel down to the size of the strain, which FP32 rounding
+// of md and F (1e-7 of their size) would swamp.
 static void launch_adj_local(dfem_scene* sc, cudaStream_t st, Gate g, const int* kptr) {
   const HostScene& s = sc->hs;
   const int nthr = std::max(s.T + s.M + s.S + s.B, s.N);
-  if (mixed(sc))
-    k_adj_local_f32<<<(nthr + 127) / 128, 128, 0, st>>>(sc->sd, g, kptr, sc->step.p, sc->hist.p, sc->y.p, sc->bb.p,
-                                                         sc->act_all.p, slot32(sc), sc->gE.p, sc->gnu.p, sc->mg.p);
-  else
-    k_adj_local<<<(nthr + 127) / 128, 128, 0, st>>>(sc->sd, g, kptr, sc->step.p, sc->hist.p, sc->y.p, sc->bb.p,
-                                                     sc->act_all.p, sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+  k_adj_local<<<(nthr + 127) / 128, 128, 0, st>>>(sc->sd, g, kptr, sc->step.p, sc->hist.p, sc->y.p, sc->bb.p,
+                                                   sc->act_all.p, sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
 }
 
 static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
-  const int N = sc->hs.N;
-  if (mixed(sc))
-    k_adj_gather_f32<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vpart.p, sc->vslot_ptr.p, slot32(sc), sc->xkb.p);
-  else
-    k_adj_gather<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
+  k_adj_gather<<<sc->nblk_v, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
 }
 
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {

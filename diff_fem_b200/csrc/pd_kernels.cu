@@ -715,140 +715,6 @@ __global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const 
   }
 }
 
-// Mixed-form adjoint of the local step: FP32 VJPs (FP64 for near-degenerate
-// elements), FP32 slots; parameter gradients accumulate in FP64.
-__global__ void __launch_bounds__(128) k_adj_local_f32(SceneDev d, Gate gate, const int* kptr, const int* step,
-                                                       const double* __restrict__ hist, const double* __restrict__ yb,
-                                                       double* bb, const double* __restrict__ act_all,
-                                                       float* __restrict__ slot, double* gE, double* gnu, double* mg) {
-  const int k = *kptr;
-  const double* x = hist + (size_t)k * 3 * d.N;
-  const double* x1 = hist + (size_t)(k + 1) * 3 * d.N;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < d.N && !gate.skip(vpart_of(d, t))) st3(bb, t, ld3(bb, t) + ld3(yb, t));
-  if (gate.skip(cons_part(d, t))) return;
-  if (t < d.T) {
-    int4 v = d.tv[t];
-    const int vi[4] = {v.x, v.y, v.z, v.w};
-    Vec3<double> xv[4], x1v[4];
-    Vec3<float> yv[4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) { xv[a] = ld3(x, vi[a]); x1v[a] = ld3(x1, vi[a]); yv[a] = to_f(ld3(yb, vi[a])); }
-    float G[4][3];
-    Mat3<float> F, F1, Y, md, mdv;
-    tet_f32(d.tinv32, d.T, t, xv, G, F);
-    tet_f32(d.tinv32, d.T, t, x1v, G, F1);
-#pragma unroll
-    for (int j = 0; j < 3; ++j) Y.c[j] = G[0][j] * yv[0] + G[1][j] * yv[1] + G[2][j] * yv[2] + G[3][j] * yv[3];
-    float ratio;
-    corot_project(F, md, mdv, &ratio);
-    Mat3<float> gF;
-    const double E = d.tE[t], nu = d.tnu[t], vol = d.tvol[t];
-    double yr = 0, yvv = 0, yh = 0;
-    if (ratio >= kDegenerateRatio) {
-#pragma unroll
-      for (int j = 0; j < 3; ++j) { yr += dot3(Y.c[j], md.c[j]); yvv += dot3(Y.c[j], mdv.c[j]); yh += dot3(Y.c[j], F1.c[j]); }
-      float wr = d.twr32[t], wv = d.twv32[t];
-      Mat3<float> gmd, gmdv;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) { gmd.c[j] = wr * Y.c[j]; gmdv.c[j] = wv * Y.c[j]; }
-      gF = corot_vjp(F, gmd, gmdv);
-    } else {  // near-degenerate element: FP64
-      double Gd[4][3];
-      load_g(d.tinv, d.T, t, Gd);
-      Vec3<double> ydv[4] = {ld3(yb, vi[0]), ld3(yb, vi[1]), ld3(yb, vi[2]), ld3(yb, vi[3])};
-      Mat3<double> Fd = deformation(Gd, xv), F1d = deformation(Gd, x1v), Yd = deformation(Gd, ydv), mdd, mdvd;
-      corot_project(Fd, mdd, mdvd);
-#pragma unroll
-      for (int j = 0; j < 3; ++j) { yr += dot3(Yd.c[j], mdd.c[j]); yvv += dot3(Yd.c[j], mdvd.c[j]); yh += dot3(Yd.c[j], F1d.c[j]); }
-      Mat3<double> gmd, gmdv;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) { gmd.c[j] = d.twr[t] * Yd.c[j]; gmdv.c[j] = d.twv[t] * Yd.c[j]; }
-      Mat3<double> gFd = corot_vjp(Fd, gmd, gmdv);
-#pragma unroll
-      for (int j = 0; j < 3; ++j) gF.c[j] = to_f(gFd.c[j]);
-    }
-    double opn = 1.0 + nu;
-    if (gE) gE[t] += vol / opn * (yr + nu * yvv) - vol * yh;
-    if (gnu) gnu[t] += E * vol / (opn * opn) * (yvv - yr);
-    int4 sl = d.tslot[t];
-    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
-#pragma unroll
-    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], G[a][0] * gF.c[0] + G[a][1] * gF.c[1] + G[a][2] * gF.c[2]);
-    return;
-  }
-  t -= d.T;
-  if (t < d.M) {
-    int4 v = d.mv[t];
-    const int vi[4] = {v.x, v.y, v.z, v.w};
-    Vec3<float> f = mk3((float)d.mfib[t], (float)d.mfib[d.M + t], (float)d.mfib[2 * d.M + t]);
-    float w = (float)d.mw[t];
-    float c[4] = {0, 0, 0, 0};
-    Vec3<double> x0 = ld3(x, vi[0]);
-    Vec3<float> Ff = mk3(0.0f, 0.0f, 0.0f);
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      float cq = (float)d.minv[(q * 3 + 0) * d.M + t] * f.x + (float)d.minv[(q * 3 + 1) * d.M + t] * f.y +
-                 (float)d.minv[(q * 3 + 2) * d.M + t] * f.z;
-      c[q + 1] = cq;
-      c[0] -= cq;
-      Ff = Ff + cq * to_f(ld3(x, vi[q + 1]) - x0);
-    }
-    Vec3<float> db = mk3(0.0f, 0.0f, 0.0f);
-#pragma unroll
-    for (int a = 0; a < 4; ++a) db = db + (w * c[a]) * to_f(ld3(yb, vi[a]));
-    float a_act = (float)act_all[(size_t)(*step) * d.nseg + d.mseg[t]];
-    mg[t] = -(double)dot3(db, Ff);
-    int4 sl = d.mslot[t];
-    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
-#pragma unroll
-    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], ((1.0f - a_act) * c[a]) * db);
-    return;
-  }
-  t -= d.M;
-  if (t < d.S) {
-    int2 v = d.sv[t];
-    float w = (float)d.ssw[t];
-    Vec3<float> db = w * to_f(ld3(yb, v.x) - ld3(yb, v.y));
-    Vec3<float> e = to_f(ld3(x, v.x) - ld3(x, v.y));
-    float inv = rsqrtf(dot3(e, e));
-    Vec3<float> eh = inv * e;
-    Vec3<float> ge = ((float)d.srest[t] * inv) * (db - dot3(eh, db) * eh);
-    int2 sl = d.sslot[t];
-    st3f(slot, sl.x, ge);
-    st3f(slot, sl.y, (-1.0f) * ge);
-    return;
-  }
-  t -= d.S;
-  if (t < d.B) {
-    int o0 = d.boff[t], o1 = d.boff[t + 1];
-    float w = (float)d.bw[t];
-    Vec3<double> xc = ld3(x, d.bv[o0]);
-    Vec3<float> db = mk3(0.0f, 0.0f, 0.0f), lap = mk3(0.0f, 0.0f, 0.0f);
-    for (int q = o0; q < o1; ++q) {
-      db = db + (w * (float)d.bbeta[q]) * to_f(ld3(yb, d.bv[q]));
-      lap = lap + (float)d.bbeta[q] * to_f(ld3(x, d.bv[q]) - xc);
-    }
-    float ln = sqrtf(dot3(lap, lap));
-    Vec3<float> gl = mk3(0.0f, 0.0f, 0.0f);
-    if (ln > 1e-25f) {
-      Vec3<float> lh = (1.0f / ln) * lap;
-      gl = (w * (float)d.brest[t] / ln) * (db - dot3(lh, db) * lh);
-    }
-    for (int q = o0; q < o1; ++q) st3f(slot, d.bslot[q], (float)d.bbeta[q] * gl);
-  }
-}
-
-__global__ void k_adj_gather_f32(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
-                                 const float* __restrict__ slot,
-                                 double* xkb) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
-  Vec3<float> acc = mk3(0.0f, 0.0f, 0.0f);
-  for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3f(slot, k);
-  st3(xkb, i, to_d(acc));
-}
-
 // xbar^k = sum of the slots (constraints without x dependence contribute nothing)
 __global__ void k_adj_gather(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
                                  const double* __restrict__ slot,

@@ -194,13 +194,8 @@ constexpr float kDegenerateRatio = 0.05f;
 //   with M_X = U^T X V, a_ij = (g_i - g_j)/(s_i - s_j), b_ij = (g_i + g_j)/(s_i + s_j);
 //   F_bar = U P_bar V^T.
 template <typename T>
-__device__ __forceinline__ Mat3<T> corot_vjp(const Mat3<T>& F, Mat3<T> gmd, const Mat3<T>& gmdv, T* s_ratio = nullptr) {
+__device__ __forceinline__ Mat3<T> corot_vjp(const Mat3<T>& F, Mat3<T> gmd, const Mat3<T>& gmdv) {
   Svd3<T> sv = svd3(F);
-  if (s_ratio) {
-    T smax = sv.s[0] > sv.s[1] ? (sv.s[0] > sv.s[2] ? sv.s[0] : sv.s[2]) : (sv.s[1] > sv.s[2] ? sv.s[1] : sv.s[2]);
-    T smin = sv.s[0] < sv.s[1] ? (sv.s[0] < sv.s[2] ? sv.s[0] : sv.s[2]) : (sv.s[1] < sv.s[2] ? sv.s[1] : sv.s[2]);
-    *s_ratio = smax > T(0) ? smin / smax : T(0);
-  }
   T g[3], J[3][3], dd[3];
   volume_projection_d(sv.s, g, J, dd);
   if (det3(F) < T(0)) gmd.c[2] = T(-1) * gmd.c[2];
