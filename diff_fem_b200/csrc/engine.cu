@@ -92,6 +92,12 @@ struct dfem_scene {
   std::vector<int> lvl_ptr;
   int max_w = 1, max_r = 0;
   std::vector<size_t> shm_fwd, shm_bwd;  // dynamic shared memory of the level kernels, per level
+  // persistent solve (one launch per solve) and the autotuned choice between it and the level kernels
+  DBuf<int> sn_parent, kid_ptr, kid, done_f, done_b, solve_ctl;
+  size_t shm_pers = 0;
+  int pers_grid = 1;
+  int solve_mode = 0;                    // 0: level kernels, 1: persistent
+  double solve_ms[2] = {0.0, 0.0};       // autotune timings (ms per solve) of the two modes
   // batch layout (a single scene is one part)
   std::vector<HostScene> parts;          // the parts of a batch (empty for a single scene)
   DBuf<int> vpart, seg_part, sn_part, part_v0, part_b0, blk_part, blk_v0;
@@ -212,6 +218,30 @@ static int upload_factor(dfem_scene* sc) {
     }
   CK(cudaFuncSetAttribute(k_fwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_f[stage_l]));
   CK(cudaFuncSetAttribute(k_bwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_b[stage_l]));
+  // persistent solve: elimination tree (children CSR), completion stamps, control words
+  {
+    std::vector<int> kp(F.nsuper + 1, 0), kd(std::max(1, F.nsuper));
+    for (int q = 0; q < F.nsuper; ++q)
+      if (F.sn_parent[q] >= 0) kp[F.sn_parent[q] + 1]++;
+    for (int q = 0; q < F.nsuper; ++q) kp[q + 1] += kp[q];
+    std::vector<int> fill(kp.begin(), kp.end() - 1);
+    for (int q = 0; q < F.nsuper; ++q)
+      if (F.sn_parent[q] >= 0) kd[fill[F.sn_parent[q]]++] = q;
+    CK(sc->sn_parent.upload(F.sn_parent));
+    CK(sc->kid_ptr.upload(kp));
+    CK(sc->kid.upload(kd));
+    if (sc->done_f.n != (size_t)F.nsuper || !sc->done_f.p) {
+      CK(sc->done_f.alloc(std::max(1, F.nsuper)));
+      CK(sc->done_b.alloc(std::max(1, F.nsuper)));
+      CK(sc->solve_ctl.alloc(4));
+    }
+    sc->shm_pers = std::max(need_f[stage_l], need_b[stage_l]);
+    CK(cudaFuncSetAttribute(k_solve_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_pers));
+    int nsm = 1, per_sm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, sc->device));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_persistent, 256, sc->shm_pers));
+    sc->pers_grid = std::max(1, std::min(nsm * std::max(1, per_sm), 2 * F.nsuper));
+  }
   if (sc->hs.nparts > 1) {
     std::vector<int> snp(F.nsuper);
     for (int q = 0; q < F.nsuper; ++q)
@@ -220,7 +250,8 @@ static int upload_factor(dfem_scene* sc) {
   }
   FactorDev fd{sc->rseg_ptr.p, sc->rseg_pos.p, sc->contrib.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p,
                sc->sn_rofs.p, sc->rowidx.p, sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->lvl_sn.p,
-               stage_l, sc->status.p, sc->hs.nparts > 1 ? sc->sn_part.p : nullptr};
+               stage_l, sc->status.p, sc->hs.nparts > 1 ? sc->sn_part.p : nullptr,
+               F.nsuper, sc->sn_parent.p, sc->kid_ptr.p, sc->kid.p, sc->done_f.p, sc->done_b.p, sc->solve_ctl.p};
   if (std::memcmp(&fd, &sc->fd, sizeof(fd)) != 0) invalidate_graphs(sc);
   sc->fd = fd;
   return DFEM_OK;
@@ -399,8 +430,13 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   return DFEM_OK;
 }
 
-// one forward step: enqueue the kernel sequence on the stream (captured into a graph)
+// The global solve Hs y = rhs: one persistent launch, or one launch per level
+// and direction (the autotuned choice for the scene).
 static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
+  if (sc->solve_mode == 1) {
+    k_solve_persistent<<<sc->pers_grid, 256, sc->shm_pers, st>>>(sc->fd, gate, rhs, y);
+    return;
+  }
   const int L = (int)sc->lvl_ptr.size() - 1;
   for (int l = 0; l < L; ++l) {
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
@@ -410,6 +446,17 @@ static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const doub
     int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
     k_bwd_level<<<nb, 256, sc->shm_bwd[l], st>>>(sc->fd, sc->lvl_ptr[l], gate, y);
   }
+}
+
+static int solve_launches(const dfem_scene* sc) {
+  return sc->solve_mode == 1 ? 1 : 2 * ((int)sc->lvl_ptr.size() - 1);
+}
+
+// Fresh completion stamps and control words of the persistent solve (each API
+// call starts from them, whatever an earlier call left behind).
+static void reset_solve_state(dfem_scene* sc) {
+  k_solve_reset<<<std::max(1, std::min(256, (sc->hs.F.nsuper + 255) / 256)), 256, 0, sc->stream>>>(
+      sc->hs.F.nsuper, sc->done_f.p, sc->done_b.p, sc->solve_ctl.p);
 }
 
 // A time step (and the adjoint of one) is a CUDA graph: pre-loop kernels, a
@@ -651,6 +698,43 @@ static int status_error(const int st4[4]) {
   return DFEM_OK;
 }
 
+// Time both solve forms on this scene's factor (10 solves each after 3 warm-up
+// solves) and keep the faster.
+static int autotune_solve(dfem_scene* sc) {
+  const size_t n3 = 3 * (size_t)sc->hs.N;
+  CK(cudaMemsetAsync(sc->rhs.p, 0, n3 * sizeof(double), sc->stream));
+  reset_solve_state(sc);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int reps = 10;
+  for (int mode = 0; mode < 2; ++mode) {
+    sc->solve_mode = mode;
+    for (int r = 0; r < 3; ++r) enqueue_solve(sc, sc->stream, kOpen, sc->rhs.p, sc->y.p);
+    cudaEventRecord(e0, sc->stream);
+    for (int r = 0; r < reps; ++r) enqueue_solve(sc, sc->stream, kOpen, sc->rhs.p, sc->y.p);
+    cudaEventRecord(e1, sc->stream);
+    cudaError_t e = cudaEventSynchronize(e1);
+    float t = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return fail(DFEM_ERR_CUDA, std::string("solve autotune: ") + cudaGetErrorString(e));
+    }
+    sc->solve_ms[mode] = (double)t / reps;
+    sc->launches += (int64_t)(reps + 3) * solve_launches(sc);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int st4[4] = {0, 0, 0, 0};
+  CK(cudaMemcpy(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost));
+  RC(status_error(st4));
+  sc->solve_mode = sc->solve_ms[1] < sc->solve_ms[0] ? 1 : 0;
+  invalidate_graphs(sc);
+  return DFEM_OK;
+}
+
 // Device side of scene creation, once sc->hs (and sc->parts for a batch) is built.
 static int create_on_device(std::unique_ptr<dfem_scene>& sc, int device, dfem_scene** out) {
   CK(cudaStreamCreate(&sc->stream));  // blocking: orders with the legacy default stream callers use
@@ -659,6 +743,8 @@ static int create_on_device(std::unique_ptr<dfem_scene>& sc, int device, dfem_sc
   CK(sc->status.alloc(4));  // before the factor upload, whose kernels report into it
   RC(upload_scene(sc.get()));
   RC(ensure_steps(sc.get(), 1));
+  CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
+  RC(autotune_solve(sc.get()));
   CK(cudaDeviceSynchronize());
   *out = sc.release();
   g_last_error.clear();
@@ -826,6 +912,7 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, 0);
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, traj_x ? 1 : 0);
   CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
+  reset_solve_state(sc);
   CK(cudaGetLastError());
   RC(ensure_graphs(sc));
   for (int st = 0; st < n_steps; ++st) CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
@@ -876,6 +963,7 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   CK(cudaMemsetAsync(sc->gact.p, 0, sizeof(double) * (size_t)sc->rec_steps * std::max(1, s.nseg), sc->stream));
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, 0);
   CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
+  reset_solve_state(sc);
   RC(ensure_graphs(sc));
   for (int st = sc->rec_steps - 1; st >= 0; --st) {
     // recompute the step's iterates from its checkpoint (the step graph re-records the same checkpoint)
@@ -960,6 +1048,24 @@ int dfem_host_factor_solve(const dfem_scene_desc* desc, const double* b, double*
   return DFEM_OK;
 }
 
+int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms) {
+  if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
+  if (request < -1 || request > 2) return fail(DFEM_ERR_INVALID, "request must be -1, 0, 1 or 2");
+  CK(cudaSetDevice(sc->device));
+  if (request == 0) {
+    CK(cudaStreamSynchronize(sc->stream));
+    CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
+    RC(autotune_solve(sc));
+    sc->rec_steps = 0;  // the tuning solves overwrote the recorded iterates
+  } else if (request > 0 && request - 1 != sc->solve_mode) {
+    sc->solve_mode = request - 1;
+    invalidate_graphs(sc);
+  }
+  if (chosen) *chosen = sc->solve_mode + 1;
+  if (ms) { ms[0] = sc->solve_ms[0]; ms[1] = sc->solve_ms[1]; }
+  return DFEM_OK;
+}
+
 int dfem_get_launch_count(const dfem_scene* sc, int64_t* count) {
   if (!sc || !count) return fail(DFEM_ERR_INVALID, "null argument");
   *count = sc->launches;
@@ -976,6 +1082,7 @@ int dfem_profile_phases(dfem_scene* sc, int32_t reps, double* ms) {
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, 0);
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->zero.p, 0);
   CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
+  reset_solve_state(sc);
   const Gate gf = kOpen, ga = kOpen;
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
@@ -1005,8 +1112,8 @@ int dfem_profile_phases(dfem_scene* sc, int32_t reps, double* ms) {
   CK(cudaMemcpyAsync(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost, sc->stream));
   CK(cudaStreamSynchronize(sc->stream));
   RC(status_error(st4));
-  // the solve phase counted one launch per call above; it is 2 * levels kernels
-  sc->launches += (int64_t)(reps + 1) * (2 * ((int64_t)sc->lvl_ptr.size() - 1) - 1);
+  // the solve phase counted one launch per call above
+  sc->launches += (int64_t)(reps + 1) * (solve_launches(sc) - 1);
   sc->rec_steps = 0;  // gates and iteration counts were overwritten: no backward of the old forward
   return DFEM_OK;
 }

@@ -160,6 +160,14 @@ struct FactorDev {
   int stage_l;   // 1: the below-diagonal blocks are staged in shared memory too
   int* status;   // error status word (6: a bounded wait gave up)
   const int* sn_part;  // batch: part of every supernode (null for a single scene)
+  // persistent solve: elimination tree, completion stamps, control words
+  int nsuper;
+  const int* sn_parent;
+  const int* kid_ptr;
+  const int* kid;
+  int* done_f;
+  int* done_b;
+  int* ctl;      // [ticket, CTAs finished, epoch, abort]
 };
 
 }  // namespace dfem

@@ -329,60 +329,64 @@ __global__ void k_gather(int N, Gate gate, const int* __restrict__ vpart, const 
   st3(rhs, i, acc);
 }
 
-// Forward solve of one level, push form: for each supernode s of the level,
-//   t   = rhs_s - (contributions pushed to s's rows by its descendants)
-//   y_s = Dinv_s t                       (warp per row)
-//   contrib[R_s] = L_{R_s,s} y_s         (thread per below-diagonal row; read by ancestors)
-// Latency rather than bandwidth bounds these kernels (a few KB per supernode).
-// At kernel entry one thread moves the supernode's dense blocks (the inverse
-// of the diagonal block and, when it fits, the below-diagonal block) into
-// shared memory with TMA bulk copies; while they are in flight the warps sum
-// each row's descendant contributions (lanes over segments).  Everything
-// after the barrier runs from shared memory.
-
-// Stage Dinv (and L_{R,s} if stage_l) of supernode s; returns false (uniformly
-// across the CTA) when the copies did not complete within the bounded wait.
+// Stage Dinv (and L_{R,s} if stage_l) of supernode s into shared memory.  The
+// proxy fence orders this CTA's earlier generic reads of the same shared
+// memory (a previous supernode of the persistent solve) before the bulk writes.
 __device__ __forceinline__ void stage_blocks_issue(const FactorDev& f, int s, int w, int r, double* Dsh, double* Lsh,
                                                    uint64_t* bar) {
   if (threadIdx.x == 0) {
     const unsigned bd = (unsigned)(((w * w + 1) & ~1) * sizeof(double));
     const unsigned bl = f.stage_l ? (unsigned)(((r * w + 1) & ~1) * sizeof(double)) : 0u;
+    fence_proxy_async_smem();
     mbar_expect_tx(bar, bd + bl);
     bulk_copy_g2s(Dsh, f.Dinv + f.sn_dofs[s], bd, bar);
     if (bl) bulk_copy_g2s(Lsh, f.Lcm + f.sn_lofs[s], bl, bar);
   }
 }
 
-// status[0] = 6 (DFEM_ERR_CAP) when the wait gave up; status[1] = the supernode,
-// status[2] = 1 (forward) / 2 (backward), status[3] counts the blocks that gave up.
-__device__ __forceinline__ bool stage_blocks_wait(const FactorDev& f, uint64_t* bar, int s, int which) {
-  const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0) ? 1 : 0) != 0;
+// A bounded wait gave up: status[0] = 6 (DFEM_ERR_CAP), status[1] = the
+// supernode, status[2] = which wait (1 forward / 2 backward staging, 3 / 4
+// persistent-solve dependency), status[3] counts the CTAs that gave up.
+__device__ __forceinline__ void record_gave_up(const FactorDev& f, int s, int which) {
+  f.status[0] = 6;
+  f.status[1] = s;
+  f.status[2] = which;
+  atomicAdd(f.status + 3, 1);
+}
+
+// Wait for the staged blocks (phase parity `phase` of the barrier); false,
+// uniformly across the CTA, when the bounded wait gave up.
+__device__ __forceinline__ bool stage_blocks_wait(const FactorDev& f, uint64_t* bar, unsigned phase, int s, int which) {
+  const bool ok = __syncthreads_and(mbar_wait_bounded(bar, phase) ? 1 : 0) != 0;
   if (!ok && threadIdx.x == 0) {
-    f.status[0] = 6;
-    f.status[1] = s;
-    f.status[2] = which;
-    atomicAdd(f.status + 3, 1);
-    mbar_wait_bounded(bar, 0);     // give in-flight copies one more bounded chance to land
+    record_gave_up(f, s, which);
+    mbar_wait_bounded(bar, phase);  // give in-flight copies one more bounded chance to land
   }
   return ok;
 }
 
-__global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, Gate gate,
-                                                   const double* __restrict__ rhs, double* y) {
-  extern __shared__ __align__(16) double sh[];  // Dinv (w*w, even) | L_{R,s} (r*w, even; if staged) | t (3w) | y_s (3w)
-  __shared__ __align__(8) uint64_t bar;
-  const int s = f.lvl_sn[lvl_begin + blockIdx.x];
-  if (gate.skip(f.sn_part ? f.sn_part[s] : 0)) return;
+// Forward solve of supernode s, push form:
+//   t   = rhs_s - (contributions pushed to s's rows by its descendants)
+//   y_s = Dinv_s t                       (warp per row)
+//   contrib[R_s] = L_{R_s,s} y_s         (thread per below-diagonal row; read by ancestors)
+// One thread moves the supernode's dense blocks (the inverse of the diagonal
+// block and, when it fits, the below-diagonal block) into shared memory with
+// TMA bulk copies (unless the caller already issued them); while they are in
+// flight the warps sum each row's descendant contributions.  Everything after
+// the barrier runs from shared memory.  Values written by other CTAs of the
+// same launch (contributions) are read through L2 (ld.cg).  Shared layout
+// (doubles): Dinv (w*w, even) | L_{R,s} (r*w, even; if staged) | t (3w) |
+// y_s (3w) | row -> segment range (w+1 ints) | gathered contributions (3 per segment).
+__device__ __forceinline__ bool fwd_supernode(const FactorDev& f, int s, const double* __restrict__ rhs, double* y,
+                                              double* sh, uint64_t* bar, unsigned phase, bool issued = false) {
   const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
   double* Dsh = sh;
   double* Lsh = sh + ((w * w + 1) & ~1);
   double* tsh = Lsh + (f.stage_l ? ((r * w + 1) & ~1) : 0);
   double* ysh = tsh + 3 * w;
-  int* psh = reinterpret_cast<int*>(ysh + 3 * w);  // row -> segment range (w+1 ints)
-  double* qsh = ysh + 3 * w + (w + 2) / 2;         // gathered contributions (3 per segment)
-  if (threadIdx.x == 0) mbar_init(&bar, 1);
-  __syncthreads();
-  stage_blocks_issue(f, s, w, r, Dsh, Lsh, &bar);
+  int* psh = reinterpret_cast<int*>(ysh + 3 * w);
+  double* qsh = ysh + 3 * w + (w + 2) / 2;
+  if (!issued) stage_blocks_issue(f, s, w, r, Dsh, Lsh, bar);
   // The descendants' contributions to this supernode's rows are one contiguous
   // range of the row-segment list (its rows are contiguous): fetch it with all
   // threads at once, then reduce each row in a fixed order.
@@ -390,7 +394,7 @@ __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, G
   for (int c = threadIdx.x; c <= w; c += blockDim.x) psh[c] = f.rseg_ptr[c0 + c] - seg0;
   for (int k = threadIdx.x; k < nseg; k += blockDim.x) {
     const double* q = f.contrib + 3 * (size_t)f.rseg_pos[seg0 + k];
-    qsh[3 * k] = q[0]; qsh[3 * k + 1] = q[1]; qsh[3 * k + 2] = q[2];
+    qsh[3 * k] = __ldcg(q); qsh[3 * k + 1] = __ldcg(q + 1); qsh[3 * k + 2] = __ldcg(q + 2);
   }
   for (int c = threadIdx.x; c < w; c += blockDim.x) {
     const int i = c0 + c;
@@ -403,7 +407,7 @@ __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, G
     tsh[3 * c] = a0; tsh[3 * c + 1] = a1; tsh[3 * c + 2] = a2;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (!stage_blocks_wait(f, &bar, s, 1)) return;  // includes the CTA barrier
+  if (!stage_blocks_wait(f, bar, phase, s, 1)) return false;  // includes the CTA barrier
   for (int c = warp; c < w; c += nw) {
     double a0 = 0, a1 = 0, a2 = 0;
     for (int k = lane; k <= c; k += 32) {
@@ -428,34 +432,31 @@ __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, G
     }
     out[3 * a] = a0; out[3 * a + 1] = a1; out[3 * a + 2] = a2;
   }
+  return true;
 }
 
-// Backward solve of one level (in place in y): for each supernode s,
+// Backward solve of supernode s (in place in y):
 //   u = y_s - L_{R,s}^T y_R  (column-major block, warp per column)
 //   y_s = Dinv_s^T u
-__global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, Gate gate, double* y) {
-  extern __shared__ __align__(16) double sh[];  // Dinv | L_{R,s} (if staged) | u (3w) | gathered ancestor rows x_R (3r)
-  __shared__ __align__(8) uint64_t bar;
-  const int s = f.lvl_sn[lvl_begin + blockIdx.x];
-  if (gate.skip(f.sn_part ? f.sn_part[s] : 0)) return;
+// Shared layout: Dinv | L_{R,s} (if staged) | u (3w) | gathered ancestor rows y_R (3r).
+__device__ __forceinline__ bool bwd_supernode(const FactorDev& f, int s, double* y, double* sh, uint64_t* bar,
+                                              unsigned phase, bool issued = false) {
   const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
   const int* R = f.rowidx + f.sn_rofs[s];
   double* Dsh = sh;
   double* Lsh = sh + ((w * w + 1) & ~1);
   double* tsh = Lsh + (f.stage_l ? ((r * w + 1) & ~1) : 0);
   double* xr = tsh + 3 * w;
-  if (threadIdx.x == 0) mbar_init(&bar, 1);
-  __syncthreads();
-  stage_blocks_issue(f, s, w, r, Dsh, Lsh, &bar);
+  if (!issued) stage_blocks_issue(f, s, w, r, Dsh, Lsh, bar);
   for (int a = threadIdx.x; a < r; a += blockDim.x) {
-    int i = R[a];
-    xr[3 * a] = y[3 * i]; xr[3 * a + 1] = y[3 * i + 1]; xr[3 * a + 2] = y[3 * i + 2];
+    const double* q = y + 3 * (size_t)R[a];
+    xr[3 * a] = __ldcg(q); xr[3 * a + 1] = __ldcg(q + 1); xr[3 * a + 2] = __ldcg(q + 2);
   }
   for (int c = threadIdx.x; c < w; c += blockDim.x) {
-    const int i = c0 + c;
-    tsh[3 * c] = y[3 * i]; tsh[3 * c + 1] = y[3 * i + 1]; tsh[3 * c + 2] = y[3 * i + 2];
+    const double* q = y + 3 * (size_t)(c0 + c);
+    tsh[3 * c] = __ldcg(q); tsh[3 * c + 1] = __ldcg(q + 1); tsh[3 * c + 2] = __ldcg(q + 2);
   }
-  if (!stage_blocks_wait(f, &bar, s, 2)) return;  // includes the CTA barrier
+  if (!stage_blocks_wait(f, bar, phase, s, 2)) return false;  // includes the CTA barrier
   const double* Lc = f.stage_l ? Lsh : f.Lcm + f.sn_lofs[s];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   // four columns per warp pass: four independent load streams per lane
@@ -491,6 +492,154 @@ __global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, G
     a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
     if (lane == 0) { y[3 * (c0 + c)] = a0; y[3 * (c0 + c) + 1] = a1; y[3 * (c0 + c) + 2] = a2; }
   }
+  return true;
+}
+
+// One level of the elimination tree per launch (one supernode per CTA; the
+// launch boundary orders the levels).
+__global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, Gate gate,
+                                                   const double* __restrict__ rhs, double* y) {
+  extern __shared__ __align__(16) double sh[];
+  __shared__ __align__(8) uint64_t bar;
+  const int s = f.lvl_sn[lvl_begin + blockIdx.x];
+  if (gate.skip(f.sn_part ? f.sn_part[s] : 0)) return;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  fwd_supernode(f, s, rhs, y, sh, &bar, 0);
+}
+
+__global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, Gate gate, double* y) {
+  extern __shared__ __align__(16) double sh[];
+  __shared__ __align__(8) uint64_t bar;
+  const int s = f.lvl_sn[lvl_begin + blockIdx.x];
+  if (gate.skip(f.sn_part ? f.sn_part[s] : 0)) return;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  bwd_supernode(f, s, y, sh, &bar, 0);
+}
+
+// Whole solve (L y = rhs, then L^T z = y, in place) in one launch.  The CTAs
+// claim work items from a ticket counter: tickets 0 .. ns-1 are the forward
+// solves of the supernodes in level order (leaves first), tickets ns .. 2ns-1
+// the backward solves in reverse level order (roots first).  A CTA starts the
+// claimed item's (read-only) block copies, then waits until the supernodes
+// the item reads are done — forward: its children in the elimination tree (a
+// child done implies its whole subtree done); backward: its parent's backward
+// solve, or its own forward solve at a root.  Every awaited item has a lower
+// ticket, so it was claimed earlier by a CTA that is running it: the waits
+// always end.  They are bounded all the same (kSpinTries polls): a CTA that
+// gives up records status 6 and raises the abort word, and every CTA then
+// stops claiming.  Completion is an epoch stamp per supernode and direction
+// (release store after the CTA's writes; acquire loads by the waiter).
+// Control words ctl: [0] ticket, [1] CTAs finished, [2] epoch (>= 1),
+// [3] abort; the last CTA to finish resets the ticket and advances the epoch
+// for the next launch.  A part of a batch whose gate is closed is skipped
+// whole (nothing outside the part depends on it).
+constexpr int kSpinTries = 1 << 22;
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Bounded wait until *flag == epoch; false on abort or when the bound is reached.
+__device__ __forceinline__ bool wait_epoch(const int* flag, int epoch, const int* abort_word) {
+  for (int i = 0; i < kSpinTries; ++i) {
+    if (ld_acquire(flag) == epoch) return true;
+    if ((i & 63) == 63) {
+      if (ld_acquire(abort_word) != 0) return false;
+      __nanosleep(64);
+    }
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, Gate gate, const double* __restrict__ rhs,
+                                                          double* y) {
+  extern __shared__ __align__(16) double sh[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int s_ticket, s_epoch, s_go;
+  const int ns = f.nsuper;
+  int* ctl = f.ctl;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    s_epoch = ld_acquire(ctl + 2);
+  }
+  __syncthreads();
+  const int epoch = s_epoch;
+  unsigned phase = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int t = atomicAdd(ctl + 0, 1);
+      s_ticket = t;
+      s_go = (t < 2 * ns && ld_acquire(ctl + 3) == 0) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_go) break;
+    const int t = s_ticket;
+    const bool fwd = t < ns;
+    const int s = fwd ? f.lvl_sn[t] : f.lvl_sn[2 * ns - 1 - t];
+    if (!gate.skip(f.sn_part ? f.sn_part[s] : 0)) {
+      // the factor blocks are read-only: start their copies before waiting on the dependencies
+      stage_blocks_issue(f, s, f.sn_w[s], f.sn_r[s], sh, sh + ((f.sn_w[s] * f.sn_w[s] + 1) & ~1), &bar);
+      if (threadIdx.x == 0) {
+        bool ok = true;
+        if (fwd) {
+          for (int k = f.kid_ptr[s]; ok && k < f.kid_ptr[s + 1]; ++k) ok = wait_epoch(f.done_f + f.kid[k], epoch, ctl + 3);
+        } else {
+          const int p = f.sn_parent[s];
+          ok = wait_epoch(p >= 0 ? f.done_b + p : f.done_f + s, epoch, ctl + 3);
+        }
+        if (!ok) {
+          if (ld_acquire(ctl + 3) == 0) record_gave_up(f, s, fwd ? 3 : 4);
+          atomicExch(ctl + 3, 1);
+        }
+        s_go = ok ? 1 : 0;
+      }
+      __syncthreads();
+      if (!s_go) {  // aborted: let this CTA's copies land before it leaves
+        mbar_wait_bounded(&bar, phase);
+        break;
+      }
+      const bool ok = fwd ? fwd_supernode(f, s, rhs, y, sh, &bar, phase, true)
+                          : bwd_supernode(f, s, y, sh, &bar, phase, true);
+      phase ^= 1u;
+      if (!ok) {
+        if (threadIdx.x == 0) atomicExch(ctl + 3, 1);
+        break;
+      }
+      __syncthreads();  // every write of the item is issued
+      if (threadIdx.x == 0) {
+        __threadfence();
+        st_release(fwd ? f.done_f + s : f.done_b + s, epoch);
+      }
+    }
+    __syncthreads();  // s_ticket / s_go are rewritten next round
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const int d = atomicAdd(ctl + 1, 1);
+    if (d == (int)gridDim.x - 1) {  // every CTA has left the claim loop
+      ctl[0] = 0;
+      ctl[1] = 0;
+      __threadfence();
+      st_release(ctl + 2, epoch + 1);
+    }
+  }
+}
+
+// Reset of the persistent solve's completion stamps and control words.
+__global__ void k_solve_reset(int ns, int* done_f, int* done_b, int* ctl) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {
+    done_f[i] = 0;
+    done_b[i] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) { ctl[0] = 0; ctl[1] = 0; ctl[2] = 1; ctl[3] = 0; }
 }
 
 // x^{k+1} = x_t + hvf; per-part convergence test for the next iteration (k read

@@ -190,6 +190,16 @@ class Scene:
         check(lib().dfem_get_contact_passes(self._h, out.ctypes.data_as(C.POINTER(C.c_int32)), int(n)))
         return out
 
+    def solve_mode(self, request: Optional[str] = None) -> dict:
+        """Form of the global solve: request None (query), "auto" (re-tune),
+        "levels" or "persistent".  Returns the form in use and the autotune's
+        ms per solve of both forms."""
+        req = {None: -1, "auto": 0, "levels": 1, "persistent": 2}[request]
+        chosen = C.c_int32()
+        ms = (C.c_double * 2)()
+        check(lib().dfem_solve_mode(self._h, req, C.byref(chosen), ms))
+        return {"mode": {1: "levels", 2: "persistent"}[chosen.value], "ms_levels": ms[0], "ms_persistent": ms[1]}
+
     def launch_count(self) -> int:
         n = C.c_int64()
         check(lib().dfem_get_launch_count(self._h, C.byref(n)))

@@ -228,6 +228,17 @@ int dfem_get_iterations(const dfem_scene *scene, int32_t *iters, int32_t n);
  * World::PreComputation + mDynamicSolver.solve (sim/fem/World.h:1089-1139,1660). */
 int dfem_host_factor_solve(const dfem_scene_desc *desc, const double *b, double *x, dfem_scene_info *info);
 
+/* The global solve's form.  request: -1 query, 0 autotune (time both forms
+ * on this scene's factor and keep the faster; done once at creation),
+ * 1 level kernels (one launch per elimination-tree level and direction),
+ * 2 persistent (both triangular sweeps in one launch, supernodes claimed in
+ * dependency order).  *chosen (may be NULL) receives the form in use (1 or 2),
+ * ms (may be NULL, 2 values) the last autotune's time per solve of each form.
+ * Both forms run the same arithmetic per supernode: results are identical.
+ * No counterpart in the reference (its solve is Eigen's SimplicialLDLT,
+ * sim/fem/World.h:1660). */
+int dfem_solve_mode(dfem_scene *scene, int32_t request, int32_t *chosen, double *ms);
+
 /* Number of kernels this scene has launched so far (CUDA-graph nodes counted
  * individually).  Instrumentation; no counterpart in the reference. */
 int dfem_get_launch_count(const dfem_scene *scene, int64_t *count);

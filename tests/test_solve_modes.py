@@ -1,0 +1,54 @@
+"""The two forms of the global solve (one launch per elimination-tree level,
+or one persistent launch whose CTAs claim supernodes in dependency order) run
+the same arithmetic per supernode, so a step, its gradient and a batch agree
+bit for bit whichever form the autotuner picked."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from diff_fem_b200 import scene as S
+from diff_fem_b200.engine import Scene
+
+pytestmark = pytest.mark.gpu
+
+
+def run(sc, d, n, mode, act=None):
+    assert sc.solve_mode(mode)["mode"] == mode
+    x = np.concatenate([q.x0.reshape(-1) for q in d]) if isinstance(d, list) else d.x0.reshape(-1)
+    xo, vo = sc.forward(x, np.zeros_like(x), n_steps=n, act=act)
+    rng = np.random.default_rng(5)
+    g = sc.backward(rng.standard_normal(x.size), rng.standard_normal(x.size))
+    return xo, vo, g, sc.iterations(n)
+
+
+@pytest.mark.parametrize("builder", ["inverse_stiffness", "muscle_beam", "cloth_sheet"])
+def test_persistent_solve_matches_level_kernels(builder):
+    d = {"inverse_stiffness": lambda: S.inverse_stiffness(nx=20, ny=6, nz=6),
+         "muscle_beam": S.muscle_beam, "cloth_sheet": lambda: S.cloth_sheet(nv=12)}[builder]()
+    sc = Scene(d)
+    info = sc.solve_mode()
+    assert info["mode"] in ("levels", "persistent") and info["ms_levels"] > 0 and info["ms_persistent"] > 0
+    act = np.random.default_rng(1).uniform(0, 1, (4, d.n_segments)) if d.n_segments else None
+    a = run(sc, d, 4, "levels", act)
+    b = run(sc, d, 4, "persistent", act)
+    for u, w in zip(a[:2], b[:2]):
+        assert np.array_equal(u, w)
+    for k in a[2]:
+        assert np.array_equal(a[2][k], b[2][k]), k
+    assert np.array_equal(a[3], b[3])
+    sc.close()
+
+
+def test_persistent_solve_in_a_batch_with_converged_parts():
+    descs = [dataclasses.replace(q, time_step=1.0 / 60.0, max_iterations=15)
+             for q in (S.inverse_stiffness(nx=10, ny=3, nz=3), S.cantilever(), S.muscle_beam())]
+    sc = Scene.batch(descs)
+    act = np.random.default_rng(2).uniform(0, 1, (3, sc.nseg))
+    a = run(sc, descs, 3, "levels", act)
+    b = run(sc, descs, 3, "persistent", act)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    for k in a[2]:
+        assert np.array_equal(a[2][k], b[2][k]), k
+    assert np.array_equal(a[3], b[3])
+    sc.close()
