@@ -85,7 +85,7 @@ struct dfem_scene {
   DBuf<int2> sv, sslot;
   DBuf<int> mseg, seg_ptr, seg_mus, boff, bv, bslot, vslot_ptr, hs_ptr, hs_col, to_user, to_internal;
   DBuf<double> hs_val;
-  DBuf<float> tinv32, twr32, twv32;  // mixed form: FP32 copies of the tet tables
+  DBuf<double> attach_k;             // per-vertex attachment stiffness (mixed form's rhs)
   // factor
   DBuf<int> rseg_ptr, rseg_pos, sn_c0, sn_w, sn_r, sn_rofs, rowidx, sn_lofs, sn_dofs, lvl_sn;
   DBuf<double> contrib, Lcm, Dinv;
@@ -152,7 +152,7 @@ static void refresh_scene_view(dfem_scene* sc) {
               sc->tslot.p, sc->mv.p, sc->minv.p, sc->mw.p, sc->mfib.p, sc->mseg.p, sc->mslot.p, sc->seg_ptr.p,
               sc->seg_mus.p, sc->sv.p, sc->srest.p, sc->ssw.p, sc->sslot.p, sc->boff.p, sc->bv.p, sc->bbeta.p,
               sc->bw.p, sc->brest.p, sc->bslot.p, sc->vslot_ptr.p, sc->attach_jd.p, sc->hs_ptr.p, sc->hs_col.p,
-              sc->hs_val.p, sc->tinv32.p, sc->twr32.p, sc->twv32.p, sc->vpart.p, sc->seg_part.p};
+              sc->hs_val.p, sc->attach_k.p, sc->vpart.p, sc->seg_part.p};
   if (std::memcmp(&sd, &sc->sd, sizeof(sd)) != 0) invalidate_graphs(sc);
   sc->sd = sd;
 }
@@ -267,10 +267,6 @@ static int upload_materials(dfem_scene* sc) {
   }
   CK(sc->twr.upload(wr));
   CK(sc->twv.upload(wv));
-  if (s.precision == DFEM_PREC_MIXED) {
-    CK(sc->twr32.upload(std::vector<float>(wr.begin(), wr.end())));
-    CK(sc->twv32.upload(std::vector<float>(wv.begin(), wv.end())));
-  }
   CK(sc->tE.upload(s.tE));
   CK(sc->tnu.upload(s.tnu));
   std::vector<int> hp(s.Hs.ptr.begin(), s.Hs.ptr.end());
@@ -293,10 +289,6 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->mass.upload(s.mass));
   CK(sc->gmask.upload(s.gmask));
   CK(sc->tinv.upload(planes(s.tinv, s.T, 9)));
-  if (s.precision == DFEM_PREC_MIXED) {
-    std::vector<double> tp = planes(s.tinv, s.T, 9);
-    CK(sc->tinv32.upload(std::vector<float>(tp.begin(), tp.end())));
-  }
   CK(sc->tvol.upload(s.tvol));
   std::vector<int4> tv(s.T), tsl(s.T);
   for (int e = 0; e < s.T; ++e) {
@@ -340,6 +332,9 @@ static int upload_scene(dfem_scene* sc) {
   for (int a = 0; a < s.A; ++a)
     for (int c = 0; c < 3; ++c) ajd[3 * (size_t)s.av[a] + c] += s.ak[a] * s.ap[3 * a + c];
   CK(sc->attach_jd.upload(ajd));
+  std::vector<double> ak(s.N, 0.0);
+  for (int a = 0; a < s.A; ++a) ak[s.av[a]] += s.ak[a];
+  CK(sc->attach_k.upload(ak));
   CK(sc->to_user.upload(s.to_user));
   CK(sc->to_internal.upload(s.to_internal));
   int rc = upload_materials(sc);
@@ -481,28 +476,32 @@ static Gate adj_gate(const dfem_scene* sc) {
   return g;
 }
 
-// The local step and its gather in the scene's precision form. The mixed form
-// writes FP32 slots into the same buffer (half of it) and accumulates them in
-// FP32; the contact phase always runs the FP64 form.
+// The local step and its gather in the scene's precision form.  The plain
+// form writes J d slots and forms c0 + sum (the reference's delta form); the
+// mixed form writes FP32 force slots (J d - L x) and forms the iterate-relative
+// rhs (k_gather_force).  Both use the same slot buffer (the mixed form half of
+// it).  The contact phase and dfem_eval_local always use the plain kernels.
 static bool mixed(const dfem_scene* sc) { return sc->hs.precision == DFEM_PREC_MIXED; }
 static float* slot32(dfem_scene* sc) { return reinterpret_cast<float*>(sc->slot.p); }
 
-static void launch_local(dfem_scene* sc, cudaStream_t st, Gate g, const double* x, const double* act, const int* step) {
+static void launch_local(dfem_scene* sc, cudaStream_t st, Gate g, const double* x, const double* act, const int* step,
+                         bool plain = false) {
   const HostScene& s = sc->hs;
   const int ncons = s.T + s.M + s.S + s.B;
   if (ncons == 0) return;
-  if (mixed(sc))
-    k_local_f32<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, g, x, act, step, slot32(sc));
+  if (mixed(sc) && !plain)
+    k_force_f32<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, g, x, act, step, slot32(sc));
   else
     k_local<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, g, x, act, step, sc->slot.p);
 }
 
-static void launch_gather(dfem_scene* sc, cudaStream_t st, Gate g, const double* c0, double* rhs) {
-  const int N = sc->hs.N;
-  if (mixed(sc))
-    k_gather_f32<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vpart.p, sc->vslot_ptr.p, slot32(sc), c0, rhs);
+// rhs of one PD iteration at the iterate x (mixed: also reads q_n and x)
+static void launch_gather(dfem_scene* sc, cudaStream_t st, Gate g, const double* c0, double* rhs, const double* x,
+                          bool plain = false) {
+  if (mixed(sc) && !plain)
+    k_gather_force<<<sc->nblk_v, 128, 0, st>>>(sc->sd, g, slot32(sc), sc->qn.p, x, rhs);
   else
-    k_gather<<<sc->nblk_v, 128, 0, st>>>(N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
+    k_gather<<<sc->nblk_v, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
 }
 
 // The adjoint of the local step runs in FP64 in both forms: its parameter
@@ -552,9 +551,9 @@ static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandl
   const HostScene& s = sc->hs;
   const Gate g = fwd_gate(sc);
   launch_local(sc, st, g, sc->xk.p, sc->act_all.p, sc->step.p);
-  launch_gather(sc, st, g, sc->c0.p, sc->rhs.p);
+  launch_gather(sc, st, g, sc->c0.p, sc->rhs.p, sc->xk.p);
   enqueue_solve(sc, st, g, sc->rhs.p, sc->y.p);
-  k_update<<<sc->nblk_p, kPartBlock, 0, st>>>(s.N, sc->pd, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->step.p,
+  k_update<<<sc->nblk_p, kPartBlock, 0, st>>>(s.N, sc->pd, mixed(sc) ? 1 : 0, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->step.p,
                                sc->flag.p, sc->iters.p, sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
   k_loop_ctl<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, s.nparts, s.K, h);
 }
@@ -1001,9 +1000,9 @@ int dfem_eval_local(dfem_scene* sc, const double* x, double* jd_out, int mem) {
   RC(copy_in(sc, x, n3, sc->io_a.p, mem));
   k_to_internal<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_internal.p, sc->io_a.p, sc->rhs.p);
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->zero.p, 0);
-  launch_local(sc, sc->stream, open, sc->rhs.p, sc->act_cur.p, sc->zero.p);
+  launch_local(sc, sc->stream, open, sc->rhs.p, sc->act_cur.p, sc->zero.p, true);
   // J d = attachment term + the constraints' slots (c0 := J_att d_att)
-  launch_gather(sc, sc->stream, open, sc->attach_jd.p, sc->io_b.p);
+  launch_gather(sc, sc->stream, open, sc->attach_jd.p, sc->io_b.p, nullptr, true);
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_b.p, sc->io_a.p);
   CK(cudaGetLastError());
   sc->launches += 5;
@@ -1101,7 +1100,7 @@ int dfem_profile_phases(dfem_scene* sc, int32_t reps, double* ms) {
   };
   int rc = DFEM_OK;
   if (!rc && ncons > 0) rc = timed(0, [&] { launch_local(sc, sc->stream, gf, sc->xk.p, sc->act_all.p, sc->step.p); });
-  if (!rc) rc = timed(1, [&] { launch_gather(sc, sc->stream, gf, sc->c0.p, sc->rhs.p); });
+  if (!rc) rc = timed(1, [&] { launch_gather(sc, sc->stream, gf, sc->c0.p, sc->rhs.p, sc->xk.p); });
   if (!rc) rc = timed(2, [&] { enqueue_solve(sc, sc->stream, gf, sc->rhs.p, sc->y.p); });
   if (!rc && ncons > 0) rc = timed(3, [&] { launch_adj_local(sc, sc->stream, ga, sc->zero.p); });
   cudaEventDestroy(e0);

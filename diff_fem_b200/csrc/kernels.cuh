@@ -96,10 +96,8 @@ struct SceneDev {
   const int* hs_ptr;
   const int* hs_col;
   const double* hs_val;
-  // mixed form: FP32 copies of the tet tables (null in the plain form)
-  const float* tinv32;
-  const float* twr32;
-  const float* twv32;
+  // per-vertex sum of attachment stiffnesses (the attachments' diagonal of Hs)
+  const double* attach_k;
   // batch: part of every vertex and muscle segment (null for a single scene)
   const int* vpart;
   const int* seg_part;

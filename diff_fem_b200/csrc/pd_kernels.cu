@@ -212,19 +212,18 @@ __device__ __forceinline__ Vec3<double> to_d(Vec3<float> a) { return mk3((double
 __device__ __forceinline__ void st3f(float* p, int i, Vec3<float> v) { p[3 * i] = v.x; p[3 * i + 1] = v.y; p[3 * i + 2] = v.z; }
 __device__ __forceinline__ Vec3<float> ld3f(const float* p, int i) { return mk3(p[3 * i], p[3 * i + 1], p[3 * i + 2]); }
 
-// F(:,j) = sum_k invDm[k][j] (x_{k+1} - x_0) from FP32 invDm planes and FP64 edges
-__device__ __forceinline__ void tet_f32(const float* inv, int n, int e, const Vec3<double> xv[4], float G[4][3],
-                                        Mat3<float>& F) {
-  Vec3<float> ds[3] = {to_f(xv[1] - xv[0]), to_f(xv[2] - xv[0]), to_f(xv[3] - xv[0])};
-#pragma unroll
-  for (int j = 0; j < 3; ++j) {
-    float a = inv[(0 * 3 + j) * n + e], b = inv[(1 * 3 + j) * n + e], c = inv[(2 * 3 + j) * n + e];
-    G[1][j] = a; G[2][j] = b; G[3][j] = c; G[0][j] = -(a + b + c);
-    F.c[j] = a * ds[0] + b * ds[1] + c * ds[2];
-  }
-}
+// ------------------------------------------------------------ mixed form ----
+//
+// The mixed form writes, per constraint, its force f_c = J_c d_c - L_c x (the
+// part of the rhs that varies with the iterate; strain-sized) as FP32 slots,
+// and iterates x^{k+1} = x^k + Hs^-1 r with
+//   r = M/h^2 (q_n - x^k) + sum_att k (p - x^k) + sum_c f_c,
+// which is the reference's map b + J d(x^k) - Hs x rearranged (Hs = M/h^2 +
+// sum_c L_c).  FP32 rounding is then relative to the forces, not to J d ~ L x.
+// Inputs of cancelling differences (F, spring lengths, Laplacians) are formed
+// in FP64 first.
 
-__global__ void __launch_bounds__(128) k_local_f32(SceneDev d, Gate gate, const double* __restrict__ x,
+__global__ void __launch_bounds__(128) k_force_f32(SceneDev d, Gate gate, const double* __restrict__ x,
                                                    const double* __restrict__ act_all, const int* step,
                                                    float* __restrict__ slot) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -232,90 +231,82 @@ __global__ void __launch_bounds__(128) k_local_f32(SceneDev d, Gate gate, const 
   if (t < d.T) {
     int4 v = d.tv[t];
     Vec3<double> xv[4] = {ld3(x, v.x), ld3(x, v.y), ld3(x, v.z), ld3(x, v.w)};
-    float G[4][3];
-    Mat3<float> F, md, mdv;
-    tet_f32(d.tinv32, d.T, t, xv, G, F);
-    float ratio;
-    corot_project(F, md, mdv, &ratio);
+    double G[4][3];
+    load_g(d.tinv, d.T, t, G);
+    const Mat3<double> F = deformation(G, xv);
+    const double wr = d.twr[t], wv = d.twv[t];
     Vec3<float> P[3];
-    if (ratio >= kDegenerateRatio) {
-      float wr = d.twr32[t], wv = d.twv32[t];
+    if (!corot_force_mixed(F, (float)wr, (float)wv, P)) {  // inverted or near-degenerate: FP64
+      Mat3<double> md, mdv;
+      corot_project(F, md, mdv);
 #pragma unroll
-      for (int j = 0; j < 3; ++j) P[j] = wr * md.c[j] + wv * mdv.c[j];
-    } else {  // near-degenerate element: FP64
-      double Gd[4][3];
-      load_g(d.tinv, d.T, t, Gd);
-      Mat3<double> Fd = deformation(Gd, xv), mdd, mdvd;
-      corot_project(Fd, mdd, mdvd);
-      double wr = d.twr[t], wv = d.twv[t];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) P[j] = to_f(wr * mdd.c[j] + wv * mdvd.c[j]);
+      for (int j = 0; j < 3; ++j) P[j] = to_f(wr * (md.c[j] - F.c[j]) + wv * (mdv.c[j] - F.c[j]));
     }
     int4 sl = d.tslot[t];
     const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
 #pragma unroll
-    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], G[a][0] * P[0] + G[a][1] * P[1] + G[a][2] * P[2]);
+    for (int a = 0; a < 4; ++a)
+      st3f(slot, sv[a], (float)G[a][0] * P[0] + (float)G[a][1] * P[1] + (float)G[a][2] * P[2]);
     return;
   }
   t -= d.T;
-  if (t < d.M) {
+  if (t < d.M) {  // -a w c_a (F f): J d - L x of the muscle constraint
     int4 v = d.mv[t];
-    Vec3<double> x0 = ld3(x, v.x);
-    Vec3<float> ds[3] = {to_f(ld3(x, v.y) - x0), to_f(ld3(x, v.z) - x0), to_f(ld3(x, v.w) - x0)};
-    Vec3<float> f = mk3((float)d.mfib[t], (float)d.mfib[d.M + t], (float)d.mfib[2 * d.M + t]);
-    float c[4] = {0, 0, 0, 0};
-    Vec3<float> Ff = mk3(0.0f, 0.0f, 0.0f);
+    const Vec3<double> x0 = ld3(x, v.x);
+    const Vec3<double> ds[3] = {ld3(x, v.y) - x0, ld3(x, v.z) - x0, ld3(x, v.w) - x0};
+    const Vec3<double> f = mk3(d.mfib[t], d.mfib[d.M + t], d.mfib[2 * d.M + t]);
+    double c[4] = {0, 0, 0, 0};
+    Vec3<double> Ff = mk3(0.0, 0.0, 0.0);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-      float ck = (float)d.minv[(k * 3 + 0) * d.M + t] * f.x + (float)d.minv[(k * 3 + 1) * d.M + t] * f.y +
-                 (float)d.minv[(k * 3 + 2) * d.M + t] * f.z;
+      double ck = d.minv[(k * 3 + 0) * d.M + t] * f.x + d.minv[(k * 3 + 1) * d.M + t] * f.y +
+                  d.minv[(k * 3 + 2) * d.M + t] * f.z;
       c[k + 1] = ck;
       c[0] -= ck;
       Ff = Ff + ck * ds[k];
     }
-    float a_act = (float)act_all[(size_t)(*step) * d.nseg + d.mseg[t]];
-    Vec3<float> p0 = (1.0f - a_act) * Ff;
-    float w = (float)d.mw[t];
+    const double a_act = act_all[(size_t)(*step) * d.nseg + d.mseg[t]];
+    const Vec3<float> p = to_f((-a_act * d.mw[t]) * Ff);
     int4 sl = d.mslot[t];
     const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
 #pragma unroll
-    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], (w * c[a]) * p0);
+    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], (float)c[a] * p);
     return;
   }
   t -= d.M;
-  if (t < d.S) {
+  if (t < d.S) {  // sqrt(w) e (rest/|e| - 1)
     int2 v = d.sv[t];
-    Vec3<float> e = to_f(ld3(x, v.x) - ld3(x, v.y));
-    Vec3<float> dd = ((float)d.srest[t] * rsqrtf(dot3(e, e))) * e;
-    float w = (float)d.ssw[t];
+    const Vec3<double> e = ld3(x, v.x) - ld3(x, v.y);
+    const double len = sqrt(dot3(e, e));
+    const Vec3<float> fs = to_f((d.ssw[t] * (d.srest[t] / len - 1.0)) * e);
     int2 sl = d.sslot[t];
-    st3f(slot, sl.x, w * dd);
-    st3f(slot, sl.y, (-w) * dd);
+    st3f(slot, sl.x, fs);
+    st3f(slot, sl.y, (-1.0f) * fs);
     return;
   }
   t -= d.S;
-  if (t < d.B) {
+  if (t < d.B) {  // w^2 beta_q (rest/|lap| - w) lap
     int o0 = d.boff[t], o1 = d.boff[t + 1];
-    Vec3<double> xc = ld3(x, d.bv[o0]);
-    Vec3<float> lap = mk3(0.0f, 0.0f, 0.0f);
-    for (int k = o0; k < o1; ++k) lap = lap + (float)d.bbeta[k] * to_f(ld3(x, d.bv[k]) - xc);  // sum beta = 0
-    float ln = sqrtf(dot3(lap, lap));
-    float w = (float)d.bw[t];
-    Vec3<float> dd = mk3(0.0f, 0.0f, 0.0f);
-    if (ln > 1e-25f) dd = (w * (float)d.brest[t] / ln) * lap;
-    for (int k = o0; k < o1; ++k) st3f(slot, d.bslot[k], (w * (float)d.bbeta[k]) * dd);
+    const Vec3<double> xc = ld3(x, d.bv[o0]);
+    Vec3<double> lap = mk3(0.0, 0.0, 0.0);
+    for (int k = o0 + 1; k < o1; ++k) lap = lap + d.bbeta[k] * (ld3(x, d.bv[k]) - xc);  // sum beta = 0
+    const double ln = sqrt(dot3(lap, lap)), w = d.bw[t];
+    const double sc = w * w * ((ln > 1e-25 ? d.brest[t] / ln : 0.0) - w);
+    const Vec3<float> fl = to_f(sc * lap);
+    for (int k = o0; k < o1; ++k) st3f(slot, d.bslot[k], (float)d.bbeta[k] * fl);
   }
 }
 
-// rhs_i = c0_i (FP64) + the FP32 sum of vertex i's slots
-__global__ void k_gather_f32(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
-                             const float* __restrict__ slot,
-                             const double* __restrict__ c0, double* __restrict__ rhs) {
+// r_i = m_i/h^2 (q_i - x_i) + attach_jd_i - attach_k_i x_i + the FP32 sum of vertex i's force slots
+__global__ void k_gather_force(SceneDev d, Gate gate, const float* __restrict__ slot, const double* __restrict__ qn,
+                               const double* __restrict__ x, double* __restrict__ rhs) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
+  if (i >= d.N || gate.skip(vpart_of(d, i))) return;
   Vec3<float> acc = mk3(0.0f, 0.0f, 0.0f);
-  for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3f(slot, k);
-  st3(rhs, i, ld3(c0, i) + to_d(acc));
+  for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) acc = acc + ld3f(slot, k);
+  const Vec3<double> xi = ld3(x, i);
+  const double m = d.mass[i] / (d.h * d.h);
+  st3(rhs, i, m * (ld3(qn, i) - xi) + ld3(d.attach_jd, i) - d.attach_k[i] * xi + to_d(acc));
 }
 
 // rhs_i = c0_i + sum of the slots of vertex i
@@ -642,10 +633,10 @@ __global__ void k_solve_reset(int ns, int* done_f, int* done_b, int* ctl) {
   if (blockIdx.x == 0 && threadIdx.x == 0) { ctl[0] = 0; ctl[1] = 0; ctl[2] = 1; ctl[3] = 0; }
 }
 
-// x^{k+1} = x_t + hvf; per-part convergence test for the next iteration (k read
-// from device memory).  Part-aligned blocks; a converged part's blocks do nothing.
-__global__ void k_update(int N, PartDev pd, const int* kptr, const double* __restrict__ xt, const double* __restrict__ z,
-                         double* xk, double* hist, const int* step, int* flag, int* iters,
+// x^{k+1}; per-part convergence test for the next iteration (k read from
+// device memory).  Part-aligned blocks; a converged part's blocks do nothing.
+__global__ void k_update(int N, PartDev pd, int from_iterate, const int* kptr, const double* __restrict__ xt,
+                         const double* __restrict__ z, double* xk, double* hist, const int* step, int* flag, int* iters,
                          double* partial, unsigned* counter, double* errv, int* status) {
   const int b = blockIdx.x, p = pd.blk_part[b];
   if (flag[p]) return;
@@ -654,7 +645,8 @@ __global__ void k_update(int N, PartDev pd, const int* kptr, const double* __res
   const int i = pd.blk_v0[b] + threadIdx.x;
   double e2 = 0;
   if (i < pv1) {
-    Vec3<double> xn = ld3(xt, i) + ld3(z, i);
+    // plain form: x^{k+1} = x_t + hvf (reference delta form); mixed form: x^{k+1} = x^k + z
+    Vec3<double> xn = (from_iterate ? ld3(xk, i) : ld3(xt, i)) + ld3(z, i);
     Vec3<double> dlt = xn - ld3(xk, i);
     e2 = dot3(dlt, dlt);
     st3(xk, i, xn);

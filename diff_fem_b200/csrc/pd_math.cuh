@@ -188,6 +188,127 @@ __device__ __forceinline__ void corot_project(const Mat3<T>& F, Mat3<T>& md, Mat
 // has a badly conditioned U/V in FP32 and is recomputed in FP64.
 constexpr float kDegenerateRatio = 0.05f;
 
+// Unit quaternion (w, x, y, z) of a nearly orthogonal matrix with det > 0
+// (Shepperd's method: the branch on the largest of trace and diagonal keeps
+// the square root away from cancellation).
+__device__ __forceinline__ void quat_from_rot(const Mat3<float>& R, float q[4]) {
+  const float m00 = R.c[0].x, m11 = R.c[1].y, m22 = R.c[2].z;
+  const float m01 = R.c[1].x, m10 = R.c[0].y, m02 = R.c[2].x, m20 = R.c[0].z, m12 = R.c[2].y, m21 = R.c[1].z;
+  const float tr = m00 + m11 + m22;
+  if (tr > 0.0f) {
+    const float S = 2.0f * sqrtf(tr + 1.0f);
+    q[0] = 0.25f * S; q[1] = (m21 - m12) / S; q[2] = (m02 - m20) / S; q[3] = (m10 - m01) / S;
+  } else if (m00 > m11 && m00 > m22) {
+    const float S = 2.0f * sqrtf(fmaxf(1.0f + m00 - m11 - m22, 1e-30f));
+    q[0] = (m21 - m12) / S; q[1] = 0.25f * S; q[2] = (m01 + m10) / S; q[3] = (m02 + m20) / S;
+  } else if (m11 > m22) {
+    const float S = 2.0f * sqrtf(fmaxf(1.0f + m11 - m00 - m22, 1e-30f));
+    q[0] = (m02 - m20) / S; q[1] = (m01 + m10) / S; q[2] = 0.25f * S; q[3] = (m12 + m21) / S;
+  } else {
+    const float S = 2.0f * sqrtf(fmaxf(1.0f + m22 - m00 - m11, 1e-30f));
+    q[0] = (m10 - m01) / S; q[1] = (m02 + m20) / S; q[2] = (m12 + m21) / S; q[3] = 0.25f * S;
+  }
+}
+
+// The rotation of quaternion q, normalised and evaluated in FP64: orthogonal
+// to FP64 round-off whatever the FP32 rounding of q.
+__device__ __forceinline__ Mat3<double> rot_from_quat(const float qf[4]) {
+  double w = qf[0], x = qf[1], y = qf[2], z = qf[3];
+  const double n = rsqrt(w * w + x * x + y * y + z * z);
+  w *= n; x *= n; y *= n; z *= n;
+  Mat3<double> R;
+  R.c[0] = mk3(1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y + w * z), 2.0 * (x * z - w * y));
+  R.c[1] = mk3(2.0 * (x * y - w * z), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z + w * x));
+  R.c[2] = mk3(2.0 * (x * z + w * y), 2.0 * (y * z - w * x), 1.0 - 2.0 * (x * x + y * y));
+  return R;
+}
+
+// Mixed-form corotated force P = wr (md - F) + wv (md_volume - F) (columns),
+// the tet's J d - L x up to the G factor, with FP32 rounding relative to the
+// strain rather than to F:
+//   1. FP32 SVD of F -> R0 = U V^T, its quaternion, and R = R(q) exactly
+//      orthogonal in FP64;
+//   2. A = R^T F in FP64, H = A - I rounded to FP32 (strain-sized; its skew
+//      part is only R0's rounding);
+//   3. polar of A = (I + Omega) S_A to first order in the tiny skew part, in
+//      the V basis: Omega_kl = 2 (V^T skew(H) V)_kl / (s_k + s_l);
+//   4. md - F = R (Omega - H);  the volume projection's 5 Newton steps run on
+//      e_k = v_k^T sym(H) v_k (= s_k - 1 to second order) with
+//      prod(1 + a) - 1 expanded, and md_volume - F = R V diag(D) V^T.
+// Returns false (caller takes the FP64 branch) for inverted or
+// near-degenerate elements.
+__device__ __forceinline__ bool corot_force_mixed(const Mat3<double>& F, float wr, float wv, Vec3<float> P[3]) {
+  Mat3<float> Ff;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) Ff.c[j] = mk3((float)F.c[j].x, (float)F.c[j].y, (float)F.c[j].z);
+  const Svd3<float> sv = svd3(Ff);
+  const float smax = fmaxf(sv.s[0], fmaxf(sv.s[1], sv.s[2]));
+  const float smin = fminf(sv.s[0], fminf(sv.s[1], sv.s[2]));
+  if (!(smax > 0.0f) || !(smin >= kDegenerateRatio * smax) || !(det3(F) > 0.0)) return false;
+  const float vj[3][3] = {{sv.v[0].x, sv.v[1].x, sv.v[2].x}, {sv.v[0].y, sv.v[1].y, sv.v[2].y}, {sv.v[0].z, sv.v[1].z, sv.v[2].z}};
+  Mat3<float> R0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) R0.c[j] = vj[j][0] * sv.u[0] + vj[j][1] * sv.u[1] + vj[j][2] * sv.u[2];
+  float q[4];
+  quat_from_rot(R0, q);
+  const Mat3<double> R = rot_from_quat(q);
+  float H[3][3];  // H[i][j] = (R^T F - I)_ij
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) H[i][j] = (float)(dot3(R.c[i], F.c[j]) - (i == j ? 1.0 : 0.0));
+  Vec3<float> Hvl[3], HTvl[3];  // H v_l and H^T v_l
+#pragma unroll
+  for (int l = 0; l < 3; ++l) {
+    const Vec3<float> v = sv.v[l];
+    Hvl[l] = mk3(H[0][0] * v.x + H[0][1] * v.y + H[0][2] * v.z, H[1][0] * v.x + H[1][1] * v.y + H[1][2] * v.z,
+                 H[2][0] * v.x + H[2][1] * v.y + H[2][2] * v.z);
+    HTvl[l] = mk3(H[0][0] * v.x + H[1][0] * v.y + H[2][0] * v.z, H[0][1] * v.x + H[1][1] * v.y + H[2][1] * v.z,
+                  H[0][2] * v.x + H[1][2] * v.y + H[2][2] * v.z);
+  }
+  float e[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) e[k] = dot3(sv.v[k], Hvl[k]);  // v^T H v = v^T sym(H) v
+  // Omega in the V basis (pairs 01, 02, 12); Omega = sum_{k<l} om_kl (v_k v_l^T - v_l v_k^T)
+  const int pk[3] = {0, 0, 1}, pl[3] = {1, 2, 2};
+  float om[3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p) {
+    const int k = pk[p], l = pl[p];
+    const float kskew = 0.5f * (dot3(sv.v[k], Hvl[l]) - dot3(sv.v[k], HTvl[l]));  // v_k^T skew(H) v_l
+    om[p] = 2.0f * kskew / (sv.s[k] + sv.s[l]);
+  }
+  // volume projection on the small quantities (same iterates as on s + D)
+  float D[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int it = 0; it < 5; ++it) {
+    const float a0 = e[0] + D[0], a1 = e[1] + D[1], a2 = e[2] + D[2];
+    const float C = (a0 + a1 + a2) + (a0 * a1 + a0 * a2 + a1 * a2) + a0 * a1 * a2;
+    const float g0 = 1.0f + a1 + a2 + a1 * a2, g1 = 1.0f + a0 + a2 + a0 * a2, g2 = 1.0f + a0 + a1 + a0 * a1;
+    const float c = (g0 * D[0] + g1 * D[1] + g2 * D[2] - C) / (g0 * g0 + g1 * g1 + g2 * g2);
+    D[0] = c * g0; D[1] = c * g1; D[2] = c * g2;
+  }
+  // B = wr (Omega - H) + wv V diag(D) V^T, then P = R B (R rounded to FP32: relative error on a small product)
+  Mat3<float> B;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    Vec3<float> col = mk3(-H[0][j], -H[1][j], -H[2][j]);
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      const int k = pk[p], l = pl[p];
+      col = col + (om[p] * vj[j][l]) * sv.v[k] - (om[p] * vj[j][k]) * sv.v[l];
+    }
+    Vec3<float> vol = (D[0] * vj[j][0]) * sv.v[0] + (D[1] * vj[j][1]) * sv.v[1] + (D[2] * vj[j][2]) * sv.v[2];
+    B.c[j] = wr * col + wv * vol;
+  }
+  Mat3<float> Rf;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) Rf.c[j] = mk3((float)R.c[j].x, (float)R.c[j].y, (float)R.c[j].z);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) P[j] = B.c[j].x * Rf.c[0] + B.c[j].y * Rf.c[1] + B.c[j].z * Rf.c[2];
+  return true;
+}
+
 // VJP of (md, md_volume) with respect to F.  gmd, gmdv: cotangents (3x3).
 //   P_bar_ij (i != j) = a_ij sym(M_G)_ij + b_ij asym(M_G)_ij + (M_R_ij - M_R_ji)/(s_i + s_j)
 //   P_bar_ii = sum_k (M_G)_kk dg_k/ds_i
