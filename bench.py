@@ -284,8 +284,15 @@ def run_ours(args):
     else:
         achieved = local_bytes / (ph[dom] * 1e-3) / 1e9
         traffic_note = f"per {dom} launch"
+    # DRAM bytes per launch of the persistent solve on this workload, from one ncu capture
+    # (dram__bytes.sum.per_second x gpu__time_duration: 21.04 GB/s x 158.0 us; the factor is
+    # mostly L2-resident, so DRAM traffic is below the algorithmic bytes)
+    solve_info = sc.solve_mode()
+    traffic = 3.32e6 if (dom == "solve" and solve_info["mode"] == "persistent" and SIM_STEPS == 60) else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "peak_source": peak_note,
+                "frac": achieved / hbm, "traffic": traffic,
+                "traffic_source": "ncu capture of k_solve_persistent (profiles/k_solve_persistent_inverse_stiffness_12800tets.md)"
+                if traffic else None, "peak_source": peak_note,
                 "algorithmic_bytes": solve_bytes if dom == "solve" else local_bytes, "per": traffic_note,
                 "phase_ms": ph, "phase_share_ms_per_bench_step": share}
 
@@ -294,7 +301,8 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": dict(workload_config(args.precision), l2="flushed between timed steps (256 MB write)",
-                           factor={"supernodes": info["n_supernodes"], "levels": info["n_levels"], "nnz": nnz}),
+                           factor={"supernodes": info["n_supernodes"], "levels": info["n_levels"], "nnz": nnz},
+                           solve=sc.solve_mode()),
             "forward_only_steps_per_s": world * fwd_rate, "pd_iterations_total": n_it,
             "e2e": e2e, "roofline": roofline, "gpu_launches": launches, "clocks": clk.summary()}
     if rank == 0 and world == 1:
@@ -412,6 +420,10 @@ def run_batch(args):
            "h2d_bytes_per_step": 8 * (2 * N3 + n * nseg + 2 * N3),
            "d2h_bytes_per_step": 8 * (2 * N3 + 2 * N3 + 2 * T + n * nseg)}
 
+    binfo = b.info()
+    b.forward(x0, v0, n_steps=1, act=act[:1].contiguous())
+    phases = b.profile_phases(reps=20)
+
     # per-scene error of this run against the FP64 batch (same scenes, same inputs)
     errs = None
     if prec == DFEM_PREC_MIXED:
@@ -488,6 +500,9 @@ def run_batch(args):
             "config": dict(batch_config(args, descs), l2="flushed between timed steps (256 MB write)",
                            setup_s=t_setup),
             "forward_only_scene_steps_per_s": world * fwd_rate, "pd_iterations_total": int(iters.max(axis=1).sum()),
+            "solve": b.solve_mode(), "phase_ms": phases, "factor": {"supernodes": binfo["n_supernodes"],
+                                                                   "levels": binfo["n_levels"],
+                                                                   "nnz": int(binfo["nnz_factor"])},
             "e2e": e2e, "error_vs_fp64": errs, "plain_fp64_one_at_a_time": plain,
             "gpu_launches": launches, "clocks": clk.summary()}
     if rank == 0:

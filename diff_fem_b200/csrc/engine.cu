@@ -18,6 +18,7 @@
 #include "../../include/dfem.h"
 #include "pd_kernels.cu"
 #include "contact_kernels.cuh"
+#include "factor_kernels.cuh"
 #include "scene.h"
 
 namespace dfem {
@@ -98,6 +99,12 @@ struct dfem_scene {
   int pers_grid = 1;
   int solve_mode = 0;                    // 0: level kernels, 1: persistent
   double solve_ms[2] = {0.0, 0.0};       // autotune timings (ms per solve) of the two modes
+  // numeric refactorisation on the GPU (material changes)
+  DBuf<double> hs_base, hc_coef, Ldw, part_reg, E_in, nu_in;
+  DBuf<int> hc_ptr, hc_tet, up_ptr, up_d, up_a0, up_a1, part_fail;
+  std::vector<double> part_reg_h;
+  size_t shm_fact = 0;
+  RefactorDev rd{};
   // batch layout (a single scene is one part)
   std::vector<HostScene> parts;          // the parts of a batch (empty for a single scene)
   DBuf<int> vpart, seg_part, sn_part, part_v0, part_b0, blk_part, blk_v0;
@@ -138,6 +145,19 @@ struct dfem_scene {
 };
 
 namespace dfem {
+
+// Run f(0) .. f(n-1) on up to hardware_concurrency host threads.
+template <typename Fn>
+static void parallel_for(int n, Fn f) {
+  const int nt = std::max(1, std::min(n, (int)std::thread::hardware_concurrency()));
+  std::atomic<int> next{0};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&] {
+      for (int i = next++; i < n; i = next++) f(i);
+    });
+  for (auto& th : pool) th.join();
+}
 
 // Captured graphs bake in device pointers; any change of them invalidates the graphs.
 static void invalidate_graphs(dfem_scene* sc) {
@@ -282,6 +302,118 @@ static std::vector<T> planes(const std::vector<T>& aos, int n, int k) {  // AoS 
   for (int e = 0; e < n; ++e)
     for (int q = 0; q < k; ++q) out[(size_t)q * n + e] = aos[(size_t)e * k + q];
   return out;
+}
+
+// Structure of the GPU refactorisation: Hs split into its E-independent base
+// and per-entry tet contributions (per part in parallel for a batch), and the
+// left-looking update lists of every supernode (descendant d, rows R_d[a0..a1)
+// inside the supernode's columns), in increasing d.
+static int upload_refactor_plan(dfem_scene* sc) {
+  HostScene& s = sc->hs;
+  std::vector<double> base, coef;
+  std::vector<int> cptr, ctet;
+  if (sc->parts.empty()) {
+    hs_split(s, base, cptr, ctet, coef);
+  } else {
+    const int np = (int)sc->parts.size();
+    std::vector<std::vector<double>> pb(np), pc(np);
+    std::vector<std::vector<int>> pp(np), pt(np);
+    parallel_for(np, [&](int p) { hs_split(sc->parts[p], pb[p], pp[p], pt[p], pc[p]); });
+    cptr = {0};
+    for (int p = 0; p < np; ++p) {
+      const int off = cptr.back(), t0 = s.part_t0[p];
+      base.insert(base.end(), pb[p].begin(), pb[p].end());
+      coef.insert(coef.end(), pc[p].begin(), pc[p].end());
+      for (size_t k = 1; k < pp[p].size(); ++k) cptr.push_back(pp[p][k] + off);
+      for (int t : pt[p]) ctet.push_back(t + t0);
+    }
+  }
+  if (base.size() != s.Hs.val.size()) return fail(DFEM_ERR_INVALID, "refactorisation plan: Hs pattern mismatch");
+  CK(sc->hs_base.upload(base));
+  CK(sc->hc_ptr.upload(cptr));
+  CK(sc->hc_tet.upload(ctet.empty() ? std::vector<int>{0} : ctet));
+  CK(sc->hc_coef.upload(coef.empty() ? std::vector<double>{0.0} : coef));
+  const SupernodalFactor& F = s.F;
+  std::vector<std::vector<int>> ud(F.nsuper), ua0(F.nsuper), ua1(F.nsuper);
+  for (int d = 0; d < F.nsuper; ++d) {
+    const int r = F.sn_r[d];
+    const int* R = &F.rowidx[F.sn_rofs[d]];
+    int b0 = 0;
+    while (b0 < r) {
+      const int p = F.col_sn[R[b0]];
+      int b1 = b0;
+      while (b1 < r && F.col_sn[R[b1]] == p) ++b1;
+      ud[p].push_back(d); ua0[p].push_back(b0); ua1[p].push_back(b1);
+      b0 = b1;
+    }
+  }
+  std::vector<int> uptr(F.nsuper + 1, 0), vd, va0, va1;
+  for (int q = 0; q < F.nsuper; ++q) {
+    vd.insert(vd.end(), ud[q].begin(), ud[q].end());
+    va0.insert(va0.end(), ua0[q].begin(), ua0[q].end());
+    va1.insert(va1.end(), ua1[q].begin(), ua1[q].end());
+    uptr[q + 1] = (int)vd.size();
+  }
+  if (vd.empty()) { vd = {0}; va0 = {0}; va1 = {0}; }
+  CK(sc->up_ptr.upload(uptr));
+  CK(sc->up_d.upload(vd));
+  CK(sc->up_a0.upload(va0));
+  CK(sc->up_a1.upload(va1));
+  CK(sc->Ldw.alloc(std::max<size_t>(1, F.Dinv.size())));
+  const int np = s.nparts;
+  sc->part_reg_h.assign(np, 0.0);
+  CK(sc->part_reg.upload(sc->part_reg_h));
+  CK(sc->part_fail.alloc(np + 1));
+  CK(sc->E_in.alloc(std::max(1, s.T)));
+  CK(sc->nu_in.alloc(std::max(1, s.T)));
+  int maxw = 1;
+  for (int w : F.sn_w) maxw = std::max(maxw, w);
+  sc->shm_fact = 2 * sizeof(double) * (size_t)maxw * maxw;
+  CK(cudaFuncSetAttribute(k_factor_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_fact));
+  sc->rd = RefactorDev{s.T, sc->tvol.p, sc->tE.p, sc->tnu.p, sc->twr.p, sc->twv.p, (int)base.size(),
+                       sc->hs_base.p, sc->hc_ptr.p, sc->hc_tet.p, sc->hc_coef.p, sc->hs_val.p, sc->hs_ptr.p,
+                       sc->hs_col.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p, sc->sn_rofs.p, sc->rowidx.p,
+                       sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->Ldw.p, sc->lvl_sn.p, sc->up_ptr.p,
+                       sc->up_d.p, sc->up_a0.p, sc->up_a1.p, np > 1 ? sc->sn_part.p : nullptr, sc->part_reg.p,
+                       sc->part_fail.p};
+  return DFEM_OK;
+}
+
+// Materials from E_in / nu_in (device), Hs values, and the factor on the GPU.
+// A part whose factorisation meets a non-positive pivot is retried with the
+// reference's regularisation sequence (0, 1e-5, x10 ..., 25 attempts); the
+// other parts keep their regularisation, so their factors are unchanged.
+static int gpu_refactor(dfem_scene* sc) {
+  const HostScene& s = sc->hs;
+  const int np = s.nparts;
+  CK(cudaMemsetAsync(sc->part_fail.p, 0, sizeof(int) * (np + 1), sc->stream));
+  if (s.T > 0) k_materials<<<(s.T + 127) / 128, 128, 0, sc->stream>>>(sc->rd, sc->E_in.p, sc->nu_in.p, np);
+  k_hs_values<<<(sc->rd.nnz + 255) / 256, 256, 0, sc->stream>>>(sc->rd);
+  sc->launches += (s.T > 0 ? 1 : 0) + 1;
+  std::vector<int> failh(np + 1);
+  CK(cudaMemcpyAsync(failh.data(), sc->part_fail.p, sizeof(int) * (np + 1), cudaMemcpyDeviceToHost, sc->stream));
+  CK(cudaStreamSynchronize(sc->stream));
+  if (failh[np]) return fail(DFEM_ERR_INVALID, "invalid material (non-finite E or nu, or nu <= -1)");
+  std::fill(sc->part_reg_h.begin(), sc->part_reg_h.end(), 0.0);
+  const int L = (int)sc->lvl_ptr.size() - 1;
+  for (int attempt = 0; attempt < 25; ++attempt) {
+    CK(cudaMemcpyAsync(sc->part_reg.p, sc->part_reg_h.data(), sizeof(double) * np, cudaMemcpyHostToDevice, sc->stream));
+    CK(cudaMemsetAsync(sc->part_fail.p, 0, sizeof(int) * np, sc->stream));
+    for (int l = 0; l < L; ++l)
+      k_factor_level<<<sc->lvl_ptr[l + 1] - sc->lvl_ptr[l], 256, sc->shm_fact, sc->stream>>>(sc->rd, sc->lvl_ptr[l]);
+    sc->launches += L;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(failh.data(), sc->part_fail.p, sizeof(int) * np, cudaMemcpyDeviceToHost, sc->stream));
+    CK(cudaStreamSynchronize(sc->stream));
+    bool any = false;
+    for (int p = 0; p < np; ++p)
+      if (failh[p]) {
+        any = true;
+        sc->part_reg_h[p] = sc->part_reg_h[p] == 0.0 ? 1e-5 : sc->part_reg_h[p] * 10.0;
+      }
+    if (!any) return DFEM_OK;
+  }
+  return fail(DFEM_ERR_FACTOR, "Cholesky factorisation failed after 25 regularisation retries");
 }
 
 static int upload_scene(dfem_scene* sc) {
@@ -742,6 +874,13 @@ static int create_on_device(std::unique_ptr<dfem_scene>& sc, int device, dfem_sc
   CK(sc->status.alloc(4));  // before the factor upload, whose kernels report into it
   RC(upload_scene(sc.get()));
   RC(ensure_steps(sc.get(), 1));
+  // every factor the engine uses comes from the GPU refactorisation
+  RC(upload_refactor_plan(sc.get()));
+  if (sc->hs.T > 0) {
+    CK(cudaMemcpyAsync(sc->E_in.p, sc->tE.p, sc->hs.T * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaMemcpyAsync(sc->nu_in.p, sc->tnu.p, sc->hs.T * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+  }
+  RC(gpu_refactor(sc.get()));
   CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
   RC(autotune_solve(sc.get()));
   CK(cudaDeviceSynchronize());
@@ -750,18 +889,6 @@ static int create_on_device(std::unique_ptr<dfem_scene>& sc, int device, dfem_sc
   return DFEM_OK;
 }
 
-// Run f(0) .. f(n-1) on up to hardware_concurrency host threads.
-template <typename Fn>
-static void parallel_for(int n, Fn f) {
-  const int nt = std::max(1, std::min(n, (int)std::thread::hardware_concurrency()));
-  std::atomic<int> next{0};
-  std::vector<std::thread> pool;
-  for (int t = 0; t < nt; ++t)
-    pool.emplace_back([&] {
-      for (int i = next++; i < n; i = next++) f(i);
-    });
-  for (auto& th : pool) th.join();
-}
 
 }  // namespace dfem
 
@@ -838,41 +965,32 @@ int dfem_scene_get_info(const dfem_scene* sc, dfem_scene_info* info) {
   info->n_vertices = s.N; info->n_tets = s.T; info->n_attach = s.A; info->n_muscle = s.M;
   info->n_springs = s.S; info->n_bending = s.B;
   info->n_supernodes = s.F.nsuper; info->n_levels = s.F.nlevels; info->nnz_factor = s.F.nnz_factor;
-  info->n_slots = s.nslots; info->device = sc->device; info->factor_regularisation = s.F.reg;
+  info->n_slots = s.nslots; info->device = sc->device;
+  info->factor_regularisation = 0.0;
+  for (double r : sc->part_reg_h) info->factor_regularisation = std::max(info->factor_regularisation, r);
   return DFEM_OK;
 }
 
 int dfem_set_materials(dfem_scene* sc, const double* youngs, const double* poisson, int mem) {
   if (!sc || !youngs || !poisson) return fail(DFEM_ERR_INVALID, "null argument");
   CK(cudaSetDevice(sc->device));
-  const int T = sc->hs.T;
-  std::vector<double> E(T), nu(T);
-  if (mem == DFEM_MEM_DEVICE) {
-    CK(cudaMemcpy(E.data(), youngs, T * sizeof(double), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(nu.data(), poisson, T * sizeof(double), cudaMemcpyDeviceToHost));
-  } else {
-    std::copy(youngs, youngs + T, E.begin());
-    std::copy(poisson, poisson + T, nu.begin());
-  }
-  std::string err;
+  HostScene& s = sc->hs;
+  const int T = s.T;
   CK(cudaStreamSynchronize(sc->stream));
-  if (sc->parts.empty()) {
-    if (!update_materials(sc->hs, E.data(), nu.data(), err)) return fail(DFEM_ERR_FACTOR, err);
-  } else {  // refactor every part on its own (its own regularisation), then copy into the union
-    const int np = (int)sc->parts.size();
-    std::vector<std::string> errs(np);
-    std::vector<int> ok(np, 1);
-    parallel_for(np, [&](int p) {
-      const int t0 = sc->hs.part_t0[p];
-      ok[p] = update_materials(sc->parts[p], E.data() + t0, nu.data() + t0, errs[p]) ? 1 : 0;
-    });
-    for (int p = 0; p < np; ++p)
-      if (!ok[p]) return fail(DFEM_ERR_FACTOR, "scene " + std::to_string(p) + ": " + errs[p]);
-    merge_numeric(sc->parts, sc->hs);
+  if (T > 0) {
+    RC(copy_in(sc, youngs, T, sc->E_in.p, mem));
+    RC(copy_in(sc, poisson, T, sc->nu_in.p, mem));
   }
-  RC(upload_materials(sc));
-  refresh_scene_view(sc);
-  CK(cudaDeviceSynchronize());
+  RC(gpu_refactor(sc));
+  if (sc->has_contact)
+    k_hs_diag<<<sc->nblk_v, 128, 0, sc->stream>>>(s.N, sc->hs_ptr.p, sc->hs_col.p, sc->hs_val.p, sc->hdiag.p);
+  // host copies of the moduli follow (the host factor is not used after creation)
+  if (T > 0) {
+    CK(cudaMemcpyAsync(s.tE.data(), sc->tE.p, T * sizeof(double), cudaMemcpyDeviceToHost, sc->stream));
+    CK(cudaMemcpyAsync(s.tnu.data(), sc->tnu.p, T * sizeof(double), cudaMemcpyDeviceToHost, sc->stream));
+  }
+  CK(cudaStreamSynchronize(sc->stream));
+  sc->rec_steps = 0;  // the recorded forward used the old factor
   return DFEM_OK;
 }
 

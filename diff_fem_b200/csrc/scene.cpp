@@ -91,7 +91,8 @@ SparseSym to_csr(int n, const Triplets& t) {
 }
 
 // Hs = M/h^2 + L_s in the numbering of the given tables (World.h:1093-1098).
-SparseSym assemble_hs(const HostScene& s) {
+// E (per tet, may be null) overrides the tets' Young's moduli.
+SparseSym assemble_hs(const HostScene& s, const double* E = nullptr) {
   Triplets t;
   const double ih2 = 1.0 / (s.h * s.h);
   for (int i = 0; i < s.N; ++i) t.add(i, i, s.mass[i] * ih2);
@@ -99,7 +100,8 @@ SparseSym assemble_hs(const HostScene& s) {
     double G[4][3];
     gcoef(&s.tinv[9 * e], G);
     // mu vol (1 + nu) G G^T = E vol G G^T (two blocks of CorotateFEMConstraint::EvaluateLMatrix)
-    double mu = s.tE[e] / (1.0 + s.tnu[e]);
+    const double Ee = E ? E[e] : s.tE[e];
+    double mu = Ee / (1.0 + s.tnu[e]);
     double w = mu * s.tvol[e] * (1.0 + s.tnu[e]);
     for (int a = 0; a < 4; ++a)
       for (int b = 0; b < 4; ++b) {
@@ -414,6 +416,38 @@ void merge_numeric(const std::vector<HostScene>& P, HostScene& u) {
     std::copy(p.F.Dinv.begin(), p.F.Dinv.end(), u.F.Dinv.begin() + d);
     u.F.reg = std::max(u.F.reg, p.F.reg);
     t += p.tE.size(); h += p.Hs.val.size(); l += p.F.Lcm.size(); d += p.F.Dinv.size();
+  }
+}
+
+void hs_split(const HostScene& s, std::vector<double>& base, std::vector<int>& cptr, std::vector<int>& ctet,
+              std::vector<double>& ccoef) {
+  const std::vector<double> zeroE(s.T, 0.0);
+  base = assemble_hs(s, zeroE.data()).val;
+  const int64_t nnz = (int64_t)s.Hs.col.size();
+  auto entry = [&](int i, int j) -> int64_t {
+    const int* c0 = s.Hs.col.data() + s.Hs.ptr[i];
+    const int* c1 = s.Hs.col.data() + s.Hs.ptr[i + 1];
+    return s.Hs.ptr[i] + (std::lower_bound(c0, c1, j) - c0);
+  };
+  // counting pass, then a fill pass in tet order (each entry's list is in tet order)
+  std::vector<int64_t> cnt(nnz + 1, 0);
+  for (int e = 0; e < s.T; ++e)
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) cnt[entry(s.tv[4 * e + a], s.tv[4 * e + b]) + 1]++;
+  for (int64_t k = 0; k < nnz; ++k) cnt[k + 1] += cnt[k];
+  cptr.assign(cnt.begin(), cnt.end());
+  ctet.resize(cnt[nnz]);
+  ccoef.resize(cnt[nnz]);
+  std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+  for (int e = 0; e < s.T; ++e) {
+    double G[4][3];
+    gcoef(&s.tinv[9 * e], G);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        const int64_t q = fill[entry(s.tv[4 * e + a], s.tv[4 * e + b])]++;
+        ctet[q] = e;
+        ccoef[q] = s.tvol[e] * (G[a][0] * G[b][0] + G[a][1] * G[b][1] + G[a][2] * G[b][2]);
+      }
   }
 }
 

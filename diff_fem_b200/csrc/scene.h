@@ -78,6 +78,12 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& hs, std::string& err)
 // Re-assemble Hs values after material changes and refactor (same structure).
 bool update_materials(HostScene& hs, const double* E_user_order, const double* nu_user_order, std::string& err);
 
+// Hs split for refactorisation on the GPU: base values (every term but the
+// tets' E vol G G^T) on Hs's pattern, and per entry of Hs the tets that touch
+// it with coefficient vol (G G^T)_ab, in tet order (CSR by entry).
+void hs_split(const HostScene& s, std::vector<double>& base, std::vector<int>& cptr, std::vector<int>& ctet,
+              std::vector<double>& ccoef);
+
 // Union of independent scenes: every table concatenated with its indices
 // offset, Hs and the supernodal factor block-diagonal, the level schedules
 // merged level by level (level l of the union = level l of every part).  The
