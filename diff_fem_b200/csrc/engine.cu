@@ -92,7 +92,15 @@ struct dfem_scene {
   DBuf<double> contrib, Lcm, Dinv;
   std::vector<int> lvl_ptr;
   int max_w = 1, max_r = 0;
-  std::vector<size_t> shm_fwd, shm_bwd;  // dynamic shared memory of the level kernels, per level
+  // Launch segments of the level-kernel solve: every level of the elimination
+  // tree, split into its small and its large supernodes (each with the
+  // shared memory of its largest member and an autotuned CTA size).
+  struct LevelSeg {
+    int begin, count, level;
+    size_t shm_f, shm_b;
+    int thr_f, thr_b;
+  };
+  std::vector<LevelSeg> segs;
   // persistent solve (one launch per solve) and the autotuned choice between it and the level kernels
   DBuf<int> sn_parent, kid_ptr, kid, done_f, done_b, solve_ctl;
   size_t shm_pers = 0;
@@ -104,6 +112,7 @@ struct dfem_scene {
   DBuf<int> hc_ptr, hc_tet, up_ptr, up_d, up_a0, up_a1, part_fail;
   std::vector<double> part_reg_h;
   size_t shm_fact = 0;
+  std::vector<size_t> shm_fact_lvl;      // dynamic shared memory of the refactorisation, per level
   RefactorDev rd{};
   // batch layout (a single scene is one part)
   std::vector<HostScene> parts;          // the parts of a batch (empty for a single scene)
@@ -178,7 +187,7 @@ static void refresh_scene_view(dfem_scene* sc) {
 }
 
 static int upload_factor(dfem_scene* sc) {
-  const SupernodalFactor& F = sc->hs.F;
+  SupernodalFactor& F = sc->hs.F;
   if (F.sn_rofs.back() > INT32_MAX / 3 || F.sn_lofs.back() > INT32_MAX || F.sn_dofs.back() > INT32_MAX)
     return fail(DFEM_ERR_INVALID, "factor too large for 32-bit offsets");
   auto to32 = [](const std::vector<int64_t>& v) { return std::vector<int>(v.begin(), v.end()); };
@@ -194,7 +203,6 @@ static int upload_factor(dfem_scene* sc) {
   CK(sc->Lcm.upload(F.Lcm));
   CK(sc->sn_dofs.upload(to32(F.sn_dofs)));
   CK(sc->Dinv.upload(F.Dinv));
-  CK(sc->lvl_sn.upload(F.lvl_sn));
   sc->lvl_ptr = F.lvl_ptr;
   sc->max_w = 1;
   for (int w : F.sn_w) sc->max_w = std::max(sc->max_w, w);
@@ -226,16 +234,40 @@ static int upload_factor(dfem_scene* sc) {
   const int stage_l = (need_f[1] <= budget && need_b[1] <= budget) ? 1 : 0;
   if (need_f[stage_l] > budget || need_b[stage_l] > budget)
     return fail(DFEM_ERR_INVALID, "supernode too large for the shared-memory staging of the triangular solves");
+  // One launch per level, with the shared memory of its largest supernode.
+  // (A split of each level into its small and large supernodes, launched one
+  // after the other, ran 10 % less kernel time but cost more in launch
+  // overhead inside the step graphs than it saved, on the 256-scene batch.)
+  // Within a level the supernodes are ordered by their shared-memory need (any
+  // order within a level is valid for every solve form and the refactorisation).
   const int L = (int)F.lvl_ptr.size() - 1;
-  sc->shm_fwd.assign(L, 0);
-  sc->shm_bwd.assign(L, 0);
-  for (int l = 0; l < L; ++l)
-    for (int k = F.lvl_ptr[l]; k < F.lvl_ptr[l + 1]; ++k) {
-      size_t nf, nb;
-      need(F.lvl_sn[k], stage_l, &nf, &nb);
-      sc->shm_fwd[l] = std::max(sc->shm_fwd[l], nf);
-      sc->shm_bwd[l] = std::max(sc->shm_bwd[l], nb);
+  const size_t small_shm = SIZE_MAX;
+  std::vector<size_t> key(F.nsuper);
+  for (int q = 0; q < F.nsuper; ++q) {
+    size_t nf, nb;
+    need(q, stage_l, &nf, &nb);
+    key[q] = std::max(nf, nb);
+  }
+  sc->segs.clear();
+  for (int l = 0; l < L; ++l) {
+    auto b = F.lvl_sn.begin() + F.lvl_ptr[l], e = F.lvl_sn.begin() + F.lvl_ptr[l + 1];
+    std::stable_sort(b, e, [&](int x, int y) { return key[x] < key[y]; });
+    int split = F.lvl_ptr[l];
+    while (split < F.lvl_ptr[l + 1] && key[F.lvl_sn[split]] <= small_shm) ++split;
+    const int cuts[3] = {F.lvl_ptr[l], split, F.lvl_ptr[l + 1]};
+    for (int g = 0; g < 2; ++g) {
+      if (cuts[g + 1] == cuts[g]) continue;
+      dfem_scene::LevelSeg sg{cuts[g], cuts[g + 1] - cuts[g], l, 0, 0, 256, 256};
+      for (int k = cuts[g]; k < cuts[g + 1]; ++k) {
+        size_t nf, nb;
+        need(F.lvl_sn[k], stage_l, &nf, &nb);
+        sg.shm_f = std::max(sg.shm_f, nf);
+        sg.shm_b = std::max(sg.shm_b, nb);
+      }
+      sc->segs.push_back(sg);
     }
+  }
+  CK(sc->lvl_sn.upload(F.lvl_sn));
   CK(cudaFuncSetAttribute(k_fwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_f[stage_l]));
   CK(cudaFuncSetAttribute(k_bwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_b[stage_l]));
   // persistent solve: elimination tree (children CSR), completion stamps, control words
@@ -368,8 +400,15 @@ static int upload_refactor_plan(dfem_scene* sc) {
   CK(sc->nu_in.alloc(std::max(1, s.T)));
   int maxw = 1;
   for (int w : F.sn_w) maxw = std::max(maxw, w);
-  sc->shm_fact = 2 * sizeof(double) * (size_t)maxw * maxw;
+  sc->shm_fact = factor_smem_bytes(maxw);
+  if (sc->shm_fact > 227 * 1024) return fail(DFEM_ERR_INVALID, "supernode too wide for the GPU refactorisation");
   CK(cudaFuncSetAttribute(k_factor_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_fact));
+  sc->shm_fact_lvl.assign(F.nlevels, 0);
+  for (int l = 0; l < F.nlevels; ++l) {
+    int mw = 1;
+    for (int k = F.lvl_ptr[l]; k < F.lvl_ptr[l + 1]; ++k) mw = std::max(mw, F.sn_w[F.lvl_sn[k]]);
+    sc->shm_fact_lvl[l] = factor_smem_bytes(mw);
+  }
   sc->rd = RefactorDev{s.T, sc->tvol.p, sc->tE.p, sc->tnu.p, sc->twr.p, sc->twv.p, (int)base.size(),
                        sc->hs_base.p, sc->hc_ptr.p, sc->hc_tet.p, sc->hc_coef.p, sc->hs_val.p, sc->hs_ptr.p,
                        sc->hs_col.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p, sc->sn_rofs.p, sc->rowidx.p,
@@ -400,7 +439,8 @@ static int gpu_refactor(dfem_scene* sc) {
     CK(cudaMemcpyAsync(sc->part_reg.p, sc->part_reg_h.data(), sizeof(double) * np, cudaMemcpyHostToDevice, sc->stream));
     CK(cudaMemsetAsync(sc->part_fail.p, 0, sizeof(int) * np, sc->stream));
     for (int l = 0; l < L; ++l)
-      k_factor_level<<<sc->lvl_ptr[l + 1] - sc->lvl_ptr[l], 256, sc->shm_fact, sc->stream>>>(sc->rd, sc->lvl_ptr[l]);
+      k_factor_level<<<sc->lvl_ptr[l + 1] - sc->lvl_ptr[l], 256, sc->shm_fact_lvl[l], sc->stream>>>(sc->rd,
+                                                                                                  sc->lvl_ptr[l]);
     sc->launches += L;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(failh.data(), sc->part_fail.p, sizeof(int) * np, cudaMemcpyDeviceToHost, sc->stream));
@@ -564,19 +604,13 @@ static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const doub
     k_solve_persistent<<<sc->pers_grid, 256, sc->shm_pers, st>>>(sc->fd, gate, rhs, y);
     return;
   }
-  const int L = (int)sc->lvl_ptr.size() - 1;
-  for (int l = 0; l < L; ++l) {
-    int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_fwd_level<<<nb, 256, sc->shm_fwd[l], st>>>(sc->fd, sc->lvl_ptr[l], gate, rhs, y);
-  }
-  for (int l = L - 1; l >= 0; --l) {
-    int nb = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l];
-    k_bwd_level<<<nb, 256, sc->shm_bwd[l], st>>>(sc->fd, sc->lvl_ptr[l], gate, y);
-  }
+  for (const auto& g : sc->segs) k_fwd_level<<<g.count, g.thr_f, g.shm_f, st>>>(sc->fd, g.begin, gate, rhs, y);
+  for (auto it = sc->segs.rbegin(); it != sc->segs.rend(); ++it)
+    k_bwd_level<<<it->count, it->thr_b, it->shm_b, st>>>(sc->fd, it->begin, gate, y);
 }
 
 static int solve_launches(const dfem_scene* sc) {
-  return sc->solve_mode == 1 ? 1 : 2 * ((int)sc->lvl_ptr.size() - 1);
+  return sc->solve_mode == 1 ? 1 : 2 * (int)sc->segs.size();
 }
 
 // Fresh completion stamps and control words of the persistent solve (each API
@@ -838,6 +872,31 @@ static int autotune_solve(dfem_scene* sc) {
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
+  // CTA size of every launch segment and direction: 64, 128 or 256 threads
+  {
+    const int cand[3] = {64, 128, 256};
+    for (auto& g : sc->segs)
+      for (int dir = 0; dir < 2; ++dir) {
+        double best = 1e30;
+        int pick = 256;
+        for (int thr : cand) {
+          auto launch = [&] {
+            if (dir == 0) k_fwd_level<<<g.count, thr, g.shm_f, sc->stream>>>(sc->fd, g.begin, kOpen, sc->rhs.p, sc->y.p);
+            else k_bwd_level<<<g.count, thr, g.shm_b, sc->stream>>>(sc->fd, g.begin, kOpen, sc->y.p);
+          };
+          launch();
+          cudaEventRecord(e0, sc->stream);
+          for (int r = 0; r < 5; ++r) launch();
+          cudaEventRecord(e1, sc->stream);
+          CK(cudaEventSynchronize(e1));
+          float t = 0;
+          CK(cudaEventElapsedTime(&t, e0, e1));
+          sc->launches += 6;
+          if (t < best) { best = t; pick = thr; }
+        }
+        (dir == 0 ? g.thr_f : g.thr_b) = pick;
+      }
+  }
   const int reps = 10;
   for (int mode = 0; mode < 2; ++mode) {
     sc->solve_mode = mode;
@@ -1162,6 +1221,48 @@ int dfem_host_factor_solve(const dfem_scene_desc* desc, const double* b, double*
     info->n_levels = hs.F.nlevels; info->nnz_factor = hs.F.nnz_factor; info->n_slots = hs.nslots;
     info->device = -1; info->factor_regularisation = hs.F.reg;
   }
+  return DFEM_OK;
+}
+
+int dfem_profile_levels(dfem_scene* sc, int32_t reps, int32_t cap, int32_t* n_segments, double* ms_fwd, double* ms_bwd,
+                        int32_t* n_supernodes, int32_t* level, int32_t* threads) {
+  if (!sc || !n_segments || reps < 1) return fail(DFEM_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(sc->device));
+  const int G = (int)sc->segs.size();
+  *n_segments = G;
+  if (!ms_fwd || !ms_bwd || cap < G) return DFEM_OK;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
+  auto time_it = [&](auto&& launch) -> double {
+    launch();
+    cudaEventRecord(e0, sc->stream);
+    for (int r = 0; r < reps; ++r) launch();
+    cudaEventRecord(e1, sc->stream);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    sc->launches += reps + 1;
+    return (double)t / reps;
+  };
+  for (int g = 0; g < G; ++g) {
+    const auto& sg = sc->segs[g];
+    if (n_supernodes) n_supernodes[g] = sg.count;
+    if (level) level[g] = sg.level;
+    if (threads) { threads[2 * g] = sg.thr_f; threads[2 * g + 1] = sg.thr_b; }
+    ms_fwd[g] = time_it([&] {
+      k_fwd_level<<<sg.count, sg.thr_f, sg.shm_f, sc->stream>>>(sc->fd, sg.begin, kOpen, sc->rhs.p, sc->y.p);
+    });
+    ms_bwd[g] = time_it([&] { k_bwd_level<<<sg.count, sg.thr_b, sg.shm_b, sc->stream>>>(sc->fd, sg.begin, kOpen, sc->y.p); });
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaGetLastError());
+  int st4[4] = {0, 0, 0, 0};
+  CK(cudaMemcpy(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost));
+  RC(status_error(st4));
+  sc->rec_steps = 0;
   return DFEM_OK;
 }
 

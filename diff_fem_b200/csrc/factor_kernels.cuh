@@ -110,7 +110,24 @@ __device__ __forceinline__ int sn_local_row(int i, int c0, int w, const int* R, 
   return (lo < r && R[lo] == i) ? w + lo : -1;
 }
 
-// Shared memory: L (w x w, column-major) | X = L^-1 (w x w, column-major); 2 w^2 doubles.
+// FP64 tensor-core tile: D (8x8) += A (8x4, row-major) * B (4x8, column-major),
+// one warp (mma.sync m8n8k4 f64).  Fragments: A[lane>>2][lane&3];
+// B[lane&3][lane>>2]; C/D rows lane>>2, columns 2*(lane&3) + {0, 1}.
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int kRowChunk = 1024;  // rows of a descendant update mapped per pass (shared int buffer)
+constexpr int kTrsmRows = 64;    // rows of the below-diagonal block staged per TRSM pass
+
+// Shared memory (doubles): L (w x w, column-major) | X = L^-1 (w x w, column-major)
+//   | S (kTrsmRows x w, row-major) ; then kRowChunk ints (update row map).
+__host__ __device__ inline size_t factor_smem_bytes(int w) {
+  return sizeof(double) * (2 * (size_t)w * w + (size_t)kTrsmRows * w) + sizeof(int) * kRowChunk;
+}
+
 __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_begin) {
   extern __shared__ __align__(16) double fsh[];
   __shared__ int s_bad;
@@ -118,11 +135,16 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
   const int part = f.sn_part ? f.sn_part[s] : 0;
   const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
   const int* R = f.rowidx + f.sn_rofs[s];
-  double* Lc = f.Lcm + f.sn_lofs[s];   // r x w, column-major
-  double* Ld = f.Ldw + f.sn_dofs[s];   // w x w, column-major
+  double* Lc = f.Lcm + f.sn_lofs[s];   // r x w, column-major (the panel's rows below)
+  double* Ld = f.Ldw + f.sn_dofs[s];   // w x w, column-major (the panel's diagonal block)
+  double* L = fsh;
+  double* X = fsh + w * w;
+  double* S = X + w * w;
+  int* rowmap = reinterpret_cast<int*>(S + kTrsmRows * w);
   const double reg = f.part_reg[part];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (threadIdx.x == 0) s_bad = 0;
-  // 1. this supernode's columns of Hs (lower part)
+  // 1. this supernode's columns of Hs (lower part) into the panel
   for (int q = threadIdx.x; q < w * w; q += blockDim.x) Ld[q] = 0.0;
   for (int q = threadIdx.x; q < r * w; q += blockDim.x) Lc[q] = 0.0;
   __syncthreads();
@@ -138,57 +160,83 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
     }
   }
   __syncthreads();
-  // 2. updates of the descendants, in list order: column block R_d[a0..a1) of s,
-  //    rows R_d[a0..r_d) : P -= L_{rows, d} L_{cols, d}^T
+  // 2. left-looking updates, in list order: for descendant d with rows R_d[a0..a1)
+  //    in this supernode's columns, P[R_d[x], R_d[y]] -= sum_k L_d[x,k] L_d[y,k]
+  //    for a0 <= y < a1, y <= x < r_d: 8x8 output tiles on the FP64 tensor cores.
   for (int u = f.up_ptr[s]; u < f.up_ptr[s + 1]; ++u) {
     const int d = f.up_d[u], a0 = f.up_a0[u], a1 = f.up_a1[u];
     const int wd = f.sn_w[d], rd = f.sn_r[d];
     const int* Rd = f.rowidx + f.sn_rofs[d];
     const double* Lcd = f.Lcm + f.sn_lofs[d];
-    for (int x = a0 + (int)threadIdx.x; x < rd; x += blockDim.x) {
-      const int a = sn_local_row(Rd[x], c0, w, R, r);
-      if (a < 0) { s_bad = 1; continue; }
-      const int yend = x < a1 ? x + 1 : a1;
-      for (int y = a0; y < yend; ++y) {
-        double acc = 0.0;
-        for (int k = 0; k < wd; ++k) acc += Lcd[k * rd + x] * Lcd[k * rd + y];
-        const int c = Rd[y] - c0;
-        if (a < w) Ld[a + c * w] -= acc; else Lc[c * r + (a - w)] -= acc;
+    const int m = a1 - a0;
+    for (int xc = a0; xc < rd; xc += kRowChunk) {
+      const int xe = min(rd, xc + kRowChunk);
+      for (int x = xc + (int)threadIdx.x; x < xe; x += blockDim.x) {
+        const int a = sn_local_row(Rd[x], c0, w, R, r);
+        if (a < 0) s_bad = 1;
+        rowmap[x - xc] = a;
       }
+      __syncthreads();
+      const int nti = (xe - xc + 7) / 8, ntj = (m + 7) / 8;
+      for (int t = warp; t < nti * ntj; t += nw) {
+        const int x0 = xc + 8 * (t / ntj), y0 = a0 + 8 * (t % ntj);
+        if (x0 + 7 < y0) continue;  // strictly upper tile
+        const int xa = x0 + (lane >> 2), yb = y0 + (lane >> 2);
+        double d0 = 0.0, d1 = 0.0;
+        const bool xin = xa < xe, yin = yb < a1;
+        // loads of 8 k-steps are issued before their tensor-core steps (L2 latency)
+        for (int kb = 0; kb < wd; kb += 32) {
+          double av[8], bv[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int ka = kb + 4 * q + (lane & 3);
+            av[q] = (xin && ka < wd) ? Lcd[(size_t)ka * rd + xa] : 0.0;
+            bv[q] = (yin && ka < wd) ? Lcd[(size_t)ka * rd + yb] : 0.0;
+          }
+#pragma unroll
+          for (int q = 0; q < 8; ++q) dmma_8x8x4(d0, d1, av[q], bv[q]);
+        }
+        const int xr = x0 + (lane >> 2);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int yc = y0 + 2 * (lane & 3) + i;
+          if (xr < xe && yc < a1 && xr >= yc) {
+            const int a = rowmap[xr - xc];
+            if (a < 0) continue;
+            const int c = Rd[yc] - c0;
+            const double v = i == 0 ? d0 : d1;
+            if (a < w) Ld[a + c * w] -= v; else Lc[c * r + (a - w)] -= v;
+          }
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
-  // 3. dense Cholesky of the diagonal block in shared memory (right looking)
-  double* L = fsh;
-  double* X = fsh + w * w;
+  // 3. dense Cholesky of the diagonal block by one warp (right looking, column by column)
   for (int q = threadIdx.x; q < w * w; q += blockDim.x) L[q] = Ld[q];
   __syncthreads();
-  for (int c = 0; c < w; ++c) {
-    if (threadIdx.x == 0) {
-      double dgl = L[c + c * w];
-      if (!(dgl > 0.0) || !isfinite(dgl)) { s_bad = 1; dgl = 1.0; }
-      L[c + c * w] = sqrt(dgl);
-    }
-    __syncthreads();
-    const double piv = L[c + c * w];
-    for (int i = c + 1 + (int)threadIdx.x; i < w; i += blockDim.x) L[i + c * w] /= piv;
-    __syncthreads();
-    const int m = w - c - 1;  // trailing (i >= j > c): pairs over the lower triangle
-    for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
-      const int i = c + 1 + q / m, j = c + 1 + q % m;
-      if (j <= i) L[i + j * w] -= L[i + c * w] * L[j + c * w];
-    }
-    __syncthreads();
-  }
-  // 4. rows below: L_{R,s} = P_R L_ss^-T (one row per thread)
-  for (int a = threadIdx.x; a < r; a += blockDim.x) {
+  if (warp == 0) {
     for (int c = 0; c < w; ++c) {
-      double v = Lc[c * r + a];
-      for (int k = 0; k < c; ++k) v -= Lc[k * r + a] * L[c + k * w];
-      Lc[c * r + a] = v / L[c + c * w];
+      double dgl = L[c + c * w];
+      const bool bad = !(dgl > 0.0) || !isfinite(dgl);
+      if (bad) dgl = 1.0;
+      const double piv = sqrt(dgl);
+      __syncwarp();
+      if (lane == 0) {
+        L[c + c * w] = piv;
+        if (bad) s_bad = 1;
+      }
+      for (int i = c + 1 + lane; i < w; i += 32) L[i + c * w] /= piv;
+      __syncwarp();
+      for (int j = c + 1; j < w; ++j) {
+        const double ljc = L[j + c * w];
+        for (int i = j + lane; i < w; i += 32) L[i + j * w] -= L[i + c * w] * ljc;
+      }
+      __syncwarp();
     }
   }
-  // 5. X = L_ss^-1 (one column per thread), stored row-major lower in Dinv
+  __syncthreads();
+  // 4. X = L_ss^-1 (one column per thread)
   for (int c = threadIdx.x; c < w; c += blockDim.x) {
     for (int i = 0; i < c; ++i) X[i + c * w] = 0.0;
     for (int i = c; i < w; ++i) {
@@ -198,10 +246,35 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
     }
   }
   __syncthreads();
-  double* Di = f.Dinv + f.sn_dofs[s];
-  for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
-    const int i = q / w, c = q % w;
-    Di[q] = X[i + c * w];
+  double* Di = f.Dinv + f.sn_dofs[s];  // row-major lower
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) Di[q] = X[(q / w) + (q % w) * w];
+  // 5. rows below: L_{R,s} = P_R X^T, kTrsmRows rows at a time (staged, then overwritten)
+  for (int rb = 0; rb < r; rb += kTrsmRows) {
+    const int nr = min(kTrsmRows, r - rb);
+    for (int q = threadIdx.x; q < nr * w; q += blockDim.x) {
+      const int x = q % nr, c = q / nr;  // coalesced along the column-major block
+      S[x * w + c] = Lc[c * r + rb + x];
+    }
+    __syncthreads();
+    const int nti = (nr + 7) / 8, ntj = (w + 7) / 8;
+    for (int t = warp; t < nti * ntj; t += nw) {
+      const int x0 = 8 * (t / ntj), y0 = 8 * (t % ntj);
+      const int xa = x0 + (lane >> 2), yb = y0 + (lane >> 2);
+      double d0 = 0.0, d1 = 0.0;
+      for (int k0 = 0; k0 < w; k0 += 4) {
+        const int ka = k0 + (lane & 3);
+        const double av = (xa < nr && ka < w) ? S[xa * w + ka] : 0.0;
+        const double bv = (yb < w && ka < w) ? X[yb + ka * w] : 0.0;  // (X^T)[k][y] = X[y][k]
+        dmma_8x8x4(d0, d1, av, bv);
+      }
+      const int xr = x0 + (lane >> 2);
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int yc = y0 + 2 * (lane & 3) + i;
+        if (xr < nr && yc < w) Lc[yc * r + rb + xr] = i == 0 ? d0 : d1;
+      }
+    }
+    __syncthreads();
   }
   if (threadIdx.x == 0 && s_bad) atomicExch(f.part_fail + part, 1);
 }

@@ -200,6 +200,19 @@ class Scene:
         check(lib().dfem_solve_mode(self._h, req, C.byref(chosen), ms))
         return {"mode": {1: "levels", 2: "persistent"}[chosen.value], "ms_levels": ms[0], "ms_persistent": ms[1]}
 
+    def profile_levels(self, reps: int = 10) -> dict:
+        """ms per launch of every forward / backward launch of the level-kernel
+        solve (a level, split into its small and large supernodes), with the
+        supernodes, level and CTA sizes of each launch."""
+        n = C.c_int32()
+        check(lib().dfem_profile_levels(self._h, int(reps), 0, C.byref(n), None, None, None, None, None))
+        G = int(n.value)
+        f, b = (C.c_double * G)(), (C.c_double * G)()
+        cnt, lvl, thr = (C.c_int32 * G)(), (C.c_int32 * G)(), (C.c_int32 * (2 * G))()
+        check(lib().dfem_profile_levels(self._h, int(reps), G, C.byref(n), f, b, cnt, lvl, thr))
+        return {"fwd_ms": list(f), "bwd_ms": list(b), "supernodes": list(cnt), "level": list(lvl),
+                "threads_fwd": list(thr)[0::2], "threads_bwd": list(thr)[1::2]}
+
     def launch_count(self) -> int:
         n = C.c_int64()
         check(lib().dfem_get_launch_count(self._h, C.byref(n)))

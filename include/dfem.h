@@ -239,6 +239,16 @@ int dfem_host_factor_solve(const dfem_scene_desc *desc, const double *b, double 
  * sim/fem/World.h:1660). */
 int dfem_solve_mode(dfem_scene *scene, int32_t request, int32_t *chosen, double *ms);
 
+/* CUDA-event timing of every launch of the level-kernel solve form (a level
+ * of the elimination tree, split into its small and its large supernodes;
+ * forward and backward, `reps` launches each on the scene's stream, ms per
+ * launch).  *n_segments receives the launch count per direction; the arrays
+ * (cap entries each, may be NULL to query the count) receive the times, the
+ * supernodes, the level of each launch and its CTA sizes (2 per launch:
+ * forward, backward).  Instrumentation; no counterpart in the reference. */
+int dfem_profile_levels(dfem_scene *scene, int32_t reps, int32_t cap, int32_t *n_segments, double *ms_fwd,
+                        double *ms_bwd, int32_t *n_supernodes, int32_t *level, int32_t *threads);
+
 /* Number of kernels this scene has launched so far (CUDA-graph nodes counted
  * individually).  Instrumentation; no counterpart in the reference. */
 int dfem_get_launch_count(const dfem_scene *scene, int64_t *count);

@@ -730,13 +730,32 @@ static void contact_basis(V3 normal, V3 B[3]) {
 
 struct ObsImpact { int face; V3 n; };
 
+/* What the adjoint of the contact phase needs from one run of it: every
+ * computed Jacobi iteration's input ori_x, its relaxed rhs (prev) after the
+ * update, whether it started its pass (prev restarts from its own rhs), the
+ * impact normals of every contact vertex at that iteration (list order), and
+ * which computed iteration produced the phase's output (0: the PD result).
+ * The detection is discrete: impacts and normals are constants of the tape,
+ * as they are on the reference's CppAD tape (collision detection runs in
+ * plain double). */
+struct ContactTape {
+  int out_src = 0;
+  std::vector<std::vector<double>> ori, prev;
+  std::vector<char> first;
+  std::vector<std::vector<std::vector<V3>>> nrm;
+  std::vector<double> hd;
+};
+
 /* Contact phase of ProjectiveDynamicsMethod (World.h:925-1023), obstacle
  * contacts only.  ori_x enters as the PD result and leaves as the returned
  * positions; x_n1 follows the reference's (x_n1, ori_x) bookkeeping exactly. */
-static void contact_phase(Scene& S, const double* x_t, const double* vwc, const double* act, double* ori_x) {
+static void contact_phase(Scene& S, const double* x_t, const double* vwc, const double* act, double* ori_x,
+                          ContactTape* tape = nullptr) {
   const int N = S.N, n3 = 3 * N, nc = (int)S.cverts.size();
   S.last_passes = 0;
+  if (tape) *tape = ContactTape();
   if (!S.collide || nc == 0 || S.obs_f.empty()) return;
+  int computed = 0, src_ori = 0;
   std::vector<std::vector<ObsImpact>> imp(nc);
   std::vector<double> xold(n3, 0.0), x_n1(ori_x, ori_x + n3), rhs(n3), prev(n3, 0.0), jd(n3), Lxt(n3), Hx(n3);
   /* L x_t = Hs x_t - M/h^2 x_t ; C = Hs - diag(Hs) */
@@ -747,6 +766,7 @@ static void contact_phase(Scene& S, const double* x_t, const double* vwc, const 
     for (auto& e : S.Hrows[i]) if (e.first == i) hd[i] = e.second;
     for (int c = 0; c < 3; ++c) Lxt[3 * i + c] = Hx[3 * i + c] - S.mass[i] * ih2 * x_t[3 * i + c];
   }
+  if (tape) tape->hd = hd;
   for (int pass = 0; pass < S.max_passes; ++pass) {
     /* detection at ori_x (vertex start positions: x_t) */
     bool any = false;
@@ -766,6 +786,7 @@ static void contact_phase(Scene& S, const double* x_t, const double* vwc, const 
     S.last_passes = pass + 1;
     for (int it = 0; it < S.K; ++it) {
       for (int k = 0; k < n3; ++k) ori_x[k] = x_n1[k];
+      src_ori = computed;
       double err = 0;
       for (int k = 0; k < n3; ++k) err = std::max(err, std::fabs(ori_x[k] - xold[k]));
       if (err < 5e-7) break;
@@ -802,8 +823,19 @@ static void contact_phase(Scene& S, const double* x_t, const double* vwc, const 
       for (int i = 0; i < N; ++i)
         for (int c = 0; c < 3; ++c) x_n1[3 * i + c] = x_t[3 * i + c] + prev[3 * i + c] / S.h / hd[i];
       for (int k = 0; k < n3; ++k) xold[k] = ori_x[k];
+      ++computed;
+      if (tape) {
+        tape->ori.emplace_back(ori_x, ori_x + n3);
+        tape->prev.push_back(prev);
+        tape->first.push_back(it == 0 ? 1 : 0);
+        std::vector<std::vector<V3>> nr(nc);
+        for (int a = 0; a < nc; ++a)
+          for (auto& r : imp[a]) nr[a].push_back(r.n);
+        tape->nrm.push_back(std::move(nr));
+      }
     }
   }
+  if (tape) tape->out_src = src_ori;
 }
 
 /* ---- adjoint ---------------------------------------------------------------- */
@@ -930,6 +962,133 @@ static void H_param_vjp(const Scene& S, const double* yb, const double* x, doubl
       }
     gE[t] -= T.vol * s;
   }
+}
+
+/* Reverse of the contact phase (test restatement).  xb: in, the cotangent of
+ * the phase's output; out, the cotangent of its input (the PD result).  xtb,
+ * vwcb accumulate the cotangents of x_t and v_wc; gE, gnu, gact those of the
+ * parameters (J d at each iteration's input; Hs through C, L x_t and diag(Hs)).
+ * Per computed iteration j (in reverse), with rhs_pre = M v_wc + h (J d(ori) -
+ * L x_t) - h C (ori - x_t), rhs_post its contact projection, prev_j =
+ * alpha rhs_post + (1 - alpha) prev_{j-1} (prev_{j-1} := rhs_pre at the first
+ * iteration of a pass) and x_n1 = x_t + prev_j / (h diag(Hs)). */
+static void contact_adjoint(const Scene& S, const double* x_t, const double* vwc, const double* act,
+                            const ContactTape& tp, double* xb, double* xtb, double* vwcb, double* gE, double* gnu,
+                            double* gact) {
+  const int N = S.N, n3 = 3 * N, nc = (int)S.cverts.size();
+  if (tp.out_src == 0) return;
+  const double h = S.h, ih2 = 1.0 / (h * h), mu = S.mu_obs, al = S.alpha;
+  std::vector<double> xn1b(xb, xb + n3), pb(n3, 0.0), hdb(N, 0.0), rpb(n3), yb(n3), orib(n3), rhs(n3), jd(n3), Lxt(n3), Hx(n3);
+  H_mul(S, x_t, Hx.data());
+  for (int i = 0; i < N; ++i)
+    for (int c = 0; c < 3; ++c) Lxt[3 * i + c] = Hx[3 * i + c] - S.mass[i] * ih2 * x_t[3 * i + c];
+  std::vector<int> cidx(N, -1);
+  for (int a = 0; a < nc; ++a) cidx[S.cverts[a]] = a;
+  for (int j = tp.out_src; j >= 1; --j) {
+    const std::vector<double>& ori = tp.ori[j - 1];
+    const std::vector<double>& prev = tp.prev[j - 1];
+    /* x_n1 = x_t + prev / (h hd) */
+    for (int i = 0; i < N; ++i)
+      for (int c = 0; c < 3; ++c) {
+        const int k = 3 * i + c;
+        xtb[k] += xn1b[k];
+        hdb[i] -= xn1b[k] * prev[k] / (h * tp.hd[i] * tp.hd[i]);
+        pb[k] += xn1b[k] / (h * tp.hd[i]);
+      }
+    /* rhs_pre at ori (recomputed) */
+    std::fill(jd.begin(), jd.end(), 0.0);
+    local_Jd(S, ori.data(), act, jd.data(), 1);
+    for (int i = 0; i < N; ++i) {
+      double cdx[3] = {0, 0, 0};
+      for (auto& e : S.Hrows[i])
+        if (e.first != i)
+          for (int c = 0; c < 3; ++c) cdx[c] += e.second * (ori[3 * e.first + c] - x_t[3 * e.first + c]);
+      for (int c = 0; c < 3; ++c)
+        rhs[3 * i + c] = S.mass[i] * vwc[3 * i + c] + h * (jd[3 * i + c] - Lxt[3 * i + c]) - h * cdx[c];
+    }
+    /* prev_j = al rhs_post + (1 - al) prev_{j-1} */
+    for (int k = 0; k < n3; ++k) rpb[k] = al * pb[k];
+    /* contact projection of the contact vertices (the last non-skipped impact wins) */
+    for (int i = 0; i < N; ++i) {
+      const int a = cidx[i];
+      if (a < 0) continue;
+      V3 f = getx(rhs.data(), i), win[3];
+      bool hit = false;
+      double r0 = 0, r1 = 0, r2 = 0;
+      for (const V3& nv : tp.nrm[j - 1][a]) {
+        V3 B[3];
+        contact_basis(nv, B);
+        double f0 = dot(B[0], f);
+        if (f0 > 0) continue;
+        hit = true;
+        win[0] = B[0]; win[1] = B[1]; win[2] = B[2];
+        r0 = -f0; r1 = -dot(B[1], f); r2 = -dot(B[2], f);
+      }
+      if (!hit) continue;
+      V3 ob = getx(rpb.data(), i);
+      double b0 = dot(win[0], ob), b1 = dot(win[1], ob), b2 = dot(win[2], ob);  /* cotangents of r0, r1', r2' */
+      double rt = std::sqrt(r1 * r1 + r2 * r2), g0 = b0, g1 = b1, g2 = b2;
+      if (rt > mu * r0) {  /* r' = mu r0 (r1, r2) / rt */
+        g0 = b0 + mu * (r1 * b1 + r2 * b2) / rt;
+        g1 = mu * r0 * (r2 * r2 * b1 - r1 * r2 * b2) / (rt * rt * rt);
+        g2 = mu * r0 * (r1 * r1 * b2 - r1 * r2 * b1) / (rt * rt * rt);
+      }
+      V3 fb = -1.0 * (g0 * win[0] + g1 * win[1] + g2 * win[2]);
+      rpb[3 * i] = fb.x; rpb[3 * i + 1] = fb.y; rpb[3 * i + 2] = fb.z;
+    }
+    if (tp.first[j - 1]) {
+      for (int k = 0; k < n3; ++k) { rpb[k] += (1.0 - al) * pb[k]; pb[k] = 0.0; }
+    } else {
+      for (int k = 0; k < n3; ++k) pb[k] = (1.0 - al) * pb[k];
+    }
+    /* rhs_pre = M v_wc + h (J d(ori) - L x_t) - h C (ori - x_t) */
+    for (int i = 0; i < N; ++i)
+      for (int c = 0; c < 3; ++c) vwcb[3 * i + c] += S.mass[i] * rpb[3 * i + c];
+    for (int k = 0; k < n3; ++k) yb[k] = h * rpb[k];
+    std::fill(orib.begin(), orib.end(), 0.0);
+    local_Jd_vjp(S, ori.data(), act, yb.data(), orib.data(), gE, gnu, gact);
+    for (int i = 0; i < N; ++i)
+      for (auto& e : S.Hrows[i]) {
+        const int jj = e.first;
+        for (int c = 0; c < 3; ++c) {
+          if (jj != i) {
+            orib[3 * jj + c] -= e.second * yb[3 * i + c];   /* -h C (ori - x_t) */
+            xtb[3 * jj + c] += e.second * yb[3 * i + c];
+          }
+          xtb[3 * jj + c] -= e.second * yb[3 * i + c];     /* -h L x_t, L x_t = Hs x_t - M/h^2 x_t */
+        }
+      }
+    for (int i = 0; i < N; ++i)
+      for (int c = 0; c < 3; ++c) xtb[3 * i + c] += S.mass[i] * ih2 * yb[3 * i + c];
+    /* Hs entries: d rhs_pre_i / d Hs_ij = -h ori_j (i != j), -h x_t_i (i == j) */
+    if (gE)
+      for (size_t t = 0; t < S.tets.size(); ++t) {
+        const Tet& T = S.tets[t];
+        double sacc = 0;
+        for (int a2 = 0; a2 < 4; ++a2)
+          for (int b2 = 0; b2 < 4; ++b2) {
+            double gg = 0;
+            for (int q = 0; q < 3; ++q) gg += T.G[a2][q] * T.G[b2][q];
+            const double* xs = a2 == b2 ? x_t : ori.data();
+            sacc += gg * dot(getx(yb.data(), T.v[a2]), getx(xs, T.v[b2]));
+          }
+        gE[t] -= T.vol * sacc;
+      }
+    xn1b = orib;  /* ori_x of iteration j is x_n1 of iteration j - 1 */
+  }
+  /* diag(Hs) entries */
+  if (gE)
+    for (size_t t = 0; t < S.tets.size(); ++t) {
+      const Tet& T = S.tets[t];
+      double sacc = 0;
+      for (int a2 = 0; a2 < 4; ++a2) {
+        double gg = 0;
+        for (int q = 0; q < 3; ++q) gg += T.G[a2][q] * T.G[a2][q];
+        sacc += gg * hdb[T.v[a2]];
+      }
+      gE[t] += T.vol * sacc;
+    }
+  std::copy(xn1b.begin(), xn1b.end(), xb);
 }
 
 }  // namespace orc
@@ -1070,8 +1229,6 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
                  double* gE, double* gnu, double* gact) {
   Scene* S = static_cast<Scene*>(s);
   if (S->rec_steps <= 0) return 5;
-  for (int p : S->rec_passes)
-    if (p > 0) { S->err = "adjoint through the contact phase is not restated"; return 5; }
   int N = S->N, n3 = 3 * N;
   int NT = (int)S->tets.size();
   std::vector<double> xb(gx_out, gx_out + n3), vb(gv_out, gv_out + n3);
@@ -1086,10 +1243,14 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
     const double* a = &S->rec_act[(size_t)st * std::max(1, S->nseg)];
     step_prep(*S, x, v, vwc.data(), qn.data());
     int it = pd_solve(*S, x, qn.data(), a, &hist, xn.data(), 1);
-    /* v' = damping (x' - x)/h; x' = x^it */
+    ContactTape tape;
+    contact_phase(*S, x, vwc.data(), a, xn.data(), &tape);
+    /* v' = damping (x' - x)/h; x' = contact phase output (x^it without contacts) */
     double c = S->damping / S->h;
-    std::vector<double> xtb(n3);
+    std::vector<double> xtb(n3), vwcb(n3, 0.0);
     for (int k = 0; k < n3; ++k) { xkb[k] = xb[k] + c * vb[k]; xtb[k] = -c * vb[k]; }
+    contact_adjoint(*S, x, vwc.data(), a, tape, xkb.data(), xtb.data(), vwcb.data(), gE, gnu,
+                    gact ? gact + (size_t)st * S->nseg : nullptr);
     std::fill(bb.begin(), bb.end(), 0.0);
     for (int k = it - 1; k >= 0; --k) {
       const double* xk = &hist[(size_t)k * n3];
@@ -1105,9 +1266,10 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
     std::vector<double> qnb(n3);
     for (int i = 0; i < N; ++i)
       for (int cc = 0; cc < 3; ++cc) qnb[3 * i + cc] = xkb[3 * i + cc] + S->mass[i] * ih2 * bb[3 * i + cc];
+    /* q_n = x + h v_wc, v_wc = v + g h mask */
     for (int k = 0; k < n3; ++k) {
       xb[k] = xtb[k] + qnb[k];
-      vb[k] = S->h * qnb[k];
+      vb[k] = S->h * qnb[k] + vwcb[k];
     }
   }
   std::copy(xb.begin(), xb.end(), gx);

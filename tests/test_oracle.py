@@ -217,3 +217,45 @@ def test_adjoint_matches_central_differences(builder):
     for adj, fd, ip, im in checks:
         assert np.array_equal(ip, it0) and np.array_equal(im, it0), "iteration count changed under perturbation"
         assert abs(adj - fd) <= 1e-5 * max(1.0, abs(fd)), (adj, fd)
+
+
+@pytest.mark.parametrize("case", ["drop", "slide"])
+def test_contact_adjoint_matches_central_differences(case):
+    """The contact phase's reverse (Jacobi sweeps, friction cone, relaxation)
+    against central differences, on a box that lands on the ground during
+    the window (impacts and normals are constants of the tape); "slide" lands
+    with a tangential velocity, so the friction cone clamps."""
+    d = S.drop_box(mu=0.3)
+    o = O.OracleScene(d)
+    n = 3 if case == "drop" else 4
+    rng = np.random.default_rng(11)
+    x = d.x0.reshape(-1).copy()
+    v = d.initial_velocity.copy() if case == "drop" else np.tile([1.0, -1.0, 0.3], d.n_vertices)
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    _, it0 = _loss(o, x, v, gx, gv, n)
+    p0 = o.contact_passes()
+    assert p0.sum() > 0
+    g = o.backward(gx, gv)
+    eps = 1e-7
+    checks = []
+    for name in ("x", "v", "E"):
+        if name == "E":
+            E, nu = d.youngs.copy(), d.poisson.copy()
+            dE = rng.standard_normal(E.size) * E
+            o.set_materials(E + eps * dE, nu); lp, ip = _loss(o, x, v, gx, gv, n); pp = o.contact_passes()
+            o.set_materials(E - eps * dE, nu); lm, im = _loss(o, x, v, gx, gv, n); pm = o.contact_passes()
+            o.set_materials(E, nu)
+            checks.append((g["E"] @ dE, (lp - lm) / (2 * eps), ip, im, pp, pm))
+            continue
+        dz = rng.standard_normal(x.size)
+        if name == "x":
+            (lp, ip), pp = _loss(o, x + eps * dz, v, gx, gv, n), o.contact_passes()
+            (lm, im), pm = _loss(o, x - eps * dz, v, gx, gv, n), o.contact_passes()
+        else:
+            (lp, ip), pp = _loss(o, x, v + eps * dz, gx, gv, n), o.contact_passes()
+            (lm, im), pm = _loss(o, x, v - eps * dz, gx, gv, n), o.contact_passes()
+        checks.append((g[name] @ dz, (lp - lm) / (2 * eps), ip, im, pp, pm))
+    for adj, fd, ip, im, pp, pm in checks:
+        assert np.array_equal(ip, it0) and np.array_equal(im, it0)
+        assert np.array_equal(pp, p0) and np.array_equal(pm, p0)
+        assert abs(adj - fd) <= 1e-4 * max(1.0, abs(fd)), (adj, fd)
