@@ -42,15 +42,16 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--sim-steps", type=int, default=None,
                    help="time steps per gradient evaluation (60 / 100 are the workloads; fewer only for profiler captures)")
-    p.add_argument("--workload", default="inverse_stiffness", choices=["inverse_stiffness", "batch"],
-                   help="inverse_stiffness: one 12,800-tet scene; batch: 256 uneven scenes in one handle")
+    p.add_argument("--workload", default="inverse_stiffness", choices=["inverse_stiffness", "batch", "star"],
+                   help="inverse_stiffness: one 12,800-tet scene; batch: 256 uneven scenes in one handle; "
+                        "star: the muscle star on the ground, gradient w.r.t. all activations")
     p.add_argument("--scenes", type=int, default=256, help="batch workload: number of scenes")
     p.add_argument("--fp64-sample", type=int, default=-1,
                    help="batch workload: scenes stepped one at a time in FP64 for the plain-form rate "
                         "(-1: every scene of the batch, 0: skip)")
     a = p.parse_args()
     global SIM_STEPS
-    SIM_STEPS = a.sim_steps if a.sim_steps is not None else (100 if a.workload == "batch" else 60)
+    SIM_STEPS = a.sim_steps if a.sim_steps is not None else {"batch": 100, "star": 200}.get(a.workload, 60)
     return a
 
 
@@ -521,12 +522,108 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------- muscle star (C3) ---
+
+STAR_METRIC = "fwd+adjoint sim steps/s (muscle star 9,840 tets on the ground, 384 segments, K=15)"
+
+
+def run_star(args):
+    """Muscle star on a ground obstacle: 200 steps forward with random chain
+    activations, then the gradient of L = |x_200 - x_0|^2 with respect to every
+    segment activation of every step (contact phase included in the adjoint)."""
+    import torch
+    from diff_fem_b200 import scene as S
+    from diff_fem_b200._capi import DFEM_PREC_FP64, DFEM_PREC_MIXED
+    from diff_fem_b200.engine import Scene
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    prec = DFEM_PREC_FP64 if args.precision == "fp64" else DFEM_PREC_MIXED
+    d = S.muscle_star(refine=2, ground=True, mu=0.5, precision=prec)
+    sc = Scene(d, device=local)
+    n = SIM_STEPS
+    rng = np.random.default_rng(42)
+    chains = d.n_segments // 6
+    act_np = np.repeat(rng.uniform(0.0, 1.0, (n, chains)), 6, axis=1)  # one value per chain per step
+    act = torch.tensor(act_np, device=dev)
+    x0 = torch.tensor(d.x0.reshape(-1), device=dev)
+    v0 = torch.zeros_like(x0)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def grad_eval():
+        x, v = sc.forward(x0, v0, n_steps=n, act=act)
+        return x, sc.backward(2.0 * (x - x0), torch.zeros_like(x))
+
+    for _ in range(max(3, args.warmup)):
+        grad_eval()
+    torch.cuda.synchronize()
+    launches0 = sc.launch_count()
+    elapsed = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            xg, gg = grad_eval()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            elapsed += e0.elapsed_time(e1) / 1e3
+    launches = sc.launch_count() - launches0
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = world * n * args.steps / elapsed
+    passes = sc.contact_passes(n)
+    iters = sc.iterations(n)
+    # end to end with host buffers
+    x0_h, v0_h, act_h = x0.cpu().pin_memory(), v0.cpu().pin_memory(), act.cpu().pin_memory()
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        xh, vh = sc.forward(x0_h, v0_h, n_steps=n, act=act_h)
+        gh = sc.backward(2.0 * (xh - x0_h.numpy()), np.zeros_like(xh))
+        _ = float(np.sum(gh["act"]))
+    t_e2e = time.perf_counter() - t1
+    n3 = 3 * d.n_vertices
+    line = {"metric": STAR_METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": f"muscle star refine 2 ({d.n_tets} tets, {d.n_vertices} vertices), "
+                                   f"{chains} chains x 6 segments, ground quad mu=0.5, h=1/60, K=15, {n} steps, "
+                                   "activations U[0,1] per chain per step (seed 42), forward + adjoint dL/da",
+                       "precision": args.precision, "contact_steps": int((passes > 0).sum()),
+                       "contact_passes_total": int(passes.sum()), "pd_iterations_total": int(iters.sum()),
+                       "l2": "flushed between timed steps (256 MB write)"},
+            "e2e": {"value": world * n * args.steps / t_e2e, "unit": "steps/s",
+                    "h2d_bytes_per_step": 8 * (2 * n3 + n * d.n_segments + 2 * n3),
+                    "d2h_bytes_per_step": 8 * (2 * n3 + 2 * n3 + 2 * d.n_tets + n * d.n_segments)},
+            "grad_act_norm": float(torch.linalg.norm(gg["act"]).item()),
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sc.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "star":
+        run_star(args)
     else:
         run_ours(args)
 

@@ -15,7 +15,10 @@
 
 namespace dfem {
 
-enum { CS_MODE = 0, CS_PASS = 1, CS_IT = 2, CS_ANY = 3, CS_ACTIVE = 4, CS_BODIES = 5, CS_SIZE = 6 };
+// state words: [mode, pass, it, any, active, loop-body executions, computed
+// Jacobi iterations, the computed iteration whose x_n1 the current ori_x is]
+enum { CS_MODE = 0, CS_PASS = 1, CS_IT = 2, CS_ANY = 3, CS_ACTIVE = 4, CS_BODIES = 5, CS_COMP = 6, CS_SRC = 7,
+       CS_SIZE = 8 };
 
 // per-step record of the phase: [passes, loop-body executions]
 __global__ void k_contact_record(const int* step, const int* state, int* rec) {
@@ -204,6 +207,14 @@ __global__ void k_contact_prep(int N, ContactDev c, double* xk, double* partial,
     Vec3<double> dl = x - ld3(c.xold, i);
     e = fmax(fabs(dl.x), fmax(fabs(dl.y), fabs(dl.z)));
   }
+  // recording for the adjoint: the impact lists this iteration will use
+  const int comp = c.state[CS_COMP];
+  if (c.rec_on && *c.rec_on && i < c.nc && comp < c.rec_cap) {
+    const int cnt = c.imp_cnt[i];
+    c.rec_cnt[(size_t)comp * c.nc + i] = cnt;
+    for (int q = 0; q < cnt; ++q)
+      st3(c.rec_n, ((size_t)comp * c.nc + i) * kMaxImpactsPerVertex + q, ld3(c.imp_n, i * kMaxImpactsPerVertex + q));
+  }
   // deterministic grid max
   __shared__ double ws[32];
   __shared__ bool last;
@@ -226,6 +237,7 @@ __global__ void k_contact_prep(int N, ContactDev c, double* xk, double* partial,
     *counter = 0u;
     bool conv = m < kConvergenceEps;
     c.state[CS_ACTIVE] = conv ? 0 : 1;
+    c.state[CS_SRC] = c.state[CS_COMP];  // ori_x is the x_n1 of the last computed iteration
     if (conv) c.state[CS_MODE] = 0;  // back to detection
   }
 }
@@ -269,6 +281,12 @@ __global__ void k_contact_rhs(SceneDev d, ContactDev c, const double* __restrict
   st3(c.prev, i, prev);
   st3(c.xn1, i, ld3(xt, i) + (1.0 / (d.h * c.hdiag[i])) * prev);
   st3(c.xold, i, ld3(xk, i));
+  const int comp = c.state[CS_COMP];
+  if (c.rec_on && *c.rec_on && comp < c.rec_cap) {
+    st3(c.rec_x + (size_t)comp * 3 * d.N, i, ld3(xk, i));
+    st3(c.rec_prev + (size_t)comp * 3 * d.N, i, prev);
+    if (i == 0) c.rec_first[comp] = first ? 1 : 0;
+  }
 }
 
 // End of a Jacobi iteration: count it; after K iterations return to detection.
@@ -279,7 +297,160 @@ __global__ void k_contact_ctl_iter(ContactDev c, int K) {
   int it = c.state[CS_IT] + 1;
   c.state[CS_IT] = it;
   c.state[CS_ACTIVE] = 0;
+  if (c.rec_on && *c.rec_on && c.state[CS_COMP] >= c.rec_cap) atomicExch(c.status, 6);  // record too small
+  c.state[CS_COMP] += 1;
   if (it >= K) c.state[CS_MODE] = 0;
+}
+
+// ---- adjoint of the contact phase ------------------------------------------------
+//
+// Reverse of the recorded Jacobi iterations j = src .. 1 of one step (the
+// detection is discrete: impacts and normals are constants, as on the
+// reference's tape).  Per iteration, with rhs_pre = M v_wc + h (J d(ori) -
+// L x_t) - h C (ori - x_t), rhs_post its contact projection, prev_j =
+// alpha rhs_post + (1 - alpha) prev_{j-1} (prev_{j-1} := rhs_pre at the first
+// iteration of a pass) and x_n1 = x_t + prev_j / (h diag(Hs)):
+//   k_cadj_rhs    cotangents of prev, rhs_post, the projection, rhs_pre;
+//                 accumulates those of x_t, v_wc and diag(Hs)
+//   (k_local at ori, then k_cadj_local: VJP of J d, parameter terms)
+//   k_cadj_hs     the C and L x_t terms; x_n1 bar of the previous iteration
+// Buffers: xn1b (x_n1 bar), pb (prev bar), hdb (diag(Hs) bar), cxtb (x_t bar),
+// vwcb (v_wc bar), yb = h rhs_pre bar.
+
+struct ContactAdj {
+  double* xn1b;
+  double* pb;
+  double* hdb;
+  double* cxtb;
+  double* vwcb;
+  double* yb;
+  double* orib;
+};
+
+__global__ void k_cadj_start(int N, double cv, double* io_a, double* io_b, ContactAdj a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const Vec3<double> gv = ld3(io_b, i);
+  st3(a.xn1b, i, ld3(io_a, i) + cv * gv);  // v' = damping (x' - x_t)/h
+  st3(a.cxtb, i, (-cv) * gv);
+  st3(a.vwcb, i, mk3(0.0, 0.0, 0.0));
+  st3(a.pb, i, mk3(0.0, 0.0, 0.0));
+  a.hdb[i] = 0.0;
+}
+
+// slot: J d at ori (k_local); xt: the step's start positions; ori, prev: the
+// recorded iteration j; first: whether it began its pass; rcnt / rn: its impacts.
+__global__ void k_cadj_rhs(SceneDev d, ContactDev c, ContactAdj a, const double* __restrict__ slot,
+                           const double* __restrict__ xt, const double* __restrict__ ori,
+                           const double* __restrict__ prev, int first, const int* __restrict__ rcnt,
+                           const double* __restrict__ rn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  const double hd = c.hdiag[i];
+  const Vec3<double> xb = ld3(a.xn1b, i), pv = ld3(prev, i);
+  st3(a.cxtb, i, ld3(a.cxtb, i) + xb);
+  a.hdb[i] -= dot3(xb, pv) / (d.h * hd * hd);
+  const Vec3<double> ptot = ld3(a.pb, i) + (1.0 / (d.h * hd)) * xb;
+  Vec3<double> rb = c.alpha * ptot;
+  const int ac = c.cidx[i];
+  if (ac >= 0 && rcnt[ac] > 0) {
+    // rhs_pre of the contact vertex, as in k_contact_rhs
+    Vec3<double> jd = ld3(d.attach_jd, i);
+    for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) jd = jd + ld3(slot, k);
+    Vec3<double> cdx = mk3(0.0, 0.0, 0.0);
+    for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) {
+      const int j = d.hs_col[k];
+      if (j != i) cdx = cdx + d.hs_val[k] * (ld3(ori, j) - ld3(xt, j));
+    }
+    const Vec3<double> f = d.mass[i] * ld3(c.vwc, i) + d.h * (jd - ld3(c.lxt, i)) - d.h * cdx;
+    Vec3<double> W[3];
+    bool hit = false;
+    double r0 = 0, r1 = 0, r2 = 0;
+    for (int q = 0; q < rcnt[ac]; ++q) {
+      Vec3<double> B[3];
+      contact_basis(ld3(rn, ac * kMaxImpactsPerVertex + q), B);
+      const double f0 = dot3(B[0], f);
+      if (f0 > 0) continue;
+      hit = true;
+      W[0] = B[0]; W[1] = B[1]; W[2] = B[2];
+      r0 = -f0; r1 = -dot3(B[1], f); r2 = -dot3(B[2], f);
+    }
+    if (hit) {  // rhs_post = r0 W0 + r1' W1 + r2' W2 (friction cone clamp)
+      const double b0 = dot3(W[0], rb), b1 = dot3(W[1], rb), b2 = dot3(W[2], rb);
+      const double rt = sqrt(r1 * r1 + r2 * r2);
+      double g0 = b0, g1 = b1, g2 = b2;
+      if (rt > c.mu * r0) {
+        g0 = b0 + c.mu * (r1 * b1 + r2 * b2) / rt;
+        g1 = c.mu * r0 * (r2 * r2 * b1 - r1 * r2 * b2) / (rt * rt * rt);
+        g2 = c.mu * r0 * (r1 * r1 * b2 - r1 * r2 * b1) / (rt * rt * rt);
+      }
+      rb = (-1.0) * (g0 * W[0] + g1 * W[1] + g2 * W[2]);
+    }
+  }
+  if (first) {
+    rb = rb + (1.0 - c.alpha) * ptot;
+    st3(a.pb, i, mk3(0.0, 0.0, 0.0));
+  } else {
+    st3(a.pb, i, (1.0 - c.alpha) * ptot);
+  }
+  st3(a.vwcb, i, ld3(a.vwcb, i) + d.mass[i] * rb);
+  st3(a.yb, i, d.h * rb);
+}
+
+// VJP of J d at ori with cotangent yb, and the Hs terms of the tets' E gradient
+__global__ void __launch_bounds__(128) k_cadj_local(SceneDev d, ContactAdj a, const double* __restrict__ ori,
+                                                    const double* __restrict__ xt, const double* __restrict__ act_all,
+                                                    const int* step, double* __restrict__ slot, double* gE,
+                                                    double* gnu, double* mg) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  adj_local_item(d, t, ori, a.yb, act_all + (size_t)(*step) * d.nseg, slot, gE, gnu, mg, nullptr, xt);
+}
+
+// orib = (sum of the slots) - C^T yb; x_t bar += (M/h^2 - Hs_ii) yb_i; the
+// result is the x_n1 bar of the previous computed iteration
+__global__ void k_cadj_hs(SceneDev d, ContactAdj a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  Vec3<double> o = ld3(a.orib, i);
+  double hii = 0.0;
+  for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) {
+    const int j = d.hs_col[k];
+    if (j != i) o = o - d.hs_val[k] * ld3(a.yb, j);
+    else hii = d.hs_val[k];
+  }
+  st3(a.cxtb, i, ld3(a.cxtb, i) + (d.mass[i] / (d.h * d.h) - hii) * ld3(a.yb, i));
+  st3(a.xn1b, i, o);
+}
+
+// after the reverse sweep: the diag(Hs) terms of the tets' E gradient
+__global__ void k_cadj_hd(SceneDev d, ContactAdj a, double* gE) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.T || !gE) return;
+  int4 v = d.tv[t];
+  const int vi[4] = {v.x, v.y, v.z, v.w};
+  double G[4][3];
+  load_g(d.tinv, d.T, t, G);
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) s += (G[q][0] * G[q][0] + G[q][1] * G[q][1] + G[q][2] * G[q][2]) * a.hdb[vi[q]];
+  gE[t] += d.tvol[t] * s;
+}
+
+// the PD part's input cotangent is the phase's input cotangent; the step's
+// own v' term went to x_t bar
+__global__ void k_cadj_to_pd(int N, ContactAdj a, double* io_a, double* io_b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  st3(io_a, i, ld3(a.xn1b, i));
+  st3(io_b, i, mk3(0.0, 0.0, 0.0));
+}
+
+// after the PD adjoint: add the contact phase's x_t and v_wc (= v) cotangents
+__global__ void k_cadj_finish(int N, ContactAdj a, double* io_a, double* io_b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  st3(io_a, i, ld3(io_a, i) + ld3(a.cxtb, i));
+  st3(io_b, i, ld3(io_b, i) + ld3(a.vwcb, i));
 }
 
 }  // namespace dfem

@@ -133,6 +133,10 @@ struct dfem_scene {
   bool has_contact = false;
   DBuf<int> cverts, cidx, obs_f, imp_cnt, imp_face, cstate, cpasses;
   DBuf<double> obs_x, hdiag, imp_n, xn1, xold, cprev, lxt, vwc;
+  // adjoint of the contact phase: the record of one step's Jacobi iterations and the reverse sweep's buffers
+  DBuf<int> crec_on, crec_first, crec_cnt;
+  DBuf<double> crec_x, crec_prev, crec_n, ca_xn1b, ca_pb, ca_hdb, ca_cxtb, ca_vwcb, ca_yb, ca_orib;
+  int crec_cap = 0;
   ContactDev cd{};
   std::vector<int> rec_passes;
   // graphs
@@ -571,9 +575,12 @@ static int upload_scene(dfem_scene* sc) {
     CK(sc->xn1.alloc(n3)); CK(sc->xold.alloc(n3)); CK(sc->cprev.alloc(n3)); CK(sc->lxt.alloc(n3)); CK(sc->vwc.alloc(n3));
     CK(sc->cstate.alloc(CS_SIZE));
     CK(cudaMemset(sc->cstate.p, 0, sizeof(int) * CS_SIZE));
+    CK(sc->crec_on.alloc(1));
+    CK(cudaMemset(sc->crec_on.p, 0, sizeof(int)));
     sc->cd = ContactDev{nc, nof, s.K, kMaxContactPasses, s.alpha, s.mu_obs, sc->cverts.p, sc->cidx.p, sc->obs_x.p,
                         sc->obs_f.p, sc->hdiag.p, sc->imp_cnt.p, sc->imp_face.p, sc->imp_n.p, sc->xn1.p, sc->xold.p,
-                        sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p};
+                        sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p, sc->crec_on.p, 0, nullptr, nullptr,
+                        nullptr, nullptr, nullptr, sc->status.p};
   }
   refresh_scene_view(sc);
   return DFEM_OK;
@@ -852,6 +859,76 @@ static int copy_out(dfem_scene* sc, const double* src, size_t n, double* dst, in
   return DFEM_OK;
 }
 
+// Record of the contact phase for its adjoint: room for `cap` computed Jacobi
+// iterations of one step (the graphs hold the record's pointers: rebuilt when
+// it grows).
+static int ensure_contact_record(dfem_scene* sc, int cap) {
+  if (!sc->has_contact || cap <= sc->crec_cap) return DFEM_OK;
+  const HostScene& s = sc->hs;
+  const size_t n3 = 3 * (size_t)s.N, nc = (size_t)sc->cd.nc;
+  CK(sc->crec_x.alloc(n3 * cap));
+  CK(sc->crec_prev.alloc(n3 * cap));
+  CK(sc->crec_first.alloc(cap));
+  CK(sc->crec_cnt.alloc(nc * cap));
+  CK(sc->crec_n.alloc(nc * cap * kMaxImpactsPerVertex * 3));
+  for (DBuf<double>* b : {&sc->ca_xn1b, &sc->ca_pb, &sc->ca_cxtb, &sc->ca_vwcb, &sc->ca_yb, &sc->ca_orib})
+    if (!b->p) CK(b->alloc(n3));
+  if (!sc->ca_hdb.p) CK(sc->ca_hdb.alloc(std::max(1, s.N)));
+  sc->crec_cap = cap;
+  sc->cd.rec_cap = cap;
+  sc->cd.rec_x = sc->crec_x.p;
+  sc->cd.rec_prev = sc->crec_prev.p;
+  sc->cd.rec_first = sc->crec_first.p;
+  sc->cd.rec_cnt = sc->crec_cnt.p;
+  sc->cd.rec_n = sc->crec_n.p;
+  invalidate_graphs(sc);
+  return DFEM_OK;
+}
+
+// Reverse of step st's contact phase, after the step graph re-ran it with
+// recording on.  In: io_a / io_b = cotangents of the step's x' and v'.  Out:
+// io_a = cotangent of the PD result (io_b = 0); the x_t and v_wc cotangents
+// wait in ca_cxtb / ca_vwcb for k_cadj_finish after the PD adjoint.
+static int contact_adjoint_step(dfem_scene* sc, int st) {
+  const HostScene& s = sc->hs;
+  const size_t n3 = 3 * (size_t)s.N;
+  const int nb = sc->nblk_v, ncons = s.T + s.M + s.S + s.B;
+  int meta[CS_SIZE];
+  CK(cudaMemcpyAsync(meta, sc->cstate.p, sizeof(meta), cudaMemcpyDeviceToHost, sc->stream));
+  CK(cudaStreamSynchronize(sc->stream));
+  const int src = meta[CS_SRC];
+  if (meta[CS_COMP] > sc->crec_cap) return fail(DFEM_ERR_CAP, "contact record too small for the recomputed step");
+  std::vector<int> first(std::max(1, src));
+  if (src > 0) CK(cudaMemcpy(first.data(), sc->crec_first.p, src * sizeof(int), cudaMemcpyDeviceToHost));
+  const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
+  const double* xt = sc->ckpt_x.p + (size_t)st * n3;
+  k_cadj_start<<<nb, 128, 0, sc->stream>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, a);
+  int launches = 1;
+  for (int j = src; j >= 1; --j) {
+    const double* ori = sc->crec_x.p + (size_t)(j - 1) * n3;
+    const double* prev = sc->crec_prev.p + (size_t)(j - 1) * n3;
+    const int* rcnt = sc->crec_cnt.p + (size_t)(j - 1) * sc->cd.nc;
+    const double* rn = sc->crec_n.p + (size_t)(j - 1) * sc->cd.nc * kMaxImpactsPerVertex * 3;
+    if (ncons > 0)
+      k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, kOpen, ori, sc->act_all.p, sc->step.p, sc->slot.p);
+    k_cadj_rhs<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->cd, a, sc->slot.p, xt, ori, prev, first[j - 1], rcnt, rn);
+    if (ncons > 0)
+      k_cadj_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, ori, xt, sc->act_all.p, sc->step.p,
+                                                                sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+    k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
+    if (s.nseg > 0)
+      k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, kOpen, sc->seg_part.p, sc->step.p,
+                                                                sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
+    k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a);
+    launches += 4 + (ncons > 0 ? 2 : 0) + (s.nseg > 0 ? 1 : 0);
+  }
+  if (s.T > 0) k_cadj_hd<<<(s.T + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, sc->gE.p);
+  k_cadj_to_pd<<<nb, 128, 0, sc->stream>>>(s.N, a, sc->io_a.p, sc->io_b.p);
+  CK(cudaGetLastError());
+  sc->launches += launches + 2;
+  return DFEM_OK;
+}
+
 // The device status word: [code, supernode, solve (1 forward / 2 backward), blocks that gave up].
 static int status_error(const int st4[4]) {
   if (st4[0] == DFEM_ERR_CAP && st4[2] > 0)
@@ -1089,6 +1166,7 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, traj_x ? 1 : 0);
   CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
   reset_solve_state(sc);
+  if (sc->has_contact) CK(cudaMemsetAsync(sc->crec_on.p, 0, sizeof(int), sc->stream));  // no recording here
   CK(cudaGetLastError());
   RC(ensure_graphs(sc));
   for (int st = 0; st < n_steps; ++st) CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
@@ -1122,10 +1200,15 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
                        double* g_youngs, double* g_poisson, double* g_act, int mem) {
   if (!sc || !gx_out || !gv_out || !gx || !gv) return fail(DFEM_ERR_INVALID, "null argument");
   if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_step_backward needs a preceding dfem_step_forward");
-  for (int st = 0; st < sc->rec_steps && 2 * st < (int)sc->rec_passes.size(); ++st)
-    if (sc->rec_passes[2 * st] > 0)
-      return fail(DFEM_ERR_STATE, "the recorded forward call had obstacle contacts; the adjoint of the contact phase is not available");
   CK(cudaSetDevice(sc->device));
+  // the contact phase's record: room for the most loop-body executions of any recorded step
+  int ccap = 0;
+  bool any_contact = false;
+  for (int st = 0; st < sc->rec_steps && 2 * st + 1 < (int)sc->rec_passes.size(); ++st) {
+    any_contact = any_contact || sc->rec_passes[2 * st] > 0;
+    ccap = std::max(ccap, sc->rec_passes[2 * st + 1]);
+  }
+  if (any_contact) RC(ensure_contact_record(sc, std::max(1, ccap)));
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N;
   const int nb = sc->nblk_v;
@@ -1141,6 +1224,7 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
   reset_solve_state(sc);
   RC(ensure_graphs(sc));
+  if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 1);
   for (int st = sc->rec_steps - 1; st >= 0; --st) {
     // recompute the step's iterates from its checkpoint (the step graph re-records the same checkpoint)
     CK(cudaMemcpyAsync(sc->xt.p, sc->ckpt_x.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
@@ -1148,8 +1232,16 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
     k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
     CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
     k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
+    const bool contact_step = sc->has_contact && sc->rec_passes[2 * st] > 0;
+    if (contact_step) RC(contact_adjoint_step(sc, st));
     CK(cudaGraphLaunch(sc->g_adj.exec, sc->stream));
+    if (contact_step) {
+      const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
+      k_cadj_finish<<<nb, 128, 0, sc->stream>>>(s.N, a, sc->io_a.p, sc->io_b.p);
+      sc->launches += 1;
+    }
   }
+  if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 0);
   sc->launches += 5;
   for (int st = 0; st < sc->rec_steps && st < (int)sc->rec_iters.size(); ++st)
     sc->launches += (int64_t)(2 + sc->g_step.outside + sc->g_adj.outside +

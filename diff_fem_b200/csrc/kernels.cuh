@@ -138,7 +138,16 @@ struct ContactDev {
   double* prev;           // 3N: relaxed rhs
   double* lxt;            // 3N: L x_t
   double* vwc;            // 3N: v + g h of the step
-  int* state;             // [mode, pass, it, any, active]
+  int* state;             // see CS_* in contact_kernels.cuh
+  // recording for the adjoint (written only while *rec_on != 0)
+  const int* rec_on;
+  int rec_cap;            // computed iterations the record holds
+  double* rec_x;          // rec_cap x 3N: each computed iteration's input ori_x
+  double* rec_prev;       // rec_cap x 3N: its relaxed rhs after the update
+  int* rec_first;         // rec_cap: whether it began its pass
+  int* rec_cnt;           // rec_cap x nc: impacts per contact vertex
+  double* rec_n;          // rec_cap x nc x kMax x 3: their normals
+  int* status;
 };
 
 struct FactorDev {

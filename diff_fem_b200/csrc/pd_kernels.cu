@@ -759,32 +759,44 @@ __global__ void k_adj_begin(int N, double c, const double* gx1, const double* gv
   st3(bb, i, mk3(0.0, 0.0, 0.0));
 }
 
-__global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const int* kptr, const int* step,
-                                                   const double* __restrict__ hist, const double* __restrict__ yb,
-                                                   double* bb, const double* __restrict__ act_all,
-                                                   double* __restrict__ slot, double* gE, double* gnu, double* mg) {
-  const int k = *kptr;
-  const double* x = hist + (size_t)k * 3 * d.N;
-  const double* x1 = hist + (size_t)(k + 1) * 3 * d.N;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < d.N && !gate.skip(vpart_of(d, t))) {  // bbar += ybar (b = M/h^2 q_n enters every iteration)
-    st3(bb, t, ld3(bb, t) + ld3(yb, t));
-  }
-  if (gate.skip(cons_part(d, t))) return;
+// VJP of constraint t's J d at positions x with cotangent yb: writes the
+// constraint's slot contributions to xbar and accumulates the parameter
+// gradients of J d.  The tets' E-gradient also takes the Hs term of the map
+// that consumed J d: PD iteration (x1 != null): -vol (G G^T) : (yb x1^T),
+// x1 the next iterate; contact rhs (xt != null): -vol (G G^T) : (yb z^T) with
+// z = x off the diagonal and x_t on it (rhs = ... - h C (x - x_t) - h L x_t).
+__device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const double* __restrict__ x,
+                                               const double* __restrict__ yb, const double* __restrict__ act_row,
+                                               double* __restrict__ slot, double* gE, double* gnu, double* mg,
+                                               const double* __restrict__ x1, const double* __restrict__ xt) {
   if (t < d.T) {
     int4 v = d.tv[t];
     const int vi[4] = {v.x, v.y, v.z, v.w};
-    Vec3<double> xv[4], yv[4], x1v[4];
+    Vec3<double> xv[4], yv[4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) { xv[a] = ld3(x, vi[a]); yv[a] = ld3(yb, vi[a]); x1v[a] = ld3(x1, vi[a]); }
+    for (int a = 0; a < 4; ++a) { xv[a] = ld3(x, vi[a]); yv[a] = ld3(yb, vi[a]); }
     double G[4][3];
     load_g(d.tinv, d.T, t, G);
-    Mat3<double> F = deformation(G, xv), F1 = deformation(G, x1v), Y = deformation(G, yv), md, mdv;
+    Mat3<double> F = deformation(G, xv), Y = deformation(G, yv), md, mdv;
     corot_project(F, md, mdv);
     double E = d.tE[t], nu = d.tnu[t], vol = d.tvol[t];
     double yr = 0, yvv = 0, yh = 0;
 #pragma unroll
-    for (int j = 0; j < 3; ++j) { yr += dot3(Y.c[j], md.c[j]); yvv += dot3(Y.c[j], mdv.c[j]); yh += dot3(Y.c[j], F1.c[j]); }
+    for (int j = 0; j < 3; ++j) { yr += dot3(Y.c[j], md.c[j]); yvv += dot3(Y.c[j], mdv.c[j]); }
+    if (x1) {
+      Vec3<double> x1v[4] = {ld3(x1, vi[0]), ld3(x1, vi[1]), ld3(x1, vi[2]), ld3(x1, vi[3])};
+      Mat3<double> F1 = deformation(G, x1v);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) yh += dot3(Y.c[j], F1.c[j]);
+    } else if (xt) {
+#pragma unroll
+      for (int j = 0; j < 3; ++j) yh += dot3(Y.c[j], F.c[j]);
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const double gaa = G[a][0] * G[a][0] + G[a][1] * G[a][1] + G[a][2] * G[a][2];
+        yh += gaa * dot3(yv[a], ld3(xt, vi[a]) - xv[a]);
+      }
+    }
     double opn = 1.0 + nu;
     if (gE) gE[t] += vol / opn * (yr + nu * yvv) - vol * yh;
     if (gnu) gnu[t] += E * vol / (opn * opn) * (yvv - yr);
@@ -815,7 +827,7 @@ __global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const 
       db = db + (w * c[a]) * ld3(yb, vi[a]);
       Ff = Ff + c[a] * ld3(x, vi[a]);
     }
-    double a_act = act_all[(size_t)(*step) * d.nseg + d.mseg[t]];
+    double a_act = act_row[d.mseg[t]];
     mg[t] = -dot3(db, Ff);
     int4 sl = d.mslot[t];
     const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
@@ -854,6 +866,21 @@ __global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const 
     }
     for (int q = o0; q < o1; ++q) st3(slot, d.bslot[q], d.bbeta[q] * gl);
   }
+}
+
+// Reverse PD iteration k (k read from device memory): local VJP at x^k with
+// the Hs term of x^{k+1}, and bbar += ybar (b = M/h^2 q_n enters every iteration).
+__global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const int* kptr, const int* step,
+                                                   const double* __restrict__ hist, const double* __restrict__ yb,
+                                                   double* bb, const double* __restrict__ act_all,
+                                                   double* __restrict__ slot, double* gE, double* gnu, double* mg) {
+  const int k = *kptr;
+  const double* x = hist + (size_t)k * 3 * d.N;
+  const double* x1 = hist + (size_t)(k + 1) * 3 * d.N;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < d.N && !gate.skip(vpart_of(d, t))) st3(bb, t, ld3(bb, t) + ld3(yb, t));
+  if (gate.skip(cons_part(d, t))) return;
+  adj_local_item(d, t, x, yb, act_all + (size_t)(*step) * d.nseg, slot, gE, gnu, mg, x1, nullptr);
 }
 
 // xbar^k = sum of the slots (constraints without x dependence contribute nothing)

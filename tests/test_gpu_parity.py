@@ -125,10 +125,30 @@ def test_obstacle_contact_forward(mu):
     assert o.contact_passes().sum() > 0
     assert np.array_equal(g.iterations(n), ro["iters"])
     assert rel(tg, ro["traj"]) < POS_TOL
-    # backward through contact is refused explicitly rather than silently wrong
-    with pytest.raises(_capi.DfemError) as e:
-        g.backward(np.ones_like(xg), np.zeros_like(vg))
-    assert e.value.code == 5
+
+
+@pytest.mark.parametrize("case", ["drop", "slide"])
+def test_obstacle_contact_adjoint(case):
+    """Adjoint through the contact phase (Jacobi sweeps, friction cone,
+    relaxation) against the oracle's restatement: x, v, E, nu gradients.
+    "slide" lands with a tangential velocity, so the friction cone clamps."""
+    d = S.drop_box(mu=0.3)
+    n = 6
+    x = d.x0.reshape(-1).copy()
+    v = d.initial_velocity.copy() if case == "drop" else np.tile([1.0, -1.0, 0.3], d.n_vertices)
+    g = Scene(d)
+    o = O.OracleScene(d)
+    xg, vg = g.forward(x, v, n_steps=n)
+    o.forward(x, v, n_steps=n)
+    assert g.contact_passes(n).sum() > 0
+    rng = np.random.default_rng(7)
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    bg, bo = g.backward(gx, gv), o.backward(gx, gv)
+    for k in ("x", "v", "E", "nu"):
+        assert rel(bg[k], bo[k]) < GRAD_TOL, (k, rel(bg[k], bo[k]))
+    # a second backward of the same forward gives the same result
+    bg2 = g.backward(gx, gv)
+    assert np.array_equal(bg["x"], bg2["x"]) and np.array_equal(bg["E"], bg2["E"])
 
 
 @pytest.mark.parametrize("builder", ["cantilever", "muscle_beam", "cloth_sheet"])
@@ -163,3 +183,22 @@ def test_nonfinite_input_reports_status():
     # the context stays usable
     xg, _ = g.forward(d.x0.reshape(-1).copy(), np.zeros_like(x), n_steps=1)
     assert np.all(np.isfinite(xg))
+
+
+def test_muscle_star_on_ground_forward_and_adjoint():
+    """The muscle star resting on its ground quad: activations drive the arms,
+    the contact phase runs every step, and the activation gradient flows
+    through it."""
+    d = S.muscle_star(refine=1, ground=True, mu=0.5)
+    n = 4
+    act = np.repeat(np.random.default_rng(42).uniform(0, 1, (n, d.n_segments // 6)), 6, axis=1)
+    g, o, (xg, vg, tg), ro = run_both(d, n, act=act)
+    assert g.contact_passes(n).sum() > 0
+    assert np.array_equal(g.contact_passes(n), o.contact_passes())
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    rng = np.random.default_rng(9)
+    gx, gv = rng.standard_normal(xg.size), rng.standard_normal(xg.size)
+    bg, bo = g.backward(gx, gv), o.backward(gx, gv)
+    for k in ("x", "v", "E", "act"):
+        assert rel(bg[k], bo[k]) < GRAD_TOL, (k, rel(bg[k], bo[k]))
