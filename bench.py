@@ -42,16 +42,17 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--sim-steps", type=int, default=None,
                    help="time steps per gradient evaluation (60 / 100 are the workloads; fewer only for profiler captures)")
-    p.add_argument("--workload", default="inverse_stiffness", choices=["inverse_stiffness", "batch", "star"],
+    p.add_argument("--workload", default="inverse_stiffness", choices=["inverse_stiffness", "batch", "star", "cloth_ball"],
                    help="inverse_stiffness: one 12,800-tet scene; batch: 256 uneven scenes in one handle; "
-                        "star: the muscle star on the ground, gradient w.r.t. all activations")
+                        "star: the muscle star on the ground, gradient w.r.t. all activations; "
+                        "cloth_ball: a 64x64 cloth dropped on a ball, gradient w.r.t. the initial velocities")
     p.add_argument("--scenes", type=int, default=256, help="batch workload: number of scenes")
     p.add_argument("--fp64-sample", type=int, default=-1,
                    help="batch workload: scenes stepped one at a time in FP64 for the plain-form rate "
                         "(-1: every scene of the batch, 0: skip)")
     a = p.parse_args()
     global SIM_STEPS
-    SIM_STEPS = a.sim_steps if a.sim_steps is not None else {"batch": 100, "star": 200}.get(a.workload, 60)
+    SIM_STEPS = a.sim_steps if a.sim_steps is not None else {"batch": 100, "star": 200, "cloth_ball": 300}.get(a.workload, 60)
     return a
 
 
@@ -527,6 +528,97 @@ def run_batch(args):
 STAR_METRIC = "fwd+adjoint sim steps/s (muscle star 9,840 tets on the ground, 384 segments, K=15)"
 
 
+def run_contact_workload(args, d, metric, workload, act_np=None, grad_key="act"):
+    """One scene with contact: n steps forward, then the adjoint of
+    L = |x_n - x_0|^2 (the gradient of interest: grad_key)."""
+    import torch
+    from diff_fem_b200.engine import Scene
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    sc = Scene(d, device=local)
+    n = SIM_STEPS
+    act = torch.tensor(act_np, device=dev) if act_np is not None else None
+    x0 = torch.tensor(d.x0.reshape(-1), device=dev)
+    v0 = torch.zeros_like(x0)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def grad_eval():
+        x, v = sc.forward(x0, v0, n_steps=n, act=act)
+        return x, sc.backward(2.0 * (x - x0), torch.zeros_like(x))
+
+    for _ in range(max(3, args.warmup)):
+        grad_eval()
+    torch.cuda.synchronize()
+    launches0 = sc.launch_count()
+    elapsed = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            xg, gg = grad_eval()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            elapsed += e0.elapsed_time(e1) / 1e3
+    launches = sc.launch_count() - launches0
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = world * n * args.steps / elapsed
+    passes = sc.contact_passes(n)
+    iters = sc.iterations(n)
+    x0_h, v0_h = x0.cpu().pin_memory(), v0.cpu().pin_memory()
+    act_h = act.cpu().pin_memory() if act is not None else None
+    t1 = time.perf_counter()
+    for _ in range(args.steps):
+        xh, vh = sc.forward(x0_h, v0_h, n_steps=n, act=act_h)
+        gh = sc.backward(2.0 * (xh - x0_h.numpy()), np.zeros_like(xh))
+        _ = float(np.sum(gh[grad_key]))
+    t_e2e = time.perf_counter() - t1
+    n3 = 3 * d.n_vertices
+    nact = 0 if act_np is None else act_np.size
+    line = {"metric": metric, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": workload, "precision": args.precision, "contact_steps": int((passes > 0).sum()),
+                       "contact_passes_total": int(passes.sum()), "pd_iterations_total": int(iters.sum()),
+                       "solve": sc.solve_mode(), "l2": "flushed between timed steps (256 MB write)"},
+            "e2e": {"value": world * n * args.steps / t_e2e, "unit": "steps/s",
+                    "h2d_bytes_per_step": 8 * (2 * n3 + nact + 2 * n3),
+                    "d2h_bytes_per_step": 8 * (2 * n3 + 2 * n3 + 2 * d.n_tets + nact)},
+            "grad_norm": float(torch.linalg.norm(gg[grad_key]).item()),
+            "gpu_launches": launches, "clocks": clk.summary()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sc.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_cloth_ball(args):
+    from diff_fem_b200 import scene as S
+    from diff_fem_b200._capi import DFEM_PREC_FP64, DFEM_PREC_MIXED
+    prec = DFEM_PREC_FP64 if args.precision == "fp64" else DFEM_PREC_MIXED
+    d = S.cloth_on_ball(precision=prec)
+    run_contact_workload(args, d, "fwd+adjoint sim steps/s (64x64 cloth on a ball, K=20)",
+                         f"cloth 64x64 (4,096 vertices, 12,033 springs, 3,844 bending stencils), membrane 1e3, "
+                         f"bending 1e-3, 0.2 kg/m^2, dropped 0.3 m onto a static ball r=0.2 ({len(d.obstacle_faces) - 2} "
+                         f"faces) above a ground quad, mu=0.3, h=1/120, K=20, {SIM_STEPS} steps, forward + adjoint dL/dv0",
+                         grad_key="v")
+
+
 def run_star(args):
     """Muscle star on a ground obstacle: 200 steps forward with random chain
     activations, then the gradient of L = |x_200 - x_0|^2 with respect to every
@@ -624,6 +716,8 @@ def main():
         run_batch(args)
     elif args.workload == "star":
         run_star(args)
+    elif args.workload == "cloth_ball":
+        run_cloth_ball(args)
     else:
         run_ours(args)
 

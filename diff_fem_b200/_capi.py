@@ -81,6 +81,7 @@ SIGNATURES = [
     ("dfem_solve_mode", C.c_int, [_VP, C.c_int32, _pi, C.POINTER(C.c_double)]),
     ("dfem_profile_levels", C.c_int, [_VP, C.c_int32, C.c_int32, _pi, C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), _pi, _pi, _pi]),
+    ("dfem_set_adjoint_budget", C.c_int, [_VP, C.c_int64]),
     ("dfem_get_launch_count", C.c_int, [_VP, C.POINTER(C.c_int64)]),
     ("dfem_profile_phases", C.c_int, [_VP, C.c_int32, C.POINTER(C.c_double)]),
     ("dfem_synchronize", C.c_int, [_VP]),

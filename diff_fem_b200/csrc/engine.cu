@@ -127,6 +127,11 @@ struct dfem_scene {
   DBuf<double> act_all, act_cur;   // per-step activations; current activations
   DBuf<double> ckpt_x, ckpt_v, traj;
   int cap_steps = 0;
+  // iterates of the last forward call: of every step when they fit the budget
+  // (the adjoint then replays no step without contact), else of one step
+  // (every step is recomputed from its checkpoint)
+  long long hist_step = 0;
+  size_t adj_budget = 0;  // set at creation: a quarter of the device memory
   // adjoint
   DBuf<double> xkb, xtb, bb, gE, gnu, mg, gact;
   // obstacle contact phase
@@ -519,7 +524,6 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->xt.alloc(n3)); CK(sc->vt.alloc(n3)); CK(sc->qn.alloc(n3)); CK(sc->c0.alloc(n3));
   CK(sc->xk.alloc(n3)); CK(sc->rhs.alloc(n3)); CK(sc->y.alloc(n3)); CK(sc->io_a.alloc(n3)); CK(sc->io_b.alloc(n3));
   CK(sc->slot.alloc(3 * (size_t)std::max(1, s.nslots)));
-  CK(sc->hist.alloc(n3 * (size_t)(s.K + 1)));
   CK(sc->xkb.alloc(n3)); CK(sc->xtb.alloc(n3)); CK(sc->bb.alloc(n3));
   CK(sc->gE.alloc(std::max(1, s.T))); CK(sc->gnu.alloc(std::max(1, s.T))); CK(sc->mg.alloc(std::max(1, s.M)));
   sc->nblk_v = (s.N + 127) / 128;
@@ -598,6 +602,10 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   CK(sc->act_all.alloc((size_t)cap * std::max(1, s.nseg)));
   CK(sc->gact.alloc((size_t)cap * std::max(1, s.nseg)));
   CK(sc->cpasses.alloc(2 * (size_t)cap));
+  const size_t rec = n3 * (size_t)(s.K + 1);
+  const bool all = rec * (size_t)cap * sizeof(double) <= sc->adj_budget;
+  CK(sc->hist.alloc(all ? rec * cap : rec));
+  sc->hist_step = all ? (long long)rec : 0;
   CK(cudaMemset(sc->cpasses.p, 0, sizeof(int) * 2 * (size_t)cap));
   sc->cap_steps = cap;
   invalidate_graphs(sc);  // graphs hold the old pointers
@@ -677,14 +685,15 @@ static void launch_gather(dfem_scene* sc, cudaStream_t st, Gate g, const double*
     k_gather<<<sc->nblk_v, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
 }
 
-// The adjoint of the local step runs in FP64 in both forms: its parameter
-// terms Y:(md - F) cancel down to the size of the strain, which FP32 rounding
-// of md and F (1e-7 of their size) would swamp.
+// The adjoint of the local step runs in FP64 in both forms.  (An FP32 VJP with
+// the parameter terms taken from the rotated-frame deviations md - F cut the
+// adjoint local step from 1.14 to 0.73 ms on the 256-scene batch, 1.5 % of the
+// batch step, but raised the activation-gradient error from 2e-7 to 1.5e-4.)
 static void launch_adj_local(dfem_scene* sc, cudaStream_t st, Gate g, const int* kptr) {
   const HostScene& s = sc->hs;
   const int nthr = std::max(s.T + s.M + s.S + s.B, s.N);
-  k_adj_local<<<(nthr + 127) / 128, 128, 0, st>>>(sc->sd, g, kptr, sc->step.p, sc->hist.p, sc->y.p, sc->bb.p,
-                                                   sc->act_all.p, sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+  k_adj_local<<<(nthr + 127) / 128, 128, 0, st>>>(sc->sd, g, kptr, sc->step.p, sc->hist.p, sc->hist_step, sc->y.p, sc->bb.p,
+                                            sc->act_all.p, sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
 }
 
 static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
@@ -693,7 +702,7 @@ static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
 
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   k_step_begin<<<sc->nblk_p, kPartBlock, 0, st>>>(sc->sd, sc->pd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
-                                   sc->hist.p, sc->ckpt_x.p, sc->ckpt_v.p, sc->flag.p, sc->iters.p,
+                                   sc->hist.p, sc->hist_step, sc->ckpt_x.p, sc->ckpt_v.p, sc->flag.p, sc->iters.p,
                                    sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p,
                                    sc->has_contact ? sc->vwc.p : nullptr);
   k_loop_enter<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, sc->hs.nparts, sc->hs.K, h);
@@ -726,7 +735,7 @@ static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandl
   launch_local(sc, st, g, sc->xk.p, sc->act_all.p, sc->step.p);
   launch_gather(sc, st, g, sc->c0.p, sc->rhs.p, sc->xk.p);
   enqueue_solve(sc, st, g, sc->rhs.p, sc->y.p);
-  k_update<<<sc->nblk_p, kPartBlock, 0, st>>>(s.N, sc->pd, mixed(sc) ? 1 : 0, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->step.p,
+  k_update<<<sc->nblk_p, kPartBlock, 0, st>>>(s.N, sc->pd, mixed(sc) ? 1 : 0, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->hist_step, sc->step.p,
                                sc->flag.p, sc->iters.p, sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
   k_loop_ctl<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, s.nparts, s.K, h);
 }
@@ -1008,6 +1017,11 @@ static int create_on_device(std::unique_ptr<dfem_scene>& sc, int device, dfem_sc
   CK(cudaStreamCreateWithFlags(&sc->stream2, cudaStreamNonBlocking));  // only used to capture loop bodies
   CK(sc->kiter.alloc(1));
   CK(sc->status.alloc(4));  // before the factor upload, whose kernels report into it
+  {
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    sc->adj_budget = total_b / 4;
+  }
   RC(upload_scene(sc.get()));
   RC(ensure_steps(sc.get(), 1));
   // every factor the engine uses comes from the GPU refactorisation
@@ -1225,14 +1239,19 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   reset_solve_state(sc);
   RC(ensure_graphs(sc));
   if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 1);
+  int recomputed = 0;
   for (int st = sc->rec_steps - 1; st >= 0; --st) {
-    // recompute the step's iterates from its checkpoint (the step graph re-records the same checkpoint)
-    CK(cudaMemcpyAsync(sc->xt.p, sc->ckpt_x.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
-    CK(cudaMemcpyAsync(sc->vt.p, sc->ckpt_v.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
-    k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
-    CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
-    k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
     const bool contact_step = sc->has_contact && sc->rec_passes[2 * st] > 0;
+    if (sc->hist_step == 0 || contact_step) {
+      // recompute the step's iterates from its checkpoint (the step graph re-records the same checkpoint);
+      // a contact step also records its contact iterations for the contact adjoint
+      CK(cudaMemcpyAsync(sc->xt.p, sc->ckpt_x.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+      CK(cudaMemcpyAsync(sc->vt.p, sc->ckpt_v.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+      k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
+      CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
+      ++recomputed;
+    }
+    k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
     if (contact_step) RC(contact_adjoint_step(sc, st));
     CK(cudaGraphLaunch(sc->g_adj.exec, sc->stream));
     if (contact_step) {
@@ -1244,8 +1263,12 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 0);
   sc->launches += 5;
   for (int st = 0; st < sc->rec_steps && st < (int)sc->rec_iters.size(); ++st)
-    sc->launches += (int64_t)(2 + sc->g_step.outside + sc->g_adj.outside +
-                              (size_t)sc->rec_iters[st] * (sc->g_step.body + sc->g_adj.body));
+    sc->launches += (int64_t)(1 + sc->g_adj.outside + (size_t)sc->rec_iters[st] * sc->g_adj.body);
+  if (recomputed > 0)  // replayed step graphs (iteration counts as recorded; contact bodies not counted)
+    for (int st = 0; st < sc->rec_steps && st < (int)sc->rec_iters.size(); ++st)
+      if (sc->hist_step == 0 || (sc->has_contact && sc->rec_passes[2 * st] > 0))
+        sc->launches += (int64_t)(1 + sc->g_step.outside + (size_t)sc->rec_iters[st] * sc->g_step.body +
+                                  (size_t)sc->rec_passes[2 * st + 1] * sc->g_step.body2);
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_a.p, sc->rhs.p);
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_b.p, sc->c0.p);
   RC(copy_out(sc, sc->rhs.p, n3, gx, mem));
@@ -1373,6 +1396,18 @@ int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms
   }
   if (chosen) *chosen = sc->solve_mode + 1;
   if (ms) { ms[0] = sc->solve_ms[0]; ms[1] = sc->solve_ms[1]; }
+  return DFEM_OK;
+}
+
+int dfem_set_adjoint_budget(dfem_scene* sc, int64_t bytes) {
+  if (!sc || bytes < 0) return fail(DFEM_ERR_INVALID, "bad argument");
+  CK(cudaSetDevice(sc->device));
+  CK(cudaStreamSynchronize(sc->stream));
+  sc->adj_budget = (size_t)bytes;
+  const int cap = std::max(1, sc->cap_steps);
+  sc->cap_steps = 0;  // reallocate the per-step buffers under the new budget
+  RC(ensure_steps(sc, cap));
+  sc->rec_steps = 0;  // the recorded forward's buffers are gone
   return DFEM_OK;
 }
 

@@ -119,7 +119,7 @@ __device__ __forceinline__ int cons_part(const SceneDev& d, int t) {
 }
 
 // Contact phase state (World::ProjectiveDynamicsMethod, sim/fem/World.h:925-1023).
-constexpr int kMaxImpactsPerVertex = 4;
+constexpr int kMaxImpactsPerVertex = 8;  // a vertex at a corner of a tessellated obstacle touches up to 6 faces
 constexpr int kMaxContactPasses = 64;       // the reference's detection loop has no cap
 constexpr double kContactThickness = 1e-4;  // arcsim Impact::thickness
 struct ContactDev {

@@ -82,14 +82,17 @@ __device__ __forceinline__ Mat3<double> deformation(const double G[4][3], const 
 
 // --------------------------------------------------------------- forward ----
 
+// hist_step: doubles between the iterate records of consecutive steps (0: one
+// record shared by all steps, the adjoint recomputes each step).
 __global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt, double* vt, double* qn,
-                             double* c0, double* xk, double* hist, double* ckpt_x, double* ckpt_v,
+                             double* c0, double* xk, double* hist, long long hist_step, double* ckpt_x, double* ckpt_v,
                              int* flag, int* iters, double* partial, unsigned* counter, double* errv,
                              int* status, double* vwc_out) {
   const int b = blockIdx.x, p = pd.blk_part[b];
   const int pv0 = pd.part_v0[p], pv1 = pd.part_v0[p + 1];
   const int i = pd.blk_v0[b] + threadIdx.x;
   const int s = *step;
+  if (hist) hist += (size_t)s * hist_step;
   double q2 = 0;
   if (i < pv1) {
     Vec3<double> x = ld3(xt, i), v = ld3(vt, i);
@@ -636,7 +639,8 @@ __global__ void k_solve_reset(int ns, int* done_f, int* done_b, int* ctl) {
 // x^{k+1}; per-part convergence test for the next iteration (k read from
 // device memory).  Part-aligned blocks; a converged part's blocks do nothing.
 __global__ void k_update(int N, PartDev pd, int from_iterate, const int* kptr, const double* __restrict__ xt,
-                         const double* __restrict__ z, double* xk, double* hist, const int* step, int* flag, int* iters,
+                         const double* __restrict__ z, double* xk, double* hist, long long hist_step, const int* step,
+                         int* flag, int* iters,
                          double* partial, unsigned* counter, double* errv, int* status) {
   const int b = blockIdx.x, p = pd.blk_part[b];
   if (flag[p]) return;
@@ -650,7 +654,7 @@ __global__ void k_update(int N, PartDev pd, int from_iterate, const int* kptr, c
     Vec3<double> dlt = xn - ld3(xk, i);
     e2 = dot3(dlt, dlt);
     st3(xk, i, xn);
-    if (hist) st3(hist + (size_t)(k + 1) * 3 * N, i, xn);
+    if (hist) st3(hist + (size_t)(*step) * hist_step + (size_t)(k + 1) * 3 * N, i, xn);
   }
   double tot;
   if (part_reduce(e2, partial, counter + p, pd.part_b0[p], pd.part_b0[p + 1] - pd.part_b0[p], &tot)) {
@@ -778,8 +782,8 @@ __device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const d
     double G[4][3];
     load_g(d.tinv, d.T, t, G);
     Mat3<double> F = deformation(G, xv), Y = deformation(G, yv), md, mdv;
-    corot_project(F, md, mdv);
     double E = d.tE[t], nu = d.tnu[t], vol = d.tvol[t];
+    corot_project(F, md, mdv);
     double yr = 0, yvv = 0, yh = 0;
 #pragma unroll
     for (int j = 0; j < 3; ++j) { yr += dot3(Y.c[j], md.c[j]); yvv += dot3(Y.c[j], mdv.c[j]); }
@@ -871,10 +875,12 @@ __device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const d
 // Reverse PD iteration k (k read from device memory): local VJP at x^k with
 // the Hs term of x^{k+1}, and bbar += ybar (b = M/h^2 q_n enters every iteration).
 __global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const int* kptr, const int* step,
-                                                   const double* __restrict__ hist, const double* __restrict__ yb,
+                                                   const double* __restrict__ hist, long long hist_step,
+                                                   const double* __restrict__ yb,
                                                    double* bb, const double* __restrict__ act_all,
                                                    double* __restrict__ slot, double* gE, double* gnu, double* mg) {
   const int k = *kptr;
+  hist += (size_t)(*step) * hist_step;
   const double* x = hist + (size_t)k * 3 * d.N;
   const double* x1 = hist + (size_t)(k + 1) * 3 * d.N;
   int t = blockIdx.x * blockDim.x + threadIdx.x;

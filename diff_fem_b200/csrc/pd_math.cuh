@@ -223,9 +223,9 @@ __device__ __forceinline__ Mat3<double> rot_from_quat(const float qf[4]) {
   return R;
 }
 
-// Mixed-form corotated force P = wr (md - F) + wv (md_volume - F) (columns),
-// the tet's J d - L x up to the G factor, with FP32 rounding relative to the
-// strain rather than to F:
+// Mixed-form corotated deviations DR = md - F and DV = md_volume - F (columns;
+// the tet's J d - L x is G (wr DR + wv DV)), with FP32 rounding relative to
+// the strain rather than to F:
 //   1. FP32 SVD of F -> R0 = U V^T, its quaternion, and R = R(q) exactly
 //      orthogonal in FP64;
 //   2. A = R^T F in FP64, H = A - I rounded to FP32 (strain-sized; its skew
@@ -237,7 +237,7 @@ __device__ __forceinline__ Mat3<double> rot_from_quat(const float qf[4]) {
 //      prod(1 + a) - 1 expanded, and md_volume - F = R V diag(D) V^T.
 // Returns false (caller takes the FP64 branch) for inverted or
 // near-degenerate elements.
-__device__ __forceinline__ bool corot_force_mixed(const Mat3<double>& F, float wr, float wv, Vec3<float> P[3]) {
+__device__ __forceinline__ bool corot_delta_mixed(const Mat3<double>& F, Vec3<float> DR[3], Vec3<float> DV[3]) {
   Mat3<float> Ff;
 #pragma unroll
   for (int j = 0; j < 3; ++j) Ff.c[j] = mk3((float)F.c[j].x, (float)F.c[j].y, (float)F.c[j].z);
@@ -288,8 +288,11 @@ __device__ __forceinline__ bool corot_force_mixed(const Mat3<double>& F, float w
     const float c = (g0 * D[0] + g1 * D[1] + g2 * D[2] - C) / (g0 * g0 + g1 * g1 + g2 * g2);
     D[0] = c * g0; D[1] = c * g1; D[2] = c * g2;
   }
-  // B = wr (Omega - H) + wv V diag(D) V^T, then P = R B (R rounded to FP32: relative error on a small product)
-  Mat3<float> B;
+  // md - F = R (Omega - H), md_volume - F = R V diag(D) V^T (R rounded to FP32:
+  // a relative error on small products)
+  Mat3<float> Rf;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) Rf.c[j] = mk3((float)R.c[j].x, (float)R.c[j].y, (float)R.c[j].z);
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
     Vec3<float> col = mk3(-H[0][j], -H[1][j], -H[2][j]);
@@ -298,14 +301,19 @@ __device__ __forceinline__ bool corot_force_mixed(const Mat3<double>& F, float w
       const int k = pk[p], l = pl[p];
       col = col + (om[p] * vj[j][l]) * sv.v[k] - (om[p] * vj[j][k]) * sv.v[l];
     }
-    Vec3<float> vol = (D[0] * vj[j][0]) * sv.v[0] + (D[1] * vj[j][1]) * sv.v[1] + (D[2] * vj[j][2]) * sv.v[2];
-    B.c[j] = wr * col + wv * vol;
+    const Vec3<float> vol = (D[0] * vj[j][0]) * sv.v[0] + (D[1] * vj[j][1]) * sv.v[1] + (D[2] * vj[j][2]) * sv.v[2];
+    DR[j] = col.x * Rf.c[0] + col.y * Rf.c[1] + col.z * Rf.c[2];
+    DV[j] = vol.x * Rf.c[0] + vol.y * Rf.c[1] + vol.z * Rf.c[2];
   }
-  Mat3<float> Rf;
+  return true;
+}
+
+// Mixed-form corotated force P = wr (md - F) + wv (md_volume - F) (columns).
+__device__ __forceinline__ bool corot_force_mixed(const Mat3<double>& F, float wr, float wv, Vec3<float> P[3]) {
+  Vec3<float> DR[3], DV[3];
+  if (!corot_delta_mixed(F, DR, DV)) return false;
 #pragma unroll
-  for (int j = 0; j < 3; ++j) Rf.c[j] = mk3((float)R.c[j].x, (float)R.c[j].y, (float)R.c[j].z);
-#pragma unroll
-  for (int j = 0; j < 3; ++j) P[j] = B.c[j].x * Rf.c[0] + B.c[j].y * Rf.c[1] + B.c[j].z * Rf.c[2];
+  for (int j = 0; j < 3; ++j) P[j] = wr * DR[j] + wv * DV[j];
   return true;
 }
 

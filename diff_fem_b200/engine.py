@@ -213,6 +213,10 @@ class Scene:
         return {"fwd_ms": list(f), "bwd_ms": list(b), "supernodes": list(cnt), "level": list(lvl),
                 "threads_fwd": list(thr)[0::2], "threads_bwd": list(thr)[1::2]}
 
+    def set_adjoint_budget(self, nbytes: int):
+        """Device memory for storing every step's iterates (the adjoint then replays no step)."""
+        check(lib().dfem_set_adjoint_budget(self._h, int(nbytes)))
+
     def launch_count(self) -> int:
         n = C.c_int64()
         check(lib().dfem_get_launch_count(self._h, C.byref(n)))

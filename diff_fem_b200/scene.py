@@ -493,6 +493,70 @@ def drop_box(nx: int = 4, ny: int = 2, nz: int = 4, height: float = 0.02, v0: fl
     return d
 
 
+def icosphere(radius: float, subdiv: int, center=(0.0, 0.0, 0.0)):
+    """Triangulated sphere (icosahedron refined `subdiv` times, vertices pushed
+    to the sphere), outward faces.  Returns (vertices (V,3), faces (F,3))."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = [np.asarray(p, np.float64) / np.linalg.norm(p) for p in v]
+    for _ in range(subdiv):
+        mid = {}
+
+        def midpoint(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                mid[key] = len(verts) - 1
+            return mid[key]
+
+        nf = []
+        for a, b, c in f:
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    X = radius * np.asarray(verts) + np.asarray(center, np.float64)
+    F = np.asarray(f, np.int32)
+    # outward orientation
+    c0 = np.asarray(center, np.float64)
+    for k, (a, b, c) in enumerate(F):
+        n = np.cross(X[b] - X[a], X[c] - X[a])
+        if np.dot(n, X[a] - c0) < 0:
+            F[k] = (a, c, b)
+    return X, F
+
+
+def cloth_on_ball(nv: int = 64, edge: float = 0.02, radius: float = 0.2, drop: float = 0.3, subdiv: int = 3,
+                  stretch: float = 1e3, bend: float = 1e-3, density: float = 0.2, mu: float = 0.3,
+                  precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Cloth on a ball: an nv x nv cloth (edge 0.02 m; 64x64: 7,938 triangles,
+    springs on every edge, bending on every interior vertex; membrane 1e3,
+    bending 1e-3, 0.2 kg/m^2, gravity on) centred `drop` m above a ball of
+    radius `radius`, and a ground quad below the ball.  The ball is a static
+    obstacle surface (an icosphere, `subdiv` refinements): soft-soft contact
+    is not built, so the ball does not deform.  Every cloth vertex is a
+    contact vertex; obstacle friction mu.  h = 1/120, 20 iterations."""
+    side = (nv - 1) * edge
+    x0, tris, springs, boff, bvert = cloth_grid(nv, nv, edge, origin=(-0.5 * side, radius + drop, -0.5 * side))
+    mass = triangle_masses(x0, tris, density)
+    bx, bf = icosphere(radius, subdiv)
+    gx, gf = ground_quad(-radius - 1e-3, 2.0)
+    ox = np.concatenate([bx, gx])
+    of = np.concatenate([bf, gf + len(bx)]).astype(np.int32)
+    return SceneDesc(
+        x0=x0, mass=mass, spring_vertices=springs, spring_weight=np.full(len(springs), stretch),
+        bend_offsets=boff, bend_vertices=bvert, bend_weight=np.full(len(boff) - 1, bend),
+        contact_vertices=np.arange(x0.shape[0], dtype=np.int32), contact_faces=tris,
+        obstacle_x=ox, obstacle_faces=of, handle_collision=True, obstacle_friction=mu,
+        time_step=1.0 / 120.0, max_iterations=20, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name=f"cloth_on_ball_{nv}x{nv}",
+    )
+
+
 # -------------------------------------------------------------------- cloth ---
 
 def cloth_grid(nv_x: int, nv_z: int, edge: float, origin=(0.0, 0.0, 0.0)):

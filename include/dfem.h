@@ -249,6 +249,15 @@ int dfem_solve_mode(dfem_scene *scene, int32_t request, int32_t *chosen, double 
 int dfem_profile_levels(dfem_scene *scene, int32_t reps, int32_t cap, int32_t *n_segments, double *ms_fwd,
                         double *ms_bwd, int32_t *n_supernodes, int32_t *level, int32_t *threads);
 
+/* Device memory (bytes) the adjoint may spend on storing the PD iterates of
+ * every step of a forward call (default: a quarter of the device's memory).  Within it the adjoint
+ * replays no step (except steps with contact, whose contact iterations it
+ * records on a replay); beyond it every step is recomputed from its
+ * checkpoint.  Results are identical either way.  Invalidates the recorded
+ * forward call.  No counterpart in the reference (its CppAD tape stores
+ * everything). */
+int dfem_set_adjoint_budget(dfem_scene *scene, int64_t bytes);
+
 /* Number of kernels this scene has launched so far (CUDA-graph nodes counted
  * individually).  Instrumentation; no counterpart in the reference. */
 int dfem_get_launch_count(const dfem_scene *scene, int64_t *count);
