@@ -88,25 +88,32 @@ struct dfem_scene {
   DBuf<double> hs_val;
   DBuf<double> attach_k;             // per-vertex attachment stiffness (mixed form's rhs)
   // factor
-  DBuf<int> rseg_ptr, rseg_pos, sn_c0, sn_w, sn_r, sn_rofs, rowidx, sn_lofs, sn_dofs, lvl_sn;
-  DBuf<double> contrib, Lcm, Dinv;
+  DBuf<int> rseg_ptr, cdst, sn_c0, sn_w, sn_r, sn_rofs, rowidx, sn_lofs, sn_dofs, lvl_sn;
+  DBuf<double> contrib, Lcm, Dinv, DinvC;
+  DBuf<SnInfo> sn_info;
   std::vector<int> lvl_ptr;
-  int max_w = 1, max_r = 0;
   // Launch segments of the level-kernel solve: every level of the elimination
-  // tree, split into its small and its large supernodes (each with the
-  // shared memory of its largest member and an autotuned CTA size).
+  // tree, split into its small supernodes (one warp each, eight per CTA) and
+  // the rest (one CTA each, autotuned CTA size); each launch gets the shared
+  // memory of its largest member.
   struct LevelSeg {
     int begin, count, level;
-    size_t shm_f, shm_b;
+    int warp;              // 1: one supernode per warp
+    int grp_f, grp_b;      // doubles of shared memory per group (warp segments)
+    size_t shm_f, shm_b;   // bytes per CTA
     int thr_f, thr_b;
   };
   std::vector<LevelSeg> segs;
   // persistent solve (one launch per solve) and the autotuned choice between it and the level kernels
-  DBuf<int> sn_parent, kid_ptr, kid, done_f, done_b, solve_ctl;
+  DBuf<int> sn_parent, sn_pos, kid_ptr, kid, done_f, done_b, solve_ctl;
   size_t shm_pers = 0;
-  int pers_grid = 1;
-  int solve_mode = 0;                    // 0: level kernels, 1: persistent
-  double solve_ms[2] = {0.0, 0.0};       // autotune timings (ms per solve) of the two modes
+  int pers_slots = 1;                    // CTAs of the persistent solve resident at once
+  // The solve runs levels 0 .. solve_cut-1 as level kernels and the rest in
+  // one persistent launch: solve_cut = number of levels is the level-kernel
+  // form, 0 the persistent form, anything between the split form.
+  int solve_cut = 0;
+  int split_cut = 0;                     // the autotune's best split (0: none)
+  double solve_ms[3] = {0.0, 0.0, 0.0};  // autotune timings (ms per solve): levels, persistent, best split
   // numeric refactorisation on the GPU (material changes)
   DBuf<double> hs_base, hc_coef, Ldw, part_reg, E_in, nu_in;
   DBuf<int> hc_ptr, hc_tet, up_ptr, up_d, up_a0, up_a1, part_fail;
@@ -195,14 +202,42 @@ static void refresh_scene_view(dfem_scene* sc) {
   sc->sd = sd;
 }
 
+// Shared memory (doubles) of one supernode's forward / backward solve, with
+// or without L_{R,s} staged; mirrors the layout in pd_kernels.cu.
+static void solve_shm_doubles(int w, int r, int nseg, bool staged, size_t* nf, size_t* nb) {
+  auto even = [](size_t v) { return (v + 1) & ~size_t(1); };
+  const size_t W = w, R = r, l = staged ? even(R * W) : 0;
+  *nf = even(even(W * W) + l + 6 * W + 3 * (size_t)nseg + (W + 2) / 2);
+  *nb = even(even(W * W) + l + 3 * W + 3 * R);
+}
+
+// Launch classes of the level-kernel solve by a supernode's shared-memory
+// need (doubles): one warp per supernode up to kWarpGroupDoubles (eight per
+// CTA); CTAs with at most kSmallCtaDoubles (several CTAs per SM); the rest.
+// A class of a level with fewer than kMinClass members joins the next larger
+// class of that level (one launch less; its members fit one wave anyway).
+constexpr size_t kWarpGroupDoubles = 512;
+constexpr size_t kSmallCtaDoubles = 3072;
+constexpr int kMinClass = 64;
+static int shm_class(size_t need) { return need <= kWarpGroupDoubles ? 0 : need <= kSmallCtaDoubles ? 1 : 2; }
+// Factors of few supernodes (one scene: latency-bound solves) stage L_{R,s}
+// whenever the solve still fits 220 KB of shared memory; factors of many
+// (batches) stage it only where that keeps the supernode in its launch class
+// and within 110 KB, so that the classes keep several CTAs per SM.
+constexpr int kFewSupernodes = 2048;
+
 static int upload_factor(dfem_scene* sc) {
   SupernodalFactor& F = sc->hs.F;
   if (F.sn_rofs.back() > INT32_MAX / 3 || F.sn_lofs.back() > INT32_MAX || F.sn_dofs.back() > INT32_MAX)
     return fail(DFEM_ERR_INVALID, "factor too large for 32-bit offsets");
-  auto to32 = [](const std::vector<int64_t>& v) { return std::vector<int>(v.begin(), v.end()); };
+  const int ns = F.nsuper;
+  // contributions grouped by destination row: below-diagonal position p writes slot cdst[p]
+  std::vector<int> cdst(std::max<size_t>(1, F.rowidx.size()));
+  for (size_t k = 0; k < F.rseg_pos.size(); ++k) cdst[F.rseg_pos[k]] = (int)k;
   CK(sc->rseg_ptr.upload(F.rseg_ptr));
-  CK(sc->rseg_pos.upload(F.rseg_pos));
+  CK(sc->cdst.upload(cdst));
   if (sc->contrib.n != 3 * F.rowidx.size() || !sc->contrib.p) CK(sc->contrib.alloc(3 * std::max<size_t>(1, F.rowidx.size())));
+  auto to32 = [](const std::vector<int64_t>& v) { return std::vector<int>(v.begin(), v.end()); };
   CK(sc->sn_c0.upload(F.sn_c0));
   CK(sc->sn_w.upload(F.sn_w));
   CK(sc->sn_r.upload(F.sn_r));
@@ -212,107 +247,129 @@ static int upload_factor(dfem_scene* sc) {
   CK(sc->Lcm.upload(F.Lcm));
   CK(sc->sn_dofs.upload(to32(F.sn_dofs)));
   CK(sc->Dinv.upload(F.Dinv));
-  sc->lvl_ptr = F.lvl_ptr;
-  sc->max_w = 1;
-  for (int w : F.sn_w) sc->max_w = std::max(sc->max_w, w);
-  sc->max_r = 0;
-  for (int r : F.sn_r) sc->max_r = std::max(sc->max_r, r);
-  // dynamic shared memory of the level kernels (doubles, blocks padded to even counts):
-  //   fwd: Dinv + [L_{R,s}] + t + y_s      bwd: Dinv + [L_{R,s}] + u + x_R
-  // L_{R,s} is staged too when the largest supernode still fits.  Each level
-  // is launched with the largest need of its own supernodes, so levels of
-  // small supernodes keep several blocks per SM.
-  auto even = [](size_t v) { return (v + 1) & ~size_t(1); };
-  auto need = [&](int q, int st, size_t* nf, size_t* nb) {
-    size_t w = F.sn_w[q], r = F.sn_r[q];
-    size_t nseg = (size_t)(F.rseg_ptr[F.sn_c0[q] + w] - F.rseg_ptr[F.sn_c0[q]]);
-    size_t l = st ? even(r * w) : 0;
-    // + row -> segment offsets ((w+1) ints) + gathered contributions (3 per segment)
-    *nf = sizeof(double) * (even(w * w) + l + 6 * w + (w + 2) / 2 + 3 * nseg);
-    *nb = sizeof(double) * (even(w * w) + l + 3 * w + 3 * r);
-  };
-  size_t need_f[2] = {0, 0}, need_b[2] = {0, 0};  // [without, with] staged L
-  for (int q = 0; q < F.nsuper; ++q)
-    for (int st = 0; st < 2; ++st) {
-      size_t nf, nb;
-      need(q, st, &nf, &nb);
-      need_f[st] = std::max(need_f[st], nf);
-      need_b[st] = std::max(need_b[st], nb);
-    }
-  const size_t budget = 220 * 1024;
-  const int stage_l = (need_f[1] <= budget && need_b[1] <= budget) ? 1 : 0;
-  if (need_f[stage_l] > budget || need_b[stage_l] > budget)
-    return fail(DFEM_ERR_INVALID, "supernode too large for the shared-memory staging of the triangular solves");
-  // One launch per level, with the shared memory of its largest supernode.
-  // (A split of each level into its small and large supernodes, launched one
-  // after the other, ran 10 % less kernel time but cost more in launch
-  // overhead inside the step graphs than it saved, on the 256-scene batch.)
-  // Within a level the supernodes are ordered by their shared-memory need (any
-  // order within a level is valid for every solve form and the refactorisation).
-  const int L = (int)F.lvl_ptr.size() - 1;
-  const size_t small_shm = SIZE_MAX;
-  std::vector<size_t> key(F.nsuper);
-  for (int q = 0; q < F.nsuper; ++q) {
-    size_t nf, nb;
-    need(q, stage_l, &nf, &nb);
-    key[q] = std::max(nf, nb);
+  {  // column-major copy of every diagonal-block inverse (forward solve)
+    std::vector<double> dc(F.Dinv.size(), 0.0);
+    parallel_for(ns, [&](int q) {
+      const int w = F.sn_w[q];
+      const double* src = F.Dinv.data() + F.sn_dofs[q];
+      double* dst = dc.data() + F.sn_dofs[q];
+      for (int i = 0; i < w; ++i)
+        for (int j = 0; j < w; ++j) dst[j * w + i] = src[i * w + j];
+    });
+    CK(sc->DinvC.upload(dc));
   }
+  sc->lvl_ptr = F.lvl_ptr;
+  // per supernode: staging of L_{R,s}, shared memory, launch class
+  const size_t budget = 220 * 1024;
+  std::vector<int> stage(ns), nseg(ns), cls(ns);
+  std::vector<size_t> need(ns);
+  size_t max_cta = 0;
+  for (int q = 0; q < ns; ++q) {
+    const int w = F.sn_w[q], r = F.sn_r[q];
+    nseg[q] = F.rseg_ptr[F.sn_c0[q] + w] - F.rseg_ptr[F.sn_c0[q]];
+    size_t uf, ub, tf, tb;
+    solve_shm_doubles(w, r, nseg[q], false, &uf, &ub);
+    solve_shm_doubles(w, r, nseg[q], true, &tf, &tb);
+    const size_t u = std::max(uf, ub), t = std::max(tf, tb);
+    if (8 * u > budget)
+      return fail(DFEM_ERR_INVALID, "supernode too large for the shared-memory staging of the triangular solves");
+    stage[q] = r > 0 && (ns <= kFewSupernodes ? 8 * t <= budget : shm_class(t) == shm_class(u) && 8 * t <= budget / 2);
+    need[q] = stage[q] ? t : u;
+    cls[q] = shm_class(need[q]);
+    max_cta = std::max(max_cta, 8 * need[q]);
+  }
+  // Within a level the supernodes are ordered by their shared-memory need (any
+  // order within a level is valid for every solve form and the
+  // refactorisation), then cut into launch classes.
+  const int L = (int)F.lvl_ptr.size() - 1;
   sc->segs.clear();
+  size_t max_warp_blk = 0, max_cta_blk = 0;
   for (int l = 0; l < L; ++l) {
     auto b = F.lvl_sn.begin() + F.lvl_ptr[l], e = F.lvl_sn.begin() + F.lvl_ptr[l + 1];
-    std::stable_sort(b, e, [&](int x, int y) { return key[x] < key[y]; });
-    int split = F.lvl_ptr[l];
-    while (split < F.lvl_ptr[l + 1] && key[F.lvl_sn[split]] <= small_shm) ++split;
-    const int cuts[3] = {F.lvl_ptr[l], split, F.lvl_ptr[l + 1]};
-    for (int g = 0; g < 2; ++g) {
-      if (cuts[g + 1] == cuts[g]) continue;
-      dfem_scene::LevelSeg sg{cuts[g], cuts[g + 1] - cuts[g], l, 0, 0, 256, 256};
-      for (int k = cuts[g]; k < cuts[g + 1]; ++k) {
+    std::stable_sort(b, e, [&](int x, int y) { return need[x] < need[y]; });
+    int cut[4] = {F.lvl_ptr[l], F.lvl_ptr[l], F.lvl_ptr[l], F.lvl_ptr[l + 1]};
+    for (int c = 1; c < 3; ++c) {
+      cut[c] = cut[c - 1];
+      while (cut[c] < F.lvl_ptr[l + 1] && cls[F.lvl_sn[cut[c]]] < c) ++cut[c];
+    }
+    for (int c = 0; c < 2; ++c)  // a small class joins the next one
+      if (cut[c + 1] - cut[c] < kMinClass && cut[c + 1] < cut[3]) cut[c + 1] = cut[c];
+    for (int c = 0; c < 3; ++c) {
+      if (cut[c + 1] == cut[c]) continue;
+      dfem_scene::LevelSeg sg{cut[c], cut[c + 1] - cut[c], l, c == 0 ? 1 : 0, 0, 0, 0, 0, 256, 256};
+      size_t mf = 0, mb = 0;
+      for (int k = cut[c]; k < cut[c + 1]; ++k) {
+        const int q = F.lvl_sn[k];
         size_t nf, nb;
-        need(F.lvl_sn[k], stage_l, &nf, &nb);
-        sg.shm_f = std::max(sg.shm_f, nf);
-        sg.shm_b = std::max(sg.shm_b, nb);
+        solve_shm_doubles(F.sn_w[q], F.sn_r[q], nseg[q], stage[q] != 0, &nf, &nb);
+        mf = std::max(mf, nf);
+        mb = std::max(mb, nb);
+      }
+      if (sg.warp) {
+        sg.grp_f = (int)mf;
+        sg.grp_b = (int)mb;
+        sg.shm_f = 8 * 8 * mf;
+        sg.shm_b = 8 * 8 * mb;
+        max_warp_blk = std::max({max_warp_blk, sg.shm_f, sg.shm_b});
+      } else {
+        sg.shm_f = 8 * mf;
+        sg.shm_b = 8 * mb;
+        max_cta_blk = std::max({max_cta_blk, sg.shm_f, sg.shm_b});
       }
       sc->segs.push_back(sg);
     }
   }
   CK(sc->lvl_sn.upload(F.lvl_sn));
-  CK(cudaFuncSetAttribute(k_fwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_f[stage_l]));
-  CK(cudaFuncSetAttribute(k_bwd_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need_b[stage_l]));
+  std::vector<int> snp(ns, 0);
+  if (sc->hs.nparts > 1)
+    for (int q = 0; q < ns; ++q)
+      snp[q] = (int)(std::upper_bound(sc->hs.part_v0.begin(), sc->hs.part_v0.end(), F.sn_c0[q]) - sc->hs.part_v0.begin()) - 1;
+  {
+    std::vector<SnInfo> info(std::max(1, ns));
+    for (int k = 0; k < ns; ++k) {
+      const int q = F.lvl_sn[k];
+      info[k] = SnInfo{F.sn_c0[q], F.sn_w[q], F.sn_r[q], (int)F.sn_rofs[q], (int)F.sn_lofs[q], (int)F.sn_dofs[q],
+                       F.rseg_ptr[F.sn_c0[q]], nseg[q], q, snp[q], stage[q], 0};
+    }
+    CK(sc->sn_info.upload(info));
+  }
+  for (auto fn : {(const void*)k_fwd_level<CtaGroup>, (const void*)k_bwd_level<CtaGroup>})
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(1, max_cta_blk)));
+  for (auto fn : {(const void*)k_fwd_level<WarpGroup>, (const void*)k_bwd_level<WarpGroup>})
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(1, max_warp_blk)));
   // persistent solve: elimination tree (children CSR), completion stamps, control words
   {
-    std::vector<int> kp(F.nsuper + 1, 0), kd(std::max(1, F.nsuper));
-    for (int q = 0; q < F.nsuper; ++q)
+    std::vector<int> kp(ns + 1, 0), kd(std::max(1, ns));
+    for (int q = 0; q < ns; ++q)
       if (F.sn_parent[q] >= 0) kp[F.sn_parent[q] + 1]++;
-    for (int q = 0; q < F.nsuper; ++q) kp[q + 1] += kp[q];
+    for (int q = 0; q < ns; ++q) kp[q + 1] += kp[q];
     std::vector<int> fill(kp.begin(), kp.end() - 1);
-    for (int q = 0; q < F.nsuper; ++q)
+    for (int q = 0; q < ns; ++q)
       if (F.sn_parent[q] >= 0) kd[fill[F.sn_parent[q]]++] = q;
     CK(sc->sn_parent.upload(F.sn_parent));
     CK(sc->kid_ptr.upload(kp));
     CK(sc->kid.upload(kd));
-    if (sc->done_f.n != (size_t)F.nsuper || !sc->done_f.p) {
-      CK(sc->done_f.alloc(std::max(1, F.nsuper)));
-      CK(sc->done_b.alloc(std::max(1, F.nsuper)));
+    if (sc->done_f.n != (size_t)ns || !sc->done_f.p) {
+      CK(sc->done_f.alloc(std::max(1, ns)));
+      CK(sc->done_b.alloc(std::max(1, ns)));
       CK(sc->solve_ctl.alloc(4));
     }
-    sc->shm_pers = std::max(need_f[stage_l], need_b[stage_l]);
+    sc->shm_pers = max_cta;
     CK(cudaFuncSetAttribute(k_solve_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_pers));
     int nsm = 1, per_sm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, sc->device));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_persistent, 256, sc->shm_pers));
-    sc->pers_grid = std::max(1, std::min(nsm * std::max(1, per_sm), 2 * F.nsuper));
+    sc->pers_slots = std::max(1, nsm * std::max(1, per_sm));
   }
-  if (sc->hs.nparts > 1) {
-    std::vector<int> snp(F.nsuper);
-    for (int q = 0; q < F.nsuper; ++q)
-      snp[q] = (int)(std::upper_bound(sc->hs.part_v0.begin(), sc->hs.part_v0.end(), F.sn_c0[q]) - sc->hs.part_v0.begin()) - 1;
-    CK(sc->sn_part.upload(snp));
+  if (sc->hs.nparts > 1) CK(sc->sn_part.upload(snp));
+  {
+    std::vector<int> pos(std::max(1, ns));
+    for (int k = 0; k < ns; ++k) pos[F.lvl_sn[k]] = k;
+    CK(sc->sn_pos.upload(pos));
   }
-  FactorDev fd{sc->rseg_ptr.p, sc->rseg_pos.p, sc->contrib.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p,
-               sc->sn_rofs.p, sc->rowidx.p, sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->lvl_sn.p,
-               stage_l, sc->status.p, sc->hs.nparts > 1 ? sc->sn_part.p : nullptr,
-               F.nsuper, sc->sn_parent.p, sc->kid_ptr.p, sc->kid.p, sc->done_f.p, sc->done_b.p, sc->solve_ctl.p};
+  FactorDev fd{sc->sn_info.p, sc->rseg_ptr.p, sc->cdst.p, sc->contrib.p, sc->rowidx.p, sc->Lcm.p, sc->Dinv.p,
+               sc->DinvC.p, sc->status.p, ns, sc->sn_pos.p, sc->sn_parent.p, sc->kid_ptr.p, sc->kid.p, sc->done_f.p,
+               sc->done_b.p, sc->solve_ctl.p};
   if (std::memcmp(&fd, &sc->fd, sizeof(fd)) != 0) invalidate_graphs(sc);
   sc->fd = fd;
   return DFEM_OK;
@@ -421,7 +478,7 @@ static int upload_refactor_plan(dfem_scene* sc) {
   sc->rd = RefactorDev{s.T, sc->tvol.p, sc->tE.p, sc->tnu.p, sc->twr.p, sc->twv.p, (int)base.size(),
                        sc->hs_base.p, sc->hc_ptr.p, sc->hc_tet.p, sc->hc_coef.p, sc->hs_val.p, sc->hs_ptr.p,
                        sc->hs_col.p, sc->sn_c0.p, sc->sn_w.p, sc->sn_r.p, sc->sn_rofs.p, sc->rowidx.p,
-                       sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->Ldw.p, sc->lvl_sn.p, sc->up_ptr.p,
+                       sc->sn_lofs.p, sc->Lcm.p, sc->sn_dofs.p, sc->Dinv.p, sc->DinvC.p, sc->Ldw.p, sc->lvl_sn.p, sc->up_ptr.p,
                        sc->up_d.p, sc->up_a0.p, sc->up_a1.p, np > 1 ? sc->sn_part.p : nullptr, sc->part_reg.p,
                        sc->part_fail.p};
   return DFEM_OK;
@@ -614,18 +671,44 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
 
 // The global solve Hs y = rhs: one persistent launch, or one launch per level
 // and direction (the autotuned choice for the scene).
-static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
-  if (sc->solve_mode == 1) {
-    k_solve_persistent<<<sc->pers_grid, 256, sc->shm_pers, st>>>(sc->fd, gate, rhs, y);
-    return;
+// One launch segment of the level-kernel solve in one direction (thr: CTA
+// size of a CTA segment; warp segments run eight warps per CTA).
+static void launch_segment(dfem_scene* sc, cudaStream_t st, const dfem_scene::LevelSeg& g, bool fwd, int thr,
+                           Gate gate, const double* rhs, double* y) {
+  if (g.warp) {
+    const int nb = (g.count + 7) / 8;
+    if (fwd) k_fwd_level<WarpGroup><<<nb, 256, g.shm_f, st>>>(sc->fd, g.begin, g.count, g.grp_f, gate, rhs, y);
+    else k_bwd_level<WarpGroup><<<nb, 256, g.shm_b, st>>>(sc->fd, g.begin, g.count, g.grp_b, gate, y);
+  } else {
+    if (fwd) k_fwd_level<CtaGroup><<<g.count, thr, g.shm_f, st>>>(sc->fd, g.begin, g.count, 0, gate, rhs, y);
+    else k_bwd_level<CtaGroup><<<g.count, thr, g.shm_b, st>>>(sc->fd, g.begin, g.count, 0, gate, y);
   }
-  for (const auto& g : sc->segs) k_fwd_level<<<g.count, g.thr_f, g.shm_f, st>>>(sc->fd, g.begin, gate, rhs, y);
+}
+
+static int n_levels(const dfem_scene* sc) { return (int)sc->lvl_ptr.size() - 1; }
+
+static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
+  const int c = sc->solve_cut;
+  for (const auto& g : sc->segs)
+    if (g.level < c) launch_segment(sc, st, g, true, g.thr_f, gate, rhs, y);
+  if (c < n_levels(sc)) {
+    const int p0 = sc->lvl_ptr[c];
+    const int grid = std::max(1, std::min(sc->pers_slots, 2 * (sc->hs.F.nsuper - p0)));
+    k_solve_persistent<<<grid, 256, sc->shm_pers, st>>>(sc->fd, p0, gate, rhs, y);
+  }
   for (auto it = sc->segs.rbegin(); it != sc->segs.rend(); ++it)
-    k_bwd_level<<<it->count, it->thr_b, it->shm_b, st>>>(sc->fd, it->begin, gate, y);
+    if (it->level < c) launch_segment(sc, st, *it, false, it->thr_b, gate, rhs, y);
 }
 
 static int solve_launches(const dfem_scene* sc) {
-  return sc->solve_mode == 1 ? 1 : 2 * (int)sc->segs.size();
+  int n = sc->solve_cut < n_levels(sc) ? 1 : 0;
+  for (const auto& g : sc->segs) n += g.level < sc->solve_cut ? 2 : 0;
+  return n;
+}
+
+// 1: level kernels, 2: persistent, 3: split
+static int solve_form(const dfem_scene* sc) {
+  return sc->solve_cut >= n_levels(sc) ? 1 : sc->solve_cut == 0 ? 2 : 3;
 }
 
 // Fresh completion stamps and control words of the persistent solve (each API
@@ -963,13 +1046,11 @@ static int autotune_solve(dfem_scene* sc) {
     const int cand[3] = {64, 128, 256};
     for (auto& g : sc->segs)
       for (int dir = 0; dir < 2; ++dir) {
+        if (g.warp) continue;
         double best = 1e30;
         int pick = 256;
         for (int thr : cand) {
-          auto launch = [&] {
-            if (dir == 0) k_fwd_level<<<g.count, thr, g.shm_f, sc->stream>>>(sc->fd, g.begin, kOpen, sc->rhs.p, sc->y.p);
-            else k_bwd_level<<<g.count, thr, g.shm_b, sc->stream>>>(sc->fd, g.begin, kOpen, sc->y.p);
-          };
+          auto launch = [&] { launch_segment(sc, sc->stream, g, dir == 0, thr, kOpen, sc->rhs.p, sc->y.p); };
           launch();
           cudaEventRecord(e0, sc->stream);
           for (int r = 0; r < 5; ++r) launch();
@@ -984,8 +1065,8 @@ static int autotune_solve(dfem_scene* sc) {
       }
   }
   const int reps = 10;
-  for (int mode = 0; mode < 2; ++mode) {
-    sc->solve_mode = mode;
+  auto time_cut = [&](int c, double* ms) -> int {
+    sc->solve_cut = c;
     for (int r = 0; r < 3; ++r) enqueue_solve(sc, sc->stream, kOpen, sc->rhs.p, sc->y.p);
     cudaEventRecord(e0, sc->stream);
     for (int r = 0; r < reps; ++r) enqueue_solve(sc, sc->stream, kOpen, sc->rhs.p, sc->y.p);
@@ -993,20 +1074,32 @@ static int autotune_solve(dfem_scene* sc) {
     cudaError_t e = cudaEventSynchronize(e1);
     float t = 0;
     if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
-    if (e != cudaSuccess) {
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
-      return fail(DFEM_ERR_CUDA, std::string("solve autotune: ") + cudaGetErrorString(e));
-    }
-    sc->solve_ms[mode] = (double)t / reps;
+    if (e != cudaSuccess) return fail(DFEM_ERR_CUDA, std::string("solve autotune: ") + cudaGetErrorString(e));
+    *ms = (double)t / reps;
     sc->launches += (int64_t)(reps + 3) * solve_launches(sc);
+    return DFEM_OK;
+  };
+  const int L = n_levels(sc);
+  int rc = time_cut(L, &sc->solve_ms[0]);
+  if (rc == DFEM_OK) rc = time_cut(0, &sc->solve_ms[1]);
+  sc->split_cut = 0;
+  sc->solve_ms[2] = 0.0;
+  for (int c = 1; c < L && rc == DFEM_OK; ++c) {
+    double ms = 0.0;
+    rc = time_cut(c, &ms);
+    if (rc == DFEM_OK && (sc->split_cut == 0 || ms < sc->solve_ms[2])) {
+      sc->split_cut = c;
+      sc->solve_ms[2] = ms;
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  RC(rc);
   int st4[4] = {0, 0, 0, 0};
   CK(cudaMemcpy(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost));
   RC(status_error(st4));
-  sc->solve_mode = sc->solve_ms[1] < sc->solve_ms[0] ? 1 : 0;
+  sc->solve_cut = sc->solve_ms[1] < sc->solve_ms[0] ? 0 : L;
+  if (sc->split_cut > 0 && sc->solve_ms[2] < std::min(sc->solve_ms[0], sc->solve_ms[1])) sc->solve_cut = sc->split_cut;
   invalidate_graphs(sc);
   return DFEM_OK;
 }
@@ -1365,11 +1458,12 @@ int dfem_profile_levels(dfem_scene* sc, int32_t reps, int32_t cap, int32_t* n_se
     const auto& sg = sc->segs[g];
     if (n_supernodes) n_supernodes[g] = sg.count;
     if (level) level[g] = sg.level;
-    if (threads) { threads[2 * g] = sg.thr_f; threads[2 * g + 1] = sg.thr_b; }
-    ms_fwd[g] = time_it([&] {
-      k_fwd_level<<<sg.count, sg.thr_f, sg.shm_f, sc->stream>>>(sc->fd, sg.begin, kOpen, sc->rhs.p, sc->y.p);
-    });
-    ms_bwd[g] = time_it([&] { k_bwd_level<<<sg.count, sg.thr_b, sg.shm_b, sc->stream>>>(sc->fd, sg.begin, kOpen, sc->y.p); });
+    if (threads) {  // 32: one supernode per warp
+      threads[2 * g] = sg.warp ? 32 : sg.thr_f;
+      threads[2 * g + 1] = sg.warp ? 32 : sg.thr_b;
+    }
+    ms_fwd[g] = time_it([&] { launch_segment(sc, sc->stream, sg, true, sg.thr_f, kOpen, sc->rhs.p, sc->y.p); });
+    ms_bwd[g] = time_it([&] { launch_segment(sc, sc->stream, sg, false, sg.thr_b, kOpen, sc->rhs.p, sc->y.p); });
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1383,19 +1477,31 @@ int dfem_profile_levels(dfem_scene* sc, int32_t reps, int32_t cap, int32_t* n_se
 
 int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms) {
   if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
-  if (request < -1 || request > 2) return fail(DFEM_ERR_INVALID, "request must be -1, 0, 1 or 2");
+  if (request < -1 || request > 3) return fail(DFEM_ERR_INVALID, "request must be -1, 0, 1, 2 or 3");
   CK(cudaSetDevice(sc->device));
   if (request == 0) {
     CK(cudaStreamSynchronize(sc->stream));
     CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
     RC(autotune_solve(sc));
     sc->rec_steps = 0;  // the tuning solves overwrote the recorded iterates
-  } else if (request > 0 && request - 1 != sc->solve_mode) {
-    sc->solve_mode = request - 1;
-    invalidate_graphs(sc);
+  } else if (request > 0) {
+    if (request == 3 && sc->split_cut == 0) return fail(DFEM_ERR_INVALID, "no split form (fewer than two levels)");
+    const int c = request == 1 ? n_levels(sc) : request == 2 ? 0 : sc->split_cut;
+    if (c != sc->solve_cut) {
+      sc->solve_cut = c;
+      invalidate_graphs(sc);
+    }
   }
-  if (chosen) *chosen = sc->solve_mode + 1;
+  if (chosen) *chosen = solve_form(sc);
   if (ms) { ms[0] = sc->solve_ms[0]; ms[1] = sc->solve_ms[1]; }
+  return DFEM_OK;
+}
+
+int dfem_solve_split(const dfem_scene* sc, int32_t* cut_level, int32_t* n_levels_out, double* ms_split) {
+  if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
+  if (cut_level) *cut_level = sc->split_cut;
+  if (n_levels_out) *n_levels_out = n_levels(sc);
+  if (ms_split) *ms_split = sc->solve_ms[2];
   return DFEM_OK;
 }
 

@@ -52,7 +52,8 @@ struct RefactorDev {
   const int* sn_lofs;
   double* Lcm;
   const int* sn_dofs;
-  double* Dinv;
+  double* Dinv;         // row-major
+  double* DinvC;        // column-major copy (forward solve)
   double* Ldw;          // diagonal-block workspace (column-major w x w per supernode)
   const int* lvl_sn;
   const int* up_ptr;    // supernode -> updates (descendant d, row range a0..a1 of R_d inside its columns)
@@ -247,7 +248,11 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
   }
   __syncthreads();
   double* Di = f.Dinv + f.sn_dofs[s];  // row-major lower
-  for (int q = threadIdx.x; q < w * w; q += blockDim.x) Di[q] = X[(q / w) + (q % w) * w];
+  double* DiC = f.DinvC + f.sn_dofs[s];
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
+    Di[q] = X[(q / w) + (q % w) * w];
+    DiC[q] = X[q];
+  }
   // 5. rows below: L_{R,s} = P_R X^T, kTrsmRows rows at a time (staged, then overwritten)
   for (int rb = 0; rb < r; rb += kTrsmRows) {
     const int nr = min(kTrsmRows, r - rb);

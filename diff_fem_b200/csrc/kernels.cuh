@@ -150,25 +150,34 @@ struct ContactDev {
   int* status;
 };
 
+// One supernode of the triangular solves, stored in level order (position
+// lvl_ptr[l] .. lvl_ptr[l+1] of level l) so that one load gives a solve
+// everything it needs before its data loads.
+struct SnInfo {
+  int c0, w, r;   // first column, width, rows below the diagonal block
+  int rofs;       // its below-diagonal rows: rowidx[rofs .. rofs + r)
+  int lofs;       // L_{R,s} (column-major r x w) at Lcm + lofs
+  int dofs;       // diagonal-block inverse at Dinv + dofs (row-major) and DinvC + dofs (column-major)
+  int seg0, nseg; // the contributions to its rows: contrib[3 seg0 .. 3 (seg0 + nseg))
+  int s;          // supernode id (elimination tree, completion stamps)
+  int part;       // batch part
+  int stage;      // 1: L_{R,s} is staged in shared memory too
+  int pad;
+};
+
 struct FactorDev {
-  const int* rseg_ptr;   // row -> its contribution slots (push-form forward solve)
-  const int* rseg_pos;
-  double* contrib;       // 3 doubles per below-diagonal row of every supernode
-  const int* sn_c0;
-  const int* sn_w;
-  const int* sn_r;
-  const int* sn_rofs;
+  const SnInfo* info;    // level order
+  const int* rseg_ptr;   // row -> its contributions: contrib[3 rseg_ptr[i] .. 3 rseg_ptr[i+1]) in a fixed order
+  const int* cdst;       // below-diagonal row position (rowidx order) -> its contribution slot
+  double* contrib;       // 3 doubles per below-diagonal row of every supernode, grouped by destination row
   const int* rowidx;
-  const int* sn_lofs;
   const double* Lcm;
-  const int* sn_dofs;
-  const double* Dinv;
-  const int* lvl_sn;
-  int stage_l;   // 1: the below-diagonal blocks are staged in shared memory too
+  const double* Dinv;    // row-major (backward solve)
+  const double* DinvC;   // column-major (forward solve)
   int* status;   // error status word (6: a bounded wait gave up)
-  const int* sn_part;  // batch: part of every supernode (null for a single scene)
   // persistent solve: elimination tree, completion stamps, control words
   int nsuper;
+  const int* sn_pos;     // supernode -> its level-order position
   const int* sn_parent;
   const int* kid_ptr;
   const int* kid;

@@ -323,24 +323,68 @@ __global__ void k_gather(int N, Gate gate, const int* __restrict__ vpart, const 
   st3(rhs, i, acc);
 }
 
-// Stage Dinv (and L_{R,s} if stage_l) of supernode s into shared memory.  The
-// proxy fence orders this CTA's earlier generic reads of the same shared
-// memory (a previous supernode of the persistent solve) before the bulk writes.
-__device__ __forceinline__ void stage_blocks_issue(const FactorDev& f, int s, int w, int r, double* Dsh, double* Lsh,
-                                                   uint64_t* bar) {
-  if (threadIdx.x == 0) {
-    const unsigned bd = (unsigned)(((w * w + 1) & ~1) * sizeof(double));
-    const unsigned bl = f.stage_l ? (unsigned)(((r * w + 1) & ~1) * sizeof(double)) : 0u;
+// ----------------------------------------------------------- solves ----
+//
+// A supernode is solved by a group of threads: a whole CTA, or one warp of a
+// CTA that solves several small supernodes side by side (one per warp).  The
+// order of every sum is fixed by the supernode alone, not by the group, so the
+// two forms, every CTA size and the persistent solve give bit-identical
+// results.
+struct CtaGroup {
+  __device__ static int rank() { return threadIdx.x; }
+  __device__ static int size() { return blockDim.x; }
+  __device__ static int warp() { return threadIdx.x >> 5; }
+  __device__ static int nwarps() { return blockDim.x >> 5; }
+  __device__ static int index_in_block() { return 0; }
+  __device__ static int per_block() { return 1; }
+  __device__ static void sync() { __syncthreads(); }
+  __device__ static bool all(bool p) { return __syncthreads_and(p ? 1 : 0) != 0; }
+};
+struct WarpGroup {
+  __device__ static int rank() { return threadIdx.x & 31; }
+  __device__ static int size() { return 32; }
+  __device__ static int warp() { return 0; }
+  __device__ static int nwarps() { return 1; }
+  __device__ static int index_in_block() { return threadIdx.x >> 5; }
+  __device__ static int per_block() { return blockDim.x >> 5; }
+  __device__ static void sync() { __syncwarp(); }
+  __device__ static bool all(bool p) {
+    const bool r = __all_sync(0xffffffffu, p) != 0;
+    __syncwarp();
+    return r;
+  }
+};
+
+__device__ __forceinline__ int even_count(int v) { return (v + 1) & ~1; }
+
+// Shared memory of one supernode solve (doubles; the bulk-copy targets start
+// at even offsets, i.e. 16-byte aligned):
+//   D (even(w*w)) | L_{R,s} (even(r*w), if staged) | t (3w) | ...
+//   forward:  ... | y_s (3w) | contributions (3 nseg) | row -> contribution range (w + 1 ints)
+//   backward: ... | x_R (3r)
+// (solve_shm_doubles in engine.cu sizes it.)
+
+// Stage the diagonal-block inverse (column-major for the forward solve,
+// row-major for the backward) and, if in.stage, L_{R,s}.  Rank 0 of the group
+// issues the bulk copies.  The proxy fence orders the group's earlier generic
+// reads of the same shared memory (a previous supernode of the persistent
+// solve) before the bulk writes.
+template <class G>
+__device__ __forceinline__ void stage_blocks_issue(const FactorDev& f, const SnInfo& in, bool fwd, double* Dsh,
+                                                   double* Lsh, uint64_t* bar) {
+  if (G::rank() == 0) {
+    const unsigned bd = (unsigned)(even_count(in.w * in.w) * sizeof(double));
+    const unsigned bl = in.stage ? (unsigned)(even_count(in.r * in.w) * sizeof(double)) : 0u;
     fence_proxy_async_smem();
     mbar_expect_tx(bar, bd + bl);
-    bulk_copy_g2s(Dsh, f.Dinv + f.sn_dofs[s], bd, bar);
-    if (bl) bulk_copy_g2s(Lsh, f.Lcm + f.sn_lofs[s], bl, bar);
+    bulk_copy_g2s(Dsh, (fwd ? f.DinvC : f.Dinv) + in.dofs, bd, bar);
+    if (bl) bulk_copy_g2s(Lsh, f.Lcm + in.lofs, bl, bar);
   }
 }
 
 // A bounded wait gave up: status[0] = 6 (DFEM_ERR_CAP), status[1] = the
 // supernode, status[2] = which wait (1 forward / 2 backward staging, 3 / 4
-// persistent-solve dependency), status[3] counts the CTAs that gave up.
+// persistent-solve dependency), status[3] counts the groups that gave up.
 __device__ __forceinline__ void record_gave_up(const FactorDev& f, int s, int which) {
   f.status[0] = 6;
   f.status[1] = s;
@@ -349,181 +393,215 @@ __device__ __forceinline__ void record_gave_up(const FactorDev& f, int s, int wh
 }
 
 // Wait for the staged blocks (phase parity `phase` of the barrier); false,
-// uniformly across the CTA, when the bounded wait gave up.
+// uniformly across the group, when the bounded wait gave up.  Includes the
+// group barrier.
+template <class G>
 __device__ __forceinline__ bool stage_blocks_wait(const FactorDev& f, uint64_t* bar, unsigned phase, int s, int which) {
-  const bool ok = __syncthreads_and(mbar_wait_bounded(bar, phase) ? 1 : 0) != 0;
-  if (!ok && threadIdx.x == 0) {
+  const bool ok = G::all(mbar_wait_bounded(bar, phase));
+  if (!ok && G::rank() == 0) {
     record_gave_up(f, s, which);
     mbar_wait_bounded(bar, phase);  // give in-flight copies one more bounded chance to land
   }
   return ok;
 }
 
-// Forward solve of supernode s, push form:
+// Forward solve of one supernode, push form:
 //   t   = rhs_s - (contributions pushed to s's rows by its descendants)
-//   y_s = Dinv_s t                       (warp per row)
-//   contrib[R_s] = L_{R_s,s} y_s         (thread per below-diagonal row; read by ancestors)
-// One thread moves the supernode's dense blocks (the inverse of the diagonal
-// block and, when it fits, the below-diagonal block) into shared memory with
-// TMA bulk copies (unless the caller already issued them); while they are in
-// flight the warps sum each row's descendant contributions.  Everything after
-// the barrier runs from shared memory.  Values written by other CTAs of the
-// same launch (contributions) are read through L2 (ld.cg).  Shared layout
-// (doubles): Dinv (w*w, even) | L_{R,s} (r*w, even; if staged) | t (3w) |
-// y_s (3w) | row -> segment range (w+1 ints) | gathered contributions (3 per segment).
-__device__ __forceinline__ bool fwd_supernode(const FactorDev& f, int s, const double* __restrict__ rhs, double* y,
-                                              double* sh, uint64_t* bar, unsigned phase, bool issued = false) {
-  const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
+//   y_s = Dinv_s t                       (one row per thread)
+//   contributions of s = L_{R_s,s} y_s   (one below-diagonal row per thread)
+// The contributions are stored grouped by destination row, so a supernode
+// reads those to its rows as one contiguous range, with all threads at once,
+// while its dense blocks are in flight; each row then sums its own in a fixed
+// order.  Values written by other CTAs of the same launch (persistent solve)
+// are read through L2 (ld.cg).
+template <class G>
+__device__ __forceinline__ bool fwd_supernode(const FactorDev& f, const SnInfo& in, const double* __restrict__ rhs,
+                                              double* y, double* sh, uint64_t* bar, unsigned phase, bool issued) {
+  const int c0 = in.c0, w = in.w, r = in.r, nseg = in.nseg;
   double* Dsh = sh;
-  double* Lsh = sh + ((w * w + 1) & ~1);
-  double* tsh = Lsh + (f.stage_l ? ((r * w + 1) & ~1) : 0);
+  double* Lsh = sh + even_count(w * w);
+  double* tsh = Lsh + (in.stage ? even_count(r * w) : 0);
   double* ysh = tsh + 3 * w;
-  int* psh = reinterpret_cast<int*>(ysh + 3 * w);
-  double* qsh = ysh + 3 * w + (w + 2) / 2;
-  if (!issued) stage_blocks_issue(f, s, w, r, Dsh, Lsh, bar);
-  // The descendants' contributions to this supernode's rows are one contiguous
-  // range of the row-segment list (its rows are contiguous): fetch it with all
-  // threads at once, then reduce each row in a fixed order.
-  const int seg0 = f.rseg_ptr[c0], nseg = f.rseg_ptr[c0 + w] - seg0;
-  for (int c = threadIdx.x; c <= w; c += blockDim.x) psh[c] = f.rseg_ptr[c0 + c] - seg0;
-  for (int k = threadIdx.x; k < nseg; k += blockDim.x) {
-    const double* q = f.contrib + 3 * (size_t)f.rseg_pos[seg0 + k];
-    qsh[3 * k] = __ldcg(q); qsh[3 * k + 1] = __ldcg(q + 1); qsh[3 * k + 2] = __ldcg(q + 2);
-  }
-  for (int c = threadIdx.x; c < w; c += blockDim.x) {
-    const int i = c0 + c;
-    tsh[3 * c] = rhs[3 * i]; tsh[3 * c + 1] = rhs[3 * i + 1]; tsh[3 * c + 2] = rhs[3 * i + 2];
-  }
-  __syncthreads();
-  for (int c = threadIdx.x; c < w; c += blockDim.x) {
+  double* qsh = ysh + 3 * w;
+  int* psh = reinterpret_cast<int*>(qsh + 3 * nseg);
+  if (!issued) stage_blocks_issue<G>(f, in, true, Dsh, Lsh, bar);
+  const int rk = G::rank(), gs = G::size();
+  const double* q = f.contrib + 3 * (size_t)in.seg0;
+#pragma unroll 8
+  for (int k = rk; k < 3 * nseg; k += gs) qsh[k] = __ldcg(q + k);
+  for (int c = rk; c <= w; c += gs) psh[c] = f.rseg_ptr[c0 + c] - in.seg0;
+  for (int k = rk; k < 3 * w; k += gs) tsh[k] = rhs[3 * (size_t)c0 + k];
+  G::sync();
+  for (int c = rk; c < w; c += gs) {
     double a0 = tsh[3 * c], a1 = tsh[3 * c + 1], a2 = tsh[3 * c + 2];
     for (int k = psh[c]; k < psh[c + 1]; ++k) { a0 -= qsh[3 * k]; a1 -= qsh[3 * k + 1]; a2 -= qsh[3 * k + 2]; }
     tsh[3 * c] = a0; tsh[3 * c + 1] = a1; tsh[3 * c + 2] = a2;
   }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (!stage_blocks_wait(f, bar, phase, s, 1)) return false;  // includes the CTA barrier
-  for (int c = warp; c < w; c += nw) {
+  if (!stage_blocks_wait<G>(f, bar, phase, in.s, 1)) return false;
+  // column-major Dinv: the threads of a warp read consecutive words
+  for (int c = rk; c < w; c += gs) {
     double a0 = 0, a1 = 0, a2 = 0;
-    for (int k = lane; k <= c; k += 32) {
-      double dv = Dsh[c * w + k];
+#pragma unroll 4
+    for (int k = 0; k <= c; ++k) {
+      const double dv = Dsh[k * w + c];
       a0 += dv * tsh[3 * k]; a1 += dv * tsh[3 * k + 1]; a2 += dv * tsh[3 * k + 2];
     }
-    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
-    if (lane == 0) {
-      y[3 * (c0 + c)] = a0; y[3 * (c0 + c) + 1] = a1; y[3 * (c0 + c) + 2] = a2;
-      ysh[3 * c] = a0; ysh[3 * c + 1] = a1; ysh[3 * c + 2] = a2;
-    }
+    ysh[3 * c] = a0; ysh[3 * c + 1] = a1; ysh[3 * c + 2] = a2;
+    double* yo = y + 3 * (size_t)(c0 + c);
+    yo[0] = a0; yo[1] = a1; yo[2] = a2;
   }
-  __syncthreads();
-  const double* Lc = f.stage_l ? Lsh : f.Lcm + f.sn_lofs[s];
-  double* out = f.contrib + 3 * (size_t)f.sn_rofs[s];
-  for (int a = threadIdx.x; a < r; a += blockDim.x) {
+  G::sync();
+  const double* Lc = in.stage ? Lsh : f.Lcm + in.lofs;
+  const int* dst = f.cdst + in.rofs;
+  for (int a = rk; a < r; a += gs) {
+    const int d = dst[a];
     double a0 = 0, a1 = 0, a2 = 0;
-#pragma unroll 16
-    for (int c = 0; c < w; ++c) {
-      double l = Lc[(size_t)c * r + a];
+    int c = 0;
+    for (; c + 16 <= w; c += 16) {  // sixteen loads in flight, then the sums in column order
+      double l[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) l[j] = Lc[(size_t)(c + j) * r + a];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const double* yc = ysh + 3 * (c + j);
+        a0 += l[j] * yc[0]; a1 += l[j] * yc[1]; a2 += l[j] * yc[2];
+      }
+    }
+    for (; c < w; ++c) {
+      const double l = Lc[(size_t)c * r + a];
       a0 += l * ysh[3 * c]; a1 += l * ysh[3 * c + 1]; a2 += l * ysh[3 * c + 2];
     }
-    out[3 * a] = a0; out[3 * a + 1] = a1; out[3 * a + 2] = a2;
+    double* o = f.contrib + 3 * (size_t)d;
+    o[0] = a0; o[1] = a1; o[2] = a2;
   }
   return true;
 }
 
-// Backward solve of supernode s (in place in y):
-//   u = y_s - L_{R,s}^T y_R  (column-major block, warp per column)
-//   y_s = Dinv_s^T u
-// Shared layout: Dinv | L_{R,s} (if staged) | u (3w) | gathered ancestor rows y_R (3r).
-__device__ __forceinline__ bool bwd_supernode(const FactorDev& f, int s, double* y, double* sh, uint64_t* bar,
-                                              unsigned phase, bool issued = false) {
-  const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
-  const int* R = f.rowidx + f.sn_rofs[s];
+// Backward solve of one supernode (in place in y):
+//   u   = y_s - L_{R,s}^T y_R   (a warp per column, lanes over rows)
+//   y_s = Dinv_s^T u            (one column per thread; row-major Dinv)
+template <class G>
+__device__ __forceinline__ bool bwd_supernode(const FactorDev& f, const SnInfo& in, double* y, double* sh,
+                                              uint64_t* bar, unsigned phase, bool issued) {
+  const int c0 = in.c0, w = in.w, r = in.r;
+  const int* R = f.rowidx + in.rofs;
   double* Dsh = sh;
-  double* Lsh = sh + ((w * w + 1) & ~1);
-  double* tsh = Lsh + (f.stage_l ? ((r * w + 1) & ~1) : 0);
+  double* Lsh = sh + even_count(w * w);
+  double* tsh = Lsh + (in.stage ? even_count(r * w) : 0);
   double* xr = tsh + 3 * w;
-  if (!issued) stage_blocks_issue(f, s, w, r, Dsh, Lsh, bar);
-  for (int a = threadIdx.x; a < r; a += blockDim.x) {
+  if (!issued) stage_blocks_issue<G>(f, in, false, Dsh, Lsh, bar);
+  const int rk = G::rank(), gs = G::size();
+  for (int a = rk; a < r; a += gs) {
     const double* q = y + 3 * (size_t)R[a];
     xr[3 * a] = __ldcg(q); xr[3 * a + 1] = __ldcg(q + 1); xr[3 * a + 2] = __ldcg(q + 2);
   }
-  for (int c = threadIdx.x; c < w; c += blockDim.x) {
-    const double* q = y + 3 * (size_t)(c0 + c);
-    tsh[3 * c] = __ldcg(q); tsh[3 * c + 1] = __ldcg(q + 1); tsh[3 * c + 2] = __ldcg(q + 2);
-  }
-  if (!stage_blocks_wait(f, bar, phase, s, 2)) return false;  // includes the CTA barrier
-  const double* Lc = f.stage_l ? Lsh : f.Lcm + f.sn_lofs[s];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = rk; k < 3 * w; k += gs) tsh[k] = __ldcg(y + 3 * (size_t)c0 + k);
+  if (!stage_blocks_wait<G>(f, bar, phase, in.s, 2)) return false;
+  const double* Lc = in.stage ? Lsh : f.Lcm + in.lofs;
+  const int lane = threadIdx.x & 31, warp = G::warp(), nw = G::nwarps();
   // four columns per warp pass: four independent load streams per lane
   for (int cb = warp; cb < w; cb += 4 * nw) {
     double acc[4][3];
 #pragma unroll
     for (int q = 0; q < 4; ++q) acc[q][0] = acc[q][1] = acc[q][2] = 0.0;
-    for (int a = lane; a < r; a += 32) {
+    const double* Lq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) Lq[q] = Lc + (size_t)min(cb + q * nw, w - 1) * r;  // clamped: unused when c >= w
+    int a = lane;
+    for (; a + 96 < r; a += 128) {  // four rows x four columns: sixteen loads in flight, then the sums in row order
+      double l[4][4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) l[j][q] = Lq[q][a + 32 * j];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double* xa = xr + 3 * (a + 32 * j);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[q][0] += l[j][q] * xa[0]; acc[q][1] += l[j][q] * xa[1]; acc[q][2] += l[j][q] * xa[2];
+        }
+      }
+    }
+    for (; a < r; a += 32) {
       const double x0 = xr[3 * a], x1 = xr[3 * a + 1], x2 = xr[3 * a + 2];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int c = cb + q * nw;
-        if (c < w) {
-          double l = Lc[(size_t)c * r + a];
-          acc[q][0] += l * x0; acc[q][1] += l * x1; acc[q][2] += l * x2;
-        }
+        const double l = Lq[q][a];
+        acc[q][0] += l * x0; acc[q][1] += l * x1; acc[q][2] += l * x2;
       }
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int c = cb + q * nw;
-      double a0 = warp_sum(acc[q][0]), a1 = warp_sum(acc[q][1]), a2 = warp_sum(acc[q][2]);
+      const double a0 = warp_sum(acc[q][0]), a1 = warp_sum(acc[q][1]), a2 = warp_sum(acc[q][2]);
       if (lane == 0 && c < w) { tsh[3 * c] -= a0; tsh[3 * c + 1] -= a1; tsh[3 * c + 2] -= a2; }
     }
   }
-  __syncthreads();
-  for (int c = warp; c < w; c += nw) {
+  G::sync();
+  for (int c = rk; c < w; c += gs) {
     double a0 = 0, a1 = 0, a2 = 0;
-    for (int k = c + lane; k < w; k += 32) {
-      double dv = Dsh[k * w + c];
+#pragma unroll 4
+    for (int k = c; k < w; ++k) {
+      const double dv = Dsh[k * w + c];
       a0 += dv * tsh[3 * k]; a1 += dv * tsh[3 * k + 1]; a2 += dv * tsh[3 * k + 2];
     }
-    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
-    if (lane == 0) { y[3 * (c0 + c)] = a0; y[3 * (c0 + c) + 1] = a1; y[3 * (c0 + c) + 2] = a2; }
+    double* yo = y + 3 * (size_t)(c0 + c);
+    yo[0] = a0; yo[1] = a1; yo[2] = a2;
   }
   return true;
 }
 
-// One level of the elimination tree per launch (one supernode per CTA; the
-// launch boundary orders the levels).
-__global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, Gate gate,
+// One level of the elimination tree per launch: supernodes lvl_begin ..
+// lvl_begin + count of the level order, one per group (a CTA, or a warp with
+// `shm_group` doubles of shared memory each); the launch boundary orders the
+// levels.
+template <class G>
+__global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, int count, int shm_group, Gate gate,
                                                    const double* __restrict__ rhs, double* y) {
   extern __shared__ __align__(16) double sh[];
-  __shared__ __align__(8) uint64_t bar;
-  const int s = f.lvl_sn[lvl_begin + blockIdx.x];
-  if (gate.skip(f.sn_part ? f.sn_part[s] : 0)) return;
-  if (threadIdx.x == 0) mbar_init(&bar, 1);
-  __syncthreads();
-  fwd_supernode(f, s, rhs, y, sh, &bar, 0);
+  __shared__ __align__(8) uint64_t bars[8];
+  const int gi = G::index_in_block(), item = blockIdx.x * G::per_block() + gi;
+  if (item >= count) return;
+  const SnInfo in = f.info[lvl_begin + item];
+  if (gate.skip(in.part)) return;
+  if (G::rank() == 0) mbar_init(bars + gi, 1);
+  G::sync();
+  fwd_supernode<G>(f, in, rhs, y, sh + (size_t)gi * shm_group, bars + gi, 0, false);
 }
 
-__global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, Gate gate, double* y) {
+template <class G>
+__global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, int count, int shm_group, Gate gate,
+                                                   double* y) {
   extern __shared__ __align__(16) double sh[];
-  __shared__ __align__(8) uint64_t bar;
-  const int s = f.lvl_sn[lvl_begin + blockIdx.x];
-  if (gate.skip(f.sn_part ? f.sn_part[s] : 0)) return;
-  if (threadIdx.x == 0) mbar_init(&bar, 1);
-  __syncthreads();
-  bwd_supernode(f, s, y, sh, &bar, 0);
+  __shared__ __align__(8) uint64_t bars[8];
+  const int gi = G::index_in_block(), item = blockIdx.x * G::per_block() + gi;
+  if (item >= count) return;
+  const SnInfo in = f.info[lvl_begin + item];
+  if (gate.skip(in.part)) return;
+  if (G::rank() == 0) mbar_init(bars + gi, 1);
+  G::sync();
+  bwd_supernode<G>(f, in, y, sh + (size_t)gi * shm_group, bars + gi, 0, false);
 }
 
-// Whole solve (L y = rhs, then L^T z = y, in place) in one launch.  The CTAs
-// claim work items from a ticket counter: tickets 0 .. ns-1 are the forward
-// solves of the supernodes in level order (leaves first), tickets ns .. 2ns-1
-// the backward solves in reverse level order (roots first).  A CTA starts the
-// claimed item's (read-only) block copies, then waits until the supernodes
-// the item reads are done — forward: its children in the elimination tree (a
-// child done implies its whole subtree done); backward: its parent's backward
-// solve, or its own forward solve at a root.  Every awaited item has a lower
-// ticket, so it was claimed earlier by a CTA that is running it: the waits
-// always end.  They are bounded all the same (kSpinTries polls): a CTA that
-// gives up records status 6 and raises the abort word, and every CTA then
-// stops claiming.  Completion is an epoch stamp per supernode and direction
+// The solve of the supernodes at level-order positions p0 .. ns-1 (L y = rhs,
+// then L^T z = y, in place) in one launch; the positions below p0 are solved
+// by level kernels before (forward) and after (backward) it — p0 = 0 is the
+// whole solve.  The CTAs claim work items from a ticket counter: with
+// n = ns - p0, tickets 0 .. n-1 are the forward solves of those supernodes in
+// level order (leaves first), tickets n .. 2n-1 the backward solves in
+// reverse level order (roots first).  A CTA claims its next ticket while it
+// solves the current one (the claim's round trip overlaps the work).  It
+// starts the claimed item's (read-only) block copies, then waits until the
+// supernodes the item reads are done — forward: its children in the
+// elimination tree at positions >= p0 (a child done implies its whole subtree
+// done); backward: its parent's backward solve, or its own forward solve at a
+// root.  Every awaited item has a lower ticket, and a CTA's claimed but
+// unstarted ticket is higher than its current one, so the lowest unfinished
+// ticket is always running with its dependencies done: the waits always end.
+// They are bounded all the same (kSpinTries polls): a CTA that gives up
+// records status 6 and raises the abort word, and every CTA then stops
+// claiming.  Completion is an epoch stamp per supernode and direction
 // (release store after the CTA's writes; acquire loads by the waiter).
 // Control words ctl: [0] ticket, [1] CTAs finished, [2] epoch (>= 1),
 // [3] abort; the last CTA to finish resets the ticket and advances the epoch
@@ -552,38 +630,45 @@ __device__ __forceinline__ bool wait_epoch(const int* flag, int epoch, const int
   return false;
 }
 
-__global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, Gate gate, const double* __restrict__ rhs,
-                                                          double* y) {
+__global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, int p0, Gate gate,
+                                                          const double* __restrict__ rhs, double* y) {
   extern __shared__ __align__(16) double sh[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ int s_ticket, s_epoch, s_go;
-  const int ns = f.nsuper;
+  const int n = f.nsuper - p0;
   int* ctl = f.ctl;
+  int next = 0;  // thread 0: the claimed next ticket
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
     s_epoch = ld_acquire(ctl + 2);
+    next = atomicAdd(ctl + 0, 1);
   }
   __syncthreads();
   const int epoch = s_epoch;
   unsigned phase = 0;
   for (;;) {
     if (threadIdx.x == 0) {
-      const int t = atomicAdd(ctl + 0, 1);
+      const int t = next;
       s_ticket = t;
-      s_go = (t < 2 * ns && ld_acquire(ctl + 3) == 0) ? 1 : 0;
+      s_go = (t < 2 * n && ld_acquire(ctl + 3) == 0) ? 1 : 0;
+      if (s_go) next = atomicAdd(ctl + 0, 1);
     }
     __syncthreads();
     if (!s_go) break;
     const int t = s_ticket;
-    const bool fwd = t < ns;
-    const int s = fwd ? f.lvl_sn[t] : f.lvl_sn[2 * ns - 1 - t];
-    if (!gate.skip(f.sn_part ? f.sn_part[s] : 0)) {
+    const bool fwd = t < n;
+    const SnInfo in = f.info[fwd ? p0 + t : p0 + 2 * n - 1 - t];
+    const int s = in.s;
+    if (!gate.skip(in.part)) {
       // the factor blocks are read-only: start their copies before waiting on the dependencies
-      stage_blocks_issue(f, s, f.sn_w[s], f.sn_r[s], sh, sh + ((f.sn_w[s] * f.sn_w[s] + 1) & ~1), &bar);
+      stage_blocks_issue<CtaGroup>(f, in, fwd, sh, sh + even_count(in.w * in.w), &bar);
       if (threadIdx.x == 0) {
         bool ok = true;
         if (fwd) {
-          for (int k = f.kid_ptr[s]; ok && k < f.kid_ptr[s + 1]; ++k) ok = wait_epoch(f.done_f + f.kid[k], epoch, ctl + 3);
+          for (int k = f.kid_ptr[s]; ok && k < f.kid_ptr[s + 1]; ++k) {
+            const int kid = f.kid[k];
+            if (f.sn_pos[kid] >= p0) ok = wait_epoch(f.done_f + kid, epoch, ctl + 3);
+          }
         } else {
           const int p = f.sn_parent[s];
           ok = wait_epoch(p >= 0 ? f.done_b + p : f.done_f + s, epoch, ctl + 3);
@@ -599,8 +684,8 @@ __global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, Gate gate
         mbar_wait_bounded(&bar, phase);
         break;
       }
-      const bool ok = fwd ? fwd_supernode(f, s, rhs, y, sh, &bar, phase, true)
-                          : bwd_supernode(f, s, y, sh, &bar, phase, true);
+      const bool ok = fwd ? fwd_supernode<CtaGroup>(f, in, rhs, y, sh, &bar, phase, true)
+                          : bwd_supernode<CtaGroup>(f, in, y, sh, &bar, phase, true);
       phase ^= 1u;
       if (!ok) {
         if (threadIdx.x == 0) atomicExch(ctl + 3, 1);

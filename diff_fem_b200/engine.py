@@ -192,13 +192,17 @@ class Scene:
 
     def solve_mode(self, request: Optional[str] = None) -> dict:
         """Form of the global solve: request None (query), "auto" (re-tune),
-        "levels" or "persistent".  Returns the form in use and the autotune's
-        ms per solve of both forms."""
-        req = {None: -1, "auto": 0, "levels": 1, "persistent": 2}[request]
+        "levels", "persistent" or "split" (level kernels below the autotuned
+        cut level, one persistent launch above).  Returns the form in use and
+        the autotune's ms per solve of each form."""
+        req = {None: -1, "auto": 0, "levels": 1, "persistent": 2, "split": 3}[request]
         chosen = C.c_int32()
         ms = (C.c_double * 2)()
         check(lib().dfem_solve_mode(self._h, req, C.byref(chosen), ms))
-        return {"mode": {1: "levels", 2: "persistent"}[chosen.value], "ms_levels": ms[0], "ms_persistent": ms[1]}
+        cut, nl, mss = C.c_int32(), C.c_int32(), C.c_double()
+        check(lib().dfem_solve_split(self._h, C.byref(cut), C.byref(nl), C.byref(mss)))
+        return {"mode": {1: "levels", 2: "persistent", 3: "split"}[chosen.value], "ms_levels": ms[0],
+                "ms_persistent": ms[1], "ms_split": mss.value, "split_level": cut.value, "levels": nl.value}
 
     def profile_levels(self, reps: int = 10) -> dict:
         """ms per launch of every forward / backward launch of the level-kernel

@@ -228,16 +228,21 @@ int dfem_get_iterations(const dfem_scene *scene, int32_t *iters, int32_t n);
  * World::PreComputation + mDynamicSolver.solve (sim/fem/World.h:1089-1139,1660). */
 int dfem_host_factor_solve(const dfem_scene_desc *desc, const double *b, double *x, dfem_scene_info *info);
 
-/* The global solve's form.  request: -1 query, 0 autotune (time both forms
- * on this scene's factor and keep the faster; done once at creation),
- * 1 level kernels (one launch per elimination-tree level and direction),
- * 2 persistent (both triangular sweeps in one launch, supernodes claimed in
- * dependency order).  *chosen (may be NULL) receives the form in use (1 or 2),
- * ms (may be NULL, 2 values) the last autotune's time per solve of each form.
- * Both forms run the same arithmetic per supernode: results are identical.
- * No counterpart in the reference (its solve is Eigen's SimplicialLDLT,
- * sim/fem/World.h:1660). */
+/* The global solve's form.  request: -1 query, 0 autotune (time every form
+ * on this scene's factor and keep the fastest; done once at creation),
+ * 1 level kernels (one launch per elimination-tree level, launch class and
+ * direction), 2 persistent (both triangular sweeps in one launch, supernodes
+ * claimed in dependency order), 3 split (the levels below the autotuned cut
+ * level as level kernels, the rest in one persistent launch).  *chosen (may
+ * be NULL) receives the form in use (1, 2 or 3), ms (may be NULL, 2 values)
+ * the last autotune's time per solve of forms 1 and 2.  Every form runs the
+ * same arithmetic per supernode: results are identical.  No counterpart in
+ * the reference (its solve is Eigen's SimplicialLDLT, sim/fem/World.h:1660). */
 int dfem_solve_mode(dfem_scene *scene, int32_t request, int32_t *chosen, double *ms);
+
+/* The split form found by the last autotune: *cut_level (0: none), the
+ * factor's number of levels, and its time per solve (ms). */
+int dfem_solve_split(const dfem_scene *scene, int32_t *cut_level, int32_t *n_levels, double *ms_split);
 
 /* CUDA-event timing of every launch of the level-kernel solve form (a level
  * of the elimination tree, split into its small and its large supernodes;

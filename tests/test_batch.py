@@ -99,3 +99,37 @@ def test_batch_rejects_mismatched_time_steps():
     descs = [S.cantilever(), S.inverse_stiffness(nx=6, ny=2, nz=2)]
     with pytest.raises(_capi.DfemError, match="time_step"):
         Scene.batch(descs)
+
+
+@pytest.mark.parametrize("form", ["auto", "levels", "split"])
+def test_large_batch_launch_classes_match_scenes(form):
+    """A batch of many supernodes (above the few-supernode staging policy):
+    launch classes per level (one supernode per warp, small and large CTAs),
+    L_{R,s} staged only where it keeps a supernode's class; each scene alone
+    stages by the other policy.  Staging moves no arithmetic: bit-identical."""
+    descs, _ = S.uneven_batch(n_scenes=32, t_hi=1e4, precision=_capi.DFEM_PREC_FP64)
+    b = Scene.batch(descs)
+    assert b.info()["n_supernodes"] > 2048
+    info = b.solve_mode(form)
+    if form != "auto":
+        assert info["mode"] == form
+    n = 2
+    x, v = concat_state(descs)
+    xb, vb = b.forward(x, v, n_steps=n)
+    rng = np.random.default_rng(4)
+    gx = rng.standard_normal(x.size)
+    gb = b.backward(gx, np.zeros_like(gx))
+    vo, to = b.offsets["vertices"], b.offsets["tets"]
+    itb = b.iterations(n)
+    for p in range(0, len(descs), 5):
+        d = descs[p]
+        s = Scene(d)
+        xs, vs = s.forward(d.x0.reshape(-1), np.zeros(3 * d.n_vertices), n_steps=n)
+        assert np.array_equal(s.iterations(n), itb[:, p]), p
+        assert np.array_equal(split(xb, vo)[p], xs), p
+        assert np.array_equal(split(vb, vo)[p], vs), p
+        gs = s.backward(split(gx, vo)[p], np.zeros(3 * d.n_vertices))
+        assert np.array_equal(split(gb["x"], vo)[p], gs["x"]), p
+        assert np.array_equal(gb["E"][to[p]:to[p + 1]], gs["E"]), p
+        s.close()
+    b.close()
