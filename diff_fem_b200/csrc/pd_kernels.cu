@@ -80,6 +80,22 @@ __device__ __forceinline__ Mat3<double> deformation(const double G[4][3], const 
   return F;
 }
 
+// Minimum resident CTAs per SM asked of the register allocator for the
+// heaviest per-constraint kernels (128 threads each): more resident warps hide
+// the FP64 latency chains better than the registers they give up (the
+// adjoint local step of the 256-scene batch: 1.12 ms at 174 registers, 0.85 ms
+// at 128 with spills to L1; the FP32 force step 0.315 -> 0.282 ms, the FP64
+// local step 0.411 -> 0.383 ms).
+#ifndef DFEM_FORCE_MIN_BLOCKS
+#define DFEM_FORCE_MIN_BLOCKS 5
+#endif
+#ifndef DFEM_ADJ_MIN_BLOCKS
+#define DFEM_ADJ_MIN_BLOCKS 4
+#endif
+#ifndef DFEM_LOCAL_MIN_BLOCKS
+#define DFEM_LOCAL_MIN_BLOCKS 5
+#endif
+
 // --------------------------------------------------------------- forward ----
 
 // hist_step: doubles between the iterate records of consecutive steps (0: one
@@ -131,7 +147,7 @@ __global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt
 
 // Local step: every constraint projects and writes its J*d contribution to its
 // slots.  One thread per constraint; constraint types are consecutive ranges.
-__global__ void __launch_bounds__(128) k_local(SceneDev d, Gate gate, const double* __restrict__ x,
+__global__ void __launch_bounds__(128, DFEM_LOCAL_MIN_BLOCKS) k_local(SceneDev d, Gate gate, const double* __restrict__ x,
                                                const double* __restrict__ act_all, const int* step,
                                                double* __restrict__ slot) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -226,7 +242,7 @@ __device__ __forceinline__ Vec3<float> ld3f(const float* p, int i) { return mk3(
 // Inputs of cancelling differences (F, spring lengths, Laplacians) are formed
 // in FP64 first.
 
-__global__ void __launch_bounds__(128) k_force_f32(SceneDev d, Gate gate, const double* __restrict__ x,
+__global__ void __launch_bounds__(128, DFEM_FORCE_MIN_BLOCKS) k_force_f32(SceneDev d, Gate gate, const double* __restrict__ x,
                                                    const double* __restrict__ act_all, const int* step,
                                                    float* __restrict__ slot) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -959,7 +975,7 @@ __device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const d
 
 // Reverse PD iteration k (k read from device memory): local VJP at x^k with
 // the Hs term of x^{k+1}, and bbar += ybar (b = M/h^2 q_n enters every iteration).
-__global__ void __launch_bounds__(128) k_adj_local(SceneDev d, Gate gate, const int* kptr, const int* step,
+__global__ void __launch_bounds__(128, DFEM_ADJ_MIN_BLOCKS) k_adj_local(SceneDev d, Gate gate, const int* kptr, const int* step,
                                                    const double* __restrict__ hist, long long hist_step,
                                                    const double* __restrict__ yb,
                                                    double* bb, const double* __restrict__ act_all,
