@@ -45,8 +45,9 @@ int report_error(int code, const std::string& msg) { return fail(code, msg); }
 struct LoopGraph {
   cudaGraphExec_t exec = nullptr;
   size_t outside = 0;  // kernels outside the loops
-  size_t body = 0;     // kernels per iteration of the first loop
+  size_t body = 0;     // kernels per iteration of the first loop (its solve in the tuned form)
   size_t body2 = 0;    // kernels per iteration of the second loop (contact phase), if any
+  size_t alt_less = 0; // kernels fewer in an iteration whose solve took the persistent form
 };
 
 template <typename T>
@@ -114,6 +115,7 @@ struct dfem_scene {
   int solve_cut = 0;
   int split_cut = 0;                     // the autotune's best split (0: none)
   double solve_ms[3] = {0.0, 0.0, 0.0};  // autotune timings (ms per solve): levels, persistent, best split
+  double select_ms[2] = {0.0, 0.0};      // batches, only the largest part active: tuned form, persistent form
   // numeric refactorisation on the GPU (material changes)
   DBuf<double> hs_base, hc_coef, Ldw, part_reg, E_in, nu_in;
   DBuf<int> hc_ptr, hc_tet, up_ptr, up_d, up_a0, up_a1, part_fail;
@@ -154,6 +156,16 @@ struct dfem_scene {
   // graphs
   LoopGraph g_step, g_adj;
   cudaStream_t stream2 = nullptr;         // capture stream of the loop bodies
+  cudaStream_t stream3 = nullptr;         // capture stream of the solve-form branches inside a body
+  // Batches: per-iteration choice of the solve form (persistent once the
+  // weight of the parts still iterating drops below select_w).
+  bool solve_select = false;
+  double select_w = 0.0;
+  DBuf<double> part_w;                    // per part: its share of the factor's entries
+  DBuf<unsigned long long> sel_count;     // [forward, adjoint]: iterations that took the persistent form
+  size_t cur_alt_less = 0;                // capture bookkeeping of the body being built
+  cudaError_t cur_capture_err = cudaSuccess;
+  unsigned long long sel_seen[2] = {0, 0}; // sel_count as last read
   DBuf<int> kiter;                        // device-side iteration counter of the loops
   int64_t launches = 0;                   // kernels launched by this scene (graph nodes included)
   int rec_steps = 0;
@@ -166,6 +178,7 @@ struct dfem_scene {
     if (g_adj.exec) cudaGraphExecDestroy(g_adj.exec);
     if (stream) cudaStreamDestroy(stream);
     if (stream2) cudaStreamDestroy(stream2);
+    if (stream3) cudaStreamDestroy(stream3);
   }
 };
 
@@ -216,15 +229,24 @@ static void solve_shm_doubles(int w, int r, int nseg, bool staged, size_t* nf, s
 // CTA); CTAs with at most kSmallCtaDoubles (several CTAs per SM); the rest.
 // A class of a level with fewer than kMinClass members joins the next larger
 // class of that level (one launch less; its members fit one wave anyway).
-constexpr size_t kWarpGroupDoubles = 512;
-constexpr size_t kSmallCtaDoubles = 3072;
+#ifndef DFEM_WARP_GROUP_DOUBLES
+#define DFEM_WARP_GROUP_DOUBLES 512
+#endif
+#ifndef DFEM_SMALL_CTA_DOUBLES
+#define DFEM_SMALL_CTA_DOUBLES 3072
+#endif
+#ifndef DFEM_FEW_SUPERNODES
+#define DFEM_FEW_SUPERNODES 2048
+#endif
+constexpr size_t kWarpGroupDoubles = DFEM_WARP_GROUP_DOUBLES;
+constexpr size_t kSmallCtaDoubles = DFEM_SMALL_CTA_DOUBLES;
 constexpr int kMinClass = 64;
 static int shm_class(size_t need) { return need <= kWarpGroupDoubles ? 0 : need <= kSmallCtaDoubles ? 1 : 2; }
 // Factors of few supernodes (one scene: latency-bound solves) stage L_{R,s}
 // whenever the solve still fits 220 KB of shared memory; factors of many
 // (batches) stage it only where that keeps the supernode in its launch class
 // and within 110 KB, so that the classes keep several CTAs per SM.
-constexpr int kFewSupernodes = 2048;
+constexpr int kFewSupernodes = DFEM_FEW_SUPERNODES;
 
 static int upload_factor(dfem_scene* sc) {
   SupernodalFactor& F = sc->hs.F;
@@ -687,8 +709,7 @@ static void launch_segment(dfem_scene* sc, cudaStream_t st, const dfem_scene::Le
 
 static int n_levels(const dfem_scene* sc) { return (int)sc->lvl_ptr.size() - 1; }
 
-static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
-  const int c = sc->solve_cut;
+static void enqueue_solve_cut(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y, int c) {
   for (const auto& g : sc->segs)
     if (g.level < c) launch_segment(sc, st, g, true, g.thr_f, gate, rhs, y);
   if (c < n_levels(sc)) {
@@ -700,10 +721,59 @@ static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const doub
     if (it->level < c) launch_segment(sc, st, *it, false, it->thr_b, gate, rhs, y);
 }
 
-static int solve_launches(const dfem_scene* sc) {
-  int n = sc->solve_cut < n_levels(sc) ? 1 : 0;
-  for (const auto& g : sc->segs) n += g.level < sc->solve_cut ? 2 : 0;
+static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
+  enqueue_solve_cut(sc, st, gate, rhs, y, sc->solve_cut);
+}
+
+static int solve_launches_cut(const dfem_scene* sc, int c) {
+  int n = c < n_levels(sc) ? 1 : 0;
+  for (const auto& g : sc->segs) n += g.level < c ? 2 : 0;
   return n;
+}
+static int solve_launches(const dfem_scene* sc) { return solve_launches_cut(sc, sc->solve_cut); }
+
+// The solve inside a loop body being captured on st.  With the per-iteration
+// choice on: a selection kernel, then a conditional IF/ELSE node whose
+// branches hold the tuned form and the persistent form (captured on stream3).
+// which: 0 forward, 1 adjoint (its counter of persistent iterations).
+static cudaError_t capture_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y, int which) {
+  if (!sc->solve_select || sc->solve_cut == 0) {
+    enqueue_solve(sc, st, gate, rhs, y);
+    return cudaGetLastError();
+  }
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  cudaGraph_t cg = nullptr;
+  cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd);
+  cudaGraphConditionalHandle h{};
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, cg, 0, cudaGraphCondAssignDefault);
+  if (e != cudaSuccess) return e;
+  k_solve_select<<<1, 256, 0, st>>>(gate, sc->part_w.p, sc->hs.nparts, sc->select_w, sc->sel_count.p + which, h);
+  e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &nd);
+  if (e != cudaSuccess) return e;
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = cudaGraphCondTypeIf;
+  p.conditional.size = 2;  // [0] condition true, [1] else
+  cudaGraphNode_t cn = nullptr;
+  e = cudaGraphAddNode(&cn, cg, deps, nd, &p);
+  if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(st, &cn, 1, cudaStreamSetCaptureDependencies);
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+    e = cudaStreamBeginCaptureToGraph(sc->stream3, p.conditional.phGraph_out[b], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) break;
+    enqueue_solve_cut(sc, sc->stream3, gate, rhs, y, b == 0 ? sc->solve_cut : 0);
+    cudaGraph_t tmp;
+    const cudaError_t e2 = cudaStreamEndCapture(sc->stream3, &tmp);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = e2;
+  }
+  // the body's node count sees the select kernel and the IF node: count the
+  // tuned branch's kernels instead of the IF node, and what the other has fewer
+  sc->cur_alt_less = (size_t)(solve_launches_cut(sc, sc->solve_cut) - solve_launches_cut(sc, 0));
+  return e;
 }
 
 // 1: level kernels, 2: persistent, 3: split
@@ -817,7 +887,8 @@ static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandl
   const Gate g = fwd_gate(sc);
   launch_local(sc, st, g, sc->xk.p, sc->act_all.p, sc->step.p);
   launch_gather(sc, st, g, sc->c0.p, sc->rhs.p, sc->xk.p);
-  enqueue_solve(sc, st, g, sc->rhs.p, sc->y.p);
+  const cudaError_t ce = capture_solve(sc, st, g, sc->rhs.p, sc->y.p, 0);
+  if (ce != cudaSuccess) sc->cur_capture_err = ce;
   k_update<<<sc->nblk_p, kPartBlock, 0, st>>>(s.N, sc->pd, mixed(sc) ? 1 : 0, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->hist_step, sc->step.p,
                                sc->flag.p, sc->iters.p, sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
   k_loop_ctl<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, s.nparts, s.K, h);
@@ -841,7 +912,8 @@ static void adj_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle 
 static void adj_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   const HostScene& s = sc->hs;
   const Gate g = adj_gate(sc);
-  enqueue_solve(sc, st, g, sc->xkb.p, sc->y.p);
+  const cudaError_t ce = capture_solve(sc, st, g, sc->xkb.p, sc->y.p, 1);
+  if (ce != cudaSuccess) sc->cur_capture_err = ce;
   launch_adj_local(sc, st, g, sc->kiter.p);
   launch_adj_gather(sc, st, g);
   if (s.nseg > 0)
@@ -870,6 +942,7 @@ static int build_loop_graph(dfem_scene* sc, const std::vector<LoopStage>& stages
   CK(cudaGraphCreate(&g, 0));
   std::string where = "capture";
   std::vector<cudaGraph_t> bodies;
+  std::vector<size_t> alt_less;
   cudaError_t e = cudaStreamBeginCaptureToGraph(sc->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     for (const LoopStage& stage : stages) {
@@ -901,9 +974,15 @@ static int build_loop_graph(dfem_scene* sc, const std::vector<LoopStage>& stages
         e = cudaStreamBeginCaptureToGraph(sc->stream2, body_g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
         where = "capture loop body";
         if (e == cudaSuccess) {
+          sc->cur_alt_less = 0;
+          sc->cur_capture_err = cudaSuccess;
           stage.body(sc, sc->stream2, h);
           cudaGraph_t tmp;
-          e = cudaStreamEndCapture(sc->stream2, &tmp);
+          const cudaError_t e2 = cudaStreamEndCapture(sc->stream2, &tmp);
+          e = cudaGetLastError();
+          if (e == cudaSuccess) e = sc->cur_capture_err;
+          if (e == cudaSuccess) e = e2;
+          alt_less.push_back(sc->cur_alt_less);
         }
       }
     }
@@ -920,8 +999,12 @@ static int build_loop_graph(dfem_scene* sc, const std::vector<LoopStage>& stages
     for (size_t k = 0; k < 2; ++k) {
       size_t inner = 0;
       if (k < bodies.size()) cudaGraphGetNodes(bodies[k], nullptr, &inner);
+      // an IF node of the solve form: its tuned branch's kernels instead of the node
+      if (k < alt_less.size() && alt_less[k] > 0)
+        inner += (size_t)solve_launches(sc) - 1;
       (k == 0 ? out->body : out->body2) = inner;
     }
+    out->alt_less = alt_less.empty() ? 0 : alt_less[0];
     e = cudaGraphInstantiate(&out->exec, g, 0);
     where = "instantiate";
   }
@@ -1032,8 +1115,76 @@ static int status_error(const int st4[4]) {
   return DFEM_OK;
 }
 
-// Time both solve forms on this scene's factor (10 solves each after 3 warm-up
-// solves) and keep the faster.
+// Batches: while the parts still iterating hold much of the work, the tuned
+// form (level kernels below the cut) is fastest; with few left, the
+// persistent form is (the level kernels launch every supernode's CTA to skip
+// it).  Each form's time per solve is modelled as linear in the active
+// weight w (the parts' shares of the factor's entries), between all parts
+// active and only the largest one; the solve switches to the persistent form
+// below the crossing.  Off for one scene or when the tuned form is the
+// persistent one.
+static int tune_solve_select(dfem_scene* sc) {
+  const HostScene& s = sc->hs;
+  sc->solve_select = false;
+  invalidate_graphs(sc);
+  if (s.nparts < 2 || sc->solve_cut == 0) return DFEM_OK;
+  const SupernodalFactor& F = s.F;
+  std::vector<double> w(s.nparts, 0.0);
+  for (int q = 0; q < F.nsuper; ++q) {
+    const int p = (int)(std::upper_bound(s.part_v0.begin(), s.part_v0.end(), F.sn_c0[q]) - s.part_v0.begin()) - 1;
+    w[p] += (double)F.sn_w[q] * (F.sn_w[q] + F.sn_r[q]);
+  }
+  double tot = 0.0;
+  for (double v : w) tot += v;
+  for (double& v : w) v /= tot;
+  const int big = (int)(std::max_element(w.begin(), w.end()) - w.begin());
+  CK(sc->part_w.upload(w));
+  if (!sc->sel_count.p) {
+    CK(sc->sel_count.alloc(2));
+    CK(cudaMemset(sc->sel_count.p, 0, 2 * sizeof(unsigned long long)));
+    sc->sel_seen[0] = sc->sel_seen[1] = 0;
+  }
+  // a gate with only the largest part open
+  std::vector<int> flags(s.nparts, 1);
+  flags[big] = 0;
+  DBuf<int> fl;
+  CK(fl.upload(flags));
+  Gate one;
+  one.flag = fl.p;
+  one.nparts = s.nparts;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  auto time_form = [&](int c, Gate g) -> double {
+    for (int r = 0; r < 3; ++r) enqueue_solve_cut(sc, sc->stream, g, sc->rhs.p, sc->y.p, c);
+    cudaEventRecord(e0, sc->stream);
+    for (int r = 0; r < 10; ++r) enqueue_solve_cut(sc, sc->stream, g, sc->rhs.p, sc->y.p, c);
+    cudaEventRecord(e1, sc->stream);
+    float t = 0;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess) return -1.0;
+    sc->launches += 13 * (int64_t)solve_launches_cut(sc, c);
+    return t / 10.0;
+  };
+  const double tc1 = time_form(sc->solve_cut, one), t01 = time_form(0, one);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaGetLastError());
+  if (tc1 < 0 || t01 < 0) return fail(DFEM_ERR_CUDA, "solve-form selection timing failed");
+  const double tcF = sc->solve_ms[sc->solve_cut == n_levels(sc) ? 0 : 2], t0F = sc->solve_ms[1];
+  const double d1 = tc1 - t01, dF = tcF - t0F;  // tuned minus persistent: one part / all parts
+  sc->select_ms[0] = tc1;
+  sc->select_ms[1] = t01;
+  if (d1 <= 0.0 || dF >= 0.0) return DFEM_OK;  // no crossing: the tuned form throughout
+  const double f1 = w[big];
+  sc->select_w = f1 + (1.0 - f1) * d1 / (d1 - dF);
+  sc->solve_select = true;
+  return DFEM_OK;
+}
+
+// Time the solve forms on this scene's factor (10 solves each after 3 warm-up
+// solves): the CTA size of every level-kernel launch, then the level-kernel
+// form, the persistent form and the split form at every cut level; keep the
+// fastest, then tune the per-iteration selection of batches.
 static int autotune_solve(dfem_scene* sc) {
   const size_t n3 = 3 * (size_t)sc->hs.N;
   CK(cudaMemsetAsync(sc->rhs.p, 0, n3 * sizeof(double), sc->stream));
@@ -1100,6 +1251,7 @@ static int autotune_solve(dfem_scene* sc) {
   RC(status_error(st4));
   sc->solve_cut = sc->solve_ms[1] < sc->solve_ms[0] ? 0 : L;
   if (sc->split_cut > 0 && sc->solve_ms[2] < std::min(sc->solve_ms[0], sc->solve_ms[1])) sc->solve_cut = sc->split_cut;
+  RC(tune_solve_select(sc));
   invalidate_graphs(sc);
   return DFEM_OK;
 }
@@ -1108,6 +1260,7 @@ static int autotune_solve(dfem_scene* sc) {
 static int create_on_device(std::unique_ptr<dfem_scene>& sc, int device, dfem_scene** out) {
   CK(cudaStreamCreate(&sc->stream));  // blocking: orders with the legacy default stream callers use
   CK(cudaStreamCreateWithFlags(&sc->stream2, cudaStreamNonBlocking));  // only used to capture loop bodies
+  CK(cudaStreamCreateWithFlags(&sc->stream3, cudaStreamNonBlocking));
   CK(sc->kiter.alloc(1));
   CK(sc->status.alloc(4));  // before the factor upload, whose kernels report into it
   {
@@ -1290,7 +1443,13 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   sc->rec_passes.assign(2 * (size_t)n_steps, 0);
   if (sc->has_contact)
     CK(cudaMemcpyAsync(sc->rec_passes.data(), sc->cpasses.p, 2 * n_steps * sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+  unsigned long long sel[2] = {0, 0};
+  if (sc->sel_count.p) CK(cudaMemcpyAsync(sel, sc->sel_count.p, sizeof(sel), cudaMemcpyDeviceToHost, sc->stream));
   CK(cudaStreamSynchronize(sc->stream));
+  if (sc->sel_count.p) {  // iterations whose solve took the persistent form launched fewer kernels
+    sc->launches -= (int64_t)((sel[0] - sc->sel_seen[0]) * sc->g_step.alt_less);
+    sc->sel_seen[0] = sel[0];
+  }
   sc->rec_iters.assign(n_steps, 0);
   for (int st = 0; st < n_steps; ++st)
     for (int p = 0; p < np; ++p) sc->rec_iters[st] = std::max(sc->rec_iters[st], it_all[(size_t)st * np + p]);
@@ -1371,7 +1530,15 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   if (g_act && s.nseg > 0) RC(copy_out(sc, sc->gact.p, (size_t)sc->rec_steps * s.nseg, g_act, mem));
   int st4[4] = {0, 0, 0, 0};
   CK(cudaMemcpyAsync(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost, sc->stream));
+  unsigned long long sel[2] = {0, 0};
+  if (sc->sel_count.p) CK(cudaMemcpyAsync(sel, sc->sel_count.p, sizeof(sel), cudaMemcpyDeviceToHost, sc->stream));
   CK(cudaStreamSynchronize(sc->stream));
+  if (sc->sel_count.p) {  // replayed forward iterations and adjoint iterations that took the persistent form
+    sc->launches -= (int64_t)((sel[0] - sc->sel_seen[0]) * sc->g_step.alt_less +
+                              (sel[1] - sc->sel_seen[1]) * sc->g_adj.alt_less);
+    sc->sel_seen[0] = sel[0];
+    sc->sel_seen[1] = sel[1];
+  }
   return status_error(st4);
 }
 
@@ -1487,13 +1654,22 @@ int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms
   } else if (request > 0) {
     if (request == 3 && sc->split_cut == 0) return fail(DFEM_ERR_INVALID, "no split form (fewer than two levels)");
     const int c = request == 1 ? n_levels(sc) : request == 2 ? 0 : sc->split_cut;
-    if (c != sc->solve_cut) {
+    if (c != sc->solve_cut || sc->solve_select) {  // a requested form is used in every iteration
       sc->solve_cut = c;
+      sc->solve_select = false;
       invalidate_graphs(sc);
     }
   }
   if (chosen) *chosen = solve_form(sc);
   if (ms) { ms[0] = sc->solve_ms[0]; ms[1] = sc->solve_ms[1]; }
+  return DFEM_OK;
+}
+
+int dfem_solve_select(const dfem_scene* sc, int32_t* on, double* weight_threshold, double* ms_one_part) {
+  if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
+  if (on) *on = sc->solve_select ? 1 : 0;
+  if (weight_threshold) *weight_threshold = sc->solve_select ? sc->select_w : 0.0;
+  if (ms_one_part) { ms_one_part[0] = sc->select_ms[0]; ms_one_part[1] = sc->select_ms[1]; }
   return DFEM_OK;
 }
 

@@ -800,6 +800,30 @@ __global__ void k_loop_ctl(int* kptr, const int* flag, int nparts, int K, cudaGr
   }
 }
 
+// Form of this iteration's solve in a batch: the summed weight (factor
+// entries) of the parts still iterating against a threshold -- 1: the form
+// tuned for the whole batch, 0: the persistent form, cheaper once few parts
+// are left.  Both forms give identical results, so the choice only moves
+// time.  sel_count counts the iterations that took the persistent form.
+__global__ void k_solve_select(Gate gate, const double* __restrict__ part_w, int nparts, double threshold,
+                               unsigned long long* sel_count, cudaGraphConditionalHandle h) {
+  __shared__ double red[256];
+  double a = 0.0;
+  for (int p = threadIdx.x; p < nparts; p += blockDim.x)
+    if (!gate.skip(p)) a += part_w[p];
+  red[threadIdx.x] = a;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const bool full = red[0] >= threshold;
+    if (!full) atomicAdd(sel_count, 1ull);
+    cudaGraphSetConditional(h, full ? 1u : 0u);
+  }
+}
+
 // Before the loop: run the body at all only if some part did not converge in the first test.
 __global__ void k_loop_enter(int* kptr, const int* flag, int nparts, int K, cudaGraphConditionalHandle h) {
   int open = 0;

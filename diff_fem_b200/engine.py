@@ -201,8 +201,12 @@ class Scene:
         check(lib().dfem_solve_mode(self._h, req, C.byref(chosen), ms))
         cut, nl, mss = C.c_int32(), C.c_int32(), C.c_double()
         check(lib().dfem_solve_split(self._h, C.byref(cut), C.byref(nl), C.byref(mss)))
+        on, thr, one = C.c_int32(), C.c_double(), (C.c_double * 2)()
+        check(lib().dfem_solve_select(self._h, C.byref(on), C.byref(thr), one))
         return {"mode": {1: "levels", 2: "persistent", 3: "split"}[chosen.value], "ms_levels": ms[0],
-                "ms_persistent": ms[1], "ms_split": mss.value, "split_level": cut.value, "levels": nl.value}
+                "ms_persistent": ms[1], "ms_split": mss.value, "split_level": cut.value, "levels": nl.value,
+                "tail_persistent_below": thr.value if on.value else None,
+                "ms_largest_part_only": [one[0], one[1]]}
 
     def profile_levels(self, reps: int = 10) -> dict:
         """ms per launch of every forward / backward launch of the level-kernel

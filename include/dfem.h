@@ -233,7 +233,9 @@ int dfem_host_factor_solve(const dfem_scene_desc *desc, const double *b, double 
  * 1 level kernels (one launch per elimination-tree level, launch class and
  * direction), 2 persistent (both triangular sweeps in one launch, supernodes
  * claimed in dependency order), 3 split (the levels below the autotuned cut
- * level as level kernels, the rest in one persistent launch).  *chosen (may
+ * level as level kernels, the rest in one persistent launch); a form
+ * requested with 1-3 is used in every iteration (no per-iteration selection,
+ * see dfem_solve_select).  *chosen (may
  * be NULL) receives the form in use (1, 2 or 3), ms (may be NULL, 2 values)
  * the last autotune's time per solve of forms 1 and 2.  Every form runs the
  * same arithmetic per supernode: results are identical.  No counterpart in
@@ -243,6 +245,13 @@ int dfem_solve_mode(dfem_scene *scene, int32_t request, int32_t *chosen, double 
 /* The split form found by the last autotune: *cut_level (0: none), the
  * factor's number of levels, and its time per solve (ms). */
 int dfem_solve_split(const dfem_scene *scene, int32_t *cut_level, int32_t *n_levels, double *ms_split);
+
+/* Batches, after an autotune: the solve of an iteration takes the persistent
+ * form when the parts still iterating hold less than *weight_threshold of the
+ * factor's entries (*on = 1; 0: the tuned form in every iteration, as after an
+ * explicit form request).  ms_one_part (may be NULL, 2 values): time per solve
+ * with only the largest part active, tuned form and persistent form. */
+int dfem_solve_select(const dfem_scene *scene, int32_t *on, double *weight_threshold, double *ms_one_part);
 
 /* CUDA-event timing of every launch of the level-kernel solve form (a level
  * of the elimination tree, split into its small and its large supernodes;

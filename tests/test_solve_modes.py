@@ -56,3 +56,26 @@ def test_persistent_solve_in_a_batch_with_converged_parts():
             assert np.array_equal(a[2][k], b[2][k]), (form, k)
         assert np.array_equal(a[3], b[3]), form
     sc.close()
+
+
+def test_batch_tail_selection_matches_fixed_form():
+    """After an autotune a batch may switch each iteration's solve to the
+    persistent form once few parts are left; the result is that of a fixed form."""
+    from diff_fem_b200 import _capi
+    descs, _ = S.uneven_batch(n_scenes=24, t_hi=8e3, precision=_capi.DFEM_PREC_FP64)
+    sc = Scene.batch(descs)
+    act = np.random.default_rng(3).uniform(0, 1, (3, sc.nseg))
+    info = sc.solve_mode("auto")
+    assert info["ms_largest_part_only"][1] > 0 or info["mode"] == "persistent"
+    x = np.concatenate([q.x0.reshape(-1) for q in descs])
+    xa, va = sc.forward(x, np.zeros_like(x), n_steps=3, act=act)
+    rng = np.random.default_rng(5)
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    ga = sc.backward(gx, gv)
+    b = run(sc, descs, 3, "levels", act)
+    assert np.array_equal(xa, b[0]) and np.array_equal(va, b[1])
+    rng = np.random.default_rng(5)
+    gb = sc.backward(rng.standard_normal(x.size), rng.standard_normal(x.size))
+    for k in ga:
+        assert np.array_equal(ga[k], gb[k]), k
+    sc.close()
