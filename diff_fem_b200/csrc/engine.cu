@@ -217,9 +217,9 @@ static void refresh_scene_view(dfem_scene* sc) {
 
 // Shared memory (doubles) of one supernode's forward / backward solve, with
 // or without L_{R,s} staged; mirrors the layout in pd_kernels.cu.
-static void solve_shm_doubles(int w, int r, int nseg, bool staged, size_t* nf, size_t* nb) {
+static void solve_shm_doubles(int w, int r, int nseg, bool staged, int cc, size_t* nf, size_t* nb) {
   auto even = [](size_t v) { return (v + 1) & ~size_t(1); };
-  const size_t W = w, R = r, l = staged ? even(R * W) : 0;
+  const size_t W = w, R = r, l = staged ? even(R * W) : 2 * (size_t)cc * R;
   *nf = even(even(W * W) + l + 6 * W + 3 * (size_t)nseg + (W + 2) / 2);
   *nb = even(even(W * W) + l + 3 * W + 3 * R);
 }
@@ -235,18 +235,15 @@ static void solve_shm_doubles(int w, int r, int nseg, bool staged, size_t* nf, s
 #ifndef DFEM_SMALL_CTA_DOUBLES
 #define DFEM_SMALL_CTA_DOUBLES 3072
 #endif
-#ifndef DFEM_FEW_SUPERNODES
-#define DFEM_FEW_SUPERNODES 2048
-#endif
 constexpr size_t kWarpGroupDoubles = DFEM_WARP_GROUP_DOUBLES;
 constexpr size_t kSmallCtaDoubles = DFEM_SMALL_CTA_DOUBLES;
 constexpr int kMinClass = 64;
 static int shm_class(size_t need) { return need <= kWarpGroupDoubles ? 0 : need <= kSmallCtaDoubles ? 1 : 2; }
-// Factors of few supernodes (one scene: latency-bound solves) stage L_{R,s}
-// whenever the solve still fits 220 KB of shared memory; factors of many
-// (batches) stage it only where that keeps the supernode in its launch class
-// and within 110 KB, so that the classes keep several CTAs per SM.
-constexpr int kFewSupernodes = DFEM_FEW_SUPERNODES;
+// L_{R,s} is staged in shared memory whenever the solve then still fits 220 KB
+// (on the 256-scene batch this ran 4 % faster than staging only where the
+// supernode keeps its launch class: the long dependency chains at the top of
+// the elimination trees gain more from the bulk copies than the launch
+// classes lose in resident CTAs).
 
 static int upload_factor(dfem_scene* sc) {
   SupernodalFactor& F = sc->hs.F;
@@ -281,22 +278,29 @@ static int upload_factor(dfem_scene* sc) {
     CK(sc->DinvC.upload(dc));
   }
   sc->lvl_ptr = F.lvl_ptr;
-  // per supernode: staging of L_{R,s}, shared memory, launch class
+  // per supernode: staging or streaming of L_{R,s}, shared memory, launch class
   const size_t budget = 220 * 1024;
-  std::vector<int> stage(ns), nseg(ns), cls(ns);
+  std::vector<int> stage(ns), nseg(ns), cls(ns), chunk(ns, 0);
   std::vector<size_t> need(ns);
   size_t max_cta = 0;
   for (int q = 0; q < ns; ++q) {
     const int w = F.sn_w[q], r = F.sn_r[q];
     nseg[q] = F.rseg_ptr[F.sn_c0[q] + w] - F.rseg_ptr[F.sn_c0[q]];
     size_t uf, ub, tf, tb;
-    solve_shm_doubles(w, r, nseg[q], false, &uf, &ub);
-    solve_shm_doubles(w, r, nseg[q], true, &tf, &tb);
+    solve_shm_doubles(w, r, nseg[q], false, 0, &uf, &ub);
+    solve_shm_doubles(w, r, nseg[q], true, 0, &tf, &tb);
     const size_t u = std::max(uf, ub), t = std::max(tf, tb);
     if (8 * u > budget)
       return fail(DFEM_ERR_INVALID, "supernode too large for the shared-memory staging of the triangular solves");
-    stage[q] = r > 0 && (ns <= kFewSupernodes ? 8 * t <= budget : shm_class(t) == shm_class(u) && 8 * t <= budget / 2);
+    stage[q] = r > 0 && 8 * t <= budget;
     need[q] = stage[q] ? t : u;
+    if (!stage[q] && r > 0) {  // stream it: the widest even chunk whose two buffers fit
+      const size_t cc = std::min<size_t>(((budget / 8 - u) / (2 * (size_t)r)) & ~size_t(1), (size_t)w);
+      if (cc >= 2) {
+        chunk[q] = (int)cc;
+        need[q] = u + 2 * cc * (size_t)r;
+      }
+    }
     cls[q] = shm_class(need[q]);
     max_cta = std::max(max_cta, 8 * need[q]);
   }
@@ -323,7 +327,7 @@ static int upload_factor(dfem_scene* sc) {
       for (int k = cut[c]; k < cut[c + 1]; ++k) {
         const int q = F.lvl_sn[k];
         size_t nf, nb;
-        solve_shm_doubles(F.sn_w[q], F.sn_r[q], nseg[q], stage[q] != 0, &nf, &nb);
+        solve_shm_doubles(F.sn_w[q], F.sn_r[q], nseg[q], stage[q] != 0, chunk[q], &nf, &nb);
         mf = std::max(mf, nf);
         mb = std::max(mb, nb);
       }
@@ -351,7 +355,7 @@ static int upload_factor(dfem_scene* sc) {
     for (int k = 0; k < ns; ++k) {
       const int q = F.lvl_sn[k];
       info[k] = SnInfo{F.sn_c0[q], F.sn_w[q], F.sn_r[q], (int)F.sn_rofs[q], (int)F.sn_lofs[q], (int)F.sn_dofs[q],
-                       F.rseg_ptr[F.sn_c0[q]], nseg[q], q, snp[q], stage[q], 0};
+                       F.rseg_ptr[F.sn_c0[q]], nseg[q], q, snp[q], stage[q], chunk[q]};
     }
     CK(sc->sn_info.upload(info));
   }

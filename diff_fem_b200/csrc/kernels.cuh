@@ -162,7 +162,7 @@ struct SnInfo {
   int s;          // supernode id (elimination tree, completion stamps)
   int part;       // batch part
   int stage;      // 1: L_{R,s} is staged in shared memory too
-  int pad;
+  int cc;         // not staged: columns per chunk of L_{R,s} streamed through two shared buffers (0: read from global)
 };
 
 struct FactorDev {

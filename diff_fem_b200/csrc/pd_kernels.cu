@@ -380,14 +380,42 @@ __device__ __forceinline__ int even_count(int v) { return (v + 1) & ~1; }
 //   backward: ... | x_R (3r)
 // (solve_shm_doubles in engine.cu sizes it.)
 
+// Rows per thread of a streamed forward panel (its accumulators live in
+// registers); a supernode with more rows than kStreamRows x the group size
+// reads L_{R,s} from global memory instead.
+constexpr int kStreamRows = 4;
+
+template <class G>
+__device__ __forceinline__ bool streamed(const SnInfo& in) {
+  return !in.stage && in.cc > 0 && in.r <= kStreamRows * G::size();
+}
+
+// Doubles of the L_{R,s} region: the whole block (staged), two chunk buffers
+// (streamed), or nothing.
+__device__ __forceinline__ int lsh_doubles(const SnInfo& in) {
+  return in.stage ? even_count(in.r * in.w) : in.cc > 0 ? 2 * in.cc * in.r : 0;
+}
+
+// Chunk k of a streamed L_{R,s} (columns k cc .. min(w, (k+1) cc), one
+// contiguous range of the column-major block; cc is even, so every chunk but
+// the last starts and ends on 16 bytes, and the last one's rounding stays
+// inside the block's even-padded storage) into buffer k & 1.
+__device__ __forceinline__ void issue_chunk(const FactorDev& f, const SnInfo& in, int k, double* Lsh, uint64_t* sbar) {
+  const int c0 = k * in.cc, nc = min(in.cc, in.w - c0);
+  const unsigned bytes = (unsigned)(even_count(nc * in.r) * sizeof(double));
+  mbar_expect_tx(sbar + (k & 1), bytes);
+  bulk_copy_g2s(Lsh + (size_t)(k & 1) * in.cc * in.r, f.Lcm + in.lofs + (size_t)c0 * in.r, bytes, sbar + (k & 1));
+}
+
 // Stage the diagonal-block inverse (column-major for the forward solve,
-// row-major for the backward) and, if in.stage, L_{R,s}.  Rank 0 of the group
-// issues the bulk copies.  The proxy fence orders the group's earlier generic
-// reads of the same shared memory (a previous supernode of the persistent
-// solve) before the bulk writes.
+// row-major for the backward) and, if in.stage, L_{R,s}; for a streamed
+// L_{R,s}, start its first two chunks.  Rank 0 of the group issues the bulk
+// copies.  The proxy fence orders the group's earlier generic reads of the
+// same shared memory (a previous supernode of the persistent solve) before
+// the bulk writes.
 template <class G>
 __device__ __forceinline__ void stage_blocks_issue(const FactorDev& f, const SnInfo& in, bool fwd, double* Dsh,
-                                                   double* Lsh, uint64_t* bar) {
+                                                   double* Lsh, uint64_t* bar, uint64_t* sbar) {
   if (G::rank() == 0) {
     const unsigned bd = (unsigned)(even_count(in.w * in.w) * sizeof(double));
     const unsigned bl = in.stage ? (unsigned)(even_count(in.r * in.w) * sizeof(double)) : 0u;
@@ -395,6 +423,19 @@ __device__ __forceinline__ void stage_blocks_issue(const FactorDev& f, const SnI
     mbar_expect_tx(bar, bd + bl);
     bulk_copy_g2s(Dsh, (fwd ? f.DinvC : f.Dinv) + in.dofs, bd, bar);
     if (bl) bulk_copy_g2s(Lsh, f.Lcm + in.lofs, bl, bar);
+    if (streamed<G>(in)) {
+      issue_chunk(f, in, 0, Lsh, sbar);
+      if (in.cc < in.w) issue_chunk(f, in, 1, Lsh, sbar);
+    }
+  }
+}
+
+// Let a streamed block's copies still in flight land (an aborted item).
+template <class G>
+__device__ __forceinline__ void drain_chunks(const SnInfo& in, uint64_t* sbar, const unsigned* sph) {
+  if (G::rank() == 0 && streamed<G>(in)) {
+    mbar_wait_bounded(sbar, sph[0]);
+    if (in.cc < in.w) mbar_wait_bounded(sbar + 1, sph[1]);
   }
 }
 
@@ -421,6 +462,100 @@ __device__ __forceinline__ bool stage_blocks_wait(const FactorDev& f, uint64_t* 
   return ok;
 }
 
+// Wait for chunk k of a streamed block (buffer k & 1); false, uniformly across
+// the group, when the bounded wait gave up (after letting the chunks still in
+// flight land).
+template <class G>
+__device__ __forceinline__ bool wait_chunk(const FactorDev& f, const SnInfo& in, int k, int nch, uint64_t* sbar,
+                                           unsigned* sph, int which) {
+  const int b = k & 1;
+  if (G::all(mbar_wait_bounded(sbar + b, sph[b]))) {
+    sph[b] ^= 1u;
+    return true;
+  }
+  if (G::rank() == 0) {
+    record_gave_up(f, in.s, which);
+    mbar_wait_bounded(sbar + b, sph[b]);
+    if (k + 1 < nch) mbar_wait_bounded(sbar + (b ^ 1), sph[b ^ 1]);
+  }
+  return false;
+}
+
+// L_{R,s} y_s into the contribution slots with L_{R,s} streamed through two
+// shared buffers: rows rk, rk + gs, .. of a thread accumulate in registers
+// over the chunks, each row's sum in column order.
+template <class G>
+__device__ __forceinline__ bool fwd_panel_stream(const FactorDev& f, const SnInfo& in, double* Lsh, uint64_t* sbar,
+                                                 unsigned* sph, const double* __restrict__ ysh) {
+  const int r = in.r, w = in.w, cc = in.cc, rk = G::rank(), gs = G::size();
+  const int nch = (w + cc - 1) / cc;
+  double acc[kStreamRows][3];
+#pragma unroll
+  for (int j = 0; j < kStreamRows; ++j) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
+  for (int k = 0; k < nch; ++k) {
+    if (!wait_chunk<G>(f, in, k, nch, sbar, sph, 5)) return false;
+    const double* Lb = Lsh + (size_t)(k & 1) * cc * r;
+    const int c0 = k * cc, nc = min(cc, w - c0);
+#pragma unroll
+    for (int j = 0; j < kStreamRows; ++j) {
+      const int a = rk + j * gs;
+      if (a < r) {
+        for (int c = 0; c < nc; ++c) {
+          const double l = Lb[c * r + a];
+          const double* yc = ysh + 3 * (c0 + c);
+          acc[j][0] += l * yc[0]; acc[j][1] += l * yc[1]; acc[j][2] += l * yc[2];
+        }
+      }
+    }
+    G::sync();  // the buffer is free again
+    if (rk == 0 && k + 2 < nch) {
+      fence_proxy_async_smem();
+      issue_chunk(f, in, k + 2, Lsh, sbar);
+    }
+  }
+  const int* dst = f.cdst + in.rofs;
+#pragma unroll
+  for (int j = 0; j < kStreamRows; ++j) {
+    const int a = rk + j * gs;
+    if (a < r) {
+      double* o = f.contrib + 3 * (size_t)dst[a];
+      o[0] = acc[j][0]; o[1] = acc[j][1]; o[2] = acc[j][2];
+    }
+  }
+  return true;
+}
+
+// u_c -= (L_{R,s}^T x_R)_c with L_{R,s} streamed: a warp per column of the
+// chunk, lanes over rows, then the warp sum (per column the same order as
+// bwd_panel).
+template <class G>
+__device__ __forceinline__ bool bwd_panel_stream(const FactorDev& f, const SnInfo& in, double* Lsh, uint64_t* sbar,
+                                                 unsigned* sph, const double* __restrict__ xr, double* tsh) {
+  const int r = in.r, w = in.w, cc = in.cc;
+  const int lane = threadIdx.x & 31, warp = G::warp(), nw = G::nwarps();
+  const int nch = (w + cc - 1) / cc;
+  for (int k = 0; k < nch; ++k) {
+    if (!wait_chunk<G>(f, in, k, nch, sbar, sph, 6)) return false;
+    const double* Lb = Lsh + (size_t)(k & 1) * cc * r;
+    const int c0 = k * cc, nc = min(cc, w - c0);
+    for (int c = warp; c < nc; c += nw) {
+      double a0 = 0, a1 = 0, a2 = 0;
+      for (int a = lane; a < r; a += 32) {
+        const double l = Lb[c * r + a];
+        a0 += l * xr[3 * a]; a1 += l * xr[3 * a + 1]; a2 += l * xr[3 * a + 2];
+      }
+      a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+      if (lane == 0) { tsh[3 * (c0 + c)] -= a0; tsh[3 * (c0 + c) + 1] -= a1; tsh[3 * (c0 + c) + 2] -= a2; }
+    }
+    G::sync();
+    if (G::rank() == 0 && k + 2 < nch) {
+      fence_proxy_async_smem();
+      issue_chunk(f, in, k + 2, Lsh, sbar);
+    }
+  }
+  return true;
+}
+
 // Forward solve of one supernode, push form:
 //   t   = rhs_s - (contributions pushed to s's rows by its descendants)
 //   y_s = Dinv_s t                       (one row per thread)
@@ -432,15 +567,16 @@ __device__ __forceinline__ bool stage_blocks_wait(const FactorDev& f, uint64_t* 
 // are read through L2 (ld.cg).
 template <class G>
 __device__ __forceinline__ bool fwd_supernode(const FactorDev& f, const SnInfo& in, const double* __restrict__ rhs,
-                                              double* y, double* sh, uint64_t* bar, unsigned phase, bool issued) {
+                                              double* y, double* sh, uint64_t* bar, unsigned phase, uint64_t* sbar,
+                                              unsigned* sph, bool issued) {
   const int c0 = in.c0, w = in.w, r = in.r, nseg = in.nseg;
   double* Dsh = sh;
   double* Lsh = sh + even_count(w * w);
-  double* tsh = Lsh + (in.stage ? even_count(r * w) : 0);
+  double* tsh = Lsh + lsh_doubles(in);
   double* ysh = tsh + 3 * w;
   double* qsh = ysh + 3 * w;
   int* psh = reinterpret_cast<int*>(qsh + 3 * nseg);
-  if (!issued) stage_blocks_issue<G>(f, in, true, Dsh, Lsh, bar);
+  if (!issued) stage_blocks_issue<G>(f, in, true, Dsh, Lsh, bar, sbar);
   const int rk = G::rank(), gs = G::size();
   const double* q = f.contrib + 3 * (size_t)in.seg0;
 #pragma unroll 8
@@ -453,7 +589,10 @@ __device__ __forceinline__ bool fwd_supernode(const FactorDev& f, const SnInfo& 
     for (int k = psh[c]; k < psh[c + 1]; ++k) { a0 -= qsh[3 * k]; a1 -= qsh[3 * k + 1]; a2 -= qsh[3 * k + 2]; }
     tsh[3 * c] = a0; tsh[3 * c + 1] = a1; tsh[3 * c + 2] = a2;
   }
-  if (!stage_blocks_wait<G>(f, bar, phase, in.s, 1)) return false;
+  if (!stage_blocks_wait<G>(f, bar, phase, in.s, 1)) {
+    drain_chunks<G>(in, sbar, sph);
+    return false;
+  }
   // column-major Dinv: the threads of a warp read consecutive words
   for (int c = rk; c < w; c += gs) {
     double a0 = 0, a1 = 0, a2 = 0;
@@ -467,6 +606,7 @@ __device__ __forceinline__ bool fwd_supernode(const FactorDev& f, const SnInfo& 
     yo[0] = a0; yo[1] = a1; yo[2] = a2;
   }
   G::sync();
+  if (streamed<G>(in)) return fwd_panel_stream<G>(f, in, Lsh, sbar, sph, ysh);
   const double* Lc = in.stage ? Lsh : f.Lcm + in.lofs;
   const int* dst = f.cdst + in.rofs;
   for (int a = rk; a < r; a += gs) {
@@ -498,23 +638,30 @@ __device__ __forceinline__ bool fwd_supernode(const FactorDev& f, const SnInfo& 
 //   y_s = Dinv_s^T u            (one column per thread; row-major Dinv)
 template <class G>
 __device__ __forceinline__ bool bwd_supernode(const FactorDev& f, const SnInfo& in, double* y, double* sh,
-                                              uint64_t* bar, unsigned phase, bool issued) {
+                                              uint64_t* bar, unsigned phase, uint64_t* sbar, unsigned* sph,
+                                              bool issued) {
   const int c0 = in.c0, w = in.w, r = in.r;
   const int* R = f.rowidx + in.rofs;
   double* Dsh = sh;
   double* Lsh = sh + even_count(w * w);
-  double* tsh = Lsh + (in.stage ? even_count(r * w) : 0);
+  double* tsh = Lsh + lsh_doubles(in);
   double* xr = tsh + 3 * w;
-  if (!issued) stage_blocks_issue<G>(f, in, false, Dsh, Lsh, bar);
+  if (!issued) stage_blocks_issue<G>(f, in, false, Dsh, Lsh, bar, sbar);
   const int rk = G::rank(), gs = G::size();
   for (int a = rk; a < r; a += gs) {
     const double* q = y + 3 * (size_t)R[a];
     xr[3 * a] = __ldcg(q); xr[3 * a + 1] = __ldcg(q + 1); xr[3 * a + 2] = __ldcg(q + 2);
   }
   for (int k = rk; k < 3 * w; k += gs) tsh[k] = __ldcg(y + 3 * (size_t)c0 + k);
-  if (!stage_blocks_wait<G>(f, bar, phase, in.s, 2)) return false;
+  if (!stage_blocks_wait<G>(f, bar, phase, in.s, 2)) {
+    drain_chunks<G>(in, sbar, sph);
+    return false;
+  }
   const double* Lc = in.stage ? Lsh : f.Lcm + in.lofs;
   const int lane = threadIdx.x & 31, warp = G::warp(), nw = G::nwarps();
+  if (streamed<G>(in)) {
+    if (!bwd_panel_stream<G>(f, in, Lsh, sbar, sph, xr, tsh)) return false;
+  } else
   // four columns per warp pass: four independent load streams per lane
   for (int cb = warp; cb < w; cb += 4 * nw) {
     double acc[4][3];
@@ -576,28 +723,32 @@ template <class G>
 __global__ void __launch_bounds__(256) k_fwd_level(FactorDev f, int lvl_begin, int count, int shm_group, Gate gate,
                                                    const double* __restrict__ rhs, double* y) {
   extern __shared__ __align__(16) double sh[];
-  __shared__ __align__(8) uint64_t bars[8];
+  __shared__ __align__(8) uint64_t bars[8][3];  // per group: blocks, stream buffers 0 and 1
   const int gi = G::index_in_block(), item = blockIdx.x * G::per_block() + gi;
   if (item >= count) return;
   const SnInfo in = f.info[lvl_begin + item];
   if (gate.skip(in.part)) return;
-  if (G::rank() == 0) mbar_init(bars + gi, 1);
+  if (G::rank() == 0)
+    for (int b = 0; b < 3; ++b) mbar_init(&bars[gi][b], 1);
   G::sync();
-  fwd_supernode<G>(f, in, rhs, y, sh + (size_t)gi * shm_group, bars + gi, 0, false);
+  unsigned sph[2] = {0u, 0u};
+  fwd_supernode<G>(f, in, rhs, y, sh + (size_t)gi * shm_group, &bars[gi][0], 0, &bars[gi][1], sph, false);
 }
 
 template <class G>
 __global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, int count, int shm_group, Gate gate,
                                                    double* y) {
   extern __shared__ __align__(16) double sh[];
-  __shared__ __align__(8) uint64_t bars[8];
+  __shared__ __align__(8) uint64_t bars[8][3];  // per group: blocks, stream buffers 0 and 1
   const int gi = G::index_in_block(), item = blockIdx.x * G::per_block() + gi;
   if (item >= count) return;
   const SnInfo in = f.info[lvl_begin + item];
   if (gate.skip(in.part)) return;
-  if (G::rank() == 0) mbar_init(bars + gi, 1);
+  if (G::rank() == 0)
+    for (int b = 0; b < 3; ++b) mbar_init(&bars[gi][b], 1);
   G::sync();
-  bwd_supernode<G>(f, in, y, sh + (size_t)gi * shm_group, bars + gi, 0, false);
+  unsigned sph[2] = {0u, 0u};
+  bwd_supernode<G>(f, in, y, sh + (size_t)gi * shm_group, &bars[gi][0], 0, &bars[gi][1], sph, false);
 }
 
 // The solve of the supernodes at level-order positions p0 .. ns-1 (L y = rhs,
@@ -650,12 +801,16 @@ __global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, int p0, G
                                                           const double* __restrict__ rhs, double* y) {
   extern __shared__ __align__(16) double sh[];
   __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t sbar[2];  // stream buffers of a streamed L_{R,s}
   __shared__ int s_ticket, s_epoch, s_go;
   const int n = f.nsuper - p0;
   int* ctl = f.ctl;
   int next = 0;  // thread 0: the claimed next ticket
+  unsigned sph[2] = {0u, 0u};  // phases of the stream buffers (every thread tracks them alike)
   if (threadIdx.x == 0) {
     mbar_init(&bar, 1);
+    mbar_init(sbar, 1);
+    mbar_init(sbar + 1, 1);
     s_epoch = ld_acquire(ctl + 2);
     next = atomicAdd(ctl + 0, 1);
   }
@@ -677,7 +832,7 @@ __global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, int p0, G
     const int s = in.s;
     if (!gate.skip(in.part)) {
       // the factor blocks are read-only: start their copies before waiting on the dependencies
-      stage_blocks_issue<CtaGroup>(f, in, fwd, sh, sh + even_count(in.w * in.w), &bar);
+      stage_blocks_issue<CtaGroup>(f, in, fwd, sh, sh + even_count(in.w * in.w), &bar, sbar);
       if (threadIdx.x == 0) {
         bool ok = true;
         if (fwd) {
@@ -697,11 +852,12 @@ __global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, int p0, G
       }
       __syncthreads();
       if (!s_go) {  // aborted: let this CTA's copies land before it leaves
-        mbar_wait_bounded(&bar, phase);
+        if (threadIdx.x == 0) mbar_wait_bounded(&bar, phase);
+        drain_chunks<CtaGroup>(in, sbar, sph);
         break;
       }
-      const bool ok = fwd ? fwd_supernode<CtaGroup>(f, in, rhs, y, sh, &bar, phase, true)
-                          : bwd_supernode<CtaGroup>(f, in, y, sh, &bar, phase, true);
+      const bool ok = fwd ? fwd_supernode<CtaGroup>(f, in, rhs, y, sh, &bar, phase, sbar, sph, true)
+                          : bwd_supernode<CtaGroup>(f, in, y, sh, &bar, phase, sbar, sph, true);
       phase ^= 1u;
       if (!ok) {
         if (threadIdx.x == 0) atomicExch(ctl + 3, 1);

@@ -103,10 +103,10 @@ def test_batch_rejects_mismatched_time_steps():
 
 @pytest.mark.parametrize("form", ["auto", "levels", "split"])
 def test_large_batch_launch_classes_match_scenes(form):
-    """A batch of many supernodes (above the few-supernode staging policy):
-    launch classes per level (one supernode per warp, small and large CTAs),
-    L_{R,s} staged only where it keeps a supernode's class; each scene alone
-    stages by the other policy.  Staging moves no arithmetic: bit-identical."""
+    """A batch of many supernodes: launch classes per level (one supernode per
+    warp, small and large CTAs), the split and tail-selected solve forms; each
+    scene alone runs its own factor's schedule and form.  Neither moves any
+    arithmetic: bit-identical."""
     descs, _ = S.uneven_batch(n_scenes=32, t_hi=1e4, precision=_capi.DFEM_PREC_FP64)
     b = Scene.batch(descs)
     assert b.info()["n_supernodes"] > 2048

@@ -241,3 +241,27 @@ def test_cloth_on_ball_forward_and_adjoint():
     bg, bo = g.backward(gx, gv), o.backward(gx, gv)
     for k in ("x", "v"):
         assert rel(bg[k], bo[k]) < GRAD_TOL, (k, rel(bg[k], bo[k]))
+
+
+@pytest.mark.parametrize("form", ["levels", "persistent"])
+def test_streamed_blocks_forward_and_adjoint(form):
+    """A 16x16x16-cube block (20,480 tets): its top supernodes' below-diagonal
+    blocks exceed the shared memory and are streamed through it in column
+    chunks, in both solve forms; against the oracle at the FP64 tolerances."""
+    d = S.inverse_stiffness(nx=16, ny=16, nz=16)
+    g = Scene(d)
+    assert g.solve_mode(form)["mode"] == form
+    o = O.OracleScene(d)
+    x = d.x0.reshape(-1).copy()
+    v = 0.05 * np.random.default_rng(1).standard_normal(x.size)
+    n = 3
+    xg, vg = g.forward(x, v, n_steps=n)
+    ro = o.forward(x, v, n_steps=n)
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(xg, ro["x"]) < POS_TOL and rel(vg, ro["v"]) < POS_TOL
+    rng = np.random.default_rng(2)
+    gx, gv = rng.standard_normal(xg.size), rng.standard_normal(xg.size)
+    bg, bo = g.backward(gx, gv), o.backward(gx, gv)
+    for k in ("x", "v", "E"):
+        assert rel(bg[k], bo[k]) < GRAD_TOL, k
+    g.close()
