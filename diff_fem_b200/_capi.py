@@ -47,6 +47,7 @@ class SceneDescC(C.Structure):
         ("handle_collision", C.c_int32), ("self_collision", C.c_int32),
         ("alpha", C.c_double), ("friction", C.c_double), ("obstacle_friction", C.c_double),
         ("precision", C.c_int32), ("checkpoint_every", C.c_int32),
+        ("underwater", C.c_int32), ("n_drag_faces", C.c_int32), ("drag_faces", _pi),
     ]
 
 

@@ -19,6 +19,7 @@
 #include "pd_kernels.cu"
 #include "contact_kernels.cuh"
 #include "factor_kernels.cuh"
+#include "drag_kernels.cuh"
 #include "scene.h"
 
 namespace dfem {
@@ -88,6 +89,10 @@ struct dfem_scene {
   DBuf<int> mseg, seg_ptr, seg_mus, boff, bv, bslot, vslot_ptr, hs_ptr, hs_col, to_user, to_internal;
   DBuf<double> hs_val;
   DBuf<double> attach_k;             // per-vertex attachment stiffness (mixed form's rhs)
+  // underwater drag: faces, every vertex's face corners, per-face forces and their adjoint
+  int nF = 0;
+  DBuf<int> df, vf_ptr, vf_face;
+  DBuf<double> fdrag, fdrag_b;
   // factor
   DBuf<int> rseg_ptr, cdst, sn_c0, sn_w, sn_r, sn_rofs, rowidx, sn_lofs, sn_dofs, lvl_sn;
   DBuf<double> contrib, Lcm, Dinv, DinvC;
@@ -210,7 +215,8 @@ static void refresh_scene_view(dfem_scene* sc) {
               sc->tslot.p, sc->mv.p, sc->minv.p, sc->mw.p, sc->mfib.p, sc->mseg.p, sc->mslot.p, sc->seg_ptr.p,
               sc->seg_mus.p, sc->sv.p, sc->srest.p, sc->ssw.p, sc->sslot.p, sc->boff.p, sc->bv.p, sc->bbeta.p,
               sc->bw.p, sc->brest.p, sc->bslot.p, sc->vslot_ptr.p, sc->attach_jd.p, sc->hs_ptr.p, sc->hs_col.p,
-              sc->hs_val.p, sc->attach_k.p, sc->vpart.p, sc->seg_part.p};
+              sc->hs_val.p, sc->attach_k.p, sc->vpart.p, sc->seg_part.p,
+              sc->nF ? sc->vf_ptr.p : nullptr, sc->nF ? sc->vf_face.p : nullptr, sc->nF ? sc->fdrag.p : nullptr};
   if (std::memcmp(&sd, &sc->sd, sizeof(sd)) != 0) invalidate_graphs(sc);
   sc->sd = sd;
 }
@@ -601,6 +607,14 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->attach_k.upload(ak));
   CK(sc->to_user.upload(s.to_user));
   CK(sc->to_internal.upload(s.to_internal));
+  sc->nF = (int)s.df.size() / 3;
+  if (sc->nF > 0) {
+    CK(sc->df.upload(s.df));
+    CK(sc->vf_ptr.upload(s.vf_ptr));
+    CK(sc->vf_face.upload(s.vf_face));
+    CK(sc->fdrag.alloc(3 * (size_t)sc->nF));
+    CK(sc->fdrag_b.alloc(18 * (size_t)sc->nF));
+  }
   int rc = upload_materials(sc);
   if (rc) return rc;
   const size_t n3 = 3 * (size_t)s.N;
@@ -858,6 +872,7 @@ static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
 }
 
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
+  if (sc->nF > 0) k_drag_faces<<<(sc->nF + 127) / 128, 128, 0, st>>>(sc->nF, sc->df.p, sc->xt.p, sc->vt.p, sc->fdrag.p);
   k_step_begin<<<sc->nblk_p, kPartBlock, 0, st>>>(sc->sd, sc->pd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
                                    sc->hist.p, sc->hist_step, sc->ckpt_x.p, sc->ckpt_v.p, sc->flag.p, sc->iters.p,
                                    sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p,
@@ -1514,6 +1529,14 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
       const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
       k_cadj_finish<<<nb, 128, 0, sc->stream>>>(s.N, a, sc->io_a.p, sc->io_b.p);
       sc->launches += 1;
+    }
+    if (sc->nF > 0) {  // v_wc = v + h f_drag(x, v) / m: io_b holds the cotangent of v_wc here
+      k_drag_adj_faces<<<(sc->nF + 127) / 128, 128, 0, sc->stream>>>(
+          sc->nF, sc->df.p, sc->mass.p, s.h, sc->ckpt_x.p + (size_t)st * n3, sc->ckpt_v.p + (size_t)st * n3,
+          sc->io_b.p, sc->fdrag_b.p);
+      k_drag_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, sc->vf_ptr.p, sc->vf_face.p, sc->fdrag_b.p, sc->io_a.p,
+                                                     sc->io_b.p);
+      sc->launches += 2;
     }
   }
   if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 0);

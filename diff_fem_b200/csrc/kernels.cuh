@@ -101,6 +101,11 @@ struct SceneDev {
   // batch: part of every vertex and muscle segment (null for a single scene)
   const int* vpart;
   const int* seg_part;
+  // underwater drag: every vertex's face corners (3 f + corner, ascending) and
+  // the per-face force of the step (null without drag faces)
+  const int* vf_ptr;
+  const int* vf_face;
+  const double* fdrag;
 };
 
 __device__ __forceinline__ int vpart_of(const SceneDev& d, int i) { return d.vpart ? d.vpart[i] : 0; }

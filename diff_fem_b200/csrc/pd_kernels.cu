@@ -3,7 +3,7 @@
 // One time step (diff_fem World::TimeStepping + ProjectiveDynamicsMethod,
 // sim/fem/World.h:673-720, 835-917) is this kernel sequence, captured once as
 // a CUDA graph and replayed for every step:
-//   k_step_begin        v_wc = v + g h, q_n = x + h v_wc, c0 = M/h^2 q_n - Hs x + J_att d_att,
+//   k_step_begin        v_wc = v + g h (+ h f_drag / m), q_n = x + h v_wc, c0 = M/h^2 q_n - Hs x + J_att d_att,
 //                       x^0 = q_n, convergence test of the reference's first iteration
 //   K x { k_local       per-constraint projection d and its J*d slot contributions
 //         k_gather      rhs_i = c0_i + sum of vertex i's slots           (ori_c - Qf x)
@@ -117,6 +117,12 @@ __global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt
     // v_wc = v + h M^-1 f_ext (f_ext = 0), q_n = x + h v_wc
     double gm = d.gmask[i] * d.h;
     Vec3<double> vwc = mk3(v.x + gm * d.g0, v.y + gm * d.g1, v.z + gm * d.g2);
+    if (d.vf_ptr) {  // underwater: the drag and lift of the vertex's faces (ascending face order)
+      Vec3<double> f = mk3(0.0, 0.0, 0.0);
+      for (int k = d.vf_ptr[i]; k < d.vf_ptr[i + 1]; ++k) f = f + ld3(d.fdrag, d.vf_face[k] / 3);
+      const double m = d.mass[i];
+      vwc = vwc + mk3(d.h * (f.x / m), d.h * (f.y / m), d.h * (f.z / m));
+    }
     if (vwc_out) st3(vwc_out, i, vwc);
     Vec3<double> q = x + d.h * vwc;
     st3(qn, i, q);

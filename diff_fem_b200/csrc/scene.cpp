@@ -156,7 +156,7 @@ void build_slots(HostScene& s) {
 
 void renumber(HostScene& s, const std::vector<int>& to_int) {
   auto remap = [&](std::vector<int>& v) { for (int& i : v) i = to_int[i]; };
-  remap(s.tv); remap(s.mv); remap(s.sv); remap(s.bv); remap(s.av); remap(s.cverts);
+  remap(s.tv); remap(s.mv); remap(s.sv); remap(s.bv); remap(s.av); remap(s.cverts); remap(s.df);
   std::vector<double> x(3 * (size_t)s.N), m(s.N), g(s.N);
   for (int i = 0; i < s.N; ++i) {
     int j = to_int[i];
@@ -225,6 +225,11 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& s, std::string& err) 
   s.alpha = d.alpha;
   s.mu_obs = d.obstacle_friction;
   s.cverts.assign(d.contact_vertices, d.contact_vertices + d.n_contact_vertices);
+  REQ(d.n_drag_faces >= 0 && (d.n_drag_faces == 0 || d.drag_faces), "descriptor: drag_faces missing");
+  REQ(inrange(d.drag_faces, 3LL * d.n_drag_faces), "descriptor: drag face vertex out of range");
+  s.underwater = d.underwater != 0;
+  if (s.underwater) std::fill(s.gmask.begin(), s.gmask.end(), 0.0);  // Environment::Step: no gravity underwater
+  s.df.assign(d.drag_faces, d.drag_faces + 3 * (size_t)d.n_drag_faces);
   s.obs_x.assign(d.obstacle_x, d.obstacle_x + 3 * (size_t)d.n_obstacle_vertices);
   s.obs_f.assign(d.obstacle_faces, d.obstacle_faces + 3 * (size_t)d.n_obstacle_faces);
 
@@ -304,6 +309,15 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& s, std::string& err) 
   for (int i = 0; i < N; ++i) { s.F.perm[i] = i; s.F.iperm[i] = i; }
   s.Hs = assemble_hs(s);
   build_slots(s);
+  {  // each vertex's drag faces, ascending
+    const int F = (int)s.df.size() / 3;
+    s.vf_ptr.assign(N + 1, 0);
+    for (int e = 0; e < 3 * F; ++e) s.vf_ptr[s.df[e] + 1]++;
+    for (int i = 0; i < N; ++i) s.vf_ptr[i + 1] += s.vf_ptr[i];
+    s.vf_face.assign(3 * (size_t)F, 0);
+    std::vector<int> fill(s.vf_ptr.begin(), s.vf_ptr.end() - 1);
+    for (int e = 0; e < 3 * F; ++e) s.vf_face[fill[s.df[e]]++] = e;  // face slot e = 3 f + corner
+  }
   s.nparts = 1;
   s.part_v0 = {0, s.N};
   s.part_t0 = {0, s.T};
@@ -334,6 +348,7 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
             p.K == a.K && p.precision == a.precision && p.checkpoint_every == a.checkpoint_every,
         "batch: scenes must share time_step, damping, gravity, max_iterations, precision and checkpoint_every");
     REQ(!(p.collide && !p.cverts.empty() && !p.obs_f.empty()), "batch: obstacle contact is supported for single scenes only");
+    REQ(p.df.empty() && !p.underwater, "batch: underwater drag is supported for single scenes only");
     REQ(p.nparts == 1, "batch: parts must be single scenes");
     totN += p.N; totT += p.T; totSlots += p.nslots; totRows += (int64_t)p.F.rowidx.size();
     totL += (int64_t)p.F.Lcm.size(); totD += (int64_t)p.F.Dinv.size();

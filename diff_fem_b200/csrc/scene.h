@@ -51,6 +51,11 @@ struct HostScene {
   std::vector<double> obs_x;
   std::vector<int> obs_f;
 
+  // underwater drag and lift: faces (3 internal ids each, outward winding)
+  // and every vertex's faces in ascending face order (CSR)
+  bool underwater = false;
+  std::vector<int> df, vf_ptr, vf_face;
+
   int nslots = 0;
   std::vector<int> vslot_ptr;           // N+1, slots sorted by vertex
 

@@ -3,6 +3,7 @@
 Follows the setup code of the reference (all setup-time, host side):
   Environment::Environment   sim/Environment.h:86-225   (Parameters, Meshes, Clothes, Obstacles)
   Dfobj::SetDfobj/Initialize sim/Dfobj.h:142-611        (tet OBJ, masses, attachments, surface, muscles)
+  Environment "Is underwater"  sim/Environment.h:161-166,236-247 (drag faces = the meshes' contours)
   Muscle / MakeMuscles       sim/Muscle.h:59-215, sim/Dfobj.h:732-790
   Dfcloth                    sim/Dfcloth.h:120-300      (edge springs w = 200, masses 1.5 * area / 3, no gravity)
   Dfobstacle                 sim/Dfobstacle.h           (static triangle mesh, unscaled)
@@ -168,7 +169,7 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
     av, ap, ak = [], [], []
     mt, mf, mk, ms = [], [], [], []
     spv, spw = [], []
-    cverts, cfaces = [], []
+    cverts, cfaces, dfaces = [], [], []
     bodies: List[Body] = []
     off, nseg_total = 0, 0
     for obj in cfg.get("Meshes", []):
@@ -186,6 +187,7 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
                 av.append(off + i); ap.append(v[i]); ak.append(k)
         faces, cv = S.surface_of(v, t)
         cverts.extend((cv + off).tolist()); cfaces.extend((faces + off).tolist())
+        dfaces.extend((faces + off).tolist())   # Dfobj::mContours (outward surface faces)
         body = Body("mesh", off, n, grav, int(obj.get("Actuator type", 0)), contours=faces, seg_offset=nseg_total)
         if "Muscle filename" in obj:
             fibres = read_muscle_file(_resolve(obj["Muscle filename"], data_root), scale)
@@ -237,5 +239,10 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
         self_collision=bool(par.get("Self-collision", True)),
         alpha=float(par.get("World Alpha", 1.0)), friction=float(par.get("World Friction", 1.0)),
         obstacle_friction=1.0, name=os.path.basename(config_path),
+        # Environment::Step: underwater meshes get drag and lift on their contours instead of gravity
+        # (Environment.h:161-166,236-247); each mesh's faces act on its own vertices
+        underwater=bool(int(par.get("Is underwater", 0))),
+        drag_faces=(np.asarray(dfaces, np.int32).reshape(-1, 3) if int(par.get("Is underwater", 0))
+                    else np.zeros((0, 3), np.int32)),
     )
     return LoadedScene(desc=desc, bodies=bodies, total_step=total_step)

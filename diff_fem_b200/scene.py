@@ -67,6 +67,8 @@ class SceneDesc:
     obstacle_friction: float = 1.0
     precision: int = DFEM_PREC_FP64
     checkpoint_every: int = 1
+    underwater: bool = False
+    drag_faces: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
     name: str = "scene"
 
     @property
@@ -138,6 +140,9 @@ class SceneDesc:
         d.friction = float(self.friction)
         d.obstacle_friction = float(self.obstacle_friction)
         d.precision = int(self.precision)
+        d.underwater = int(bool(self.underwater))
+        d.n_drag_faces = int(np.asarray(self.drag_faces).reshape(-1, 3).shape[0])
+        d.drag_faces = P(self.drag_faces, _i32, C.c_int32)
         d.checkpoint_every = int(self.checkpoint_every)
         return d, keep
 
@@ -463,6 +468,25 @@ def surface_of(x0: np.ndarray, tets: np.ndarray):
                 seen.add(v)
                 verts.append(v)
     return np.asarray(out_f, np.int32), np.asarray(verts, np.int32)
+
+
+def underwater_block(nx: int = 4, ny: int = 2, nz: int = 3, edge: float = 0.05, speed: float = 0.6,
+                     precision: int = DFEM_PREC_FP64, seed: int = 3):
+    """A soft block moving through still water (underwater drag and lift on
+    its outward surface faces, no gravity).  Returns (desc, initial velocity
+    (N,3)): a uniform swim velocity plus a seeded per-vertex wobble."""
+    x0, tets = cube_grid(nx, ny, nz, edge)
+    mass = lumped_masses(x0, tets, 1000.0 * nx * ny * nz * edge ** 3, True)
+    faces, _ = surface_of(x0, tets)
+    T = tets.shape[0]
+    d = SceneDesc(
+        x0=x0, mass=mass, tets=tets, youngs=np.full(T, 3e4), poisson=np.full(T, 0.3),
+        time_step=1.0 / 60.0, max_iterations=10, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        underwater=True, drag_faces=faces, precision=precision, name=f"underwater_block_{nx}x{ny}x{nz}")
+    rng = np.random.default_rng(seed)
+    v0 = np.tile(np.array([speed, 0.25 * speed, -0.4 * speed]), (x0.shape[0], 1))
+    v0 += 0.1 * speed * rng.standard_normal(v0.shape)
+    return d, v0
 
 
 def ground_quad(y: float, half: float, center=(0.0, 0.0)):

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define DFEM_ABI_VERSION 2
+#define DFEM_ABI_VERSION 3
 
 enum dfem_status {
   DFEM_OK = 0,
@@ -117,6 +117,15 @@ typedef struct dfem_scene_desc {
   double obstacle_friction;       /* obstacle mu (diff_fem hardcodes 1)              */
   int32_t precision;              /* enum dfem_precision                             */
   int32_t checkpoint_every;       /* adjoint checkpoint interval in steps (>= 1)     */
+
+  /* underwater drag and lift (Environment::Step underwater branch,
+   * Dfobj::ComputeDragForces, sim/Environment.h:236-247, sim/Dfobj.h:904-998):
+   * with underwater != 0 no vertex receives gravity and every drag face adds
+   * its drag + lift force (computed from the step's start state) to its three
+   * vertices as the external force of World::TimeStepping */
+  int32_t underwater;             /* "Is underwater"                                 */
+  int32_t n_drag_faces;
+  const int32_t *drag_faces;      /* 3 per face, global vertex ids, outward winding  */
 } dfem_scene_desc;
 
 typedef struct dfem_scene dfem_scene;  /* opaque */

@@ -24,7 +24,8 @@
  *   - AttachmentConstraint                                sim/fem/Constraint/AttachmentConstraint.h:70-99
  *   - SpringConstraint                                    sim/fem/Constraint/SpringConstraint.h:51-144
  *   - BendingConstraint                                   sim/fem/Constraint/BendingConstraint.h:66-187,220-300
- *   - Environment::Step gravity                           sim/Environment.h:228-259
+ *   - Environment::Step gravity / underwater branch        sim/Environment.h:228-259
+ *   - Dfobj::ComputeDragForces, Cd, Cl                    sim/Dfobj.h:803-838,904-998
  *   - Dfobj::Initialize tet re-orientation and masses     sim/Dfobj.h:442-525
  *
  * Choices that differ in mechanism but not in result:
@@ -280,6 +281,9 @@ struct Scene {
   std::vector<V3> obs_x;
   std::vector<std::array<int, 3>> obs_f;
   int last_passes = 0;
+  /* underwater drag and lift (Dfobj::ComputeDragForces) */
+  bool underwater = false;
+  std::vector<std::array<int, 3>> drag_f;
   /* envelope Cholesky of Hs in RCM order */
   std::vector<int> perm, iperm;  /* perm[new] = old */
   std::vector<int> first;        /* first column of row i in the envelope */
@@ -592,14 +596,141 @@ static int pd_solve(const Scene& S, const double* x, const double* qn, const dou
   return it;
 }
 
+/* ---- underwater drag and lift ---------------------------------------------
+ * Dfobj::ComputeDragForces (sim/Dfobj.h:904-998) per surface face p1 p2 p3
+ * (outward winding) with vertex velocities v1 v2 v3, water at rest:
+ *   v_rel = -(v1+v2+v3)/3 (face skipped when |v_rel| < 1e-6), u = v_rel/|v_rel|,
+ *   d = -n (n the unit face normal), area = |(p2-p1) x (p3-p1)| / 2,
+ *   c = d.u, aoa = pi/2 - acos(c) (= asin c); only faces with c > 0:
+ *   drag = 500 area Cd(aoa) |v_rel|^2 u with Cd = (1-0)(1-cos 2 aoa)/2 + 0 = c^2,
+ *   lift = 500 area Cl(aoa) |v_rel|^2 (normalize(u x d) x u), Cl the piecewise
+ *   linear table of Dfobj::Cl in degrees with the 85 degree cutoff,
+ *   each clipped to norm 1e3; each vertex of the face receives (drag + lift)/3.
+ * Written once for double and once for a forward-mode dual number (value and
+ * three derivatives) that the adjoint uses, seeding one input vector at a time. */
+struct Dual3 {
+  double v = 0, d[3] = {0, 0, 0};
+  Dual3(double a = 0.0) : v(a) {}
+};
+static inline Dual3 dconst(double a) { return Dual3(a); }
+static inline double val(double a) { return a; }
+static inline double val(const Dual3& a) { return a.v; }
+static inline Dual3 operator+(const Dual3& a, const Dual3& b) { Dual3 r; r.v = a.v + b.v; for (int k = 0; k < 3; ++k) r.d[k] = a.d[k] + b.d[k]; return r; }
+static inline Dual3 operator-(const Dual3& a, const Dual3& b) { Dual3 r; r.v = a.v - b.v; for (int k = 0; k < 3; ++k) r.d[k] = a.d[k] - b.d[k]; return r; }
+static inline Dual3 operator*(const Dual3& a, const Dual3& b) { Dual3 r; r.v = a.v * b.v; for (int k = 0; k < 3; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k]; return r; }
+static inline Dual3 operator/(const Dual3& a, const Dual3& b) { Dual3 r; r.v = a.v / b.v; for (int k = 0; k < 3; ++k) r.d[k] = (a.d[k] - r.v * b.d[k]) / b.v; return r; }
+static inline Dual3 dsqrt(const Dual3& a) { Dual3 r; r.v = std::sqrt(a.v); for (int k = 0; k < 3; ++k) r.d[k] = a.d[k] / (2.0 * r.v); return r; }
+static inline double dsqrt(double a) { return std::sqrt(a); }
+static inline Dual3 dasin(const Dual3& a) { Dual3 r; r.v = std::asin(a.v); double q = 1.0 / std::sqrt(1.0 - a.v * a.v); for (int k = 0; k < 3; ++k) r.d[k] = a.d[k] * q; return r; }
+static inline double dasin(double a) { return std::asin(a); }
+
+template <typename T> struct TV3 { T x, y, z; };
+template <typename T> static inline TV3<T> tadd(const TV3<T>& a, const TV3<T>& b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <typename T> static inline TV3<T> tsub(const TV3<T>& a, const TV3<T>& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <typename T> static inline TV3<T> tscale(const T& s, const TV3<T>& a) { return {s * a.x, s * a.y, s * a.z}; }
+template <typename T> static inline T tdot(const TV3<T>& a, const TV3<T>& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <typename T> static inline TV3<T> tcross(const TV3<T>& a, const TV3<T>& b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+/* Dfobj::Cl (sim/Dfobj.h:813-838) with cutoff 85 and the table
+   x = {-90, -10, -5, 15, 90}, y = {-0.5, -1.26, 0, 1.8, 0.5} (degrees):
+   linear interpolation on the first matching segment. */
+template <typename T> static T lift_coefficient(const T& aoa) {
+  static const double xs[5] = {-90, -10, -5, 15, 90}, ys[5] = {-0.5, -1.26, 0.0, 1.8, 0.5};
+  const T theta = T(180.0 / M_PI) * aoa;
+  const double th = val(theta);
+  const T zero(0.0);
+  if (std::fabs(th) > 85.0) return zero;
+  for (int k = 0; k < 4; ++k) {
+    const bool in = (k < 2) ? (xs[k] <= th && th < xs[k + 1]) : (xs[k] <= th && th <= xs[k + 1]);
+    if (in) {
+      const T t = T(1.0 / (xs[k + 1] - xs[k])) * (theta - T(xs[k]));
+      return T(ys[k + 1] - ys[k]) * t + T(ys[k]);   /* (1 - t) y_k + t y_{k+1} */
+    }
+  }
+  return zero;
+}
+
+/* The force one face adds to each of its three vertices. */
+template <typename T>
+static TV3<T> drag_face_force(const TV3<T>& p1, const TV3<T>& p2, const TV3<T>& p3, const TV3<T>& v1,
+                              const TV3<T>& v2, const TV3<T>& v3) {
+  const TV3<T> zero{T(0.0), T(0.0), T(0.0)};
+  const TV3<T> vrel = tscale(T(-1.0 / 3.0), tadd(tadd(v1, v2), v3));
+  const T s2 = tdot(vrel, vrel);
+  const T s = dsqrt(s2);
+  if (val(s) < 1e-6) return zero;
+  const TV3<T> u = tscale(T(1.0) / s, vrel);
+  const TV3<T> nv = tcross(tsub(p2, p1), tsub(p3, p1));
+  const T an = dsqrt(tdot(nv, nv));
+  const T area = T(0.5) * an;
+  const TV3<T> dd = tscale(T(-1.0) / an, nv);
+  const T c = tdot(dd, u);
+  if (!(val(c) > 0.0)) return zero;
+  TV3<T> fd = tscale(T(500.0) * area * (c * c) * s2, u);
+  /* Cl vanishes above 85 degrees; c >= 1 (rounding) lies there too */
+  const T cl = val(c) < 1.0 ? lift_coefficient(dasin(c)) : T(0.0);
+  const TV3<T> w = tcross(u, dd);
+  const T wn2 = tdot(w, w);
+  TV3<T> fl = zero;
+  if (val(wn2) > 0.0) {
+    const TV3<T> dl = tcross(tscale(T(1.0) / dsqrt(wn2), w), u);
+    fl = tscale(T(500.0) * area * cl * s2, dl);
+  }
+  const double fmax = 1.0e3;
+  const T fdn = dsqrt(tdot(fd, fd)), fln = dsqrt(tdot(fl, fl));
+  if (val(fdn) > fmax) fd = tscale(T(fmax) / fdn, fd);
+  if (val(fln) > fmax) fl = tscale(T(fmax) / fln, fl);
+  return tscale(T(1.0 / 3.0), tadd(fd, fl));
+}
+
+
+static inline TV3<double> tv(const double* x, int i) { return {x[3 * i], x[3 * i + 1], x[3 * i + 2]}; }
+
+/* Per-vertex external force f_ext of the step (zero unless underwater). */
+static void drag_forces(const Scene& S, const double* x, const double* v, double* f) {
+  std::fill(f, f + 3 * S.N, 0.0);
+  for (const auto& fc : S.drag_f) {
+    const TV3<double> g = drag_face_force(tv(x, fc[0]), tv(x, fc[1]), tv(x, fc[2]), tv(v, fc[0]), tv(v, fc[1]), tv(v, fc[2]));
+    for (int k = 0; k < 3; ++k) {
+      f[3 * fc[k]] += g.x; f[3 * fc[k] + 1] += g.y; f[3 * fc[k] + 2] += g.z;
+    }
+  }
+}
+
+/* Cotangents of x and v from the cotangent fb of the per-vertex drag force. */
+static void drag_forces_vjp(const Scene& S, const double* x, const double* v, const double* fb, double* xb, double* vb) {
+  for (const auto& fc : S.drag_f) {
+    double gb[3] = {0, 0, 0};
+    for (int k = 0; k < 3; ++k)
+      for (int c = 0; c < 3; ++c) gb[c] += fb[3 * fc[k] + c];
+    for (int q = 0; q < 6; ++q) {  /* seed input vector q: p1 p2 p3 v1 v2 v3 */
+      TV3<Dual3> in[6];
+      for (int j = 0; j < 6; ++j) {
+        const double* src = j < 3 ? x : v;
+        const int vi = fc[j % 3];
+        in[j] = {dconst(src[3 * vi]), dconst(src[3 * vi + 1]), dconst(src[3 * vi + 2])};
+      }
+      in[q].x.d[0] = 1.0; in[q].y.d[1] = 1.0; in[q].z.d[2] = 1.0;
+      const TV3<Dual3> g = drag_face_force(in[0], in[1], in[2], in[3], in[4], in[5]);
+      double* out = (q < 3 ? xb : vb) + 3 * fc[q % 3];
+      for (int k = 0; k < 3; ++k) out[k] += gb[0] * g.x.d[k] + gb[1] * g.y.d[k] + gb[2] * g.z.d[k];
+    }
+  }
+}
+
 static void step_prep(const Scene& S, const double* x, const double* v, double* vwc, double* qn) {
-  /* Environment::Step adds g*h to v of gravity-enabled bodies; TimeStepping:
-     v_wc = v + h M^-1 f_ext (f_ext = 0), q_n = x + h v_wc. */
+  /* Environment::Step adds g*h to v of gravity-enabled bodies (none when
+     underwater, which sets the drag force instead); TimeStepping:
+     v_wc = v + h M^-1 f_ext, q_n = x + h v_wc. */
+  std::vector<double> f(3 * (size_t)S.N, 0.0);
+  if (!S.drag_f.empty()) drag_forces(S, x, v, f.data());
   for (int i = 0; i < S.N; ++i) {
-    double gm = S.gmask[i];
+    double gm = S.underwater ? 0.0 : S.gmask[i];
     double g3[3] = {S.g.x, S.g.y, S.g.z};
     for (int c = 0; c < 3; ++c) {
-      vwc[3 * i + c] = v[3 * i + c] + gm * g3[c] * S.h;
+      vwc[3 * i + c] = v[3 * i + c] + gm * g3[c] * S.h + S.h * (f[3 * i + c] / S.mass[i]);
       qn[3 * i + c] = x[3 * i + c] + S.h * vwc[3 * i + c];
     }
   }
@@ -1164,6 +1295,9 @@ void* orc_create(const dfem_scene_desc* d) {
     S->obs_x.push_back(V3{d->obstacle_x[3 * k], d->obstacle_x[3 * k + 1], d->obstacle_x[3 * k + 2]});
   for (int k = 0; k < d->n_obstacle_faces; ++k)
     S->obs_f.push_back({d->obstacle_faces[3 * k], d->obstacle_faces[3 * k + 1], d->obstacle_faces[3 * k + 2]});
+  S->underwater = d->underwater != 0;
+  for (int k = 0; k < d->n_drag_faces; ++k)
+    S->drag_f.push_back({d->drag_faces[3 * k], d->drag_faces[3 * k + 1], d->drag_faces[3 * k + 2]});
   S->h = d->time_step;
   S->K = d->max_iterations;
   S->damping = d->damping;
@@ -1266,10 +1400,16 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
     std::vector<double> qnb(n3);
     for (int i = 0; i < N; ++i)
       for (int cc = 0; cc < 3; ++cc) qnb[3 * i + cc] = xkb[3 * i + cc] + S->mass[i] * ih2 * bb[3 * i + cc];
-    /* q_n = x + h v_wc, v_wc = v + g h mask */
+    /* q_n = x + h v_wc, v_wc = v + g h mask + h M^-1 f_ext(x, v) */
     for (int k = 0; k < n3; ++k) {
       xb[k] = xtb[k] + qnb[k];
       vb[k] = S->h * qnb[k] + vwcb[k];
+    }
+    if (!S->drag_f.empty()) {
+      std::vector<double> fb(n3), vwct(vb);  /* vb holds the cotangent of v_wc here */
+      for (int i = 0; i < N; ++i)
+        for (int cc = 0; cc < 3; ++cc) fb[3 * i + cc] = S->h / S->mass[i] * vwct[3 * i + cc];
+      drag_forces_vjp(*S, x, v, fb.data(), xb.data(), vb.data());
     }
   }
   std::copy(xb.begin(), xb.end(), gx);

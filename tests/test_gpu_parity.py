@@ -265,3 +265,25 @@ def test_streamed_blocks_forward_and_adjoint(form):
     for k in ("x", "v", "E"):
         assert rel(bg[k], bo[k]) < GRAD_TOL, k
     g.close()
+
+
+def test_underwater_drag_forward_and_adjoint():
+    """Underwater drag and lift on the surface faces (per-face forces from the
+    step's start state, gathered per vertex into v_wc) and their adjoint,
+    against the oracle at the FP64 tolerances."""
+    d, v0 = S.underwater_block()
+    g = Scene(d)
+    o = O.OracleScene(d)
+    x = d.x0.reshape(-1).copy()
+    v = v0.reshape(-1).copy()
+    n = 4
+    xg, vg = g.forward(x, v, n_steps=n)
+    ro = o.forward(x, v, n_steps=n)
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(xg, ro["x"]) < POS_TOL and rel(vg, ro["v"]) < POS_TOL
+    rng = np.random.default_rng(4)
+    gx, gv = rng.standard_normal(xg.size), rng.standard_normal(xg.size)
+    bg, bo = g.backward(gx, gv), o.backward(gx, gv)
+    for k in ("x", "v", "E"):
+        assert rel(bg[k], bo[k]) < GRAD_TOL, k
+    g.close()

@@ -52,3 +52,20 @@ def test_reference_scenes_load():
     c = loader.load_scene("cloth_ball/cloth_ball.json", 3, data_root=REF_DATA)
     assert [bd.kind for bd in c.bodies] == ["mesh", "cloth"] and c.desc.spring_weight.size > 0
     assert np.all(c.desc.spring_weight == 200.0) and not c.desc.gravity_mask[c.bodies[1].offset:].any()
+
+
+@pytest.mark.skipif(not os.path.exists(REF_DATA), reason="reference data not mounted")
+def test_reference_underwater_scene_loads():
+    """octopus.json sets "Is underwater": its mesh gets drag and lift on its
+    outward surface faces instead of gravity; the oracle steps it.  (fish.json
+    has a trailing comma that the reference's JSON parser rejects too.)"""
+    L = loader.load_scene("octopus/octopus.json", 2, data_root=REF_DATA)
+    d = L.desc
+    assert d.underwater and d.drag_faces.shape[0] > 0 and d.drag_faces.max() < d.n_vertices
+    assert np.array_equal(np.sort(d.drag_faces, axis=1), np.sort(d.contact_faces, axis=1))
+    o = O.OracleScene(d)
+    v = np.tile([0.3, 0.0, 0.0], d.n_vertices)
+    r = o.forward(d.x0.reshape(-1).copy(), v, n_steps=2)
+    assert np.all(np.isfinite(r["x"]))
+    mom0 = 0.3 * d.mass.sum()
+    assert (d.mass * r["v"].reshape(-1, 3)[:, 0]).sum() < mom0   # the water slows it
