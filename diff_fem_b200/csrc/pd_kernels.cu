@@ -869,11 +869,11 @@ __global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, int p0, G
         if (threadIdx.x == 0) atomicExch(ctl + 3, 1);
         break;
       }
-      __syncthreads();  // every write of the item is issued
-      if (threadIdx.x == 0) {
-        __threadfence();
-        st_release(fwd ? f.done_f + s : f.done_b + s, epoch);
-      }
+      // every write of the item precedes the stamp: the CTA barrier orders the
+      // other threads' writes before thread 0's release store, whose release
+      // semantics (cumulative, gpu scope) make them visible to the acquirer
+      __syncthreads();
+      if (threadIdx.x == 0) st_release(fwd ? f.done_f + s : f.done_b + s, epoch);
     }
     __syncthreads();  // s_ticket / s_go are rewritten next round
   }
