@@ -117,9 +117,14 @@ struct dfem_scene {
   // The solve runs levels 0 .. solve_cut-1 as level kernels and the rest in
   // one persistent launch: solve_cut = number of levels is the level-kernel
   // form, 0 the persistent form, anything between the split form.
+  // solve_cut = -1: the cluster form (one thread-block cluster walks the levels)
   int solve_cut = 0;
   int split_cut = 0;                     // the autotune's best split (0: none)
-  double solve_ms[3] = {0.0, 0.0, 0.0};  // autotune timings (ms per solve): levels, persistent, best split
+  double solve_ms[4] = {0.0, 0.0, 0.0, 0.0};  // autotune timings (ms per solve): levels, persistent, best split, cluster
+  DBuf<int> lvl_ptr_d, lvl_warp_d;       // cluster form: level starts, end of each level's warp-sized supernodes
+  size_t shm_cluster = 0;
+  int shm_cluster_warp = 0;              // doubles of shared memory per warp item
+  bool cluster_ok = false;
   double select_ms[2] = {0.0, 0.0};      // batches, only the largest part active: tuned form, persistent form
   // numeric refactorisation on the GPU (material changes)
   DBuf<double> hs_base, hc_coef, Ldw, part_reg, E_in, nu_in;
@@ -352,6 +357,24 @@ static int upload_factor(dfem_scene* sc) {
     }
   }
   CK(sc->lvl_sn.upload(F.lvl_sn));
+  {  // cluster form: each level's warp-sized supernodes are a prefix of the level (sorted by need)
+    std::vector<int> lw(L);
+    size_t wneed = 0, cneed = 0;
+    for (int l = 0; l < L; ++l) {
+      int k = F.lvl_ptr[l];
+      while (k < F.lvl_ptr[l + 1] && cls[F.lvl_sn[k]] == 0) wneed = std::max(wneed, need[F.lvl_sn[k++]]);
+      lw[l] = k;
+      for (; k < F.lvl_ptr[l + 1]; ++k) cneed = std::max(cneed, need[F.lvl_sn[k]]);
+    }
+    CK(sc->lvl_ptr_d.upload(F.lvl_ptr));
+    CK(sc->lvl_warp_d.upload(lw));
+    sc->shm_cluster_warp = (int)((wneed + 1) & ~size_t(1));
+    sc->shm_cluster = std::max<size_t>(16 * 8 * (size_t)sc->shm_cluster_warp, 8 * cneed);
+    sc->cluster_ok = sc->shm_cluster <= budget &&
+                     cudaFuncSetAttribute(k_solve_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)std::max<size_t>(1, sc->shm_cluster)) == cudaSuccess;
+    cudaGetLastError();
+  }
   std::vector<int> snp(ns, 0);
   if (sc->hs.nparts > 1)
     for (int q = 0; q < ns; ++q)
@@ -727,7 +750,28 @@ static void launch_segment(dfem_scene* sc, cudaStream_t st, const dfem_scene::Le
 
 static int n_levels(const dfem_scene* sc) { return (int)sc->lvl_ptr.size() - 1; }
 
+static void launch_cluster_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(kClusterCtas);
+  cfg.blockDim = dim3(512);
+  cfg.dynamicSmemBytes = sc->shm_cluster;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kClusterCtas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_solve_cluster, sc->fd, (int)sc->lvl_ptr.size() - 1, (const int*)sc->lvl_ptr_d.p,
+                     (const int*)sc->lvl_warp_d.p, sc->shm_cluster_warp, gate, rhs, y);
+}
+
 static void enqueue_solve_cut(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y, int c) {
+  if (c < 0) {
+    launch_cluster_solve(sc, st, gate, rhs, y);
+    return;
+  }
   for (const auto& g : sc->segs)
     if (g.level < c) launch_segment(sc, st, g, true, g.thr_f, gate, rhs, y);
   if (c < n_levels(sc)) {
@@ -744,6 +788,7 @@ static void enqueue_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const doub
 }
 
 static int solve_launches_cut(const dfem_scene* sc, int c) {
+  if (c < 0) return 1;
   int n = c < n_levels(sc) ? 1 : 0;
   for (const auto& g : sc->segs) n += g.level < c ? 2 : 0;
   return n;
@@ -794,9 +839,9 @@ static cudaError_t capture_solve(dfem_scene* sc, cudaStream_t st, Gate gate, con
   return e;
 }
 
-// 1: level kernels, 2: persistent, 3: split
+// 1: level kernels, 2: persistent, 3: split, 4: cluster
 static int solve_form(const dfem_scene* sc) {
-  return sc->solve_cut >= n_levels(sc) ? 1 : sc->solve_cut == 0 ? 2 : 3;
+  return sc->solve_cut < 0 ? 4 : sc->solve_cut >= n_levels(sc) ? 1 : sc->solve_cut == 0 ? 2 : 3;
 }
 
 // Fresh completion stamps and control words of the persistent solve (each API
@@ -1200,6 +1245,9 @@ static int tune_solve_select(dfem_scene* sc) {
   return DFEM_OK;
 }
 
+// Factors up to this many supernodes also try the cluster form.
+constexpr int kClusterMaxSupernodes = 4096;
+
 // Time the solve forms on this scene's factor (10 solves each after 3 warm-up
 // solves): the CTA size of every level-kernel launch, then the level-kernel
 // form, the persistent form and the split form at every cut level; keep the
@@ -1241,7 +1289,8 @@ static int autotune_solve(dfem_scene* sc) {
     cudaEventRecord(e0, sc->stream);
     for (int r = 0; r < reps; ++r) enqueue_solve(sc, sc->stream, kOpen, sc->rhs.p, sc->y.p);
     cudaEventRecord(e1, sc->stream);
-    cudaError_t e = cudaEventSynchronize(e1);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
     float t = 0;
     if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
     if (e != cudaSuccess) return fail(DFEM_ERR_CUDA, std::string("solve autotune: ") + cudaGetErrorString(e));
@@ -1262,6 +1311,17 @@ static int autotune_solve(dfem_scene* sc) {
       sc->solve_ms[2] = ms;
     }
   }
+  // the cluster form: factors of few supernodes (one cluster walks them all)
+  sc->solve_ms[3] = 0.0;
+  if (rc == DFEM_OK && sc->cluster_ok && sc->hs.F.nsuper <= kClusterMaxSupernodes) {
+    rc = time_cut(-1, &sc->solve_ms[3]);
+    if (rc != DFEM_OK) {  // a launch the device refuses (cluster shape): not a candidate
+      cudaGetLastError();
+      sc->cluster_ok = false;
+      sc->solve_ms[3] = 0.0;
+      rc = DFEM_OK;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   RC(rc);
@@ -1270,6 +1330,10 @@ static int autotune_solve(dfem_scene* sc) {
   RC(status_error(st4));
   sc->solve_cut = sc->solve_ms[1] < sc->solve_ms[0] ? 0 : L;
   if (sc->split_cut > 0 && sc->solve_ms[2] < std::min(sc->solve_ms[0], sc->solve_ms[1])) sc->solve_cut = sc->split_cut;
+  {
+    const double best = sc->solve_cut == 0 ? sc->solve_ms[1] : sc->solve_cut == L ? sc->solve_ms[0] : sc->solve_ms[2];
+    if (sc->solve_ms[3] > 0.0 && sc->solve_ms[3] < best) sc->solve_cut = -1;
+  }
   RC(tune_solve_select(sc));
   invalidate_graphs(sc);
   return DFEM_OK;
@@ -1671,7 +1735,7 @@ int dfem_profile_levels(dfem_scene* sc, int32_t reps, int32_t cap, int32_t* n_se
 
 int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms) {
   if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
-  if (request < -1 || request > 3) return fail(DFEM_ERR_INVALID, "request must be -1, 0, 1, 2 or 3");
+  if (request < -1 || request > 4) return fail(DFEM_ERR_INVALID, "request must be -1, 0, 1, 2, 3 or 4");
   CK(cudaSetDevice(sc->device));
   if (request == 0) {
     CK(cudaStreamSynchronize(sc->stream));
@@ -1680,7 +1744,8 @@ int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms
     sc->rec_steps = 0;  // the tuning solves overwrote the recorded iterates
   } else if (request > 0) {
     if (request == 3 && sc->split_cut == 0) return fail(DFEM_ERR_INVALID, "no split form (fewer than two levels)");
-    const int c = request == 1 ? n_levels(sc) : request == 2 ? 0 : sc->split_cut;
+    if (request == 4 && !sc->cluster_ok) return fail(DFEM_ERR_INVALID, "no cluster form for this factor");
+    const int c = request == 1 ? n_levels(sc) : request == 2 ? 0 : request == 3 ? sc->split_cut : -1;
     if (c != sc->solve_cut || sc->solve_select) {  // a requested form is used in every iteration
       sc->solve_cut = c;
       sc->solve_select = false;
@@ -1697,6 +1762,12 @@ int dfem_solve_select(const dfem_scene* sc, int32_t* on, double* weight_threshol
   if (on) *on = sc->solve_select ? 1 : 0;
   if (weight_threshold) *weight_threshold = sc->solve_select ? sc->select_w : 0.0;
   if (ms_one_part) { ms_one_part[0] = sc->select_ms[0]; ms_one_part[1] = sc->select_ms[1]; }
+  return DFEM_OK;
+}
+
+int dfem_solve_times(const dfem_scene* sc, double* ms) {
+  if (!sc || !ms) return fail(DFEM_ERR_INVALID, "null argument");
+  for (int k = 0; k < 4; ++k) ms[k] = sc->solve_ms[k];
   return DFEM_OK;
 }
 

@@ -890,6 +890,70 @@ __global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, int p0, G
   }
 }
 
+// Whole solve in one thread-block cluster (kClusterCtas CTAs of 512 threads),
+// for factors of few supernodes: the levels in order (leaves first, then
+// back), each level's small supernodes (level-order positions lvl_ptr[l] ..
+// lvl_warp[l]) one per warp of the cluster, then its other supernodes one per
+// CTA; a cluster barrier (release / acquire) between levels orders the
+// contributions and solution values the next level reads.  The per-level
+// handoff is one hardware barrier instead of a completion stamp per
+// supernode.  Every CTA takes every barrier: a supernode whose bounded copy
+// wait gave up records the error status and the CTA carries on.
+constexpr int kClusterCtas = 8;
+
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+__global__ void __launch_bounds__(512) k_solve_cluster(FactorDev f, int nlev, const int* __restrict__ lvl_ptr,
+                                                       const int* __restrict__ lvl_warp, int shm_warp, Gate gate,
+                                                       const double* __restrict__ rhs, double* y) {
+  extern __shared__ __align__(16) double sh[];
+  __shared__ __align__(8) uint64_t wbar[16][3];  // per warp: blocks, stream buffers
+  __shared__ __align__(8) uint64_t cbar[3];      // CTA items
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  const int rank = (int)cluster_rank();
+  if (lane == 0)
+    for (int b = 0; b < 3; ++b) mbar_init(&wbar[warp][b], 1);
+  if (threadIdx.x == 0)
+    for (int b = 0; b < 3; ++b) mbar_init(&cbar[b], 1);
+  __syncthreads();
+  unsigned wph = 0, wsph[2] = {0u, 0u};  // this warp's barrier phases
+  unsigned cph = 0, csph[2] = {0u, 0u};  // the CTA barriers' phases (uniform over the CTA)
+  double* wsh = sh + (size_t)warp * shm_warp;
+  for (int pass = 0; pass < 2; ++pass) {
+    const bool fwd = pass == 0;
+    for (int k = 0; k < nlev; ++k) {
+      const int l = fwd ? k : nlev - 1 - k;
+      const int p0 = lvl_ptr[l], pw = lvl_warp[l], p1 = lvl_ptr[l + 1];
+      for (int item = p0 + rank * nwarp + warp; item < pw; item += kClusterCtas * nwarp) {
+        const SnInfo in = f.info[item];
+        if (gate.skip(in.part)) continue;
+        __syncwarp();  // the warp's reads of its region precede the next bulk writes into it
+        if (fwd) fwd_supernode<WarpGroup>(f, in, rhs, y, wsh, &wbar[warp][0], wph, &wbar[warp][1], wsph, false);
+        else bwd_supernode<WarpGroup>(f, in, y, wsh, &wbar[warp][0], wph, &wbar[warp][1], wsph, false);
+        wph ^= 1u;
+      }
+      __syncthreads();  // the warps' regions overlap the CTA items' region
+      for (int item = pw + rank; item < p1; item += kClusterCtas) {
+        const SnInfo in = f.info[item];
+        if (gate.skip(in.part)) continue;
+        if (fwd) fwd_supernode<CtaGroup>(f, in, rhs, y, sh, &cbar[0], cph, &cbar[1], csph, false);
+        else bwd_supernode<CtaGroup>(f, in, y, sh, &cbar[0], cph, &cbar[1], csph, false);
+        cph ^= 1u;
+        __syncthreads();  // the CTA's reads of the region precede the next item's bulk writes
+      }
+      cluster_sync_all();
+    }
+  }
+}
+
 // Reset of the persistent solve's completion stamps and control words.
 __global__ void k_solve_reset(int ns, int* done_f, int* done_b, int* ctl) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += gridDim.x * blockDim.x) {

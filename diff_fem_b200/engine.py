@@ -192,10 +192,11 @@ class Scene:
 
     def solve_mode(self, request: Optional[str] = None) -> dict:
         """Form of the global solve: request None (query), "auto" (re-tune),
-        "levels", "persistent" or "split" (level kernels below the autotuned
-        cut level, one persistent launch above).  Returns the form in use and
+        "levels", "persistent", "split" (level kernels below the autotuned
+        cut level, one persistent launch above) or "cluster" (one thread-block
+        cluster walks the levels).  Returns the form in use and
         the autotune's ms per solve of each form."""
-        req = {None: -1, "auto": 0, "levels": 1, "persistent": 2, "split": 3}[request]
+        req = {None: -1, "auto": 0, "levels": 1, "persistent": 2, "split": 3, "cluster": 4}[request]
         chosen = C.c_int32()
         ms = (C.c_double * 2)()
         check(lib().dfem_solve_mode(self._h, req, C.byref(chosen), ms))
@@ -203,7 +204,10 @@ class Scene:
         check(lib().dfem_solve_split(self._h, C.byref(cut), C.byref(nl), C.byref(mss)))
         on, thr, one = C.c_int32(), C.c_double(), (C.c_double * 2)()
         check(lib().dfem_solve_select(self._h, C.byref(on), C.byref(thr), one))
-        return {"mode": {1: "levels", 2: "persistent", 3: "split"}[chosen.value], "ms_levels": ms[0],
+        t4 = (C.c_double * 4)()
+        check(lib().dfem_solve_times(self._h, t4))
+        return {"mode": {1: "levels", 2: "persistent", 3: "split", 4: "cluster"}[chosen.value], "ms_levels": ms[0],
+                "ms_cluster": t4[3],
                 "ms_persistent": ms[1], "ms_split": mss.value, "split_level": cut.value, "levels": nl.value,
                 "tail_persistent_below": thr.value if on.value else None,
                 "ms_largest_part_only": [one[0], one[1]]}

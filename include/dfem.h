@@ -242,14 +242,20 @@ int dfem_host_factor_solve(const dfem_scene_desc *desc, const double *b, double 
  * 1 level kernels (one launch per elimination-tree level, launch class and
  * direction), 2 persistent (both triangular sweeps in one launch, supernodes
  * claimed in dependency order), 3 split (the levels below the autotuned cut
- * level as level kernels, the rest in one persistent launch); a form
- * requested with 1-3 is used in every iteration (no per-iteration selection,
- * see dfem_solve_select).  *chosen (may
- * be NULL) receives the form in use (1, 2 or 3), ms (may be NULL, 2 values)
+ * level as level kernels, the rest in one persistent launch), 4 cluster
+ * (one thread-block cluster walks the levels, a cluster barrier between
+ * levels; tried for factors of up to 4096 supernodes); a form requested with
+ * 1-4 is used in every iteration (no per-iteration selection, see
+ * dfem_solve_select).  *chosen (may
+ * be NULL) receives the form in use (1-4), ms (may be NULL, 2 values)
  * the last autotune's time per solve of forms 1 and 2.  Every form runs the
  * same arithmetic per supernode: results are identical.  No counterpart in
  * the reference (its solve is Eigen's SimplicialLDLT, sim/fem/World.h:1660). */
 int dfem_solve_mode(dfem_scene *scene, int32_t request, int32_t *chosen, double *ms);
+
+/* The last autotune's time per solve (ms) of the level-kernel, persistent,
+ * best split and cluster forms (0: not timed). */
+int dfem_solve_times(const dfem_scene *scene, double *ms);
 
 /* The split form found by the last autotune: *cut_level (0: none), the
  * factor's number of levels, and its time per solve (ms). */

@@ -1,6 +1,7 @@
 """The forms of the global solve (one launch per elimination-tree level, one
-persistent launch whose CTAs claim supernodes in dependency order, or level
-kernels below a cut level and the persistent launch above it) run the same
+persistent launch whose CTAs claim supernodes in dependency order, level
+kernels below a cut level and the persistent launch above it, or one
+thread-block cluster walking the levels) run the same
 arithmetic per supernode, so a step, its gradient and a batch agree bit for
 bit whichever form the autotuner picked."""
 import dataclasses
@@ -29,11 +30,12 @@ def test_persistent_solve_matches_level_kernels(builder):
          "muscle_beam": S.muscle_beam, "cloth_sheet": lambda: S.cloth_sheet(nv=12)}[builder]()
     sc = Scene(d)
     info = sc.solve_mode()
-    assert info["mode"] in ("levels", "persistent", "split") and info["ms_levels"] > 0 and info["ms_persistent"] > 0
+    assert info["mode"] in ("levels", "persistent", "split", "cluster") and info["ms_levels"] > 0 and info["ms_persistent"] > 0
     assert info["split_level"] > 0 and info["ms_split"] > 0  # these factors have more than one level
+    assert info["ms_cluster"] > 0  # few supernodes: the cluster form is a candidate
     act = np.random.default_rng(1).uniform(0, 1, (4, d.n_segments)) if d.n_segments else None
     a = run(sc, d, 4, "levels", act)
-    for form in ("persistent", "split"):
+    for form in ("persistent", "split", "cluster"):
         b = run(sc, d, 4, form, act)
         for u, w in zip(a[:2], b[:2]):
             assert np.array_equal(u, w), form
@@ -49,7 +51,7 @@ def test_persistent_solve_in_a_batch_with_converged_parts():
     sc = Scene.batch(descs)
     act = np.random.default_rng(2).uniform(0, 1, (3, sc.nseg))
     a = run(sc, descs, 3, "levels", act)
-    for form in ("persistent", "split"):
+    for form in ("persistent", "split", "cluster"):
         b = run(sc, descs, 3, form, act)
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), form
         for k in a[2]:
