@@ -20,10 +20,27 @@ namespace dfem {
 enum { CS_MODE = 0, CS_PASS = 1, CS_IT = 2, CS_ANY = 3, CS_ACTIVE = 4, CS_BODIES = 5, CS_COMP = 6, CS_SRC = 7,
        CS_SIZE = 8 };
 
-// per-step record of the phase: [passes, loop-body executions]
-__global__ void k_contact_record(const int* step, const int* state, int* rec) {
-  rec[2 * (*step)] = state[CS_PASS];
-  rec[2 * (*step) + 1] = state[CS_BODIES];
+// per-step record of the phase: [passes, loop-body executions]; while the
+// forward steps record their contact iterations, the step's place in the
+// record (the next step's records follow it when it fit)
+__global__ void k_contact_record(const int* step, const int* state, int* rec, ContactDev c) {
+  const int s = *step;
+  rec[2 * s] = state[CS_PASS];
+  rec[2 * s + 1] = state[CS_BODIES];
+  if (c.rec_on && *c.rec_on == 2) {
+    const int base = *c.rec_base, comp = state[CS_COMP];
+    const int ok = base + comp <= c.rec_cap ? 1 : 0;
+    int* m = c.rec_meta + 4 * (size_t)s;
+    m[0] = base; m[1] = comp; m[2] = state[CS_SRC]; m[3] = ok;
+    if (ok) *c.rec_base = base + comp;
+  }
+}
+
+// record index of the current computed iteration (-1: not recording or no room)
+__device__ __forceinline__ int rec_index(const ContactDev& c) {
+  if (!c.rec_on || *c.rec_on == 0) return -1;
+  const int k = *c.rec_base + c.state[CS_COMP];
+  return k < c.rec_cap ? k : -1;
 }
 
 // ---- vertex-face CCD (one vertex moving p0 -> p1, static face q0 q1 q2) ----
@@ -139,15 +156,30 @@ __device__ __forceinline__ void contact_basis(Vec3<double> nrm, Vec3<double> B[3
 // ---- phase kernels ---------------------------------------------------------------
 
 // Before the loop: x_n1 = PD result, xold = 0, L x_t, empty impact lists.
+// L x_t at vertex i (Hs x_t - M/h^2 x_t), the contact rhs's elastic term.
+__device__ __forceinline__ Vec3<double> contact_lxt(const SceneDev& d, int i, const double* xt) {
+  Vec3<double> acc = mk3(0.0, 0.0, 0.0);
+  for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) acc = acc + d.hs_val[k] * ld3(xt, d.hs_col[k]);
+  return acc - (d.mass[i] / (d.h * d.h)) * ld3(xt, i);
+}
+
+// The step inputs the contact adjoint reads (v_wc and L x_t of the step with
+// start state xt, vt), for a step whose contact iterations the forward
+// recorded (no replay computes them); the same arithmetic as the forward.
+__global__ void k_contact_step_inputs(SceneDev d, ContactDev c, const double* xt, const double* vt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  st3(c.vwc, i, step_vwc(d, i, ld3(vt, i)));
+  st3(c.lxt, i, contact_lxt(d, i, xt));
+}
+
 __global__ void k_contact_begin(SceneDev d, ContactDev c, const double* xt, const double* xk,
                                 cudaGraphConditionalHandle h) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < d.N) {
     st3(c.xn1, i, ld3(xk, i));
     st3(c.xold, i, mk3(0.0, 0.0, 0.0));
-    Vec3<double> acc = mk3(0.0, 0.0, 0.0);
-    for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) acc = acc + d.hs_val[k] * ld3(xt, d.hs_col[k]);
-    st3(c.lxt, i, acc - (d.mass[i] / (d.h * d.h)) * ld3(xt, i));
+    st3(c.lxt, i, contact_lxt(d, i, xt));
   }
   if (i < c.nc) c.imp_cnt[i] = 0;
   if (i == 0) {
@@ -208,12 +240,13 @@ __global__ void k_contact_prep(int N, ContactDev c, double* xk, double* partial,
     e = fmax(fabs(dl.x), fmax(fabs(dl.y), fabs(dl.z)));
   }
   // recording for the adjoint: the impact lists this iteration will use
-  const int comp = c.state[CS_COMP];
-  if (c.rec_on && *c.rec_on && i < c.nc && comp < c.rec_cap) {
+  const int rk = rec_index(c);
+  if (rk >= 0 && i < c.nc) {
     const int cnt = c.imp_cnt[i];
-    c.rec_cnt[(size_t)comp * c.nc + i] = cnt;
-    for (int q = 0; q < cnt; ++q)
-      st3(c.rec_n, ((size_t)comp * c.nc + i) * kMaxImpactsPerVertex + q, ld3(c.imp_n, i * kMaxImpactsPerVertex + q));
+    c.rec_cnt[(size_t)rk * c.nc + i] = cnt;
+    // 64-bit offset to the vertex's normals (the record spans billions of doubles)
+    double* rn = c.rec_n + ((size_t)rk * c.nc + i) * kMaxImpactsPerVertex * 3;
+    for (int q = 0; q < cnt; ++q) st3(rn, q, ld3(c.imp_n, i * kMaxImpactsPerVertex + q));
   }
   // deterministic grid max
   __shared__ double ws[32];
@@ -281,11 +314,11 @@ __global__ void k_contact_rhs(SceneDev d, ContactDev c, const double* __restrict
   st3(c.prev, i, prev);
   st3(c.xn1, i, ld3(xt, i) + (1.0 / (d.h * c.hdiag[i])) * prev);
   st3(c.xold, i, ld3(xk, i));
-  const int comp = c.state[CS_COMP];
-  if (c.rec_on && *c.rec_on && comp < c.rec_cap) {
-    st3(c.rec_x + (size_t)comp * 3 * d.N, i, ld3(xk, i));
-    st3(c.rec_prev + (size_t)comp * 3 * d.N, i, prev);
-    if (i == 0) c.rec_first[comp] = first ? 1 : 0;
+  const int rk = rec_index(c);
+  if (rk >= 0) {
+    st3(c.rec_x + (size_t)rk * 3 * d.N, i, ld3(xk, i));
+    st3(c.rec_prev + (size_t)rk * 3 * d.N, i, prev);
+    if (i == 0) c.rec_first[rk] = first ? 1 : 0;
   }
 }
 
@@ -297,7 +330,8 @@ __global__ void k_contact_ctl_iter(ContactDev c, int K) {
   int it = c.state[CS_IT] + 1;
   c.state[CS_IT] = it;
   c.state[CS_ACTIVE] = 0;
-  if (c.rec_on && *c.rec_on && c.state[CS_COMP] >= c.rec_cap) atomicExch(c.status, 6);  // record too small
+  if (c.rec_on && *c.rec_on == 1 && *c.rec_base + c.state[CS_COMP] >= c.rec_cap)
+    atomicExch(c.status, 6);  // the replayed step's record is too small
   c.state[CS_COMP] += 1;
   if (it >= K) c.state[CS_MODE] = 0;
 }

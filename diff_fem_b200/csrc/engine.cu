@@ -72,6 +72,7 @@ struct DBuf {
     if (h.empty()) return cudaSuccess;
     return cudaMemcpy(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
   }
+  void swap(DBuf& o) { std::swap(p, o.p); std::swap(n, o.n); }
 };
 
 }  // namespace dfem
@@ -161,6 +162,13 @@ struct dfem_scene {
   DBuf<int> crec_on, crec_first, crec_cnt;
   DBuf<double> crec_x, crec_prev, crec_n, ca_xn1b, ca_pb, ca_hdb, ca_cxtb, ca_vwcb, ca_yb, ca_orib;
   int crec_cap = 0;
+  // forward recording of every step's contact iterations (when the steps'
+  // iterates are stored too, the adjoint then replays no contact step)
+  DBuf<int> crec_base, crec_meta;
+  std::vector<int> crec_meta_h;          // per step of the last forward: [first record, iterations, source, recorded]
+  bool crec_fwd = false;                 // the last forward recorded
+  int crec_used = 0;                     // records the last forward's steps occupy
+  int crec_target = 0;                   // records the next forward asks for
   ContactDev cd{};
   std::vector<int> rec_passes;
   // graphs
@@ -701,10 +709,12 @@ static int upload_scene(dfem_scene* sc) {
     CK(cudaMemset(sc->cstate.p, 0, sizeof(int) * CS_SIZE));
     CK(sc->crec_on.alloc(1));
     CK(cudaMemset(sc->crec_on.p, 0, sizeof(int)));
+    CK(sc->crec_base.alloc(1));
+    CK(cudaMemset(sc->crec_base.p, 0, sizeof(int)));
     sc->cd = ContactDev{nc, nof, s.K, kMaxContactPasses, s.alpha, s.mu_obs, sc->cverts.p, sc->cidx.p, sc->obs_x.p,
                         sc->obs_f.p, sc->hdiag.p, sc->imp_cnt.p, sc->imp_face.p, sc->imp_n.p, sc->xn1.p, sc->xold.p,
                         sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p, sc->crec_on.p, 0, nullptr, nullptr,
-                        nullptr, nullptr, nullptr, sc->status.p};
+                        nullptr, nullptr, nullptr, sc->status.p, sc->crec_base.p, nullptr};
   }
   refresh_scene_view(sc);
   return DFEM_OK;
@@ -727,6 +737,10 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   CK(sc->hist.alloc(all ? rec * cap : rec));
   sc->hist_step = all ? (long long)rec : 0;
   CK(cudaMemset(sc->cpasses.p, 0, sizeof(int) * 2 * (size_t)cap));
+  if (sc->has_contact) {
+    CK(sc->crec_meta.alloc(4 * (size_t)cap));
+    sc->cd.rec_meta = sc->crec_meta.p;
+  }
   sc->cap_steps = cap;
   invalidate_graphs(sc);  // graphs hold the old pointers
   return DFEM_OK;
@@ -960,7 +974,7 @@ static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandl
 
 static void step_post(dfem_scene* sc, cudaStream_t st) {
   const int nb = sc->nblk_v;
-  if (sc->has_contact) k_contact_record<<<1, 1, 0, st>>>(sc->step.p, sc->cstate.p, sc->cpasses.p);
+  if (sc->has_contact) k_contact_record<<<1, 1, 0, st>>>(sc->step.p, sc->cstate.p, sc->cpasses.p, sc->cd);
   k_step_end<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->xk.p, sc->traj.p, sc->to_user.p,
                                  sc->write_traj.p);
   k_next_step<<<1, 1, 0, st>>>(sc->step.p);
@@ -1099,17 +1113,33 @@ static int copy_out(dfem_scene* sc, const double* src, size_t n, double* dst, in
 }
 
 // Record of the contact phase for its adjoint: room for `cap` computed Jacobi
-// iterations of one step (the graphs hold the record's pointers: rebuilt when
-// it grows).
-static int ensure_contact_record(dfem_scene* sc, int cap) {
+// iterations; records 0 .. keep-1 survive a growth (the graphs hold the
+// record's pointers: rebuilt when it grows).
+static int ensure_contact_record(dfem_scene* sc, int cap, int keep = 0) {
   if (!sc->has_contact || cap <= sc->crec_cap) return DFEM_OK;
   const HostScene& s = sc->hs;
-  const size_t n3 = 3 * (size_t)s.N, nc = (size_t)sc->cd.nc;
-  CK(sc->crec_x.alloc(n3 * cap));
-  CK(sc->crec_prev.alloc(n3 * cap));
-  CK(sc->crec_first.alloc(cap));
-  CK(sc->crec_cnt.alloc(nc * cap));
-  CK(sc->crec_n.alloc(nc * cap * kMaxImpactsPerVertex * 3));
+  const size_t n3 = 3 * (size_t)s.N, nc = (size_t)sc->cd.nc, nn = nc * kMaxImpactsPerVertex * 3;
+  keep = std::min(keep, sc->crec_cap);
+  DBuf<double> x, prev, nrm;
+  DBuf<int> first, cnt;
+  CK(x.alloc(n3 * cap));
+  CK(prev.alloc(n3 * cap));
+  CK(first.alloc(cap));
+  CK(cnt.alloc(nc * cap));
+  CK(nrm.alloc(nn * cap));
+  if (keep > 0) {
+    CK(cudaMemcpyAsync(x.p, sc->crec_x.p, sizeof(double) * n3 * keep, cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaMemcpyAsync(prev.p, sc->crec_prev.p, sizeof(double) * n3 * keep, cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaMemcpyAsync(first.p, sc->crec_first.p, sizeof(int) * keep, cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaMemcpyAsync(cnt.p, sc->crec_cnt.p, sizeof(int) * nc * keep, cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaMemcpyAsync(nrm.p, sc->crec_n.p, sizeof(double) * nn * keep, cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaStreamSynchronize(sc->stream));
+  }
+  sc->crec_x.swap(x);
+  sc->crec_prev.swap(prev);
+  sc->crec_first.swap(first);
+  sc->crec_cnt.swap(cnt);
+  sc->crec_n.swap(nrm);
   for (DBuf<double>* b : {&sc->ca_xn1b, &sc->ca_pb, &sc->ca_cxtb, &sc->ca_vwcb, &sc->ca_yb, &sc->ca_orib})
     if (!b->p) CK(b->alloc(n3));
   if (!sc->ca_hdb.p) CK(sc->ca_hdb.alloc(std::max(1, s.N)));
@@ -1124,30 +1154,48 @@ static int ensure_contact_record(dfem_scene* sc, int cap) {
   return DFEM_OK;
 }
 
-// Reverse of step st's contact phase, after the step graph re-ran it with
-// recording on.  In: io_a / io_b = cotangents of the step's x' and v'.  Out:
-// io_a = cotangent of the PD result (io_b = 0); the x_t and v_wc cotangents
-// wait in ca_cxtb / ca_vwcb for k_cadj_finish after the PD adjoint.
-static int contact_adjoint_step(dfem_scene* sc, int st) {
+// Device bytes of one record (one computed Jacobi iteration of the contact phase).
+static size_t contact_record_bytes(const dfem_scene* sc) {
+  const size_t n3 = 3 * (size_t)sc->hs.N, nc = (size_t)sc->cd.nc;
+  return sizeof(double) * 2 * n3 + sizeof(int) * (1 + nc) + sizeof(double) * nc * kMaxImpactsPerVertex * 3;
+}
+
+// Reverse of step st's contact phase, from its record: the forward's (base,
+// iterations, source from crec_meta_h) or, after the step graph re-ran the
+// step with recording on, the replay's (base = rbase, the rest from the
+// contact state).  In: io_a / io_b = cotangents of the step's x' and v'.
+// Out: io_a = cotangent of the PD result (io_b = 0); the x_t and v_wc
+// cotangents wait in ca_cxtb / ca_vwcb for k_cadj_finish after the PD adjoint.
+static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase) {
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N;
   const int nb = sc->nblk_v, ncons = s.T + s.M + s.S + s.B;
-  int meta[CS_SIZE];
-  CK(cudaMemcpyAsync(meta, sc->cstate.p, sizeof(meta), cudaMemcpyDeviceToHost, sc->stream));
-  CK(cudaStreamSynchronize(sc->stream));
-  const int src = meta[CS_SRC];
-  if (meta[CS_COMP] > sc->crec_cap) return fail(DFEM_ERR_CAP, "contact record too small for the recomputed step");
+  int base = rbase, comp = 0, src = 0;
+  if (recorded) {
+    base = sc->crec_meta_h[4 * (size_t)st];
+    comp = sc->crec_meta_h[4 * (size_t)st + 1];
+    src = sc->crec_meta_h[4 * (size_t)st + 2];
+  } else {
+    int meta[CS_SIZE];
+    CK(cudaMemcpyAsync(meta, sc->cstate.p, sizeof(meta), cudaMemcpyDeviceToHost, sc->stream));
+    CK(cudaStreamSynchronize(sc->stream));
+    comp = meta[CS_COMP];
+    src = meta[CS_SRC];
+  }
+  if (base + comp > sc->crec_cap) return fail(DFEM_ERR_CAP, "contact record too small for the recomputed step");
   std::vector<int> first(std::max(1, src));
-  if (src > 0) CK(cudaMemcpy(first.data(), sc->crec_first.p, src * sizeof(int), cudaMemcpyDeviceToHost));
+  if (src > 0)
+    CK(cudaMemcpy(first.data(), sc->crec_first.p + base, src * sizeof(int), cudaMemcpyDeviceToHost));
   const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
   const double* xt = sc->ckpt_x.p + (size_t)st * n3;
   k_cadj_start<<<nb, 128, 0, sc->stream>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, a);
   int launches = 1;
   for (int j = src; j >= 1; --j) {
-    const double* ori = sc->crec_x.p + (size_t)(j - 1) * n3;
-    const double* prev = sc->crec_prev.p + (size_t)(j - 1) * n3;
-    const int* rcnt = sc->crec_cnt.p + (size_t)(j - 1) * sc->cd.nc;
-    const double* rn = sc->crec_n.p + (size_t)(j - 1) * sc->cd.nc * kMaxImpactsPerVertex * 3;
+    const size_t r = (size_t)base + (j - 1);
+    const double* ori = sc->crec_x.p + r * n3;
+    const double* prev = sc->crec_prev.p + r * n3;
+    const int* rcnt = sc->crec_cnt.p + r * sc->cd.nc;
+    const double* rn = sc->crec_n.p + r * sc->cd.nc * kMaxImpactsPerVertex * 3;
     if (ncons > 0)
       k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, kOpen, ori, sc->act_all.p, sc->step.p, sc->slot.p);
     k_cadj_rhs<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->cd, a, sc->slot.p, xt, ori, prev, first[j - 1], rcnt, rn);
@@ -1509,7 +1557,25 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   k_set_int<<<1, 1, 0, sc->stream>>>(sc->write_traj.p, traj_x ? 1 : 0);
   CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
   reset_solve_state(sc);
-  if (sc->has_contact) CK(cudaMemsetAsync(sc->crec_on.p, 0, sizeof(int), sc->stream));  // no recording here
+  // With every step's iterates stored, the contact steps also record their
+  // contact iterations, in a row, within what the adjoint budget leaves: the
+  // adjoint then replays none of them (a step that does not fit is replayed).
+  bool fwd_rec = false;
+  size_t rec_budget = 0;
+  if (sc->has_contact) {
+    const size_t hist_bytes = sizeof(double) * sc->hist.n;
+    rec_budget = sc->hist_step != 0 && sc->adj_budget > hist_bytes
+                     ? (sc->adj_budget - hist_bytes) / contact_record_bytes(sc) : 0;
+    rec_budget = std::min<size_t>(rec_budget, INT32_MAX / 2);
+    const int want = (int)std::min<size_t>(rec_budget, sc->crec_target > 0 ? (size_t)sc->crec_target
+                                                                             : 4 * (size_t)n_steps);
+    fwd_rec = want >= 1;
+    if (fwd_rec) RC(ensure_contact_record(sc, want));
+    const int on = fwd_rec ? 2 : 0;
+    CK(cudaMemcpyAsync(sc->crec_on.p, &on, sizeof(int), cudaMemcpyHostToDevice, sc->stream));
+    CK(cudaMemsetAsync(sc->crec_base.p, 0, sizeof(int), sc->stream));
+    CK(cudaStreamSynchronize(sc->stream));  // `on` is a host local
+  }
   CK(cudaGetLastError());
   RC(ensure_graphs(sc));
   for (int st = 0; st < n_steps; ++st) CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
@@ -1526,6 +1592,13 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   sc->rec_passes.assign(2 * (size_t)n_steps, 0);
   if (sc->has_contact)
     CK(cudaMemcpyAsync(sc->rec_passes.data(), sc->cpasses.p, 2 * n_steps * sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+  int rec_used = 0;
+  sc->crec_meta_h.assign(4 * (size_t)n_steps, 0);
+  if (fwd_rec) {
+    CK(cudaMemcpyAsync(sc->crec_meta_h.data(), sc->crec_meta.p, sizeof(int) * 4 * n_steps, cudaMemcpyDeviceToHost,
+                       sc->stream));
+    CK(cudaMemcpyAsync(&rec_used, sc->crec_base.p, sizeof(int), cudaMemcpyDeviceToHost, sc->stream));
+  }
   unsigned long long sel[2] = {0, 0};
   if (sc->sel_count.p) CK(cudaMemcpyAsync(sel, sc->sel_count.p, sizeof(sel), cudaMemcpyDeviceToHost, sc->stream));
   CK(cudaStreamSynchronize(sc->stream));
@@ -1536,6 +1609,13 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
   sc->rec_iters.assign(n_steps, 0);
   for (int st = 0; st < n_steps; ++st)
     for (int p = 0; p < np; ++p) sc->rec_iters[st] = std::max(sc->rec_iters[st], it_all[(size_t)st * np + p]);
+  sc->crec_fwd = fwd_rec;
+  sc->crec_used = rec_used;
+  if (fwd_rec) {  // the next forward asks for room for all of this one's records
+    size_t need = 0;
+    for (int st = 0; st < n_steps; ++st) need += (size_t)sc->crec_meta_h[4 * (size_t)st + 1];
+    sc->crec_target = (int)std::min(rec_budget, std::max<size_t>(need + need / 8 + 16, (size_t)sc->crec_target));
+  }
   sc->launches += 7;
   for (int st = 0; st < n_steps; ++st)
     sc->launches += (int64_t)(sc->g_step.outside + (size_t)sc->rec_iters[st] * sc->g_step.body +
@@ -1550,14 +1630,20 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   if (!sc || !gx_out || !gv_out || !gx || !gv) return fail(DFEM_ERR_INVALID, "null argument");
   if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_step_backward needs a preceding dfem_step_forward");
   CK(cudaSetDevice(sc->device));
-  // the contact phase's record: room for the most loop-body executions of any recorded step
+  // contact steps the forward recorded need no replay; the others are replayed
+  // with recording on, into records after the forward's (room for the most
+  // loop-body executions of any of them)
   int ccap = 0;
   bool any_contact = false;
+  std::vector<char> recorded(std::max(1, sc->rec_steps), 0);
   for (int st = 0; st < sc->rec_steps && 2 * st + 1 < (int)sc->rec_passes.size(); ++st) {
-    any_contact = any_contact || sc->rec_passes[2 * st] > 0;
-    ccap = std::max(ccap, sc->rec_passes[2 * st + 1]);
+    const bool c = sc->rec_passes[2 * st] > 0;
+    any_contact = any_contact || c;
+    recorded[st] = c && sc->crec_fwd && 4 * st + 3 < (int)sc->crec_meta_h.size() && sc->crec_meta_h[4 * st + 3] == 1;
+    if (c && !recorded[st]) ccap = std::max(ccap, sc->rec_passes[2 * st + 1]);
   }
-  if (any_contact) RC(ensure_contact_record(sc, std::max(1, ccap)));
+  const int rbase = sc->crec_fwd ? sc->crec_used : 0;
+  if (any_contact) RC(ensure_contact_record(sc, rbase + std::max(1, ccap), rbase));
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N;
   const int nb = sc->nblk_v;
@@ -1573,11 +1659,14 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   CK(cudaMemsetAsync(sc->status.p, 0, 4 * sizeof(int), sc->stream));
   reset_solve_state(sc);
   RC(ensure_graphs(sc));
-  if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 1);
+  if (any_contact) {
+    k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 1);
+    k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_base.p, rbase);
+  }
   int recomputed = 0;
   for (int st = sc->rec_steps - 1; st >= 0; --st) {
     const bool contact_step = sc->has_contact && sc->rec_passes[2 * st] > 0;
-    if (sc->hist_step == 0 || contact_step) {
+    if (sc->hist_step == 0 || (contact_step && !recorded[st])) {
       // recompute the step's iterates from its checkpoint (the step graph re-records the same checkpoint);
       // a contact step also records its contact iterations for the contact adjoint
       CK(cudaMemcpyAsync(sc->xt.p, sc->ckpt_x.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
@@ -1587,7 +1676,14 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
       ++recomputed;
     }
     k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
-    if (contact_step) RC(contact_adjoint_step(sc, st));
+    if (contact_step && recorded[st]) {  // the step's v_wc and L x_t, which a replay would have left behind
+      const double* cx = sc->ckpt_x.p + (size_t)st * n3;
+      const double* cv = sc->ckpt_v.p + (size_t)st * n3;
+      if (sc->nF > 0) k_drag_faces<<<(sc->nF + 127) / 128, 128, 0, sc->stream>>>(sc->nF, sc->df.p, cx, cv, sc->fdrag.p);
+      k_contact_step_inputs<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->cd, cx, cv);
+      sc->launches += 1 + (sc->nF > 0 ? 1 : 0);
+    }
+    if (contact_step) RC(contact_adjoint_step(sc, st, recorded[st] != 0, rbase));
     CK(cudaGraphLaunch(sc->g_adj.exec, sc->stream));
     if (contact_step) {
       const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
@@ -1609,7 +1705,7 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
     sc->launches += (int64_t)(1 + sc->g_adj.outside + (size_t)sc->rec_iters[st] * sc->g_adj.body);
   if (recomputed > 0)  // replayed step graphs (iteration counts as recorded; contact bodies not counted)
     for (int st = 0; st < sc->rec_steps && st < (int)sc->rec_iters.size(); ++st)
-      if (sc->hist_step == 0 || (sc->has_contact && sc->rec_passes[2 * st] > 0))
+      if (sc->hist_step == 0 || (sc->has_contact && sc->rec_passes[2 * st] > 0 && !recorded[st]))
         sc->launches += (int64_t)(1 + sc->g_step.outside + (size_t)sc->rec_iters[st] * sc->g_step.body +
                                   (size_t)sc->rec_passes[2 * st + 1] * sc->g_step.body2);
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_a.p, sc->rhs.p);

@@ -144,7 +144,9 @@ struct ContactDev {
   double* lxt;            // 3N: L x_t
   double* vwc;            // 3N: v + g h of the step
   int* state;             // see CS_* in contact_kernels.cuh
-  // recording for the adjoint (written only while *rec_on != 0)
+  // recording for the adjoint (written only while *rec_on != 0): 1 = a step
+  // the adjoint replays (a record too small is an error), 2 = the forward
+  // steps in a row (a step that does not fit is marked unrecorded and replayed)
   const int* rec_on;
   int rec_cap;            // computed iterations the record holds
   double* rec_x;          // rec_cap x 3N: each computed iteration's input ori_x
@@ -153,6 +155,8 @@ struct ContactDev {
   int* rec_cnt;           // rec_cap x nc: impacts per contact vertex
   double* rec_n;          // rec_cap x nc x kMax x 3: their normals
   int* status;
+  int* rec_base;          // the current step's first record (computed iteration j of it is record base + j)
+  int* rec_meta;          // forward recording, per step: [first record, computed iterations, source, recorded]
 };
 
 // One supernode of the triangular solves, stored in level order (position

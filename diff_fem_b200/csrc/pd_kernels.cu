@@ -100,6 +100,20 @@ __device__ __forceinline__ Mat3<double> deformation(const double G[4][3], const 
 
 // hist_step: doubles between the iterate records of consecutive steps (0: one
 // record shared by all steps, the adjoint recomputes each step).
+// v_wc of vertex i: v + g h (gravity-enabled vertices) + h f_drag / m (underwater: the
+// drag and lift of the vertex's faces, ascending face order, from d.fdrag).
+__device__ __forceinline__ Vec3<double> step_vwc(const SceneDev& d, int i, Vec3<double> v) {
+  double gm = d.gmask[i] * d.h;
+  Vec3<double> vwc = mk3(v.x + gm * d.g0, v.y + gm * d.g1, v.z + gm * d.g2);
+  if (d.vf_ptr) {
+    Vec3<double> f = mk3(0.0, 0.0, 0.0);
+    for (int k = d.vf_ptr[i]; k < d.vf_ptr[i + 1]; ++k) f = f + ld3(d.fdrag, d.vf_face[k] / 3);
+    const double m = d.mass[i];
+    vwc = vwc + mk3(d.h * (f.x / m), d.h * (f.y / m), d.h * (f.z / m));
+  }
+  return vwc;
+}
+
 __global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt, double* vt, double* qn,
                              double* c0, double* xk, double* hist, long long hist_step, double* ckpt_x, double* ckpt_v,
                              int* flag, int* iters, double* partial, unsigned* counter, double* errv,
@@ -115,14 +129,7 @@ __global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt
     if (ckpt_x) { st3(ckpt_x + (size_t)s * 3 * d.N, i, x); st3(ckpt_v + (size_t)s * 3 * d.N, i, v); }
     // Environment::Step adds g h to v (gravity-enabled bodies); TimeStepping:
     // v_wc = v + h M^-1 f_ext (f_ext = 0), q_n = x + h v_wc
-    double gm = d.gmask[i] * d.h;
-    Vec3<double> vwc = mk3(v.x + gm * d.g0, v.y + gm * d.g1, v.z + gm * d.g2);
-    if (d.vf_ptr) {  // underwater: the drag and lift of the vertex's faces (ascending face order)
-      Vec3<double> f = mk3(0.0, 0.0, 0.0);
-      for (int k = d.vf_ptr[i]; k < d.vf_ptr[i + 1]; ++k) f = f + ld3(d.fdrag, d.vf_face[k] / 3);
-      const double m = d.mass[i];
-      vwc = vwc + mk3(d.h * (f.x / m), d.h * (f.y / m), d.h * (f.z / m));
-    }
+    const Vec3<double> vwc = step_vwc(d, i, v);
     if (vwc_out) st3(vwc_out, i, vwc);
     Vec3<double> q = x + d.h * vwc;
     st3(qn, i, q);
