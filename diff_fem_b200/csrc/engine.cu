@@ -146,6 +146,7 @@ struct dfem_scene {
   DBuf<int> flag, iters, step, status, write_traj, zero;
   DBuf<double> act_all, act_cur;   // per-step activations; current activations
   DBuf<double> ckpt_x, ckpt_v, traj;
+  DBuf<double> seg_x, seg_v;           // checkpoint_every > 1: the start states of one segment, regenerated by the adjoint
   int cap_steps = 0;
   // iterates of the last forward call: of every step when they fit the budget
   // (the adjoint then replays no step without contact), else of one step
@@ -725,8 +726,14 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   const HostScene& s = sc->hs;
   int cap = std::max(n_steps, 2 * sc->cap_steps);
   const size_t n3 = 3 * (size_t)s.N;
-  CK(sc->ckpt_x.alloc(n3 * cap));
-  CK(sc->ckpt_v.alloc(n3 * cap));
+  const int kc = std::max(1, s.checkpoint_every);
+  const size_t nck = ((size_t)cap + kc - 1) / kc;  // one checkpoint per kc steps
+  CK(sc->ckpt_x.alloc(n3 * nck));
+  CK(sc->ckpt_v.alloc(n3 * nck));
+  if (kc > 1 && !sc->seg_x.p) {
+    CK(sc->seg_x.alloc(n3 * kc));
+    CK(sc->seg_v.alloc(n3 * kc));
+  }
   CK(sc->traj.alloc(n3 * cap));
   CK(sc->iters.alloc((size_t)cap * sc->hs.nparts));
   CK(sc->act_all.alloc((size_t)cap * std::max(1, s.nseg)));
@@ -933,7 +940,8 @@ static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   if (sc->nF > 0) k_drag_faces<<<(sc->nF + 127) / 128, 128, 0, st>>>(sc->nF, sc->df.p, sc->xt.p, sc->vt.p, sc->fdrag.p);
   k_step_begin<<<sc->nblk_p, kPartBlock, 0, st>>>(sc->sd, sc->pd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
-                                   sc->hist.p, sc->hist_step, sc->ckpt_x.p, sc->ckpt_v.p, sc->flag.p, sc->iters.p,
+                                   sc->hist.p, sc->hist_step, std::max(1, sc->hs.checkpoint_every), sc->ckpt_x.p,
+                                   sc->ckpt_v.p, sc->flag.p, sc->iters.p,
                                    sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p,
                                    sc->has_contact ? sc->vwc.p : nullptr);
   k_loop_enter<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, sc->hs.nparts, sc->hs.K, h);
@@ -1166,7 +1174,7 @@ static size_t contact_record_bytes(const dfem_scene* sc) {
 // contact state).  In: io_a / io_b = cotangents of the step's x' and v'.
 // Out: io_a = cotangent of the PD result (io_b = 0); the x_t and v_wc
 // cotangents wait in ca_cxtb / ca_vwcb for k_cadj_finish after the PD adjoint.
-static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase) {
+static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase, const double* xt) {
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N;
   const int nb = sc->nblk_v, ncons = s.T + s.M + s.S + s.B;
@@ -1187,7 +1195,6 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
   if (src > 0)
     CK(cudaMemcpy(first.data(), sc->crec_first.p + base, src * sizeof(int), cudaMemcpyDeviceToHost));
   const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
-  const double* xt = sc->ckpt_x.p + (size_t)st * n3;
   k_cadj_start<<<nb, 128, 0, sc->stream>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, a);
   int launches = 1;
   for (int j = src; j >= 1; --j) {
@@ -1663,50 +1670,83 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
     k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 1);
     k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_base.p, rbase);
   }
+  // Checkpoints are kept every kc steps.  Working back one segment [s0, end)
+  // at a time, the adjoint first regenerates the segment's start states from
+  // its checkpoint (steps s0 .. end-2 forward again, no contact recording)
+  // when anything below reads them: the replays (iterates not stored, or a
+  // contact step not recorded), the contact adjoint and the drag adjoint.
+  const int kc = std::max(1, s.checkpoint_every);
+  const bool need_states = sc->hist_step == 0 || any_contact || sc->nF > 0;
+  int seg0 = 0;
+  auto sx = [&](int st) { return kc == 1 ? sc->ckpt_x.p + (size_t)st * n3 : sc->seg_x.p + (size_t)(st - seg0) * n3; };
+  auto sv = [&](int st) { return kc == 1 ? sc->ckpt_v.p + (size_t)st * n3 : sc->seg_v.p + (size_t)(st - seg0) * n3; };
+  std::vector<int> rerun(std::max(1, sc->rec_steps), 0);  // step graphs run again, per step (launch statistics)
   int recomputed = 0;
-  for (int st = sc->rec_steps - 1; st >= 0; --st) {
-    const bool contact_step = sc->has_contact && sc->rec_passes[2 * st] > 0;
-    if (sc->hist_step == 0 || (contact_step && !recorded[st])) {
-      // recompute the step's iterates from its checkpoint (the step graph re-records the same checkpoint);
-      // a contact step also records its contact iterations for the contact adjoint
-      CK(cudaMemcpyAsync(sc->xt.p, sc->ckpt_x.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
-      CK(cudaMemcpyAsync(sc->vt.p, sc->ckpt_v.p + (size_t)st * n3, n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+  for (int seg_end = sc->rec_steps; seg_end > 0; seg_end = seg0) {
+    seg0 = ((seg_end - 1) / kc) * kc;
+    if (kc > 1 && need_states) {
+      CK(cudaMemcpyAsync(sc->xt.p, sc->ckpt_x.p + (size_t)(seg0 / kc) * n3, n3 * sizeof(double),
+                         cudaMemcpyDeviceToDevice, sc->stream));
+      CK(cudaMemcpyAsync(sc->vt.p, sc->ckpt_v.p + (size_t)(seg0 / kc) * n3, n3 * sizeof(double),
+                         cudaMemcpyDeviceToDevice, sc->stream));
+      if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 0);
+      for (int q = seg0; q < seg_end; ++q) {
+        CK(cudaMemcpyAsync(sc->seg_x.p + (size_t)(q - seg0) * n3, sc->xt.p, n3 * sizeof(double),
+                           cudaMemcpyDeviceToDevice, sc->stream));
+        CK(cudaMemcpyAsync(sc->seg_v.p + (size_t)(q - seg0) * n3, sc->vt.p, n3 * sizeof(double),
+                           cudaMemcpyDeviceToDevice, sc->stream));
+        if (q + 1 < seg_end) {
+          k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, q);
+          CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
+          rerun[q] += 1;
+          ++recomputed;
+        }
+      }
+      if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 1);
+    }
+    for (int st = seg_end - 1; st >= seg0; --st) {
+      const bool contact_step = sc->has_contact && sc->rec_passes[2 * st] > 0;
+      if (sc->hist_step == 0 || (contact_step && !recorded[st])) {
+        // recompute the step's iterates from its start state (the step graph re-records the same values);
+        // a contact step also records its contact iterations for the contact adjoint
+        CK(cudaMemcpyAsync(sc->xt.p, sx(st), n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+        CK(cudaMemcpyAsync(sc->vt.p, sv(st), n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+        k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
+        CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
+        rerun[st] += 1;
+        ++recomputed;
+      }
       k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
-      CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
-      ++recomputed;
-    }
-    k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
-    if (contact_step && recorded[st]) {  // the step's v_wc and L x_t, which a replay would have left behind
-      const double* cx = sc->ckpt_x.p + (size_t)st * n3;
-      const double* cv = sc->ckpt_v.p + (size_t)st * n3;
-      if (sc->nF > 0) k_drag_faces<<<(sc->nF + 127) / 128, 128, 0, sc->stream>>>(sc->nF, sc->df.p, cx, cv, sc->fdrag.p);
-      k_contact_step_inputs<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->cd, cx, cv);
-      sc->launches += 1 + (sc->nF > 0 ? 1 : 0);
-    }
-    if (contact_step) RC(contact_adjoint_step(sc, st, recorded[st] != 0, rbase));
-    CK(cudaGraphLaunch(sc->g_adj.exec, sc->stream));
-    if (contact_step) {
-      const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
-      k_cadj_finish<<<nb, 128, 0, sc->stream>>>(s.N, a, sc->io_a.p, sc->io_b.p);
-      sc->launches += 1;
-    }
-    if (sc->nF > 0) {  // v_wc = v + h f_drag(x, v) / m: io_b holds the cotangent of v_wc here
-      k_drag_adj_faces<<<(sc->nF + 127) / 128, 128, 0, sc->stream>>>(
-          sc->nF, sc->df.p, sc->mass.p, s.h, sc->ckpt_x.p + (size_t)st * n3, sc->ckpt_v.p + (size_t)st * n3,
-          sc->io_b.p, sc->fdrag_b.p);
-      k_drag_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, sc->vf_ptr.p, sc->vf_face.p, sc->fdrag_b.p, sc->io_a.p,
-                                                     sc->io_b.p);
-      sc->launches += 2;
+      if (contact_step && recorded[st]) {  // the step's v_wc and L x_t, which a replay would have left behind
+        if (sc->nF > 0)
+          k_drag_faces<<<(sc->nF + 127) / 128, 128, 0, sc->stream>>>(sc->nF, sc->df.p, sx(st), sv(st), sc->fdrag.p);
+        k_contact_step_inputs<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->cd, sx(st), sv(st));
+        sc->launches += 1 + (sc->nF > 0 ? 1 : 0);
+      }
+      if (contact_step) RC(contact_adjoint_step(sc, st, recorded[st] != 0, rbase, sx(st)));
+      CK(cudaGraphLaunch(sc->g_adj.exec, sc->stream));
+      if (contact_step) {
+        const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
+        k_cadj_finish<<<nb, 128, 0, sc->stream>>>(s.N, a, sc->io_a.p, sc->io_b.p);
+        sc->launches += 1;
+      }
+      if (sc->nF > 0) {  // v_wc = v + h f_drag(x, v) / m: io_b holds the cotangent of v_wc here
+        k_drag_adj_faces<<<(sc->nF + 127) / 128, 128, 0, sc->stream>>>(sc->nF, sc->df.p, sc->mass.p, s.h, sx(st), sv(st),
+                                                                        sc->io_b.p, sc->fdrag_b.p);
+        k_drag_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, sc->vf_ptr.p, sc->vf_face.p, sc->fdrag_b.p, sc->io_a.p,
+                                                       sc->io_b.p);
+        sc->launches += 2;
+      }
     }
   }
   if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 0);
   sc->launches += 5;
   for (int st = 0; st < sc->rec_steps && st < (int)sc->rec_iters.size(); ++st)
     sc->launches += (int64_t)(1 + sc->g_adj.outside + (size_t)sc->rec_iters[st] * sc->g_adj.body);
-  if (recomputed > 0)  // replayed step graphs (iteration counts as recorded; contact bodies not counted)
+  if (recomputed > 0)  // step graphs run again (iteration counts as recorded)
     for (int st = 0; st < sc->rec_steps && st < (int)sc->rec_iters.size(); ++st)
-      if (sc->hist_step == 0 || (sc->has_contact && sc->rec_passes[2 * st] > 0 && !recorded[st]))
-        sc->launches += (int64_t)(1 + sc->g_step.outside + (size_t)sc->rec_iters[st] * sc->g_step.body +
+      if (rerun[st])
+        sc->launches += (int64_t)rerun[st] * (int64_t)(1 + sc->g_step.outside + (size_t)sc->rec_iters[st] * sc->g_step.body +
                                   (size_t)sc->rec_passes[2 * st + 1] * sc->g_step.body2);
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_a.p, sc->rhs.p);
   k_to_user<<<nb, 128, 0, sc->stream>>>(s.N, sc->to_user.p, sc->io_b.p, sc->c0.p);

@@ -115,7 +115,8 @@ __device__ __forceinline__ Vec3<double> step_vwc(const SceneDev& d, int i, Vec3<
 }
 
 __global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt, double* vt, double* qn,
-                             double* c0, double* xk, double* hist, long long hist_step, double* ckpt_x, double* ckpt_v,
+                             double* c0, double* xk, double* hist, long long hist_step, int ckpt_every,
+                             double* ckpt_x, double* ckpt_v,
                              int* flag, int* iters, double* partial, unsigned* counter, double* errv,
                              int* status, double* vwc_out) {
   const int b = blockIdx.x, p = pd.blk_part[b];
@@ -126,7 +127,11 @@ __global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt
   double q2 = 0;
   if (i < pv1) {
     Vec3<double> x = ld3(xt, i), v = ld3(vt, i);
-    if (ckpt_x) { st3(ckpt_x + (size_t)s * 3 * d.N, i, x); st3(ckpt_v + (size_t)s * 3 * d.N, i, v); }
+    if (ckpt_x && s % ckpt_every == 0) {  // the start state of every ckpt_every-th step
+      const size_t slot = (size_t)(s / ckpt_every) * 3 * d.N;
+      st3(ckpt_x + slot, i, x);
+      st3(ckpt_v + slot, i, v);
+    }
     // Environment::Step adds g h to v (gravity-enabled bodies); TimeStepping:
     // v_wc = v + h M^-1 f_ext (f_ext = 0), q_n = x + h v_wc
     const Vec3<double> vwc = step_vwc(d, i, v);
