@@ -666,7 +666,9 @@ def run_star(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     prec = DFEM_PREC_FP64 if args.precision == "fp64" else DFEM_PREC_MIXED
-    d = S.muscle_star(refine=2, ground=True, mu=0.5, precision=prec)
+    import dataclasses
+    # checkpoints every 20 steps, as the workload specifies (the adjoint regenerates each segment)
+    d = dataclasses.replace(S.muscle_star(refine=2, ground=True, mu=0.5, precision=prec), checkpoint_every=20)
     sc = Scene(d, device=local)
     n = SIM_STEPS
     rng = np.random.default_rng(42)
@@ -720,7 +722,8 @@ def run_star(args):
             "data": "synthetic",
             "config": {"workload": f"muscle star refine 2 ({d.n_tets} tets, {d.n_vertices} vertices), "
                                    f"{chains} chains x 6 segments, ground quad mu=0.5, h=1/60, K=15, {n} steps, "
-                                   "activations U[0,1] per chain per step (seed 42), forward + adjoint dL/da",
+                                   "activations U[0,1] per chain per step (seed 42), forward + adjoint dL/da, "
+                                   f"checkpoints every {d.checkpoint_every} steps",
                        "precision": args.precision, "contact_steps": int((passes > 0).sum()),
                        "contact_passes_total": int(passes.sum()), "pd_iterations_total": int(iters.sum()),
                        "l2": "flushed between timed steps (256 MB write)"},
