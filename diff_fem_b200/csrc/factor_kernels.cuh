@@ -213,30 +213,34 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
       __syncthreads();
     }
   }
-  // 3. dense Cholesky of the diagonal block by one warp (right looking, column by column)
+  // 3. dense Cholesky of the diagonal block (right looking)
   for (int q = threadIdx.x; q < w * w; q += blockDim.x) L[q] = Ld[q];
   __syncthreads();
-  if (warp == 0) {
-    for (int c = 0; c < w; ++c) {
-      double dgl = L[c + c * w];
-      const bool bad = !(dgl > 0.0) || !isfinite(dgl);
-      if (bad) dgl = 1.0;
-      const double piv = sqrt(dgl);
-      __syncwarp();
-      if (lane == 0) {
-        L[c + c * w] = piv;
-        if (bad) s_bad = 1;
-      }
-      for (int i = c + 1 + lane; i < w; i += 32) L[i + c * w] /= piv;
-      __syncwarp();
-      for (int j = c + 1; j < w; ++j) {
-        const double ljc = L[j + c * w];
-        for (int i = j + lane; i < w; i += 32) L[i + j * w] -= L[i + c * w] * ljc;
-      }
-      __syncwarp();
+  // (column by column; the scaling and the trailing update of each column are
+  // spread over the CTA: every element sees the same operations in the same
+  // order as with one thread per row)
+  for (int c = 0; c < w; ++c) {
+    double dgl = L[c + c * w];
+    const bool bad = !(dgl > 0.0) || !isfinite(dgl);
+    if (bad) dgl = 1.0;
+    const double piv = sqrt(dgl);
+    __syncthreads();  // every thread has read the pivot before it is overwritten
+    if (threadIdx.x == 0) {
+      L[c + c * w] = piv;
+      if (bad) s_bad = 1;
     }
+    for (int i = c + 1 + (int)threadIdx.x; i < w; i += blockDim.x) L[i + c * w] /= piv;
+    __syncthreads();
+    const int m = w - c - 1;  // trailing block: rows and columns c+1 .. w-1, lower part
+    for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
+      const int jj = q / m, ii = q % m;
+      if (ii < jj) continue;
+      const int i = c + 1 + ii, j = c + 1 + jj;
+      const double ljc = L[j + c * w];
+      L[i + j * w] -= L[i + c * w] * ljc;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   // 4. X = L_ss^-1 (one column per thread)
   for (int c = threadIdx.x; c < w; c += blockDim.x) {
     for (int i = 0; i < c; ++i) X[i + c * w] = 0.0;
