@@ -225,7 +225,8 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& s, std::string& err) 
   s.alpha = d.alpha;
   s.mu_obs = d.obstacle_friction;
   s.cverts.assign(d.contact_vertices, d.contact_vertices + d.n_contact_vertices);
-  REQ(d.n_drag_faces >= 0 && (d.n_drag_faces == 0 || d.drag_faces), "descriptor: drag_faces missing");
+  REQ(d.n_drag_faces >= 0 && d.n_drag_faces < INT32_MAX / 3 && (d.n_drag_faces == 0 || d.drag_faces),
+      "descriptor: drag_faces missing or too many");
   REQ(inrange(d.drag_faces, 3LL * d.n_drag_faces), "descriptor: drag face vertex out of range");
   s.underwater = d.underwater != 0;
   if (s.underwater) std::fill(s.gmask.begin(), s.gmask.end(), 0.0);  // Environment::Step: no gravity underwater
@@ -342,28 +343,29 @@ void cat_ptr(std::vector<T>& dst, const std::vector<T>& src, O off) {
 bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err) {
   REQ(!P.empty(), "batch: no scenes");
   const HostScene& a = P[0];
-  int64_t totN = 0, totT = 0, totSlots = 0, totRows = 0, totL = 0, totD = 0;
+  int64_t totN = 0, totT = 0, totSlots = 0, totRows = 0, totL = 0, totD = 0, totF = 0;
   for (const HostScene& p : P) {
     REQ(p.h == a.h && p.damping == a.damping && p.g[0] == a.g[0] && p.g[1] == a.g[1] && p.g[2] == a.g[2] &&
             p.K == a.K && p.precision == a.precision && p.checkpoint_every == a.checkpoint_every,
         "batch: scenes must share time_step, damping, gravity, max_iterations, precision and checkpoint_every");
     REQ(!(p.collide && !p.cverts.empty() && !p.obs_f.empty()), "batch: obstacle contact is supported for single scenes only");
-    REQ(p.df.empty() && !p.underwater, "batch: underwater drag is supported for single scenes only");
     REQ(p.nparts == 1, "batch: parts must be single scenes");
     totN += p.N; totT += p.T; totSlots += p.nslots; totRows += (int64_t)p.F.rowidx.size();
-    totL += (int64_t)p.F.Lcm.size(); totD += (int64_t)p.F.Dinv.size();
+    totL += (int64_t)p.F.Lcm.size(); totD += (int64_t)p.F.Dinv.size(); totF += (int64_t)p.df.size() / 3;
   }
   REQ(totN < INT32_MAX / 3 && totT < INT32_MAX / 4 && totSlots < INT32_MAX / 3 && totRows < INT32_MAX / 3 &&
-          totL < INT32_MAX && totD < INT32_MAX,
+          totL < INT32_MAX && totD < INT32_MAX && totF < INT32_MAX / 3,
       "batch: total size exceeds the 32-bit index range of the kernels");
   u = HostScene();
   u.h = a.h; u.damping = a.damping; u.g[0] = a.g[0]; u.g[1] = a.g[1]; u.g[2] = a.g[2];
   u.K = a.K; u.precision = a.precision; u.checkpoint_every = a.checkpoint_every;
   u.collide = false;
+  u.underwater = false;
   u.nparts = (int)P.size();
   u.part_v0 = {0}; u.part_t0 = {0}; u.part_seg0 = {0};
   u.seg_ptr = {0}; u.boff = {0}; u.vslot_ptr = {0};
   u.Hs.ptr = {0};
+  u.vf_ptr = {0};
   SupernodalFactor& F = u.F;
   F.sn_rofs = {0}; F.sn_lofs = {0}; F.sn_dofs = {0}; F.rseg_ptr = {0};
   int voff = 0, moff = 0, segoff = 0, slotoff = 0, bvoff = 0, snoff = 0, rsegoff = 0;
@@ -384,6 +386,12 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
     cat_ptr(u.vslot_ptr, p.vslot_ptr, slotoff);
     cat_ptr(u.Hs.ptr, p.Hs.ptr, hsoff); cat_off(u.Hs.col, p.Hs.col, voff); cat(u.Hs.val, p.Hs.val);
     cat_off(u.to_internal, p.to_internal, voff); cat_off(u.to_user, p.to_user, voff);
+    // drag faces (gravity is already off per vertex in underwater parts); face
+    // slots 3 f + corner shift by the face slots of the earlier parts
+    const int fslot = (int)u.df.size();
+    cat_off(u.df, p.df, voff);
+    cat_ptr(u.vf_ptr, p.vf_ptr, fslot); cat_off(u.vf_face, p.vf_face, fslot);
+    u.underwater = u.underwater || p.underwater;
     // factor (block diagonal)
     const SupernodalFactor& G = p.F;
     cat_off(F.perm, G.perm, voff); cat_off(F.iperm, G.iperm, voff);

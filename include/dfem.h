@@ -153,7 +153,9 @@ int dfem_scene_create(const dfem_scene_desc *desc, int device, dfem_scene **out)
  * them), its own factor and its own regularisation retry; the triangular
  * solves of all parts share one level schedule.  The scenes must share
  * time_step, damping, gravity, max_iterations, precision and
- * checkpoint_every; obstacle contact is not supported in a batch. */
+ * checkpoint_every; obstacle contact is not supported in a batch.  Parts
+ * may mix underwater and dry scenes: drag faces stay with their part's
+ * vertices, and gravity follows each part's own underwater flag. */
 int dfem_scene_create_batch(const dfem_scene_desc *descs, int32_t n_scenes, int device, dfem_scene **out);
 
 /* Part layout of a scene handle (a single scene is one part).  The offset

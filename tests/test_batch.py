@@ -77,6 +77,48 @@ def test_batch_matches_scenes_one_at_a_time(precision):
     b.close()
 
 
+@pytest.mark.parametrize("precision,every", [(_capi.DFEM_PREC_FP64, 1), (_capi.DFEM_PREC_MIXED, 1),
+                                             (_capi.DFEM_PREC_MIXED, 3)])
+def test_batch_with_underwater_parts_matches_scenes(precision, every):
+    """Underwater parts (drag and lift on their faces, no gravity) batched
+    with dry ones: each part's trajectory, iteration counts and gradients are
+    the scene's own, bit for bit, with checkpoints every step or every third
+    (the adjoint then regenerates the segments' drag inputs)."""
+    (wa, va), (wb, vb_) = S.underwater_block(), S.underwater_block(nx=3, ny=3, nz=2, speed=0.9, seed=5)
+    dry = S.muscle_beam()
+    descs = [dataclasses.replace(d, checkpoint_every=every)
+             for d in harmonise([wa, dry, wb], precision)]
+    vels = [va.reshape(-1), np.tile([0.2, 0.1, -0.3], dry.n_vertices), vb_.reshape(-1)]
+    n = 5
+    b = Scene.batch(descs)
+    vo, to, so = b.offsets["vertices"], b.offsets["tets"], b.offsets["segments"]
+    nseg = [d.n_segments for d in descs]
+    rng = np.random.default_rng(11)
+    acts = [rng.uniform(0, 1, (n, k)) for k in nseg]
+    x = np.concatenate([d.x0.reshape(-1) for d in descs])
+    v = np.concatenate(vels)
+    xb, vb, tb = b.forward(x, v, n_steps=n, act=np.concatenate(acts, axis=1), traj=True)
+    itb = b.iterations(n)
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    gb = b.backward(gx, gv)
+    for p, d in enumerate(descs):
+        s = Scene(d)
+        xs, vs, ts = s.forward(d.x0.reshape(-1), vels[p], n_steps=n, act=acts[p] if nseg[p] else None, traj=True)
+        assert np.array_equal(s.iterations(n), itb[:, p]), p
+        assert np.array_equal(split(xb, vo)[p], xs), p
+        assert np.array_equal(split(vb, vo)[p], vs), p
+        assert np.array_equal(tb[:, 3 * vo[p]: 3 * vo[p + 1]], ts), p
+        gs = s.backward(split(gx, vo)[p], split(gv, vo)[p])
+        for k in ("x", "v"):
+            assert np.array_equal(split(gb[k], vo)[p], gs[k]), (p, k)
+        for k in ("E", "nu"):
+            assert np.array_equal(gb[k][to[p]:to[p + 1]], gs[k]), (p, k)
+        if nseg[p]:
+            assert np.array_equal(gb["act"][:, so[p]:so[p + 1]], gs["act"]), p
+        s.close()
+    b.close()
+
+
 def test_batch_set_materials_refactors_each_part():
     descs = harmonise([S.inverse_stiffness(nx=8, ny=3, nz=3, seed=s) for s in (1, 2, 3)])
     b = Scene.batch(descs)
