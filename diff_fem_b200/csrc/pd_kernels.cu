@@ -84,8 +84,9 @@ __device__ __forceinline__ Mat3<double> deformation(const double G[4][3], const 
 // heaviest per-constraint kernels (128 threads each): more resident warps hide
 // the FP64 latency chains better than the registers they give up (the
 // adjoint local step of the 256-scene batch: 1.12 ms at 174 registers, 0.85 ms
-// at 128 with spills to L1; the FP32 force step 0.315 -> 0.282 ms, the FP64
-// local step 0.411 -> 0.383 ms).
+// at 128 with spills to L1; the mixed force step, then with an FP32 tail after
+// its SVD, 0.315 -> 0.282 ms, the FP64 local step 0.411 -> 0.383 ms; the
+// mixed force step with its FP64 tail takes 0.311 ms at 96 registers).
 #ifndef DFEM_FORCE_MIN_BLOCKS
 #define DFEM_FORCE_MIN_BLOCKS 5
 #endif
@@ -258,7 +259,8 @@ __device__ __forceinline__ Vec3<float> ld3f(const float* p, int i) { return mk3(
 // which is the reference's map b + J d(x^k) - Hs x rearranged (Hs = M/h^2 +
 // sum_c L_c).  FP32 rounding is then relative to the forces, not to J d ~ L x.
 // Inputs of cancelling differences (F, spring lengths, Laplacians) are formed
-// in FP64 first.
+// in FP64 first; each slot is rounded to FP32 once, from an FP64 value, and a
+// vertex's slots are summed in FP64.
 
 __global__ void __launch_bounds__(128, DFEM_FORCE_MIN_BLOCKS) k_force_f32(SceneDev d, Gate gate, const double* __restrict__ x,
                                                    const double* __restrict__ act_all, const int* step,
@@ -272,18 +274,18 @@ __global__ void __launch_bounds__(128, DFEM_FORCE_MIN_BLOCKS) k_force_f32(SceneD
     load_g(d.tinv, d.T, t, G);
     const Mat3<double> F = deformation(G, xv);
     const double wr = d.twr[t], wv = d.twv[t];
-    Vec3<float> P[3];
-    if (!corot_force_mixed(F, (float)wr, (float)wv, P)) {  // inverted or near-degenerate: FP64
+    Vec3<double> P[3];
+    if (!corot_force_mixed(F, wr, wv, P)) {  // inverted or near-degenerate: FP64
       Mat3<double> md, mdv;
       corot_project(F, md, mdv);
 #pragma unroll
-      for (int j = 0; j < 3; ++j) P[j] = to_f(wr * (md.c[j] - F.c[j]) + wv * (mdv.c[j] - F.c[j]));
+      for (int j = 0; j < 3; ++j) P[j] = wr * (md.c[j] - F.c[j]) + wv * (mdv.c[j] - F.c[j]);
     }
+    // corner forces G_a P (their sum cancels to zero), each rounded once into its FP32 slot
     int4 sl = d.tslot[t];
     const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
-      st3f(slot, sv[a], (float)G[a][0] * P[0] + (float)G[a][1] * P[1] + (float)G[a][2] * P[2]);
+    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], to_f(G[a][0] * P[0] + G[a][1] * P[1] + G[a][2] * P[2]));
     return;
   }
   t -= d.T;
@@ -303,11 +305,11 @@ __global__ void __launch_bounds__(128, DFEM_FORCE_MIN_BLOCKS) k_force_f32(SceneD
       Ff = Ff + ck * ds[k];
     }
     const double a_act = act_all[(size_t)(*step) * d.nseg + d.mseg[t]];
-    const Vec3<float> p = to_f((-a_act * d.mw[t]) * Ff);
+    const Vec3<double> p = (-a_act * d.mw[t]) * Ff;
     int4 sl = d.mslot[t];
     const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
 #pragma unroll
-    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], (float)c[a] * p);
+    for (int a = 0; a < 4; ++a) st3f(slot, sv[a], to_f(c[a] * p));
     return;
   }
   t -= d.M;
@@ -329,21 +331,22 @@ __global__ void __launch_bounds__(128, DFEM_FORCE_MIN_BLOCKS) k_force_f32(SceneD
     for (int k = o0 + 1; k < o1; ++k) lap = lap + d.bbeta[k] * (ld3(x, d.bv[k]) - xc);  // sum beta = 0
     const double ln = sqrt(dot3(lap, lap)), w = d.bw[t];
     const double sc = w * w * ((ln > 1e-25 ? d.brest[t] / ln : 0.0) - w);
-    const Vec3<float> fl = to_f(sc * lap);
-    for (int k = o0; k < o1; ++k) st3f(slot, d.bslot[k], (float)d.bbeta[k] * fl);
+    const Vec3<double> fl = sc * lap;
+    for (int k = o0; k < o1; ++k) st3f(slot, d.bslot[k], to_f(d.bbeta[k] * fl));
   }
 }
 
-// r_i = m_i/h^2 (q_i - x_i) + attach_jd_i - attach_k_i x_i + the FP32 sum of vertex i's force slots
+// r_i = m_i/h^2 (q_i - x_i) + attach_jd_i - attach_k_i x_i + the sum of vertex i's FP32 force
+// slots, accumulated in FP64 (the slots' own rounding is then the only FP32 error of the rhs)
 __global__ void k_gather_force(SceneDev d, Gate gate, const float* __restrict__ slot, const double* __restrict__ qn,
                                const double* __restrict__ x, double* __restrict__ rhs) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.N || gate.skip(vpart_of(d, i))) return;
-  Vec3<float> acc = mk3(0.0f, 0.0f, 0.0f);
-  for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) acc = acc + ld3f(slot, k);
+  Vec3<double> acc = mk3(0.0, 0.0, 0.0);
+  for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) acc = acc + to_d(ld3f(slot, k));
   const Vec3<double> xi = ld3(x, i);
   const double m = d.mass[i] / (d.h * d.h);
-  st3(rhs, i, m * (ld3(qn, i) - xi) + ld3(d.attach_jd, i) - d.attach_k[i] * xi + to_d(acc));
+  st3(rhs, i, m * (ld3(qn, i) - xi) + ld3(d.attach_jd, i) - d.attach_k[i] * xi + acc);
 }
 
 // rhs_i = c0_i + sum of the slots of vertex i

@@ -224,20 +224,22 @@ __device__ __forceinline__ Mat3<double> rot_from_quat(const float qf[4]) {
 }
 
 // Mixed-form corotated deviations DR = md - F and DV = md_volume - F (columns;
-// the tet's J d - L x is G (wr DR + wv DV)), with FP32 rounding relative to
-// the strain rather than to F:
+// the tet's J d - L x is G (wr DR + wv DV)).  Only the SVD runs in FP32; its
+// error enters the deviations at second order:
 //   1. FP32 SVD of F -> R0 = U V^T, its quaternion, and R = R(q) exactly
 //      orthogonal in FP64;
-//   2. A = R^T F in FP64, H = A - I rounded to FP32 (strain-sized; its skew
-//      part is only R0's rounding);
+//   2. A = R^T F, H = A - I in FP64 (strain-sized; its skew part is only
+//      R0's rounding);
 //   3. polar of A = (I + Omega) S_A to first order in the tiny skew part, in
 //      the V basis: Omega_kl = 2 (V^T skew(H) V)_kl / (s_k + s_l);
 //   4. md - F = R (Omega - H);  the volume projection's 5 Newton steps run on
 //      e_k = v_k^T sym(H) v_k (= s_k - 1 to second order) with
 //      prod(1 + a) - 1 expanded, and md_volume - F = R V diag(D) V^T.
-// Returns false (caller takes the FP64 branch) for inverted or
+// Steps 2-4 are FP64 arithmetic on the FP32 singular vectors (the one FP32
+// rounding of the force is then the caller's store into its slots).
+// Returns false (caller takes the full FP64 branch) for inverted or
 // near-degenerate elements.
-__device__ __forceinline__ bool corot_delta_mixed(const Mat3<double>& F, Vec3<float> DR[3], Vec3<float> DV[3]) {
+__device__ __forceinline__ bool corot_delta_mixed(const Mat3<double>& F, Vec3<double> DR[3], Vec3<double> DV[3]) {
   Mat3<float> Ff;
 #pragma unroll
   for (int j = 0; j < 3; ++j) Ff.c[j] = mk3((float)F.c[j].x, (float)F.c[j].y, (float)F.c[j].z);
@@ -245,72 +247,73 @@ __device__ __forceinline__ bool corot_delta_mixed(const Mat3<double>& F, Vec3<fl
   const float smax = fmaxf(sv.s[0], fmaxf(sv.s[1], sv.s[2]));
   const float smin = fminf(sv.s[0], fminf(sv.s[1], sv.s[2]));
   if (!(smax > 0.0f) || !(smin >= kDegenerateRatio * smax) || !(det3(F) > 0.0)) return false;
-  const float vj[3][3] = {{sv.v[0].x, sv.v[1].x, sv.v[2].x}, {sv.v[0].y, sv.v[1].y, sv.v[2].y}, {sv.v[0].z, sv.v[1].z, sv.v[2].z}};
+  const float vjf[3][3] = {{sv.v[0].x, sv.v[1].x, sv.v[2].x}, {sv.v[0].y, sv.v[1].y, sv.v[2].y},
+                           {sv.v[0].z, sv.v[1].z, sv.v[2].z}};
   Mat3<float> R0;
 #pragma unroll
-  for (int j = 0; j < 3; ++j) R0.c[j] = vj[j][0] * sv.u[0] + vj[j][1] * sv.u[1] + vj[j][2] * sv.u[2];
+  for (int j = 0; j < 3; ++j) R0.c[j] = vjf[j][0] * sv.u[0] + vjf[j][1] * sv.u[1] + vjf[j][2] * sv.u[2];
   float q[4];
   quat_from_rot(R0, q);
   const Mat3<double> R = rot_from_quat(q);
-  float H[3][3];  // H[i][j] = (R^T F - I)_ij
+  Vec3<double> v[3];  // the FP32 right singular vectors, widened
+#pragma unroll
+  for (int k = 0; k < 3; ++k) v[k] = mk3((double)sv.v[k].x, (double)sv.v[k].y, (double)sv.v[k].z);
+  double H[3][3];  // H[i][j] = (R^T F - I)_ij
 #pragma unroll
   for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) H[i][j] = (float)(dot3(R.c[i], F.c[j]) - (i == j ? 1.0 : 0.0));
-  Vec3<float> Hvl[3], HTvl[3];  // H v_l and H^T v_l
+    for (int j = 0; j < 3; ++j) H[i][j] = dot3(R.c[i], F.c[j]) - (i == j ? 1.0 : 0.0);
+  Vec3<double> Hvl[3], HTvl[3];  // H v_l and H^T v_l
 #pragma unroll
   for (int l = 0; l < 3; ++l) {
-    const Vec3<float> v = sv.v[l];
-    Hvl[l] = mk3(H[0][0] * v.x + H[0][1] * v.y + H[0][2] * v.z, H[1][0] * v.x + H[1][1] * v.y + H[1][2] * v.z,
-                 H[2][0] * v.x + H[2][1] * v.y + H[2][2] * v.z);
-    HTvl[l] = mk3(H[0][0] * v.x + H[1][0] * v.y + H[2][0] * v.z, H[0][1] * v.x + H[1][1] * v.y + H[2][1] * v.z,
-                  H[0][2] * v.x + H[1][2] * v.y + H[2][2] * v.z);
+    const Vec3<double> w = v[l];
+    Hvl[l] = mk3(H[0][0] * w.x + H[0][1] * w.y + H[0][2] * w.z, H[1][0] * w.x + H[1][1] * w.y + H[1][2] * w.z,
+                 H[2][0] * w.x + H[2][1] * w.y + H[2][2] * w.z);
+    HTvl[l] = mk3(H[0][0] * w.x + H[1][0] * w.y + H[2][0] * w.z, H[0][1] * w.x + H[1][1] * w.y + H[2][1] * w.z,
+                  H[0][2] * w.x + H[1][2] * w.y + H[2][2] * w.z);
   }
-  float e[3];
+  double e[3];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) e[k] = dot3(sv.v[k], Hvl[k]);  // v^T H v = v^T sym(H) v
+  for (int k = 0; k < 3; ++k) e[k] = dot3(v[k], Hvl[k]);  // v^T H v = v^T sym(H) v
   // Omega in the V basis (pairs 01, 02, 12); Omega = sum_{k<l} om_kl (v_k v_l^T - v_l v_k^T)
   const int pk[3] = {0, 0, 1}, pl[3] = {1, 2, 2};
-  float om[3];
+  double om[3];
 #pragma unroll
   for (int p = 0; p < 3; ++p) {
     const int k = pk[p], l = pl[p];
-    const float kskew = 0.5f * (dot3(sv.v[k], Hvl[l]) - dot3(sv.v[k], HTvl[l]));  // v_k^T skew(H) v_l
-    om[p] = 2.0f * kskew / (sv.s[k] + sv.s[l]);
+    const double kskew = 0.5 * (dot3(v[k], Hvl[l]) - dot3(v[k], HTvl[l]));  // v_k^T skew(H) v_l
+    om[p] = 2.0 * kskew / ((double)sv.s[k] + (double)sv.s[l]);
   }
   // volume projection on the small quantities (same iterates as on s + D)
-  float D[3] = {0.0f, 0.0f, 0.0f};
+  double D[3] = {0.0, 0.0, 0.0};
 #pragma unroll
   for (int it = 0; it < 5; ++it) {
-    const float a0 = e[0] + D[0], a1 = e[1] + D[1], a2 = e[2] + D[2];
-    const float C = (a0 + a1 + a2) + (a0 * a1 + a0 * a2 + a1 * a2) + a0 * a1 * a2;
-    const float g0 = 1.0f + a1 + a2 + a1 * a2, g1 = 1.0f + a0 + a2 + a0 * a2, g2 = 1.0f + a0 + a1 + a0 * a1;
-    const float c = (g0 * D[0] + g1 * D[1] + g2 * D[2] - C) / (g0 * g0 + g1 * g1 + g2 * g2);
+    const double a0 = e[0] + D[0], a1 = e[1] + D[1], a2 = e[2] + D[2];
+    const double C = (a0 + a1 + a2) + (a0 * a1 + a0 * a2 + a1 * a2) + a0 * a1 * a2;
+    const double g0 = 1.0 + a1 + a2 + a1 * a2, g1 = 1.0 + a0 + a2 + a0 * a2, g2 = 1.0 + a0 + a1 + a0 * a1;
+    const double c = (g0 * D[0] + g1 * D[1] + g2 * D[2] - C) / (g0 * g0 + g1 * g1 + g2 * g2);
     D[0] = c * g0; D[1] = c * g1; D[2] = c * g2;
   }
-  // md - F = R (Omega - H), md_volume - F = R V diag(D) V^T (R rounded to FP32:
-  // a relative error on small products)
-  Mat3<float> Rf;
-#pragma unroll
-  for (int j = 0; j < 3; ++j) Rf.c[j] = mk3((float)R.c[j].x, (float)R.c[j].y, (float)R.c[j].z);
+  // md - F = R (Omega - H), md_volume - F = R V diag(D) V^T
+  const double vj[3][3] = {{v[0].x, v[1].x, v[2].x}, {v[0].y, v[1].y, v[2].y}, {v[0].z, v[1].z, v[2].z}};
 #pragma unroll
   for (int j = 0; j < 3; ++j) {
-    Vec3<float> col = mk3(-H[0][j], -H[1][j], -H[2][j]);
+    Vec3<double> col = mk3(-H[0][j], -H[1][j], -H[2][j]);
 #pragma unroll
     for (int p = 0; p < 3; ++p) {
       const int k = pk[p], l = pl[p];
-      col = col + (om[p] * vj[j][l]) * sv.v[k] - (om[p] * vj[j][k]) * sv.v[l];
+      col = col + (om[p] * vj[j][l]) * v[k] - (om[p] * vj[j][k]) * v[l];
     }
-    const Vec3<float> vol = (D[0] * vj[j][0]) * sv.v[0] + (D[1] * vj[j][1]) * sv.v[1] + (D[2] * vj[j][2]) * sv.v[2];
-    DR[j] = col.x * Rf.c[0] + col.y * Rf.c[1] + col.z * Rf.c[2];
-    DV[j] = vol.x * Rf.c[0] + vol.y * Rf.c[1] + vol.z * Rf.c[2];
+    const Vec3<double> vol = (D[0] * vj[j][0]) * v[0] + (D[1] * vj[j][1]) * v[1] + (D[2] * vj[j][2]) * v[2];
+    DR[j] = col.x * R.c[0] + col.y * R.c[1] + col.z * R.c[2];
+    DV[j] = vol.x * R.c[0] + vol.y * R.c[1] + vol.z * R.c[2];
   }
   return true;
 }
 
 // Mixed-form corotated force P = wr (md - F) + wv (md_volume - F) (columns).
-__device__ __forceinline__ bool corot_force_mixed(const Mat3<double>& F, float wr, float wv, Vec3<float> P[3]) {
-  Vec3<float> DR[3], DV[3];
+__device__ __forceinline__ bool corot_force_mixed(const Mat3<double>& F, double wr, double wv, Vec3<double> P[3]) {
+  Vec3<double> DR[3], DV[3];
   if (!corot_delta_mixed(F, DR, DV)) return false;
 #pragma unroll
   for (int j = 0; j < 3; ++j) P[j] = wr * DR[j] + wv * DV[j];

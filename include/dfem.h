@@ -46,7 +46,9 @@ enum dfem_mem { DFEM_MEM_HOST = 0, DFEM_MEM_DEVICE = 1 };
 
 enum dfem_precision {
   DFEM_PREC_FP64 = 0,   /* plain form: everything FP64                          */
-  DFEM_PREC_MIXED = 1   /* FP32 projections/contact, FP64 factor + residual     */
+  DFEM_PREC_MIXED = 1   /* FP32 tet SVD and per-constraint force slots; FP64
+                           projection tail, slot sums, factor, solves, state,
+                           contact phase and adjoint                            */
 };
 
 /*
