@@ -16,9 +16,10 @@
 namespace dfem {
 
 // state words: [mode, pass, it, any, active, loop-body executions, computed
-// Jacobi iterations, the computed iteration whose x_n1 the current ori_x is]
+// Jacobi iterations, the computed iteration whose x_n1 the current ori_x is,
+// obstacle impacts in the lists, self groups of this pass, of the last pass]
 enum { CS_MODE = 0, CS_PASS = 1, CS_IT = 2, CS_ANY = 3, CS_ACTIVE = 4, CS_BODIES = 5, CS_COMP = 6, CS_SRC = 7,
-       CS_SIZE = 8 };
+       CS_NOBS = 8, CS_NGRP = 9, CS_NGRP_PREV = 10, CS_SIZE = 11 };
 
 // per-step record of the phase: [passes, loop-body executions]; while the
 // forward steps record their contact iterations, the step's place in the
@@ -146,6 +147,74 @@ __device__ bool vf_impact(Vec3<double> p0, Vec3<double> p1, Vec3<double> q0, Vec
 }
 
 // contact basis [n, t, b] (CollisionBrutal::computeBasis)
+// Vertex (p0 -> p1) against a moving face (qs -> qe): arcsim's vf_collision_test
+// + collision_test (sim/utils/arcsim/collision.cpp:118-128, 211-274) with the
+// swept boxes of the vertex and the face dilated by thickness * mult.  On an
+// impact returns its time t, distance |d| and normal (the face's start normal,
+// against the vertex's approach; not unit length).
+__device__ bool vf_impact_moving(Vec3<double> p0, Vec3<double> p1, const Vec3<double> qs[3], const Vec3<double> qe[3],
+                                 double mult, Vec3<double>* n_out, double* t_out, double* d_out) {
+  const double thick = kContactThickness * mult;
+  {
+    const double plo[3] = {fmin(p0.x, p1.x), fmin(p0.y, p1.y), fmin(p0.z, p1.z)};
+    const double phi[3] = {fmax(p0.x, p1.x), fmax(p0.y, p1.y), fmax(p0.z, p1.z)};
+    double flo[3] = {1e300, 1e300, 1e300}, fhi[3] = {-1e300, -1e300, -1e300};
+    for (int k = 0; k < 3; ++k) {
+      flo[0] = fmin(flo[0], fmin(qs[k].x, qe[k].x)); fhi[0] = fmax(fhi[0], fmax(qs[k].x, qe[k].x));
+      flo[1] = fmin(flo[1], fmin(qs[k].y, qe[k].y)); fhi[1] = fmax(fhi[1], fmax(qs[k].y, qe[k].y));
+      flo[2] = fmin(flo[2], fmin(qs[k].z, qe[k].z)); fhi[2] = fmax(fhi[2], fmax(qs[k].z, qe[k].z));
+    }
+    for (int c = 0; c < 3; ++c)
+      if (phi[c] < flo[c] - thick || plo[c] > fhi[c] + thick) return false;
+  }
+  const Vec3<double> v0 = p1 - p0;
+  const Vec3<double> x1 = qs[0] - p0, x2 = qs[1] - p0, x3 = qs[2] - p0;
+  const Vec3<double> v1 = (qe[0] - qs[0]) - v0, v2 = (qe[1] - qs[1]) - v0, v3 = (qe[2] - qs[2]) - v0;
+  const double a0 = stp3(x1, x2, x3);
+  const double a1 = stp3(v1, x2, x3) + stp3(x1, v2, x3) + stp3(x1, x2, v3);
+  const double a2 = stp3(x1, v2, v3) + stp3(v1, x2, v3) + stp3(v1, v2, x3);
+  const double a3 = stp3(v1, v2, v3);
+  double t[4];
+  int nsol = ccd_cubic(a3, a2, a1, a0, t);
+  t[nsol++] = 1;
+  for (int i = 0; i < nsol; ++i) {
+    if (t[i] < 0 || t[i] > 1) continue;
+    const Vec3<double> xt = p0 + t[i] * v0;
+    const Vec3<double> y0 = qs[0] + t[i] * (qe[0] - qs[0]), y1 = qs[1] + t[i] * (qe[1] - qs[1]),
+                       y2 = qs[2] + t[i] * (qe[2] - qs[2]);
+    Vec3<double> n = cross3(unit3(y1 - y0), unit3(y2 - y0));
+    double d, w1, w2, w3;
+    if (dot3(n, n) < 1e-6) {
+      d = INFINITY; w1 = w2 = w3 = 0.0;
+    } else {
+      n = unit3(n);
+      d = dot3(xt - y0, n);
+      const double b0 = stp3(y1 - xt, y2 - xt, n), b1 = stp3(y2 - xt, y0 - xt, n), b2 = stp3(y0 - xt, y1 - xt, n);
+      const double sb = b0 + b1 + b2;
+      w1 = -b0 / sb; w2 = -b1 / sb; w3 = -b2 / sb;
+    }
+    bool inside = fmin(fmin(-w1, -w2), -w3) >= -1e-6;
+    if (t[i] == 1) {
+      inside = inside || sqrt(dot3(xt - y0, xt - y0)) < thick || sqrt(dot3(xt - y1, xt - y1)) < thick ||
+               sqrt(dot3(xt - y2, xt - y2)) < thick;
+      Vec3<double> e;
+      e = xt - y0 - (dot3(xt - y0, y1 - y0) / dot3(y1 - y0, y1 - y0)) * (y1 - y0);
+      inside = inside || sqrt(dot3(e, e)) < thick;
+      e = xt - y1 - (dot3(xt - y1, y2 - y1) / dot3(y2 - y1, y2 - y1)) * (y2 - y1);
+      inside = inside || sqrt(dot3(e, e)) < thick;
+      e = xt - y2 - (dot3(xt - y2, y0 - y2) / dot3(y0 - y2, y0 - y2)) * (y0 - y2);
+      inside = inside || sqrt(dot3(e, e)) < thick;
+    }
+    const Vec3<double> fn = cross3(unit3(qs[1] - qs[0]), unit3(qs[2] - qs[0]));
+    if (dot3(n, w1 * v1 + w2 * v2 + w3 * v3) > 0) n = (-1.0) * fn; else n = fn;
+    if (fabs(d) < thick && inside) {
+      *n_out = n; *t_out = t[i]; *d_out = fabs(d);
+      return true;
+    }
+  }
+  return false;
+}
+
 __device__ __forceinline__ void contact_basis(Vec3<double> nrm, Vec3<double> B[3]) {
   Vec3<double> tg = cross3(nrm, mk3(1.0, 0.0, 0.0));
   if (sqrt(dot3(tg, tg)) < 1e-15) tg = cross3(nrm, mk3(0.0, 1.0, 0.0));
@@ -181,10 +250,13 @@ __global__ void k_contact_begin(SceneDev d, ContactDev c, const double* xt, cons
     st3(c.xold, i, mk3(0.0, 0.0, 0.0));
     st3(c.lxt, i, contact_lxt(d, i, xt));
   }
-  if (i < c.nc) c.imp_cnt[i] = 0;
+  if (i < c.nc) {
+    c.imp_cnt[i] = 0;
+    if (c.ncf > 0) c.simp_cnt[i] = 0;
+  }
   if (i == 0) {
     for (int k = 0; k < CS_SIZE; ++k) c.state[k] = 0;
-    cudaGraphSetConditional(h, (c.nc > 0 && c.nof > 0) ? 1u : 0u);
+    cudaGraphSetConditional(h, (c.nc > 0 && (c.nof > 0 || c.ncf > 0)) ? 1u : 0u);
   }
 }
 
@@ -209,16 +281,48 @@ __global__ void k_contact_detect(ContactDev c, const double* xt, const double* x
       slot = cnt;
       c.imp_face[a * kMaxImpactsPerVertex + slot] = f;
       c.imp_cnt[a] = cnt + 1;
+      atomicAdd(&c.state[CS_NOBS], 1);
     }
     st3(c.imp_n, a * kMaxImpactsPerVertex + slot, n);
   }
   if (any) atomicOr(&c.state[CS_ANY], 1);
+  // soft impacts (thickness x 2) against every soft face not holding the
+  // vertex, faces ascending; a face met again refreshes its entry in place
+  if (c.ncf > 0 && c.on_face[a]) {
+    for (int f = 0; f < c.ncf; ++f) {
+      const int* cf = c.cfaces + 3 * f;
+      if (cf[0] == a || cf[1] == a || cf[2] == a) continue;
+      Vec3<double> qs[3], qe[3];
+      for (int k = 0; k < 3; ++k) {
+        const int gq = c.cverts[cf[k]];
+        qs[k] = ld3(xt, gq);
+        qe[k] = ld3(xk, gq);
+      }
+      Vec3<double> n;
+      double t, dd;
+      if (!vf_impact_moving(p0, p1, qs, qe, 2.0, &n, &t, &dd)) continue;
+      const int base = a * kMaxSelfImpacts;
+      int cnt = c.simp_cnt[a], slot = -1;
+      for (int q = 0; q < cnt; ++q)
+        if (c.simp_face[base + q] == f) { slot = q; break; }
+      if (slot < 0) {
+        if (cnt >= kMaxSelfImpacts) { atomicExch(status, 6); continue; }
+        slot = cnt;
+        c.simp_face[base + slot] = f;
+        c.simp_cnt[a] = cnt + 1;
+      }
+      c.simp_td[2 * (base + slot)] = t;
+      c.simp_td[2 * (base + slot) + 1] = dd;
+      st3(c.simp_n, base + slot, n);
+    }
+  }
 }
 
 // After detection: finish when nothing was hit (or the pass cap is reached), else start Jacobi iterations.
 __global__ void k_contact_ctl_detect(ContactDev c, cudaGraphConditionalHandle h) {
   if (c.state[CS_MODE] != 0) return;
-  if (c.state[CS_ANY] == 0 || c.state[CS_PASS] >= c.max_passes) {
+  const bool same_groups = c.ncf == 0 || c.state[CS_NGRP] == c.state[CS_NGRP_PREV];
+  if ((c.state[CS_ANY] == 0 && same_groups) || c.state[CS_PASS] >= c.max_passes) {
     cudaGraphSetConditional(h, 0u);
     return;
   }
@@ -334,6 +438,298 @@ __global__ void k_contact_ctl_iter(ContactDev c, int K) {
     atomicExch(c.status, 6);  // the replayed step's record is too small
   c.state[CS_COMP] += 1;
   if (it >= K) c.state[CS_MODE] = 0;
+}
+
+// ---- soft-soft (self) contact ------------------------------------------------
+//
+// CollisionBrutal::getSelfCollisionsInfo (collisionBrutal.h:645-700): each
+// contact vertex's closest soft impact of the step (smallest t; at t = 1 the
+// smallest distance; earlier list entries otherwise), its vertices grouped by
+// face.  Groups are kept per face (g_ptr / g_mem, members ascending), the
+// group normal is its first member's impact normal.  Run in detection mode
+// after k_contact_detect; the pass ends when no new obstacle impact appeared
+// and the number of groups did not change (BaseUpdateCollisions' return).
+
+__global__ void k_self_reset(ContactDev c) {
+  if (c.state[CS_MODE] != 0) return;
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < c.ncf) { c.g_cnt[f] = 0; c.g_fill[f] = 0; }
+  if (f == 0) { c.state[CS_NGRP_PREV] = c.state[CS_NGRP]; c.state[CS_NGRP] = 0; }
+}
+
+__global__ void k_self_closest(ContactDev c) {
+  if (c.state[CS_MODE] != 0) return;
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= c.nc) return;
+  const int base = a * kMaxSelfImpacts, cnt = c.simp_cnt[a];
+  int best = -1;
+  for (int q = 0; q < cnt; ++q) {
+    if (best < 0) { best = q; continue; }
+    const double t = c.simp_td[2 * (base + q)], bt = c.simp_td[2 * (base + best)];
+    if (t < bt) { best = q; continue; }
+    if (bt == 1.0 && c.simp_td[2 * (base + best) + 1] > c.simp_td[2 * (base + q) + 1]) best = q;
+  }
+  c.cf_slot[a] = best;
+  c.cf_face[a] = best >= 0 ? c.simp_face[base + best] : -1;
+  if (best >= 0) atomicAdd(&c.g_cnt[c.simp_face[base + best]], 1);
+}
+
+// one block: g_ptr = exclusive scan of g_cnt, and the number of groups
+__global__ void k_self_scan(ContactDev c) {
+  if (c.state[CS_MODE] != 0) return;
+  __shared__ int sh[1024];
+  __shared__ int carry_s, groups_s;
+  const int tid = threadIdx.x, bs = blockDim.x;
+  if (tid == 0) { carry_s = 0; groups_s = 0; }
+  __syncthreads();
+  for (int base = 0; base < c.ncf; base += bs) {
+    const int f = base + tid;
+    const int v = f < c.ncf ? c.g_cnt[f] : 0;
+    sh[tid] = v;
+    const int nz = __syncthreads_count(v > 0);
+    for (int off = 1; off < bs; off <<= 1) {  // inclusive Hillis-Steele scan
+      const int add = tid >= off ? sh[tid - off] : 0;
+      __syncthreads();
+      sh[tid] += add;
+      __syncthreads();
+    }
+    if (f < c.ncf) c.g_ptr[f] = carry_s + sh[tid] - v;
+    __syncthreads();
+    if (tid == 0) { carry_s += sh[bs - 1]; groups_s += nz; }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    c.g_ptr[c.ncf] = carry_s;
+    c.state[CS_NGRP] = groups_s;
+  }
+}
+
+__global__ void k_self_fill(ContactDev c) {
+  if (c.state[CS_MODE] != 0) return;
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= c.nc) return;
+  const int f = c.cf_face[a];
+  if (f < 0) return;
+  const int pos = atomicAdd(&c.g_fill[f], 1);
+  c.g_mem[c.g_ptr[f] + pos] = a;
+}
+
+// members ascending (the fill order is arbitrary); group normal; member slots
+__global__ void k_self_sort(ContactDev c, int* status) {
+  if (c.state[CS_MODE] != 0) return;
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= c.ncf) return;
+  const int cnt = c.g_cnt[f];
+  if (cnt == 0) return;
+  if (cnt > kMaxGroupMembers) atomicExch(status, 6);
+  int* m = c.g_mem + c.g_ptr[f];
+  for (int k = 1; k < cnt; ++k) {
+    const int v = m[k];
+    int j = k - 1;
+    while (j >= 0 && m[j] > v) { m[j + 1] = m[j]; --j; }
+    m[j + 1] = v;
+  }
+  for (int k = 0; k < cnt; ++k) c.m_slot[m[k]] = c.g_ptr[f] + k;
+  const int a0 = m[0];
+  st3(c.g_n, f, ld3(c.simp_n, a0 * kMaxSelfImpacts + c.cf_slot[a0]));
+}
+
+__device__ __forceinline__ Vec3<double> to_local3(const Vec3<double> B[3], Vec3<double> p) {
+  return mk3(p.x * B[0].x + p.y * B[0].y + p.z * B[0].z, p.x * B[1].x + p.y * B[1].y + p.z * B[1].z,
+             p.x * B[2].x + p.y * B[2].y + p.z * B[2].z);
+}
+__device__ __forceinline__ Vec3<double> to_world3(const Vec3<double> B[3], Vec3<double> r) {
+  return mk3(r.x * B[0].x + r.y * B[1].x + r.z * B[2].x, r.x * B[0].y + r.y * B[1].y + r.z * B[2].y,
+             r.x * B[0].z + r.y * B[1].z + r.z * B[2].z);
+}
+__device__ __forceinline__ Vec3<double> div3(Vec3<double> a, double s) { return mk3(a.x / s, a.y / s, a.z / s); }
+
+// World::do_solve_friction (World.h:1246-1315) on local-frame momenta: the
+// sticking set (face + sticking members) moves tangentially together; sliding
+// members receive mu times their normal force against their own slip, the
+// sticking set mu f_n (sliding) along the mean slip.
+__device__ void group_friction(Vec3<double> p0, double m0, Vec3<double>& r0, const Vec3<double>* ps, const double* ms,
+                               Vec3<double>* rs, const unsigned char* stick, int n, double mu) {
+  Vec3<double> pstick = p0;
+  double mstick = m0;
+  for (int k = 0; k < n; ++k)
+    if (stick[k]) { pstick = pstick + ps[k]; mstick = mstick + ms[k]; }
+  Vec3<double> pslide = mk3(0.0, 0.0, 0.0);
+  double mslide = 0.0, fn = 0.0;
+  for (int k = 0; k < n; ++k)
+    if (!stick[k]) { pslide = pslide + ps[k]; mslide = mslide + ms[k]; fn = fn + rs[k].x; }
+  const Vec3<double> v = div3(pstick, mstick);
+  r0.y = v.y * m0 - p0.y;
+  r0.z = v.z * m0 - p0.z;
+  for (int k = 0; k < n; ++k)
+    if (stick[k]) { rs[k].y = v.y * ms[k] - ps[k].y; rs[k].z = v.z * ms[k] - ps[k].z; }
+  if (mslide > 0) {
+    Vec3<double> rel = div3(pslide, mslide) - div3(pstick, mstick);
+    rel = div3(rel, sqrt(rel.y * rel.y + rel.z * rel.z));
+    const double mult = mu * fn / (mslide + mstick);
+    r0.y = r0.y + rel.y * mult * m0;
+    r0.z = r0.z + rel.z * mult * m0;
+    for (int k = 0; k < n; ++k)
+      if (stick[k]) { rs[k].y = rs[k].y + rel.y * mult * ms[k]; rs[k].z = rs[k].z + rel.z * mult * ms[k]; }
+    const Vec3<double> abs_v0 = div3(p0 + r0, m0);
+    for (int k = 0; k < n; ++k)
+      if (!stick[k]) {
+        Vec3<double> rk = div3(ps[k], ms[k]) - abs_v0;
+        rk = div3(rk, sqrt(rk.y * rk.y + rk.z * rk.z));
+        const double mk = -mu * rs[k].x * ms[k] / (ms[k] + mstick);
+        rs[k].y = mk * rk.y;
+        rs[k].z = mk * rk.z;
+      }
+  }
+}
+
+// One face group per thread (World.h:1462-1531): members approaching the face
+// (normal relative velocity <= 0) and the face reach one normal velocity;
+// tangential forces from the stick/slide iteration; the face's vertices end
+// with the face's common velocity.  Inputs P = rhs + obstacle reactions,
+// masses diag(Hs).
+__global__ void k_self_exchange(ContactDev c) {
+  if (c.state[CS_MODE] != 1 || c.state[CS_ACTIVE] == 0 || c.state[CS_NGRP] == 0) return;
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= c.ncf) return;
+  const int cnt = min(c.g_cnt[f], kMaxGroupMembers);
+  if (cnt == 0) return;
+  Vec3<double> B[3];
+  contact_basis(ld3(c.g_n, f), B);
+  Vec3<double> P[3];
+  double mf[3];
+  for (int i = 0; i < 3; ++i) {
+    const int a = c.cfaces[3 * f + i];
+    P[i] = ld3(c.rhs_pre, a) + ld3(c.cnext, a);
+    mf[i] = c.hdiag[c.cverts[a]];
+  }
+  const int* mem = c.g_mem + c.g_ptr[f];
+  const double m0 = mf[0] + mf[1] + mf[2];
+  const Vec3<double> f0 = to_local3(B, (P[0] + P[1]) + P[2]);
+  int inc[kMaxGroupMembers];
+  double ms[kMaxGroupMembers];
+  Vec3<double> fs[kMaxGroupMembers], rs[kMaxGroupMembers];
+  unsigned char stick[kMaxGroupMembers];
+  int n = 0;
+  double sm = 0.0, smv = 0.0;
+  for (int k = 0; k < cnt; ++k) {
+    const int a = mem[k];
+    const Vec3<double> pk = ld3(c.rhs_pre, a) + ld3(c.cnext, a);
+    const double mk = c.hdiag[c.cverts[a]];
+    const Vec3<double> fl = to_local3(B, pk);
+    if (fl.x / mk - f0.x / m0 <= 0) {
+      inc[n] = k; ms[n] = mk; fs[n] = fl;
+      sm = sm + mk; smv = smv + fl.x;
+      ++n;
+    }
+  }
+  Vec3<double> r0 = mk3(0.0, 0.0, 0.0);
+  for (int k = 0; k < n; ++k) {
+    const double fn = (f0.x + smv) * ms[k] / (m0 + sm) - fs[k].x;
+    rs[k] = mk3(0.0 + fn, 0.0, 0.0);
+    r0.x = r0.x - fn;
+    stick[k] = 1;
+  }
+  for (int round = 0; round <= n; ++round) {  // each round unsticks at least one member
+    group_friction(f0, m0, r0, fs, ms, rs, stick, n, c.mu_self);
+    bool changed = false;
+    for (int k = 0; k < n; ++k)
+      if (stick[k] && rs[k].y * rs[k].y + rs[k].z * rs[k].z > c.mu_self * rs[k].x * rs[k].x) {
+        changed = true;
+        stick[k] = 0;
+      }
+    if (!changed) break;
+  }
+  const Vec3<double> v0 = div3(to_world3(B, f0) + to_world3(B, r0), m0);
+  for (int i = 0; i < 3; ++i) st3(c.g_outF, 3 * f + i, mf[i] * v0 - P[i]);
+  const int gp = c.g_ptr[f];
+  for (int k = 0; k < cnt; ++k) st3(c.g_outM, gp + k, mk3(0.0, 0.0, 0.0));
+  for (int k = 0; k < n; ++k) st3(c.g_outM, gp + inc[k], to_world3(B, rs[k]));
+}
+
+// Jacobi iteration with self contact on, part A (per vertex): rhs before
+// CollisionHandling; non-contact vertices finish here (relaxation, update);
+// contact vertices keep it and their obstacle reaction, seen with the
+// remembered self forces (forces + m_self_contact_forces[current]).
+__global__ void k_contact_rhs_pre(SceneDev d, ContactDev c, const double* __restrict__ slot, const double* xt,
+                                  const double* xk) {
+  if (c.state[CS_MODE] != 1 || c.state[CS_ACTIVE] == 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  Vec3<double> jd = ld3(d.attach_jd, i);
+  for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) jd = jd + ld3(slot, k);
+  Vec3<double> cdx = mk3(0.0, 0.0, 0.0);
+  for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) {
+    int j = d.hs_col[k];
+    if (j != i) cdx = cdx + d.hs_val[k] * (ld3(xk, j) - ld3(xt, j));
+  }
+  const Vec3<double> rhs = d.mass[i] * ld3(c.vwc, i) + d.h * (jd - ld3(c.lxt, i)) - d.h * cdx;
+  const int a = c.cidx[i];
+  if (a < 0) {
+    const bool first = c.state[CS_IT] == 0;
+    Vec3<double> prev = first ? rhs : ld3(c.prev, i);
+    prev = c.alpha * rhs + (1.0 - c.alpha) * prev;
+    st3(c.prev, i, prev);
+    st3(c.xn1, i, ld3(xt, i) + (1.0 / (d.h * c.hdiag[i])) * prev);
+    st3(c.xold, i, ld3(xk, i));
+    return;
+  }
+  st3(c.rhs_pre, a, rhs);
+  const Vec3<double> f = rhs + ld3(c.sc_cur, a);
+  Vec3<double> out = mk3(0.0, 0.0, 0.0);
+  int hit = 0;
+  const int cnt = c.imp_cnt[a];
+  for (int q = 0; q < cnt; ++q) {
+    Vec3<double> B[3];
+    contact_basis(ld3(c.imp_n, a * kMaxImpactsPerVertex + q), B);
+    double f0 = dot3(B[0], f), f1 = dot3(B[1], f), f2 = dot3(B[2], f);
+    if (f0 > 0) continue;  // take-off
+    double r0 = -f0, r1 = -f1, r2 = -f2;
+    double rt = sqrt(r1 * r1 + r2 * r2);
+    if (rt > c.mu * r0) { r1 *= c.mu * r0 / rt; r2 *= c.mu * r0 / rt; }
+    out = r0 * B[0] + r1 * B[1] + r2 * B[2];
+    hit = 1;
+  }
+  c.chit[a] = hit;
+  st3(c.cnext, a, out);
+}
+
+// Part C (per contact vertex): CollisionHandling's result and the update.
+//   no contact at all: rhs unchanged, remembered self forces unchanged;
+//   no self group: hit vertices rhs := B r, remembered self forces := 0;
+//   self groups: rhs += B r + self forces (face vertices of the groups, faces
+//   ascending, then the vertex's own member force), remembered := self forces.
+__global__ void k_contact_rhs_post(SceneDev d, ContactDev c, const double* xt, const double* xk) {
+  if (c.state[CS_MODE] != 1 || c.state[CS_ACTIVE] == 0) return;
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= c.nc) return;
+  const int i = c.cverts[a];
+  const Vec3<double> rhs = ld3(c.rhs_pre, a);
+  Vec3<double> post = rhs;
+  const int nobs = c.state[CS_NOBS], ngrp = c.state[CS_NGRP];
+  if (ngrp == 0) {
+    if (nobs > 0) {
+      if (c.chit[a]) post = ld3(c.cnext, a);
+      st3(c.sc_cur, a, mk3(0.0, 0.0, 0.0));
+    }
+  } else {
+    Vec3<double> sn = mk3(0.0, 0.0, 0.0);
+    for (int k = c.cvf_ptr[a]; k < c.cvf_ptr[a + 1]; ++k) {
+      const int f = c.cvf_face[k];
+      if (c.g_cnt[f] == 0) continue;
+      const int corner = c.cfaces[3 * f] == a ? 0 : (c.cfaces[3 * f + 1] == a ? 1 : 2);
+      sn = sn + ld3(c.g_outF, 3 * f + corner);
+    }
+    if (c.cf_face[a] >= 0) sn = sn + ld3(c.g_outM, c.m_slot[a]);
+    post = rhs + (ld3(c.cnext, a) + sn);
+    st3(c.sc_cur, a, sn);
+  }
+  const bool first = c.state[CS_IT] == 0;
+  Vec3<double> prev = first ? rhs : ld3(c.prev, i);
+  prev = c.alpha * post + (1.0 - c.alpha) * prev;
+  st3(c.prev, i, prev);
+  st3(c.xn1, i, ld3(xt, i) + (1.0 / (d.h * c.hdiag[i])) * prev);
+  st3(c.xold, i, ld3(xk, i));
 }
 
 // ---- adjoint of the contact phase ------------------------------------------------

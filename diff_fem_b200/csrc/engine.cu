@@ -159,6 +159,11 @@ struct dfem_scene {
   bool has_contact = false;
   DBuf<int> cverts, cidx, obs_f, imp_cnt, imp_face, cstate, cpasses;
   DBuf<double> obs_x, hdiag, imp_n, xn1, xold, cprev, lxt, vwc;
+  // soft-soft contact (forward only: the adjoint refuses these scenes)
+  bool self_contact = false;
+  DBuf<int> s_cfaces, s_cvf_ptr, s_cvf_face, s_on_face, s_simp_cnt, s_simp_face, s_cf_face, s_cf_slot, s_m_slot,
+      s_g_cnt, s_g_fill, s_g_ptr, s_g_mem, s_chit;
+  DBuf<double> s_simp_td, s_simp_n, s_g_n, s_g_outF, s_g_outM, s_sc_cur, s_rhs_pre, s_cnext;
   // adjoint of the contact phase: the record of one step's Jacobi iterations and the reverse sweep's buffers
   DBuf<int> crec_on, crec_first, crec_cnt;
   DBuf<double> crec_x, crec_prev, crec_n, ca_xn1b, ca_pb, ca_hdb, ca_cxtb, ca_vwcb, ca_yb, ca_orib;
@@ -689,7 +694,8 @@ static int upload_scene(dfem_scene* sc) {
   CK(cudaMemset(sc->act_cur.p, 0, sizeof(double) * std::max(1, s.nseg)));
   // obstacle contact phase
   const int nc = (int)s.cverts.size(), nof = (int)s.obs_f.size() / 3;
-  sc->has_contact = s.collide && nc > 0 && nof > 0;
+  sc->self_contact = s.self_collide;
+  sc->has_contact = s.collide && nc > 0 && (nof > 0 || sc->self_contact);
   if (sc->has_contact) {
     std::vector<int> cidx(s.N, -1);
     for (int a = 0; a < nc; ++a) cidx[s.cverts[a]] = a;
@@ -716,6 +722,32 @@ static int upload_scene(dfem_scene* sc) {
                         sc->obs_f.p, sc->hdiag.p, sc->imp_cnt.p, sc->imp_face.p, sc->imp_n.p, sc->xn1.p, sc->xold.p,
                         sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p, sc->crec_on.p, 0, nullptr, nullptr,
                         nullptr, nullptr, nullptr, sc->status.p, sc->crec_base.p, nullptr};
+    if (sc->self_contact) {
+      const int ncf = (int)s.cfaces.size() / 3;
+      CK(sc->s_cfaces.upload(s.cfaces));
+      CK(sc->s_cvf_ptr.upload(s.cvf_ptr));
+      CK(sc->s_cvf_face.upload(s.cvf_face));
+      CK(sc->s_on_face.upload(s.on_face));
+      CK(sc->s_simp_cnt.alloc(nc));
+      CK(sc->s_simp_face.alloc((size_t)nc * kMaxSelfImpacts));
+      CK(sc->s_simp_td.alloc((size_t)nc * kMaxSelfImpacts * 2));
+      CK(sc->s_simp_n.alloc((size_t)nc * kMaxSelfImpacts * 3));
+      CK(sc->s_cf_face.alloc(nc)); CK(sc->s_cf_slot.alloc(nc)); CK(sc->s_m_slot.alloc(nc));
+      CK(sc->s_g_cnt.alloc(ncf)); CK(sc->s_g_fill.alloc(ncf)); CK(sc->s_g_ptr.alloc((size_t)ncf + 1));
+      CK(sc->s_g_mem.alloc(nc)); CK(sc->s_chit.alloc(nc));
+      CK(sc->s_g_n.alloc(3 * (size_t)ncf)); CK(sc->s_g_outF.alloc(9 * (size_t)ncf)); CK(sc->s_g_outM.alloc(3 * (size_t)nc));
+      CK(sc->s_sc_cur.alloc(3 * (size_t)nc)); CK(sc->s_rhs_pre.alloc(3 * (size_t)nc)); CK(sc->s_cnext.alloc(3 * (size_t)nc));
+      CK(cudaMemset(sc->s_g_cnt.p, 0, sizeof(int) * ncf));
+      CK(cudaMemset(sc->s_sc_cur.p, 0, sizeof(double) * 3 * (size_t)nc));
+      ContactDev& c = sc->cd;
+      c.ncf = ncf; c.mu_self = s.mu_self;
+      c.cfaces = sc->s_cfaces.p; c.cvf_ptr = sc->s_cvf_ptr.p; c.cvf_face = sc->s_cvf_face.p; c.on_face = sc->s_on_face.p;
+      c.simp_cnt = sc->s_simp_cnt.p; c.simp_face = sc->s_simp_face.p; c.simp_td = sc->s_simp_td.p;
+      c.simp_n = sc->s_simp_n.p; c.cf_face = sc->s_cf_face.p; c.cf_slot = sc->s_cf_slot.p; c.m_slot = sc->s_m_slot.p;
+      c.g_cnt = sc->s_g_cnt.p; c.g_fill = sc->s_g_fill.p; c.g_ptr = sc->s_g_ptr.p; c.g_mem = sc->s_g_mem.p;
+      c.g_n = sc->s_g_n.p; c.g_outF = sc->s_g_outF.p; c.g_outM = sc->s_g_outM.p; c.sc_cur = sc->s_sc_cur.p;
+      c.rhs_pre = sc->s_rhs_pre.p; c.cnext = sc->s_cnext.p; c.chit = sc->s_chit.p;
+    }
   }
   refresh_scene_view(sc);
   return DFEM_OK;
@@ -958,13 +990,27 @@ static void contact_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHa
   const int nb = sc->nblk_v;
   const int ncons = s.T + s.M + s.S + s.B;
   k_contact_detect<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd, sc->xt.p, sc->xk.p, sc->status.p);
+  const int ncf = sc->cd.ncf;
+  if (sc->self_contact) {  // the pass's self groups
+    k_self_reset<<<(ncf + 127) / 128, 128, 0, st>>>(sc->cd);
+    k_self_closest<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd);
+    k_self_scan<<<1, 1024, 0, st>>>(sc->cd);
+    k_self_fill<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd);
+    k_self_sort<<<(ncf + 127) / 128, 128, 0, st>>>(sc->cd, sc->status.p);
+  }
   k_contact_ctl_detect<<<1, 1, 0, st>>>(sc->cd, h);
   k_contact_prep<<<nb, 128, 0, st>>>(s.N, sc->cd, sc->xk.p, sc->partial.p, sc->counter.p);
   Gate active;
   active.active = sc->cstate.p + CS_ACTIVE;
   if (ncons > 0)
     k_local<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, active, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p);
-  k_contact_rhs<<<nb, 128, 0, st>>>(sc->sd, sc->cd, sc->slot.p, sc->xt.p, sc->xk.p);
+  if (sc->self_contact) {
+    k_contact_rhs_pre<<<nb, 128, 0, st>>>(sc->sd, sc->cd, sc->slot.p, sc->xt.p, sc->xk.p);
+    k_self_exchange<<<(ncf + 127) / 128, 128, 0, st>>>(sc->cd);
+    k_contact_rhs_post<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->sd, sc->cd, sc->xt.p, sc->xk.p);
+  } else {
+    k_contact_rhs<<<nb, 128, 0, st>>>(sc->sd, sc->cd, sc->slot.p, sc->xt.p, sc->xk.p);
+  }
   k_contact_ctl_iter<<<1, 1, 0, st>>>(sc->cd, s.K);
 }
 
@@ -1576,11 +1622,13 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
     rec_budget = std::min<size_t>(rec_budget, INT32_MAX / 2);
     const int want = (int)std::min<size_t>(rec_budget, sc->crec_target > 0 ? (size_t)sc->crec_target
                                                                              : 4 * (size_t)n_steps);
-    fwd_rec = want >= 1;
+    fwd_rec = want >= 1 && !sc->self_contact;  // soft-soft contact has no adjoint to record for
     if (fwd_rec) RC(ensure_contact_record(sc, want));
     const int on = fwd_rec ? 2 : 0;
     CK(cudaMemcpyAsync(sc->crec_on.p, &on, sizeof(int), cudaMemcpyHostToDevice, sc->stream));
     CK(cudaMemsetAsync(sc->crec_base.p, 0, sizeof(int), sc->stream));
+    // each forward call starts with no remembered self forces
+    if (sc->self_contact) CK(cudaMemsetAsync(sc->s_sc_cur.p, 0, sizeof(double) * 3 * (size_t)sc->cd.nc, sc->stream));
     CK(cudaStreamSynchronize(sc->stream));  // `on` is a host local
   }
   CK(cudaGetLastError());
@@ -1636,6 +1684,8 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
                        double* g_youngs, double* g_poisson, double* g_act, int mem) {
   if (!sc || !gx_out || !gv_out || !gx || !gv) return fail(DFEM_ERR_INVALID, "null argument");
   if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_step_backward needs a preceding dfem_step_forward");
+  if (sc->self_contact)
+    return fail(DFEM_ERR_INVALID, "the adjoint of soft-soft (self) contact is not built; this scene runs forward only");
   CK(cudaSetDevice(sc->device));
   // contact steps the forward recorded need no replay; the others are replayed
   // with recording on, into records after the forward's (room for the most

@@ -157,7 +157,34 @@ struct ContactDev {
   int* status;
   int* rec_base;          // the current step's first record (computed iteration j of it is record base + j)
   int* rec_meta;          // forward recording, per step: [first record, computed iterations, source, recorded]
+  // soft-soft (self) contact; ncf == 0: off
+  int ncf;                // soft contact faces
+  double mu_self;         // "World Friction"
+  const int* cfaces;      // 3 per soft face: contact indices
+  const int* cvf_ptr;     // nc + 1: each contact vertex's soft faces (cvf_face, ascending)
+  const int* cvf_face;
+  const int* on_face;     // nc: 1 if the vertex lies on a soft face
+  int* simp_cnt;          // nc: the step's soft impacts per vertex (list order)
+  int* simp_face;         // nc * kMaxSelfImpacts
+  double* simp_td;        // nc * kMaxSelfImpacts * 2: time t, distance |d|
+  double* simp_n;         // nc * kMaxSelfImpacts * 3: normal
+  int* cf_face;           // nc: face of the vertex's closest impact this pass (-1: none)
+  int* cf_slot;           // nc: that impact's list slot
+  int* m_slot;            // nc: the vertex's position in g_mem
+  int* g_cnt;             // ncf: members of each face's group this pass
+  int* g_fill;            // ncf: fill cursor
+  int* g_ptr;             // ncf + 1: exclusive scan of g_cnt
+  int* g_mem;             // nc: members grouped by face, ascending within a group
+  double* g_n;            // 3 ncf: group normal (its first member's impact normal)
+  double* g_outF;         // 9 ncf: a group's self forces on its face's three vertices
+  double* g_outM;         // 3 nc: a member's self force (by its g_mem position)
+  double* sc_cur;         // 3 nc: self forces of the last CollisionHandling call that swapped buffers
+  double* rhs_pre;        // 3 nc: contact vertices' rhs before this iteration's CollisionHandling
+  double* cnext;          // 3 nc: obstacle reactions of this iteration (self contact on)
+  int* chit;              // nc: the vertex has an obstacle reaction this iteration
 };
+constexpr int kMaxSelfImpacts = 16;      // soft impacts per contact vertex in one step
+constexpr int kMaxGroupMembers = 64;     // members of one face group
 
 // One supernode of the triangular solves, stored in level order (position
 // lvl_ptr[l] .. lvl_ptr[l+1] of level l) so that one load gives a solve

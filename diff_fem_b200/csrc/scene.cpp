@@ -225,6 +225,36 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& s, std::string& err) 
   s.alpha = d.alpha;
   s.mu_obs = d.obstacle_friction;
   s.cverts.assign(d.contact_vertices, d.contact_vertices + d.n_contact_vertices);
+  // soft-soft contact (World::m_handle_self_collision, on only with collision
+  // handling): the soft faces, by contact index (indices survive the
+  // renumbering below, which maps the contact vertices in place)
+  s.mu_self = d.friction;
+  s.self_collide = s.collide && d.self_collision != 0 && d.n_contact_faces > 0 && !s.cverts.empty();
+  if (s.self_collide) {
+    REQ(d.contact_faces, "descriptor: contact_faces missing");
+    REQ(d.n_contact_faces < INT32_MAX / 9, "descriptor: too many contact faces");
+    const int nc = (int)s.cverts.size();
+    std::vector<int> cid(N, -1);
+    for (int a = 0; a < nc; ++a) {
+      REQ(cid[s.cverts[a]] < 0, "descriptor: contact vertex listed twice");
+      cid[s.cverts[a]] = a;
+    }
+    s.cfaces.resize(3 * (size_t)d.n_contact_faces);
+    s.on_face.assign(nc, 0);
+    s.cvf_ptr.assign(nc + 1, 0);
+    for (int64_t k = 0; k < 3LL * d.n_contact_faces; ++k) {
+      const int gv = d.contact_faces[k];
+      REQ(gv >= 0 && gv < N && cid[gv] >= 0, "descriptor: contact face vertex is not a contact vertex");
+      s.cfaces[k] = cid[gv];
+      s.on_face[cid[gv]] = 1;
+      s.cvf_ptr[cid[gv] + 1]++;
+    }
+    for (int a = 0; a < nc; ++a) s.cvf_ptr[a + 1] += s.cvf_ptr[a];
+    s.cvf_face.assign(s.cvf_ptr[nc], 0);
+    std::vector<int> fill(s.cvf_ptr.begin(), s.cvf_ptr.end() - 1);
+    for (int f = 0; f < d.n_contact_faces; ++f)  // faces ascending per vertex
+      for (int q = 0; q < 3; ++q) s.cvf_face[fill[s.cfaces[3 * f + q]]++] = f;
+  }
   REQ(d.n_drag_faces >= 0 && d.n_drag_faces < INT32_MAX / 3 && (d.n_drag_faces == 0 || d.drag_faces),
       "descriptor: drag_faces missing or too many");
   REQ(inrange(d.drag_faces, 3LL * d.n_drag_faces), "descriptor: drag face vertex out of range");
@@ -349,6 +379,7 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
             p.K == a.K && p.precision == a.precision && p.checkpoint_every == a.checkpoint_every,
         "batch: scenes must share time_step, damping, gravity, max_iterations, precision and checkpoint_every");
     REQ(!(p.collide && !p.cverts.empty() && !p.obs_f.empty()), "batch: obstacle contact is supported for single scenes only");
+    REQ(!p.self_collide, "batch: soft-soft contact is supported for single scenes only");
     REQ(p.nparts == 1, "batch: parts must be single scenes");
     totN += p.N; totT += p.T; totSlots += p.nslots; totRows += (int64_t)p.F.rowidx.size();
     totL += (int64_t)p.F.Lcm.size(); totD += (int64_t)p.F.Dinv.size(); totF += (int64_t)p.df.size() / 3;

@@ -50,6 +50,11 @@ struct HostScene {
   std::vector<int> cverts;
   std::vector<double> obs_x;
   std::vector<int> obs_f;
+  // soft-soft (self) contact: soft faces as contact indices (3 each), each
+  // contact vertex's soft faces ascending (CSR), and whether it lies on one
+  bool self_collide = false;
+  double mu_self = 1.0;
+  std::vector<int> cfaces, cvf_ptr, cvf_face, on_face;
 
   // underwater drag and lift: faces (3 internal ids each, outward winding)
   // and every vertex's faces in ascending face order (CSR)

@@ -581,6 +581,51 @@ def cloth_on_ball(nv: int = 64, edge: float = 0.02, radius: float = 0.2, drop: f
     )
 
 
+def cloth_on_block(nv: int = 4, edge: float = 0.014, block=(2, 1, 2), block_edge: float = 0.03, gap: float = 0.004,
+                   offset=(0.0031, -0.0047),
+                   v0: float = -0.6, stretch: float = 200.0, bend: float = 1e-3, density: float = 0.3,
+                   block_E: float = 5e4, mu_self: float = 0.3, mu_ground: float = 0.5, alpha: float = 0.5,
+                   precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Soft-soft contact case: an nv x nv cloth falling (initial velocity v0
+    m/s, `gap` m above) onto a soft tet block that rests on a ground quad.
+    Contact vertices are every cloth vertex and the block's surface
+    vertices; contact faces are the cloth's triangles and the block's surface
+    triangles; self-collision on (soft-soft friction mu_self = "World
+    Friction"), obstacle friction mu_ground.  The cloth is centred over the
+    block shifted by `offset` (x, z), so that no vertex lies over an edge of
+    the other surface's triangles.  Contact relaxation ("World Alpha")
+    `alpha`: a vertex shared by several hit faces receives every group's
+    correction, and unrelaxed Jacobi sweeps (alpha = 1) can diverge on the
+    larger blocks.  h = 1/120, 20 iterations."""
+    nx, ny, nz = block
+    bx0, btets = cube_grid(nx, ny, nz, block_edge)
+    bmass = lumped_masses(bx0, btets, 1000.0 * nx * ny * nz * block_edge ** 3, True)
+    bfaces, bverts = surface_of(bx0, btets)
+    top = ny * block_edge
+    side = (nv - 1) * edge
+    cx, cz = 0.5 * nx * block_edge, 0.5 * nz * block_edge
+    x0c, tris, springs, boff, bvert = cloth_grid(nv, nv, edge, origin=(cx - 0.5 * side + offset[0], top + gap,
+                                                                 cz - 0.5 * side + offset[1]))
+    mc = triangle_masses(x0c, tris, density)
+    nc = x0c.shape[0]
+    gx, gf = ground_quad(-1e-3, 1.0, center=(cx, cz))
+    T = btets.shape[0]
+    d = SceneDesc(
+        x0=np.concatenate([x0c, bx0]), mass=np.concatenate([mc, bmass]),
+        tets=btets + nc, youngs=np.full(T, block_E), poisson=np.full(T, 0.3),
+        spring_vertices=springs, spring_weight=np.full(len(springs), stretch),
+        bend_offsets=boff, bend_vertices=bvert, bend_weight=np.full(len(boff) - 1, bend),
+        contact_vertices=np.concatenate([np.arange(nc), bverts + nc]).astype(np.int32),
+        contact_faces=np.concatenate([tris, bfaces + nc]).astype(np.int32),
+        obstacle_x=gx, obstacle_faces=gf, handle_collision=True, self_collision=True,
+        friction=mu_self, obstacle_friction=mu_ground, alpha=alpha,
+        time_step=1.0 / 120.0, max_iterations=20, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name=f"cloth_{nv}x{nv}_on_block_{nx}x{ny}x{nz}",
+    )
+    d.initial_velocity = np.concatenate([np.tile([0.0, v0, 0.0], nc), np.zeros(3 * bx0.shape[0])])
+    return d
+
+
 # -------------------------------------------------------------------- cloth ---
 
 def cloth_grid(nv_x: int, nv_z: int, edge: float, origin=(0.0, 0.0, 0.0)):

@@ -44,6 +44,8 @@ def lib() -> C.CDLL:
         L.orc_lumped_masses.argtypes = [C.c_int, pd, C.c_int, pi, C.c_double, C.c_int, pd]
         L.orc_eval_local.argtypes = [vp, pd, pd, pd]
         L.orc_contact_passes.argtypes = [vp, pi, C.c_int]
+        L.orc_set_detection_replay.argtypes = [vp, C.c_int]
+        L.orc_self_group.argtypes = [pd, pd, pd, C.c_int, C.c_double, pd, pi]
         L.orc_vf_impact.argtypes = [pd, pd, pd, pd, pd, C.c_double, pd]
         L.orc_corot_project.argtypes = [pd, pd, pd]
         L.orc_corot_vjp.argtypes = [pd, pd, pd, pd]
@@ -132,6 +134,11 @@ class OracleScene:
         lib().orc_eval_local(self.h, _pd(x), _pd(a), _pd(out))
         return out
 
+    def detection_replay(self, mode: int):
+        """0: detect; 1: record each step's contact passes (impact normals,
+        self groups) on the next forward; 2: replay the recorded passes."""
+        lib().orc_set_detection_replay(self.h, int(mode))
+
     def contact_passes(self):
         out = np.zeros(max(1, self._steps), np.int32)
         lib().orc_contact_passes(self.h, _pi(out), self._steps)
@@ -191,3 +198,16 @@ def lumped_masses(x0, tets, total_mass, is_mass_same=True):
     m = np.zeros(n)
     lib().orc_lumped_masses(n, _pd(x0), tets.size // 4, _pi(tets), float(total_mass), int(is_mass_same), _pd(m))
     return m
+
+
+def self_group(normal, P, m, mu):
+    """One soft-contact face group's exchange: P = (3 + k, 3) forces of the
+    face's vertices then of the group's k vertices, m their masses.  Returns
+    (self forces (3 + k, 3), membership of the k group vertices)."""
+    P = np.ascontiguousarray(P, np.float64).reshape(-1, 3)
+    m = np.ascontiguousarray(m, np.float64)
+    k = P.shape[0] - 3
+    out = np.zeros_like(P)
+    inc = np.zeros(max(1, k), np.int32)
+    lib().orc_self_group(_pd(np.ascontiguousarray(normal, np.float64)), _pd(P), _pd(m), k, float(mu), _pd(out), _pi(inc))
+    return out, inc[:k].astype(bool)

@@ -46,6 +46,7 @@
 #include <queue>
 #include <string>
 #include <vector>
+#include <map>
 #include <array>
 #include <limits>
 #include <thread>
@@ -262,6 +263,10 @@ static double mean_value(V3 a, V3 b, V3 c) {
   return num / bend_sin(a, b, c);
 }
 
+/* SelfCollisionInfo: a face, its normal (the first member's impact normal) and
+ * the contact vertices whose closest impact is on it, ascending. */
+struct SelfGroup { int f; V3 n; std::vector<int> verts; };
+
 struct Scene {
   int N = 0;
   std::vector<double> x0, mass, gmask;
@@ -281,6 +286,21 @@ struct Scene {
   std::vector<V3> obs_x;
   std::vector<std::array<int, 3>> obs_f;
   int last_passes = 0;
+  /* soft-soft (self) contact: the self branch of CollisionHandling
+     (World.h:1446-1537), CollisionBrutal::getSelfCollisionsInfo
+     (collisionBrutal.h:645-700), arcsim soft impacts (collision.cpp:29-120) */
+  bool self_collide = false;
+  double mu_self = 1.0;                     /* World Friction */
+  std::vector<std::array<int, 3>> cfaces;   /* soft contact faces, contact-vertex ids */
+  std::vector<char> on_face;                /* contact vertex lies on a soft face */
+  std::vector<double> sc_cur;               /* self forces of the last swapping call, 3 per contact vertex */
+  /* detection replay for derivative tests: 1 records each step's passes
+     (impact normals per contact vertex, self groups), 2 replays them instead
+     of detecting, so that perturbed runs keep the detection's outputs, which
+     the adjoint treats as constants */
+  struct PassRecord { std::vector<std::vector<V3>> normals; std::vector<SelfGroup> groups; };
+  int freeze = 0, cur_step = 0;
+  std::vector<std::vector<PassRecord>> frz;
   /* underwater drag and lift (Dfobj::ComputeDragForces) */
   bool underwater = false;
   std::vector<std::array<int, 3>> drag_f;
@@ -298,6 +318,7 @@ struct Scene {
   std::vector<double> rec_act;             /* per step activations */
   std::vector<int> rec_iters;
   std::vector<int> rec_passes;             /* contact passes per step */
+  std::vector<double> rec_sc;              /* sc_cur at each step's start */
 };
 
 static void add_H(std::vector<std::vector<std::pair<int, double>>>& rows, int i, int j, double v) {
@@ -859,35 +880,359 @@ static void contact_basis(V3 normal, V3 B[3]) {
   B[0] = normalize(normal); B[1] = tg; B[2] = bt;
 }
 
+/* vertex (p0 -> p1) against a moving face (q*s -> q*e): arcsim's
+ * vf_collision_test + collision_test (collision.cpp:118-128, 211-274) with the
+ * swept boxes of the vertex and of the face dilated by thickness * mult.
+ * Returns the impact's time t, distance |d| and normal (the face's start
+ * normal, oriented against the vertex's approach, not unit length). */
+static bool vf_impact_moving(V3 p0, V3 p1, const V3 qs[3], const V3 qe[3], double mult, V3* n_out, double* t_out,
+                             double* d_out) {
+  const double thick = kThickness * mult;
+  const double pv[2][3] = {{p0.x, p0.y, p0.z}, {p1.x, p1.y, p1.z}};
+  for (int c = 0; c < 3; ++c) {
+    double lo = std::min(pv[0][c], pv[1][c]), hi = std::max(pv[0][c], pv[1][c]);
+    double flo = 1e300, fhi = -1e300;
+    for (int k = 0; k < 3; ++k) {
+      const double a = c == 0 ? qs[k].x : (c == 1 ? qs[k].y : qs[k].z);
+      const double b = c == 0 ? qe[k].x : (c == 1 ? qe[k].y : qe[k].z);
+      flo = std::min(flo, std::min(a, b));
+      fhi = std::max(fhi, std::max(a, b));
+    }
+    if (hi < flo - thick || lo > fhi + thick) return false;
+  }
+  V3 x0 = p0, v0 = p1 - p0;
+  V3 x1 = qs[0] - x0, x2 = qs[1] - x0, x3 = qs[2] - x0;
+  V3 v1 = (qe[0] - qs[0]) - v0, v2 = (qe[1] - qs[1]) - v0, v3 = (qe[2] - qs[2]) - v0;
+  double a0 = stp(x1, x2, x3);
+  double a1 = stp(v1, x2, x3) + stp(x1, v2, x3) + stp(x1, x2, v3);
+  double a2 = stp(x1, v2, v3) + stp(v1, x2, v3) + stp(v1, v2, x3);
+  double a3 = stp(v1, v2, v3);
+  double t[4];
+  int nsol = ccd_cubic(a3, a2, a1, a0, t);
+  t[nsol++] = 1;
+  for (int i = 0; i < nsol; ++i) {
+    if (t[i] < 0 || t[i] > 1) continue;
+    V3 xt = p0 + t[i] * v0;
+    V3 y0 = qs[0] + t[i] * (qe[0] - qs[0]), y1 = qs[1] + t[i] * (qe[1] - qs[1]), y2 = qs[2] + t[i] * (qe[2] - qs[2]);
+    V3 n{0, 0, 0};
+    double w[4] = {0, 0, 0, 0};
+    double d = signed_vf(xt, y0, y1, y2, &n, w);
+    bool inside = std::min(std::min(-w[1], -w[2]), -w[3]) >= -1e-6;
+    if (t[i] == 1) {
+      inside = inside || norm(xt - y0) < thick || norm(xt - y1) < thick || norm(xt - y2) < thick;
+      inside = inside || norm(xt - y0 - (dot(xt - y0, y1 - y0) / dot(y1 - y0, y1 - y0)) * (y1 - y0)) < thick;
+      inside = inside || norm(xt - y1 - (dot(xt - y1, y2 - y1) / dot(y2 - y1, y2 - y1)) * (y2 - y1)) < thick;
+      inside = inside || norm(xt - y2 - (dot(xt - y2, y0 - y2) / dot(y0 - y2, y0 - y2)) * (y0 - y2)) < thick;
+    }
+    V3 fn = cross(normalize(qs[1] - qs[0]), normalize(qs[2] - qs[0]));
+    if (dot(n, w[1] * v1 + w[2] * v2 + w[3] * v3) > 0) n = -1.0 * fn; else n = fn;
+    if (std::fabs(d) < thick && inside) {
+      *n_out = n; *t_out = t[i]; *d_out = std::fabs(d);
+      return true;
+    }
+  }
+  return false;
+}
+
+/* A soft impact of contact vertex a against soft face f (its node 4-tuple is
+ * (a, face)); the step's list keeps one per tuple, refreshed in place. */
+struct SelfImpact { int a, f; double t, d; V3 n; };
+
+/* getSelfCollisionsInfo (collisionBrutal.h:645-700): per vertex the impact of
+ * smallest t (ties at t = 1: smallest distance; earlier list entries win
+ * otherwise), then the vertices grouped by face in ascending vertex order. */
+static std::vector<SelfGroup> self_groups(const std::vector<SelfImpact>& simp) {
+  std::map<int, int> closest;
+  for (int i = 0; i < (int)simp.size(); ++i) {
+    auto it = closest.find(simp[i].a);
+    if (it == closest.end()) { closest[simp[i].a] = i; continue; }
+    const SelfImpact& old = simp[it->second];
+    if (simp[i].t < old.t) { it->second = i; continue; }
+    if (old.t == 1 && old.d > simp[i].d) it->second = i;
+  }
+  std::vector<SelfGroup> out;
+  for (auto& kv : closest) {
+    const SelfImpact& im = simp[kv.second];
+    int g = -1;
+    for (int q = 0; q < (int)out.size(); ++q) if (out[q].f == im.f) { g = q; break; }
+    if (g >= 0) out[g].verts.push_back(kv.first);
+    else out.push_back(SelfGroup{im.f, im.n, {kv.first}});
+  }
+  return out;
+}
+
+/* forward-mode dual number with one derivative per input of a face group */
+struct DN {
+  double v = 0;
+  std::vector<double> d;
+  DN(double a = 0.0) : v(a) {}
+};
+static inline double val(const DN& a) { return a.v; }
+static inline DN dn_combine(const DN& a, const DN& b, double v, double ca, double cb) {
+  DN r(v);
+  const size_t n = std::max(a.d.size(), b.d.size());
+  r.d.assign(n, 0.0);
+  for (size_t k = 0; k < a.d.size(); ++k) r.d[k] += ca * a.d[k];
+  for (size_t k = 0; k < b.d.size(); ++k) r.d[k] += cb * b.d[k];
+  return r;
+}
+static inline DN operator+(const DN& a, const DN& b) { return dn_combine(a, b, a.v + b.v, 1.0, 1.0); }
+static inline DN operator-(const DN& a, const DN& b) { return dn_combine(a, b, a.v - b.v, 1.0, -1.0); }
+static inline DN operator*(const DN& a, const DN& b) { return dn_combine(a, b, a.v * b.v, b.v, a.v); }
+static inline DN operator/(const DN& a, const DN& b) {
+  const double q = a.v / b.v;
+  return dn_combine(a, b, q, 1.0 / b.v, -q / b.v);
+}
+static inline DN dsqrt(const DN& a) {
+  DN r(std::sqrt(a.v));
+  r.d.assign(a.d.size(), 0.0);
+  for (size_t k = 0; k < a.d.size(); ++k) r.d[k] = a.d[k] / (2.0 * r.v);
+  return r;
+}
+
+/* local frame [n, t, b] and back (local_basis^T f, local_basis r) */
+template <typename T> static inline TV3<T> to_local(const V3 B[3], const TV3<T>& p) {
+  return {p.x * B[0].x + p.y * B[0].y + p.z * B[0].z, p.x * B[1].x + p.y * B[1].y + p.z * B[1].z,
+          p.x * B[2].x + p.y * B[2].y + p.z * B[2].z};
+}
+template <typename T> static inline TV3<T> to_world(const V3 B[3], const TV3<T>& r) {
+  return {r.x * B[0].x + r.y * B[1].x + r.z * B[2].x, r.x * B[0].y + r.y * B[1].y + r.z * B[2].y,
+          r.x * B[0].z + r.y * B[1].z + r.z * B[2].z};
+}
+template <typename T> static inline TV3<T> tdiv(const TV3<T>& a, const T& s) { return {a.x / s, a.y / s, a.z / s}; }
+
+/* World::do_solve_friction (World.h:1246-1315): the sticking set (face +
+ * sticking vertices) moves tangentially together; sliding vertices receive
+ * mu times their normal force against their tangential slip, and the sticking
+ * set the opposite sum. */
+template <typename T>
+static void solve_group_friction(const TV3<T>& p0, const T& m0, TV3<T>& r0, const std::vector<TV3<T>>& ps,
+                                 const std::vector<T>& ms, std::vector<TV3<T>>& rs, const std::vector<char>& stick,
+                                 double mu) {
+  TV3<T> pstick = p0;
+  T mstick = m0;
+  const int n = (int)stick.size();
+  for (int k = 0; k < n; ++k)
+    if (stick[k]) { pstick = tadd(pstick, ps[k]); mstick = mstick + ms[k]; }
+  TV3<T> pslide{T(0.0), T(0.0), T(0.0)};
+  T mslide(0.0), fn(0.0);
+  for (int k = 0; k < n; ++k)
+    if (!stick[k]) { pslide = tadd(pslide, ps[k]); mslide = mslide + ms[k]; fn = fn + rs[k].x; }
+  const TV3<T> v = tdiv(pstick, mstick);
+  r0.y = v.y * m0 - p0.y;
+  r0.z = v.z * m0 - p0.z;
+  for (int k = 0; k < n; ++k)
+    if (stick[k]) { rs[k].y = v.y * ms[k] - ps[k].y; rs[k].z = v.z * ms[k] - ps[k].z; }
+  if (val(mslide) > 0) {
+    TV3<T> rel = tsub(tdiv(pslide, mslide), tdiv(pstick, mstick));
+    const T tl = dsqrt(rel.y * rel.y + rel.z * rel.z);
+    rel = tdiv(rel, tl);
+    const T mult = T(mu) * fn / (mslide + mstick);
+    r0.y = r0.y + rel.y * mult * m0;
+    r0.z = r0.z + rel.z * mult * m0;
+    for (int k = 0; k < n; ++k)
+      if (stick[k]) { rs[k].y = rs[k].y + rel.y * mult * ms[k]; rs[k].z = rs[k].z + rel.z * mult * ms[k]; }
+    const TV3<T> abs_v0 = tdiv(tadd(p0, r0), m0);
+    for (int k = 0; k < n; ++k)
+      if (!stick[k]) {
+        TV3<T> rk = tsub(tdiv(ps[k], ms[k]), abs_v0);
+        const T tk = dsqrt(rk.y * rk.y + rk.z * rk.z);
+        rk = tdiv(rk, tk);
+        const T mk = T(-mu) * rs[k].x * ms[k] / (ms[k] + mstick);
+        rs[k].y = mk * rk.y;
+        rs[k].z = mk * rk.z;
+      }
+  }
+}
+
+/* One face group of the self branch of CollisionHandling (World.h:1462-1531).
+ * P = forces + obstacle reactions of the face's vertices (P[0..2]) and of the
+ * group's vertices (PL), masses = diag(Hs) (World::getVertexMass).  The group
+ * vertices approaching the face (normal relative velocity <= 0) and the face
+ * reach one normal velocity (the face's normal and tangential momenta are
+ * pooled); their tangential forces come from the stick/slide iteration.  The
+ * face's vertices end with the face's common velocity: outF[i] = v0 m_i - P_i;
+ * a group vertex k receives outL[k] = B rs_k (zero if it left the group).
+ * incl (when non-null) receives the membership decisions. */
+template <typename T>
+static void self_group_exchange(const V3 B[3], const TV3<T> P[3], const T mf[3], const std::vector<TV3<T>>& PL,
+                                const std::vector<T>& mL, double mu, TV3<T> outF[3], std::vector<TV3<T>>& outL,
+                                std::vector<char>* incl_out) {
+  const T m0 = mf[0] + mf[1] + mf[2];
+  const TV3<T> f0 = to_local(B, tadd(tadd(P[0], P[1]), P[2]));
+  std::vector<int> inc;
+  for (int k = 0; k < (int)PL.size(); ++k) {
+    const TV3<T> f = to_local(B, PL[k]);
+    if (val(f.x / mL[k] - f0.x / m0) <= 0) inc.push_back(k);
+  }
+  if (incl_out) {
+    incl_out->assign(PL.size(), 0);
+    for (int k : inc) (*incl_out)[k] = 1;
+  }
+  std::vector<T> ms;
+  std::vector<TV3<T>> fs;
+  T sm(0.0), smv(0.0);
+  for (int k : inc) {
+    ms.push_back(mL[k]);
+    sm = sm + ms.back();
+    fs.push_back(to_local(B, PL[k]));
+    smv = smv + fs.back().x;
+  }
+  const int n = (int)inc.size();
+  TV3<T> r0{T(0.0), T(0.0), T(0.0)};
+  std::vector<TV3<T>> rs(n, TV3<T>{T(0.0), T(0.0), T(0.0)});
+  for (int k = 0; k < n; ++k) {
+    const T fn = (f0.x + smv) * ms[k] / (m0 + sm) - fs[k].x;
+    rs[k].x = rs[k].x + fn;
+    r0.x = r0.x - fn;
+  }
+  std::vector<char> stick(n, 1);
+  for (;;) {
+    solve_group_friction(f0, m0, r0, fs, ms, rs, stick, mu);
+    bool changed = false;
+    for (int k = 0; k < n; ++k)
+      if (stick[k] && val(rs[k].y * rs[k].y + rs[k].z * rs[k].z) > val(T(mu) * rs[k].x * rs[k].x)) {
+        changed = true;
+        stick[k] = 0;
+      }
+    if (!changed) break;
+  }
+  const TV3<T> v0 = tdiv(tadd(to_world(B, f0), to_world(B, r0)), m0);
+  for (int i = 0; i < 3; ++i) outF[i] = tsub(tscale(mf[i], v0), P[i]);
+  outL.assign(PL.size(), TV3<T>{T(0.0), T(0.0), T(0.0)});
+  for (int k = 0; k < n; ++k) outL[inc[k]] = to_world(B, rs[k]);
+}
+
 struct ObsImpact { int face; V3 n; };
 
 /* What the adjoint of the contact phase needs from one run of it: every
  * computed Jacobi iteration's input ori_x, its relaxed rhs (prev) after the
  * update, whether it started its pass (prev restarts from its own rhs), the
- * impact normals of every contact vertex at that iteration (list order), and
- * which computed iteration produced the phase's output (0: the PD result).
- * The detection is discrete: impacts and normals are constants of the tape,
- * as they are on the reference's CppAD tape (collision detection runs in
- * plain double). */
+ * impact normals of every contact vertex at that iteration (list order), the
+ * mode of its CollisionHandling call, the pass's self-contact groups and the
+ * self-force state before the call, and which computed iteration produced the
+ * phase's output (0: the PD result).  The detection is discrete: impacts,
+ * normals, groups and the stick/slide and membership decisions are constants
+ * of the tape, as they are on the reference's CppAD tape (collision
+ * detection runs in plain double). */
 struct ContactTape {
   int out_src = 0;
   std::vector<std::vector<double>> ori, prev;
   std::vector<char> first;
   std::vector<std::vector<std::vector<V3>>> nrm;
   std::vector<double> hd;
+  std::vector<char> mode;
+  std::vector<int> gpass;
+  std::vector<std::vector<SelfGroup>> groups;
+  std::vector<std::vector<double>> sc_in;
 };
 
-/* Contact phase of ProjectiveDynamicsMethod (World.h:925-1023), obstacle
- * contacts only.  ori_x enters as the PD result and leaves as the returned
- * positions; x_n1 follows the reference's (x_n1, ori_x) bookkeeping exactly. */
+/* The winning obstacle reaction of one contact vertex: the last impact whose
+ * normal force is compressive (World.h:1364-1430: every later impact of the
+ * vertex overwrites the earlier ones). */
+struct ObsWin { bool hit = false; V3 B[3]; double r[3] = {0, 0, 0}; };
+static ObsWin obstacle_reaction(V3 f, const std::vector<V3>& normals, double mu) {
+  ObsWin w;
+  for (const V3& nv : normals) {
+    V3 B[3];
+    contact_basis(nv, B);
+    double fl[3] = {dot(B[0], f), dot(B[1], f), dot(B[2], f)};
+    if (fl[0] > 0) continue;
+    double rr[3] = {-fl[0], -fl[1], -fl[2]};
+    double rt = std::sqrt(rr[1] * rr[1] + rr[2] * rr[2]);
+    if (rt > mu * rr[0]) { rr[1] *= mu * rr[0] / rt; rr[2] *= mu * rr[0] / rt; }
+    w.hit = true;
+    w.B[0] = B[0]; w.B[1] = B[1]; w.B[2] = B[2];
+    w.r[0] = rr[0]; w.r[1] = rr[1]; w.r[2] = rr[2];
+  }
+  return w;
+}
+static inline V3 reaction_world(const ObsWin& w) { return w.r[0] * w.B[0] + w.r[1] * w.B[1] + w.r[2] * w.B[2]; }
+
+/* CollisionHandling (World.h:1317-1537) on the rhs of the contact vertices.
+ * sc is the self-force state (m_self_contact_forces[m_current_index]), read
+ * by the obstacle reactions and replaced by this call's self forces.  Returns
+ * the mode: 0 = no contact (nothing changes, no buffer swap); 1 = no self
+ * group (each obstacle-hit vertex's rhs := B r, the state becomes zero when
+ * self contact is on); 2 = with self groups (rhs += obstacle reactions + self
+ * forces of the groups, which see forces + obstacle reactions). */
+static int collision_handling(const Scene& S, double* rhs, const std::vector<std::vector<V3>>& normals,
+                              const std::vector<SelfGroup>& groups, const std::vector<double>& hd,
+                              std::vector<double>& sc) {
+  const int nc = (int)S.cverts.size();
+  int nb_obs = 0;
+  for (auto& l : normals) nb_obs += (int)l.size();
+  const int nb_self = S.self_collide ? (int)groups.size() : 0;
+  if (nb_obs == 0 && nb_self == 0) return 0;
+  const V3 zero{0, 0, 0};
+  std::vector<V3> forces(nc), cnext(nc, zero), snext(nc, zero);
+  for (int a = 0; a < nc; ++a) forces[a] = getx(rhs, S.cverts[a]);
+  for (int a = 0; a < nc; ++a) {
+    const int gv = S.cverts[a];
+    const V3 f = S.self_collide ? forces[a] + getx(sc.data(), a) : forces[a];
+    const ObsWin w = obstacle_reaction(f, normals[a], S.mu_obs);
+    if (!w.hit) continue;
+    const V3 out = reaction_world(w);
+    if (nb_self == 0) { rhs[3 * gv] = out.x; rhs[3 * gv + 1] = out.y; rhs[3 * gv + 2] = out.z; }
+    if (S.self_collide) cnext[a] = out;
+  }
+  if (nb_self > 0) {
+    for (const SelfGroup& g : groups) {
+      V3 B[3];
+      contact_basis(g.n, B);
+      TV3<double> P[3], oF[3];
+      double mf[3];
+      for (int i = 0; i < 3; ++i) {
+        const int a = S.cfaces[g.f][i];
+        const V3 q = forces[a] + cnext[a];
+        P[i] = {q.x, q.y, q.z};
+        mf[i] = hd[S.cverts[a]];
+      }
+      std::vector<TV3<double>> PL, oL;
+      std::vector<double> mL;
+      for (int a : g.verts) {
+        const V3 q = forces[a] + cnext[a];
+        PL.push_back({q.x, q.y, q.z});
+        mL.push_back(hd[S.cverts[a]]);
+      }
+      self_group_exchange(B, P, mf, PL, mL, S.mu_self, oF, oL, nullptr);
+      for (int i = 0; i < 3; ++i) {
+        V3& o = snext[S.cfaces[g.f][i]];
+        o = o + V3{oF[i].x, oF[i].y, oF[i].z};
+      }
+      for (size_t k = 0; k < g.verts.size(); ++k) {
+        V3& o = snext[g.verts[k]];
+        o = o + V3{oL[k].x, oL[k].y, oL[k].z};
+      }
+    }
+    for (int a = 0; a < nc; ++a) {
+      const int gv = S.cverts[a];
+      const V3 add = cnext[a] + snext[a];
+      rhs[3 * gv] += add.x; rhs[3 * gv + 1] += add.y; rhs[3 * gv + 2] += add.z;
+    }
+  }
+  if (S.self_collide)
+    for (int a = 0; a < nc; ++a) { sc[3 * a] = snext[a].x; sc[3 * a + 1] = snext[a].y; sc[3 * a + 2] = snext[a].z; }
+  return nb_self > 0 ? 2 : 1;
+}
+
+/* Contact phase of ProjectiveDynamicsMethod (World.h:925-1023) with obstacle
+ * and (when on) soft-soft contacts.  ori_x enters as the PD result and leaves
+ * as the returned positions; x_n1 follows the reference's (x_n1, ori_x)
+ * bookkeeping exactly.  A pass ends the phase when it finds no new obstacle
+ * impact and the number of self groups did not change
+ * (CollisionBrutal::BaseUpdateCollisions' return value). */
 static void contact_phase(Scene& S, const double* x_t, const double* vwc, const double* act, double* ori_x,
                           ContactTape* tape = nullptr) {
   const int N = S.N, n3 = 3 * N, nc = (int)S.cverts.size();
   S.last_passes = 0;
   if (tape) *tape = ContactTape();
-  if (!S.collide || nc == 0 || S.obs_f.empty()) return;
+  const bool soft = S.self_collide && !S.cfaces.empty();
+  if (!S.collide || nc == 0 || (S.obs_f.empty() && !soft)) return;
   int computed = 0, src_ori = 0;
   std::vector<std::vector<ObsImpact>> imp(nc);
+  std::vector<SelfImpact> simp;
+  std::vector<SelfGroup> groups;
   std::vector<double> xold(n3, 0.0), x_n1(ori_x, ori_x + n3), rhs(n3), prev(n3, 0.0), jd(n3), Lxt(n3), Hx(n3);
   /* L x_t = Hs x_t - M/h^2 x_t ; C = Hs - diag(Hs) */
   H_mul(S, x_t, Hx.data());
@@ -898,7 +1243,14 @@ static void contact_phase(Scene& S, const double* x_t, const double* vwc, const 
     for (int c = 0; c < 3; ++c) Lxt[3 * i + c] = Hx[3 * i + c] - S.mass[i] * ih2 * x_t[3 * i + c];
   }
   if (tape) tape->hd = hd;
+  if (S.freeze == 1 && (int)S.frz.size() <= S.cur_step) S.frz.resize(S.cur_step + 1);
   for (int pass = 0; pass < S.max_passes; ++pass) {
+    std::vector<std::vector<V3>> normals(nc);
+    if (S.freeze == 2) {
+      if (S.cur_step >= (int)S.frz.size() || pass >= (int)S.frz[S.cur_step].size()) break;
+      normals = S.frz[S.cur_step][pass].normals;
+      groups = S.frz[S.cur_step][pass].groups;
+    } else {
     /* detection at ori_x (vertex start positions: x_t) */
     bool any = false;
     for (int a = 0; a < nc; ++a) {
@@ -913,8 +1265,37 @@ static void contact_phase(Scene& S, const double* x_t, const double* vwc, const 
         if (!found) imp[a].push_back({f, n});
       }
     }
-    if (!any) break;
+    const int ngroups_prev = (int)groups.size();
+    if (soft) {
+      /* soft impacts (thickness x 2), vertex ascending then face ascending;
+         a tuple found again is refreshed in place, a new one appended */
+      for (int a = 0; a < nc; ++a) {
+        if (!S.on_face[a]) continue;
+        const int gv = S.cverts[a];
+        const V3 p0 = getx(x_t, gv), p1 = getx(ori_x, gv);
+        for (int f = 0; f < (int)S.cfaces.size(); ++f) {
+          const std::array<int, 3>& cf = S.cfaces[f];
+          if (cf[0] == a || cf[1] == a || cf[2] == a) continue;
+          V3 qs[3], qe[3];
+          for (int k = 0; k < 3; ++k) { qs[k] = getx(x_t, S.cverts[cf[k]]); qe[k] = getx(ori_x, S.cverts[cf[k]]); }
+          V3 n;
+          double t, d;
+          if (!vf_impact_moving(p0, p1, qs, qe, 2.0, &n, &t, &d)) continue;
+          bool found = false;
+          for (auto& r : simp)
+            if (r.a == a && r.f == f) { r.t = t; r.d = d; r.n = n; found = true; break; }
+          if (!found) simp.push_back(SelfImpact{a, f, t, d, n});
+        }
+      }
+      groups = self_groups(simp);
+    }
+    if (!any && ngroups_prev == (int)groups.size()) break;
+    for (int a = 0; a < nc; ++a)
+      for (auto& r : imp[a]) normals[a].push_back(r.n);
+    if (S.freeze == 1) S.frz[S.cur_step].push_back(Scene::PassRecord{normals, groups});
+    }
     S.last_passes = pass + 1;
+    if (tape) tape->groups.push_back(groups);
     for (int it = 0; it < S.K; ++it) {
       for (int k = 0; k < n3; ++k) ori_x[k] = x_n1[k];
       src_ori = computed;
@@ -933,23 +1314,8 @@ static void contact_phase(Scene& S, const double* x_t, const double* vwc, const 
           rhs[3 * i + c] = S.mass[i] * vwc[3 * i + c] + S.h * (jd[3 * i + c] - Lxt[3 * i + c]) - S.h * cdx[c];
       }
       if (it == 0) prev = rhs;
-      /* CollisionHandling, obstacle contacts, no self-collision: rhs of the
-         contact vertex := B r (overwritten; the last contact wins) */
-      for (int a = 0; a < nc; ++a) {
-        int gv = S.cverts[a];
-        V3 f = getx(rhs.data(), gv);
-        for (auto& r : imp[a]) {
-          V3 B[3];
-          contact_basis(r.n, B);
-          double fl[3] = {dot(B[0], f), dot(B[1], f), dot(B[2], f)};
-          if (fl[0] > 0) continue;
-          double rr[3] = {-fl[0], -fl[1], -fl[2]};
-          double rt = std::sqrt(rr[1] * rr[1] + rr[2] * rr[2]);
-          if (rt > S.mu_obs * rr[0]) { rr[1] *= S.mu_obs * rr[0] / rt; rr[2] *= S.mu_obs * rr[0] / rt; }
-          V3 out = rr[0] * B[0] + rr[1] * B[1] + rr[2] * B[2];
-          rhs[3 * gv] = out.x; rhs[3 * gv + 1] = out.y; rhs[3 * gv + 2] = out.z;
-        }
-      }
+      if (tape) tape->sc_in.push_back(S.sc_cur);
+      const int mode = collision_handling(S, rhs.data(), normals, groups, hd, S.sc_cur);
       for (int k = 0; k < n3; ++k) prev[k] = S.alpha * rhs[k] + (1.0 - S.alpha) * prev[k];
       for (int i = 0; i < N; ++i)
         for (int c = 0; c < 3; ++c) x_n1[3 * i + c] = x_t[3 * i + c] + prev[3 * i + c] / S.h / hd[i];
@@ -959,10 +1325,9 @@ static void contact_phase(Scene& S, const double* x_t, const double* vwc, const 
         tape->ori.emplace_back(ori_x, ori_x + n3);
         tape->prev.push_back(prev);
         tape->first.push_back(it == 0 ? 1 : 0);
-        std::vector<std::vector<V3>> nr(nc);
-        for (int a = 0; a < nc; ++a)
-          for (auto& r : imp[a]) nr[a].push_back(r.n);
-        tape->nrm.push_back(std::move(nr));
+        tape->nrm.push_back(normals);
+        tape->mode.push_back((char)mode);
+        tape->gpass.push_back((int)tape->groups.size() - 1);
       }
     }
   }
@@ -1103,19 +1468,139 @@ static void H_param_vjp(const Scene& S, const double* yb, const double* x, doubl
  * L x_t) - h C (ori - x_t), rhs_post its contact projection, prev_j =
  * alpha rhs_post + (1 - alpha) prev_{j-1} (prev_{j-1} := rhs_pre at the first
  * iteration of a pass) and x_n1 = x_t + prev_j / (h diag(Hs)). */
+/* Cotangent of f from the cotangent ob of the winning reaction
+ * out = B c(r), r = -B^T f, c the friction-cone clamp (r1, r2) -> mu r0 (r1, r2) / |(r1, r2)|. */
+static V3 reaction_vjp(const ObsWin& w, V3 f, V3 ob, double mu) {
+  const double r0 = -dot(w.B[0], f), r1 = -dot(w.B[1], f), r2 = -dot(w.B[2], f);
+  const double b0 = dot(w.B[0], ob), b1 = dot(w.B[1], ob), b2 = dot(w.B[2], ob);
+  const double rt = std::sqrt(r1 * r1 + r2 * r2);
+  double g0 = b0, g1 = b1, g2 = b2;
+  if (rt > mu * r0) {
+    g0 = b0 + mu * (r1 * b1 + r2 * b2) / rt;
+    g1 = mu * r0 * (r2 * r2 * b1 - r1 * r2 * b2) / (rt * rt * rt);
+    g2 = mu * r0 * (r1 * r1 * b2 - r1 * r2 * b1) / (rt * rt * rt);
+  }
+  return -1.0 * (g0 * w.B[0] + g1 * w.B[1] + g2 * w.B[2]);
+}
+
+/* VJP of collision_handling at one computed iteration (same inputs as the
+ * forward call): rb holds the cotangent of the rhs after the call and leaves
+ * with the cotangent before it (contact vertices; other entries pass through);
+ * scb likewise for the self-force state; hdb receives the cotangents of the
+ * masses diag(Hs). */
+static void collision_handling_vjp(const Scene& S, int mode, const double* rhs_pre,
+                                   const std::vector<std::vector<V3>>& normals, const std::vector<SelfGroup>& groups,
+                                   const std::vector<double>& sc_in, const std::vector<double>& hd, double* rb,
+                                   std::vector<double>& scb, double* hdb) {
+  if (mode == 0) return;
+  const int nc = (int)S.cverts.size();
+  const double mu = S.mu_obs;
+  const V3 zero{0, 0, 0};
+  std::vector<V3> forces(nc), cnext(nc, zero), Fb(nc, zero), Cb(nc, zero);
+  std::vector<ObsWin> win(nc);
+  std::vector<V3> fobs(nc);
+  std::vector<double> scb_in(3 * (size_t)nc, 0.0);
+  for (int a = 0; a < nc; ++a) {
+    forces[a] = getx(rhs_pre, S.cverts[a]);
+    fobs[a] = S.self_collide ? forces[a] + getx(sc_in.data(), a) : forces[a];
+    win[a] = obstacle_reaction(fobs[a], normals[a], mu);
+    if (win[a].hit && S.self_collide) cnext[a] = reaction_world(win[a]);
+  }
+  if (mode == 1) {
+    for (int a = 0; a < nc; ++a) {
+      if (!win[a].hit) continue;
+      const int gv = S.cverts[a];
+      const V3 fb = reaction_vjp(win[a], fobs[a], getx(rb, gv), mu);
+      rb[3 * gv] = fb.x; rb[3 * gv + 1] = fb.y; rb[3 * gv + 2] = fb.z;
+      if (S.self_collide) { scb_in[3 * a] = fb.x; scb_in[3 * a + 1] = fb.y; scb_in[3 * a + 2] = fb.z; }
+    }
+    if (S.self_collide) scb = scb_in;
+    return;
+  }
+  std::vector<V3> Sb(nc);
+  for (int a = 0; a < nc; ++a) {
+    const V3 r = getx(rb, S.cverts[a]);
+    Sb[a] = r + getx(scb.data(), a);
+    Cb[a] = r;
+    Fb[a] = r;
+  }
+  for (const SelfGroup& g : groups) {
+    V3 B[3];
+    contact_basis(g.n, B);
+    const int nv = (int)g.verts.size(), nin = 12 + 4 * nv;
+    auto seed = [&](double v, int idx) { DN d(v); d.d.assign(nin, 0.0); d.d[idx] = 1.0; return d; };
+    TV3<DN> P[3], oF[3];
+    DN mf[3];
+    for (int i = 0; i < 3; ++i) {
+      const int a = S.cfaces[g.f][i];
+      const V3 q = forces[a] + cnext[a];
+      P[i] = {seed(q.x, 3 * i), seed(q.y, 3 * i + 1), seed(q.z, 3 * i + 2)};
+      mf[i] = seed(hd[S.cverts[a]], 9 + i);
+    }
+    std::vector<TV3<DN>> PL, oL;
+    std::vector<DN> mL;
+    for (int k = 0; k < nv; ++k) {
+      const int a = g.verts[k];
+      const V3 q = forces[a] + cnext[a];
+      PL.push_back({seed(q.x, 12 + 3 * k), seed(q.y, 12 + 3 * k + 1), seed(q.z, 12 + 3 * k + 2)});
+      mL.push_back(seed(hd[S.cverts[a]], 12 + 3 * nv + k));
+    }
+    self_group_exchange(B, P, mf, PL, mL, S.mu_self, oF, oL, nullptr);
+    std::vector<double> gin(nin, 0.0);
+    auto acc = [&](const TV3<DN>& o, V3 cot) {
+      const DN* c[3] = {&o.x, &o.y, &o.z};
+      const double w[3] = {cot.x, cot.y, cot.z};
+      for (int q = 0; q < 3; ++q)
+        for (size_t k = 0; k < c[q]->d.size(); ++k) gin[k] += w[q] * c[q]->d[k];
+    };
+    for (int i = 0; i < 3; ++i) acc(oF[i], Sb[S.cfaces[g.f][i]]);
+    for (int k = 0; k < nv; ++k) acc(oL[k], Sb[g.verts[k]]);
+    for (int i = 0; i < 3; ++i) {
+      const int a = S.cfaces[g.f][i];
+      const V3 pb{gin[3 * i], gin[3 * i + 1], gin[3 * i + 2]};
+      Fb[a] = Fb[a] + pb;
+      Cb[a] = Cb[a] + pb;
+      hdb[S.cverts[a]] += gin[9 + i];
+    }
+    for (int k = 0; k < nv; ++k) {
+      const int a = g.verts[k];
+      const V3 pb{gin[12 + 3 * k], gin[12 + 3 * k + 1], gin[12 + 3 * k + 2]};
+      Fb[a] = Fb[a] + pb;
+      Cb[a] = Cb[a] + pb;
+      hdb[S.cverts[a]] += gin[12 + 3 * nv + k];
+    }
+  }
+  for (int a = 0; a < nc; ++a) {
+    if (win[a].hit) {
+      const V3 fb = reaction_vjp(win[a], fobs[a], Cb[a], mu);
+      Fb[a] = Fb[a] + fb;
+      scb_in[3 * a] = fb.x; scb_in[3 * a + 1] = fb.y; scb_in[3 * a + 2] = fb.z;
+    }
+    const int gv = S.cverts[a];
+    rb[3 * gv] = Fb[a].x; rb[3 * gv + 1] = Fb[a].y; rb[3 * gv + 2] = Fb[a].z;
+  }
+  scb = scb_in;
+}
+
+/* Adjoint of contact_phase.  xb: cotangent of the phase's output (in) and of
+ * its input, the PD result (out); scb: cotangent of the self-force state at
+ * the phase's end (in) and at its start (out).  Runs over every computed
+ * iteration: one after the output's source still feeds the state. */
 static void contact_adjoint(const Scene& S, const double* x_t, const double* vwc, const double* act,
                             const ContactTape& tp, double* xb, double* xtb, double* vwcb, double* gE, double* gnu,
-                            double* gact) {
-  const int N = S.N, n3 = 3 * N, nc = (int)S.cverts.size();
-  if (tp.out_src == 0) return;
-  const double h = S.h, ih2 = 1.0 / (h * h), mu = S.mu_obs, al = S.alpha;
-  std::vector<double> xn1b(xb, xb + n3), pb(n3, 0.0), hdb(N, 0.0), rpb(n3), yb(n3), orib(n3), rhs(n3), jd(n3), Lxt(n3), Hx(n3);
+                            double* gact, std::vector<double>& scb) {
+  const int N = S.N, n3 = 3 * N;
+  const int total = (int)tp.ori.size();
+  if (total == 0) return;
+  const double h = S.h, ih2 = 1.0 / (h * h), al = S.alpha;
+  std::vector<double> xout(xb, xb + n3), xn1b(n3, 0.0), pb(n3, 0.0), hdb(N, 0.0), rpb(n3), yb(n3), orib(n3),
+      rhs(n3), jd(n3), Lxt(n3), Hx(n3);
   H_mul(S, x_t, Hx.data());
   for (int i = 0; i < N; ++i)
     for (int c = 0; c < 3; ++c) Lxt[3 * i + c] = Hx[3 * i + c] - S.mass[i] * ih2 * x_t[3 * i + c];
-  std::vector<int> cidx(N, -1);
-  for (int a = 0; a < nc; ++a) cidx[S.cverts[a]] = a;
-  for (int j = tp.out_src; j >= 1; --j) {
+  for (int j = total; j >= 1; --j) {
+    if (j == tp.out_src)
+      for (int k = 0; k < n3; ++k) xn1b[k] += xout[k];
     const std::vector<double>& ori = tp.ori[j - 1];
     const std::vector<double>& prev = tp.prev[j - 1];
     /* x_n1 = x_t + prev / (h hd) */
@@ -1139,34 +1624,10 @@ static void contact_adjoint(const Scene& S, const double* x_t, const double* vwc
     }
     /* prev_j = al rhs_post + (1 - al) prev_{j-1} */
     for (int k = 0; k < n3; ++k) rpb[k] = al * pb[k];
-    /* contact projection of the contact vertices (the last non-skipped impact wins) */
-    for (int i = 0; i < N; ++i) {
-      const int a = cidx[i];
-      if (a < 0) continue;
-      V3 f = getx(rhs.data(), i), win[3];
-      bool hit = false;
-      double r0 = 0, r1 = 0, r2 = 0;
-      for (const V3& nv : tp.nrm[j - 1][a]) {
-        V3 B[3];
-        contact_basis(nv, B);
-        double f0 = dot(B[0], f);
-        if (f0 > 0) continue;
-        hit = true;
-        win[0] = B[0]; win[1] = B[1]; win[2] = B[2];
-        r0 = -f0; r1 = -dot(B[1], f); r2 = -dot(B[2], f);
-      }
-      if (!hit) continue;
-      V3 ob = getx(rpb.data(), i);
-      double b0 = dot(win[0], ob), b1 = dot(win[1], ob), b2 = dot(win[2], ob);  /* cotangents of r0, r1', r2' */
-      double rt = std::sqrt(r1 * r1 + r2 * r2), g0 = b0, g1 = b1, g2 = b2;
-      if (rt > mu * r0) {  /* r' = mu r0 (r1, r2) / rt */
-        g0 = b0 + mu * (r1 * b1 + r2 * b2) / rt;
-        g1 = mu * r0 * (r2 * r2 * b1 - r1 * r2 * b2) / (rt * rt * rt);
-        g2 = mu * r0 * (r1 * r1 * b2 - r1 * r2 * b1) / (rt * rt * rt);
-      }
-      V3 fb = -1.0 * (g0 * win[0] + g1 * win[1] + g2 * win[2]);
-      rpb[3 * i] = fb.x; rpb[3 * i + 1] = fb.y; rpb[3 * i + 2] = fb.z;
-    }
+    static const std::vector<SelfGroup> kNoGroups;
+    const int gp = tp.gpass[j - 1];
+    collision_handling_vjp(S, tp.mode[j - 1], rhs.data(), tp.nrm[j - 1], gp >= 0 ? tp.groups[gp] : kNoGroups,
+                           tp.sc_in[j - 1], tp.hd, rpb.data(), scb, hdb.data());
     if (tp.first[j - 1]) {
       for (int k = 0; k < n3; ++k) { rpb[k] += (1.0 - al) * pb[k]; pb[k] = 0.0; }
     } else {
@@ -1207,6 +1668,8 @@ static void contact_adjoint(const Scene& S, const double* x_t, const double* vwc
       }
     xn1b = orib;  /* ori_x of iteration j is x_n1 of iteration j - 1 */
   }
+  if (tp.out_src == 0)
+    for (int k = 0; k < n3; ++k) xn1b[k] += xout[k];
   /* diag(Hs) entries */
   if (gE)
     for (size_t t = 0; t < S.tets.size(); ++t) {
@@ -1295,6 +1758,25 @@ void* orc_create(const dfem_scene_desc* d) {
     S->obs_x.push_back(V3{d->obstacle_x[3 * k], d->obstacle_x[3 * k + 1], d->obstacle_x[3 * k + 2]});
   for (int k = 0; k < d->n_obstacle_faces; ++k)
     S->obs_f.push_back({d->obstacle_faces[3 * k], d->obstacle_faces[3 * k + 1], d->obstacle_faces[3 * k + 2]});
+  /* soft contact faces (global vertex ids) as contact-vertex ids */
+  S->self_collide = S->collide && d->self_collision != 0;
+  S->mu_self = d->friction;
+  {
+    std::vector<int> cid(N, -1);
+    for (int a = 0; a < (int)S->cverts.size(); ++a) cid[S->cverts[a]] = a;
+    S->on_face.assign(S->cverts.size(), 0);
+    for (int k = 0; S->self_collide && k < d->n_contact_faces; ++k) {
+      std::array<int, 3> f;
+      for (int q = 0; q < 3; ++q) {
+        const int gv = d->contact_faces[3 * k + q];
+        f[q] = (gv >= 0 && gv < N) ? cid[gv] : -1;
+        if (f[q] < 0) { S->err = "contact face vertex is not a contact vertex"; delete S; return nullptr; }
+      }
+      S->cfaces.push_back(f);
+      for (int q = 0; q < 3; ++q) S->on_face[f[q]] = 1;
+    }
+    S->sc_cur.assign(3 * S->cverts.size(), 0.0);
+  }
   S->underwater = d->underwater != 0;
   for (int k = 0; k < d->n_drag_faces; ++k)
     S->drag_f.push_back({d->drag_faces[3 * k], d->drag_faces[3 * k + 1], d->drag_faces[3 * k + 2]});
@@ -1333,9 +1815,16 @@ int orc_forward(void* s, const double* x, const double* v, const double* act, in
   S->rec_act.assign((size_t)n_steps * std::max(1, S->nseg), 0.0);
   S->rec_iters.assign(n_steps, 0);
   S->rec_passes.assign(n_steps, 0);
+  /* each forward call starts with no remembered self forces */
+  const size_t nsc = S->sc_cur.size();
+  std::fill(S->sc_cur.begin(), S->sc_cur.end(), 0.0);
+  S->rec_sc.assign((size_t)n_steps * nsc, 0.0);
+  if (S->freeze == 1) S->frz.assign(n_steps, {});
   std::vector<double> zero_act(std::max(1, S->nseg), 0.0);
   for (int st = 0; st < n_steps; ++st) {
     const double* a = act ? act + (size_t)st * S->nseg : zero_act.data();
+    std::copy(S->sc_cur.begin(), S->sc_cur.end(), S->rec_sc.begin() + (size_t)st * nsc);
+    S->cur_step = st;
     std::copy(xc.begin(), xc.end(), S->rec_x.begin() + (size_t)st * n3);
     std::copy(vc.begin(), vc.end(), S->rec_v.begin() + (size_t)st * n3);
     if (S->nseg > 0) std::copy(a, a + S->nseg, S->rec_act.begin() + (size_t)st * S->nseg);
@@ -1371,6 +1860,8 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
   if (gact) std::fill(gact, gact + (size_t)S->rec_steps * S->nseg, 0.0);
   std::vector<double> vwc(n3), qn(n3), xn(n3), hist, ybar(n3), xkb(n3), bb(n3), tmp(n3);
   double ih2 = 1.0 / (S->h * S->h);
+  const size_t nsc = S->sc_cur.size();
+  std::vector<double> scb(nsc, 0.0);  /* cotangent of the self-force state carried between steps */
   for (int st = S->rec_steps - 1; st >= 0; --st) {
     const double* x = &S->rec_x[(size_t)st * n3];
     const double* v = &S->rec_v[(size_t)st * n3];
@@ -1378,13 +1869,18 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
     step_prep(*S, x, v, vwc.data(), qn.data());
     int it = pd_solve(*S, x, qn.data(), a, &hist, xn.data(), 1);
     ContactTape tape;
+    std::copy(S->rec_sc.begin() + (size_t)st * nsc, S->rec_sc.begin() + (size_t)(st + 1) * nsc, S->sc_cur.begin());
+    S->cur_step = st;
+    const int freeze0 = S->freeze;
+    if (freeze0 == 1) S->freeze = 2;  /* re-runs replay what the forward recorded */
     contact_phase(*S, x, vwc.data(), a, xn.data(), &tape);
+    S->freeze = freeze0;
     /* v' = damping (x' - x)/h; x' = contact phase output (x^it without contacts) */
     double c = S->damping / S->h;
     std::vector<double> xtb(n3), vwcb(n3, 0.0);
     for (int k = 0; k < n3; ++k) { xkb[k] = xb[k] + c * vb[k]; xtb[k] = -c * vb[k]; }
     contact_adjoint(*S, x, vwc.data(), a, tape, xkb.data(), xtb.data(), vwcb.data(), gE, gnu,
-                    gact ? gact + (size_t)st * S->nseg : nullptr);
+                    gact ? gact + (size_t)st * S->nseg : nullptr, scb);
     std::fill(bb.begin(), bb.end(), 0.0);
     for (int k = it - 1; k >= 0; --k) {
       const double* xk = &hist[(size_t)k * n3];
@@ -1420,6 +1916,35 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
 /* J d(x) of all constraints (World::EvaluateDVector + mJ * d, World.h:898-901);
  * act = per-segment activations (may be NULL = all zero). */
 /* contact passes of each step of the last forward call */
+/* One face group's exchange (self_group_exchange) for tests: normal n (3),
+ * P = forces + reactions of the face's 3 vertices then of the n_list group
+ * vertices (3 each), masses m (3 + n_list); out receives the self forces of
+ * the same vertices (3 each), incl the membership of the group vertices. */
+int orc_self_group(const double* n, const double* P, const double* m, int n_list, double mu, double* out, int* incl) {
+  V3 B[3];
+  contact_basis(V3{n[0], n[1], n[2]}, B);
+  TV3<double> Pf[3], oF[3];
+  double mf[3];
+  for (int i = 0; i < 3; ++i) { Pf[i] = {P[3 * i], P[3 * i + 1], P[3 * i + 2]}; mf[i] = m[i]; }
+  std::vector<TV3<double>> PL, oL;
+  std::vector<double> mL;
+  for (int k = 0; k < n_list; ++k) {
+    PL.push_back({P[9 + 3 * k], P[9 + 3 * k + 1], P[9 + 3 * k + 2]});
+    mL.push_back(m[3 + k]);
+  }
+  std::vector<char> inc;
+  self_group_exchange(B, Pf, mf, PL, mL, mu, oF, oL, &inc);
+  for (int i = 0; i < 3; ++i) { out[3 * i] = oF[i].x; out[3 * i + 1] = oF[i].y; out[3 * i + 2] = oF[i].z; }
+  for (int k = 0; k < n_list; ++k) {
+    out[9 + 3 * k] = oL[k].x; out[9 + 3 * k + 1] = oL[k].y; out[9 + 3 * k + 2] = oL[k].z;
+    incl[k] = inc[k];
+  }
+  return 0;
+}
+
+/* detection replay mode for derivative tests (0 off, 1 record, 2 replay) */
+void orc_set_detection_replay(void* s, int mode) { static_cast<Scene*>(s)->freeze = mode; }
+
 int orc_contact_passes(void* s, int* out, int n) {
   Scene* S = static_cast<Scene*>(s);
   for (int k = 0; k < n && k < (int)S->rec_passes.size(); ++k) out[k] = S->rec_passes[k];

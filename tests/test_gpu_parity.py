@@ -127,6 +127,42 @@ def test_obstacle_contact_forward(mu):
     assert rel(tg, ro["traj"]) < POS_TOL
 
 
+@pytest.mark.parametrize("case", ["small", "wide"])
+def test_soft_contact_forward(case):
+    """Soft-soft contact (self-collision on): a cloth dropped onto a soft block
+    that rests on a ground quad.  Soft CCD both ways (cloth vertices on block
+    faces, block vertices on cloth faces), face groups with the stick/slide
+    exchange, the self forces remembered between iterations and steps, and
+    the block's obstacle contacts, against the oracle."""
+    if case == "small":
+        d, n = S.cloth_on_block(), 10
+    else:
+        d, n = S.cloth_on_block(nv=8, edge=0.0071, block=(3, 1, 3), block_edge=0.02), 8
+    x = d.x0.reshape(-1).copy()
+    v = d.initial_velocity.copy()
+    g = Scene(d)
+    o = O.OracleScene(d)
+    xg, vg, tg = g.forward(x, v, n_steps=n, traj=True)
+    ro = o.forward(x, v, n_steps=n, traj=True)
+    assert o.contact_passes().sum() > 0
+    assert np.array_equal(g.contact_passes(n), o.contact_passes())
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    assert rel(vg, ro["v"]) < POS_TOL
+    g.close()
+
+
+def test_soft_contact_adjoint_is_refused():
+    """The adjoint of soft-soft contact is not built: backward says so."""
+    d = S.cloth_on_block()
+    g = Scene(d)
+    x = d.x0.reshape(-1).copy()
+    g.forward(x, d.initial_velocity.copy(), n_steps=2)
+    with pytest.raises(_capi.DfemError, match="soft-soft"):
+        g.backward(np.ones_like(x), np.zeros_like(x))
+    g.close()
+
+
 @pytest.mark.parametrize("case", ["drop", "slide"])
 def test_obstacle_contact_adjoint(case):
     """Adjoint through the contact phase (Jacobi sweeps, friction cone,

@@ -298,3 +298,96 @@ def test_underwater_drag_forces_and_adjoint():
         assert np.array_equal(ip, it0) and np.array_equal(im, it0)
         fd = (lp - lm) / (2 * eps)
         assert abs(g[name] @ dz - fd) <= 1e-5 * max(1.0, abs(fd)), (name, g[name] @ dz, fd)
+
+
+def test_self_group_exchange_invariants():
+    """One soft-contact face group (World.h:1462-1531): the normal self
+    forces sum to zero; the face's vertices end with one common velocity;
+    every approaching group vertex ends with the face's normal velocity; a
+    receding one is left alone; with a large friction coefficient every
+    member sticks (common full velocity) and the full self forces sum to
+    zero.  (With sliding members the reference's friction does not balance:
+    the sticking set receives mu f_n along the mean slip, each sliding
+    vertex mu r_n m_k / (m_k + m_stick) along its own slip; its sanity
+    assert in do_solve_friction is compiled out.)"""
+    rng = np.random.default_rng(17)
+    for trial in range(20):
+        k = int(rng.integers(1, 6))
+        nrm = rng.standard_normal(3)
+        P = rng.standard_normal((3 + k, 3))
+        m = rng.uniform(0.5, 2.0, 3 + k)
+        mu = 1e9 if trial % 2 else 0.3
+        out, inc = O.self_group(nrm, P, m, mu)
+        scale = np.abs(P).max()
+        n = nrm / np.linalg.norm(nrm)
+        assert abs(out.sum(0) @ n) <= 1e-12 * scale * (3 + k)
+        if mu > 1e6:
+            assert np.abs(out.sum(0)).max() <= 1e-12 * scale * (3 + k)
+        vel = (P + out) / m[:, None]
+        assert np.allclose(vel[0], vel[1], atol=1e-12 * scale) and np.allclose(vel[0], vel[2], atol=1e-12 * scale)
+        face_vn = (P[:3].sum(0) @ n) / m[:3].sum()
+        for q in range(k):
+            rel = (P[3 + q] @ n) / m[3 + q] - face_vn
+            assert inc[q] == (rel <= 0)
+            if inc[q]:
+                assert abs(vel[3 + q] @ n - vel[0] @ n) <= 1e-10 * max(1.0, scale)
+                if mu > 1e6:
+                    assert np.allclose(vel[3 + q], vel[0], atol=1e-10 * max(1.0, scale))
+            else:
+                assert np.all(out[3 + q] == 0)
+
+
+def test_soft_contact_keeps_the_cloth_on_the_block():
+    """Self-collision on: a cloth dropped onto a soft block (both are soft
+    contact surfaces) stays above the block's top; with it off the cloth
+    falls through the block."""
+    d = S.cloth_on_block()
+    nc = 16
+    x = d.x0.reshape(-1).copy()
+    v = d.initial_velocity.copy()
+    o = O.OracleScene(d)
+    r = o.forward(x, v, n_steps=8, traj=True)
+    tr = r["traj"].reshape(8, -1, 3)
+    assert o.contact_passes().sum() > 0
+    for s in range(8):
+        assert tr[s, :nc, 1].min() > tr[s, nc:, 1].max()
+    off = O.OracleScene(dataclasses.replace(d, self_collision=False))
+    tr2 = off.forward(x, v, n_steps=8, traj=True)["traj"].reshape(8, -1, 3)
+    assert tr2[:, :nc, 1].min() < 0.02
+
+
+def test_soft_contact_adjoint_matches_central_differences():
+    """The soft-contact adjoint (face groups by forward-mode duals, the
+    self-force state carried between Jacobi iterations and steps) against
+    central differences.  The detection's outputs (normals from the faces'
+    start positions, groups) are constants of the tape, as on the
+    reference's tape, so the perturbed runs replay the recorded detection."""
+    d = S.cloth_on_block()
+    o = O.OracleScene(d)
+    n = 3
+    rng = np.random.default_rng(5)
+    x = d.x0.reshape(-1).copy()
+    v = d.initial_velocity.copy()
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    o.detection_replay(1)
+    _, it0 = _loss(o, x, v, gx, gv, n)
+    assert o.contact_passes().sum() >= n
+    g = o.backward(gx, gv)
+    o.detection_replay(2)
+    eps = 1e-7
+    E, nu = d.youngs.copy(), d.poisson.copy()
+    dE = rng.standard_normal(E.size) * E
+    o.set_materials(E + eps * dE, nu); lp, ip = _loss(o, x, v, gx, gv, n)
+    o.set_materials(E - eps * dE, nu); lm, im = _loss(o, x, v, gx, gv, n)
+    o.set_materials(E, nu)
+    checks = [(g["E"] @ dE, (lp - lm) / (2 * eps), ip, im)]
+    for name in ("x", "v"):
+        dz = rng.standard_normal(x.size)
+        if name == "x":
+            (lp, ip), (lm, im) = _loss(o, x + eps * dz, v, gx, gv, n), _loss(o, x - eps * dz, v, gx, gv, n)
+        else:
+            (lp, ip), (lm, im) = _loss(o, x, v + eps * dz, gx, gv, n), _loss(o, x, v - eps * dz, gx, gv, n)
+        checks.append((g[name] @ dz, (lp - lm) / (2 * eps), ip, im))
+    for adj, fd, ip, im in checks:
+        assert np.array_equal(ip, it0) and np.array_equal(im, it0)
+        assert abs(adj - fd) <= 1e-5 * max(1.0, abs(fd)), (adj, fd)
