@@ -665,6 +665,11 @@ __global__ void k_contact_rhs_pre(SceneDev d, ContactDev c, const double* __rest
   }
   const Vec3<double> rhs = d.mass[i] * ld3(c.vwc, i) + d.h * (jd - ld3(c.lxt, i)) - d.h * cdx;
   const int a = c.cidx[i];
+  const int rk = rec_index(c);
+  if (rk >= 0) {
+    st3(c.rec_x + (size_t)rk * 3 * d.N, i, ld3(xk, i));
+    if (i == 0) c.rec_first[rk] = c.state[CS_IT] == 0 ? 1 : 0;
+  }
   if (a < 0) {
     const bool first = c.state[CS_IT] == 0;
     Vec3<double> prev = first ? rhs : ld3(c.prev, i);
@@ -672,6 +677,7 @@ __global__ void k_contact_rhs_pre(SceneDev d, ContactDev c, const double* __rest
     st3(c.prev, i, prev);
     st3(c.xn1, i, ld3(xt, i) + (1.0 / (d.h * c.hdiag[i])) * prev);
     st3(c.xold, i, ld3(xk, i));
+    if (rk >= 0) st3(c.rec_prev + (size_t)rk * 3 * d.N, i, prev);
     return;
   }
   st3(c.rhs_pre, a, rhs);
@@ -730,6 +736,41 @@ __global__ void k_contact_rhs_post(SceneDev d, ContactDev c, const double* xt, c
   st3(c.prev, i, prev);
   st3(c.xn1, i, ld3(xt, i) + (1.0 / (d.h * c.hdiag[i])) * prev);
   st3(c.xold, i, ld3(xk, i));
+  const int rk = rec_index(c);
+  if (rk >= 0) st3(c.rec_prev + (size_t)rk * 3 * d.N, i, prev);
+}
+
+// Record of a computed iteration's soft-contact inputs for the adjoint (after
+// k_contact_rhs_pre, before k_contact_rhs_post replaces the remembered forces).
+__global__ void k_self_record(ContactDev c) {
+  if (c.state[CS_MODE] != 1 || c.state[CS_ACTIVE] == 0) return;
+  const int rk = rec_index(c);
+  if (rk < 0) return;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nc = c.nc, ncf = c.ncf;
+  int* si = c.rec_si + (size_t)rk * self_rec_si_stride(nc, ncf);
+  double* sd = c.rec_sd + (size_t)rk * self_rec_sd_stride(nc, ncf);
+  if (k < nc) {
+    si[k] = c.cf_face[k];
+    si[nc + k] = c.m_slot[k];
+    si[2 * nc + k] = c.g_mem[k];
+    st3(sd, k, ld3(c.sc_cur, k));
+  }
+  if (k < ncf) {
+    si[3 * nc + k] = c.g_cnt[k];
+    st3(sd + 3 * (size_t)nc, k, ld3(c.g_n, k));
+  }
+  if (k <= ncf) si[3 * nc + ncf + k] = c.g_ptr[k];
+  if (k == 0) {
+    si[3 * nc + 2 * ncf + 1] = c.state[CS_NOBS];
+    si[3 * nc + 2 * ncf + 2] = c.state[CS_NGRP];
+  }
+}
+
+// The remembered self forces at the start of the current step.
+__global__ void k_self_save(ContactDev c, const int* step) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < 3 * c.nc) c.sc_hist[(size_t)(*step) * 3 * c.nc + k] = c.sc_cur[k];
 }
 
 // ---- adjoint of the contact phase ------------------------------------------------
@@ -755,13 +796,53 @@ struct ContactAdj {
   double* vwcb;
   double* yb;
   double* orib;
+  // soft-soft contact: cotangent of the remembered self forces (3 nc, carried
+  // between iterations and steps), per contact vertex the relaxation total and
+  // the rhs_post cotangent, the groups' input cotangents by slot (P of the
+  // face's vertices 9 ncf, of the members 3 nc; masses 3 ncf, nc), and the
+  // cotangent of the phase's output until its source iteration (3N)
+  double* scb = nullptr;
+  double* ptot = nullptr;
+  double* sbp = nullptr;
+  double* gPF = nullptr;
+  double* gPM = nullptr;
+  double* gmF = nullptr;
+  double* gmM = nullptr;
+  double* xout = nullptr;
 };
 
-__global__ void k_cadj_start(int N, double cv, double* io_a, double* io_b, ContactAdj a) {
+// one recorded iteration's soft-contact inputs (views into rec_si / rec_sd)
+struct SelfRec {
+  const int* cf_face;
+  const int* m_slot;
+  const int* g_mem;
+  const int* g_cnt;
+  const int* g_ptr;
+  const int* nobs;
+  const int* ngrp;
+  const double* sc_in;
+  const double* g_n;
+};
+__host__ __device__ inline SelfRec self_rec_view(const ContactDev& c, size_t r) {
+  const int nc = c.nc, ncf = c.ncf;
+  const int* si = c.rec_si + r * self_rec_si_stride(nc, ncf);
+  const double* sd = c.rec_sd + r * self_rec_sd_stride(nc, ncf);
+  return SelfRec{si, si + nc, si + 2 * (size_t)nc, si + 3 * (size_t)nc, si + 3 * (size_t)nc + ncf,
+                 si + 3 * (size_t)nc + 2 * (size_t)ncf + 1, si + 3 * (size_t)nc + 2 * (size_t)ncf + 2, sd,
+                 sd + 3 * (size_t)nc};
+}
+
+__global__ void k_cadj_start(int N, double cv, double* io_a, double* io_b, ContactAdj a, int defer) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const Vec3<double> gv = ld3(io_b, i);
-  st3(a.xn1b, i, ld3(io_a, i) + cv * gv);  // v' = damping (x' - x_t)/h
+  const Vec3<double> xo = ld3(io_a, i) + cv * gv;  // v' = damping (x' - x_t)/h
+  if (defer) {  // soft contact: the output's cotangent enters at its source iteration
+    st3(a.xout, i, xo);
+    st3(a.xn1b, i, mk3(0.0, 0.0, 0.0));
+  } else {
+    st3(a.xn1b, i, xo);
+  }
   st3(a.cxtb, i, (-cv) * gv);
   st3(a.vwcb, i, mk3(0.0, 0.0, 0.0));
   st3(a.pb, i, mk3(0.0, 0.0, 0.0));
@@ -838,6 +919,344 @@ __global__ void __launch_bounds__(128) k_cadj_local(SceneDev d, ContactAdj a, co
 
 // orib = (sum of the slots) - C^T yb; x_t bar += (M/h^2 - Hs_ii) yb_i; the
 // result is the x_n1 bar of the previous computed iteration
+__global__ void k_cadj_add_xout(int N, ContactAdj a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) st3(a.xn1b, i, ld3(a.xn1b, i) + ld3(a.xout, i));
+}
+
+// winning obstacle reaction of contact vertex ac for force f (recorded normals)
+__device__ __forceinline__ bool obstacle_winner(const ContactDev& c, int ac, Vec3<double> f, const int* rcnt,
+                                                const double* rn, Vec3<double> W[3], double& r0, double& r1, double& r2) {
+  bool hit = false;
+  for (int q = 0; q < rcnt[ac]; ++q) {
+    Vec3<double> B[3];
+    contact_basis(ld3(rn, ac * kMaxImpactsPerVertex + q), B);
+    const double f0 = dot3(B[0], f);
+    if (f0 > 0) continue;
+    hit = true;
+    W[0] = B[0]; W[1] = B[1]; W[2] = B[2];
+    r0 = -f0; r1 = -dot3(B[1], f); r2 = -dot3(B[2], f);
+  }
+  return hit;
+}
+// cotangent of f from the cotangent ob of the reaction B c(-B^T f) (c: cone clamp)
+__device__ __forceinline__ Vec3<double> reaction_vjp(const Vec3<double> W[3], double r0, double r1, double r2,
+                                                     Vec3<double> ob, double mu) {
+  const double b0 = dot3(W[0], ob), b1 = dot3(W[1], ob), b2 = dot3(W[2], ob);
+  const double rt = sqrt(r1 * r1 + r2 * r2);
+  double g0 = b0, g1 = b1, g2 = b2;
+  if (rt > mu * r0) {
+    g0 = b0 + mu * (r1 * b1 + r2 * b2) / rt;
+    g1 = mu * r0 * (r2 * r2 * b1 - r1 * r2 * b2) / (rt * rt * rt);
+    g2 = mu * r0 * (r1 * r1 * b2 - r1 * r2 * b1) / (rt * rt * rt);
+  }
+  return (-1.0) * (g0 * W[0] + g1 * W[1] + g2 * W[2]);
+}
+
+// Soft-contact adjoint of one recorded iteration, part A (per vertex): the
+// relaxation's cotangents; non-contact vertices finish; contact vertices keep
+// rhs_pre, their obstacle reaction (with the recorded remembered forces), the
+// relaxation total and the cotangent of rhs_post for parts G and B.
+__global__ void k_cadj_self_a(SceneDev d, ContactDev c, ContactAdj a, SelfRec rv, const double* __restrict__ slot,
+                              const double* __restrict__ xt, const double* __restrict__ ori,
+                              const double* __restrict__ prev, int first, const int* __restrict__ rcnt,
+                              const double* __restrict__ rn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  const double hd = c.hdiag[i];
+  const Vec3<double> xb = ld3(a.xn1b, i), pv = ld3(prev, i);
+  st3(a.cxtb, i, ld3(a.cxtb, i) + xb);
+  a.hdb[i] -= dot3(xb, pv) / (d.h * hd * hd);
+  const Vec3<double> ptot = ld3(a.pb, i) + (1.0 / (d.h * hd)) * xb;
+  Vec3<double> rb = c.alpha * ptot;
+  const int ac = c.cidx[i];
+  if (ac < 0) {
+    if (first) {
+      rb = rb + (1.0 - c.alpha) * ptot;
+      st3(a.pb, i, mk3(0.0, 0.0, 0.0));
+    } else {
+      st3(a.pb, i, (1.0 - c.alpha) * ptot);
+    }
+    st3(a.vwcb, i, ld3(a.vwcb, i) + d.mass[i] * rb);
+    st3(a.yb, i, d.h * rb);
+    return;
+  }
+  Vec3<double> jd = ld3(d.attach_jd, i);
+  for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) jd = jd + ld3(slot, k);
+  Vec3<double> cdx = mk3(0.0, 0.0, 0.0);
+  for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) {
+    const int j = d.hs_col[k];
+    if (j != i) cdx = cdx + d.hs_val[k] * (ld3(ori, j) - ld3(xt, j));
+  }
+  const Vec3<double> f = d.mass[i] * ld3(c.vwc, i) + d.h * (jd - ld3(c.lxt, i)) - d.h * cdx;
+  st3(c.rhs_pre, ac, f);
+  Vec3<double> W[3];
+  double r0 = 0, r1 = 0, r2 = 0;
+  const bool hit = obstacle_winner(c, ac, f + ld3(rv.sc_in, ac), rcnt, rn, W, r0, r1, r2);
+  c.chit[ac] = hit ? 1 : 0;
+  if (hit) {
+    const double rt = sqrt(r1 * r1 + r2 * r2);
+    double q1 = r1, q2 = r2;
+    if (rt > c.mu * r0) { q1 *= c.mu * r0 / rt; q2 *= c.mu * r0 / rt; }
+    st3(c.cnext, ac, r0 * W[0] + q1 * W[1] + q2 * W[2]);
+  } else {
+    st3(c.cnext, ac, mk3(0.0, 0.0, 0.0));
+  }
+  st3(a.ptot, ac, ptot);
+  st3(a.sbp, ac, rb);
+}
+
+// Part G (one thread per face group, iterations with groups): the reverse of
+// k_self_exchange.  The tangential outputs depend only on the last
+// stick/slide round (each round recomputes them from the normal parts and the
+// stick set), so the forward is recomputed and that round reversed.  Writes
+// the cotangents of the inputs P and masses by slot.
+__global__ void k_cadj_self_group(ContactDev c, ContactAdj a, SelfRec rv) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= c.ncf || *rv.ngrp == 0) return;
+  const int cnt = min(rv.g_cnt[f], kMaxGroupMembers);
+  if (cnt == 0) return;
+  const double mu = c.mu_self;
+  Vec3<double> B[3];
+  contact_basis(ld3(rv.g_n, f), B);
+  int fa[3];
+  Vec3<double> P[3];
+  double mf[3];
+  for (int i = 0; i < 3; ++i) {
+    fa[i] = c.cfaces[3 * f + i];
+    P[i] = ld3(c.rhs_pre, fa[i]) + ld3(c.cnext, fa[i]);
+    mf[i] = c.hdiag[c.cverts[fa[i]]];
+  }
+  const int* mem = rv.g_mem + rv.g_ptr[f];
+  const double m0 = mf[0] + mf[1] + mf[2];
+  const Vec3<double> f0 = to_local3(B, (P[0] + P[1]) + P[2]);
+  int inc[kMaxGroupMembers];
+  double ms[kMaxGroupMembers];
+  Vec3<double> fs[kMaxGroupMembers], rs[kMaxGroupMembers];
+  unsigned char stick[kMaxGroupMembers];
+  int n = 0;
+  double sm = 0.0, smv = 0.0;
+  for (int k = 0; k < cnt; ++k) {
+    const int am = mem[k];
+    const Vec3<double> pk = ld3(c.rhs_pre, am) + ld3(c.cnext, am);
+    const double mk = c.hdiag[c.cverts[am]];
+    const Vec3<double> fl = to_local3(B, pk);
+    if (fl.x / mk - f0.x / m0 <= 0) {
+      inc[n] = k; ms[n] = mk; fs[n] = fl;
+      sm = sm + mk; smv = smv + fl.x;
+      ++n;
+    }
+  }
+  Vec3<double> r0 = mk3(0.0, 0.0, 0.0);
+  for (int k = 0; k < n; ++k) {
+    const double fn = (f0.x + smv) * ms[k] / (m0 + sm) - fs[k].x;
+    rs[k] = mk3(0.0 + fn, 0.0, 0.0);
+    r0.x = r0.x - fn;
+    stick[k] = 1;
+  }
+  for (int round = 0; round <= n; ++round) {
+    group_friction(f0, m0, r0, fs, ms, rs, stick, n, mu);
+    bool changed = false;
+    for (int k = 0; k < n; ++k)
+      if (stick[k] && rs[k].y * rs[k].y + rs[k].z * rs[k].z > mu * rs[k].x * rs[k].x) { changed = true; stick[k] = 0; }
+    if (!changed) break;
+  }
+  // the last round's intermediates (same operations as group_friction)
+  Vec3<double> pstick = f0, pslide = mk3(0.0, 0.0, 0.0);
+  double mstick = m0, mslide = 0.0;
+  for (int k = 0; k < n; ++k)
+    if (stick[k]) { pstick = pstick + fs[k]; mstick = mstick + ms[k]; }
+  for (int k = 0; k < n; ++k)
+    if (!stick[k]) { pslide = pslide + fs[k]; mslide = mslide + ms[k]; }
+  const Vec3<double> v = div3(pstick, mstick);
+  Vec3<double> rel = mk3(0.0, 0.0, 0.0), absv0 = mk3(0.0, 0.0, 0.0);
+  double tl = 1.0, mult = 0.0;
+  double tk[kMaxGroupMembers], mkk[kMaxGroupMembers];
+  Vec3<double> rk[kMaxGroupMembers];
+  if (mslide > 0) {
+    rel = div3(pslide, mslide) - div3(pstick, mstick);
+    tl = sqrt(rel.y * rel.y + rel.z * rel.z);
+    rel = div3(rel, tl);
+    double fnS = 0.0;
+    for (int k = 0; k < n; ++k)
+      if (!stick[k]) fnS = fnS + rs[k].x;
+    mult = mu * fnS / (mslide + mstick);
+    absv0 = div3(f0 + r0, m0);
+    for (int k = 0; k < n; ++k)
+      if (!stick[k]) {
+        rk[k] = div3(fs[k], ms[k]) - absv0;
+        tk[k] = sqrt(rk[k].y * rk[k].y + rk[k].z * rk[k].z);
+        rk[k] = div3(rk[k], tk[k]);
+        mkk[k] = -mu * rs[k].x * ms[k] / (ms[k] + mstick);
+      }
+  }
+  const Vec3<double> v0 = div3(to_world3(B, f0) + to_world3(B, r0), m0);
+  // reverse: outputs outF_i = mf_i v0 - P_i, outM_k = B rs_k
+  Vec3<double> Pb[3], v0b = mk3(0.0, 0.0, 0.0);
+  double mfb[3];
+  for (int i = 0; i < 3; ++i) {
+    const Vec3<double> G = ld3(a.sbp, fa[i]) + ld3(a.scb, fa[i]);
+    v0b = v0b + mf[i] * G;
+    mfb[i] = dot3(v0, G);
+    Pb[i] = (-1.0) * G;
+  }
+  Vec3<double> rsb[kMaxGroupMembers], fsb[kMaxGroupMembers];
+  double msb[kMaxGroupMembers];
+  for (int k = 0; k < n; ++k) {
+    const int am = mem[inc[k]];
+    rsb[k] = to_local3(B, ld3(a.sbp, am) + ld3(a.scb, am));
+    fsb[k] = mk3(0.0, 0.0, 0.0);
+    msb[k] = 0.0;
+  }
+  // v0 = (B f0 + B r0) / m0
+  const Vec3<double> ub = div3(v0b, m0);
+  double m0b = -dot3(v0b, v0) / m0;
+  Vec3<double> f0b = to_local3(B, ub), r0b = to_local3(B, ub);
+  double mstickb = 0.0, mslideb = 0.0, fnSb = 0.0;
+  Vec3<double> pstickb = mk3(0.0, 0.0, 0.0), pslideb = mk3(0.0, 0.0, 0.0);
+  if (mslide > 0) {
+    Vec3<double> absv0b = mk3(0.0, 0.0, 0.0);
+    for (int k = 0; k < n; ++k) {
+      if (stick[k]) continue;
+      const double mkb = rsb[k].y * rk[k].y + rsb[k].z * rk[k].z;
+      const double ry = mkk[k] * rsb[k].y, rz = mkk[k] * rsb[k].z;
+      rsb[k].y = 0.0; rsb[k].z = 0.0;
+      const double den = ms[k] + mstick;
+      rsb[k].x += mkb * (-mu) * ms[k] / den;
+      msb[k] += mkb * (-mu * rs[k].x) * mstick / (den * den);
+      mstickb += mkb * (mu * rs[k].x * ms[k]) / (den * den);
+      const double dp = rk[k].y * ry + rk[k].z * rz;
+      const double wy = (ry - rk[k].y * dp) / tk[k], wz = (rz - rk[k].z * dp) / tk[k];
+      fsb[k].y += wy / ms[k]; fsb[k].z += wz / ms[k];
+      msb[k] -= (fs[k].y * wy + fs[k].z * wz) / (ms[k] * ms[k]);
+      absv0b.y -= wy; absv0b.z -= wz;
+    }
+    f0b = f0b + (1.0 / m0) * absv0b;
+    r0b = r0b + (1.0 / m0) * absv0b;
+    m0b -= dot3(absv0b, absv0) / m0;
+    Vec3<double> relb = mk3(0.0, 0.0, 0.0);
+    double multb = 0.0;
+    for (int k = 0; k < n; ++k) {
+      if (!stick[k]) continue;
+      relb.y += rsb[k].y * mult * ms[k]; relb.z += rsb[k].z * mult * ms[k];
+      multb += (rsb[k].y * rel.y + rsb[k].z * rel.z) * ms[k];
+      msb[k] += (rsb[k].y * rel.y + rsb[k].z * rel.z) * mult;
+    }
+    relb.y += r0b.y * mult * m0; relb.z += r0b.z * mult * m0;
+    multb += (r0b.y * rel.y + r0b.z * rel.z) * m0;
+    m0b += (r0b.y * rel.y + r0b.z * rel.z) * mult;
+    const double dm = mslide + mstick;
+    fnSb += multb * mu / dm;
+    mslideb -= multb * mult / dm;
+    mstickb -= multb * mult / dm;
+    const double dr = rel.y * relb.y + rel.z * relb.z;
+    const double qy = (relb.y - rel.y * dr) / tl, qz = (relb.z - rel.z * dr) / tl;
+    pslideb.y += qy / mslide; pslideb.z += qz / mslide;
+    mslideb -= (pslide.y * qy + pslide.z * qz) / (mslide * mslide);
+    pstickb.y -= qy / mstick; pstickb.z -= qz / mstick;
+    mstickb += (pstick.y * qy + pstick.z * qz) / (mstick * mstick);
+  }
+  Vec3<double> vb = mk3(0.0, 0.0, 0.0);
+  for (int k = 0; k < n; ++k) {
+    if (!stick[k]) continue;
+    vb.y += rsb[k].y * ms[k]; vb.z += rsb[k].z * ms[k];
+    msb[k] += rsb[k].y * v.y + rsb[k].z * v.z;
+    fsb[k].y -= rsb[k].y; fsb[k].z -= rsb[k].z;
+    rsb[k].y = 0.0; rsb[k].z = 0.0;
+  }
+  vb.y += r0b.y * m0; vb.z += r0b.z * m0;
+  m0b += r0b.y * v.y + r0b.z * v.z;
+  f0b.y -= r0b.y; f0b.z -= r0b.z;
+  pstickb.y += vb.y / mstick; pstickb.z += vb.z / mstick;
+  mstickb -= (v.y * vb.y + v.z * vb.z) / mstick;
+  for (int k = 0; k < n; ++k) {
+    if (stick[k]) { fsb[k] = fsb[k] + pstickb; msb[k] += mstickb; }
+    else { fsb[k] = fsb[k] + pslideb; msb[k] += mslideb; rsb[k].x += fnSb; }
+  }
+  f0b = f0b + pstickb;
+  m0b += mstickb;
+  // normal parts: rs_k.x = fn_k, r0.x = -sum fn_k,
+  // fn_k = (f0.x + smv) ms_k / (m0 + sm) - fs_k.x
+  const double A = f0.x + smv, D = m0 + sm;
+  double smb = 0.0, smvb = 0.0;
+  for (int k = 0; k < n; ++k) {
+    const double fnb = rsb[k].x - r0b.x;
+    f0b.x += fnb * ms[k] / D;
+    smvb += fnb * ms[k] / D;
+    msb[k] += fnb * A / D;
+    m0b -= fnb * A * ms[k] / (D * D);
+    smb -= fnb * A * ms[k] / (D * D);
+    fsb[k].x -= fnb;
+  }
+  for (int k = 0; k < n; ++k) { msb[k] += smb; fsb[k].x += smvb; }
+  const Vec3<double> F0wb = to_world3(B, f0b);
+  for (int i = 0; i < 3; ++i) {
+    st3(a.gPF, 3 * f + i, Pb[i] + F0wb);
+    a.gmF[3 * f + i] = mfb[i] + m0b;
+  }
+  const int gp = rv.g_ptr[f];
+  for (int k = 0; k < cnt; ++k) { st3(a.gPM, gp + k, mk3(0.0, 0.0, 0.0)); a.gmM[gp + k] = 0.0; }
+  for (int k = 0; k < n; ++k) {
+    st3(a.gPM, gp + inc[k], to_world3(B, fsb[k]));
+    a.gmM[gp + inc[k]] = msb[k];
+  }
+}
+
+// Part B (per contact vertex): CollisionHandling's reverse by its outcome
+// (as k_contact_rhs_post), the reaction's VJP, the relaxation's remainder;
+// the remembered forces' cotangent before the call replaces the one after.
+__global__ void k_cadj_self_b(SceneDev d, ContactDev c, ContactAdj a, SelfRec rv, int first,
+                              const int* __restrict__ rcnt, const double* __restrict__ rn) {
+  const int ac = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ac >= c.nc) return;
+  const int i = c.cverts[ac];
+  const Vec3<double> post_b = ld3(a.sbp, ac), ptot = ld3(a.ptot, ac);
+  const int nobs = *rv.nobs, ngrp = *rv.ngrp;
+  Vec3<double> rb = post_b;
+  if (nobs > 0 || ngrp > 0) {
+    Vec3<double> W[3];
+    double r0 = 0, r1 = 0, r2 = 0;
+    const bool hit = obstacle_winner(c, ac, ld3(c.rhs_pre, ac) + ld3(rv.sc_in, ac), rcnt, rn, W, r0, r1, r2);
+    Vec3<double> scb_in = mk3(0.0, 0.0, 0.0);
+    if (ngrp == 0) {
+      if (hit) {
+        rb = reaction_vjp(W, r0, r1, r2, post_b, c.mu);
+        scb_in = rb;
+      }
+    } else {
+      Vec3<double> gsum = mk3(0.0, 0.0, 0.0);
+      double hsum = 0.0;
+      for (int k = c.cvf_ptr[ac]; k < c.cvf_ptr[ac + 1]; ++k) {
+        const int f = c.cvf_face[k];
+        if (rv.g_cnt[f] == 0) continue;
+        const int corner = c.cfaces[3 * f] == ac ? 0 : (c.cfaces[3 * f + 1] == ac ? 1 : 2);
+        gsum = gsum + ld3(a.gPF, 3 * f + corner);
+        hsum += a.gmF[3 * f + corner];
+      }
+      if (rv.cf_face[ac] >= 0) {
+        gsum = gsum + ld3(a.gPM, rv.m_slot[ac]);
+        hsum += a.gmM[rv.m_slot[ac]];
+      }
+      rb = post_b + gsum;
+      if (hit) {
+        const Vec3<double> fb = reaction_vjp(W, r0, r1, r2, post_b + gsum, c.mu);
+        rb = rb + fb;
+        scb_in = fb;
+      }
+      a.hdb[i] += hsum;
+    }
+    st3(a.scb, ac, scb_in);
+  }
+  if (first) {
+    rb = rb + (1.0 - c.alpha) * ptot;
+    st3(a.pb, i, mk3(0.0, 0.0, 0.0));
+  } else {
+    st3(a.pb, i, (1.0 - c.alpha) * ptot);
+  }
+  st3(a.vwcb, i, ld3(a.vwcb, i) + d.mass[i] * rb);
+  st3(a.yb, i, d.h * rb);
+}
+
 __global__ void k_cadj_hs(SceneDev d, ContactAdj a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.N) return;

@@ -164,6 +164,9 @@ struct dfem_scene {
   DBuf<int> s_cfaces, s_cvf_ptr, s_cvf_face, s_on_face, s_simp_cnt, s_simp_face, s_cf_face, s_cf_slot, s_m_slot,
       s_g_cnt, s_g_fill, s_g_ptr, s_g_mem, s_chit;
   DBuf<double> s_simp_td, s_simp_n, s_g_n, s_g_outF, s_g_outM, s_sc_cur, s_rhs_pre, s_cnext;
+  DBuf<int> crec_si;                      // soft-contact records (per computed iteration)
+  DBuf<double> crec_sd, s_sc_hist;        // ...; remembered self forces at each step's start
+  DBuf<double> ca_scb, ca_ptot, ca_sbp, ca_gPF, ca_gPM, ca_gmF, ca_gmM, ca_xout;  // its adjoint
   // adjoint of the contact phase: the record of one step's Jacobi iterations and the reverse sweep's buffers
   DBuf<int> crec_on, crec_first, crec_cnt;
   DBuf<double> crec_x, crec_prev, crec_n, ca_xn1b, ca_pb, ca_hdb, ca_cxtb, ca_vwcb, ca_yb, ca_orib;
@@ -780,6 +783,10 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
     CK(sc->crec_meta.alloc(4 * (size_t)cap));
     sc->cd.rec_meta = sc->crec_meta.p;
   }
+  if (sc->self_contact) {
+    CK(sc->s_sc_hist.alloc(3 * (size_t)sc->cd.nc * cap));
+    sc->cd.sc_hist = sc->s_sc_hist.p;
+  }
   sc->cap_steps = cap;
   invalidate_graphs(sc);  // graphs hold the old pointers
   return DFEM_OK;
@@ -970,6 +977,7 @@ static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
 }
 
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
+  if (sc->self_contact) k_self_save<<<(3 * sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd, sc->step.p);
   if (sc->nF > 0) k_drag_faces<<<(sc->nF + 127) / 128, 128, 0, st>>>(sc->nF, sc->df.p, sc->xt.p, sc->vt.p, sc->fdrag.p);
   k_step_begin<<<sc->nblk_p, kPartBlock, 0, st>>>(sc->sd, sc->pd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
                                    sc->hist.p, sc->hist_step, std::max(1, sc->hs.checkpoint_every), sc->ckpt_x.p,
@@ -1006,6 +1014,7 @@ static void contact_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHa
     k_local<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, active, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p);
   if (sc->self_contact) {
     k_contact_rhs_pre<<<nb, 128, 0, st>>>(sc->sd, sc->cd, sc->slot.p, sc->xt.p, sc->xk.p);
+    k_self_record<<<(std::max(sc->cd.nc, ncf + 1) + 127) / 128, 128, 0, st>>>(sc->cd);
     k_self_exchange<<<(ncf + 127) / 128, 128, 0, st>>>(sc->cd);
     k_contact_rhs_post<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->sd, sc->cd, sc->xt.p, sc->xk.p);
   } else {
@@ -1197,6 +1206,29 @@ static int ensure_contact_record(dfem_scene* sc, int cap, int keep = 0) {
   for (DBuf<double>* b : {&sc->ca_xn1b, &sc->ca_pb, &sc->ca_cxtb, &sc->ca_vwcb, &sc->ca_yb, &sc->ca_orib})
     if (!b->p) CK(b->alloc(n3));
   if (!sc->ca_hdb.p) CK(sc->ca_hdb.alloc(std::max(1, s.N)));
+  if (sc->self_contact) {
+    const int ncf = sc->cd.ncf;
+    const size_t si = self_rec_si_stride((int)nc, ncf), sd = self_rec_sd_stride((int)nc, ncf);
+    DBuf<int> rsi;
+    DBuf<double> rsd;
+    CK(rsi.alloc(si * cap));
+    CK(rsd.alloc(sd * cap));
+    if (keep > 0) {
+      CK(cudaMemcpyAsync(rsi.p, sc->crec_si.p, sizeof(int) * si * keep, cudaMemcpyDeviceToDevice, sc->stream));
+      CK(cudaMemcpyAsync(rsd.p, sc->crec_sd.p, sizeof(double) * sd * keep, cudaMemcpyDeviceToDevice, sc->stream));
+      CK(cudaStreamSynchronize(sc->stream));
+    }
+    sc->crec_si.swap(rsi);
+    sc->crec_sd.swap(rsd);
+    sc->cd.rec_si = sc->crec_si.p;
+    sc->cd.rec_sd = sc->crec_sd.p;
+    for (DBuf<double>* b : {&sc->ca_scb, &sc->ca_ptot, &sc->ca_sbp, &sc->ca_gPM})
+      if (!b->p) CK(b->alloc(3 * nc));
+    if (!sc->ca_gmM.p) CK(sc->ca_gmM.alloc(nc));
+    if (!sc->ca_gPF.p) CK(sc->ca_gPF.alloc(9 * (size_t)ncf));
+    if (!sc->ca_gmF.p) CK(sc->ca_gmF.alloc(3 * (size_t)ncf));
+    if (!sc->ca_xout.p) CK(sc->ca_xout.alloc(n3));
+  }
   sc->crec_cap = cap;
   sc->cd.rec_cap = cap;
   sc->cd.rec_x = sc->crec_x.p;
@@ -1211,7 +1243,19 @@ static int ensure_contact_record(dfem_scene* sc, int cap, int keep = 0) {
 // Device bytes of one record (one computed Jacobi iteration of the contact phase).
 static size_t contact_record_bytes(const dfem_scene* sc) {
   const size_t n3 = 3 * (size_t)sc->hs.N, nc = (size_t)sc->cd.nc;
-  return sizeof(double) * 2 * n3 + sizeof(int) * (1 + nc) + sizeof(double) * nc * kMaxImpactsPerVertex * 3;
+  size_t b = sizeof(double) * 2 * n3 + sizeof(int) * (1 + nc) + sizeof(double) * nc * kMaxImpactsPerVertex * 3;
+  if (sc->self_contact)
+    b += sizeof(int) * self_rec_si_stride((int)nc, sc->cd.ncf) + sizeof(double) * self_rec_sd_stride((int)nc, sc->cd.ncf);
+  return b;
+}
+
+static ContactAdj make_cadj(dfem_scene* sc) {
+  ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
+  if (sc->self_contact) {
+    a.scb = sc->ca_scb.p; a.ptot = sc->ca_ptot.p; a.sbp = sc->ca_sbp.p; a.gPF = sc->ca_gPF.p;
+    a.gPM = sc->ca_gPM.p; a.gmF = sc->ca_gmF.p; a.gmM = sc->ca_gmM.p; a.xout = sc->ca_xout.p;
+  }
+  return a;
 }
 
 // Reverse of step st's contact phase, from its record: the forward's (base,
@@ -1237,13 +1281,44 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
     src = meta[CS_SRC];
   }
   if (base + comp > sc->crec_cap) return fail(DFEM_ERR_CAP, "contact record too small for the recomputed step");
-  std::vector<int> first(std::max(1, src));
-  if (src > 0)
-    CK(cudaMemcpy(first.data(), sc->crec_first.p + base, src * sizeof(int), cudaMemcpyDeviceToHost));
-  const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
-  k_cadj_start<<<nb, 128, 0, sc->stream>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, a);
+  // soft contact: every computed iteration feeds the remembered self forces,
+  // so the sweep starts at the last one and the output enters at its source
+  const bool soft = sc->self_contact;
+  const int top = soft ? comp : src;
+  std::vector<int> first(std::max(1, top));
+  if (top > 0)
+    CK(cudaMemcpy(first.data(), sc->crec_first.p + base, top * sizeof(int), cudaMemcpyDeviceToHost));
+  const ContactAdj a = make_cadj(sc);
+  k_cadj_start<<<nb, 128, 0, sc->stream>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, a, soft ? 1 : 0);
   int launches = 1;
-  for (int j = src; j >= 1; --j) {
+  for (int j = top; j >= 1; --j) {
+    if (soft) {
+      if (j == src) {
+        k_cadj_add_xout<<<nb, 128, 0, sc->stream>>>(s.N, a);
+        ++launches;
+      }
+      const size_t r = (size_t)base + (j - 1);
+      const double* ori = sc->crec_x.p + r * n3;
+      const double* prev = sc->crec_prev.p + r * n3;
+      const int* rcnt = sc->crec_cnt.p + r * sc->cd.nc;
+      const double* rn = sc->crec_n.p + r * sc->cd.nc * kMaxImpactsPerVertex * 3;
+      const SelfRec rv = self_rec_view(sc->cd, r);
+      if (ncons > 0)
+        k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, kOpen, ori, sc->act_all.p, sc->step.p, sc->slot.p);
+      k_cadj_self_a<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->cd, a, rv, sc->slot.p, xt, ori, prev, first[j - 1], rcnt, rn);
+      k_cadj_self_group<<<(sc->cd.ncf + 127) / 128, 128, 0, sc->stream>>>(sc->cd, a, rv);
+      k_cadj_self_b<<<(sc->cd.nc + 127) / 128, 128, 0, sc->stream>>>(sc->sd, sc->cd, a, rv, first[j - 1], rcnt, rn);
+      if (ncons > 0)
+        k_cadj_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, ori, xt, sc->act_all.p, sc->step.p,
+                                                                  sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+      k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
+      if (s.nseg > 0)
+        k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, kOpen, sc->seg_part.p, sc->step.p,
+                                                                  sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
+      k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a);
+      launches += 6 + (ncons > 0 ? 2 : 0) + (s.nseg > 0 ? 1 : 0);
+      continue;
+    }
     const size_t r = (size_t)base + (j - 1);
     const double* ori = sc->crec_x.p + r * n3;
     const double* prev = sc->crec_prev.p + r * n3;
@@ -1261,6 +1336,10 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
                                                                 sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
     k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a);
     launches += 4 + (ncons > 0 ? 2 : 0) + (s.nseg > 0 ? 1 : 0);
+  }
+  if (soft && src == 0) {  // the output is the PD result itself
+    k_cadj_add_xout<<<nb, 128, 0, sc->stream>>>(s.N, a);
+    ++launches;
   }
   if (s.T > 0) k_cadj_hd<<<(s.T + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, sc->gE.p);
   k_cadj_to_pd<<<nb, 128, 0, sc->stream>>>(s.N, a, sc->io_a.p, sc->io_b.p);
@@ -1684,8 +1763,6 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
                        double* g_youngs, double* g_poisson, double* g_act, int mem) {
   if (!sc || !gx_out || !gv_out || !gx || !gv) return fail(DFEM_ERR_INVALID, "null argument");
   if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_step_backward needs a preceding dfem_step_forward");
-  if (sc->self_contact)
-    return fail(DFEM_ERR_INVALID, "the adjoint of soft-soft (self) contact is not built; this scene runs forward only");
   CK(cudaSetDevice(sc->device));
   // contact steps the forward recorded need no replay; the others are replayed
   // with recording on, into records after the forward's (room for the most
@@ -1701,6 +1778,8 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   }
   const int rbase = sc->crec_fwd ? sc->crec_used : 0;
   if (any_contact) RC(ensure_contact_record(sc, rbase + std::max(1, ccap), rbase));
+  if (sc->self_contact && sc->ca_scb.p)  // the final remembered self forces are not an output
+    CK(cudaMemsetAsync(sc->ca_scb.p, 0, sizeof(double) * 3 * (size_t)sc->cd.nc, sc->stream));
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N;
   const int nb = sc->nblk_v;
@@ -1740,6 +1819,9 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
       CK(cudaMemcpyAsync(sc->vt.p, sc->ckpt_v.p + (size_t)(seg0 / kc) * n3, n3 * sizeof(double),
                          cudaMemcpyDeviceToDevice, sc->stream));
       if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 0);
+      if (sc->self_contact)  // the segment's first step starts from its remembered self forces
+        CK(cudaMemcpyAsync(sc->s_sc_cur.p, sc->s_sc_hist.p + (size_t)seg0 * 3 * sc->cd.nc,
+                           sizeof(double) * 3 * (size_t)sc->cd.nc, cudaMemcpyDeviceToDevice, sc->stream));
       for (int q = seg0; q < seg_end; ++q) {
         CK(cudaMemcpyAsync(sc->seg_x.p + (size_t)(q - seg0) * n3, sc->xt.p, n3 * sizeof(double),
                            cudaMemcpyDeviceToDevice, sc->stream));
@@ -1761,6 +1843,9 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
         // a contact step also records its contact iterations for the contact adjoint
         CK(cudaMemcpyAsync(sc->xt.p, sx(st), n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
         CK(cudaMemcpyAsync(sc->vt.p, sv(st), n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+        if (sc->self_contact)
+          CK(cudaMemcpyAsync(sc->s_sc_cur.p, sc->s_sc_hist.p + (size_t)st * 3 * sc->cd.nc,
+                             sizeof(double) * 3 * (size_t)sc->cd.nc, cudaMemcpyDeviceToDevice, sc->stream));
         k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
         CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
         rerun[st] += 1;
@@ -1776,7 +1861,7 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
       if (contact_step) RC(contact_adjoint_step(sc, st, recorded[st] != 0, rbase, sx(st)));
       CK(cudaGraphLaunch(sc->g_adj.exec, sc->stream));
       if (contact_step) {
-        const ContactAdj a{sc->ca_xn1b.p, sc->ca_pb.p, sc->ca_hdb.p, sc->ca_cxtb.p, sc->ca_vwcb.p, sc->ca_yb.p, sc->ca_orib.p};
+        const ContactAdj a = make_cadj(sc);
         k_cadj_finish<<<nb, 128, 0, sc->stream>>>(s.N, a, sc->io_a.p, sc->io_b.p);
         sc->launches += 1;
       }

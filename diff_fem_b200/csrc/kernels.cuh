@@ -182,9 +182,18 @@ struct ContactDev {
   double* rhs_pre;        // 3 nc: contact vertices' rhs before this iteration's CollisionHandling
   double* cnext;          // 3 nc: obstacle reactions of this iteration (self contact on)
   int* chit;              // nc: the vertex has an obstacle reaction this iteration
+  // records of soft contact for the adjoint (per computed iteration, at the
+  // record index of rec_index): rec_si = [cf_face, m_slot, g_mem (nc each),
+  // g_cnt (ncf), g_ptr (ncf + 1), obstacle impacts, groups], rec_sd =
+  // [remembered self forces before the call (3 nc), g_n (3 ncf)]
+  int* rec_si;
+  double* rec_sd;
+  double* sc_hist;        // steps x 3 nc: the remembered self forces at each step's start
 };
+__host__ __device__ inline size_t self_rec_si_stride(int nc, int ncf) { return 3 * (size_t)nc + 2 * (size_t)ncf + 3; }
+__host__ __device__ inline size_t self_rec_sd_stride(int nc, int ncf) { return 3 * (size_t)nc + 3 * (size_t)ncf; }
 constexpr int kMaxSelfImpacts = 16;      // soft impacts per contact vertex in one step
-constexpr int kMaxGroupMembers = 64;     // members of one face group
+constexpr int kMaxGroupMembers = 32;     // members of one face group
 
 // One supernode of the triangular solves, stored in level order (position
 // lvl_ptr[l] .. lvl_ptr[l+1] of level l) so that one load gives a solve
