@@ -115,8 +115,8 @@ typedef struct dfem_scene_desc {
   int32_t handle_collision;       /* "Handle collision"                              */
   int32_t self_collision;         /* "Self-collision": soft-soft contact between the
                                      contact vertices and the contact faces (every
-                                     face vertex must be a contact vertex); forward
-                                     only: dfem_step_backward refuses such scenes */
+                                     face vertex must be a contact vertex; single
+                                     scenes, not batches)                          */
   double alpha;                   /* "World Alpha" relaxation of the contact rhs     */
   double friction;                /* "World Friction" (soft-soft contact mu)         */
   double obstacle_friction;       /* obstacle mu (diff_fem hardcodes 1)              */
