@@ -626,6 +626,52 @@ def cloth_on_block(nv: int = 4, edge: float = 0.014, block=(2, 1, 2), block_edge
     return d
 
 
+def soft_ball(radius: float, subdiv: int, center=(0.0, 0.0, 0.0), density: float = 1000.0):
+    """Tet-meshed ball: one tet from the centre to every face of an icosphere
+    (`subdiv` refinements: 20 * 4^subdiv tets).  Returns (vertices: surface
+    then centre, tets, surface faces (outward), surface vertex ids, masses)."""
+    X, F = icosphere(radius, subdiv, center)
+    c = len(X)
+    x0 = np.concatenate([X, np.asarray(center, np.float64)[None]])
+    tets = np.concatenate([np.full((len(F), 1), c, np.int32), F], axis=1).astype(np.int32)
+    mass = lumped_masses(x0, tets, density * 4.0 / 3.0 * np.pi * radius ** 3, True)
+    return x0, tets, F.astype(np.int32), np.arange(c, dtype=np.int32), mass
+
+
+def cloth_on_soft_ball(nv: int = 64, edge: float = 0.02, radius: float = 0.2, drop: float = 0.3, subdiv: int = 4,
+                       stretch: float = 1e3, bend: float = 1e-3, density: float = 0.2, ball_E: float = 5e4,
+                       mu: float = 0.3, alpha: float = 0.5, precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Cloth on a soft ball (soft-soft contact): the cloth of cloth_on_ball
+    (nv x nv, edge 0.02 m, membrane 1e3, bending 1e-3, 0.2 kg/m^2, gravity on)
+    centred `drop` m above a tet-meshed ball (radius 0.2 m, 20 * 4^subdiv
+    tets: 5,120 at subdiv 4; E = ball_E, nu 0.3, 1000 kg/m^3, gravity on)
+    that rests on a ground quad.  Self-collision on: the cloth's vertices and
+    triangles and the ball's surface are the soft contact surface ("World
+    Friction" mu); ground friction mu; relaxation alpha.  h = 1/120, 20
+    iterations."""
+    side = (nv - 1) * edge
+    # the cloth's corner offset off the ball's symmetry planes
+    xc, tris, springs, boff, bvert = cloth_grid(nv, nv, edge, origin=(-0.5 * side + 0.0013, radius + drop,
+                                                                   -0.5 * side - 0.0021))
+    mc = triangle_masses(xc, tris, density)
+    xb, btets, bfaces, bsurf, mb = soft_ball(radius, subdiv)
+    nc = xc.shape[0]
+    gx, gf = ground_quad(-radius - 1e-3, 2.0)
+    T = btets.shape[0]
+    return SceneDesc(
+        x0=np.concatenate([xc, xb]), mass=np.concatenate([mc, mb]),
+        tets=btets + nc, youngs=np.full(T, ball_E), poisson=np.full(T, 0.3),
+        spring_vertices=springs, spring_weight=np.full(len(springs), stretch),
+        bend_offsets=boff, bend_vertices=bvert, bend_weight=np.full(len(boff) - 1, bend),
+        contact_vertices=np.concatenate([np.arange(nc), bsurf + nc]).astype(np.int32),
+        contact_faces=np.concatenate([tris, bfaces + nc]).astype(np.int32),
+        obstacle_x=gx, obstacle_faces=gf, handle_collision=True, self_collision=True,
+        friction=mu, obstacle_friction=mu, alpha=alpha,
+        time_step=1.0 / 120.0, max_iterations=20, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name=f"cloth_{nv}x{nv}_on_soft_ball_{T}",
+    )
+
+
 # -------------------------------------------------------------------- cloth ---
 
 def cloth_grid(nv_x: int, nv_z: int, edge: float, origin=(0.0, 0.0, 0.0)):

@@ -3,7 +3,8 @@
  *
  * This is the drop-in boundary for the hot path of diff_fem: one time step of
  * local–global projective dynamics (corotated FEM tets, muscle segments,
- * attachments, cloth strain/bending springs, obstacle contact with friction)
+ * attachments, cloth strain/bending springs, obstacle and soft-soft contact
+ * with friction, underwater drag)
  * and the vector–Jacobian product (VJP) of that step.
  *
  * Conventions

@@ -154,7 +154,7 @@ def test_soft_contact_forward(case):
     g.close()
 
 
-@pytest.mark.parametrize("case,every", [("small", 1), ("small", 2), ("wide", 1)])
+@pytest.mark.parametrize("case,every", [("small", 1), ("small", 2), ("wide", 1), ("ball", 1)])
 def test_soft_contact_adjoint(case, every):
     """Adjoint of soft-soft contact (group exchange reversed per computed
     iteration, the remembered self forces' cotangent carried between
@@ -163,8 +163,11 @@ def test_soft_contact_adjoint(case, every):
     adjoint (forward-mode duals per group; pinned by central differences)."""
     if case == "small":
         d, n = S.cloth_on_block(), 4
-    else:
+    elif case == "wide":
         d, n = S.cloth_on_block(nv=8, edge=0.0071, block=(3, 1, 3), block_edge=0.02), 3
+    else:  # a cloth draping over a small soft ball on the ground
+        d, n = S.cloth_on_soft_ball(nv=12, edge=0.02, radius=0.08, drop=0.03, subdiv=2), 14
+        d.initial_velocity = np.zeros(3 * d.n_vertices)
     v = d.initial_velocity.copy()
     d = dataclasses.replace(d, checkpoint_every=every)
     x = d.x0.reshape(-1).copy()
