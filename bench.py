@@ -42,19 +42,17 @@ def parse():
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--sim-steps", type=int, default=None,
                    help="time steps per gradient evaluation (60 / 100 are the workloads; fewer only for profiler captures)")
-    p.add_argument("--workload", default="inverse_stiffness",
-                   choices=["inverse_stiffness", "batch", "star", "cloth_ball", "cloth_soft_ball"],
+    p.add_argument("--workload", default="inverse_stiffness", choices=["inverse_stiffness", "batch", "star", "cloth_ball"],
                    help="inverse_stiffness: one 12,800-tet scene; batch: 256 uneven scenes in one handle; "
                         "star: the muscle star on the ground, gradient w.r.t. all activations; "
-                        "cloth_ball: a 64x64 cloth dropped on a ball, gradient w.r.t. the initial velocities; "
-                        "cloth_soft_ball: the same cloth on a soft 5,120-tet ball (soft-soft contact)")
+                        "cloth_ball: a 64x64 cloth dropped on a ball, gradient w.r.t. the initial velocities")
     p.add_argument("--scenes", type=int, default=256, help="batch workload: number of scenes")
     p.add_argument("--fp64-sample", type=int, default=-1,
                    help="batch workload: scenes stepped one at a time in FP64 for the plain-form rate "
                         "(-1: every scene of the batch, 0: skip)")
     a = p.parse_args()
     global SIM_STEPS
-    SIM_STEPS = a.sim_steps if a.sim_steps is not None else {"batch": 100, "star": 200, "cloth_ball": 300, "cloth_soft_ball": 300}.get(a.workload, 60)
+    SIM_STEPS = a.sim_steps if a.sim_steps is not None else {"batch": 100, "star": 200, "cloth_ball": 300}.get(a.workload, 60)
     return a
 
 
@@ -649,19 +647,6 @@ def run_cloth_ball(args):
                          grad_key="v")
 
 
-def run_cloth_soft_ball(args):
-    from diff_fem_b200 import scene as S
-    from diff_fem_b200._capi import DFEM_PREC_FP64, DFEM_PREC_MIXED
-    prec = DFEM_PREC_FP64 if args.precision == "fp64" else DFEM_PREC_MIXED
-    d = S.cloth_on_soft_ball(precision=prec)
-    run_contact_workload(args, d, "fwd+adjoint sim steps/s (64x64 cloth on a soft ball, K=20)",
-                         f"cloth 64x64 (4,096 vertices, 12,033 springs, 3,844 bending stencils), membrane 1e3, "
-                         f"bending 1e-3, 0.2 kg/m^2, dropped 0.3 m onto a soft ball r=0.2 ({d.n_tets} tets, E=5e4) "
-                         f"on a ground quad; soft-soft contact (cloth and ball surfaces, mu=0.3, alpha=0.5), "
-                         f"ground mu=0.3, h=1/120, K=20, {SIM_STEPS} steps, forward + adjoint dL/dv0",
-                         grad_key="v")
-
-
 def run_star(args):
     """Muscle star on a ground obstacle: 200 steps forward with random chain
     activations, then the gradient of L = |x_200 - x_0|^2 with respect to every
@@ -764,8 +749,6 @@ def main():
         run_star(args)
     elif args.workload == "cloth_ball":
         run_cloth_ball(args)
-    elif args.workload == "cloth_soft_ball":
-        run_cloth_soft_ball(args)
     else:
         run_ours(args)
 
