@@ -286,34 +286,66 @@ __global__ void k_contact_detect(ContactDev c, const double* xt, const double* x
     st3(c.imp_n, a * kMaxImpactsPerVertex + slot, n);
   }
   if (any) atomicOr(&c.state[CS_ANY], 1);
-  // soft impacts (thickness x 2) against every soft face not holding the
-  // vertex, faces ascending; a face met again refreshes its entry in place
-  if (c.ncf > 0 && c.on_face[a]) {
-    for (int f = 0; f < c.ncf; ++f) {
+}
+
+// Soft impacts (thickness x 2) of contact vertex a (one warp per vertex) against
+// every soft face not holding it: the lanes test 32 consecutive faces, then
+// lane 0 applies the hits in ascending face order (a face met again refreshes
+// its entry in place, a new one is appended), as one thread looping over the
+// faces would.
+__global__ void k_self_detect(ContactDev c, const double* xt, const double* xk, int* status) {
+  if (c.state[CS_MODE] != 0) return;
+  const int lane = threadIdx.x & 31;
+  const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (a >= c.nc || !c.on_face[a]) return;  // uniform over the warp
+  const int gv = c.cverts[a];
+  const Vec3<double> p0 = ld3(xt, gv), p1 = ld3(xk, gv);
+  const int base = a * kMaxSelfImpacts;
+  for (int f0 = 0; f0 < c.ncf; f0 += 32) {
+    const int f = f0 + lane;
+    bool hit = false;
+    Vec3<double> n = mk3(0.0, 0.0, 0.0);
+    double t = 0.0, dd = 0.0;
+    if (f < c.ncf) {
       const int* cf = c.cfaces + 3 * f;
-      if (cf[0] == a || cf[1] == a || cf[2] == a) continue;
-      Vec3<double> qs[3], qe[3];
-      for (int k = 0; k < 3; ++k) {
-        const int gq = c.cverts[cf[k]];
-        qs[k] = ld3(xt, gq);
-        qe[k] = ld3(xk, gq);
+      if (cf[0] != a && cf[1] != a && cf[2] != a) {
+        Vec3<double> qs[3], qe[3];
+        for (int k = 0; k < 3; ++k) {
+          const int gq = c.cverts[cf[k]];
+          qs[k] = ld3(xt, gq);
+          qe[k] = ld3(xk, gq);
+        }
+        hit = vf_impact_moving(p0, p1, qs, qe, 2.0, &n, &t, &dd);
       }
-      Vec3<double> n;
-      double t, dd;
-      if (!vf_impact_moving(p0, p1, qs, qe, 2.0, &n, &t, &dd)) continue;
-      const int base = a * kMaxSelfImpacts;
-      int cnt = c.simp_cnt[a], slot = -1;
-      for (int q = 0; q < cnt; ++q)
-        if (c.simp_face[base + q] == f) { slot = q; break; }
-      if (slot < 0) {
-        if (cnt >= kMaxSelfImpacts) { atomicExch(status, 6); continue; }
-        slot = cnt;
-        c.simp_face[base + slot] = f;
-        c.simp_cnt[a] = cnt + 1;
+    }
+    unsigned mask = __ballot_sync(0xffffffffu, hit);
+    while (mask) {
+      const int src = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const double nx = __shfl_sync(0xffffffffu, n.x, src), ny = __shfl_sync(0xffffffffu, n.y, src),
+                   nz = __shfl_sync(0xffffffffu, n.z, src);
+      const double ts = __shfl_sync(0xffffffffu, t, src), ds = __shfl_sync(0xffffffffu, dd, src);
+      if (lane == 0) {
+        const int fh = f0 + src;
+        int cnt = c.simp_cnt[a], slot = -1;
+        for (int q = 0; q < cnt; ++q)
+          if (c.simp_face[base + q] == fh) { slot = q; break; }
+        if (slot < 0) {
+          if (cnt >= kMaxSelfImpacts) {
+            atomicExch(status, 6);
+          } else {
+            slot = cnt;
+            c.simp_face[base + slot] = fh;
+            c.simp_cnt[a] = cnt + 1;
+          }
+        }
+        if (slot >= 0) {
+          c.simp_td[2 * (base + slot)] = ts;
+          c.simp_td[2 * (base + slot) + 1] = ds;
+          st3(c.simp_n, base + slot, mk3(nx, ny, nz));
+        }
       }
-      c.simp_td[2 * (base + slot)] = t;
-      c.simp_td[2 * (base + slot) + 1] = dd;
-      st3(c.simp_n, base + slot, n);
+      __syncwarp();
     }
   }
 }

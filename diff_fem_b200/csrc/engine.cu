@@ -999,7 +999,8 @@ static void contact_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHa
   const int ncons = s.T + s.M + s.S + s.B;
   k_contact_detect<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd, sc->xt.p, sc->xk.p, sc->status.p);
   const int ncf = sc->cd.ncf;
-  if (sc->self_contact) {  // the pass's self groups
+  if (sc->self_contact) {  // soft impacts, then the pass's self groups
+    k_self_detect<<<(int)(((int64_t)sc->cd.nc * 32 + 127) / 128), 128, 0, st>>>(sc->cd, sc->xt.p, sc->xk.p, sc->status.p);
     k_self_reset<<<(ncf + 127) / 128, 128, 0, st>>>(sc->cd);
     k_self_closest<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd);
     k_self_scan<<<1, 1024, 0, st>>>(sc->cd);
