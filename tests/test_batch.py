@@ -137,6 +137,12 @@ def test_batch_set_materials_refactors_each_part():
     b.close()
 
 
+def test_batch_rejects_soft_contact():
+    d = dataclasses.replace(S.cloth_on_block(), obstacle_x=np.zeros((0, 3)), obstacle_faces=np.zeros((0, 3), np.int32))
+    with pytest.raises(_capi.DfemError, match="soft-soft"):
+        Scene.batch([d, d])
+
+
 def test_batch_rejects_mismatched_time_steps():
     descs = [S.cantilever(), S.inverse_stiffness(nx=6, ny=2, nz=2)]
     with pytest.raises(_capi.DfemError, match="time_step"):

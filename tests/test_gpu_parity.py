@@ -129,7 +129,7 @@ def test_obstacle_contact_forward(mu):
     assert rel(tg, ro["traj"]) < POS_TOL
 
 
-@pytest.mark.parametrize("case", ["small", "wide"])
+@pytest.mark.parametrize("case", ["small", "wide", "no_ground"])
 def test_soft_contact_forward(case):
     """Soft-soft contact (self-collision on): a cloth dropped onto a soft block
     that rests on a ground quad.  Soft CCD both ways (cloth vertices on block
@@ -138,8 +138,13 @@ def test_soft_contact_forward(case):
     the block's obstacle contacts, against the oracle."""
     if case == "small":
         d, n = S.cloth_on_block(), 10
-    else:
+    elif case == "wide":
         d, n = S.cloth_on_block(nv=8, edge=0.0071, block=(3, 1, 3), block_edge=0.02), 8
+    else:  # soft contact only: no obstacle face at all (the block falls too)
+        d, n = S.cloth_on_block(), 8
+        v0 = d.initial_velocity
+        d = dataclasses.replace(d, obstacle_x=np.zeros((0, 3)), obstacle_faces=np.zeros((0, 3), np.int32))
+        d.initial_velocity = v0
     x = d.x0.reshape(-1).copy()
     v = d.initial_velocity.copy()
     g = Scene(d)
