@@ -799,10 +799,12 @@ __global__ void k_self_record(ContactDev c) {
   }
 }
 
-// The remembered self forces at the start of the current step.
-__global__ void k_self_save(ContactDev c, const int* step) {
+// Every time step starts with no remembered self forces: World::TimeStepping
+// calls updateCollisionScene before the PD solve (sim/fem/World.h:700), which
+// zeroes the self-collision force buffers (World.h:742-753).
+__global__ void k_self_clear(ContactDev c) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < 3 * c.nc) c.sc_hist[(size_t)(*step) * 3 * c.nc + k] = c.sc_cur[k];
+  if (k < 3 * c.nc) c.sc_cur[k] = 0.0;
 }
 
 // ---- adjoint of the contact phase ------------------------------------------------

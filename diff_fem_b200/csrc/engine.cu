@@ -10,7 +10,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <thread>
 #include <string>
 #include <vector>
@@ -42,6 +44,25 @@ int report_error(int code, const std::string& msg) { return fail(code, msg); }
   } while (0)
 
 #define RC(x) do { int rc_ = (x); if (rc_) return rc_; } while (0)
+
+// A kernel's dynamic shared-memory limit (cudaFuncAttributeMaxDynamicSharedMemorySize)
+// is a property of the kernel in the process, per device, not of a scene: it
+// only ever grows here, so creating a scene that needs less never lowers the
+// limit that an earlier, larger scene's launches rely on.
+static cudaError_t raise_smem_limit(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> limit;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  bytes = std::max<size_t>(1, bytes);
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& cur = limit[{fn, dev}];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
 
 struct LoopGraph {
   cudaGraphExec_t exec = nullptr;
@@ -126,6 +147,7 @@ struct dfem_scene {
   size_t shm_cluster = 0;
   int shm_cluster_warp = 0;              // doubles of shared memory per warp item
   bool cluster_ok = false;
+  cudaError_t cluster_launch_err = cudaSuccess;  // the last refused cluster launch (read and cleared by its checks)
   double select_ms[2] = {0.0, 0.0};      // batches, only the largest part active: tuned form, persistent form
   // numeric refactorisation on the GPU (material changes)
   DBuf<double> hs_base, hc_coef, Ldw, part_reg, E_in, nu_in;
@@ -165,7 +187,7 @@ struct dfem_scene {
       s_g_cnt, s_g_fill, s_g_ptr, s_g_mem, s_chit;
   DBuf<double> s_simp_td, s_simp_n, s_g_n, s_g_outF, s_g_outM, s_sc_cur, s_rhs_pre, s_cnext;
   DBuf<int> crec_si;                      // soft-contact records (per computed iteration)
-  DBuf<double> crec_sd, s_sc_hist;        // ...; remembered self forces at each step's start
+  DBuf<double> crec_sd;
   DBuf<double> ca_scb, ca_ptot, ca_sbp, ca_gPF, ca_gPM, ca_gmF, ca_gmM, ca_xout;  // its adjoint
   // adjoint of the contact phase: the record of one step's Jacobi iterations and the reverse sweep's buffers
   DBuf<int> crec_on, crec_first, crec_cnt;
@@ -387,9 +409,7 @@ static int upload_factor(dfem_scene* sc) {
     CK(sc->lvl_warp_d.upload(lw));
     sc->shm_cluster_warp = (int)((wneed + 1) & ~size_t(1));
     sc->shm_cluster = std::max<size_t>(16 * 8 * (size_t)sc->shm_cluster_warp, 8 * cneed);
-    sc->cluster_ok = sc->shm_cluster <= budget &&
-                     cudaFuncSetAttribute(k_solve_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)std::max<size_t>(1, sc->shm_cluster)) == cudaSuccess;
+    sc->cluster_ok = sc->shm_cluster <= budget && raise_smem_limit((const void*)k_solve_cluster, sc->shm_cluster) == cudaSuccess;
     cudaGetLastError();
   }
   std::vector<int> snp(ns, 0);
@@ -406,9 +426,9 @@ static int upload_factor(dfem_scene* sc) {
     CK(sc->sn_info.upload(info));
   }
   for (auto fn : {(const void*)k_fwd_level<CtaGroup>, (const void*)k_bwd_level<CtaGroup>})
-    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(1, max_cta_blk)));
+    CK(raise_smem_limit(fn, max_cta_blk));
   for (auto fn : {(const void*)k_fwd_level<WarpGroup>, (const void*)k_bwd_level<WarpGroup>})
-    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(1, max_warp_blk)));
+    CK(raise_smem_limit(fn, max_warp_blk));
   // persistent solve: elimination tree (children CSR), completion stamps, control words
   {
     std::vector<int> kp(ns + 1, 0), kd(std::max(1, ns));
@@ -427,7 +447,7 @@ static int upload_factor(dfem_scene* sc) {
       CK(sc->solve_ctl.alloc(4));
     }
     sc->shm_pers = max_cta;
-    CK(cudaFuncSetAttribute(k_solve_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_pers));
+    CK(raise_smem_limit((const void*)k_solve_persistent, sc->shm_pers));
     int nsm = 1, per_sm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, sc->device));
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_persistent, 256, sc->shm_pers));
@@ -540,7 +560,7 @@ static int upload_refactor_plan(dfem_scene* sc) {
   for (int w : F.sn_w) maxw = std::max(maxw, w);
   sc->shm_fact = factor_smem_bytes(maxw);
   if (sc->shm_fact > 227 * 1024) return fail(DFEM_ERR_INVALID, "supernode too wide for the GPU refactorisation");
-  CK(cudaFuncSetAttribute(k_factor_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sc->shm_fact));
+  CK(raise_smem_limit((const void*)k_factor_level, sc->shm_fact));
   sc->shm_fact_lvl.assign(F.nlevels, 0);
   for (int l = 0; l < F.nlevels; ++l) {
     int mw = 1;
@@ -783,10 +803,6 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
     CK(sc->crec_meta.alloc(4 * (size_t)cap));
     sc->cd.rec_meta = sc->crec_meta.p;
   }
-  if (sc->self_contact) {
-    CK(sc->s_sc_hist.alloc(3 * (size_t)sc->cd.nc * cap));
-    sc->cd.sc_hist = sc->s_sc_hist.p;
-  }
   sc->cap_steps = cap;
   invalidate_graphs(sc);  // graphs hold the old pointers
   return DFEM_OK;
@@ -810,7 +826,7 @@ static void launch_segment(dfem_scene* sc, cudaStream_t st, const dfem_scene::Le
 
 static int n_levels(const dfem_scene* sc) { return (int)sc->lvl_ptr.size() - 1; }
 
-static void launch_cluster_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
+static cudaError_t launch_cluster_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(kClusterCtas);
   cfg.blockDim = dim3(512);
@@ -823,13 +839,17 @@ static void launch_cluster_solve(dfem_scene* sc, cudaStream_t st, Gate gate, con
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, k_solve_cluster, sc->fd, (int)sc->lvl_ptr.size() - 1, (const int*)sc->lvl_ptr_d.p,
-                     (const int*)sc->lvl_warp_d.p, sc->shm_cluster_warp, gate, rhs, y);
+  return cudaLaunchKernelEx(&cfg, k_solve_cluster, sc->fd, (int)sc->lvl_ptr.size() - 1, (const int*)sc->lvl_ptr_d.p,
+                            (const int*)sc->lvl_warp_d.p, sc->shm_cluster_warp, gate, rhs, y);
 }
 
+// Launch errors surface through cudaGetLastError, which every caller checks;
+// the cluster launch's return value is also kept for the autotune, which drops
+// the cluster form when the device refuses its launch.
 static void enqueue_solve_cut(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y, int c) {
   if (c < 0) {
-    launch_cluster_solve(sc, st, gate, rhs, y);
+    const cudaError_t e = launch_cluster_solve(sc, st, gate, rhs, y);
+    if (e != cudaSuccess) sc->cluster_launch_err = e;
     return;
   }
   for (const auto& g : sc->segs)
@@ -977,7 +997,7 @@ static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
 }
 
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
-  if (sc->self_contact) k_self_save<<<(3 * sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd, sc->step.p);
+  if (sc->self_contact) k_self_clear<<<(3 * sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd);
   if (sc->nF > 0) k_drag_faces<<<(sc->nF + 127) / 128, 128, 0, st>>>(sc->nF, sc->df.p, sc->xt.p, sc->vt.p, sc->fdrag.p);
   k_step_begin<<<sc->nblk_p, kPartBlock, 0, st>>>(sc->sd, sc->pd, sc->step.p, sc->xt.p, sc->vt.p, sc->qn.p, sc->c0.p, sc->xk.p,
                                    sc->hist.p, sc->hist_step, std::max(1, sc->hs.checkpoint_every), sc->ckpt_x.p,
@@ -1283,8 +1303,11 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
   }
   if (base + comp > sc->crec_cap) return fail(DFEM_ERR_CAP, "contact record too small for the recomputed step");
   // soft contact: every computed iteration feeds the remembered self forces,
-  // so the sweep starts at the last one and the output enters at its source
+  // so the sweep starts at the last one and the output enters at its source;
+  // the step's final remembered forces are zeroed before the next step reads
+  // them (World.h:742-753), so their cotangent starts at zero
   const bool soft = sc->self_contact;
+  if (soft) CK(cudaMemsetAsync(sc->ca_scb.p, 0, sizeof(double) * 3 * (size_t)sc->cd.nc, sc->stream));
   const int top = soft ? comp : src;
   std::vector<int> first(std::max(1, top));
   if (top > 0)
@@ -1495,11 +1518,15 @@ static int autotune_solve(dfem_scene* sc) {
   // the cluster form: factors of few supernodes (one cluster walks them all)
   sc->solve_ms[3] = 0.0;
   if (rc == DFEM_OK && sc->cluster_ok && sc->hs.F.nsuper <= kClusterMaxSupernodes) {
+    sc->cluster_launch_err = cudaSuccess;
     rc = time_cut(-1, &sc->solve_ms[3]);
+    if (rc == DFEM_OK && sc->cluster_launch_err != cudaSuccess) rc = DFEM_ERR_CUDA;
     if (rc != DFEM_OK) {  // a launch the device refuses (cluster shape): not a candidate
       cudaGetLastError();
       sc->cluster_ok = false;
+      sc->cluster_launch_err = cudaSuccess;
       sc->solve_ms[3] = 0.0;
+      g_last_error.clear();  // the dropped candidate is not an error of the scene
       rc = DFEM_OK;
     }
   }
@@ -1707,8 +1734,6 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
     const int on = fwd_rec ? 2 : 0;
     CK(cudaMemcpyAsync(sc->crec_on.p, &on, sizeof(int), cudaMemcpyHostToDevice, sc->stream));
     CK(cudaMemsetAsync(sc->crec_base.p, 0, sizeof(int), sc->stream));
-    // each forward call starts with no remembered self forces
-    if (sc->self_contact) CK(cudaMemsetAsync(sc->s_sc_cur.p, 0, sizeof(double) * 3 * (size_t)sc->cd.nc, sc->stream));
     CK(cudaStreamSynchronize(sc->stream));  // `on` is a host local
   }
   CK(cudaGetLastError());
@@ -1779,8 +1804,6 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
   }
   const int rbase = sc->crec_fwd ? sc->crec_used : 0;
   if (any_contact) RC(ensure_contact_record(sc, rbase + std::max(1, ccap), rbase));
-  if (sc->self_contact && sc->ca_scb.p)  // the final remembered self forces are not an output
-    CK(cudaMemsetAsync(sc->ca_scb.p, 0, sizeof(double) * 3 * (size_t)sc->cd.nc, sc->stream));
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N;
   const int nb = sc->nblk_v;
@@ -1820,9 +1843,6 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
       CK(cudaMemcpyAsync(sc->vt.p, sc->ckpt_v.p + (size_t)(seg0 / kc) * n3, n3 * sizeof(double),
                          cudaMemcpyDeviceToDevice, sc->stream));
       if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 0);
-      if (sc->self_contact)  // the segment's first step starts from its remembered self forces
-        CK(cudaMemcpyAsync(sc->s_sc_cur.p, sc->s_sc_hist.p + (size_t)seg0 * 3 * sc->cd.nc,
-                           sizeof(double) * 3 * (size_t)sc->cd.nc, cudaMemcpyDeviceToDevice, sc->stream));
       for (int q = seg0; q < seg_end; ++q) {
         CK(cudaMemcpyAsync(sc->seg_x.p + (size_t)(q - seg0) * n3, sc->xt.p, n3 * sizeof(double),
                            cudaMemcpyDeviceToDevice, sc->stream));
@@ -1844,9 +1864,6 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
         // a contact step also records its contact iterations for the contact adjoint
         CK(cudaMemcpyAsync(sc->xt.p, sx(st), n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
         CK(cudaMemcpyAsync(sc->vt.p, sv(st), n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
-        if (sc->self_contact)
-          CK(cudaMemcpyAsync(sc->s_sc_cur.p, sc->s_sc_hist.p + (size_t)st * 3 * sc->cd.nc,
-                             sizeof(double) * 3 * (size_t)sc->cd.nc, cudaMemcpyDeviceToDevice, sc->stream));
         k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
         CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
         rerun[st] += 1;

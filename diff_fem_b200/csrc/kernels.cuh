@@ -178,7 +178,8 @@ struct ContactDev {
   double* g_n;            // 3 ncf: group normal (its first member's impact normal)
   double* g_outF;         // 9 ncf: a group's self forces on its face's three vertices
   double* g_outM;         // 3 nc: a member's self force (by its g_mem position)
-  double* sc_cur;         // 3 nc: self forces of the last CollisionHandling call that swapped buffers
+  double* sc_cur;         // 3 nc: self forces of the step's last CollisionHandling call that swapped buffers
+                          // (zero at every step's start)
   double* rhs_pre;        // 3 nc: contact vertices' rhs before this iteration's CollisionHandling
   double* cnext;          // 3 nc: obstacle reactions of this iteration (self contact on)
   int* chit;              // nc: the vertex has an obstacle reaction this iteration
@@ -188,7 +189,6 @@ struct ContactDev {
   // [remembered self forces before the call (3 nc), g_n (3 ncf)]
   int* rec_si;
   double* rec_sd;
-  double* sc_hist;        // steps x 3 nc: the remembered self forces at each step's start
 };
 __host__ __device__ inline size_t self_rec_si_stride(int nc, int ncf) { return 3 * (size_t)nc + 2 * (size_t)ncf + 3; }
 __host__ __device__ inline size_t self_rec_sd_stride(int nc, int ncf) { return 3 * (size_t)nc + 3 * (size_t)ncf; }

@@ -14,6 +14,12 @@
 // contents.  Each call writes every scratch entry it reads before reading it,
 // so nothing has to start at zero; but calls that overlap on the GPU (two
 // streams, or two host threads) race on it and must be serialised by the caller.
+//
+// Indices are checked on the device: a tet vertex outside [0, n_vertices) or
+// an incidence slot outside [0, 4 n_tets) is skipped (no access is made through
+// it), the affected output vertex is set to NaN, and a second file-scope word
+// records the fault; the next call on the device reads that word first and
+// returns DFEM_ERR_INVALID if it is set (then clears it).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -26,6 +32,7 @@ namespace dfem {
 namespace {
 
 static __device__ __align__(256) double g_noalloc_slots[(size_t)DFEM_NOALLOC_MAX_TETS * 12];
+static __device__ int g_noalloc_bad_index;  // 1: a call met an index out of range (see above)
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
@@ -39,18 +46,26 @@ namespace {
 
 int set_err(int code, const std::string& m) { return report_error(code, m); }
 
-__global__ void k_noalloc_tets(int T, const double* __restrict__ x, const int* __restrict__ tets,
+__global__ void k_noalloc_tets(int N, int T, const double* __restrict__ x, const int* __restrict__ tets,
                                const double* __restrict__ inv_dm, const double* __restrict__ w_rot,
                                const double* __restrict__ w_vol, double* __restrict__ slots) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= T) return;
   int vi[4];
   Vec3<double> xv[4];
+  bool bad = false;
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
     vi[a] = tets[4 * t + a];
-    xv[a] = mk3(x[3 * vi[a]], x[3 * vi[a] + 1], x[3 * vi[a] + 2]);
+    bad = bad || vi[a] < 0 || vi[a] >= N;
   }
+  if (bad) {  // skip the tet: its slots become NaN, which the gather passes on
+    g_noalloc_bad_index = 1;
+    for (int k = 0; k < 12; ++k) slots[12 * (size_t)t + k] = __longlong_as_double(0x7ff8000000000000LL);
+    return;
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) xv[a] = mk3(x[3 * vi[a]], x[3 * vi[a] + 1], x[3 * vi[a] + 2]);
   // G[v][j]: F(:,j) = sum_v G[v][j] x_v, from invDm (row-major)
   double G[4][3];
 #pragma unroll
@@ -74,14 +89,22 @@ __global__ void k_noalloc_tets(int T, const double* __restrict__ x, const int* _
   }
 }
 
-__global__ void k_noalloc_gather(int N, const int* __restrict__ vtx_ptr, const int* __restrict__ vtx_slot,
+__global__ void k_noalloc_gather(int N, int T, const int* __restrict__ vtx_ptr, const int* __restrict__ vtx_slot,
                                  const double* __restrict__ slots, double* __restrict__ out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double a0 = 0, a1 = 0, a2 = 0;
-  for (int k = vtx_ptr[i]; k < vtx_ptr[i + 1]; ++k) {
-    const double* q = slots + 3 * (size_t)vtx_slot[k];
+  const int k0 = vtx_ptr[i], k1 = vtx_ptr[i + 1];
+  bool bad = k0 < 0 || k1 < k0 || k1 > 4 * T;
+  for (int k = k0; !bad && k < k1; ++k) {
+    const int sl = vtx_slot[k];
+    if (sl < 0 || sl >= 4 * T) { bad = true; break; }
+    const double* q = slots + 3 * (size_t)sl;
     a0 += q[0]; a1 += q[1]; a2 += q[2];
+  }
+  if (bad) {
+    g_noalloc_bad_index = 1;
+    a0 = a1 = a2 = __longlong_as_double(0x7ff8000000000000LL);
   }
   out[3 * i] = a0; out[3 * i + 1] = a1; out[3 * i + 2] = a2;
 }
@@ -121,8 +144,25 @@ extern "C" int dfem_eval_corotated_noalloc(int32_t n_vertices, int32_t n_tets, c
     slots = g_slots_addr[dev];
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (n_tets > 0) k_noalloc_tets<<<(n_tets + 127) / 128, 128, 0, s>>>(n_tets, x, tets, inv_dm, w_rot, w_vol, slots);
-  k_noalloc_gather<<<(n_vertices + 127) / 128, 128, 0, s>>>(n_vertices, vtx_ptr, vtx_slot, slots, jd_out);
+  {
+    // an earlier call on this device met an index out of range: report it once
+    // (this waits for the work already queued on `stream`)
+    int bad = 0;
+    e = cudaMemcpyFromSymbolAsync(&bad, g_noalloc_bad_index, sizeof(int), 0, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_err(DFEM_ERR_CUDA, cudaGetErrorString(e));
+    if (bad) {
+      const int zero = 0;
+      e = cudaMemcpyToSymbolAsync(g_noalloc_bad_index, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return set_err(DFEM_ERR_CUDA, cudaGetErrorString(e));
+      return set_err(DFEM_ERR_INVALID, "dfem_eval_corotated_noalloc: an earlier call met a vertex index or incidence "
+                                       "slot out of range (its outputs were NaN)");
+    }
+  }
+  if (n_tets > 0)
+    k_noalloc_tets<<<(n_tets + 127) / 128, 128, 0, s>>>(n_vertices, n_tets, x, tets, inv_dm, w_rot, w_vol, slots);
+  k_noalloc_gather<<<(n_vertices + 127) / 128, 128, 0, s>>>(n_vertices, n_tets, vtx_ptr, vtx_slot, slots, jd_out);
   e = cudaGetLastError();
   if (e != cudaSuccess) return set_err(DFEM_ERR_CUDA, cudaGetErrorString(e));
   return DFEM_OK;

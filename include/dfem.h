@@ -217,13 +217,21 @@ int dfem_eval_local(dfem_scene *scene, const double *x, double *jd_out, int mem)
  * row-major Dm^-1 per tet), w_rot = mu*vol and w_vol = nu*mu*vol (T each),
  * the vertex -> (4*tet + corner) incidence CSR vtx_ptr (N+1) / vtx_slot (4T)
  * and jd_out (3N) are caller-owned device buffers; the work is enqueued on
- * `stream` (a cudaStream_t, NULL = default stream) and not synchronised.
+ * `stream` (a cudaStream_t, NULL = default stream) and not waited for.
  * The per-(tet, corner) scratch is a static device array of
  * DFEM_NOALLOC_MAX_TETS * 12 doubles (6 MiB) that every GPU loading the
  * library holds until exit; n_tets above the limit is rejected with
  * DFEM_ERR_INVALID.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress), so make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU race. */
+ * address (cudaGetSymbolAddress), so make it before any stream capture; the
+ * address is kept for the life of the process, so a cudaDeviceReset between
+ * calls is not supported.  All calls share the array: calls that overlap on
+ * the GPU race.
+ * Index ranges: tets entries in [0, n_vertices); vtx_ptr non-decreasing from
+ * 0 to at most 4*n_tets; vtx_slot entries in [0, 4*n_tets).  The device skips
+ * an index out of range (the affected outputs become NaN) and records it; the
+ * next call on the device then first waits for `stream`, and returns
+ * DFEM_ERR_INVALID (clearing the record).  Each call therefore also waits
+ * for the work queued on `stream` before it, not for its own. */
 #define DFEM_NOALLOC_MAX_TETS 65536
 int dfem_eval_corotated_noalloc(int32_t n_vertices, int32_t n_tets, const double *x, const int32_t *tets,
                                 const double *inv_dm, const double *w_rot, const double *w_vol,

@@ -318,7 +318,6 @@ struct Scene {
   std::vector<double> rec_act;             /* per step activations */
   std::vector<int> rec_iters;
   std::vector<int> rec_passes;             /* contact passes per step */
-  std::vector<double> rec_sc;              /* sc_cur at each step's start */
 };
 
 static void add_H(std::vector<std::vector<std::pair<int, double>>>& rows, int i, int j, double v) {
@@ -1815,15 +1814,14 @@ int orc_forward(void* s, const double* x, const double* v, const double* act, in
   S->rec_act.assign((size_t)n_steps * std::max(1, S->nseg), 0.0);
   S->rec_iters.assign(n_steps, 0);
   S->rec_passes.assign(n_steps, 0);
-  /* each forward call starts with no remembered self forces */
-  const size_t nsc = S->sc_cur.size();
-  std::fill(S->sc_cur.begin(), S->sc_cur.end(), 0.0);
-  S->rec_sc.assign((size_t)n_steps * nsc, 0.0);
   if (S->freeze == 1) S->frz.assign(n_steps, {});
   std::vector<double> zero_act(std::max(1, S->nseg), 0.0);
   for (int st = 0; st < n_steps; ++st) {
     const double* a = act ? act + (size_t)st * S->nseg : zero_act.data();
-    std::copy(S->sc_cur.begin(), S->sc_cur.end(), S->rec_sc.begin() + (size_t)st * nsc);
+    /* every step starts with no remembered contact forces: World::TimeStepping
+     * calls updateCollisionScene before the PD solve (World.h:700), which zeroes
+     * the self-collision force buffers (World.h:742-753) */
+    std::fill(S->sc_cur.begin(), S->sc_cur.end(), 0.0);
     S->cur_step = st;
     std::copy(xc.begin(), xc.end(), S->rec_x.begin() + (size_t)st * n3);
     std::copy(vc.begin(), vc.end(), S->rec_v.begin() + (size_t)st * n3);
@@ -1861,7 +1859,7 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
   std::vector<double> vwc(n3), qn(n3), xn(n3), hist, ybar(n3), xkb(n3), bb(n3), tmp(n3);
   double ih2 = 1.0 / (S->h * S->h);
   const size_t nsc = S->sc_cur.size();
-  std::vector<double> scb(nsc, 0.0);  /* cotangent of the self-force state carried between steps */
+  std::vector<double> scb(nsc, 0.0);  /* cotangent of the self-force state within a step */
   for (int st = S->rec_steps - 1; st >= 0; --st) {
     const double* x = &S->rec_x[(size_t)st * n3];
     const double* v = &S->rec_v[(size_t)st * n3];
@@ -1869,7 +1867,11 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
     step_prep(*S, x, v, vwc.data(), qn.data());
     int it = pd_solve(*S, x, qn.data(), a, &hist, xn.data(), 1);
     ContactTape tape;
-    std::copy(S->rec_sc.begin() + (size_t)st * nsc, S->rec_sc.begin() + (size_t)(st + 1) * nsc, S->sc_cur.begin());
+    /* the step's contact phase starts from zero remembered forces (World.h:742-753)
+     * and its final ones are zeroed before anything reads them: no cotangent
+     * crosses the step boundary */
+    std::fill(S->sc_cur.begin(), S->sc_cur.end(), 0.0);
+    std::fill(scb.begin(), scb.end(), 0.0);
     S->cur_step = st;
     const int freeze0 = S->freeze;
     if (freeze0 == 1) S->freeze = 2;  /* re-runs replay what the forward recorded */

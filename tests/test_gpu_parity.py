@@ -134,8 +134,8 @@ def test_soft_contact_forward(case):
     """Soft-soft contact (self-collision on): a cloth dropped onto a soft block
     that rests on a ground quad.  Soft CCD both ways (cloth vertices on block
     faces, block vertices on cloth faces), face groups with the stick/slide
-    exchange, the self forces remembered between iterations and steps, and
-    the block's obstacle contacts, against the oracle."""
+    exchange, the self forces remembered between the iterations of a step,
+    and the block's obstacle contacts, against the oracle."""
     if case == "small":
         d, n = S.cloth_on_block(), 10
     elif case == "wide":
@@ -159,12 +159,55 @@ def test_soft_contact_forward(case):
     g.close()
 
 
+def test_soft_contact_steps_carry_no_remembered_forces():
+    """Every step starts with zero remembered contact forces
+    (World::TimeStepping -> updateCollisionScene, World.h:700,742-753): a
+    3-step forward equals three 1-step forwards bit for bit, on the GPU as in
+    the oracle."""
+    d = S.cloth_on_block()
+    x = d.x0.reshape(-1).copy()
+    v = d.initial_velocity.copy()
+    g = Scene(d)
+    x3, v3 = g.forward(x, v, n_steps=3)
+    xs, vs = x, v
+    passes = 0
+    for _ in range(3):
+        xs, vs = g.forward(xs, vs, n_steps=1)
+        passes += int(g.contact_passes(1).sum())
+    assert passes > 0
+    assert np.array_equal(x3, xs) and np.array_equal(v3, vs)
+    g.close()
+
+
+def test_scene_created_after_a_larger_one_leaves_its_kernels_usable():
+    """The kernels' shared-memory limits are process-wide: a small scene
+    created after a large one must not lower them under the large scene's
+    launches (refactorisation, solves, autotune)."""
+    big = S.inverse_stiffness()
+    g_big = Scene(big)
+    x = big.x0.reshape(-1).copy()
+    v = np.zeros_like(x)
+    x_ref, v_ref = g_big.forward(x, v, n_steps=2)
+    small = S.inverse_stiffness(nx=4, ny=2, nz=2)
+    g_small = Scene(small)
+    xs = small.x0.reshape(-1).copy()
+    g_small.forward(xs, np.zeros_like(xs), n_steps=2)
+    g_big.set_materials(big.youngs, big.poisson)
+    x2, v2 = g_big.forward(x, v, n_steps=2)
+    assert np.array_equal(x2, x_ref) and np.array_equal(v2, v_ref)
+    g_big.solve_mode("auto")
+    x3, _ = g_big.forward(x, v, n_steps=2)
+    assert np.array_equal(x3, x_ref)
+    g_small.close()
+    g_big.close()
+
+
 @pytest.mark.parametrize("case,every", [("small", 1), ("small", 2), ("wide", 1), ("ball", 1)])
 def test_soft_contact_adjoint(case, every):
     """Adjoint of soft-soft contact (group exchange reversed per computed
-    iteration, the remembered self forces' cotangent carried between
-    iterations and steps, replays from the saved start-of-step forces,
-    checkpoints every step or every second step) against the oracle's
+    iteration, the remembered self forces' cotangent carried between the
+    iterations of a step, checkpoints every step or every second step)
+    against the oracle's
     adjoint (forward-mode duals per group; pinned by central differences)."""
     if case == "small":
         d, n = S.cloth_on_block(), 4

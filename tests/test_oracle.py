@@ -356,9 +356,24 @@ def test_soft_contact_keeps_the_cloth_on_the_block():
     assert tr2[:, :nc, 1].min() < 0.02
 
 
+def test_soft_contact_steps_carry_no_remembered_forces():
+    """Every time step starts with zero remembered contact forces
+    (World::TimeStepping -> updateCollisionScene, World.h:700,742-753), so a
+    2-step forward equals two 1-step forwards bit for bit."""
+    d = S.cloth_on_block()
+    x = d.x0.reshape(-1).copy()
+    v = d.initial_velocity.copy()
+    o = O.OracleScene(d)
+    r2 = o.forward(x, v, n_steps=2)
+    assert o.contact_passes().sum() > 0
+    r1 = o.forward(x, v, n_steps=1)
+    r1b = o.forward(r1["x"], r1["v"], n_steps=1)
+    assert np.array_equal(r2["x"], r1b["x"]) and np.array_equal(r2["v"], r1b["v"])
+
+
 def test_soft_contact_adjoint_matches_central_differences():
     """The soft-contact adjoint (face groups by forward-mode duals, the
-    self-force state carried between Jacobi iterations and steps) against
+    self-force state carried between the Jacobi iterations of a step) against
     central differences.  The detection's outputs (normals from the faces'
     start positions, groups) are constants of the tape, as on the
     reference's tape, so the perturbed runs replay the recorded detection."""

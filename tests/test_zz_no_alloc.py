@@ -76,6 +76,40 @@ def test_noalloc_matches_allocating_path_on_two_calls():
         assert err < TOL, (call, err)
 
 
+def test_noalloc_reports_an_index_out_of_range_on_the_next_call():
+    """A tet vertex index out of range is skipped on the device (no access is
+    made through it; the affected outputs are NaN); the next call reports it
+    with DFEM_ERR_INVALID, and the call after that runs normally."""
+    import torch
+
+    d = S.inverse_stiffness(nx=6, ny=2, nz=2)
+    tets, inv, w_rot, w_vol, ptr, slots = raw_arrays(d)
+    dev = torch.device("cuda", 0)
+    T = lambda a, dt: torch.tensor(np.ascontiguousarray(a), dtype=dt, device=dev)
+    bad = tets.copy()
+    bad[3, 2] = d.n_vertices  # one past the last vertex
+    args = [T(inv, torch.float64), T(w_rot, torch.float64), T(w_vol, torch.float64), T(ptr, torch.int32),
+            T(slots, torch.int32)]
+    tx = T(d.x0.reshape(-1), torch.float64)
+    out = torch.zeros(3 * d.n_vertices, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    lib = _capi.lib()
+
+    def call(t):
+        return lib.dfem_eval_corotated_noalloc(d.n_vertices, d.n_tets, tx.data_ptr(), t.data_ptr(),
+                                               *[a.data_ptr() for a in args], out.data_ptr(), stream.cuda_stream)
+
+    assert call(T(bad, torch.int32)) == 0
+    stream.synchronize()
+    got = out.cpu().numpy().reshape(-1, 3)
+    assert np.isnan(got[tets[3]]).all() and np.isfinite(np.delete(got, tets[3], axis=0)).all()
+    assert call(T(tets, torch.int32)) == 1
+    assert b"out of range" in lib.dfem_last_error()
+    assert call(T(tets, torch.int32)) == 0
+    stream.synchronize()
+    assert np.isfinite(out.cpu().numpy()).all()
+
+
 def test_noalloc_rejects_sizes_beyond_the_static_limit():
     lib = _capi.lib()
     rc = lib.dfem_eval_corotated_noalloc(10, 65536 + 1, None, None, None, None, None, None, None, None, None)
