@@ -81,7 +81,7 @@ SIGNATURES = [
     ("dfem_host_factor_solve", C.c_int, [C.POINTER(SceneDescC), _VP, _VP, C.POINTER(SceneInfoC)]),
     ("dfem_solve_mode", C.c_int, [_VP, C.c_int32, _pi, C.POINTER(C.c_double)]),
     ("dfem_solve_split", C.c_int, [_VP, _pi, _pi, C.POINTER(C.c_double)]),
-    ("dfem_solve_times", C.c_int, [_VP, C.POINTER(C.c_double)]),
+    ("dfem_solve_times", C.c_int, [_VP, C.POINTER(C.c_double), C.c_int32]),
     ("dfem_solve_select", C.c_int, [_VP, _pi, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     ("dfem_profile_levels", C.c_int, [_VP, C.c_int32, C.c_int32, _pi, C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), _pi, _pi, _pi]),

@@ -22,6 +22,8 @@
 #include "contact_kernels.cuh"
 #include "factor_kernels.cuh"
 #include "drag_kernels.cuh"
+#include "resident_solve.cuh"
+#include "resident_plan.h"
 #include "scene.h"
 
 namespace dfem {
@@ -142,12 +144,24 @@ struct dfem_scene {
   // solve_cut = -1: the cluster form (one thread-block cluster walks the levels)
   int solve_cut = 0;
   int split_cut = 0;                     // the autotune's best split (0: none)
-  double solve_ms[4] = {0.0, 0.0, 0.0, 0.0};  // autotune timings (ms per solve): levels, persistent, best split, cluster
+  double solve_ms[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // autotune timings (ms per solve): levels, persistent, best split,
+                                                     // cluster, resident
   DBuf<int> lvl_ptr_d, lvl_warp_d;       // cluster form: level starts, end of each level's warp-sized supernodes
   size_t shm_cluster = 0;
   int shm_cluster_warp = 0;              // doubles of shared memory per warp item
   bool cluster_ok = false;
   cudaError_t cluster_launch_err = cudaSuccess;  // the last refused cluster launch (read and cleared by its checks)
+  // resident form (solve_cut = -2): the factor in the distributed shared memory of one cluster
+  bool res_ok = false;
+  int res_ctas = 0;
+  size_t shm_res = 0;
+  DBuf<ResSn> res_sn;
+  DBuf<int> res_sched, res_tsh;
+  DBuf<int2> res_cdst, res_xsrc;
+  DBuf<double> res_img;
+  DBuf<long long> res_img_ofs;
+  DBuf<ResPack> res_pack;
+  ResDev rdv{};
   double select_ms[2] = {0.0, 0.0};      // batches, only the largest part active: tuned form, persistent form
   // numeric refactorisation on the GPU (material changes)
   DBuf<double> hs_base, hc_coef, Ldw, part_reg, E_in, nu_in;
@@ -294,6 +308,8 @@ static int shm_class(size_t need) { return need <= kWarpGroupDoubles ? 0 : need 
 // supernode keeps its launch class: the long dependency chains at the top of
 // the elimination trees gain more from the bulk copies than the launch
 // classes lose in resident CTAs).
+
+static int plan_resident(dfem_scene* sc, const std::vector<int>& nseg, const std::vector<int>& cdst);
 
 static int upload_factor(dfem_scene* sc) {
   SupernodalFactor& F = sc->hs.F;
@@ -459,12 +475,86 @@ static int upload_factor(dfem_scene* sc) {
     for (int k = 0; k < ns; ++k) pos[F.lvl_sn[k]] = k;
     CK(sc->sn_pos.upload(pos));
   }
+  RC(plan_resident(sc, nseg, cdst));
   FactorDev fd{sc->sn_info.p, sc->rseg_ptr.p, sc->cdst.p, sc->contrib.p, sc->rowidx.p, sc->Lcm.p, sc->Dinv.p,
                sc->DinvC.p, sc->status.p, ns, sc->sn_pos.p, sc->sn_parent.p, sc->kid_ptr.p, sc->kid.p, sc->done_f.p,
                sc->done_b.p, sc->solve_ctl.p};
   if (std::memcmp(&fd, &sc->fd, sizeof(fd)) != 0) invalidate_graphs(sc);
   sc->fd = fd;
   return DFEM_OK;
+}
+
+// The resident solve form (k_solve_resident): a single scene whose factor
+// fits the shared memory of one cluster.  The widest cluster the device
+// schedules with the full shared memory per CTA (16, else 8), then the layout
+// of plan_resident_layout (resident_plan.cpp): owners, shared-memory offsets,
+// contribution and solution address tables, and the images with their row
+// tables; the blocks are copied into the images after every refactorisation.
+static int plan_resident(dfem_scene* sc, const std::vector<int>& nseg, const std::vector<int>& cdst) {
+  sc->res_ok = false;
+  const HostScene& s = sc->hs;
+  const SupernodalFactor& F = s.F;
+  if (s.nparts != 1 || F.nsuper == 0 || F.nlevels == 0) return DFEM_OK;
+  int optin = 0;
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, sc->device));
+  const size_t cap_bytes = optin > 2048 ? (size_t)optin - 1024 : 0;  // the static mbarrier and a margin
+  CK(cudaFuncSetAttribute((const void*)k_solve_resident, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  CK(raise_smem_limit((const void*)k_solve_resident, cap_bytes));
+  int C = 0;
+  for (int c : {16, 8}) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(512);
+    cfg.dynamicSmemBytes = cap_bytes;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, (const void*)k_solve_resident, &cfg) == cudaSuccess && n >= 1) {
+      C = c;
+      break;
+    }
+    cudaGetLastError();
+  }
+  ResidentPlan P;
+  if (C == 0 || !plan_resident_layout(F, nseg, cdst, C, cap_bytes, P)) return DFEM_OK;
+  std::vector<ResSn> rsn;
+  for (const auto& it : P.items)
+    rsn.push_back(ResSn{it.c0, it.w, it.r, it.dofs, it.lofs, it.pofs, it.qofs, it.yofs, it.rofs, it.s});
+  std::vector<ResPack> pk;
+  for (const auto& q : P.pack) pk.push_back(ResPack{q.w, q.r, q.src_d, q.src_l, q.dst_d, q.dst_l});
+  const size_t nrow = std::max<size_t>(1, P.cdst_rank.size());
+  std::vector<int2> rc(nrow, make_int2(0, 0)), rx(nrow, make_int2(0, 0));
+  for (size_t p = 0; p < P.cdst_rank.size(); ++p) {
+    rc[p] = make_int2(P.cdst_rank[p], P.cdst_ofs[p]);
+    rx[p] = make_int2(P.xsrc_rank[p], P.xsrc_ofs[p]);
+  }
+  CK(sc->res_sn.upload(rsn));
+  CK(sc->res_sched.upload(P.sched));
+  CK(sc->res_tsh.upload(P.tsh));
+  CK(sc->res_cdst.upload(rc));
+  CK(sc->res_xsrc.upload(rx));
+  CK(sc->res_img.upload(P.img));
+  CK(sc->res_img_ofs.upload(P.img_ofs));
+  CK(sc->res_pack.upload(pk));
+  CK(raise_smem_limit((const void*)k_solve_resident, 8 * P.smem_doubles));
+  sc->res_ctas = C;
+  sc->shm_res = 8 * P.smem_doubles;
+  sc->rdv = ResDev{sc->res_sn.p, sc->res_sched.p, sc->res_cdst.p, sc->res_xsrc.p, sc->res_img.p, sc->res_img_ofs.p,
+                   sc->res_tsh.p, P.L, (int)P.smem_doubles, sc->status.p};
+  sc->res_ok = true;
+  return DFEM_OK;
+}
+
+// The factor's blocks into the resident images (after a refactorisation).
+static void pack_resident(dfem_scene* sc) {
+  if (!sc->res_ok) return;
+  k_res_pack<<<sc->hs.F.nsuper, 256, 0, sc->stream>>>(sc->res_pack.p, sc->Dinv.p, sc->Lcm.p, sc->res_img.p);
+  sc->launches += 1;
 }
 
 static int upload_materials(dfem_scene* sc) {
@@ -609,7 +699,10 @@ static int gpu_refactor(dfem_scene* sc) {
         any = true;
         sc->part_reg_h[p] = sc->part_reg_h[p] == 0.0 ? 1e-5 : sc->part_reg_h[p] * 10.0;
       }
-    if (!any) return DFEM_OK;
+    if (!any) {
+      pack_resident(sc);
+      return DFEM_OK;
+    }
   }
   return fail(DFEM_ERR_FACTOR, "Cholesky factorisation failed after 25 regularisation retries");
 }
@@ -843,12 +936,28 @@ static cudaError_t launch_cluster_solve(dfem_scene* sc, cudaStream_t st, Gate ga
                             (const int*)sc->lvl_warp_d.p, sc->shm_cluster_warp, gate, rhs, y);
 }
 
+static cudaError_t launch_resident_solve(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(sc->res_ctas);
+  cfg.blockDim = dim3(512);
+  cfg.dynamicSmemBytes = sc->shm_res;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = sc->res_ctas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_solve_resident, sc->rdv, gate, rhs, y);
+}
+
 // Launch errors surface through cudaGetLastError, which every caller checks;
 // the cluster launch's return value is also kept for the autotune, which drops
 // the cluster form when the device refuses its launch.
 static void enqueue_solve_cut(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y, int c) {
-  if (c < 0) {
-    const cudaError_t e = launch_cluster_solve(sc, st, gate, rhs, y);
+  if (c < 0) {  // -1: cluster form, -2: resident form
+    const cudaError_t e = c == -2 ? launch_resident_solve(sc, st, gate, rhs, y) : launch_cluster_solve(sc, st, gate, rhs, y);
     if (e != cudaSuccess) sc->cluster_launch_err = e;
     return;
   }
@@ -919,9 +1028,9 @@ static cudaError_t capture_solve(dfem_scene* sc, cudaStream_t st, Gate gate, con
   return e;
 }
 
-// 1: level kernels, 2: persistent, 3: split, 4: cluster
+// 1: level kernels, 2: persistent, 3: split, 4: cluster, 5: resident
 static int solve_form(const dfem_scene* sc) {
-  return sc->solve_cut < 0 ? 4 : sc->solve_cut >= n_levels(sc) ? 1 : sc->solve_cut == 0 ? 2 : 3;
+  return sc->solve_cut == -2 ? 5 : sc->solve_cut < 0 ? 4 : sc->solve_cut >= n_levels(sc) ? 1 : sc->solve_cut == 0 ? 2 : 3;
 }
 
 // Fresh completion stamps and control words of the persistent solve (each API
@@ -1372,11 +1481,20 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
   return DFEM_OK;
 }
 
-// The device status word: [code, supernode, solve (1 forward / 2 backward), blocks that gave up].
+// The device status word: [code, supernode, which wait or check, blocks that gave up].
 static int status_error(const int st4[4]) {
-  if (st4[0] == DFEM_ERR_CAP && st4[2] > 0)
-    return fail(DFEM_ERR_CAP, "a staged-copy wait of the " + std::string(st4[2] == 1 ? "forward" : "backward") +
-                                  " solve gave up (supernode " + std::to_string(st4[1]) + ", " +
+  static const char* const what[] = {"",
+                                     "a staged-copy wait of the forward solve",
+                                     "a staged-copy wait of the backward solve",
+                                     "a dependency wait of the persistent forward solve",
+                                     "a dependency wait of the persistent backward solve",
+                                     "a streamed-block wait of the forward solve",
+                                     "a streamed-block wait of the backward solve",
+                                     "the resident solve's image copy",
+                                     "a resident-solve contribution address check",
+                                     "a resident-solve solution address check"};
+  if (st4[0] == DFEM_ERR_CAP && st4[2] > 0 && st4[2] <= 9)
+    return fail(DFEM_ERR_CAP, std::string(what[st4[2]]) + " gave up (supernode " + std::to_string(st4[1]) + ", " +
                                   std::to_string(st4[3]) + " blocks)");
   if (st4[0] == DFEM_ERR_CAP) return fail(DFEM_ERR_CAP, "a bounded loop gave up (contact impacts per vertex)");
   if (st4[0]) return fail(DFEM_ERR_NONFINITE, "non-finite value in the PD iteration");
@@ -1530,6 +1648,21 @@ static int autotune_solve(dfem_scene* sc) {
       rc = DFEM_OK;
     }
   }
+  // the resident form: single scenes whose factor fits one cluster's shared memory
+  sc->solve_ms[4] = 0.0;
+  if (rc == DFEM_OK && sc->res_ok) {
+    sc->cluster_launch_err = cudaSuccess;
+    rc = time_cut(-2, &sc->solve_ms[4]);
+    if (rc == DFEM_OK && sc->cluster_launch_err != cudaSuccess) rc = DFEM_ERR_CUDA;
+    if (rc != DFEM_OK) {  // a launch the device refuses: not a candidate
+      cudaGetLastError();
+      sc->res_ok = false;
+      sc->cluster_launch_err = cudaSuccess;
+      sc->solve_ms[4] = 0.0;
+      g_last_error.clear();
+      rc = DFEM_OK;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   RC(rc);
@@ -1539,8 +1672,9 @@ static int autotune_solve(dfem_scene* sc) {
   sc->solve_cut = sc->solve_ms[1] < sc->solve_ms[0] ? 0 : L;
   if (sc->split_cut > 0 && sc->solve_ms[2] < std::min(sc->solve_ms[0], sc->solve_ms[1])) sc->solve_cut = sc->split_cut;
   {
-    const double best = sc->solve_cut == 0 ? sc->solve_ms[1] : sc->solve_cut == L ? sc->solve_ms[0] : sc->solve_ms[2];
-    if (sc->solve_ms[3] > 0.0 && sc->solve_ms[3] < best) sc->solve_cut = -1;
+    double best = sc->solve_cut == 0 ? sc->solve_ms[1] : sc->solve_cut == L ? sc->solve_ms[0] : sc->solve_ms[2];
+    if (sc->solve_ms[3] > 0.0 && sc->solve_ms[3] < best) { sc->solve_cut = -1; best = sc->solve_ms[3]; }
+    if (sc->solve_ms[4] > 0.0 && sc->solve_ms[4] < best) sc->solve_cut = -2;
   }
   RC(tune_solve_select(sc));
   invalidate_graphs(sc);
@@ -2024,7 +2158,7 @@ int dfem_profile_levels(dfem_scene* sc, int32_t reps, int32_t cap, int32_t* n_se
 
 int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms) {
   if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
-  if (request < -1 || request > 4) return fail(DFEM_ERR_INVALID, "request must be -1, 0, 1, 2, 3 or 4");
+  if (request < -1 || request > 5) return fail(DFEM_ERR_INVALID, "request must be -1, 0, 1, 2, 3, 4 or 5");
   CK(cudaSetDevice(sc->device));
   if (request == 0) {
     CK(cudaStreamSynchronize(sc->stream));
@@ -2034,7 +2168,8 @@ int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms
   } else if (request > 0) {
     if (request == 3 && sc->split_cut == 0) return fail(DFEM_ERR_INVALID, "no split form (fewer than two levels)");
     if (request == 4 && !sc->cluster_ok) return fail(DFEM_ERR_INVALID, "no cluster form for this factor");
-    const int c = request == 1 ? n_levels(sc) : request == 2 ? 0 : request == 3 ? sc->split_cut : -1;
+    if (request == 5 && !sc->res_ok) return fail(DFEM_ERR_INVALID, "no resident form for this scene");
+    const int c = request == 1 ? n_levels(sc) : request == 2 ? 0 : request == 3 ? sc->split_cut : request == 4 ? -1 : -2;
     if (c != sc->solve_cut || sc->solve_select) {  // a requested form is used in every iteration
       sc->solve_cut = c;
       sc->solve_select = false;
@@ -2054,9 +2189,9 @@ int dfem_solve_select(const dfem_scene* sc, int32_t* on, double* weight_threshol
   return DFEM_OK;
 }
 
-int dfem_solve_times(const dfem_scene* sc, double* ms) {
-  if (!sc || !ms) return fail(DFEM_ERR_INVALID, "null argument");
-  for (int k = 0; k < 4; ++k) ms[k] = sc->solve_ms[k];
+int dfem_solve_times(const dfem_scene* sc, double* ms, int32_t n) {
+  if (!sc || !ms || n < 0) return fail(DFEM_ERR_INVALID, "bad argument");
+  for (int k = 0; k < std::min(n, 5); ++k) ms[k] = sc->solve_ms[k];
   return DFEM_OK;
 }
 

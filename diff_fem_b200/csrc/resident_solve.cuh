@@ -1,0 +1,241 @@
+// resident_solve.cuh — the global solve with the whole factor resident in the
+// distributed shared memory of one thread-block cluster.
+//
+// A small factor (a single scene of up to a few MB of blocks) is split over
+// the C CTAs of one cluster (C = 16 where the device allows it): every
+// supernode has an owner CTA that holds its diagonal-block inverse and its
+// below-diagonal block in shared memory for the whole launch, loaded at the
+// start by one bulk copy per CTA from a per-CTA image in global memory.  The
+// sweeps walk the levels of the elimination tree with a cluster barrier
+// between levels; the forward sweep pushes a supernode's contributions
+// L_{R,s} y_s straight into the shared-memory inbox of the supernode owning
+// each destination row (st.shared::cluster), the backward sweep pulls the
+// ancestors' solution values x_R from their owners' shared memory
+// (ld.shared::cluster).  A chain step is a hardware cluster barrier plus the
+// supernode's dense work in shared memory, instead of a completion stamp
+// polled through L2 and the re-staging of the blocks.
+//
+// Every sum runs in the order of fwd_supernode / bwd_supernode (pd_kernels.cu):
+// contributions per row in their grouped order, diagonal-block products one
+// thread per row in increasing k, panel products one thread per row in
+// increasing column (forward) or per column lanes over rows and a warp sum
+// (backward).  The results are bit-identical to the other solve forms.
+#pragma once
+// included after pd_kernels.cu (warp_sum, cluster_rank, cluster_sync_all)
+#include "kernels.cuh"
+
+namespace dfem {
+
+// One supernode of the resident solve; offsets in doubles from the owner
+// CTA's dynamic shared memory.
+struct ResSn {
+  int c0, w, r;      // first column, width, rows below
+  int dofs;          // Dinv, packed lower triangle by rows (row i at dofs + i (i + 1) / 2)
+  int lofs;          // L_{R,s} (column-major, r x w)
+  int pofs;          // row -> contribution range of its inbox (w + 1 ints)
+  int qofs;          // inbox: 3 doubles per contribution to its rows, grouped by row
+  int yofs;          // its solution values (3 per column)
+  int rofs;          // its below-diagonal rows in the factor's rowidx (the cdst / xsrc tables)
+  int s;             // supernode id (error reports)
+};
+
+struct ResDev {
+  const ResSn* sn;          // grouped by owner CTA, then by level
+  const int* sched;         // C x (L + 1): CTA q's items of level l are sn[sched[q (L+1) + l] .. sched[q (L+1) + l + 1])
+  const int2* cdst;         // per below-diagonal row position: (CTA, shared offset) of its contribution slot
+  const int2* xsrc;         // per below-diagonal row position: (CTA, shared offset) of the row's solution values
+  const double* img;        // every CTA's image (blocks and row tables), back to back
+  const long long* img_ofs; // C + 1 offsets into img (doubles, even)
+  const int* tsh_ofs;       // per CTA: scratch t (3 w_max) and, after it, x_R (3 r_max)
+  int nlev;
+  int smem_doubles;         // dynamic shared memory of every CTA (doubles)
+  int* status;              // error status word (as FactorDev::status)
+};
+
+__device__ __forceinline__ uint32_t cluster_map(const void* p, unsigned rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_addr(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_cluster_f64(uint32_t addr, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+}
+__device__ __forceinline__ double ld_cluster_f64(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(addr) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void res_fail(const ResDev& d, int s, int which) {
+  d.status[0] = 6;
+  d.status[1] = s;
+  d.status[2] = which;
+  atomicAdd(d.status + 3, 1);
+}
+
+// Forward solve of one supernode (order of fwd_supernode).
+__device__ __forceinline__ void res_forward(const ResDev& d, const ResSn& in, double* sh, double* t) {
+  const int w = in.w, r = in.r, tid = threadIdx.x, nt = blockDim.x;
+  const double* D = sh + in.dofs;
+  const double* L = sh + in.lofs;
+  const int* prow = reinterpret_cast<const int*>(sh + in.pofs);
+  const double* q = sh + in.qofs;
+  double* ysh = sh + in.yofs;  // holds rhs_s on entry
+  for (int c = tid; c < w; c += nt) {
+    double a0 = ysh[3 * c], a1 = ysh[3 * c + 1], a2 = ysh[3 * c + 2];
+    for (int k = prow[c]; k < prow[c + 1]; ++k) { a0 -= q[3 * k]; a1 -= q[3 * k + 1]; a2 -= q[3 * k + 2]; }
+    t[3 * c] = a0; t[3 * c + 1] = a1; t[3 * c + 2] = a2;
+  }
+  __syncthreads();
+  for (int c = tid; c < w; c += nt) {
+    double a0 = 0, a1 = 0, a2 = 0;
+    const double* Dc = D + (size_t)c * (c + 1) / 2;
+#pragma unroll 4
+    for (int k = 0; k <= c; ++k) {
+      const double dv = Dc[k];
+      a0 += dv * t[3 * k]; a1 += dv * t[3 * k + 1]; a2 += dv * t[3 * k + 2];
+    }
+    ysh[3 * c] = a0; ysh[3 * c + 1] = a1; ysh[3 * c + 2] = a2;
+  }
+  __syncthreads();
+  for (int a = tid; a < r; a += nt) {
+    double a0 = 0, a1 = 0, a2 = 0;
+    int c = 0;
+    for (; c + 16 <= w; c += 16) {  // sixteen loads in flight, then the sums in column order
+      double l[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) l[j] = L[(size_t)(c + j) * r + a];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const double* yc = ysh + 3 * (c + j);
+        a0 += l[j] * yc[0]; a1 += l[j] * yc[1]; a2 += l[j] * yc[2];
+      }
+    }
+    for (; c < w; ++c) {
+      const double l = L[(size_t)c * r + a];
+      a0 += l * ysh[3 * c]; a1 += l * ysh[3 * c + 1]; a2 += l * ysh[3 * c + 2];
+    }
+    const int2 dst = d.cdst[in.rofs + a];
+    if ((unsigned)dst.x >= gridDim.x || dst.y < 0 || dst.y + 3 > d.smem_doubles) {
+      res_fail(d, in.s, 8);
+      continue;
+    }
+    const uint32_t o = cluster_map(sh + dst.y, (unsigned)dst.x);
+    st_cluster_f64(o, a0); st_cluster_f64(o + 8, a1); st_cluster_f64(o + 16, a2);
+  }
+  __syncthreads();  // t is reused by the next item
+}
+
+// Backward solve of one supernode (order of bwd_supernode).
+__device__ __forceinline__ void res_backward(const ResDev& d, const ResSn& in, double* sh, double* t, double* xr) {
+  const int w = in.w, r = in.r, tid = threadIdx.x, nt = blockDim.x;
+  const double* D = sh + in.dofs;
+  const double* L = sh + in.lofs;
+  double* ysh = sh + in.yofs;  // holds y_s of the forward sweep on entry
+  for (int a = tid; a < r; a += nt) {
+    const int2 src = d.xsrc[in.rofs + a];
+    if ((unsigned)src.x >= gridDim.x || src.y < 0 || src.y + 3 > d.smem_doubles) {
+      res_fail(d, in.s, 9);
+      xr[3 * a] = xr[3 * a + 1] = xr[3 * a + 2] = 0.0;
+      continue;
+    }
+    const uint32_t o = cluster_map(sh + src.y, (unsigned)src.x);
+    xr[3 * a] = ld_cluster_f64(o); xr[3 * a + 1] = ld_cluster_f64(o + 8); xr[3 * a + 2] = ld_cluster_f64(o + 16);
+  }
+  for (int k = tid; k < 3 * w; k += nt) t[k] = ysh[k];
+  __syncthreads();
+  const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  for (int c = warp; c < w; c += nw) {
+    double a0 = 0, a1 = 0, a2 = 0;
+    const double* Lc = L + (size_t)c * r;
+    for (int a = lane; a < r; a += 32) {
+      const double l = Lc[a];
+      a0 += l * xr[3 * a]; a1 += l * xr[3 * a + 1]; a2 += l * xr[3 * a + 2];
+    }
+    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+    if (lane == 0) { t[3 * c] -= a0; t[3 * c + 1] -= a1; t[3 * c + 2] -= a2; }
+  }
+  __syncthreads();
+  for (int c = tid; c < w; c += nt) {
+    double a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll 4
+    for (int k = c; k < w; ++k) {
+      const double dv = D[(size_t)k * (k + 1) / 2 + c];
+      a0 += dv * t[3 * k]; a1 += dv * t[3 * k + 1]; a2 += dv * t[3 * k + 2];
+    }
+    ysh[3 * c] = a0; ysh[3 * c + 1] = a1; ysh[3 * c + 2] = a2;
+  }
+  __syncthreads();
+}
+
+// Both sweeps in one launch of one cluster (grid = cluster = C CTAs).  Every
+// CTA takes every cluster barrier, whatever happens to its own work, so the
+// barriers always complete; a bounded wait that gives up records status 6 and
+// the CTA skips its arithmetic (the solve's result is then invalid, and the
+// caller reports DFEM_ERR_CAP).
+__global__ void __launch_bounds__(512, 1) k_solve_resident(ResDev d, Gate gate, const double* __restrict__ rhs,
+                                                           double* y) {
+  extern __shared__ __align__(16) double sh[];
+  __shared__ __align__(8) uint64_t bar;
+  if (gate.skip(0)) return;  // uniform over the cluster: before any barrier
+  const unsigned rank = cluster_rank();
+  const int L1 = d.nlev + 1;
+  const int* sched = d.sched + (size_t)rank * L1;
+  const long long i0 = d.img_ofs[rank], i1 = d.img_ofs[rank + 1];
+  const unsigned bytes = (unsigned)((i1 - i0) * sizeof(double));
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    if (bytes > 0) {
+      mbar_expect_tx(&bar, bytes);
+      bulk_copy_g2s(sh, d.img + i0, bytes, &bar);
+    }
+  }
+  // rhs of the owned columns into their solution regions
+  for (int it = sched[0]; it < sched[d.nlev]; ++it) {
+    const ResSn in = d.sn[it];
+    for (int k = threadIdx.x; k < 3 * in.w; k += blockDim.x) sh[in.yofs + k] = rhs[3 * (size_t)in.c0 + k];
+  }
+  cluster_sync_all();  // every CTA of the cluster runs: its shared memory may be written
+  const bool ok = __syncthreads_and(bytes == 0 || mbar_wait_bounded(&bar, 0)) != 0;
+  if (!ok && threadIdx.x == 0) res_fail(d, -1, 7);
+  double* t = sh + d.tsh_ofs[rank];
+  double* xr = sh + d.tsh_ofs[rank + (int)gridDim.x];
+  for (int l = 0; l < d.nlev; ++l) {
+    if (ok)
+      for (int it = sched[l]; it < sched[l + 1]; ++it) res_forward(d, d.sn[it], sh, t);
+    cluster_sync_all();  // the level's contributions have landed in their owners' inboxes
+  }
+  for (int l = d.nlev - 1; l >= 0; --l) {
+    if (ok)
+      for (int it = sched[l]; it < sched[l + 1]; ++it) res_backward(d, d.sn[it], sh, t, xr);
+    cluster_sync_all();  // the level's solution values are final; no CTA reads another's after the last one
+  }
+  if (ok) {
+    for (int it = sched[0]; it < sched[d.nlev]; ++it) {
+      const ResSn in = d.sn[it];
+      for (int k = threadIdx.x; k < 3 * in.w; k += blockDim.x) y[3 * (size_t)in.c0 + k] = sh[in.yofs + k];
+    }
+  } else if (threadIdx.x == 0 && bytes > 0) {
+    mbar_wait_bounded(&bar, 0);  // give the image copy one more bounded chance to land before the CTA exits
+  }
+}
+
+// Copy of the factor's blocks (device arrays of the refactorisation) into the
+// resident images: one CTA per supernode, after every refactorisation.
+struct ResPack {
+  int w, r;
+  int src_d, src_l;      // Dinv (row-major w x w) and Lcm (column-major r x w) offsets in the factor arrays
+  long long dst_d, dst_l; // offsets in the image array
+};
+
+__global__ void k_res_pack(const ResPack* __restrict__ pk, const double* __restrict__ Dinv, const double* __restrict__ Lcm,
+                           double* img) {
+  const ResPack p = pk[blockIdx.x];
+  for (int k = threadIdx.x; k < p.w * p.w; k += blockDim.x) {  // the lower triangle, packed by rows
+    const int i = k / p.w, j = k - i * p.w;
+    if (j <= i) img[p.dst_d + (size_t)i * (i + 1) / 2 + j] = Dinv[p.src_d + k];
+  }
+  for (int k = threadIdx.x; k < p.r * p.w; k += blockDim.x) img[p.dst_l + k] = Lcm[p.src_l + k];
+}
+
+}  // namespace dfem

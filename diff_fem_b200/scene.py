@@ -147,6 +147,37 @@ class SceneDesc:
         return d, keep
 
 
+def save_npz(desc: SceneDesc, path: str) -> None:
+    """Every field of a scene descriptor into one compressed .npz file."""
+    import dataclasses as _dc
+    out = {}
+    for f in _dc.fields(desc):
+        v = getattr(desc, f.name)
+        if v is None:
+            continue
+        out[f.name] = np.asarray(v)
+    np.savez_compressed(path, **out)
+
+
+def load_npz(path: str) -> SceneDesc:
+    """A scene descriptor written by save_npz."""
+    import dataclasses as _dc
+    z = np.load(path, allow_pickle=False)
+    kw = {}
+    for f in _dc.fields(SceneDesc):
+        if f.name not in z.files:
+            continue
+        v = z[f.name]
+        if v.ndim == 0:
+            v = v.item()
+            if f.name in ("handle_collision", "self_collision", "underwater"):
+                v = bool(v)
+        elif f.name == "gravity":
+            v = tuple(float(t) for t in v)
+        kw[f.name] = v
+    return SceneDesc(**kw)
+
+
 # ------------------------------------------------------------------ meshes ---
 
 # 5-tet split of the unit cube; corners indexed by (i, j, k) bits.  Parity 0

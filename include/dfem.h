@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define DFEM_ABI_VERSION 3
+#define DFEM_ABI_VERSION 4
 
 enum dfem_status {
   DFEM_OK = 0,
@@ -260,18 +260,23 @@ int dfem_host_factor_solve(const dfem_scene_desc *desc, const double *b, double 
  * claimed in dependency order), 3 split (the levels below the autotuned cut
  * level as level kernels, the rest in one persistent launch), 4 cluster
  * (one thread-block cluster walks the levels, a cluster barrier between
- * levels; tried for factors of up to 4096 supernodes); a form requested with
- * 1-4 is used in every iteration (no per-iteration selection, see
+ * levels; tried for factors of up to 4096 supernodes), 5 resident (single
+ * scenes whose factor fits the shared memory of one thread-block cluster of
+ * up to 16 CTAs: every block stays in shared memory for the launch,
+ * contributions and solution values move between the CTAs over distributed
+ * shared memory, a cluster barrier between levels); a form requested with
+ * 1-5 is used in every iteration (no per-iteration selection, see
  * dfem_solve_select).  *chosen (may
- * be NULL) receives the form in use (1-4), ms (may be NULL, 2 values)
+ * be NULL) receives the form in use (1-5), ms (may be NULL, 2 values)
  * the last autotune's time per solve of forms 1 and 2.  Every form runs the
  * same arithmetic per supernode: results are identical.  No counterpart in
  * the reference (its solve is Eigen's SimplicialLDLT, sim/fem/World.h:1660). */
 int dfem_solve_mode(dfem_scene *scene, int32_t request, int32_t *chosen, double *ms);
 
 /* The last autotune's time per solve (ms) of the level-kernel, persistent,
- * best split and cluster forms (0: not timed). */
-int dfem_solve_times(const dfem_scene *scene, double *ms);
+ * best split, cluster and resident forms (0: not timed); writes the first
+ * min(n, 5) of them. */
+int dfem_solve_times(const dfem_scene *scene, double *ms, int32_t n);
 
 /* The split form found by the last autotune: *cut_level (0: none), the
  * factor's number of levels, and its time per solve (ms). */

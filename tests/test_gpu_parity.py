@@ -458,3 +458,37 @@ def test_checkpoints_every_k_steps_give_identical_gradients(case, budget):
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     for key in out[0][2]:
         assert np.array_equal(out[0][2][key], out[1][2][key]), key
+
+
+@pytest.mark.parametrize("name,pre", [("bridgesus", 0), ("baymax", 20), ("cloth_ball", 68), ("octopus", 0)])
+def test_reference_data_scenes_forward_and_adjoint(name, pre):
+    """Four of diff_fem's own data scenes (tests/golden/ref_scenes, written by
+    make_ref_scenes.py from its data directory): 10 steps forward and adjoint
+    against the oracle.  baymax and cloth_ball start from the oracle's state
+    `pre` steps in, a few steps before their first contact, so the window
+    holds contact passes (baymax: the ground obstacle; cloth_ball: soft-soft
+    contact with the ball)."""
+    import os
+    d = S.load_npz(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_scenes", name + ".npz"))
+    x = d.x0.reshape(-1).copy()
+    v = np.tile([0.3, 0.0, 0.0], d.n_vertices) if d.underwater else np.zeros_like(x)
+    o = O.OracleScene(d)
+    if pre:
+        r = o.forward(x, v, n_steps=pre)
+        x, v = r["x"], r["v"]
+    rng = np.random.default_rng(21)
+    act = rng.uniform(0, 1, (10, d.n_segments)) if d.n_segments else None
+    g = Scene(d)
+    xg, vg, tg = g.forward(x, v, n_steps=10, act=act, traj=True)
+    ro = o.forward(x, v, n_steps=10, act=act, traj=True)
+    if name in ("baymax", "cloth_ball"):
+        assert o.contact_passes().sum() > 0
+        assert np.array_equal(g.contact_passes(10), o.contact_passes())
+    assert np.array_equal(g.iterations(10), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    assert rel(vg, ro["v"]) < POS_TOL
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    bg, bo = g.backward(gx, gv), o.backward(gx, gv)
+    for k in ("x", "v", "E") + (("act",) if d.n_segments else ()):
+        assert rel(bg[k], bo[k]) < GRAD_TOL, (k, rel(bg[k], bo[k]))
+    g.close()

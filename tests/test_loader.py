@@ -9,7 +9,9 @@ from diff_fem_b200.engine import host_factor_solve
 from oracle import oracle as O
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REF_DATA = "/root/reference/data"
+# diff_fem's data directory, when available (the tests reading it skip otherwise;
+# tests/golden/ref_scenes holds four of its scenes as descriptors)
+REF_DATA = os.environ.get("DIFF_FEM_DATA", "")
 
 
 def test_fixture_scene_loads():
@@ -38,7 +40,7 @@ def test_surface_extraction_and_orientation():
         assert np.dot(n, x0[f].mean(axis=0) - c) > 0
 
 
-@pytest.mark.skipif(not os.path.exists(REF_DATA), reason="reference data not mounted")
+@pytest.mark.skipif(not REF_DATA or not os.path.isdir(REF_DATA), reason="DIFF_FEM_DATA not set")
 def test_reference_scenes_load():
     """The reference's own data scenes (read in place, not copied)."""
     d = loader.load_scene("bridgesus/bridgesus.json", 3, data_root=REF_DATA).desc
@@ -54,7 +56,7 @@ def test_reference_scenes_load():
     assert np.all(c.desc.spring_weight == 200.0) and not c.desc.gravity_mask[c.bodies[1].offset:].any()
 
 
-@pytest.mark.skipif(not os.path.exists(REF_DATA), reason="reference data not mounted")
+@pytest.mark.skipif(not REF_DATA or not os.path.isdir(REF_DATA), reason="DIFF_FEM_DATA not set")
 def test_reference_underwater_scene_loads():
     """octopus.json sets "Is underwater": its mesh gets drag and lift on its
     outward surface faces instead of gravity; the oracle steps it.  (fish.json
@@ -69,3 +71,36 @@ def test_reference_underwater_scene_loads():
     assert np.all(np.isfinite(r["x"]))
     mom0 = 0.3 * d.mass.sum()
     assert (d.mass * r["v"].reshape(-1, 3)[:, 0]).sum() < mom0   # the water slows it
+
+
+@pytest.mark.skipif(not REF_DATA or not os.path.isdir(REF_DATA), reason="DIFF_FEM_DATA not set")
+def test_reference_scene_fixtures_match_the_data():
+    """tests/golden/ref_scenes/*.npz are what the loader makes of the data scenes."""
+    import dataclasses
+    for name, rel, n in [("bridgesus", "bridgesus/bridgesus.json", 3), ("baymax", "baymax/baymax.json", 3),
+                         ("cloth_ball", "cloth_ball/cloth_ball.json", 3), ("octopus", "octopus/octopus.json", 2)]:
+        a = loader.load_scene(rel, n, data_root=REF_DATA).desc
+        b = S.load_npz(os.path.join(GOLDEN, "ref_scenes", name + ".npz"))
+        for f in dataclasses.fields(a):
+            u, w = getattr(a, f.name), getattr(b, f.name)
+            if u is None or w is None:
+                assert u is None and w is None, (name, f.name)
+            elif isinstance(u, np.ndarray):
+                assert np.array_equal(u, w), (name, f.name)
+            else:
+                assert u == w, (name, f.name)
+
+
+def test_reference_scene_fixtures_step_in_the_oracle():
+    """The four data-scene fixtures (bridgesus: attachments of stiffness 1e20;
+    baymax: ground contact; cloth_ball: a cloth and a ball with self-collision;
+    octopus: underwater drag) run forward and backward in the oracle."""
+    for name in ("bridgesus", "baymax", "cloth_ball", "octopus"):
+        d = S.load_npz(os.path.join(GOLDEN, "ref_scenes", name + ".npz"))
+        o = O.OracleScene(d)
+        x = d.x0.reshape(-1).copy()
+        v = np.tile([0.3, 0.0, 0.0], d.n_vertices) if d.underwater else np.zeros_like(x)
+        r = o.forward(x, v, n_steps=3)
+        assert np.all(np.isfinite(r["x"])), name
+        b = o.backward(np.ones_like(x), np.zeros_like(x))
+        assert np.all(np.isfinite(b["x"])), name

@@ -2,10 +2,11 @@
 
 diff_fem ships no tests, golden vectors or output fixtures, and cannot be
 built here, so the oracle is pinned by known-answer invariants of the
-reference's algorithm, central finite differences of the hand-written
-adjoint, and the committed golden fixtures in tests/golden/ (generated by
-tests/golden/make_golden.py from the oracle itself, so later changes to the
-oracle are caught).
+reference's algorithm (rest state, free fall, the projection's rules, the
+kron structure of L, the soft-contact exchange's conservation laws) and by
+central finite differences of the hand-written adjoint.  tests/golden/ holds
+scene inputs in the reference's file formats (written by
+tests/golden/make_fixtures.py), not oracle outputs.
 """
 import dataclasses
 

@@ -1,9 +1,10 @@
 """The forms of the global solve (one launch per elimination-tree level, one
 persistent launch whose CTAs claim supernodes in dependency order, level
-kernels below a cut level and the persistent launch above it, or one
-thread-block cluster walking the levels) run the same
-arithmetic per supernode, so a step, its gradient and a batch agree bit for
-bit whichever form the autotuner picked."""
+kernels below a cut level and the persistent launch above it, one
+thread-block cluster walking the levels, or one cluster holding the whole
+factor in its distributed shared memory) run the same arithmetic per
+supernode, so a step, its gradient and a batch agree bit for bit whichever
+form the autotuner picked."""
 import dataclasses
 
 import numpy as np
@@ -30,12 +31,14 @@ def test_persistent_solve_matches_level_kernels(builder):
          "muscle_beam": S.muscle_beam, "cloth_sheet": lambda: S.cloth_sheet(nv=12)}[builder]()
     sc = Scene(d)
     info = sc.solve_mode()
-    assert info["mode"] in ("levels", "persistent", "split", "cluster") and info["ms_levels"] > 0 and info["ms_persistent"] > 0
+    assert info["mode"] in ("levels", "persistent", "split", "cluster", "resident")
+    assert info["ms_levels"] > 0 and info["ms_persistent"] > 0
     assert info["split_level"] > 0 and info["ms_split"] > 0  # these factors have more than one level
     assert info["ms_cluster"] > 0  # few supernodes: the cluster form is a candidate
+    assert info["ms_resident"] > 0  # small factors: the resident form is a candidate
     act = np.random.default_rng(1).uniform(0, 1, (4, d.n_segments)) if d.n_segments else None
     a = run(sc, d, 4, "levels", act)
-    for form in ("persistent", "split", "cluster"):
+    for form in ("persistent", "split", "cluster", "resident"):
         b = run(sc, d, 4, form, act)
         for u, w in zip(a[:2], b[:2]):
             assert np.array_equal(u, w), form
@@ -80,4 +83,21 @@ def test_batch_tail_selection_matches_fixed_form():
     gb = sc.backward(rng.standard_normal(x.size), rng.standard_normal(x.size))
     for k in ga:
         assert np.array_equal(ga[k], gb[k]), k
+    sc.close()
+
+
+def test_resident_solve_on_the_inverse_stiffness_beam():
+    """The 12,800-tet beam (213 supernodes, 10 levels): its factor fits the
+    shared memory of one 16-CTA cluster; 6 steps forward and adjoint agree bit
+    for bit with the persistent form."""
+    d = S.inverse_stiffness()
+    sc = Scene(d)
+    info = sc.solve_mode()
+    assert info["ms_resident"] > 0
+    a = run(sc, d, 6, "persistent")
+    b = run(sc, d, 6, "resident")
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    for k in a[2]:
+        assert np.array_equal(a[2][k], b[2][k]), k
+    assert np.array_equal(a[3], b[3])
     sc.close()
