@@ -13,6 +13,13 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdfem.so")
 
 DFEM_OK = 0
+DFEM_ERR_INVALID = 1
+DFEM_ERR_CUDA = 2
+DFEM_ERR_FACTOR = 3
+DFEM_ERR_NONFINITE = 4
+DFEM_ERR_STATE = 5
+DFEM_ERR_CAP = 6
+DFEM_ERR_NOMEM = 7
 DFEM_MEM_HOST = 0
 DFEM_MEM_DEVICE = 1
 DFEM_PREC_FP64 = 0
@@ -91,6 +98,8 @@ SIGNATURES = [
     ("dfem_synchronize", C.c_int, [_VP]),
     ("dfem_last_error", C.c_char_p, []),
     ("dfem_abi_version", C.c_int, []),
+    ("dfem_set_limit", C.c_int, [_VP, C.c_int32, C.c_int64]),
+    ("dfem_debug_fail_allocations", C.c_int, [C.c_int64]),
 ]
 
 _lib = None

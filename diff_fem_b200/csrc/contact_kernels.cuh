@@ -37,6 +37,12 @@ __global__ void k_contact_record(const int* step, const int* state, int* rec, Co
   }
 }
 
+// A cap was reached: status[0] = DFEM_ERR_CAP, status[2] = which (kCap*); the
+// first error of the call is the one reported.
+__device__ __forceinline__ void cap_reached(int* status, int which) {
+  if (atomicCAS(status, 0, 6) == 0) atomicExch(status + 2, which);
+}
+
 // record index of the current computed iteration (-1: not recording or no room)
 __device__ __forceinline__ int rec_index(const ContactDev& c) {
   if (!c.rec_on || *c.rec_on == 0) return -1;
@@ -277,7 +283,7 @@ __global__ void k_contact_detect(ContactDev c, const double* xt, const double* x
     for (int q = 0; q < cnt; ++q)
       if (c.imp_face[a * kMaxImpactsPerVertex + q] == f) slot = q;
     if (slot < 0) {
-      if (cnt >= kMaxImpactsPerVertex) { atomicExch(status, 6); continue; }
+      if (cnt >= c.max_impacts) { cap_reached(status, kCapImpacts); continue; }
       slot = cnt;
       c.imp_face[a * kMaxImpactsPerVertex + slot] = f;
       c.imp_cnt[a] = cnt + 1;
@@ -331,8 +337,8 @@ __global__ void k_self_detect(ContactDev c, const double* xt, const double* xk, 
         for (int q = 0; q < cnt; ++q)
           if (c.simp_face[base + q] == fh) { slot = q; break; }
         if (slot < 0) {
-          if (cnt >= kMaxSelfImpacts) {
-            atomicExch(status, 6);
+          if (cnt >= c.max_self_impacts) {
+            cap_reached(status, kCapSoftImpacts);
           } else {
             slot = cnt;
             c.simp_face[base + slot] = fh;
@@ -354,7 +360,12 @@ __global__ void k_self_detect(ContactDev c, const double* xt, const double* xk, 
 __global__ void k_contact_ctl_detect(ContactDev c, cudaGraphConditionalHandle h) {
   if (c.state[CS_MODE] != 0) return;
   const bool same_groups = c.ncf == 0 || c.state[CS_NGRP] == c.state[CS_NGRP_PREV];
-  if ((c.state[CS_ANY] == 0 && same_groups) || c.state[CS_PASS] >= c.max_passes) {
+  if (c.state[CS_ANY] == 0 && same_groups) {
+    cudaGraphSetConditional(h, 0u);
+    return;
+  }
+  if (c.state[CS_PASS] >= c.max_passes) {  // new impacts, but no pass left: the phase ends with an error
+    cap_reached(c.status, kCapContactPasses);
     cudaGraphSetConditional(h, 0u);
     return;
   }
@@ -553,7 +564,7 @@ __global__ void k_self_sort(ContactDev c, int* status) {
   if (f >= c.ncf) return;
   const int cnt = c.g_cnt[f];
   if (cnt == 0) return;
-  if (cnt > kMaxGroupMembers) atomicExch(status, 6);
+  if (cnt > c.max_members) cap_reached(status, kCapGroupMembers);
   int* m = c.g_mem + c.g_ptr[f];
   for (int k = 1; k < cnt; ++k) {
     const int v = m[k];

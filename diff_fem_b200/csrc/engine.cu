@@ -42,8 +42,13 @@ int report_error(int code, const std::string& msg) { return fail(code, msg); }
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \
     if (e_ != cudaSuccess)                                                                   \
-      return fail(DFEM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
+      return fail(e_ == cudaErrorMemoryAllocation ? DFEM_ERR_NOMEM : DFEM_ERR_CUDA,         \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                       \
   } while (0)
+
+// Allocation-failure injection of dfem_debug_fail_allocations: the calling
+// thread's device allocations fail once this many more have succeeded (-1: off).
+static thread_local long long g_alloc_budget = -1;
 
 #define RC(x) do { int rc_ = (x); if (rc_) return rc_; } while (0)
 
@@ -83,6 +88,8 @@ struct DBuf {
     if (p) { cudaFree(p); p = nullptr; }
     n = count;
     if (count == 0) return cudaSuccess;
+    if (g_alloc_budget == 0) { n = 0; return cudaErrorMemoryAllocation; }
+    if (g_alloc_budget > 0) --g_alloc_budget;
     return cudaMalloc(&p, count * sizeof(T));
   }
   // copies into the existing allocation when the size is unchanged, so device
@@ -236,6 +243,7 @@ struct dfem_scene {
   int nblk_v = 1;   // blocks of the vertex-parallel kernels
   SceneDev sd{};
   FactorDev fd{};
+  int spin_tries = kSpinTries;            // polls of a persistent-solve dependency wait (dfem_set_limit)
   ~dfem_scene() {
     if (g_step.exec) cudaGraphExecDestroy(g_step.exec);
     if (g_adj.exec) cudaGraphExecDestroy(g_adj.exec);
@@ -478,7 +486,7 @@ static int upload_factor(dfem_scene* sc) {
   RC(plan_resident(sc, nseg, cdst));
   FactorDev fd{sc->sn_info.p, sc->rseg_ptr.p, sc->cdst.p, sc->contrib.p, sc->rowidx.p, sc->Lcm.p, sc->Dinv.p,
                sc->DinvC.p, sc->status.p, ns, sc->sn_pos.p, sc->sn_parent.p, sc->kid_ptr.p, sc->kid.p, sc->done_f.p,
-               sc->done_b.p, sc->solve_ctl.p};
+               sc->done_b.p, sc->solve_ctl.p, sc->spin_tries};
   if (std::memcmp(&fd, &sc->fd, sizeof(fd)) != 0) invalidate_graphs(sc);
   sc->fd = fd;
   return DFEM_OK;
@@ -834,7 +842,8 @@ static int upload_scene(dfem_scene* sc) {
     CK(cudaMemset(sc->crec_on.p, 0, sizeof(int)));
     CK(sc->crec_base.alloc(1));
     CK(cudaMemset(sc->crec_base.p, 0, sizeof(int)));
-    sc->cd = ContactDev{nc, nof, s.K, kMaxContactPasses, s.alpha, s.mu_obs, sc->cverts.p, sc->cidx.p, sc->obs_x.p,
+    sc->cd = ContactDev{nc, nof, s.K, kMaxContactPasses, kMaxImpactsPerVertex, kMaxSelfImpacts, kMaxGroupMembers,
+                        s.alpha, s.mu_obs, sc->cverts.p, sc->cidx.p, sc->obs_x.p,
                         sc->obs_f.p, sc->hdiag.p, sc->imp_cnt.p, sc->imp_face.p, sc->imp_n.p, sc->xn1.p, sc->xold.p,
                         sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p, sc->crec_on.p, 0, nullptr, nullptr,
                         nullptr, nullptr, nullptr, sc->status.p, sc->crec_base.p, nullptr};
@@ -873,6 +882,12 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   if (n_steps <= sc->cap_steps) return DFEM_OK;
   const HostScene& s = sc->hs;
   int cap = std::max(n_steps, 2 * sc->cap_steps);
+  // the buffers below are reallocated in place: until all of them succeed the
+  // scene has no per-step buffers (a failed allocation leaves cap_steps = 0,
+  // so the next call allocates again) and no recorded forward
+  sc->cap_steps = 0;
+  sc->rec_steps = 0;
+  invalidate_graphs(sc);
   const size_t n3 = 3 * (size_t)s.N;
   const int kc = std::max(1, s.checkpoint_every);
   const size_t nck = ((size_t)cap + kc - 1) / kc;  // one checkpoint per kc steps
@@ -1309,9 +1324,24 @@ static int copy_out(dfem_scene* sc, const double* src, size_t n, double* dst, in
 // iterations; records 0 .. keep-1 survive a growth (the graphs hold the
 // record's pointers: rebuilt when it grows).
 static int ensure_contact_record(dfem_scene* sc, int cap, int keep = 0) {
-  if (!sc->has_contact || cap <= sc->crec_cap) return DFEM_OK;
+  if (!sc->has_contact) return DFEM_OK;
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N, nc = (size_t)sc->cd.nc, nn = nc * kMaxImpactsPerVertex * 3;
+  // the reverse sweep's buffers (sizes fixed by the scene) first: a failed
+  // allocation below then leaves the record as it was
+  for (DBuf<double>* b : {&sc->ca_xn1b, &sc->ca_pb, &sc->ca_cxtb, &sc->ca_vwcb, &sc->ca_yb, &sc->ca_orib})
+    if (!b->p) CK(b->alloc(n3));
+  if (!sc->ca_hdb.p) CK(sc->ca_hdb.alloc(std::max(1, s.N)));
+  if (sc->self_contact) {
+    const int ncf = sc->cd.ncf;
+    for (DBuf<double>* b : {&sc->ca_scb, &sc->ca_ptot, &sc->ca_sbp, &sc->ca_gPM})
+      if (!b->p) CK(b->alloc(3 * nc));
+    if (!sc->ca_gmM.p) CK(sc->ca_gmM.alloc(nc));
+    if (!sc->ca_gPF.p) CK(sc->ca_gPF.alloc(9 * (size_t)ncf));
+    if (!sc->ca_gmF.p) CK(sc->ca_gmF.alloc(3 * (size_t)ncf));
+    if (!sc->ca_xout.p) CK(sc->ca_xout.alloc(n3));
+  }
+  if (cap <= sc->crec_cap) return DFEM_OK;
   keep = std::min(keep, sc->crec_cap);
   DBuf<double> x, prev, nrm;
   DBuf<int> first, cnt;
@@ -1320,6 +1350,17 @@ static int ensure_contact_record(dfem_scene* sc, int cap, int keep = 0) {
   CK(first.alloc(cap));
   CK(cnt.alloc(nc * cap));
   CK(nrm.alloc(nn * cap));
+  DBuf<int> rsi;
+  DBuf<double> rsd;
+  if (sc->self_contact) {
+    const size_t si = self_rec_si_stride((int)nc, sc->cd.ncf), sd = self_rec_sd_stride((int)nc, sc->cd.ncf);
+    CK(rsi.alloc(si * cap));
+    CK(rsd.alloc(sd * cap));
+    if (keep > 0) {
+      CK(cudaMemcpyAsync(rsi.p, sc->crec_si.p, sizeof(int) * si * keep, cudaMemcpyDeviceToDevice, sc->stream));
+      CK(cudaMemcpyAsync(rsd.p, sc->crec_sd.p, sizeof(double) * sd * keep, cudaMemcpyDeviceToDevice, sc->stream));
+    }
+  }
   if (keep > 0) {
     CK(cudaMemcpyAsync(x.p, sc->crec_x.p, sizeof(double) * n3 * keep, cudaMemcpyDeviceToDevice, sc->stream));
     CK(cudaMemcpyAsync(prev.p, sc->crec_prev.p, sizeof(double) * n3 * keep, cudaMemcpyDeviceToDevice, sc->stream));
@@ -1333,31 +1374,11 @@ static int ensure_contact_record(dfem_scene* sc, int cap, int keep = 0) {
   sc->crec_first.swap(first);
   sc->crec_cnt.swap(cnt);
   sc->crec_n.swap(nrm);
-  for (DBuf<double>* b : {&sc->ca_xn1b, &sc->ca_pb, &sc->ca_cxtb, &sc->ca_vwcb, &sc->ca_yb, &sc->ca_orib})
-    if (!b->p) CK(b->alloc(n3));
-  if (!sc->ca_hdb.p) CK(sc->ca_hdb.alloc(std::max(1, s.N)));
   if (sc->self_contact) {
-    const int ncf = sc->cd.ncf;
-    const size_t si = self_rec_si_stride((int)nc, ncf), sd = self_rec_sd_stride((int)nc, ncf);
-    DBuf<int> rsi;
-    DBuf<double> rsd;
-    CK(rsi.alloc(si * cap));
-    CK(rsd.alloc(sd * cap));
-    if (keep > 0) {
-      CK(cudaMemcpyAsync(rsi.p, sc->crec_si.p, sizeof(int) * si * keep, cudaMemcpyDeviceToDevice, sc->stream));
-      CK(cudaMemcpyAsync(rsd.p, sc->crec_sd.p, sizeof(double) * sd * keep, cudaMemcpyDeviceToDevice, sc->stream));
-      CK(cudaStreamSynchronize(sc->stream));
-    }
     sc->crec_si.swap(rsi);
     sc->crec_sd.swap(rsd);
     sc->cd.rec_si = sc->crec_si.p;
     sc->cd.rec_sd = sc->crec_sd.p;
-    for (DBuf<double>* b : {&sc->ca_scb, &sc->ca_ptot, &sc->ca_sbp, &sc->ca_gPM})
-      if (!b->p) CK(b->alloc(3 * nc));
-    if (!sc->ca_gmM.p) CK(sc->ca_gmM.alloc(nc));
-    if (!sc->ca_gPF.p) CK(sc->ca_gPF.alloc(9 * (size_t)ncf));
-    if (!sc->ca_gmF.p) CK(sc->ca_gmF.alloc(3 * (size_t)ncf));
-    if (!sc->ca_xout.p) CK(sc->ca_xout.alloc(n3));
   }
   sc->crec_cap = cap;
   sc->cd.rec_cap = cap;
@@ -1496,6 +1517,14 @@ static int status_error(const int st4[4]) {
   if (st4[0] == DFEM_ERR_CAP && st4[2] > 0 && st4[2] <= 9)
     return fail(DFEM_ERR_CAP, std::string(what[st4[2]]) + " gave up (supernode " + std::to_string(st4[1]) + ", " +
                                   std::to_string(st4[3]) + " blocks)");
+  if (st4[0] == DFEM_ERR_CAP && st4[2] == kCapContactPasses)
+    return fail(DFEM_ERR_CAP, "the contact phase still found new impacts after its last detection pass (pass cap)");
+  if (st4[0] == DFEM_ERR_CAP && st4[2] == kCapImpacts)
+    return fail(DFEM_ERR_CAP, "a contact vertex hit more obstacle faces than the impacts kept per vertex");
+  if (st4[0] == DFEM_ERR_CAP && st4[2] == kCapSoftImpacts)
+    return fail(DFEM_ERR_CAP, "a contact vertex hit more soft faces than the soft impacts kept per vertex");
+  if (st4[0] == DFEM_ERR_CAP && st4[2] == kCapGroupMembers)
+    return fail(DFEM_ERR_CAP, "a soft-contact face group has more members than the cap");
   if (st4[0] == DFEM_ERR_CAP) return fail(DFEM_ERR_CAP, "a bounded loop gave up (contact impacts per vertex)");
   if (st4[0]) return fail(DFEM_ERR_NONFINITE, "non-finite value in the PD iteration");
   return DFEM_OK;
@@ -2264,6 +2293,45 @@ int dfem_profile_phases(dfem_scene* sc, int32_t reps, double* ms) {
   // the solve phase counted one launch per call above
   sc->launches += (int64_t)(reps + 1) * (solve_launches(sc) - 1);
   sc->rec_steps = 0;  // gates and iteration counts were overwritten: no backward of the old forward
+  return DFEM_OK;
+}
+
+int dfem_set_limit(dfem_scene* sc, int32_t which, int64_t value) {
+  if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(sc->device));
+  CK(cudaStreamSynchronize(sc->stream));
+  const bool dflt = value < 0;
+  switch (which) {
+    case DFEM_LIMIT_CONTACT_PASSES:
+    case DFEM_LIMIT_IMPACTS_PER_VERTEX:
+    case DFEM_LIMIT_SOFT_IMPACTS_PER_VERTEX:
+    case DFEM_LIMIT_GROUP_MEMBERS: {
+      const int cap = which == DFEM_LIMIT_CONTACT_PASSES ? kMaxContactPasses
+                      : which == DFEM_LIMIT_IMPACTS_PER_VERTEX ? kMaxImpactsPerVertex
+                      : which == DFEM_LIMIT_SOFT_IMPACTS_PER_VERTEX ? kMaxSelfImpacts : kMaxGroupMembers;
+      if (!dflt && value > cap) return fail(DFEM_ERR_INVALID, "limit above the built-in cap " + std::to_string(cap));
+      const int v = dflt ? cap : (int)value;
+      ContactDev& c = sc->cd;
+      (which == DFEM_LIMIT_CONTACT_PASSES ? c.max_passes : which == DFEM_LIMIT_IMPACTS_PER_VERTEX ? c.max_impacts
+       : which == DFEM_LIMIT_SOFT_IMPACTS_PER_VERTEX ? c.max_self_impacts : c.max_members) = v;
+      break;
+    }
+    case DFEM_LIMIT_SOLVE_WAIT_POLLS:
+      if (!dflt && (value < 1 || value > kSpinTries))
+        return fail(DFEM_ERR_INVALID, "poll limit must be in [1, " + std::to_string(kSpinTries) + "]");
+      sc->spin_tries = dflt ? kSpinTries : (int)value;
+      sc->fd.spin_tries = sc->spin_tries;
+      break;
+    default:
+      return fail(DFEM_ERR_INVALID, "unknown limit");
+  }
+  invalidate_graphs(sc);  // the kernels' parameters changed
+  sc->rec_steps = 0;
+  return DFEM_OK;
+}
+
+int dfem_debug_fail_allocations(int64_t after) {
+  g_alloc_budget = after < 0 ? -1 : after;
   return DFEM_OK;
 }
 

@@ -127,8 +127,15 @@ __device__ __forceinline__ int cons_part(const SceneDev& d, int t) {
 constexpr int kMaxImpactsPerVertex = 8;  // a vertex at a corner of a tessellated obstacle touches up to 6 faces
 constexpr int kMaxContactPasses = 64;       // the reference's detection loop has no cap
 constexpr double kContactThickness = 1e-4;  // arcsim Impact::thickness
+// Status word codes of the caps (status[2] when status[0] == DFEM_ERR_CAP); the
+// solves use 1-9 (pd_kernels.cu, resident_solve.cuh).
+enum { kCapContactPasses = 10, kCapImpacts = 11, kCapSoftImpacts = 12, kCapGroupMembers = 13 };
+
 struct ContactDev {
   int nc, nof, K, max_passes;
+  int max_impacts;        // obstacle impacts kept per vertex (<= kMaxImpactsPerVertex)
+  int max_self_impacts;   // soft impacts kept per vertex (<= kMaxSelfImpacts)
+  int max_members;        // members of one face group (<= kMaxGroupMembers)
   double alpha, mu;
   const int* cverts;      // contact vertices (internal ids)
   const int* cidx;        // N: contact index or -1
@@ -229,6 +236,7 @@ struct FactorDev {
   int* done_f;
   int* done_b;
   int* ctl;      // [ticket, CTAs finished, epoch, abort]
+  int spin_tries;  // polls of a persistent-solve dependency wait before it gives up
 };
 
 }  // namespace dfem

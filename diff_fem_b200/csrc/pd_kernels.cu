@@ -787,7 +787,8 @@ __global__ void __launch_bounds__(256) k_bwd_level(FactorDev f, int lvl_begin, i
 // root.  Every awaited item has a lower ticket, and a CTA's claimed but
 // unstarted ticket is higher than its current one, so the lowest unfinished
 // ticket is always running with its dependencies done: the waits always end.
-// They are bounded all the same (kSpinTries polls): a CTA that gives up
+// They are bounded all the same (FactorDev::spin_tries polls, kSpinTries
+// unless lowered by dfem_set_limit): a CTA that gives up
 // records status 6 and raises the abort word, and every CTA then stops
 // claiming.  Completion is an epoch stamp per supernode and direction
 // (release store after the CTA's writes; acquire loads by the waiter).
@@ -807,8 +808,8 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 }
 
 // Bounded wait until *flag == epoch; false on abort or when the bound is reached.
-__device__ __forceinline__ bool wait_epoch(const int* flag, int epoch, const int* abort_word) {
-  for (int i = 0; i < kSpinTries; ++i) {
+__device__ __forceinline__ bool wait_epoch(const int* flag, int epoch, const int* abort_word, int tries) {
+  for (int i = 0; i < tries; ++i) {
     if (ld_acquire(flag) == epoch) return true;
     if ((i & 63) == 63) {
       if (ld_acquire(abort_word) != 0) return false;
@@ -859,11 +860,11 @@ __global__ void __launch_bounds__(256) k_solve_persistent(FactorDev f, int p0, G
         if (fwd) {
           for (int k = f.kid_ptr[s]; ok && k < f.kid_ptr[s + 1]; ++k) {
             const int kid = f.kid[k];
-            if (f.sn_pos[kid] >= p0) ok = wait_epoch(f.done_f + kid, epoch, ctl + 3);
+            if (f.sn_pos[kid] >= p0) ok = wait_epoch(f.done_f + kid, epoch, ctl + 3, f.spin_tries);
           }
         } else {
           const int p = f.sn_parent[s];
-          ok = wait_epoch(p >= 0 ? f.done_b + p : f.done_f + s, epoch, ctl + 3);
+          ok = wait_epoch(p >= 0 ? f.done_b + p : f.done_f + s, epoch, ctl + 3, f.spin_tries);
         }
         if (!ok) {
           if (ld_acquire(ctl + 3) == 0) record_gave_up(f, s, fwd ? 3 : 4);

@@ -226,6 +226,15 @@ class Scene:
         return {"fwd_ms": list(f), "bwd_ms": list(b), "supernodes": list(cnt), "level": list(lvl),
                 "threads_fwd": list(thr)[0::2], "threads_bwd": list(thr)[1::2]}
 
+    LIMITS = {"contact_passes": 0, "impacts_per_vertex": 1, "soft_impacts_per_vertex": 2, "group_members": 3,
+              "solve_wait_polls": 4}
+
+    def set_limit(self, which: str, value: int = -1):
+        """Lower one of the engine's caps for this scene (value < 0: the
+        built-in cap again); a call that reaches it raises DfemError with
+        DFEM_ERR_CAP.  See dfem_set_limit."""
+        check(lib().dfem_set_limit(self._h, self.LIMITS[which], int(value)))
+
     def set_adjoint_budget(self, nbytes: int):
         """Device memory for storing every step's iterates (the adjoint then replays no step)."""
         check(lib().dfem_set_adjoint_budget(self._h, int(nbytes)))

@@ -22,6 +22,11 @@ import numpy as np
 from . import scene as S
 
 
+class SceneFormatError(ValueError):
+    """A scene file (JSON, OBJ or muscle file) that cannot be read: the message
+    names the file and, for line-based files, the line."""
+
+
 def _resolve(path: str, root: Optional[str]) -> str:
     if os.path.isabs(path) and os.path.exists(path):
         return path
@@ -36,18 +41,32 @@ def read_obj(path: str, scale: float = 1.0):
     """Vertices, 't' tetrahedra (0-based, OBJMesh) and 'f' triangles (1-based in the file)."""
     v, t, f = [], [], []
     with open(path) as fh:
-        for line in fh:
+        for ln, line in enumerate(fh, 1):
             p = line.split()
             if not p:
                 continue
-            if p[0] == "v":
-                v.append([float(p[1]), float(p[2]), float(p[3])])
-            elif p[0] == "t":
-                t.append([int(p[1]), int(p[2]), int(p[3]), int(p[4])])
-            elif p[0] == "f":
-                f.append([int(q.split("/")[0]) - 1 for q in p[1:4]])
-    return (np.asarray(v, np.float64).reshape(-1, 3) * scale, np.asarray(t, np.int32).reshape(-1, 4),
-            np.asarray(f, np.int32).reshape(-1, 3))
+            try:
+                if p[0] == "v":
+                    v.append([float(p[1]), float(p[2]), float(p[3])])
+                elif p[0] == "t":
+                    t.append([int(p[1]), int(p[2]), int(p[3]), int(p[4])])
+                elif p[0] == "f":
+                    f.append([int(q.split("/")[0]) - 1 for q in p[1:4]])
+                    if len(f[-1]) != 3:
+                        raise IndexError
+            except (ValueError, IndexError):
+                raise SceneFormatError(f"{path}:{ln}: malformed '{p[0]}' line: {line.strip()!r}") from None
+    V = np.asarray(v, np.float64).reshape(-1, 3)
+    T = np.asarray(t, np.int32).reshape(-1, 4)
+    F = np.asarray(f, np.int32).reshape(-1, 3)
+    if V.shape[0] == 0:
+        raise SceneFormatError(f"{path}: no vertices")
+    if not np.all(np.isfinite(V)):
+        raise SceneFormatError(f"{path}: non-finite vertex coordinates")
+    for name, a in (("tet", T), ("face", F)):
+        if a.size and (a.min() < 0 or a.max() >= V.shape[0]):
+            raise SceneFormatError(f"{path}: {name} vertex index out of range [0, {V.shape[0]})")
+    return V * scale, T, F
 
 
 # ------------------------------------------------------------------- muscles ---
@@ -123,16 +142,20 @@ def muscle_constraints_from_fibres(x0, tets, fibres, stiffness, n_sampling=50):
 def read_muscle_file(path: str, scale: float):
     fibres, cur, cur_id = [], [], None
     with open(path) as fh:
-        for line in fh:
+        for ln, line in enumerate(fh, 1):
             p = line.split()
             if len(p) < 5:
                 continue
-            fid = int(p[0])
+            try:
+                fid = int(p[0])
+                pt = [float(p[2]) * scale, float(p[3]) * scale, float(p[4]) * scale]
+            except ValueError:
+                raise SceneFormatError(f"{path}:{ln}: malformed muscle row: {line.strip()!r}") from None
             if cur_id is not None and fid != cur_id:
                 fibres.append(np.asarray(cur))
                 cur = []
             cur_id = fid
-            cur.append([float(p[2]) * scale, float(p[3]) * scale, float(p[4]) * scale])
+            cur.append(pt)
     if cur:
         fibres.append(np.asarray(cur))
     return fibres
@@ -161,7 +184,16 @@ class LoadedScene:
 
 
 def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] = None) -> LoadedScene:
-    cfg = json.load(open(_resolve(config_path, data_root)))
+    path = _resolve(config_path, data_root)
+    try:
+        with open(path) as fh:
+            cfg = json.load(fh)
+    except json.JSONDecodeError as ex:
+        raise SceneFormatError(f"{path}: invalid JSON: {ex}") from None
+    if not isinstance(cfg, dict) or not isinstance(cfg.get("Parameters"), list) or not cfg["Parameters"]:
+        raise SceneFormatError(f"{path}: no \"Parameters\" list")
+    if not cfg.get("Meshes") and not cfg.get("Clothes"):
+        raise SceneFormatError(f"{path}: no \"Meshes\" or \"Clothes\"")
     par = cfg["Parameters"][0]
     hz = int(par.get("Simulation HZ", 200))
     xs, masses, gmask = [], [], []
@@ -184,6 +216,8 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
         if "Attach Verts" in obj:
             k = float(obj["Attach Stiffness"])
             for i in sorted(set(int(q) for q in obj["Attach Verts"])):
+                if not 0 <= i < n:
+                    raise SceneFormatError(f"{path}: attach vertex {i} out of range [0, {n})")
                 av.append(off + i); ap.append(v[i]); ak.append(k)
         faces, cv = S.surface_of(v, t)
         cverts.extend((cv + off).tolist()); cfaces.extend((faces + off).tolist())
@@ -208,6 +242,8 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
         if "Attach Verts" in obj:
             k = float(obj["Attach Stiffness"])
             for i in sorted(set(int(q) for q in obj["Attach Verts"])):
+                if not 0 <= i < n:
+                    raise SceneFormatError(f"{path}: attach vertex {i} out of range [0, {n})")
                 av.append(off + i); ap.append(v[i]); ak.append(k)
         seen = set()
         for tri in f:

@@ -319,6 +319,35 @@ int dfem_get_launch_count(const dfem_scene *scene, int64_t *count);
  * local step.  Instrumentation (diff_fem's TIMER_* macros, sim/utils/timer.h). */
 int dfem_profile_phases(dfem_scene *scene, int32_t reps, double *ms);
 
+/* Bounds of the engine's capped loops and waits, lowered for a scene (tests
+ * of the failure paths, or a caller that wants a tighter bound); value < 0
+ * restores the built-in cap, values above it are rejected.  When a bound is
+ * reached the call that met it returns DFEM_ERR_CAP (the kernels finish
+ * normally; the handle stays usable) and its results are not valid.
+ *   DFEM_LIMIT_CONTACT_PASSES           detection passes of a step's contact
+ *                                       phase that may still find new impacts
+ *                                       (0..64; the reference's loop is uncapped,
+ *                                       sim/fem/World.h:928-1022)
+ *   DFEM_LIMIT_IMPACTS_PER_VERTEX       obstacle faces a contact vertex may hit (0..8)
+ *   DFEM_LIMIT_SOFT_IMPACTS_PER_VERTEX  soft faces a contact vertex may hit in a step (0..16)
+ *   DFEM_LIMIT_GROUP_MEMBERS            members of one soft-contact face group (0..32)
+ *   DFEM_LIMIT_SOLVE_WAIT_POLLS         polls of a dependency wait of the persistent
+ *                                       solve form (1..2^22)
+ * No counterpart in the reference. */
+enum dfem_limit {
+  DFEM_LIMIT_CONTACT_PASSES = 0,
+  DFEM_LIMIT_IMPACTS_PER_VERTEX = 1,
+  DFEM_LIMIT_SOFT_IMPACTS_PER_VERTEX = 2,
+  DFEM_LIMIT_GROUP_MEMBERS = 3,
+  DFEM_LIMIT_SOLVE_WAIT_POLLS = 4
+};
+int dfem_set_limit(dfem_scene *scene, int32_t which, int64_t value);
+
+/* Failure injection for tests: the calling thread's device allocations by the
+ * engine fail (DFEM_ERR_NOMEM) once `after` more have succeeded; after < 0
+ * turns it off.  Thread-local; no counterpart in the reference. */
+int dfem_debug_fail_allocations(int64_t after);
+
 /* Synchronise the scene's stream. */
 int dfem_synchronize(dfem_scene *scene);
 

@@ -104,3 +104,42 @@ def test_reference_scene_fixtures_step_in_the_oracle():
         assert np.all(np.isfinite(r["x"])), name
         b = o.backward(np.ones_like(x), np.zeros_like(x))
         assert np.all(np.isfinite(b["x"])), name
+
+
+def _write(tmp_path, name, text):
+    p = tmp_path / name
+    p.write_text(text)
+    return str(p)
+
+
+def test_corrupt_scene_files_raise_clear_errors(tmp_path):
+    """Malformed JSON, a JSON without bodies, OBJ files with bad lines or
+    indices, a malformed muscle row and an attachment out of range are
+    refused with SceneFormatError naming the file (and line)."""
+    good_obj = "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 0 0 1\nt 0 1 2 3\n"
+    obj = _write(tmp_path, "m.obj", good_obj)
+
+    count = [0]
+
+    def scene(mesh, extra=""):
+        count[0] += 1
+        return _write(tmp_path, "s%d.json" % count[0],
+                      '{"Parameters": [{"Simulation HZ": 100}], "Meshes": [{"Obj filename": "%s"%s}]}' % (mesh, extra))
+
+    cases = [
+        (_write(tmp_path, "bad.json", '{"Parameters": [{"Simulation HZ": 100}], '), "invalid JSON"),
+        (_write(tmp_path, "empty.json", '{"Parameters": [{}]}'), "Meshes"),
+        (scene(_write(tmp_path, "a.obj", good_obj + "v 1 x 0\n")), "a.obj:6"),
+        (scene(_write(tmp_path, "b.obj", good_obj + "t 0 1 2\n")), "b.obj:6"),
+        (scene(_write(tmp_path, "c.obj", good_obj + "t 0 1 2 9\n")), "out of range"),
+        (scene(_write(tmp_path, "d.obj", "t 0 1 2 3\n")), "no vertices"),
+        (scene(obj, ', "Attach Verts": [7], "Attach Stiffness": 1e8'), "attach vertex 7"),
+        (scene(obj, ', "Muscle filename": "%s"' % _write(tmp_path, "m.muscle", "0 0 0.1 0.1 0.1\n0 1 nan? 0 0\n")),
+         "m.muscle:2"),
+    ]
+    for path, what in cases:
+        with pytest.raises(loader.SceneFormatError) as ex:
+            loader.load_scene(path, 1)
+        assert what in str(ex.value), (what, str(ex.value))
+    with pytest.raises(FileNotFoundError):
+        loader.load_scene(str(tmp_path / "missing.json"), 1)
