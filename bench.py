@@ -354,7 +354,9 @@ def batch_config(args, descs) -> dict:
         "scenes": len(descs), "tets_total": int(sum(T)), "vertices_total": int(sum(d.n_vertices for d in descs)),
         "tets_min": int(min(T)), "tets_max": int(max(T)), "sim_steps_per_bench_step": SIM_STEPS,
         **({} if SIM_STEPS == 100 else {"note": "reduced time steps: profiler capture only, not a bench value"}),
-        "precision": args.precision, "parallelism": "one batch handle per GPU (replicas)",
+        "precision": args.precision,
+        "parallelism": "scenes split across the GPUs by longest-processing-time placement; one batch handle "
+                       "per GPU holding its share (no collective inside a step)",
     }
 
 
@@ -368,6 +370,7 @@ def run_batch(args):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    from diff_fem_b200 import shard
     if world > 1:
         import torch.distributed as dist
         from datetime import timedelta
@@ -375,15 +378,25 @@ def run_batch(args):
     dev = torch.device("cuda", local)
     prec = DFEM_PREC_FP64 if args.precision == "fp64" else DFEM_PREC_MIXED
     t0 = time.perf_counter()
-    descs, _ = S.uneven_batch(n_scenes=args.scenes, precision=prec)
+    all_descs, _ = S.uneven_batch(n_scenes=args.scenes, precision=prec)
+    # the scenes split across the ranks by longest-processing-time placement on
+    # their tet counts (shard.assign_scenes: every rank computes the same split);
+    # each rank builds one batch handle of its own share, no data-path collective
+    costs = [d.n_tets for d in all_descs]
+    placement = shard.assign_scenes(costs, world)
+    mine = placement[rank]
+    descs = [all_descs[i] for i in mine]
     b = Scene.batch(descs, device=local)
     t_setup = time.perf_counter() - t0
     n = SIM_STEPS
     x0 = torch.tensor(np.concatenate([d.x0.reshape(-1) for d in descs]), device=dev)
     v0 = torch.zeros_like(x0)
+    # activations of every scene of the job (seed 42), then this rank's columns
     rng = np.random.default_rng(42)
-    act_np = rng.uniform(0.0, 1.0, (n, b.nseg))
-    act = torch.tensor(act_np, device=dev)
+    seg0 = np.concatenate([[0], np.cumsum([d.n_segments for d in all_descs])]).astype(int)
+    act_all = rng.uniform(0.0, 1.0, (n, int(seg0[-1])))
+    act_np = np.concatenate([act_all[:, seg0[i]:seg0[i + 1]] for i in mine], axis=1) if mine else act_all[:, :0]
+    act = torch.tensor(np.ascontiguousarray(act_np), device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -413,8 +426,9 @@ def run_batch(args):
         t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t.item())
-    value = world * len(descs) * n * args.steps / elapsed
+    value = len(all_descs) * n * args.steps / elapsed  # every rank's scenes over the slowest rank's time
     iters = b.iterations(n)
+    loads = [float(sum(costs[i] for i in p)) for p in placement]
 
     # forward-only rate
     torch.cuda.synchronize()
@@ -423,7 +437,7 @@ def run_batch(args):
     b.forward(x0, v0, n_steps=n, act=act)
     ef1.record(stream)
     torch.cuda.synchronize()
-    fwd_rate = len(descs) * n / (ef0.elapsed_time(ef1) / 1e3)
+    fwd_rate = len(descs) * n / (ef0.elapsed_time(ef1) / 1e3)  # this rank's
 
     # end to end with host buffers (pinned), copies inside the timed region
     x0_h = x0.cpu().pin_memory()
@@ -438,7 +452,11 @@ def run_batch(args):
         _ = float(np.sum(gh["E"])) + float(np.sum(gh["act"]))
         t_e2e += time.perf_counter() - t1
     N3, T, nseg = 3 * b.N, b.T, b.nseg
-    e2e = {"value": world * len(descs) * n * args.steps / t_e2e, "unit": "scene-steps/s",
+    if world > 1:
+        t = torch.tensor([t_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = {"value": len(all_descs) * n * args.steps / t_e2e, "unit": "scene-steps/s",
            "h2d_bytes_per_step": 8 * (2 * N3 + n * nseg + 2 * N3),
            "d2h_bytes_per_step": 8 * (2 * N3 + 2 * N3 + 2 * T + n * nseg)}
 
@@ -449,8 +467,8 @@ def run_batch(args):
     # per-scene error of this run against the FP64 batch (same scenes, same inputs)
     errs = None
     if prec == DFEM_PREC_MIXED:
-        d64, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_FP64)
-        b64 = Scene.batch(d64, device=local)
+        d64_all, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_FP64)
+        b64 = Scene.batch([d64_all[i] for i in mine], device=local)
         x64, v64 = b64.forward(x0, v0, n_steps=n, act=act)
         g64 = b64.backward(2.0 * (x64 - x0), torch.zeros_like(x64))
         vo, to, so = b.offsets["vertices"], b.offsets["tets"], b.offsets["segments"]
@@ -489,7 +507,8 @@ def run_batch(args):
     # plain FP64 form, scenes one at a time (a sample spread over the size range)
     plain = None
     if args.fp64_sample != 0:
-        d64, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_FP64)
+        d64_all, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_FP64)
+        d64 = [d64_all[i] for i in mine]
         k = len(d64) if args.fp64_sample < 0 else min(args.fp64_sample, len(d64))
         idx = np.linspace(0, len(d64) - 1, k).astype(int)
         tsum, tets = 0.0, 0
@@ -536,9 +555,14 @@ def run_batch(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
-            "config": dict(batch_config(args, descs), l2="flushed between timed steps (256 MB write)",
+            "config": dict(batch_config(args, all_descs), l2="flushed between timed steps (256 MB write)",
                            setup_s=t_setup),
-            "forward_only_scene_steps_per_s": world * fwd_rate, "pd_iterations_total": int(iters.max(axis=1).sum()),
+            "forward_only_scene_steps_per_s": world * fwd_rate if world == 1 else None,
+            "placement": {"scenes_per_rank": [len(p) for p in placement], "tets_per_rank": loads,
+                          "imbalance_max_over_mean": max(loads) / (sum(loads) / world) if sum(loads) else 1.0,
+                          "rule": "longest-processing-time on tet counts (diff_fem_b200.shard.assign_scenes)",
+                          "measured_on_hardware": world == 1 or "yes (this run)"},
+            "pd_iterations_total": int(iters.max(axis=1).sum()),
             "solve": b.solve_mode(), "phase_ms": phases, "factor": {"supernodes": binfo["n_supernodes"],
                                                                    "levels": binfo["n_levels"],
                                                                    "nnz": int(binfo["nnz_factor"])},

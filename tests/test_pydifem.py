@@ -52,6 +52,46 @@ def test_sim_act_gradient_wrt_actions(env):
     assert tau.grad is not None and torch.isfinite(tau.grad).all()
 
 
+def test_sim_act_tau_gradient_matches_central_differences(env):
+    """dL/dtau through sim_act (Normalizer::NormToReal, Muscle::SetActivationLevels
+    propagation, the step's activation adjoint) against central differences of
+    forward_act along a random direction; the environment's phase and
+    activation levels are reset before every evaluation."""
+    import torch
+    from diff_fem_b200 import pydifem as pd
+    from diff_fem_b200.api_diff import sim_act
+    n_act = sum(o.mActions.size for o in env.mDfobjs)
+    phase0 = env.mPhase
+    levels0 = [o.GetActivationLevelsAggregate() for o in env.mDfobjs]
+    x0 = env.mSoftWorld.mX.copy()
+    v0 = 0.05 * np.random.default_rng(3).standard_normal(x0.size)
+
+    def reset():
+        env.mPhase = phase0
+        for o, lv in zip(env.mDfobjs, levels0):
+            o.SetActivationLevelsAggregate(lv)
+
+    def loss(tau):
+        reset()
+        x, _, _, _ = pd.forward_act(x0, v0, [], [], tau, env, True)
+        return float((x.reshape(-1, 3)[:, 0] ** 2).sum())
+
+    tau0 = np.random.default_rng(4).uniform(-1.0, 1.0, n_act)
+    reset()
+    q = torch.tensor(x0, dtype=torch.float64)
+    qd = torch.tensor(v0, dtype=torch.float64)
+    tau = torch.tensor(tau0, dtype=torch.float64, requires_grad=True)
+    jq = torch.zeros(0, dtype=torch.float64)
+    qn, _, _, _ = sim_act(q, qd, jq, jq, tau, env, True)
+    (qn.reshape(-1, 3)[:, 0] ** 2).sum().backward()
+    g = tau.grad.numpy()
+    assert np.abs(g).max() > 0
+    d = np.random.default_rng(5).standard_normal(n_act)
+    eps = 1e-4
+    fd = (loss(tau0 + eps * d) - loss(tau0 - eps * d)) / (2 * eps)
+    assert abs(g @ d - fd) <= 1e-5 * max(abs(fd), 1e-12), (g @ d, fd)
+
+
 def test_sim_all_gradient_matches_finite_difference(env):
     import torch
     from diff_fem_b200 import pydifem as pd
