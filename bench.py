@@ -30,6 +30,12 @@ sys.path.insert(0, ROOT)
 
 SIM_STEPS = 60
 METRIC = "fwd+adjoint sim steps/s (inverse stiffness 12,800 tets, K=20)"
+
+# DRAM bytes per launch of the global solve on the inverse-stiffness workload,
+# by solve form, from one ncu capture each (dram__bytes_read.sum +
+# dram__bytes_write.sum; the factor is largely L2-resident between solves, so
+# this is below the algorithmic bytes).  Not measured by a bench run.
+SOLVE_DRAM_BYTES = {"persistent": 4.36e6}
 UNIT = "steps/s"
 
 
@@ -47,6 +53,8 @@ def parse():
                         "star: the muscle star on the ground, gradient w.r.t. all activations; "
                         "cloth_ball: a 64x64 cloth dropped on a ball, gradient w.r.t. the initial velocities")
     p.add_argument("--scenes", type=int, default=256, help="batch workload: number of scenes")
+    p.add_argument("--no-north-star", action="store_true",
+                   help="skip the mixed/FP64 and batched/one-at-a-time comparison of the default line")
     p.add_argument("--fp64-sample", type=int, default=-1,
                    help="batch workload: scenes stepped one at a time in FP64 for the plain-form rate "
                         "(-1: every scene of the batch, 0: skip)")
@@ -305,14 +313,12 @@ def run_ours(args):
     else:
         achieved = local_bytes / (ph[dom] * 1e-3) / 1e9
         traffic_note = f"per {dom} launch"
-    # DRAM bytes per launch of the persistent solve on this workload, from one ncu capture
-    # (dram__bytes_read.sum 4.36 MB + dram__bytes_write.sum 0 per launch; the factor is
-    # mostly L2-resident, so DRAM traffic is below the algorithmic bytes)
     solve_info = sc.solve_mode()
-    traffic = 4.36e6 if (dom == "solve" and solve_info["mode"] == "persistent" and SIM_STEPS == 60) else None
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": traffic,
-                "traffic_source": "ncu capture of k_solve_persistent (profiles/k_solve_persistent_inverse_stiffness_12800tets.md)"
+    traffic = SOLVE_DRAM_BYTES.get(solve_info["mode"]) if (dom == "solve" and SIM_STEPS == 60) else None
+    roofline = {"bound": "hbm", "kernel": dom, "solve_form": solve_info["mode"], "achieved": achieved, "peak": hbm,
+                "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch from one earlier ncu "
+                                  "capture of this solve form on this workload (not measured by this run)"
                 if traffic else None, "peak_source": peak_note,
                 "algorithmic_bytes": solve_bytes if dom == "solve" else local_bytes, "per": traffic_note,
                 "phase_ms": ph, "phase_share_ms_per_bench_step": share}
@@ -332,11 +338,173 @@ def run_ours(args):
             line["cpu_baseline"] = oracle_sample(1, 2)
         except Exception as ex:  # the baseline must not kill the GPU line
             line["cpu_baseline"] = {"value": None, "error": str(ex)}
+    sc.close()
+    if rank == 0 and world == 1 and not args.no_north_star:
+        try:
+            line["north_star"] = north_star_extras(args, local)
+        except Exception as ex:  # the comparison must not kill the GPU line
+            line["north_star"] = {"error": f"{type(ex).__name__}: {ex}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    sc.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------------ north star ---
+
+def _rel(a, b) -> float:
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def north_star_extras(args, local: int) -> dict:
+    """The comparison the metric names: mixed FP32/FP64 against plain FP64,
+    batched against one scene at a time, each with its error.
+    (1) The 12,800-tet inverse-stiffness problem in both precisions, each
+        against the FP64 oracle on the host (same moduli and target, 60 steps
+        forward + adjoint): positions x_60 and dL/dE.
+    (2) The 256-scene uneven batch (100 steps forward + adjoint): batched mixed,
+        batched FP64, and plain FP64 one scene per handle on a stratified
+        sample of 16 scenes; errors of the mixed batch against the FP64 batch.
+    Timed with CUDA events on the engine's stream, L2 flushed between timed
+    evaluations; a few evaluations each (the headline value above is the
+    long-run number)."""
+    import torch
+    from diff_fem_b200 import scene as S
+    from diff_fem_b200._capi import DFEM_PREC_FP64, DFEM_PREC_MIXED
+    from diff_fem_b200.engine import Scene
+    from oracle import oracle as O
+
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def timed(fn, reps, warm=1):
+        out = None
+        for _ in range(warm):
+            out = fn()
+        tot = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1) / 1e3
+        return tot / max(1, reps), out
+
+    res = {}
+    # (1) inverse stiffness, FP64 and mixed against the oracle
+    n = 60
+    d64 = S.inverse_stiffness()
+    T = d64.n_tets
+    Et = S.log_uniform_moduli(T, 5678)
+    x0 = d64.x0.reshape(-1).copy()
+    v0 = np.zeros_like(x0)
+    threads = os.cpu_count() or 1
+    o = O.OracleScene(d64)
+    o.set_materials(Et, d64.poisson)
+    tgt = o.forward(x0, v0, n_steps=n, threads=threads)["x"]
+    o.set_materials(d64.youngs, d64.poisson)
+    ro = o.forward(x0, v0, n_steps=n, threads=threads)
+    bo = o.backward(2.0 * (ro["x"] - tgt), np.zeros_like(x0))
+    c2 = {}
+    for name, prec in (("fp64", DFEM_PREC_FP64), ("mixed", DFEM_PREC_MIXED)):
+        d = S.inverse_stiffness(precision=prec)
+        sc = Scene(d, device=local)
+        E0 = torch.tensor(d.youngs, device=dev)
+        nu = torch.tensor(d.poisson, device=dev)
+        xt, vt, tg = (torch.tensor(a, device=dev) for a in (x0, v0, tgt))
+
+        def grad_eval():
+            sc.set_materials(E0, nu)
+            x, _ = sc.forward(xt, vt, n_steps=n)
+            g = sc.backward(2.0 * (x - tg), torch.zeros_like(x))
+            return x, g["E"]
+
+        t, (x, gE) = timed(grad_eval, 3)
+        c2[name] = {"value": n / t, "unit": "steps/s", "solve": sc.solve_mode()["mode"],
+                    "pos_rel_err_vs_oracle": _rel(x.cpu().numpy(), ro["x"]),
+                    "grad_E_rel_err_vs_oracle": _rel(gE.cpu().numpy(), bo["E"])}
+        sc.close()
+    c2["mixed_over_fp64"] = c2["mixed"]["value"] / c2["fp64"]["value"]
+    c2["workload"] = "inverse stiffness 12,800 tets, 60 steps forward + adjoint dL/dE incl. refactorisation"
+    c2["oracle"] = f"FP64 C++ oracle on the host ({threads} threads), same moduli and target"
+    res["inverse_stiffness"] = c2
+
+    # (2) the uneven batch: batched mixed, batched FP64, plain FP64 one at a time
+    nb = 100
+    dm, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_MIXED)
+    dd, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_FP64)
+    xb = torch.tensor(np.concatenate([d.x0.reshape(-1) for d in dm]), device=dev)
+    vb = torch.zeros_like(xb)
+    nseg = sum(d.n_segments for d in dm)
+    act = torch.tensor(np.random.default_rng(42).uniform(0.0, 1.0, (nb, nseg)), device=dev)
+    out = {}
+    for name, descs, reps in (("mixed", dm, 2), ("fp64", dd, 1)):
+        t0 = time.perf_counter()
+        b = Scene.batch(descs, device=local)
+        setup = time.perf_counter() - t0
+
+        def batch_eval():
+            x, _ = b.forward(xb, vb, n_steps=nb, act=act)
+            return x, b.backward(2.0 * (x - xb), torch.zeros_like(x))
+
+        t, (x, g) = timed(batch_eval, reps)
+        out[name] = {"value": len(descs) * nb / t, "unit": "scene-steps/s", "setup_s": setup,
+                     "x": x.cpu().numpy(), "E": g["E"].cpu().numpy(), "act": g["act"].cpu().numpy(),
+                     "iters": b.iterations(nb), "offsets": b.offsets}
+        b.close()
+    # plain FP64, one scene per handle: a sample stratified by size
+    order = np.argsort([d.n_tets for d in dd], kind="stable")
+    sample = order[np.linspace(0, len(dd) - 1, min(16, len(dd))).astype(int)]
+    vo, so = out["fp64"]["offsets"]["vertices"], out["fp64"]["offsets"]["segments"]
+    tsum = 0.0
+    for q in sample:
+        sc = Scene(dd[q], device=local)
+        xq = xb[3 * vo[q]:3 * vo[q + 1]].contiguous()
+        aq = act[:, so[q]:so[q + 1]].contiguous() if so[q + 1] > so[q] else None
+
+        def one():
+            x, _ = sc.forward(xq, torch.zeros_like(xq), n_steps=nb, act=aq)
+            return sc.backward(2.0 * (x - xq), torch.zeros_like(x))
+
+        t, _ = timed(one, 1)
+        tsum += t
+        sc.close()
+    plain = len(sample) * nb / tsum
+    # errors of the mixed batch against the FP64 batch, per scene
+    to = out["fp64"]["offsets"]["tets"]
+    same = np.all(out["mixed"]["iters"] == out["fp64"]["iters"], axis=0)
+    pe, ge = [], []
+    for p in range(len(dd)):
+        a0, a1 = 3 * vo[p], 3 * vo[p + 1]
+        pe.append(_rel(out["mixed"]["x"][a0:a1], out["fp64"]["x"][a0:a1]))
+        ge.append(_rel(out["mixed"]["E"][to[p]:to[p + 1]], out["fp64"]["E"][to[p]:to[p + 1]]))
+    pe, ge = np.asarray(pe), np.asarray(ge)
+    res["batch"] = {
+        "workload": f"{len(dd)} uneven scenes (tets log-uniform in [1e3, 5e4], beams and muscle stars), "
+                    f"{nb} steps forward + adjoint",
+        "mixed_batched": {"value": out["mixed"]["value"], "unit": "scene-steps/s", "setup_s": out["mixed"]["setup_s"]},
+        "fp64_batched": {"value": out["fp64"]["value"], "unit": "scene-steps/s", "setup_s": out["fp64"]["setup_s"]},
+        "fp64_one_at_a_time": {"value": plain, "unit": "scene-steps/s", "scenes_sampled": int(len(sample)),
+                               "sample": "16 scenes evenly spaced in size order, one handle each"},
+        "mixed_batched_over_fp64_one_at_a_time": out["mixed"]["value"] / plain,
+        "fp64_batched_over_fp64_one_at_a_time": out["fp64"]["value"] / plain,
+        "mixed_over_fp64_batched": out["mixed"]["value"] / out["fp64"]["value"],
+        "error_mixed_vs_fp64": {
+            "scenes_with_equal_iteration_counts": int(same.sum()), "scenes": int(len(dd)),
+            "pos_rel_max": float(pe[same].max()) if same.any() else None,
+            "pos_rel_median": float(np.median(pe[same])) if same.any() else None,
+            "grad_E_rel_max": float(ge[same].max()) if same.any() else None,
+            "grad_E_rel_median": float(np.median(ge[same])) if same.any() else None,
+            "grad_act_rel_max": _rel(out["mixed"]["act"], out["fp64"]["act"]),
+            "other_scenes_pos_rel_max": float(pe[~same].max()) if (~same).any() else None},
+        "target": ">= 10x batched mixed over plain FP64, at <= 1e-6 position and <= 1e-4 gradient error",
+    }
+    return res
 
 
 # ------------------------------------------------------------ batch (C5) ---
