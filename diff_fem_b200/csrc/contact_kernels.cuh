@@ -266,7 +266,48 @@ __global__ void k_contact_begin(SceneDev d, ContactDev c, const double* xt, cons
   }
 }
 
-// Detection pass (mode 0): every contact vertex against every obstacle face.
+__device__ __forceinline__ int bp_cell(const ContactDev& c, double v, int k) {
+  const double u = floor((v - c.bp_org[k]) * c.bp_inv);
+  return u < 0.0 ? 0 : (u >= (double)(c.bp_dim[k] - 1) ? c.bp_dim[k] - 1 : (int)u);
+}
+
+// Candidate obstacle faces of the swept box [lo, hi] from the grid, ascending
+// and without repeats; false when the box covers too many cells or gathers
+// too many faces (the caller then tests every face).
+__device__ __forceinline__ bool bp_candidates(const ContactDev& c, Vec3<double> lo, Vec3<double> hi, int* cand, int* ncand) {
+  if (c.bp_max_cells <= 0 || c.bp_dim[0] <= 0) return false;
+  const double l[3] = {lo.x - kBroadPad, lo.y - kBroadPad, lo.z - kBroadPad};
+  const double h[3] = {hi.x + kBroadPad, hi.y + kBroadPad, hi.z + kBroadPad};
+  int i0[3], i1[3];
+  long long cells = 1;
+  for (int k = 0; k < 3; ++k) {
+    i0[k] = bp_cell(c, l[k], k);
+    i1[k] = bp_cell(c, h[k], k);
+    cells *= (long long)(i1[k] - i0[k] + 1);
+  }
+  if (cells > c.bp_max_cells) return false;
+  int n = 0;
+  for (int z = i0[2]; z <= i1[2]; ++z)
+    for (int y = i0[1]; y <= i1[1]; ++y)
+      for (int x = i0[0]; x <= i1[0]; ++x) {
+        const int cell = (z * c.bp_dim[1] + y) * c.bp_dim[0] + x;
+        for (int k = c.bp_ptr[cell]; k < c.bp_ptr[cell + 1]; ++k) {
+          const int f = c.bp_face[k];
+          int j = n;  // insertion into the ascending list, repeats dropped
+          while (j > 0 && cand[j - 1] > f) --j;
+          if (j > 0 && cand[j - 1] == f) continue;
+          if (n == kBroadMaxCandidates) return false;
+          for (int q = n; q > j; --q) cand[q] = cand[q - 1];
+          cand[j] = f;
+          ++n;
+        }
+      }
+  *ncand = n;
+  return true;
+}
+
+// Detection pass (mode 0): every contact vertex against the obstacle faces
+// (the broad phase's candidates, or all of them), in ascending face order.
 __global__ void k_contact_detect(ContactDev c, const double* xt, const double* xk, int* status) {
   if (c.state[CS_MODE] != 0) return;
   int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,7 +315,13 @@ __global__ void k_contact_detect(ContactDev c, const double* xt, const double* x
   int gv = c.cverts[a];
   Vec3<double> p0 = ld3(xt, gv), p1 = ld3(xk, gv);
   bool any = false;
-  for (int f = 0; f < c.nof; ++f) {
+  int cand[kBroadMaxCandidates];
+  int ncand = 0;
+  const bool culled = bp_candidates(c, mk3(fmin(p0.x, p1.x), fmin(p0.y, p1.y), fmin(p0.z, p1.z)),
+                                    mk3(fmax(p0.x, p1.x), fmax(p0.y, p1.y), fmax(p0.z, p1.z)), cand, &ncand);
+  const int nf = culled ? ncand : c.nof;
+  for (int k = 0; k < nf; ++k) {
+    const int f = culled ? cand[k] : k;
     Vec3<double> n;
     const int* fv = c.obs_f + 3 * f;
     if (!vf_impact(p0, p1, ld3(c.obs_x, fv[0]), ld3(c.obs_x, fv[1]), ld3(c.obs_x, fv[2]), 1.0, &n)) continue;

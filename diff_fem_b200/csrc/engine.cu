@@ -201,6 +201,7 @@ struct dfem_scene {
   // obstacle contact phase
   bool has_contact = false;
   DBuf<int> cverts, cidx, obs_f, imp_cnt, imp_face, cstate, cpasses;
+  DBuf<int> bp_ptr, bp_face;             // broad phase of the obstacle detection
   DBuf<double> obs_x, hdiag, imp_n, xn1, xold, cprev, lxt, vwc;
   // soft-soft contact (forward only: the adjoint refuses these scenes)
   bool self_contact = false;
@@ -715,6 +716,101 @@ static int gpu_refactor(dfem_scene* sc) {
   return fail(DFEM_ERR_FACTOR, "Cholesky factorisation failed after 25 regularisation retries");
 }
 
+// Uniform grid over the static obstacle faces for the detection's broad phase
+// (the reference rebuilds an arcsim BVH over them at every detection,
+// sim/utils/arcsim/collision.cpp:29-37): cell size twice the median extent of
+// a face box, grown until the grid has at most 2^20 cells; every face listed,
+// in ascending order, in every cell that its box dilated by kBroadPad touches.
+// Cells are located with the same monotone formula as bp_cell on the device,
+// so a vertex's query (its swept box, dilated alike) meets every face whose
+// dilated box it overlaps: the culling drops no impact.  No grid (every face
+// is tested) for fewer than 16 faces or more than 2^24 cell entries.
+static int build_obstacle_grid(dfem_scene* sc) {
+  const HostScene& s = sc->hs;
+  ContactDev& c = sc->cd;
+  const int nof = (int)s.obs_f.size() / 3;
+  c.bp_max_cells = kBroadDefaultCells;
+  c.bp_dim[0] = c.bp_dim[1] = c.bp_dim[2] = 0;
+  c.bp_ptr = nullptr;
+  c.bp_face = nullptr;
+  if (nof < 16) return DFEM_OK;
+  std::vector<double> lo(3 * (size_t)nof), hi(3 * (size_t)nof), ext(nof);
+  double glo[3] = {1e300, 1e300, 1e300}, ghi[3] = {-1e300, -1e300, -1e300};
+  for (int f = 0; f < nof; ++f) {
+    double e = 0.0;
+    for (int k = 0; k < 3; ++k) {
+      double a = 1e300, b = -1e300;
+      for (int q = 0; q < 3; ++q) {
+        const double v = s.obs_x[3 * (size_t)s.obs_f[3 * f + q] + k];
+        a = std::min(a, v);
+        b = std::max(b, v);
+      }
+      e = std::max(e, b - a);
+      lo[3 * f + k] = a - kBroadPad;
+      hi[3 * f + k] = b + kBroadPad;
+      glo[k] = std::min(glo[k], lo[3 * f + k]);
+      ghi[k] = std::max(ghi[k], hi[3 * f + k]);
+    }
+    ext[f] = e;
+  }
+  std::vector<double> se(ext);
+  std::nth_element(se.begin(), se.begin() + nof / 2, se.end());
+  const double diag = std::sqrt((ghi[0] - glo[0]) * (ghi[0] - glo[0]) + (ghi[1] - glo[1]) * (ghi[1] - glo[1]) +
+                                (ghi[2] - glo[2]) * (ghi[2] - glo[2]));
+  double h = std::max({2.0 * se[nof / 2], 1e-6 * diag, 1e-9});
+  int dim[3];
+  for (;;) {
+    long long cells = 1;
+    for (int k = 0; k < 3; ++k) {
+      dim[k] = std::max(1, (int)std::ceil((ghi[k] - glo[k]) / h));
+      cells *= dim[k];
+    }
+    if (cells <= (1 << 20)) break;
+    h *= 1.26;
+  }
+  const double inv = 1.0 / h;
+  auto cell = [&](double v, int k) {  // bp_cell on the device
+    const double u = std::floor((v - glo[k]) * inv);
+    return u < 0.0 ? 0 : (u >= (double)(dim[k] - 1) ? dim[k] - 1 : (int)u);
+  };
+  const size_t ncell = (size_t)dim[0] * dim[1] * dim[2];
+  std::vector<int> ptr(ncell + 1, 0);
+  size_t total = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    std::vector<int> fill;
+    std::vector<int> face;
+    if (pass == 1) {
+      for (size_t q = 0; q < ncell; ++q) ptr[q + 1] += ptr[q];
+      fill.assign(ptr.begin(), ptr.end() - 1);
+      face.resize(ptr[ncell]);
+    }
+    for (int f = 0; f < nof; ++f) {
+      int i0[3], i1[3];
+      for (int k = 0; k < 3; ++k) { i0[k] = cell(lo[3 * f + k], k); i1[k] = cell(hi[3 * f + k], k); }
+      for (int z = i0[2]; z <= i1[2]; ++z)
+        for (int y = i0[1]; y <= i1[1]; ++y)
+          for (int x = i0[0]; x <= i1[0]; ++x) {
+            const size_t q = ((size_t)z * dim[1] + y) * dim[0] + x;
+            if (pass == 0) {
+              ptr[q + 1]++;
+              if (++total > (size_t)(1 << 24)) return DFEM_OK;  // too many entries: no grid
+            } else {
+              face[fill[q]++] = f;
+            }
+          }
+    }
+    if (pass == 1) {
+      CK(sc->bp_ptr.upload(ptr));
+      CK(sc->bp_face.upload(face.empty() ? std::vector<int>{0} : face));
+    }
+  }
+  for (int k = 0; k < 3; ++k) { c.bp_dim[k] = dim[k]; c.bp_org[k] = glo[k]; }
+  c.bp_inv = inv;
+  c.bp_ptr = sc->bp_ptr.p;
+  c.bp_face = sc->bp_face.p;
+  return DFEM_OK;
+}
+
 static int upload_scene(dfem_scene* sc) {
   HostScene& s = sc->hs;
   CK(sc->mass.upload(s.mass));
@@ -843,10 +939,12 @@ static int upload_scene(dfem_scene* sc) {
     CK(sc->crec_base.alloc(1));
     CK(cudaMemset(sc->crec_base.p, 0, sizeof(int)));
     sc->cd = ContactDev{nc, nof, s.K, kMaxContactPasses, kMaxImpactsPerVertex, kMaxSelfImpacts, kMaxGroupMembers,
+                        kBroadDefaultCells, {0, 0, 0}, {0.0, 0.0, 0.0}, 0.0, nullptr, nullptr,
                         s.alpha, s.mu_obs, sc->cverts.p, sc->cidx.p, sc->obs_x.p,
                         sc->obs_f.p, sc->hdiag.p, sc->imp_cnt.p, sc->imp_face.p, sc->imp_n.p, sc->xn1.p, sc->xold.p,
                         sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p, sc->crec_on.p, 0, nullptr, nullptr,
                         nullptr, nullptr, nullptr, sc->status.p, sc->crec_base.p, nullptr};
+    RC(build_obstacle_grid(sc));
     if (sc->self_contact) {
       const int ncf = (int)s.cfaces.size() / 3;
       CK(sc->s_cfaces.upload(s.cfaces));
@@ -2316,6 +2414,10 @@ int dfem_set_limit(dfem_scene* sc, int32_t which, int64_t value) {
        : which == DFEM_LIMIT_SOFT_IMPACTS_PER_VERTEX ? c.max_self_impacts : c.max_members) = v;
       break;
     }
+    case DFEM_LIMIT_BROAD_PHASE_CELLS:
+      if (!dflt && value > 4096) return fail(DFEM_ERR_INVALID, "broad-phase cell limit must be in [0, 4096]");
+      sc->cd.bp_max_cells = dflt ? kBroadDefaultCells : (int)value;
+      break;
     case DFEM_LIMIT_SOLVE_WAIT_POLLS:
       if (!dflt && (value < 1 || value > kSpinTries))
         return fail(DFEM_ERR_INVALID, "poll limit must be in [1, " + std::to_string(kSpinTries) + "]");

@@ -131,11 +131,26 @@ constexpr double kContactThickness = 1e-4;  // arcsim Impact::thickness
 // solves use 1-9 (pd_kernels.cu, resident_solve.cuh).
 enum { kCapContactPasses = 10, kCapImpacts = 11, kCapSoftImpacts = 12, kCapGroupMembers = 13 };
 
+// Broad phase of the obstacle detection: a uniform grid over the static
+// obstacle faces' boxes dilated by kBroadPad; a vertex tests the faces of the
+// cells its swept box (dilated alike) covers, in ascending face order, and
+// every face when that box covers more than bp_max_cells cells or gathers
+// more than kBroadMaxCandidates faces.
+constexpr double kBroadPad = 2.5e-4;          // > the obstacle contact thickness (1e-4)
+constexpr int kBroadMaxCandidates = 128;
+constexpr int kBroadDefaultCells = 64;
+
 struct ContactDev {
   int nc, nof, K, max_passes;
   int max_impacts;        // obstacle impacts kept per vertex (<= kMaxImpactsPerVertex)
   int max_self_impacts;   // soft impacts kept per vertex (<= kMaxSelfImpacts)
   int max_members;        // members of one face group (<= kMaxGroupMembers)
+  int bp_max_cells;       // broad phase: cells a query may cover (0: every face is tested)
+  int bp_dim[3];          // grid cells per axis (0: no grid)
+  double bp_org[3];       // grid origin
+  double bp_inv;          // 1 / cell size
+  const int* bp_ptr;      // cells + 1: each cell's faces bp_face[bp_ptr[c] .. bp_ptr[c + 1]) (ascending)
+  const int* bp_face;
   double alpha, mu;
   const int* cverts;      // contact vertices (internal ids)
   const int* cidx;        // N: contact index or -1

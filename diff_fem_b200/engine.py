@@ -227,7 +227,7 @@ class Scene:
                 "threads_fwd": list(thr)[0::2], "threads_bwd": list(thr)[1::2]}
 
     LIMITS = {"contact_passes": 0, "impacts_per_vertex": 1, "soft_impacts_per_vertex": 2, "group_members": 3,
-              "solve_wait_polls": 4}
+              "solve_wait_polls": 4, "broad_phase_cells": 5}
 
     def set_limit(self, which: str, value: int = -1):
         """Lower one of the engine's caps for this scene (value < 0: the

@@ -333,13 +333,19 @@ int dfem_profile_phases(dfem_scene *scene, int32_t reps, double *ms);
  *   DFEM_LIMIT_GROUP_MEMBERS            members of one soft-contact face group (0..32)
  *   DFEM_LIMIT_SOLVE_WAIT_POLLS         polls of a dependency wait of the persistent
  *                                       solve form (1..2^22)
+ *   DFEM_LIMIT_BROAD_PHASE_CELLS        grid cells a contact vertex's swept box may
+ *                                       cover in the obstacle detection's broad phase
+ *                                       before the vertex tests every obstacle face
+ *                                       (0..4096, default 64; 0: no broad phase).
+ *                                       Never an error: results are identical either way.
  * No counterpart in the reference. */
 enum dfem_limit {
   DFEM_LIMIT_CONTACT_PASSES = 0,
   DFEM_LIMIT_IMPACTS_PER_VERTEX = 1,
   DFEM_LIMIT_SOFT_IMPACTS_PER_VERTEX = 2,
   DFEM_LIMIT_GROUP_MEMBERS = 3,
-  DFEM_LIMIT_SOLVE_WAIT_POLLS = 4
+  DFEM_LIMIT_SOLVE_WAIT_POLLS = 4,
+  DFEM_LIMIT_BROAD_PHASE_CELLS = 5
 };
 int dfem_set_limit(dfem_scene *scene, int32_t which, int64_t value);
 
