@@ -99,6 +99,7 @@ SIGNATURES = [
     ("dfem_last_error", C.c_char_p, []),
     ("dfem_abi_version", C.c_int, []),
     ("dfem_set_limit", C.c_int, [_VP, C.c_int32, C.c_int64]),
+    ("dfem_set_option", C.c_int, [_VP, C.c_int32, C.c_int64]),
     ("dfem_debug_fail_allocations", C.c_int, [C.c_int64]),
 ]
 

@@ -11,6 +11,8 @@
 //   state = [mode (0 detect, 1 Jacobi), pass, it, any, active]
 // whose body runs at most max_passes * (K + 2) + 1 times.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "kernels.cuh"
 
 namespace dfem {
@@ -19,7 +21,7 @@ namespace dfem {
 // Jacobi iterations, the computed iteration whose x_n1 the current ori_x is,
 // obstacle impacts in the lists, self groups of this pass, of the last pass]
 enum { CS_MODE = 0, CS_PASS = 1, CS_IT = 2, CS_ANY = 3, CS_ACTIVE = 4, CS_BODIES = 5, CS_COMP = 6, CS_SRC = 7,
-       CS_NOBS = 8, CS_NGRP = 9, CS_NGRP_PREV = 10, CS_SIZE = 11 };
+       CS_NOBS = 8, CS_NGRP = 9, CS_NGRP_PREV = 10, CS_FANY0 = 11, CS_FANY1 = 12, CS_SIZE = 13 };
 
 // per-step record of the phase: [passes, loop-body executions]; while the
 // forward steps record their contact iterations, the step's place in the
@@ -248,9 +250,8 @@ __global__ void k_contact_step_inputs(SceneDev d, ContactDev c, const double* xt
   st3(c.lxt, i, contact_lxt(d, i, xt));
 }
 
-__global__ void k_contact_begin(SceneDev d, ContactDev c, const double* xt, const double* xk,
-                                cudaGraphConditionalHandle h) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void contact_begin_item(const SceneDev& d, const ContactDev& c, int i, const double* xt,
+                                                   const double* xk) {
   if (i < d.N) {
     st3(c.xn1, i, ld3(xk, i));
     st3(c.xold, i, mk3(0.0, 0.0, 0.0));
@@ -260,6 +261,12 @@ __global__ void k_contact_begin(SceneDev d, ContactDev c, const double* xt, cons
     c.imp_cnt[i] = 0;
     if (c.ncf > 0) c.simp_cnt[i] = 0;
   }
+}
+
+__global__ void k_contact_begin(SceneDev d, ContactDev c, const double* xt, const double* xk,
+                                cudaGraphConditionalHandle h) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  contact_begin_item(d, c, i, xt, xk);
   if (i == 0) {
     for (int k = 0; k < CS_SIZE; ++k) c.state[k] = 0;
     cudaGraphSetConditional(h, (c.nc > 0 && (c.nof > 0 || c.ncf > 0)) ? 1u : 0u);
@@ -306,12 +313,11 @@ __device__ __forceinline__ bool bp_candidates(const ContactDev& c, Vec3<double> 
   return true;
 }
 
-// Detection pass (mode 0): every contact vertex against the obstacle faces
-// (the broad phase's candidates, or all of them), in ascending face order.
-__global__ void k_contact_detect(ContactDev c, const double* xt, const double* xk, int* status) {
-  if (c.state[CS_MODE] != 0) return;
-  int a = blockIdx.x * blockDim.x + threadIdx.x;
-  if (a >= c.nc) return;
+// Detection of contact vertex a against the obstacle faces (the broad
+// phase's candidates, or all of them), in ascending face order; true when it
+// hit a face.
+__device__ __forceinline__ bool contact_detect_item(const ContactDev& c, int a, const double* xt, const double* xk,
+                                                    int* status) {
   int gv = c.cverts[a];
   Vec3<double> p0 = ld3(xt, gv), p1 = ld3(xk, gv);
   bool any = false;
@@ -338,7 +344,15 @@ __global__ void k_contact_detect(ContactDev c, const double* xt, const double* x
     }
     st3(c.imp_n, a * kMaxImpactsPerVertex + slot, n);
   }
-  if (any) atomicOr(&c.state[CS_ANY], 1);
+  return any;
+}
+
+// Detection pass (mode 0): every contact vertex.
+__global__ void k_contact_detect(ContactDev c, const double* xt, const double* xk, int* status) {
+  if (c.state[CS_MODE] != 0) return;
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= c.nc) return;
+  if (contact_detect_item(c, a, xt, xk, status)) atomicOr(&c.state[CS_ANY], 1);
 }
 
 // Soft impacts (thickness x 2) of contact vertex a (one warp per vertex) against
@@ -423,9 +437,9 @@ __global__ void k_contact_ctl_detect(ContactDev c, cudaGraphConditionalHandle h)
 }
 
 // Jacobi iteration, part 1 (mode 1): ori_x = x_n1 and the max-norm test against xold.
-__global__ void k_contact_prep(int N, ContactDev c, double* xk, double* partial, unsigned* counter) {
-  if (c.state[CS_MODE] != 1) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+// ori_x = x_n1 at vertex i, its max-norm change; record of contact vertex i's
+// impact lists for the iteration with record index rk (-1: none).
+__device__ __forceinline__ double contact_prep_item(const ContactDev& c, int i, int N, double* xk, int rk) {
   double e = 0;
   if (i < N) {
     Vec3<double> x = ld3(c.xn1, i);
@@ -434,7 +448,6 @@ __global__ void k_contact_prep(int N, ContactDev c, double* xk, double* partial,
     e = fmax(fabs(dl.x), fmax(fabs(dl.y), fabs(dl.z)));
   }
   // recording for the adjoint: the impact lists this iteration will use
-  const int rk = rec_index(c);
   if (rk >= 0 && i < c.nc) {
     const int cnt = c.imp_cnt[i];
     c.rec_cnt[(size_t)rk * c.nc + i] = cnt;
@@ -442,6 +455,13 @@ __global__ void k_contact_prep(int N, ContactDev c, double* xk, double* partial,
     double* rn = c.rec_n + ((size_t)rk * c.nc + i) * kMaxImpactsPerVertex * 3;
     for (int q = 0; q < cnt; ++q) st3(rn, q, ld3(c.imp_n, i * kMaxImpactsPerVertex + q));
   }
+  return e;
+}
+
+__global__ void k_contact_prep(int N, ContactDev c, double* xk, double* partial, unsigned* counter) {
+  if (c.state[CS_MODE] != 1) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = contact_prep_item(c, i, N, xk, rec_index(c));
   // deterministic grid max
   __shared__ double ws[32];
   __shared__ bool last;
@@ -474,11 +494,11 @@ __global__ void k_contact_prep(int N, ContactDev c, double* xk, double* partial,
 //   contact vertex: rhs := B r, r = -B^T rhs with the tangential part clamped to mu r_n (last impact wins)
 //   prev = alpha rhs + (1 - alpha) prev  (prev = rhs before the contact step on the first iteration)
 //   x_n1 = x_t + prev / (h diag(Hs)),  xold = ori_x
-__global__ void k_contact_rhs(SceneDev d, ContactDev c, const double* __restrict__ slot, const double* xt,
-                              const double* xk) {
-  if (c.state[CS_MODE] != 1 || c.state[CS_ACTIVE] == 0) return;
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.N) return;
+// The Jacobi update of vertex i (obstacle contact only): rhs, the friction
+// cone of its impacts, relaxation, x_n1; first: the pass's first iteration;
+// rk: record index (-1: none).
+__device__ __forceinline__ void contact_rhs_item(const SceneDev& d, const ContactDev& c, int i, const double* slot,
+                                                 const double* xt, const double* xk, bool first, int rk) {
   Vec3<double> jd = ld3(d.attach_jd, i);
   for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) jd = jd + ld3(slot, k);
   Vec3<double> cdx = mk3(0.0, 0.0, 0.0);
@@ -487,7 +507,6 @@ __global__ void k_contact_rhs(SceneDev d, ContactDev c, const double* __restrict
     if (j != i) cdx = cdx + d.hs_val[k] * (ld3(xk, j) - ld3(xt, j));
   }
   Vec3<double> rhs = d.mass[i] * ld3(c.vwc, i) + d.h * (jd - ld3(c.lxt, i)) - d.h * cdx;
-  const bool first = c.state[CS_IT] == 0;
   Vec3<double> prev = first ? rhs : ld3(c.prev, i);
   int a = c.cidx[i];
   if (a >= 0) {
@@ -508,12 +527,19 @@ __global__ void k_contact_rhs(SceneDev d, ContactDev c, const double* __restrict
   st3(c.prev, i, prev);
   st3(c.xn1, i, ld3(xt, i) + (1.0 / (d.h * c.hdiag[i])) * prev);
   st3(c.xold, i, ld3(xk, i));
-  const int rk = rec_index(c);
   if (rk >= 0) {
     st3(c.rec_x + (size_t)rk * 3 * d.N, i, ld3(xk, i));
     st3(c.rec_prev + (size_t)rk * 3 * d.N, i, prev);
     if (i == 0) c.rec_first[rk] = first ? 1 : 0;
   }
+}
+
+__global__ void k_contact_rhs(SceneDev d, ContactDev c, const double* __restrict__ slot, const double* xt,
+                              const double* xk) {
+  if (c.state[CS_MODE] != 1 || c.state[CS_ACTIVE] == 0) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  contact_rhs_item(d, c, i, slot, xt, xk, c.state[CS_IT] == 0, rec_index(c));
 }
 
 // End of a Jacobi iteration: count it; after K iterations return to detection.
@@ -528,6 +554,106 @@ __global__ void k_contact_ctl_iter(ContactDev c, int K) {
     atomicExch(c.status, 6);  // the replayed step's record is too small
   c.state[CS_COMP] += 1;
   if (it >= K) c.state[CS_MODE] = 0;
+}
+
+// ---- the obstacle contact phase in one cooperative launch --------------------
+//
+// The whole phase of a step without soft contact as one kernel whose CTAs are
+// all resident (a cooperative launch): the state machine of the conditional
+// loop of the kernels above — detection; Jacobi iterations until the
+// max-norm change of ori_x drops below EPS or K iterations ran; detection
+// again, until a detection finds no impact — with grid-wide barriers between
+// its phases instead of kernel boundaries (3 barriers per Jacobi iteration, 1
+// per detection, against 6 launches per loop body).  Every phase runs its
+// kernel's per-item code (contact_detect_item, contact_prep_item, local_item,
+// contact_rhs_item) in a grid-stride loop, so the arithmetic and the records
+// for the adjoint are those of the loop of kernels, bit for bit.  Every
+// thread keeps an identical copy of the state machine, updated from values
+// read after a barrier; thread 0 writes the final state (passes, loop-body
+// executions, computed iterations, source iteration) to c.state for the
+// step's record.  The detections' hit flags alternate between two words, so
+// clearing one never races with reading the other.
+__device__ __forceinline__ int rec_index_at(const ContactDev& c, int comp) {
+  if (!c.rec_on || *c.rec_on == 0) return -1;
+  const int k = *c.rec_base + comp;
+  return k < c.rec_cap ? k : -1;
+}
+
+__global__ void __launch_bounds__(128) k_contact_fused(SceneDev d, ContactDev c, const double* xt, double* xk,
+                                                       const double* act_all, const int* step, double* slot,
+                                                       double* partial, int* status) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double ws[4];
+  __shared__ double s_m;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
+  const bool lead = tid == 0;
+  const int ncons = d.T + d.M + d.S + d.B, nv = max(d.N, c.nc);
+  for (int i = tid; i < nv; i += nthr) contact_begin_item(d, c, i, xt, xk);
+  if (lead)
+    for (int k = 0; k < CS_SIZE; ++k) c.state[k] = 0;
+  if (!(c.nc > 0 && c.nof > 0)) return;  // uniform, before any barrier
+  grid.sync();
+  int mode = 0, pass = 0, it = 0, bodies = 0, comp = 0, src = 0, ndet = 0;
+  const int cap = c.max_passes * (c.K + 2) + 2;
+  for (;;) {
+    bodies += 1;
+    if (mode == 0) {  // detection pass (k_contact_detect, k_contact_ctl_detect)
+      int* flag = c.state + ((ndet & 1) ? CS_FANY1 : CS_FANY0);
+      for (int a = tid; a < c.nc; a += nthr)
+        if (contact_detect_item(c, a, xt, xk, status)) atomicOr(flag, 1);
+      grid.sync();
+      const bool any = *(volatile int*)flag != 0;
+      if (lead) c.state[(ndet & 1) ? CS_FANY0 : CS_FANY1] = 0;  // the other word: read a barrier ago
+      ++ndet;
+      if (!any) break;
+      if (pass >= c.max_passes) {
+        if (lead) cap_reached(status, kCapContactPasses);
+        break;
+      }
+      mode = 1;
+      it = 0;
+      pass += 1;
+    }
+    // one Jacobi iteration (k_contact_prep, k_local, k_contact_rhs, k_contact_ctl_iter)
+    const int rk = rec_index_at(c, comp);
+    double e = 0.0;
+    for (int i = tid; i < nv; i += nthr) e = fmax(e, contact_prep_item(c, i, d.N, xk, rk));
+    for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
+    __syncthreads();
+    if (threadIdx.x == 0) partial[blockIdx.x] = fmax(fmax(ws[0], ws[1]), fmax(ws[2], ws[3]));
+    grid.sync();
+    if (threadIdx.x < 32) {  // every CTA forms the same maximum (order-independent)
+      double m = 0.0;
+      for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) m = fmax(m, __ldcg(partial + b));
+      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (threadIdx.x == 0) s_m = m;
+    }
+    __syncthreads();
+    const bool conv = s_m < kConvergenceEps;
+    src = comp;
+    if (conv) {
+      mode = 0;  // back to detection
+    } else {
+      for (int t = tid; t < ncons; t += nthr) local_item(d, t, xk, act_all, step, slot);
+      grid.sync();
+      for (int i = tid; i < d.N; i += nthr) contact_rhs_item(d, c, i, slot, xt, xk, it == 0, rk);
+      grid.sync();
+      it += 1;
+      if (lead && c.rec_on && *c.rec_on == 1 && *c.rec_base + comp >= c.rec_cap) atomicExch(status, 6);
+      comp += 1;
+      if (it >= c.K) mode = 0;
+    }
+    if (bodies > cap) {  // unreachable: passes and iterations are bounded above
+      if (lead) cap_reached(status, kCapContactPasses);
+      break;
+    }
+  }
+  if (lead) {
+    c.state[CS_MODE] = mode; c.state[CS_PASS] = pass; c.state[CS_IT] = it; c.state[CS_BODIES] = bodies;
+    c.state[CS_COMP] = comp; c.state[CS_SRC] = src;
+  }
 }
 
 // ---- soft-soft (self) contact ------------------------------------------------

@@ -202,6 +202,12 @@ struct dfem_scene {
   bool has_contact = false;
   DBuf<int> cverts, cidx, obs_f, imp_cnt, imp_face, cstate, cpasses;
   DBuf<int> bp_ptr, bp_face;             // broad phase of the obstacle detection
+  // the obstacle contact phase as one cooperative launch (k_contact_fused) or
+  // as the conditional loop of kernels
+  bool fused_ok = false;                 // scene has obstacle contact only and the device runs the launch
+  bool fused_on = true;                  // dfem_set_option(DFEM_OPTION_FUSED_CONTACT)
+  int fused_grid = 0;
+  DBuf<double> fpartial;
   DBuf<double> obs_x, hdiag, imp_n, xn1, xold, cprev, lxt, vwc;
   // soft-soft contact (forward only: the adjoint refuses these scenes)
   bool self_contact = false;
@@ -945,6 +951,17 @@ static int upload_scene(dfem_scene* sc) {
                         sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p, sc->crec_on.p, 0, nullptr, nullptr,
                         nullptr, nullptr, nullptr, sc->status.p, sc->crec_base.p, nullptr};
     RC(build_obstacle_grid(sc));
+    if (!sc->self_contact) {  // the fused phase: every CTA resident (cooperative launch)
+      int nsm = 1, occ = 0, coop = 0;
+      CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, sc->device));
+      CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, sc->device));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_contact_fused, 128, 0));
+      const int ncons = s.T + s.M + s.S + s.B;
+      const int want = std::max(1, (std::max(ncons, s.N) + 127) / 128);
+      sc->fused_grid = std::min(nsm * occ, want);
+      sc->fused_ok = coop != 0 && occ > 0;
+      if (sc->fused_ok) CK(sc->fpartial.alloc(std::max(1, sc->fused_grid)));
+    }
     if (sc->self_contact) {
       const int ncf = (int)s.cfaces.size() / 3;
       CK(sc->s_cfaces.upload(s.cfaces));
@@ -1278,8 +1295,28 @@ static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandl
   k_loop_ctl<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, s.nparts, s.K, h);
 }
 
+static bool fused_contact(const dfem_scene* sc) { return sc->has_contact && sc->fused_ok && sc->fused_on; }
+
+// The obstacle contact phase of the step as one cooperative launch.
+static cudaError_t launch_contact_fused(dfem_scene* sc, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(sc->fused_grid);
+  cfg.blockDim = dim3(128);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_contact_fused, sc->sd, sc->cd, (const double*)sc->xt.p, sc->xk.p,
+                            (const double*)sc->act_all.p, (const int*)sc->step.p, sc->slot.p, sc->fpartial.p,
+                            sc->status.p);
+}
+
 static void step_post(dfem_scene* sc, cudaStream_t st) {
   const int nb = sc->nblk_v;
+  if (fused_contact(sc)) launch_contact_fused(sc, st);  // a refused launch surfaces through cudaGetLastError
   if (sc->has_contact) k_contact_record<<<1, 1, 0, st>>>(sc->step.p, sc->cstate.p, sc->cpasses.p, sc->cd);
   k_step_end<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->xk.p, sc->traj.p, sc->to_user.p,
                                  sc->write_traj.p);
@@ -1400,7 +1437,7 @@ static int build_loop_graph(dfem_scene* sc, const std::vector<LoopStage>& stages
 static int ensure_graphs(dfem_scene* sc) {
   if (!sc->g_step.exec) {
     std::vector<LoopStage> st{{step_pre, step_body}};
-    if (sc->has_contact) st.push_back({contact_pre, contact_body});
+    if (sc->has_contact && !fused_contact(sc)) st.push_back({contact_pre, contact_body});
     RC(build_loop_graph(sc, st, step_post, &sc->g_step));
   }
   if (!sc->g_adj.exec) RC(build_loop_graph(sc, {{adj_pre, adj_body}}, adj_post, &sc->g_adj));
@@ -2428,6 +2465,23 @@ int dfem_set_limit(dfem_scene* sc, int32_t which, int64_t value) {
       return fail(DFEM_ERR_INVALID, "unknown limit");
   }
   invalidate_graphs(sc);  // the kernels' parameters changed
+  sc->rec_steps = 0;
+  return DFEM_OK;
+}
+
+int dfem_set_option(dfem_scene* sc, int32_t which, int64_t value) {
+  if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
+  CK(cudaSetDevice(sc->device));
+  CK(cudaStreamSynchronize(sc->stream));
+  switch (which) {
+    case DFEM_OPTION_FUSED_CONTACT:
+      if (value != 0 && value != 1) return fail(DFEM_ERR_INVALID, "value must be 0 or 1");
+      sc->fused_on = value != 0;
+      break;
+    default:
+      return fail(DFEM_ERR_INVALID, "unknown option");
+  }
+  invalidate_graphs(sc);
   sc->rec_steps = 0;
   return DFEM_OK;
 }

@@ -164,13 +164,13 @@ __global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt
   }
 }
 
-// Local step: every constraint projects and writes its J*d contribution to its
-// slots.  One thread per constraint; constraint types are consecutive ranges.
-__global__ void __launch_bounds__(128, DFEM_LOCAL_MIN_BLOCKS) k_local(SceneDev d, Gate gate, const double* __restrict__ x,
-                                               const double* __restrict__ act_all, const int* step,
-                                               double* __restrict__ slot) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gate.skip(cons_part(d, t))) return;
+// Local step of constraint t (tets, muscles, springs, bending stencils in
+// that order): its projection and its J*d contribution to its slots.  The
+// pointers are not restrict-qualified: a kernel that writes x in an earlier
+// phase of the same launch (k_contact_fused) must not read it through the
+// read-only data path.
+__device__ __forceinline__ void local_item(const SceneDev& d, int t, const double* x, const double* act_all,
+                                           const int* step, double* slot) {
   if (t < d.T) {
     // corotated FEM (CorotateFEMConstraint::EvaluateDVector + EvaluateJMatrix)
     int4 v = d.tv[t];
@@ -237,6 +237,16 @@ __global__ void __launch_bounds__(128, DFEM_LOCAL_MIN_BLOCKS) k_local(SceneDev d
     if (ln > 1e-25) dd = (w * d.brest[t] / ln) * lap;
     for (int k = o0; k < o1; ++k) st3(slot, d.bslot[k], (w * d.bbeta[k]) * dd);
   }
+}
+
+// Local step: every constraint projects and writes its J*d contribution to its
+// slots.  One thread per constraint; constraint types are consecutive ranges.
+__global__ void __launch_bounds__(128, DFEM_LOCAL_MIN_BLOCKS) k_local(SceneDev d, Gate gate, const double* __restrict__ x,
+                                               const double* __restrict__ act_all, const int* step,
+                                               double* __restrict__ slot) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gate.skip(cons_part(d, t))) return;
+  local_item(d, t, x, act_all, step, slot);
 }
 
 // ---- mixed form: FP32 projections, FP32 slots and accumulation ----------------

@@ -235,6 +235,12 @@ class Scene:
         DFEM_ERR_CAP.  See dfem_set_limit."""
         check(lib().dfem_set_limit(self._h, self.LIMITS[which], int(value)))
 
+    OPTIONS = {"fused_contact": 0}
+
+    def set_option(self, which: str, value: int):
+        """An execution option (results are identical either way); see dfem_set_option."""
+        check(lib().dfem_set_option(self._h, self.OPTIONS[which], int(value)))
+
     def set_adjoint_budget(self, nbytes: int):
         """Device memory for storing every step's iterates (the adjoint then replays no step)."""
         check(lib().dfem_set_adjoint_budget(self._h, int(nbytes)))

@@ -517,3 +517,38 @@ def test_obstacle_broad_phase_matches_testing_every_face():
     assert out[0][2].sum() > 0
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("case", ["box", "star", "cloth"])
+def test_fused_contact_phase_matches_the_loop_of_kernels(case):
+    """The obstacle contact phase as one cooperative launch (the default)
+    gives the same trajectories, contact passes, iteration counts and
+    gradients, bit for bit, as the conditional graph loop of kernels."""
+    if case == "box":
+        d, n = S.drop_box(), 6
+        v = d.initial_velocity.copy()
+        act = None
+    elif case == "star":
+        d, n = S.muscle_star(refine=1), 8
+        v = None
+        act = np.random.default_rng(3).uniform(0, 1, (n, d.n_segments))
+    else:
+        d, n = S.cloth_on_ball(nv=16, radius=0.08, drop=0.01, subdiv=3), 16
+        v = None
+    x = d.x0.reshape(-1).copy()
+    v = np.zeros_like(x) if v is None else v
+    rng = np.random.default_rng(9)
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    out = []
+    for fused in (1, 0):
+        g = Scene(d)
+        g.set_option("fused_contact", fused)
+        xg, vg, tg = g.forward(x, v, n_steps=n, act=act, traj=True)
+        res = [tg, vg, g.contact_passes(n), g.iterations(n)]
+        b = g.backward(gx, gv)
+        res += [b[k] for k in ("x", "v", "E")] + ([b["act"]] if act is not None else [])
+        out.append(res)
+        g.close()
+    assert out[0][2].sum() > 0
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
