@@ -1069,12 +1069,9 @@ __global__ void k_cadj_start(int N, double cv, double* io_a, double* io_b, Conta
 
 // slot: J d at ori (k_local); xt: the step's start positions; ori, prev: the
 // recorded iteration j; first: whether it began its pass; rcnt / rn: its impacts.
-__global__ void k_cadj_rhs(SceneDev d, ContactDev c, ContactAdj a, const double* __restrict__ slot,
-                           const double* __restrict__ xt, const double* __restrict__ ori,
-                           const double* __restrict__ prev, int first, const int* __restrict__ rcnt,
-                           const double* __restrict__ rn) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.N) return;
+__device__ __forceinline__ void cadj_rhs_item(const SceneDev& d, const ContactDev& c, const ContactAdj& a, int i,
+                                              const double* slot, const double* xt, const double* ori,
+                                              const double* prev, int first, const int* rcnt, const double* rn) {
   const double hd = c.hdiag[i];
   const Vec3<double> xb = ld3(a.xn1b, i), pv = ld3(prev, i);
   st3(a.cxtb, i, ld3(a.cxtb, i) + xb);
@@ -1124,6 +1121,15 @@ __global__ void k_cadj_rhs(SceneDev d, ContactDev c, ContactAdj a, const double*
   }
   st3(a.vwcb, i, ld3(a.vwcb, i) + d.mass[i] * rb);
   st3(a.yb, i, d.h * rb);
+}
+
+__global__ void k_cadj_rhs(SceneDev d, ContactDev c, ContactAdj a, const double* __restrict__ slot,
+                           const double* __restrict__ xt, const double* __restrict__ ori,
+                           const double* __restrict__ prev, int first, const int* __restrict__ rcnt,
+                           const double* __restrict__ rn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  cadj_rhs_item(d, c, a, i, slot, xt, ori, prev, first, rcnt, rn);
 }
 
 // VJP of J d at ori with cotangent yb, and the Hs terms of the tets' E gradient
@@ -1475,9 +1481,7 @@ __global__ void k_cadj_self_b(SceneDev d, ContactDev c, ContactAdj a, SelfRec rv
   st3(a.yb, i, d.h * rb);
 }
 
-__global__ void k_cadj_hs(SceneDev d, ContactAdj a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.N) return;
+__device__ __forceinline__ void cadj_hs_item(const SceneDev& d, const ContactAdj& a, int i) {
   Vec3<double> o = ld3(a.orib, i);
   double hii = 0.0;
   for (int k = d.hs_ptr[i]; k < d.hs_ptr[i + 1]; ++k) {
@@ -1489,10 +1493,14 @@ __global__ void k_cadj_hs(SceneDev d, ContactAdj a) {
   st3(a.xn1b, i, o);
 }
 
+__global__ void k_cadj_hs(SceneDev d, ContactAdj a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  cadj_hs_item(d, a, i);
+}
+
 // after the reverse sweep: the diag(Hs) terms of the tets' E gradient
-__global__ void k_cadj_hd(SceneDev d, ContactAdj a, double* gE) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= d.T || !gE) return;
+__device__ __forceinline__ void cadj_hd_item(const SceneDev& d, const ContactAdj& a, int t, double* gE) {
   int4 v = d.tv[t];
   const int vi[4] = {v.x, v.y, v.z, v.w};
   double G[4][3];
@@ -1501,6 +1509,74 @@ __global__ void k_cadj_hd(SceneDev d, ContactAdj a, double* gE) {
 #pragma unroll
   for (int q = 0; q < 4; ++q) s += (G[q][0] * G[q][0] + G[q][1] * G[q][1] + G[q][2] * G[q][2]) * a.hdb[vi[q]];
   gE[t] += d.tvol[t] * s;
+}
+
+__global__ void k_cadj_hd(SceneDev d, ContactAdj a, double* gE) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= d.T || !gE) return;
+  cadj_hd_item(d, a, t, gE);
+}
+
+// The reverse sweep of a step's obstacle contact phase (no soft contact) in
+// one cooperative launch: k_cadj_start, then for the recorded computed
+// iterations j = top .. 1 (records base + j - 1) the chain of
+// contact_adjoint_step's kernels — local step at the iteration's input, the
+// rhs VJP, the local VJP, the slot gather with the Hs terms and the
+// segments' activation sums — with grid-wide barriers between them, then
+// the diag(Hs) terms of dL/dE and the PD part's cotangent.  Same per-item
+// code and order as the kernels: bit-identical results.  The records' pass
+// flags are read on the device (the kernels' path copies them to the host).
+__global__ void __launch_bounds__(128) k_cadj_fused(SceneDev d, ContactDev c, ContactAdj a, const double* xt,
+                                                    const double* act_all, const int* step, double* slot, double* gE,
+                                                    double* gnu, double* mg, double* gact, int base, int top, double cv,
+                                                    double* io_a, double* io_b) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
+  const int ncons = d.T + d.M + d.S + d.B;
+  const size_t n3 = 3 * (size_t)d.N;
+  const int st = *step;
+  const double* act_row = act_all + (size_t)st * d.nseg;
+  for (int i = tid; i < d.N; i += nthr) {  // k_cadj_start
+    const Vec3<double> gv = ld3(io_b, i);
+    st3(a.xn1b, i, ld3(io_a, i) + cv * gv);
+    st3(a.cxtb, i, (-cv) * gv);
+    st3(a.vwcb, i, mk3(0.0, 0.0, 0.0));
+    st3(a.pb, i, mk3(0.0, 0.0, 0.0));
+    a.hdb[i] = 0.0;
+  }
+  grid.sync();
+  for (int j = top; j >= 1; --j) {
+    const size_t r = (size_t)base + (j - 1);
+    const double* ori = c.rec_x + r * n3;
+    const double* prev = c.rec_prev + r * n3;
+    const int* rcnt = c.rec_cnt + r * c.nc;
+    const double* rn = c.rec_n + r * c.nc * kMaxImpactsPerVertex * 3;
+    const int first = c.rec_first[r];
+    for (int t = tid; t < ncons; t += nthr) local_item(d, t, ori, act_all, step, slot);
+    grid.sync();
+    for (int i = tid; i < d.N; i += nthr) cadj_rhs_item(d, c, a, i, slot, xt, ori, prev, first, rcnt, rn);
+    grid.sync();
+    for (int t = tid; t < ncons; t += nthr) adj_local_item(d, t, ori, a.yb, act_row, slot, gE, gnu, mg, nullptr, xt);
+    grid.sync();
+    for (int i = tid; i < d.N; i += nthr) {  // k_adj_gather, then k_cadj_hs on the same vertex
+      Vec3<double> acc = mk3(0.0, 0.0, 0.0);
+      for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
+      st3(a.orib, i, acc);
+      cadj_hs_item(d, a, i);
+    }
+    for (int q = tid; q < d.nseg; q += nthr) {  // k_seg_reduce
+      double sum = 0;
+      for (int k = d.seg_ptr[q]; k < d.seg_ptr[q + 1]; ++k) sum += mg[d.seg_mus[k]];
+      gact[(size_t)st * d.nseg + q] += sum;
+    }
+    grid.sync();
+  }
+  for (int t = tid; t < d.T; t += nthr) cadj_hd_item(d, a, t, gE);
+  for (int i = tid; i < d.N; i += nthr) {  // k_cadj_to_pd
+    st3(io_a, i, ld3(a.xn1b, i));
+    st3(io_b, i, mk3(0.0, 0.0, 0.0));
+  }
 }
 
 // the PD part's input cotangent is the phase's input cotangent; the step's

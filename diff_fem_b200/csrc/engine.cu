@@ -206,7 +206,8 @@ struct dfem_scene {
   // as the conditional loop of kernels
   bool fused_ok = false;                 // scene has obstacle contact only and the device runs the launch
   bool fused_on = true;                  // dfem_set_option(DFEM_OPTION_FUSED_CONTACT)
-  int fused_grid = 0;
+  int fused_grid = 0;                    // CTAs of k_contact_fused (all resident)
+  int cadj_grid = 0;                     // CTAs of k_cadj_fused (all resident)
   DBuf<double> fpartial;
   DBuf<double> obs_x, hdiag, imp_n, xn1, xold, cprev, lxt, vwc;
   // soft-soft contact (forward only: the adjoint refuses these scenes)
@@ -952,14 +953,16 @@ static int upload_scene(dfem_scene* sc) {
                         nullptr, nullptr, nullptr, sc->status.p, sc->crec_base.p, nullptr};
     RC(build_obstacle_grid(sc));
     if (!sc->self_contact) {  // the fused phase: every CTA resident (cooperative launch)
-      int nsm = 1, occ = 0, coop = 0;
+      int nsm = 1, occ = 0, occ_a = 0, coop = 0;
       CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, sc->device));
       CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, sc->device));
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_contact_fused, 128, 0));
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_cadj_fused, 128, 0));
       const int ncons = s.T + s.M + s.S + s.B;
       const int want = std::max(1, (std::max(ncons, s.N) + 127) / 128);
       sc->fused_grid = std::min(nsm * occ, want);
-      sc->fused_ok = coop != 0 && occ > 0;
+      sc->cadj_grid = std::min(nsm * occ_a, want);
+      sc->fused_ok = coop != 0 && occ > 0 && occ_a > 0;
       if (sc->fused_ok) CK(sc->fpartial.alloc(std::max(1, sc->fused_grid)));
     }
     if (sc->self_contact) {
@@ -1567,6 +1570,23 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
     src = meta[CS_SRC];
   }
   if (base + comp > sc->crec_cap) return fail(DFEM_ERR_CAP, "contact record too small for the recomputed step");
+  if (!sc->self_contact && fused_contact(sc)) {  // the whole reverse sweep in one cooperative launch
+    const ContactAdj a = make_cadj(sc);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(sc->cadj_grid);
+    cfg.blockDim = dim3(128);
+    cfg.stream = sc->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, k_cadj_fused, sc->sd, sc->cd, a, xt, (const double*)sc->act_all.p,
+                          (const int*)sc->step.p, sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p, sc->gact.p, base, src,
+                          s.damping / s.h, sc->io_a.p, sc->io_b.p));
+    sc->launches += 1;
+    return DFEM_OK;
+  }
   // soft contact: every computed iteration feeds the remembered self forces,
   // so the sweep starts at the last one and the output enters at its source;
   // the step's final remembered forces are zeroed before the next step reads

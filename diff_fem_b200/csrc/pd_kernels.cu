@@ -1146,10 +1146,11 @@ __global__ void k_adj_begin(int N, double c, const double* gx1, const double* gv
 // that consumed J d: PD iteration (x1 != null): -vol (G G^T) : (yb x1^T),
 // x1 the next iterate; contact rhs (xt != null): -vol (G G^T) : (yb z^T) with
 // z = x off the diagonal and x_t on it (rhs = ... - h C (x - x_t) - h L x_t).
-__device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const double* __restrict__ x,
-                                               const double* __restrict__ yb, const double* __restrict__ act_row,
-                                               double* __restrict__ slot, double* gE, double* gnu, double* mg,
-                                               const double* __restrict__ x1, const double* __restrict__ xt) {
+// (Plain pointers: k_cadj_fused writes yb earlier in the same launch; the
+// kernels that call it keep their parameters restrict-qualified.)
+__device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const double* x, const double* yb,
+                                               const double* act_row, double* slot, double* gE, double* gnu,
+                                               double* mg, const double* x1, const double* xt) {
   if (t < d.T) {
     int4 v = d.tv[t];
     const int vi[4] = {v.x, v.y, v.z, v.w};
