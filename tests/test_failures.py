@@ -89,7 +89,7 @@ def test_injected_allocation_failures_map_to_nomem():
             try:
                 Scene(d).close()
             except _capi.DfemError as ex:
-                assert ex.value.code == _capi.DFEM_ERR_NOMEM, str(ex.value)
+                assert ex.code == _capi.DFEM_ERR_NOMEM, str(ex)
                 failed += 1
     finally:
         lib.dfem_debug_fail_allocations(-1)
