@@ -1146,6 +1146,35 @@ __global__ void k_adj_begin(int N, double c, const double* gx1, const double* gv
 // that consumed J d: PD iteration (x1 != null): -vol (G G^T) : (yb x1^T),
 // x1 the next iterate; contact rhs (xt != null): -vol (G G^T) : (yb z^T) with
 // z = x off the diagonal and x_t on it (rhs = ... - h C (x - x_t) - h L x_t).
+// VJP of muscle constraint t (LinearMuscleConstraint): its slots and the
+// activation term mg[t].  Not inlined: the kernels that call it (the PD
+// adjoint, the contact adjoint as kernels or as one cooperative launch) then
+// run one compiled copy of its arithmetic, so their activation gradients
+// agree bit for bit.
+__device__ __noinline__ void muscle_vjp(const SceneDev& d, int t, const double* x, const double* yb,
+                                        const double* act_row, double* slot, double* mg) {
+  int4 v = d.mv[t];
+  const int vi[4] = {v.x, v.y, v.z, v.w};
+  double G[4][3];
+  load_g(d.minv, d.M, t, G);
+  Vec3<double> f = mk3(d.mfib[t], d.mfib[d.M + t], d.mfib[2 * d.M + t]);
+  double w = d.mw[t];
+  double c[4];
+  Vec3<double> db = mk3(0.0, 0.0, 0.0), Ff = mk3(0.0, 0.0, 0.0);
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    c[a] = G[a][0] * f.x + G[a][1] * f.y + G[a][2] * f.z;
+    db = db + (w * c[a]) * ld3(yb, vi[a]);
+    Ff = Ff + c[a] * ld3(x, vi[a]);
+  }
+  double a_act = act_row[d.mseg[t]];
+  mg[t] = -dot3(db, Ff);
+  int4 sl = d.mslot[t];
+  const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+  for (int a = 0; a < 4; ++a) st3(slot, sv[a], ((1.0 - a_act) * c[a]) * db);
+}
+
 // (Plain pointers: k_cadj_fused writes yb earlier in the same launch; the
 // kernels that call it keep their parameters restrict-qualified.)
 __device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const double* x, const double* yb,
@@ -1161,7 +1190,8 @@ __device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const d
     load_g(d.tinv, d.T, t, G);
     Mat3<double> F = deformation(G, xv), Y = deformation(G, yv), md, mdv;
     double E = d.tE[t], nu = d.tnu[t], vol = d.tvol[t];
-    corot_project(F, md, mdv);
+    const Svd3<double> fsv = svd3(F);  // one SVD for the projection and its VJP
+    corot_project_sv(fsv, F, md, mdv);
     double yr = 0, yvv = 0, yh = 0;
 #pragma unroll
     for (int j = 0; j < 3; ++j) { yr += dot3(Y.c[j], md.c[j]); yvv += dot3(Y.c[j], mdv.c[j]); }
@@ -1186,7 +1216,7 @@ __device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const d
     Mat3<double> gmd, gmdv;
 #pragma unroll
     for (int j = 0; j < 3; ++j) { gmd.c[j] = wr * Y.c[j]; gmdv.c[j] = wv * Y.c[j]; }
-    Mat3<double> gF = corot_vjp(F, gmd, gmdv);
+    Mat3<double> gF = corot_vjp_sv(fsv, F, gmd, gmdv);
     int4 sl = d.tslot[t];
     const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
 #pragma unroll
@@ -1195,26 +1225,7 @@ __device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const d
   }
   t -= d.T;
   if (t < d.M) {
-    int4 v = d.mv[t];
-    const int vi[4] = {v.x, v.y, v.z, v.w};
-    double G[4][3];
-    load_g(d.minv, d.M, t, G);
-    Vec3<double> f = mk3(d.mfib[t], d.mfib[d.M + t], d.mfib[2 * d.M + t]);
-    double w = d.mw[t];
-    double c[4];
-    Vec3<double> db = mk3(0.0, 0.0, 0.0), Ff = mk3(0.0, 0.0, 0.0);
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      c[a] = G[a][0] * f.x + G[a][1] * f.y + G[a][2] * f.z;
-      db = db + (w * c[a]) * ld3(yb, vi[a]);
-      Ff = Ff + c[a] * ld3(x, vi[a]);
-    }
-    double a_act = act_row[d.mseg[t]];
-    mg[t] = -dot3(db, Ff);
-    int4 sl = d.mslot[t];
-    const int sv[4] = {sl.x, sl.y, sl.z, sl.w};
-#pragma unroll
-    for (int a = 0; a < 4; ++a) st3(slot, sv[a], ((1.0 - a_act) * c[a]) * db);
+    muscle_vjp(d, t, x, yb, act_row, slot, mg);
     return;
   }
   t -= d.M;

@@ -162,10 +162,12 @@ __device__ __forceinline__ void volume_projection_d(const T s[3], T g[3], T J[3]
   dd[0] = r0; dd[1] = r1; dd[2] = r2;
 }
 
-// md (reflected rotation) and md_volume of the corotated constraint
+// md (reflected rotation) and md_volume of the corotated constraint, from the
+// SVD of F (corot_project computes it; the adjoint shares one SVD between the
+// projection and its VJP)
 template <typename T>
-__device__ __forceinline__ void corot_project(const Mat3<T>& F, Mat3<T>& md, Mat3<T>& mdv, T* s_ratio = nullptr) {
-  Svd3<T> sv = svd3(F);
+__device__ __forceinline__ void corot_project_sv(const Svd3<T>& sv, const Mat3<T>& F, Mat3<T>& md, Mat3<T>& mdv,
+                                                 T* s_ratio = nullptr) {
   if (s_ratio) {  // smallest / largest singular value (conditioning of the element)
     T smax = sv.s[0] > sv.s[1] ? (sv.s[0] > sv.s[2] ? sv.s[0] : sv.s[2]) : (sv.s[1] > sv.s[2] ? sv.s[1] : sv.s[2]);
     T smin = sv.s[0] < sv.s[1] ? (sv.s[0] < sv.s[2] ? sv.s[0] : sv.s[2]) : (sv.s[1] < sv.s[2] ? sv.s[1] : sv.s[2]);
@@ -181,6 +183,12 @@ __device__ __forceinline__ void corot_project(const Mat3<T>& F, Mat3<T>& md, Mat
     mdv.c[j] = (g[0] * vj[j][0]) * sv.u[0] + (g[1] * vj[j][1]) * sv.u[1] + (g[2] * vj[j][2]) * sv.u[2];
   }
   if (det3(F) < T(0)) md.c[2] = T(-1) * md.c[2];
+}
+
+template <typename T>
+__device__ __forceinline__ void corot_project(const Mat3<T>& F, Mat3<T>& md, Mat3<T>& mdv, T* s_ratio = nullptr) {
+  const Svd3<T> sv = svd3(F);
+  corot_project_sv(sv, F, md, mdv, s_ratio);
 }
 
 // Near-degenerate test for the mixed form: an element whose smallest singular
@@ -326,8 +334,8 @@ __device__ __forceinline__ bool corot_force_mixed(const Mat3<double>& F, double 
 //   with M_X = U^T X V, a_ij = (g_i - g_j)/(s_i - s_j), b_ij = (g_i + g_j)/(s_i + s_j);
 //   F_bar = U P_bar V^T.
 template <typename T>
-__device__ __forceinline__ Mat3<T> corot_vjp(const Mat3<T>& F, Mat3<T> gmd, const Mat3<T>& gmdv) {
-  Svd3<T> sv = svd3(F);
+__device__ __forceinline__ Mat3<T> corot_vjp_sv(const Svd3<T>& sv, const Mat3<T>& F, Mat3<T> gmd,
+                                                const Mat3<T>& gmdv) {
   T g[3], J[3][3], dd[3];
   volume_projection_d(sv.s, g, J, dd);
   if (det3(F) < T(0)) gmd.c[2] = T(-1) * gmd.c[2];
@@ -373,6 +381,12 @@ __device__ __forceinline__ Mat3<T> corot_vjp(const Mat3<T>& F, Mat3<T> gmd, cons
     out.c[c] = acc;
   }
   return out;
+}
+
+template <typename T>
+__device__ __forceinline__ Mat3<T> corot_vjp(const Mat3<T>& F, Mat3<T> gmd, const Mat3<T>& gmdv) {
+  const Svd3<T> sv = svd3(F);
+  return corot_vjp_sv(sv, F, gmd, gmdv);
 }
 
 }  // namespace dfem

@@ -84,7 +84,8 @@ void tet_forward(const Cnt G[4][3], const Vec3<Cnt> xv[4], Cnt wr, Cnt wv) {
 void tet_adjoint(const Cnt G[4][3], const Vec3<Cnt> xv[4], const Vec3<Cnt> yv[4], const Vec3<Cnt> x1v[4], Cnt E, Cnt nu,
                  Cnt vol, Cnt wr, Cnt wv) {
   Mat3<Cnt> F = deformation(G, xv), Y = deformation(G, yv), md, mdv;
-  dfem::corot_project(F, md, mdv);
+  const dfem::Svd3<Cnt> sv = dfem::svd3(F);  // one SVD for the projection and its VJP
+  dfem::corot_project_sv(sv, F, md, mdv);
   Cnt yr = 0.0, yvv = 0.0, yh = 0.0;
   for (int j = 0; j < 3; ++j) { yr += dfem::dot3(Y.c[j], md.c[j]); yvv += dfem::dot3(Y.c[j], mdv.c[j]); }
   Mat3<Cnt> F1 = deformation(G, x1v);
@@ -95,7 +96,7 @@ void tet_adjoint(const Cnt G[4][3], const Vec3<Cnt> xv[4], const Vec3<Cnt> yv[4]
   (void)s0; (void)s1;
   Mat3<Cnt> gmd, gmdv;
   for (int j = 0; j < 3; ++j) { gmd.c[j] = wr * Y.c[j]; gmdv.c[j] = wv * Y.c[j]; }
-  Mat3<Cnt> gF = dfem::corot_vjp(F, gmd, gmdv);
+  Mat3<Cnt> gF = dfem::corot_vjp_sv(sv, F, gmd, gmdv);
   for (int a = 0; a < 4; ++a) {
     volatile double sink = (G[a][0] * gF.c[0] + G[a][1] * gF.c[1] + G[a][2] * gF.c[2]).x.v;
     (void)sink;

@@ -535,6 +535,7 @@ def test_fused_contact_phase_matches_the_loop_of_kernels(case):
     else:
         d, n = S.cloth_on_ball(nv=16, radius=0.08, drop=0.01, subdiv=3), 16
         v = None
+        act = None
     x = d.x0.reshape(-1).copy()
     v = np.zeros_like(x) if v is None else v
     rng = np.random.default_rng(9)
