@@ -20,6 +20,8 @@ DFEM_ERR_NONFINITE = 4
 DFEM_ERR_STATE = 5
 DFEM_ERR_CAP = 6
 DFEM_ERR_NOMEM = 7
+DFEM_ERR_UNSUPPORTED = 8
+DFEM_JOINT_PRISMATIC, DFEM_JOINT_ROTATIONAL, DFEM_JOINT_ALL = 0, 1, 2
 DFEM_MEM_HOST = 0
 DFEM_MEM_DEVICE = 1
 DFEM_PREC_FP64 = 0
@@ -28,6 +30,7 @@ DFEM_PREC_MIXED = 1
 STATUS_NAMES = {
     0: "DFEM_OK", 1: "DFEM_ERR_INVALID", 2: "DFEM_ERR_CUDA", 3: "DFEM_ERR_FACTOR",
     4: "DFEM_ERR_NONFINITE", 5: "DFEM_ERR_STATE", 6: "DFEM_ERR_CAP", 7: "DFEM_ERR_NOMEM",
+    8: "DFEM_ERR_UNSUPPORTED",
 }
 
 _pd = C.POINTER(C.c_double)
@@ -44,6 +47,7 @@ class SceneDescC(C.Structure):
         ("n_muscle", C.c_int32), ("muscle_tets", _pi), ("muscle_fiber", _pd), ("muscle_stiffness", _pd),
         ("muscle_segment", _pi), ("n_segments", C.c_int32),
         ("n_springs", C.c_int32), ("spring_vertices", _pi), ("spring_rest", _pd), ("spring_weight", _pd),
+        ("spring_channel", _pi),
         ("n_bending", C.c_int32), ("bend_offsets", _pi), ("bend_vertices", _pi), ("bend_weight", _pd),
         ("n_contact_vertices", C.c_int32), ("contact_vertices", _pi),
         ("n_contact_faces", C.c_int32), ("contact_faces", _pi),
@@ -55,6 +59,8 @@ class SceneDescC(C.Structure):
         ("alpha", C.c_double), ("friction", C.c_double), ("obstacle_friction", C.c_double),
         ("precision", C.c_int32), ("checkpoint_every", C.c_int32),
         ("underwater", C.c_int32), ("n_drag_faces", C.c_int32), ("drag_faces", _pi),
+        ("n_links", C.c_int32), ("link_parent", _pi), ("link_type", _pi), ("link_joint", _pd),
+        ("link_axis", _pd), ("link_offsets", _pi), ("link_vertices", _pi), ("link_channel", _pi),
     ]
 
 
@@ -78,6 +84,8 @@ SIGNATURES = [
     ("dfem_scene_get_info", C.c_int, [_VP, C.POINTER(SceneInfoC)]),
     ("dfem_set_materials", C.c_int, [_VP, _VP, _VP, C.c_int]),
     ("dfem_set_activations", C.c_int, [_VP, _VP, C.c_int]),
+    ("dfem_set_joint_state", C.c_int, [_VP, _pd, _pd]),
+    ("dfem_get_joint_state", C.c_int, [_VP, _pd, _pd]),
     ("dfem_step_forward", C.c_int, [_VP, _VP, _VP, _VP, C.c_int32, _VP, _VP, _VP, C.c_int]),
     ("dfem_step_backward", C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, C.c_int]),
     ("dfem_eval_local", C.c_int, [_VP, _VP, _VP, C.c_int]),

@@ -1567,7 +1567,7 @@ __global__ void __launch_bounds__(128) k_cadj_fused(SceneDev d, ContactDev c, Co
     }
     for (int q = tid; q < d.nseg; q += nthr) {  // k_seg_reduce
       double sum = 0;
-      for (int k = d.seg_ptr[q]; k < d.seg_ptr[q + 1]; ++k) sum += mg[d.seg_mus[k]];
+      for (int k = d.seg_ptr[q]; k < d.seg_ptr[q + 1]; ++k) sum += mg[member_slot(d.M, d.seg_mus[k])];
       gact[(size_t)st * d.nseg + q] += sum;
     }
     grid.sync();

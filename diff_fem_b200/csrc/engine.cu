@@ -23,6 +23,7 @@
 #include "factor_kernels.cuh"
 #include "drag_kernels.cuh"
 #include "resident_solve.cuh"
+#include "skeleton_kernels.cuh"
 #include "resident_plan.h"
 #include "scene.h"
 
@@ -117,6 +118,7 @@ struct dfem_scene {
   DBuf<double> mass, gmask, tinv, twr, twv, tvol, tE, tnu, minv, mw, mfib, srest, ssw, bbeta, bw, brest, attach_jd;
   DBuf<int4> tv, tslot, mv, mslot;
   DBuf<int2> sv, sslot;
+  DBuf<int> sch;
   DBuf<int> mseg, seg_ptr, seg_mus, boff, bv, bslot, vslot_ptr, hs_ptr, hs_col, to_user, to_internal;
   DBuf<double> hs_val;
   DBuf<double> attach_k;             // per-vertex attachment stiffness (mixed form's rhs)
@@ -162,9 +164,7 @@ struct dfem_scene {
   bool res_ok = false;
   int res_ctas = 0;
   size_t shm_res = 0;
-  DBuf<ResSn> res_sn;
-  DBuf<int> res_sched, res_tsh;
-  DBuf<int2> res_cdst, res_xsrc;
+  DBuf<int> res_head;
   DBuf<double> res_img;
   DBuf<long long> res_img_ofs;
   DBuf<ResPack> res_pack;
@@ -196,6 +196,14 @@ struct dfem_scene {
   // (every step is recomputed from its checkpoint)
   long long hist_step = 0;
   size_t adj_budget = 0;  // set at creation: a quarter of the device memory
+  // articulated skeleton (links whose vertices move rigidly)
+  bool skel_on = false;
+  int sk_nq = 0;                         // joint-state length 12 + L - 1
+  DBuf<SkelLink> sk_link;
+  DBuf<SkelState> sk_st;
+  DBuf<int> sk_rv, sk_rlink, sk_ridx, sk_perm;
+  DBuf<double> sk_rest, sk_cinv, sk_zcm, sk_jq, sk_jqd, sk_v0, sk_w, sk_rr, sk_q, sk_tv, sk_kt, sk_sm, sk_rhs, sk_sol;
+  SkelDev skd{};
   // adjoint
   DBuf<double> xkb, xtb, bb, gE, gnu, mg, gact;
   // obstacle contact phase
@@ -287,7 +295,8 @@ static void refresh_scene_view(dfem_scene* sc) {
   SceneDev sd{s.N, s.T, s.M, s.S, s.B, s.nseg, s.h, s.damping, s.g[0], s.g[1], s.g[2],
               sc->mass.p, sc->gmask.p, sc->tv.p, sc->tinv.p, sc->twr.p, sc->twv.p, sc->tvol.p, sc->tE.p, sc->tnu.p,
               sc->tslot.p, sc->mv.p, sc->minv.p, sc->mw.p, sc->mfib.p, sc->mseg.p, sc->mslot.p, sc->seg_ptr.p,
-              sc->seg_mus.p, sc->sv.p, sc->srest.p, sc->ssw.p, sc->sslot.p, sc->boff.p, sc->bv.p, sc->bbeta.p,
+              sc->seg_mus.p, sc->sv.p, sc->srest.p, sc->ssw.p, sc->sslot.p,
+              s.sch.empty() ? nullptr : sc->sch.p, sc->boff.p, sc->bv.p, sc->bbeta.p,
               sc->bw.p, sc->brest.p, sc->bslot.p, sc->vslot_ptr.p, sc->attach_jd.p, sc->hs_ptr.p, sc->hs_col.p,
               sc->hs_val.p, sc->attach_k.p, sc->vpart.p, sc->seg_part.p,
               sc->nF ? sc->vf_ptr.p : nullptr, sc->nF ? sc->vf_face.p : nullptr, sc->nF ? sc->fdrag.p : nullptr};
@@ -538,30 +547,16 @@ static int plan_resident(dfem_scene* sc, const std::vector<int>& nseg, const std
   }
   ResidentPlan P;
   if (C == 0 || !plan_resident_layout(F, nseg, cdst, C, cap_bytes, P)) return DFEM_OK;
-  std::vector<ResSn> rsn;
-  for (const auto& it : P.items)
-    rsn.push_back(ResSn{it.c0, it.w, it.r, it.dofs, it.lofs, it.pofs, it.qofs, it.yofs, it.rofs, it.s});
   std::vector<ResPack> pk;
   for (const auto& q : P.pack) pk.push_back(ResPack{q.w, q.r, q.src_d, q.src_l, q.dst_d, q.dst_l});
-  const size_t nrow = std::max<size_t>(1, P.cdst_rank.size());
-  std::vector<int2> rc(nrow, make_int2(0, 0)), rx(nrow, make_int2(0, 0));
-  for (size_t p = 0; p < P.cdst_rank.size(); ++p) {
-    rc[p] = make_int2(P.cdst_rank[p], P.cdst_ofs[p]);
-    rx[p] = make_int2(P.xsrc_rank[p], P.xsrc_ofs[p]);
-  }
-  CK(sc->res_sn.upload(rsn));
-  CK(sc->res_sched.upload(P.sched));
-  CK(sc->res_tsh.upload(P.tsh));
-  CK(sc->res_cdst.upload(rc));
-  CK(sc->res_xsrc.upload(rx));
+  CK(sc->res_head.upload(P.head_len));
   CK(sc->res_img.upload(P.img));
   CK(sc->res_img_ofs.upload(P.img_ofs));
   CK(sc->res_pack.upload(pk));
   CK(raise_smem_limit((const void*)k_solve_resident, 8 * P.smem_doubles));
   sc->res_ctas = C;
   sc->shm_res = 8 * P.smem_doubles;
-  sc->rdv = ResDev{sc->res_sn.p, sc->res_sched.p, sc->res_cdst.p, sc->res_xsrc.p, sc->res_img.p, sc->res_img_ofs.p,
-                   sc->res_tsh.p, P.L, (int)P.smem_doubles, sc->status.p};
+  sc->rdv = ResDev{sc->res_img.p, sc->res_img_ofs.p, sc->res_head.p, P.L, (int)P.smem_doubles, sc->status.p};
   sc->res_ok = true;
   return DFEM_OK;
 }
@@ -818,6 +813,8 @@ static int build_obstacle_grid(dfem_scene* sc) {
   return DFEM_OK;
 }
 
+static int upload_skeleton(dfem_scene* sc);
+
 static int upload_scene(dfem_scene* sc) {
   HostScene& s = sc->hs;
   CK(sc->mass.upload(s.mass));
@@ -855,6 +852,7 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->sslot.upload(ssl));
   CK(sc->srest.upload(s.srest));
   CK(sc->ssw.upload(s.ssw));
+  if (!s.sch.empty()) CK(sc->sch.upload(s.sch));
   CK(sc->boff.upload(s.boff));
   CK(sc->bv.upload(s.bv));
   CK(sc->bslot.upload(s.bslot));
@@ -886,7 +884,7 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->xk.alloc(n3)); CK(sc->rhs.alloc(n3)); CK(sc->y.alloc(n3)); CK(sc->io_a.alloc(n3)); CK(sc->io_b.alloc(n3));
   CK(sc->slot.alloc(3 * (size_t)std::max(1, s.nslots)));
   CK(sc->xkb.alloc(n3)); CK(sc->xtb.alloc(n3)); CK(sc->bb.alloc(n3));
-  CK(sc->gE.alloc(std::max(1, s.T))); CK(sc->gnu.alloc(std::max(1, s.T))); CK(sc->mg.alloc(std::max(1, s.M)));
+  CK(sc->gE.alloc(std::max(1, s.T))); CK(sc->gnu.alloc(std::max(1, s.T))); CK(sc->mg.alloc(std::max(1, s.M + (s.sch.empty() ? 0 : s.S))));
   sc->nblk_v = (s.N + 127) / 128;
   // part tables: part-aligned blocks of the reducing vertex kernels
   const int np = s.nparts;
@@ -917,8 +915,14 @@ static int upload_scene(dfem_scene* sc) {
   CK(sc->zero.alloc(1));
   CK(cudaMemset(sc->counter.p, 0, sizeof(unsigned) * np));
   CK(cudaMemset(sc->status.p, 0, 4 * sizeof(int)));
-  CK(sc->act_cur.alloc(std::max(1, s.nseg)));
-  CK(cudaMemset(sc->act_cur.p, 0, sizeof(double) * std::max(1, s.nseg)));
+  // activations until set: muscle segments 0, pneumatic channels 1
+  // (PneumaticConstraint::mActivationLevel = 1, pneumaticEasy.h:31)
+  {
+    std::vector<double> a0(std::max(1, s.nseg), 0.0);
+    for (int c : s.sch)
+      if (c >= 0) a0[c] = 1.0;
+    CK(sc->act_cur.upload(a0));
+  }
   // obstacle contact phase
   const int nc = (int)s.cverts.size(), nof = (int)s.obs_f.size() / 3;
   sc->self_contact = s.self_collide;
@@ -992,7 +996,111 @@ static int upload_scene(dfem_scene* sc) {
       c.rhs_pre = sc->s_rhs_pre.p; c.cnext = sc->s_cnext.p; c.chit = sc->s_chit.p;
     }
   }
+  if (s.L > 0) RC(upload_skeleton(sc));
   refresh_scene_view(sc);
+  return DFEM_OK;
+}
+
+// Skeleton tables and the dense blocks of the Schur formulation
+// (skeleton_kernels.cuh): Z = Hs^-1 E_R (the columns of Hs^-1 at the rigid
+// vertices, three per host solve) and C^-1 = ((Hs^-1)_RR)^-1 = Hs_RR - Hs_RF
+// Hs_FF^-1 Hs_FR (World.h:1134-1135), by a dense Cholesky of C on the host.
+static int upload_skeleton(dfem_scene* sc) {
+  const HostScene& s = sc->hs;
+  const int N = s.N, L = s.L, nr = s.loff[L], ndof = 6 + L - 1;
+  std::vector<SkelLink> lk(L);
+  std::vector<int> rlink(nr), ridx(N, -1);
+  int sdof = 12;
+  for (int l = 0; l < L; ++l) {
+    SkelLink& k = lk[l];
+    std::memset(&k, 0, sizeof(k));
+    k.parent = s.lparent[l];
+    k.type = s.ltype[l];
+    k.chan = s.lchan[l];
+    k.dof = l == 0 ? 0 : 6 + l - 1;
+    k.sdof = l == 0 ? 0 : sdof++;
+    k.r0 = s.loff[l];
+    k.r1 = s.loff[l + 1];
+    for (int c = 0; c < 3; ++c) {
+      k.joint[c] = s.ljoint[3 * l + c];
+      k.axis[c] = s.laxis[3 * l + c];
+      k.d0[c] = l == 0 ? k.joint[c] : k.joint[c] - s.ljoint[3 * k.parent + c];  // Link: d0 = joint - parent->joint
+    }
+    const double* a = k.axis;
+    if (k.type == DFEM_JOINT_ROTATIONAL) {
+      const double nx[9] = {0, -a[2], a[1], a[2], 0, -a[0], -a[1], a[0], 0};
+      for (int i = 0; i < 9; ++i) { k.nx[i] = nx[i]; k.nnt[i] = a[i / 3] * a[i % 3]; }
+    }
+    for (int j = k.r0; j < k.r1; ++j) { rlink[j] = l; ridx[s.lvert[j]] = j; }
+  }
+  // Z and C from the host factor (internal numbering, three columns per solve)
+  std::vector<double> zcm((size_t)nr * N), C((size_t)nr * nr);
+  {
+    std::vector<double> b(3 * (size_t)N), x(3 * (size_t)N);
+    for (int j0 = 0; j0 < nr; j0 += 3) {
+      std::fill(b.begin(), b.end(), 0.0);
+      for (int c = 0; c < 3 && j0 + c < nr; ++c) b[3 * (size_t)s.lvert[j0 + c] + c] = 1.0;
+      host_solve(s.F, b.data(), x.data());
+      for (int c = 0; c < 3 && j0 + c < nr; ++c)
+        for (int i = 0; i < N; ++i) zcm[(size_t)(j0 + c) * N + i] = x[3 * (size_t)i + c];
+    }
+    for (int i = 0; i < nr; ++i)
+      for (int j = 0; j < nr; ++j) C[(size_t)i * nr + j] = 0.5 * (zcm[(size_t)j * N + s.lvert[i]] + zcm[(size_t)i * N + s.lvert[j]]);
+  }
+  // C^-1 by Cholesky C = G G^T, then solving for the identity
+  std::vector<double> G(C), cinv((size_t)nr * nr, 0.0);
+  for (int i = 0; i < nr; ++i) {
+    for (int j = 0; j <= i; ++j) {
+      double v = G[(size_t)i * nr + j];
+      for (int k = 0; k < j; ++k) v -= G[(size_t)i * nr + k] * G[(size_t)j * nr + k];
+      if (i == j) {
+        if (!(v > 0.0) || !std::isfinite(v)) return fail(DFEM_ERR_FACTOR, "skeleton: the rigid block of Hs^-1 is not positive definite");
+        G[(size_t)i * nr + i] = std::sqrt(v);
+      } else {
+        G[(size_t)i * nr + j] = v / G[(size_t)j * nr + j];
+      }
+    }
+  }
+  for (int col = 0; col < nr; ++col) {
+    std::vector<double> y(nr, 0.0);
+    for (int i = 0; i < nr; ++i) {
+      double v = i == col ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) v -= G[(size_t)i * nr + k] * y[k];
+      y[i] = v / G[(size_t)i * nr + i];
+    }
+    for (int i = nr - 1; i >= 0; --i) {
+      double v = y[i];
+      for (int k = i + 1; k < nr; ++k) v -= G[(size_t)k * nr + i] * y[k];
+      y[i] = v / G[(size_t)i * nr + i];
+    }
+    for (int i = 0; i < nr; ++i) cinv[(size_t)i * nr + col] = y[i];
+  }
+  CK(sc->sk_link.upload(lk));
+  CK(sc->sk_st.alloc(L));
+  CK(cudaMemset(sc->sk_st.p, 0, sizeof(SkelState) * L));
+  CK(sc->sk_rv.upload(std::vector<int>(s.lvert.begin(), s.lvert.end())));
+  CK(sc->sk_rlink.upload(rlink));
+  CK(sc->sk_ridx.upload(ridx));
+  CK(sc->sk_rest.upload(s.lrest));
+  CK(sc->sk_cinv.upload(cinv));
+  CK(sc->sk_zcm.upload(zcm));
+  sc->sk_nq = 12 + L - 1;
+  if (!sc->skel_on) {  // a new scene starts from the identity and zero magnitudes
+    std::vector<double> q0(sc->sk_nq, 0.0);
+    q0[0] = q0[4] = q0[8] = 1.0;
+    CK(sc->sk_jq.upload(q0));
+    CK(sc->sk_jqd.upload(q0));
+  }
+  CK(sc->sk_v0.alloc(3 * (size_t)nr)); CK(sc->sk_w.alloc(3 * (size_t)nr)); CK(sc->sk_rr.alloc(3 * (size_t)nr));
+  CK(sc->sk_q.alloc(3 * (size_t)nr));
+  CK(sc->sk_tv.alloc(3 * (size_t)nr * ndof)); CK(sc->sk_kt.alloc(3 * (size_t)nr * ndof));
+  CK(sc->sk_sm.alloc((size_t)ndof * ndof)); CK(sc->sk_rhs.alloc(ndof)); CK(sc->sk_sol.alloc(ndof));
+  CK(sc->sk_perm.alloc(ndof));
+  sc->skd = SkelDev{L, ndof, nr, N, sc->sk_link.p, sc->sk_st.p, sc->sk_rv.p, sc->sk_rlink.p, sc->sk_ridx.p,
+                    sc->sk_rest.p, sc->sk_cinv.p, sc->sk_zcm.p, sc->sk_jq.p, sc->sk_jqd.p, sc->sk_v0.p, sc->sk_w.p,
+                    sc->sk_rr.p, sc->sk_q.p, sc->sk_tv.p, sc->sk_kt.p, sc->sk_sm.p, sc->sk_rhs.p, sc->sk_sol.p,
+                    sc->sk_perm.p};
+  sc->skel_on = true;
   return DFEM_OK;
 }
 
@@ -1246,6 +1354,7 @@ static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle
                                    sc->ckpt_v.p, sc->flag.p, sc->iters.p,
                                    sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p,
                                    sc->has_contact ? sc->vwc.p : nullptr);
+  if (sc->skel_on) k_skel_begin<<<1, 128, 0, st>>>(sc->skd, sc->xk.p);
   k_loop_enter<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, sc->hs.nparts, sc->hs.K, h);
 }
 
@@ -1293,6 +1402,10 @@ static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandl
   launch_gather(sc, st, g, sc->c0.p, sc->rhs.p, sc->xk.p);
   const cudaError_t ce = capture_solve(sc, st, g, sc->rhs.p, sc->y.p, 0);
   if (ce != cudaSuccess) sc->cur_capture_err = ce;
+  if (sc->skel_on) {  // the links' system, then the free vertices' share of the rigid multiplier
+    k_skel_stage<<<1, 256, 0, st>>>(sc->skd, sc->xt.p, sc->y.p, sc->act_all.p, sc->step.p, s.nseg);
+    k_skel_apply<<<sc->nblk_v, 128, 0, st>>>(sc->skd, sc->y.p);
+  }
   k_update<<<sc->nblk_p, kPartBlock, 0, st>>>(s.N, sc->pd, mixed(sc) ? 1 : 0, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->hist_step, sc->step.p,
                                sc->flag.p, sc->iters.p, sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p);
   k_loop_ctl<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, s.nparts, s.K, h);
@@ -1321,6 +1434,7 @@ static void step_post(dfem_scene* sc, cudaStream_t st) {
   const int nb = sc->nblk_v;
   if (fused_contact(sc)) launch_contact_fused(sc, st);  // a refused launch surfaces through cudaGetLastError
   if (sc->has_contact) k_contact_record<<<1, 1, 0, st>>>(sc->step.p, sc->cstate.p, sc->cpasses.p, sc->cd);
+  if (sc->skel_on) k_skel_end<<<1, 32, 0, st>>>(sc->skd);
   k_step_end<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->xk.p, sc->traj.p, sc->to_user.p,
                                  sc->write_traj.p);
   k_next_step<<<1, 1, 0, st>>>(sc->step.p);
@@ -1341,7 +1455,7 @@ static void adj_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle
   launch_adj_local(sc, st, g, sc->kiter.p);
   launch_adj_gather(sc, st, g);
   if (s.nseg > 0)
-    k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, st>>>(s.nseg, g, sc->seg_part.p, sc->step.p, sc->seg_ptr.p,
+    k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, st>>>(s.nseg, s.M, g, sc->seg_part.p, sc->step.p, sc->seg_ptr.p,
                                                        sc->seg_mus.p, sc->mg.p, sc->gact.p);
   k_adj_loop_ctl<<<1, 1, 0, st>>>(sc->kiter.p, h);
 }
@@ -1622,7 +1736,7 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
                                                                   sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
       k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
       if (s.nseg > 0)
-        k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, kOpen, sc->seg_part.p, sc->step.p,
+        k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, s.M, kOpen, sc->seg_part.p, sc->step.p,
                                                                   sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
       k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a);
       launches += 6 + (ncons > 0 ? 2 : 0) + (s.nseg > 0 ? 1 : 0);
@@ -1641,7 +1755,7 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
                                                                 sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
     k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
     if (s.nseg > 0)
-      k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, kOpen, sc->seg_part.p, sc->step.p,
+      k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, s.M, kOpen, sc->seg_part.p, sc->step.p,
                                                                 sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
     k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a);
     launches += 4 + (ncons > 0 ? 2 : 0) + (s.nseg > 0 ? 1 : 0);
@@ -1989,13 +2103,42 @@ int dfem_set_materials(dfem_scene* sc, const double* youngs, const double* poiss
   RC(gpu_refactor(sc));
   if (sc->has_contact)
     k_hs_diag<<<sc->nblk_v, 128, 0, sc->stream>>>(s.N, sc->hs_ptr.p, sc->hs_col.p, sc->hs_val.p, sc->hdiag.p);
-  // host copies of the moduli follow (the host factor is not used after creation)
+  // host copies of the moduli follow (the host factor is used after creation
+  // only by the skeleton's Schur blocks, refactored here for them)
   if (T > 0) {
     CK(cudaMemcpyAsync(s.tE.data(), sc->tE.p, T * sizeof(double), cudaMemcpyDeviceToHost, sc->stream));
     CK(cudaMemcpyAsync(s.tnu.data(), sc->tnu.p, T * sizeof(double), cudaMemcpyDeviceToHost, sc->stream));
   }
   CK(cudaStreamSynchronize(sc->stream));
+  if (sc->skel_on) {
+    std::string err;
+    const std::vector<double> E(s.tE), nu(s.tnu);
+    if (!update_materials(s, E.data(), nu.data(), err)) return fail(DFEM_ERR_FACTOR, err);
+    RC(upload_skeleton(sc));
+  }
   sc->rec_steps = 0;  // the recorded forward used the old factor
+  return DFEM_OK;
+}
+
+int dfem_set_joint_state(dfem_scene* sc, const double* jq, const double* jqd) {
+  if (!sc || !jq || !jqd) return fail(DFEM_ERR_INVALID, "null argument");
+  if (!sc->skel_on) return fail(DFEM_ERR_INVALID, "the scene has no skeleton");
+  CK(cudaSetDevice(sc->device));
+  CK(cudaStreamSynchronize(sc->stream));
+  for (int i = 0; i < sc->sk_nq; ++i)
+    if (!std::isfinite(jq[i]) || !std::isfinite(jqd[i])) return fail(DFEM_ERR_INVALID, "non-finite joint state");
+  CK(cudaMemcpy(sc->sk_jq.p, jq, sizeof(double) * sc->sk_nq, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(sc->sk_jqd.p, jqd, sizeof(double) * sc->sk_nq, cudaMemcpyHostToDevice));
+  return DFEM_OK;
+}
+
+int dfem_get_joint_state(const dfem_scene* sc, double* jq, double* jqd) {
+  if (!sc || !jq || !jqd) return fail(DFEM_ERR_INVALID, "null argument");
+  if (!sc->skel_on) return fail(DFEM_ERR_INVALID, "the scene has no skeleton");
+  CK(cudaSetDevice(sc->device));
+  CK(cudaStreamSynchronize(sc->stream));
+  CK(cudaMemcpy(jq, sc->sk_jq.p, sizeof(double) * sc->sk_nq, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(jqd, sc->sk_jqd.p, sizeof(double) * sc->sk_nq, cudaMemcpyDeviceToHost));
   return DFEM_OK;
 }
 
@@ -2107,6 +2250,7 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
                        double* g_youngs, double* g_poisson, double* g_act, int mem) {
   if (!sc || !gx_out || !gv_out || !gx || !gv) return fail(DFEM_ERR_INVALID, "null argument");
   if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_step_backward needs a preceding dfem_step_forward");
+  if (sc->skel_on) return fail(DFEM_ERR_UNSUPPORTED, "no adjoint through skeleton links");
   CK(cudaSetDevice(sc->device));
   // contact steps the forward recorded need no replay; the others are replayed
   // with recording on, into records after the forward's (room for the most

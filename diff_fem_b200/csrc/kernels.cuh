@@ -74,13 +74,14 @@ struct SceneDev {
   const double* mfib;   // 3 planes of M
   const int* mseg;
   const int4* mslot;
-  const int* seg_ptr;
-  const int* seg_mus;
+  const int* seg_ptr;   // channel -> members CSR
+  const int* seg_mus;   // member: muscle m as m, pneumatic spring k as -(k+1)
   // springs
   const int2* sv;
   const double* srest;
   const double* ssw;
   const int2* sslot;
+  const int* sch;       // activation channel per spring (-1 plain); null without pneumatic springs
   // bending
   const int* boff;
   const int* bv;
@@ -109,6 +110,10 @@ struct SceneDev {
 };
 
 __device__ __forceinline__ int vpart_of(const SceneDev& d, int i) { return d.vpart ? d.vpart[i] : 0; }
+
+// Index into the activation-term array mg of channel member k (seg_mus):
+// muscle m at m, pneumatic spring s at M + s.
+__host__ __device__ __forceinline__ int member_slot(int M, int k) { return k >= 0 ? k : M - 1 - k; }
 
 // part of constraint t (tets, muscles, springs, bending stencils in that order)
 __device__ __forceinline__ int cons_part(const SceneDev& d, int t) {

@@ -164,6 +164,16 @@ __global__ void k_step_begin(SceneDev d, PartDev pd, const int* step, double* xt
   }
 }
 
+// Projected length of spring t: its rest length, times its channel's
+// activation for a pneumatic spring (md = m_rest_length * mActivationLevel * e,
+// pneumaticEasy.h:133-147).
+__device__ __forceinline__ double spring_length(const SceneDev& d, int t, const double* act_row) {
+  const double r = d.srest[t];
+  if (!d.sch) return r;
+  const int c = d.sch[t];
+  return c < 0 ? r : r * act_row[c];
+}
+
 // Local step of constraint t (tets, muscles, springs, bending stencils in
 // that order): its projection and its J*d contribution to its slots.  The
 // pointers are not restrict-qualified: a kernel that writes x in an earlier
@@ -215,10 +225,11 @@ __device__ __forceinline__ void local_item(const SceneDev& d, int t, const doubl
   }
   t -= d.M;
   if (t < d.S) {
-    // spring (SpringConstraint::EvaluateDVector): d = rest * (x0-x1)/|x0-x1|, J = sqrt(w) [I; -I]
+    // spring (SpringConstraint::EvaluateDVector): d = rest * (x0-x1)/|x0-x1|, J = sqrt(w) [I; -I];
+    // pneumatic spring (PneumaticConstraint::EvaluateDVector): rest * activation
     int2 v = d.sv[t];
     Vec3<double> e = ld3(x, v.x) - ld3(x, v.y);
-    Vec3<double> dd = (d.srest[t] * rsqrt(dot3(e, e))) * e;
+    Vec3<double> dd = (spring_length(d, t, act_all + (size_t)(*step) * d.nseg) * rsqrt(dot3(e, e))) * e;
     double w = d.ssw[t];
     int2 sl = d.sslot[t];
     st3(slot, sl.x, w * dd);
@@ -327,7 +338,8 @@ __global__ void __launch_bounds__(128, DFEM_FORCE_MIN_BLOCKS) k_force_f32(SceneD
     int2 v = d.sv[t];
     const Vec3<double> e = ld3(x, v.x) - ld3(x, v.y);
     const double len = sqrt(dot3(e, e));
-    const Vec3<float> fs = to_f((d.ssw[t] * (d.srest[t] / len - 1.0)) * e);
+    const Vec3<float> fs =
+        to_f((d.ssw[t] * (spring_length(d, t, act_all + (size_t)(*step) * d.nseg) / len - 1.0)) * e);
     int2 sl = d.sslot[t];
     st3f(slot, sl.x, fs);
     st3f(slot, sl.y, (-1.0f) * fs);
@@ -1236,7 +1248,9 @@ __device__ __forceinline__ void adj_local_item(const SceneDev& d, int t, const d
     Vec3<double> e = ld3(x, v.x) - ld3(x, v.y);
     double inv = rsqrt(dot3(e, e));
     Vec3<double> eh = inv * e;
-    Vec3<double> ge = (d.srest[t] * inv) * (db - dot3(eh, db) * eh);
+    // a pneumatic spring's activation term: d md / d a = rest * eh
+    if (d.sch && d.sch[t] >= 0) mg[d.M + t] = d.srest[t] * dot3(db, eh);
+    Vec3<double> ge = (spring_length(d, t, act_row) * inv) * (db - dot3(eh, db) * eh);
     int2 sl = d.sslot[t];
     st3(slot, sl.x, ge);
     st3(slot, sl.y, (-1.0) * ge);
@@ -1289,13 +1303,14 @@ __global__ void k_adj_gather(int N, Gate gate, const int* __restrict__ vpart, co
   st3(xkb, i, acc);
 }
 
-// activation gradient of the step: sum over the muscle constraints of each segment
-__global__ void k_seg_reduce(int nseg, Gate gate, const int* seg_part, const int* step, const int* seg_ptr,
+// activation gradient of the step: sum over the members of each channel
+// (muscle constraints, then pneumatic springs)
+__global__ void k_seg_reduce(int nseg, int M, Gate gate, const int* seg_part, const int* step, const int* seg_ptr,
                              const int* seg_mus, const double* mg, double* gact) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nseg || gate.skip(seg_part ? seg_part[q] : 0)) return;
   double s = 0;
-  for (int k = seg_ptr[q]; k < seg_ptr[q + 1]; ++k) s += mg[seg_mus[k]];
+  for (int k = seg_ptr[q]; k < seg_ptr[q + 1]; ++k) s += mg[member_slot(M, seg_mus[k])];
   gact[(size_t)(*step) * nseg + q] += s;
 }
 

@@ -23,31 +23,21 @@
 #pragma once
 // included after pd_kernels.cu (warp_sum, cluster_rank, cluster_sync_all)
 #include "kernels.cuh"
+#include "resident_plan.h"
 
 namespace dfem {
 
-// One supernode of the resident solve; offsets in doubles from the owner
-// CTA's dynamic shared memory.
-struct ResSn {
-  int c0, w, r;      // first column, width, rows below
-  int dofs;          // Dinv, packed lower triangle by rows (row i at dofs + i (i + 1) / 2)
-  int lofs;          // L_{R,s} (column-major, r x w)
-  int pofs;          // row -> contribution range of its inbox (w + 1 ints)
-  int qofs;          // inbox: 3 doubles per contribution to its rows, grouped by row
-  int yofs;          // its solution values (3 per column)
-  int rofs;          // its below-diagonal rows in the factor's rowidx (the cdst / xsrc tables)
-  int s;             // supernode id (error reports)
-};
-
+// Every CTA's metadata lives in its image (resident_plan.h): a header (item
+// count, the first item of each level, prefix sums for the flat loops), the
+// item records (ResItem) and per item the address tables of its pushes and
+// pulls (32-bit words rank << 24 | offset).  No step of the sweeps waits on
+// a global-memory load; the header and items arrive by a small first bulk
+// copy, so the right-hand side is fetched while the blocks are in flight.
 struct ResDev {
-  const ResSn* sn;          // grouped by owner CTA, then by level
-  const int* sched;         // C x (L + 1): CTA q's items of level l are sn[sched[q (L+1) + l] .. sched[q (L+1) + l + 1])
-  const int2* cdst;         // per below-diagonal row position: (CTA, shared offset) of its contribution slot
-  const int2* xsrc;         // per below-diagonal row position: (CTA, shared offset) of the row's solution values
-  const double* img;        // every CTA's image (blocks and row tables), back to back
+  const double* img;        // every CTA's image, back to back
   const long long* img_ofs; // C + 1 offsets into img (doubles, even)
-  const int* tsh_ofs;       // per CTA: scratch t (3 w_max) and, after it, x_R (3 r_max)
-  int nlev;
+  const int* head_len;      // per CTA: doubles of the header + items part of its image
+  int nlev;                 // levels (every CTA takes 2 nlev + 1 cluster barriers)
   int smem_doubles;         // dynamic shared memory of every CTA (doubles)
   int* status;              // error status word (as FactorDev::status)
 };
@@ -73,12 +63,21 @@ __device__ __forceinline__ void res_fail(const ResDev& d, int s, int which) {
   atomicAdd(d.status + 3, 1);
 }
 
+// A packed address (rank << 24 | offset) checked against the cluster and the
+// shared memory; false (and the error recorded) when out of range.
+__device__ __forceinline__ bool res_addr_ok(const ResDev& d, uint32_t v, int s, int which) {
+  if ((v >> 24) < gridDim.x && (int)(v & 0xFFFFFFu) + 3 <= d.smem_doubles) return true;
+  res_fail(d, s, which);
+  return false;
+}
+
 // Forward solve of one supernode (order of fwd_supernode).
-__device__ __forceinline__ void res_forward(const ResDev& d, const ResSn& in, double* sh, double* t) {
+__device__ __forceinline__ void res_forward(const ResDev& d, const ResItem& in, double* sh, double* t) {
   const int w = in.w, r = in.r, tid = threadIdx.x, nt = blockDim.x;
   const double* D = sh + in.dofs;
   const double* L = sh + in.lofs;
   const int* prow = reinterpret_cast<const int*>(sh + in.pofs);
+  const uint32_t* push = reinterpret_cast<const uint32_t*>(sh + in.tofs);
   const double* q = sh + in.qofs;
   double* ysh = sh + in.yofs;  // holds rhs_s on entry
   for (int c = tid; c < w; c += nt) {
@@ -115,31 +114,28 @@ __device__ __forceinline__ void res_forward(const ResDev& d, const ResSn& in, do
       const double l = L[(size_t)c * r + a];
       a0 += l * ysh[3 * c]; a1 += l * ysh[3 * c + 1]; a2 += l * ysh[3 * c + 2];
     }
-    const int2 dst = d.cdst[in.rofs + a];
-    if ((unsigned)dst.x >= gridDim.x || dst.y < 0 || dst.y + 3 > d.smem_doubles) {
-      res_fail(d, in.s, 8);
-      continue;
-    }
-    const uint32_t o = cluster_map(sh + dst.y, (unsigned)dst.x);
+    const uint32_t dst = push[a];
+    if (!res_addr_ok(d, dst, in.s, 8)) continue;
+    const uint32_t o = cluster_map(sh + (dst & 0xFFFFFFu), dst >> 24);
     st_cluster_f64(o, a0); st_cluster_f64(o + 8, a1); st_cluster_f64(o + 16, a2);
   }
   __syncthreads();  // t is reused by the next item
 }
 
 // Backward solve of one supernode (order of bwd_supernode).
-__device__ __forceinline__ void res_backward(const ResDev& d, const ResSn& in, double* sh, double* t, double* xr) {
+__device__ __forceinline__ void res_backward(const ResDev& d, const ResItem& in, double* sh, double* t, double* xr) {
   const int w = in.w, r = in.r, tid = threadIdx.x, nt = blockDim.x;
   const double* D = sh + in.dofs;
   const double* L = sh + in.lofs;
+  const uint32_t* pull = reinterpret_cast<const uint32_t*>(sh + in.tofs) + r;
   double* ysh = sh + in.yofs;  // holds y_s of the forward sweep on entry
   for (int a = tid; a < r; a += nt) {
-    const int2 src = d.xsrc[in.rofs + a];
-    if ((unsigned)src.x >= gridDim.x || src.y < 0 || src.y + 3 > d.smem_doubles) {
-      res_fail(d, in.s, 9);
+    const uint32_t src = pull[a];
+    if (!res_addr_ok(d, src, in.s, 9)) {
       xr[3 * a] = xr[3 * a + 1] = xr[3 * a + 2] = 0.0;
       continue;
     }
-    const uint32_t o = cluster_map(sh + src.y, (unsigned)src.x);
+    const uint32_t o = cluster_map(sh + (src & 0xFFFFFFu), src >> 24);
     xr[3 * a] = ld_cluster_f64(o); xr[3 * a + 1] = ld_cluster_f64(o + 8); xr[3 * a + 2] = ld_cluster_f64(o + 16);
   }
   for (int k = tid; k < 3 * w; k += nt) t[k] = ysh[k];
@@ -168,55 +164,77 @@ __device__ __forceinline__ void res_backward(const ResDev& d, const ResSn& in, d
   __syncthreads();
 }
 
+// Element j of the CTA's solution regions (j < 3 sum(w)): its item and the
+// offset in it, from the prefix sums cum[] (few items per CTA: linear scan).
+__device__ __forceinline__ int res_item_of(const int* cum, int n, int j) {
+  int i = 0;
+  while (i + 1 < n && cum[i + 1] <= j) ++i;
+  return i;
+}
+
 // Both sweeps in one launch of one cluster (grid = cluster = C CTAs).  Every
-// CTA takes every cluster barrier, whatever happens to its own work, so the
-// barriers always complete; a bounded wait that gives up records status 6 and
-// the CTA skips its arithmetic (the solve's result is then invalid, and the
-// caller reports DFEM_ERR_CAP).
+// CTA takes every cluster barrier (2 nlev + 1 of them), whatever happens to
+// its own work, so the barriers always complete; a bounded wait that gives up
+// records status 6 and the CTA skips its arithmetic (the solve's result is
+// then invalid, and the caller reports DFEM_ERR_CAP).
 __global__ void __launch_bounds__(512, 1) k_solve_resident(ResDev d, Gate gate, const double* __restrict__ rhs,
                                                            double* y) {
   extern __shared__ __align__(16) double sh[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar[2];
   if (gate.skip(0)) return;  // uniform over the cluster: before any barrier
   const unsigned rank = cluster_rank();
-  const int L1 = d.nlev + 1;
-  const int* sched = d.sched + (size_t)rank * L1;
   const long long i0 = d.img_ofs[rank], i1 = d.img_ofs[rank + 1];
-  const unsigned bytes = (unsigned)((i1 - i0) * sizeof(double));
+  const int hl = d.head_len[rank];
+  const unsigned bh = (unsigned)(hl * sizeof(double)), bb = (unsigned)((i1 - i0 - hl) * sizeof(double));
   if (threadIdx.x == 0) {
-    mbar_init(&bar, 1);
-    if (bytes > 0) {
-      mbar_expect_tx(&bar, bytes);
-      bulk_copy_g2s(sh, d.img + i0, bytes, &bar);
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_expect_tx(&bar[0], bh);
+    bulk_copy_g2s(sh, d.img + i0, bh, &bar[0]);
+    if (bb > 0) {
+      mbar_expect_tx(&bar[1], bb);
+      bulk_copy_g2s(sh + hl, d.img + i0 + hl, bb, &bar[1]);
     }
   }
-  // rhs of the owned columns into their solution regions
-  for (int it = sched[0]; it < sched[d.nlev]; ++it) {
-    const ResSn in = d.sn[it];
-    for (int k = threadIdx.x; k < 3 * in.w; k += blockDim.x) sh[in.yofs + k] = rhs[3 * (size_t)in.c0 + k];
+  __syncthreads();  // the barriers are initialised before anyone waits on them
+  const bool okh = __syncthreads_and(mbar_wait_bounded(&bar[0], 0)) != 0;
+  const int* hdr = reinterpret_cast<const int*>(sh);
+  const int n = okh ? hdr[0] : 0;
+  const ResItem* items = reinterpret_cast<const ResItem*>(sh + (okh ? hdr[5] : 0));
+  const int* sched = hdr + kResHeadInts;
+  const int* cum = sched + d.nlev + 1;
+  const int ncols3 = okh ? hdr[2] : 0;
+  // the right-hand side of the owned columns into their solution regions
+  for (int j = threadIdx.x; j < ncols3; j += blockDim.x) {
+    const int i = res_item_of(cum, n, j);
+    const int k = j - cum[i];
+    sh[items[i].yofs + k] = rhs[3 * (size_t)items[i].c0 + k];
   }
   cluster_sync_all();  // every CTA of the cluster runs: its shared memory may be written
-  const bool ok = __syncthreads_and(bytes == 0 || mbar_wait_bounded(&bar, 0)) != 0;
+  const bool okb = __syncthreads_and(bb == 0 || mbar_wait_bounded(&bar[1], 0)) != 0;
+  const bool ok = okh && okb;
   if (!ok && threadIdx.x == 0) res_fail(d, -1, 7);
-  double* t = sh + d.tsh_ofs[rank];
-  double* xr = sh + d.tsh_ofs[rank + (int)gridDim.x];
+  double* t = sh + (ok ? hdr[3] : 0);
+  double* xr = sh + (ok ? hdr[4] : 0);
   for (int l = 0; l < d.nlev; ++l) {
     if (ok)
-      for (int it = sched[l]; it < sched[l + 1]; ++it) res_forward(d, d.sn[it], sh, t);
+      for (int it = sched[l]; it < sched[l + 1]; ++it) res_forward(d, items[it], sh, t);
     cluster_sync_all();  // the level's contributions have landed in their owners' inboxes
   }
   for (int l = d.nlev - 1; l >= 0; --l) {
     if (ok)
-      for (int it = sched[l]; it < sched[l + 1]; ++it) res_backward(d, d.sn[it], sh, t, xr);
+      for (int it = sched[l]; it < sched[l + 1]; ++it) res_backward(d, items[it], sh, t, xr);
     cluster_sync_all();  // the level's solution values are final; no CTA reads another's after the last one
   }
   if (ok) {
-    for (int it = sched[0]; it < sched[d.nlev]; ++it) {
-      const ResSn in = d.sn[it];
-      for (int k = threadIdx.x; k < 3 * in.w; k += blockDim.x) y[3 * (size_t)in.c0 + k] = sh[in.yofs + k];
+    for (int j = threadIdx.x; j < ncols3; j += blockDim.x) {
+      const int i = res_item_of(cum, n, j);
+      const int k = j - cum[i];
+      y[3 * (size_t)items[i].c0 + k] = sh[items[i].yofs + k];
     }
-  } else if (threadIdx.x == 0 && bytes > 0) {
-    mbar_wait_bounded(&bar, 0);  // give the image copy one more bounded chance to land before the CTA exits
+  } else if (threadIdx.x == 0) {  // give the copies one more bounded chance to land before the CTA exits
+    mbar_wait_bounded(&bar[0], 0);
+    if (bb > 0) mbar_wait_bounded(&bar[1], 0);
   }
 }
 

@@ -156,7 +156,7 @@ void build_slots(HostScene& s) {
 
 void renumber(HostScene& s, const std::vector<int>& to_int) {
   auto remap = [&](std::vector<int>& v) { for (int& i : v) i = to_int[i]; };
-  remap(s.tv); remap(s.mv); remap(s.sv); remap(s.bv); remap(s.av); remap(s.cverts); remap(s.df);
+  remap(s.tv); remap(s.mv); remap(s.sv); remap(s.bv); remap(s.av); remap(s.cverts); remap(s.df); remap(s.lvert);
   std::vector<double> x(3 * (size_t)s.N), m(s.N), g(s.N);
   for (int i = 0; i < s.N; ++i) {
     int j = to_int[i];
@@ -278,15 +278,6 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& s, std::string& err) 
     REQ(element(d.x0, d.muscle_tets + 4 * m, &s.mv[4 * m], &s.minv[9 * m], s.mvol[m]), "descriptor: degenerate muscle tet");
     REQ(s.mseg[m] >= 0 && s.mseg[m] < s.nseg, "descriptor: muscle segment id out of range");
   }
-  s.seg_ptr.assign(s.nseg + 1, 0);
-  for (int m = 0; m < s.M; ++m) s.seg_ptr[s.mseg[m] + 1]++;
-  for (int q = 0; q < s.nseg; ++q) s.seg_ptr[q + 1] += s.seg_ptr[q];
-  s.seg_mus.assign(s.M, 0);
-  {
-    std::vector<int> fill(s.seg_ptr.begin(), s.seg_ptr.end() - 1);
-    for (int m = 0; m < s.M; ++m) s.seg_mus[fill[s.mseg[m]]++] = m;
-  }
-
   s.S = d.n_springs;
   s.sv.assign(d.spring_vertices, d.spring_vertices + 2 * (size_t)s.S);
   s.srest.resize(s.S); s.ssw.resize(s.S);
@@ -295,7 +286,77 @@ bool build_host_scene(const dfem_scene_desc& d, HostScene& s, std::string& err) 
     REQ(i0 != i1, "descriptor: spring with identical vertices");
     s.srest[k] = d.spring_rest ? d.spring_rest[k] : normp(sub(pt(d.x0, i0), pt(d.x0, i1)));  // getEdgeLength
     REQ(d.spring_weight[k] >= 0, "descriptor: negative spring weight");
-    s.ssw[k] = std::sqrt(d.spring_weight[k]);  // SpringConstraint: mStretch = sqrt(weight)
+    // SpringConstraint and PneumaticConstraint alike: mStretch = sqrt(weight)
+    s.ssw[k] = std::sqrt(d.spring_weight[k]);
+  }
+  // pneumatic springs (Dfobj.h:232-251 builds one per consecutive pair of a
+  // "Volume Verts" polyline; SetActions sets each one's activation directly)
+  bool any_channel = false;
+  if (d.spring_channel)
+    for (int k = 0; k < s.S; ++k) {
+      REQ(d.spring_channel[k] >= -1 && d.spring_channel[k] < s.nseg, "descriptor: spring channel out of range");
+      any_channel = any_channel || d.spring_channel[k] >= 0;
+    }
+  if (any_channel) s.sch.assign(d.spring_channel, d.spring_channel + s.S);
+
+  // channel -> members CSR (muscle m as m, pneumatic spring k as -(k+1)),
+  // muscles first, each in ascending order
+  s.seg_ptr.assign(s.nseg + 1, 0);
+  for (int m = 0; m < s.M; ++m) s.seg_ptr[s.mseg[m] + 1]++;
+  for (int k = 0; k < (int)s.sch.size(); ++k)
+    if (s.sch[k] >= 0) s.seg_ptr[s.sch[k] + 1]++;
+  for (int q = 0; q < s.nseg; ++q) s.seg_ptr[q + 1] += s.seg_ptr[q];
+  s.seg_mus.assign(s.seg_ptr[s.nseg], 0);
+  {
+    std::vector<int> fill(s.seg_ptr.begin(), s.seg_ptr.end() - 1);
+    for (int m = 0; m < s.M; ++m) s.seg_mus[fill[s.mseg[m]]++] = m;
+    for (int k = 0; k < (int)s.sch.size(); ++k)
+      if (s.sch[k] >= 0) s.seg_mus[fill[s.sch[k]]++] = -(k + 1);
+  }
+
+  // articulated skeleton (Dfobj.h:254-288, World::AddBody World.h:499-545)
+  REQ(d.n_links >= 0 && d.n_links <= kMaxLinks, "descriptor: n_links out of range");
+  if (d.n_links > 0) {
+    REQ(d.link_parent && d.link_type && d.link_joint && d.link_axis && d.link_offsets && d.link_vertices,
+        "descriptor: link arrays missing");
+    REQ(d.precision == DFEM_PREC_FP64, "descriptor: skeleton links need the FP64 form");
+    REQ(!d.handle_collision, "descriptor: skeleton links with collision handling are not supported (the "
+        "reference's contact phase solves the rigid vertices with the free-vertex factor)");
+    s.L = d.n_links;
+    s.lparent.assign(d.link_parent, d.link_parent + s.L);
+    s.ltype.assign(d.link_type, d.link_type + s.L);
+    s.lchan.assign(s.L, -1);
+    if (d.link_channel) s.lchan.assign(d.link_channel, d.link_channel + s.L);
+    s.loff.assign(d.link_offsets, d.link_offsets + s.L + 1);
+    s.ljoint.assign(d.link_joint, d.link_joint + 3 * (size_t)s.L);
+    s.laxis.assign(3 * (size_t)s.L, 0.0);
+    REQ(s.loff[0] == 0, "descriptor: link_offsets must start at 0");
+    REQ(s.lparent[0] == -1 && s.ltype[0] == DFEM_JOINT_ALL, "descriptor: link 0 must be the root, of joint type ALL");
+    for (int l = 0; l < s.L; ++l) {
+      REQ(s.loff[l + 1] > s.loff[l], "descriptor: every link needs at least one vertex");
+      REQ(s.lchan[l] >= -1 && s.lchan[l] < s.nseg, "descriptor: link torque channel out of range");
+      for (int c = 0; c < 3; ++c) REQ(std::isfinite(s.ljoint[3 * l + c]), "descriptor: non-finite joint position");
+      if (l == 0) continue;
+      REQ(s.lparent[l] >= 0 && s.lparent[l] < l, "descriptor: a link's parent must precede it");
+      REQ(s.ltype[l] == DFEM_JOINT_ROTATIONAL || s.ltype[l] == DFEM_JOINT_PRISMATIC,
+          "descriptor: non-root links must be ROTATIONAL or PRISMATIC");
+      const double* a = d.link_axis + 3 * l;
+      const double n = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+      REQ(std::isfinite(n) && n > 0, "descriptor: zero or non-finite joint axis");
+      for (int c = 0; c < 3; ++c) s.laxis[3 * l + c] = a[c] / n;  // jointAxis / jointAxis.norm()
+    }
+    const int nr = s.loff[s.L];
+    REQ(nr <= kMaxRigidVertices, "descriptor: too many link vertices");
+    s.lvert.assign(d.link_vertices, d.link_vertices + nr);
+    REQ(inrange(s.lvert.data(), nr), "descriptor: link vertex out of range");
+    std::vector<char> used(N, 0);
+    s.lrest.resize(3 * (size_t)nr);
+    for (int k = 0; k < nr; ++k) {
+      REQ(!used[s.lvert[k]], "descriptor: a vertex belongs to two links");
+      used[s.lvert[k]] = 1;
+      for (int c = 0; c < 3; ++c) s.lrest[3 * k + c] = d.x0[3 * (size_t)s.lvert[k] + c];  // Link::restpos
+    }
+    REQ(nr < N, "descriptor: every vertex is rigid");
   }
 
   s.B = d.n_bending;
@@ -380,6 +441,7 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
         "batch: scenes must share time_step, damping, gravity, max_iterations, precision and checkpoint_every");
     REQ(!(p.collide && !p.cverts.empty() && !p.obs_f.empty()), "batch: obstacle contact is supported for single scenes only");
     REQ(!p.self_collide, "batch: soft-soft contact is supported for single scenes only");
+    REQ(p.L == 0, "batch: skeleton links are supported for single scenes only");
     REQ(p.nparts == 1, "batch: parts must be single scenes");
     totN += p.N; totT += p.T; totSlots += p.nslots; totRows += (int64_t)p.F.rowidx.size();
     totL += (int64_t)p.F.Lcm.size(); totD += (int64_t)p.F.Dinv.size(); totF += (int64_t)p.df.size() / 3;
@@ -399,7 +461,9 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
   u.vf_ptr = {0};
   SupernodalFactor& F = u.F;
   F.sn_rofs = {0}; F.sn_lofs = {0}; F.sn_dofs = {0}; F.rseg_ptr = {0};
-  int voff = 0, moff = 0, segoff = 0, slotoff = 0, bvoff = 0, snoff = 0, rsegoff = 0;
+  int voff = 0, moff = 0, soff = 0, segoff = 0, slotoff = 0, bvoff = 0, snoff = 0, rsegoff = 0;
+  bool any_channel = false;
+  for (const HostScene& p : P) any_channel = any_channel || !p.sch.empty();
   int64_t hsoff = 0, rofs = 0, lofs = 0, dofs = 0;
   std::vector<int> sn_base(P.size());
   for (size_t q = 0; q < P.size(); ++q) {
@@ -409,7 +473,8 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
     cat_off(u.tslot, p.tslot, slotoff);
     cat_off(u.mv, p.mv, voff); cat(u.minv, p.minv); cat(u.mvol, p.mvol); cat(u.mk, p.mk); cat(u.mfib, p.mfib);
     cat_off(u.mseg, p.mseg, segoff); cat_off(u.mslot, p.mslot, slotoff);
-    cat_ptr(u.seg_ptr, p.seg_ptr, moff); cat_off(u.seg_mus, p.seg_mus, moff);
+    cat_ptr(u.seg_ptr, p.seg_ptr, (int)u.seg_mus.size());
+    for (int k : p.seg_mus) u.seg_mus.push_back(k >= 0 ? k + moff : k - soff);
     cat_off(u.sv, p.sv, voff); cat_off(u.sslot, p.sslot, slotoff); cat(u.srest, p.srest); cat(u.ssw, p.ssw);
     cat_ptr(u.boff, p.boff, bvoff); cat_off(u.bv, p.bv, voff); cat_off(u.bslot, p.bslot, slotoff);
     cat(u.bbeta, p.bbeta); cat(u.bw, p.bw); cat(u.brest, p.brest);
@@ -437,7 +502,11 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
     F.reg = std::max(F.reg, G.reg);
     F.nlevels = std::max(F.nlevels, G.nlevels);
     sn_base[q] = snoff;
-    voff += p.N; moff += p.M; segoff += p.nseg; slotoff += p.nslots; bvoff += (int)p.bv.size();
+    if (any_channel) {
+      if (p.sch.empty()) u.sch.insert(u.sch.end(), p.S, -1);
+      else for (int c : p.sch) u.sch.push_back(c < 0 ? -1 : c + segoff);
+    }
+    voff += p.N; moff += p.M; soff += p.S; segoff += p.nseg; slotoff += p.nslots; bvoff += (int)p.bv.size();
     snoff += G.nsuper; rsegoff += (int)G.rseg_pos.size();
     hsoff += p.Hs.ptr[p.N]; rofs += (int64_t)G.rowidx.size(); lofs += (int64_t)G.Lcm.size(); dofs += (int64_t)G.Dinv.size();
     u.T += p.T; u.M += p.M; u.S += p.S; u.B += p.B; u.A += p.A;

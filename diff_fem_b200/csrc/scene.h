@@ -15,6 +15,12 @@
 
 namespace dfem {
 
+// Skeleton limits: links (the root's 6 dofs plus one per other link form the
+// dense system of World::ComputeSolution) and rigid vertices (the dense
+// Schur complement of the free vertices, World.h:1134-1135).
+constexpr int kMaxLinks = 64;
+constexpr int kMaxRigidVertices = 2048;
+
 struct HostScene {
   int N = 0;
   std::vector<double> x0, mass, gmask;  // internal order
@@ -30,11 +36,12 @@ struct HostScene {
   std::vector<int> mv;                  // 4M
   std::vector<double> minv, mvol, mk, mfib;  // 9M, M, M, 3M
   std::vector<int> mseg, mslot;
-  std::vector<int> seg_ptr, seg_mus;    // CSR segment -> muscle constraints
+  std::vector<int> seg_ptr, seg_mus;    // CSR channel -> members: muscle m as m, pneumatic spring s as -(s+1)
 
   int S = 0;                            // springs
   std::vector<int> sv, sslot;           // 2S
   std::vector<double> srest, ssw;       // rest length, sqrt(weight)
+  std::vector<int> sch;                 // activation channel of each spring (-1 = plain); empty if none
 
   int B = 0;                            // bending stencils
   std::vector<int> boff, bv, bslot;     // CSR (centre first), slots
@@ -60,6 +67,14 @@ struct HostScene {
   // and every vertex's faces in ascending face order (CSR)
   bool underwater = false;
   std::vector<int> df, vf_ptr, vf_face;
+
+  // articulated skeleton (Link tree; link 0 the root): per link parent,
+  // joint type (enum dfem_joint), torque channel, joint position and unit
+  // axis (3 each), and its vertices (CSR, internal ids) with their rest
+  // positions (3 each); the links' dofs are 6 for the root, 1 for the others
+  int L = 0;
+  std::vector<int> lparent, ltype, lchan, loff, lvert;
+  std::vector<double> ljoint, laxis, lrest;
 
   int nslots = 0;
   std::vector<int> vslot_ptr;           // N+1, slots sorted by vertex

@@ -122,6 +122,34 @@ class Scene:
         p, m, k = _ptr(act)
         check(lib().dfem_set_activations(self._h, p, m))
 
+    @property
+    def n_joint_state(self) -> int:
+        """Length of the skeleton's joint state (12 + links - 1), 0 without links."""
+        d = self.desc if not isinstance(self.desc, list) else None
+        nl = int(np.asarray(d.link_parent).size) if d is not None else 0
+        return 12 + nl - 1 if nl else 0
+
+    def joint_state(self):
+        """(jq, jqd): World::mJointQ / mJointQd of the skeleton after the last
+        forward call (the root's T, row-major R then d, and the other links'
+        magnitudes; jqd the previous step's)."""
+        n = self.n_joint_state
+        jq, jqd = np.zeros(n), np.zeros(n)
+        if n:
+            P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+            check(lib().dfem_get_joint_state(self._h, P(jq), P(jqd)))
+        return jq, jqd
+
+    def set_joint_state(self, jq, jqd):
+        n = self.n_joint_state
+        jq = np.ascontiguousarray(jq, np.float64).reshape(-1)
+        jqd = np.ascontiguousarray(jqd, np.float64).reshape(-1)
+        if jq.size != n or jqd.size != n:
+            raise ValueError(f"joint state needs {n} values each")
+        if n:
+            P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+            check(lib().dfem_set_joint_state(self._h, P(jq), P(jqd)))
+
     def forward(self, x, v, n_steps: int = 1, act=None, traj: bool = False):
         """Run n_steps steps from (x, v).  Returns (x_out, v_out[, traj]) in the
         input's memory kind (numpy for host input, CUDA tensors for device input)."""

@@ -2,7 +2,8 @@
 
 Follows the setup code of the reference (all setup-time, host side):
   Environment::Environment   sim/Environment.h:86-225   (Parameters, Meshes, Clothes, Obstacles)
-  Dfobj::SetDfobj/Initialize sim/Dfobj.h:142-611        (tet OBJ, masses, attachments, surface, muscles)
+  Dfobj::SetDfobj/Initialize sim/Dfobj.h:142-611        (tet OBJ, masses, attachments, surface, muscles,
+                                                          pneumatic "Volume Verts" springs, "Bones")
   Environment "Is underwater"  sim/Environment.h:161-166,236-247 (drag faces = the meshes' contours)
   Muscle / MakeMuscles       sim/Muscle.h:59-215, sim/Dfobj.h:732-790
   Dfcloth                    sim/Dfcloth.h:120-300      (edge springs w = 200, masses 1.5 * area / 3, no gravity)
@@ -174,6 +175,10 @@ class Body:
     segments_per_muscle: int = 50
     contours: Optional[np.ndarray] = None   # surface faces for OBJ output (local ids)
     seg_offset: int = 0
+    n_pneumatic: int = 0      # pneumatic springs ("Volume Verts"), one activation channel each
+    pneumatic_offset: int = 0  # first channel of the pneumatic springs
+    n_links: int = 0          # skeleton links ("Bones"); link torques on channels
+    torque_offset: int = 0    # first channel of the joint torques (links 1..n_links-1)
 
 
 @dataclass
@@ -200,7 +205,8 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
     tets, E, NU = [], [], []
     av, ap, ak = [], [], []
     mt, mf, mk, ms = [], [], [], []
-    spv, spw = [], []
+    spv, spw, spc, spr = [], [], [], []
+    lpar, ltyp, ljnt, lax, loff, lvt, lch = [], [], [], [], [0], [], []
     cverts, cfaces, dfaces = [], [], []
     bodies: List[Body] = []
     off, nseg_total = 0, 0
@@ -229,6 +235,46 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
             mt.append(a + off); mf.append(b); mk.append(c); ms.append(d + nseg_total)
             body.n_muscles = len(fibres)
             nseg_total += nseg
+        if "Volume Verts" in obj:
+            # Dfobj.h:231-251: each polyline of "Volume Verts" becomes one
+            # PneumaticConstraint per consecutive vertex pair, rest length from
+            # the scaled mesh, weight = "Muscle Stiffness"; Dfobj::SetActions
+            # (actuator type 3) drives each one's activation directly
+            kp = float(obj.get("Muscle Stiffness", 5e5))
+            body.pneumatic_offset = nseg_total
+            for line in obj["Volume Verts"]:
+                ids = [int(q) for q in line]
+                for i0, i1 in zip(ids[:-1], ids[1:]):
+                    if not (0 <= i0 < n and 0 <= i1 < n) or i0 == i1:
+                        raise SceneFormatError(f"{path}: bad volume vertex pair ({i0}, {i1}) for {n} vertices")
+                    spv.append((i0 + off, i1 + off)); spw.append(kp)
+                    spr.append(float(np.linalg.norm(v[i0] - v[i1]))); spc.append(nseg_total)
+                    nseg_total += 1
+                    body.n_pneumatic += 1
+        if "Bones" in obj:
+            # Dfobj.h:254-288: one Link per bone; "Joint Pos" unscaled (plus the
+            # mesh offset, zero here), "Joint Axis" normalised, the bone's
+            # vertices rigid.  The joint torques of actuator type 1
+            # (World::mJointTorque) go on one channel per non-root link.
+            if lpar:
+                raise SceneFormatError(f"{path}: bones on more than one mesh (one skeleton root per scene)")
+            kinds = {"ALL": 2, "ROTATIONAL": 1, "PRISMATIC": 0}
+            body.torque_offset = nseg_total
+            for li, bone in enumerate(obj["Bones"]):
+                jt = kinds.get(bone.get("Joint Type"))
+                if jt is None:
+                    raise SceneFormatError(f"{path}: bone {li}: unknown joint type {bone.get('Joint Type')!r}")
+                lpar.append(int(bone["Parent ID"])); ltyp.append(jt)
+                ljnt.append([float(q) for q in bone["Joint Pos"]]); lax.append([float(q) for q in bone["Joint Axis"]])
+                ids = [int(q) for q in bone["Vertices"]]
+                if any(not 0 <= q < n for q in ids):
+                    raise SceneFormatError(f"{path}: bone {li}: vertex out of range [0, {n})")
+                lvt.extend(q + off for q in ids); loff.append(len(lvt))
+                if li > 0:
+                    lch.append(nseg_total); nseg_total += 1
+                else:
+                    lch.append(-1)
+            body.n_links = len(lpar)
         bodies.append(body)
         off += n
     for obj in cfg.get("Clothes", []):
@@ -239,6 +285,7 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
         xs.append(v); masses.append(S.triangle_masses(v, f, 1.5)); gmask.append(np.zeros(n, np.uint8))
         for a, b in edges:
             spv.append((a + off, b + off)); spw.append(200.0)  # CollisionMesh::getEdgeConstraint
+            spr.append(float(np.linalg.norm(v[a] - v[b]))); spc.append(-1)
         if "Attach Verts" in obj:
             k = float(obj["Attach Stiffness"])
             for i in sorted(set(int(q) for q in obj["Attach Verts"])):
@@ -266,6 +313,14 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
         muscle_tets=cat(mt, (0, 4), np.int32), muscle_fiber=cat(mf, (0, 3), np.float64),
         muscle_stiffness=cat(mk, (0,), np.float64), muscle_segment=cat(ms, (0,), np.int32), n_segments=nseg_total,
         spring_vertices=np.asarray(spv, np.int32).reshape(-1, 2), spring_weight=np.asarray(spw, np.float64),
+        # explicit rest lengths only with pneumatic springs (otherwise the
+        # engine takes getEdgeLength of x0, as before)
+        spring_rest=np.asarray(spr, np.float64) if any(c >= 0 for c in spc) else None,
+        spring_channel=np.asarray(spc, np.int32) if any(c >= 0 for c in spc) else None,
+        link_parent=np.asarray(lpar, np.int32), link_type=np.asarray(ltyp, np.int32),
+        link_joint=np.asarray(ljnt, np.float64).reshape(-1, 3), link_axis=np.asarray(lax, np.float64).reshape(-1, 3),
+        link_offsets=np.asarray(loff, np.int32), link_vertices=np.asarray(lvt, np.int32),
+        link_channel=np.asarray(lch, np.int32) if lch else None,
         contact_vertices=np.asarray(cverts, np.int32), contact_faces=np.asarray(cfaces, np.int32).reshape(-1, 3),
         obstacle_x=cat(ox, (0, 3), np.float64), obstacle_faces=cat(of, (0, 3), np.int32),
         time_step=1.0 / hz, max_iterations=int(par.get("Max Iteration", 30)),

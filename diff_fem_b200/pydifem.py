@@ -13,11 +13,13 @@ Same functions, argument order and meaning as the reference's pybind11 module
 
 Differences: values are FP64 numpy arrays (the reference returns float lists
 that api_diff.py truncates to float32); gradients come from the engine's
-adjoint instead of a CppAD tape; articulated bones (jq, jqd) are not part of
-this engine and stay empty.  The actuator front-end of type 2 (muscles:
+adjoint instead of a CppAD tape; the joint state (jq, jqd) of an articulated
+skeleton is stepped forward (backward_act through links is not supported).  The actuator front-end of type 2 (muscles:
 Normalizer::NormToReal, Muscle::SetActivationLevels with the SetKey table,
 sim/Normalizer.h:94-112, sim/Muscle.h:224-261, sim/Dfobj.h:628-667) is
-evaluated with torch so that dL/dtau follows from the engine's dL/d(activation).
+evaluated with torch so that dL/dtau follows from the engine's dL/d(activation);
+type 3 (pneumatic springs, sim/Dfobj.h:326-330) maps tau to the springs'
+activation channels one to one.
 """
 from __future__ import annotations
 
@@ -88,8 +90,13 @@ class Dfobj:
         self.body = body
         self.mNumUnknown = 3 * body.n
         self.n_muscles = body.n_muscles
-        self.mActions = np.zeros(4 * self.n_muscles if body.actuator_type == 2 else 0)
+        n_act = {1: max(0, body.n_links - 1), 2: 4 * self.n_muscles, 3: body.n_pneumatic}.get(body.actuator_type, 0)
+        self.mActions = np.zeros(n_act)
         self.levels = np.zeros((self.n_muscles, 50))
+        # PneumaticConstraint::mActivationLevel starts at 1 (pneumaticEasy.h:31)
+        self.pneumatic_levels = np.ones(body.n_pneumatic)
+        # World::mJointTorque of the non-root links (World.h:372-373: zero at start)
+        self.torques = np.zeros(max(0, body.n_links - 1))
         self.keys = _muscle_keys(self.n_muscles) if self.n_muscles else np.zeros((50, 0))
 
     def GetActivationLevelsAggregate(self) -> np.ndarray:
@@ -133,26 +140,45 @@ class Environment:
         self.mDfobjs = [Dfobj(b) for b in loaded.bodies if b.kind == "mesh"]
         self.mPhase = 0
         self.total_step = loaded.total_step
+        self._jq0 = self.scene.joint_state()[0]  # World::Initialize: the links' WriteT (World.h:369-370)
+        self.mSoftWorld.mJointQ = self._jq0.copy()
+        self.mSoftWorld.mJointQd = self._jq0.copy()
+        self.mSoftWorld.mJointTorque = np.zeros(max(0, self._jq0.size - 12))
         self._E = np.asarray(self.desc.youngs, np.float64).copy()
         self._nu = np.asarray(self.desc.poisson, np.float64).copy()
 
-    # segment activations of every muscle of every body, in engine order
+    # activation channels of the engine: every body's muscle segments at its
+    # seg_offset, its pneumatic springs at its pneumatic_offset
     def segment_activations(self) -> np.ndarray:
-        parts = [o.levels.reshape(-1) for o in self.mDfobjs if o.n_muscles]
-        acts = np.concatenate(parts) if parts else np.zeros(0)
-        n = self.desc.n_segments
-        out = np.zeros(n)
-        out[: min(n, acts.size)] = acts[:n]
+        out = np.zeros(self.desc.n_segments)
+        for o in self.mDfobjs:
+            if o.n_muscles:
+                lv = o.levels.reshape(-1)
+                out[o.body.seg_offset:o.body.seg_offset + lv.size] = lv
+            if o.body.n_pneumatic:
+                out[o.body.pneumatic_offset:o.body.pneumatic_offset + o.body.n_pneumatic] = o.pneumatic_levels
+            if o.torques.size:
+                out[o.body.torque_offset:o.body.torque_offset + o.torques.size] = o.torques
         return out
 
     def SetActions(self, tau) -> None:
+        """Dfobj::SetActions (sim/Dfobj.h:315-331): type 1 sets the joint
+        torques (World::mJointTorque), type 2 goes through the muscle
+        front-end, type 3 sets each pneumatic spring's activation directly."""
         k = 0
         for o in self.mDfobjs:
             n = o.mActions.size
-            if n and o.body.actuator_type == 2:
+            if n and o.body.actuator_type == 1:
+                o.torques = np.asarray(tau[k:k + n], np.float64).copy()
+                o.mActions = o.torques.copy()
+                self.mSoftWorld.mJointTorque = o.torques.copy()
+            elif n and o.body.actuator_type == 2:
                 t = torch.as_tensor(np.asarray(tau[k:k + n], np.float64))
                 o.levels = o.activation_from_actions(t, self.mPhase, torch.as_tensor(o.levels)).numpy()
                 o.mActions = np.asarray(tau[k:k + n], np.float64).copy()
+            elif n and o.body.actuator_type == 3:
+                o.pneumatic_levels = np.asarray(tau[k:k + n], np.float64).copy()
+                o.mActions = o.pneumatic_levels.copy()
             k += n
 
     def IncPhase(self) -> None:
@@ -161,6 +187,12 @@ class Environment:
     def Reset(self) -> None:
         for o in self.mDfobjs:
             o.levels[:] = 0.0
+            o.pneumatic_levels[:] = 1.0
+            o.torques[:] = 0.0
+        if self.scene.n_joint_state:
+            self.scene.set_joint_state(self._jq0, self._jq0)
+            self.mSoftWorld.mJointQ = self._jq0.copy()
+            self.mSoftWorld.mJointQd = self._jq0.copy()
         self.mPhase = 0
         self.mSoftWorld.mX = self.desc.x0.reshape(-1).copy()
         self.mSoftWorld.mV[:] = 0.0
@@ -187,10 +219,22 @@ def forward_act(q, qd, jq, jqd, tau, env: Environment, is_act: bool):
         env.SetActions(np.asarray(tau, np.float64))
         env.IncPhase()
     act = env.segment_activations()
+    _set_joints(env, jq, jqd)
     x, v = env.scene.forward(np.asarray(q, np.float64), np.asarray(qd, np.float64), n_steps=1,
                              act=act.reshape(1, -1) if act.size else None)
     env.mSoftWorld.mX, env.mSoftWorld.mV = x.copy(), v.copy()
-    return [x, v, np.zeros(0), np.zeros(0)]
+    njq, njqd = env.scene.joint_state()
+    env.mSoftWorld.mJointQ, env.mSoftWorld.mJointQd = njq.copy(), njqd.copy()
+    return [x, v, njq, njqd]
+
+
+def _set_joints(env: Environment, jq, jqd) -> None:
+    """Environment::Step writes jq / jqd into World::mJointQ / mJointQd before
+    stepping (sim/Environment.h:278-279); empty arrays keep the current state."""
+    jq = np.asarray(jq, np.float64).reshape(-1)
+    jqd = np.asarray(jqd, np.float64).reshape(-1)
+    if env.scene.n_joint_state and jq.size:
+        env.scene.set_joint_state(jq, jqd)
 
 
 def backward_act(q, qd, jq, jqd, tau, dldq, dldqd, dldjq, dldjqd, env: Environment, is_act: bool):
@@ -198,27 +242,38 @@ def backward_act(q, qd, jq, jqd, tau, dldq, dldqd, dldjq, dldjqd, env: Environme
         return _backward_act(q, qd, jq, jqd, tau, dldq, dldqd, dldjq, dldjqd, env, is_act)
 
 
+def _channels_t(env: Environment, tau_t, is_act: bool):
+    """The step's activation channels as a torch vector, differentiable in
+    tau through the actuator front-ends (types 2 and 3)."""
+    out = torch.as_tensor(env.segment_activations()).clone()
+    k = 0
+    for o in env.mDfobjs:
+        n = o.mActions.size
+        b = o.body
+        if is_act and n and b.actuator_type == 1:
+            out = torch.cat([out[:b.torque_offset], tau_t[k:k + n], out[b.torque_offset + n:]])
+        elif is_act and n and b.actuator_type == 2:
+            lv = o.activation_from_actions(tau_t[k:k + n], env.mPhase, torch.as_tensor(o.levels)).reshape(-1)
+            out = torch.cat([out[:b.seg_offset], lv, out[b.seg_offset + lv.numel():]])
+        elif is_act and n and b.actuator_type == 3:
+            out = torch.cat([out[:b.pneumatic_offset], tau_t[k:k + n], out[b.pneumatic_offset + n:]])
+        k += n
+    return out
+
+
 def _backward_act(q, qd, jq, jqd, tau, dldq, dldqd, dldjq, dldjqd, env: Environment, is_act: bool):
     tau_t = torch.tensor(np.asarray(tau, np.float64), requires_grad=True)
-    acts_t = []
+    chan = _channels_t(env, tau_t, is_act)
     if is_act:
-        k = 0
-        for o in env.mDfobjs:
-            n = o.mActions.size
-            if n and o.body.actuator_type == 2:
-                acts_t.append(o.activation_from_actions(tau_t[k:k + n], env.mPhase, torch.as_tensor(o.levels)).reshape(-1))
-            elif o.n_muscles:
-                acts_t.append(torch.as_tensor(o.levels.reshape(-1)))
-            k += n
         env.mPhase += 1
-    act_np = (torch.cat(acts_t).detach().numpy() if acts_t else env.segment_activations())[: env.desc.n_segments]
+    act_np = chan.detach().numpy()
+    _set_joints(env, jq, jqd)
     env.scene.forward(np.asarray(q, np.float64), np.asarray(qd, np.float64), n_steps=1,
                       act=act_np.reshape(1, -1) if act_np.size else None)
     g = env.scene.backward(np.asarray(dldq, np.float64), np.asarray(dldqd, np.float64))
     dtau = np.zeros(len(tau))
-    if is_act and acts_t and g["act"].size:
-        flat = torch.cat(acts_t)[: env.desc.n_segments]
-        (gt,) = torch.autograd.grad(flat, tau_t, torch.as_tensor(g["act"][0]), allow_unused=True)
+    if is_act and chan.requires_grad and g["act"].size:
+        (gt,) = torch.autograd.grad(chan, tau_t, torch.as_tensor(g["act"][0]), allow_unused=True)
         if gt is not None:
             dtau = gt.numpy()
     return [g["x"], g["v"], np.zeros(0), np.zeros(0), dtau]

@@ -49,6 +49,7 @@ class SceneDesc:
     spring_vertices: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
     spring_rest: Optional[np.ndarray] = None
     spring_weight: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    spring_channel: Optional[np.ndarray] = None  # -1 plain, c >= 0 pneumatic (activation channel c)
     bend_offsets: np.ndarray = field(default_factory=lambda: np.zeros(1, np.int32))
     bend_vertices: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
     bend_weight: np.ndarray = field(default_factory=lambda: np.zeros(0))
@@ -69,6 +70,14 @@ class SceneDesc:
     checkpoint_every: int = 1
     underwater: bool = False
     drag_faces: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.int32))
+    # articulated skeleton ("Bones"): link 0 the root (joint type ALL)
+    link_parent: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    link_type: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    link_joint: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    link_axis: np.ndarray = field(default_factory=lambda: np.zeros((0, 3)))
+    link_offsets: np.ndarray = field(default_factory=lambda: np.zeros(1, np.int32))
+    link_vertices: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    link_channel: Optional[np.ndarray] = None
     name: str = "scene"
 
     @property
@@ -117,6 +126,7 @@ class SceneDesc:
         d.spring_vertices = P(self.spring_vertices, _i32, C.c_int32)
         d.spring_rest = P(self.spring_rest, _f64, C.c_double)
         d.spring_weight = P(self.spring_weight, _f64, C.c_double)
+        d.spring_channel = P(self.spring_channel, _i32, C.c_int32)
         d.n_bending = int(np.asarray(self.bend_weight).size)
         d.bend_offsets = P(self.bend_offsets, _i32, C.c_int32)
         d.bend_vertices = P(self.bend_vertices, _i32, C.c_int32)
@@ -143,6 +153,14 @@ class SceneDesc:
         d.underwater = int(bool(self.underwater))
         d.n_drag_faces = int(np.asarray(self.drag_faces).reshape(-1, 3).shape[0])
         d.drag_faces = P(self.drag_faces, _i32, C.c_int32)
+        d.n_links = int(np.asarray(self.link_parent).size)
+        d.link_parent = P(self.link_parent, _i32, C.c_int32)
+        d.link_type = P(self.link_type, _i32, C.c_int32)
+        d.link_joint = P(self.link_joint, _f64, C.c_double)
+        d.link_axis = P(self.link_axis, _f64, C.c_double)
+        d.link_offsets = P(self.link_offsets, _i32, C.c_int32)
+        d.link_vertices = P(self.link_vertices, _i32, C.c_int32)
+        d.link_channel = P(self.link_channel, _i32, C.c_int32)
         d.checkpoint_every = int(self.checkpoint_every)
         return d, keep
 
@@ -329,6 +347,72 @@ def muscle_beam(nx: int = 8, ny: int = 3, nz: int = 3, n_chains: int = 2, n_seg:
         muscle_tets=mt, muscle_fiber=mf, muscle_stiffness=mk, muscle_segment=ms, n_segments=len(segs),
         time_step=1.0 / 60.0, max_iterations=15, damping=0.9999, gravity=(0.0, -9.8, 0.0),
         precision=precision, name=f"muscle_beam_{nx}x{ny}x{nz}",
+    )
+
+
+def pneumatic_beam(nx: int = 8, ny: int = 3, nz: int = 3, stiffness: float = 1e5, muscle_segments: int = 2,
+                   precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Small beam driven by pneumatic springs (actuator type 3 of Dfobj.h:
+    "Volume Verts" polylines, one PneumaticConstraint per consecutive vertex
+    pair, weight = "Muscle Stiffness", each on its own activation channel),
+    plus one muscle chain so that muscle segments (channels 0..) and
+    pneumatic springs (the channels after them) share one activation row.
+    Left end pinned."""
+    edge = 0.05
+    x0, tets = cube_grid(nx, ny, nz, edge)
+    mass = lumped_masses(x0, tets, 1000.0 * nx * ny * nz * edge ** 3, True)
+    L = nx * edge
+    segs = [((L * s / muscle_segments, 0.5 * edge, 0.5 * edge), (L * (s + 1) / muscle_segments, 0.5 * edge, 0.5 * edge))
+            for s in range(muscle_segments)]
+    mt, mf, mk, ms = muscle_constraints(x0, tets, segs, 5e3) if muscle_segments else (
+        np.zeros((0, 4), np.int32), np.zeros((0, 3)), np.zeros(0), np.zeros(0, np.int32))
+    # polylines along x on the top face (two rows) and the bottom face (one row)
+    lines = []
+    for (yv, zv) in ((ny * edge, 0.0), (ny * edge, nz * edge), (0.0, nz * edge)):
+        on = np.nonzero(np.isclose(x0[:, 1], yv) & np.isclose(x0[:, 2], zv))[0]
+        lines.append(on[np.argsort(x0[on, 0])])
+    spv, spr, spc = [], [], []
+    ch = len(segs)
+    for line in lines:
+        for i0, i1 in zip(line[:-1], line[1:]):
+            spv.append((i0, i1)); spr.append(float(np.linalg.norm(x0[i0] - x0[i1]))); spc.append(ch)
+            ch += 1
+    pins = np.nonzero(np.isclose(x0[:, 0], 0.0))[0].astype(np.int32)
+    T = tets.shape[0]
+    return SceneDesc(
+        x0=x0, mass=mass, tets=tets, youngs=np.full(T, 5e4), poisson=np.full(T, 0.3),
+        attach_vertex=pins, attach_target=x0[pins], attach_stiffness=np.full(pins.size, 1e8),
+        muscle_tets=mt, muscle_fiber=mf, muscle_stiffness=mk, muscle_segment=ms, n_segments=ch,
+        spring_vertices=np.asarray(spv, np.int32), spring_rest=np.asarray(spr), spring_weight=np.full(len(spv), stiffness),
+        spring_channel=np.asarray(spc, np.int32),
+        time_step=1.0 / 60.0, max_iterations=15, damping=0.9999, gravity=(0.0, -9.8, 0.0),
+        precision=precision, name=f"pneumatic_beam_{nx}x{ny}x{nz}",
+    )
+
+
+def articulated_beam(nx: int = 8, ny: int = 2, nz: int = 2, gravity=(0.0, -9.8, 0.0), torques: bool = True,
+                     precision: int = DFEM_PREC_FP64) -> SceneDesc:
+    """Small beam with an articulated skeleton (Link tree of Dfobj.h "Bones"):
+    the root (joint type ALL) holds the left face, a ROTATIONAL link (axis z,
+    joint at the middle face's centre) the middle face, and a PRISMATIC link
+    (axis x, child of the rotational one) the right face; the two non-root
+    links' joint torques are activation channels 0 and 1."""
+    edge = 0.05
+    x0, tets = cube_grid(nx, ny, nz, edge)
+    mass = lumped_masses(x0, tets, 1000.0 * nx * ny * nz * edge ** 3, True)
+    L = nx * edge
+    faces = [np.nonzero(np.isclose(x0[:, 0], xv))[0].astype(np.int32) for xv in (0.0, edge * (nx // 2), L)]
+    joints = np.array([[0.0, 0.0, 0.0], [edge * (nx // 2), 0.5 * ny * edge, 0.5 * nz * edge], [L, 0.5 * ny * edge, 0.5 * nz * edge]])
+    T = tets.shape[0]
+    return SceneDesc(
+        x0=x0, mass=mass, tets=tets, youngs=np.full(T, 5e4), poisson=np.full(T, 0.3),
+        n_segments=2 if torques else 0,
+        link_parent=np.array([-1, 0, 1], np.int32), link_type=np.array([2, 1, 0], np.int32),
+        link_joint=joints, link_axis=np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 1.0], [1.0, 0.0, 0.0]]),
+        link_offsets=np.cumsum([0] + [f.size for f in faces]).astype(np.int32),
+        link_vertices=np.concatenate(faces), link_channel=np.array([-1, 0, 1], np.int32) if torques else None,
+        time_step=1.0 / 100.0, max_iterations=20, damping=0.9999, gravity=gravity,
+        precision=precision, name=f"articulated_beam_{nx}x{ny}x{nz}",
     )
 
 

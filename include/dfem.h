@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define DFEM_ABI_VERSION 4
+#define DFEM_ABI_VERSION 5
 
 enum dfem_status {
   DFEM_OK = 0,
@@ -40,7 +40,8 @@ enum dfem_status {
   DFEM_ERR_NONFINITE = 4,     /* NaN/Inf met in a step (status word set on GPU)  */
   DFEM_ERR_STATE = 5,         /* call out of order (e.g. backward before forward)*/
   DFEM_ERR_CAP = 6,           /* a bounded loop or wait hit its cap              */
-  DFEM_ERR_NOMEM = 7          /* allocation failed                               */
+  DFEM_ERR_NOMEM = 7,         /* allocation failed                               */
+  DFEM_ERR_UNSUPPORTED = 8    /* feature combination the engine does not serve   */
 };
 
 enum dfem_mem { DFEM_MEM_HOST = 0, DFEM_MEM_DEVICE = 1 };
@@ -84,13 +85,19 @@ typedef struct dfem_scene_desc {
   const double *muscle_fiber;     /* 3*n_muscle unit fibre directions                */
   const double *muscle_stiffness; /* n_muscle: muscle stiffness x distance weight    */
   const int32_t *muscle_segment;  /* n_muscle segment ids in [0, n_segments)         */
-  int32_t n_segments;
+  int32_t n_segments;             /* activation channels: muscle segments and the
+                                     channels of pneumatic springs (spring_channel) */
 
   /* cloth strain springs (SpringConstraint) */
   int32_t n_springs;
   const int32_t *spring_vertices; /* 2*n_springs                                     */
   const double *spring_rest;      /* n_springs rest lengths (NULL = from x0)         */
   const double *spring_weight;    /* n_springs weights w (J and L use sqrt(w))       */
+  const int32_t *spring_channel;  /* n_springs activation channels, or NULL: -1 = plain
+                                     spring; c in [0, n_segments) = pneumatic spring
+                                     (PneumaticConstraint, sim/fem/Constraint/
+                                     pneumaticEasy.h:133-147) whose projection uses
+                                     rest * activation[c] as its length             */
 
   /* cloth bending stencils (BendingConstraint): centre vertex then 1-ring in order */
   int32_t n_bending;
@@ -132,7 +139,31 @@ typedef struct dfem_scene_desc {
   int32_t underwater;             /* "Is underwater"                                 */
   int32_t n_drag_faces;
   const int32_t *drag_faces;      /* 3 per face, global vertex ids, outward winding  */
+
+  /* articulated skeleton ("Bones", read by Dfobj.h:254-288 into Link objects,
+   * sim/constants.h:28-247, registered by World::AddBody, World.h:499-545):
+   * link 0 is the one root (DFEM_JOINT_ALL: 6 dofs, a linearised rotation w
+   * and a translation l); every other link has a parent of lower index and
+   * one dof (DFEM_JOINT_ROTATIONAL: an angle about its axis;
+   * DFEM_JOINT_PRISMATIC: a distance along it).  The vertices of a link move
+   * rigidly with it; the other vertices are solved with the links through
+   * the Schur complement of World::ComputeSolution (World.h:1600-1670).
+   * Single FP64 scenes without contact; no adjoint (dfem_step_backward
+   * returns DFEM_ERR_UNSUPPORTED). */
+  int32_t n_links;
+  const int32_t *link_parent;     /* parent link, -1 for link 0                       */
+  const int32_t *link_type;       /* enum dfem_joint                                  */
+  const double *link_joint;       /* 3 per link: "Joint Pos"                          */
+  const double *link_axis;        /* 3 per link: unit "Joint Axis" (root: unused)    */
+  const int32_t *link_offsets;    /* n_links+1 offsets into link_vertices             */
+  const int32_t *link_vertices;   /* the links' vertices (each in at most one link)   */
+  const int32_t *link_channel;    /* n_links activation channels of the joint torques
+                                     (World::mJointTorque, World.h:1638-1640) of the
+                                     non-root links, -1 = none (NULL = none)       */
 } dfem_scene_desc;
+
+/* Joint types of the skeleton links (Link::JointType). */
+enum dfem_joint { DFEM_JOINT_PRISMATIC = 0, DFEM_JOINT_ROTATIONAL = 1, DFEM_JOINT_ALL = 2 };
 
 typedef struct dfem_scene dfem_scene;  /* opaque */
 
@@ -180,6 +211,16 @@ int dfem_set_materials(dfem_scene *scene, const double *youngs, const double *po
 /* Muscle activation per segment for the next forward call(s).  Replaces
  * MuscleSegment::SetActivationLevel (sim/MuscleSegment.h:72-78). */
 int dfem_set_activations(dfem_scene *scene, const double *activations, int mem);
+
+/* Skeleton joint state (World::mJointQ / mJointQd as Link::WriteT lays them
+ * out, sim/constants.h:206-221): the root's T (R row-major, 9 values; d, 3)
+ * then the magnitude of every other link; jqd holds the previous step's
+ * values (prevTr, prevmag).  12 + n_links - 1 doubles each (host memory).
+ * dfem_step_forward starts from this state and leaves its end state here
+ * (Link::ReadT / WriteT around every step, World.h:681-682,712-713).  A new
+ * scene starts from the identity and zero magnitudes. */
+int dfem_set_joint_state(dfem_scene *scene, const double *jq, const double *jqd);
+int dfem_get_joint_state(const dfem_scene *scene, double *jq, double *jqd);
 
 /* Run n_steps time steps from (x, v); writes the final state, and optionally
  * every step's positions to traj_x ((n_steps) * 3N, may be NULL).

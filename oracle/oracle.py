@@ -54,6 +54,9 @@ def lib() -> C.CDLL:
         L.orc_hs_coo.argtypes = [vp, pi, pi, pd, C.c_int64]
         L.orc_full_L_triplets.restype = C.c_int64
         L.orc_full_L_triplets.argtypes = [vp, pi, pi, pd, C.c_int64]
+        L.orc_joint_state_size.argtypes = [vp]
+        L.orc_set_joint_state.argtypes = [vp, pd, pd]
+        L.orc_get_joint_state.argtypes = [vp, pd, pd]
         _lib = L
     return _lib
 
@@ -125,6 +128,23 @@ class OracleScene:
             raise RuntimeError(f"oracle: backward failed ({rc})")
         return {"x": ox, "v": ov, "E": gE[: self.T], "nu": gnu[: self.T],
                 "act": ga[: self._steps * self.nseg].reshape(self._steps, self.nseg)}
+
+    def joint_state(self):
+        """(jq, jqd): World::mJointQ / mJointQd of the skeleton (empty without links)."""
+        n = lib().orc_joint_state_size(self.h)
+        jq, jqd = np.zeros(max(1, n)), np.zeros(max(1, n))
+        if n:
+            lib().orc_get_joint_state(self.h, _pd(jq), _pd(jqd))
+        return jq[:n], jqd[:n]
+
+    def set_joint_state(self, jq, jqd):
+        n = lib().orc_joint_state_size(self.h)
+        jq = np.ascontiguousarray(jq, np.float64).reshape(-1)
+        jqd = np.ascontiguousarray(jqd, np.float64).reshape(-1)
+        if jq.size != n or jqd.size != n:
+            raise ValueError(f"joint state needs {n} values each")
+        if n:
+            lib().orc_set_joint_state(self.h, _pd(jq), _pd(jqd))
 
     def eval_local(self, x, act=None):
         """J d(x) of all constraints (3N)."""

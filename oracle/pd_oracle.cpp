@@ -17,7 +17,9 @@
  * What it restates (paths relative to the diff_fem repository):
  *   - World::TimeStepping / UpdatePositionsAndVelocities   sim/fem/World.h:673-720,757-766
  *   - World::ProjectiveDynamicsMethod main loop           sim/fem/World.h:835-917
- *   - World::ComputeSolution (no-bones branch)            sim/fem/World.h:1601-1670
+ *   - World::ComputeSolution (both branches)              sim/fem/World.h:1601-1670
+ *   - Link: kinematics, tildaV, UpdateT, guessNext        sim/constants.h:28-247
+ *   - Schur complement of the free vertices (bones)       sim/fem/World.h:1100-1135
  *   - World::PreComputation / FactorizeLDLT (retry)       sim/fem/World.h:1089-1139,1212-1232
  *   - CorotateFEMConstraint (F, SVD, reflection, volume)   sim/fem/Constraint/CorotateFEMConstraint.h:64-392
  *   - LinearMuscleConstraint                              sim/fem/Constraint/LinearMuscleConstraint.h:91-270
@@ -267,6 +269,42 @@ static double mean_value(V3 a, V3 b, V3 c) {
  * the contact vertices whose closest impact is on it, ascending. */
 struct SelfGroup { int f; V3 n; std::vector<int> verts; };
 
+/* ---- articulated skeleton: Link (sim/constants.h:28-247) ------------------ */
+struct Xf { M3 R; V3 d; };  /* Transformation: x -> R x + d */
+static Xf xf_identity() {
+  Xf t{};
+  at(t.R, 0, 0) = at(t.R, 1, 1) = at(t.R, 2, 2) = 1.0;
+  t.d = V3{0, 0, 0};
+  return t;
+}
+static inline V3 mv(const M3& a, V3 v) {
+  return V3{at(a, 0, 0) * v.x + at(a, 0, 1) * v.y + at(a, 0, 2) * v.z,
+            at(a, 1, 0) * v.x + at(a, 1, 1) * v.y + at(a, 1, 2) * v.z,
+            at(a, 2, 0) * v.x + at(a, 2, 1) * v.y + at(a, 2, 2) * v.z};
+}
+static inline Xf xf_mul(const Xf& a, const Xf& b) { return Xf{mul(a.R, b.R), mv(a.R, b.d) + a.d}; }
+static inline V3 xf_apply(const Xf& a, V3 v) { return mv(a.R, v) + a.d; }
+
+struct LinkO {
+  int parent = -1, type = DFEM_JOINT_ALL, dof = 0, sdof = 0, chan = -1;
+  V3 joint{0, 0, 0}, axis{0, 0, 0}, d0{0, 0, 0};
+  M3 nx{}, nnt{};                 /* cross-product matrix of the axis, axis axis^T */
+  int r0 = 0, r1 = 0;             /* its rigid vertices [r0, r1) */
+  double mag = 0, prevmag = 0;
+  Xf T = xf_identity(), Tr = xf_identity(), prevTr = xf_identity(), prefix = xf_identity(),
+     dT = xf_identity(), suffix = xf_identity();
+};
+
+struct Skel {
+  int L = 0, ndof = 0, nq = 0;    /* links, dofs (6 + L - 1), joint-state length (12 + L - 1) */
+  std::vector<LinkO> links;
+  std::vector<int> rv;            /* rigid vertex j -> vertex id, in link order */
+  std::vector<V3> rest;           /* Link::restpos */
+  std::vector<int> ridx;          /* vertex -> rigid index or -1 */
+  std::vector<double> jq, jqd;    /* World::mJointQ / mJointQd */
+  std::vector<double> Srr;        /* nr x nr: Hs_RR - Hs_RF Hs_FF^-1 Hs_FR (scalar) */
+};
+
 struct Scene {
   int N = 0;
   std::vector<double> x0, mass, gmask;
@@ -274,7 +312,7 @@ struct Scene {
   std::vector<int> att_v; std::vector<V3> att_p; std::vector<double> att_k;
   std::vector<Tet> mtets; std::vector<V3> mfib; std::vector<double> mk; std::vector<int> mseg; int nseg = 0;
   std::vector<double> seg_act;
-  std::vector<int> sp_v; std::vector<double> sp_rest, sp_w;
+  std::vector<int> sp_v, sp_ch; std::vector<double> sp_rest, sp_w;  /* sp_ch: -1 or a pneumatic spring's channel */
   std::vector<Bend> bends;
   double h = 0.01, damping = 1.0; int K = 10; V3 g{0, 0, 0};
   /* contact: World::ProjectiveDynamicsMethod contact phase (World.h:925-1023),
@@ -311,6 +349,11 @@ struct Scene {
   std::vector<double> env;
   std::vector<std::vector<std::pair<int, double>>> Hrows; /* Hs rows (old numbering) */
   double reg = 0.0;
+  /* skeleton: the links and a second envelope factor of Hs with the rigid
+     vertices' rows and columns replaced by the identity, i.e. of Qf (World.h:1100-1128) */
+  Skel skel;
+  Scene* qf = nullptr;
+  ~Scene() { delete qf; }
   std::string err;
   /* recorded forward trajectory for the adjoint */
   int rec_steps = 0;
@@ -574,7 +617,10 @@ static void local_Jd(const Scene& S, const double* x, const double* act, double*
   for (size_t s = 0; s < S.sp_w.size(); ++s) {
     int i0 = S.sp_v[2 * s], i1 = S.sp_v[2 * s + 1];
     V3 e = getx(x, i0) - getx(x, i1);
-    V3 d = (S.sp_rest[s] / norm(e)) * e;  /* SpringConstraint.h:135-144 */
+    /* SpringConstraint.h:135-144; a pneumatic spring projects to rest * activation
+       (PneumaticConstraint::EvaluateDVector, pneumaticEasy.h:133-147) */
+    double len = S.sp_ch[s] >= 0 ? S.sp_rest[s] * act[S.sp_ch[s]] : S.sp_rest[s];
+    V3 d = (len / norm(e)) * e;
     double w = std::sqrt(S.sp_w[s]);
     addx(f, i0, w * d);
     addx(f, i1, -w * d);
@@ -587,6 +633,360 @@ static void local_Jd(const Scene& S, const double* x, const double* act, double*
     if (ln > 1e-25) d = (B.w * B.rest_norm / ln) * lap;  /* BendingConstraint.h:164-187 */
     for (size_t a = 0; a < B.v.size(); ++a) addx(f, B.v[a], (B.w * B.beta[a]) * d);
   }
+}
+
+/* ---- articulated skeleton: kinematics and the rigid branch ----------------
+ * Link::ComputeV0NTr, ComputeTildaV, UpdateT, guessNext, ReadT/WriteT
+ * (sim/constants.h:83-228) and World::ComputeSolution's rigid branch
+ * (World.h:1600-1670).  Links are visited in index order (parents first), which
+ * gives the same values as the reference's depth-first recursion: a link reads
+ * only its parent's prefix and Tr. */
+
+/* Dense solve A X = B (n x n, k right-hand sides, row-major) by LU with full
+ * pivoting (the largest |a| of the remaining block is the pivot), like
+ * Eigen::FullPivLU::solve for an invertible A. */
+static void fullpiv_solve(int n, int k, std::vector<double> A, const double* B, double* X) {
+  std::vector<int> rp(n), cp(n);
+  std::iota(rp.begin(), rp.end(), 0);
+  std::iota(cp.begin(), cp.end(), 0);
+  std::vector<double> Bw(B, B + (size_t)n * k);
+  for (int p = 0; p < n; ++p) {
+    int pr = p, pc = p;
+    double best = -1.0;
+    for (int r = p; r < n; ++r)
+      for (int c = p; c < n; ++c)
+        if (std::fabs(A[(size_t)r * n + c]) > best) { best = std::fabs(A[(size_t)r * n + c]); pr = r; pc = c; }
+    if (pr != p) {
+      for (int c = 0; c < n; ++c) std::swap(A[(size_t)p * n + c], A[(size_t)pr * n + c]);
+      for (int c = 0; c < k; ++c) std::swap(Bw[(size_t)p * k + c], Bw[(size_t)pr * k + c]);
+    }
+    if (pc != p) {
+      for (int r = 0; r < n; ++r) std::swap(A[(size_t)r * n + p], A[(size_t)r * n + pc]);
+      std::swap(cp[p], cp[pc]);
+    }
+    const double piv = A[(size_t)p * n + p];
+    for (int r = p + 1; r < n; ++r) {
+      const double f = A[(size_t)r * n + p] / piv;
+      A[(size_t)r * n + p] = f;
+      for (int c = p + 1; c < n; ++c) A[(size_t)r * n + c] -= f * A[(size_t)p * n + c];
+      for (int c = 0; c < k; ++c) Bw[(size_t)r * k + c] -= f * Bw[(size_t)p * k + c];
+    }
+  }
+  std::vector<double> Y((size_t)n * k);
+  for (int r = n - 1; r >= 0; --r)
+    for (int c = 0; c < k; ++c) {
+      double v = Bw[(size_t)r * k + c];
+      for (int q = r + 1; q < n; ++q) v -= A[(size_t)r * n + q] * Y[(size_t)q * k + c];
+      Y[(size_t)r * k + c] = v / A[(size_t)r * n + r];
+    }
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < k; ++c) X[(size_t)cp[r] * k + c] = Y[(size_t)r * k + c];
+}
+
+/* Transformation::linearize: the rotation U V^T of the SVD of R */
+static Xf xf_linearize(const Xf& t) {
+  SVD3 sv = svd3(t.R);
+  return Xf{mulT(sv.U, sv.V), t.d};
+}
+
+static M3 m3_from_rows(const double* r) {
+  M3 a{};
+  for (int i = 0; i < 9; ++i) at(a, i / 3, i % 3) = r[i];
+  return a;
+}
+
+/* Link::ReadT for every link; the root's Tr (not part of the joint state) is
+ * linearize(T), its value after the previous step's last ComputeV0NTr. */
+static void skel_read(Skel& K) {
+  for (LinkO& k : K.links) {
+    if (k.type == DFEM_JOINT_ALL) {
+      k.T = Xf{m3_from_rows(&K.jq[k.sdof]), V3{K.jq[k.sdof + 9], K.jq[k.sdof + 10], K.jq[k.sdof + 11]}};
+      k.prevTr = Xf{m3_from_rows(&K.jqd[k.sdof]), V3{K.jqd[k.sdof + 9], K.jqd[k.sdof + 10], K.jqd[k.sdof + 11]}};
+      k.Tr = xf_linearize(k.T);
+    } else {
+      k.mag = K.jq[k.sdof];
+      k.prevmag = K.jqd[k.sdof];
+    }
+  }
+}
+
+static void skel_write(Skel& K) {
+  for (const LinkO& k : K.links) {
+    if (k.type == DFEM_JOINT_ALL) {
+      for (int i = 0; i < 9; ++i) { K.jq[k.sdof + i] = at(k.T.R, i / 3, i % 3); K.jqd[k.sdof + i] = at(k.prevTr.R, i / 3, i % 3); }
+      const double td[3] = {k.T.d.x, k.T.d.y, k.T.d.z}, pd[3] = {k.prevTr.d.x, k.prevTr.d.y, k.prevTr.d.z};
+      for (int i = 0; i < 3; ++i) { K.jq[k.sdof + 9 + i] = td[i]; K.jqd[k.sdof + 9 + i] = pd[i]; }
+    } else {
+      K.jq[k.sdof] = k.mag;
+      K.jqd[k.sdof] = k.prevmag;
+    }
+  }
+}
+
+/* Link::guessNext */
+static void skel_guess(Skel& K) {
+  for (LinkO& k : K.links) {
+    if (k.type == DFEM_JOINT_ALL) {
+      k.T.d = 2.0 * k.Tr.d - k.prevTr.d;
+      double B[9], X[9];
+      std::vector<double> A(9);
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) { A[3 * r + c] = at(k.prevTr.R, r, c); B[3 * r + c] = at(k.Tr.R, r, c); }
+      fullpiv_solve(3, 3, A, B, X);  /* prevTr.R^-1 Tr.R */
+      k.T.R = mul(k.Tr.R, m3_from_rows(X));
+      k.prevTr = k.Tr;
+    } else {
+      const double t = k.mag;
+      k.mag = 2.0 * k.mag - k.prevmag;
+      k.prevmag = t;
+    }
+  }
+}
+
+/* Link::ComputeV0NTr: every link's Tr and prefix, and V0 (3 per rigid vertex) */
+static void skel_v0(Skel& K, std::vector<double>& V0) {
+  V0.assign(3 * K.rv.size(), 0.0);
+  for (LinkO& k : K.links) {
+    if (k.type == DFEM_JOINT_ALL) {
+      k.Tr = xf_linearize(k.T);
+    } else if (k.type == DFEM_JOINT_ROTATIONAL) {
+      const double C = std::cos(k.mag), S = std::sin(k.mag);
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) at(k.Tr.R, r, c) = (C * (r == c ? 1.0 : 0.0) + S * at(k.nx, r, c)) + (1.0 - C) * at(k.nnt, r, c);
+      k.Tr.d = k.d0;
+    } else {
+      k.Tr.d = k.mag * k.axis + k.d0;
+    }
+    if (k.parent >= 0) k.prefix = xf_mul(K.links[k.parent].prefix, K.links[k.parent].Tr);
+    const Xf M = xf_mul(k.prefix, k.Tr);
+    for (int j = k.r0; j < k.r1; ++j) {
+      const V3 p = xf_apply(M, K.rest[j] - k.joint);
+      V0[3 * j] = p.x; V0[3 * j + 1] = p.y; V0[3 * j + 2] = p.z;
+    }
+  }
+}
+
+/* Link::ComputeTildaV: dV0/ds (3 nr x ndof, row-major) at the state of the
+ * last skel_v0 */
+static void skel_tildav(Skel& K, const std::vector<double>& V0, std::vector<double>& TV) {
+  const int nd = K.ndof;
+  TV.assign(3 * K.rv.size() * (size_t)nd, 0.0);
+  for (LinkO& k : K.links) {
+    if (k.type == DFEM_JOINT_ROTATIONAL) {
+      const double C = std::cos(k.mag), S = std::sin(k.mag);
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) at(k.dT.R, r, c) = (-S * (r == c ? 1.0 : 0.0) + C * at(k.nx, r, c)) + S * at(k.nnt, r, c);
+    } else if (k.type == DFEM_JOINT_PRISMATIC) {
+      k.dT.R = M3{};
+      k.dT.d = k.axis;
+    }
+  }
+  for (int l = 0; l < K.L; ++l) {
+    LinkO& me = K.links[l];
+    me.suffix = xf_identity();
+    for (int cur = l; K.links[cur].parent >= 0; cur = K.links[cur].parent)
+      K.links[K.links[cur].parent].suffix = xf_mul(K.links[cur].Tr, K.links[cur].suffix);
+    for (int j = me.r0; j < me.r1; ++j) {
+      const V3 vinit = K.rest[j] - me.joint;
+      double* row[3] = {&TV[(3 * (size_t)j) * nd], &TV[(3 * (size_t)j + 1) * nd], &TV[(3 * (size_t)j + 2) * nd]};
+      int cur = l;
+      for (; K.links[cur].parent >= 0; cur = K.links[cur].parent) {
+        const LinkO& c = K.links[cur];
+        V3 t = (c.type == DFEM_JOINT_ROTATIONAL) ? mv(c.prefix.R, mv(c.dT.R, xf_apply(c.suffix, vinit)))
+                                                 : mv(c.prefix.R, c.dT.d);
+        row[0][c.dof] = t.x; row[1][c.dof] = t.y; row[2][c.dof] = t.z;
+      }
+      const int c0 = K.links[cur].dof;
+      const double vx = V0[3 * j], vy = V0[3 * j + 1], vz = V0[3 * j + 2];
+      row[0][c0 + 1] = vz;  row[0][c0 + 2] = -vy;
+      row[1][c0 + 0] = -vz; row[1][c0 + 2] = vx;
+      row[2][c0 + 0] = vy;  row[2][c0 + 1] = -vx;
+      row[0][c0 + 3] = 1.0; row[1][c0 + 4] = 1.0; row[2][c0 + 5] = 1.0;
+    }
+  }
+}
+
+/* Link::UpdateT */
+static void skel_update(Skel& K, const std::vector<double>& s) {
+  for (LinkO& k : K.links) {
+    if (k.type == DFEM_JOINT_PRISMATIC) {
+      k.mag += s[k.dof];
+    } else if (k.type == DFEM_JOINT_ROTATIONAL) {
+      const double C = std::cos(k.mag), S = std::sin(k.mag);
+      k.mag = std::atan2(S + C * s[k.dof], C - S * s[k.dof]);
+    } else {
+      const V3 w{s[k.dof], s[k.dof + 1], s[k.dof + 2]}, l{s[k.dof + 3], s[k.dof + 4], s[k.dof + 5]};
+      M3 t{};
+      at(t, 0, 0) = 1; at(t, 0, 1) = -w.z; at(t, 0, 2) = w.y;
+      at(t, 1, 0) = w.z; at(t, 1, 1) = 1; at(t, 1, 2) = -w.x;
+      at(t, 2, 0) = -w.y; at(t, 2, 1) = w.x; at(t, 2, 2) = 1;
+      k.T.R = mul(t, k.Tr.R);
+      k.T.d = mv(t, k.Tr.d) + l;
+    }
+  }
+}
+
+/* Qf^-1 b on the free vertices (b's rigid entries are ignored) */
+static void qf_solve(const Scene& S, const double* b, double* x) {
+  std::vector<double> bb(b, b + 3 * (size_t)S.N);
+  for (int v : S.skel.rv)
+    for (int c = 0; c < 3; ++c) bb[3 * (size_t)v + c] = 0.0;
+  solve(*S.qf, bb.data(), x);
+}
+
+/* y = H_{rows, cols} x restricted: rows/cols each "free" (-1) or "rigid" (1),
+ * x and y full 3N vectors (entries outside `cols` / `rows` ignored / zero) */
+static void H_block_mul(const Scene& S, int rows, int cols, const double* x, double* y) {
+  const std::vector<int>& ri = S.skel.ridx;
+  for (int i = 0; i < S.N; ++i) {
+    double a = 0, b = 0, c = 0;
+    if ((ri[i] >= 0 ? 1 : -1) == rows)
+      for (auto& e : S.Hrows[i]) {
+        if ((ri[e.first] >= 0 ? 1 : -1) != cols) continue;
+        a += e.second * x[3 * e.first]; b += e.second * x[3 * e.first + 1]; c += e.second * x[3 * e.first + 2];
+      }
+    y[3 * i] = a; y[3 * i + 1] = b; y[3 * i + 2] = c;
+  }
+}
+
+/* QbMmQcLQfm1QcLT = Qb_M - Qc_L Qf^-1 Qc_L^T (World.h:1134-1135), scalar
+ * (kron(., I3) in the reference), one Qf solve per three rigid vertices */
+static bool skel_precompute(Scene& S) {
+  Skel& K = S.skel;
+  const int N = S.N, nr = (int)K.rv.size();
+  std::vector<std::vector<std::pair<int, double>>> rows(N);
+  for (int i = 0; i < N; ++i) {
+    if (K.ridx[i] >= 0) { rows[i].push_back({i, 1.0}); continue; }
+    for (auto& e : S.Hrows[i])
+      if (K.ridx[e.first] < 0) rows[i].push_back(e);
+  }
+  delete S.qf;
+  S.qf = new Scene();
+  S.qf->N = N;
+  S.qf->Hrows.swap(rows);
+  rcm_order(*S.qf);
+  if (!factor(*S.qf)) { S.err = "Qf factorisation failed"; return false; }
+  K.Srr.assign((size_t)nr * nr, 0.0);
+  std::vector<double> b(3 * (size_t)N), w(3 * (size_t)N);
+  for (int j0 = 0; j0 < nr; j0 += 3) {
+    std::fill(b.begin(), b.end(), 0.0);
+    for (int c = 0; c < 3 && j0 + c < nr; ++c)
+      for (auto& e : S.Hrows[K.rv[j0 + c]])  /* column r_j of Hs (symmetric) on the free rows */
+        if (K.ridx[e.first] < 0) b[3 * (size_t)e.first + c] = e.second;
+    solve(*S.qf, b.data(), w.data());
+    for (int c = 0; c < 3 && j0 + c < nr; ++c)
+      for (int i = 0; i < nr; ++i) {
+        double v = 0, acc = 0;
+        for (auto& e : S.Hrows[K.rv[i]]) {
+          if (e.first == K.rv[j0 + c]) v = e.second;
+          if (K.ridx[e.first] < 0) acc += e.second * w[3 * (size_t)e.first + c];
+        }
+        K.Srr[(size_t)i * nr + j0 + c] = v - acc;
+      }
+  }
+  return true;
+}
+
+/* ProjectiveDynamicsMethod with bones: the rigid vertices follow the links,
+ * the free ones are solved through the Schur complement (ComputeSolution's
+ * rigid branch, World.h:1611-1669) */
+static int pd_solve_skel(Scene& S, const double* x, const double* qn, const double* act, double* out, int nthreads) {
+  Skel& K = S.skel;
+  const int N = S.N, n3 = 3 * N, nr = (int)K.rv.size(), nd = K.ndof;
+  std::vector<double> b(n3), xk(qn, qn + n3), xold(n3, 0.0), c(n3), t1(n3), t2(n3), V0, TV;
+  const double ih2 = 1.0 / (S.h * S.h);
+  for (int i = 0; i < N; ++i)
+    for (int q = 0; q < 3; ++q) b[3 * i + q] = S.mass[i] * ih2 * qn[3 * i + q];
+  std::vector<double> Xfree(x, x + n3);           /* mNonrigidX */
+  for (int v : K.rv) for (int q = 0; q < 3; ++q) Xfree[3 * (size_t)v + q] = 0.0;
+  std::vector<double> HffX(n3), HrfX(n3);
+  H_block_mul(S, -1, -1, Xfree.data(), HffX.data());   /* Qf mNonrigidX */
+  H_block_mul(S, 1, -1, Xfree.data(), HrfX.data());    /* Qc_L mNonrigidX */
+  /* S = tildaV^T kron(Srr, I3) tildaV, assembled per iteration */
+  auto rigid_full = [&](const std::vector<double>& vr, std::vector<double>& full) {
+    std::fill(full.begin(), full.end(), 0.0);
+    for (int j = 0; j < nr; ++j)
+      for (int q = 0; q < 3; ++q) full[3 * (size_t)K.rv[j] + q] = vr[3 * j + q];
+  };
+  skel_read(K);
+  skel_guess(K);
+  int it = 0;
+  std::vector<double> full(n3), HfrV(n3), HrrV(n3), mcf(n3), sr(n3), Hrsr(n3), hvf(n3), vs(3 * (size_t)nr);
+  for (int i = 0; i < S.K; ++i) {
+    skel_v0(K, V0);
+    for (int j = 0; j < nr; ++j)
+      for (int q = 0; q < 3; ++q) xk[3 * (size_t)K.rv[j] + q] = V0[3 * j + q];
+    double e2 = 0;
+    for (int k = 0; k < n3; ++k) { double d = xk[k] - xold[k]; e2 += d * d; }
+    if (std::sqrt(e2) / n3 < 5e-7) break;  /* EPS, World.h:891-895 */
+    xold = xk;
+    std::copy(b.begin(), b.end(), c.begin());
+    local_Jd(S, xk.data(), act, c.data(), nthreads);       /* ori_c = b + J d */
+    skel_tildav(K, V0, TV);
+    rigid_full(V0, full);
+    H_block_mul(S, -1, 1, full.data(), HfrV.data());        /* Qc_L^T V0 */
+    H_block_mul(S, 1, 1, full.data(), HrrV.data());         /* Qb_M V0 */
+    for (int k = 0; k < n3; ++k) mcf[k] = c[k] - HfrV[k] - HffX[k];
+    std::vector<double> mcs(nd, 0.0), rr(3 * (size_t)nr);
+    for (int j = 0; j < nr; ++j)
+      for (int q = 0; q < 3; ++q) {
+        const size_t g = 3 * (size_t)K.rv[j] + q;
+        rr[3 * j + q] = c[g] - HrrV[g] - HrfX[g];
+      }
+    for (int a = 0; a < nd; ++a) {
+      double v = 0;
+      for (int r = 0; r < 3 * nr; ++r) v += TV[(size_t)r * nd + a] * rr[r];
+      mcs[a] = v;
+    }
+    for (int l = 1; l < K.L; ++l)                          /* mcs[6+i] += mJointTorque[i] */
+      if (K.links[l].chan >= 0) mcs[K.links[l].dof] += act[K.links[l].chan];
+    std::vector<double> Sm((size_t)nd * nd, 0.0), KT(3 * (size_t)nr * nd);
+    for (int i2 = 0; i2 < nr; ++i2)                         /* kron(Srr, I3) tildaV */
+      for (int q = 0; q < 3; ++q)
+        for (int a = 0; a < nd; ++a) {
+          double v = 0;
+          for (int j = 0; j < nr; ++j) v += K.Srr[(size_t)i2 * nr + j] * TV[(3 * (size_t)j + q) * nd + a];
+          KT[(3 * (size_t)i2 + q) * nd + a] = v;
+        }
+    for (int a = 0; a < nd; ++a)
+      for (int bq = 0; bq < nd; ++bq) {
+        double v = 0;
+        for (int r = 0; r < 3 * nr; ++r) v += TV[(size_t)r * nd + a] * KT[(size_t)r * nd + bq];
+        Sm[(size_t)a * nd + bq] = v;
+      }
+    for (int k = 0; k < n3; ++k) t1[k] = -mcf[k];
+    qf_solve(S, t1.data(), sr.data());                      /* solve_result = Qf^-1 (-mcf) */
+    H_block_mul(S, 1, -1, sr.data(), Hrsr.data());          /* Qc_L solve_result */
+    std::vector<double> tmp(nd), sv(nd);
+    for (int a = 0; a < nd; ++a) {
+      double v = 0;
+      for (int j = 0; j < nr; ++j)
+        for (int q = 0; q < 3; ++q) v += TV[(3 * (size_t)j + q) * nd + a] * Hrsr[3 * (size_t)K.rv[j] + q];
+      tmp[a] = mcs[a] + v;
+    }
+    fullpiv_solve(nd, 1, Sm, tmp.data(), sv.data());        /* S.fullPivLu().solve(tmp) */
+    for (int j = 0; j < nr; ++j)                            /* tildaV s */
+      for (int q = 0; q < 3; ++q) {
+        double v = 0;
+        for (int a = 0; a < nd; ++a) v += TV[(3 * (size_t)j + q) * nd + a] * sv[a];
+        vs[3 * j + q] = v;
+      }
+    rigid_full(vs, full);
+    H_block_mul(S, -1, 1, full.data(), t2.data());          /* Qc^T s = Qc_L^T tildaV s */
+    for (int k = 0; k < n3; ++k) t1[k] = mcf[k] - t2[k];
+    qf_solve(S, t1.data(), hvf.data());
+    skel_update(K, sv);
+    for (int v = 0; v < N; ++v)
+      if (K.ridx[v] < 0)
+        for (int q = 0; q < 3; ++q) xk[3 * (size_t)v + q] = x[3 * (size_t)v + q] + hvf[3 * (size_t)v + q];
+    ++it;
+  }
+  skel_v0(K, V0);
+  for (int j = 0; j < nr; ++j)
+    for (int q = 0; q < 3; ++q) xk[3 * (size_t)K.rv[j] + q] = V0[3 * j + q];
+  skel_write(K);
+  std::copy(xk.begin(), xk.end(), out);
+  return it;
 }
 
 /* ProjectiveDynamicsMethod (World.h:835-917) with the iterate history */
@@ -1425,7 +1825,12 @@ static void local_Jd_vjp(const Scene& S, const double* x, const double* act, con
     V3 e = getx(x, i0) - getx(x, i1);
     double n = norm(e);
     V3 eh = (1.0 / n) * e;
-    V3 ge = (S.sp_rest[s] / n) * (db - dot(eh, db) * eh);
+    double len = S.sp_rest[s];
+    if (S.sp_ch[s] >= 0) {
+      len *= act[S.sp_ch[s]];
+      if (gact) gact[S.sp_ch[s]] += S.sp_rest[s] * dot(db, eh);
+    }
+    V3 ge = (len / n) * (db - dot(eh, db) * eh);
     addx(xb, i0, ge);
     addx(xb, i1, -1.0 * ge);
   }
@@ -1723,6 +2128,7 @@ void* orc_create(const dfem_scene_desc* d) {
     double rest = d->spring_rest ? d->spring_rest[s] : norm(getx(d->x0, i0) - getx(d->x0, i1));
     S->sp_rest.push_back(rest);
     S->sp_w.push_back(d->spring_weight[s]);
+    S->sp_ch.push_back(d->spring_channel ? d->spring_channel[s] : -1);
   }
   for (int b = 0; b < d->n_bending; ++b) {
     Bend B;
@@ -1783,10 +2189,72 @@ void* orc_create(const dfem_scene_desc* d) {
   S->K = d->max_iterations;
   S->damping = d->damping;
   S->g = V3{d->gravity[0], d->gravity[1], d->gravity[2]};
+  if (d->n_links > 0) {  /* Dfobj.h:254-288, World::AddBody (World.h:499-545) */
+    Skel& K = S->skel;
+    K.L = d->n_links;
+    K.ridx.assign(N, -1);
+    int dof = 0, sdof = 0;
+    for (int l = 0; l < K.L; ++l) {
+      LinkO k;
+      k.parent = d->link_parent[l];
+      k.type = d->link_type[l];
+      k.chan = d->link_channel ? d->link_channel[l] : -1;
+      k.joint = V3{d->link_joint[3 * l], d->link_joint[3 * l + 1], d->link_joint[3 * l + 2]};
+      k.dof = dof; k.sdof = sdof;
+      dof += (k.parent < 0) ? 6 : 1;
+      sdof += (k.parent < 0) ? 12 : 1;
+      if (k.parent >= 0) {
+        V3 a{d->link_axis[3 * l], d->link_axis[3 * l + 1], d->link_axis[3 * l + 2]};
+        k.axis = (1.0 / norm(a)) * a;
+        k.d0 = k.joint - K.links[k.parent].joint;
+        if (k.type == DFEM_JOINT_ROTATIONAL) {
+          at(k.nx, 0, 1) = -k.axis.z; at(k.nx, 0, 2) = k.axis.y;
+          at(k.nx, 1, 0) = k.axis.z;  at(k.nx, 1, 2) = -k.axis.x;
+          at(k.nx, 2, 0) = -k.axis.y; at(k.nx, 2, 1) = k.axis.x;
+          const double ax[3] = {k.axis.x, k.axis.y, k.axis.z};
+          for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c) at(k.nnt, r, c) = ax[r] * ax[c];
+        }
+      } else {
+        k.d0 = k.joint;
+      }
+      k.r0 = (int)K.rv.size();
+      for (int q = d->link_offsets[l]; q < d->link_offsets[l + 1]; ++q) {
+        const int v = d->link_vertices[q];
+        K.ridx[v] = (int)K.rv.size();
+        K.rv.push_back(v);
+        K.rest.push_back(getx(d->x0, v));
+      }
+      k.r1 = (int)K.rv.size();
+      K.links.push_back(k);
+    }
+    K.ndof = dof;
+    K.nq = sdof;
+    K.jq.assign(sdof, 0.0);
+    K.jqd.assign(sdof, 0.0);
+    skel_write(K);  /* World::Initialize writes the fresh links (World.h:369-370) */
+  }
   assemble_H(*S);
   rcm_order(*S);
   if (!factor(*S)) { delete S; return nullptr; }
+  if (S->skel.L > 0 && !skel_precompute(*S)) { delete S; return nullptr; }
   return S;
+}
+
+int orc_joint_state_size(void* s) { return static_cast<Scene*>(s)->skel.nq; }
+
+int orc_set_joint_state(void* s, const double* jq, const double* jqd) {
+  Skel& K = static_cast<Scene*>(s)->skel;
+  std::copy(jq, jq + K.nq, K.jq.begin());
+  std::copy(jqd, jqd + K.nq, K.jqd.begin());
+  return 0;
+}
+
+int orc_get_joint_state(void* s, double* jq, double* jqd) {
+  const Skel& K = static_cast<Scene*>(s)->skel;
+  std::copy(K.jq.begin(), K.jq.end(), jq);
+  std::copy(K.jqd.begin(), K.jqd.end(), jqd);
+  return 0;
 }
 
 void orc_destroy(void* s) { delete static_cast<Scene*>(s); }
@@ -1798,7 +2266,8 @@ int orc_set_materials(void* s, const double* E, const double* nu) {
   for (size_t t = 0; t < S->tets.size(); ++t) { S->E[t] = E[t]; S->nu[t] = nu[t]; }
   assemble_H(*S);
   rcm_order(*S);
-  return factor(*S) ? 0 : 3;
+  if (!factor(*S)) return 3;
+  return (S->skel.L > 0 && !skel_precompute(*S)) ? 3 : 0;
 }
 
 /* Forward: n_steps steps from (x, v); act = n_steps * n_segments (may be NULL);
@@ -1815,7 +2284,10 @@ int orc_forward(void* s, const double* x, const double* v, const double* act, in
   S->rec_iters.assign(n_steps, 0);
   S->rec_passes.assign(n_steps, 0);
   if (S->freeze == 1) S->frz.assign(n_steps, {});
+  /* without activations: muscle segments 0, pneumatic channels 1 (pneumaticEasy.h:31) */
   std::vector<double> zero_act(std::max(1, S->nseg), 0.0);
+  for (int c : S->sp_ch)
+    if (c >= 0) zero_act[c] = 1.0;
   for (int st = 0; st < n_steps; ++st) {
     const double* a = act ? act + (size_t)st * S->nseg : zero_act.data();
     /* every step starts with no remembered contact forces: World::TimeStepping
@@ -1827,7 +2299,8 @@ int orc_forward(void* s, const double* x, const double* v, const double* act, in
     std::copy(vc.begin(), vc.end(), S->rec_v.begin() + (size_t)st * n3);
     if (S->nseg > 0) std::copy(a, a + S->nseg, S->rec_act.begin() + (size_t)st * S->nseg);
     step_prep(*S, xc.data(), vc.data(), vwc.data(), qn.data());
-    int it = pd_solve(*S, xc.data(), qn.data(), a, nullptr, xn.data(), nthreads);
+    int it = S->skel.L > 0 ? pd_solve_skel(*S, xc.data(), qn.data(), a, xn.data(), nthreads)
+                           : pd_solve(*S, xc.data(), qn.data(), a, nullptr, xn.data(), nthreads);
     contact_phase(*S, xc.data(), vwc.data(), a, xn.data());
     S->rec_passes[st] = S->last_passes;
     S->rec_iters[st] = it;
@@ -1850,6 +2323,7 @@ int orc_backward(void* s, const double* gx_out, const double* gv_out, double* gx
                  double* gE, double* gnu, double* gact) {
   Scene* S = static_cast<Scene*>(s);
   if (S->rec_steps <= 0) return 5;
+  if (S->skel.L > 0) { S->err = "no adjoint for skeleton scenes"; return 8; }
   int N = S->N, n3 = 3 * N;
   int NT = (int)S->tets.size();
   std::vector<double> xb(gx_out, gx_out + n3), vb(gv_out, gv_out + n3);

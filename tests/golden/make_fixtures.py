@@ -2,7 +2,8 @@
 a JSON scene ("Parameters", "Meshes", "Obstacles"), a tet OBJ ('v' + 't' lines,
 0-based tets), a triangle OBJ obstacle ('f' lines, 1-based) and a muscle file
 ('fibre segment x y z' rows).  The meshes are synthetic (a cube-grid beam and
-a ground quad); run `python tests/golden/make_fixtures.py` to regenerate.
+a ground quad; pneumatic.json drives the beam with "Volume Verts" springs);
+run `python tests/golden/make_fixtures.py` to regenerate.
 """
 import json
 import os
@@ -45,6 +46,21 @@ def main():
     }
     with open(os.path.join(out, "beam.json"), "w") as f:
         json.dump(scene, f, indent=1)
+    # the same beam driven by pneumatic springs (actuator type 3): three
+    # "Volume Verts" polylines along x on the beam's top and bottom edges
+    lines = []
+    for y, z in ((2.0, 0.0), (2.0, 2.0), (0.0, 2.0)):
+        on = np.nonzero(np.isclose(x0[:, 1], y) & np.isclose(x0[:, 2], z))[0]
+        lines.append([int(i) for i in on[np.argsort(x0[on, 0])]])
+    pneu = {
+        "Parameters": [{"Simulation HZ": 100, "Handle collision": False, "Self-collision": False,
+                        "Gravity": [0.0, -9.8, 0.0], "Max Iteration": 10}],
+        "Meshes": [{"Obj filename": "beam_scene/beam_tet.obj", "Scale": 0.05, "Youngs Modulus": 5e4,
+                    "Poisson Ratio": 0.3, "Mass": 1.2, "Attach Verts": pins, "Attach Stiffness": 1e8,
+                    "Muscle Stiffness": 1e5, "Actuator type": 3, "Volume Verts": lines}],
+    }
+    with open(os.path.join(out, "pneumatic.json"), "w") as f:
+        json.dump(pneu, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -73,6 +73,30 @@ def test_muscles_forward_and_adjoint():
         assert rel(bg[k], bo[k]) < GRAD_TOL, k
 
 
+def test_pneumatic_springs_forward_and_adjoint():
+    """Pneumatic springs (PneumaticConstraint: length rest * activation) on
+    their own activation channels after one muscle chain's segments: positions,
+    and gradients including dL/d(activation) of both kinds of channel; then
+    the default activations (muscles 0, pneumatic channels 1)."""
+    d = S.pneumatic_beam()
+    n = 5
+    act = np.random.default_rng(12).uniform(0.6, 1.4, (n, d.n_segments))
+    g, o, (xg, vg, tg), ro = run_both(d, n, act=act)
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    rng = np.random.default_rng(13)
+    gx, gv = rng.standard_normal(xg.size), rng.standard_normal(xg.size)
+    bg, bo = g.backward(gx, gv), o.backward(gx, gv)
+    for k in ("x", "v", "E", "nu", "act"):
+        assert rel(bg[k], bo[k]) < GRAD_TOL, k
+    assert np.abs(bg["act"][:, 2:]).max() > 0  # the pneumatic channels
+    x = d.x0.reshape(-1).copy()
+    xg, vg = g.forward(x, np.zeros_like(x), n_steps=3)
+    ro = o.forward(x, np.zeros_like(x), n_steps=3)
+    assert rel(xg, ro["x"]) < POS_TOL
+    g.close()
+
+
 def test_cloth_forward_and_adjoint():
     d = S.cloth_sheet(nv=10)
     n = 6
@@ -460,11 +484,13 @@ def test_checkpoints_every_k_steps_give_identical_gradients(case, budget):
         assert np.array_equal(out[0][2][key], out[1][2][key]), key
 
 
-@pytest.mark.parametrize("name,pre", [("bridgesus", 0), ("baymax", 20), ("cloth_ball", 68), ("octopus", 0)])
+@pytest.mark.parametrize("name,pre", [("bridgesus", 0), ("baymax", 20), ("cloth_ball", 68), ("octopus", 0),
+                                      ("droneman", 0)])
 def test_reference_data_scenes_forward_and_adjoint(name, pre):
-    """Four of diff_fem's own data scenes (tests/golden/ref_scenes, written by
+    """Five of diff_fem's own data scenes (tests/golden/ref_scenes, written by
     make_ref_scenes.py from its data directory): 10 steps forward and adjoint
-    against the oracle.  baymax and cloth_ball start from the oracle's state
+    against the oracle (droneman: its 48 pneumatic springs on random
+    activations).  baymax and cloth_ball start from the oracle's state
     `pre` steps in, a few steps before their first contact, so the window
     holds contact passes (baymax: the ground obstacle; cloth_ball: soft-soft
     contact with the ball)."""
@@ -553,3 +579,49 @@ def test_fused_contact_phase_matches_the_loop_of_kernels(case):
     assert out[0][2].sum() > 0
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("case", ["articulated_beam", "baymax_skeleton"])
+def test_skeleton_forward_matches_oracle(case):
+    """Articulated skeleton (Link tree, World::ComputeSolution's rigid branch):
+    trajectory, iteration counts and joint state (World::mJointQ / mJointQd)
+    against the oracle, which solves the reference's Schur form literally
+    (two Qf solves, the precomputed Qb_M - Qc_L Qf^-1 Qc_L^T); the engine uses
+    the equivalent multiplier form on the step's full solve.  A second call
+    continues from the joint state the first left; set_joint_state restarts
+    from a given state; the adjoint is refused."""
+    import os
+    rng = np.random.default_rng(31)
+    if case == "articulated_beam":
+        d = S.articulated_beam()
+        n = 8
+        act = np.tile([0.5, 2.0], (n, 1)) * rng.uniform(0.5, 1.5, (n, 2))
+    else:
+        d = S.load_npz(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_scenes",
+                                    "baymax_skeleton.npz"))
+        n = 10
+        act = rng.uniform(-20.0, 20.0, (n, d.n_segments))
+    x = d.x0.reshape(-1).copy()
+    v = np.zeros_like(x)
+    g, o, (xg, vg, tg), ro = run_both(d, n, act=act, x=x, v=v)
+    assert np.array_equal(g.iterations(n), ro["iters"])
+    assert rel(tg, ro["traj"]) < POS_TOL
+    assert rel(vg, ro["v"]) < POS_TOL
+    jg, jdg = g.joint_state()
+    jo, jdo = o.joint_state()
+    assert np.abs(jg - jo).max() < 1e-9 and np.abs(jdg - jdo).max() < 1e-9
+    assert np.abs(jg[12:]).max() > 1e-3  # the torques moved the joints
+    # continue from the state the first call left
+    xg2, vg2 = g.forward(xg, vg, n_steps=2, act=act[:2])
+    ro2 = o.forward(ro["x"], ro["v"], n_steps=2, act=act[:2])
+    assert rel(xg2, ro2["x"]) < POS_TOL
+    # restart from a given joint state
+    g.set_joint_state(jo, jdo)
+    o.set_joint_state(jo, jdo)
+    xg3, _ = g.forward(ro["x"], ro["v"], n_steps=2, act=act[:2])
+    ro3 = o.forward(ro["x"], ro["v"], n_steps=2, act=act[:2])
+    assert rel(xg3, ro3["x"]) < POS_TOL
+    with pytest.raises(_capi.DfemError) as ex:
+        g.backward(np.ones_like(x), np.ones_like(x))
+    assert ex.value.code == _capi.DFEM_ERR_UNSUPPORTED
+    g.close()

@@ -143,3 +143,55 @@ def test_corrupt_scene_files_raise_clear_errors(tmp_path):
         assert what in str(ex.value), (what, str(ex.value))
     with pytest.raises(FileNotFoundError):
         loader.load_scene(str(tmp_path / "missing.json"), 1)
+
+
+def test_volume_verts_become_pneumatic_springs():
+    """Dfobj.h:231-251: one pneumatic spring per consecutive pair of every
+    "Volume Verts" polyline (rest length from the scaled mesh, weight =
+    "Muscle Stiffness"), each on its own activation channel."""
+    import json
+    L = loader.load_scene("beam_scene/pneumatic.json", 1, data_root=GOLDEN)
+    d = L.desc
+    with open(os.path.join(GOLDEN, "beam_scene", "pneumatic.json")) as fh:
+        lines = json.load(fh)["Meshes"][0]["Volume Verts"]
+    pairs = [(a, b) for line in lines for a, b in zip(line[:-1], line[1:])]
+    assert np.array_equal(d.spring_vertices, np.asarray(pairs))
+    assert np.array_equal(d.spring_channel, np.arange(len(pairs)))
+    assert d.n_segments == len(pairs) and L.bodies[0].n_pneumatic == len(pairs)
+    x = d.x0.reshape(-1, 3)
+    assert np.allclose(d.spring_rest, [np.linalg.norm(x[a] - x[b]) for a, b in pairs], rtol=0, atol=1e-15)
+    assert np.allclose(d.spring_rest, 0.05)  # unit cube edges at "Scale" 0.05
+    assert np.all(d.spring_weight == 1e5)
+
+
+def test_bones_become_skeleton_links(tmp_path):
+    """Dfobj.h:254-288: one link per bone (parent, joint type, unscaled joint
+    position, normalised axis, the bone's vertices); the joint torques of the
+    non-root links are activation channels after the muscle segments."""
+    import json
+    src = json.load(open(os.path.join(GOLDEN, "beam_scene", "beam.json")))
+    mesh = src["Meshes"][0]
+    for k in ("Muscle filename", "Attach Verts", "Attach Stiffness"):
+        mesh.pop(k)
+    mesh["Actuator type"] = 1
+    mesh["Obj filename"] = os.path.join(GOLDEN, "beam_scene", "beam_tet.obj")
+    mesh["Bones"] = [
+        {"Parent ID": -1, "Joint Type": "ALL", "Joint Pos": [0, 0, 0], "Joint Axis": [0, 0, 0], "Vertices": [0, 1, 2]},
+        {"Parent ID": 0, "Joint Type": "ROTATIONAL", "Joint Pos": [0.1, 0.05, 0.05], "Joint Axis": [0, 0, 2],
+         "Vertices": [30, 31]},
+    ]
+    src["Parameters"][0]["Handle collision"] = False
+    src.pop("Obstacles")
+    path = tmp_path / "bones.json"
+    path.write_text(json.dumps(src))
+    L = loader.load_scene(str(path), 1, data_root=str(tmp_path))
+    d = L.desc
+    assert list(d.link_parent) == [-1, 0] and list(d.link_type) == [2, 1]
+    assert np.array_equal(d.link_offsets, [0, 3, 5]) and np.array_equal(d.link_vertices, [0, 1, 2, 30, 31])
+    assert np.allclose(d.link_joint[1], [0.1, 0.05, 0.05]) and np.allclose(d.link_axis[1], [0, 0, 2])
+    assert list(d.link_channel) == [-1, 0] and d.n_segments == 1 and L.bodies[0].n_links == 2
+    bad = json.loads(path.read_text())
+    bad["Meshes"][0]["Bones"][1]["Joint Type"] = "HINGE"
+    path.write_text(json.dumps(bad))
+    with pytest.raises(loader.SceneFormatError):
+        loader.load_scene(str(path), 1, data_root=str(tmp_path))

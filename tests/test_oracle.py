@@ -185,36 +185,40 @@ def _loss(o, x, v, gx, gv, n, act=None):
     return gx @ r["x"] + gv @ r["v"], r["iters"]
 
 
-@pytest.mark.parametrize("builder", ["cantilever", "muscle_beam", "cloth_sheet"])
+@pytest.mark.parametrize("builder", ["cantilever", "muscle_beam", "cloth_sheet", "pneumatic_beam"])
 def test_adjoint_matches_central_differences(builder):
+    """Each case draws from its own seed (the check needs iteration counts
+    that no perturbation changes, a property of the draw, so the draw must
+    not depend on which tests ran before)."""
     d = getattr(S, builder)()
     o = O.OracleScene(d)
     n = 3
-    x = d.x0.reshape(-1) + 1e-3 * RNG.standard_normal(3 * d.n_vertices)
-    v = 0.05 * RNG.standard_normal(3 * d.n_vertices)
-    gx = RNG.standard_normal(x.size)
-    gv = RNG.standard_normal(x.size)
-    act = RNG.uniform(0, 1, (n, d.n_segments)) if d.n_segments else None
+    rng = np.random.default_rng({"cantilever": 101, "muscle_beam": 102, "cloth_sheet": 103, "pneumatic_beam": 104}[builder])
+    x = d.x0.reshape(-1) + 1e-3 * rng.standard_normal(3 * d.n_vertices)
+    v = 0.05 * rng.standard_normal(3 * d.n_vertices)
+    gx = rng.standard_normal(x.size)
+    gv = rng.standard_normal(x.size)
+    act = rng.uniform(0, 1, (n, d.n_segments)) if d.n_segments else None
     _, it0 = _loss(o, x, v, gx, gv, n, act)
     g = o.backward(gx, gv)
     checks = []
-    dx = RNG.standard_normal(x.size)
+    dx = rng.standard_normal(x.size)
     eps = 1e-6
     (lp, ip), (lm, im) = _loss(o, x + eps * dx, v, gx, gv, n, act), _loss(o, x - eps * dx, v, gx, gv, n, act)
     checks.append((g["x"] @ dx, (lp - lm) / (2 * eps), ip, im))
-    dv = RNG.standard_normal(x.size)
+    dv = rng.standard_normal(x.size)
     (lp, ip), (lm, im) = _loss(o, x, v + eps * dv, gx, gv, n, act), _loss(o, x, v - eps * dv, gx, gv, n, act)
     checks.append((g["v"] @ dv, (lp - lm) / (2 * eps), ip, im))
     if d.n_tets:
         E, nu = d.youngs.copy(), d.poisson.copy()
-        dE = RNG.standard_normal(E.size) * E
+        dE = rng.standard_normal(E.size) * E
         rel = 1e-5
         o.set_materials(E + rel * dE, nu); lp, ip = _loss(o, x, v, gx, gv, n, act)
         o.set_materials(E - rel * dE, nu); lm, im = _loss(o, x, v, gx, gv, n, act)
         o.set_materials(E, nu)
         checks.append((g["E"] @ dE, (lp - lm) / (2 * rel), ip, im))
     if act is not None:
-        da = RNG.standard_normal(act.shape)
+        da = rng.standard_normal(act.shape)
         (lp, ip), (lm, im) = _loss(o, x, v, gx, gv, n, act + eps * da), _loss(o, x, v, gx, gv, n, act - eps * da)
         checks.append((np.sum(g["act"] * da), (lp - lm) / (2 * eps), ip, im))
     for adj, fd, ip, im in checks:
@@ -407,3 +411,70 @@ def test_soft_contact_adjoint_matches_central_differences():
     for adj, fd, ip, im in checks:
         assert np.array_equal(ip, it0) and np.array_equal(im, it0)
         assert abs(adj - fd) <= 1e-5 * max(1.0, abs(fd)), (adj, fd)
+
+
+# ---- articulated skeleton (Link, sim/constants.h; World::ComputeSolution's rigid branch)
+
+def _damped_fall(h, g, damping, n):
+    """Centre-of-mass displacement of n damped free-fall steps from rest:
+    x_{k+1} = x_k + h v_k + h^2 g, v_{k+1} = damping (x_{k+1} - x_k) / h."""
+    x, v = 0.0, 0.0
+    for _ in range(n):
+        dx = h * v + h * h * g
+        x += dx
+        v = damping * dx / h
+    return x
+
+
+def test_skeleton_rest_state_is_a_fixed_point():
+    d = S.articulated_beam(gravity=(0.0, 0.0, 0.0))
+    o = O.OracleScene(d)
+    x = d.x0.reshape(-1).copy()
+    r = o.forward(x, np.zeros_like(x), n_steps=3)
+    jq, jqd = o.joint_state()
+    assert np.abs(r["x"] - x).max() < 1e-14
+    eye = np.r_[np.eye(3).reshape(-1), np.zeros(3 + 2)]
+    assert np.abs(jq - eye).max() < 1e-14 and np.abs(jqd - eye).max() < 1e-14
+
+
+def test_skeleton_links_stay_rigid_and_the_centre_of_mass_falls_freely():
+    """Each link's vertices keep their rest distances (V0 = prefix Tr (rest -
+    joint) with rotations); the centre of mass follows damped free fall (the
+    link system's root-translation rows make the reaction on the rigid
+    vertices sum to zero; what remains is the second-order gap between the
+    linearised link update the solve assumed and UpdateT's)."""
+    d = S.articulated_beam()
+    o = O.OracleScene(d)
+    n = 6
+    x = d.x0.reshape(-1).copy()
+    act = np.tile([0.5, 2.0], (n, 1))
+    r = o.forward(x, np.zeros_like(x), n_steps=n, act=act)
+    X, X0 = r["x"].reshape(-1, 3), x.reshape(-1, 3)
+    for l in range(3):
+        vs = d.link_vertices[d.link_offsets[l]:d.link_offsets[l + 1]]
+        D = np.linalg.norm(X[vs][:, None] - X[vs][None], axis=2)
+        D0 = np.linalg.norm(X0[vs][:, None] - X0[vs][None], axis=2)
+        assert np.abs(D - D0).max() < 1e-13, l
+    m = d.mass
+    com = (m[:, None] * (X - X0)).sum(0) / m.sum()
+    fall = _damped_fall(d.time_step, -9.8, d.damping, n)
+    assert abs(com[1] - fall) < 1e-6 * abs(fall) and abs(com[0]) < 1e-6 * abs(fall) and abs(com[2]) < 1e-12
+    jq, jqd = o.joint_state()
+    assert jq.size == 14 and abs(jq[12]) > 1e-3 and abs(jq[13]) > 1e-4  # the torques turned / slid the links
+    R = jq[:9].reshape(3, 3)
+    assert abs(np.linalg.det(R) - 1.0) < 1e-3  # T.R = (I + [w]x) Tr.R: a rotation to first order
+
+
+def test_skeleton_joint_state_round_trip_and_determinism():
+    d = S.articulated_beam()
+    x = d.x0.reshape(-1).copy()
+    act = np.tile([0.5, 2.0], (4, 1))
+    a = O.OracleScene(d)
+    ra = a.forward(x, np.zeros_like(x), n_steps=4, act=act)
+    b = O.OracleScene(d)
+    rb1 = b.forward(x, np.zeros_like(x), n_steps=2, act=act[:2])
+    jq, jqd = b.joint_state()
+    c = O.OracleScene(d)
+    c.set_joint_state(jq, jqd)
+    rc = c.forward(rb1["x"], rb1["v"], n_steps=2, act=act[2:])
+    assert np.array_equal(rc["x"], ra["x"]) and np.array_equal(c.joint_state()[0], a.joint_state()[0])

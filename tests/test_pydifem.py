@@ -108,3 +108,73 @@ def test_sim_all_gradient_matches_finite_difference(env):
     lm = pd.forward_all(x0.numpy(), v0.numpy(), [5e4 - eps, 0.3], env)[0].reshape(-1, 3)[:, 1].mean()
     fd = (lp - lm) / (2 * eps)
     assert abs(g - fd) <= 1e-4 * max(abs(fd), 1e-12)
+
+
+def test_pneumatic_actions_gradient_matches_central_differences():
+    """Actuator type 3 (Dfobj::SetActions sets each pneumatic spring's
+    activation to its action): dL/dtau of backward_act against central
+    differences of forward_act, on the beam fixture's "Volume Verts" springs."""
+    from diff_fem_b200 import loader, pydifem as pd
+    env = pd.Environment(loader.load_scene("beam_scene/pneumatic.json", 1, data_root=GOLDEN))
+    n_act = sum(o.mActions.size for o in env.mDfobjs)
+    assert n_act == env.desc.n_segments == 18
+    x0 = env.mSoftWorld.mX.copy()
+    v0 = 0.05 * np.random.default_rng(6).standard_normal(x0.size)
+    tau0 = np.random.default_rng(7).uniform(0.7, 1.3, n_act)
+    w = np.random.default_rng(8).standard_normal(x0.size)
+
+    def loss(tau):
+        x, _, _, _ = pd.forward_act(x0, v0, [], [], tau, env, True)
+        return float(w @ x)
+
+    _, _, _, _, dtau = pd.backward_act(x0, v0, [], [], tau0, w, np.zeros_like(w), [], [], env, True)
+    assert np.abs(dtau).max() > 0
+    d = np.random.default_rng(9).standard_normal(n_act)
+    eps = 1e-6
+    fd = (loss(tau0 + eps * d) - loss(tau0 - eps * d)) / (2 * eps)
+    assert abs(dtau @ d - fd) <= 1e-6 * max(abs(fd), 1e-12), (dtau @ d, fd)
+
+
+def test_skeleton_joint_state_through_forward_act(tmp_path):
+    """Actuator type 1: forward_act takes and returns the joint state
+    (jq, jqd: World::mJointQ / mJointQd) and tau are the joint torques
+    (World::mJointTorque); against the oracle stepped with the same state and
+    torque channel."""
+    import json
+    from diff_fem_b200 import loader, pydifem as pd
+    from oracle import oracle as O
+    src = json.load(open(os.path.join(GOLDEN, "beam_scene", "beam.json")))
+    mesh = src["Meshes"][0]
+    for k in ("Muscle filename", "Attach Verts", "Attach Stiffness"):
+        mesh.pop(k)
+    mesh["Actuator type"] = 1
+    mesh["Obj filename"] = os.path.join(GOLDEN, "beam_scene", "beam_tet.obj")
+    L = loader.load_scene(os.path.join(GOLDEN, "beam_scene", "beam.json"), 1, data_root=GOLDEN)
+    x0 = L.desc.x0.reshape(-1, 3)
+    left = [int(i) for i in np.nonzero(np.isclose(x0[:, 0], 0.0))[0]]
+    mid = [int(i) for i in np.nonzero(np.isclose(x0[:, 0], 0.15))[0]]
+    mesh["Bones"] = [
+        {"Parent ID": -1, "Joint Type": "ALL", "Joint Pos": [0, 0, 0], "Joint Axis": [0, 0, 0], "Vertices": left},
+        {"Parent ID": 0, "Joint Type": "ROTATIONAL", "Joint Pos": [0.15, 0.05, 0.05], "Joint Axis": [0, 0, 1],
+         "Vertices": mid},
+    ]
+    src["Parameters"][0]["Handle collision"] = False
+    src.pop("Obstacles")
+    path = tmp_path / "bones.json"
+    path.write_text(json.dumps(src))
+    env = pd.Environment(loader.load_scene(str(path), 1, data_root=str(tmp_path)))
+    assert sum(o.mActions.size for o in env.mDfobjs) == 1
+    o = O.OracleScene(env.desc)
+    q, qd = env.mSoftWorld.mX.copy(), env.mSoftWorld.mV.copy()
+    jq, jqd = env.mSoftWorld.mJointQ.copy(), env.mSoftWorld.mJointQd.copy()
+    assert jq.size == 13 and np.array_equal(jq[:9], np.eye(3).reshape(-1))
+    for step in range(3):
+        tau = np.array([0.3 * (step + 1)])
+        q2, qd2, jq2, jqd2 = pd.forward_act(q, qd, jq, jqd, tau, env, True)
+        o.set_joint_state(jq, jqd)
+        r = o.forward(q, qd, n_steps=1, act=tau.reshape(1, 1))
+        jo, jdo = o.joint_state()
+        assert np.abs(q2 - r["x"]).max() < 1e-9 * max(1.0, np.abs(r["x"]).max())
+        assert np.abs(jq2 - jo).max() < 1e-9 and np.abs(jqd2 - jdo).max() < 1e-9
+        q, qd, jq, jqd = q2, qd2, jq2, jqd2
+    assert abs(jq[12]) > 1e-4
