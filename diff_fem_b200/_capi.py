@@ -104,6 +104,10 @@ SIGNATURES = [
     ("dfem_get_launch_count", C.c_int, [_VP, C.POINTER(C.c_int64)]),
     ("dfem_profile_phases", C.c_int, [_VP, C.c_int32, C.POINTER(C.c_double)]),
     ("dfem_synchronize", C.c_int, [_VP]),
+    ("dfem_obj_writer_create", C.c_int, [C.c_int32, _pi, _pi, _pi, C.POINTER(C.c_char_p), C.c_int32, C.POINTER(_VP)]),
+    ("dfem_obj_writer_enqueue", C.c_int, [_VP, _VP, C.c_char_p, _VP, C.c_int]),
+    ("dfem_obj_writer_flush", C.c_int, [_VP]),
+    ("dfem_obj_writer_destroy", C.c_int, [_VP]),
     ("dfem_last_error", C.c_char_p, []),
     ("dfem_abi_version", C.c_int, []),
     ("dfem_set_limit", C.c_int, [_VP, C.c_int32, C.c_int64]),

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdfem.so")
-SOURCES = ["engine.cu", "noalloc.cu", "scene.cpp", "cholesky.cpp", "resident_plan.cpp"]
+SOURCES = ["engine.cu", "noalloc.cu", "scene.cpp", "cholesky.cpp", "resident_plan.cpp", "obj_writer.cpp"]
 HEADERS = ["pd_kernels.cu", "pd_math.cuh", "kernels.cuh", "factor_kernels.cuh", "contact_kernels.cuh", "tma.cuh",
            "resident_solve.cuh", "drag_kernels.cuh", "skeleton_kernels.cuh",
            "scene.h", "cholesky.h", "resident_plan.h"]

@@ -815,6 +815,10 @@ static int build_obstacle_grid(dfem_scene* sc) {
 
 static int upload_skeleton(dfem_scene* sc);
 
+// for the OBJ writer (obj_writer.cpp): the stream and device of a scene
+cudaStream_t scene_stream(dfem_scene* sc) { return sc->stream; }
+int scene_device(dfem_scene* sc) { return sc->device; }
+
 static int upload_scene(dfem_scene* sc) {
   HostScene& s = sc->hs;
   CK(sc->mass.upload(s.mass));

@@ -296,3 +296,48 @@ def host_factor_solve(desc, b) -> tuple:
     inf = _capi.SceneInfoC()
     check(lib().dfem_host_factor_solve(C.byref(cdesc), b.ctypes.data, x.ctypes.data, C.byref(inf)))
     return x, {name: getattr(inf, name) for name, _ in inf._fields_}
+
+
+class ObjWriter:
+    """Asynchronous per-step OBJ output (dfem_obj_writer_*): Environment::SaveObj
+    / Save (sim/Environment.h:295-327) as a queue of staging slots drained by a
+    host thread.  bodies: list of (vertex_count, faces (F, 3) body-local ids,
+    file-name suffix); states are 3N in the bodies' order, numpy (host) or
+    CUDA tensors (copied on the scene's stream)."""
+
+    def __init__(self, bodies, depth: int = 4):
+        nv = [int(b[0]) for b in bodies]
+        fc = [np.asarray(b[1], np.int32).reshape(-1, 3) for b in bodies]
+        self._voff = np.cumsum([0] + nv).astype(np.int32)
+        self._foff = np.cumsum([0] + [f.shape[0] for f in fc]).astype(np.int32)
+        self._faces = np.ascontiguousarray(np.concatenate(fc) if fc else np.zeros((0, 3), np.int32), np.int32)
+        self._suffix = (C.c_char_p * len(bodies))(*[str(b[2]).encode() for b in bodies])
+        P = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        h = C.c_void_p()
+        check(lib().dfem_obj_writer_create(len(bodies), P(self._voff), P(self._foff), P(self._faces),
+                                           self._suffix, int(depth), C.byref(h)))
+        self._h = h
+        self._keep = []
+
+    def write(self, prefix: str, x, scene: Optional["Scene"] = None):
+        p, m, keep = _ptr(x)
+        if m == DFEM_MEM_DEVICE:
+            if scene is None:
+                raise ValueError("a device state needs the scene whose stream produced it")
+            _sync_torch(x)
+        check(lib().dfem_obj_writer_enqueue(self._h, scene.handle if scene is not None else None,
+                                            str(prefix).encode(), p, m))
+
+    def flush(self):
+        check(lib().dfem_obj_writer_flush(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().dfem_obj_writer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

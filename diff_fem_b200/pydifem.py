@@ -29,12 +29,16 @@ from typing import List, Optional
 import numpy as np
 
 from . import loader
-from .engine import Scene
+from .engine import ObjWriter, Scene
 
 try:
     import torch
 except Exception:  # pragma: no cover
     torch = None
+
+
+def _is_cuda(a) -> bool:
+    return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
 
 
 def vector2double(v) -> List[float]:
@@ -144,6 +148,7 @@ class Environment:
         self.mSoftWorld.mJointQ = self._jq0.copy()
         self.mSoftWorld.mJointQd = self._jq0.copy()
         self.mSoftWorld.mJointTorque = np.zeros(max(0, self._jq0.size - 12))
+        self._obj = None  # the OBJ writer, made on the first SaveObj
         self._E = np.asarray(self.desc.youngs, np.float64).copy()
         self._nu = np.asarray(self.desc.poisson, np.float64).copy()
 
@@ -198,16 +203,25 @@ class Environment:
         self.mSoftWorld.mV[:] = 0.0
 
     def SaveObj(self, filename: str, x) -> None:
-        """Environment::SaveObj: one OBJ per body (vertices + surface faces)."""
-        x = np.asarray(x, np.float64).reshape(-1, 3)
-        for i, b in enumerate(self.loaded.bodies):
-            tag = "_DfObj" if b.kind == "mesh" else "_DfCloths"
-            idx = i if b.kind == "mesh" else i - len(self.mDfobjs)
-            with open(f"{filename}{tag}{idx}.obj", "w") as fh:
-                for p in x[b.offset:b.offset + b.n]:
-                    fh.write("v %06f %06f %06f\n" % tuple(p))
-                for f in (b.contours if b.contours is not None else []):
-                    fh.write("f %d %d %d\n" % (f[0] + 1, f[1] + 1, f[2] + 1))
+        """Environment::SaveObj: one OBJ per body (vertices + surface faces),
+        written asynchronously by the engine's OBJ writer (x: numpy, or a CUDA
+        tensor produced on this scene's stream); FlushObj waits for the files."""
+        if self._obj is None:
+            bodies = []
+            for i, b in enumerate(self.loaded.bodies):
+                tag = "_DfObj" if b.kind == "mesh" else "_DfCloths"
+                idx = i if b.kind == "mesh" else i - len(self.mDfobjs)
+                faces = b.contours if b.contours is not None else np.zeros((0, 3), np.int32)
+                bodies.append((b.n, faces, f"{tag}{idx}.obj"))
+            self._obj = ObjWriter(bodies)
+        if _is_cuda(x):
+            self._obj.write(filename, x, scene=self.scene)
+        else:
+            self._obj.write(filename, np.asarray(x, np.float64).reshape(-1))
+
+    def FlushObj(self) -> None:
+        if self._obj is not None:
+            self._obj.flush()
 
 
 def init_env(total_step: int, config_path: str, device: int = 0) -> Environment:
@@ -293,6 +307,7 @@ def forward_all(q, qd, tau, env: Environment, write_obj: Optional[str] = None):
         os.makedirs(os.path.dirname(write_obj) or ".", exist_ok=True)
         for s in range(n):
             env.SaveObj(f"{write_obj}{s:03d}", traj[s])
+        env.FlushObj()
     env.mSoftWorld.mX, env.mSoftWorld.mV = x.copy(), v.copy()
     return [x, v]
 

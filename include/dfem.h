@@ -408,6 +408,32 @@ int dfem_debug_fail_allocations(int64_t after);
 /* Synchronise the scene's stream. */
 int dfem_synchronize(dfem_scene *scene);
 
+/*
+ * Asynchronous per-step OBJ output.  Replaces Environment::SaveObj / Save
+ * (sim/Environment.h:295-327): for every body, `prefix + suffix[b]` receives
+ * "v %06f %06f %06f" lines for the body's vertices and "f %d %d %d" lines
+ * (1-based) for its surface faces.  dfem_obj_writer_enqueue copies the state
+ * into one of `depth` staging slots (pinned host memory when a device is
+ * present) and returns; a host thread formats and writes the files.  A
+ * device state is copied on the scene's stream after the work already queued
+ * there (the step that produced it), so the writes overlap the next steps.
+ * Enqueue blocks only while every slot is in flight.
+ */
+typedef struct dfem_obj_writer dfem_obj_writer;  /* opaque */
+
+/* Bodies: vertex_offsets (n_bodies+1) into the 3N state (user order),
+ * face_offsets (n_bodies+1) into faces (3 body-local vertex ids each),
+ * suffixes (n_bodies file-name suffixes, e.g. "_DfObj0.obj"). */
+int dfem_obj_writer_create(int32_t n_bodies, const int32_t *vertex_offsets, const int32_t *face_offsets,
+                           const int32_t *faces, const char *const *suffixes, int32_t depth,
+                           dfem_obj_writer **out);
+/* Queue one state x (3 * vertex_offsets[n_bodies] doubles; mem: enum
+ * dfem_mem; a device state needs `scene`, whose stream orders the copy). */
+int dfem_obj_writer_enqueue(dfem_obj_writer *writer, dfem_scene *scene, const char *prefix, const double *x, int mem);
+/* Wait until every queued state is written; returns the first write error. */
+int dfem_obj_writer_flush(dfem_obj_writer *writer);
+int dfem_obj_writer_destroy(dfem_obj_writer *writer);
+
 /* Last error message of the calling thread ("" if none). */
 const char *dfem_last_error(void);
 

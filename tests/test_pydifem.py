@@ -178,3 +178,21 @@ def test_skeleton_joint_state_through_forward_act(tmp_path):
         assert np.abs(jq2 - jo).max() < 1e-9 and np.abs(jqd2 - jdo).max() < 1e-9
         q, qd, jq, jqd = q2, qd2, jq2, jqd2
     assert abs(jq[12]) > 1e-4
+
+
+def test_save_obj_from_device_and_host_states(env, tmp_path):
+    """Environment::SaveObj through the asynchronous writer: a CUDA state is
+    copied on the scene's stream, a host state directly; both files carry the
+    reference's format."""
+    import torch
+    from diff_fem_b200 import pydifem as pd
+    x = env.mSoftWorld.mX.copy()
+    xn, _, _, _ = pd.forward_act(x, np.zeros_like(x), [], [], np.zeros(0), env, False)
+    env.SaveObj(str(tmp_path / "host"), xn)
+    env.SaveObj(str(tmp_path / "dev"), torch.tensor(xn, device="cuda"))
+    env.FlushObj()
+    a = (tmp_path / "host_DfObj0.obj").read_text()
+    b = (tmp_path / "dev_DfObj0.obj").read_text()
+    assert a == b and a.startswith("v ") and "\nf " in a
+    X = xn.reshape(-1, 3)
+    assert a.splitlines()[0] == "v %06f %06f %06f" % tuple(X[0])
