@@ -516,7 +516,8 @@ def batch_config(args, descs) -> dict:
     T = [d.n_tets for d in descs]
     return {
         "workload": f"{len(descs)} independent scenes, tets log-uniform in [1e3, 5e4] (seed 7): beams "
-                    "(x=0 pinned, per-tet E~logU[1e4,1e6]) alternating with 8-arm muscle stars (no ground), "
+                    "(x=0 pinned, per-tet E~logU[1e4,1e6]) alternating with 8-arm muscle stars, each on its own "
+                    "ground quad (mu=0.5, obstacle contact inside the batch), "
                     "h=1/60, K=15, random activations per segment per step (seed 42), "
                     f"{SIM_STEPS} steps forward + adjoint of L=|x_end - x_0|^2",
         "scenes": len(descs), "tets_total": int(sum(T)), "vertices_total": int(sum(d.n_vertices for d in descs)),

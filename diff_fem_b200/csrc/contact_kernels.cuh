@@ -314,8 +314,8 @@ __device__ __forceinline__ bool bp_candidates(const ContactDev& c, Vec3<double> 
 }
 
 // Detection of contact vertex a against the obstacle faces (the broad
-// phase's candidates, or all of them), in ascending face order; true when it
-// hit a face.
+// phase's candidates, or all of them — in a batch, all of its part's), in
+// ascending face order; true when it hit a face.
 __device__ __forceinline__ bool contact_detect_item(const ContactDev& c, int a, const double* xt, const double* xk,
                                                     int* status) {
   int gv = c.cverts[a];
@@ -325,9 +325,10 @@ __device__ __forceinline__ bool contact_detect_item(const ContactDev& c, int a, 
   int ncand = 0;
   const bool culled = bp_candidates(c, mk3(fmin(p0.x, p1.x), fmin(p0.y, p1.y), fmin(p0.z, p1.z)),
                                     mk3(fmax(p0.x, p1.x), fmax(p0.y, p1.y), fmax(p0.z, p1.z)), cand, &ncand);
-  const int nf = culled ? ncand : c.nof;
+  const int f0 = c.np > 1 ? c.pf0[c.cpart[a]] : 0;
+  const int nf = culled ? ncand : (c.np > 1 ? c.pf0[c.cpart[a] + 1] - f0 : c.nof);
   for (int k = 0; k < nf; ++k) {
-    const int f = culled ? cand[k] : k;
+    const int f = culled ? cand[k] : f0 + k;
     Vec3<double> n;
     const int* fv = c.obs_f + 3 * f;
     if (!vf_impact(p0, p1, ld3(c.obs_x, fv[0]), ld3(c.obs_x, fv[1]), ld3(c.obs_x, fv[2]), 1.0, &n)) continue;
@@ -439,22 +440,28 @@ __global__ void k_contact_ctl_detect(ContactDev c, cudaGraphConditionalHandle h)
 // Jacobi iteration, part 1 (mode 1): ori_x = x_n1 and the max-norm test against xold.
 // ori_x = x_n1 at vertex i, its max-norm change; record of contact vertex i's
 // impact lists for the iteration with record index rk (-1: none).
+// ori_x = x_n1 at vertex i and its max-norm change
+__device__ __forceinline__ double contact_prep_vertex(const ContactDev& c, int i, double* xk) {
+  Vec3<double> x = ld3(c.xn1, i);
+  st3(xk, i, x);
+  Vec3<double> dl = x - ld3(c.xold, i);
+  return fmax(fabs(dl.x), fmax(fabs(dl.y), fabs(dl.z)));
+}
+
+// recording for the adjoint: the impact lists of contact vertex a this
+// iteration will use, at record index rk
+__device__ __forceinline__ void contact_prep_record(const ContactDev& c, int a, int rk) {
+  const int cnt = c.imp_cnt[a];
+  c.rec_cnt[(size_t)rk * c.nc + a] = cnt;
+  // 64-bit offset to the vertex's normals (the record spans billions of doubles)
+  double* rn = c.rec_n + ((size_t)rk * c.nc + a) * kMaxImpactsPerVertex * 3;
+  for (int q = 0; q < cnt; ++q) st3(rn, q, ld3(c.imp_n, a * kMaxImpactsPerVertex + q));
+}
+
 __device__ __forceinline__ double contact_prep_item(const ContactDev& c, int i, int N, double* xk, int rk) {
   double e = 0;
-  if (i < N) {
-    Vec3<double> x = ld3(c.xn1, i);
-    st3(xk, i, x);
-    Vec3<double> dl = x - ld3(c.xold, i);
-    e = fmax(fabs(dl.x), fmax(fabs(dl.y), fabs(dl.z)));
-  }
-  // recording for the adjoint: the impact lists this iteration will use
-  if (rk >= 0 && i < c.nc) {
-    const int cnt = c.imp_cnt[i];
-    c.rec_cnt[(size_t)rk * c.nc + i] = cnt;
-    // 64-bit offset to the vertex's normals (the record spans billions of doubles)
-    double* rn = c.rec_n + ((size_t)rk * c.nc + i) * kMaxImpactsPerVertex * 3;
-    for (int q = 0; q < cnt; ++q) st3(rn, q, ld3(c.imp_n, i * kMaxImpactsPerVertex + q));
-  }
+  if (i < N) e = contact_prep_vertex(c, i, xk);
+  if (rk >= 0 && i < c.nc) contact_prep_record(c, i, rk);
   return e;
 }
 
@@ -530,7 +537,7 @@ __device__ __forceinline__ void contact_rhs_item(const SceneDev& d, const Contac
   if (rk >= 0) {
     st3(c.rec_x + (size_t)rk * 3 * d.N, i, ld3(xk, i));
     st3(c.rec_prev + (size_t)rk * 3 * d.N, i, prev);
-    if (i == 0) c.rec_first[rk] = first ? 1 : 0;
+    if (i == 0 && c.np <= 1) c.rec_first[rk] = first ? 1 : 0;  // batches: per part, by their phase kernel
   }
 }
 
@@ -654,6 +661,167 @@ __global__ void __launch_bounds__(128) k_contact_fused(SceneDev d, ContactDev c,
     c.state[CS_MODE] = mode; c.state[CS_PASS] = pass; c.state[CS_IT] = it; c.state[CS_BODIES] = bodies;
     c.state[CS_COMP] = comp; c.state[CS_SRC] = src;
   }
+}
+
+// ---- the obstacle contact phase of a batch ---------------------------------
+//
+// Every part (scene) of a batch runs the state machine of k_contact_fused on
+// its own: its own detections, Jacobi iterations, convergence test, passes
+// and records.  One cooperative launch advances all of them in rounds — a
+// detection phase for the parts in detection mode, then one Jacobi iteration
+// for the parts in iteration mode — with grid-wide barriers shared by all
+// parts.  A part's sequence of operations, and so its arithmetic, is the one
+// it has alone (the items are those of k_contact_fused; a part's maximum is
+// taken over its own vertices).  Each CTA keeps an identical copy of the
+// per-part state in shared memory, updated from values read after a barrier.
+// Records: the computed iteration j of part p is record base + j of its
+// vertices (parts own disjoint rows of a record), its pass flag at
+// rec_first[(base + j) np + p].
+enum { PS_MODE = 0, PS_PASS = 1, PS_IT = 2, PS_COMP = 3, PS_SRC = 4, PS_DONE = 5, PS_RUN = 6, PS_SIZE = 7 };
+constexpr int kMaxContactParts = 1024;
+
+__device__ __forceinline__ int rec_index_part(const ContactDev& c, int comp) { return rec_index_at(c, comp); }
+
+__global__ void __launch_bounds__(128) k_contact_fused_parts(SceneDev d, ContactDev c, const double* xt, double* xk,
+                                                             const double* act_all, const int* step, double* slot,
+                                                             int* status) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ int sp[];  // PS_SIZE x np
+  __shared__ int s_flag;
+  const int np = c.np;
+  int* s_mode = sp + PS_MODE * np;
+  int* s_pass = sp + PS_PASS * np;
+  int* s_it = sp + PS_IT * np;
+  int* s_comp = sp + PS_COMP * np;
+  int* s_src = sp + PS_SRC * np;
+  int* s_done = sp + PS_DONE * np;
+  int* s_run = sp + PS_RUN * np;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
+  const bool lead = tid == 0;
+  const int ncons = d.T + d.M + d.S + d.B, nv = max(d.N, c.nc);
+  for (int i = tid; i < nv; i += nthr) contact_begin_item(d, c, i, xt, xk);
+  for (int q = tid; q < 2 * np; q += nthr) { c.pany[q] = 0; c.pe[q] = 0ull; }
+  if (lead)
+    for (int k = 0; k < CS_SIZE; ++k) c.state[k] = 0;
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
+    s_mode[p] = 0; s_pass[p] = 0; s_it[p] = 0; s_comp[p] = 0; s_src[p] = 0; s_run[p] = 0;
+    s_done[p] = (c.pf0[p + 1] == c.pf0[p]) ? 1 : 0;  // a part without obstacle faces has no phase
+  }
+  grid.sync();
+  const int cap = c.max_passes * (c.K + 2) + 2;
+  int rounds = 0;
+  for (;;) {
+    rounds += 1;
+    // detection for the parts in detection mode (k_contact_detect)
+    int* anyf = c.pany + (rounds & 1) * np;
+    for (int a = tid; a < c.nc; a += nthr) {
+      const int p = c.cpart[a];
+      if (s_mode[p] == 0 && !s_done[p] && contact_detect_item(c, a, xt, xk, status)) atomicOr(anyf + p, 1);
+    }
+    grid.sync();
+    // k_contact_ctl_detect per part
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+      if (s_done[p] || s_mode[p] != 0) continue;
+      if (((volatile int*)anyf)[p] == 0) {
+        s_done[p] = 1;
+      } else if (s_pass[p] >= c.max_passes) {
+        if (blockIdx.x == 0) cap_reached(status, kCapContactPasses);
+        s_done[p] = 1;
+      } else {
+        s_mode[p] = 1; s_it[p] = 0; s_pass[p] += 1;
+      }
+    }
+    if (lead)  // the other parity's flags: read a round ago
+      for (int p = 0; p < np; ++p) c.pany[((rounds + 1) & 1) * np + p] = 0;
+    if (threadIdx.x == 0) s_flag = 0;
+    __syncthreads();
+    for (int p = threadIdx.x; p < np; p += blockDim.x)
+      if (!s_done[p]) s_flag = 1;
+    __syncthreads();
+    if (!s_flag) break;  // every CTA reads the same state
+    // one Jacobi iteration for the parts in iteration mode (k_contact_prep ..)
+    unsigned long long* pe = c.pe + (rounds & 1) * np;
+    const int lane = threadIdx.x & 31;
+    for (int i0 = tid - lane; i0 < d.N; i0 += nthr) {  // warp-uniform trip count
+      const int i = i0 + lane;
+      const int p = i < d.N ? vpart_of(d, i) : -1;
+      const bool on = p >= 0 && s_mode[p] == 1 && !s_done[p];
+      double e = on ? contact_prep_vertex(c, i, xk) : 0.0;
+      // a warp within one part reduces first (lane 0 is in range); the
+      // per-part maximum (of doubles >= 0, as ordered bit patterns) does not
+      // depend on the order of the atomics
+      const int p0 = __shfl_sync(0xffffffffu, p, 0);
+      if (__all_sync(0xffffffffu, p == p0 || p < 0)) {
+        for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+        if (lane == 0 && on) atomicMax(pe + p, (unsigned long long)__double_as_longlong(e));
+      } else if (on) {
+        atomicMax(pe + p, (unsigned long long)__double_as_longlong(e));
+      }
+    }
+    for (int a = tid; a < c.nc; a += nthr) {
+      const int p = c.cpart[a];
+      if (s_mode[p] != 1 || s_done[p]) continue;
+      const int rk = rec_index_part(c, s_comp[p]);
+      if (rk >= 0) contact_prep_record(c, a, rk);
+    }
+    grid.sync();
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+      s_run[p] = 0;
+      if (s_done[p] || s_mode[p] != 1) continue;
+      const double m = __longlong_as_double((long long)((volatile unsigned long long*)pe)[p]);
+      s_src[p] = s_comp[p];
+      if (m < kConvergenceEps) s_mode[p] = 0;  // back to detection
+      else s_run[p] = 1;
+    }
+    if (lead)  // the other parity's maxima: read a round ago
+      for (int p = 0; p < np; ++p) c.pe[((rounds + 1) & 1) * np + p] = 0ull;
+    __syncthreads();
+    for (int t = tid; t < ncons; t += nthr)
+      if (s_run[cons_part(d, t)]) local_item(d, t, xk, act_all, step, slot);
+    grid.sync();
+    for (int i = tid; i < d.N; i += nthr) {
+      const int p = vpart_of(d, i);
+      if (s_run[p]) contact_rhs_item(d, c, i, slot, xt, xk, s_it[p] == 0, rec_index_part(c, s_comp[p]));
+    }
+    for (int p = tid; p < np; p += nthr)
+      if (s_run[p]) {
+        const int rk = rec_index_part(c, s_comp[p]);
+        if (rk >= 0) c.rec_first[(size_t)rk * np + p] = s_it[p] == 0 ? 1 : 0;
+      }
+    grid.sync();
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+      if (!s_run[p]) continue;
+      if (blockIdx.x == 0 && c.rec_on && *c.rec_on == 1 && *c.rec_base + s_comp[p] >= c.rec_cap) atomicExch(status, 6);
+      s_it[p] += 1;
+      s_comp[p] += 1;
+      if (s_it[p] >= c.K) s_mode[p] = 0;
+    }
+    __syncthreads();
+    if (rounds > cap) {  // unreachable: every part's passes and iterations are bounded
+      if (lead) cap_reached(status, kCapContactPasses);
+      break;
+    }
+  }
+  if (blockIdx.x == 0) {
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+      c.pst[PS_MODE * np + p] = s_mode[p]; c.pst[PS_PASS * np + p] = s_pass[p]; c.pst[PS_IT * np + p] = s_it[p];
+      c.pst[PS_COMP * np + p] = s_comp[p]; c.pst[PS_SRC * np + p] = s_src[p];
+    }
+    if (threadIdx.x == 0) {
+      int mp = 0, mc = 0;
+      for (int p = 0; p < np; ++p) { mp = max(mp, s_pass[p]); mc = max(mc, s_comp[p]); }
+      c.state[CS_MODE] = 0; c.state[CS_PASS] = mp; c.state[CS_IT] = 0; c.state[CS_BODIES] = rounds;
+      c.state[CS_COMP] = mc; c.state[CS_SRC] = 0;
+    }
+  }
+}
+
+// per-step record of a batch's phase: every part's source iteration (forward recording)
+__global__ void k_contact_record_parts(const int* step, ContactDev c) {
+  if (!(c.rec_on && *c.rec_on == 2)) return;
+  const int s = *step;
+  for (int p = threadIdx.x; p < c.np; p += blockDim.x) c.psrc[(size_t)s * c.np + p] = c.pst[PS_SRC * c.np + p];
 }
 
 // ---- soft-soft (self) contact ------------------------------------------------
@@ -1566,6 +1734,73 @@ __global__ void __launch_bounds__(128) k_cadj_fused(SceneDev d, ContactDev c, Co
       cadj_hs_item(d, a, i);
     }
     for (int q = tid; q < d.nseg; q += nthr) {  // k_seg_reduce
+      double sum = 0;
+      for (int k = d.seg_ptr[q]; k < d.seg_ptr[q + 1]; ++k) sum += mg[member_slot(d.M, d.seg_mus[k])];
+      gact[(size_t)st * d.nseg + q] += sum;
+    }
+    grid.sync();
+  }
+  for (int t = tid; t < d.T; t += nthr) cadj_hd_item(d, a, t, gE);
+  for (int i = tid; i < d.N; i += nthr) {  // k_cadj_to_pd
+    st3(io_a, i, ld3(a.xn1b, i));
+    st3(io_b, i, mk3(0.0, 0.0, 0.0));
+  }
+}
+
+// The reverse sweep of a batch's obstacle contact phase in one cooperative
+// launch: k_cadj_fused for every part, part p reversing its own computed
+// iterations top[p] .. 1 (its records base + j - 1, pass flags
+// rec_first[(base + j - 1) np + p]); the sweeps run side by side, iteration j
+// of every part that has one in the same round.  Same per-item code as
+// k_cadj_fused.
+__global__ void __launch_bounds__(128) k_cadj_fused_parts(SceneDev d, ContactDev c, ContactAdj a, const double* xt,
+                                                          const double* act_all, const int* step, double* slot,
+                                                          double* gE, double* gnu, double* mg, double* gact, int base,
+                                                          const int* top, double cv, double* io_a, double* io_b) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
+  const int ncons = d.T + d.M + d.S + d.B, np = c.np;
+  const size_t n3 = 3 * (size_t)d.N;
+  const int st = *step;
+  const double* act_row = act_all + (size_t)st * d.nseg;
+  for (int i = tid; i < d.N; i += nthr) {  // k_cadj_start
+    const Vec3<double> gv = ld3(io_b, i);
+    st3(a.xn1b, i, ld3(io_a, i) + cv * gv);
+    st3(a.cxtb, i, (-cv) * gv);
+    st3(a.vwcb, i, mk3(0.0, 0.0, 0.0));
+    st3(a.pb, i, mk3(0.0, 0.0, 0.0));
+    a.hdb[i] = 0.0;
+  }
+  int jmax = 0;
+  for (int p = 0; p < np; ++p) jmax = max(jmax, top[p]);
+  grid.sync();
+  for (int j = jmax; j >= 1; --j) {
+    const size_t r = (size_t)base + (j - 1);
+    const double* ori = c.rec_x + r * n3;
+    const double* prev = c.rec_prev + r * n3;
+    const int* rcnt = c.rec_cnt + r * c.nc;
+    const double* rn = c.rec_n + r * c.nc * kMaxImpactsPerVertex * 3;
+    for (int t = tid; t < ncons; t += nthr)
+      if (j <= top[cons_part(d, t)]) local_item(d, t, ori, act_all, step, slot);
+    grid.sync();
+    for (int i = tid; i < d.N; i += nthr) {
+      const int p = vpart_of(d, i);
+      if (j <= top[p]) cadj_rhs_item(d, c, a, i, slot, xt, ori, prev, c.rec_first[r * np + p], rcnt, rn);
+    }
+    grid.sync();
+    for (int t = tid; t < ncons; t += nthr)
+      if (j <= top[cons_part(d, t)]) adj_local_item(d, t, ori, a.yb, act_row, slot, gE, gnu, mg, nullptr, xt);
+    grid.sync();
+    for (int i = tid; i < d.N; i += nthr) {  // k_adj_gather, then k_cadj_hs on the same vertex
+      if (j > top[vpart_of(d, i)]) continue;
+      Vec3<double> acc = mk3(0.0, 0.0, 0.0);
+      for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
+      st3(a.orib, i, acc);
+      cadj_hs_item(d, a, i);
+    }
+    for (int q = tid; q < d.nseg; q += nthr) {  // k_seg_reduce
+      if (j > top[d.seg_part ? d.seg_part[q] : 0]) continue;
       double sum = 0;
       for (int k = d.seg_ptr[q]; k < d.seg_ptr[q + 1]; ++k) sum += mg[member_slot(d.M, d.seg_mus[k])];
       gact[(size_t)st * d.nseg + q] += sum;

@@ -228,6 +228,10 @@ struct dfem_scene {
   DBuf<double> ca_scb, ca_ptot, ca_sbp, ca_gPF, ca_gPM, ca_gmF, ca_gmM, ca_xout;  // its adjoint
   // adjoint of the contact phase: the record of one step's Jacobi iterations and the reverse sweep's buffers
   DBuf<int> crec_on, crec_first, crec_cnt;
+  // batched contact: contact vertices' parts, parts' obstacle faces, per-part phase state
+  int cnp = 0;                           // parts of a batch with contact (0: single scene)
+  DBuf<int> c_cpart, c_pf0, c_pst, c_pany, c_psrc;
+  DBuf<unsigned long long> c_pe;
   DBuf<double> crec_x, crec_prev, crec_n, ca_xn1b, ca_pb, ca_hdb, ca_cxtb, ca_vwcb, ca_yb, ca_orib;
   int crec_cap = 0;
   // forward recording of every step's contact iterations (when the steps'
@@ -959,13 +963,36 @@ static int upload_scene(dfem_scene* sc) {
                         sc->obs_f.p, sc->hdiag.p, sc->imp_cnt.p, sc->imp_face.p, sc->imp_n.p, sc->xn1.p, sc->xold.p,
                         sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p, sc->crec_on.p, 0, nullptr, nullptr,
                         nullptr, nullptr, nullptr, sc->status.p, sc->crec_base.p, nullptr};
-    RC(build_obstacle_grid(sc));
+    if (s.nparts > 1) {  // a batch: per-part contact state, no broad phase
+      const int np = s.nparts;
+      if (np > kMaxContactParts)
+        return fail(DFEM_ERR_UNSUPPORTED, "batch: obstacle contact needs at most " + std::to_string(kMaxContactParts) + " scenes");
+      sc->cnp = np;
+      CK(sc->c_cpart.upload(s.cpart));
+      CK(sc->c_pf0.upload(s.pobs_f0));
+      CK(sc->c_pst.alloc((size_t)PS_SIZE * np));
+      CK(cudaMemset(sc->c_pst.p, 0, sizeof(int) * PS_SIZE * np));
+      CK(sc->c_pany.alloc(2 * (size_t)np));
+      CK(sc->c_pe.alloc(2 * (size_t)np));
+      ContactDev& c = sc->cd;
+      c.np = np; c.cpart = sc->c_cpart.p; c.pf0 = sc->c_pf0.p; c.pst = sc->c_pst.p;
+      c.pany = sc->c_pany.p; c.pe = sc->c_pe.p;
+    } else {
+      RC(build_obstacle_grid(sc));
+    }
     if (!sc->self_contact) {  // the fused phase: every CTA resident (cooperative launch)
       int nsm = 1, occ = 0, occ_a = 0, coop = 0;
       CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, sc->device));
       CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, sc->device));
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_contact_fused, 128, 0));
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_cadj_fused, 128, 0));
+      if (sc->cnp > 0) {
+        const size_t shm = sizeof(int) * PS_SIZE * (size_t)sc->cnp;
+        CK(raise_smem_limit((const void*)k_contact_fused_parts, shm));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_contact_fused_parts, 128, shm));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_cadj_fused_parts, 128, 0));
+      } else {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_contact_fused, 128, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_a, k_cadj_fused, 128, 0));
+      }
       const int ncons = s.T + s.M + s.S + s.B;
       const int want = std::max(1, (std::max(ncons, s.N) + 127) / 128);
       sc->fused_grid = std::min(nsm * occ, want);
@@ -973,6 +1000,8 @@ static int upload_scene(dfem_scene* sc) {
       sc->fused_ok = coop != 0 && occ > 0 && occ_a > 0;
       if (sc->fused_ok) CK(sc->fpartial.alloc(std::max(1, sc->fused_grid)));
     }
+    if (sc->cnp > 0 && !sc->fused_ok)
+      return fail(DFEM_ERR_UNSUPPORTED, "batch: obstacle contact needs the cooperative contact phase on this device");
     if (sc->self_contact) {
       const int ncf = (int)s.cfaces.size() / 3;
       CK(sc->s_cfaces.upload(s.cfaces));
@@ -1137,6 +1166,10 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   CK(sc->hist.alloc(all ? rec * cap : rec));
   sc->hist_step = all ? (long long)rec : 0;
   CK(cudaMemset(sc->cpasses.p, 0, sizeof(int) * 2 * (size_t)cap));
+  if (sc->has_contact && sc->cnp > 0) {
+    CK(sc->c_psrc.alloc((size_t)cap * sc->cnp));
+    sc->cd.psrc = sc->c_psrc.p;
+  }
   if (sc->has_contact) {
     CK(sc->crec_meta.alloc(4 * (size_t)cap));
     sc->cd.rec_meta = sc->crec_meta.p;
@@ -1429,6 +1462,11 @@ static cudaError_t launch_contact_fused(dfem_scene* sc, cudaStream_t st) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  if (sc->cnp > 0) {
+    cfg.dynamicSmemBytes = sizeof(int) * PS_SIZE * (size_t)sc->cnp;
+    return cudaLaunchKernelEx(&cfg, k_contact_fused_parts, sc->sd, sc->cd, (const double*)sc->xt.p, sc->xk.p,
+                              (const double*)sc->act_all.p, (const int*)sc->step.p, sc->slot.p, sc->status.p);
+  }
   return cudaLaunchKernelEx(&cfg, k_contact_fused, sc->sd, sc->cd, (const double*)sc->xt.p, sc->xk.p,
                             (const double*)sc->act_all.p, (const int*)sc->step.p, sc->slot.p, sc->fpartial.p,
                             sc->status.p);
@@ -1438,6 +1476,7 @@ static void step_post(dfem_scene* sc, cudaStream_t st) {
   const int nb = sc->nblk_v;
   if (fused_contact(sc)) launch_contact_fused(sc, st);  // a refused launch surfaces through cudaGetLastError
   if (sc->has_contact) k_contact_record<<<1, 1, 0, st>>>(sc->step.p, sc->cstate.p, sc->cpasses.p, sc->cd);
+  if (sc->has_contact && sc->cnp > 0) k_contact_record_parts<<<1, 256, 0, st>>>(sc->step.p, sc->cd);
   if (sc->skel_on) k_skel_end<<<1, 32, 0, st>>>(sc->skd);
   k_step_end<<<nb, 128, 0, st>>>(sc->sd, sc->step.p, sc->xt.p, sc->vt.p, sc->xk.p, sc->traj.p, sc->to_user.p,
                                  sc->write_traj.p);
@@ -1603,7 +1642,8 @@ static int ensure_contact_record(dfem_scene* sc, int cap, int keep = 0) {
   DBuf<int> first, cnt;
   CK(x.alloc(n3 * cap));
   CK(prev.alloc(n3 * cap));
-  CK(first.alloc(cap));
+  const size_t fw = std::max(1, sc->cnp);  // pass flags per record: one per part in a batch
+  CK(first.alloc(fw * cap));
   CK(cnt.alloc(nc * cap));
   CK(nrm.alloc(nn * cap));
   DBuf<int> rsi;
@@ -1620,7 +1660,7 @@ static int ensure_contact_record(dfem_scene* sc, int cap, int keep = 0) {
   if (keep > 0) {
     CK(cudaMemcpyAsync(x.p, sc->crec_x.p, sizeof(double) * n3 * keep, cudaMemcpyDeviceToDevice, sc->stream));
     CK(cudaMemcpyAsync(prev.p, sc->crec_prev.p, sizeof(double) * n3 * keep, cudaMemcpyDeviceToDevice, sc->stream));
-    CK(cudaMemcpyAsync(first.p, sc->crec_first.p, sizeof(int) * keep, cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaMemcpyAsync(first.p, sc->crec_first.p, sizeof(int) * fw * keep, cudaMemcpyDeviceToDevice, sc->stream));
     CK(cudaMemcpyAsync(cnt.p, sc->crec_cnt.p, sizeof(int) * nc * keep, cudaMemcpyDeviceToDevice, sc->stream));
     CK(cudaMemcpyAsync(nrm.p, sc->crec_n.p, sizeof(double) * nn * keep, cudaMemcpyDeviceToDevice, sc->stream));
     CK(cudaStreamSynchronize(sc->stream));
@@ -1688,6 +1728,24 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
     src = meta[CS_SRC];
   }
   if (base + comp > sc->crec_cap) return fail(DFEM_ERR_CAP, "contact record too small for the recomputed step");
+  if (sc->cnp > 0) {  // a batch: every part's reverse sweep in one cooperative launch
+    const ContactAdj a = make_cadj(sc);
+    const int* top = recorded ? sc->c_psrc.p + (size_t)st * sc->cnp : sc->c_pst.p + (size_t)PS_SRC * sc->cnp;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(sc->cadj_grid);
+    cfg.blockDim = dim3(128);
+    cfg.stream = sc->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, k_cadj_fused_parts, sc->sd, sc->cd, a, xt, (const double*)sc->act_all.p,
+                          (const int*)sc->step.p, sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p, sc->gact.p, base, top,
+                          s.damping / s.h, sc->io_a.p, sc->io_b.p));
+    sc->launches += 1;
+    return DFEM_OK;
+  }
   if (!sc->self_contact && fused_contact(sc)) {  // the whole reverse sweep in one cooperative launch
     const ContactAdj a = make_cadj(sc);
     cudaLaunchConfig_t cfg = {};
@@ -2644,6 +2702,8 @@ int dfem_set_option(dfem_scene* sc, int32_t which, int64_t value) {
   switch (which) {
     case DFEM_OPTION_FUSED_CONTACT:
       if (value != 0 && value != 1) return fail(DFEM_ERR_INVALID, "value must be 0 or 1");
+      if (value == 0 && sc->cnp > 0)
+        return fail(DFEM_ERR_UNSUPPORTED, "a batch's contact phase runs only as the cooperative launch");
       sc->fused_on = value != 0;
       break;
     default:

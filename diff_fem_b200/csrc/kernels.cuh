@@ -216,6 +216,16 @@ struct ContactDev {
   // [remembered self forces before the call (3 nc), g_n (3 ncf)]
   int* rec_si;
   double* rec_sd;
+  // batches (np > 1, obstacle contact only): the part of each contact vertex,
+  // each part's obstacle faces [pf0[p], pf0[p+1]), and the phase's per-part
+  // state; the broad phase is off (a part's faces are tested in order)
+  int np;
+  const int* cpart;       // nc
+  const int* pf0;         // np + 1
+  int* pst;               // np x PS_SIZE (contact_kernels.cuh)
+  unsigned long long* pe; // 2 x np: per-part max-norm change of ori_x (bits of a double >= 0), two parities
+  int* pany;              // 2 x np: per-part detection hit flags, two parities
+  int* psrc;              // per step x np: each part's source iteration (forward recording)
 };
 __host__ __device__ inline size_t self_rec_si_stride(int nc, int ncf) { return 3 * (size_t)nc + 2 * (size_t)ncf + 3; }
 __host__ __device__ inline size_t self_rec_sd_stride(int nc, int ncf) { return 3 * (size_t)nc + 3 * (size_t)ncf; }

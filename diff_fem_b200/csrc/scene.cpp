@@ -439,7 +439,6 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
     REQ(p.h == a.h && p.damping == a.damping && p.g[0] == a.g[0] && p.g[1] == a.g[1] && p.g[2] == a.g[2] &&
             p.K == a.K && p.precision == a.precision && p.checkpoint_every == a.checkpoint_every,
         "batch: scenes must share time_step, damping, gravity, max_iterations, precision and checkpoint_every");
-    REQ(!(p.collide && !p.cverts.empty() && !p.obs_f.empty()), "batch: obstacle contact is supported for single scenes only");
     REQ(!p.self_collide, "batch: soft-soft contact is supported for single scenes only");
     REQ(p.L == 0, "batch: skeleton links are supported for single scenes only");
     REQ(p.nparts == 1, "batch: parts must be single scenes");
@@ -452,7 +451,17 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
   u = HostScene();
   u.h = a.h; u.damping = a.damping; u.g[0] = a.g[0]; u.g[1] = a.g[1]; u.g[2] = a.g[2];
   u.K = a.K; u.precision = a.precision; u.checkpoint_every = a.checkpoint_every;
-  u.collide = false;
+  // obstacle contact: every part keeps its own contact vertices and obstacle
+  // faces; the phase's parameters are shared
+  auto contact_part = [](const HostScene& p) { return p.collide && !p.cverts.empty() && !p.obs_f.empty(); };
+  const HostScene* c0 = nullptr;
+  for (const HostScene& p : P)
+    if (contact_part(p)) {
+      if (!c0) c0 = &p;
+      REQ(p.alpha == c0->alpha && p.mu_obs == c0->mu_obs, "batch: contact scenes must share alpha and the obstacle friction");
+    }
+  u.collide = c0 != nullptr;
+  if (c0) { u.alpha = c0->alpha; u.mu_obs = c0->mu_obs; u.pobs_f0 = {0}; }
   u.underwater = false;
   u.nparts = (int)P.size();
   u.part_v0 = {0}; u.part_t0 = {0}; u.part_seg0 = {0};
@@ -505,6 +514,15 @@ bool merge_parts(const std::vector<HostScene>& P, HostScene& u, std::string& err
     if (any_channel) {
       if (p.sch.empty()) u.sch.insert(u.sch.end(), p.S, -1);
       else for (int c : p.sch) u.sch.push_back(c < 0 ? -1 : c + segoff);
+    }
+    if (c0) {
+      if (contact_part(p)) {
+        const int ov = (int)u.obs_x.size() / 3;
+        for (int v : p.cverts) { u.cverts.push_back(v + voff); u.cpart.push_back((int)q); }
+        cat(u.obs_x, p.obs_x);
+        cat_off(u.obs_f, p.obs_f, ov);
+      }
+      u.pobs_f0.push_back((int)u.obs_f.size() / 3);
     }
     voff += p.N; moff += p.M; soff += p.S; segoff += p.nseg; slotoff += p.nslots; bvoff += (int)p.bv.size();
     snoff += G.nsuper; rsegoff += (int)G.rseg_pos.size();

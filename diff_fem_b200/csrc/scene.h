@@ -57,6 +57,9 @@ struct HostScene {
   std::vector<int> cverts;
   std::vector<double> obs_x;
   std::vector<int> obs_f;
+  // batches: the part of each contact vertex, and each part's obstacle faces
+  // [pobs_f0[p], pobs_f0[p+1]) (empty for a single scene)
+  std::vector<int> cpart, pobs_f0;
   // soft-soft (self) contact: soft faces as contact indices (3 each), each
   // contact vertex's soft faces ascending (CSR), and whether it lies on one
   bool self_collide = false;

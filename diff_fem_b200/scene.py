@@ -508,14 +508,15 @@ def muscle_star(refine: int = 2, chains_per_arm: int = 8, seg_per_chain: int = 6
 
 
 def uneven_batch(n_scenes: int = 256, seed: int = 7, t_lo: float = 1e3, t_hi: float = 5e4,
-                 precision: int = DFEM_PREC_FP64, max_iterations: int = 15):
+                 precision: int = DFEM_PREC_FP64, max_iterations: int = 15, ground: bool = True):
     """Batch of independent scenes of uneven size: tet counts log-uniform in
     [t_lo, t_hi] from `seed`, alternating beams (cube-grid bars as the
     cantilever / inverse-stiffness scenes, cross-section ny = nz, length 5x the
-    width, x = 0 face pinned) and muscle stars without ground (arm length and
-    refinement chosen to approach the target count).  Per-scene log-uniform
-    moduli in [1e4, 1e6] Pa.  All share h = 1/60, 15 iterations, damping 0.9999
-    and gravity.  Returns (descs, target tet counts)."""
+    width, x = 0 face pinned) and muscle stars, each on its own ground
+    obstacle with `ground` (arm length and refinement chosen to approach the
+    target count).  Per-scene log-uniform moduli in [1e4, 1e6] Pa.  All share
+    h = 1/60, 15 iterations, damping 0.9999 and gravity.  Returns (descs,
+    target tet counts)."""
     import dataclasses
     rng = np.random.default_rng(seed)
     targets = np.exp(rng.uniform(np.log(t_lo), np.log(t_hi), size=n_scenes))
@@ -537,7 +538,7 @@ def uneven_batch(n_scenes: int = 256, seed: int = 7, t_lo: float = 1e3, t_hi: fl
         else:
             refine = 1 if tgt < 2460 * 1.7 else (2 if tgt < 9840 * 1.7 else 3)
             if refine not in stars:
-                stars[refine] = muscle_star(refine=refine, chains_per_arm=min(8, 4 * refine), ground=False,
+                stars[refine] = muscle_star(refine=refine, chains_per_arm=min(8, 4 * refine), ground=ground,
                                             precision=precision)
             base = stars[refine]
             d = dataclasses.replace(base, youngs=log_uniform_moduli(base.n_tets, 1000 + q),

@@ -155,7 +155,7 @@ def test_large_batch_launch_classes_match_scenes(form):
     warp, small and large CTAs), the split and tail-selected solve forms; each
     scene alone runs its own factor's schedule and form.  Neither moves any
     arithmetic: bit-identical."""
-    descs, _ = S.uneven_batch(n_scenes=32, t_hi=1e4, precision=_capi.DFEM_PREC_FP64)
+    descs, _ = S.uneven_batch(n_scenes=32, t_hi=1e4, precision=_capi.DFEM_PREC_FP64, ground=False)
     b = Scene.batch(descs)
     assert b.info()["n_supernodes"] > 2048
     info = b.solve_mode(form)
@@ -181,3 +181,60 @@ def test_large_batch_launch_classes_match_scenes(form):
         assert np.array_equal(gb["E"][to[p]:to[p + 1]], gs["E"]), p
         s.close()
     b.close()
+
+
+def test_batch_with_obstacle_contact_matches_scenes():
+    """Obstacle contact inside a batch: boxes dropped on their own grounds (one
+    with friction clamping, one landing faster) and a muscle beam without
+    contact.  The contact parts' trajectories, contact passes, iteration
+    counts and gradients are the scene's own bit for bit (each part runs its
+    own detection passes, Jacobi iterations and convergence test in the
+    batched cooperative phase); the part without contact matches to rounding
+    (its adjoint passes through the phase's cotangent bookkeeping)."""
+    a = S.drop_box(mu=0.3)
+    b_ = S.drop_box(nx=3, ny=2, nz=3, height=0.03, v0=-1.5, mu=0.3)
+    dry = S.muscle_beam()
+    descs = harmonise([a, b_, dry])
+    vels = [a.initial_velocity, b_.initial_velocity, np.zeros(3 * dry.n_vertices)]
+    n = 8
+    bt = Scene.batch(descs)
+    vo, to, so = bt.offsets["vertices"], bt.offsets["tets"], bt.offsets["segments"]
+    nseg = [d.n_segments for d in descs]
+    rng = np.random.default_rng(17)
+    acts = [rng.uniform(0, 1, (n, k)) for k in nseg]
+    x = np.concatenate([d.x0.reshape(-1) for d in descs])
+    v = np.concatenate(vels)
+    xb, vb, tb = bt.forward(x, v, n_steps=n, act=np.concatenate(acts, axis=1), traj=True)
+    itb = bt.iterations(n)
+    passes_b = bt.contact_passes(n)
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    gb = bt.backward(gx, gv)
+    passes = []
+    for p, d in enumerate(descs):
+        s = Scene(d)
+        xs, vs, ts = s.forward(d.x0.reshape(-1), vels[p], n_steps=n, act=acts[p] if nseg[p] else None, traj=True)
+        assert np.array_equal(s.iterations(n), itb[:, p]), p
+        assert np.array_equal(split(xb, vo)[p], xs), p
+        assert np.array_equal(split(vb, vo)[p], vs), p
+        assert np.array_equal(tb[:, 3 * vo[p]: 3 * vo[p + 1]], ts), p
+        gs = s.backward(split(gx, vo)[p], split(gv, vo)[p])
+        contact = p < 2
+        if contact:
+            passes.append(s.contact_passes(n))
+            assert passes[-1].sum() > 0, p
+        for k in ("x", "v"):
+            if contact:
+                assert np.array_equal(split(gb[k], vo)[p], gs[k]), (p, k)
+            else:
+                assert np.allclose(split(gb[k], vo)[p], gs[k], rtol=1e-12, atol=1e-12 * np.abs(gs[k]).max()), (p, k)
+        for k in ("E", "nu"):
+            if contact:
+                assert np.array_equal(gb[k][to[p]:to[p + 1]], gs[k]), (p, k)
+            else:
+                assert np.allclose(gb[k][to[p]:to[p + 1]], gs[k], rtol=1e-12, atol=1e-12 * np.abs(gs[k]).max()), (p, k)
+        if nseg[p]:
+            assert np.allclose(gb["act"][:, so[p]:so[p + 1]], gs["act"], rtol=1e-12,
+                               atol=1e-12 * np.abs(gs["act"]).max()), p
+        s.close()
+    assert np.array_equal(passes_b, np.maximum(passes[0], passes[1]))  # a batch reports its parts' most passes
+    bt.close()

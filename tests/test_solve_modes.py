@@ -67,7 +67,7 @@ def test_batch_tail_selection_matches_fixed_form():
     """After an autotune a batch may switch each iteration's solve to the
     persistent form once few parts are left; the result is that of a fixed form."""
     from diff_fem_b200 import _capi
-    descs, _ = S.uneven_batch(n_scenes=24, t_hi=8e3, precision=_capi.DFEM_PREC_FP64)
+    descs, _ = S.uneven_batch(n_scenes=24, t_hi=8e3, precision=_capi.DFEM_PREC_FP64, ground=False)
     sc = Scene.batch(descs)
     act = np.random.default_rng(3).uniform(0, 1, (3, sc.nseg))
     info = sc.solve_mode("auto")
