@@ -164,6 +164,107 @@ __device__ __forceinline__ void res_backward(const ResDev& d, const ResItem& in,
   __syncthreads();
 }
 
+// Small supernodes (w <= 32 columns, r <= 64 rows below) run one per warp,
+// with the column values in registers (lane c holds column c, lanes hold rows
+// lane and lane + 32) and shuffles instead of shared scratch and block
+// barriers; every sum keeps the order of res_forward / res_backward (the
+// products in increasing k or column, the backward's lane sums over rows a =
+// lane, lane + 32 and the same butterfly), so the results are bit-identical.
+__device__ __forceinline__ bool res_warp_item(const ResItem& in) { return in.w <= 32 && in.r <= 64; }
+
+__device__ __forceinline__ void res_forward_warp(const ResDev& d, const ResItem& in, double* sh) {
+  const int w = in.w, r = in.r, lane = threadIdx.x & 31;
+  const double* D = sh + in.dofs;
+  const double* L = sh + in.lofs;
+  const int* prow = reinterpret_cast<const int*>(sh + in.pofs);
+  const uint32_t* push = reinterpret_cast<const uint32_t*>(sh + in.tofs);
+  const double* q = sh + in.qofs;
+  double* ysh = sh + in.yofs;
+  double t0 = 0, t1 = 0, t2 = 0;
+  if (lane < w) {
+    t0 = ysh[3 * lane]; t1 = ysh[3 * lane + 1]; t2 = ysh[3 * lane + 2];
+    for (int k = prow[lane]; k < prow[lane + 1]; ++k) { t0 -= q[3 * k]; t1 -= q[3 * k + 1]; t2 -= q[3 * k + 2]; }
+  }
+  double y0 = 0, y1 = 0, y2 = 0;
+  const double* Dc = D + (size_t)lane * (lane + 1) / 2;
+  for (int k = 0; k < w; ++k) {
+    const double s0 = __shfl_sync(0xffffffffu, t0, k), s1 = __shfl_sync(0xffffffffu, t1, k),
+                 s2 = __shfl_sync(0xffffffffu, t2, k);
+    if (lane < w && k <= lane) {
+      const double dv = Dc[k];
+      y0 += dv * s0; y1 += dv * s1; y2 += dv * s2;
+    }
+  }
+  if (lane < w) { ysh[3 * lane] = y0; ysh[3 * lane + 1] = y1; ysh[3 * lane + 2] = y2; }
+  for (int a0r = 0; a0r < r; a0r += 32) {  // warp-uniform
+    const int a = a0r + lane;
+    double b0 = 0, b1 = 0, b2 = 0;
+    for (int c = 0; c < w; ++c) {
+      const double u0 = __shfl_sync(0xffffffffu, y0, c), u1 = __shfl_sync(0xffffffffu, y1, c),
+                   u2 = __shfl_sync(0xffffffffu, y2, c);
+      if (a < r) {
+        const double l = L[(size_t)c * r + a];
+        b0 += l * u0; b1 += l * u1; b2 += l * u2;
+      }
+    }
+    if (a < r) {
+      const uint32_t dst = push[a];
+      if (res_addr_ok(d, dst, in.s, 8)) {
+        const uint32_t o = cluster_map(sh + (dst & 0xFFFFFFu), dst >> 24);
+        st_cluster_f64(o, b0); st_cluster_f64(o + 8, b1); st_cluster_f64(o + 16, b2);
+      }
+    }
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void res_backward_warp(const ResDev& d, const ResItem& in, double* sh) {
+  const int w = in.w, r = in.r, lane = threadIdx.x & 31;
+  const double* D = sh + in.dofs;
+  const double* L = sh + in.lofs;
+  const uint32_t* pull = reinterpret_cast<const uint32_t*>(sh + in.tofs) + r;
+  double* ysh = sh + in.yofs;
+  double xa[2][3] = {{0, 0, 0}, {0, 0, 0}};  // rows lane, lane + 32
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    const int a = lane + 32 * m;
+    if (a < r) {
+      const uint32_t src = pull[a];
+      if (res_addr_ok(d, src, in.s, 9)) {
+        const uint32_t o = cluster_map(sh + (src & 0xFFFFFFu), src >> 24);
+        xa[m][0] = ld_cluster_f64(o); xa[m][1] = ld_cluster_f64(o + 8); xa[m][2] = ld_cluster_f64(o + 16);
+      }
+    }
+  }
+  double t0 = 0, t1 = 0, t2 = 0;
+  if (lane < w) { t0 = ysh[3 * lane]; t1 = ysh[3 * lane + 1]; t2 = ysh[3 * lane + 2]; }
+  for (int c = 0; c < w; ++c) {
+    const double* Lc = L + (size_t)c * r;
+    double a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+      const int a = lane + 32 * m;
+      if (a < r) {
+        const double l = Lc[a];
+        a0 += l * xa[m][0]; a1 += l * xa[m][1]; a2 += l * xa[m][2];
+      }
+    }
+    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+    if (lane == c) { t0 -= a0; t1 -= a1; t2 -= a2; }
+  }
+  double y0 = 0, y1 = 0, y2 = 0;
+  for (int k = 0; k < w; ++k) {
+    const double s0 = __shfl_sync(0xffffffffu, t0, k), s1 = __shfl_sync(0xffffffffu, t1, k),
+                 s2 = __shfl_sync(0xffffffffu, t2, k);
+    if (lane < w && k >= lane) {
+      const double dv = D[(size_t)k * (k + 1) / 2 + lane];
+      y0 += dv * s0; y1 += dv * s1; y2 += dv * s2;
+    }
+  }
+  if (lane < w) { ysh[3 * lane] = y0; ysh[3 * lane + 1] = y1; ysh[3 * lane + 2] = y2; }
+  __syncwarp();
+}
+
 // Element j of the CTA's solution regions (j < 3 sum(w)): its item and the
 // offset in it, from the prefix sums cum[] (few items per CTA: linear scan).
 __device__ __forceinline__ int res_item_of(const int* cum, int n, int j) {
@@ -216,14 +317,27 @@ __global__ void __launch_bounds__(512, 1) k_solve_resident(ResDev d, Gate gate, 
   if (!ok && threadIdx.x == 0) res_fail(d, -1, 7);
   double* t = sh + (ok ? hdr[3] : 0);
   double* xr = sh + (ok ? hdr[4] : 0);
+  // a level's supernodes are independent: its small ones one per warp, side
+  // by side, then its large ones by the whole CTA
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int l = 0; l < d.nlev; ++l) {
-    if (ok)
-      for (int it = sched[l]; it < sched[l + 1]; ++it) res_forward(d, items[it], sh, t);
+    if (ok) {
+      for (int it = sched[l], e = 0; it < sched[l + 1]; ++it)
+        if (res_warp_item(items[it]) && (e++ % nw) == warp) res_forward_warp(d, items[it], sh);
+      __syncthreads();
+      for (int it = sched[l]; it < sched[l + 1]; ++it)
+        if (!res_warp_item(items[it])) res_forward(d, items[it], sh, t);
+    }
     cluster_sync_all();  // the level's contributions have landed in their owners' inboxes
   }
   for (int l = d.nlev - 1; l >= 0; --l) {
-    if (ok)
-      for (int it = sched[l]; it < sched[l + 1]; ++it) res_backward(d, items[it], sh, t, xr);
+    if (ok) {
+      for (int it = sched[l], e = 0; it < sched[l + 1]; ++it)
+        if (res_warp_item(items[it]) && (e++ % nw) == warp) res_backward_warp(d, items[it], sh);
+      __syncthreads();
+      for (int it = sched[l]; it < sched[l + 1]; ++it)
+        if (!res_warp_item(items[it])) res_backward(d, items[it], sh, t, xr);
+    }
     cluster_sync_all();  // the level's solution values are final; no CTA reads another's after the last one
   }
   if (ok) {

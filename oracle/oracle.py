@@ -84,8 +84,11 @@ class OracleScene:
         self._steps = 0
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().orc_destroy(self.h)
+        if getattr(self, "h", None) and lib is not None:  # module globals may be gone at interpreter exit
+            try:
+                lib().orc_destroy(self.h)
+            except Exception:
+                pass
             self.h = None
 
     @property
