@@ -177,6 +177,7 @@ class Body:
     seg_offset: int = 0
     n_pneumatic: int = 0      # pneumatic springs ("Volume Verts"), one activation channel each
     pneumatic_offset: int = 0  # first channel of the pneumatic springs
+    n_segments: int = 0       # muscle segments (activation channels from seg_offset)
     n_links: int = 0          # skeleton links ("Bones"); link torques on channels
     torque_offset: int = 0    # first channel of the joint torques (links 1..n_links-1)
 
@@ -234,6 +235,7 @@ def load_scene(config_path: str, total_step: int = 1, data_root: Optional[str] =
             a, b, c, d, nseg = muscle_constraints_from_fibres(v, t, fibres, float(obj.get("Muscle Stiffness", 5e5)))
             mt.append(a + off); mf.append(b); mk.append(c); ms.append(d + nseg_total)
             body.n_muscles = len(fibres)
+            body.n_segments = nseg
             nseg_total += nseg
         if "Volume Verts" in obj:
             # Dfobj.h:231-251: each polyline of "Volume Verts" becomes one

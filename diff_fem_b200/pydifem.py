@@ -157,8 +157,8 @@ class Environment:
     def segment_activations(self) -> np.ndarray:
         out = np.zeros(self.desc.n_segments)
         for o in self.mDfobjs:
-            if o.n_muscles:
-                lv = o.levels.reshape(-1)
+            if o.n_muscles:  # the flattened level table over the body's segments (truncated or zero-padded)
+                lv = o.levels.reshape(-1)[: o.body.n_segments]
                 out[o.body.seg_offset:o.body.seg_offset + lv.size] = lv
             if o.body.n_pneumatic:
                 out[o.body.pneumatic_offset:o.body.pneumatic_offset + o.body.n_pneumatic] = o.pneumatic_levels
@@ -258,7 +258,7 @@ def backward_act(q, qd, jq, jqd, tau, dldq, dldqd, dldjq, dldjqd, env: Environme
 
 def _channels_t(env: Environment, tau_t, is_act: bool):
     """The step's activation channels as a torch vector, differentiable in
-    tau through the actuator front-ends (types 2 and 3)."""
+    tau through the actuator front-ends (types 1, 2 and 3)."""
     out = torch.as_tensor(env.segment_activations()).clone()
     k = 0
     for o in env.mDfobjs:
@@ -268,6 +268,7 @@ def _channels_t(env: Environment, tau_t, is_act: bool):
             out = torch.cat([out[:b.torque_offset], tau_t[k:k + n], out[b.torque_offset + n:]])
         elif is_act and n and b.actuator_type == 2:
             lv = o.activation_from_actions(tau_t[k:k + n], env.mPhase, torch.as_tensor(o.levels)).reshape(-1)
+            lv = lv[: b.n_segments]
             out = torch.cat([out[:b.seg_offset], lv, out[b.seg_offset + lv.numel():]])
         elif is_act and n and b.actuator_type == 3:
             out = torch.cat([out[:b.pneumatic_offset], tau_t[k:k + n], out[b.pneumatic_offset + n:]])
