@@ -86,12 +86,16 @@ __device__ __forceinline__ Mat3<double> deformation(const double G[4][3], const 
 // adjoint local step of the 256-scene batch: 1.12 ms at 174 registers, 0.85 ms
 // at 128 with spills to L1; the mixed force step, then with an FP32 tail after
 // its SVD, 0.315 -> 0.282 ms, the FP64 local step 0.411 -> 0.383 ms; the
-// mixed force step with its FP64 tail takes 0.311 ms at 96 registers).
+// mixed force step with its FP64 tail takes 0.311 ms at 96 registers).  With
+// the adjoint's projection and VJP sharing one SVD, three CTAs (168 registers,
+// 40 bytes of spills) beat four (128, 360 bytes of spills) and two (255):
+// 32-scene batch 104.6 / 107.1 / 135.3 us, inverse-stiffness beam 13.6 /
+// 14.5 / 13.6 us per launch.
 #ifndef DFEM_FORCE_MIN_BLOCKS
 #define DFEM_FORCE_MIN_BLOCKS 5
 #endif
 #ifndef DFEM_ADJ_MIN_BLOCKS
-#define DFEM_ADJ_MIN_BLOCKS 4
+#define DFEM_ADJ_MIN_BLOCKS 3
 #endif
 #ifndef DFEM_LOCAL_MIN_BLOCKS
 #define DFEM_LOCAL_MIN_BLOCKS 5

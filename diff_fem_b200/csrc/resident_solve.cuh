@@ -171,6 +171,7 @@ __device__ __forceinline__ void res_backward(const ResDev& d, const ResItem& in,
 // products in increasing k or column, the backward's lane sums over rows a =
 // lane, lane + 32 and the same butterfly), so the results are bit-identical.
 __device__ __forceinline__ bool res_warp_item(const ResItem& in) { return in.w <= 32 && in.r <= 64; }
+constexpr int kResWarpMin = 8;  // small items of a CTA at one level from which they run one per warp
 
 __device__ __forceinline__ void res_forward_warp(const ResDev& d, const ResItem& in, double* sh) {
   const int w = in.w, r = in.r, lane = threadIdx.x & 31;
@@ -317,26 +318,38 @@ __global__ void __launch_bounds__(512, 1) k_solve_resident(ResDev d, Gate gate, 
   if (!ok && threadIdx.x == 0) res_fail(d, -1, 7);
   double* t = sh + (ok ? hdr[3] : 0);
   double* xr = sh + (ok ? hdr[4] : 0);
-  // a level's supernodes are independent: its small ones one per warp, side
-  // by side, then its large ones by the whole CTA
+  // a level's supernodes are independent: when the CTA holds at least
+  // kResWarpMin small ones at a level they run one per warp, side by side
+  // (then the large ones by the whole CTA); with fewer, every item runs on
+  // the whole CTA, whose shorter per-item latency then sets the level's pace
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int l = 0; l < d.nlev; ++l) {
     if (ok) {
-      for (int it = sched[l], e = 0; it < sched[l + 1]; ++it)
-        if (res_warp_item(items[it]) && (e++ % nw) == warp) res_forward_warp(d, items[it], sh);
-      __syncthreads();
+      int ne = 0;
+      for (int it = sched[l]; it < sched[l + 1]; ++it) ne += res_warp_item(items[it]) ? 1 : 0;
+      const bool by_warp = ne >= kResWarpMin;
+      if (by_warp) {
+        for (int it = sched[l], e = 0; it < sched[l + 1]; ++it)
+          if (res_warp_item(items[it]) && (e++ % nw) == warp) res_forward_warp(d, items[it], sh);
+        __syncthreads();
+      }
       for (int it = sched[l]; it < sched[l + 1]; ++it)
-        if (!res_warp_item(items[it])) res_forward(d, items[it], sh, t);
+        if (!by_warp || !res_warp_item(items[it])) res_forward(d, items[it], sh, t);
     }
     cluster_sync_all();  // the level's contributions have landed in their owners' inboxes
   }
   for (int l = d.nlev - 1; l >= 0; --l) {
     if (ok) {
-      for (int it = sched[l], e = 0; it < sched[l + 1]; ++it)
-        if (res_warp_item(items[it]) && (e++ % nw) == warp) res_backward_warp(d, items[it], sh);
-      __syncthreads();
+      int ne = 0;
+      for (int it = sched[l]; it < sched[l + 1]; ++it) ne += res_warp_item(items[it]) ? 1 : 0;
+      const bool by_warp = ne >= kResWarpMin;
+      if (by_warp) {
+        for (int it = sched[l], e = 0; it < sched[l + 1]; ++it)
+          if (res_warp_item(items[it]) && (e++ % nw) == warp) res_backward_warp(d, items[it], sh);
+        __syncthreads();
+      }
       for (int it = sched[l]; it < sched[l + 1]; ++it)
-        if (!res_warp_item(items[it])) res_backward(d, items[it], sh, t, xr);
+        if (!by_warp || !res_warp_item(items[it])) res_backward(d, items[it], sh, t, xr);
     }
     cluster_sync_all();  // the level's solution values are final; no CTA reads another's after the last one
   }

@@ -196,3 +196,50 @@ def test_save_obj_from_device_and_host_states(env, tmp_path):
     assert a == b and a.startswith("v ") and "\nf " in a
     X = xn.reshape(-1, 3)
     assert a.splitlines()[0] == "v %06f %06f %06f" % tuple(X[0])
+
+
+def test_demo_sus_loop_through_sim_all_matches_oracle():
+    """python/demo_sus.py's optimisation loop on the suspended bridge
+    (tests/golden/ref_scenes/bridgesus.npz): tau = t_scale * max(tau, 0.01)
+    (forward_all uses tau[0] = E and tau[1] = nu on every tet), sim_all over
+    the scene's 10 steps, loss = |mean(q) - target|, loss.backward(), an Adam
+    step; dL/dtau and dL/dx0 against the oracle's adjoint of the same run,
+    for two optimiser steps."""
+    import torch
+    from diff_fem_b200 import loader, pydifem as pd, scene as S
+    from diff_fem_b200.api_diff import sim_all
+    from oracle import oracle as O
+    d = S.load_npz(os.path.join(GOLDEN, "ref_scenes", "bridgesus.npz"))
+    L = loader.LoadedScene(desc=d, bodies=[loader.Body("mesh", 0, d.n_vertices, True)], total_step=10)
+    env = pd.Environment(L)
+    init_x = torch.tensor(env.mSoftWorld.mX, dtype=torch.float64, requires_grad=True)
+    init_v = torch.zeros_like(init_x, requires_grad=True)
+    init_tau = torch.tensor([1.0, 1.0] * 4, dtype=torch.float64, requires_grad=True)
+    t_scale = torch.tensor([2e5, 0.4] * 4, dtype=torch.float64)
+    target = init_x.detach().reshape(-1, 3).mean(0) + torch.tensor([0.0, -0.05, 0.0], dtype=torch.float64)
+    opt = torch.optim.Adam([init_tau], lr=0.2)
+    x0 = init_x.detach().numpy().copy()
+    N = d.n_vertices
+    for it in range(2):
+        opt.zero_grad()
+        tau = t_scale * torch.maximum(init_tau, init_tau * 0 + 0.01)
+        q, qd = sim_all(init_x, init_v, tau, env)
+        loss = (q.reshape(-1, 3).mean(0) - target).norm()
+        loss.backward()
+        E, nu = float(tau[0]), float(tau[1])
+        o = O.OracleScene(d)
+        o.set_materials(np.full(d.n_tets, E), np.full(d.n_tets, nu))
+        r = o.forward(x0, np.zeros_like(x0), n_steps=10)
+        diff = r["x"].reshape(-1, 3).mean(0) - target.numpy()
+        gq = np.tile(diff / np.linalg.norm(diff) / N, N)
+        g = o.backward(gq, np.zeros_like(gq))
+        assert abs(float(loss) - np.linalg.norm(diff)) <= 1e-9 * np.linalg.norm(diff)
+        want = np.zeros(8)
+        want[0] = g["E"].sum() * 2e5 * (1.0 if float(init_tau[0]) > 0.01 else 0.0)
+        want[1] = g["nu"].sum() * 0.4 * (1.0 if float(init_tau[1]) > 0.01 else 0.0)
+        got = init_tau.grad.numpy()
+        assert np.abs(got - want).max() <= 1e-7 * np.abs(want).max(), (got, want)
+        assert np.abs(init_x.grad.numpy() - g["x"]).max() <= 1e-7 * np.abs(g["x"]).max()
+        init_x.grad = None
+        opt.step()
+        env.mPhase = 0
