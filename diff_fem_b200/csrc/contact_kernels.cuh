@@ -677,7 +677,7 @@ __global__ void __launch_bounds__(128) k_contact_fused(SceneDev d, ContactDev c,
 // Records: the computed iteration j of part p is record base + j of its
 // vertices (parts own disjoint rows of a record), its pass flag at
 // rec_first[(base + j) np + p].
-enum { PS_MODE = 0, PS_PASS = 1, PS_IT = 2, PS_COMP = 3, PS_SRC = 4, PS_DONE = 5, PS_RUN = 6, PS_SIZE = 7 };
+enum { PS_MODE = 0, PS_PASS = 1, PS_IT = 2, PS_COMP = 3, PS_SRC = 4, PS_DONE = 5, PS_RUN = 6, PS_SKIP = 7, PS_SIZE = 8 };
 constexpr int kMaxContactParts = 1024;
 
 __device__ __forceinline__ int rec_index_part(const ContactDev& c, int comp) { return rec_index_at(c, comp); }
@@ -822,6 +822,159 @@ __global__ void k_contact_record_parts(const int* step, ContactDev c) {
   if (!(c.rec_on && *c.rec_on == 2)) return;
   const int s = *step;
   for (int p = threadIdx.x; p < c.np; p += blockDim.x) c.psrc[(size_t)s * c.np + p] = c.pst[PS_SRC * c.np + p];
+}
+
+// ---- the batched phase as a conditional loop of kernels ---------------------
+//
+// The same per-part state machine as k_contact_fused_parts, one kernel per
+// phase, each with its own occupancy (the cooperative launch holds the
+// largest per-item register set on every CTA): the state lives in c.pst
+// (PS_* rows of np), the phase kernels read it, one-block control kernels
+// advance it, and the last one decides whether the graph's loop runs again.
+// Per part the operations and their order are those of the cooperative form.
+__device__ __forceinline__ int& pst_at(const ContactDev& c, int row, int p) { return c.pst[row * c.np + p]; }
+
+__global__ void k_cparts_begin(SceneDev d, ContactDev c, const double* xt, const double* xk,
+                               cudaGraphConditionalHandle h) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  contact_begin_item(d, c, i, xt, xk);
+  if (blockIdx.x == 0) {
+    for (int p = threadIdx.x; p < c.np; p += blockDim.x) {
+      pst_at(c, PS_MODE, p) = 0; pst_at(c, PS_PASS, p) = 0; pst_at(c, PS_IT, p) = 0; pst_at(c, PS_COMP, p) = 0;
+      pst_at(c, PS_SRC, p) = 0; pst_at(c, PS_RUN, p) = 0; pst_at(c, PS_SKIP, p) = 1;
+      pst_at(c, PS_DONE, p) = (c.pf0[p + 1] == c.pf0[p]) ? 1 : 0;  // a part without obstacle faces has no phase
+      c.pany[p] = 0;
+      c.pe[p] = 0ull;
+    }
+    if (threadIdx.x == 0) {
+      for (int k = 0; k < CS_SIZE; ++k) c.state[k] = 0;
+      cudaGraphSetConditional(h, (c.nc > 0 && c.nof > 0) ? 1u : 0u);
+    }
+  }
+}
+
+// detection for the parts in detection mode
+__global__ void k_cparts_detect(ContactDev c, const double* xt, const double* xk, int* status) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= c.nc) return;
+  const int p = c.cpart[a];
+  if (pst_at(c, PS_MODE, p) != 0 || pst_at(c, PS_DONE, p)) return;
+  if (contact_detect_item(c, a, xt, xk, status)) atomicOr(c.pany + p, 1);
+}
+
+// after detection (k_contact_ctl_detect per part); clears the parts' maxima
+__global__ void k_cparts_ctl_detect(ContactDev c, int* status) {
+  for (int p = threadIdx.x; p < c.np; p += blockDim.x) {
+    c.pe[p] = 0ull;
+    if (pst_at(c, PS_DONE, p) || pst_at(c, PS_MODE, p) != 0) continue;
+    const int any = c.pany[p];
+    c.pany[p] = 0;
+    if (!any) {
+      pst_at(c, PS_DONE, p) = 1;
+    } else if (pst_at(c, PS_PASS, p) >= c.max_passes) {
+      cap_reached(status, kCapContactPasses);
+      pst_at(c, PS_DONE, p) = 1;
+    } else {
+      pst_at(c, PS_MODE, p) = 1; pst_at(c, PS_IT, p) = 0; pst_at(c, PS_PASS, p) += 1;
+    }
+  }
+}
+
+// ori_x = x_n1 on the vertices of the parts in iteration mode, and each
+// part's max-norm change (part-aligned blocks; the maximum of doubles >= 0
+// as ordered bit patterns does not depend on the order of the atomics)
+__global__ void k_cparts_prep(PartDev pd, ContactDev c, double* xk) {
+  __shared__ double ws[32];
+  const int b = blockIdx.x, p = pd.blk_part[b];
+  if (pst_at(c, PS_MODE, p) != 1 || pst_at(c, PS_DONE, p)) return;  // uniform over the block
+  const int i = pd.blk_v0[b] + threadIdx.x;
+  double e = i < pd.part_v0[p + 1] ? contact_prep_vertex(c, i, xk) : 0.0;
+  for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x + 31) / 32; ++w) m = fmax(m, ws[w]);
+    atomicMax(c.pe + p, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+// the impact lists each iterating part's contact vertices use, into its records
+__global__ void k_cparts_record(ContactDev c) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= c.nc) return;
+  const int p = c.cpart[a];
+  if (pst_at(c, PS_MODE, p) != 1 || pst_at(c, PS_DONE, p)) return;
+  const int rk = rec_index_at(c, pst_at(c, PS_COMP, p));
+  if (rk >= 0) contact_prep_record(c, a, rk);
+}
+
+// per part: converged (back to detection) or one more Jacobi iteration
+// (PS_RUN; PS_SKIP is its complement, the gate of the local step)
+__global__ void k_cparts_ctl_conv(ContactDev c) {
+  for (int p = threadIdx.x; p < c.np; p += blockDim.x) {
+    pst_at(c, PS_RUN, p) = 0;
+    pst_at(c, PS_SKIP, p) = 1;
+    if (pst_at(c, PS_DONE, p) || pst_at(c, PS_MODE, p) != 1) continue;
+    const double m = __longlong_as_double((long long)c.pe[p]);
+    pst_at(c, PS_SRC, p) = pst_at(c, PS_COMP, p);
+    if (m < kConvergenceEps) {
+      pst_at(c, PS_MODE, p) = 0;
+    } else {
+      pst_at(c, PS_RUN, p) = 1;
+      pst_at(c, PS_SKIP, p) = 0;
+    }
+  }
+}
+
+// the Jacobi update of the iterating parts' vertices (contact_rhs_item), and
+// each part's pass flag for its record
+__global__ void k_cparts_rhs(SceneDev d, PartDev pd, ContactDev c, const double* __restrict__ slot, const double* xt,
+                             const double* xk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  const int p = vpart_of(d, i);
+  if (!pst_at(c, PS_RUN, p)) return;
+  const int first = pst_at(c, PS_IT, p) == 0 ? 1 : 0;
+  const int rk = rec_index_at(c, pst_at(c, PS_COMP, p));
+  contact_rhs_item(d, c, i, slot, xt, xk, first != 0, rk);
+  if (i == pd.part_v0[p] && rk >= 0) c.rec_first[(size_t)rk * c.np + p] = first;
+}
+
+// end of a round: count the iterations, and loop while some part is not done
+__global__ void k_cparts_ctl_iter(ContactDev c, int K, int* status, cudaGraphConditionalHandle h) {
+  __shared__ int s_open, s_pass, s_comp;
+  if (threadIdx.x == 0) { s_open = 0; s_pass = 0; s_comp = 0; }
+  __syncthreads();
+  for (int p = threadIdx.x; p < c.np; p += blockDim.x) {
+    if (pst_at(c, PS_RUN, p)) {
+      if (c.rec_on && *c.rec_on == 1 && *c.rec_base + pst_at(c, PS_COMP, p) >= c.rec_cap) atomicExch(status, 6);
+      pst_at(c, PS_IT, p) += 1;
+      pst_at(c, PS_COMP, p) += 1;
+      if (pst_at(c, PS_IT, p) >= K) pst_at(c, PS_MODE, p) = 0;
+    }
+    if (!pst_at(c, PS_DONE, p)) s_open = 1;
+    atomicMax(&s_pass, pst_at(c, PS_PASS, p));
+    atomicMax(&s_comp, pst_at(c, PS_COMP, p));
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int rounds = c.state[CS_BODIES] + 1;
+    c.state[CS_BODIES] = rounds;
+    c.state[CS_PASS] = s_pass;
+    c.state[CS_COMP] = s_comp;
+    bool open = s_open != 0;
+    if (open && rounds > c.max_passes * (K + 2) + 2) {  // unreachable: every part's passes and iterations are bounded
+      cap_reached(status, kCapContactPasses);
+      open = false;
+    }
+    cudaGraphSetConditional(h, open ? 1u : 0u);
+  }
+}
+
+// reverse sweep gate: part p takes part in computed iteration j when j <= top[p]
+__global__ void k_cparts_gate(ContactDev c, const int* top, int j) {
+  for (int p = threadIdx.x; p < c.np; p += blockDim.x) pst_at(c, PS_SKIP, p) = j > top[p] ? 1 : 0;
 }
 
 // ---- soft-soft (self) contact ------------------------------------------------
@@ -1300,12 +1453,25 @@ __global__ void k_cadj_rhs(SceneDev d, ContactDev c, ContactAdj a, const double*
   cadj_rhs_item(d, c, a, i, slot, xt, ori, prev, first, rcnt, rn);
 }
 
+// cadj_rhs_item for the vertices of the parts in the sweep, each with its own pass flag
+__global__ void k_cadj_rhs_parts(SceneDev d, ContactDev c, ContactAdj a, const double* __restrict__ slot,
+                                 const double* __restrict__ xt, const double* __restrict__ ori,
+                                 const double* __restrict__ prev, const int* __restrict__ first,
+                                 const int* __restrict__ rcnt, const double* __restrict__ rn) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.N) return;
+  const int p = vpart_of(d, i);
+  if (pst_at(c, PS_SKIP, p)) return;
+  cadj_rhs_item(d, c, a, i, slot, xt, ori, prev, first[p], rcnt, rn);
+}
+
 // VJP of J d at ori with cotangent yb, and the Hs terms of the tets' E gradient
 __global__ void __launch_bounds__(128) k_cadj_local(SceneDev d, ContactAdj a, const double* __restrict__ ori,
                                                     const double* __restrict__ xt, const double* __restrict__ act_all,
                                                     const int* step, double* __restrict__ slot, double* gE,
-                                                    double* gnu, double* mg) {
+                                                    double* gnu, double* mg, Gate gate) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gate.skip(cons_part(d, t))) return;
   adj_local_item(d, t, ori, a.yb, act_all + (size_t)(*step) * d.nseg, slot, gE, gnu, mg, nullptr, xt);
 }
 
@@ -1661,9 +1827,9 @@ __device__ __forceinline__ void cadj_hs_item(const SceneDev& d, const ContactAdj
   st3(a.xn1b, i, o);
 }
 
-__global__ void k_cadj_hs(SceneDev d, ContactAdj a) {
+__global__ void k_cadj_hs(SceneDev d, ContactAdj a, Gate gate) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= d.N) return;
+  if (i >= d.N || gate.skip(vpart_of(d, i))) return;
   cadj_hs_item(d, a, i);
 }
 

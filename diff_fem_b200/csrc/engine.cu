@@ -1000,8 +1000,7 @@ static int upload_scene(dfem_scene* sc) {
       sc->fused_ok = coop != 0 && occ > 0 && occ_a > 0;
       if (sc->fused_ok) CK(sc->fpartial.alloc(std::max(1, sc->fused_grid)));
     }
-    if (sc->cnp > 0 && !sc->fused_ok)
-      return fail(DFEM_ERR_UNSUPPORTED, "batch: obstacle contact needs the cooperative contact phase on this device");
+    if (sc->cnp > 0) sc->fused_on = false;  // batches: the loop of kernels unless the cooperative form is asked for
     if (sc->self_contact) {
       const int ncf = (int)s.cfaces.size() / 3;
       CK(sc->s_cfaces.upload(s.cfaces));
@@ -1398,6 +1397,10 @@ static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle
 // obstacle contact phase (second conditional loop of the step graph)
 static void contact_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   const int n = std::max(sc->hs.N, sc->cd.nc);
+  if (sc->cnp > 0) {  // a batch: per-part state machines
+    k_cparts_begin<<<(n + 127) / 128, 128, 0, st>>>(sc->sd, sc->cd, sc->xt.p, sc->xk.p, h);
+    return;
+  }
   k_contact_begin<<<(n + 127) / 128, 128, 0, st>>>(sc->sd, sc->cd, sc->xt.p, sc->xk.p, h);
 }
 
@@ -1405,6 +1408,21 @@ static void contact_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHa
   const HostScene& s = sc->hs;
   const int nb = sc->nblk_v;
   const int ncons = s.T + s.M + s.S + s.B;
+  if (sc->cnp > 0) {  // a batch: one round of every part's state machine
+    const int nca = (sc->cd.nc + 127) / 128;
+    k_cparts_detect<<<nca, 128, 0, st>>>(sc->cd, sc->xt.p, sc->xk.p, sc->status.p);
+    k_cparts_ctl_detect<<<1, 256, 0, st>>>(sc->cd, sc->status.p);
+    k_cparts_prep<<<sc->nblk_p, kPartBlock, 0, st>>>(sc->pd, sc->cd, sc->xk.p);
+    k_cparts_record<<<nca, 128, 0, st>>>(sc->cd);
+    k_cparts_ctl_conv<<<1, 256, 0, st>>>(sc->cd);
+    Gate run;
+    run.flag = sc->c_pst.p + (size_t)PS_SKIP * sc->cnp;
+    if (ncons > 0)
+      k_local<<<(ncons + 127) / 128, 128, 0, st>>>(sc->sd, run, sc->xk.p, sc->act_all.p, sc->step.p, sc->slot.p);
+    k_cparts_rhs<<<nb, 128, 0, st>>>(sc->sd, sc->pd, sc->cd, sc->slot.p, sc->xt.p, sc->xk.p);
+    k_cparts_ctl_iter<<<1, 256, 0, st>>>(sc->cd, s.K, sc->status.p, h);
+    return;
+  }
   k_contact_detect<<<(sc->cd.nc + 127) / 128, 128, 0, st>>>(sc->cd, sc->xt.p, sc->xk.p, sc->status.p);
   const int ncf = sc->cd.ncf;
   if (sc->self_contact) {  // soft impacts, then the pass's self groups
@@ -1728,6 +1746,45 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
     src = meta[CS_SRC];
   }
   if (base + comp > sc->crec_cap) return fail(DFEM_ERR_CAP, "contact record too small for the recomputed step");
+  if (sc->cnp > 0 && !fused_contact(sc)) {  // a batch: every part's reverse sweep, a loop of gated kernels
+    const int np = sc->cnp;
+    const int* top = recorded ? sc->c_psrc.p + (size_t)st * np : sc->c_pst.p + (size_t)PS_SRC * np;
+    std::vector<int> toph(np);
+    CK(cudaMemcpyAsync(toph.data(), top, sizeof(int) * np, cudaMemcpyDeviceToHost, sc->stream));
+    CK(cudaStreamSynchronize(sc->stream));
+    const int jmax = *std::max_element(toph.begin(), toph.end());
+    const ContactAdj a = make_cadj(sc);
+    Gate g;
+    g.flag = sc->c_pst.p + (size_t)PS_SKIP * np;
+    k_cadj_start<<<nb, 128, 0, sc->stream>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, a, 0);
+    int launches = 1;
+    for (int j = jmax; j >= 1; --j) {
+      const size_t r = (size_t)base + (j - 1);
+      const double* ori = sc->crec_x.p + r * n3;
+      const double* prev = sc->crec_prev.p + r * n3;
+      const int* rcnt = sc->crec_cnt.p + r * sc->cd.nc;
+      const double* rn = sc->crec_n.p + r * sc->cd.nc * kMaxImpactsPerVertex * 3;
+      k_cparts_gate<<<1, 256, 0, sc->stream>>>(sc->cd, top, j);
+      if (ncons > 0)
+        k_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, g, ori, sc->act_all.p, sc->step.p, sc->slot.p);
+      k_cadj_rhs_parts<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->cd, a, sc->slot.p, xt, ori, prev,
+                                                   sc->crec_first.p + r * np, rcnt, rn);
+      if (ncons > 0)
+        k_cadj_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, ori, xt, sc->act_all.p, sc->step.p,
+                                                                  sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p, g);
+      k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
+      if (s.nseg > 0)
+        k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, s.M, g, sc->seg_part.p, sc->step.p,
+                                                                  sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
+      k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a, g);
+      launches += 5 + (ncons > 0 ? 2 : 0) + (s.nseg > 0 ? 1 : 0);
+    }
+    if (s.T > 0) k_cadj_hd<<<(s.T + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, sc->gE.p);
+    k_cadj_to_pd<<<nb, 128, 0, sc->stream>>>(s.N, a, sc->io_a.p, sc->io_b.p);
+    CK(cudaGetLastError());
+    sc->launches += launches + 2;
+    return DFEM_OK;
+  }
   if (sc->cnp > 0) {  // a batch: every part's reverse sweep in one cooperative launch
     const ContactAdj a = make_cadj(sc);
     const int* top = recorded ? sc->c_psrc.p + (size_t)st * sc->cnp : sc->c_pst.p + (size_t)PS_SRC * sc->cnp;
@@ -1795,12 +1852,12 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
       k_cadj_self_b<<<(sc->cd.nc + 127) / 128, 128, 0, sc->stream>>>(sc->sd, sc->cd, a, rv, first[j - 1], rcnt, rn);
       if (ncons > 0)
         k_cadj_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, ori, xt, sc->act_all.p, sc->step.p,
-                                                                  sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+                                                                  sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p, kOpen);
       k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
       if (s.nseg > 0)
         k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, s.M, kOpen, sc->seg_part.p, sc->step.p,
                                                                   sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
-      k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a);
+      k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a, kOpen);
       launches += 6 + (ncons > 0 ? 2 : 0) + (s.nseg > 0 ? 1 : 0);
       continue;
     }
@@ -1814,12 +1871,12 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
     k_cadj_rhs<<<nb, 128, 0, sc->stream>>>(sc->sd, sc->cd, a, sc->slot.p, xt, ori, prev, first[j - 1], rcnt, rn);
     if (ncons > 0)
       k_cadj_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, ori, xt, sc->act_all.p, sc->step.p,
-                                                                sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p);
+                                                                sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p, kOpen);
     k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
     if (s.nseg > 0)
       k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, s.M, kOpen, sc->seg_part.p, sc->step.p,
                                                                 sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
-    k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a);
+    k_cadj_hs<<<nb, 128, 0, sc->stream>>>(sc->sd, a, kOpen);
     launches += 4 + (ncons > 0 ? 2 : 0) + (s.nseg > 0 ? 1 : 0);
   }
   if (soft && src == 0) {  // the output is the PD result itself
@@ -2702,8 +2759,8 @@ int dfem_set_option(dfem_scene* sc, int32_t which, int64_t value) {
   switch (which) {
     case DFEM_OPTION_FUSED_CONTACT:
       if (value != 0 && value != 1) return fail(DFEM_ERR_INVALID, "value must be 0 or 1");
-      if (value == 0 && sc->cnp > 0)
-        return fail(DFEM_ERR_UNSUPPORTED, "a batch's contact phase runs only as the cooperative launch");
+      if (value == 1 && sc->cnp > 0 && !sc->fused_ok)
+        return fail(DFEM_ERR_UNSUPPORTED, "the device cannot run the batch's cooperative contact phase");
       sc->fused_on = value != 0;
       break;
     default:

@@ -391,11 +391,12 @@ enum dfem_limit {
 int dfem_set_limit(dfem_scene *scene, int32_t which, int64_t value);
 
 /* Execution options of a scene; results are identical under every setting.
- *   DFEM_OPTION_FUSED_CONTACT  1 (default): a step's obstacle contact phase
- *                              (scenes without soft-soft contact) runs as one
- *                              cooperative launch with grid-wide barriers
- *                              between its detection and Jacobi phases; 0: as a
- *                              conditional graph loop of kernels.
+ *   DFEM_OPTION_FUSED_CONTACT  1 (default for single scenes): a step's obstacle
+ *                              contact phase (scenes without soft-soft contact)
+ *                              runs as one cooperative launch with grid-wide
+ *                              barriers between its detection and Jacobi phases;
+ *                              0 (default for batches): as a conditional graph
+ *                              loop of kernels (batches: gated per scene).
  * No counterpart in the reference. */
 enum dfem_option { DFEM_OPTION_FUSED_CONTACT = 0 };
 int dfem_set_option(dfem_scene *scene, int32_t which, int64_t value);

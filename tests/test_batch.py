@@ -183,14 +183,16 @@ def test_large_batch_launch_classes_match_scenes(form):
     b.close()
 
 
-def test_batch_with_obstacle_contact_matches_scenes():
+@pytest.mark.parametrize("form", ["loop", "cooperative"])
+def test_batch_with_obstacle_contact_matches_scenes(form):
     """Obstacle contact inside a batch: boxes dropped on their own grounds (one
     with friction clamping, one landing faster) and a muscle beam without
     contact.  The contact parts' trajectories, contact passes, iteration
     counts and gradients are the scene's own bit for bit (each part runs its
-    own detection passes, Jacobi iterations and convergence test in the
-    batched cooperative phase); the part without contact matches to rounding
-    (its adjoint passes through the phase's cotangent bookkeeping)."""
+    own detection passes, Jacobi iterations and convergence test, as a loop
+    of gated kernels or in one cooperative launch); the part without contact
+    matches to rounding (its adjoint passes through the phase's cotangent
+    bookkeeping)."""
     a = S.drop_box(mu=0.3)
     b_ = S.drop_box(nx=3, ny=2, nz=3, height=0.03, v0=-1.5, mu=0.3)
     dry = S.muscle_beam()
@@ -198,6 +200,7 @@ def test_batch_with_obstacle_contact_matches_scenes():
     vels = [a.initial_velocity, b_.initial_velocity, np.zeros(3 * dry.n_vertices)]
     n = 8
     bt = Scene.batch(descs)
+    bt.set_option("fused_contact", 1 if form == "cooperative" else 0)
     vo, to, so = bt.offsets["vertices"], bt.offsets["tets"], bt.offsets["segments"]
     nseg = [d.n_segments for d in descs]
     rng = np.random.default_rng(17)
