@@ -434,76 +434,84 @@ def north_star_extras(args, local: int) -> dict:
     c2["oracle"] = f"FP64 C++ oracle on the host ({threads} threads), same moduli and target"
     res["inverse_stiffness"] = c2
 
-    # (2) the uneven batch: batched mixed, batched FP64, plain FP64 one at a time
-    nb = 100
-    dm, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_MIXED)
-    dd, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_FP64)
-    xb = torch.tensor(np.concatenate([d.x0.reshape(-1) for d in dm]), device=dev)
-    vb = torch.zeros_like(xb)
-    nseg = sum(d.n_segments for d in dm)
-    act = torch.tensor(np.random.default_rng(42).uniform(0.0, 1.0, (nb, nseg)), device=dev)
-    out = {}
-    for name, descs, reps in (("mixed", dm, 2), ("fp64", dd, 1)):
-        t0 = time.perf_counter()
-        b = Scene.batch(descs, device=local)
-        setup = time.perf_counter() - t0
+    # (2) the uneven batch: batched mixed, batched FP64, plain FP64 one at a time;
+    #     as specified (stars on their grounds) and without the grounds
+    def batch_block(ground):
+        nb = 100
+        dm, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_MIXED, ground=ground)
+        dd, _ = S.uneven_batch(n_scenes=args.scenes, precision=DFEM_PREC_FP64, ground=ground)
+        xb = torch.tensor(np.concatenate([d.x0.reshape(-1) for d in dm]), device=dev)
+        vb = torch.zeros_like(xb)
+        nseg = sum(d.n_segments for d in dm)
+        act = torch.tensor(np.random.default_rng(42).uniform(0.0, 1.0, (nb, nseg)), device=dev)
+        out = {}
+        for name, descs, reps in (("mixed", dm, 2), ("fp64", dd, 1)):
+            t0 = time.perf_counter()
+            b = Scene.batch(descs, device=local)
+            setup = time.perf_counter() - t0
 
-        def batch_eval():
-            x, _ = b.forward(xb, vb, n_steps=nb, act=act)
-            return x, b.backward(2.0 * (x - xb), torch.zeros_like(x))
+            def batch_eval():
+                x, _ = b.forward(xb, vb, n_steps=nb, act=act)
+                return x, b.backward(2.0 * (x - xb), torch.zeros_like(x))
 
-        t, (x, g) = timed(batch_eval, reps)
-        out[name] = {"value": len(descs) * nb / t, "unit": "scene-steps/s", "setup_s": setup,
-                     "x": x.cpu().numpy(), "E": g["E"].cpu().numpy(), "act": g["act"].cpu().numpy(),
-                     "iters": b.iterations(nb), "offsets": b.offsets}
-        b.close()
-    # plain FP64, one scene per handle: a sample stratified by size
-    order = np.argsort([d.n_tets for d in dd], kind="stable")
-    sample = order[np.linspace(0, len(dd) - 1, min(16, len(dd))).astype(int)]
-    vo, so = out["fp64"]["offsets"]["vertices"], out["fp64"]["offsets"]["segments"]
-    tsum = 0.0
-    for q in sample:
-        sc = Scene(dd[q], device=local)
-        xq = xb[3 * vo[q]:3 * vo[q + 1]].contiguous()
-        aq = act[:, so[q]:so[q + 1]].contiguous() if so[q + 1] > so[q] else None
+            t, (x, g) = timed(batch_eval, reps)
+            out[name] = {"value": len(descs) * nb / t, "unit": "scene-steps/s", "setup_s": setup,
+                         "x": x.cpu().numpy(), "E": g["E"].cpu().numpy(), "act": g["act"].cpu().numpy(),
+                         "iters": b.iterations(nb), "offsets": b.offsets}
+            b.close()
+        # plain FP64, one scene per handle: a sample stratified by size
+        order = np.argsort([d.n_tets for d in dd], kind="stable")
+        sample = order[np.linspace(0, len(dd) - 1, min(16, len(dd))).astype(int)]
+        vo, so = out["fp64"]["offsets"]["vertices"], out["fp64"]["offsets"]["segments"]
+        tsum = 0.0
+        for q in sample:
+            sc = Scene(dd[q], device=local)
+            xq = xb[3 * vo[q]:3 * vo[q + 1]].contiguous()
+            aq = act[:, so[q]:so[q + 1]].contiguous() if so[q + 1] > so[q] else None
 
-        def one():
-            x, _ = sc.forward(xq, torch.zeros_like(xq), n_steps=nb, act=aq)
-            return sc.backward(2.0 * (x - xq), torch.zeros_like(x))
+            def one():
+                x, _ = sc.forward(xq, torch.zeros_like(xq), n_steps=nb, act=aq)
+                return sc.backward(2.0 * (x - xq), torch.zeros_like(x))
 
-        t, _ = timed(one, 1)
-        tsum += t
-        sc.close()
-    plain = len(sample) * nb / tsum
-    # errors of the mixed batch against the FP64 batch, per scene
-    to = out["fp64"]["offsets"]["tets"]
-    same = np.all(out["mixed"]["iters"] == out["fp64"]["iters"], axis=0)
-    pe, ge = [], []
-    for p in range(len(dd)):
-        a0, a1 = 3 * vo[p], 3 * vo[p + 1]
-        pe.append(_rel(out["mixed"]["x"][a0:a1], out["fp64"]["x"][a0:a1]))
-        ge.append(_rel(out["mixed"]["E"][to[p]:to[p + 1]], out["fp64"]["E"][to[p]:to[p + 1]]))
-    pe, ge = np.asarray(pe), np.asarray(ge)
-    res["batch"] = {
-        "workload": f"{len(dd)} uneven scenes (tets log-uniform in [1e3, 5e4], beams and muscle stars), "
-                    f"{nb} steps forward + adjoint",
-        "mixed_batched": {"value": out["mixed"]["value"], "unit": "scene-steps/s", "setup_s": out["mixed"]["setup_s"]},
-        "fp64_batched": {"value": out["fp64"]["value"], "unit": "scene-steps/s", "setup_s": out["fp64"]["setup_s"]},
-        "fp64_one_at_a_time": {"value": plain, "unit": "scene-steps/s", "scenes_sampled": int(len(sample)),
-                               "sample": "16 scenes evenly spaced in size order, one handle each"},
-        "mixed_batched_over_fp64_one_at_a_time": out["mixed"]["value"] / plain,
-        "fp64_batched_over_fp64_one_at_a_time": out["fp64"]["value"] / plain,
-        "mixed_over_fp64_batched": out["mixed"]["value"] / out["fp64"]["value"],
-        "error_mixed_vs_fp64": {
-            "scenes_with_equal_iteration_counts": int(same.sum()), "scenes": int(len(dd)),
-            "pos_rel_max": float(pe[same].max()) if same.any() else None,
-            "pos_rel_median": float(np.median(pe[same])) if same.any() else None,
-            "grad_E_rel_max": float(ge[same].max()) if same.any() else None,
-            "grad_E_rel_median": float(np.median(ge[same])) if same.any() else None,
-            "grad_act_rel_max": _rel(out["mixed"]["act"], out["fp64"]["act"]),
-            "other_scenes_pos_rel_max": float(pe[~same].max()) if (~same).any() else None},
-        "target": ">= 10x batched mixed over plain FP64, at <= 1e-6 position and <= 1e-4 gradient error",
-    }
+            t, _ = timed(one, 1)
+            tsum += t
+            sc.close()
+        plain = len(sample) * nb / tsum
+        # errors of the mixed batch against the FP64 batch, per scene
+        to = out["fp64"]["offsets"]["tets"]
+        same = np.all(out["mixed"]["iters"] == out["fp64"]["iters"], axis=0)
+        pe, ge = [], []
+        for p in range(len(dd)):
+            a0, a1 = 3 * vo[p], 3 * vo[p + 1]
+            pe.append(_rel(out["mixed"]["x"][a0:a1], out["fp64"]["x"][a0:a1]))
+            ge.append(_rel(out["mixed"]["E"][to[p]:to[p + 1]], out["fp64"]["E"][to[p]:to[p + 1]]))
+        pe, ge = np.asarray(pe), np.asarray(ge)
+        return {
+            "workload": f"{len(dd)} uneven scenes (tets log-uniform in [1e3, 5e4], beams and muscle stars"
+                        + (", the stars on their grounds" if ground else ", no grounds") + f"), {nb} steps forward + adjoint",
+            "mixed_batched": {"value": out["mixed"]["value"], "unit": "scene-steps/s", "setup_s": out["mixed"]["setup_s"]},
+            "fp64_batched": {"value": out["fp64"]["value"], "unit": "scene-steps/s", "setup_s": out["fp64"]["setup_s"]},
+            "fp64_one_at_a_time": {"value": plain, "unit": "scene-steps/s", "scenes_sampled": int(len(sample)),
+                                   "sample": "16 scenes evenly spaced in size order, one handle each"},
+            "mixed_batched_over_fp64_one_at_a_time": out["mixed"]["value"] / plain,
+            "fp64_batched_over_fp64_one_at_a_time": out["fp64"]["value"] / plain,
+            "mixed_over_fp64_batched": out["mixed"]["value"] / out["fp64"]["value"],
+            "error_mixed_vs_fp64": {
+                "scenes_with_equal_iteration_counts": int(same.sum()), "scenes": int(len(dd)),
+                "pos_rel_max": float(pe[same].max()) if same.any() else None,
+                "pos_rel_median": float(np.median(pe[same])) if same.any() else None,
+                "grad_E_rel_max": float(ge[same].max()) if same.any() else None,
+                "grad_E_rel_median": float(np.median(ge[same])) if same.any() else None,
+                "grad_act_rel_max": _rel(out["mixed"]["act"], out["fp64"]["act"]),
+                "other_scenes_pos_rel_max": float(pe[~same].max()) if (~same).any() else None},
+            "target": ">= 10x batched mixed over plain FP64, at <= 1e-6 position and <= 1e-4 gradient error",
+        }
+
+    res["batch"] = batch_block(True)
+    res["batch_without_ground"] = batch_block(False)
+    res["batch_without_ground"]["note"] = ("the same scenes without obstacle contact: over 100 steps the contact "
+                                           "phase's stick/slide and impact decisions amplify the mixed form's "
+                                           "rounding, so the error target is met only without them")
     return res
 
 
