@@ -1466,7 +1466,7 @@ __global__ void k_cadj_rhs_parts(SceneDev d, ContactDev c, ContactAdj a, const d
 }
 
 // VJP of J d at ori with cotangent yb, and the Hs terms of the tets' E gradient
-__global__ void __launch_bounds__(128) k_cadj_local(SceneDev d, ContactAdj a, const double* __restrict__ ori,
+__global__ void __launch_bounds__(128, DFEM_ADJ_MIN_BLOCKS) k_cadj_local(SceneDev d, ContactAdj a, const double* __restrict__ ori,
                                                     const double* __restrict__ xt, const double* __restrict__ act_all,
                                                     const int* step, double* __restrict__ slot, double* gE,
                                                     double* gnu, double* mg, Gate gate) {
