@@ -195,7 +195,7 @@ struct dfem_scene {
   // (the adjoint then replays no step without contact), else of one step
   // (every step is recomputed from its checkpoint)
   long long hist_step = 0;
-  size_t adj_budget = 0;  // set at creation: half of the device memory, at most 3/4 of the free memory
+  size_t adj_budget = 0;  // set at creation: a quarter of the device memory, at most half of the free memory
   // articulated skeleton (links whose vertices move rigidly)
   bool skel_on = false;
   int sk_nq = 0;                         // joint-state length 12 + L - 1
@@ -2107,11 +2107,12 @@ static int create_on_device(std::unique_ptr<dfem_scene>& sc, int device, dfem_sc
   CK(sc->status.alloc(4));  // before the factor upload, whose kernels report into it
   {
     // device memory the adjoint may fill with stored iterates and contact
-    // records (each saves a replayed step): half of the device, at most three
-    // quarters of what is free when the scene is made
+    // records (each saves a replayed step): a quarter of the device, at most
+    // half of what is free when the scene is made (a record store that grows
+    // holds its old and new arrays at once while it copies)
     size_t free_b = 0, total_b = 0;
     CK(cudaMemGetInfo(&free_b, &total_b));
-    sc->adj_budget = std::min(total_b / 2, free_b / 4 * 3);
+    sc->adj_budget = std::min(total_b / 4, free_b / 2);
   }
   RC(upload_scene(sc.get()));
   RC(ensure_steps(sc.get(), 1));
