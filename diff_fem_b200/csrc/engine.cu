@@ -1656,6 +1656,15 @@ static int ensure_contact_record(dfem_scene* sc, int cap, int keep = 0) {
   }
   if (cap <= sc->crec_cap) return DFEM_OK;
   keep = std::min(keep, sc->crec_cap);
+  if (keep == 0 && sc->crec_cap > 0) {  // nothing to copy: release the old record before the new one is made
+    sc->crec_x.alloc(0); sc->crec_prev.alloc(0); sc->crec_first.alloc(0); sc->crec_cnt.alloc(0); sc->crec_n.alloc(0);
+    if (sc->self_contact) { sc->crec_si.alloc(0); sc->crec_sd.alloc(0); }
+    sc->crec_cap = 0;
+    sc->cd.rec_cap = 0;
+    sc->cd.rec_x = sc->cd.rec_prev = sc->cd.rec_n = nullptr;
+    sc->cd.rec_first = sc->cd.rec_cnt = nullptr;
+    invalidate_graphs(sc);
+  }
   DBuf<double> x, prev, nrm;
   DBuf<int> first, cnt;
   CK(x.alloc(n3 * cap));
@@ -2314,7 +2323,16 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
     const int want = (int)std::min<size_t>(rec_budget, sc->crec_target > 0 ? (size_t)sc->crec_target
                                                                              : 4 * (size_t)n_steps);
     fwd_rec = want >= 1 && !sc->self_contact;  // soft-soft contact has no adjoint to record for
-    if (fwd_rec) RC(ensure_contact_record(sc, want));
+    if (fwd_rec) {
+      const int rc = ensure_contact_record(sc, want);
+      if (rc == DFEM_ERR_NOMEM) {  // no room to record: the adjoint replays the contact steps
+        cudaGetLastError();
+        g_last_error.clear();
+        fwd_rec = false;
+      } else {
+        RC(rc);
+      }
+    }
     const int on = fwd_rec ? 2 : 0;
     CK(cudaMemcpyAsync(sc->crec_on.p, &on, sizeof(int), cudaMemcpyHostToDevice, sc->stream));
     CK(cudaMemsetAsync(sc->crec_base.p, 0, sizeof(int), sc->stream));
@@ -2387,8 +2405,23 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
     recorded[st] = c && sc->crec_fwd && 4 * st + 3 < (int)sc->crec_meta_h.size() && sc->crec_meta_h[4 * st + 3] == 1;
     if (c && !recorded[st]) ccap = std::max(ccap, sc->rec_passes[2 * st + 1]);
   }
-  const int rbase = sc->crec_fwd ? sc->crec_used : 0;
-  if (any_contact) RC(ensure_contact_record(sc, rbase + std::max(1, ccap), rbase));
+  int rbase = sc->crec_fwd ? sc->crec_used : 0;
+  if (any_contact) {
+    const int rc = ensure_contact_record(sc, rbase + std::max(1, ccap), rbase);
+    if (rc == DFEM_ERR_NOMEM && rbase > 0) {
+      // no room for the replays beside the forward's records: drop them, and
+      // replay every contact step (same results, more time)
+      cudaGetLastError();
+      g_last_error.clear();
+      rbase = 0;
+      sc->crec_fwd = false;
+      for (int st = 0; st < sc->rec_steps; ++st)
+        if (recorded[st]) { recorded[st] = false; ccap = std::max(ccap, sc->rec_passes[2 * st + 1]); }
+      RC(ensure_contact_record(sc, std::max(1, ccap), 0));
+    } else {
+      RC(rc);
+    }
+  }
   const HostScene& s = sc->hs;
   const size_t n3 = 3 * (size_t)s.N;
   const int nb = sc->nblk_v;

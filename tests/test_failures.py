@@ -108,3 +108,41 @@ def test_injected_allocation_failures_map_to_nomem():
     for a, b in zip(ref, again):
         assert np.array_equal(a, b)
     sc.close()
+
+
+def test_record_store_allocation_failure_falls_back_to_replays():
+    """A forward whose contact-record store cannot grow runs without
+    recording, and the adjoint replays its contact steps: the gradients equal
+    those of a run that replays every step, bit for bit, wherever among the
+    store's arrays the allocation fails."""
+    lib = _capi.lib()
+    d = S.drop_box(mu=0.3)
+    n = 4
+    x = d.x0.reshape(-1).copy()
+    v = np.tile([1.0, -1.0, 0.3], d.n_vertices)
+    rng = np.random.default_rng(8)
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    ref = Scene(d)
+    ref.set_adjoint_budget(0)
+    ref.forward(x, v, n_steps=n)
+    assert ref.contact_passes(n).sum() > 0
+    want = ref.backward(gx, gv)
+    ref.close()
+    g = Scene(d)
+    g.forward(x, v, n_steps=n)  # records every contact step; the next forward asks for a larger store
+    g.backward(gx, gv)
+    try:
+        for after in range(5):
+            lib.dfem_debug_fail_allocations(after)
+            g.forward(x, v, n_steps=n)
+            lib.dfem_debug_fail_allocations(-1)
+            got = g.backward(gx, gv)
+            for k in ("x", "v", "E", "nu"):
+                assert np.array_equal(got[k], want[k]), (after, k)
+    finally:
+        lib.dfem_debug_fail_allocations(-1)
+    g.forward(x, v, n_steps=n)
+    got = g.backward(gx, gv)
+    for k in ("x", "v", "E", "nu"):
+        assert np.array_equal(got[k], want[k]), k
+    g.close()
