@@ -86,6 +86,8 @@ SIGNATURES = [
     ("dfem_set_activations", C.c_int, [_VP, _VP, C.c_int]),
     ("dfem_set_joint_state", C.c_int, [_VP, _pd, _pd]),
     ("dfem_get_joint_state", C.c_int, [_VP, _pd, _pd]),
+    ("dfem_set_joint_state_grad", C.c_int, [_VP, _pd, _pd]),
+    ("dfem_get_joint_state_grad", C.c_int, [_VP, _pd, _pd]),
     ("dfem_step_forward", C.c_int, [_VP, _VP, _VP, _VP, C.c_int32, _VP, _VP, _VP, C.c_int]),
     ("dfem_step_backward", C.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP, C.c_int]),
     ("dfem_eval_local", C.c_int, [_VP, _VP, _VP, C.c_int]),

@@ -35,7 +35,9 @@ class SimAct(torch.autograd.Function):
         dq, dqd, djq, djqd, dtau = pd.backward_act(_np(q), _np(qd), _np(jq), _np(jqd), _np(tau), _np(dldq), _np(dldqd),
                                                    _np(dldjq), _np(dldjqd), env, ctx.is_act)
         dt = q.dtype
-        return (torch.tensor(dq, dtype=dt), torch.tensor(dqd, dtype=dt), torch.zeros_like(jq), torch.zeros_like(jqd),
+        gjq = torch.tensor(djq, dtype=jq.dtype) if np.size(djq) == jq.numel() else torch.zeros_like(jq)
+        gjqd = torch.tensor(djqd, dtype=jqd.dtype) if np.size(djqd) == jqd.numel() else torch.zeros_like(jqd)
+        return (torch.tensor(dq, dtype=dt), torch.tensor(dqd, dtype=dt), gjq, gjqd,
                 torch.tensor(dtau, dtype=tau.dtype), None, None)
 
 

@@ -24,6 +24,7 @@
 #include "drag_kernels.cuh"
 #include "resident_solve.cuh"
 #include "skeleton_kernels.cuh"
+#include "skeleton_adjoint.cuh"
 #include "resident_plan.h"
 #include "scene.h"
 
@@ -203,6 +204,9 @@ struct dfem_scene {
   DBuf<SkelState> sk_st;
   DBuf<int> sk_rv, sk_rlink, sk_ridx, sk_perm;
   DBuf<double> sk_rest, sk_cinv, sk_zcm, sk_jq, sk_jqd, sk_v0, sk_w, sk_rr, sk_q, sk_tv, sk_kt, sk_sm, sk_rhs, sk_sol;
+  // the adjoint's history (per step and iteration) and work buffers
+  DBuf<double> sk_hist, sk_jin, sk_thb, sk_sb, sk_gjq, sk_gjqd, sk_mu2, sk_mu3, sk_dlt, sk_jfin;
+  std::vector<double> sk_gout;           // cotangents of the next backward's output (jq, jqd); empty: zero
   SkelDev skd{};
   // adjoint
   DBuf<double> xkb, xtb, bb, gE, gnu, mg, gact;
@@ -819,6 +823,19 @@ static int build_obstacle_grid(dfem_scene* sc) {
 
 static int upload_skeleton(dfem_scene* sc);
 
+// the skeleton view's history and adjoint pointers (set by upload_skeleton and
+// by ensure_steps, which sizes the history)
+static void skel_bind(dfem_scene* sc) {
+  SkelDev& k = sc->skd;
+  k.nq = sc->sk_nq;
+  k.K = sc->hs.K;
+  k.hstride = (long long)k.nq + k.ndof + 3LL * k.nr;
+  k.hist = sc->sk_hist.p;
+  k.jin = sc->sk_jin.p;
+  k.thb = sc->sk_thb.p; k.sb = sc->sk_sb.p; k.gjq = sc->sk_gjq.p; k.gjqd = sc->sk_gjqd.p;
+  k.mu2 = sc->sk_mu2.p; k.mu3 = sc->sk_mu3.p; k.dlt = sc->sk_dlt.p;
+}
+
 // for the OBJ writer (obj_writer.cpp): the stream and device of a scene
 cudaStream_t scene_stream(dfem_scene* sc) { return sc->stream; }
 int scene_device(dfem_scene* sc) { return sc->device; }
@@ -1128,11 +1145,19 @@ static int upload_skeleton(dfem_scene* sc) {
   CK(sc->sk_tv.alloc(3 * (size_t)nr * ndof)); CK(sc->sk_kt.alloc(3 * (size_t)nr * ndof));
   CK(sc->sk_sm.alloc((size_t)ndof * ndof)); CK(sc->sk_rhs.alloc(ndof)); CK(sc->sk_sol.alloc(ndof));
   CK(sc->sk_perm.alloc(ndof));
+  const int nq = sc->sk_nq;
+  if (!sc->sk_thb.p) {
+    CK(sc->sk_thb.alloc(nq)); CK(sc->sk_sb.alloc(ndof)); CK(sc->sk_gjq.alloc(nq)); CK(sc->sk_gjqd.alloc(nq));
+    CK(sc->sk_mu2.alloc(3 * (size_t)nr)); CK(sc->sk_mu3.alloc(ndof)); CK(sc->sk_dlt.alloc(3 * (size_t)nr));
+    CK(sc->sk_jfin.alloc(2 * (size_t)nq));
+  }
   sc->skd = SkelDev{L, ndof, nr, N, sc->sk_link.p, sc->sk_st.p, sc->sk_rv.p, sc->sk_rlink.p, sc->sk_ridx.p,
                     sc->sk_rest.p, sc->sk_cinv.p, sc->sk_zcm.p, sc->sk_jq.p, sc->sk_jqd.p, sc->sk_v0.p, sc->sk_w.p,
                     sc->sk_rr.p, sc->sk_q.p, sc->sk_tv.p, sc->sk_kt.p, sc->sk_sm.p, sc->sk_rhs.p, sc->sk_sol.p,
                     sc->sk_perm.p};
+  skel_bind(sc);
   sc->skel_on = true;
+  invalidate_graphs(sc);  // the graphs hold the view's pointers
   return DFEM_OK;
 }
 
@@ -1172,6 +1197,12 @@ static int ensure_steps(dfem_scene* sc, int n_steps) {
   if (sc->has_contact) {
     CK(sc->crec_meta.alloc(4 * (size_t)cap));
     sc->cd.rec_meta = sc->crec_meta.p;
+  }
+  if (sc->skel_on) {  // the links' history: every step's iterations (a few hundred doubles each)
+    const size_t hs = (size_t)sc->sk_nq + sc->skd.ndof + 3 * (size_t)sc->skd.nr;
+    CK(sc->sk_hist.alloc((size_t)cap * (s.K + 1) * hs));
+    CK(sc->sk_jin.alloc((size_t)cap * 2 * sc->sk_nq));
+    skel_bind(sc);
   }
   sc->cap_steps = cap;
   invalidate_graphs(sc);  // graphs hold the old pointers
@@ -1390,7 +1421,7 @@ static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle
                                    sc->ckpt_v.p, sc->flag.p, sc->iters.p,
                                    sc->partial.p, sc->counter.p, sc->errv.p, sc->status.p,
                                    sc->has_contact ? sc->vwc.p : nullptr);
-  if (sc->skel_on) k_skel_begin<<<1, 128, 0, st>>>(sc->skd, sc->xk.p);
+  if (sc->skel_on) k_skel_begin<<<1, 128, 0, st>>>(sc->skd, sc->xk.p, sc->step.p, sc->hist.p, sc->hist_step);
   k_loop_enter<<<1, 256, 0, st>>>(sc->kiter.p, sc->flag.p, sc->hs.nparts, sc->hs.K, h);
 }
 
@@ -1458,7 +1489,7 @@ static void step_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandl
   const cudaError_t ce = capture_solve(sc, st, g, sc->rhs.p, sc->y.p, 0);
   if (ce != cudaSuccess) sc->cur_capture_err = ce;
   if (sc->skel_on) {  // the links' system, then the free vertices' share of the rigid multiplier
-    k_skel_stage<<<1, 256, 0, st>>>(sc->skd, sc->xt.p, sc->y.p, sc->act_all.p, sc->step.p, s.nseg);
+    k_skel_stage<<<1, 256, 0, st>>>(sc->skd, sc->xt.p, sc->y.p, sc->act_all.p, sc->step.p, s.nseg, sc->kiter.p);
     k_skel_apply<<<sc->nblk_v, 128, 0, st>>>(sc->skd, sc->y.p);
   }
   k_update<<<sc->nblk_p, kPartBlock, 0, st>>>(s.N, sc->pd, mixed(sc) ? 1 : 0, sc->kiter.p, sc->xt.p, sc->y.p, sc->xk.p, sc->hist.p, sc->hist_step, sc->step.p,
@@ -1506,22 +1537,37 @@ static void adj_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle 
   // the cotangent of the step's output lives in io_a (x) / io_b (v); k_adj_end overwrites it with the input's
   k_adj_begin<<<sc->nblk_v, 128, 0, st>>>(s.N, s.damping / s.h, sc->io_a.p, sc->io_b.p, sc->xkb.p, sc->xtb.p, sc->bb.p);
   k_adj_loop_enter<<<1, 256, 0, st>>>(sc->kiter.p, sc->iters.p, sc->step.p, s.nparts, s.K, h);
+  if (sc->skel_on) {  // theta-bar of the last iterate: the output jq's cotangent and its rigid rows' V0
+    k_skel_adj_init<<<1, 32, 0, st>>>(sc->skd);
+    k_skel_adj_theta<<<sc->sk_nq, kSkelAdjThreads, 0, st>>>(sc->skd, sc->kiter.p, sc->step.p, 1, 0, sc->xkb.p);
+  }
 }
 
 static void adj_body(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
   const HostScene& s = sc->hs;
   const Gate g = adj_gate(sc);
+  if (sc->skel_on) k_skel_adj_upd<<<1, 64, 0, st>>>(sc->skd, sc->kiter.p, sc->step.p, sc->xkb.p);
   const cudaError_t ce = capture_solve(sc, st, g, sc->xkb.p, sc->y.p, 1);
   if (ce != cudaSuccess) sc->cur_capture_err = ce;
+  if (sc->skel_on) {  // the KKT adjoint of the rigid stage: y becomes mu1
+    k_skel_adj_stage<<<1, 256, 0, st>>>(sc->skd, sc->kiter.p, sc->step.p, sc->y.p, sc->hist.p, sc->hist_step,
+                                        sc->gact.p, s.nseg);
+    k_skel_adj_apply<<<sc->nblk_v, 128, 0, st>>>(sc->skd, sc->y.p);
+  }
   launch_adj_local(sc, st, g, sc->kiter.p);
   launch_adj_gather(sc, st, g);
   if (s.nseg > 0)
     k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, st>>>(s.nseg, s.M, g, sc->seg_part.p, sc->step.p, sc->seg_ptr.p,
                                                        sc->seg_mus.p, sc->mg.p, sc->gact.p);
+  if (sc->skel_on) {  // the moduli's rigid-row term, then theta-bar^k
+    if (s.T > 0) k_skel_adj_ecorr<<<(s.T + 127) / 128, 128, 0, st>>>(sc->sd, sc->skd, sc->y.p, sc->gE.p);
+    k_skel_adj_theta<<<sc->sk_nq, kSkelAdjThreads, 0, st>>>(sc->skd, sc->kiter.p, sc->step.p, 0, 1, sc->xkb.p);
+  }
   k_adj_loop_ctl<<<1, 1, 0, st>>>(sc->kiter.p, h);
 }
 
 static void adj_post(dfem_scene* sc, cudaStream_t st) {
+  if (sc->skel_on) k_skel_adj_end<<<1, 64, 0, st>>>(sc->skd, sc->step.p, sc->xkb.p);
   k_adj_end<<<sc->nblk_v, 128, 0, st>>>(sc->sd, sc->xkb.p, sc->xtb.p, sc->bb.p, sc->io_a.p, sc->io_b.p);
 }
 
@@ -2274,6 +2320,25 @@ int dfem_get_joint_state(const dfem_scene* sc, double* jq, double* jqd) {
   return DFEM_OK;
 }
 
+int dfem_set_joint_state_grad(dfem_scene* sc, const double* gjq, const double* gjqd) {
+  if (!sc || !gjq || !gjqd) return fail(DFEM_ERR_INVALID, "null argument");
+  if (!sc->skel_on) return fail(DFEM_ERR_INVALID, "the scene has no skeleton");
+  const int nq = sc->sk_nq;
+  sc->sk_gout.assign(gjq, gjq + nq);
+  sc->sk_gout.insert(sc->sk_gout.end(), gjqd, gjqd + nq);
+  return DFEM_OK;
+}
+
+int dfem_get_joint_state_grad(const dfem_scene* sc, double* gjq, double* gjqd) {
+  if (!sc || !gjq || !gjqd) return fail(DFEM_ERR_INVALID, "null argument");
+  if (!sc->skel_on) return fail(DFEM_ERR_INVALID, "the scene has no skeleton");
+  CK(cudaSetDevice(sc->device));
+  CK(cudaStreamSynchronize(sc->stream));
+  CK(cudaMemcpy(gjq, sc->sk_gjq.p, sizeof(double) * sc->sk_nq, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(gjqd, sc->sk_gjqd.p, sizeof(double) * sc->sk_nq, cudaMemcpyDeviceToHost));
+  return DFEM_OK;
+}
+
 int dfem_set_activations(dfem_scene* sc, const double* act, int mem) {
   if (!sc || (!act && sc->hs.nseg > 0)) return fail(DFEM_ERR_INVALID, "null argument");
   CK(cudaSetDevice(sc->device));
@@ -2391,8 +2456,30 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
                        double* g_youngs, double* g_poisson, double* g_act, int mem) {
   if (!sc || !gx_out || !gv_out || !gx || !gv) return fail(DFEM_ERR_INVALID, "null argument");
   if (sc->rec_steps <= 0) return fail(DFEM_ERR_STATE, "dfem_step_backward needs a preceding dfem_step_forward");
-  if (sc->skel_on) return fail(DFEM_ERR_UNSUPPORTED, "no adjoint through skeleton links");
   CK(cudaSetDevice(sc->device));
+  const int nq = sc->sk_nq;
+  // the joint state a replayed step starts from (restored to the forward's final one at the end)
+  auto joint_state_at = [&](int st) -> int {
+    CK(cudaMemcpyAsync(sc->sk_jq.p, sc->sk_jin.p + 2 * (size_t)st * nq, nq * sizeof(double), cudaMemcpyDeviceToDevice,
+                       sc->stream));
+    CK(cudaMemcpyAsync(sc->sk_jqd.p, sc->sk_jin.p + (2 * (size_t)st + 1) * nq, nq * sizeof(double),
+                       cudaMemcpyDeviceToDevice, sc->stream));
+    return DFEM_OK;
+  };
+  if (sc->skel_on) {
+    CK(cudaMemcpyAsync(sc->sk_jfin.p, sc->sk_jq.p, nq * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaMemcpyAsync(sc->sk_jfin.p + nq, sc->sk_jqd.p, nq * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+    if (sc->sk_gout.size() == 2 * (size_t)nq) {
+      CK(cudaMemcpyAsync(sc->sk_gjq.p, sc->sk_gout.data(), nq * sizeof(double), cudaMemcpyHostToDevice, sc->stream));
+      CK(cudaMemcpyAsync(sc->sk_gjqd.p, sc->sk_gout.data() + nq, nq * sizeof(double), cudaMemcpyHostToDevice,
+                         sc->stream));
+      CK(cudaStreamSynchronize(sc->stream));  // the host vector is released below
+    } else {
+      CK(cudaMemsetAsync(sc->sk_gjq.p, 0, nq * sizeof(double), sc->stream));
+      CK(cudaMemsetAsync(sc->sk_gjqd.p, 0, nq * sizeof(double), sc->stream));
+    }
+    sc->sk_gout.clear();
+  }
   // contact steps the forward recorded need no replay; the others are replayed
   // with recording on, into records after the forward's (room for the most
   // loop-body executions of any of them)
@@ -2461,6 +2548,7 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
       CK(cudaMemcpyAsync(sc->vt.p, sc->ckpt_v.p + (size_t)(seg0 / kc) * n3, n3 * sizeof(double),
                          cudaMemcpyDeviceToDevice, sc->stream));
       if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 0);
+      if (sc->skel_on) RC(joint_state_at(seg0));
       for (int q = seg0; q < seg_end; ++q) {
         CK(cudaMemcpyAsync(sc->seg_x.p + (size_t)(q - seg0) * n3, sc->xt.p, n3 * sizeof(double),
                            cudaMemcpyDeviceToDevice, sc->stream));
@@ -2482,6 +2570,7 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
         // a contact step also records its contact iterations for the contact adjoint
         CK(cudaMemcpyAsync(sc->xt.p, sx(st), n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
         CK(cudaMemcpyAsync(sc->vt.p, sv(st), n3 * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+        if (sc->skel_on) RC(joint_state_at(st));
         k_set_int<<<1, 1, 0, sc->stream>>>(sc->step.p, st);
         CK(cudaGraphLaunch(sc->g_step.exec, sc->stream));
         rerun[st] += 1;
@@ -2511,6 +2600,10 @@ int dfem_step_backward(dfem_scene* sc, const double* gx_out, const double* gv_ou
     }
   }
   if (any_contact) k_set_int<<<1, 1, 0, sc->stream>>>(sc->crec_on.p, 0);
+  if (sc->skel_on) {
+    CK(cudaMemcpyAsync(sc->sk_jq.p, sc->sk_jfin.p, nq * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+    CK(cudaMemcpyAsync(sc->sk_jqd.p, sc->sk_jfin.p + nq, nq * sizeof(double), cudaMemcpyDeviceToDevice, sc->stream));
+  }
   sc->launches += 5;
   for (int st = 0; st < sc->rec_steps && st < (int)sc->rec_iters.size(); ++st)
     sc->launches += (int64_t)(1 + sc->g_adj.outside + (size_t)sc->rec_iters[st] * sc->g_adj.body);

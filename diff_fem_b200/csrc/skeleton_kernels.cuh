@@ -63,7 +63,38 @@ struct SkelDev {
   double* rhs;            // ndof
   double* sol;            // ndof
   int* perm;              // ndof column permutation of the LU
+  // history for the adjoint: per step and PD iteration k, the joint state
+  // theta^k (jq layout: the root's T, then one magnitude per link) | the link
+  // system's solution s^k | the multiplier q^k; per step its input (jq, jqd)
+  int nq, K;
+  long long hstride;      // nq + ndof + 3 nr
+  double* hist;           // steps x (K + 1) x hstride
+  double* jin;            // steps x 2 nq
+  // adjoint work
+  double* thb;            // nq: cotangent of the current theta
+  double* sb;             // ndof: cotangent of s
+  double* gjq;            // nq: cotangent of the step's output jq (input jq after the step's adjoint)
+  double* gjqd;           // nq: the same for jqd
+  double* mu2;            // 3 nr: rigid block of the KKT adjoint
+  double* mu3;            // ndof: link block of the KKT adjoint
+  double* dlt;            // 3 nr: linear rigid positions minus the iterate's
 };
+
+__device__ __forceinline__ double* sk_hrow(const SkelDev& k, int step, int it) {
+  return k.hist + ((long long)step * (k.K + 1) + it) * k.hstride;
+}
+
+// theta (jq layout) of the current link states, and back
+__device__ __forceinline__ void sk_pack(const SkelDev& k, int l, double* th) {
+  const SkelLink& lk = k.link[l];
+  const SkelState& s = k.st[l];
+  if (lk.type == DFEM_JOINT_ALL) {
+    for (int i = 0; i < 9; ++i) th[lk.sdof + i] = s.T.R[i];
+    for (int i = 0; i < 3; ++i) th[lk.sdof + 9 + i] = s.T.d[i];
+  } else {
+    th[lk.sdof] = s.mag;
+  }
+}
 
 // ---- 3x3 and transformation helpers (row-major R) ---------------------------
 __device__ __forceinline__ void sk_identity(SkelXf& t) {
@@ -240,62 +271,8 @@ __device__ __forceinline__ void sk_v0(const SkelDev& k, int j, double* o) {
   sk_apply(k.st[k.rlink[j]].M, v, o);
 }
 
-// Step start: Link::ReadT (the root's Tr = linearize(T), its value after the
-// previous step's last ComputeV0NTr), guessNext, ComputeV0NTr; the rigid
-// vertices of the first iterate are V0.  One block.
-__global__ void k_skel_begin(SkelDev k, double* xk) {
-  if (threadIdx.x == 0) {
-    for (int l = 0; l < k.L; ++l) {
-      const SkelLink& lk = k.link[l];
-      SkelState& s = k.st[l];
-      if (lk.type == DFEM_JOINT_ALL) {
-        for (int i = 0; i < 9; ++i) { s.T.R[i] = k.jq[lk.sdof + i]; s.prevTr.R[i] = k.jqd[lk.sdof + i]; }
-        for (int i = 0; i < 3; ++i) { s.T.d[i] = k.jq[lk.sdof + 9 + i]; s.prevTr.d[i] = k.jqd[lk.sdof + 9 + i]; }
-        s.Tr = sk_linearize(s.T);
-        // guessNext: T.d = 2 Tr.d - prevTr.d, T.R = Tr.R prevTr.R^-1 Tr.R, prevTr = Tr
-        for (int i = 0; i < 3; ++i) s.T.d[i] = 2.0 * s.Tr.d[i] - s.prevTr.d[i];
-        double A[9], B[9], X[9];
-        int cp[3];
-        for (int i = 0; i < 9; ++i) { A[i] = s.prevTr.R[i]; B[i] = s.Tr.R[i]; }
-        sk_fullpiv_small(3, 3, A, B, X, cp);
-        sk_mm(s.Tr.R, X, s.T.R);
-        s.prevTr = s.Tr;
-      } else {
-        s.mag = k.jq[lk.sdof];
-        s.prevmag = k.jqd[lk.sdof];
-        const double t = s.mag;
-        s.mag = 2.0 * s.mag - s.prevmag;
-        s.prevmag = t;
-      }
-      if (l == 0) sk_identity(s.prefix);
-      if (lk.type == DFEM_JOINT_PRISMATIC) {  // Tr.R of a prismatic link stays the identity
-        for (int i = 0; i < 9; ++i) s.Tr.R[i] = (i % 4 == 0) ? 1.0 : 0.0;
-      }
-    }
-    sk_kinematics(k);
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < k.nr; j += blockDim.x) {
-    double p[3];
-    sk_v0(k, j, p);
-    const int v = k.rv[j];
-    for (int c = 0; c < 3; ++c) { k.v0[3 * j + c] = p[c]; xk[3 * (size_t)v + c] = p[c]; }
-  }
-}
-
-// One PD iteration's rigid stage (one block), after the solve wrote
-// z = u - x_t: the link system, the multiplier q, UpdateT and the new V0
-// (z of the rigid vertices becomes V0 - x_t).
-__global__ void k_skel_stage(SkelDev k, const double* xt, double* z, const double* act_all, const int* step,
-                             int nseg) {
-  const int tid = threadIdx.x, nt = blockDim.x, nr = k.nr, nd = k.ndof;
-  // u_R - V0
-  for (int e = tid; e < 3 * nr; e += nt) {
-    const int j = e / 3, c = e % 3;
-    const size_t g = 3 * (size_t)k.rv[j] + c;
-    k.w[e] = (xt[g] + z[g]) - k.v0[e];
-  }
-  // dT of every rotational / prismatic link (ComputeTildaV)
+// dT of every rotational / prismatic link (ComputeTildaV), threads over links
+__device__ void sk_dt(const SkelDev& k, int tid, int nt) {
   for (int l = tid; l < k.L; l += nt) {
     const SkelLink& lk = k.link[l];
     SkelState& s = k.st[l];
@@ -307,8 +284,12 @@ __global__ void k_skel_stage(SkelDev k, const double* xt, double* z, const doubl
       for (int i = 0; i < 3; ++i) s.dT.d[i] = lk.axis[i];
     }
   }
-  __syncthreads();
-  // tildaV: one rigid vertex per thread, walking its chain to the root
+}
+
+// tildaV (Link::ComputeTildaV): one rigid vertex per thread, walking its chain
+// to the root (V0 of the current links in k.v0)
+__device__ void sk_tildav(const SkelDev& k, int tid, int nt) {
+  const int nr = k.nr, nd = k.ndof;
   for (int j = tid; j < nr; j += nt) {
     double* row0 = k.tv + (3 * (size_t)j) * nd;
     double* row1 = row0 + nd;
@@ -344,8 +325,11 @@ __global__ void k_skel_stage(SkelDev k, const double* xt, double* z, const doubl
     row2[c0 + 0] = vy;  row2[c0 + 1] = -vx;
     row0[c0 + 3] = 1.0; row1[c0 + 4] = 1.0; row2[c0 + 5] = 1.0;
   }
-  __syncthreads();
-  // rr = C^-1 (u_R - V0) and kt = C^-1 tildaV, per component
+}
+
+// rr = C^-1 (u_R - V0) and kt = C^-1 tildaV, per component
+__device__ void sk_cinv_products(const SkelDev& k, int tid, int nt) {
+  const int nr = k.nr, nd = k.ndof;
   for (int e = tid; e < 3 * nr; e += nt) {
     const int i = e / 3, c = e % 3;
     double acc = 0.0;
@@ -358,6 +342,87 @@ __global__ void k_skel_stage(SkelDev k, const double* xt, double* z, const doubl
     for (int j = 0; j < nr; ++j) acc += k.cinv[(size_t)i * nr + j] * k.tv[(3 * (size_t)j + c) * nd + a];
     k.kt[e] = acc;
   }
+}
+
+// Step start: Link::ReadT (the root's Tr = linearize(T), its value after the
+// previous step's last ComputeV0NTr), guessNext, ComputeV0NTr; the rigid
+// vertices of the first iterate are V0 (also in the stored iterate 0).  The
+// step's input joint state and theta^0 go to the adjoint's history.  One block.
+__global__ void k_skel_begin(SkelDev k, double* xk, const int* step, double* hist_x, long long hist_step) {
+  const int st = *step;
+  if (k.jin)
+    for (int i = threadIdx.x; i < k.nq; i += blockDim.x) {
+      k.jin[2 * (size_t)st * k.nq + i] = k.jq[i];
+      k.jin[(2 * (size_t)st + 1) * k.nq + i] = k.jqd[i];
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int l = 0; l < k.L; ++l) {
+      const SkelLink& lk = k.link[l];
+      SkelState& s = k.st[l];
+      if (lk.type == DFEM_JOINT_ALL) {
+        for (int i = 0; i < 9; ++i) { s.T.R[i] = k.jq[lk.sdof + i]; s.prevTr.R[i] = k.jqd[lk.sdof + i]; }
+        for (int i = 0; i < 3; ++i) { s.T.d[i] = k.jq[lk.sdof + 9 + i]; s.prevTr.d[i] = k.jqd[lk.sdof + 9 + i]; }
+        s.Tr = sk_linearize(s.T);
+        // guessNext: T.d = 2 Tr.d - prevTr.d, T.R = Tr.R prevTr.R^-1 Tr.R, prevTr = Tr
+        for (int i = 0; i < 3; ++i) s.T.d[i] = 2.0 * s.Tr.d[i] - s.prevTr.d[i];
+        double A[9], B[9], X[9];
+        int cp[3];
+        for (int i = 0; i < 9; ++i) { A[i] = s.prevTr.R[i]; B[i] = s.Tr.R[i]; }
+        sk_fullpiv_small(3, 3, A, B, X, cp);
+        sk_mm(s.Tr.R, X, s.T.R);
+        s.prevTr = s.Tr;
+      } else {
+        s.mag = k.jq[lk.sdof];
+        s.prevmag = k.jqd[lk.sdof];
+        const double t = s.mag;
+        s.mag = 2.0 * s.mag - s.prevmag;
+        s.prevmag = t;
+      }
+      if (l == 0) sk_identity(s.prefix);
+      if (lk.type == DFEM_JOINT_PRISMATIC) {  // Tr.R of a prismatic link stays the identity
+        for (int i = 0; i < 9; ++i) s.Tr.R[i] = (i % 4 == 0) ? 1.0 : 0.0;
+      }
+    }
+    sk_kinematics(k);
+  }
+  __syncthreads();
+  if (k.hist)
+    for (int l = threadIdx.x; l < k.L; l += blockDim.x) sk_pack(k, l, sk_hrow(k, st, 0));
+  double* hx = hist_x ? hist_x + (size_t)st * hist_step : nullptr;
+  for (int j = threadIdx.x; j < k.nr; j += blockDim.x) {
+    double p[3];
+    sk_v0(k, j, p);
+    const int v = k.rv[j];
+    for (int c = 0; c < 3; ++c) {
+      k.v0[3 * j + c] = p[c];
+      xk[3 * (size_t)v + c] = p[c];
+      if (hx) hx[3 * (size_t)v + c] = p[c];
+    }
+  }
+}
+
+// One PD iteration's rigid stage (one block), after the solve wrote
+// z = u - x_t: the link system, the multiplier q, UpdateT and the new V0
+// (z of the rigid vertices becomes V0 - x_t).  s, q and the new theta of
+// iteration k (*kptr) go to the adjoint's history.
+__global__ void k_skel_stage(SkelDev k, const double* xt, double* z, const double* act_all, const int* step,
+                             int nseg, const int* kptr) {
+  const int tid = threadIdx.x, nt = blockDim.x, nr = k.nr, nd = k.ndof;
+  const int it = *kptr;
+  double* h0 = k.hist ? sk_hrow(k, *step, it) : nullptr;
+  double* h1 = k.hist ? sk_hrow(k, *step, it + 1) : nullptr;
+  // u_R - V0
+  for (int e = tid; e < 3 * nr; e += nt) {
+    const int j = e / 3, c = e % 3;
+    const size_t g = 3 * (size_t)k.rv[j] + c;
+    k.w[e] = (xt[g] + z[g]) - k.v0[e];
+  }
+  sk_dt(k, tid, nt);
+  __syncthreads();
+  sk_tildav(k, tid, nt);
+  __syncthreads();
+  sk_cinv_products(k, tid, nt);
   __syncthreads();
   // S = tildaV^T C^-1 tildaV and tmp = tildaV^T rr + tau (mcs[6+i] += mJointTorque[i])
   for (int e = tid; e < nd * nd; e += nt) {
@@ -388,7 +453,10 @@ __global__ void k_skel_stage(SkelDev k, const double* xt, double* z, const doubl
     double acc = 0.0;
     for (int j = 0; j < nr; ++j) acc += k.cinv[(size_t)i * nr + j] * k.rr[3 * j + c];
     k.q[e] = acc;
+    if (h0) h0[k.nq + nd + e] = acc;
   }
+  if (h0)
+    for (int a = tid; a < nd; a += nt) h0[k.nq + a] = k.sol[a];
   // Link::UpdateT
   for (int l = tid; l < k.L; l += nt) {
     const SkelLink& lk = k.link[l];
@@ -406,6 +474,7 @@ __global__ void k_skel_stage(SkelDev k, const double* xt, double* z, const doubl
       sk_mv(t, s.Tr.d, td);
       for (int i = 0; i < 3; ++i) s.T.d[i] = td[i] + sv[3 + i];
     }
+    if (h1) sk_pack(k, l, h1);
   }
   __syncthreads();
   if (tid == 0) sk_kinematics(k);

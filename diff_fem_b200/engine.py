@@ -175,8 +175,19 @@ class Scene:
         self._last_steps = n_steps
         return (xo, vo, tr) if traj else (xo, vo)
 
-    def backward(self, gx, gv):
-        """VJP of the last forward call.  Returns dict with x, v, E, nu, act."""
+    def backward(self, gx, gv, gjq=None, gjqd=None):
+        """VJP of the last forward call.  Returns dict with x, v, E, nu, act;
+        with a skeleton also jq, jqd (the gradient w.r.t. the joint state the
+        forward started from; gjq / gjqd: cotangents of its end state, zero
+        when omitted)."""
+        nq = self.n_joint_state
+        if nq and (gjq is not None or gjqd is not None):
+            a = np.zeros(nq) if gjq is None else np.ascontiguousarray(gjq, np.float64).reshape(-1)
+            b = np.zeros(nq) if gjqd is None else np.ascontiguousarray(gjqd, np.float64).reshape(-1)
+            if a.size != nq or b.size != nq:
+                raise ValueError(f"joint state cotangents need {nq} values each")
+            P = lambda t: t.ctypes.data_as(C.POINTER(C.c_double))
+            check(lib().dfem_set_joint_state_grad(self._h, P(a), P(b)))
         dev = _is_cuda_tensor(gx)
         n3 = 3 * self.N
         if dev:
@@ -192,7 +203,13 @@ class Scene:
         check(lib().dfem_step_backward(self._h, p[0], p[1], p[2], p[3], p[4], p[5], p[6] if self.nseg else None, mem))
         act = ga[: self._last_steps * self.nseg]
         act = act.reshape(self._last_steps, self.nseg)
-        return {"x": ox, "v": ov, "E": gE[: self.T], "nu": gnu[: self.T], "act": act}
+        out = {"x": ox, "v": ov, "E": gE[: self.T], "nu": gnu[: self.T], "act": act}
+        if nq:
+            ja, jb = np.zeros(nq), np.zeros(nq)
+            P = lambda t: t.ctypes.data_as(C.POINTER(C.c_double))
+            check(lib().dfem_get_joint_state_grad(self._h, P(ja), P(jb)))
+            out["jq"], out["jqd"] = ja, jb
+        return out
 
     def eval_local(self, x):
         """J d(x): the local step's contribution to the global rhs at positions x."""

@@ -13,8 +13,9 @@ Same functions, argument order and meaning as the reference's pybind11 module
 
 Differences: values are FP64 numpy arrays (the reference returns float lists
 that api_diff.py truncates to float32); gradients come from the engine's
-adjoint instead of a CppAD tape; the joint state (jq, jqd) of an articulated
-skeleton is stepped forward (backward_act through links is not supported).  The actuator front-end of type 2 (muscles:
+adjoint instead of a CppAD tape, through an articulated skeleton's links too
+(djq, djqd from dldjq, dldjqd; the joint torques of actuator type 1 in
+dtau).  The actuator front-end of type 2 (muscles:
 Normalizer::NormToReal, Muscle::SetActivationLevels with the SetKey table,
 sim/Normalizer.h:94-112, sim/Muscle.h:224-261, sim/Dfobj.h:628-667) is
 evaluated with torch so that dL/dtau follows from the engine's dL/d(activation);
@@ -285,13 +286,16 @@ def _backward_act(q, qd, jq, jqd, tau, dldq, dldqd, dldjq, dldjqd, env: Environm
     _set_joints(env, jq, jqd)
     env.scene.forward(np.asarray(q, np.float64), np.asarray(qd, np.float64), n_steps=1,
                       act=act_np.reshape(1, -1) if act_np.size else None)
-    g = env.scene.backward(np.asarray(dldq, np.float64), np.asarray(dldqd, np.float64))
+    nq = env.scene.n_joint_state
+    gj = (np.asarray(dldjq, np.float64).reshape(-1), np.asarray(dldjqd, np.float64).reshape(-1)) \
+        if nq and np.asarray(dldjq).size else (None, None)
+    g = env.scene.backward(np.asarray(dldq, np.float64), np.asarray(dldqd, np.float64), *gj)
     dtau = np.zeros(len(tau))
     if is_act and chan.requires_grad and g["act"].size:
         (gt,) = torch.autograd.grad(chan, tau_t, torch.as_tensor(g["act"][0]), allow_unused=True)
         if gt is not None:
             dtau = gt.numpy()
-    return [g["x"], g["v"], np.zeros(0), np.zeros(0), dtau]
+    return [g["x"], g["v"], g.get("jq", np.zeros(0)), g.get("jqd", np.zeros(0)), dtau]
 
 
 def forward_all(q, qd, tau, env: Environment, write_obj: Optional[str] = None):

@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define DFEM_ABI_VERSION 5
+#define DFEM_ABI_VERSION 6
 
 enum dfem_status {
   DFEM_OK = 0,
@@ -148,8 +148,9 @@ typedef struct dfem_scene_desc {
    * DFEM_JOINT_PRISMATIC: a distance along it).  The vertices of a link move
    * rigidly with it; the other vertices are solved with the links through
    * the Schur complement of World::ComputeSolution (World.h:1600-1670).
-   * Single FP64 scenes without contact; no adjoint (dfem_step_backward
-   * returns DFEM_ERR_UNSUPPORTED). */
+   * Single FP64 scenes without contact.  dfem_step_backward differentiates
+   * through the links too: dfem_set_joint_state_grad /
+   * dfem_get_joint_state_grad carry the joint state's cotangents. */
   int32_t n_links;
   const int32_t *link_parent;     /* parent link, -1 for link 0                       */
   const int32_t *link_type;       /* enum dfem_joint                                  */
@@ -221,6 +222,15 @@ int dfem_set_activations(dfem_scene *scene, const double *activations, int mem);
  * scene starts from the identity and zero magnitudes. */
 int dfem_set_joint_state(dfem_scene *scene, const double *jq, const double *jqd);
 int dfem_get_joint_state(const dfem_scene *scene, double *jq, double *jqd);
+
+/* Cotangents dL/djq, dL/djqd of the joint state after the last forward's
+ * final step, for the next dfem_step_backward only (without this call they
+ * are zero); after it, dfem_get_joint_state_grad reads dL/djq, dL/djqd of the
+ * joint state the forward started from.  The dldjq / dldjqd inputs and the
+ * ansjq / ansjqd outputs of backward_act (python/pydifem.cc:91-180).  The
+ * joint torques' gradient is the one of their activation channels. */
+int dfem_set_joint_state_grad(dfem_scene *scene, const double *gjq, const double *gjqd);
+int dfem_get_joint_state_grad(const dfem_scene *scene, double *gjq, double *gjqd);
 
 /* Run n_steps time steps from (x, v); writes the final state, and optionally
  * every step's positions to traj_x ((n_steps) * 3N, may be NULL).

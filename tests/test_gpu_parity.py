@@ -589,7 +589,7 @@ def test_skeleton_forward_matches_oracle(case):
     (two Qf solves, the precomputed Qb_M - Qc_L Qf^-1 Qc_L^T); the engine uses
     the equivalent multiplier form on the step's full solve.  A second call
     continues from the joint state the first left; set_joint_state restarts
-    from a given state; the adjoint is refused."""
+    from a given state."""
     import os
     rng = np.random.default_rng(31)
     if case == "articulated_beam":
@@ -621,7 +621,106 @@ def test_skeleton_forward_matches_oracle(case):
     xg3, _ = g.forward(ro["x"], ro["v"], n_steps=2, act=act[:2])
     ro3 = o.forward(ro["x"], ro["v"], n_steps=2, act=act[:2])
     assert rel(xg3, ro3["x"]) < POS_TOL
-    with pytest.raises(_capi.DfemError) as ex:
-        g.backward(np.ones_like(x), np.ones_like(x))
-    assert ex.value.code == _capi.DFEM_ERR_UNSUPPORTED
     g.close()
+
+
+def _skeleton_case(name):
+    """A skeleton scene at a fixed PD iteration count (the count then cannot
+    change under the finite-difference perturbations), its start state a few
+    steps in (rotated root, moved joints) and per-step torque activations."""
+    import os
+    rng = np.random.default_rng(41)
+    if name == "articulated_beam":
+        d = dataclasses.replace(S.articulated_beam(), max_iterations=6)
+        act0 = np.tile([0.5, 2.0], (4, 1))
+        n = 3
+    else:
+        d = S.load_npz(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_scenes",
+                                    "baymax_skeleton.npz"))
+        d = dataclasses.replace(d, max_iterations=5)
+        act0 = rng.uniform(-20.0, 20.0, (4, d.n_segments))
+        n = 2
+    o = O.OracleScene(d)
+    x = d.x0.reshape(-1).copy()
+    v = np.tile([0.2, 0.1, -0.1], d.n_vertices)
+    r0 = o.forward(x, v, n_steps=4, act=act0)
+    jq, jqd = o.joint_state()
+    act = (act0[:n] if act0.shape[0] >= n else act0) * rng.uniform(0.7, 1.3, (n, d.n_segments))
+    return d, o, r0["x"], r0["v"], jq, jqd, act, n
+
+
+@pytest.mark.parametrize("case", ["articulated_beam", "baymax_skeleton"])
+def test_skeleton_adjoint_matches_oracle_finite_differences(case):
+    """The adjoint through the links (backward_act's dq, dqd, djq, djqd and the
+    joint torques' dtau, CppAD in the reference): every gradient against
+    central differences of the oracle's forward along random directions of x,
+    v, the joint state (jq, jqd; the root's T need not be a rotation), the
+    torque activations and Young's moduli, for L = gx.x' + gv.v' + gjq.jq' +
+    gjqd.jqd' after n steps."""
+    d, o, x, v, jq, jqd, act, n = _skeleton_case(case)
+    rng = np.random.default_rng(43)
+    n3 = x.size
+    nq = jq.size
+    gx, gv = rng.standard_normal(n3), rng.standard_normal(n3)
+    gjq, gjqd = rng.standard_normal(nq), rng.standard_normal(nq)
+    E0 = np.asarray(d.youngs, np.float64).copy()
+    nu0 = np.asarray(d.poisson, np.float64).copy()
+    g = Scene(d)
+    g.set_joint_state(jq, jqd)
+    xg, vg = g.forward(x, v, n_steps=n, act=act)
+    assert np.all(g.iterations(n) == d.max_iterations)
+    jg, jdg = g.joint_state()
+    grad = g.backward(gx, gv, gjq, gjqd)
+    jg2, jdg2 = g.joint_state()  # the backward leaves the forward's final joint state
+    assert np.array_equal(jg, jg2) and np.array_equal(jdg, jdg2)
+
+    def loss(xx, vv, q, qd, aa, E):
+        o.set_materials(E, nu0)
+        o.set_joint_state(q, qd)
+        r = o.forward(xx, vv, n_steps=n, act=aa)
+        assert np.all(r["iters"] == d.max_iterations)
+        q1, qd1 = o.joint_state()
+        return gx @ r["x"] + gv @ r["v"] + gjq @ q1 + gjqd @ qd1
+
+    base = dict(xx=x, vv=v, q=jq, qd=jqd, aa=act, E=E0)
+    dirs = {
+        "x": ("xx", 1e-3 * rng.standard_normal(n3)),
+        "v": ("vv", 1e-2 * rng.standard_normal(n3)),
+        "jq": ("q", 1e-3 * rng.standard_normal(nq)),
+        "jqd": ("qd", 1e-3 * rng.standard_normal(nq)),
+        "act": ("aa", 1e-2 * np.abs(act).max(initial=1.0) * rng.standard_normal(act.shape)),
+        "E": ("E", 1e-3 * E0 * rng.standard_normal(E0.size)),
+    }
+    for key, (arg, dirn) in dirs.items():
+        h = 1e-3
+        lp = loss(**{**base, arg: base[arg] + h * dirn})
+        lm = loss(**{**base, arg: base[arg] - h * dirn})
+        fd = (lp - lm) / (2 * h)
+        an = float(np.sum(np.asarray(grad[key]).reshape(-1) * dirn.reshape(-1)))
+        assert abs(fd - an) <= 1e-5 * max(abs(fd), abs(an)) + 1e-9, (key, fd, an)
+        assert abs(an) > 1e-6, (key, an)  # each direction moves the loss
+    g.close()
+
+
+def test_skeleton_adjoint_replays_and_checkpoints_are_identical():
+    """With every step replayed from its checkpoint (no stored iterates) and
+    with checkpoints every second step, the replays restart the links from
+    each step's stored input joint state: the same gradients, bit for bit."""
+    d, o, x, v, jq, jqd, act, n = _skeleton_case("articulated_beam")
+    n = 5
+    act = np.tile(act[:1], (n, 1))
+    rng = np.random.default_rng(44)
+    gx, gv = rng.standard_normal(x.size), rng.standard_normal(x.size)
+    gjq, gjqd = rng.standard_normal(jq.size), rng.standard_normal(jq.size)
+    out = []
+    for every, budget in ((1, None), (1, 0), (2, None), (2, 0)):
+        g = Scene(dataclasses.replace(d, checkpoint_every=every))
+        if budget is not None:
+            g.set_adjoint_budget(budget)
+        g.set_joint_state(jq, jqd)
+        g.forward(x, v, n_steps=n, act=act)
+        out.append(g.backward(gx, gv, gjq, gjqd))
+        g.close()
+    for r in out[1:]:
+        for key in ("x", "v", "E", "nu", "act", "jq", "jqd"):
+            assert np.array_equal(out[0][key], r[key]), key

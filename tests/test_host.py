@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
     assert len(names) >= 10
     for n in names:
         assert hasattr(lib, n), n
-    assert lib.dfem_abi_version() == 5
+    assert lib.dfem_abi_version() == 6
 
 
 def test_ctypes_descriptor_matches_header():

@@ -159,6 +159,7 @@ def test_skeleton_joint_state_through_forward_act(tmp_path):
          "Vertices": mid},
     ]
     src["Parameters"][0]["Handle collision"] = False
+    src["Parameters"][0]["Max Iteration"] = 4  # reached in every step: a fixed map for the differences below
     src.pop("Obstacles")
     path = tmp_path / "bones.json"
     path.write_text(json.dumps(src))
@@ -178,6 +179,36 @@ def test_skeleton_joint_state_through_forward_act(tmp_path):
         assert np.abs(jq2 - jo).max() < 1e-9 and np.abs(jqd2 - jdo).max() < 1e-9
         q, qd, jq, jqd = q2, qd2, jq2, jqd2
     assert abs(jq[12]) > 1e-4
+    # backward_act through the links: dq, djq, djqd and the torque's dtau
+    # against central differences of the oracle's step (fixed iteration count
+    # of the scene: max_iterations is reached in every step here)
+    rng = np.random.default_rng(5)
+    n3, nq = q.size, jq.size
+    dldq, dldqd = rng.standard_normal(n3), rng.standard_normal(n3)
+    dldjq, dldjqd = rng.standard_normal(nq), rng.standard_normal(nq)
+    tau = np.array([0.7])
+    env.mPhase = 0
+    dq, dqd, djq, djqd, dtau = pd.backward_act(q, qd, jq, jqd, tau, dldq, dldqd, dldjq, dldjqd, env, True)
+    assert djq.size == nq and djqd.size == nq and dtau.size == 1
+
+    def loss(qq, qqd, a, b, t):
+        o.set_joint_state(a, b)
+        r = o.forward(qq, qqd, n_steps=1, act=np.reshape(t, (1, 1)))
+        ja, jb = o.joint_state()
+        return dldq @ r["x"] + dldqd @ r["v"] + dldjq @ ja + dldjqd @ jb, r["iters"]
+
+    _, iters = loss(q, qd, jq, jqd, tau)
+    assert iters[0] == 4
+    h = 1e-6
+    args = (q, qd, jq, jqd, tau)
+    for name, grad, k in (("q", dq, 0), ("qd", dqd, 1), ("jq", djq, 2), ("jqd", djqd, 3), ("tau", dtau, 4)):
+        dirn = rng.standard_normal(np.size(args[k]))
+        ap, am = list(args), list(args)
+        ap[k] = np.asarray(args[k], np.float64) + h * dirn.reshape(np.shape(args[k]))
+        am[k] = np.asarray(args[k], np.float64) - h * dirn.reshape(np.shape(args[k]))
+        fd = (loss(*ap)[0] - loss(*am)[0]) / (2 * h)
+        an = float(np.asarray(grad).reshape(-1) @ dirn)
+        assert abs(fd - an) <= 1e-5 * max(abs(fd), abs(an)) + 1e-8, (name, fd, an)
 
 
 def test_save_obj_from_device_and_host_states(env, tmp_path):
