@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdfem.so")
 SOURCES = ["engine.cu", "noalloc.cu", "scene.cpp", "cholesky.cpp", "resident_plan.cpp", "obj_writer.cpp"]
 HEADERS = ["pd_kernels.cu", "pd_math.cuh", "kernels.cuh", "factor_kernels.cuh", "contact_kernels.cuh", "tma.cuh",
-           "resident_solve.cuh", "drag_kernels.cuh", "skeleton_kernels.cuh", "skeleton_adjoint.cuh",
+           "resident_solve.cuh", "drag_kernels.cuh", "skeleton_kernels.cuh", "skeleton_adjoint.cuh", "dense_solve.cuh",
            "scene.h", "cholesky.h", "resident_plan.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

@@ -1,0 +1,241 @@
+// Dense-inverse form of the global solve, for single scenes small enough that
+// X = Hs^-1 (N x N, FP64) fits comfortably in HBM (and mostly in L2).  Each
+// solve is then one matrix-vector product over three right-hand sides, a
+// stream of N^2 doubles with no dependency chain, instead of the 2 x levels
+// dependent steps of the supernodal triangular solves.
+//
+// X is rebuilt from the GPU supernodal factor after every refactorisation:
+//   1. the factor L (its diagonal blocks L_ss, kept by k_factor_level, and the
+//      panels L_{R,s}) scattered into a dense lower-triangular N_p x N_p matrix
+//      (N_p = N rounded up to 64; the padding is the identity),
+//   2. the inverses of its 64 x 64 diagonal tiles (all tiles at once),
+//   3. W = L^-1 tile column by tile column, last to first (LAPACK's blocked
+//      triangular inverse): W_Ij = -(sum_{K=j+1..I} W_IK L_Kj) W_jj,
+//   4. X = W^T W (lower tiles, mirrored: X is exactly symmetric).
+// Products of 64 x 64 tiles run on the FP64 tensor cores (mma.sync m8n8k4)
+// from shared memory in a fixed order, so X and every solve are
+// deterministic.  The solve's result agrees with the triangular solves'
+// to rounding (the same factor, applied as one inverse).
+#pragma once
+
+// (included by engine.cu after pd_kernels.cu: warp_sum, Gate, SnInfo, FactorDev)
+#include "factor_kernels.cuh"
+
+namespace dfem {
+
+constexpr int kDenseTile = 64;
+constexpr int kDenseLd = kDenseTile + 1;  // padded shared-memory row (doubles)
+constexpr size_t kDenseSmem = 2 * (size_t)kDenseTile * kDenseLd * sizeof(double);
+
+struct DenseDev {
+  int N, Np, nb;        // vertices, padded size, tiles per side
+  double* A;            // N_p x N_p row-major: L, then X
+  double* W;            // N_p x N_p row-major: L^-1 (lower tiles)
+  double* Linv;         // nb x 64 x 64 row-major: inverses of L's diagonal tiles
+};
+
+// P (64 x 64, [row][k]) times Q^T (Q [col][k]) added to the warp's eight 8x8
+// output tiles: warp w holds rows 8w .. 8w+7, tile t columns 8t .. 8t+7;
+// d[t][i] is row 8w + (lane >> 2), column 8t + 2 (lane & 3) + i.
+__device__ __forceinline__ void dense_mma(const double* P, const double* Q, double d[8][2]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const double* pa = P + (8 * w + (lane >> 2)) * kDenseLd + (lane & 3);
+  const double* qb = Q + (lane >> 2) * kDenseLd + (lane & 3);
+#pragma unroll 4
+  for (int k0 = 0; k0 < kDenseTile; k0 += 4) {
+    const double a = pa[k0];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) dmma_8x8x4(d[t][0], d[t][1], a, qb[8 * t * kDenseLd + k0]);
+  }
+}
+
+// tile (I, J) of a row-major N_p x N_p matrix into shared memory, as stored or transposed
+__device__ __forceinline__ void dense_load(const double* M, int Np, int I, int J, bool trans, double* S) {
+  const double* src = M + (size_t)I * kDenseTile * Np + (size_t)J * kDenseTile;
+  for (int q = threadIdx.x; q < kDenseTile * kDenseTile; q += blockDim.x) {
+    const int r = q / kDenseTile, c = q % kDenseTile;  // coalesced along rows of M
+    const double v = src[(size_t)r * Np + c];
+    if (trans) S[c * kDenseLd + r] = v; else S[r * kDenseLd + c] = v;
+  }
+}
+
+__device__ __forceinline__ void dense_zero(double d[8][2]) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t) d[t][0] = d[t][1] = 0.0;
+}
+
+// the warp's output tiles to shared memory ([row][col]), scaled by s
+__device__ __forceinline__ void dense_store_sh(const double d[8][2], double s, double* S) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int r = 8 * w + (lane >> 2);
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int c = 8 * t + 2 * (lane & 3);
+    S[r * kDenseLd + c] = s * d[t][0];
+    S[r * kDenseLd + c + 1] = s * d[t][1];
+  }
+}
+
+// 1. the supernodal factor into the dense lower triangle (A zeroed before):
+// one CTA per supernode; the padding rows get a unit diagonal
+__global__ void k_dense_scatter(DenseDev dd, FactorDev f, const double* __restrict__ Ldw,
+                                const int* __restrict__ sn_dofs) {
+  const int s = blockIdx.x;
+  if (s == 0)
+    for (int i = dd.N + threadIdx.x; i < dd.Np; i += blockDim.x) dd.A[(size_t)i * dd.Np + i] = 1.0;
+  const SnInfo in = f.info[s];
+  const int c0 = in.c0, w = in.w, r = in.r;
+  const double* Ld = Ldw + sn_dofs[in.s];
+  const double* Lc = f.Lcm + in.lofs;
+  const int* R = f.rowidx + in.rofs;
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
+    const int i = q % w, c = q / w;
+    if (i >= c) dd.A[(size_t)(c0 + i) * dd.Np + c0 + c] = Ld[i + c * w];
+  }
+  for (int q = threadIdx.x; q < r * w; q += blockDim.x) {
+    const int a = q % r, c = q / r;
+    dd.A[(size_t)R[a] * dd.Np + c0 + c] = Lc[(size_t)c * r + a];
+  }
+}
+
+// 2. inverse of diagonal tile J of L (lower triangular; one column per
+// thread, forward substitution), to Linv and as W_JJ
+__global__ void __launch_bounds__(256) k_dense_tile_inv(DenseDev dd) {
+  extern __shared__ __align__(16) double dsh[];
+  double* S = dsh;
+  double* X = dsh + kDenseTile * kDenseLd;
+  const int J = blockIdx.x;
+  dense_load(dd.A, dd.Np, J, J, false, S);
+  __syncthreads();
+  const int c = threadIdx.x;
+  if (c < kDenseTile) {
+    for (int i = 0; i < c; ++i) X[i * kDenseLd + c] = 0.0;
+    for (int i = c; i < kDenseTile; ++i) {
+      double v = (i == c) ? 1.0 : 0.0;
+      for (int k = c; k < i; ++k) v -= S[i * kDenseLd + k] * X[k * kDenseLd + c];
+      X[i * kDenseLd + c] = v / S[i * kDenseLd + i];
+    }
+  }
+  __syncthreads();
+  double* Li = dd.Linv + (size_t)J * kDenseTile * kDenseTile;
+  double* Wd = dd.W + (size_t)J * kDenseTile * dd.Np + (size_t)J * kDenseTile;
+  for (int q = threadIdx.x; q < kDenseTile * kDenseTile; q += blockDim.x) {
+    const int r = q / kDenseTile, cc = q % kDenseTile;
+    const double v = X[r * kDenseLd + cc];
+    Li[q] = v;
+    Wd[(size_t)r * dd.Np + cc] = v;
+  }
+}
+
+// 3. tile column j of W = L^-1 (tiles I > j, one per CTA):
+//    T = sum_{K=j+1..I} W_IK L_Kj, then W_Ij = -T W_jj.
+__global__ void __launch_bounds__(256) k_dense_trtri(DenseDev dd, int j) {
+  extern __shared__ __align__(16) double dsh[];
+  double* P = dsh;
+  double* Q = dsh + kDenseTile * kDenseLd;
+  const int I = j + 1 + blockIdx.x;
+  double d[8][2];
+  dense_zero(d);
+  for (int K = j + 1; K <= I; ++K) {
+    dense_load(dd.W, dd.Np, I, K, false, P);  // W_IK [row][k]
+    dense_load(dd.A, dd.Np, K, j, true, Q);   // L_Kj as [col][k]
+    __syncthreads();
+    dense_mma(P, Q, d);
+    __syncthreads();
+  }
+  dense_store_sh(d, -1.0, P);  // -T [row][k]
+  {
+    const double* Li = dd.Linv + (size_t)j * kDenseTile * kDenseTile;  // W_jj [k][col] -> Q [col][k]
+    for (int q = threadIdx.x; q < kDenseTile * kDenseTile; q += blockDim.x) {
+      const int k = q / kDenseTile, c = q % kDenseTile;
+      Q[c * kDenseLd + k] = Li[q];
+    }
+  }
+  __syncthreads();
+  dense_zero(d);
+  dense_mma(P, Q, d);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* Wt = dd.W + (size_t)I * kDenseTile * dd.Np + (size_t)j * kDenseTile;
+  const int r = 8 * w + (lane >> 2);
+#pragma unroll
+  for (int t = 0; t < 8; ++t) {
+    const int c = 8 * t + 2 * (lane & 3);
+    Wt[(size_t)r * dd.Np + c] = d[t][0];
+    Wt[(size_t)r * dd.Np + c + 1] = d[t][1];
+  }
+}
+
+// 4. X = W^T W: tile (I, J), I >= J, sum over K = I .. nb-1 of W_KI^T W_KJ;
+// written to (I, J) and transposed to (J, I)
+__global__ void __launch_bounds__(256) k_dense_lauum(DenseDev dd) {
+  extern __shared__ __align__(16) double dsh[];
+  double* P = dsh;
+  double* Q = dsh + kDenseTile * kDenseLd;
+  const int b = blockIdx.x;
+  int I = (int)((sqrt(8.0 * b + 1.0) - 1.0) * 0.5);
+  while ((I + 1) * (I + 2) / 2 <= b) ++I;
+  while (I * (I + 1) / 2 > b) --I;
+  const int J = b - I * (I + 1) / 2;
+  double d[8][2];
+  dense_zero(d);
+  for (int K = I; K < dd.nb; ++K) {
+    dense_load(dd.W, dd.Np, K, I, true, P);  // W_KI as [row i][k]
+    dense_load(dd.W, dd.Np, K, J, true, Q);  // W_KJ as [col j][k]
+    __syncthreads();
+    dense_mma(P, Q, d);
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* Xa = dd.A + (size_t)I * kDenseTile * dd.Np + (size_t)J * kDenseTile;
+  double* Xb = dd.A + (size_t)J * kDenseTile * dd.Np + (size_t)I * kDenseTile;
+  const int r = 8 * w + (lane >> 2);
+#pragma unroll
+  for (int t = 0; t < 8; ++t)
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const int c = 8 * t + 2 * (lane & 3) + e;
+      if (I == J && r < c) continue;  // a diagonal tile is defined by its lower triangle
+      Xa[(size_t)r * dd.Np + c] = d[t][e];
+      Xb[(size_t)c * dd.Np + r] = d[t][e];
+    }
+}
+
+// The solve: y_i = sum_j X_ij rhs_j (three components), one warp per row,
+// lanes over the columns in a fixed order, then the warp's fixed reduction
+// tree.  rhs is read through the read-only path (it is the same for every row).
+constexpr int kDenseSolveWarps = 8;
+__global__ void __launch_bounds__(32 * kDenseSolveWarps) k_dense_solve(DenseDev dd, Gate gate,
+                                                                      const double* __restrict__ rhs, double* y) {
+  const int i = blockIdx.x * kDenseSolveWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (i >= dd.N || gate.skip(0)) return;
+  const double* row = dd.A + (size_t)i * dd.Np;
+  double acc[4][3];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = acc[u][2] = 0.0;
+  int j = lane;
+  for (; j + 96 < dd.N; j += 128) {  // four columns per lane in flight
+    double x[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) x[u] = row[j + 32 * u];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double* rr = rhs + 3 * (size_t)(j + 32 * u);
+      acc[u][0] += x[u] * __ldg(rr); acc[u][1] += x[u] * __ldg(rr + 1); acc[u][2] += x[u] * __ldg(rr + 2);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {  // the row's last columns
+    const int jj = j + 32 * u;
+    if (jj < dd.N) {
+      const double xv = row[jj];
+      const double* rr = rhs + 3 * (size_t)jj;
+      acc[u][0] += xv * __ldg(rr); acc[u][1] += xv * __ldg(rr + 1); acc[u][2] += xv * __ldg(rr + 2);
+    }
+  }
+  double o[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) o[c] = warp_sum((acc[0][c] + acc[1][c]) + (acc[2][c] + acc[3][c]));
+  if (lane == 0) { y[3 * (size_t)i] = o[0]; y[3 * (size_t)i + 1] = o[1]; y[3 * (size_t)i + 2] = o[2]; }
+}
+
+}  // namespace dfem

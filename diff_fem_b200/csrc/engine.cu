@@ -25,6 +25,7 @@
 #include "resident_solve.cuh"
 #include "skeleton_kernels.cuh"
 #include "skeleton_adjoint.cuh"
+#include "dense_solve.cuh"
 #include "resident_plan.h"
 #include "scene.h"
 
@@ -154,8 +155,14 @@ struct dfem_scene {
   // solve_cut = -1: the cluster form (one thread-block cluster walks the levels)
   int solve_cut = 0;
   int split_cut = 0;                     // the autotune's best split (0: none)
-  double solve_ms[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // autotune timings (ms per solve): levels, persistent, best split,
-                                                     // cluster, resident
+  double solve_ms[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // autotune timings (ms per solve): levels, persistent,
+                                                          // best split, cluster, resident, dense
+  // dense-inverse form (solve_cut = -3): X = Hs^-1 rebuilt after every refactorisation
+  bool dense_ok = false;                 // the scene qualifies (single part, N <= kDenseMaxN)
+  bool dense_built = false;
+  double dense_build_ms = 0.0;
+  DBuf<double> dn_A, dn_W, dn_Linv;
+  DenseDev dd{};
   DBuf<int> lvl_ptr_d, lvl_warp_d;       // cluster form: level starts, end of each level's warp-sized supernodes
   size_t shm_cluster = 0;
   int shm_cluster_warp = 0;              // doubles of shared memory per warp item
@@ -685,6 +692,46 @@ static int upload_refactor_plan(dfem_scene* sc) {
   return DFEM_OK;
 }
 
+// Largest single scene (vertices) served by the dense-inverse form: X and its
+// workspace take 2 N_p^2 doubles (268 MB at 4,096 vertices).
+constexpr int kDenseMaxN = 4096;
+// The dense form is kept when its saving per solve, over this many solves,
+// exceeds the time to rebuild X after a refactorisation.
+constexpr double kDenseAmortSolves = 100.0;
+
+static void dense_release(dfem_scene* sc) {
+  sc->dn_A.alloc(0);
+  sc->dn_W.alloc(0);
+  sc->dn_Linv.alloc(0);
+  sc->dense_built = false;
+  sc->dd = DenseDev{};
+}
+
+// X = Hs^-1 from the current GPU factor (dense_solve.cuh), on the scene's stream.
+static int dense_build(dfem_scene* sc) {
+  const int N = sc->hs.N, nb = (N + kDenseTile - 1) / kDenseTile, Np = nb * kDenseTile;
+  const size_t nn = (size_t)Np * Np;
+  if (!sc->dn_A.p || sc->dn_A.n != nn) {
+    CK(raise_smem_limit((const void*)k_dense_tile_inv, kDenseSmem));
+    CK(raise_smem_limit((const void*)k_dense_trtri, kDenseSmem));
+    CK(raise_smem_limit((const void*)k_dense_lauum, kDenseSmem));
+    sc->dense_built = false;
+    CK(sc->dn_A.alloc(nn));
+    CK(sc->dn_W.alloc(nn));
+    CK(sc->dn_Linv.alloc((size_t)nb * kDenseTile * kDenseTile));
+  }
+  sc->dd = DenseDev{N, Np, nb, sc->dn_A.p, sc->dn_W.p, sc->dn_Linv.p};
+  CK(cudaMemsetAsync(sc->dn_A.p, 0, nn * sizeof(double), sc->stream));
+  k_dense_scatter<<<sc->hs.F.nsuper, 256, 0, sc->stream>>>(sc->dd, sc->fd, sc->Ldw.p, sc->sn_dofs.p);
+  k_dense_tile_inv<<<nb, 256, kDenseSmem, sc->stream>>>(sc->dd);
+  for (int j = nb - 2; j >= 0; --j) k_dense_trtri<<<nb - 1 - j, 256, kDenseSmem, sc->stream>>>(sc->dd, j);
+  k_dense_lauum<<<nb * (nb + 1) / 2, 256, kDenseSmem, sc->stream>>>(sc->dd);
+  sc->launches += 3 + std::max(0, nb - 1);
+  CK(cudaGetLastError());
+  sc->dense_built = true;
+  return DFEM_OK;
+}
+
 // Materials from E_in / nu_in (device), Hs values, and the factor on the GPU.
 // A part whose factorisation meets a non-positive pivot is retried with the
 // reference's regularisation sequence (0, 1e-5, x10 ..., 25 attempts); the
@@ -720,6 +767,8 @@ static int gpu_refactor(dfem_scene* sc) {
       }
     if (!any) {
       pack_resident(sc);
+      sc->dense_built = false;  // X follows the factor (only while the dense form is in use)
+      if (sc->solve_cut == -3) RC(dense_build(sc));
       return DFEM_OK;
     }
   }
@@ -1264,6 +1313,11 @@ static cudaError_t launch_resident_solve(dfem_scene* sc, cudaStream_t st, Gate g
 // the cluster launch's return value is also kept for the autotune, which drops
 // the cluster form when the device refuses its launch.
 static void enqueue_solve_cut(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y, int c) {
+  if (c == -3) {  // the dense-inverse form
+    k_dense_solve<<<(sc->hs.N + kDenseSolveWarps - 1) / kDenseSolveWarps, 32 * kDenseSolveWarps, 0, st>>>(
+        sc->dd, gate, rhs, y);
+    return;
+  }
   if (c < 0) {  // -1: cluster form, -2: resident form
     const cudaError_t e = c == -2 ? launch_resident_solve(sc, st, gate, rhs, y) : launch_cluster_solve(sc, st, gate, rhs, y);
     if (e != cudaSuccess) sc->cluster_launch_err = e;
@@ -1336,9 +1390,10 @@ static cudaError_t capture_solve(dfem_scene* sc, cudaStream_t st, Gate gate, con
   return e;
 }
 
-// 1: level kernels, 2: persistent, 3: split, 4: cluster, 5: resident
+// 1: level kernels, 2: persistent, 3: split, 4: cluster, 5: resident, 6: dense inverse
 static int solve_form(const dfem_scene* sc) {
-  return sc->solve_cut == -2 ? 5 : sc->solve_cut < 0 ? 4 : sc->solve_cut >= n_levels(sc) ? 1 : sc->solve_cut == 0 ? 2 : 3;
+  return sc->solve_cut == -3 ? 6 : sc->solve_cut == -2 ? 5 : sc->solve_cut < 0 ? 4
+       : sc->solve_cut >= n_levels(sc) ? 1 : sc->solve_cut == 0 ? 2 : 3;
 }
 
 // Fresh completion stamps and control words of the persistent solve (each API
@@ -2137,6 +2192,32 @@ static int autotune_solve(dfem_scene* sc) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  // the dense-inverse form: single scenes up to kDenseMaxN vertices whose X
+  // and workspace take at most an eighth of the free memory
+  sc->solve_ms[5] = 0.0;
+  sc->dense_build_ms = 0.0;
+  {
+    const size_t np = (size_t)((sc->hs.N + kDenseTile - 1) / kDenseTile) * kDenseTile;
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    sc->dense_ok = sc->hs.nparts == 1 && sc->hs.N <= kDenseMaxN && 2 * np * np * sizeof(double) <= free_b / 8;
+  }
+  if (rc == DFEM_OK && sc->dense_ok) {
+    cudaEventRecord(e0, sc->stream);
+    int rb = dense_build(sc);
+    cudaEventRecord(e1, sc->stream);
+    float tb = 0.0f;
+    if (rb == DFEM_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&tb, e0, e1) != cudaSuccess))
+      rb = DFEM_ERR_CUDA;
+    sc->dense_build_ms = tb;
+    if (rb == DFEM_OK) rb = time_cut(-3, &sc->solve_ms[5]);
+    if (rb != DFEM_OK) {  // no room or a refused launch: not a candidate
+      cudaGetLastError();
+      g_last_error.clear();
+      dense_release(sc);
+      sc->solve_ms[5] = 0.0;
+    }
+  }
   RC(rc);
   int st4[4] = {0, 0, 0, 0};
   CK(cudaMemcpy(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost));
@@ -2146,8 +2227,10 @@ static int autotune_solve(dfem_scene* sc) {
   {
     double best = sc->solve_cut == 0 ? sc->solve_ms[1] : sc->solve_cut == L ? sc->solve_ms[0] : sc->solve_ms[2];
     if (sc->solve_ms[3] > 0.0 && sc->solve_ms[3] < best) { sc->solve_cut = -1; best = sc->solve_ms[3]; }
-    if (sc->solve_ms[4] > 0.0 && sc->solve_ms[4] < best) sc->solve_cut = -2;
+    if (sc->solve_ms[4] > 0.0 && sc->solve_ms[4] < best) { sc->solve_cut = -2; best = sc->solve_ms[4]; }
+    if (sc->solve_ms[5] > 0.0 && (best - sc->solve_ms[5]) * kDenseAmortSolves > sc->dense_build_ms) sc->solve_cut = -3;
   }
+  if (sc->solve_cut != -3 && sc->dn_A.p) dense_release(sc);
   RC(tune_solve_select(sc));
   invalidate_graphs(sc);
   return DFEM_OK;
@@ -2735,7 +2818,7 @@ int dfem_profile_levels(dfem_scene* sc, int32_t reps, int32_t cap, int32_t* n_se
 
 int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms) {
   if (!sc) return fail(DFEM_ERR_INVALID, "null argument");
-  if (request < -1 || request > 5) return fail(DFEM_ERR_INVALID, "request must be -1, 0, 1, 2, 3, 4 or 5");
+  if (request < -1 || request > 6) return fail(DFEM_ERR_INVALID, "request must be -1, 0, 1, 2, 3, 4, 5 or 6");
   CK(cudaSetDevice(sc->device));
   if (request == 0) {
     CK(cudaStreamSynchronize(sc->stream));
@@ -2746,7 +2829,15 @@ int dfem_solve_mode(dfem_scene* sc, int32_t request, int32_t* chosen, double* ms
     if (request == 3 && sc->split_cut == 0) return fail(DFEM_ERR_INVALID, "no split form (fewer than two levels)");
     if (request == 4 && !sc->cluster_ok) return fail(DFEM_ERR_INVALID, "no cluster form for this factor");
     if (request == 5 && !sc->res_ok) return fail(DFEM_ERR_INVALID, "no resident form for this scene");
-    const int c = request == 1 ? n_levels(sc) : request == 2 ? 0 : request == 3 ? sc->split_cut : request == 4 ? -1 : -2;
+    if (request == 6) {
+      if (!sc->dense_ok) return fail(DFEM_ERR_INVALID, "no dense form for this scene (a batch, or too many vertices)");
+      if (!sc->dense_built) {
+        CK(cudaStreamSynchronize(sc->stream));
+        RC(dense_build(sc));
+      }
+    }
+    const int c = request == 1 ? n_levels(sc) : request == 2 ? 0 : request == 3 ? sc->split_cut : request == 4 ? -1
+                : request == 5 ? -2 : -3;
     if (c != sc->solve_cut || sc->solve_select) {  // a requested form is used in every iteration
       sc->solve_cut = c;
       sc->solve_select = false;
@@ -2768,7 +2859,7 @@ int dfem_solve_select(const dfem_scene* sc, int32_t* on, double* weight_threshol
 
 int dfem_solve_times(const dfem_scene* sc, double* ms, int32_t n) {
   if (!sc || !ms || n < 0) return fail(DFEM_ERR_INVALID, "bad argument");
-  for (int k = 0; k < std::min(n, 5); ++k) ms[k] = sc->solve_ms[k];
+  for (int k = 0; k < std::min(n, 6); ++k) ms[k] = sc->solve_ms[k];
   return DFEM_OK;
 }
 

@@ -241,6 +241,8 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
     }
     __syncthreads();
   }
+  // the factored diagonal block stays in the workspace (the dense-inverse form reads it)
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) Ld[q] = L[q];
   // 4. X = L_ss^-1 (one column per thread)
   for (int c = threadIdx.x; c < w; c += blockDim.x) {
     for (int i = 0; i < c; ++i) X[i + c * w] = 0.0;

@@ -239,10 +239,13 @@ class Scene:
         """Form of the global solve: request None (query), "auto" (re-tune),
         "levels", "persistent", "split" (level kernels below the autotuned
         cut level, one persistent launch above), "cluster" (one thread-block
-        cluster walks the levels) or "resident" (the factor held in one
-        cluster's shared memory).  Returns the form in use and the autotune's
-        ms per solve of each form."""
-        req = {None: -1, "auto": 0, "levels": 1, "persistent": 2, "split": 3, "cluster": 4, "resident": 5}[request]
+        cluster walks the levels), "resident" (the factor held in one
+        cluster's shared memory) or "dense" (one product with Hs^-1, rebuilt
+        from the factor after every refactorisation; single scenes up to 4,096
+        vertices).  Returns the form in use and the autotune's ms per solve of
+        each form."""
+        req = {None: -1, "auto": 0, "levels": 1, "persistent": 2, "split": 3, "cluster": 4, "resident": 5,
+               "dense": 6}[request]
         chosen = C.c_int32()
         ms = (C.c_double * 2)()
         check(lib().dfem_solve_mode(self._h, req, C.byref(chosen), ms))
@@ -250,10 +253,11 @@ class Scene:
         check(lib().dfem_solve_split(self._h, C.byref(cut), C.byref(nl), C.byref(mss)))
         on, thr, one = C.c_int32(), C.c_double(), (C.c_double * 2)()
         check(lib().dfem_solve_select(self._h, C.byref(on), C.byref(thr), one))
-        t5 = (C.c_double * 5)()
-        check(lib().dfem_solve_times(self._h, t5, 5))
-        return {"mode": {1: "levels", 2: "persistent", 3: "split", 4: "cluster", 5: "resident"}[chosen.value],
-                "ms_levels": ms[0], "ms_cluster": t5[3], "ms_resident": t5[4],
+        t6 = (C.c_double * 6)()
+        check(lib().dfem_solve_times(self._h, t6, 6))
+        return {"mode": {1: "levels", 2: "persistent", 3: "split", 4: "cluster", 5: "resident",
+                         6: "dense"}[chosen.value],
+                "ms_levels": ms[0], "ms_cluster": t6[3], "ms_resident": t6[4], "ms_dense": t6[5],
                 "ms_persistent": ms[1], "ms_split": mss.value, "split_level": cut.value, "levels": nl.value,
                 "tail_persistent_below": thr.value if on.value else None,
                 "ms_largest_part_only": [one[0], one[1]]}

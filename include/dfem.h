@@ -315,18 +315,23 @@ int dfem_host_factor_solve(const dfem_scene_desc *desc, const double *b, double 
  * scenes whose factor fits the shared memory of one thread-block cluster of
  * up to 16 CTAs: every block stays in shared memory for the launch,
  * contributions and solution values move between the CTAs over distributed
- * shared memory, a cluster barrier between levels); a form requested with
- * 1-5 is used in every iteration (no per-iteration selection, see
+ * shared memory, a cluster barrier between levels), 6 dense (single scenes
+ * of at most 4,096 vertices: X = Hs^-1 is formed from the factor after every
+ * refactorisation, N_p^2 doubles twice with N_p = N rounded up to 64, and a
+ * solve is one product with X; the autotune keeps it when its saving over
+ * 100 solves exceeds the rebuild); a form requested with
+ * 1-6 is used in every iteration (no per-iteration selection, see
  * dfem_solve_select).  *chosen (may
- * be NULL) receives the form in use (1-5), ms (may be NULL, 2 values)
- * the last autotune's time per solve of forms 1 and 2.  Every form runs the
- * same arithmetic per supernode: results are identical.  No counterpart in
+ * be NULL) receives the form in use (1-6), ms (may be NULL, 2 values)
+ * the last autotune's time per solve of forms 1 and 2.  Forms 1-5 run the
+ * same arithmetic per supernode: their results are identical; form 6 agrees
+ * with them to rounding (and is deterministic).  No counterpart in
  * the reference (its solve is Eigen's SimplicialLDLT, sim/fem/World.h:1660). */
 int dfem_solve_mode(dfem_scene *scene, int32_t request, int32_t *chosen, double *ms);
 
 /* The last autotune's time per solve (ms) of the level-kernel, persistent,
- * best split, cluster and resident forms (0: not timed); writes the first
- * min(n, 5) of them. */
+ * best split, cluster, resident and dense forms (0: not timed); writes the
+ * first min(n, 6) of them. */
 int dfem_solve_times(const dfem_scene *scene, double *ms, int32_t n);
 
 /* The split form found by the last autotune: *cut_level (0: none), the

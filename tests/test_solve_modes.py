@@ -31,7 +31,7 @@ def test_persistent_solve_matches_level_kernels(builder):
          "muscle_beam": S.muscle_beam, "cloth_sheet": lambda: S.cloth_sheet(nv=12)}[builder]()
     sc = Scene(d)
     info = sc.solve_mode()
-    assert info["mode"] in ("levels", "persistent", "split", "cluster", "resident")
+    assert info["mode"] in ("levels", "persistent", "split", "cluster", "resident", "dense")
     assert info["ms_levels"] > 0 and info["ms_persistent"] > 0
     assert info["split_level"] > 0 and info["ms_split"] > 0  # these factors have more than one level
     assert info["ms_cluster"] > 0  # few supernodes: the cluster form is a candidate
@@ -100,4 +100,49 @@ def test_resident_solve_on_the_inverse_stiffness_beam():
     for k in a[2]:
         assert np.array_equal(a[2][k], b[2][k]), k
     assert np.array_equal(a[3], b[3])
+    sc.close()
+
+
+@pytest.mark.parametrize("builder", ["inverse_stiffness", "muscle_beam", "cloth_sheet"])
+def test_dense_inverse_form_matches_the_triangular_solves(builder):
+    """The dense-inverse form (X = Hs^-1 from the factor, one product per
+    solve) agrees with the supernodal triangular solves to rounding, forward
+    and adjoint, is deterministic, and follows a material update."""
+    d = {"inverse_stiffness": lambda: S.inverse_stiffness(nx=20, ny=6, nz=6),
+         "muscle_beam": S.muscle_beam, "cloth_sheet": lambda: S.cloth_sheet(nv=12)}[builder]()
+    sc = Scene(d)
+    assert sc.solve_mode()["ms_dense"] > 0  # single small scenes: a candidate
+    act = np.random.default_rng(1).uniform(0, 1, (4, d.n_segments)) if d.n_segments else None
+    a = run(sc, d, 4, "persistent", act)
+    b = run(sc, d, 4, "dense", act)
+    c = run(sc, d, 4, "dense", act)
+
+    def rel(u, w):
+        return np.abs(u - w).max() / max(np.abs(w).max(), 1e-300)
+
+    assert rel(b[0], a[0]) < 1e-12 and rel(b[1], a[1]) < 1e-10
+    for k in a[2]:
+        if a[2][k].size:
+            assert rel(b[2][k], a[2][k]) < 1e-9, k
+    assert np.array_equal(a[3], b[3])
+    for u, w in zip(b[:2], c[:2]):
+        assert np.array_equal(u, w)
+    for k in b[2]:
+        assert np.array_equal(b[2][k], c[2][k]), k
+    if d.n_tets:
+        E = np.asarray(d.youngs) * np.random.default_rng(2).uniform(0.5, 2.0, d.n_tets)
+        sc.set_materials(E, d.poisson)
+        e = run(sc, d, 4, "dense", act)
+        f = run(sc, d, 4, "persistent", act)
+        assert rel(e[0], f[0]) < 1e-12 and not np.array_equal(e[0], b[0])
+    sc.close()
+
+
+def test_dense_inverse_form_is_refused_for_batches():
+    from diff_fem_b200 import _capi
+    sc = Scene.batch([S.cantilever(), S.muscle_beam()])
+    assert sc.solve_mode()["ms_dense"] == 0
+    with pytest.raises(_capi.DfemError) as ex:
+        sc.solve_mode("dense")
+    assert ex.value.code == _capi.DFEM_ERR_INVALID
     sc.close()
