@@ -2190,8 +2190,6 @@ static int autotune_solve(dfem_scene* sc) {
       rc = DFEM_OK;
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   // the dense-inverse form: single scenes up to kDenseMaxN vertices whose X
   // and workspace take at most an eighth of the free memory
   sc->solve_ms[5] = 0.0;
@@ -2199,7 +2197,7 @@ static int autotune_solve(dfem_scene* sc) {
   {
     const size_t np = (size_t)((sc->hs.N + kDenseTile - 1) / kDenseTile) * kDenseTile;
     size_t free_b = 0, total_b = 0;
-    CK(cudaMemGetInfo(&free_b, &total_b));
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
     sc->dense_ok = sc->hs.nparts == 1 && sc->hs.N <= kDenseMaxN && 2 * np * np * sizeof(double) <= free_b / 8;
   }
   if (rc == DFEM_OK && sc->dense_ok) {
@@ -2218,6 +2216,8 @@ static int autotune_solve(dfem_scene* sc) {
       sc->solve_ms[5] = 0.0;
     }
   }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
   RC(rc);
   int st4[4] = {0, 0, 0, 0};
   CK(cudaMemcpy(st4, sc->status.p, sizeof(st4), cudaMemcpyDeviceToHost));
