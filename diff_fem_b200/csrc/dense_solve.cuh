@@ -9,8 +9,10 @@
 //      panels L_{R,s}) scattered into a dense lower-triangular N_p x N_p matrix
 //      (N_p = N rounded up to 64; the padding is the identity),
 //   2. the inverses of its 64 x 64 diagonal tiles (all tiles at once),
-//   3. W = L^-1 tile column by tile column, last to first (LAPACK's blocked
-//      triangular inverse): W_Ij = -(sum_{K=j+1..I} W_IK L_Kj) W_jj,
+//   3. W = L^-1 by doubling diagonal ranges, bottom up: with the inverses of
+//      ranges A = [a, m) and C = [m, b) known, the block below them is
+//      W_CA = -(W_CC L_CA) W_AA (two tile-products per level, every range of
+//      the level in one launch; log2(tiles) levels),
 //   4. X = W^T W (lower tiles, mirrored: X is exactly symmetric).
 // Products of 64 x 64 tiles run on the FP64 tensor cores (mma.sync m8n8k4)
 // from shared memory in a fixed order, so X and every solve are
@@ -31,6 +33,7 @@ struct DenseDev {
   int N, Np, nb;        // vertices, padded size, tiles per side
   double* A;            // N_p x N_p row-major: L, then X
   double* W;            // N_p x N_p row-major: L^-1 (lower tiles)
+  double* T;            // N_p x N_p row-major: W_CC L_CA of the current level
   double* Linv;         // nb x 64 x 64 row-major: inverses of L's diagonal tiles
 };
 
@@ -62,18 +65,6 @@ __device__ __forceinline__ void dense_load(const double* M, int Np, int I, int J
 __device__ __forceinline__ void dense_zero(double d[8][2]) {
 #pragma unroll
   for (int t = 0; t < 8; ++t) d[t][0] = d[t][1] = 0.0;
-}
-
-// the warp's output tiles to shared memory ([row][col]), scaled by s
-__device__ __forceinline__ void dense_store_sh(const double d[8][2], double s, double* S) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int r = 8 * w + (lane >> 2);
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const int c = 8 * t + 2 * (lane & 3);
-    S[r * kDenseLd + c] = s * d[t][0];
-    S[r * kDenseLd + c + 1] = s * d[t][1];
-  }
 }
 
 // 1. the supernodal factor into the dense lower triangle (A zeroed before):
@@ -127,42 +118,65 @@ __global__ void __launch_bounds__(256) k_dense_tile_inv(DenseDev dd) {
   }
 }
 
-// 3. tile column j of W = L^-1 (tiles I > j, one per CTA):
-//    T = sum_{K=j+1..I} W_IK L_Kj, then W_Ij = -T W_jj.
-__global__ void __launch_bounds__(256) k_dense_trtri(DenseDev dd, int j) {
-  extern __shared__ __align__(16) double dsh[];
-  double* P = dsh;
-  double* Q = dsh + kDenseTile * kDenseLd;
-  const int I = j + 1 + blockIdx.x;
-  double d[8][2];
-  dense_zero(d);
-  for (int K = j + 1; K <= I; ++K) {
-    dense_load(dd.W, dd.Np, I, K, false, P);  // W_IK [row][k]
-    dense_load(dd.A, dd.Np, K, j, true, Q);   // L_Kj as [col][k]
-    __syncthreads();
-    dense_mma(P, Q, d);
-    __syncthreads();
-  }
-  dense_store_sh(d, -1.0, P);  // -T [row][k]
-  {
-    const double* Li = dd.Linv + (size_t)j * kDenseTile * kDenseTile;  // W_jj [k][col] -> Q [col][k]
-    for (int q = threadIdx.x; q < kDenseTile * kDenseTile; q += blockDim.x) {
-      const int k = q / kDenseTile, c = q % kDenseTile;
-      Q[c * kDenseLd + k] = Li[q];
-    }
-  }
-  __syncthreads();
-  dense_zero(d);
-  dense_mma(P, Q, d);
+// 3. one level of the triangular inverse (ranges of s tiles; blockIdx.y the
+// pair of ranges A = [a, m), C = [m, b) with a = 2 s y, m = a + s,
+// b = min(a + 2 s, nb); blockIdx.x the tile (I, J) of C x A):
+//   t: T_IJ = sum_{K=m..I} W_IK L_KJ       w: W_IJ = -sum_{K=J..m-1} T_IK W_KJ
+__device__ __forceinline__ bool dense_level_tile(const DenseDev& dd, int s, int& I, int& J, int& a, int& m) {
+  a = 2 * s * blockIdx.y;
+  m = a + s;
+  const int b = min(a + 2 * s, dd.nb);
+  I = m + (int)blockIdx.x / s;
+  J = a + (int)blockIdx.x % s;
+  return m < dd.nb && I < b;
+}
+
+__device__ __forceinline__ void dense_store_tile(const double d[8][2], double sc, double* M, int Np, int I, int J) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double* Wt = dd.W + (size_t)I * kDenseTile * dd.Np + (size_t)j * kDenseTile;
+  double* o = M + (size_t)I * kDenseTile * Np + (size_t)J * kDenseTile;
   const int r = 8 * w + (lane >> 2);
 #pragma unroll
   for (int t = 0; t < 8; ++t) {
     const int c = 8 * t + 2 * (lane & 3);
-    Wt[(size_t)r * dd.Np + c] = d[t][0];
-    Wt[(size_t)r * dd.Np + c + 1] = d[t][1];
+    o[(size_t)r * Np + c] = sc * d[t][0];
+    o[(size_t)r * Np + c + 1] = sc * d[t][1];
   }
+}
+
+__global__ void __launch_bounds__(256) k_dense_trtri_t(DenseDev dd, int s) {
+  extern __shared__ __align__(16) double dsh[];
+  double* P = dsh;
+  double* Q = dsh + kDenseTile * kDenseLd;
+  int I, J, a, m;
+  if (!dense_level_tile(dd, s, I, J, a, m)) return;
+  double d[8][2];
+  dense_zero(d);
+  for (int K = m; K <= I; ++K) {
+    dense_load(dd.W, dd.Np, I, K, false, P);  // W_IK [row][k]
+    dense_load(dd.A, dd.Np, K, J, true, Q);   // L_KJ as [col][k]
+    __syncthreads();
+    dense_mma(P, Q, d);
+    __syncthreads();
+  }
+  dense_store_tile(d, 1.0, dd.T, dd.Np, I, J);
+}
+
+__global__ void __launch_bounds__(256) k_dense_trtri_w(DenseDev dd, int s) {
+  extern __shared__ __align__(16) double dsh[];
+  double* P = dsh;
+  double* Q = dsh + kDenseTile * kDenseLd;
+  int I, J, a, m;
+  if (!dense_level_tile(dd, s, I, J, a, m)) return;
+  double d[8][2];
+  dense_zero(d);
+  for (int K = J; K < m; ++K) {
+    dense_load(dd.T, dd.Np, I, K, false, P);  // T_IK [row][k]
+    dense_load(dd.W, dd.Np, K, J, true, Q);   // W_KJ as [col][k]
+    __syncthreads();
+    dense_mma(P, Q, d);
+    __syncthreads();
+  }
+  dense_store_tile(d, -1.0, dd.W, dd.Np, I, J);
 }
 
 // 4. X = W^T W: tile (I, J), I >= J, sum over K = I .. nb-1 of W_KI^T W_KJ;
@@ -200,42 +214,53 @@ __global__ void __launch_bounds__(256) k_dense_lauum(DenseDev dd) {
     }
 }
 
-// The solve: y_i = sum_j X_ij rhs_j (three components), one warp per row,
-// lanes over the columns in a fixed order, then the warp's fixed reduction
-// tree.  rhs is read through the read-only path (it is the same for every row).
-constexpr int kDenseSolveWarps = 8;
-__global__ void __launch_bounds__(32 * kDenseSolveWarps) k_dense_solve(DenseDev dd, Gate gate,
+// The solve: y_i = sum_j X_ij rhs_j (three components).  One CTA of 1024
+// threads per SM stages rhs in shared memory (x, y, z planes, zero past N),
+// then one warp per row (rows dealt round-robin over the CTAs) streams the row in 16-byte pairs, eight per lane in
+// flight, each lane summing its columns in a fixed order, then the warp's
+// fixed reduction tree.  X's padding columns are zero.  Shared memory: 3 N_p
+// doubles.
+constexpr int kDenseSolveThreads = 1024;
+__global__ void __launch_bounds__(kDenseSolveThreads, 1) k_dense_solve(DenseDev dd, Gate gate,
                                                                       const double* __restrict__ rhs, double* y) {
-  const int i = blockIdx.x * kDenseSolveWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-  if (i >= dd.N || gate.skip(0)) return;
-  const double* row = dd.A + (size_t)i * dd.Np;
-  double acc[4][3];
-#pragma unroll
-  for (int u = 0; u < 4; ++u) acc[u][0] = acc[u][1] = acc[u][2] = 0.0;
-  int j = lane;
-  for (; j + 96 < dd.N; j += 128) {  // four columns per lane in flight
-    double x[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) x[u] = row[j + 32 * u];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const double* rr = rhs + 3 * (size_t)(j + 32 * u);
-      acc[u][0] += x[u] * __ldg(rr); acc[u][1] += x[u] * __ldg(rr + 1); acc[u][2] += x[u] * __ldg(rr + 2);
-    }
+  extern __shared__ __align__(16) double bsh[];
+  if (gate.skip(0)) return;
+  const int Np = dd.Np, N = dd.N;
+  for (int j = threadIdx.x; j < Np; j += blockDim.x) {
+    const bool in = j < N;
+    bsh[j] = in ? rhs[3 * (size_t)j] : 0.0;
+    bsh[Np + j] = in ? rhs[3 * (size_t)j + 1] : 0.0;
+    bsh[2 * Np + j] = in ? rhs[3 * (size_t)j + 2] : 0.0;
   }
+  __syncthreads();
+  const double2* bx = reinterpret_cast<const double2*>(bsh);
+  const double2* by = reinterpret_cast<const double2*>(bsh + Np);
+  const double2* bz = reinterpret_cast<const double2*>(bsh + 2 * Np);
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5, np2 = Np / 2;
+  for (int i = (threadIdx.x >> 5) * gridDim.x + blockIdx.x; i < N; i += gridDim.x * nw) {  // rows spread over all CTAs
+    const double2* row = reinterpret_cast<const double2*>(dd.A + (size_t)i * Np);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int q0 = lane; q0 < np2; q0 += 256) {
+      double2 x[8];
 #pragma unroll
-  for (int u = 0; u < 4; ++u) {  // the row's last columns
-    const int jj = j + 32 * u;
-    if (jj < dd.N) {
-      const double xv = row[jj];
-      const double* rr = rhs + 3 * (size_t)jj;
-      acc[u][0] += xv * __ldg(rr); acc[u][1] += xv * __ldg(rr + 1); acc[u][2] += xv * __ldg(rr + 2);
+      for (int u = 0; u < 8; ++u) {
+        const int k = q0 + 32 * u;
+        x[u] = k < np2 ? __ldcg(row + k) : make_double2(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = q0 + 32 * u;
+        if (k < np2) {
+          const double2 b0 = bx[k], b1 = by[k], b2 = bz[k];
+          a0 += x[u].x * b0.x + x[u].y * b0.y;
+          a1 += x[u].x * b1.x + x[u].y * b1.y;
+          a2 += x[u].x * b2.x + x[u].y * b2.y;
+        }
+      }
     }
+    a0 = warp_sum(a0); a1 = warp_sum(a1); a2 = warp_sum(a2);
+    if (lane == 0) { y[3 * (size_t)i] = a0; y[3 * (size_t)i + 1] = a1; y[3 * (size_t)i + 2] = a2; }
   }
-  double o[3];
-#pragma unroll
-  for (int c = 0; c < 3; ++c) o[c] = warp_sum((acc[0][c] + acc[1][c]) + (acc[2][c] + acc[3][c]));
-  if (lane == 0) { y[3 * (size_t)i] = o[0]; y[3 * (size_t)i + 1] = o[1]; y[3 * (size_t)i + 2] = o[2]; }
 }
 
 }  // namespace dfem

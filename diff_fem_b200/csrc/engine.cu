@@ -161,8 +161,9 @@ struct dfem_scene {
   bool dense_ok = false;                 // the scene qualifies (single part, N <= kDenseMaxN)
   bool dense_built = false;
   double dense_build_ms = 0.0;
-  DBuf<double> dn_A, dn_W, dn_Linv;
+  DBuf<double> dn_A, dn_W, dn_T, dn_Linv;
   DenseDev dd{};
+  int dense_grid = 1;                    // CTAs of the dense solve (one per SM at most)
   DBuf<int> lvl_ptr_d, lvl_warp_d;       // cluster form: level starts, end of each level's warp-sized supernodes
   size_t shm_cluster = 0;
   int shm_cluster_warp = 0;              // doubles of shared memory per warp item
@@ -702,6 +703,7 @@ constexpr double kDenseAmortSolves = 100.0;
 static void dense_release(dfem_scene* sc) {
   sc->dn_A.alloc(0);
   sc->dn_W.alloc(0);
+  sc->dn_T.alloc(0);
   sc->dn_Linv.alloc(0);
   sc->dense_built = false;
   sc->dd = DenseDev{};
@@ -713,20 +715,31 @@ static int dense_build(dfem_scene* sc) {
   const size_t nn = (size_t)Np * Np;
   if (!sc->dn_A.p || sc->dn_A.n != nn) {
     CK(raise_smem_limit((const void*)k_dense_tile_inv, kDenseSmem));
-    CK(raise_smem_limit((const void*)k_dense_trtri, kDenseSmem));
+    CK(raise_smem_limit((const void*)k_dense_trtri_t, kDenseSmem));
+    CK(raise_smem_limit((const void*)k_dense_trtri_w, kDenseSmem));
     CK(raise_smem_limit((const void*)k_dense_lauum, kDenseSmem));
+    CK(raise_smem_limit((const void*)k_dense_solve, 3 * (size_t)Np * sizeof(double)));
+    int nsm = 1;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, sc->device));
+    sc->dense_grid = std::max(1, std::min(nsm, N));
     sc->dense_built = false;
     CK(sc->dn_A.alloc(nn));
     CK(sc->dn_W.alloc(nn));
+    CK(sc->dn_T.alloc(nn));
     CK(sc->dn_Linv.alloc((size_t)nb * kDenseTile * kDenseTile));
   }
-  sc->dd = DenseDev{N, Np, nb, sc->dn_A.p, sc->dn_W.p, sc->dn_Linv.p};
+  sc->dd = DenseDev{N, Np, nb, sc->dn_A.p, sc->dn_W.p, sc->dn_T.p, sc->dn_Linv.p};
   CK(cudaMemsetAsync(sc->dn_A.p, 0, nn * sizeof(double), sc->stream));
   k_dense_scatter<<<sc->hs.F.nsuper, 256, 0, sc->stream>>>(sc->dd, sc->fd, sc->Ldw.p, sc->sn_dofs.p);
   k_dense_tile_inv<<<nb, 256, kDenseSmem, sc->stream>>>(sc->dd);
-  for (int j = nb - 2; j >= 0; --j) k_dense_trtri<<<nb - 1 - j, 256, kDenseSmem, sc->stream>>>(sc->dd, j);
+  int levels = 0;
+  for (int w = 1; w < nb; w *= 2, ++levels) {
+    const dim3 grid(w * w, (nb + 2 * w - 1) / (2 * w));
+    k_dense_trtri_t<<<grid, 256, kDenseSmem, sc->stream>>>(sc->dd, w);
+    k_dense_trtri_w<<<grid, 256, kDenseSmem, sc->stream>>>(sc->dd, w);
+  }
   k_dense_lauum<<<nb * (nb + 1) / 2, 256, kDenseSmem, sc->stream>>>(sc->dd);
-  sc->launches += 3 + std::max(0, nb - 1);
+  sc->launches += 3 + 2 * levels;
   CK(cudaGetLastError());
   sc->dense_built = true;
   return DFEM_OK;
@@ -1314,7 +1327,7 @@ static cudaError_t launch_resident_solve(dfem_scene* sc, cudaStream_t st, Gate g
 // the cluster form when the device refuses its launch.
 static void enqueue_solve_cut(dfem_scene* sc, cudaStream_t st, Gate gate, const double* rhs, double* y, int c) {
   if (c == -3) {  // the dense-inverse form
-    k_dense_solve<<<(sc->hs.N + kDenseSolveWarps - 1) / kDenseSolveWarps, 32 * kDenseSolveWarps, 0, st>>>(
+    k_dense_solve<<<sc->dense_grid, kDenseSolveThreads, 3 * (size_t)sc->dd.Np * sizeof(double), st>>>(
         sc->dd, gate, rhs, y);
     return;
   }
@@ -2201,8 +2214,9 @@ static int autotune_solve(dfem_scene* sc) {
     sc->dense_ok = sc->hs.nparts == 1 && sc->hs.N <= kDenseMaxN && 2 * np * np * sizeof(double) <= free_b / 8;
   }
   if (rc == DFEM_OK && sc->dense_ok) {
+    int rb = dense_build(sc);  // allocates X and its workspace; the rebuild after a refactorisation is timed
     cudaEventRecord(e0, sc->stream);
-    int rb = dense_build(sc);
+    if (rb == DFEM_OK) rb = dense_build(sc);
     cudaEventRecord(e1, sc->stream);
     float tb = 0.0f;
     if (rb == DFEM_OK && (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&tb, e0, e1) != cudaSuccess))
@@ -2860,6 +2874,7 @@ int dfem_solve_select(const dfem_scene* sc, int32_t* on, double* weight_threshol
 int dfem_solve_times(const dfem_scene* sc, double* ms, int32_t n) {
   if (!sc || !ms || n < 0) return fail(DFEM_ERR_INVALID, "bad argument");
   for (int k = 0; k < std::min(n, 6); ++k) ms[k] = sc->solve_ms[k];
+  if (n > 6) ms[6] = sc->dense_build_ms;
   return DFEM_OK;
 }
 

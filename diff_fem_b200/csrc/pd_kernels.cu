@@ -376,14 +376,27 @@ __global__ void k_gather_force(SceneDev d, Gate gate, const float* __restrict__ 
 }
 
 // rhs_i = c0_i + sum of the slots of vertex i
+// acc + slot[k0] + ... + slot[k1 - 1], in that order; eight slots' loads are
+// issued before their sums (the chain of adds no longer waits on each load)
+__device__ __forceinline__ Vec3<double> sum_slots(Vec3<double> acc, const double* __restrict__ slot, int k0, int k1) {
+  int k = k0;
+  for (; k + 8 <= k1; k += 8) {
+    Vec3<double> v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = ld3(slot, k + u);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc = acc + v[u];
+  }
+  for (; k < k1; ++k) acc = acc + ld3(slot, k);
+  return acc;
+}
+
 __global__ void k_gather(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
                              const double* __restrict__ slot,
                          const double* __restrict__ c0, double* __restrict__ rhs) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
-  Vec3<double> acc = ld3(c0, i);
-  for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
-  st3(rhs, i, acc);
+  st3(rhs, i, sum_slots(ld3(c0, i), slot, vslot_ptr[i], vslot_ptr[i + 1]));
 }
 
 // ----------------------------------------------------------- solves ----
@@ -1302,9 +1315,7 @@ __global__ void k_adj_gather(int N, Gate gate, const int* __restrict__ vpart, co
                              double* xkb) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
-  Vec3<double> acc = mk3(0.0, 0.0, 0.0);
-  for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
-  st3(xkb, i, acc);
+  st3(xkb, i, sum_slots(mk3(0.0, 0.0, 0.0), slot, vslot_ptr[i], vslot_ptr[i + 1]));
 }
 
 // activation gradient of the step: sum over the members of each channel

@@ -253,11 +253,11 @@ class Scene:
         check(lib().dfem_solve_split(self._h, C.byref(cut), C.byref(nl), C.byref(mss)))
         on, thr, one = C.c_int32(), C.c_double(), (C.c_double * 2)()
         check(lib().dfem_solve_select(self._h, C.byref(on), C.byref(thr), one))
-        t6 = (C.c_double * 6)()
-        check(lib().dfem_solve_times(self._h, t6, 6))
+        t6 = (C.c_double * 7)()
+        check(lib().dfem_solve_times(self._h, t6, 7))
         return {"mode": {1: "levels", 2: "persistent", 3: "split", 4: "cluster", 5: "resident",
                          6: "dense"}[chosen.value],
-                "ms_levels": ms[0], "ms_cluster": t6[3], "ms_resident": t6[4], "ms_dense": t6[5],
+                "ms_levels": ms[0], "ms_cluster": t6[3], "ms_resident": t6[4], "ms_dense": t6[5], "ms_dense_build": t6[6],
                 "ms_persistent": ms[1], "ms_split": mss.value, "split_level": cut.value, "levels": nl.value,
                 "tail_persistent_below": thr.value if on.value else None,
                 "ms_largest_part_only": [one[0], one[1]]}

@@ -330,8 +330,8 @@ int dfem_host_factor_solve(const dfem_scene_desc *desc, const double *b, double 
 int dfem_solve_mode(dfem_scene *scene, int32_t request, int32_t *chosen, double *ms);
 
 /* The last autotune's time per solve (ms) of the level-kernel, persistent,
- * best split, cluster, resident and dense forms (0: not timed); writes the
- * first min(n, 6) of them. */
+ * best split, cluster, resident and dense forms (0: not timed), then the
+ * time to build the dense form's inverse; writes the first min(n, 7). */
 int dfem_solve_times(const dfem_scene *scene, double *ms, int32_t n);
 
 /* The split form found by the last autotune: *cut_level (0: none), the

@@ -140,7 +140,8 @@ def test_dense_inverse_form_matches_the_triangular_solves(builder):
 
 def test_dense_inverse_form_is_refused_for_batches():
     from diff_fem_b200 import _capi
-    sc = Scene.batch([S.cantilever(), S.muscle_beam()])
+    descs = [dataclasses.replace(q, time_step=1.0 / 60.0, max_iterations=15) for q in (S.cantilever(), S.muscle_beam())]
+    sc = Scene.batch(descs)
     assert sc.solve_mode()["ms_dense"] == 0
     with pytest.raises(_capi.DfemError) as ex:
         sc.solve_mode("dense")
