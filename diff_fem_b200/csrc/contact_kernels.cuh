@@ -1893,7 +1893,7 @@ __global__ void __launch_bounds__(128) k_cadj_fused(SceneDev d, ContactDev c, Co
     grid.sync();
     for (int t = tid; t < ncons; t += nthr) adj_local_item(d, t, ori, a.yb, act_row, slot, gE, gnu, mg, nullptr, xt);
     grid.sync();
-    for (int i = tid; i < d.N; i += nthr) {  // k_adj_gather, then k_cadj_hs on the same vertex
+    for (int i = tid; i < d.N; i += nthr) {  // k_adj_gather_seq, then k_cadj_hs on the same vertex
       Vec3<double> acc = mk3(0.0, 0.0, 0.0);
       for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
       st3(a.orib, i, acc);
@@ -1958,7 +1958,7 @@ __global__ void __launch_bounds__(128) k_cadj_fused_parts(SceneDev d, ContactDev
     for (int t = tid; t < ncons; t += nthr)
       if (j <= top[cons_part(d, t)]) adj_local_item(d, t, ori, a.yb, act_row, slot, gE, gnu, mg, nullptr, xt);
     grid.sync();
-    for (int i = tid; i < d.N; i += nthr) {  // k_adj_gather, then k_cadj_hs on the same vertex
+    for (int i = tid; i < d.N; i += nthr) {  // k_adj_gather_seq, then k_cadj_hs on the same vertex
       if (j > top[vpart_of(d, i)]) continue;
       Vec3<double> acc = mk3(0.0, 0.0, 0.0);
       for (int k = d.vslot_ptr[i]; k < d.vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);

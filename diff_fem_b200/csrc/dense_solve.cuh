@@ -37,34 +37,92 @@ struct DenseDev {
   double* Linv;         // nb x 64 x 64 row-major: inverses of L's diagonal tiles
 };
 
-// P (64 x 64, [row][k]) times Q^T (Q [col][k]) added to the warp's eight 8x8
-// output tiles: warp w holds rows 8w .. 8w+7, tile t columns 8t .. 8t+7;
-// d[t][i] is row 8w + (lane >> 2), column 8t + 2 (lane & 3) + i.
-__device__ __forceinline__ void dense_mma(const double* P, const double* Q, double d[8][2]) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const double* pa = P + (8 * w + (lane >> 2)) * kDenseLd + (lane & 3);
-  const double* qb = Q + (lane >> 2) * kDenseLd + (lane & 3);
-#pragma unroll 4
+constexpr int kDenseThreads = 128;  // CTA of the tile products: four warps, a 32 x 32 quadrant each
+
+// P (64 x 64, [row][k]) times Q^T (Q [col][k]) added to the warp's 4 x 4 8x8
+// output tiles: warp w holds the quadrant rows 32 (w >> 1) .., columns
+// 32 (w & 1) ..; d[i][j][e] is row qr + 8 i + (lane >> 2), column
+// qc + 8 j + 2 (lane & 3) + e.  Per k-step of four: four A and four B
+// fragments from shared memory feed sixteen FP64 tensor-core products.
+__device__ __forceinline__ void dense_quadrant(int& qr, int& qc) {
+  const int w = threadIdx.x >> 5;
+  qr = 32 * (w >> 1);
+  qc = 32 * (w & 1);
+}
+
+__device__ __forceinline__ void dense_mma(const double* P, const double* Q, double d[4][4][2]) {
+  const int lane = threadIdx.x & 31;
+  int qr, qc;
+  dense_quadrant(qr, qc);
+  const double* pa = P + (qr + (lane >> 2)) * kDenseLd + (lane & 3);
+  const double* qb = Q + (qc + (lane >> 2)) * kDenseLd + (lane & 3);
+#pragma unroll 2
   for (int k0 = 0; k0 < kDenseTile; k0 += 4) {
-    const double a = pa[k0];
+    double a[4], b[4];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) dmma_8x8x4(d[t][0], d[t][1], a, qb[8 * t * kDenseLd + k0]);
+    for (int i = 0; i < 4; ++i) a[i] = pa[8 * i * kDenseLd + k0];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) b[j] = qb[8 * j * kDenseLd + k0];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dmma_8x8x4(d[i][j][0], d[i][j][1], a[i], b[j]);
   }
 }
 
-// tile (I, J) of a row-major N_p x N_p matrix into shared memory, as stored or transposed
+// tile (I, J) of a row-major N_p x N_p matrix into shared memory, as stored or
+// transposed: 16-byte loads along the rows of M, all of a thread's loads
+// issued before its shared-memory stores
 __device__ __forceinline__ void dense_load(const double* M, int Np, int I, int J, bool trans, double* S) {
   const double* src = M + (size_t)I * kDenseTile * Np + (size_t)J * kDenseTile;
-  for (int q = threadIdx.x; q < kDenseTile * kDenseTile; q += blockDim.x) {
-    const int r = q / kDenseTile, c = q % kDenseTile;  // coalesced along rows of M
-    const double v = src[(size_t)r * Np + c];
-    if (trans) S[c * kDenseLd + r] = v; else S[r * kDenseLd + c] = v;
+  constexpr int kPairs = kDenseTile * kDenseTile / 2, kPer = kPairs / kDenseThreads;
+  double2 v[kPer];
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int q = threadIdx.x + kDenseThreads * u, r = q / (kDenseTile / 2), c = 2 * (q % (kDenseTile / 2));
+    v[u] = __ldcg(reinterpret_cast<const double2*>(src + (size_t)r * Np + c));
+  }
+#pragma unroll
+  for (int u = 0; u < kPer; ++u) {
+    const int q = threadIdx.x + kDenseThreads * u, r = q / (kDenseTile / 2), c = 2 * (q % (kDenseTile / 2));
+    if (trans) {
+      S[c * kDenseLd + r] = v[u].x;
+      S[(c + 1) * kDenseLd + r] = v[u].y;
+    } else {
+      S[r * kDenseLd + c] = v[u].x;
+      S[r * kDenseLd + c + 1] = v[u].y;
+    }
   }
 }
 
-__device__ __forceinline__ void dense_zero(double d[8][2]) {
+__device__ __forceinline__ void dense_zero(double d[4][4][2]) {
 #pragma unroll
-  for (int t = 0; t < 8; ++t) d[t][0] = d[t][1] = 0.0;
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) d[i][j][0] = d[i][j][1] = 0.0;
+}
+
+// the warp's output tiles, scaled by sc, to tile (I, J) of M (transp: to (J, I)
+// transposed as well; skip_upper: only the lower triangle of a diagonal tile)
+__device__ __forceinline__ void dense_store(const double d[4][4][2], double sc, double* M, int Np, int I, int J,
+                                            bool transp, bool skip_upper) {
+  const int lane = threadIdx.x & 31;
+  int qr, qc;
+  dense_quadrant(qr, qc);
+  double* o = M + (size_t)I * kDenseTile * Np + (size_t)J * kDenseTile;
+  double* ot = M + (size_t)J * kDenseTile * Np + (size_t)I * kDenseTile;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int r = qr + 8 * i + (lane >> 2), c = qc + 8 * j + 2 * (lane & 3) + e;
+        if (skip_upper && r < c) continue;
+        const double v = sc * d[i][j][e];
+        o[(size_t)r * Np + c] = v;
+        if (transp) ot[(size_t)c * Np + r] = v;
+      }
 }
 
 // 1. the supernodal factor into the dense lower triangle (A zeroed before):
@@ -91,7 +149,7 @@ __global__ void k_dense_scatter(DenseDev dd, FactorDev f, const double* __restri
 
 // 2. inverse of diagonal tile J of L (lower triangular; one column per
 // thread, forward substitution), to Linv and as W_JJ
-__global__ void __launch_bounds__(256) k_dense_tile_inv(DenseDev dd) {
+__global__ void __launch_bounds__(kDenseThreads) k_dense_tile_inv(DenseDev dd) {
   extern __shared__ __align__(16) double dsh[];
   double* S = dsh;
   double* X = dsh + kDenseTile * kDenseLd;
@@ -131,25 +189,13 @@ __device__ __forceinline__ bool dense_level_tile(const DenseDev& dd, int s, int&
   return m < dd.nb && I < b;
 }
 
-__device__ __forceinline__ void dense_store_tile(const double d[8][2], double sc, double* M, int Np, int I, int J) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double* o = M + (size_t)I * kDenseTile * Np + (size_t)J * kDenseTile;
-  const int r = 8 * w + (lane >> 2);
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const int c = 8 * t + 2 * (lane & 3);
-    o[(size_t)r * Np + c] = sc * d[t][0];
-    o[(size_t)r * Np + c + 1] = sc * d[t][1];
-  }
-}
-
-__global__ void __launch_bounds__(256) k_dense_trtri_t(DenseDev dd, int s) {
+__global__ void __launch_bounds__(kDenseThreads) k_dense_trtri_t(DenseDev dd, int s) {
   extern __shared__ __align__(16) double dsh[];
   double* P = dsh;
   double* Q = dsh + kDenseTile * kDenseLd;
   int I, J, a, m;
   if (!dense_level_tile(dd, s, I, J, a, m)) return;
-  double d[8][2];
+  double d[4][4][2];
   dense_zero(d);
   for (int K = m; K <= I; ++K) {
     dense_load(dd.W, dd.Np, I, K, false, P);  // W_IK [row][k]
@@ -158,16 +204,16 @@ __global__ void __launch_bounds__(256) k_dense_trtri_t(DenseDev dd, int s) {
     dense_mma(P, Q, d);
     __syncthreads();
   }
-  dense_store_tile(d, 1.0, dd.T, dd.Np, I, J);
+  dense_store(d, 1.0, dd.T, dd.Np, I, J, false, false);
 }
 
-__global__ void __launch_bounds__(256) k_dense_trtri_w(DenseDev dd, int s) {
+__global__ void __launch_bounds__(kDenseThreads) k_dense_trtri_w(DenseDev dd, int s) {
   extern __shared__ __align__(16) double dsh[];
   double* P = dsh;
   double* Q = dsh + kDenseTile * kDenseLd;
   int I, J, a, m;
   if (!dense_level_tile(dd, s, I, J, a, m)) return;
-  double d[8][2];
+  double d[4][4][2];
   dense_zero(d);
   for (int K = J; K < m; ++K) {
     dense_load(dd.T, dd.Np, I, K, false, P);  // T_IK [row][k]
@@ -176,12 +222,12 @@ __global__ void __launch_bounds__(256) k_dense_trtri_w(DenseDev dd, int s) {
     dense_mma(P, Q, d);
     __syncthreads();
   }
-  dense_store_tile(d, -1.0, dd.W, dd.Np, I, J);
+  dense_store(d, -1.0, dd.W, dd.Np, I, J, false, false);
 }
 
 // 4. X = W^T W: tile (I, J), I >= J, sum over K = I .. nb-1 of W_KI^T W_KJ;
 // written to (I, J) and transposed to (J, I)
-__global__ void __launch_bounds__(256) k_dense_lauum(DenseDev dd) {
+__global__ void __launch_bounds__(kDenseThreads) k_dense_lauum(DenseDev dd) {
   extern __shared__ __align__(16) double dsh[];
   double* P = dsh;
   double* Q = dsh + kDenseTile * kDenseLd;
@@ -190,7 +236,7 @@ __global__ void __launch_bounds__(256) k_dense_lauum(DenseDev dd) {
   while ((I + 1) * (I + 2) / 2 <= b) ++I;
   while (I * (I + 1) / 2 > b) --I;
   const int J = b - I * (I + 1) / 2;
-  double d[8][2];
+  double d[4][4][2];
   dense_zero(d);
   for (int K = I; K < dd.nb; ++K) {
     dense_load(dd.W, dd.Np, K, I, true, P);  // W_KI as [row i][k]
@@ -199,19 +245,7 @@ __global__ void __launch_bounds__(256) k_dense_lauum(DenseDev dd) {
     dense_mma(P, Q, d);
     __syncthreads();
   }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double* Xa = dd.A + (size_t)I * kDenseTile * dd.Np + (size_t)J * kDenseTile;
-  double* Xb = dd.A + (size_t)J * kDenseTile * dd.Np + (size_t)I * kDenseTile;
-  const int r = 8 * w + (lane >> 2);
-#pragma unroll
-  for (int t = 0; t < 8; ++t)
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const int c = 8 * t + 2 * (lane & 3) + e;
-      if (I == J && r < c) continue;  // a diagonal tile is defined by its lower triangle
-      Xa[(size_t)r * dd.Np + c] = d[t][e];
-      Xb[(size_t)c * dd.Np + r] = d[t][e];
-    }
+  dense_store(d, 1.0, dd.A, dd.Np, I, J, true, I == J);  // a diagonal tile is defined by its lower triangle
 }
 
 // The solve: y_i = sum_j X_ij rhs_j (three components).  One CTA of 1024

@@ -731,14 +731,14 @@ static int dense_build(dfem_scene* sc) {
   sc->dd = DenseDev{N, Np, nb, sc->dn_A.p, sc->dn_W.p, sc->dn_T.p, sc->dn_Linv.p};
   CK(cudaMemsetAsync(sc->dn_A.p, 0, nn * sizeof(double), sc->stream));
   k_dense_scatter<<<sc->hs.F.nsuper, 256, 0, sc->stream>>>(sc->dd, sc->fd, sc->Ldw.p, sc->sn_dofs.p);
-  k_dense_tile_inv<<<nb, 256, kDenseSmem, sc->stream>>>(sc->dd);
+  k_dense_tile_inv<<<nb, kDenseThreads, kDenseSmem, sc->stream>>>(sc->dd);
   int levels = 0;
   for (int w = 1; w < nb; w *= 2, ++levels) {
     const dim3 grid(w * w, (nb + 2 * w - 1) / (2 * w));
-    k_dense_trtri_t<<<grid, 256, kDenseSmem, sc->stream>>>(sc->dd, w);
-    k_dense_trtri_w<<<grid, 256, kDenseSmem, sc->stream>>>(sc->dd, w);
+    k_dense_trtri_t<<<grid, kDenseThreads, kDenseSmem, sc->stream>>>(sc->dd, w);
+    k_dense_trtri_w<<<grid, kDenseThreads, kDenseSmem, sc->stream>>>(sc->dd, w);
   }
-  k_dense_lauum<<<nb * (nb + 1) / 2, 256, kDenseSmem, sc->stream>>>(sc->dd);
+  k_dense_lauum<<<nb * (nb + 1) / 2, kDenseThreads, kDenseSmem, sc->stream>>>(sc->dd);
   sc->launches += 3 + 2 * levels;
   CK(cudaGetLastError());
   sc->dense_built = true;
@@ -1463,7 +1463,7 @@ static void launch_gather(dfem_scene* sc, cudaStream_t st, Gate g, const double*
   if (mixed(sc) && !plain)
     k_gather_force<<<sc->nblk_v, 128, 0, st>>>(sc->sd, g, slot32(sc), sc->qn.p, x, rhs);
   else
-    k_gather<<<sc->nblk_v, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
+    k_gather<<<(sc->hs.N + 3) / 4, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
 }
 
 // The adjoint of the local step runs in FP64 in both forms.  (An FP32 VJP with
@@ -1478,7 +1478,7 @@ static void launch_adj_local(dfem_scene* sc, cudaStream_t st, Gate g, const int*
 }
 
 static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
-  k_adj_gather<<<sc->nblk_v, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
+  k_adj_gather<<<(sc->hs.N + 3) / 4, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
 }
 
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
@@ -1895,7 +1895,7 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
       if (ncons > 0)
         k_cadj_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, ori, xt, sc->act_all.p, sc->step.p,
                                                                   sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p, g);
-      k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
+      k_adj_gather_seq<<<nb, 128, 0, sc->stream>>>(s.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
       if (s.nseg > 0)
         k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, s.M, g, sc->seg_part.p, sc->step.p,
                                                                   sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
@@ -1976,7 +1976,7 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
       if (ncons > 0)
         k_cadj_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, ori, xt, sc->act_all.p, sc->step.p,
                                                                   sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p, kOpen);
-      k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
+      k_adj_gather_seq<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
       if (s.nseg > 0)
         k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, s.M, kOpen, sc->seg_part.p, sc->step.p,
                                                                   sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);
@@ -1995,7 +1995,7 @@ static int contact_adjoint_step(dfem_scene* sc, int st, bool recorded, int rbase
     if (ncons > 0)
       k_cadj_local<<<(ncons + 127) / 128, 128, 0, sc->stream>>>(sc->sd, a, ori, xt, sc->act_all.p, sc->step.p,
                                                                 sc->slot.p, sc->gE.p, sc->gnu.p, sc->mg.p, kOpen);
-    k_adj_gather<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
+    k_adj_gather_seq<<<nb, 128, 0, sc->stream>>>(s.N, kOpen, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, a.orib);
     if (s.nseg > 0)
       k_seg_reduce<<<(s.nseg + 127) / 128, 128, 0, sc->stream>>>(s.nseg, s.M, kOpen, sc->seg_part.p, sc->step.p,
                                                                 sc->seg_ptr.p, sc->seg_mus.p, sc->mg.p, sc->gact.p);

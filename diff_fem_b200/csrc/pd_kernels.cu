@@ -376,27 +376,22 @@ __global__ void k_gather_force(SceneDev d, Gate gate, const float* __restrict__ 
 }
 
 // rhs_i = c0_i + sum of the slots of vertex i
-// acc + slot[k0] + ... + slot[k1 - 1], in that order; eight slots' loads are
-// issued before their sums (the chain of adds no longer waits on each load)
-__device__ __forceinline__ Vec3<double> sum_slots(Vec3<double> acc, const double* __restrict__ slot, int k0, int k1) {
-  int k = k0;
-  for (; k + 8 <= k1; k += 8) {
-    Vec3<double> v[8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u) v[u] = ld3(slot, k + u);
-#pragma unroll
-    for (int u = 0; u < 8; ++u) acc = acc + v[u];
-  }
-  for (; k < k1; ++k) acc = acc + ld3(slot, k);
-  return acc;
+// Sum of a vertex's slots by one warp: lane l adds slots k0 + l, k0 + l + 32,
+// ... in order, then the warp's fixed reduction tree (all lanes get the sum).
+__device__ __forceinline__ Vec3<double> warp_sum_slots(const double* __restrict__ slot, int k0, int k1) {
+  Vec3<double> acc = mk3(0.0, 0.0, 0.0);
+  for (int k = k0 + (int)(threadIdx.x & 31); k < k1; k += 32) acc = acc + ld3(slot, k);
+  return mk3(warp_sum(acc.x), warp_sum(acc.y), warp_sum(acc.z));
 }
 
+// rhs = c0 + J d: one warp per vertex (32 vertices' threads per 1024)
 __global__ void k_gather(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
                              const double* __restrict__ slot,
                          const double* __restrict__ c0, double* __restrict__ rhs) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
-  st3(rhs, i, sum_slots(ld3(c0, i), slot, vslot_ptr[i], vslot_ptr[i + 1]));
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;  // uniform over the warp
+  const Vec3<double> s = warp_sum_slots(slot, vslot_ptr[i], vslot_ptr[i + 1]);
+  if ((threadIdx.x & 31) == 0) st3(rhs, i, ld3(c0, i) + s);
 }
 
 // ----------------------------------------------------------- solves ----
@@ -1310,12 +1305,24 @@ __global__ void __launch_bounds__(128, DFEM_ADJ_MIN_BLOCKS) k_adj_local(SceneDev
 }
 
 // xbar^k = sum of the slots (constraints without x dependence contribute nothing)
+// xbar = the slots' sum, one thread per vertex in slot order: the contact
+// adjoint's kernel form (its cooperative form sums each vertex the same way)
+__global__ void k_adj_gather_seq(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
+                                 const double* __restrict__ slot, double* xkb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
+  Vec3<double> acc = mk3(0.0, 0.0, 0.0);
+  for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
+  st3(xkb, i, acc);
+}
+
 __global__ void k_adj_gather(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
                                  const double* __restrict__ slot,
                              double* xkb) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);  // one warp per vertex
   if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
-  st3(xkb, i, sum_slots(mk3(0.0, 0.0, 0.0), slot, vslot_ptr[i], vslot_ptr[i + 1]));
+  const Vec3<double> s = warp_sum_slots(slot, vslot_ptr[i], vslot_ptr[i + 1]);
+  if ((threadIdx.x & 31) == 0) st3(xkb, i, s);
 }
 
 // activation gradient of the step: sum over the members of each channel
