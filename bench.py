@@ -304,16 +304,23 @@ def run_ours(args):
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     peak_note = "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
     nnz = int(info["nnz_factor"])
-    solve_bytes = 2 * nnz * 8 + 96 * N                       # 2 sweeps x the factor's FP64 values + in/out vectors
+    solve_info = sc.solve_mode()
+    if solve_info["mode"] == "dense":
+        # the dense-inverse form reads the N rows x N_p columns of Hs^-1 (FP64) once; rhs in, y out
+        n_p = -(-N // 64) * 64
+        solve_bytes = N * n_p * 8 + 48 * N
+        solve_note = "per solve (the N x N_p FP64 rows of Hs^-1 once, rhs in, y out; k_dense_solve)"
+    else:
+        solve_bytes = 2 * nnz * 8 + 96 * N                   # 2 sweeps x the factor's FP64 values + in/out vectors
+        solve_note = "per solve (both sweeps)"
     local_bytes = T * (16 + 72 + 16) + N * 72                 # tet tables + x, b, rhs per vertex
     dom = max(share, key=share.get)
     if dom == "solve":
         achieved = solve_bytes / (ph["solve"] * 1e-3) / 1e9
-        traffic_note = "per solve (both sweeps)"
+        traffic_note = solve_note
     else:
         achieved = local_bytes / (ph[dom] * 1e-3) / 1e9
         traffic_note = f"per {dom} launch"
-    solve_info = sc.solve_mode()
     traffic = SOLVE_DRAM_BYTES.get(solve_info["mode"]) if (dom == "solve" and SIM_STEPS == 60) else None
     roofline = {"bound": "hbm", "kernel": dom, "solve_form": solve_info["mode"], "achieved": achieved, "peak": hbm,
                 "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,

@@ -138,11 +138,11 @@ __global__ void k_dense_scatter(DenseDev dd, FactorDev f, const double* __restri
   const double* Lc = f.Lcm + in.lofs;
   const int* R = f.rowidx + in.rofs;
   for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
-    const int i = q % w, c = q / w;
+    const int i = q / w, c = q % w;
     if (i >= c) dd.A[(size_t)(c0 + i) * dd.Np + c0 + c] = Ld[i + c * w];
   }
-  for (int q = threadIdx.x; q < r * w; q += blockDim.x) {
-    const int a = q % r, c = q / r;
+  for (int q = threadIdx.x; q < r * w; q += blockDim.x) {  // consecutive threads: consecutive columns of a row
+    const int a = q / w, c = q % w;
     dd.A[(size_t)R[a] * dd.Np + c0 + c] = Lc[(size_t)c * r + a];
   }
 }
