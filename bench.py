@@ -33,9 +33,10 @@ METRIC = "fwd+adjoint sim steps/s (inverse stiffness 12,800 tets, K=20)"
 
 # DRAM bytes per launch of the global solve on the inverse-stiffness workload,
 # by solve form, from one ncu capture each (dram__bytes_read.sum +
-# dram__bytes_write.sum; the factor is largely L2-resident between solves, so
-# this is below the algorithmic bytes).  Not measured by a bench run.
-SOLVE_DRAM_BYTES = {"persistent": 4.36e6}
+# dram__bytes_write.sum; the persistent form's factor is largely L2-resident
+# between solves, so its figure is below the algorithmic bytes; the dense
+# form reads Hs^-1 from DRAM once per solve).  Not measured by a bench run.
+SOLVE_DRAM_BYTES = {"persistent": 4.36e6, "dense": 88.51e6 + 2.93e6}
 UNIT = "steps/s"
 
 
