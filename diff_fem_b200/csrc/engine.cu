@@ -185,6 +185,8 @@ struct dfem_scene {
   std::vector<double> part_reg_h;
   size_t shm_fact = 0;
   std::vector<size_t> shm_fact_lvl;      // dynamic shared memory of the refactorisation, per level
+  std::vector<int> fact_shares;          // per level: CTAs per supernode of the split form (0: one launch)
+  std::vector<int> fact_w;               // per level: widest supernode
   RefactorDev rd{};
   // batch layout (a single scene is one part)
   std::vector<HostScene> parts;          // the parts of a batch (empty for a single scene)
@@ -678,11 +680,22 @@ static int upload_refactor_plan(dfem_scene* sc) {
   sc->shm_fact = factor_smem_bytes(maxw);
   if (sc->shm_fact > 227 * 1024) return fail(DFEM_ERR_INVALID, "supernode too wide for the GPU refactorisation");
   CK(raise_smem_limit((const void*)k_factor_level, sc->shm_fact));
+  CK(raise_smem_limit((const void*)k_factor_diag, sc->shm_fact));
+  CK(raise_smem_limit((const void*)k_factor_trsm, sc->shm_fact));
+  int nsm = 1;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, sc->device));
   sc->shm_fact_lvl.assign(F.nlevels, 0);
+  sc->fact_shares.assign(F.nlevels, 0);
+  sc->fact_w.assign(F.nlevels, 1);
   for (int l = 0; l < F.nlevels; ++l) {
     int mw = 1;
     for (int k = F.lvl_ptr[l]; k < F.lvl_ptr[l + 1]; ++k) mw = std::max(mw, F.sn_w[F.lvl_sn[k]]);
     sc->shm_fact_lvl[l] = factor_smem_bytes(mw);
+    sc->fact_w[l] = mw;
+    // levels of few supernodes (the top of the tree) leave most SMs idle in
+    // the one-launch form: their updates and rows below spread over CTAs
+    const int cnt = F.lvl_ptr[l + 1] - F.lvl_ptr[l];
+    if (cnt * kFactorSplitRatio <= nsm) sc->fact_shares[l] = std::min(kFactorMaxShares, nsm / cnt);
   }
   sc->rd = RefactorDev{s.T, sc->tvol.p, sc->tE.p, sc->tnu.p, sc->twr.p, sc->twv.p, (int)base.size(),
                        sc->hs_base.p, sc->hc_ptr.p, sc->hc_tet.p, sc->hc_coef.p, sc->hs_val.p, sc->hs_ptr.p,
@@ -765,10 +778,20 @@ static int gpu_refactor(dfem_scene* sc) {
   for (int attempt = 0; attempt < 25; ++attempt) {
     CK(cudaMemcpyAsync(sc->part_reg.p, sc->part_reg_h.data(), sizeof(double) * np, cudaMemcpyHostToDevice, sc->stream));
     CK(cudaMemsetAsync(sc->part_fail.p, 0, sizeof(int) * np, sc->stream));
-    for (int l = 0; l < L; ++l)
-      k_factor_level<<<sc->lvl_ptr[l + 1] - sc->lvl_ptr[l], 256, sc->shm_fact_lvl[l], sc->stream>>>(sc->rd,
-                                                                                                  sc->lvl_ptr[l]);
-    sc->launches += L;
+    for (int l = 0; l < L; ++l) {
+      const int cnt = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l], p0 = sc->lvl_ptr[l], sh = sc->fact_shares[l];
+      if (sh == 0) {
+        k_factor_level<<<cnt, 256, sc->shm_fact_lvl[l], sc->stream>>>(sc->rd, p0);
+        sc->launches += 1;
+        continue;
+      }
+      const size_t w = (size_t)sc->fact_w[l];
+      k_factor_scatter<<<cnt, 256, 0, sc->stream>>>(sc->rd, p0);
+      k_factor_update<<<dim3(cnt, sh), 256, 0, sc->stream>>>(sc->rd, p0);
+      k_factor_diag<<<cnt, 256, 2 * w * w * sizeof(double), sc->stream>>>(sc->rd, p0);
+      k_factor_trsm<<<dim3(cnt, sh), 256, (w * w + kTrsmRows * w) * sizeof(double), sc->stream>>>(sc->rd, p0);
+      sc->launches += 4;
+    }
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(failh.data(), sc->part_fail.p, sizeof(int) * np, cudaMemcpyDeviceToHost, sc->stream));
     CK(cudaStreamSynchronize(sc->stream));

@@ -120,6 +120,11 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                : "d"(a), "d"(b));
 }
 
+// split form of a level: used where supernodes x kFactorSplitRatio <= SMs,
+// with min(kFactorMaxShares, SMs / supernodes) CTAs per supernode
+constexpr int kFactorSplitRatio = 8;
+constexpr int kFactorMaxShares = 16;
+
 constexpr int kRowChunk = 1024;  // rows of a descendant update mapped per pass (shared int buffer)
 constexpr int kTrsmRows = 64;    // rows of the below-diagonal block staged per TRSM pass
 
@@ -129,25 +134,40 @@ __host__ __device__ inline size_t factor_smem_bytes(int w) {
   return sizeof(double) * (2 * (size_t)w * w + (size_t)kTrsmRows * w) + sizeof(int) * kRowChunk;
 }
 
-__global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_begin) {
-  extern __shared__ __align__(16) double fsh[];
-  __shared__ int s_bad;
-  const int s = f.lvl_sn[lvl_begin + blockIdx.x];
-  const int part = f.sn_part ? f.sn_part[s] : 0;
-  const int c0 = f.sn_c0[s], w = f.sn_w[s], r = f.sn_r[s];
-  const int* R = f.rowidx + f.sn_rofs[s];
-  double* Lc = f.Lcm + f.sn_lofs[s];   // r x w, column-major (the panel's rows below)
-  double* Ld = f.Ldw + f.sn_dofs[s];   // w x w, column-major (the panel's diagonal block)
-  double* L = fsh;
-  double* X = fsh + w * w;
-  double* S = X + w * w;
-  int* rowmap = reinterpret_cast<int*>(S + kTrsmRows * w);
-  const double reg = f.part_reg[part];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (threadIdx.x == 0) s_bad = 0;
-  // 1. this supernode's columns of Hs (lower part) into the panel
-  for (int q = threadIdx.x; q < w * w; q += blockDim.x) Ld[q] = 0.0;
-  for (int q = threadIdx.x; q < r * w; q += blockDim.x) Lc[q] = 0.0;
+// The phases of one supernode's factorisation, each run by a whole CTA.  The
+// one-launch form (k_factor_level) runs them all in one CTA; the top levels of
+// the tree, with few supernodes, split them over launches so that the
+// descendant updates and the rows below the diagonal block spread over
+// several CTAs per supernode (k_factor_scatter, k_factor_update,
+// k_factor_diag, k_factor_trsm).  Each entry is computed by the same
+// instructions in the same order either way.
+
+struct FlSn {  // one supernode's layout
+  int s, part, c0, w, r;
+  const int* R;
+  double* Lc;  // r x w, column-major (the panel's rows below)
+  double* Ld;  // w x w, column-major (the panel's diagonal block)
+};
+
+__device__ __forceinline__ FlSn fl_sn(const RefactorDev& f, int s) {
+  FlSn o;
+  o.s = s;
+  o.part = f.sn_part ? f.sn_part[s] : 0;
+  o.c0 = f.sn_c0[s];
+  o.w = f.sn_w[s];
+  o.r = f.sn_r[s];
+  o.R = f.rowidx + f.sn_rofs[s];
+  o.Lc = f.Lcm + f.sn_lofs[s];
+  o.Ld = f.Ldw + f.sn_dofs[s];
+  return o;
+}
+
+// 1. this supernode's columns of Hs (lower part) into the panel
+__device__ __forceinline__ void fl_scatter(const RefactorDev& f, const FlSn& n, int* s_bad) {
+  const double reg = f.part_reg[n.part];
+  const int c0 = n.c0, w = n.w, r = n.r;
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) n.Ld[q] = 0.0;
+  for (int q = threadIdx.x; q < r * w; q += blockDim.x) n.Lc[q] = 0.0;
   __syncthreads();
   for (int c = threadIdx.x; c < w; c += blockDim.x) {
     const int j = c0 + c;
@@ -155,16 +175,24 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
       const int i = f.hs_col[k];
       if (i < j) continue;
       const double v = f.hs_val[k] + (i == j ? reg : 0.0);
-      const int a = sn_local_row(i, c0, w, R, r);
-      if (a < 0) { s_bad = 1; continue; }
-      if (a < w) Ld[a + c * w] = v; else Lc[c * r + (a - w)] = v;
+      const int a = sn_local_row(i, c0, w, n.R, r);
+      if (a < 0) { *s_bad = 1; continue; }
+      if (a < w) n.Ld[a + c * w] = v; else n.Lc[c * r + (a - w)] = v;
     }
   }
   __syncthreads();
-  // 2. left-looking updates, in list order: for descendant d with rows R_d[a0..a1)
-  //    in this supernode's columns, P[R_d[x], R_d[y]] -= sum_k L_d[x,k] L_d[y,k]
-  //    for a0 <= y < a1, y <= x < r_d: 8x8 output tiles on the FP64 tensor cores.
-  for (int u = f.up_ptr[s]; u < f.up_ptr[s + 1]; ++u) {
+}
+
+// 2. left-looking updates, in list order: for descendant d with rows R_d[a0..a1)
+//    in this supernode's columns, P[R_d[x], R_d[y]] -= sum_k L_d[x,k] L_d[y,k]
+//    for a0 <= y < a1, y <= x < r_d: 8x8 output tiles on the FP64 tensor cores.
+//    Only the panel rows (local index: columns first, then R_s) in [lo, hi)
+//    are written; tiles none of whose rows map there are skipped.
+__device__ __forceinline__ void fl_update(const RefactorDev& f, const FlSn& n, int* rowmap, int lo, int hi,
+                                          int* s_bad) {
+  const int c0 = n.c0, w = n.w, r = n.r;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int u = f.up_ptr[n.s]; u < f.up_ptr[n.s + 1]; ++u) {
     const int d = f.up_d[u], a0 = f.up_a0[u], a1 = f.up_a1[u];
     const int wd = f.sn_w[d], rd = f.sn_r[d];
     const int* Rd = f.rowidx + f.sn_rofs[d];
@@ -173,8 +201,8 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
     for (int xc = a0; xc < rd; xc += kRowChunk) {
       const int xe = min(rd, xc + kRowChunk);
       for (int x = xc + (int)threadIdx.x; x < xe; x += blockDim.x) {
-        const int a = sn_local_row(Rd[x], c0, w, R, r);
-        if (a < 0) s_bad = 1;
+        const int a = sn_local_row(Rd[x], c0, w, n.R, r);
+        if (a < 0) *s_bad = 1;
         rowmap[x - xc] = a;
       }
       __syncthreads();
@@ -182,6 +210,10 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
       for (int t = warp; t < nti * ntj; t += nw) {
         const int x0 = xc + 8 * (t / ntj), y0 = a0 + 8 * (t % ntj);
         if (x0 + 7 < y0) continue;  // strictly upper tile
+        if (lo > 0 || hi < w + r) {  // rows map monotonically: the tile's first and last row bound its range
+          const int af = rowmap[x0 - xc], al = rowmap[min(x0 + 7, xe - 1) - xc];
+          if ((al >= 0 && al < lo) || af >= hi) continue;
+        }
         const int xa = x0 + (lane >> 2), yb = y0 + (lane >> 2);
         double d0 = 0.0, d1 = 0.0;
         const bool xin = xa < xe, yin = yb < a1;
@@ -203,18 +235,24 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
           const int yc = y0 + 2 * (lane & 3) + i;
           if (xr < xe && yc < a1 && xr >= yc) {
             const int a = rowmap[xr - xc];
-            if (a < 0) continue;
+            if (a < lo || a >= hi) continue;  // (a < 0 too)
             const int c = Rd[yc] - c0;
             const double v = i == 0 ? d0 : d1;
-            if (a < w) Ld[a + c * w] -= v; else Lc[c * r + (a - w)] -= v;
+            if (a < w) n.Ld[a + c * w] -= v; else n.Lc[c * r + (a - w)] -= v;
           }
         }
       }
       __syncthreads();
     }
   }
-  // 3. dense Cholesky of the diagonal block (right looking)
-  for (int q = threadIdx.x; q < w * w; q += blockDim.x) L[q] = Ld[q];
+}
+
+// 3. dense Cholesky of the diagonal block (right looking) in L (shared), kept
+//    in the workspace Ld; 4. X = L_ss^-1 (one column per thread) into Dinv
+//    (row-major) and DinvC (column-major)
+__device__ __forceinline__ void fl_diag(const RefactorDev& f, const FlSn& n, double* L, double* X, int* s_bad) {
+  const int w = n.w;
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) L[q] = n.Ld[q];
   __syncthreads();
   // (column by column; the scaling and the trailing update of each column are
   // spread over the CTA: every element sees the same operations in the same
@@ -227,7 +265,7 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
     __syncthreads();  // every thread has read the pivot before it is overwritten
     if (threadIdx.x == 0) {
       L[c + c * w] = piv;
-      if (bad) s_bad = 1;
+      if (bad) *s_bad = 1;
     }
     for (int i = c + 1 + (int)threadIdx.x; i < w; i += blockDim.x) L[i + c * w] /= piv;
     __syncthreads();
@@ -242,8 +280,7 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
     __syncthreads();
   }
   // the factored diagonal block stays in the workspace (the dense-inverse form reads it)
-  for (int q = threadIdx.x; q < w * w; q += blockDim.x) Ld[q] = L[q];
-  // 4. X = L_ss^-1 (one column per thread)
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) n.Ld[q] = L[q];
   for (int c = threadIdx.x; c < w; c += blockDim.x) {
     for (int i = 0; i < c; ++i) X[i + c * w] = 0.0;
     for (int i = c; i < w; ++i) {
@@ -253,18 +290,24 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
     }
   }
   __syncthreads();
-  double* Di = f.Dinv + f.sn_dofs[s];  // row-major lower
-  double* DiC = f.DinvC + f.sn_dofs[s];
+  double* Di = f.Dinv + f.sn_dofs[n.s];  // row-major lower
+  double* DiC = f.DinvC + f.sn_dofs[n.s];
   for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
     Di[q] = X[(q / w) + (q % w) * w];
     DiC[q] = X[q];
   }
-  // 5. rows below: L_{R,s} = P_R X^T, kTrsmRows rows at a time (staged, then overwritten)
-  for (int rb = 0; rb < r; rb += kTrsmRows) {
+}
+
+// 5. rows below: L_{R,s} = P_R X^T, kTrsmRows rows at a time (staged in S,
+//    then overwritten), row chunks rb0, rb0 + rbs, ...
+__device__ __forceinline__ void fl_trsm(const FlSn& n, const double* X, double* S, int rb0, int rbs) {
+  const int w = n.w, r = n.r;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int rb = rb0; rb < r; rb += rbs) {
     const int nr = min(kTrsmRows, r - rb);
     for (int q = threadIdx.x; q < nr * w; q += blockDim.x) {
       const int x = q % nr, c = q / nr;  // coalesced along the column-major block
-      S[x * w + c] = Lc[c * r + rb + x];
+      S[x * w + c] = n.Lc[c * r + rb + x];
     }
     __syncthreads();
     const int nti = (nr + 7) / 8, ntj = (w + 7) / 8;
@@ -282,12 +325,75 @@ __global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_beg
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
         const int yc = y0 + 2 * (lane & 3) + i;
-        if (xr < nr && yc < w) Lc[yc * r + rb + xr] = i == 0 ? d0 : d1;
+        if (xr < nr && yc < w) n.Lc[yc * r + rb + xr] = i == 0 ? d0 : d1;
       }
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0 && s_bad) atomicExch(f.part_fail + part, 1);
+}
+
+// The one-launch form: one CTA per supernode of the level (shared memory as
+// factor_smem_bytes).
+__global__ void __launch_bounds__(256) k_factor_level(RefactorDev f, int lvl_begin) {
+  extern __shared__ __align__(16) double fsh[];
+  __shared__ int s_bad;
+  const FlSn n = fl_sn(f, f.lvl_sn[lvl_begin + blockIdx.x]);
+  double* L = fsh;
+  double* X = fsh + n.w * n.w;
+  double* S = X + n.w * n.w;
+  int* rowmap = reinterpret_cast<int*>(S + kTrsmRows * n.w);
+  if (threadIdx.x == 0) s_bad = 0;
+  fl_scatter(f, n, &s_bad);
+  fl_update(f, n, rowmap, 0, n.w + n.r, &s_bad);
+  fl_diag(f, n, L, X, &s_bad);
+  fl_trsm(n, X, S, 0, kTrsmRows);
+  if (threadIdx.x == 0 && s_bad) atomicExch(f.part_fail + n.part, 1);
+}
+
+// The split form of one level (blockIdx.x: the supernode; blockIdx.y: its
+// share of the work, gridDim.y shares).
+__global__ void __launch_bounds__(256) k_factor_scatter(RefactorDev f, int lvl_begin) {
+  __shared__ int s_bad;
+  const FlSn n = fl_sn(f, f.lvl_sn[lvl_begin + blockIdx.x]);
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
+  fl_scatter(f, n, &s_bad);
+  if (threadIdx.x == 0 && s_bad) atomicExch(f.part_fail + n.part, 1);
+}
+
+// the panel rows (local index) of share y: [y ceil((w + r) / shares), ...)
+__global__ void __launch_bounds__(256) k_factor_update(RefactorDev f, int lvl_begin) {
+  __shared__ int s_bad;
+  __shared__ int rowmap[kRowChunk];
+  const FlSn n = fl_sn(f, f.lvl_sn[lvl_begin + blockIdx.x]);
+  const int rows = n.w + n.r, per = (rows + gridDim.y - 1) / gridDim.y;
+  const int lo = blockIdx.y * per, hi = min(rows, lo + per);
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
+  if (lo < hi) fl_update(f, n, rowmap, lo, hi, &s_bad);
+  if (threadIdx.x == 0 && s_bad) atomicExch(f.part_fail + n.part, 1);
+}
+
+__global__ void __launch_bounds__(256) k_factor_diag(RefactorDev f, int lvl_begin) {
+  extern __shared__ __align__(16) double fsh[];
+  __shared__ int s_bad;
+  const FlSn n = fl_sn(f, f.lvl_sn[lvl_begin + blockIdx.x]);
+  if (threadIdx.x == 0) s_bad = 0;
+  fl_diag(f, n, fsh, fsh + n.w * n.w, &s_bad);
+  if (threadIdx.x == 0 && s_bad) atomicExch(f.part_fail + n.part, 1);
+}
+
+// row chunks y, y + shares, ... of the rows below (X read back from DinvC)
+__global__ void __launch_bounds__(256) k_factor_trsm(RefactorDev f, int lvl_begin) {
+  extern __shared__ __align__(16) double fsh[];
+  const FlSn n = fl_sn(f, f.lvl_sn[lvl_begin + blockIdx.x]);
+  if (n.r <= (int)blockIdx.y * kTrsmRows) return;
+  double* X = fsh;
+  double* S = fsh + n.w * n.w;
+  const double* DiC = f.DinvC + f.sn_dofs[n.s];
+  for (int q = threadIdx.x; q < n.w * n.w; q += blockDim.x) X[q] = DiC[q];
+  __syncthreads();
+  fl_trsm(n, X, S, blockIdx.y * kTrsmRows, gridDim.y * kTrsmRows);
 }
 
 }  // namespace dfem
