@@ -32,7 +32,7 @@ __global__ void k_contact_record(const int* step, const int* state, int* rec, Co
   rec[2 * s + 1] = state[CS_BODIES];
   if (c.rec_on && *c.rec_on == 2) {
     const int base = *c.rec_base, comp = state[CS_COMP];
-    const int ok = base + comp <= c.rec_cap ? 1 : 0;
+    const int ok = base + comp <= c.rec_fwd_cap ? 1 : 0;
     int* m = c.rec_meta + 4 * (size_t)s;
     m[0] = base; m[1] = comp; m[2] = state[CS_SRC]; m[3] = ok;
     if (ok) *c.rec_base = base + comp;

@@ -255,6 +255,7 @@ struct dfem_scene {
   bool crec_fwd = false;                 // the last forward recorded
   int crec_used = 0;                     // records the last forward's steps occupy
   int crec_target = 0;                   // records the next forward asks for
+  int crec_reserve = 0;                  // records kept free for the adjoint's replay of one step
   ContactDev cd{};
   std::vector<int> rec_passes;
   // graphs
@@ -2282,12 +2283,14 @@ static int create_on_device(std::unique_ptr<dfem_scene>& sc, int device, dfem_sc
   CK(sc->status.alloc(4));  // before the factor upload, whose kernels report into it
   {
     // device memory the adjoint may fill with stored iterates and contact
-    // records (each saves a replayed step): a quarter of the device, at most
-    // half of what is free when the scene is made (a record store that grows
-    // holds its old and new arrays at once while it copies)
+    // records (each saves a replayed step): 45 % of the device, at most 60 %
+    // of what is free when the scene is made.  The forward leaves room in the
+    // record store for one replayed step, so the adjoint rarely grows it (a
+    // growing store holds its old and new arrays at once; when that does not
+    // fit, the adjoint drops the forward's records and replays every step).
     size_t free_b = 0, total_b = 0;
     CK(cudaMemGetInfo(&free_b, &total_b));
-    sc->adj_budget = std::min(total_b / 4, free_b / 2);
+    sc->adj_budget = std::min(total_b / 100 * 45, free_b / 100 * 60);
   }
   RC(upload_scene(sc.get()));
   RC(ensure_steps(sc.get(), 1));
@@ -2505,17 +2508,27 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
     rec_budget = sc->hist_step != 0 && sc->adj_budget > hist_bytes
                      ? (sc->adj_budget - hist_bytes) / contact_record_bytes(sc) : 0;
     rec_budget = std::min<size_t>(rec_budget, INT32_MAX / 2);
-    const int want = (int)std::min<size_t>(rec_budget, sc->crec_target > 0 ? (size_t)sc->crec_target
-                                                                             : 4 * (size_t)n_steps);
+    // the store: the forward's records plus room for the adjoint's replay of
+    // one step (the most loop-body executions of a step in the last forward)
+    const size_t tgt = sc->crec_target > 0 ? (size_t)sc->crec_target : 4 * (size_t)n_steps;
+    const int total = (int)std::min<size_t>(rec_budget, tgt + (size_t)sc->crec_reserve);
+    const int want = std::max(0, total - sc->crec_reserve);
     fwd_rec = want >= 1 && !sc->self_contact;  // soft-soft contact has no adjoint to record for
     if (fwd_rec) {
-      const int rc = ensure_contact_record(sc, want);
+      const int rc = ensure_contact_record(sc, total);
       if (rc == DFEM_ERR_NOMEM) {  // no room to record: the adjoint replays the contact steps
         cudaGetLastError();
         g_last_error.clear();
         fwd_rec = false;
       } else {
         RC(rc);
+      }
+    }
+    if (fwd_rec) {  // the forward's share of the store (the graphs hold it: rebuilt when it changes)
+      const int fwd_cap = std::max(want, (int)std::min<size_t>((size_t)sc->crec_cap, rec_budget) - sc->crec_reserve);
+      if (sc->cd.rec_fwd_cap != fwd_cap) {
+        sc->cd.rec_fwd_cap = fwd_cap;
+        invalidate_graphs(sc);
       }
     }
     const int on = fwd_rec ? 2 : 0;
@@ -2562,6 +2575,11 @@ int dfem_step_forward(dfem_scene* sc, const double* x, const double* v, const do
     size_t need = 0;
     for (int st = 0; st < n_steps; ++st) need += (size_t)sc->crec_meta_h[4 * (size_t)st + 1];
     sc->crec_target = (int)std::min(rec_budget, std::max<size_t>(need + need / 8 + 16, (size_t)sc->crec_target));
+  }
+  if (sc->has_contact) {  // room the next forward leaves for one replayed step
+    int most = 0;
+    for (int st = 0; st < n_steps; ++st) most = std::max(most, sc->rec_passes[2 * (size_t)st + 1]);
+    sc->crec_reserve = std::max(sc->crec_reserve, most + 1);
   }
   sc->launches += 7;
   for (int st = 0; st < n_steps; ++st)

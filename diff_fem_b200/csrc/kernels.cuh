@@ -176,6 +176,7 @@ struct ContactDev {
   // steps in a row (a step that does not fit is marked unrecorded and replayed)
   const int* rec_on;
   int rec_cap;            // computed iterations the record holds
+  int rec_fwd_cap;        // of which the forward may fill (the rest: room for the adjoint's replays)
   double* rec_x;          // rec_cap x 3N: each computed iteration's input ori_x
   double* rec_prev;       // rec_cap x 3N: its relaxed rhs after the update
   int* rec_first;         // rec_cap: whether it began its pass
