@@ -1064,7 +1064,7 @@ static int upload_scene(dfem_scene* sc) {
                         kBroadDefaultCells, {0, 0, 0}, {0.0, 0.0, 0.0}, 0.0, nullptr, nullptr,
                         s.alpha, s.mu_obs, sc->cverts.p, sc->cidx.p, sc->obs_x.p,
                         sc->obs_f.p, sc->hdiag.p, sc->imp_cnt.p, sc->imp_face.p, sc->imp_n.p, sc->xn1.p, sc->xold.p,
-                        sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p, sc->crec_on.p, 0, nullptr, nullptr,
+                        sc->cprev.p, sc->lxt.p, sc->vwc.p, sc->cstate.p, sc->crec_on.p, 0, 0, nullptr, nullptr,
                         nullptr, nullptr, nullptr, sc->status.p, sc->crec_base.p, nullptr};
     if (s.nparts > 1) {  // a batch: per-part contact state, no broad phase
       const int np = s.nparts;
