@@ -40,6 +40,18 @@ SOLVE_DRAM_BYTES = {"persistent": 4.36e6, "dense": 88.51e6 + 2.93e6}
 UNIT = "steps/s"
 
 
+def pin_triangular(sc) -> bool:
+    """Put a scene on the fastest of its supernodal triangular-solve forms (the
+    plain form) when the autotune chose the dense inverse; True if it did."""
+    info = sc.solve_mode()
+    if info["mode"] != "dense":
+        return False
+    tri = {"levels": info["ms_levels"], "persistent": info["ms_persistent"], "split": info["ms_split"],
+           "cluster": info["ms_cluster"], "resident": info["ms_resident"]}
+    sc.solve_mode(min((v, k) for k, v in tri.items() if v > 0)[1])
+    return True
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -471,7 +483,10 @@ def north_star_extras(args, local: int) -> dict:
         order = np.argsort([d.n_tets for d in dd], kind="stable")
         sample = order[np.linspace(0, len(dd) - 1, min(16, len(dd))).astype(int)]
         vo, so = out["fp64"]["offsets"]["vertices"], out["fp64"]["offsets"]["segments"]
-        tsum = 0.0
+        # the plain form is the supernodal triangular solve (the fastest of its
+        # forms per scene); the dense-inverse form small single scenes may
+        # take instead is timed beside it
+        tsum, tsum_auto, n_dense = 0.0, 0.0, 0
         for q in sample:
             sc = Scene(dd[q], device=local)
             xq = xb[3 * vo[q]:3 * vo[q + 1]].contiguous()
@@ -482,9 +497,14 @@ def north_star_extras(args, local: int) -> dict:
                 return sc.backward(2.0 * (x - xq), torch.zeros_like(x))
 
             t, _ = timed(one, 1)
+            tsum_auto += t
+            if pin_triangular(sc):
+                n_dense += 1
+                t, _ = timed(one, 1)
             tsum += t
             sc.close()
         plain = len(sample) * nb / tsum
+        plain_auto = len(sample) * nb / tsum_auto
         # errors of the mixed batch against the FP64 batch, per scene
         to = out["fp64"]["offsets"]["tets"]
         same = np.all(out["mixed"]["iters"] == out["fp64"]["iters"], axis=0)
@@ -500,7 +520,12 @@ def north_star_extras(args, local: int) -> dict:
             "mixed_batched": {"value": out["mixed"]["value"], "unit": "scene-steps/s", "setup_s": out["mixed"]["setup_s"]},
             "fp64_batched": {"value": out["fp64"]["value"], "unit": "scene-steps/s", "setup_s": out["fp64"]["setup_s"]},
             "fp64_one_at_a_time": {"value": plain, "unit": "scene-steps/s", "scenes_sampled": int(len(sample)),
-                                   "sample": "16 scenes evenly spaced in size order, one handle each"},
+                                   "sample": "16 scenes evenly spaced in size order, one handle each",
+                                   "solve": "supernodal triangular solve (fastest of its forms per scene)"},
+            "fp64_one_at_a_time_any_form": {"value": plain_auto, "unit": "scene-steps/s",
+                                            "scenes_with_dense_inverse": n_dense,
+                                            "solve": "the autotuned form, the dense inverse included"},
+            "mixed_batched_over_fp64_one_at_a_time_any_form": out["mixed"]["value"] / plain_auto,
             "mixed_batched_over_fp64_one_at_a_time": out["mixed"]["value"] / plain,
             "fp64_batched_over_fp64_one_at_a_time": out["fp64"]["value"] / plain,
             "mixed_over_fp64_batched": out["mixed"]["value"] / out["fp64"]["value"],
@@ -700,6 +725,7 @@ def run_batch(args):
         vo, so = b.offsets["vertices"], b.offsets["segments"]
         for q in idx:
             sc = Scene(d64[q], device=local)
+            pin_triangular(sc)
             xq = x0[3 * vo[q]:3 * vo[q + 1]].contiguous()
             aq = act[:, so[q]:so[q + 1]].contiguous() if so[q + 1] > so[q] else None
             xs, _ = sc.forward(xq, torch.zeros_like(xq), n_steps=n, act=aq)  # warm-up (graph build)
@@ -717,7 +743,8 @@ def run_batch(args):
         rate = len(idx) * n / tsum
         plain = {"value": rate, "unit": "scene-steps/s", "scenes": int(len(idx)), "mean_tets": tets / len(idx),
                  "batch_mean_tets": b.T / b.nparts, "ratio_batch_over_plain": value / world / rate,
-                 "form": "plain FP64 engine, one scene per handle, forward + adjoint, CUDA-event timed"}
+                 "form": "plain FP64 engine (supernodal triangular solve), one scene per handle, forward + "
+                         "adjoint, CUDA-event timed"}
 
     # roofline of the dominant phase (the global solve, both sweeps), CUDA events on the engine's stream
     peaks = {}
