@@ -444,7 +444,7 @@ def north_star_extras(args, local: int) -> dict:
             g = sc.backward(2.0 * (x - tg), torch.zeros_like(x))
             return x, g["E"]
 
-        t, (x, gE) = timed(grad_eval, 3)
+        t, (x, gE) = timed(grad_eval, 10)
         c2[name] = {"value": n / t, "unit": "steps/s", "solve": sc.solve_mode()["mode"],
                     "pos_rel_err_vs_oracle": _rel(x.cpu().numpy(), ro["x"]),
                     "grad_E_rel_err_vs_oracle": _rel(gE.cpu().numpy(), bo["E"])}
