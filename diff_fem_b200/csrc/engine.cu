@@ -228,6 +228,7 @@ struct dfem_scene {
   // as the conditional loop of kernels
   bool fused_ok = false;                 // scene has obstacle contact only and the device runs the launch
   bool fused_on = true;                  // dfem_set_option(DFEM_OPTION_FUSED_CONTACT)
+  bool split_factor = true;              // dfem_set_option(DFEM_OPTION_SPLIT_FACTOR)
   int fused_grid = 0;                    // CTAs of k_contact_fused (all resident)
   int cadj_grid = 0;                     // CTAs of k_cadj_fused (all resident)
   DBuf<double> fpartial;
@@ -780,7 +781,8 @@ static int gpu_refactor(dfem_scene* sc) {
     CK(cudaMemcpyAsync(sc->part_reg.p, sc->part_reg_h.data(), sizeof(double) * np, cudaMemcpyHostToDevice, sc->stream));
     CK(cudaMemsetAsync(sc->part_fail.p, 0, sizeof(int) * np, sc->stream));
     for (int l = 0; l < L; ++l) {
-      const int cnt = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l], p0 = sc->lvl_ptr[l], sh = sc->fact_shares[l];
+      const int cnt = sc->lvl_ptr[l + 1] - sc->lvl_ptr[l], p0 = sc->lvl_ptr[l];
+      const int sh = sc->split_factor ? sc->fact_shares[l] : 0;
       if (sh == 0) {
         k_factor_level<<<cnt, 256, sc->shm_fact_lvl[l], sc->stream>>>(sc->rd, p0);
         sc->launches += 1;
@@ -3039,6 +3041,10 @@ int dfem_set_option(dfem_scene* sc, int32_t which, int64_t value) {
       if (value == 1 && sc->cnp > 0 && !sc->fused_ok)
         return fail(DFEM_ERR_UNSUPPORTED, "the device cannot run the batch's cooperative contact phase");
       sc->fused_on = value != 0;
+      break;
+    case DFEM_OPTION_SPLIT_FACTOR:
+      if (value != 0 && value != 1) return fail(DFEM_ERR_INVALID, "value must be 0 or 1");
+      sc->split_factor = value != 0;
       break;
     default:
       return fail(DFEM_ERR_INVALID, "unknown option");

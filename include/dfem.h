@@ -413,8 +413,13 @@ int dfem_set_limit(dfem_scene *scene, int32_t which, int64_t value);
  *                              barriers between its detection and Jacobi phases;
  *                              0 (default for batches): as a conditional graph
  *                              loop of kernels (batches: gated per scene).
+ *   DFEM_OPTION_SPLIT_FACTOR   1 (default): the refactorisation runs the levels
+ *                              of few supernodes split over launches (several
+ *                              CTAs per supernode); 0: one CTA per supernode
+ *                              everywhere.  Applies from the next
+ *                              refactorisation (dfem_set_materials).
  * No counterpart in the reference. */
-enum dfem_option { DFEM_OPTION_FUSED_CONTACT = 0 };
+enum dfem_option { DFEM_OPTION_FUSED_CONTACT = 0, DFEM_OPTION_SPLIT_FACTOR = 1 };
 int dfem_set_option(dfem_scene *scene, int32_t which, int64_t value);
 
 /* Failure injection for tests: the calling thread's device allocations by the

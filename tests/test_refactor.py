@@ -64,3 +64,24 @@ def test_regularisation_retry_is_per_part():
     assert s0.info()["factor_regularisation"] == 0.0
     s0.close()
     b.close()
+
+
+def test_split_refactorisation_levels_match_one_launch():
+    """The top levels of the tree (few supernodes) refactor split over four
+    launches with several CTAs per supernode; every factor entry sees the same
+    operations as in the one-CTA-per-supernode kernel: forward and adjoint
+    agree bit for bit with the split switched off."""
+    d = S.inverse_stiffness()
+    out = []
+    for split in (1, 0):
+        g = Scene(d)
+        g.solve_mode("persistent")
+        g.set_option("split_factor", split)
+        g.set_materials(np.asarray(d.youngs), np.asarray(d.poisson))
+        x = d.x0.reshape(-1).copy()
+        xo, vo = g.forward(x, np.zeros_like(x), n_steps=3)
+        gr = g.backward(np.ones_like(x), np.zeros_like(x))
+        out.append((xo, vo, gr["x"], gr["E"]))
+        g.close()
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
