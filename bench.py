@@ -66,7 +66,7 @@ def parse():
                         "star: the muscle star on the ground, gradient w.r.t. all activations; "
                         "cloth_ball: a 64x64 cloth dropped on a ball, gradient w.r.t. the initial velocities")
     p.add_argument("--scenes", type=int, default=256, help="batch workload: number of scenes")
-    p.add_argument("--no-north-star", action="store_true",
+    p.add_argument("--no-comparison", action="store_true",
                    help="skip the mixed/FP64 and batched/one-at-a-time comparison of the default line")
     p.add_argument("--fp64-sample", type=int, default=-1,
                    help="batch workload: scenes stepped one at a time in FP64 for the plain-form rate "
@@ -359,25 +359,25 @@ def run_ours(args):
         except Exception as ex:  # the baseline must not kill the GPU line
             line["cpu_baseline"] = {"value": None, "error": str(ex)}
     sc.close()
-    if rank == 0 and world == 1 and not args.no_north_star:
+    if rank == 0 and world == 1 and not args.no_comparison:
         try:
-            line["north_star"] = north_star_extras(args, local)
+            line["comparison"] = comparison_extras(args, local)
         except Exception as ex:  # the comparison must not kill the GPU line
-            line["north_star"] = {"error": f"{type(ex).__name__}: {ex}"}
+            line["comparison"] = {"error": f"{type(ex).__name__}: {ex}"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
-# ------------------------------------------------------------ north star ---
+# ------------------------------------------------------------ comparison ---
 
 def _rel(a, b) -> float:
     a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-def north_star_extras(args, local: int) -> dict:
+def comparison_extras(args, local: int) -> dict:
     """The comparison the metric names: mixed FP32/FP64 against plain FP64,
     batched against one scene at a time, each with its error.
     (1) The 12,800-tet inverse-stiffness problem in both precisions, each
