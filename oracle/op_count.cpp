@@ -12,7 +12,7 @@
 // build's (one-sided Jacobi on the columns of F, which the oracle restates too).
 // Counted: add/sub, mul, div, sqrt/rsqrt, comparisons; a fused multiply-add
 // counts as one mul and one add.  The count depends on F through the number
-// of Jacobi sweeps; the driver (op_count.py) averages it over a scene's tets.
+// of Jacobi sweeps; its caller (op_count.py) averages it over a scene's tets.
 #include <cmath>
 #include <cstdint>
 
