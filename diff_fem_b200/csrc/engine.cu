@@ -2406,14 +2406,15 @@ int dfem_set_materials(dfem_scene* sc, const double* youngs, const double* poiss
   RC(gpu_refactor(sc));
   if (sc->has_contact)
     k_hs_diag<<<sc->nblk_v, 128, 0, sc->stream>>>(s.N, sc->hs_ptr.p, sc->hs_col.p, sc->hs_val.p, sc->hdiag.p);
-  // host copies of the moduli follow (the host factor is used after creation
-  // only by the skeleton's Schur blocks, refactored here for them)
-  if (T > 0) {
-    CK(cudaMemcpyAsync(s.tE.data(), sc->tE.p, T * sizeof(double), cudaMemcpyDeviceToHost, sc->stream));
-    CK(cudaMemcpyAsync(s.tnu.data(), sc->tnu.p, T * sizeof(double), cudaMemcpyDeviceToHost, sc->stream));
-  }
-  CK(cudaStreamSynchronize(sc->stream));
+  // the host factor is used after creation only by the skeleton's Schur
+  // blocks: with links, the host copies of the moduli follow and it is
+  // refactored for them (without, the call returns with the device work queued)
   if (sc->skel_on) {
+    if (T > 0) {
+      CK(cudaMemcpyAsync(s.tE.data(), sc->tE.p, T * sizeof(double), cudaMemcpyDeviceToHost, sc->stream));
+      CK(cudaMemcpyAsync(s.tnu.data(), sc->tnu.p, T * sizeof(double), cudaMemcpyDeviceToHost, sc->stream));
+    }
+    CK(cudaStreamSynchronize(sc->stream));
     std::string err;
     const std::vector<double> E(s.tE), nu(s.tnu);
     if (!update_materials(s, E.data(), nu.data(), err)) return fail(DFEM_ERR_FACTOR, err);
