@@ -303,9 +303,9 @@ def run_ours(args):
     sc.forward(x0, v0, n_steps=1)
     ph = sc.profile_phases(reps=50)
     n_it = int(iters.sum())
-    # the adjoint replays no step when every step's iterates fit the default adjoint budget (a quarter of
+    # the adjoint replays no step when every step's iterates fit the default adjoint budget (45 % of
     # the device memory): then one forward and one adjoint solve per PD iteration, else also a replay
-    stored = 3 * N * 8 * (d.max_iterations + 1) * SIM_STEPS <= torch.cuda.get_device_properties(dev).total_memory // 4
+    stored = 3 * N * 8 * (d.max_iterations + 1) * SIM_STEPS <= torch.cuda.get_device_properties(dev).total_memory * 45 // 100
     runs = 1 if stored else 2
     share = {"local": runs * n_it * ph["local"], "solve": (runs + 1) * n_it * ph["solve"],
              "adj_local": n_it * ph["adj_local"], "gather": (runs + 1) * n_it * ph["gather"]}

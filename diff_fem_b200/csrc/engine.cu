@@ -206,7 +206,7 @@ struct dfem_scene {
   // (the adjoint then replays no step without contact), else of one step
   // (every step is recomputed from its checkpoint)
   long long hist_step = 0;
-  size_t adj_budget = 0;  // set at creation: a quarter of the device memory, at most half of the free memory
+  size_t adj_budget = 0;  // set at creation: 45 % of the device memory, at most 60 % of the free memory
   // articulated skeleton (links whose vertices move rigidly)
   bool skel_on = false;
   int sk_nq = 0;                         // joint-state length 12 + L - 1

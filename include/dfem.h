@@ -356,7 +356,7 @@ int dfem_profile_levels(dfem_scene *scene, int32_t reps, int32_t cap, int32_t *n
                         double *ms_bwd, int32_t *n_supernodes, int32_t *level, int32_t *threads);
 
 /* Device memory (bytes) the adjoint may spend on storing the PD iterates of
- * every step of a forward call (default: a quarter of the device's memory, at most half of the
+ * every step of a forward call (default: 45 % of the device's memory, at most 60 % of the
  * memory free when the scene is made).  Within it the adjoint
  * replays no step (except steps with contact, whose contact iterations it
  * records on a replay); beyond it every step is recomputed from its
