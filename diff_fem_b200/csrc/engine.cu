@@ -229,6 +229,7 @@ struct dfem_scene {
   bool fused_ok = false;                 // scene has obstacle contact only and the device runs the launch
   bool fused_on = true;                  // dfem_set_option(DFEM_OPTION_FUSED_CONTACT)
   bool split_factor = true;              // dfem_set_option(DFEM_OPTION_SPLIT_FACTOR)
+  int gather_form = 0;                   // dfem_set_option(DFEM_OPTION_GATHER): 0 by size, 1 warp, 2 thread
   int fused_grid = 0;                    // CTAs of k_contact_fused (all resident)
   int cadj_grid = 0;                     // CTAs of k_cadj_fused (all resident)
   DBuf<double> fpartial;
@@ -1484,10 +1485,18 @@ static void launch_local(dfem_scene* sc, cudaStream_t st, Gate g, const double* 
 }
 
 // rhs of one PD iteration at the iterate x (mixed: also reads q_n and x)
+// the slot sums one thread per vertex (large scenes) or one warp per vertex
+// (small ones, latency-bound); the sums are the same bit for bit
+static bool gather_threads(const dfem_scene* sc) {
+  return sc->gather_form == 2 || (sc->gather_form == 0 && sc->hs.N >= kGatherThreadMin);
+}
+
 static void launch_gather(dfem_scene* sc, cudaStream_t st, Gate g, const double* c0, double* rhs, const double* x,
                           bool plain = false) {
   if (mixed(sc) && !plain)
     k_gather_force<<<sc->nblk_v, 128, 0, st>>>(sc->sd, g, slot32(sc), sc->qn.p, x, rhs);
+  else if (gather_threads(sc))
+    k_gather_t<<<sc->nblk_v, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
   else
     k_gather<<<(sc->hs.N + 3) / 4, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, c0, rhs);
 }
@@ -1504,7 +1513,10 @@ static void launch_adj_local(dfem_scene* sc, cudaStream_t st, Gate g, const int*
 }
 
 static void launch_adj_gather(dfem_scene* sc, cudaStream_t st, Gate g) {
-  k_adj_gather<<<(sc->hs.N + 3) / 4, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
+  if (gather_threads(sc))
+    k_adj_gather_t<<<sc->nblk_v, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
+  else
+    k_adj_gather<<<(sc->hs.N + 3) / 4, 128, 0, st>>>(sc->hs.N, g, sc->vpart.p, sc->vslot_ptr.p, sc->slot.p, sc->xkb.p);
 }
 
 static void step_pre(dfem_scene* sc, cudaStream_t st, cudaGraphConditionalHandle h) {
@@ -3042,6 +3054,10 @@ int dfem_set_option(dfem_scene* sc, int32_t which, int64_t value) {
       if (value == 1 && sc->cnp > 0 && !sc->fused_ok)
         return fail(DFEM_ERR_UNSUPPORTED, "the device cannot run the batch's cooperative contact phase");
       sc->fused_on = value != 0;
+      break;
+    case DFEM_OPTION_GATHER:
+      if (value < 0 || value > 2) return fail(DFEM_ERR_INVALID, "value must be 0, 1 or 2");
+      sc->gather_form = (int)value;
       break;
     case DFEM_OPTION_SPLIT_FACTOR:
       if (value != 0 && value != 1) return fail(DFEM_ERR_INVALID, "value must be 0 or 1");

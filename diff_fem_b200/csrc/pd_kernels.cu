@@ -384,6 +384,44 @@ __device__ __forceinline__ Vec3<double> warp_sum_slots(const double* __restrict_
   return mk3(warp_sum(acc.x), warp_sum(acc.y), warp_sum(acc.z));
 }
 
+// The same sum by one thread, bit for bit: the lanes' partial sums (lane l:
+// +0 + slot k0 + l + slot k0 + l + 32 + ...) combined by the warp's reduction
+// tree, which is pairwise summation over the lanes in bit-reversed order
+// (floating-point addition is commutative, so only the tree's shape matters).
+__device__ __forceinline__ Vec3<double> thread_sum_slots(const double* __restrict__ slot, int k0, int k1) {
+  Vec3<double> stk[5];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {  // unrolled: every index into stk is a constant
+    const int l = (int)(__brev((unsigned)j) >> 27);
+    Vec3<double> x = mk3(0.0, 0.0, 0.0);
+    for (int k = k0 + l; k < k1; k += 32) x = x + ld3(slot, k);
+    int b = 0;
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+      if (b == q && ((j >> q) & 1)) {
+        x = stk[q] + x;
+        b = q + 1;
+      }
+    if (j == 31) return x;  // the whole tree
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+      if (q == b) stk[q] = x;
+  }
+  return stk[0];  // not reached
+}
+
+// the slot sums' form: one warp per vertex below this many vertices (latency),
+// one thread per vertex from it on (the same sums, bit for bit)
+constexpr int kGatherThreadMin = 65536;
+
+// rhs = c0 + J d, one thread per vertex
+__global__ void k_gather_t(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
+                           const double* __restrict__ slot, const double* __restrict__ c0, double* __restrict__ rhs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
+  st3(rhs, i, ld3(c0, i) + thread_sum_slots(slot, vslot_ptr[i], vslot_ptr[i + 1]));
+}
+
 // rhs = c0 + J d: one warp per vertex (32 vertices' threads per 1024)
 __global__ void k_gather(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
                              const double* __restrict__ slot,
@@ -1314,6 +1352,14 @@ __global__ void k_adj_gather_seq(int N, Gate gate, const int* __restrict__ vpart
   Vec3<double> acc = mk3(0.0, 0.0, 0.0);
   for (int k = vslot_ptr[i]; k < vslot_ptr[i + 1]; ++k) acc = acc + ld3(slot, k);
   st3(xkb, i, acc);
+}
+
+// xbar = the slots' sum, one thread per vertex (k_adj_gather's sums)
+__global__ void k_adj_gather_t(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,
+                               const double* __restrict__ slot, double* xkb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N || gate.skip(vpart ? vpart[i] : 0)) return;
+  st3(xkb, i, thread_sum_slots(slot, vslot_ptr[i], vslot_ptr[i + 1]));
 }
 
 __global__ void k_adj_gather(int N, Gate gate, const int* __restrict__ vpart, const int* __restrict__ vslot_ptr,

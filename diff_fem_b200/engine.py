@@ -284,7 +284,7 @@ class Scene:
         DFEM_ERR_CAP.  See dfem_set_limit."""
         check(lib().dfem_set_limit(self._h, self.LIMITS[which], int(value)))
 
-    OPTIONS = {"fused_contact": 0, "split_factor": 1}
+    OPTIONS = {"fused_contact": 0, "split_factor": 1, "gather": 2}
 
     def set_option(self, which: str, value: int):
         """An execution option (results are identical either way); see dfem_set_option."""

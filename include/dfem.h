@@ -418,8 +418,12 @@ int dfem_set_limit(dfem_scene *scene, int32_t which, int64_t value);
  *                              CTAs per supernode); 0: one CTA per supernode
  *                              everywhere.  Applies from the next
  *                              refactorisation (dfem_set_materials).
+ *   DFEM_OPTION_GATHER         0 (default): the per-vertex sums of the local
+ *                              step's slots one warp per vertex below 65,536
+ *                              vertices, one thread per vertex from there; 1:
+ *                              one warp per vertex; 2: one thread per vertex.
  * No counterpart in the reference. */
-enum dfem_option { DFEM_OPTION_FUSED_CONTACT = 0, DFEM_OPTION_SPLIT_FACTOR = 1 };
+enum dfem_option { DFEM_OPTION_FUSED_CONTACT = 0, DFEM_OPTION_SPLIT_FACTOR = 1, DFEM_OPTION_GATHER = 2 };
 int dfem_set_option(dfem_scene *scene, int32_t which, int64_t value);
 
 /* Failure injection for tests: the calling thread's device allocations by the

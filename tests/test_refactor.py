@@ -85,3 +85,24 @@ def test_split_refactorisation_levels_match_one_launch():
         g.close()
     for a, b in zip(*out):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("builder", ["inverse_stiffness", "muscle_beam"])
+def test_thread_and_warp_gathers_agree_bit_for_bit(builder):
+    """The per-vertex sums of the local step's slots: one warp per vertex
+    (small scenes) or one thread per vertex emulating the warp's lanes and
+    reduction tree (large scenes); forced either way, forward and adjoint
+    agree bit for bit."""
+    d = {"inverse_stiffness": S.inverse_stiffness, "muscle_beam": S.muscle_beam}[builder]()
+    act = np.random.default_rng(3).uniform(0, 1, (3, d.n_segments)) if d.n_segments else None
+    out = []
+    for form in (1, 2):
+        g = Scene(d)
+        g.set_option("gather", form)
+        x = d.x0.reshape(-1).copy()
+        xo, vo = g.forward(x, 0.01 * np.ones_like(x), n_steps=3, act=act)
+        gr = g.backward(np.ones_like(x), np.zeros_like(x))
+        out.append([xo, vo] + [gr[k] for k in ("x", "v", "E", "nu", "act")])
+        g.close()
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
