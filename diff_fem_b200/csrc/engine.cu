@@ -729,7 +729,7 @@ static void dense_release(dfem_scene* sc) {
 static int dense_build(dfem_scene* sc) {
   const int N = sc->hs.N, nb = (N + kDenseTile - 1) / kDenseTile, Np = nb * kDenseTile;
   const size_t nn = (size_t)Np * Np;
-  if (!sc->dn_A.p || sc->dn_A.n != nn) {
+  if (!sc->dn_A.p || !sc->dn_W.p || !sc->dn_T.p || !sc->dn_Linv.p || sc->dn_A.n != nn) {
     CK(raise_smem_limit((const void*)k_dense_tile_inv, kDenseSmem));
     CK(raise_smem_limit((const void*)k_dense_trtri_t, kDenseSmem));
     CK(raise_smem_limit((const void*)k_dense_trtri_w, kDenseSmem));
@@ -739,10 +739,15 @@ static int dense_build(dfem_scene* sc) {
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, sc->device));
     sc->dense_grid = std::max(1, std::min(nsm, N));
     sc->dense_built = false;
-    CK(sc->dn_A.alloc(nn));
-    CK(sc->dn_W.alloc(nn));
-    CK(sc->dn_T.alloc(nn));
-    CK(sc->dn_Linv.alloc((size_t)nb * kDenseTile * kDenseTile));
+    // all four or none: a failed allocation leaves no buffers behind
+    cudaError_t e = sc->dn_A.alloc(nn);
+    if (e == cudaSuccess) e = sc->dn_W.alloc(nn);
+    if (e == cudaSuccess) e = sc->dn_T.alloc(nn);
+    if (e == cudaSuccess) e = sc->dn_Linv.alloc((size_t)nb * kDenseTile * kDenseTile);
+    if (e != cudaSuccess) {
+      dense_release(sc);
+      CK(e);
+    }
   }
   sc->dd = DenseDev{N, Np, nb, sc->dn_A.p, sc->dn_W.p, sc->dn_T.p, sc->dn_Linv.p};
   CK(cudaMemsetAsync(sc->dn_A.p, 0, nn * sizeof(double), sc->stream));
