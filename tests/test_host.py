@@ -126,3 +126,50 @@ def test_obj_writer_writes_the_reference_format(tmp_path):
     w.close()
     with pytest.raises(_capi.DfemError):
         ObjWriter([(2, np.array([[0, 1, 2]]), "_a.obj")])  # face vertex out of range
+
+
+def _warp_tree(slots):
+    """The warp form of a vertex's slot sum: lane l adds slots l, l + 32, ...
+    from +0, then the xor butterfly (offsets 16, 8, 4, 2, 1)."""
+    v = [0.0] * 32
+    for l in range(32):
+        for k in range(l, len(slots), 32):
+            v[l] = v[l] + slots[k]
+    for o in (16, 8, 4, 2, 1):
+        v = [v[l] + v[l ^ o] for l in range(32)]
+    return v
+
+
+def _thread_tree(slots):
+    """The thread form: the same lane partials, pairwise-summed over the
+    lanes in bit-reversed order with a five-entry stack."""
+    stk = [None] * 5
+    for j in range(32):
+        lane = int(f"{j:05b}"[::-1], 2)
+        x = 0.0
+        for k in range(lane, len(slots), 32):
+            x = x + slots[k]
+        b = 0
+        while b < 5 and (j >> b) & 1:
+            x = stk[b] + x
+            b += 1
+        if j == 31:
+            return x
+        stk[b] = x
+
+
+def test_thread_gather_reproduces_the_warp_reduction_bit_for_bit():
+    """k_gather_t / k_adj_gather_t emulate k_gather / k_adj_gather: every lane
+    of the butterfly ends with the same sum, and the thread's pairwise tree
+    over bit-reversed lanes is that sum, bit for bit (signed zeros included)."""
+    import struct
+    rng = np.random.default_rng(11)
+    bits = lambda a: struct.pack("<d", a)
+    for n in list(range(0, 70)) + [95, 96, 97, 130]:
+        for scale in (1.0, 1e-300, 1e300):
+            slots = list(rng.standard_normal(n) * scale * 10.0 ** rng.integers(-8, 8, n))
+            if n > 3:
+                slots[1], slots[2] = -0.0, 0.0
+            w = _warp_tree(slots)
+            assert len({bits(a) for a in w}) == 1
+            assert bits(_thread_tree(slots)) == bits(w[0]), n
